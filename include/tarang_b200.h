@@ -1,0 +1,169 @@
+/*
+ * tarang_b200.h -- C ABI of libtarang_b200.so, the sm_100a implementation of
+ * Tarang.jl's IMEX timestep hot path for RealFourier(x) x ChebyshevT(z) tau
+ * problems (2D Boussinesq Rayleigh-Benard convection).
+ *
+ * Every entry point returns a tb_status; nothing throws or aborts across the
+ * ABI.  Pointers are borrowed for the duration of the call only.  Device
+ * buffers are owned by the library.  Calls on one plan are not thread-safe
+ * (one CUDA stream per plan); distinct plans may be used concurrently.
+ *
+ * Array conventions (identical to the reference's column-major storage):
+ *   grid field        real    (Nx, Nz) column-major  -> element (x, z) at x + z*Nx
+ *   coefficient field complex (Nx/2+1, Nz) column-major, interleaved (re, im)
+ *                     -> element (k, n) at 2*(k + n*(Nx/2+1))
+ *   tau field         complex (Nx/2+1) per tau variable
+ */
+#ifndef TARANG_B200_H
+#define TARANG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int tb_status;
+enum {
+  TB_OK = 0,
+  TB_EINVAL = 1,        /* bad argument, shape or descriptor                  */
+  TB_ENOMEM = 2,        /* device allocation failed                           */
+  TB_ESINGULAR = 3,     /* a tau system is singular; tb_last_error names mode */
+  TB_ETIMEOUT = 4,      /* a bounded device wait gave up                      */
+  TB_ECUDA = 5,         /* CUDA runtime error (message in tb_last_error)      */
+  TB_ENOTSUPPORTED = 6, /* size/feature outside what the kernels implement    */
+  TB_EBUDGET = 7,       /* request exceeds the HBM budget of a server         */
+  TB_ESTATE = 8         /* call order violated (e.g. solve before factor)     */
+};
+
+typedef struct tb_context tb_context;
+typedef struct tb_plan tb_plan;
+
+/* Where a host-visible pointer lives. */
+enum { TB_HOST = 0, TB_DEVICE = 1 };
+
+/* Time steppers (src/core/timesteppers/types.jl:49-167, 217). */
+enum { TB_RK222 = 0, TB_RK443 = 1, TB_SBDF1 = 2, TB_SBDF2 = 3 };
+
+/* Equation programs.  TB_PROGRAM_RBC is the Boussinesq system of
+ * test/test_subproblem_rk.jl:50-57 (first-order tau formulation with
+ * lift(., -1) on the last ChebyshevT mode). */
+enum { TB_PROGRAM_RBC = 0 };
+
+/* Arithmetic of the step. */
+enum { TB_PREC_F64 = 0, TB_PREC_MIXED = 1 };
+
+/* Field selectors for tb_set_state / tb_get_state. */
+enum {
+  TB_FIELD_B = 0, TB_FIELD_UX = 1, TB_FIELD_UZ = 2, TB_FIELD_P = 3,
+  TB_FIELD_TAU = 4 /* 7 x (Nx/2+1) complex: tau_p, tau_b1, tau_b2, tau_u1x, tau_u1z, tau_u2x, tau_u2z */
+};
+
+typedef struct tb_problem_desc {
+  int ndim;          /* 2                                                        */
+  int Nx, Ny, Nz;    /* grid sizes (Ny ignored in 2D)                            */
+  double Lx, Ly, Lz; /* x in [0,Lx), z in [0,Lz]                                 */
+  double dealias;    /* 3/2 padding factor along Fourier axes                    */
+  int precision;     /* TB_PREC_*                                                */
+  int timestepper;   /* TB_RK222 ...                                             */
+  int program;       /* TB_PROGRAM_RBC                                           */
+  double kappa, nu;  /* b diffusivity, kinematic viscosity                       */
+  double b_bottom;   /* value of b at z = 0   (BC "b(z=0) = ...")               */
+  double b_top;      /* value of b at z = Lz  (BC "b(z=Lz) = ...")              */
+} tb_problem_desc;
+
+/* -------------------------------------------------------------------------
+ * Context and errors.  Replaces the device selection the reference does
+ * through CUDA.jl when arch=GPU() (src/core/architectures.jl:107).
+ * ---------------------------------------------------------------------- */
+tb_status tb_context_create(int device, tb_context** out);
+tb_status tb_context_destroy(tb_context* ctx);
+const char* tb_last_error(const tb_context* ctx);
+const char* tb_status_string(tb_status s);
+int tb_version(void);
+
+/* -------------------------------------------------------------------------
+ * Timestep plan.  Replaces InitialValueSolver(problem, ts; dt) for arch=GPU()
+ * (src/core/solvers/solver_types.jl:468-573, 993): builds the per-Fourier-mode
+ * tau operators that build_matrices! assembles
+ * (src/core/subsystems/subproblem_matrix_build.jl:11-309) in the library's own
+ * banded form and allocates all device state.
+ * ---------------------------------------------------------------------- */
+tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan** out);
+tb_status tb_plan_destroy(tb_plan* plan);
+
+/* Coefficient-space state I/O (the fields' coefficient layout, :c).
+ * where = TB_HOST or TB_DEVICE.  Replaces get_coeff_data/set on state fields. */
+tb_status tb_set_state(tb_plan* plan, int field, const void* data, int where);
+tb_status tb_get_state(tb_plan* plan, int field, void* data, int where);
+
+/* Advance nsteps steps of size dt.  Replaces step!(solver, dt)
+ * (src/core/solvers/solver_stepping.jl:24-38) through
+ * _dispatch_step! -> step_subproblem_rk! / step_subproblem_multistep!
+ * (src/core/timesteppers/dispatch.jl:22-230).  The first call for a new dt
+ * factors the tau systems (once per (dt, a_ii)); later calls replay a CUDA
+ * graph of one step. */
+tb_status tb_step(tb_plan* plan, double dt, int nsteps);
+tb_status tb_sim_time(const tb_plan* plan, double* t, long long* iteration);
+/* Wait for the plan's stream (the step is asynchronous otherwise). */
+tb_status tb_synchronize(tb_plan* plan);
+
+/* Device-side timing of the last tb_step call in milliseconds (CUDA events on
+ * the plan's stream), and a per-kernel-class breakdown accumulated since the
+ * last reset: out[0] transforms+products, out[1] tau solves, out[2] stage
+ * updates (filled only when profiling is on, which disables graph replay). */
+tb_status tb_last_step_ms(const tb_plan* plan, float* ms);
+tb_status tb_set_profiling(tb_plan* plan, int on);
+tb_status tb_kernel_times(tb_plan* plan, double* out3, int reset);
+/* Host-only query of the banded layout the plan compiler builds for the RBC
+ * tau system (no GPU needed): info4 = {band rows n, border size nb, kl, ku}
+ * for parity class cls (0 or 1). */
+tb_status tb_tau_layout_query(int Nz, double Lx, double Lz, int cls, int* info4);
+/* Number of kernels one step launches (for launch accounting). */
+tb_status tb_kernels_per_step(const tb_plan* plan, int* n);
+
+/* -------------------------------------------------------------------------
+ * Transform backend.  Replaces Tarang._gpu_forward_transform_backend! /
+ * _gpu_backward_transform_backend!(::GPU, field)
+ * (src/core/transforms/transform_gpu.jl:181-205; implemented by the CUDA
+ * extension at ext/cuda/transforms.jl:234-243,510 and
+ * ext/cuda/mixed_transforms.jl:229-424).  Forward: grid (Nx,Nz) real ->
+ * coefficients (Nx/2+1,Nz) complex: unnormalised rfft along x, DCT-I along z
+ * scaled 1/(Nz-1) with halved endpoints and flipped odd degrees
+ * (transform_chebyshev.jl:135-244).  Backward is the exact inverse of that
+ * chain (irfft ignores Im of the DC/Nyquist bins).  Pointers are device
+ * pointers.  nfields fields stored back to back.
+ * ---------------------------------------------------------------------- */
+tb_status tb_transform_forward(tb_plan* plan, const double* grid, double* coeff, int nfields);
+tb_status tb_transform_backward(tb_plan* plan, const double* coeff, double* grid, int nfields);
+
+/* 3/2-dealiased product of two grid fields on the plan's (Nx, Nz) grid.
+ * Replaces evaluate_transform_multiply -> evaluate_padded_multiply
+ * (src/core/nonlinear/nonlinear_evaluation.jl:115-213,
+ * src/core/nonlinear/nonlinear_padding.jl:359-443).  Device pointers. */
+tb_status tb_dealiased_multiply(tb_plan* plan, const double* a_grid, const double* b_grid, double* out_grid);
+
+/* RHS program: F = -(u.grad) f for f in (b, ux, uz), coefficient space in and
+ * out.  Replaces execute_lazy_rhs_buffered! for the RBC program
+ * (src/core/solvers/lazy_rhs.jl:1542-1561).  in: 3 coefficient fields
+ * (b, ux, uz) back to back; out: 3 coefficient fields.  Device pointers. */
+tb_status tb_rhs_advection(tb_plan* plan, const double* coeff_in, double* coeff_out);
+
+/* -------------------------------------------------------------------------
+ * Batched dense complex LU, one n x n matrix per slice.  Replaces
+ * BatchedDenseLU batched_factor!/batched_solve!
+ * (src/tools/batched_matsolvers.jl:57-123; CUDA getrf/getrs strided batched at
+ * ext/cuda/batched_matsolvers.jl:80-125).  A: device, column-major n x n
+ * complex128 per slice, overwritten by the factors; piv: device int32 n*batch.
+ * On a singular slice returns TB_ESINGULAR and writes the first singular
+ * slice index to *bad_slice (the reference names the mode and raises).
+ * ---------------------------------------------------------------------- */
+tb_status tb_batched_lu_factor(tb_context* ctx, int n, int batch, double* A, int* piv, int* bad_slice);
+tb_status tb_batched_lu_solve(tb_context* ctx, int n, int batch, const double* A, const int* piv,
+                              double* B /* n x batch complex, overwritten by X */);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TARANG_B200_H */

@@ -1,0 +1,599 @@
+"""CPU oracle for the Tarang.jl IMEX timestep hot path (TEST INFRASTRUCTURE ONLY).
+
+This module restates, in NumPy/SciPy Float64, the algorithm Tarang.jl v1.0.73 runs
+on its CPU path for a RealFourier(x) x ChebyshevT(z) tau problem, specialised to
+the 2D Boussinesq Rayleigh-Benard system of ``test/test_subproblem_rk.jl:50-57``.
+It is the checker for the CUDA library and is imported only by ``tests/``,
+``__graft_entry__.smoke()`` and the ``cpu_baseline`` / reference leg of
+``bench.py``.  Nothing in the shipped library imports or calls it.
+
+Parity status: the reference is Julia (FFTW + SuiteSparse) and cannot run in
+this environment, so the oracle is pinned against the reference's own analytic
+known-answer tests (transform round trips, spectral derivatives, 3/2-dealiased
+products, tau-method boundary enforcement, the tau_method.md Poisson quick
+start) which ``tests/test_oracle_known_answers.py`` re-runs.  Bitwise FFTW
+rounding is not reproduced; every comparison is a relative tolerance.
+
+Array layout follows the reference's column-major storage exactly: a grid
+field of logical size (Nx, Nz) is a NumPy array of shape (Nz, Nx) in C order,
+a coefficient field (Nx/2+1, Nz) is shape (Nz, Nk).  Axis 1 is x, axis 0 is z.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import scipy.fft as sfft
+import scipy.linalg as sla
+
+# ---------------------------------------------------------------------------
+# Grids and wavenumbers
+# ---------------------------------------------------------------------------
+
+
+def fourier_grid(N: int, L: float, x0: float = 0.0) -> np.ndarray:
+    """x_j = x0 + j L/N  (src/core/basis/basis_interface.jl:81-98, _native_grid(::RealFourier))."""
+    return x0 + np.arange(N) * (L / N)
+
+
+def cheb_grid(N: int, a: float, b: float) -> np.ndarray:
+    """Gauss-Lobatto z_j = a + (b-a)/2 (1 - cos(pi j/(N-1)))  (basis_interface.jl:107-121).
+
+    The native grid is -cos(pi k/(N-1)), so z_0 = a (bottom wall) and z_{N-1} = b.
+    """
+    native = -np.cos(np.pi * np.arange(N) / (N - 1))
+    return (b - a) / 2.0 * native + (b + a) / 2.0
+
+
+def wavenumbers_rfft(N: int, L: float) -> np.ndarray:
+    """k = 2pi/L [0..N/2]  (src/core/basis/basis_wavenumbers.jl:68-79)."""
+    return (2.0 * np.pi / L) * np.arange(N // 2 + 1)
+
+
+# ---------------------------------------------------------------------------
+# Transforms (reference conventions)
+# ---------------------------------------------------------------------------
+
+
+def cheb_forward(g: np.ndarray, axis: int = 0) -> np.ndarray:
+    """ChebyshevT forward: REDFT00, x1/(N-1), halve both endpoints, flip odd degrees.
+
+    src/core/transforms/transform_chebyshev.jl:135-183.  Complex input is
+    transformed as separate real and imaginary parts (the same thing, since the
+    map is real-linear).
+    """
+    N = g.shape[axis]
+    out = sfft.dct(np.real(g), type=1, axis=axis) + (
+        1j * sfft.dct(np.imag(g), type=1, axis=axis) if np.iscomplexobj(g) else 0.0
+    )
+    out = np.asarray(out) / (N - 1)
+    sl = [slice(None)] * out.ndim
+    sl[axis] = 0
+    out[tuple(sl)] *= 0.5
+    sl[axis] = N - 1
+    out[tuple(sl)] *= 0.5
+    sl[axis] = slice(1, None, 2)
+    out[tuple(sl)] *= -1.0
+    return out
+
+
+def cheb_backward(c: np.ndarray, axis: int = 0) -> np.ndarray:
+    """ChebyshevT backward: flip odd, double endpoints, REDFT00, /2 (transform_chebyshev.jl:187-244)."""
+    N = c.shape[axis]
+    s = np.array(c, dtype=c.dtype, copy=True)
+    sl = [slice(None)] * s.ndim
+    sl[axis] = slice(1, None, 2)
+    s[tuple(sl)] *= -1.0
+    sl[axis] = 0
+    s[tuple(sl)] *= 2.0
+    sl[axis] = N - 1
+    s[tuple(sl)] *= 2.0
+    out = sfft.dct(np.real(s), type=1, axis=axis) + (
+        1j * sfft.dct(np.imag(s), type=1, axis=axis) if np.iscomplexobj(s) else 0.0
+    )
+    return np.asarray(out) / 2.0
+
+
+def forward_2d(g: np.ndarray) -> np.ndarray:
+    """Grid (Nz, Nx) real -> coefficients (Nz, Nx/2+1) complex.
+
+    RealFourier first (unnormalised rfft, transform_fourier.jl:7-31), then
+    ChebyshevT along z (the reference's forward order, mixed_transforms.jl:229-330).
+    """
+    return cheb_forward(np.fft.rfft(g, axis=1), axis=0)
+
+
+def backward_2d(c: np.ndarray, Nx: int) -> np.ndarray:
+    """Coefficients (Nz, Nk) -> grid (Nz, Nx).  irfft divides by N and, like
+    FFTW's c2r, ignores the imaginary parts of the DC and Nyquist bins
+    (transform_fourier.jl:287-313)."""
+    return np.fft.irfft(cheb_backward(c, axis=0), n=Nx, axis=1)
+
+
+# ---------------------------------------------------------------------------
+# Chebyshev operators in the T basis
+# ---------------------------------------------------------------------------
+
+
+def cheb_diff_matrix(N: int, L: float) -> np.ndarray:
+    """Dense T->T first-derivative matrix, scaled by 2/L.
+
+    Row 0 weight j, rows k>=1 weight 2j, nonzero only for j>k with j-k odd
+    (basis_operators.jl:826-853; scaling :754-770).
+    """
+    D = np.zeros((N, N))
+    for k in range(N - 1):
+        for j in range(k + 1, N):
+            if (j - k) % 2 == 1:
+                D[k, j] = float(j) if k == 0 else 2.0 * j
+    return D * (2.0 / L)
+
+
+def cheb_eval_row(N: int, zeta: float) -> np.ndarray:
+    """Row T_n(zeta), zeta in [-1,1] (the stored-basis Interpolate row,
+    matrices_subproblem_operators.jl:263-308)."""
+    return np.cos(np.arange(N) * np.arccos(np.clip(zeta, -1.0, 1.0)))
+
+
+def cheb_integ_row(N: int, L: float) -> np.ndarray:
+    """w_n = int_0^L T_n dz = L/2 * 2/(1-n^2) for even n, 0 for odd n.
+
+    The reference builds it by quadrature (matrices_subproblem_operators.jl:353-364);
+    the odd entries come out at round-off level and are removed by the 1e-12 entry
+    cutoff (subproblem_matrix_build.jl:88-100), so the exact row is used here.
+    """
+    w = np.zeros(N)
+    for n in range(0, N, 2):
+        w[n] = L / 2.0 * 2.0 / (1.0 - n * n)
+    return w
+
+
+# ---------------------------------------------------------------------------
+# 3/2-dealiased product (nonlinear_padding.jl:58-443)
+# ---------------------------------------------------------------------------
+
+
+def padded_length(N: int, factor: float = 1.5) -> int:
+    """M = ceil(factor N), bumped to even (nonlinear_padding.jl:103-108)."""
+    M = int(math.ceil(factor * N))
+    if M % 2 == 1:
+        M += 1
+    return M
+
+
+def padded_multiply(a: np.ndarray, b: np.ndarray, factor: float = 1.5) -> np.ndarray:
+    """Grid (Nz, Nx) x grid (Nz, Nx) -> dealiased product on the same grid.
+
+    Full complex FFT along x, zero-pad N->M with the even-N Nyquist bin split
+    X/2 at +-N/2, inverse FFT, multiply, forward FFT, fold -N/2 back into the
+    Nyquist bin, truncate, inverse FFT on N points, real part times M/N
+    (nonlinear_padding.jl:182-226, 294-346, 359-443).  The Chebyshev axis is not
+    padded (:86-103).
+    """
+    N = a.shape[1]
+    if N <= 4:
+        raise ValueError("padded product is skipped by the reference for N <= 4")
+    M = padded_length(N, factor)
+    Nh = N // 2
+    n_neg = N - Nh - 1
+
+    def pad(x):
+        s = np.fft.fft(x.astype(complex), axis=1)
+        p = np.zeros((x.shape[0], M), dtype=complex)
+        p[:, : Nh + 1] = s[:, : Nh + 1]
+        if n_neg > 0:
+            p[:, M - n_neg :] = s[:, N - n_neg :]
+        if N % 2 == 0 and M > N:
+            p[:, Nh] *= 0.5
+            p[:, M - Nh] = p[:, Nh]
+        return np.fft.ifft(p, axis=1)
+
+    prod = pad(a) * pad(b)
+    P = np.fft.fft(prod, axis=1)
+    if N % 2 == 0 and M > N:
+        P[:, Nh] += P[:, M - Nh]
+    R = np.zeros((a.shape[0], N), dtype=complex)
+    R[:, : Nh + 1] = P[:, : Nh + 1]
+    if n_neg > 0:
+        R[:, N - n_neg :] = P[:, M - n_neg :]
+    r = np.fft.ifft(R, axis=1)
+    return np.real(r) * (M / N)
+
+
+# ---------------------------------------------------------------------------
+# 2D Rayleigh-Benard tau problem
+# ---------------------------------------------------------------------------
+
+# Tableaus (src/core/timesteppers/types.jl:49-167)
+_G2 = 1.0 - 1.0 / math.sqrt(2.0)
+RK222 = dict(
+    name="RK222",
+    AE=np.array([[0.0, 0.0, 0.0], [_G2, 0.0, 0.0], [_G2, 1.0 - _G2, 0.0]]),
+    AI=np.array([[0.0, 0.0, 0.0], [0.0, _G2, 0.0], [0.0, 1.0 - _G2, _G2]]),
+    bE=np.array([0.0, 1.0 - _G2, _G2]),
+    bI=np.array([0.0, 1.0 - _G2, _G2]),
+    c=np.array([0.0, _G2, 1.0]),
+)
+_G3 = 0.4358665215084590
+RK443 = dict(
+    name="RK443",
+    AE=np.array(
+        [
+            [0.0, 0.0, 0.0, 0.0],
+            [0.4358665215084590, 0.0, 0.0, 0.0],
+            [0.3212788860285571, 0.3966543747256624, 0.0, 0.0],
+            [-0.105858296071263, 0.5529291479590279, 0.5529291481122351, 0.0],
+        ]
+    ),
+    AI=np.array(
+        [
+            [0.0, 0.0, 0.0, 0.0],
+            [0.0, _G3, 0.0, 0.0],
+            [0.0, 0.2820667392457805, _G3, 0.0],
+            [0.0, 1.208496649176010, -0.6443631706844688, _G3],
+        ]
+    ),
+    bE=np.array([0.0, 1.208496649176010, -0.6443631706844688, 0.4358665215084590]),
+    bI=np.array([0.0, 1.208496649176010, -0.6443631706844688, _G3]),
+    c=np.array([0.0, _G3, 0.7179332607542195, 1.0]),
+)
+TABLEAUS = {"RK222": RK222, "RK443": RK443}
+
+
+def sbdf_coefs(order: int, dt: float, dt_prev: Optional[float] = None):
+    """SBDF1/SBDF2 (a, b, c) tuples (step_subproblem_multistep.jl:536-553)."""
+    if order == 1:
+        return (1.0 / dt, -1.0 / dt), (1.0,), (0.0, 1.0)
+    w1 = dt / (dt if dt_prev is None else dt_prev)
+    a = ((1.0 + 2.0 * w1) / ((1.0 + w1) * dt), -(1.0 + w1) / dt, w1 * w1 / ((1.0 + w1) * dt))
+    return a, (1.0,), (0.0, 1.0 + w1, -w1)
+
+
+@dataclass
+class RBCParams:
+    Nx: int
+    Nz: int
+    Lx: float = 4.0
+    Lz: float = 1.0
+    Ra: float = 2e6
+    Pr: float = 1.0
+    dealias: float = 1.5
+    b_bottom: float = None  # value of b at z=0 (defaults to Lz)
+    b_top: float = 0.0
+
+    @property
+    def kappa(self) -> float:
+        return (self.Ra * self.Pr) ** -0.5
+
+    @property
+    def nu(self) -> float:
+        return (self.Ra / self.Pr) ** -0.5
+
+    def bottom(self) -> float:
+        return self.Lz if self.b_bottom is None else self.b_bottom
+
+
+def rbc_initial_b(p: RBCParams, seed: int = 42, amp: float = 1e-3) -> np.ndarray:
+    """b0 = Lz - z + amp z (Lz - z) xi on the (x,z) grid, xi ~ N(0,1) from PCG64(seed).
+
+    The reference draws xi with Julia's RNG (field_layout_operations.jl:34-60),
+    which cannot be reproduced here; this seeded NumPy draw is fed identically to
+    the oracle and to the CUDA library.  Returned in grid layout (Nz, Nx).
+    """
+    rng = np.random.default_rng(seed)
+    xi = rng.standard_normal((p.Nx, p.Nz)).T  # (Nz, Nx), drawn in Julia (x,z) order
+    z = cheb_grid(p.Nz, 0.0, p.Lz)[:, None]
+    return (p.Lz - z) + amp * z * (p.Lz - z) * xi
+
+
+class RBC2D:
+    """Per-Fourier-mode tau system and IMEX steppers for 2D Boussinesq RBC.
+
+    Unknown order inside one mode vector (the oracle's own; the reference's
+    pre_right permutation only reorders):
+        [p(Nz), b(Nz), ux(Nz), uz(Nz), tau_p, tau_b1, tau_b2, tau_u1x, tau_u1z, tau_u2x, tau_u2z]
+    with tau_p present only at kx = 0 (valid-mode filtering,
+    subproblem_matrix_build.jl:102-168).  Equation order:
+        [continuity(Nz), b(Nz), u_x(Nz), u_z(Nz),
+         b(z=0), u_x(z=0), u_z(z=0), b(z=Lz), u_x(z=Lz), u_z(z=Lz), integ(p)]
+    with integ(p) present only at kx = 0.
+    """
+
+    TAU_NAMES = ("tau_p", "tau_b1", "tau_b2", "tau_u1x", "tau_u1z", "tau_u2x", "tau_u2z")
+
+    def __init__(self, p: RBCParams):
+        self.p = p
+        Nx, Nz = p.Nx, p.Nz
+        self.Nk = Nx // 2 + 1
+        self.kx = wavenumbers_rfft(Nx, p.Lx)
+        self.D = cheb_diff_matrix(Nz, p.Lz)
+        self.D2 = self.D @ self.D
+        self.z = cheb_grid(Nz, 0.0, p.Lz)
+        self._mats: Dict[int, Tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]] = {}
+        self._lu: Dict[Tuple[int, float, float], tuple] = {}
+        # state: coefficient fields (Nz, Nk) complex, taus (7, Nk) complex
+        self.b = np.zeros((Nz, self.Nk), complex)
+        self.ux = np.zeros_like(self.b)
+        self.uz = np.zeros_like(self.b)
+        self.pr = np.zeros_like(self.b)
+        self.tau = np.zeros((7, self.Nk), complex)
+        self.sim_time = 0.0
+        self.iteration = 0
+        self._ms_hist: List[Tuple[np.ndarray, np.ndarray]] = []  # SBDF (MX, F) history, newest first
+        self._ms_dt_prev: Optional[float] = None
+
+    # -- per-mode matrices (subproblem_matrix_build.jl:11-309) --------------
+    def n_unknowns(self, m: int) -> int:
+        return 4 * self.p.Nz + (7 if m == 0 else 6)
+
+    def mode_matrices(self, m: int):
+        """Dense M, L (complex), BC-row index list and ALG_F for Fourier mode m."""
+        if m in self._mats:
+            return self._mats[m]
+        p = self.p
+        N = p.Nz
+        kx = self.kx[m]
+        ikx = 1j * kx
+        D, D2 = self.D, self.D2
+        I = np.eye(N)
+        eN1 = np.zeros(N)
+        eN1[N - 1] = 1.0  # lift(., -1) -> unit column e_{N-1} (matrices_subproblem_operators.jl:218-260)
+        De = D @ eN1
+        has_tp = m == 0
+        ntau = 7 if has_tp else 6
+        n = 4 * N + ntau
+        # column offsets
+        cp, cb, cux, cuz = 0, N, 2 * N, 3 * N
+        t0 = 4 * N
+        tcol = {}
+        names = self.TAU_NAMES if has_tp else self.TAU_NAMES[1:]
+        for i, nm in enumerate(names):
+            tcol[nm] = t0 + i
+        # row offsets
+        rc, rb, rx, rz = 0, N, 2 * N, 3 * N
+        r_bc = 4 * N
+        M = np.zeros((n, n), complex)
+        L = np.zeros((n, n), complex)
+        kap, nu = p.kappa, p.nu
+        lap = -kx * kx * I + D2
+        # trace(grad_u) + tau_p = 0
+        L[rc : rc + N, cux : cux + N] += ikx * I
+        L[rc : rc + N, cuz : cuz + N] += D
+        L[rc : rc + N, tcol["tau_u1z"]] += eN1
+        if has_tp:
+            L[rc, tcol["tau_p"]] += 1.0  # 0-D field -> T_0 row (subproblem_expr_helpers.jl:189-193)
+        # dt(b) - kappa div(grad_b) + lift(tau_b2) = -u.grad(b)
+        M[rb : rb + N, cb : cb + N] += I
+        L[rb : rb + N, cb : cb + N] += -kap * lap
+        L[rb : rb + N, tcol["tau_b1"]] += -kap * De
+        L[rb : rb + N, tcol["tau_b2"]] += eN1
+        # dt(u) - nu div(grad_u) + grad(p) - b ez + lift(tau_u2) = -u.grad(u)
+        M[rx : rx + N, cux : cux + N] += I
+        L[rx : rx + N, cux : cux + N] += -nu * lap
+        L[rx : rx + N, tcol["tau_u1x"]] += -nu * De
+        L[rx : rx + N, cp : cp + N] += ikx * I
+        L[rx : rx + N, tcol["tau_u2x"]] += eN1
+        M[rz : rz + N, cuz : cuz + N] += I
+        L[rz : rz + N, cuz : cuz + N] += -nu * lap
+        L[rz : rz + N, tcol["tau_u1z"]] += -nu * De
+        L[rz : rz + N, cp : cp + N] += D
+        L[rz : rz + N, cb : cb + N] += -I
+        L[rz : rz + N, tcol["tau_u2z"]] += eN1
+        # boundary conditions (Interpolate rows, T_n(-1) at z=0 and T_n(1) at z=Lz)
+        bot = cheb_eval_row(N, -1.0)
+        top = cheb_eval_row(N, 1.0)
+        L[r_bc + 0, cb : cb + N] = bot
+        L[r_bc + 1, cux : cux + N] = bot
+        L[r_bc + 2, cuz : cuz + N] = bot
+        L[r_bc + 3, cb : cb + N] = top
+        L[r_bc + 4, cux : cux + N] = top
+        L[r_bc + 5, cuz : cuz + N] = top
+        bc_rows = list(range(r_bc, r_bc + 6))
+        alg_f = np.zeros(n, complex)
+        if m == 0:
+            # constant BC value v projects to v*Nx at kx=0 (subproblem_rhs.jl:99-115)
+            alg_f[r_bc + 0] = p.bottom() * p.Nx
+            alg_f[r_bc + 3] = p.b_top * p.Nx
+            # integ(p) = 0 : Lx * int T_n dz
+            L[r_bc + 6, cp : cp + N] = p.Lx * cheb_integ_row(N, p.Lz)
+            bc_rows.append(r_bc + 6)
+        # entry cutoff 1e-12 (subproblem_matrix_build.jl:88-100)
+        L[np.abs(L) < 1e-12] = 0.0
+        out = (M, L, np.array(bc_rows), alg_f)
+        self._mats[m] = out
+        return out
+
+    # -- gather/scatter between fields and mode vectors ---------------------
+    def gather(self, m: int, b, ux, uz, pr, tau) -> np.ndarray:
+        taus = tau[:, m] if m == 0 else tau[1:, m]
+        return np.concatenate([pr[:, m], b[:, m], ux[:, m], uz[:, m], taus])
+
+    def scatter(self, m: int, x: np.ndarray, b, ux, uz, pr, tau) -> None:
+        N = self.p.Nz
+        pr[:, m] = x[0:N]
+        b[:, m] = x[N : 2 * N]
+        ux[:, m] = x[2 * N : 3 * N]
+        uz[:, m] = x[3 * N : 4 * N]
+        if m == 0:
+            tau[:, m] = x[4 * N :]
+        else:
+            tau[0, m] = 0.0
+            tau[1:, m] = x[4 * N :]
+
+    def equation_F(self, m: int, Fb, Fux, Fuz) -> np.ndarray:
+        """gather_eqn_F!: PDE rows get the F coefficients, algebraic rows stay zero
+        (subproblem_rhs.jl:411-482)."""
+        N = self.p.Nz
+        n = self.n_unknowns(m)
+        f = np.zeros(n, complex)
+        f[N : 2 * N] = Fb[:, m]
+        f[2 * N : 3 * N] = Fux[:, m]
+        f[3 * N : 4 * N] = Fuz[:, m]
+        return f
+
+    def mass_solve(self, m: int, rhs: np.ndarray) -> np.ndarray:
+        """Min-norm least squares of the 0/1 selection M_min (SPQR on CPU,
+        step_subproblem_rk.jl:873-905): copy the b/u rows, zero p and taus."""
+        N = self.p.Nz
+        x = np.zeros_like(rhs)
+        x[N : 4 * N] = rhs[N : 4 * N]
+        return x
+
+    def _lhs_lu(self, m: int, alpha: float, beta: float):
+        key = (m, alpha, beta)
+        lu = self._lu.get(key)
+        if lu is None:
+            M, L, _, _ = self.mode_matrices(m)
+            A = alpha * M + beta * L
+            lu = sla.lu_factor(A)
+            if np.min(np.abs(np.diag(lu[0]))) == 0.0:
+                raise np.linalg.LinAlgError(f"singular tau matrix at mode {m}")
+            self._lu[key] = lu
+        return lu
+
+    # -- state helpers -------------------------------------------------------
+    def set_b_grid(self, bg: np.ndarray) -> None:
+        self.b = forward_2d(bg)
+
+    def fields(self):
+        return self.b, self.ux, self.uz, self.pr, self.tau
+
+    def projected(self, c: np.ndarray) -> np.ndarray:
+        """A c->g->c round trip through rfft/irfft drops Im of the DC and Nyquist
+        x-modes (the re-gather hazard of step_subproblem_rk_batched.jl:33-37)."""
+        out = np.array(c, copy=True)
+        out[:, 0] = out[:, 0].real
+        if self.p.Nx % 2 == 0:
+            out[:, self.p.Nx // 2] = out[:, self.p.Nx // 2].real
+        return out
+
+    # -- RHS: lazy evaluator semantics (lazy_rhs.jl:712-1157) -----------------
+    def rhs(self, b, ux, uz):
+        """F = -(u.grad f) for f in (b, ux, uz); returns coefficient fields."""
+        p = self.p
+        Nx = p.Nx
+        bg, uxg, uzg = (backward_2d(c, Nx) for c in (b, ux, uz))
+        kmul = (1j * self.kx)[None, :]
+
+        def dx(g):
+            return backward_2d(kmul * forward_2d(g), Nx)
+
+        def dz(g):
+            return backward_2d(self.D @ forward_2d(g), Nx)
+
+        out = []
+        for fg in (bg, uxg, uzg):
+            t1 = padded_multiply(uxg, dx(fg), p.dealias)
+            t2 = padded_multiply(uzg, dz(fg), p.dealias)
+            out.append(forward_2d(-(t1 + t2)))
+        return out
+
+    # -- IMEX Runge-Kutta (step_subproblem_rk.jl:393-739) ---------------------
+    def step_rk(self, dt: float, ts: dict) -> None:
+        Nk = self.Nk
+        s = ts["AE"].shape[0]
+        AE, AI, bE, bI = ts["AE"], ts["AI"], ts["bE"], ts["bI"]
+        x0 = [self.gather(m, *self.fields()) for m in range(Nk)]
+        MX0 = [self.mode_matrices(m)[0] @ x0[m] for m in range(Nk)]
+        F: List[List[np.ndarray]] = []
+        LX: List[List[np.ndarray]] = []
+        for i in range(s):
+            a_ii = AI[i, i]
+            xs = []
+            for m in range(Nk):
+                M, L, bc, algf = self.mode_matrices(m)
+                rhs = MX0[m].copy()
+                for j in range(i):
+                    if abs(dt * AE[i, j]) > 1e-14:
+                        rhs += dt * AE[i, j] * F[j][m]
+                    if abs(dt * AI[i, j]) > 1e-14:
+                        rhs -= dt * AI[i, j] * LX[j][m]
+                if abs(a_ii) < 1e-14:
+                    x = self.mass_solve(m, rhs)
+                else:
+                    rhs[bc] = dt * a_ii * algf[bc]
+                    x = sla.lu_solve(self._lhs_lu(m, 1.0, dt * a_ii), rhs)
+                xs.append(x)
+            for m in range(Nk):
+                self.scatter(m, xs[m], *self.fields())
+            Fb, Fux, Fuz = self.rhs(self.b, self.ux, self.uz)
+            pb, pux, puz = (self.projected(c) for c in (self.b, self.ux, self.uz))
+            F.append([self.equation_F(m, Fb, Fux, Fuz) for m in range(Nk)])
+            LX.append(
+                [self.mode_matrices(m)[1] @ self.gather(m, pb, pux, puz, self.pr, self.tau) for m in range(Nk)]
+            )
+        for m in range(Nk):
+            rhs = MX0[m].copy()
+            for j in range(s):
+                if abs(dt * bE[j]) > 1e-14:
+                    rhs += dt * bE[j] * F[j][m]
+                if abs(dt * bI[j]) > 1e-14:
+                    rhs -= dt * bI[j] * LX[j][m]
+            self.scatter(m, self.mass_solve(m, rhs), *self.fields())
+        self.sim_time += dt
+        self.iteration += 1
+
+    # -- SBDF1/SBDF2 (step_subproblem_multistep.jl:197-405) -------------------
+    def step_sbdf(self, dt: float, order: int = 2) -> None:
+        Nk = self.Nk
+        use_order = 1 if (order == 1 or len(self._ms_hist) < 1) else 2
+        a, bcoef, c = sbdf_coefs(use_order, dt, self._ms_dt_prev)
+        Fb, Fux, Fuz = self.rhs(self.b, self.ux, self.uz)
+        pb, pux, puz = (self.projected(cf) for cf in (self.b, self.ux, self.uz))
+        MXc, Fc = [], []
+        for m in range(Nk):
+            M = self.mode_matrices(m)[0]
+            MXc.append(M @ self.gather(m, pb, pux, puz, self.pr, self.tau))
+            Fc.append(self.equation_F(m, Fb, Fux, Fuz))
+        hist = [(MXc, Fc)] + self._ms_hist
+        xs = []
+        for m in range(Nk):
+            M, L, bc, algf = self.mode_matrices(m)
+            rhs = np.zeros(self.n_unknowns(m), complex)
+            for k in range(1, len(c)):
+                if abs(c[k]) >= 1e-14 and k - 1 < len(hist):
+                    rhs += c[k] * hist[k - 1][1][m]
+            for k in range(1, len(a)):
+                if abs(a[k]) >= 1e-14 and k - 1 < len(hist):
+                    rhs -= a[k] * hist[k - 1][0][m]
+            rhs[bc] = bcoef[0] * algf[bc]
+            xs.append(sla.lu_solve(self._lhs_lu(m, a[0], bcoef[0]), rhs))
+        for m in range(Nk):
+            self.scatter(m, xs[m], *self.fields())
+        self._ms_hist = hist[:1] if order == 1 else hist[:2]
+        self._ms_dt_prev = dt
+        self.sim_time += dt
+        self.iteration += 1
+
+    def step(self, dt: float, scheme: str) -> None:
+        if scheme in TABLEAUS:
+            self.step_rk(dt, TABLEAUS[scheme])
+        elif scheme == "SBDF1":
+            self.step_sbdf(dt, 1)
+        elif scheme == "SBDF2":
+            self.step_sbdf(dt, 2)
+        else:
+            raise ValueError(scheme)
+
+    def state_dict(self) -> Dict[str, np.ndarray]:
+        return dict(b=self.b.copy(), ux=self.ux.copy(), uz=self.uz.copy(), p=self.pr.copy(), tau=self.tau.copy())
+
+
+def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    """Relative L2 error ||a-b|| / ||b|| (0 when both vanish)."""
+    nb = np.linalg.norm(b)
+    na = np.linalg.norm(a - b)
+    if nb == 0.0:
+        return float(na)
+    return float(na / nb)
+
+
+def run_rbc(p: RBCParams, scheme: str, dt: float, nsteps: int, seed: int = 42) -> RBC2D:
+    """Build the RBC problem with the seeded initial b and advance nsteps."""
+    sim = RBC2D(p)
+    sim.set_b_grid(rbc_initial_b(p, seed))
+    for _ in range(nsteps):
+        sim.step(dt, scheme)
+    return sim

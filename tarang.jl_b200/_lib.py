@@ -1,0 +1,101 @@
+"""ctypes binding of libtarang_b200.so (the C ABI declared in include/tarang_b200.h).
+
+The shared library is built in-tree by ``tarang.jl_b200/csrc/Makefile``.  There is
+no CPU fallback: if the library is missing or cannot be loaded, importing this
+module raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, Structure, c_char_p, c_double, c_float, c_int, c_longlong, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtarang_b200.so")
+
+TB_OK, TB_EINVAL, TB_ENOMEM, TB_ESINGULAR, TB_ETIMEOUT, TB_ECUDA, TB_ENOTSUPPORTED, TB_EBUDGET, TB_ESTATE = range(9)
+TB_HOST, TB_DEVICE = 0, 1
+TB_RK222, TB_RK443, TB_SBDF1, TB_SBDF2 = 0, 1, 2, 3
+TB_PROGRAM_RBC = 0
+TB_PREC_F64, TB_PREC_MIXED = 0, 1
+TB_FIELD_B, TB_FIELD_UX, TB_FIELD_UZ, TB_FIELD_P, TB_FIELD_TAU = range(5)
+
+
+class tb_problem_desc(Structure):
+    _fields_ = [
+        ("ndim", c_int),
+        ("Nx", c_int),
+        ("Ny", c_int),
+        ("Nz", c_int),
+        ("Lx", c_double),
+        ("Ly", c_double),
+        ("Lz", c_double),
+        ("dealias", c_double),
+        ("precision", c_int),
+        ("timestepper", c_int),
+        ("program", c_int),
+        ("kappa", c_double),
+        ("nu", c_double),
+        ("b_bottom", c_double),
+        ("b_top", c_double),
+    ]
+
+
+class TarangError(RuntimeError):
+    """Raised when a library call returns a non-OK tb_status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[tb_status {status}] {message}")
+        self.status = status
+
+
+# name -> (restype, argtypes); every symbol include/tarang_b200.h declares.
+SIGNATURES = {
+    "tb_context_create": (c_int, [c_int, POINTER(c_void_p)]),
+    "tb_context_destroy": (c_int, [c_void_p]),
+    "tb_last_error": (c_char_p, [c_void_p]),
+    "tb_status_string": (c_char_p, [c_int]),
+    "tb_version": (c_int, []),
+    "tb_plan_create": (c_int, [c_void_p, POINTER(tb_problem_desc), POINTER(c_void_p)]),
+    "tb_plan_destroy": (c_int, [c_void_p]),
+    "tb_set_state": (c_int, [c_void_p, c_int, c_void_p, c_int]),
+    "tb_get_state": (c_int, [c_void_p, c_int, c_void_p, c_int]),
+    "tb_step": (c_int, [c_void_p, c_double, c_int]),
+    "tb_sim_time": (c_int, [c_void_p, POINTER(c_double), POINTER(c_longlong)]),
+    "tb_synchronize": (c_int, [c_void_p]),
+    "tb_last_step_ms": (c_int, [c_void_p, POINTER(c_float)]),
+    "tb_set_profiling": (c_int, [c_void_p, c_int]),
+    "tb_kernel_times": (c_int, [c_void_p, POINTER(c_double), c_int]),
+    "tb_kernels_per_step": (c_int, [c_void_p, POINTER(c_int)]),
+    "tb_tau_layout_query": (c_int, [c_int, c_double, c_double, c_int, POINTER(c_int)]),
+    "tb_transform_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "tb_transform_backward": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "tb_dealiased_multiply": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "tb_rhs_advection": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "tb_batched_lu_factor": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, POINTER(c_int)]),
+    "tb_batched_lu_solve": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+}
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is missing: build it with `make -C tarang.jl_b200/csrc` "
+            "(there is no CPU fallback for the B200 path)"
+        )
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = load()
+
+
+def check(status: int, ctx=None) -> None:
+    if status != TB_OK:
+        msg = lib.tb_last_error(ctx)
+        text = msg.decode() if msg else lib.tb_status_string(status).decode()
+        raise TarangError(status, text)

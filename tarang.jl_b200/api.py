@@ -1,0 +1,459 @@
+"""Host-side mirror of Tarang.jl's user API for the arch=GPU() timestep path.
+
+Names and argument meanings follow the reference so that a script written
+against Tarang.jl reads the same here (Julia's ``!`` suffix dropped):
+
+    domain = ChannelDomain(256, 64; Lx=4.0, Lz=1.0)      src/extras/quick_domains.jl:109-121
+    b = ScalarField(domain, "b"); u = VectorField(domain, "u")
+    problem = IVP([p, b, u, tau_p, ...])                 src/core/problems/
+    add_equation(problem, "...") / add_bc(problem, "...")
+    solver = InitialValueSolver(problem, RK222(), dt=0.125)   src/core/solvers/solver_types.jl:993
+    step(solver, dt) / run(solver, stop_time=...)        src/core/solvers/solver_stepping.jl:24-205
+
+Everything numerical runs in libtarang_b200.so.  The equation strings are
+matched against the Boussinesq template of test/test_subproblem_rk.jl:50-57
+(the program the library implements); any other system raises
+NotImplementedError instead of falling back to a CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import re
+from ctypes import byref, c_double, c_float, c_int, c_longlong, c_void_p
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import TarangError, check, lib
+
+# ---------------------------------------------------------------------------
+# Architectures and contexts (src/core/architectures.jl:107)
+# ---------------------------------------------------------------------------
+
+
+class CPU:
+    """The reference's CPU architecture; not served by this library."""
+
+
+class GPU:
+    def __init__(self, device: int = 0):
+        self.device = device
+
+
+_CONTEXTS: Dict[int, c_void_p] = {}
+
+
+def _context(device: int = 0) -> c_void_p:
+    ctx = _CONTEXTS.get(device)
+    if ctx is None:
+        ctx = c_void_p()
+        check(lib.tb_context_create(device, byref(ctx)))
+        _CONTEXTS[device] = ctx
+    return ctx
+
+
+# ---------------------------------------------------------------------------
+# Bases and domains
+# ---------------------------------------------------------------------------
+
+
+class RealFourier:
+    def __init__(self, name: str = "x", size: int = 64, bounds=(0.0, 2 * math.pi), dealias: float = 1.0):
+        self.name, self.size, self.bounds, self.dealias = name, int(size), tuple(map(float, bounds)), float(dealias)
+
+    @property
+    def length(self) -> float:
+        return self.bounds[1] - self.bounds[0]
+
+
+class ChebyshevT(RealFourier):
+    pass
+
+
+class Domain:
+    def __init__(self, bases: Sequence, arch=None):
+        self.bases = tuple(bases)
+        self.arch = arch if arch is not None else GPU()
+        if isinstance(self.arch, CPU):
+            raise NotImplementedError("the B200 library serves arch=GPU() only")
+        self.xbasis, self.zbasis = self.bases
+        self._tplan = None
+
+    @property
+    def Nx(self) -> int:
+        return self.xbasis.size
+
+    @property
+    def Nz(self) -> int:
+        return self.zbasis.size
+
+    @property
+    def Nk(self) -> int:
+        return self.Nx // 2 + 1
+
+    def grids(self):
+        """(x, z) grids: x_j = j Lx/Nx, z_j = Lz/2 (1 - cos(pi j/(Nz-1))) (basis_interface.jl:81-121)."""
+        x = self.xbasis.bounds[0] + np.arange(self.Nx) * self.xbasis.length / self.Nx
+        a, b = self.zbasis.bounds
+        z = (b - a) / 2 * (-np.cos(np.pi * np.arange(self.Nz) / (self.Nz - 1))) + (b + a) / 2
+        return x, z
+
+    def transform_plan(self) -> "Plan":
+        """A plan used only for field transforms (physics parameters unused)."""
+        if self._tplan is None:
+            self._tplan = Plan(self, kappa=1.0, nu=1.0, b_bottom=0.0, b_top=0.0, timestepper=L.TB_RK222)
+        return self._tplan
+
+
+def ChannelDomain(Nx: int, Nz: int, Lx: float = 2 * math.pi, Lz: float = 2.0, dtype=np.float64, arch=None,
+                  dealias: float = 1.5) -> Domain:
+    """RealFourier(x in [0,Lx)) x ChebyshevT(z in [0,Lz]) with the given dealias (quick_domains.jl:109-121)."""
+    if dtype not in (np.float64, float):
+        raise NotImplementedError("the FP64 path stores Float64 fields")
+    return Domain((RealFourier("x", Nx, (0.0, Lx), dealias), ChebyshevT("z", Nz, (0.0, Lz), dealias)), arch)
+
+
+# ---------------------------------------------------------------------------
+# Plans (the C ABI object behind a solver)
+# ---------------------------------------------------------------------------
+
+_TS = {"RK222": L.TB_RK222, "RK443": L.TB_RK443, "SBDF1": L.TB_SBDF1, "SBDF2": L.TB_SBDF2}
+
+
+class Plan:
+    def __init__(self, domain: Domain, kappa: float, nu: float, b_bottom: float, b_top: float, timestepper: int,
+                 precision: int = L.TB_PREC_F64):
+        self.domain = domain
+        self.ctx = _context(domain.arch.device)
+        d = L.tb_problem_desc()
+        d.ndim = 2
+        d.Nx, d.Ny, d.Nz = domain.Nx, 1, domain.Nz
+        d.Lx, d.Ly, d.Lz = domain.xbasis.length, 1.0, domain.zbasis.length
+        d.dealias = domain.xbasis.dealias if domain.xbasis.dealias > 1 else 1.5
+        d.precision = precision
+        d.timestepper = timestepper
+        d.program = L.TB_PROGRAM_RBC
+        d.kappa, d.nu, d.b_bottom, d.b_top = kappa, nu, b_bottom, b_top
+        self.desc = d
+        self.ptr = c_void_p()
+        check(lib.tb_plan_create(self.ctx, byref(d), byref(self.ptr)), self.ctx)
+
+    def __del__(self):
+        ptr = getattr(self, "ptr", None)
+        if ptr:
+            lib.tb_plan_destroy(ptr)
+            self.ptr = None
+
+    # state I/O (host numpy, coefficient layout (Nz, Nk) complex128)
+    def set_state(self, field: int, arr: np.ndarray) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.complex128)
+        check(lib.tb_set_state(self.ptr, field, a.ctypes.data_as(c_void_p), L.TB_HOST), self.ctx)
+
+    def get_state(self, field: int) -> np.ndarray:
+        shape = (7, self.domain.Nk) if field == L.TB_FIELD_TAU else (self.domain.Nz, self.domain.Nk)
+        out = np.empty(shape, np.complex128)
+        check(lib.tb_get_state(self.ptr, field, out.ctypes.data_as(c_void_p), L.TB_HOST), self.ctx)
+        return out
+
+    def step(self, dt: float, nsteps: int = 1) -> None:
+        check(lib.tb_step(self.ptr, float(dt), int(nsteps)), self.ctx)
+
+    def last_step_ms(self) -> float:
+        ms = c_float()
+        check(lib.tb_last_step_ms(self.ptr, byref(ms)), self.ctx)
+        return ms.value
+
+    def kernels_per_step(self) -> int:
+        n = c_int()
+        check(lib.tb_kernels_per_step(self.ptr, byref(n)), self.ctx)
+        return n.value
+
+    # device transforms (torch tensors provide device memory)
+    def forward(self, grid: np.ndarray) -> np.ndarray:
+        import torch
+
+        g = torch.as_tensor(np.ascontiguousarray(grid, dtype=np.float64), device="cuda")
+        nf = g.numel() // (self.domain.Nz * self.domain.Nx)
+        c = torch.empty(nf * self.domain.Nz * self.domain.Nk * 2, dtype=torch.float64, device="cuda")
+        check(lib.tb_transform_forward(self.ptr, c_void_p(g.data_ptr()), c_void_p(c.data_ptr()), nf), self.ctx)
+        out = c.cpu().numpy().view(np.complex128)
+        return out.reshape(grid.shape[:-2] + (self.domain.Nz, self.domain.Nk))
+
+    def backward(self, coeff: np.ndarray) -> np.ndarray:
+        import torch
+
+        c = torch.as_tensor(np.ascontiguousarray(coeff, dtype=np.complex128).view(np.float64), device="cuda")
+        nf = c.numel() // (2 * self.domain.Nz * self.domain.Nk)
+        g = torch.empty(nf * self.domain.Nz * self.domain.Nx, dtype=torch.float64, device="cuda")
+        check(lib.tb_transform_backward(self.ptr, c_void_p(c.data_ptr()), c_void_p(g.data_ptr()), nf), self.ctx)
+        return g.cpu().numpy().reshape(coeff.shape[:-2] + (self.domain.Nz, self.domain.Nx))
+
+    def dealiased_multiply(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+        import torch
+
+        ta = torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
+        tb_ = torch.as_tensor(np.ascontiguousarray(b, dtype=np.float64), device="cuda")
+        out = torch.empty_like(ta)
+        check(lib.tb_dealiased_multiply(self.ptr, c_void_p(ta.data_ptr()), c_void_p(tb_.data_ptr()),
+                                        c_void_p(out.data_ptr())), self.ctx)
+        return out.cpu().numpy()
+
+    def rhs_advection(self, b: np.ndarray, ux: np.ndarray, uz: np.ndarray):
+        import torch
+
+        inp = np.ascontiguousarray(np.stack([b, ux, uz]), dtype=np.complex128)
+        ti = torch.as_tensor(inp.view(np.float64), device="cuda")
+        to = torch.empty_like(ti)
+        check(lib.tb_rhs_advection(self.ptr, c_void_p(ti.data_ptr()), c_void_p(to.data_ptr())), self.ctx)
+        o = to.cpu().numpy().view(np.complex128)
+        return o[0], o[1], o[2]
+
+
+# ---------------------------------------------------------------------------
+# Fields
+# ---------------------------------------------------------------------------
+
+
+class ScalarField:
+    """A scalar field on a domain (or a tau field with ``bases=(xbasis,)`` / ``()``).
+
+    Data are held in coefficient layout (Nz, Nx/2+1) complex, the reference's
+    ``:c`` storage; ``f["g"]`` / ``f["c"]`` read and write grid / coefficient data.
+    """
+
+    def __init__(self, domain: Domain, name: str, bases: Optional[tuple] = None):
+        self.domain = domain
+        self.name = name
+        self.bases = domain.bases if bases is None else tuple(bases)
+        self._coeff = np.zeros((domain.Nz, domain.Nk), np.complex128) if len(self.bases) == 2 else np.zeros(
+            domain.Nk, np.complex128)
+        self._solver = None
+        self._slot = None  # (field selector, row) inside the solver's plan
+
+    def _pull(self) -> None:
+        if self._solver is not None:
+            sel, row = self._slot
+            data = self._solver.plan.get_state(sel)
+            self._coeff = data if row is None else data[row].copy()
+
+    def _push(self) -> None:
+        if self._solver is not None:
+            sel, row = self._slot
+            if row is None:
+                self._solver.plan.set_state(sel, self._coeff)
+            else:
+                taus = self._solver.plan.get_state(sel)
+                taus[row] = self._coeff
+                self._solver.plan.set_state(sel, taus)
+
+    def __getitem__(self, layout: str) -> np.ndarray:
+        self._pull()
+        if layout == "c":
+            return self._coeff.copy()
+        if layout == "g":
+            if len(self.bases) != 2:
+                raise NotImplementedError("grid view of tau fields")
+            return self.domain.transform_plan().backward(self._coeff)
+        raise KeyError(layout)
+
+    def __setitem__(self, layout: str, value) -> None:
+        if layout == "c":
+            self._coeff = np.array(value, dtype=np.complex128).reshape(self._coeff.shape)
+        elif layout == "g":
+            g = np.broadcast_to(np.asarray(value, dtype=np.float64), (self.domain.Nz, self.domain.Nx))
+            self._coeff = self.domain.transform_plan().forward(np.ascontiguousarray(g))
+        else:
+            raise KeyError(layout)
+        self._push()
+
+
+class VectorField:
+    def __init__(self, domain: Domain, name: str, bases: Optional[tuple] = None):
+        self.domain = domain
+        self.name = name
+        self.components = [ScalarField(domain, f"{name}_{c}", bases) for c in ("x", "z")]
+
+
+def unit_vector_fields(domain: Domain):
+    """Constant unit vectors (ex, ez); used only as tokens in equation strings."""
+    return ("ex", "ez")
+
+
+# ---------------------------------------------------------------------------
+# Problems, time steppers, solvers
+# ---------------------------------------------------------------------------
+
+
+class IVP:
+    def __init__(self, variables: List):
+        self.variables = list(variables)
+        self.parameters: Dict[str, object] = {}
+        self.equations: List[str] = []
+        self.bcs: List[str] = []
+
+
+def add_parameters(problem: IVP, **kw) -> None:
+    problem.parameters.update(kw)
+
+
+def add_equation(problem: IVP, eq: str) -> None:
+    problem.equations.append(eq)
+
+
+def add_bc(problem: IVP, bc: str) -> None:
+    problem.bcs.append(bc)
+
+
+class _TS:
+    name = ""
+
+    def __repr__(self):
+        return self.name + "()"
+
+
+class RK222(_TS):
+    name = "RK222"
+
+
+class RK443(_TS):
+    name = "RK443"
+
+
+class SBDF1(_TS):
+    name = "SBDF1"
+
+
+class SBDF2(_TS):
+    name = "SBDF2"
+
+
+def _norm(s: str) -> str:
+    s = s.replace(" ", "").replace("∂t", "dt").replace("τ_lift", "lift").replace("·", "⋅")
+    return s
+
+
+def _value(tok: str, params: Dict[str, object]) -> float:
+    try:
+        return float(tok)
+    except ValueError:
+        if tok in params:
+            return float(params[tok])
+        raise NotImplementedError(f"boundary value {tok!r} is not a number or scalar parameter")
+
+
+def _match_boussinesq(problem: IVP):
+    """Recognise the Boussinesq system of test/test_subproblem_rk.jl:50-57."""
+    P = problem.parameters
+    eqs = [_norm(e) for e in problem.equations]
+    cont = scal = mom = None
+    for e in eqs:
+        m = re.fullmatch(r"trace\(grad_(\w+)\)\+(\w+)=0", e)
+        if m:
+            cont = m
+            continue
+        m = re.fullmatch(r"dt\((\w+)\)-(\w+)\*div\(grad_\1\)\+lift\((\w+)\)=-(\w+)⋅∇\(\1\)", e)
+        if m:
+            scal = m
+            continue
+        m = re.fullmatch(r"dt\((\w+)\)-(\w+)\*div\(grad_\1\)\+∇\((\w+)\)-(\w+)\*ez\+lift\((\w+)\)=-\1⋅∇\(\1\)", e)
+        if m:
+            mom = m
+            continue
+        raise NotImplementedError(f"equation not in the supported Boussinesq program: {e!r}")
+    if not (cont and scal and mom):
+        raise NotImplementedError("the B200 path implements the full Boussinesq system (continuity, b, u)")
+    bname, kname = scal.group(1), scal.group(2)
+    uname, nname, pname = mom.group(1), mom.group(2), mom.group(3)
+    if mom.group(4) != bname or scal.group(4) != uname or cont.group(1) != uname:
+        raise NotImplementedError("inconsistent field names in the Boussinesq system")
+    Lz = None
+    bvals = {}
+    saw_integ = False
+    for bc in (_norm(b) for b in problem.bcs):
+        m = re.fullmatch(r"(\w+)\(z=([\w.+-]+)\)=([\w.+-]+)", bc)
+        if m:
+            fld, zpos, val = m.group(1), m.group(2), m.group(3)
+            z = _value(zpos, P)
+            v = _value(val, P)
+            if fld == bname:
+                bvals[z] = v
+            elif fld == uname:
+                if v != 0.0:
+                    raise NotImplementedError("only no-slip velocity walls are implemented")
+            else:
+                raise NotImplementedError(f"boundary condition on unknown field {fld!r}")
+            continue
+        if re.fullmatch(rf"integ\({pname}\)=0", bc):
+            saw_integ = True
+            continue
+        raise NotImplementedError(f"boundary condition not supported: {bc!r}")
+    if len(bvals) != 2 or not saw_integ:
+        raise NotImplementedError("expected b at both walls and integ(p) = 0")
+    z0, z1 = sorted(bvals)
+    return dict(kappa=_value(kname, P), nu=_value(nname, P), b_bottom=bvals[z0], b_top=bvals[z1],
+                names=dict(b=bname, u=uname, p=pname))
+
+
+class InitialValueSolver:
+    """Builds the library plan for the problem and binds its fields to the plan's state."""
+
+    def __init__(self, problem: IVP, timestepper: _TS, dt: Optional[float] = None):
+        spec = _match_boussinesq(problem)
+        fields = {}
+        domain = None
+        for v in problem.variables:
+            if isinstance(v, VectorField):
+                fields[v.name] = v
+                domain = v.domain
+            else:
+                fields[v.name] = v
+                if len(v.bases) == 2:
+                    domain = v.domain
+        self.domain = domain
+        self.problem = problem
+        self.timestepper = timestepper
+        self.dt = dt
+        self.plan = Plan(domain, spec["kappa"], spec["nu"], spec["b_bottom"], spec["b_top"], _TS[timestepper.name])
+        names = spec["names"]
+        b, u, p = fields[names["b"]], fields[names["u"]], fields[names["p"]]
+        binds = [(b, (L.TB_FIELD_B, None)), (u.components[0], (L.TB_FIELD_UX, None)),
+                 (u.components[1], (L.TB_FIELD_UZ, None)), (p, (L.TB_FIELD_P, None))]
+        for f, slot in binds:
+            f._solver, f._slot = self, slot
+            f._push()
+        self.sim_time = 0.0
+        self.iteration = 0
+
+    def step(self, dt: Optional[float] = None, nsteps: int = 1) -> None:
+        dt = self.dt if dt is None else dt
+        if dt is None:
+            raise ValueError("dt not given")
+        self.plan.step(dt, nsteps)
+        t, it = c_double(), c_longlong()
+        check(lib.tb_sim_time(self.plan.ptr, byref(t), byref(it)), self.plan.ctx)
+        self.sim_time, self.iteration = t.value, it.value
+
+
+def step(solver: InitialValueSolver, dt: Optional[float] = None) -> None:
+    """step!(solver, dt) (solver_stepping.jl:24-38)."""
+    solver.step(dt)
+
+
+def run(solver: InitialValueSolver, stop_time: Optional[float] = None, stop_iteration: Optional[int] = None,
+        log_interval: int = 0, dt: Optional[float] = None) -> None:
+    """run!(solver; stop_time, stop_iteration) (solver_stepping.jl:115-205), fixed dt."""
+    dt = solver.dt if dt is None else dt
+    if dt is None:
+        raise ValueError("dt not given")
+    n = None
+    if stop_iteration is not None:
+        n = int(stop_iteration) - solver.iteration
+    if stop_time is not None:
+        nt = int(math.ceil((stop_time - solver.sim_time) / dt - 1e-9))
+        n = nt if n is None else min(n, nt)
+    if n is None:
+        raise ValueError("give stop_time or stop_iteration")
+    if n > 0:
+        solver.step(dt, n)

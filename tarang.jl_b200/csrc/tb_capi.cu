@@ -1,0 +1,778 @@
+// C ABI of libtarang_b200: contexts, plans, state I/O and the timestep driver.
+//
+// The driver mirrors the reference's step loop for a GPU plan:
+//   RK222 / RK443 : step_subproblem_rk!          (step_subproblem_rk.jl:393-739)
+//   SBDF1 / SBDF2 : step_subproblem_multistep!   (step_subproblem_multistep.jl:197-405),
+//                   SBDF2 starting with one SBDF1 step (step_multistep.jl:341-356)
+// One step is captured once per dt as a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+
+#include "tb_internal.h"
+#include "tb_kernels.cuh"
+
+using namespace tb;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  void alloc(size_t b) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = b;
+    if (b == 0) return;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      throw Error{TB_ENOMEM, std::string("cudaMalloc(") + std::to_string(b) + "): " + cudaGetErrorString(e)};
+    }
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+template <class T>
+void upload(DevBuf& d, const std::vector<T>& h) {
+  d.alloc(h.size() * sizeof(T));
+  if (!h.empty()) TB_CUDA_TRY(cudaMemcpy(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+}
+
+struct ClassTables {
+  DevBuf row_eq, row_k, col_unk, col_k, left_unk, left_k, bc_rhs, band, bord, c2_z, c2_nz, c1_z, c1_nz;
+};
+
+struct FactorSet {
+  double alpha = 0, beta = 0;
+  DevBuf piv[2], Lm[2], U[2], Bd[2], Cm[2], Sinv[2];
+};
+
+struct Tableau {
+  int s;
+  double AE[4][4], AI[4][4], bE[4], bI[4];
+};
+
+Tableau tableau(int ts) {
+  Tableau t{};
+  if (ts == TB_RK222) {
+    const double g = 1.0 - 1.0 / std::sqrt(2.0);
+    t.s = 3;
+    double AE[3][3] = {{0, 0, 0}, {g, 0, 0}, {g, 1 - g, 0}};
+    double AI[3][3] = {{0, 0, 0}, {0, g, 0}, {0, 1 - g, g}};
+    double b[3] = {0, 1 - g, g};
+    for (int i = 0; i < 3; ++i) {
+      t.bE[i] = b[i];
+      t.bI[i] = b[i];
+      for (int j = 0; j < 3; ++j) {
+        t.AE[i][j] = AE[i][j];
+        t.AI[i][j] = AI[i][j];
+      }
+    }
+  } else {
+    const double g = 0.4358665215084590;
+    t.s = 4;
+    double AE[4][4] = {{0, 0, 0, 0},
+                       {0.4358665215084590, 0, 0, 0},
+                       {0.3212788860285571, 0.3966543747256624, 0, 0},
+                       {-0.105858296071263, 0.5529291479590279, 0.5529291481122351, 0}};
+    double AI[4][4] = {{0, 0, 0, 0}, {0, g, 0, 0}, {0, 0.2820667392457805, g, 0},
+                       {0, 1.208496649176010, -0.6443631706844688, g}};
+    double bE[4] = {0.0, 1.208496649176010, -0.6443631706844688, 0.4358665215084590};
+    double bI[4] = {0.0, 1.208496649176010, -0.6443631706844688, g};
+    for (int i = 0; i < 4; ++i) {
+      t.bE[i] = bE[i];
+      t.bI[i] = bI[i];
+      for (int j = 0; j < 4; ++j) {
+        t.AE[i][j] = AE[i][j];
+        t.AI[i][j] = AI[i][j];
+      }
+    }
+  }
+  return t;
+}
+
+}  // namespace
+
+struct tb_plan {
+  tb_context* ctx = nullptr;
+  tb_problem_desc d{};
+  int Nx = 0, Nz = 0, Nk = 0, M = 0;
+  double k0 = 0, s = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  size_t plane = 0;  // Nz * Nk complex entries
+  // state and work arrays
+  DevBuf X, tau, G, H, MX0, FP[4], LXP[4], Fprev, MXprev, Rsb, tmpgrid;
+  // transform constants
+  DevBuf bwdstack, bwd, fwd, sfwd, s3, twM, twN;
+  FftPlan fpM{}, fpN{};
+  // tau layout
+  TauLayout lay;
+  ClassTables ct[2];
+  std::vector<std::unique_ptr<FactorSet>> factors;
+  DevBuf err_mode;
+  // stepping state
+  double sim_time = 0.0;
+  long long iteration = 0;
+  int ms_history = 0;  // SBDF: number of stored history levels
+  double graph_dt = -1.0;
+  int graph_kind = -1;
+  cudaGraphExec_t gexec = nullptr;
+  int kernels_per_step = 0;
+
+  ~tb_plan() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  double2* Xp(int f) const { return X.as<double2>() + (size_t)f * plane; }
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+tb_status fail(tb_context* ctx, const Error& e) {
+  if (ctx) ctx->last_error = e.msg;
+  g_err = e.msg;
+  return e.code;
+}
+
+template <class F>
+tb_status guard(tb_context* ctx, F&& fn) {
+  try {
+    fn();
+    return TB_OK;
+  } catch (const Error& e) {
+    return fail(ctx, e);
+  } catch (const std::bad_alloc&) {
+    return fail(ctx, Error{TB_ENOMEM, "host allocation failed"});
+  } catch (...) {
+    return fail(ctx, Error{TB_EINVAL, "unexpected internal error"});
+  }
+}
+
+void check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw Error{TB_ECUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+std::vector<double2> twiddles(int n) {
+  std::vector<double2> t(n);
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int k = 0; k < n; ++k) {
+    long double a = -2.0L * pi * (long double)k / (long double)n;
+    t[k] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  return t;
+}
+
+ClassDev class_dev(tb_plan* P, int c, FactorSet* f) {
+  ClassDev cd{};
+  const ClassLayout& L = P->lay.cls[c];
+  ClassTables& T = P->ct[c];
+  cd.n = L.n;
+  cd.nb = L.nb;
+  cd.kl = L.kl;
+  cd.ku = L.ku;
+  cd.row_eq = T.row_eq.as<short>();
+  cd.row_k = T.row_k.as<short>();
+  cd.col_unk = T.col_unk.as<short>();
+  cd.col_k = T.col_k.as<short>();
+  cd.left_unk = T.left_unk.as<short>();
+  cd.left_k = T.left_k.as<short>();
+  cd.bc_rhs = T.bc_rhs.as<double>();
+  cd.band = T.band.as<Coef>();
+  cd.bord = T.bord.as<Coef>();
+  cd.c2_z = T.c2_z.as<double>();
+  cd.c2_nz = T.c2_nz.as<double>();
+  cd.c1_z = T.c1_z.as<double>();
+  cd.c1_nz = T.c1_nz.as<double>();
+  if (f) {
+    cd.piv = f->piv[c].as<unsigned char>();
+    cd.Lm = f->Lm[c].as<double>();
+    cd.U = f->U[c].as<double>();
+    cd.Bd = f->Bd[c].as<double>();
+    cd.Cm = f->Cm[c].as<double>();
+    cd.Sinv = f->Sinv[c].as<double>();
+  }
+  return cd;
+}
+
+TauArgs tau_args(tb_plan* P, FactorSet* f, const double2* rhsP) {
+  TauArgs a{};
+  a.cls[0] = class_dev(P, 0, f);
+  a.cls[1] = class_dev(P, 1, f);
+  a.Nz = P->Nz;
+  a.Nk = P->Nk;
+  a.Nx = P->Nx;
+  a.k0 = P->k0;
+  a.alpha = f ? f->alpha : 0.0;
+  a.beta = f ? f->beta : 0.0;
+  a.X = P->X.as<double2>();
+  a.tau = P->tau.as<double2>();
+  a.rhsP = rhsP;
+  a.err_mode = P->err_mode.as<int>();
+  return a;
+}
+
+FactorSet* get_factors(tb_plan* P, double alpha, double beta) {
+  for (auto& f : P->factors)
+    if (f->alpha == alpha && f->beta == beta) return f.get();
+  // keep at most two sets (SBDF needs the SBDF1 and SBDF2 left-hand sides)
+  if (P->factors.size() >= 2) P->factors.erase(P->factors.begin());
+  auto fs = std::make_unique<FactorSet>();
+  fs->alpha = alpha;
+  fs->beta = beta;
+  const int Nk = P->Nk;
+  for (int c = 0; c < 2; ++c) {
+    const ClassLayout& L = P->lay.cls[c];
+    const size_t n = L.n, nb = L.nb, w = L.kl + L.ku + 1;
+    fs->piv[c].alloc(n * Nk);
+    fs->Lm[c].alloc(n * L.kl * Nk * sizeof(double));
+    fs->U[c].alloc(n * w * Nk * sizeof(double));
+    fs->Bd[c].alloc(n * nb * Nk * sizeof(double));
+    fs->Cm[c].alloc(n * nb * Nk * sizeof(double));
+    fs->Sinv[c].alloc(nb * nb * Nk * sizeof(double));
+  }
+  const int nmax = std::max(P->lay.cls[0].n, P->lay.cls[1].n);
+  DevBuf scratch;
+  scratch.alloc(tau_factor_scratch_doubles(nmax, Nk) * sizeof(double));
+  int neg = 0x7fffffff;
+  TB_CUDA_TRY(cudaMemcpyAsync(P->err_mode.p, &neg, sizeof(int), cudaMemcpyHostToDevice, P->st));
+  TauArgs a = tau_args(P, fs.get(), nullptr);
+  a.scratch = scratch.as<double>();
+  launch_tau_factor(a, P->st);
+  check_launch("tau factor");
+  int bad = 0;
+  TB_CUDA_TRY(cudaMemcpyAsync(&bad, P->err_mode.p, sizeof(int), cudaMemcpyDeviceToHost, P->st));
+  TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  if (bad != neg)
+    throw Error{TB_ESINGULAR, "singular tau system at Fourier mode " + std::to_string(bad) +
+                                  " (kx = " + std::to_string(bad * P->k0) + ")"};
+  P->factors.push_back(std::move(fs));
+  return P->factors.back().get();
+}
+
+// F = -(u.grad) f in C^(2) rows (sfwd) or T coefficients (fwd) for f = b, ux, uz.
+void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
+  const int N = P->Nz;
+  const int ncol = 2 * P->Nk;
+  GemmBatch bt{};
+  for (int f = 0; f < 3; ++f) {
+    bt.in[f] = reinterpret_cast<const double*>(Xin + (size_t)f * P->plane);
+    bt.out[2 * f + 0] = reinterpret_cast<double*>(P->G.as<double2>() + (size_t)(2 * f) * P->plane);
+    bt.out[2 * f + 1] = reinterpret_cast<double*>(P->G.as<double2>() + (size_t)(2 * f + 1) * P->plane);
+  }
+  launch_gemm_f64(P->bwdstack.as<double>(), 2 * N, N, bt, 3, ncol, ncol, ncol, N, 2, P->st);
+  XProdArgs xa{};
+  for (int f = 0; f < 3; ++f) {
+    xa.val[f] = P->G.as<double2>() + (size_t)(2 * f) * P->plane;
+    xa.dz[f] = P->G.as<double2>() + (size_t)(2 * f + 1) * P->plane;
+    xa.out[f] = P->H.as<double2>() + (size_t)f * P->plane;
+  }
+  xa.tw = P->twM.as<double2>();
+  xa.fp = P->fpM;
+  xa.Nx = P->Nx;
+  xa.Nk = P->Nk;
+  xa.M = P->M;
+  xa.Nz = N;
+  xa.k0 = P->k0;
+  launch_xprod(xa, P->st);
+  GemmBatch bf{};
+  for (int f = 0; f < 3; ++f) {
+    bf.in[f] = reinterpret_cast<const double*>(P->H.as<double2>() + (size_t)f * P->plane);
+    bf.out[f] = reinterpret_cast<double*>(out3 + (size_t)f * P->plane);
+  }
+  launch_gemm_f64(c2rows ? P->sfwd.as<double>() : P->fwd.as<double>(), N, N, bf, 3, ncol, ncol, ncol, N, 1, P->st);
+}
+
+void enqueue_rk_step(tb_plan* P, double dt) {
+  const Tableau T = tableau(P->d.timestepper);
+  const double gamma = T.AI[1][1];
+  const double beta = dt * gamma;
+  FactorSet* fs = get_factors(P, 1.0, beta);  // done before capture by the caller
+  const long long cnt = 4LL * (long long)P->plane;
+  double2* X = P->X.as<double2>();
+  launch_mass_apply(X, P->MX0.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 0, P->st);
+  int nk = 1;
+  for (int i = 0; i < T.s; ++i) {
+    if (i > 0) {
+      LinComb lc{};
+      lc.in[lc.n] = P->MX0.as<double2>();
+      lc.w[lc.n++] = 1.0;
+      for (int j = 0; j < i; ++j) {
+        if (std::fabs(dt * T.AE[i][j]) > 1e-14) {
+          lc.in[lc.n] = P->FP[j].as<double2>();
+          lc.w[lc.n++] = dt * T.AE[i][j];
+        }
+        if (std::fabs(dt * T.AI[i][j]) > 1e-14) {
+          lc.in[lc.n] = P->LXP[j].as<double2>();
+          lc.w[lc.n++] = -dt * T.AI[i][j];
+        }
+      }
+      launch_lincomb(lc, P->LXP[i].as<double2>(), cnt, P->st);
+      TauArgs a = tau_args(P, fs, P->LXP[i].as<double2>());
+      launch_tau_solve(a, P->st);
+      launch_lx_finalize(P->LXP[i].as<double2>(), X, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, P->k0, P->s,
+                         P->d.kappa, P->d.nu, beta, P->st);
+      nk += 3;
+    }
+    enqueue_rhs(P, X, P->FP[i].as<double2>() + P->plane, true);
+    nk += 3;
+  }
+  LinComb lc{};
+  lc.in[lc.n] = P->MX0.as<double2>();
+  lc.w[lc.n++] = 1.0;
+  for (int j = 0; j < T.s; ++j) {
+    if (std::fabs(dt * T.bE[j]) > 1e-14) {
+      lc.in[lc.n] = P->FP[j].as<double2>();
+      lc.w[lc.n++] = dt * T.bE[j];
+    }
+    if (std::fabs(dt * T.bI[j]) > 1e-14) {
+      lc.in[lc.n] = P->LXP[j].as<double2>();
+      lc.w[lc.n++] = -dt * T.bI[j];
+    }
+  }
+  launch_rk_final(lc, X, P->tau.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->st);
+  nk += 1;
+  P->kernels_per_step = nk;
+}
+
+// SBDF1/SBDF2 coefficients for constant dt (step_subproblem_multistep.jl:536-553).
+struct SbdfCoefs {
+  double a0, a1, a2, c1, c2;
+};
+SbdfCoefs sbdf_coefs(int order, double dt) {
+  SbdfCoefs k{};
+  if (order == 1) {
+    k.a0 = 1.0 / dt;
+    k.a1 = -1.0 / dt;
+    k.c1 = 1.0;
+  } else {
+    const double w1 = 1.0;
+    k.a0 = (1.0 + 2.0 * w1) / ((1.0 + w1) * dt);
+    k.a1 = -(1.0 + w1) / dt;
+    k.a2 = w1 * w1 / ((1.0 + w1) * dt);
+    k.c1 = 1.0 + w1;
+    k.c2 = -w1;
+  }
+  return k;
+}
+
+// One SBDF step of the given order (1 or 2); history of (F, MX) in Fprev/MXprev.
+void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
+  const SbdfCoefs K = sbdf_coefs(order, dt);
+  const double a0 = K.a0, a1 = K.a1, a2 = K.a2, c1 = K.c1, c2 = K.c2;
+  FactorSet* fs = get_factors(P, a0, 1.0);
+  const long long cnt = 4LL * (long long)P->plane;
+  double2* X = P->X.as<double2>();
+  double2* Fcur = P->FP[0].as<double2>();
+  double2* MXcur = P->MX0.as<double2>();
+  enqueue_rhs(P, X, Fcur + P->plane, true);
+  launch_mass_apply(X, MXcur, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 1, P->st);
+  LinComb lc{};
+  lc.in[lc.n] = Fcur;
+  lc.w[lc.n++] = c1;
+  lc.in[lc.n] = MXcur;
+  lc.w[lc.n++] = -a1;
+  if (order == 2) {
+    lc.in[lc.n] = P->Fprev.as<double2>();
+    lc.w[lc.n++] = c2;
+    lc.in[lc.n] = P->MXprev.as<double2>();
+    lc.w[lc.n++] = -a2;
+  }
+  launch_lincomb(lc, P->Rsb.as<double2>(), cnt, P->st);
+  TauArgs a = tau_args(P, fs, P->Rsb.as<double2>());
+  launch_tau_solve(a, P->st);
+  TB_CUDA_TRY(cudaMemcpyAsync(P->Fprev.p, Fcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
+  TB_CUDA_TRY(cudaMemcpyAsync(P->MXprev.p, MXcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
+  P->kernels_per_step = 3 + 1 + 1 + 1;
+}
+
+void drop_graph(tb_plan* P) {
+  if (P->gexec) cudaGraphExecDestroy(P->gexec);
+  P->gexec = nullptr;
+  P->graph_dt = -1.0;
+  P->graph_kind = -1;
+}
+
+// Capture one step of `kind` (0 = RK, 1 = SBDF1, 2 = SBDF2) for dt.
+void capture_step(tb_plan* P, double dt, int kind) {
+  drop_graph(P);
+  cudaGraph_t g = nullptr;
+  TB_CUDA_TRY(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeThreadLocal));
+  try {
+    if (kind == 0)
+      enqueue_rk_step(P, dt);
+    else
+      enqueue_sbdf_step(P, dt, kind);
+  } catch (...) {
+    cudaStreamEndCapture(P->st, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  TB_CUDA_TRY(cudaStreamEndCapture(P->st, &g));
+  cudaError_t e = cudaGraphInstantiate(&P->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) throw Error{TB_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+  P->graph_dt = dt;
+  P->graph_kind = kind;
+}
+
+void validate_desc(const tb_problem_desc* d) {
+  TB_REQUIRE(d != nullptr, TB_EINVAL, "null problem descriptor");
+  TB_REQUIRE(d->ndim == 2, TB_ENOTSUPPORTED, "only 2D Fourier x Chebyshev plans are implemented");
+  TB_REQUIRE(d->program == TB_PROGRAM_RBC, TB_ENOTSUPPORTED, "unknown equation program");
+  TB_REQUIRE(d->Nx >= 6 && d->Nx % 2 == 0, TB_EINVAL, "Nx must be even and >= 6");
+  TB_REQUIRE(d->Nz >= 8 && d->Nz <= 32767, TB_EINVAL, "Nz must be in [8, 32767]");
+  TB_REQUIRE(d->Lx > 0 && d->Lz > 0, TB_EINVAL, "domain lengths must be positive");
+  TB_REQUIRE(std::fabs(d->dealias - 1.5) < 1e-12, TB_ENOTSUPPORTED, "only dealias = 3/2 is implemented");
+  TB_REQUIRE(d->timestepper >= TB_RK222 && d->timestepper <= TB_SBDF2, TB_EINVAL, "unknown timestepper");
+  TB_REQUIRE(d->precision == TB_PREC_F64, TB_ENOTSUPPORTED, "precision mode not implemented in this build");
+  TB_REQUIRE(d->kappa > 0 && d->nu > 0, TB_EINVAL, "kappa and nu must be positive");
+}
+
+}  // namespace
+
+extern "C" {
+
+int tb_version(void) { return 1; }
+
+const char* tb_status_string(tb_status s) {
+  switch (s) {
+    case TB_OK: return "ok";
+    case TB_EINVAL: return "invalid argument";
+    case TB_ENOMEM: return "out of device memory";
+    case TB_ESINGULAR: return "singular tau system";
+    case TB_ETIMEOUT: return "device wait timed out";
+    case TB_ECUDA: return "CUDA error";
+    case TB_ENOTSUPPORTED: return "not supported";
+    case TB_EBUDGET: return "over HBM budget";
+    case TB_ESTATE: return "invalid call order";
+    default: return "unknown status";
+  }
+}
+
+tb_status tb_context_create(int device, tb_context** out) {
+  if (!out) return TB_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    g_err = std::string("no CUDA device: ") + cudaGetErrorString(e);
+    return TB_ECUDA;
+  }
+  if (device < 0 || device >= ndev) {
+    g_err = "device index out of range";
+    return TB_EINVAL;
+  }
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    g_err = cudaGetErrorString(e);
+    return TB_ECUDA;
+  }
+  tb_context* c = new (std::nothrow) tb_context();
+  if (!c) return TB_ENOMEM;
+  c->device = device;
+  *out = c;
+  return TB_OK;
+}
+
+tb_status tb_context_destroy(tb_context* ctx) {
+  delete ctx;
+  return TB_OK;
+}
+
+const char* tb_last_error(const tb_context* ctx) { return ctx ? ctx->last_error.c_str() : g_err.c_str(); }
+
+tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan** out) {
+  if (!ctx || !out) return TB_EINVAL;
+  *out = nullptr;
+  std::unique_ptr<tb_plan> P(new (std::nothrow) tb_plan());
+  if (!P) return TB_ENOMEM;
+  tb_status s = guard(ctx, [&] {
+    validate_desc(desc);
+    TB_CUDA_TRY(cudaSetDevice(ctx->device));
+    P->ctx = ctx;
+    P->d = *desc;
+    P->Nx = desc->Nx;
+    P->Nz = desc->Nz;
+    P->Nk = desc->Nx / 2 + 1;
+    int M = (int)std::ceil(1.5 * desc->Nx);
+    if (M % 2) ++M;
+    P->M = M;
+    P->k0 = 2.0 * M_PI / desc->Lx;
+    P->s = 2.0 / desc->Lz;
+    P->plane = (size_t)P->Nz * P->Nk;
+    TB_REQUIRE(make_fft_plan(P->M, &P->fpM) && make_fft_plan(P->Nx, &P->fpN), TB_ENOTSUPPORTED,
+               "Nx must be of the form 2^a 3^b");
+    TB_REQUIRE(xprod_smem_bytes(P->M) <= 227 * 1024, TB_ENOTSUPPORTED, "Nx too large for the fused x kernel");
+    TB_CUDA_TRY(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
+    TB_CUDA_TRY(cudaEventCreate(&P->ev0));
+    TB_CUDA_TRY(cudaEventCreate(&P->ev1));
+    TB_CUDA_TRY(set_transform_smem_limits(227 * 1024));
+    // transforms
+    ChebMats cm = build_cheb_mats(P->Nz, desc->Lz);
+    std::vector<double> stack(cm.bwd);
+    stack.insert(stack.end(), cm.bwd_d.begin(), cm.bwd_d.end());
+    upload(P->bwdstack, stack);
+    upload(P->bwd, cm.bwd);
+    upload(P->fwd, cm.fwd);
+    upload(P->sfwd, cm.sfwd);
+    upload(P->s3, cm.s3);
+    upload(P->twM, twiddles(P->M));
+    upload(P->twN, twiddles(P->Nx));
+    // tau layout
+    P->lay = build_rbc_layout(P->Nz, desc->Lx, desc->Lz, desc->kappa, desc->nu, (double)desc->Nx,
+                              desc->b_bottom, desc->b_top);
+    for (int c = 0; c < 2; ++c) {
+      const ClassLayout& L = P->lay.cls[c];
+      TB_REQUIRE(L.kl <= kTauKL && L.ku <= kTauKU && L.nb <= 4, TB_ENOTSUPPORTED, "unexpected tau band shape");
+      // pad the band template to the compiled (kTauKL, kTauKU) shape
+      const int WC = kTauKL + kTauKU + 1;
+      std::vector<Coef> band((size_t)L.n * WC, Coef{0, 0, 0, 0});
+      for (int r = 0; r < L.n; ++r)
+        for (int d = 0; d < L.kl + L.ku + 1; ++d)
+          band[(size_t)r * WC + (d - L.kl + kTauKL)] = L.band[(size_t)r * (L.kl + L.ku + 1) + d];
+      P->lay.cls[c].band = band;
+      P->lay.cls[c].kl = kTauKL;
+      P->lay.cls[c].ku = kTauKU;
+      auto to_short = [](const std::vector<int>& v) { return std::vector<short>(v.begin(), v.end()); };
+      ClassTables& T = P->ct[c];
+      upload(T.row_eq, to_short(L.row_eq));
+      upload(T.row_k, to_short(L.row_k));
+      upload(T.col_unk, to_short(L.col_unk));
+      upload(T.col_k, to_short(L.col_k));
+      upload(T.left_unk, to_short(L.left_unk));
+      upload(T.left_k, to_short(L.left_k));
+      upload(T.bc_rhs, L.bc_rhs);
+      upload(T.band, band);
+      upload(T.bord, L.bord);
+      upload(T.c2_z, L.c2_z);
+      upload(T.c2_nz, L.c2_nz);
+      upload(T.c1_z, L.c1_z);
+      upload(T.c1_nz, L.c1_nz);
+    }
+    P->err_mode.alloc(sizeof(int));
+    // state and work arrays
+    const size_t pb = P->plane * sizeof(double2);
+    P->X.alloc(4 * pb);
+    P->tau.alloc(7 * P->Nk * sizeof(double2));
+    P->G.alloc(6 * pb);
+    P->H.alloc(3 * pb);
+    P->MX0.alloc(4 * pb);
+    for (int i = 0; i < 4; ++i) {
+      P->FP[i].alloc(4 * pb);
+      P->LXP[i].alloc(4 * pb);
+    }
+    const bool sbdf = desc->timestepper == TB_SBDF1 || desc->timestepper == TB_SBDF2;
+    if (sbdf) {
+      P->Fprev.alloc(4 * pb);
+      P->MXprev.alloc(4 * pb);
+      P->Rsb.alloc(4 * pb);
+    }
+    P->tmpgrid.alloc(P->plane * sizeof(double2));
+    TB_CUDA_TRY(cudaMemsetAsync(P->X.p, 0, P->X.bytes, P->st));
+    TB_CUDA_TRY(cudaMemsetAsync(P->tau.p, 0, P->tau.bytes, P->st));
+    TB_CUDA_TRY(cudaMemsetAsync(P->MX0.p, 0, P->MX0.bytes, P->st));
+    for (int i = 0; i < 4; ++i) {
+      TB_CUDA_TRY(cudaMemsetAsync(P->FP[i].p, 0, P->FP[i].bytes, P->st));
+      TB_CUDA_TRY(cudaMemsetAsync(P->LXP[i].p, 0, P->LXP[i].bytes, P->st));
+    }
+    if (sbdf) {
+      TB_CUDA_TRY(cudaMemsetAsync(P->Fprev.p, 0, P->Fprev.bytes, P->st));
+      TB_CUDA_TRY(cudaMemsetAsync(P->MXprev.p, 0, P->MXprev.bytes, P->st));
+    }
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  });
+  if (s != TB_OK) return s;
+  *out = P.release();
+  return TB_OK;
+}
+
+tb_status tb_plan_destroy(tb_plan* plan) {
+  if (!plan) return TB_OK;
+  cudaStreamSynchronize(plan->st);
+  delete plan;
+  return TB_OK;
+}
+
+tb_status tb_set_state(tb_plan* P, int field, const void* data, int where) {
+  if (!P || !data) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_REQUIRE(field >= TB_FIELD_B && field <= TB_FIELD_TAU, TB_EINVAL, "bad field selector");
+    void* dst = field == TB_FIELD_TAU ? P->tau.p : (void*)P->Xp(field);
+    size_t bytes = field == TB_FIELD_TAU ? P->tau.bytes : P->plane * sizeof(double2);
+    TB_CUDA_TRY(cudaMemcpyAsync(dst, data, bytes, where == TB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                P->st));
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+    P->ms_history = 0;  // a new state restarts multistep history
+  });
+}
+
+tb_status tb_get_state(tb_plan* P, int field, void* data, int where) {
+  if (!P || !data) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_REQUIRE(field >= TB_FIELD_B && field <= TB_FIELD_TAU, TB_EINVAL, "bad field selector");
+    const void* src = field == TB_FIELD_TAU ? P->tau.p : (const void*)P->Xp(field);
+    size_t bytes = field == TB_FIELD_TAU ? P->tau.bytes : P->plane * sizeof(double2);
+    TB_CUDA_TRY(cudaMemcpyAsync(data, src, bytes, where == TB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                P->st));
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  });
+}
+
+tb_status tb_step(tb_plan* P, double dt, int nsteps) {
+  if (!P) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_REQUIRE(dt > 0 && std::isfinite(dt), TB_EINVAL, "dt must be positive and finite");
+    TB_REQUIRE(nsteps >= 0, TB_EINVAL, "nsteps must be >= 0");
+    TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
+    const int ts = P->d.timestepper;
+    TB_CUDA_TRY(cudaEventRecord(P->ev0, P->st));
+    for (int i = 0; i < nsteps; ++i) {
+      int kind = 0;
+      if (ts == TB_SBDF1) kind = 1;
+      if (ts == TB_SBDF2) kind = (P->ms_history >= 1) ? 2 : 1;
+      if (kind == 0) {
+        const Tableau T = tableau(ts);
+        get_factors(P, 1.0, dt * T.AI[1][1]);
+      } else {
+        get_factors(P, sbdf_coefs(kind, dt).a0, 1.0);
+      }
+      if (!(P->gexec && P->graph_dt == dt && P->graph_kind == kind)) capture_step(P, dt, kind);
+      TB_CUDA_TRY(cudaGraphLaunch(P->gexec, P->st));
+      P->sim_time += dt;
+      P->iteration += 1;
+      if (kind != 0) P->ms_history = 1;
+    }
+    TB_CUDA_TRY(cudaEventRecord(P->ev1, P->st));
+    TB_CUDA_TRY(cudaEventSynchronize(P->ev1));
+    TB_CUDA_TRY(cudaEventElapsedTime(&P->last_ms, P->ev0, P->ev1));
+    TB_CUDA_TRY(cudaGetLastError());
+  });
+}
+
+tb_status tb_sim_time(const tb_plan* P, double* t, long long* it) {
+  if (!P) return TB_EINVAL;
+  if (t) *t = P->sim_time;
+  if (it) *it = P->iteration;
+  return TB_OK;
+}
+
+tb_status tb_synchronize(tb_plan* P) {
+  if (!P) return TB_EINVAL;
+  return guard(P->ctx, [&] { TB_CUDA_TRY(cudaStreamSynchronize(P->st)); });
+}
+
+tb_status tb_last_step_ms(const tb_plan* P, float* ms) {
+  if (!P || !ms) return TB_EINVAL;
+  *ms = P->last_ms;
+  return TB_OK;
+}
+
+tb_status tb_set_profiling(tb_plan* P, int on) {
+  (void)on;
+  return P ? TB_OK : TB_EINVAL;
+}
+
+tb_status tb_kernel_times(tb_plan* P, double* out3, int reset) {
+  (void)reset;
+  if (!P || !out3) return TB_EINVAL;
+  out3[0] = out3[1] = out3[2] = 0.0;
+  return TB_OK;
+}
+
+tb_status tb_tau_layout_query(int Nz, double Lx, double Lz, int cls, int* info4) {
+  if (!info4 || cls < 0 || cls > 1) return TB_EINVAL;
+  if (Nz < 8 || Nz > 32767 || !(Lx > 0) || !(Lz > 0)) return TB_EINVAL;
+  try {
+    TauLayout L = build_rbc_layout(Nz, Lx, Lz, 1.0, 1.0, 1.0, 0.0, 0.0);
+    info4[0] = L.cls[cls].n;
+    info4[1] = L.cls[cls].nb;
+    info4[2] = L.cls[cls].kl;
+    info4[3] = L.cls[cls].ku;
+    return TB_OK;
+  } catch (const Error& e) {
+    g_err = e.msg;
+    return e.code;
+  }
+}
+
+tb_status tb_kernels_per_step(const tb_plan* P, int* n) {
+  if (!P || !n) return TB_EINVAL;
+  *n = P->kernels_per_step;
+  return TB_OK;
+}
+
+tb_status tb_transform_forward(tb_plan* P, const double* grid, double* coeff, int nfields) {
+  if (!P || !grid || !coeff || nfields < 1) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    const size_t gsz = (size_t)P->Nz * P->Nx;
+    for (int f = 0; f < nfields; ++f) {
+      double2* mixed = P->tmpgrid.as<double2>();
+      launch_x_rfft(grid + f * gsz, mixed, P->Nz, P->Nx, P->fpN, P->twN.as<double2>(), P->st);
+      GemmBatch bt{};
+      bt.in[0] = reinterpret_cast<const double*>(mixed);
+      bt.out[0] = coeff + f * 2 * P->plane;
+      launch_gemm_f64(P->fwd.as<double>(), P->Nz, P->Nz, bt, 1, 2 * P->Nk, 2 * P->Nk, 2 * P->Nk, P->Nz, 1, P->st);
+      check_launch("transform forward");
+    }
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  });
+}
+
+tb_status tb_transform_backward(tb_plan* P, const double* coeff, double* grid, int nfields) {
+  if (!P || !grid || !coeff || nfields < 1) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    const size_t gsz = (size_t)P->Nz * P->Nx;
+    for (int f = 0; f < nfields; ++f) {
+      double2* mixed = P->tmpgrid.as<double2>();
+      GemmBatch bt{};
+      bt.in[0] = coeff + f * 2 * P->plane;
+      bt.out[0] = reinterpret_cast<double*>(mixed);
+      launch_gemm_f64(P->bwd.as<double>(), P->Nz, P->Nz, bt, 1, 2 * P->Nk, 2 * P->Nk, 2 * P->Nk, P->Nz, 1, P->st);
+      launch_x_irfft(mixed, grid + f * gsz, P->Nz, P->Nx, P->fpN, P->twN.as<double2>(), P->st);
+      check_launch("transform backward");
+    }
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  });
+}
+
+tb_status tb_dealiased_multiply(tb_plan* P, const double* a, const double* b, double* out) {
+  if (!P || !a || !b || !out) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    launch_x_dealias_mul(a, b, out, P->Nz, P->Nx, P->M, P->fpN, P->twN.as<double2>(), P->fpM,
+                         P->twM.as<double2>(), P->st);
+    check_launch("dealiased multiply");
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  });
+}
+
+tb_status tb_rhs_advection(tb_plan* P, const double* coeff_in, double* coeff_out) {
+  if (!P || !coeff_in || !coeff_out) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    enqueue_rhs(P, reinterpret_cast<const double2*>(coeff_in), reinterpret_cast<double2*>(coeff_out), false);
+    check_launch("rhs advection");
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  });
+}
+
+}  // extern "C"
