@@ -1,0 +1,451 @@
+#!/usr/bin/env python
+"""Throughput of the 2D Rayleigh-Benard IMEX timestep on B200 (steps/s).
+
+Workload (default): ChannelDomain(1024, 256; Lx=4, Lz=1), Boussinesq with tau/lift
+boundary conditions, Ra=1e8, Pr=1, RK443, dt=0.01, Float64, seeded initial noise
+1e-3 z(Lz-z) (the 1024x256 Rayleigh-Benard configuration of the benchmark plan).
+One "step" is one timestep of that problem; the step is a CUDA graph replayed by
+the library.  With N GPUs each rank runs an independent replica (the 2D path has
+no cross-GPU exchange), the timed region is bracketed by barriers and the
+device time is the max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `--impl reference` times the CPU restatement of
+the reference's algorithm (oracle/, NumPy + SciPy SuperLU, single thread) on the
+same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=None)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scheme", choices=["RK443", "RK222", "SBDF2"], default="RK443")
+    ap.add_argument("--config", choices=["c2", "c1"], default="c2")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only; used for the barrier and the max)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clock sampling during the timed region (NVML)
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    REASONS = {
+        "gpu_idle": 0x1,
+        "applications_clocks_setting": 0x2,
+        "sw_power_cap": 0x4,
+        "hw_slowdown": 0x8,
+        "sync_boost": 0x10,
+        "sw_thermal_slowdown": 0x20,
+        "hw_thermal_slowdown": 0x40,
+        "hw_power_brake_slowdown": 0x80,
+    }
+
+    def __init__(self, device: int, period: float = 0.005):
+        self.device, self.period = device, period
+        self.samples, self.reasons = [], set()
+        self._stop = threading.Event()
+        self.ok = False
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, bit in self.REASONS.items():
+                    if r & bit and name != "gpu_idle":
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# per-kernel algorithmic work (bytes moved by the algorithm, or flops)
+# ---------------------------------------------------------------------------
+def kernel_work(name: str, cfg, scheme: str):
+    """(kind, amount per launch) with kind 'bytes' or 'flops'."""
+    nk = cfg.Nx // 2 + 1
+    plane = cfg.Nz * nk * 16
+    N = cfg.Nz
+    nb = {0: 3, 1: 4}
+    n = 2 * N  # band rows per parity class
+    if name == "z_backward_gemm":
+        return "flops", 2.0 * (2 * N) * N * (2 * nk) * 3
+    if name == "z_forward_gemm":
+        return "flops", 2.0 * N * N * (2 * nk) * 3
+    if name == "x_fft_products":
+        return "bytes", 9.0 * plane
+    if name == "tau_solve":
+        # factors: pivots (1 B) + L (4) + U (13) + border (nb) + C multipliers (nb) doubles per row,
+        # Schur inverse; rhs read (4 planes) and unknowns written (4 planes + taus)
+        fac = sum(nk * (n * (1 + 8 * (4 + 13 + 2 * nb[c])) + 8 * nb[c] ** 2) for c in (0, 1))
+        return "bytes", fac + 4.0 * plane + 4.0 * plane
+    if name == "stage_lincomb":
+        return "bytes", None  # depends on the stage; reported only if dominant
+    if name == "lx_finalize":
+        return "bytes", (4 + 3 + 4) * plane
+    if name == "rk_final":
+        return "bytes", None
+    if name == "mass_apply":
+        return "bytes", (3 + 4) * plane
+    return "bytes", None
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, cfg, scheme, dist):
+    """CPU restatement of the reference's algorithm, timed on the host cores."""
+    if dist.rank != 0:
+        return
+    from oracle.tarang_oracle import RBCParams, run_rbc, rbc_initial_b, RBC2D
+
+    p = RBCParams(Nx=cfg.Nx, Nz=cfg.Nz, Lx=cfg.Lx, Lz=cfg.Lz, Ra=cfg.Ra, Pr=cfg.Pr)
+    sim = RBC2D(p)
+    sim.set_b_grid(rbc_initial_b(p, cfg.seed))
+    for _ in range(args.warmup):
+        sim.step(cfg.dt, scheme)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.step(cfg.dt, scheme)
+    el = time.perf_counter() - t0
+    v = args.steps / el
+    out = {
+        "impl": "reference",
+        "metric": f"RBC 2D steps/s ({cfg.Nx}x{cfg.Nz}, {scheme}, Float64)",
+        "value": v,
+        "unit": "steps/s",
+        "n_gpus": 0,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 / v,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded PCG64 noise)",
+        "config": workload_config(cfg, scheme, args),
+        "cpu_baseline": {
+            "value": v,
+            "unit": "steps/s",
+            "cores": 1,
+            "kind": "port",
+            "sample": f"{args.steps} steps after {args.warmup} warm-up steps (the first factors the tau LHS) "
+                      f"of the full {cfg.Nx}x{cfg.Nz} problem; NumPy/SciPy restatement (SuperLU per mode), "
+                      "single thread; Julia is absent so the reference itself cannot run",
+        },
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def workload_config(cfg, scheme, args):
+    return {
+        "workload": f"2D Rayleigh-Benard {cfg.Nx}x{cfg.Nz} Float64 {scheme} dt={cfg.dt}",
+        "Nx": cfg.Nx,
+        "Nz": cfg.Nz,
+        "Lx": cfg.Lx,
+        "Lz": cfg.Lz,
+        "Ra": cfg.Ra,
+        "Pr": cfg.Pr,
+        "dt": cfg.dt,
+        "timestepper": scheme,
+        "dealias": 1.5,
+        "global_batch": 1 if args.gpus in (None, 1) else args.gpus,
+        "parallelism": "replicas",
+        "l2": "working set (state, stage vectors, tau factors ~0.2 GB) exceeds the 126 MB L2",
+    }
+
+
+def cpu_baseline(cfg, scheme, nsteps):
+    from oracle.tarang_oracle import RBCParams, RBC2D, rbc_initial_b
+
+    p = RBCParams(Nx=cfg.Nx, Nz=cfg.Nz, Lx=cfg.Lx, Lz=cfg.Lz, Ra=cfg.Ra, Pr=cfg.Pr)
+    sim = RBC2D(p)
+    sim.set_b_grid(rbc_initial_b(p, cfg.seed))
+    sim.step(cfg.dt, scheme)  # warm-up: includes the per-mode sparse LU factorisation
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        sim.step(cfg.dt, scheme)
+    el = time.perf_counter() - t0
+    return {
+        "value": nsteps / el,
+        "unit": "steps/s",
+        "cores": 1,
+        "kind": "port",
+        "sample": f"{nsteps} steps of the full {cfg.Nx}x{cfg.Nz} {scheme} problem after one warm-up step; "
+                  "NumPy/SciPy restatement of the reference CPU path (SuperLU per Fourier mode), single thread",
+    }
+
+
+def run_ours(args, cfg, scheme, dist):
+    import numpy as np
+    import torch
+
+    from __graft_entry__ import load_package
+
+    tb = load_package()
+    from tarang_b200 import workloads as W
+    from tarang_b200._lib import TB_FIELD_B, TB_FIELD_P, TB_FIELD_TAU, TB_FIELD_UX, TB_FIELD_UZ
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    dom = tb.ChannelDomain(cfg.Nx, cfg.Nz, Lx=cfg.Lx, Lz=cfg.Lz, arch=tb.GPU(dev))
+    ts = {"RK222": 0, "RK443": 1, "SBDF2": 3}[scheme]
+    plan = tb.Plan(dom, cfg.kappa, cfg.nu, cfg.Lz, 0.0, ts)
+    b0 = plan.forward(W.rbc_initial_grid(cfg))
+    plan.set_state(TB_FIELD_B, b0)
+
+    # warm-up (the first call factors the tau systems and captures the step graph)
+    plan.step(cfg.dt, args.warmup)
+
+    # timed region: K graph replays, device time from CUDA events on the plan's stream
+    dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        plan.step(cfg.dt, args.steps)
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms_local = plan.last_step_ms()
+    ms = dist.max(ms_local)
+    value = dist.world * args.steps / (ms / 1e3)
+    kps = plan.kernels_per_step()
+
+    # per-kernel breakdown (eager launches with CUDA events around each kernel)
+    nprof = max(3, min(20, args.steps))
+    plan.set_profiling(True)
+    plan.step(cfg.dt, nprof)
+    prof = plan.profile()
+    plan.set_profiling(False)
+    tot = sum(v[0] for v in prof.values())
+    shares = {k: v[0] / tot for k, v in prof.items()}
+    top = max(prof, key=lambda k: prof[k][0])
+    peaks, peak_src = measured_peaks()
+    kind, work = kernel_work(top, cfg, scheme)
+    avg_ms = prof[top][0] / prof[top][1]
+    roof = None
+    if work is not None:
+        if kind == "bytes":
+            ach = work / (avg_ms / 1e3) / 1e9
+            peak = peaks.get("hbm_gbs")
+            roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                    "traffic": None, "kernel": top, "algorithmic_bytes_per_launch": work}
+        else:
+            ach = work / (avg_ms / 1e3) / 1e12
+            peak = fp64_peak_tflops()
+            roof = {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                    "frac": ach / peak if peak else None, "traffic": None, "kernel": top,
+                    "flops_per_launch": work, "peak_source": "cuBLAS FP64 GEMM (torch.matmul float64) measured in bench"}
+        roof["avg_launch_ms"] = avg_ms
+        roof["peak_source"] = roof.get("peak_source", f"MEASURED_PEAKS.json ({peak_src})")
+    model = W.step_model_bytes(cfg, scheme)
+    step_roof = {"bytes_per_step_model": model, "achieved_gbs": model / (ms / args.steps / 1e3) / 1e9,
+                 "peak_gbs": peaks.get("hbm_gbs")}
+    step_roof["frac"] = step_roof["achieved_gbs"] / step_roof["peak_gbs"]
+
+    # end to end through the C ABI with host buffers: per step, upload the state
+    # from pinned host memory, one step, download the state
+    nk = cfg.Nx // 2 + 1
+    host = {f: torch.empty((cfg.Nz, nk), dtype=torch.complex128, pin_memory=True).numpy()
+            for f in (TB_FIELD_B, TB_FIELD_UX, TB_FIELD_UZ, TB_FIELD_P)}
+    host[TB_FIELD_TAU] = torch.empty((7, nk), dtype=torch.complex128, pin_memory=True).numpy()
+    for f in host:
+        host[f][...] = plan.get_state(f)
+    ne = args.e2e_steps
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(ne):
+        for f, a in host.items():
+            plan.set_state(f, a)
+        plan.step(cfg.dt, 1)
+        for f in host:
+            tb.lib.tb_get_state(plan.ptr, f, host[f].ctypes.data_as(__import__("ctypes").c_void_p), 0)
+    e2e_el = dist.max(time.perf_counter() - t0)
+    sbytes = W.state_bytes(cfg)
+    e2e = {"value": dist.world * ne / e2e_el, "unit": "steps/s", "h2d_bytes_per_step": sbytes,
+           "d2h_bytes_per_step": sbytes, "steps": ne,
+           "what": "per step: tb_set_state of b,ux,uz,p,taus from pinned host memory, tb_step(1), "
+                   "tb_get_state of all fields to host"}
+
+    finite = all(np.isfinite(plan.get_state(f)).all() for f in (TB_FIELD_B, TB_FIELD_UZ))
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(cfg, scheme, args.cpu_steps)
+    if dist.rank == 0:
+        out = {
+            "metric": f"RBC 2D steps/s ({cfg.Nx}x{cfg.Nz}, {scheme}, Float64)",
+            "value": value,
+            "unit": "steps/s",
+            "n_gpus": dist.world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded PCG64 noise, the benchmark configuration's initial condition)",
+            "config": workload_config(cfg, scheme, args),
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "gpu_launches": kps * args.steps,
+            "kernels_per_step": kps,
+            "roofline": roof,
+            "step_roofline": step_roof,
+            "kernel_shares": {k: round(v, 4) for k, v in sorted(shares.items(), key=lambda x: -x[1])},
+            "kernel_avg_ms": {k: prof[k][0] / prof[k][1] for k in prof},
+            "cpu_baseline": cpu,
+            "finite": bool(finite),
+        }
+        print(json.dumps(out), flush=True)
+
+
+_FP64_PEAK = None
+
+
+def fp64_peak_tflops():
+    global _FP64_PEAK
+    if _FP64_PEAK is None:
+        import torch
+
+        n = 8192
+        a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = 1e30
+        for _ in range(3):
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        _FP64_PEAK = 2.0 * n ** 3 / (best / 1e3) / 1e12
+        del a, b
+    return _FP64_PEAK
+
+
+def main():
+    args = parse_args()
+    dist = Dist()
+    if args.gpus is None:
+        args.gpus = dist.world
+    sys.path.insert(0, os.path.join(ROOT, "tarang.jl_b200"))
+    from __graft_entry__ import load_package
+
+    if args.impl == "ours":
+        load_package()
+    import importlib
+
+    spec = importlib.util.spec_from_file_location("tb_workloads", os.path.join(ROOT, "tarang.jl_b200", "workloads.py"))
+    W = importlib.util.module_from_spec(spec)
+    sys.modules["tb_workloads"] = W
+    spec.loader.exec_module(W)
+    cfg = W.C2 if args.config == "c2" else W.C1
+    scheme = args.scheme if args.config == "c2" else "RK222"
+    try:
+        if args.impl == "reference":
+            run_reference(args, cfg, scheme, dist)
+        else:
+            run_ours(args, cfg, scheme, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -110,12 +110,18 @@ tb_status tb_sim_time(const tb_plan* plan, double* t, long long* iteration);
 tb_status tb_synchronize(tb_plan* plan);
 
 /* Device-side timing of the last tb_step call in milliseconds (CUDA events on
- * the plan's stream), and a per-kernel-class breakdown accumulated since the
- * last reset: out[0] transforms+products, out[1] tau solves, out[2] stage
- * updates (filled only when profiling is on, which disables graph replay). */
+ * the plan's stream). */
 tb_status tb_last_step_ms(const tb_plan* plan, float* ms);
+/* Per-kernel timing (the library's own tracing, standing in for the
+ * reference's opt-in transform counters, transform_fourier.jl:49-65).  With
+ * profiling on, tb_step launches the step eagerly (no graph replay) with CUDA
+ * events around every kernel and accumulates (total ms, launches) per kernel
+ * name; entries are listed in name order. */
 tb_status tb_set_profiling(tb_plan* plan, int on);
-tb_status tb_kernel_times(tb_plan* plan, double* out3, int reset);
+tb_status tb_profile_count(const tb_plan* plan, int* n);
+tb_status tb_profile_entry(const tb_plan* plan, int i, char* name, int name_len, double* ms_total,
+                           long long* launches);
+tb_status tb_profile_reset(tb_plan* plan);
 /* Host-only query of the banded layout the plan compiler builds for the RBC
  * tau system (no GPU needed): info4 = {band rows n, border size nb, kl, ku}
  * for parity class cls (0 or 1). */

@@ -27,6 +27,8 @@ from typing import Dict, List, Optional, Sequence, Tuple
 import numpy as np
 import scipy.fft as sfft
 import scipy.linalg as sla
+import scipy.sparse as sps
+import scipy.sparse.linalg as spsl
 
 # ---------------------------------------------------------------------------
 # Grids and wavenumbers
@@ -329,67 +331,71 @@ class RBC2D:
         return 4 * self.p.Nz + (7 if m == 0 else 6)
 
     def mode_matrices(self, m: int):
-        """Dense M, L (complex), BC-row index list and ALG_F for Fourier mode m."""
+        """Sparse (CSR) M, L (complex), BC-row index list and ALG_F for Fourier mode m.
+
+        Same entries the reference's build_matrices! assembles for this system
+        (matrices_subproblem_operators.jl:19-330), including the 1e-12 entry
+        cutoff applied to every block entry (subproblem_matrix_build.jl:88-100).
+        """
         if m in self._mats:
             return self._mats[m]
         p = self.p
         N = p.Nz
         kx = self.kx[m]
         ikx = 1j * kx
-        D, D2 = self.D, self.D2
-        I = np.eye(N)
-        eN1 = np.zeros(N)
-        eN1[N - 1] = 1.0  # lift(., -1) -> unit column e_{N-1} (matrices_subproblem_operators.jl:218-260)
-        De = D @ eN1
         has_tp = m == 0
         ntau = 7 if has_tp else 6
         n = 4 * N + ntau
-        # column offsets
         cp, cb, cux, cuz = 0, N, 2 * N, 3 * N
-        t0 = 4 * N
-        tcol = {}
         names = self.TAU_NAMES if has_tp else self.TAU_NAMES[1:]
-        for i, nm in enumerate(names):
-            tcol[nm] = t0 + i
-        # row offsets
-        rc, rb, rx, rz = 0, N, 2 * N, 3 * N
-        r_bc = 4 * N
-        M = np.zeros((n, n), complex)
-        L = np.zeros((n, n), complex)
+        tcol = {nm: 4 * N + i for i, nm in enumerate(names)}
+        rc, rb, rx, rz, r_bc = 0, N, 2 * N, 3 * N, 4 * N
         kap, nu = p.kappa, p.nu
-        lap = -kx * kx * I + D2
+        Lr, Lc, Lv = [], [], []
+        idx = np.arange(N)
+        dr, dc = np.nonzero(self.D)
+        d2r, d2c = np.nonzero(self.D2)
+        De = self.D[:, N - 1]
+        der = np.nonzero(De)[0]
+
+        def add(r0, c0, rr, cc, vv):
+            vv = np.broadcast_to(np.asarray(vv, dtype=complex), np.shape(rr))
+            keep = np.abs(vv) >= 1e-12  # entry cutoff
+            Lr.append(r0 + np.asarray(rr)[keep])
+            Lc.append(c0 + np.asarray(cc)[keep])
+            Lv.append(vv[keep])
+
+        def lap_block(r0, c0, coef):
+            # coef * (-kx^2 I + D2): diagonal and strictly-upper parts are disjoint
+            add(r0, c0, idx, idx, -coef * kx * kx * np.ones(N))
+            add(r0, c0, d2r, d2c, coef * self.D2[d2r, d2c])
+
         # trace(grad_u) + tau_p = 0
-        L[rc : rc + N, cux : cux + N] += ikx * I
-        L[rc : rc + N, cuz : cuz + N] += D
-        L[rc : rc + N, tcol["tau_u1z"]] += eN1
+        add(rc, cux, idx, idx, ikx * np.ones(N))
+        add(rc, cuz, dr, dc, self.D[dr, dc])
+        add(rc, tcol["tau_u1z"], [N - 1], [0], [1.0])
         if has_tp:
-            L[rc, tcol["tau_p"]] += 1.0  # 0-D field -> T_0 row (subproblem_expr_helpers.jl:189-193)
+            add(rc, tcol["tau_p"], [0], [0], [1.0])  # 0-D field -> T_0 row (subproblem_expr_helpers.jl:189-193)
         # dt(b) - kappa div(grad_b) + lift(tau_b2) = -u.grad(b)
-        M[rb : rb + N, cb : cb + N] += I
-        L[rb : rb + N, cb : cb + N] += -kap * lap
-        L[rb : rb + N, tcol["tau_b1"]] += -kap * De
-        L[rb : rb + N, tcol["tau_b2"]] += eN1
+        lap_block(rb, cb, -kap)
+        add(rb, tcol["tau_b1"], der, np.zeros_like(der), -kap * De[der])
+        add(rb, tcol["tau_b2"], [N - 1], [0], [1.0])
         # dt(u) - nu div(grad_u) + grad(p) - b ez + lift(tau_u2) = -u.grad(u)
-        M[rx : rx + N, cux : cux + N] += I
-        L[rx : rx + N, cux : cux + N] += -nu * lap
-        L[rx : rx + N, tcol["tau_u1x"]] += -nu * De
-        L[rx : rx + N, cp : cp + N] += ikx * I
-        L[rx : rx + N, tcol["tau_u2x"]] += eN1
-        M[rz : rz + N, cuz : cuz + N] += I
-        L[rz : rz + N, cuz : cuz + N] += -nu * lap
-        L[rz : rz + N, tcol["tau_u1z"]] += -nu * De
-        L[rz : rz + N, cp : cp + N] += D
-        L[rz : rz + N, cb : cb + N] += -I
-        L[rz : rz + N, tcol["tau_u2z"]] += eN1
-        # boundary conditions (Interpolate rows, T_n(-1) at z=0 and T_n(1) at z=Lz)
+        lap_block(rx, cux, -nu)
+        add(rx, tcol["tau_u1x"], der, np.zeros_like(der), -nu * De[der])
+        add(rx, cp, idx, idx, ikx * np.ones(N))
+        add(rx, tcol["tau_u2x"], [N - 1], [0], [1.0])
+        lap_block(rz, cuz, -nu)
+        add(rz, tcol["tau_u1z"], der, np.zeros_like(der), -nu * De[der])
+        add(rz, cp, dr, dc, self.D[dr, dc])
+        add(rz, cb, idx, idx, -np.ones(N))
+        add(rz, tcol["tau_u2z"], [N - 1], [0], [1.0])
+        # boundary conditions: T_n(-1) at z=0, T_n(1) at z=Lz (Interpolate rows)
         bot = cheb_eval_row(N, -1.0)
         top = cheb_eval_row(N, 1.0)
-        L[r_bc + 0, cb : cb + N] = bot
-        L[r_bc + 1, cux : cux + N] = bot
-        L[r_bc + 2, cuz : cuz + N] = bot
-        L[r_bc + 3, cb : cb + N] = top
-        L[r_bc + 4, cux : cux + N] = top
-        L[r_bc + 5, cuz : cuz + N] = top
+        zero = np.zeros(N, int)
+        for i, (col, row) in enumerate(((cb, bot), (cux, bot), (cuz, bot), (cb, top), (cux, top), (cuz, top))):
+            add(r_bc + i, col, zero, idx, row)
         bc_rows = list(range(r_bc, r_bc + 6))
         alg_f = np.zeros(n, complex)
         if m == 0:
@@ -397,13 +403,21 @@ class RBC2D:
             alg_f[r_bc + 0] = p.bottom() * p.Nx
             alg_f[r_bc + 3] = p.b_top * p.Nx
             # integ(p) = 0 : Lx * int T_n dz
-            L[r_bc + 6, cp : cp + N] = p.Lx * cheb_integ_row(N, p.Lz)
+            add(r_bc + 6, cp, zero, idx, p.Lx * cheb_integ_row(N, p.Lz))
             bc_rows.append(r_bc + 6)
-        # entry cutoff 1e-12 (subproblem_matrix_build.jl:88-100)
-        L[np.abs(L) < 1e-12] = 0.0
+        L = sps.coo_matrix((np.concatenate(Lv), (np.concatenate(Lr), np.concatenate(Lc))), shape=(n, n)).tocsr()
+        L.sum_duplicates()
+        Mi = np.concatenate([cb + idx, cux + idx, cuz + idx])
+        Mr = np.concatenate([rb + idx, rx + idx, rz + idx])
+        M = sps.coo_matrix((np.ones(3 * N, complex), (Mr, Mi)), shape=(n, n)).tocsr()
         out = (M, L, np.array(bc_rows), alg_f)
         self._mats[m] = out
         return out
+
+    def dense_mode_matrices(self, m: int):
+        """Dense copies of mode_matrices (small sizes / tests)."""
+        M, L, bc, af = self.mode_matrices(m)
+        return M.toarray(), L.toarray(), bc, af
 
     # -- gather/scatter between fields and mode vectors ---------------------
     def gather(self, m: int, b, ux, uz, pr, tau) -> np.ndarray:
@@ -442,14 +456,20 @@ class RBC2D:
         return x
 
     def _lhs_lu(self, m: int, alpha: float, beta: float):
+        """Sparse LU of alpha M + beta L, cached per (mode, alpha, beta).
+
+        The reference factors the same matrix with UMFPACK (SparseLUSolver,
+        src/tools/matsolvers.jl:65-147); SuperLU (splu) is the SciPy equivalent.
+        """
         key = (m, alpha, beta)
         lu = self._lu.get(key)
         if lu is None:
             M, L, _, _ = self.mode_matrices(m)
-            A = alpha * M + beta * L
-            lu = sla.lu_factor(A)
-            if np.min(np.abs(np.diag(lu[0]))) == 0.0:
-                raise np.linalg.LinAlgError(f"singular tau matrix at mode {m}")
+            A = (alpha * M + beta * L).tocsc()
+            try:
+                lu = spsl.splu(A)
+            except RuntimeError as e:
+                raise np.linalg.LinAlgError(f"singular tau matrix at mode {m}: {e}")
             self._lu[key] = lu
         return lu
 
@@ -514,7 +534,7 @@ class RBC2D:
                     x = self.mass_solve(m, rhs)
                 else:
                     rhs[bc] = dt * a_ii * algf[bc]
-                    x = sla.lu_solve(self._lhs_lu(m, 1.0, dt * a_ii), rhs)
+                    x = self._lhs_lu(m, 1.0, dt * a_ii).solve(rhs)
                 xs.append(x)
             for m in range(Nk):
                 self.scatter(m, xs[m], *self.fields())
@@ -559,7 +579,7 @@ class RBC2D:
                 if abs(a[k]) >= 1e-14 and k - 1 < len(hist):
                     rhs -= a[k] * hist[k - 1][0][m]
             rhs[bc] = bcoef[0] * algf[bc]
-            xs.append(sla.lu_solve(self._lhs_lu(m, a[0], bcoef[0]), rhs))
+            xs.append(self._lhs_lu(m, a[0], bcoef[0]).solve(rhs))
         for m in range(Nk):
             self.scatter(m, xs[m], *self.fields())
         self._ms_hist = hist[:1] if order == 1 else hist[:2]

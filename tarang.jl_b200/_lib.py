@@ -65,7 +65,9 @@ SIGNATURES = {
     "tb_synchronize": (c_int, [c_void_p]),
     "tb_last_step_ms": (c_int, [c_void_p, POINTER(c_float)]),
     "tb_set_profiling": (c_int, [c_void_p, c_int]),
-    "tb_kernel_times": (c_int, [c_void_p, POINTER(c_double), c_int]),
+    "tb_profile_count": (c_int, [c_void_p, POINTER(c_int)]),
+    "tb_profile_entry": (c_int, [c_void_p, c_int, c_char_p, c_int, POINTER(c_double), POINTER(c_longlong)]),
+    "tb_profile_reset": (c_int, [c_void_p]),
     "tb_kernels_per_step": (c_int, [c_void_p, POINTER(c_int)]),
     "tb_tau_layout_query": (c_int, [c_int, c_double, c_double, c_int, POINTER(c_int)]),
     "tb_transform_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),

@@ -165,6 +165,23 @@ class Plan:
         check(lib.tb_last_step_ms(self.ptr, byref(ms)), self.ctx)
         return ms.value
 
+    def set_profiling(self, on: bool) -> None:
+        check(lib.tb_set_profiling(self.ptr, 1 if on else 0), self.ctx)
+        if on:
+            check(lib.tb_profile_reset(self.ptr), self.ctx)
+
+    def profile(self) -> Dict[str, tuple]:
+        """{kernel name: (total ms, launches)} accumulated while profiling was on."""
+        n = c_int()
+        check(lib.tb_profile_count(self.ptr, byref(n)), self.ctx)
+        out = {}
+        buf = ctypes.create_string_buffer(64)
+        for i in range(n.value):
+            ms, cnt = c_double(), c_longlong()
+            check(lib.tb_profile_entry(self.ptr, i, buf, 64, byref(ms), byref(cnt)), self.ctx)
+            out[buf.value.decode()] = (ms.value, cnt.value)
+        return out
+
     def kernels_per_step(self) -> int:
         n = c_int()
         check(lib.tb_kernels_per_step(self.ptr, byref(n)), self.ctx)

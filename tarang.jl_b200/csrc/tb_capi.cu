@@ -57,7 +57,7 @@ struct ClassTables {
 
 struct FactorSet {
   double alpha = 0, beta = 0;
-  DevBuf piv[2], Lm[2], U[2], Bd[2], Cm[2], Sinv[2];
+  DevBuf FR, BR, SI;  // solve-layout factor records (see tb_kernels.cuh)
 };
 
 struct Tableau {
@@ -118,13 +118,16 @@ struct tb_plan {
   // state and work arrays
   DevBuf X, tau, G, H, MX0, FP[4], LXP[4], Fprev, MXprev, Rsb, tmpgrid;
   // transform constants
-  DevBuf bwdstack, bwd, fwd, sfwd, s3, twM, twN;
+  DevBuf bwd, fwd, s3, twM, twN;
+  // parity halves of the Chebyshev matrices (H = ceil(Nz/2) rows/cols)
+  DevBuf bEv, bOv, bEd, bOd, fE, fO, sfE, sfO;
+  int Hz = 0, Ke = 0, Ko = 0;  // Hz = ceil(Nz/2)
   FftPlan fpM{}, fpN{};
   // tau layout
   TauLayout lay;
   ClassTables ct[2];
   std::vector<std::unique_ptr<FactorSet>> factors;
-  DevBuf err_mode;
+  DevBuf err_mode, rhs_off;
   // stepping state
   double sim_time = 0.0;
   long long iteration = 0;
@@ -133,8 +136,22 @@ struct tb_plan {
   int graph_kind = -1;
   cudaGraphExec_t gexec = nullptr;
   int kernels_per_step = 0;
+  // profiling: eager launches bracketed by events, accumulated per kernel name
+  bool profiling = false;
+  struct ProfRec {
+    std::string name;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfRec> pending;
+  std::vector<cudaEvent_t> event_pool;
+  std::map<std::string, std::pair<double, long long>> prof;  // name -> (ms, launches)
 
   ~tb_plan() {
+    for (auto e : event_pool) cudaEventDestroy(e);
+    for (auto& r : pending) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
     if (gexec) cudaGraphExecDestroy(gexec);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -173,6 +190,47 @@ void check_launch(const char* what) {
   if (e != cudaSuccess) throw Error{TB_ECUDA, std::string(what) + ": " + cudaGetErrorString(e)};
 }
 
+cudaEvent_t take_event(tb_plan* P) {
+  if (!P->event_pool.empty()) {
+    cudaEvent_t e = P->event_pool.back();
+    P->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  TB_CUDA_TRY(cudaEventCreate(&e));
+  return e;
+}
+
+// Runs fn (which enqueues one kernel) and, in profiling mode, brackets it with events.
+template <class F>
+void timed(tb_plan* P, const char* name, F&& fn) {
+  if (!P->profiling) {
+    fn();
+    return;
+  }
+  cudaEvent_t a = take_event(P), b = take_event(P);
+  TB_CUDA_TRY(cudaEventRecord(a, P->st));
+  fn();
+  TB_CUDA_TRY(cudaEventRecord(b, P->st));
+  P->pending.push_back({name, a, b});
+}
+
+void collect_profile(tb_plan* P) {
+  TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  for (auto& r : P->pending) {
+    float ms = 0.f;
+    TB_CUDA_TRY(cudaEventElapsedTime(&ms, r.a, r.b));
+    auto& acc = P->prof[r.name];
+    acc.first += ms;
+    acc.second += 1;
+    P->event_pool.push_back(r.a);
+    P->event_pool.push_back(r.b);
+  }
+  P->pending.clear();
+}
+
+inline int pad16k(int k) { return (k + 15) / 16 * 16; }
+
 std::vector<double2> twiddles(int n) {
   std::vector<double2> t(n);
   const long double pi = 3.141592653589793238462643383279502884L;
@@ -205,12 +263,9 @@ ClassDev class_dev(tb_plan* P, int c, FactorSet* f) {
   cd.c1_z = T.c1_z.as<double>();
   cd.c1_nz = T.c1_nz.as<double>();
   if (f) {
-    cd.piv = f->piv[c].as<unsigned char>();
-    cd.Lm = f->Lm[c].as<double>();
-    cd.U = f->U[c].as<double>();
-    cd.Bd = f->Bd[c].as<double>();
-    cd.Cm = f->Cm[c].as<double>();
-    cd.Sinv = f->Sinv[c].as<double>();
+    cd.FR = f->FR.as<double>();
+    cd.BR = f->BR.as<double>();
+    cd.SI = f->SI.as<double>();
   }
   return cd;
 }
@@ -228,6 +283,8 @@ TauArgs tau_args(tb_plan* P, FactorSet* f, const double2* rhsP) {
   a.X = P->X.as<double2>();
   a.tau = P->tau.as<double2>();
   a.rhsP = rhsP;
+  a.npad = (P->lay.cls[0].n + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
+  a.rhs_off = P->rhs_off.as<int>();
   a.err_mode = P->err_mode.as<int>();
   return a;
 }
@@ -241,16 +298,14 @@ FactorSet* get_factors(tb_plan* P, double alpha, double beta) {
   fs->alpha = alpha;
   fs->beta = beta;
   const int Nk = P->Nk;
-  for (int c = 0; c < 2; ++c) {
-    const ClassLayout& L = P->lay.cls[c];
-    const size_t n = L.n, nb = L.nb, w = L.kl + L.ku + 1;
-    fs->piv[c].alloc(n * Nk);
-    fs->Lm[c].alloc(n * L.kl * Nk * sizeof(double));
-    fs->U[c].alloc(n * w * Nk * sizeof(double));
-    fs->Bd[c].alloc(n * nb * Nk * sizeof(double));
-    fs->Cm[c].alloc(n * nb * Nk * sizeof(double));
-    fs->Sinv[c].alloc(nb * nb * Nk * sizeof(double));
-  }
+  const size_t groups = (size_t)(Nk + kSolveModes - 1) / kSolveModes;
+  const size_t n = (P->lay.cls[0].n + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
+  fs->FR.alloc(groups * n * 2 * kFwdRec * kSolveModes * sizeof(double));
+  fs->BR.alloc(groups * n * 2 * kBwdRec * kSolveModes * sizeof(double));
+  fs->SI.alloc(groups * 2 * 16 * kSolveModes * sizeof(double));
+  TB_CUDA_TRY(cudaMemsetAsync(fs->FR.p, 0, fs->FR.bytes, P->st));
+  TB_CUDA_TRY(cudaMemsetAsync(fs->BR.p, 0, fs->BR.bytes, P->st));
+  TB_CUDA_TRY(cudaMemsetAsync(fs->SI.p, 0, fs->SI.bytes, P->st));
   const int nmax = std::max(P->lay.cls[0].n, P->lay.cls[1].n);
   DevBuf scratch;
   scratch.alloc(tau_factor_scratch_doubles(nmax, Nk) * sizeof(double));
@@ -272,19 +327,27 @@ FactorSet* get_factors(tb_plan* P, double alpha, double beta) {
 
 // F = -(u.grad) f in C^(2) rows (sfwd) or T coefficients (fwd) for f = b, ux, uz.
 void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
-  const int N = P->Nz;
+  const int N = P->Nz, H = P->Hz;
   const int ncol = 2 * P->Nk;
+  const size_t hplane = (size_t)H * P->Nk;
+  double2* G = P->G.as<double2>();
+  auto gp = [&](int f, int w) { return G + (size_t)(4 * f + w) * hplane; };  // w: 0 ev, 1 ov, 2 ed, 3 od
   GemmBatch bt{};
+  int nb = 0;
   for (int f = 0; f < 3; ++f) {
-    bt.in[f] = reinterpret_cast<const double*>(Xin + (size_t)f * P->plane);
-    bt.out[2 * f + 0] = reinterpret_cast<double*>(P->G.as<double2>() + (size_t)(2 * f) * P->plane);
-    bt.out[2 * f + 1] = reinterpret_cast<double*>(P->G.as<double2>() + (size_t)(2 * f + 1) * P->plane);
+    const double* in = reinterpret_cast<const double*>(Xin + (size_t)f * P->plane);
+    const double* Am[4] = {P->bEv.as<double>(), P->bOv.as<double>(), P->bEd.as<double>(), P->bOd.as<double>()};
+    for (int w = 0; w < 4; ++w)
+      bt.item[nb++] = GemmItem{Am[w], in, reinterpret_cast<double*>(gp(f, w)), H, (w & 1) ? P->Ko : P->Ke,
+                               pad16k((w & 1) ? P->Ko : P->Ke), GEMM_PARITY, w & 1};
   }
-  launch_gemm_f64(P->bwdstack.as<double>(), 2 * N, N, bt, 3, ncol, ncol, ncol, N, 2, P->st);
+  timed(P, "z_backward_gemm", [&] { launch_gemm_f64(bt, nb, ncol, ncol, ncol, N, P->st); });
   XProdArgs xa{};
   for (int f = 0; f < 3; ++f) {
-    xa.val[f] = P->G.as<double2>() + (size_t)(2 * f) * P->plane;
-    xa.dz[f] = P->G.as<double2>() + (size_t)(2 * f + 1) * P->plane;
+    xa.ev[f] = gp(f, 0);
+    xa.ov[f] = gp(f, 1);
+    xa.ed[f] = gp(f, 2);
+    xa.od[f] = gp(f, 3);
     xa.out[f] = P->H.as<double2>() + (size_t)f * P->plane;
   }
   xa.tw = P->twM.as<double2>();
@@ -294,13 +357,18 @@ void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
   xa.M = P->M;
   xa.Nz = N;
   xa.k0 = P->k0;
-  launch_xprod(xa, P->st);
+  timed(P, "x_fft_products", [&] { launch_xprod(xa, P->st); });
   GemmBatch bf{};
+  nb = 0;
   for (int f = 0; f < 3; ++f) {
-    bf.in[f] = reinterpret_cast<const double*>(P->H.as<double2>() + (size_t)f * P->plane);
-    bf.out[f] = reinterpret_cast<double*>(out3 + (size_t)f * P->plane);
+    const double* in = reinterpret_cast<const double*>(P->H.as<double2>() + (size_t)f * P->plane);
+    double* out = reinterpret_cast<double*>(out3 + (size_t)f * P->plane);
+    bf.item[nb++] = GemmItem{c2rows ? P->sfE.as<double>() : P->fE.as<double>(), in, out, P->Ke, H, pad16k(H), GEMM_MIRROR, 0};
+    if (P->Ko > 0)
+      bf.item[nb++] =
+          GemmItem{c2rows ? P->sfO.as<double>() : P->fO.as<double>(), in, out, P->Ko, H, pad16k(H), GEMM_MIRROR, 1};
   }
-  launch_gemm_f64(c2rows ? P->sfwd.as<double>() : P->fwd.as<double>(), N, N, bf, 3, ncol, ncol, ncol, N, 1, P->st);
+  timed(P, "z_forward_gemm", [&] { launch_gemm_f64(bf, nb, ncol, ncol, ncol, N, P->st); });
 }
 
 void enqueue_rk_step(tb_plan* P, double dt) {
@@ -310,7 +378,7 @@ void enqueue_rk_step(tb_plan* P, double dt) {
   FactorSet* fs = get_factors(P, 1.0, beta);  // done before capture by the caller
   const long long cnt = 4LL * (long long)P->plane;
   double2* X = P->X.as<double2>();
-  launch_mass_apply(X, P->MX0.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 0, P->st);
+  timed(P, "mass_apply", [&] { launch_mass_apply(X, P->MX0.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 0, P->st); });
   int nk = 1;
   for (int i = 0; i < T.s; ++i) {
     if (i > 0) {
@@ -327,11 +395,13 @@ void enqueue_rk_step(tb_plan* P, double dt) {
           lc.w[lc.n++] = -dt * T.AI[i][j];
         }
       }
-      launch_lincomb(lc, P->LXP[i].as<double2>(), cnt, P->st);
+      timed(P, "stage_lincomb", [&] { launch_lincomb(lc, P->LXP[i].as<double2>(), cnt, P->st); });
       TauArgs a = tau_args(P, fs, P->LXP[i].as<double2>());
-      launch_tau_solve(a, P->st);
-      launch_lx_finalize(P->LXP[i].as<double2>(), X, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, P->k0, P->s,
-                         P->d.kappa, P->d.nu, beta, P->st);
+      timed(P, "tau_solve", [&] { launch_tau_solve(a, P->st); });
+      timed(P, "lx_finalize", [&] {
+        launch_lx_finalize(P->LXP[i].as<double2>(), X, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, P->k0, P->s,
+                           P->d.kappa, P->d.nu, beta, P->st);
+      });
       nk += 3;
     }
     enqueue_rhs(P, X, P->FP[i].as<double2>() + P->plane, true);
@@ -350,7 +420,7 @@ void enqueue_rk_step(tb_plan* P, double dt) {
       lc.w[lc.n++] = -dt * T.bI[j];
     }
   }
-  launch_rk_final(lc, X, P->tau.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->st);
+  timed(P, "rk_final", [&] { launch_rk_final(lc, X, P->tau.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->st); });
   nk += 1;
   P->kernels_per_step = nk;
 }
@@ -386,7 +456,7 @@ void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
   double2* Fcur = P->FP[0].as<double2>();
   double2* MXcur = P->MX0.as<double2>();
   enqueue_rhs(P, X, Fcur + P->plane, true);
-  launch_mass_apply(X, MXcur, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 1, P->st);
+  timed(P, "mass_apply", [&] { launch_mass_apply(X, MXcur, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 1, P->st); });
   LinComb lc{};
   lc.in[lc.n] = Fcur;
   lc.w[lc.n++] = c1;
@@ -398,9 +468,9 @@ void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
     lc.in[lc.n] = P->MXprev.as<double2>();
     lc.w[lc.n++] = -a2;
   }
-  launch_lincomb(lc, P->Rsb.as<double2>(), cnt, P->st);
+  timed(P, "stage_lincomb", [&] { launch_lincomb(lc, P->Rsb.as<double2>(), cnt, P->st); });
   TauArgs a = tau_args(P, fs, P->Rsb.as<double2>());
-  launch_tau_solve(a, P->st);
+  timed(P, "tau_solve", [&] { launch_tau_solve(a, P->st); });
   TB_CUDA_TRY(cudaMemcpyAsync(P->Fprev.p, Fcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
   TB_CUDA_TRY(cudaMemcpyAsync(P->MXprev.p, MXcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
   P->kernels_per_step = 3 + 1 + 1 + 1;
@@ -523,19 +593,45 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
     P->plane = (size_t)P->Nz * P->Nk;
     TB_REQUIRE(make_fft_plan(P->M, &P->fpM) && make_fft_plan(P->Nx, &P->fpN), TB_ENOTSUPPORTED,
                "Nx must be of the form 2^a 3^b");
-    TB_REQUIRE(xprod_smem_bytes(P->M) <= 227 * 1024, TB_ENOTSUPPORTED, "Nx too large for the fused x kernel");
+    TB_REQUIRE(xprod_smem_bytes(P->M, P->Nk) <= 227 * 1024, TB_ENOTSUPPORTED, "Nx too large for the fused x kernel");
     TB_CUDA_TRY(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
     TB_CUDA_TRY(cudaEventCreate(&P->ev0));
     TB_CUDA_TRY(cudaEventCreate(&P->ev1));
     TB_CUDA_TRY(set_transform_smem_limits(227 * 1024));
+    TB_CUDA_TRY(set_tau_smem_limits(227 * 1024));
     // transforms
     ChebMats cm = build_cheb_mats(P->Nz, desc->Lz);
-    std::vector<double> stack(cm.bwd);
-    stack.insert(stack.end(), cm.bwd_d.begin(), cm.bwd_d.end());
-    upload(P->bwdstack, stack);
-    upload(P->bwd, cm.bwd);
-    upload(P->fwd, cm.fwd);
-    upload(P->sfwd, cm.sfwd);
+    const int N = P->Nz;
+    P->Hz = (N + 1) / 2;
+    P->Ke = (N + 1) / 2;
+    P->Ko = N / 2;
+    auto pad16 = [](int k) { return (k + 15) / 16 * 16; };
+    auto cols_of = [&](const std::vector<double>& m, int par) {  // rows j < H, columns n = 2k + par
+      const int K = par ? P->Ko : P->Ke, Kp = pad16(K);
+      std::vector<double> o((size_t)P->Hz * Kp, 0.0);
+      for (int j = 0; j < P->Hz; ++j)
+        for (int k = 0; k < K; ++k) o[(size_t)j * Kp + k] = m[(size_t)j * N + 2 * k + par];
+      return o;
+    };
+    auto rows_of = [&](const std::vector<double>& m, int par) {  // rows n = 2r + par, columns j < H
+      const int R = par ? P->Ko : P->Ke, Kp = pad16(P->Hz);
+      std::vector<double> o((size_t)R * Kp, 0.0);
+      for (int r = 0; r < R; ++r)
+        for (int j = 0; j < P->Hz; ++j) o[(size_t)r * Kp + j] = m[(size_t)(2 * r + par) * N + j];
+      return o;
+    };
+    std::vector<double> bwdp((size_t)N * pad16(N), 0.0);
+    for (int j = 0; j < N; ++j)
+      for (int n = 0; n < N; ++n) bwdp[(size_t)j * pad16(N) + n] = cm.bwd[(size_t)j * N + n];
+    upload(P->bEv, cols_of(cm.bwd, 0));
+    upload(P->bOv, cols_of(cm.bwd, 1));
+    upload(P->bEd, cols_of(cm.bwd_d, 0));
+    upload(P->bOd, cols_of(cm.bwd_d, 1));
+    upload(P->fE, rows_of(cm.fwd, 0));
+    upload(P->fO, rows_of(cm.fwd, 1));
+    upload(P->sfE, rows_of(cm.sfwd, 0));
+    upload(P->sfO, rows_of(cm.sfwd, 1));
+    upload(P->bwd, bwdp);
     upload(P->s3, cm.s3);
     upload(P->twM, twiddles(P->M));
     upload(P->twN, twiddles(P->Nx));
@@ -570,12 +666,23 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
       upload(T.c1_z, L.c1_z);
       upload(T.c1_nz, L.c1_nz);
     }
+    TB_REQUIRE(P->lay.cls[0].n == P->lay.cls[1].n, TB_ENOTSUPPORTED, "parity classes of unequal size");
+    TB_REQUIRE(tau_solve_smem_bytes((P->lay.cls[0].n + kTauRowPad - 1) / kTauRowPad * kTauRowPad) <= 227 * 1024,
+               TB_ENOTSUPPORTED, "Nz too large for the staged tau solve");
     P->err_mode.alloc(sizeof(int));
+    {
+      const int n = P->lay.cls[0].n;
+      std::vector<int> ro((size_t)2 * n);
+      for (int j = 0; j < n; ++j)
+        for (int cc = 0; cc < 2; ++cc)
+          ro[2 * j + cc] = (P->lay.cls[cc].row_eq[j] * P->Nz + P->lay.cls[cc].row_k[j]) * P->Nk;
+      upload(P->rhs_off, ro);
+    }
     // state and work arrays
     const size_t pb = P->plane * sizeof(double2);
     P->X.alloc(4 * pb);
     P->tau.alloc(7 * P->Nk * sizeof(double2));
-    P->G.alloc(6 * pb);
+    P->G.alloc(12 * (size_t)((P->Nz + 1) / 2) * P->Nk * sizeof(double2));
     P->H.alloc(3 * pb);
     P->MX0.alloc(4 * pb);
     for (int i = 0; i < 4; ++i) {
@@ -657,8 +764,16 @@ tb_status tb_step(tb_plan* P, double dt, int nsteps) {
       } else {
         get_factors(P, sbdf_coefs(kind, dt).a0, 1.0);
       }
-      if (!(P->gexec && P->graph_dt == dt && P->graph_kind == kind)) capture_step(P, dt, kind);
-      TB_CUDA_TRY(cudaGraphLaunch(P->gexec, P->st));
+      if (P->profiling) {
+        if (kind == 0)
+          enqueue_rk_step(P, dt);
+        else
+          enqueue_sbdf_step(P, dt, kind);
+        check_launch("profiled step");
+      } else {
+        if (!(P->gexec && P->graph_dt == dt && P->graph_kind == kind)) capture_step(P, dt, kind);
+        TB_CUDA_TRY(cudaGraphLaunch(P->gexec, P->st));
+      }
       P->sim_time += dt;
       P->iteration += 1;
       if (kind != 0) P->ms_history = 1;
@@ -667,6 +782,7 @@ tb_status tb_step(tb_plan* P, double dt, int nsteps) {
     TB_CUDA_TRY(cudaEventSynchronize(P->ev1));
     TB_CUDA_TRY(cudaEventElapsedTime(&P->last_ms, P->ev0, P->ev1));
     TB_CUDA_TRY(cudaGetLastError());
+    if (P->profiling) collect_profile(P);
   });
 }
 
@@ -689,14 +805,30 @@ tb_status tb_last_step_ms(const tb_plan* P, float* ms) {
 }
 
 tb_status tb_set_profiling(tb_plan* P, int on) {
-  (void)on;
-  return P ? TB_OK : TB_EINVAL;
+  if (!P) return TB_EINVAL;
+  P->profiling = on != 0;
+  return TB_OK;
 }
 
-tb_status tb_kernel_times(tb_plan* P, double* out3, int reset) {
-  (void)reset;
-  if (!P || !out3) return TB_EINVAL;
-  out3[0] = out3[1] = out3[2] = 0.0;
+tb_status tb_profile_count(const tb_plan* P, int* n) {
+  if (!P || !n) return TB_EINVAL;
+  *n = (int)P->prof.size();
+  return TB_OK;
+}
+
+tb_status tb_profile_entry(const tb_plan* P, int i, char* name, int name_len, double* ms_total, long long* launches) {
+  if (!P || i < 0 || i >= (int)P->prof.size() || !name || name_len < 1) return TB_EINVAL;
+  auto it = P->prof.begin();
+  std::advance(it, i);
+  std::snprintf(name, (size_t)name_len, "%s", it->first.c_str());
+  if (ms_total) *ms_total = it->second.first;
+  if (launches) *launches = it->second.second;
+  return TB_OK;
+}
+
+tb_status tb_profile_reset(tb_plan* P) {
+  if (!P) return TB_EINVAL;
+  P->prof.clear();
   return TB_OK;
 }
 
@@ -730,9 +862,11 @@ tb_status tb_transform_forward(tb_plan* P, const double* grid, double* coeff, in
       double2* mixed = P->tmpgrid.as<double2>();
       launch_x_rfft(grid + f * gsz, mixed, P->Nz, P->Nx, P->fpN, P->twN.as<double2>(), P->st);
       GemmBatch bt{};
-      bt.in[0] = reinterpret_cast<const double*>(mixed);
-      bt.out[0] = coeff + f * 2 * P->plane;
-      launch_gemm_f64(P->fwd.as<double>(), P->Nz, P->Nz, bt, 1, 2 * P->Nk, 2 * P->Nk, 2 * P->Nk, P->Nz, 1, P->st);
+      bt.item[0] = GemmItem{P->fE.as<double>(), reinterpret_cast<const double*>(mixed), coeff + f * 2 * P->plane, P->Ke,
+                            P->Hz, pad16k(P->Hz), GEMM_MIRROR, 0};
+      bt.item[1] = GemmItem{P->fO.as<double>(), reinterpret_cast<const double*>(mixed), coeff + f * 2 * P->plane, P->Ko,
+                            P->Hz, pad16k(P->Hz), GEMM_MIRROR, 1};
+      launch_gemm_f64(bt, P->Ko > 0 ? 2 : 1, 2 * P->Nk, 2 * P->Nk, 2 * P->Nk, P->Nz, P->st);
       check_launch("transform forward");
     }
     TB_CUDA_TRY(cudaStreamSynchronize(P->st));
@@ -746,9 +880,9 @@ tb_status tb_transform_backward(tb_plan* P, const double* coeff, double* grid, i
     for (int f = 0; f < nfields; ++f) {
       double2* mixed = P->tmpgrid.as<double2>();
       GemmBatch bt{};
-      bt.in[0] = coeff + f * 2 * P->plane;
-      bt.out[0] = reinterpret_cast<double*>(mixed);
-      launch_gemm_f64(P->bwd.as<double>(), P->Nz, P->Nz, bt, 1, 2 * P->Nk, 2 * P->Nk, 2 * P->Nk, P->Nz, 1, P->st);
+      bt.item[0] = GemmItem{P->bwd.as<double>(), coeff + f * 2 * P->plane, reinterpret_cast<double*>(mixed), P->Nz,
+                            P->Nz, pad16k(P->Nz), GEMM_PLAIN, 0};
+      launch_gemm_f64(bt, 1, 2 * P->Nk, 2 * P->Nk, 2 * P->Nk, P->Nz, P->st);
       launch_x_irfft(mixed, grid + f * gsz, P->Nz, P->Nx, P->fpN, P->twN.as<double2>(), P->st);
       check_launch("transform backward");
     }

@@ -7,24 +7,27 @@
 
 namespace tb {
 
-// Up to this many inputs (and 2x outputs) per batched GEMM launch.
-constexpr int kGemmMaxBatch = 6;
-
-struct GemmBatch {
-  const double* in[kGemmMaxBatch];
-  double* out[2 * kGemmMaxBatch];
+// Batched Chebyshev-direction GEMM (see tb_transforms.cu for the row maps).
+enum { GEMM_PLAIN = 0, GEMM_PARITY = 1, GEMM_MIRROR = 2 };
+constexpr int kGemmMaxBatch = 12;
+struct GemmItem {
+  const double* A;  // M x Kpad row-major, columns K..Kpad-1 zero (Kpad a multiple of 16)
+  const double* B;  // input rows (ldb doubles apart; ldb even)
+  double* C;        // output rows (ldc)
+  int M, K, Kpad, mode, par;
 };
-
-// C[r][c] = sum_k A[r][k] * B[k][c] for each batch entry.  A: Mo x K
-// row-major (shared), B: K x ncol (ldb), output row r goes to
-// out[b*nsplit + r/rows_per_out] at row r % rows_per_out (ldc).
-void launch_gemm_f64(const double* A, int Mo, int K, const GemmBatch& bt, int nbatch, int ncol, int ldb,
-                     int ldc, int rows_per_out, int nsplit, cudaStream_t st);
+struct GemmBatch {
+  GemmItem item[kGemmMaxBatch];
+};
+void launch_gemm_f64(const GemmBatch& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, cudaStream_t st);
 
 struct XProdArgs {
-  // mixed-space inputs (Nz x Nk complex): values and z-derivatives of b, ux, uz
-  const double2* val[3];
-  const double2* dz[3];
+  // mixed-space inputs as even/odd Chebyshev half planes (ceil(Nz/2) x Nk
+  // complex) of the values (ev, ov) and z-derivatives (ed, od) of b, ux, uz
+  const double2* ev[3];
+  const double2* ov[3];
+  const double2* ed[3];
+  const double2* od[3];
   double2* out[3];       // mixed-space products -(u.grad f) (Nz x Nk complex)
   const double2* tw;     // exp(-2 pi i t / M), t < M
   FftPlan fp;            // length M plan
@@ -32,7 +35,7 @@ struct XProdArgs {
   double k0;             // 2 pi / Lx
 };
 void launch_xprod(const XProdArgs& a, cudaStream_t st);
-size_t xprod_smem_bytes(int M);
+size_t xprod_smem_bytes(int M, int Nk);
 // Raise the dynamic shared-memory limit of the transform kernels (once per plan).
 cudaError_t set_transform_smem_limits(int bytes);
 // Scratch (doubles) the factorisation needs for nmax band rows and Nk modes.
@@ -52,6 +55,19 @@ void launch_x_dealias_mul(const double* a, const double* b, double* out, int nro
 // ---- tau system kernels ----
 // Compiled band shape of the per-class tau systems (lower / upper bandwidth).
 constexpr int kTauKL = 4, kTauKU = 8;
+// The solve streams per-row factor records of kSolveModes consecutive Fourier
+// modes: forward record = pivot offset, kTauKL multipliers, 4 boundary-row
+// multipliers; backward record = 1/diag, kTauKL+kTauKU U entries, 4 border
+// entries and the encoded store target of the band column (each entry
+// kSolveModes doubles, mode fastest).
+constexpr int kSolveModes = 4;
+constexpr int kFwdRec = 1 + kTauKL + 4;
+constexpr int kBwdRec = 1 + kTauKL + kTauKU + 4 + 1;
+// Register windows of the solve sweeps; band rows are padded to a multiple of
+// their least common multiple (kTauRowPad) with identity rows.
+constexpr int kFwdWin = kTauKL + 2;
+constexpr int kBwdWin = kTauKL + kTauKU;
+constexpr int kTauRowPad = 12;
 struct ClassDev {
   int n, nb, kl, ku;
   const short* row_eq;
@@ -67,18 +83,18 @@ struct ClassDev {
   const double* c2_nz;
   const double* c1_z; // nb x nb
   const double* c1_nz;
-  // factors (mode fastest)
-  unsigned char* piv;  // n x Nk
-  double* Lm;          // n x kl x Nk
-  double* U;           // n x (kl+ku+1) x Nk ; U[j][0] = 1/diag
-  double* Bd;          // n x nb x Nk
-  double* Cm;          // n x nb x Nk
-  double* Sinv;        // nb x nb x Nk
+  // factors, shared by both classes (set on cls[0]):
+  //   FR[group][row][class][kFwdRec][kSolveModes], BR[group][row][class][kBwdRec][kSolveModes],
+  //   SI[group][class][4][4][kSolveModes]
+  double* FR;
+  double* BR;
+  double* SI;
 };
 
 struct TauArgs {
   ClassDev cls[2];
   int Nz, Nk, Nx;
+  int npad;            // band rows padded to a multiple of kTauRowPad
   double k0;           // 2 pi / Lx
   double alpha, beta;  // LHS = alpha M + beta L
   // state (T space): X[4][Nz][Nk] (b, ux, uz, p), tau[7][Nk]
@@ -86,11 +102,15 @@ struct TauArgs {
   double2* tau;
   // P-space right-hand side (cont, b, mx, mz) x Nz x Nk
   const double2* rhsP;
+  // element offset of band row j's right-hand side in rhsP, [row][class]
+  const int* rhs_off;
   double* scratch;     // factor workspace
   int* err_mode;       // first singular mode, or -1
 };
 void launch_tau_factor(const TauArgs& a, cudaStream_t st);
 void launch_tau_solve(const TauArgs& a, cudaStream_t st);
+cudaError_t set_tau_smem_limits(int bytes);
+size_t tau_solve_smem_bytes(int npad);
 
 struct LinComb {
   const double2* in[12];

@@ -99,7 +99,12 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
         Bd[(size_t)p * NBMAX + b] = t;
       }
     }
-    C.piv[(size_t)j * Nk + m] = (unsigned char)(p - j);
+    const int g = m / kSolveModes, mm = m % kSolveModes;
+    double* fr = C.FR + ((((size_t)g * a.npad + j) * 2 + c) * kFwdRec) * kSolveModes + mm;
+    double* br = C.BR + ((((size_t)g * a.npad + j) * 2 + c) * kBwdRec) * kSolveModes + mm;
+    // pivot offset, plus 16 when this band row's right-hand side is a u_x momentum
+    // row (scaled by -i on load)
+    fr[0] = (double)(p - j) + (C.row_eq[j] == EQ_MX ? 16.0 : 0.0);
     const double dinv = 1.0 / W[(size_t)j * WW + KL];
     for (int t = 0; t < KL; ++t) {
       const int i = j + 1 + t;
@@ -111,19 +116,36 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
           W[(size_t)i * WW + (cc - i + KL)] -= l * W[(size_t)j * WW + (cc - j + KL)];
         for (int b = 0; b < nb; ++b) Bd[(size_t)i * NBMAX + b] -= l * Bd[(size_t)j * NBMAX + b];
       }
-      C.Lm[((size_t)j * KL + t) * Nk + m] = l;
+      fr[(1 + t) * kSolveModes] = l;
     }
     for (int q = 0; q < nb; ++q) {
       const double cq = Cr[(size_t)q * nmax + j] * dinv;
       Cr[(size_t)q * nmax + j] = 0.0;
       for (int cc = j + 1; cc <= clast; ++cc) Cr[(size_t)q * nmax + cc] -= cq * W[(size_t)j * WW + (cc - j + KL)];
       for (int b = 0; b < nb; ++b) C1[q * NBMAX + b] -= cq * Bd[(size_t)j * NBMAX + b];
-      C.Cm[((size_t)j * nb + q) * Nk + m] = cq;
+      fr[(1 + KL + q) * kSolveModes] = cq;
     }
-    C.U[((size_t)j * W1 + 0) * Nk + m] = dinv;
-    for (int t = 1; t < W1; ++t)
-      C.U[((size_t)j * W1 + t) * Nk + m] = (j + t < n) ? W[(size_t)j * WW + KL + t] : 0.0;
-    for (int b = 0; b < nb; ++b) C.Bd[((size_t)j * nb + b) * Nk + m] = Bd[(size_t)j * NBMAX + b];
+    for (int q = nb; q < NBMAX; ++q) fr[(1 + KL + q) * kSolveModes] = 0.0;
+    br[0] = dinv;
+    for (int t = 1; t < W1; ++t) br[t * kSolveModes] = (j + t < n) ? W[(size_t)j * WW + KL + t] : 0.0;
+    for (int b = 0; b < NBMAX; ++b) br[(W1 + b) * kSolveModes] = (b < nb) ? Bd[(size_t)j * NBMAX + b] : 0.0;
+    {
+      // store target of this band column: element offset (per mode) into X or the tau
+      // array, encoded as offset*2 + (1 if the unknown is scaled by i), bit-cast
+      const int unk = C.col_unk[j], kk = C.col_k[j];
+      const long long off = unk < 4 ? ((long long)unk * a.Nz + kk) * Nk : (long long)4 * a.Nz * Nk + (long long)(unk - UK_TAU0) * Nk;
+      br[(W1 + NBMAX) * kSolveModes] = __longlong_as_double(2 * off + (realified(unk) ? 1 : 0));
+    }
+  }
+  // padding rows n..npad-1: identity rows with no right-hand side and no store
+  for (int j = n; j < a.npad; ++j) {
+    const int g = m / kSolveModes, mm = m % kSolveModes;
+    double* fr = C.FR + ((((size_t)g * a.npad + j) * 2 + c) * kFwdRec) * kSolveModes + mm;
+    double* br = C.BR + ((((size_t)g * a.npad + j) * 2 + c) * kBwdRec) * kSolveModes + mm;
+    for (int t = 0; t < kFwdRec; ++t) fr[t * kSolveModes] = 0.0;
+    br[0] = 1.0;
+    for (int t = 1; t < kBwdRec - 1; ++t) br[t * kSolveModes] = 0.0;
+    br[(kBwdRec - 1) * kSolveModes] = __longlong_as_double(-1LL);
   }
   // invert the nb x nb Schur complement (Gauss-Jordan, partial pivoting)
   double Aug[NBMAX][2 * NBMAX];
@@ -159,89 +181,238 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
         for (int b = 0; b < 2 * NBMAX; ++b) Aug[q][b] -= f * Aug[col][b];
     }
   }
-  for (int q = 0; q < nb; ++q)
-    for (int b = 0; b < nb; ++b) C.Sinv[((size_t)q * nb + b) * Nk + m] = Aug[q][NBMAX + b];
+  {
+    const int g = m / kSolveModes, mm = m % kSolveModes;
+    double* si = C.SI + (((size_t)g * 2 + c) * NBMAX * NBMAX) * kSolveModes + mm;
+    for (int q = 0; q < NBMAX; ++q)
+      for (int b = 0; b < NBMAX; ++b)
+        si[(q * NBMAX + b) * kSolveModes] = (q < nb && b < nb) ? Aug[q][NBMAX + b] : 0.0;
+  }
 }
 
 // ---------------------------------------------------------------------------
-// Solve: one thread per (mode, class); the real and imaginary parts of the
-// right-hand side are the two columns of a double2.
+// Solve: one warp per group of kSolveModes Fourier modes.  Lane (c, mm) with
+// c = lane / kSolveModes < 2 runs the forward and backward sweeps of parity
+// class c for mode g*kSolveModes + mm (real and imaginary parts together as a
+// double2).  The factor rows of the group are contiguous records that the
+// whole warp streams into a shared-memory ring with cp.async, kRowsPerStage
+// rows per stage and kStages stages deep; the forward sweep's intermediate y
+// stays in shared memory for the backward sweep.
 // ---------------------------------------------------------------------------
+constexpr int kRowsPerStage = 12;  // a multiple of the forward and backward window lengths
+constexpr int kStages = 6;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = valid ? 16 : 0;  // src-size 0 zero-fills the destination
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
 template <int KL, int KU>
-__global__ void __launch_bounds__(128) k_tau_solve(TauArgs a) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  const int c = blockIdx.y;
-  if (m >= a.Nk) return;
-  const ClassDev& C = a.cls[c];
-  const int n = C.n, nb = C.nb;
-  const int Nk = a.Nk, Nz = a.Nz;
+__global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
+  static_assert(KL + 2 == kFwdWin && KL + KU == kBwdWin, "window sizes follow the band shape");
+  constexpr int MP = kSolveModes;
   constexpr int W1 = KL + KU + 1;
-  auto addr = [&](int unk, int k) -> double2* {
-    return unk < 4 ? a.X + ((size_t)unk * Nz + k) * Nk + m : a.tau + (size_t)(unk - UK_TAU0) * Nk + m;
-  };
-  auto load_rhs = [&](int r) -> double2 {
-    const int e = C.row_eq[r], k = C.row_k[r];
-    double2 v = a.rhsP[((size_t)e * Nz + k) * Nk + m];
-    if (e == EQ_MX) v = make_double2(v.y, -v.x);  // row scaled by -i
-    return v;
-  };
-  double2 y[KL + 1];
-#pragma unroll
-  for (int t = 0; t <= KL; ++t) y[t] = (t < n) ? load_rhs(t) : make_double2(0.0, 0.0);
-  double2 z[NBMAX];
-#pragma unroll
-  for (int b = 0; b < NBMAX; ++b) z[b] = make_double2((b < nb && m == 0) ? a.beta * C.bc_rhs[b] : 0.0, 0.0);
-  for (int j = 0; j < n; ++j) {
-    const int p = C.piv[(size_t)j * Nk + m];
-    double2 yj = y[0];
-#pragma unroll
-    for (int t = 1; t <= KL; ++t)
-      if (t == p) {
-        yj = y[t];
-        y[t] = y[0];
+  constexpr int FREC = 2 * kFwdRec * MP;  // doubles per forward row (both classes)
+  constexpr int BREC = 2 * kBwdRec * MP;  // doubles per backward row
+  constexpr int RREC = 2 * MP;            // double2 rhs entries per row (class, mode)
+  constexpr int R = kRowsPerStage;
+  constexpr int NL = 4 * MP;              // distinct lanes; lanes NL..31 mirror lanes 0..NL-1
+  static_assert(NL <= 32 && 32 % NL == 0, "lane layout");
+  extern __shared__ __align__(16) double smem[];
+  const int np = a.npad;
+  const int Nk = a.Nk;
+  const int g = blockIdx.x;
+  const int lane = threadIdx.x;
+  const int ln = lane % NL;
+  // ln = c*2*MP + part*MP + mm : class c, real (part 0) / imaginary (part 1) column, mode mm.
+  // Mirror lanes repeat the same arithmetic (so the unrolled sweeps stay branch free) and
+  // only the owner lanes store.
+  const int c = ln / (2 * MP), part = (ln / MP) & 1, mm = ln % MP;
+  const bool owner = lane < NL;
+  const int m = g * MP + mm;
+  const bool live = owner && m < Nk;
+  constexpr int FSTAGE = R * (FREC + 2 * RREC);
+  constexpr int BSTAGE = R * BREC;
+  constexpr int STAGE = FSTAGE > BSTAGE ? FSTAGE : BSTAGE;
+  double* ring = smem;
+  double* ysave = smem + (size_t)kStages * STAGE;                  // [row][ln]
+  int* rofs = reinterpret_cast<int*>(ysave + (size_t)np * NL);  // [row][class] rhs offset, -1: none
+  for (int q = lane; q < 2 * np; q += 32) rofs[q] = (q < 2 * a.cls[0].n) ? a.rhs_off[q] : -1;
+  __syncwarp();
+  const double* FRg = a.cls[0].FR + (size_t)g * np * FREC;
+  const double* BRg = a.cls[0].BR + (size_t)g * np * BREC;
+  const int nstage = np / R;
+
+  // ---- forward sweep: y = L^-1 P r (rows 0..np-1), boundary rows accumulate z ----
+  auto issue_fwd = [&](int s) {
+    if (s < nstage) {
+      double* dst = ring + (size_t)(s % kStages) * STAGE;
+      const int r0 = s * R;
+      for (int q = lane; q < R * FREC / 2; q += 32) cp_async16(dst + 2 * q, FRg + (size_t)r0 * FREC + 2 * q, true);
+      double2* rdst = reinterpret_cast<double2*>(dst + R * FREC);
+      for (int q = lane; q < R * RREC; q += 32) {
+        const int r = q / RREC, cc = (q / MP) % 2, md = q % MP;
+        const int mq = g * MP + md;
+        const int off = rofs[2 * (r0 + r) + cc];
+        const bool ok = off >= 0 && mq < Nk;
+        cp_async16(rdst + q, a.rhsP + (ok ? (size_t)off + mq : 0), ok);
       }
-    *addr(C.col_unk[j], C.col_k[j]) = yj;
+    }
+    cp_async_commit();
+  };
+  for (int s = 0; s < kStages - 1; ++s) issue_fwd(s);
+  // right-hand side of row j (j < np) for this lane: u_x momentum rows are
+  // scaled by -i, i.e. (re, im) -> (im, -re)
+  auto rhs_row = [&](int j) -> double {
+    const int s = j / R, r = j % R;
+    const double* base = ring + (size_t)(s % kStages) * STAGE;
+    const double* rb = base + R * FREC + (size_t)(r * RREC + c * MP + mm) * 2;
+    const bool rot = base[(size_t)r * FREC + c * kFwdRec * MP + mm] >= 8.0;
+    const double v = rb[part ^ (rot ? 1 : 0)];
+    return (rot && part) ? -v : v;
+  };
+  double y[kFwdWin];
+  double z[NBMAX];
 #pragma unroll
-    for (int t = 1; t <= KL; ++t) y[t] = cfma(-C.Lm[((size_t)j * KL + (t - 1)) * Nk + m], yj, y[t]);
+  for (int b = 0; b < NBMAX; ++b) z[b] = (part == 0 && m == 0 && b < a.cls[c].nb) ? a.beta * a.cls[c].bc_rhs[b] : 0.0;
+  for (int j0 = 0; j0 < np; j0 += kFwdWin) {
+    const int s = j0 / R;
+    if (j0 % R == 0) {
+      issue_fwd(s + kStages - 1);
+      cp_async_wait<kStages - 2>();  // stages s and s+1 are resident
+      __syncwarp();
+      if (s == 0) {
 #pragma unroll
-    for (int b = 0; b < NBMAX; ++b)
-      if (b < nb) z[b] = cfma(-C.Cm[((size_t)j * nb + b) * Nk + m], yj, z[b]);
+        for (int t = 0; t < kFwdWin; ++t) y[t] = rhs_row(t);
+      }
+    }
+    const double* st = ring + (size_t)(s % kStages) * STAGE + (size_t)(j0 - s * R) * FREC + c * kFwdRec * MP + mm;
+    // rows j0 .. j0+kFwdWin-1; the right-hand sides entering the window are rows
+    // j0+kFwdWin .. j0+2 kFwdWin-1, resident in stage s or s+1 (or past the end)
+    double incoming[kFwdWin];
 #pragma unroll
-    for (int t = 0; t < KL; ++t) y[t] = y[t + 1];
-    y[KL] = (j + KL + 1 < n) ? load_rhs(j + KL + 1) : make_double2(0.0, 0.0);
+    for (int u = 0; u < kFwdWin; ++u) {
+      const int jn = j0 + kFwdWin + u;
+      incoming[u] = (jn < np) ? rhs_row(jn < np ? jn : 0) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kFwdWin; ++u) {
+      const int j = j0 + u;
+      const double* rec = st + (size_t)u * FREC;
+      const double pf = rec[0];
+      const int p = (int)(pf >= 8.0 ? pf - 16.0 : pf);
+      double yj = y[u % kFwdWin];
+#pragma unroll
+      for (int t = 1; t <= KL; ++t) {
+        const bool sw = (t == p);
+        const double yt = y[(u + t) % kFwdWin];
+        y[(u + t) % kFwdWin] = sw ? yj : yt;
+        yj = sw ? yt : yj;
+      }
+      ysave[(size_t)j * NL + ln] = yj;
+#pragma unroll
+      for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-rec[t * MP], yj, y[(u + t) % kFwdWin]);
+#pragma unroll
+      for (int b = 0; b < NBMAX; ++b) z[b] = fma(-rec[(1 + KL + b) * MP], yj, z[b]);
+      y[u % kFwdWin] = incoming[u];
+    }
+    if ((j0 + kFwdWin) % R == 0) __syncwarp();  // the ring slot of stage s may be refilled next
   }
-  double2 x1[NBMAX];
+  cp_async_wait<0>();
+  __syncwarp();
+
+  // ---- border unknowns from the Schur complement ----
+  double x1[NBMAX];
+  {
+    const double* si = a.cls[0].SI + ((size_t)g * 2 + c) * NBMAX * NBMAX * MP + mm;
 #pragma unroll
-  for (int q = 0; q < NBMAX; ++q) {
-    double2 acc = make_double2(0.0, 0.0);
+    for (int q = 0; q < NBMAX; ++q) {
+      double acc = 0.0;
 #pragma unroll
-    for (int b = 0; b < NBMAX; ++b)
-      if (q < nb && b < nb) acc = cfma(C.Sinv[((size_t)q * nb + b) * Nk + m], z[b], acc);
-    x1[q] = acc;
+      for (int b = 0; b < NBMAX; ++b) acc = fma(si[(q * NBMAX + b) * MP], z[b], acc);
+      x1[q] = acc;
+    }
   }
-  double2 xw[W1];
+
+  // ---- backward sweep: x = U^-1 (y - B x1), rows np-1..0 ----
+  auto issue_bwd = [&](int s) {
+    if (s < nstage) {
+      double* dst = ring + (size_t)(s % kStages) * STAGE;
+      const int lo = np - (s + 1) * R;
+      for (int q = lane; q < R * BREC / 2; q += 32) cp_async16(dst + 2 * q, BRg + (size_t)lo * BREC + 2 * q, true);
+    }
+    cp_async_commit();
+  };
+  for (int s = 0; s < kStages - 1; ++s) issue_bwd(s);
+  double xw[kBwdWin];  // x_{j+t} lives in slot (j+t) % kBwdWin
 #pragma unroll
-  for (int t = 0; t < W1; ++t) xw[t] = make_double2(0.0, 0.0);
-  for (int j = n - 1; j >= 0; --j) {
-    const int unk = C.col_unk[j];
-    double2* ptr = addr(unk, C.col_k[j]);
-    double2 s = *ptr;
+  for (int t = 0; t < kBwdWin; ++t) xw[t] = 0.0;
+  const size_t xplanes = (size_t)4 * a.Nz * Nk;
+  double* Xd = reinterpret_cast<double*>(a.X);
+  double* Td = reinterpret_cast<double*>(a.tau);
+  static_assert(kBwdWin == R, "one backward block per stage");
+  for (int s = 0; s < nstage; ++s) {
+    issue_bwd(s + kStages - 1);
+    cp_async_wait<kStages - 1>();
+    __syncwarp();
+    const int q0 = np - (s + 1) * R;  // rows q0+R-1 .. q0, q0 % kBwdWin == 0
+    const double* st = ring + (size_t)(s % kStages) * STAGE + c * kBwdRec * MP + mm;
+    double xs[kBwdWin];
 #pragma unroll
-    for (int t = 1; t < W1; ++t) s = cfma(-C.U[((size_t)j * W1 + t) * Nk + m], xw[t], s);
+    for (int u = 0; u < kBwdWin; ++u) {
+      const int j = q0 + kBwdWin - 1 - u;  // j % kBwdWin == kBwdWin-1-u
+      const double* rec = st + (size_t)(kBwdWin - 1 - u) * BREC;
+      double acc0 = ysave[(size_t)j * NL + ln];
+      double acc1 = 0.0, acc2 = 0.0;
 #pragma unroll
-    for (int b = 0; b < NBMAX; ++b)
-      if (b < nb) s = cfma(-C.Bd[((size_t)j * nb + b) * Nk + m], x1[b], s);
-    const double dinv = C.U[((size_t)j * W1) * Nk + m];
-    const double2 xj = make_double2(s.x * dinv, s.y * dinv);
-    *ptr = realified(unk) ? make_double2(-xj.y, xj.x) : xj;
+      for (int b = 0; b < NBMAX; ++b) acc1 = fma(-rec[(W1 + b) * MP], x1[b], acc1);
 #pragma unroll
-    for (int t = W1 - 1; t >= 2; --t) xw[t] = xw[t - 1];
-    xw[1] = xj;
+      for (int t = kBwdWin; t >= 2; --t) {
+        const int sl = (kBwdWin - 1 - u + t) % kBwdWin;
+        if (t % 3 == 0)
+          acc0 = fma(-rec[t * MP], xw[sl], acc0);
+        else if (t % 3 == 1)
+          acc1 = fma(-rec[t * MP], xw[sl], acc1);
+        else
+          acc2 = fma(-rec[t * MP], xw[sl], acc2);
+      }
+      const double sacc = fma(-rec[1 * MP], xw[(kBwdWin - u) % kBwdWin], acc0 + (acc1 + acc2));
+      const double xj = sacc * rec[0];
+      xw[(kBwdWin - 1 - u) % kBwdWin] = xj;
+      xs[u] = xj;
+    }
+    // stores for the block, undoing the i-scaling of u_x and its taus
+    // (ux = i vx: re = -vx_im, im = vx_re)
+#pragma unroll
+    for (int u = 0; u < kBwdWin; ++u) {
+      const double* rec = st + (size_t)(kBwdWin - 1 - u) * BREC;
+      const double partner = __shfl_xor_sync(0xffffffffu, xs[u], MP);
+      const long long code = __double_as_longlong(rec[(kBwdRec - 1) * MP]);
+      const size_t off = (size_t)(code >> 1);
+      const double v = (code & 1) ? (part ? partner : -partner) : xs[u];
+      double* dst = off < xplanes ? Xd + 2 * (off + m) : Td + 2 * (off - xplanes + m);
+      if (live && code >= 0) dst[part] = v;
+    }
+    __syncwarp();
   }
-  for (int b = 0; b < nb; ++b) {
-    const int unk = C.left_unk[b];
-    const double2 v = x1[b];
-    *addr(unk, C.left_k[b]) = realified(unk) ? make_double2(-v.y, v.x) : v;
+  cp_async_wait<0>();
+  // border unknowns
+#pragma unroll
+  for (int b = 0; b < NBMAX; ++b) {
+    const double partner = __shfl_xor_sync(0xffffffffu, x1[b], MP);
+    if (live && b < a.cls[c].nb) {
+      const int unk = a.cls[c].left_unk[b];
+      const int k = a.cls[c].left_k[b];
+      const double v = realified(unk) ? (part ? partner : -partner) : x1[b];
+      double* dst = unk < 4 ? Xd + 2 * (((size_t)unk * a.Nz + k) * Nk + m) : Td + 2 * ((size_t)(unk - UK_TAU0) * Nk + m);
+      dst[part] = v;
+    }
   }
 }
 
@@ -325,26 +496,47 @@ __global__ void k_lx_finalize(double2* __restrict__ LX, const double2* __restric
   }
 }
 
-__global__ void k_rk_final(LinComb lc, double2* __restrict__ X, const double* __restrict__ s3, int Nz, int Nk) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+// Final RK update X_f = S^{-1} y, y = linear combination of the stage vectors
+// in C^(2) rows.  S is upper triangular with offsets 0, +2, +4, so each
+// (field, parity, mode) column is a short backward recurrence.  The CTA first
+// forms y for all rows of its 32 modes in shared memory (256 threads, loads
+// independent), then warp 0 runs the recurrences from shared memory.
+__global__ void __launch_bounds__(256) k_rk_final(LinComb lc, double2* __restrict__ X, const double* __restrict__ s3,
+                                                  int Nz, int Nk) {
+  extern __shared__ double2 ys[];  // [rows of this parity][32]
   const int f = blockIdx.y >> 1, par = blockIdx.y & 1;
-  if (m >= Nk) return;
+  const int m0 = blockIdx.x * 32;
+  const int mm = threadIdx.x % 32, ks = threadIdx.x / 32;
+  const int m = m0 + mm;
   const size_t plane = (size_t)Nz * Nk;
-  int k = Nz - 1;
-  if ((k & 1) != par) --k;
-  double2 x2 = make_double2(0.0, 0.0), x4 = make_double2(0.0, 0.0);  // x_{k+2}, x_{k+4}
-  for (; k >= 0; k -= 2) {
-    const size_t i = (size_t)(1 + f) * plane + (size_t)k * Nk + m;
+  const int K = (Nz - par + 1) / 2;  // rows k = par + 2 ri
+  for (int ri = ks; ri < K; ri += 8) {
+    const int k = par + 2 * ri;
     double2 y = make_double2(0.0, 0.0);
-    for (int t = 0; t < lc.n; ++t) y = cfma(lc.w[t], lc.in[t][i], y);
-    y = cfma(-s3[3 * k + 1], x2, y);
-    y = cfma(-s3[3 * k + 2], x4, y);
-    const double inv = 1.0 / s3[3 * k];
-    const double2 x = make_double2(y.x * inv, y.y * inv);
-    X[(size_t)f * plane + (size_t)k * Nk + m] = x;
-    x4 = x2;
-    x2 = x;
+    if (m < Nk) {
+      const size_t i = (size_t)(1 + f) * plane + (size_t)k * Nk + m;
+      for (int t = 0; t < lc.n; ++t) y = cfma(lc.w[t], lc.in[t][i], y);
+    }
+    ys[ri * 32 + mm] = y;
   }
+  __syncthreads();
+  if (ks == 0) {
+    double2 x2 = make_double2(0.0, 0.0), x4 = make_double2(0.0, 0.0);
+    for (int ri = K - 1; ri >= 0; --ri) {
+      const int k = par + 2 * ri;
+      double2 y = ys[ri * 32 + mm];
+      y = cfma(-s3[3 * k + 1], x2, y);
+      y = cfma(-s3[3 * k + 2], x4, y);
+      const double inv = 1.0 / s3[3 * k];
+      const double2 x = make_double2(y.x * inv, y.y * inv);
+      ys[ri * 32 + mm] = x;
+      x4 = x2;
+      x2 = x;
+    }
+  }
+  __syncthreads();
+  if (m < Nk)
+    for (int ri = ks; ri < K; ri += 8) X[(size_t)f * plane + (size_t)(par + 2 * ri) * Nk + m] = ys[ri * 32 + mm];
 }
 
 template <int KL, int KU>
@@ -354,15 +546,32 @@ void factor_impl(const TauArgs& a, cudaStream_t st) {
   k_tau_factor<KL, KU><<<grid, 64, 0, st>>>(a, nmax);
 }
 
+size_t solve_smem_bytes(int npad) {
+  constexpr int MP = kSolveModes;
+  const size_t FREC = 2 * kFwdRec * MP, BREC = 2 * kBwdRec * MP, RREC = 2 * MP;
+  const size_t FSTAGE = kRowsPerStage * (FREC + 2 * RREC), BSTAGE = kRowsPerStage * BREC;
+  const size_t STAGE = FSTAGE > BSTAGE ? FSTAGE : BSTAGE;
+  return (kStages * STAGE) * sizeof(double) + (size_t)npad * 4 * MP * sizeof(double) + (size_t)npad * 2 * sizeof(int);
+}
+
 template <int KL, int KU>
 void solve_impl(const TauArgs& a, cudaStream_t st) {
-  dim3 grid((a.Nk + 127) / 128, 2);
-  k_tau_solve<KL, KU><<<grid, 128, 0, st>>>(a);
+  const int groups = (a.Nk + kSolveModes - 1) / kSolveModes;
+  const size_t smem = solve_smem_bytes(a.npad);
+  k_tau_solve<KL, KU><<<groups, 32, smem, st>>>(a);
 }
 
 }  // namespace
 
 size_t tau_factor_scratch_doubles(int nmax, int Nk);
+
+cudaError_t set_tau_smem_limits(int bytes) {
+  cudaError_t e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_rk_final, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+size_t tau_solve_smem_bytes(int n) { return solve_smem_bytes(n); }
 
 // Supported band shape: the RBC layout gives kl = 4, ku = 8 for every Nz >= 8
 // (narrower layouts are zero-padded to it by the plan).
@@ -400,8 +609,9 @@ void launch_lx_finalize(double2* LX, const double2* X, const double* s3, int Nz,
 
 void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* s3, int Nz, int Nk,
                      cudaStream_t st) {
-  dim3 grid((Nk + 127) / 128, 6);
-  k_rk_final<<<grid, 128, 0, st>>>(lc, X, s3, Nz, Nk);
+  dim3 grid((Nk + 31) / 32, 6);
+  const size_t smem = (size_t)((Nz + 1) / 2) * 32 * sizeof(double2);
+  k_rk_final<<<grid, 256, smem, st>>>(lc, X, s3, Nz, Nk);
   cudaMemsetAsync(X + (size_t)3 * Nz * Nk, 0, sizeof(double2) * (size_t)Nz * Nk, st);
   cudaMemsetAsync(tau, 0, sizeof(double2) * 7 * (size_t)Nk, st);
 }

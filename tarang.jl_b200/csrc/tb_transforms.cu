@@ -17,74 +17,154 @@
 namespace tb {
 
 // ---------------------------------------------------------------------------
-// FP64 batched GEMM, 64x64 output tile, 16-deep K slices, 4x4 per thread.
+// FP64 batched GEMM for the Chebyshev direction on the FP64 tensor cores
+// (mma.sync m8n8k4 .f64).  CTA tile 64 x 64 (4 warps, 32 x 32 each), 16-deep
+// K slices double-buffered in shared memory with cp.async.  Each batch entry
+// carries its own A (rows padded to a multiple of 16 doubles) and a B-row map:
+//   GEMM_PLAIN   : B row k = in[k]
+//   GEMM_PARITY  : B row k = in[2k + par]              (even / odd coefficients)
+//   GEMM_MIRROR  : B row j = in[j] + sgn in[N-1-j]     (grid rows folded about
+//                  the mid-plane; sgn = +1 for par 0, -1 for par 1; the middle
+//                  row of odd N counts once / not at all)
+// and an output-row map (row r -> out row r, or 2r + par for GEMM_MIRROR).
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int GBM = 64, GBN = 64, GBK = 16;
+constexpr int GBM = 64, GBN = 64, GBK = 16, GTH = 128;
+constexpr int ASTR = GBK + 4;  // padded shared row strides (doubles)
+constexpr int BSTR = GBN + 8;
+constexpr size_t kGemmSmem = (2 * GBM * ASTR + 4 * GBK * BSTR) * sizeof(double);
 
-__global__ void __launch_bounds__(256) k_gemm_f64(const double* __restrict__ A, int Mo, int K, GemmBatch bt,
-                                                  int ncol, int ldb, int ldc, int rows_per_out, int nsplit) {
-  __shared__ double As[GBK][GBM + 1];
-  __shared__ double Bs[GBK][GBN];
-  const int b = blockIdx.z;
-  const double* __restrict__ B = bt.in[b];
+__device__ __forceinline__ void g_cp16(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void g_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void g_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void g_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ldb, int ldc, int Nrows) {
+  extern __shared__ __align__(16) double gsm[];
+  double (*As)[GBM * ASTR] = reinterpret_cast<double (*)[GBM * ASTR]>(gsm);
+  double (*Bs)[GBK * BSTR] = reinterpret_cast<double (*)[GBK * BSTR]>(gsm + 2 * GBM * ASTR);
+  double (*Bm)[GBK * BSTR] = reinterpret_cast<double (*)[GBK * BSTR]>(gsm + 2 * GBM * ASTR + 2 * GBK * BSTR);  // mirror partners
+  const GemmItem& it = bt.item[blockIdx.z];
+  const double* __restrict__ A = it.A;
+  const double* __restrict__ B = it.B;
+  const int Mo = it.M, K = it.K, Kp = it.Kpad, mode = it.mode, par = it.par;
   const int row0 = blockIdx.y * GBM, col0 = blockIdx.x * GBN;
-  const int tid = threadIdx.x;
-  const int tx = tid % 16, ty = tid / 16;
-  double acc[4][4];
+  if (row0 >= Mo) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int gid = lane >> 2, tig = lane & 3;
+  const bool mirror = mode == GEMM_MIRROR;
+  const int ntiles = (K + GBK - 1) / GBK;
+
+  auto load_tile = [&](int t, int buf) {
+    const int k0 = t * GBK;
+    // A: 64 rows x 16 doubles = 512 chunks of 16 B, 4 per thread
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int ch = tid + q * GTH;
+      const int r = ch >> 3, kc = (ch & 7) * 2;
+      const int gr = row0 + r;
+      const bool ok = gr < Mo;
+      g_cp16(&As[buf][r * ASTR + kc], A + (size_t)(ok ? gr : 0) * Kp + k0 + kc, ok);
+    }
+    // B: 16 rows x 64 doubles = 512 chunks, 4 per thread (8 with the mirror partner)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int ch = tid + q * GTH;
+      const int kk = ch >> 5, cc = (ch & 31) * 2;
+      const int gk = k0 + kk, gc = col0 + cc;
+      const bool ok = gk < K && gc < ncol;
+      int srow = gk;
+      if (mode == GEMM_PARITY) srow = 2 * gk + par;
+      g_cp16(&Bs[buf][kk * BSTR + cc], B + (size_t)(ok ? srow : 0) * ldb + (ok ? gc : 0), ok);
+      if (mirror) {
+        const int jm = Nrows - 1 - gk;
+        const bool okm = ok && jm != gk;  // the middle row of odd N has no partner
+        g_cp16(&Bm[buf][kk * BSTR + cc], B + (size_t)(okm ? jm : 0) * ldb + (okm ? gc : 0), okm);
+      }
+    }
+    g_commit();
+  };
+
+  double acc[4][4][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  for (int k0 = 0; k0 < K; k0 += GBK) {
-    // A tile: 64 rows x 16 k -> 1024 values, 4 per thread
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      int idx = tid + q * 256;
-      int r = idx / GBK, kk = idx % GBK;
-      int gr = row0 + r, gk = k0 + kk;
-      As[kk][r] = (gr < Mo && gk < K) ? A[(size_t)gr * K + gk] : 0.0;
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      int idx = tid + q * 256;
-      int kk = idx / GBN, c = idx % GBN;
-      int gk = k0 + kk, gc = col0 + c;
-      Bs[kk][c] = (gk < K && gc < ncol) ? B[(size_t)gk * ldb + gc] : 0.0;
-    }
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  const double sgn = par ? -1.0 : 1.0;
+  // the middle row of odd N contributes once to the even sum and not at all to the odd one
+  const int midk = (mirror && (Nrows & 1)) ? (Nrows - 1) / 2 : -1;
+
+  load_tile(0, 0);
+  for (int t = 0; t < ntiles; ++t) {
+    const int buf = t & 1;
+    if (t + 1 < ntiles)
+      load_tile(t + 1, buf ^ 1);
+    else
+      g_commit();
+    g_wait1();
     __syncthreads();
+    const double* as = As[buf];
+    const double* bs = Bs[buf];
+    const double* bm = Bm[buf];
 #pragma unroll
-    for (int kk = 0; kk < GBK; ++kk) {
-      double a[4], bb[4];
+    for (int ks = 0; ks < GBK / 4; ++ks) {
+      const int kk = ks * 4 + tig;
+      double a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+      for (int i = 0; i < 4; ++i) a[i] = as[(wm * 32 + i * 8 + gid) * ASTR + kk];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bb[j] = Bs[kk][tx + 16 * j];
+      for (int j = 0; j < 4; ++j) {
+        const int cidx = kk * BSTR + wn * 32 + j * 8 + gid;
+        double v = bs[cidx];
+        if (mirror) {
+          const int gk = t * GBK + kk;
+          v = (gk == midk) ? (par ? 0.0 : v) : fma(sgn, bm[cidx], v);
+        }
+        b[j] = v;
+      }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
     }
     __syncthreads();
   }
+  g_wait0();
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    int gr = row0 + ty * 4 + i;
+    const int gr = row0 + wm * 32 + i * 8 + gid;
     if (gr >= Mo) continue;
-    double* C = bt.out[b * nsplit + gr / rows_per_out] + (size_t)(gr % rows_per_out) * ldc;
+    const int orow = mirror ? 2 * gr + par : gr;
+    double* C = it.C + (size_t)orow * ldc;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      int gc = col0 + tx + 16 * j;
-      if (gc < ncol) C[gc] = acc[i][j];
+      const int gc = col0 + wn * 32 + j * 8 + tig * 2;
+      if (gc + 1 < ncol) {
+        *reinterpret_cast<double2*>(C + gc) = make_double2(acc[i][j][0], acc[i][j][1]);
+      } else if (gc < ncol) {
+        C[gc] = acc[i][j][0];
+      }
     }
   }
 }
 }  // namespace
 
-void launch_gemm_f64(const double* A, int Mo, int K, const GemmBatch& bt, int nbatch, int ncol, int ldb,
-                     int ldc, int rows_per_out, int nsplit, cudaStream_t st) {
-  dim3 grid((ncol + GBN - 1) / GBN, (Mo + GBM - 1) / GBM, nbatch);
-  k_gemm_f64<<<grid, 256, 0, st>>>(A, Mo, K, bt, ncol, ldb, ldc, rows_per_out, nsplit);
+void launch_gemm_f64(const GemmBatch& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, cudaStream_t st) {
+  int mmax = 0;
+  for (int b = 0; b < nbatch; ++b) mmax = bt.item[b].M > mmax ? bt.item[b].M : mmax;
+  dim3 grid((ncol + GBN - 1) / GBN, (mmax + GBM - 1) / GBM, nbatch);
+  k_gemm_f64<<<grid, GTH, kGemmSmem, st>>>(bt, ncol, ldb, ldc, Nrows);
 }
 
 // ---------------------------------------------------------------------------
@@ -195,14 +275,33 @@ __global__ void __launch_bounds__(256) k_xprod(XProdArgs a) {
   double2* Y = sm + M;
   double2* W = sm + 2 * M;
   double2* P = sm + 3 * M;  // prod_b + i prod_ux
-  double* Puz = reinterpret_cast<double*>(sm + 4 * M);
+  double* Puz = reinterpret_cast<double*>(sm + 4 * M);  // after the products are formed
+  double2* Rrows = sm + 4 * M + (M + 1) / 2;              // the 6 combined input rows (6 Nk entries)
   const int z = blockIdx.x;
   const size_t ro = (size_t)z * Nk;
   const int half = M / 2;
+  // Grid row z from the even/odd Chebyshev half planes: rows z < H are E + O,
+  // mirrored rows N-1-z are E - O for values and -E + O for z-derivatives.
+  double2* R = Rrows;
+  {
+    const int Nz = a.Nz;
+    const int zm = Nz - 1 - z;
+    const bool lower = z <= zm;
+    const int zr = lower ? z : zm;
+    const size_t rr = (size_t)zr * Nk;
+    for (int k = threadIdx.x; k < Nk; k += blockDim.x)
+      for (int f = 0; f < 3; ++f) {
+        const double2 ev = a.ev[f][rr + k], ov = a.ov[f][rr + k];
+        const double2 ed = a.ed[f][rr + k], od = a.od[f][rr + k];
+        R[(2 * f) * Nk + k] = lower ? make_double2(ev.x + ov.x, ev.y + ov.y) : make_double2(ev.x - ov.x, ev.y - ov.y);
+        R[(2 * f + 1) * Nk + k] = lower ? make_double2(ed.x + od.x, ed.y + od.y) : make_double2(od.x - ed.x, od.y - ed.y);
+      }
+  }
+  __syncthreads();
   // 1. velocity spectrum
   {
-    const double2* gx = a.val[1] + ro;
-    const double2* gz = a.val[2] + ro;
+    const double2* gx = R + 2 * Nk;
+    const double2* gz = R + 4 * Nk;
     for (int k = threadIdx.x; k < M; k += blockDim.x) {
       double2 v;
       if (k <= half) {
@@ -219,8 +318,8 @@ __global__ void __launch_bounds__(256) k_xprod(XProdArgs a) {
   double2* F0 = (U == X) ? Y : X;  // free buffers: F0 and W
   // 2. gradients of each field and the advection products
   for (int f = 0; f < 3; ++f) {
-    const double2* gv = a.val[f] + ro;
-    const double2* gd = a.dz[f] + ro;
+    const double2* gv = R + (2 * f) * Nk;
+    const double2* gd = R + (2 * f + 1) * Nk;
     for (int k = threadIdx.x; k < M; k += blockDim.x) {
       int q = (k <= half) ? k : M - k;
       double2 Ax = make_double2(0.0, 0.0);
@@ -399,16 +498,20 @@ __global__ void __launch_bounds__(256) k_x_dealias_mul(const double* __restrict_
 
 cudaError_t set_transform_smem_limits(int bytes) {
   cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem)) != cudaSuccess)
+    return e;
   if ((e = cudaFuncSetAttribute(k_xprod, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_x_rfft, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_x_irfft, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_x_dealias_mul, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-size_t xprod_smem_bytes(int M) { return (size_t)M * (4 * sizeof(double2) + sizeof(double)); }
+size_t xprod_smem_bytes(int M, int Nk) {
+  return (size_t)M * 4 * sizeof(double2) + (size_t)((M + 1) / 2) * sizeof(double2) + (size_t)6 * Nk * sizeof(double2);
+}
 
 void launch_xprod(const XProdArgs& a, cudaStream_t st) {
-  size_t smem = xprod_smem_bytes(a.M);
+  size_t smem = xprod_smem_bytes(a.M, a.Nk);
   k_xprod<<<a.Nz, 256, smem, st>>>(a);
 }
 

@@ -1,0 +1,109 @@
+"""Seeded synthetic workloads for the benchmark configurations.
+
+The reference seeds its initial noise with Julia's RNG
+(src/core/field/field_layout/field_layout_operations.jl:34-60), which cannot be
+reproduced here; these workloads draw the same kind of noise from NumPy's
+PCG64 so that the CPU oracle and the library see identical arrays.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class RBCConfig:
+    """2D Rayleigh-Benard: ChannelDomain(Nx, Nz; Lx, Lz), Boussinesq with tau/lift BCs."""
+
+    Nx: int = 1024
+    Nz: int = 256
+    Lx: float = 4.0
+    Lz: float = 1.0
+    Ra: float = 1e8
+    Pr: float = 1.0
+    dt: float = 0.01
+    scheme: str = "RK443"
+    seed: int = 42
+    noise: float = 1e-3
+
+    @property
+    def kappa(self) -> float:  # free-fall scaling, test/test_subproblem_rk.jl:23-24
+        return (self.Ra * self.Pr) ** -0.5
+
+    @property
+    def nu(self) -> float:
+        return (self.Ra / self.Pr) ** -0.5
+
+
+C1 = RBCConfig(Nx=256, Nz=64, Ra=2e6, dt=0.125, scheme="RK222")
+C2 = RBCConfig(Nx=1024, Nz=256, Ra=1e8, dt=0.01, scheme="RK443")
+
+
+def rbc_initial_grid(cfg: RBCConfig) -> np.ndarray:
+    """b0 = Lz - z + noise * z (Lz - z) xi on the (Nz, Nx) grid, xi ~ N(0,1) from PCG64(seed)."""
+    rng = np.random.default_rng(cfg.seed)
+    xi = rng.standard_normal((cfg.Nx, cfg.Nz)).T
+    z = (cfg.Lz / 2.0 * (1.0 - np.cos(np.pi * np.arange(cfg.Nz) / (cfg.Nz - 1))))[:, None]
+    return (cfg.Lz - z) + cfg.noise * z * (cfg.Lz - z) * xi
+
+
+def state_bytes(cfg: RBCConfig) -> int:
+    """Bytes of the coefficient state (b, ux, uz, p and 7 taus), complex128."""
+    nk = cfg.Nx // 2 + 1
+    return 16 * (4 * cfg.Nz * nk + 7 * nk)
+
+
+TABLEAU_PATTERNS = {
+    # (AE nonzero pattern, AI nonzero pattern, bE, bI) of src/core/timesteppers/types.jl:49-167
+    "RK222": (
+        [[0, 0, 0], [1, 0, 0], [1, 1, 0]],
+        [[0, 0, 0], [0, 1, 0], [0, 1, 1]],
+        [0, 1, 1],
+        [0, 1, 1],
+    ),
+    "RK443": (
+        [[0, 0, 0, 0], [1, 0, 0, 0], [1, 1, 0, 0], [1, 1, 1, 0]],
+        [[0, 0, 0, 0], [0, 1, 0, 0], [0, 1, 1, 0], [0, 1, 1, 1]],
+        [0, 1, 1, 1],
+        [0, 1, 1, 1],
+    ),
+}
+
+
+def step_model_bytes(cfg: RBCConfig, scheme: str) -> float:
+    """Algorithmic HBM bytes of one step under the hot-path byte model.
+
+    C = one complex coefficient field, V = one equation-space vector over all
+    modes, Phi = the per-mode bordered-banded LHS at nominal size (n*848 B).
+    Per stage: read MX0, read every F_j / LX_j with a nonzero tableau entry,
+    read Phi if a_ii != 0, write X_i, RHS reads the 3 advected fields and
+    writes 3 F fields; if L X_i is used later: read X_i, read Phi, write LX_i.
+    Plus the pre-stage M X_n (2V) and the final update.  SBDF2: one RHS,
+    one solve and the history terms.
+    """
+    nk = cfg.Nx // 2 + 1
+    n = 4 * cfg.Nz + 7
+    C = nk * cfg.Nz * 16.0
+    V = nk * n * 16.0
+    Phi = nk * n * 848.0
+    if scheme == "SBDF2":
+        # nominal multistep count: the RHS (6C), the solve and the L X history term
+        # each read Phi, plus the state / history / F vectors (12 V)
+        return 2 * Phi + 12 * V + 6 * C
+    AE, AI, bE, bI = TABLEAU_PATTERNS[scheme]
+    s = len(bE)
+    total = 2 * V
+    for i in range(s):
+        total += V
+        for j in range(i):
+            total += V * (AE[i][j] + AI[i][j])
+        if AI[i][i]:
+            total += Phi
+        total += V + 6 * C
+        used_later = any(AI[k][i] for k in range(i + 1, s)) or bI[i]
+        if used_later:
+            total += 2 * V + Phi
+    total += V + sum(V * (bE[j] + bI[j]) for j in range(s)) + 2 * V
+    return total

@@ -1,0 +1,86 @@
+"""Generate the golden fixtures used by the parity tests.
+
+Run from the repository root:  python tests/golden/make_golden.py
+
+The fixtures are outputs of the CPU oracle (oracle/tarang_oracle.py) on seeded
+inputs at sizes the oracle finishes in seconds.  The oracle itself is pinned to
+the reference's analytic known-answer tests (tests/test_oracle_known_answers.py);
+these files freeze its outputs so that both the oracle and the CUDA library are
+checked against the same numbers on every run.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.tarang_oracle import (  # noqa: E402
+    RBC2D,
+    RBCParams,
+    backward_2d,
+    forward_2d,
+    padded_multiply,
+    rbc_initial_b,
+    run_rbc,
+)
+
+CASES = [
+    # name, Nx, Nz, Ra, scheme, dt, nsteps
+    ("rbc_rk222_32x16", 32, 16, 2e6, "RK222", 0.125, 6),
+    ("rbc_rk443_48x24", 48, 24, 1e8, "RK443", 0.01, 6),
+    ("rbc_sbdf2_32x16", 32, 16, 1e8, "SBDF2", 0.01, 6),
+    ("rbc_rk222_64x17", 64, 17, 1e6, "RK222", 0.05, 5),
+]
+
+
+def make_transform_fixture(path: str) -> None:
+    rng = np.random.default_rng(2024)
+    out = {}
+    for Nx, Nz in ((16, 11), (24, 16), (96, 24)):
+        g = rng.standard_normal((Nz, Nx))
+        a = rng.standard_normal((Nz, Nx))
+        b = rng.standard_normal((Nz, Nx))
+        c = forward_2d(rng.standard_normal((Nz, Nx)))
+        key = f"{Nx}x{Nz}"
+        out[f"grid_{key}"] = g
+        out[f"coeff_{key}"] = forward_2d(g)
+        out[f"bcoeff_{key}"] = c
+        out[f"bgrid_{key}"] = backward_2d(c, Nx)
+        out[f"a_{key}"] = a
+        out[f"b_{key}"] = b
+        out[f"prod_{key}"] = padded_multiply(a, b)
+        p = RBCParams(Nx=Nx, Nz=Nz)
+        sim = RBC2D(p)
+        ins = [forward_2d(rng.standard_normal((Nz, Nx))) for _ in range(3)]
+        outs = sim.rhs(*ins)
+        for i in range(3):
+            out[f"rhs_in{i}_{key}"] = ins[i]
+            out[f"rhs_out{i}_{key}"] = outs[i]
+    np.savez_compressed(path, **out)
+
+
+def make_step_fixture(path: str, Nx, Nz, Ra, scheme, dt, nsteps) -> None:
+    p = RBCParams(Nx=Nx, Nz=Nz, Lx=4.0, Lz=1.0, Ra=Ra, Pr=1.0)
+    b0 = forward_2d(rbc_initial_b(p, 42))
+    sim = run_rbc(p, scheme, dt, nsteps, seed=42)
+    np.savez_compressed(
+        path,
+        Nx=Nx, Nz=Nz, Ra=Ra, dt=dt, nsteps=nsteps, scheme=scheme,
+        b0=b0, b=sim.b, ux=sim.ux, uz=sim.uz, p=sim.pr, tau=sim.tau,
+    )
+
+
+def main() -> None:
+    make_transform_fixture(os.path.join(HERE, "transforms.npz"))
+    for name, Nx, Nz, Ra, scheme, dt, ns in CASES:
+        make_step_fixture(os.path.join(HERE, f"{name}.npz"), Nx, Nz, Ra, scheme, dt, ns)
+    print("wrote fixtures to", HERE)
+
+
+if __name__ == "__main__":
+    main()
