@@ -52,15 +52,20 @@ class Dist:
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.backend = None
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                    device_id=torch.device("cuda", self.local))
+            self.backend = os.environ.get("TB_DIST_BACKEND", "nccl")
+            if self.backend == "nccl":
+                torch.cuda.set_device(self.local)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                        device_id=torch.device("cuda", self.local))
+            else:
+                dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=120))
             self.pg = dist
 
     def barrier(self):
@@ -72,7 +77,8 @@ class Dist:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -165,16 +171,24 @@ def kernel_work(name: str, cfg, scheme: str):
     nb = {0: 3, 1: 4}
     n = 2 * N  # band rows per parity class
     if name == "z_backward_gemm":
-        return "flops", 2.0 * (2 * N) * N * (2 * nk) * 3
+        # values and z-derivatives from the even/odd coefficient halves: per field
+        # (H x Ke + H x Ko) x 2 multiply-adds per column, H = ceil(Nz/2)
+        H = (N + 1) // 2
+        return "flops", 2.0 * 2 * H * N * (2 * nk) * 3
     if name == "z_forward_gemm":
-        return "flops", 2.0 * N * N * (2 * nk) * 3
+        H = (N + 1) // 2
+        return "flops", 2.0 * N * H * (2 * nk) * 3
     if name == "x_fft_products":
+        # reads 12 half planes (values, z-derivatives; even/odd) and writes 3 planes
         return "bytes", 9.0 * plane
     if name == "tau_solve":
-        # factors: pivots (1 B) + L (4) + U (13) + border (nb) + C multipliers (nb) doubles per row,
-        # Schur inverse; rhs read (4 planes) and unknowns written (4 planes + taus)
-        fac = sum(nk * (n * (1 + 8 * (4 + 13 + 2 * nb[c])) + 8 * nb[c] ** 2) for c in (0, 1))
-        return "bytes", fac + 4.0 * plane + 4.0 * plane
+        # streamed factor records (forward 9 + backward 18 doubles per row, class, mode,
+        # rows padded to a multiple of 12) + Schur inverses; rhs read (4 planes);
+        # unknowns written (4 planes + taus)
+        npad = (n + 11) // 12 * 12
+        groups = (nk + 3) // 4
+        fac = groups * 4 * (npad * 2 * (9 + 18) * 8 + 2 * 16 * 8)
+        return "bytes", fac + 4.0 * plane + 4.0 * plane + 7 * nk * 16
     if name == "stage_lincomb":
         return "bytes", None  # depends on the stage; reported only if dominant
     if name == "lx_finalize":

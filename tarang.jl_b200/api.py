@@ -119,7 +119,7 @@ def ChannelDomain(Nx: int, Nz: int, Lx: float = 2 * math.pi, Lz: float = 2.0, dt
 # Plans (the C ABI object behind a solver)
 # ---------------------------------------------------------------------------
 
-_TS = {"RK222": L.TB_RK222, "RK443": L.TB_RK443, "SBDF1": L.TB_SBDF1, "SBDF2": L.TB_SBDF2}
+_TS_IDS = {"RK222": L.TB_RK222, "RK443": L.TB_RK443, "SBDF1": L.TB_SBDF1, "SBDF2": L.TB_SBDF2}
 
 
 class Plan:
@@ -432,7 +432,7 @@ class InitialValueSolver:
         self.problem = problem
         self.timestepper = timestepper
         self.dt = dt
-        self.plan = Plan(domain, spec["kappa"], spec["nu"], spec["b_bottom"], spec["b_top"], _TS[timestepper.name])
+        self.plan = Plan(domain, spec["kappa"], spec["nu"], spec["b_bottom"], spec["b_top"], _TS_IDS[timestepper.name])
         names = spec["names"]
         b, u, p = fields[names["b"]], fields[names["u"]], fields[names["p"]]
         binds = [(b, (L.TB_FIELD_B, None)), (u.components[0], (L.TB_FIELD_UX, None)),

@@ -1,0 +1,52 @@
+"""The N>1 plumbing of bench.py on CPU: two gloo ranks, replicas only.
+
+Each rank runs the reference arm on a tiny slice of work; rank 0 alone prints
+the JSON line, both ranks exit 0, and the barrier / max-over-ranks helpers
+agree across ranks."""
+import json
+import os
+import subprocess
+import sys
+
+from __graft_entry__ import ROOT
+
+
+def _run_two_ranks(code: str, port: int):
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE="2", MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port), TB_DIST_BACKEND="gloo", PYTHONPATH=ROOT)
+        procs.append(subprocess.Popen([sys.executable, "-c", code], env=env, cwd=ROOT, stdout=subprocess.PIPE,
+                                      stderr=subprocess.PIPE, text=True))
+    outs = [p.communicate(timeout=180) for p in procs]
+    return [(p.returncode, o, e) for p, (o, e) in zip(procs, outs)]
+
+
+def test_dist_barrier_and_max_over_ranks():
+    code = (
+        "import bench\n"
+        "d = bench.Dist()\n"
+        "d.barrier()\n"
+        "print(d.max(float(d.rank) * 10 + 1))\n"
+        "d.close()\n"
+    )
+    res = _run_two_ranks(code, 29611)
+    for rc, out, err in res:
+        assert rc == 0, err
+        assert float(out.strip().splitlines()[-1]) == 11.0
+
+
+def test_reference_arm_prints_once_under_two_ranks():
+    code = (
+        "import sys\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--config', 'c1', '--steps', '1', '--warmup', '0']\n"
+        "import bench\n"
+        "bench.main()\n"
+    )
+    res = _run_two_ranks(code, 29623)
+    assert all(rc == 0 for rc, _, _ in res), [e[-2000:] for _, _, e in res]
+    lines0 = [l for l in res[0][1].splitlines() if l.startswith("{")]
+    lines1 = [l for l in res[1][1].splitlines() if l.startswith("{")]
+    assert len(lines0) == 1 and not lines1
+    d = json.loads(lines0[0])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0

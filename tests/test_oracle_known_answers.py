@@ -1,0 +1,203 @@
+"""The CPU oracle against the reference's own known-answer tests.
+
+Each case restates an analytic check from the reference test suite or docs:
+  - transform round trip / known Chebyshev coefficients  test/test_gpu_fc_2d_complete.jl:66-190
+  - spectral derivatives vs analytic                    test/test_gpu_fc_2d_complete.jl:195-260
+  - 3/2-dealiased products (incl. the Nyquist case)     test/test_gpu_fc_2d_complete.jl:262-330
+  - Chebyshev D, BC rows, integration weights           test/test_chebyshev.jl:126-400
+  - tau-method Poisson quick start u = z(1-z)           docs/src/pages/tau_method.md:35-85
+  - walls enforced after nonlinear steps                test/test_gpu_fc_2d_complete.jl:395-420
+  - RBC builds and steps finitely                        test/test_subproblem_rk.jl:19-110
+  - min-norm mass solve = least squares                  test/test_batched_mass_solve.jl:169-220
+  - time-stepper order on an exact linear solution      test/test_timestepper_boundaries.jl:78-176
+"""
+import numpy as np
+import numpy.polynomial.chebyshev as npc
+import pytest
+
+from oracle.tarang_oracle import (
+    RBC2D,
+    RBCParams,
+    backward_2d,
+    cheb_diff_matrix,
+    cheb_eval_row,
+    cheb_forward,
+    cheb_grid,
+    cheb_integ_row,
+    fourier_grid,
+    forward_2d,
+    padded_length,
+    padded_multiply,
+    rbc_initial_b,
+    rel_l2,
+    run_rbc,
+    wavenumbers_rfft,
+)
+
+
+def test_grids_and_wavenumbers():
+    z = cheb_grid(9, 0.0, 1.0)
+    assert z[0] == pytest.approx(0.0, abs=1e-15) and z[-1] == pytest.approx(1.0)
+    assert np.all(np.diff(z) > 0)
+    assert np.allclose(fourier_grid(8, 2 * np.pi), np.arange(8) * np.pi / 4)
+    assert np.allclose(wavenumbers_rfft(8, 4.0), 2 * np.pi / 4 * np.arange(5))
+    assert padded_length(12) == 18 and padded_length(256) == 384 and padded_length(1024) == 1536
+    assert padded_length(6) == 10  # ceil(9) bumped to even
+
+
+def test_transform_roundtrip_and_known_coefficients():
+    Nx, Nz = 8, 9
+    x = fourier_grid(Nx, 2 * np.pi)
+    z = cheb_grid(Nz, 0.0, 1.0)
+    prof = 1 + z + 0.25 * (2 * z**2 - 1)
+    g = prof[:, None] * np.sin(2 * x)[None, :]
+    c = forward_2d(g)
+    assert np.abs(backward_2d(c, Nx) - g).max() < 1e-14
+    # sin(2x) -> rfft bin 2 = -i Nx/2 ; profile's Chebyshev-T coefficients on [0,1]
+    X = 2 * z - 1
+    want = npc.chebfit(X, prof, Nz - 1)
+    assert np.allclose(c[:, 2], -1j * Nx / 2 * want, atol=1e-13)
+    assert np.abs(np.delete(c, 2, axis=1)).max() < 1e-13
+
+
+def test_spectral_derivatives_match_analytic():
+    Nx, Nz = 16, 11
+    x = fourier_grid(Nx, 2 * np.pi)
+    z = cheb_grid(Nz, 0.0, 1.0)
+    prof, dprof = z**2 * (1 - z), 2 * z - 3 * z**2
+    g = prof[:, None] * np.sin(2 * x)[None, :]
+    c = forward_2d(g)
+    k = wavenumbers_rfft(Nx, 2 * np.pi)
+    D = cheb_diff_matrix(Nz, 1.0)
+    gx = backward_2d(1j * k[None, :] * c, Nx)
+    gz = backward_2d(D @ c, Nx)
+    assert np.abs(gx - prof[:, None] * 2 * np.cos(2 * x)[None, :]).max() < 2e-10
+    assert np.abs(gz - dprof[:, None] * np.sin(2 * x)[None, :]).max() < 2e-10
+
+
+def test_dealiased_product_resolved_case_is_pointwise():
+    Nx, Nz = 12, 9
+    x = fourier_grid(Nx, 2 * np.pi)
+    z = cheb_grid(Nz, 0.0, 1.0)
+    a = (1 + z)[:, None] * np.cos(2 * x)[None, :]
+    b = (1 - z)[:, None] * np.sin(3 * x)[None, :]
+    assert np.abs(padded_multiply(a, b) - a * b).max() < 3e-9
+
+
+def test_dealiased_product_nyquist_case():
+    # cos(6x)(1+z) * cos(6x)(1-z) on 12 points: the Nyquist bin is split X/2 at
+    # +-6 on the 18-point grid, cos(12x) aliases onto +-6 there, and truncation
+    # folds both images back into the Nyquist bin.  Worked by hand from
+    # nonlinear_padding.jl:182-226, 294-346, 359-443:
+    #   result = (1 - z^2) (1 + cos(6x)) / 2
+    Nx, Nz = 12, 9
+    x = fourier_grid(Nx, 2 * np.pi)
+    z = cheb_grid(Nz, 0.0, 1.0)
+    a = (1 + z)[:, None] * np.cos(6 * x)[None, :]
+    b = (1 - z)[:, None] * np.cos(6 * x)[None, :]
+    want = (1 - z**2)[:, None] * (1 + np.cos(6 * x))[None, :] / 2
+    assert np.abs(padded_multiply(a, b) - want).max() < 1e-14
+
+
+def test_chebyshev_operator_rows():
+    N = 12
+    D = cheb_diff_matrix(N, 2.0)  # [-1, 1]
+    for n in range(N):
+        e = np.zeros(N)
+        e[n] = 1
+        want = npc.chebder(e) if n > 0 else np.zeros(1)
+        got = D @ e
+        assert np.allclose(got[: len(want)], want) and np.allclose(got[len(want):], 0)
+    assert np.allclose(cheb_eval_row(N, 1.0), 1) and np.allclose(cheb_eval_row(N, -1.0), (-1.0) ** np.arange(N))
+    w = cheb_integ_row(N, 1.0)
+    for n in range(N):
+        e = np.zeros(N)
+        e[n] = 1
+        I = npc.chebint(e, lbnd=-1)
+        assert w[n] == pytest.approx(0.5 * npc.chebval(1.0, I), abs=1e-14)
+
+
+def test_tau_poisson_quick_start():
+    # D^2 u + tau1 e_{N-1} + tau2 e_{N-2} = -2 e_0, u(0) = u(1) = 0  ->  u = z(1-z)
+    N = 16
+    D = cheb_diff_matrix(N, 1.0)
+    A = np.zeros((N + 2, N + 2))
+    A[:N, :N] = D @ D
+    A[N - 1, N] = 1.0
+    A[N - 2, N + 1] = 1.0
+    A[N, :N] = cheb_eval_row(N, -1.0)
+    A[N + 1, :N] = cheb_eval_row(N, 1.0)
+    rhs = np.zeros(N + 2)
+    rhs[0] = -2.0
+    sol = np.linalg.solve(A, rhs)
+    z = cheb_grid(N, 0.0, 1.0)
+    u = cheb_forward(np.eye(N))  # unused columns; evaluate through the backward map
+    from oracle.tarang_oracle import cheb_backward
+
+    ug = cheb_backward(sol[:N])
+    assert np.abs(ug - z * (1 - z)).max() < 1e-14
+    assert abs(sol[N]) < 1e-12 and abs(sol[N + 1]) < 1e-12
+
+
+def test_rbc_builds_and_enforces_walls():
+    p = RBCParams(Nx=16, Nz=8, Lx=4.0, Lz=1.0, Ra=1e4)
+    sim = RBC2D(p)
+    for m in (0, 3):
+        M, L, bc, af = sim.mode_matrices(m)
+        assert M.shape == L.shape == (sim.n_unknowns(m),) * 2
+        assert len(bc) == (7 if m == 0 else 6)
+    sim.set_b_grid(rbc_initial_b(p))
+    for _ in range(5):
+        sim.step(0.01, "RK222")
+    bg = backward_2d(sim.b, p.Nx)
+    uz = backward_2d(sim.uz, p.Nx)
+    assert np.isfinite(bg).all() and np.isfinite(uz).all()
+    assert np.abs(bg[0] - p.Lz).max() < 1e-8 and np.abs(bg[-1]).max() < 1e-8
+    assert np.abs(uz[0]).max() < 1e-8 and np.abs(uz[-1]).max() < 1e-8
+
+
+def test_mass_solve_is_min_norm_least_squares():
+    p = RBCParams(Nx=8, Nz=8)
+    sim = RBC2D(p)
+    M = sim.dense_mode_matrices(2)[0]
+    rhs = np.random.default_rng(0).standard_normal(M.shape[0]) + 0j
+    want = np.linalg.lstsq(M, rhs, rcond=None)[0]
+    assert np.allclose(sim.mass_solve(2, rhs), want, atol=1e-14)
+
+
+def test_sparse_and_dense_tau_solves_agree():
+    # batched-vs-per-mode parity analogue (test_mode_batch_parity.jl:411-455): 1e-12
+    p = RBCParams(Nx=16, Nz=12, Ra=1e6)
+    sim = RBC2D(p)
+    rng = np.random.default_rng(1)
+    for m in (0, 1, 8):
+        M, L, _, _ = sim.dense_mode_matrices(m)
+        A = M + 0.05 * L
+        r = rng.standard_normal(A.shape[0]) + 1j * rng.standard_normal(A.shape[0])
+        x_sparse = sim._lhs_lu(m, 1.0, 0.05).solve(r)
+        x_dense = np.linalg.solve(A, r)
+        assert rel_l2(x_sparse, x_dense) < 1e-12
+
+
+def _diffusion_error(scheme, dt, T=0.4):
+    # Horizontally uniform b: no flow develops and b diffuses exactly,
+    # b = Lz - z + A exp(-kappa pi^2 t) sin(pi z), Lz = 1.
+    p = RBCParams(Nx=8, Nz=24, Lx=4.0, Lz=1.0, Ra=25.0, Pr=1.0)
+    sim = RBC2D(p)
+    z = cheb_grid(p.Nz, 0.0, 1.0)
+    A = 0.3
+    g = np.repeat(((1 - z) + A * np.sin(np.pi * z))[:, None], p.Nx, axis=1)
+    sim.set_b_grid(g)
+    n = int(round(T / dt))
+    for _ in range(n):
+        sim.step(dt, scheme)
+    exact = (1 - z) + A * np.exp(-p.kappa * np.pi**2 * n * dt) * np.sin(np.pi * z)
+    return np.abs(backward_2d(sim.b, p.Nx)[:, 0] - exact).max()
+
+
+@pytest.mark.parametrize("scheme,order", [("RK222", 2), ("RK443", 3), ("SBDF2", 2)])
+def test_timestepper_order_on_exact_diffusion(scheme, order):
+    e1 = _diffusion_error(scheme, 0.1)
+    e2 = _diffusion_error(scheme, 0.05)
+    rate = np.log2(e1 / e2)
+    assert rate > order - 0.3, (scheme, e1, e2, rate)
