@@ -345,6 +345,14 @@ def run_ours(args, cfg, scheme, dist):
                     "flops_per_launch": work, "peak_source": "cuBLAS FP64 GEMM (torch.matmul float64) measured in bench"}
         roof["avg_launch_ms"] = avg_ms
         roof["peak_source"] = roof.get("peak_source", f"MEASURED_PEAKS.json ({peak_src})")
+        # DRAM traffic per launch from the committed ncu capture of this workload
+        tpath = os.path.join(ROOT, "profiles", f"traffic_{cfg.Nx}x{cfg.Nz}_{scheme.lower()}.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                tr = json.load(f)
+            if top in tr:
+                roof["traffic"] = tr[top]
+                roof["traffic_source"] = tpath.replace(ROOT + os.sep, "")
     model = W.step_model_bytes(cfg, scheme)
     step_roof = {"bytes_per_step_model": model, "achieved_gbs": model / (ms / args.steps / 1e3) / 1e9,
                  "peak_gbs": peaks.get("hbm_gbs")}
