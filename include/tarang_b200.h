@@ -150,6 +150,19 @@ tb_status tb_transform_backward(tb_plan* plan, const double* coeff, double* grid
  * src/core/nonlinear/nonlinear_padding.jl:359-443).  Device pointers. */
 tb_status tb_dealiased_multiply(tb_plan* plan, const double* a_grid, const double* b_grid, double* out_grid);
 
+/* The same 3/2-dealiased product without a plan and without allocating any
+ * device memory (no counterpart in the reference).  For callers that must not
+ * let a library call cudaMalloc -- a host runtime that owns a device memory
+ * pool, or a process whose device footprint is fixed after start-up.  a_grid,
+ * b_grid, out_grid: the caller's device buffers, Nz rows of Nx doubles.  The
+ * FFT twiddles live in a static device array of the library (80 KiB per GPU,
+ * held until exit), so Nx <= 2048 (else TB_ENOTSUPPORTED).  Calls share that
+ * array: calls that overlap on the GPU race.  The first call on a device
+ * resolves the array's address (once per device); make it before any stream
+ * capture.  Runs on the legacy default stream and returns when done. */
+tb_status tb_dealiased_multiply_noalloc(int device, int Nx, int Nz, const double* a_grid, const double* b_grid,
+                                        double* out_grid);
+
 /* RHS program: F = -(u.grad) f for f in (b, ux, uz), coefficient space in and
  * out.  Replaces execute_lazy_rhs_buffered! for the RBC program
  * (src/core/solvers/lazy_rhs.jl:1542-1561).  in: 3 coefficient fields

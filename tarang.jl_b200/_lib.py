@@ -73,6 +73,7 @@ SIGNATURES = {
     "tb_transform_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
     "tb_transform_backward": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
     "tb_dealiased_multiply": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "tb_dealiased_multiply_noalloc": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "tb_rhs_advection": (c_int, [c_void_p, c_void_p, c_void_p]),
     "tb_batched_lu_factor": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, POINTER(c_int)]),
     "tb_batched_lu_solve": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),

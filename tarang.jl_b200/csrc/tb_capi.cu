@@ -165,6 +165,12 @@ namespace {
 
 thread_local std::string g_err;
 
+}  // namespace
+
+void tb::set_thread_error(const std::string& msg) { g_err = msg; }
+
+namespace {
+
 tb_status fail(tb_context* ctx, const Error& e) {
   if (ctx) ctx->last_error = e.msg;
   g_err = e.msg;

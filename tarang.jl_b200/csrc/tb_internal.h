@@ -83,6 +83,9 @@ struct TauLayout {
   ClassLayout cls[2];
 };
 
+// Records a message for tb_last_error(NULL) on the calling thread.
+void set_thread_error(const std::string& msg);
+
 // Builds the banded layout for the RBC program (host, once per plan).
 TauLayout build_rbc_layout(int Nz, double Lx, double Lz, double kappa, double nu, double Nx_scale,
                            double b_bottom, double b_top);
