@@ -675,6 +675,7 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
     TB_REQUIRE(P->lay.cls[0].n == P->lay.cls[1].n, TB_ENOTSUPPORTED, "parity classes of unequal size");
     TB_REQUIRE(tau_solve_smem_bytes((P->lay.cls[0].n + kTauRowPad - 1) / kTauRowPad * kTauRowPad) <= 227 * 1024,
                TB_ENOTSUPPORTED, "Nz too large for the staged tau solve");
+    TB_REQUIRE(rk_final_smem_bytes(P->Nz) <= 227 * 1024, TB_ENOTSUPPORTED, "Nz too large for the final RK update");
     P->err_mode.alloc(sizeof(int));
     {
       const int n = P->lay.cls[0].n;

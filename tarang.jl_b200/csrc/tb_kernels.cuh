@@ -58,10 +58,10 @@ constexpr int kTauKL = 4, kTauKU = 8;
 // The solve streams per-row factor records of kSolveModes consecutive Fourier
 // modes: forward record = pivot offset, kTauKL multipliers, 4 boundary-row
 // multipliers; backward record = 1/diag, kTauKL+kTauKU U entries, 4 border
-// entries and the encoded store target of the band column (each entry
-// kSolveModes doubles, mode fastest).
+// entries and the encoded store target of the band column (one contiguous
+// record per mode, an even number of doubles so a lane reads it 16 bytes at a time).
 constexpr int kSolveModes = 4;
-constexpr int kFwdRec = 1 + kTauKL + 4;
+constexpr int kFwdRec = 1 + kTauKL + 4 + 1;  // pivot, multipliers, border, pad to 16 B
 constexpr int kBwdRec = 1 + kTauKL + kTauKU + 4 + 1;
 // Register windows of the solve sweeps; band rows are padded to a multiple of
 // their least common multiple (kTauRowPad) with identity rows.
@@ -84,7 +84,7 @@ struct ClassDev {
   const double* c1_z; // nb x nb
   const double* c1_nz;
   // factors, shared by both classes (set on cls[0]):
-  //   FR[group][row][class][kFwdRec][kSolveModes], BR[group][row][class][kBwdRec][kSolveModes],
+  //   FR[group][row][class][kSolveModes][kFwdRec], BR[group][row][class][kSolveModes][kBwdRec],
   //   SI[group][class][4][4][kSolveModes]
   double* FR;
   double* BR;
@@ -129,5 +129,6 @@ void launch_lx_finalize(double2* LX, const double2* X, const double* s3, int Nz,
 // X_f = S^{-1} (lincomb)[1+f] for f = b, ux, uz; p and taus zeroed.
 void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* s3, int Nz, int Nk,
                      cudaStream_t st);
+size_t rk_final_smem_bytes(int Nz);
 
 }  // namespace tb

@@ -322,6 +322,7 @@ bool make_fft_plan(int n, FftPlan* out) {
   FftPlan p;
   p.n = n;
   int r = n, ns = 0;
+  while (r % 8 == 0 && ns < 16) { p.radix[ns++] = 8; r /= 8; }
   while (r % 4 == 0 && ns < 16) { p.radix[ns++] = 4; r /= 4; }
   while (r % 2 == 0 && ns < 16) { p.radix[ns++] = 2; r /= 2; }
   while (r % 3 == 0 && ns < 16) { p.radix[ns++] = 3; r /= 3; }

@@ -33,6 +33,19 @@ __device__ __forceinline__ bool realified(int unk) {
   return unk == UK_UX || unk == UK_TAU0 + 3 || unk == UK_TAU0 + 5;
 }
 
+// Solve-layout factor records: for group g = m / kSolveModes and band row j the
+// records of both classes and the group's modes are contiguous,
+// FR[g][j][class][mode % kSolveModes][kFwdRec] (and BR likewise), so one lane
+// reads its own record with 16-byte loads and the group's rows stream as a block.
+__device__ __forceinline__ double* fwd_record(double* FR, int npad, int m, int j, int c) {
+  const int g = m / kSolveModes, mm = m % kSolveModes;
+  return FR + ((((size_t)g * npad + j) * 2 + c) * kSolveModes + mm) * kFwdRec;
+}
+__device__ __forceinline__ double* bwd_record(double* BR, int npad, int m, int j, int c) {
+  const int g = m / kSolveModes, mm = m % kSolveModes;
+  return BR + ((((size_t)g * npad + j) * 2 + c) * kSolveModes + mm) * kBwdRec;
+}
+
 // ---------------------------------------------------------------------------
 // Factorisation: one thread per (mode, class).  Banded LU with partial
 // pivoting restricted to the band of the bulk rows; the boundary rows are
@@ -99,12 +112,10 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
         Bd[(size_t)p * NBMAX + b] = t;
       }
     }
-    const int g = m / kSolveModes, mm = m % kSolveModes;
-    double* fr = C.FR + ((((size_t)g * a.npad + j) * 2 + c) * kFwdRec) * kSolveModes + mm;
-    double* br = C.BR + ((((size_t)g * a.npad + j) * 2 + c) * kBwdRec) * kSolveModes + mm;
-    // pivot offset, plus 16 when this band row's right-hand side is a u_x momentum
-    // row (scaled by -i on load)
-    fr[0] = (double)(p - j) + (C.row_eq[j] == EQ_MX ? 16.0 : 0.0);
+    double* fr = fwd_record(C.FR, a.npad, m, j, c);
+    double* br = bwd_record(C.BR, a.npad, m, j, c);
+    // pivot offset p - j in 0..KL, stored as the integer bits of the slot
+    fr[0] = __longlong_as_double((long long)(p - j));
     const double dinv = 1.0 / W[(size_t)j * WW + KL];
     for (int t = 0; t < KL; ++t) {
       const int i = j + 1 + t;
@@ -116,36 +127,36 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
           W[(size_t)i * WW + (cc - i + KL)] -= l * W[(size_t)j * WW + (cc - j + KL)];
         for (int b = 0; b < nb; ++b) Bd[(size_t)i * NBMAX + b] -= l * Bd[(size_t)j * NBMAX + b];
       }
-      fr[(1 + t) * kSolveModes] = l;
+      fr[1 + t] = l;
     }
     for (int q = 0; q < nb; ++q) {
       const double cq = Cr[(size_t)q * nmax + j] * dinv;
       Cr[(size_t)q * nmax + j] = 0.0;
       for (int cc = j + 1; cc <= clast; ++cc) Cr[(size_t)q * nmax + cc] -= cq * W[(size_t)j * WW + (cc - j + KL)];
       for (int b = 0; b < nb; ++b) C1[q * NBMAX + b] -= cq * Bd[(size_t)j * NBMAX + b];
-      fr[(1 + KL + q) * kSolveModes] = cq;
+      fr[1 + KL + q] = cq;
     }
-    for (int q = nb; q < NBMAX; ++q) fr[(1 + KL + q) * kSolveModes] = 0.0;
+    for (int q = nb; q < NBMAX; ++q) fr[1 + KL + q] = 0.0;
+    for (int q = 1 + KL + NBMAX; q < kFwdRec; ++q) fr[q] = 0.0;
     br[0] = dinv;
-    for (int t = 1; t < W1; ++t) br[t * kSolveModes] = (j + t < n) ? W[(size_t)j * WW + KL + t] : 0.0;
-    for (int b = 0; b < NBMAX; ++b) br[(W1 + b) * kSolveModes] = (b < nb) ? Bd[(size_t)j * NBMAX + b] : 0.0;
+    for (int t = 1; t < W1; ++t) br[t] = (j + t < n) ? W[(size_t)j * WW + KL + t] : 0.0;
+    for (int b = 0; b < NBMAX; ++b) br[W1 + b] = (b < nb) ? Bd[(size_t)j * NBMAX + b] : 0.0;
     {
       // store target of this band column: element offset (per mode) into X or the tau
       // array, encoded as offset*2 + (1 if the unknown is scaled by i), bit-cast
       const int unk = C.col_unk[j], kk = C.col_k[j];
       const long long off = unk < 4 ? ((long long)unk * a.Nz + kk) * Nk : (long long)4 * a.Nz * Nk + (long long)(unk - UK_TAU0) * Nk;
-      br[(W1 + NBMAX) * kSolveModes] = __longlong_as_double(2 * off + (realified(unk) ? 1 : 0));
+      br[W1 + NBMAX] = __longlong_as_double(2 * off + (realified(unk) ? 1 : 0));
     }
   }
   // padding rows n..npad-1: identity rows with no right-hand side and no store
   for (int j = n; j < a.npad; ++j) {
-    const int g = m / kSolveModes, mm = m % kSolveModes;
-    double* fr = C.FR + ((((size_t)g * a.npad + j) * 2 + c) * kFwdRec) * kSolveModes + mm;
-    double* br = C.BR + ((((size_t)g * a.npad + j) * 2 + c) * kBwdRec) * kSolveModes + mm;
-    for (int t = 0; t < kFwdRec; ++t) fr[t * kSolveModes] = 0.0;
+    double* fr = fwd_record(C.FR, a.npad, m, j, c);
+    double* br = bwd_record(C.BR, a.npad, m, j, c);
+    for (int t = 0; t < kFwdRec; ++t) fr[t] = 0.0;
     br[0] = 1.0;
-    for (int t = 1; t < kBwdRec - 1; ++t) br[t * kSolveModes] = 0.0;
-    br[(kBwdRec - 1) * kSolveModes] = __longlong_as_double(-1LL);
+    for (int t = 1; t < kBwdRec - 1; ++t) br[t] = 0.0;
+    br[kBwdRec - 1] = __longlong_as_double(-1LL);
   }
   // invert the nb x nb Schur complement (Gauss-Jordan, partial pivoting)
   double Aug[NBMAX][2 * NBMAX];
@@ -191,13 +202,15 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
 }
 
 // ---------------------------------------------------------------------------
-// Solve: one warp per group of kSolveModes Fourier modes.  Lane (c, mm) with
-// c = lane / kSolveModes < 2 runs the forward and backward sweeps of parity
-// class c for mode g*kSolveModes + mm (real and imaginary parts together as a
-// double2).  The factor rows of the group are contiguous records that the
-// whole warp streams into a shared-memory ring with cp.async, kRowsPerStage
-// rows per stage and kStages stages deep; the forward sweep's intermediate y
-// stays in shared memory for the backward sweep.
+// Solve: one warp per group of kSolveModes Fourier modes.  Lane (c, part, mm)
+// runs the forward and backward sweeps of parity class c for mode
+// g*kSolveModes + mm on the real (part 0) or imaginary (part 1) column.  The
+// factor rows of the group are contiguous records that the whole warp streams
+// into a shared-memory ring with cp.async, kRowsPerStage rows per stage and
+// kStages stages deep; each lane then pulls its own records of a window of rows
+// into registers with 16-byte loads before the window's arithmetic, so the
+// sequential sweeps wait on no shared-memory load.  The forward sweep's
+// intermediate y stays in shared memory for the backward sweep.
 // ---------------------------------------------------------------------------
 constexpr int kRowsPerStage = 12;  // a multiple of the forward and backward window lengths
 constexpr int kStages = 6;
@@ -216,14 +229,19 @@ __device__ __forceinline__ void cp_async_wait() {
 template <int KL, int KU>
 __global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
   static_assert(KL + 2 == kFwdWin && KL + KU == kBwdWin, "window sizes follow the band shape");
+  static_assert(kFwdRec == KL + NBMAX + 2 && kFwdRec % 2 == 0, "forward record: pivot, l, border, pad");
+  static_assert(kBwdRec == KL + KU + NBMAX + 2 && kBwdRec % 2 == 0, "backward record: 1/d, u, border, code");
   constexpr int MP = kSolveModes;
   constexpr int W1 = KL + KU + 1;
-  constexpr int FREC = 2 * kFwdRec * MP;  // doubles per forward row (both classes)
-  constexpr int BREC = 2 * kBwdRec * MP;  // doubles per backward row
+  constexpr int FREC = 2 * MP * kFwdRec;  // doubles per forward row (both classes)
+  constexpr int BREC = 2 * MP * kBwdRec;  // doubles per backward row
   constexpr int RREC = 2 * MP;            // double2 rhs entries per row (class, mode)
+  constexpr int FV = kFwdRec / 2, BV = kBwdRec / 2;  // 16-byte words per record
   constexpr int R = kRowsPerStage;
   constexpr int NL = 4 * MP;              // distinct lanes; lanes NL..31 mirror lanes 0..NL-1
+  constexpr int BSUB = 4;                 // backward rows whose records are held in registers at once
   static_assert(NL <= 32 && 32 % NL == 0, "lane layout");
+  static_assert(kBwdWin % BSUB == 0, "backward sub-blocks");
   extern __shared__ __align__(16) double smem[];
   const int np = a.npad;
   const int Nk = a.Nk;
@@ -234,6 +252,7 @@ __global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
   // Mirror lanes repeat the same arithmetic (so the unrolled sweeps stay branch free) and
   // only the owner lanes store.
   const int c = ln / (2 * MP), part = (ln / MP) & 1, mm = ln % MP;
+  const int slot = c * MP + mm;  // this lane's record within a row
   const bool owner = lane < NL;
   const int m = g * MP + mm;
   const bool live = owner && m < Nk;
@@ -243,7 +262,13 @@ __global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
   double* ring = smem;
   double* ysave = smem + (size_t)kStages * STAGE;                  // [row][ln]
   int* rofs = reinterpret_cast<int*>(ysave + (size_t)np * NL);  // [row][class] rhs offset, -1: none
-  for (int q = lane; q < 2 * np; q += 32) rofs[q] = (q < 2 * a.cls[0].n) ? a.rhs_off[q] : -1;
+  unsigned char* rrot = reinterpret_cast<unsigned char*>(rofs + 2 * np);  // [row][class] 1: u_x momentum row
+  for (int q = lane; q < 2 * np; q += 32) {
+    const int row = q / 2, cc = q % 2;
+    const bool in = row < a.cls[cc].n;
+    rofs[q] = (q < 2 * a.cls[0].n) ? a.rhs_off[q] : -1;
+    rrot[q] = (in && a.cls[cc].row_eq[row] == EQ_MX) ? 1 : 0;
+  }
   __syncwarp();
   const double* FRg = a.cls[0].FR + (size_t)g * np * FREC;
   const double* BRg = a.cls[0].BR + (size_t)g * np * BREC;
@@ -271,11 +296,10 @@ __global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
   // scaled by -i, i.e. (re, im) -> (im, -re)
   auto rhs_row = [&](int j) -> double {
     const int s = j / R, r = j % R;
-    const double* base = ring + (size_t)(s % kStages) * STAGE;
-    const double* rb = base + R * FREC + (size_t)(r * RREC + c * MP + mm) * 2;
-    const bool rot = base[(size_t)r * FREC + c * kFwdRec * MP + mm] >= 8.0;
-    const double v = rb[part ^ (rot ? 1 : 0)];
-    return (rot && part) ? -v : v;
+    const double* rb = ring + (size_t)(s % kStages) * STAGE + R * FREC + (size_t)(r * RREC + slot) * 2;
+    const int rot = rrot[2 * j + c];
+    const double v = rb[part ^ rot];
+    return (rot & part) ? -v : v;
   };
   double y[kFwdWin];
   double z[NBMAX];
@@ -292,9 +316,16 @@ __global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
         for (int t = 0; t < kFwdWin; ++t) y[t] = rhs_row(t);
       }
     }
-    const double* st = ring + (size_t)(s % kStages) * STAGE + (size_t)(j0 - s * R) * FREC + c * kFwdRec * MP + mm;
-    // rows j0 .. j0+kFwdWin-1; the right-hand sides entering the window are rows
-    // j0+kFwdWin .. j0+2 kFwdWin-1, resident in stage s or s+1 (or past the end)
+    // this lane's records of rows j0 .. j0+kFwdWin-1, loaded up front
+    const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % kStages) * STAGE +
+                                                         (size_t)(j0 - s * R) * FREC + (size_t)slot * kFwdRec);
+    double2 rv[kFwdWin][FV];
+#pragma unroll
+    for (int u = 0; u < kFwdWin; ++u)
+#pragma unroll
+      for (int v = 0; v < FV; ++v) rv[u][v] = st[u * (FREC / 2) + v];
+    // the right-hand sides entering the window are rows j0+kFwdWin .. j0+2 kFwdWin-1,
+    // resident in stage s or s+1 (or past the end)
     double incoming[kFwdWin];
 #pragma unroll
     for (int u = 0; u < kFwdWin; ++u) {
@@ -303,11 +334,9 @@ __global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
     }
 #pragma unroll
     for (int u = 0; u < kFwdWin; ++u) {
-      const int j = j0 + u;
-      const double* rec = st + (size_t)u * FREC;
-      const double pf = rec[0];
-      const int p = (int)(pf >= 8.0 ? pf - 16.0 : pf);
-      double yj = y[u % kFwdWin];
+      auto rec = [&](int k) -> double { return (k & 1) ? rv[u][k >> 1].y : rv[u][k >> 1].x; };
+      const int p = __double2loint(rv[u][0].x);
+      double yj = y[u];
 #pragma unroll
       for (int t = 1; t <= KL; ++t) {
         const bool sw = (t == p);
@@ -315,12 +344,12 @@ __global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
         y[(u + t) % kFwdWin] = sw ? yj : yt;
         yj = sw ? yt : yj;
       }
-      ysave[(size_t)j * NL + ln] = yj;
+      ysave[(size_t)(j0 + u) * NL + ln] = yj;
 #pragma unroll
-      for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-rec[t * MP], yj, y[(u + t) % kFwdWin]);
+      for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-rec(t), yj, y[(u + t) % kFwdWin]);
 #pragma unroll
-      for (int b = 0; b < NBMAX; ++b) z[b] = fma(-rec[(1 + KL + b) * MP], yj, z[b]);
-      y[u % kFwdWin] = incoming[u];
+      for (int b = 0; b < NBMAX; ++b) z[b] = fma(-rec(1 + KL + b), yj, z[b]);
+      y[u] = incoming[u];
     }
     if ((j0 + kFwdWin) % R == 0) __syncwarp();  // the ring slot of stage s may be refilled next
   }
@@ -362,42 +391,51 @@ __global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
     cp_async_wait<kStages - 1>();
     __syncwarp();
     const int q0 = np - (s + 1) * R;  // rows q0+R-1 .. q0, q0 % kBwdWin == 0
-    const double* st = ring + (size_t)(s % kStages) * STAGE + c * kBwdRec * MP + mm;
-    double xs[kBwdWin];
+    const double2* st =
+        reinterpret_cast<const double2*>(ring + (size_t)(s % kStages) * STAGE + (size_t)slot * kBwdRec);
 #pragma unroll
-    for (int u = 0; u < kBwdWin; ++u) {
-      const int j = q0 + kBwdWin - 1 - u;  // j % kBwdWin == kBwdWin-1-u
-      const double* rec = st + (size_t)(kBwdWin - 1 - u) * BREC;
-      double acc0 = ysave[(size_t)j * NL + ln];
-      double acc1 = 0.0, acc2 = 0.0;
+    for (int h = 0; h < kBwdWin / BSUB; ++h) {
+      // records of rows q0+kBwdWin-1-u for u = h*BSUB .. h*BSUB+BSUB-1
+      double2 rv[BSUB][BV];
 #pragma unroll
-      for (int b = 0; b < NBMAX; ++b) acc1 = fma(-rec[(W1 + b) * MP], x1[b], acc1);
+      for (int w = 0; w < BSUB; ++w)
 #pragma unroll
-      for (int t = kBwdWin; t >= 2; --t) {
-        const int sl = (kBwdWin - 1 - u + t) % kBwdWin;
-        if (t % 3 == 0)
-          acc0 = fma(-rec[t * MP], xw[sl], acc0);
-        else if (t % 3 == 1)
-          acc1 = fma(-rec[t * MP], xw[sl], acc1);
-        else
-          acc2 = fma(-rec[t * MP], xw[sl], acc2);
+        for (int v = 0; v < BV; ++v) rv[w][v] = st[(kBwdWin - 1 - (h * BSUB + w)) * (BREC / 2) + v];
+      double xs[BSUB];
+#pragma unroll
+      for (int w = 0; w < BSUB; ++w) {
+        const int u = h * BSUB + w;
+        const int j = q0 + kBwdWin - 1 - u;  // j % kBwdWin == kBwdWin-1-u
+        auto rec = [&](int k) -> double { return (k & 1) ? rv[w][k >> 1].y : rv[w][k >> 1].x; };
+        double acc0 = ysave[(size_t)j * NL + ln];
+        double acc1 = 0.0, acc2 = 0.0;
+#pragma unroll
+        for (int b = 0; b < NBMAX; ++b) acc1 = fma(-rec(W1 + b), x1[b], acc1);
+#pragma unroll
+        for (int t = kBwdWin; t >= 2; --t) {
+          const int sl = (kBwdWin - 1 - u + t) % kBwdWin;
+          if (t % 3 == 0)
+            acc0 = fma(-rec(t), xw[sl], acc0);
+          else if (t % 3 == 1)
+            acc1 = fma(-rec(t), xw[sl], acc1);
+          else
+            acc2 = fma(-rec(t), xw[sl], acc2);
+        }
+        const double sacc = fma(-rec(1), xw[(kBwdWin - u) % kBwdWin], acc0 + (acc1 + acc2));
+        const double xj = sacc * rec(0);
+        xw[(kBwdWin - 1 - u) % kBwdWin] = xj;
+        xs[w] = xj;
       }
-      const double sacc = fma(-rec[1 * MP], xw[(kBwdWin - u) % kBwdWin], acc0 + (acc1 + acc2));
-      const double xj = sacc * rec[0];
-      xw[(kBwdWin - 1 - u) % kBwdWin] = xj;
-      xs[u] = xj;
-    }
-    // stores for the block, undoing the i-scaling of u_x and its taus
-    // (ux = i vx: re = -vx_im, im = vx_re)
+      // stores, undoing the i-scaling of u_x and its taus (ux = i vx: re = -vx_im, im = vx_re)
 #pragma unroll
-    for (int u = 0; u < kBwdWin; ++u) {
-      const double* rec = st + (size_t)(kBwdWin - 1 - u) * BREC;
-      const double partner = __shfl_xor_sync(0xffffffffu, xs[u], MP);
-      const long long code = __double_as_longlong(rec[(kBwdRec - 1) * MP]);
-      const size_t off = (size_t)(code >> 1);
-      const double v = (code & 1) ? (part ? partner : -partner) : xs[u];
-      double* dst = off < xplanes ? Xd + 2 * (off + m) : Td + 2 * (off - xplanes + m);
-      if (live && code >= 0) dst[part] = v;
+      for (int w = 0; w < BSUB; ++w) {
+        const double partner = __shfl_xor_sync(0xffffffffu, xs[w], MP);
+        const long long code = __double_as_longlong(rv[w][BV - 1].y);
+        const size_t off = (size_t)(code >> 1);
+        const double v = (code & 1) ? (part ? partner : -partner) : xs[w];
+        double* dst = off < xplanes ? Xd + 2 * (off + m) : Td + 2 * (off - xplanes + m);
+        if (live && code >= 0) dst[part] = v;
+      }
     }
     __syncwarp();
   }
@@ -416,11 +454,16 @@ __global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
   }
 }
 
+template <int N>
 __global__ void k_lincomb(LinComb lc, double2* __restrict__ out, long long count) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
        i += (long long)gridDim.x * blockDim.x) {
+    double2 v[N];
+#pragma unroll
+    for (int t = 0; t < N; ++t) v[t] = lc.in[t][i];  // all loads in flight before the sums
     double2 acc = make_double2(0.0, 0.0);
-    for (int t = 0; t < lc.n; ++t) acc = cfma(lc.w[t], lc.in[t][i], acc);
+#pragma unroll
+    for (int t = 0; t < N; ++t) acc = cfma(lc.w[t], v[t], acc);
     out[i] = acc;
   }
 }
@@ -496,38 +539,60 @@ __global__ void k_lx_finalize(double2* __restrict__ LX, const double2* __restric
   }
 }
 
-// Final RK update X_f = S^{-1} y, y = linear combination of the stage vectors
-// in C^(2) rows.  S is upper triangular with offsets 0, +2, +4, so each
-// (field, parity, mode) column is a short backward recurrence.  The CTA first
-// forms y for all rows of its 32 modes in shared memory (256 threads, loads
-// independent), then warp 0 runs the recurrences from shared memory.
+// Final RK update X_f = S^{-1} y for f = b, ux, uz, where y is the stage
+// combination of the b / u_x / u_z equation rows (C^(2) space).  S is upper
+// triangular with offsets 0, +2, +4, so each (field, parity, mode) column is a
+// short backward recurrence.  A CTA owns 32 modes of one (field, parity): its
+// 256 threads form y for all rows into shared memory (independent, coalesced
+// loads) together with the S entries of those rows and the reciprocal
+// diagonal, warp 0 runs the 32 recurrences out of shared memory, and all
+// threads write X back.
+template <int N>
 __global__ void __launch_bounds__(256) k_rk_final(LinComb lc, double2* __restrict__ X, const double* __restrict__ s3,
                                                   int Nz, int Nk) {
-  extern __shared__ double2 ys[];  // [rows of this parity][32]
+  extern __shared__ double2 ys[];  // [rows of this parity][32], then 3 doubles per row
   const int f = blockIdx.y >> 1, par = blockIdx.y & 1;
   const int m0 = blockIdx.x * 32;
   const int mm = threadIdx.x % 32, ks = threadIdx.x / 32;
   const int m = m0 + mm;
   const size_t plane = (size_t)Nz * Nk;
   const int K = (Nz - par + 1) / 2;  // rows k = par + 2 ri
-  for (int ri = ks; ri < K; ri += 8) {
-    const int k = par + 2 * ri;
-    double2 y = make_double2(0.0, 0.0);
-    if (m < Nk) {
-      const size_t i = (size_t)(1 + f) * plane + (size_t)k * Nk + m;
-      for (int t = 0; t < lc.n; ++t) y = cfma(lc.w[t], lc.in[t][i], y);
+  double* sk = reinterpret_cast<double*>(ys + (size_t)K * 32);  // [ri][3]: 1/S_kk, S_k,k+2, S_k,k+4
+  for (int q = threadIdx.x; q < K; q += blockDim.x) {
+    const int k = par + 2 * q;
+    sk[3 * q] = 1.0 / s3[3 * k];
+    sk[3 * q + 1] = s3[3 * k + 1];
+    sk[3 * q + 2] = s3[3 * k + 2];
+  }
+  const size_t base = (size_t)(1 + f) * plane;  // equation rows b, mx, mz follow continuity
+  const int mc = m < Nk ? m : Nk - 1;           // clamped column: loads stay in bounds
+  for (int r0 = ks; r0 < K; r0 += 16) {
+    const int r1 = (r0 + 8 < K) ? r0 + 8 : r0;
+    const size_t e0 = base + (size_t)(par + 2 * r0) * Nk + mc;
+    const size_t e1 = base + (size_t)(par + 2 * r1) * Nk + mc;
+    double2 v0[N], v1[N];
+#pragma unroll
+    for (int t = 0; t < N; ++t) {
+      v0[t] = lc.in[t][e0];
+      v1[t] = lc.in[t][e1];
     }
-    ys[ri * 32 + mm] = y;
+    double2 a0 = make_double2(0.0, 0.0), a1 = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int t = 0; t < N; ++t) {
+      a0 = cfma(lc.w[t], v0[t], a0);
+      a1 = cfma(lc.w[t], v1[t], a1);
+    }
+    ys[r0 * 32 + mm] = a0;
+    if (r0 + 8 < K) ys[(r0 + 8) * 32 + mm] = a1;
   }
   __syncthreads();
   if (ks == 0) {
     double2 x2 = make_double2(0.0, 0.0), x4 = make_double2(0.0, 0.0);
     for (int ri = K - 1; ri >= 0; --ri) {
-      const int k = par + 2 * ri;
       double2 y = ys[ri * 32 + mm];
-      y = cfma(-s3[3 * k + 1], x2, y);
-      y = cfma(-s3[3 * k + 2], x4, y);
-      const double inv = 1.0 / s3[3 * k];
+      y = cfma(-sk[3 * ri + 1], x2, y);
+      y = cfma(-sk[3 * ri + 2], x4, y);
+      const double inv = sk[3 * ri];
       const double2 x = make_double2(y.x * inv, y.y * inv);
       ys[ri * 32 + mm] = x;
       x4 = x2;
@@ -551,7 +616,8 @@ size_t solve_smem_bytes(int npad) {
   const size_t FREC = 2 * kFwdRec * MP, BREC = 2 * kBwdRec * MP, RREC = 2 * MP;
   const size_t FSTAGE = kRowsPerStage * (FREC + 2 * RREC), BSTAGE = kRowsPerStage * BREC;
   const size_t STAGE = FSTAGE > BSTAGE ? FSTAGE : BSTAGE;
-  return (kStages * STAGE) * sizeof(double) + (size_t)npad * 4 * MP * sizeof(double) + (size_t)npad * 2 * sizeof(int);
+  return (kStages * STAGE) * sizeof(double) + (size_t)npad * 4 * MP * sizeof(double) + (size_t)npad * 2 * sizeof(int) +
+         (size_t)npad * 2;
 }
 
 template <int KL, int KU>
@@ -568,7 +634,15 @@ size_t tau_factor_scratch_doubles(int nmax, int Nk);
 cudaError_t set_tau_smem_limits(int bytes) {
   cudaError_t e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_rk_final, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  const void* fns[] = {(const void*)k_rk_final<1>,  (const void*)k_rk_final<2>,  (const void*)k_rk_final<3>,
+                       (const void*)k_rk_final<4>,  (const void*)k_rk_final<5>,  (const void*)k_rk_final<6>,
+                       (const void*)k_rk_final<7>,  (const void*)k_rk_final<8>,  (const void*)k_rk_final<9>,
+                       (const void*)k_rk_final<10>, (const void*)k_rk_final<11>, (const void*)k_rk_final<12>};
+  for (const void* fn : fns) {
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 size_t tau_solve_smem_bytes(int n) { return solve_smem_bytes(n); }
@@ -588,7 +662,17 @@ void launch_lincomb(const LinComb& lc, double2* out, long long count, cudaStream
   int blocks = (int)((count + 255) / 256);
   if (blocks > 148 * 16) blocks = 148 * 16;
   if (blocks < 1) blocks = 1;
-  k_lincomb<<<blocks, 256, 0, st>>>(lc, out, count);
+#define TB_LINCOMB_CASE(N) \
+  case N:                    \
+    k_lincomb<N><<<blocks, 256, 0, st>>>(lc, out, count); \
+    break;
+  switch (lc.n) {
+    TB_LINCOMB_CASE(1) TB_LINCOMB_CASE(2) TB_LINCOMB_CASE(3) TB_LINCOMB_CASE(4) TB_LINCOMB_CASE(5) TB_LINCOMB_CASE(6)
+    TB_LINCOMB_CASE(7) TB_LINCOMB_CASE(8) TB_LINCOMB_CASE(9) TB_LINCOMB_CASE(10) TB_LINCOMB_CASE(11) TB_LINCOMB_CASE(12)
+    default:
+      throw Error{TB_EINVAL, "linear combination of more than 12 stage vectors"};
+  }
+#undef TB_LINCOMB_CASE
 }
 
 void launch_mass_apply(const double2* X, double2* MX, const double* s3, int Nz, int Nk, int Nx, int project,
@@ -610,10 +694,25 @@ void launch_lx_finalize(double2* LX, const double2* X, const double* s3, int Nz,
 void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* s3, int Nz, int Nk,
                      cudaStream_t st) {
   dim3 grid((Nk + 31) / 32, 6);
-  const size_t smem = (size_t)((Nz + 1) / 2) * 32 * sizeof(double2);
-  k_rk_final<<<grid, 256, smem, st>>>(lc, X, s3, Nz, Nk);
+  const size_t smem = rk_final_smem_bytes(Nz);
+#define TB_RKFINAL_CASE(N) \
+  case N:                   \
+    k_rk_final<N><<<grid, 256, smem, st>>>(lc, X, s3, Nz, Nk); \
+    break;
+  switch (lc.n) {
+    TB_RKFINAL_CASE(1) TB_RKFINAL_CASE(2) TB_RKFINAL_CASE(3) TB_RKFINAL_CASE(4) TB_RKFINAL_CASE(5) TB_RKFINAL_CASE(6)
+    TB_RKFINAL_CASE(7) TB_RKFINAL_CASE(8) TB_RKFINAL_CASE(9) TB_RKFINAL_CASE(10) TB_RKFINAL_CASE(11) TB_RKFINAL_CASE(12)
+    default:
+      throw Error{TB_EINVAL, "linear combination of more than 12 stage vectors"};
+  }
+#undef TB_RKFINAL_CASE
   cudaMemsetAsync(X + (size_t)3 * Nz * Nk, 0, sizeof(double2) * (size_t)Nz * Nk, st);
   cudaMemsetAsync(tau, 0, sizeof(double2) * 7 * (size_t)Nk, st);
+}
+
+size_t rk_final_smem_bytes(int Nz) {
+  const size_t K = (size_t)(Nz + 1) / 2;
+  return K * 32 * sizeof(double2) + K * 3 * sizeof(double);
 }
 
 }  // namespace tb

@@ -180,54 +180,121 @@ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_doub
 __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 
-// One Stockham pass of radix R (Govindaraju et al. formulation: read
-// in[idx + r n/R], twiddle by w^(j r n/(Ns R)), R-point DFT, write
-// out[(idx/Ns) Ns R + idx%Ns + r Ns]).  Output ends in natural order.
+// Logical -> physical index of an FFT buffer.  With SW the low three bits are
+// XORed with the next three, so the stride-R stores of a Stockham pass
+// (R <= 8 consecutive elements per thread) and the unit-stride loads both hit
+// eight distinct 16-byte bank groups per quarter warp.  Buffers are sized to a
+// multiple of 8 elements so the permutation stays inside them.
+template <bool SW>
+__device__ __forceinline__ int fidx(int i) {
+  return SW ? (i ^ ((i >> 3) & 7)) : i;
+}
+
+// exp(sign 2 pi i t / n) for 0 <= t < n from a table of exp(-2 pi i t / n),
+// t < n/2 (the upper half is the negated lower half).
+__device__ __forceinline__ double2 twid(const double2* tw, int t, int h, int sign) {
+  const bool hi = t >= h;
+  double2 w = tw[hi ? t - h : t];
+  if (hi) w = make_double2(-w.x, -w.y);
+  if (sign > 0) w.y = -w.y;
+  return w;
+}
+
+// multiply by exp(sign i pi/2): -i for the forward transform, +i for the inverse
+__device__ __forceinline__ double2 rot4(double2 d, int sign) {
+  return (sign < 0) ? make_double2(d.y, -d.x) : make_double2(-d.y, d.x);
+}
+
+__device__ __forceinline__ void dft4(double2& x0, double2& x1, double2& x2, double2& x3, int sign) {
+  const double2 t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = rot4(csub(x1, x3), sign);
+  x0 = cadd(t0, t2);
+  x1 = cadd(t1, t3);
+  x2 = csub(t0, t2);
+  x3 = csub(t1, t3);
+}
+
+// In-register DFT of length R (unnormalised, exponent sign), natural order.
 template <int R>
-__device__ __forceinline__ void fft_pass(const double2* __restrict__ in, double2* __restrict__ out, int n, int Ns,
-                                         const double2* __restrict__ tw, int sign) {
-  const int nR = n / R;
-  const int tstride = n / (Ns * R);
-  for (int idx = threadIdx.x; idx < nR; idx += blockDim.x) {
-    const int j = idx % Ns, k = idx / Ns;
-    double2 v[R];
+__device__ __forceinline__ void dft_small(double2 (&v)[R], int sign) {
+  if constexpr (R == 2) {
+    const double2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (R == 3) {
+    const double h = 0.86602540378443864676372317075294;  // sqrt(3)/2
+    const double2 sm = cadd(v[1], v[2]), df = csub(v[1], v[2]);
+    const double2 base = make_double2(v[0].x - 0.5 * sm.x, v[0].y - 0.5 * sm.y);
+    const double2 rot = make_double2(-sign * h * df.y, sign * h * df.x);  // i sign h df
+    v[0] = cadd(v[0], sm);
+    v[1] = cadd(base, rot);
+    v[2] = csub(base, rot);
+  } else if constexpr (R == 4) {
+    dft4(v[0], v[1], v[2], v[3], sign);
+  } else {  // R == 8, one radix-2 decimation-in-frequency step then two DFT-4
+    const double r = 0.70710678118654752440084436210485;  // 1/sqrt(2)
+    const double s = (double)sign;
+    double2 a[4], b[4];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      double2 x = in[idx + r * nR];
-      if (r > 0) {
-        double2 w = tw[j * r * tstride];
-        if (sign > 0) w.y = -w.y;
-        x = cmul(x, w);
-      }
-      v[r] = x;
+    for (int n = 0; n < 4; ++n) {
+      a[n] = cadd(v[n], v[n + 4]);
+      b[n] = csub(v[n], v[n + 4]);
     }
-    const int ob = k * Ns * R + j;
-    if (R == 2) {
-      out[ob] = cadd(v[0], v[1]);
-      out[ob + Ns] = csub(v[0], v[1]);
-    } else if (R == 4) {
-      double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
-      double2 t2 = cadd(v[1], v[3]), d = csub(v[1], v[3]);
-      // forward: -i d ; inverse: +i d
-      double2 t3 = (sign < 0) ? make_double2(d.y, -d.x) : make_double2(-d.y, d.x);
-      out[ob] = cadd(t0, t2);
-      out[ob + Ns] = cadd(t1, t3);
-      out[ob + 2 * Ns] = csub(t0, t2);
-      out[ob + 3 * Ns] = csub(t1, t3);
-    } else {  // R == 3
-      const double h = 0.86602540378443864676372317075294;  // sqrt(3)/2
-      double2 sm = cadd(v[1], v[2]), df = csub(v[1], v[2]);
-      double2 base = make_double2(v[0].x - 0.5 * sm.x, v[0].y - 0.5 * sm.y);
-      double2 rot = make_double2(-sign * h * df.y, sign * h * df.x);  // i sign h df
-      out[ob] = cadd(v[0], sm);
-      out[ob + Ns] = cadd(base, rot);
-      out[ob + 2 * Ns] = csub(base, rot);
+    // b_n *= exp(sign 2 pi i n / 8)
+    b[1] = make_double2(r * (b[1].x - s * b[1].y), r * (b[1].y + s * b[1].x));
+    b[2] = rot4(b[2], sign);
+    b[3] = make_double2(r * (-b[3].x - s * b[3].y), r * (-b[3].y + s * b[3].x));
+    dft4(a[0], a[1], a[2], a[3], sign);
+    dft4(b[0], b[1], b[2], b[3], sign);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[2 * k] = a[k];
+      v[2 * k + 1] = b[k];
     }
   }
 }
 
+// One Stockham pass of radix R (Govindaraju et al. formulation: read
+// in[idx + r n/R], twiddle by w^(j r n/(Ns R)), R-point DFT, write
+// out[(idx/Ns) Ns R + idx%Ns + r Ns]).  Output ends in natural order.
+template <int R, bool SW>
+__device__ __forceinline__ void fft_pass(const double2* __restrict__ in, double2* __restrict__ out, int n, int Ns,
+                                         const double2* __restrict__ tw, int sign) {
+  const int nR = n / R;
+  const int tstride = n / (Ns * R);
+  const int h = n >> 1;
+  for (int idx = threadIdx.x; idx < nR; idx += blockDim.x) {
+    const int j = idx % Ns, k = idx / Ns;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = in[fidx<SW>(idx + r * nR)];
+    if (Ns > 1) {
+      const int e = j * tstride;  // r e < n for every r < R
+      if constexpr (R == 8) {
+        const double2 w1 = twid(tw, e, h, sign), w2 = twid(tw, 2 * e, h, sign), w4 = twid(tw, 4 * e, h, sign);
+        const double2 w3 = cmul(w1, w2);
+        v[1] = cmul(v[1], w1);
+        v[2] = cmul(v[2], w2);
+        v[3] = cmul(v[3], w3);
+        v[4] = cmul(v[4], w4);
+        v[5] = cmul(v[5], cmul(w1, w4));
+        v[6] = cmul(v[6], cmul(w2, w4));
+        v[7] = cmul(v[7], cmul(w3, w4));
+      } else {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid(tw, r * e, h, sign));
+      }
+    }
+    dft_small<R>(v, sign);
+    const int ob = k * Ns * R + j;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out[fidx<SW>(ob + r * Ns)] = v[r];
+  }
+}
+
 // Returns the buffer holding the result (a or b).  sign = -1 forward, +1 inverse
-// (both unnormalised).  tw[t] = exp(-2 pi i t / n).
+// (both unnormalised).  tw[t] = exp(-2 pi i t / n) for t < n/2 (a longer table
+// works too).
+template <bool SW = false>
 __device__ double2* fft_cta(double2* a, double2* b, const FftPlan& fp, const double2* __restrict__ tw, int sign) {
   const int n = fp.n;
   int Ns = 1;
@@ -235,12 +302,14 @@ __device__ double2* fft_cta(double2* a, double2* b, const FftPlan& fp, const dou
   double2* out = b;
   for (int s = 0; s < fp.nstages; ++s) {
     const int R = fp.radix[s];
-    if (R == 4)
-      fft_pass<4>(in, out, n, Ns, tw, sign);
+    if (R == 8)
+      fft_pass<8, SW>(in, out, n, Ns, tw, sign);
+    else if (R == 4)
+      fft_pass<4, SW>(in, out, n, Ns, tw, sign);
     else if (R == 2)
-      fft_pass<2>(in, out, n, Ns, tw, sign);
+      fft_pass<2, SW>(in, out, n, Ns, tw, sign);
     else
-      fft_pass<3>(in, out, n, Ns, tw, sign);
+      fft_pass<3, SW>(in, out, n, Ns, tw, sign);
     __syncthreads();
     double2* t = in;
     in = out;
@@ -268,124 +337,125 @@ __device__ __forceinline__ double2 pack2_mirror(double2 A, double2 B) {
   return make_double2(A.x + B.y, -A.y + B.x);
 }
 
-__global__ void __launch_bounds__(256) k_xprod(XProdArgs a) {
+// Row-wise advection products on the 3/2-padded x grid.  One CTA per grid row
+// z (two CTAs per SM): four swizzled FFT buffers of M complex entries and the
+// half twiddle table live in shared memory; the six mixed-space input rows are
+// read straight from the even/odd Chebyshev half planes (L2-resident after
+// the z GEMM), each entry once per spectrum it feeds.
+//   1. U = ifft(ux + i uz)                      (velocity on the padded grid)
+//   2. for f in b, ux, uz: G = ifft(d_x f + i d_z f); prod_f = -(u G.x + w G.y)
+//   3. fft(prod_b + i prod_ux), fft(prod_uz), unpacked and truncated to Nk bins
+__global__ void __launch_bounds__(256, 2) k_xprod(XProdArgs a) {
   extern __shared__ double2 sm[];
   const int M = a.M, N = a.Nx, Nk = a.Nk;
-  double2* X = sm;          // velocity on the padded grid: ux + i uz
-  double2* Y = sm + M;
-  double2* W = sm + 2 * M;
-  double2* P = sm + 3 * M;  // prod_b + i prod_ux
-  double* Puz = reinterpret_cast<double*>(sm + 4 * M);  // after the products are formed
-  double2* Rrows = sm + 4 * M + (M + 1) / 2;              // the 6 combined input rows (6 Nk entries)
-  const int z = blockIdx.x;
-  const size_t ro = (size_t)z * Nk;
-  const int half = M / 2;
+  const int Ms = (M + 7) & ~7;
+  double2* S0 = sm;
+  double2* S1 = sm + Ms;
+  double2* S2 = sm + 2 * Ms;
+  double2* S3 = sm + 3 * Ms;
+  double2* tw = sm + 4 * Ms;  // exp(-2 pi i t / M), t < M/2
+  const int half = M / 2, hN = N / 2;
+  for (int t = threadIdx.x; t < half; t += blockDim.x) tw[t] = a.tw[t];
   // Grid row z from the even/odd Chebyshev half planes: rows z < H are E + O,
   // mirrored rows N-1-z are E - O for values and -E + O for z-derivatives.
-  double2* R = Rrows;
-  {
-    const int Nz = a.Nz;
-    const int zm = Nz - 1 - z;
-    const bool lower = z <= zm;
-    const int zr = lower ? z : zm;
-    const size_t rr = (size_t)zr * Nk;
-    for (int k = threadIdx.x; k < Nk; k += blockDim.x)
-      for (int f = 0; f < 3; ++f) {
-        const double2 ev = a.ev[f][rr + k], ov = a.ov[f][rr + k];
-        const double2 ed = a.ed[f][rr + k], od = a.od[f][rr + k];
-        R[(2 * f) * Nk + k] = lower ? make_double2(ev.x + ov.x, ev.y + ov.y) : make_double2(ev.x - ov.x, ev.y - ov.y);
-        R[(2 * f + 1) * Nk + k] = lower ? make_double2(ed.x + od.x, ed.y + od.y) : make_double2(od.x - ed.x, od.y - ed.y);
-      }
-  }
-  __syncthreads();
+  const int z = blockIdx.x;
+  const int zm = a.Nz - 1 - z;
+  const bool lower = z <= zm;
+  const size_t rr = (size_t)(lower ? z : zm) * Nk;
+  auto value = [&](int f, int q) -> double2 {
+    const double2 e = a.ev[f][rr + q], o = a.ov[f][rr + q];
+    return lower ? make_double2(e.x + o.x, e.y + o.y) : make_double2(e.x - o.x, e.y - o.y);
+  };
+  auto deriv = [&](int f, int q) -> double2 {
+    const double2 e = a.ed[f][rr + q], o = a.od[f][rr + q];
+    return lower ? make_double2(e.x + o.x, e.y + o.y) : make_double2(o.x - e.x, o.y - e.y);
+  };
+  // padded operand bin q of a half spectrum value v (DC / Nyquist real, Nyquist halved)
+  auto hbin = [&](double2 v, int q) -> double2 {
+    if (q == 0) return make_double2(v.x, 0.0);
+    if (q == hN) return make_double2(0.5 * v.x, 0.0);
+    return v;
+  };
+  // spectrum of A + i B on the padded grid from half spectra A_q, B_q (q <= N/2)
+  auto put2 = [&](double2* dst, int q, double2 A, double2 B) {
+    dst[fidx<true>(q)] = pack2(A, B);
+    if (q > 0) dst[fidx<true>(M - q)] = pack2_mirror(A, B);
+  };
+  auto zero_gap = [&](double2* dst) {  // bins N/2 < k < M - N/2 are zero
+    for (int k = hN + 1 + threadIdx.x; k < M - hN; k += blockDim.x) dst[fidx<true>(k)] = make_double2(0.0, 0.0);
+  };
   // 1. velocity spectrum
-  {
-    const double2* gx = R + 2 * Nk;
-    const double2* gz = R + 4 * Nk;
-    for (int k = threadIdx.x; k < M; k += blockDim.x) {
-      double2 v;
-      if (k <= half) {
-        v = pack2(half_bin(gx, k, N), half_bin(gz, k, N));
-      } else {
-        int q = M - k;
-        v = pack2_mirror(half_bin(gx, q, N), half_bin(gz, q, N));
-      }
-      X[k] = v;
-    }
-  }
+  for (int q = threadIdx.x; q <= hN; q += blockDim.x) put2(S0, q, hbin(value(1, q), q), hbin(value(2, q), q));
+  zero_gap(S0);
   __syncthreads();
-  double2* U = fft_cta(X, Y, a.fp, a.tw, +1);
-  double2* F0 = (U == X) ? Y : X;  // free buffers: F0 and W
+  double2* U = fft_cta<true>(S0, S1, a.fp, tw, +1);
+  double2* P = (U == S0) ? S1 : S0;  // prod_b + i prod_ux
+  double2* Q = nullptr;              // prod_uz (real parts)
   // 2. gradients of each field and the advection products
   for (int f = 0; f < 3; ++f) {
-    const double2* gv = R + (2 * f) * Nk;
-    const double2* gd = R + (2 * f + 1) * Nk;
-    for (int k = threadIdx.x; k < M; k += blockDim.x) {
-      int q = (k <= half) ? k : M - k;
+    for (int q = threadIdx.x; q <= hN; q += blockDim.x) {
       double2 Ax = make_double2(0.0, 0.0);
-      if (q > 0 && q < N / 2) {
-        double kk = a.k0 * q;
-        double2 g = gv[q];
+      if (q > 0 && q < hN) {
+        const double kk = a.k0 * q;
+        const double2 g = value(f, q);
         Ax = make_double2(-kk * g.y, kk * g.x);  // i k g
       }
-      double2 Az = half_bin(gd, q, N);
-      F0[k] = (k <= half) ? pack2(Ax, Az) : pack2_mirror(Ax, Az);
+      put2(S2, q, Ax, hbin(deriv(f, q), q));
     }
+    zero_gap(S2);
     __syncthreads();
-    double2* G = fft_cta(F0, W, a.fp, a.tw, +1);
+    double2* G = fft_cta<true>(S2, S3, a.fp, tw, +1);
+    double2* Gf = (G == S2) ? S3 : S2;  // the pass buffer left free
     for (int p = threadIdx.x; p < M; p += blockDim.x) {
-      double2 u = U[p], g = G[p];
-      double pr = -(u.x * g.x + u.y * g.y);
+      const int ps = fidx<true>(p);
+      const double2 u = U[ps], g = G[ps];
+      const double pr = -(u.x * g.x + u.y * g.y);
       if (f == 0)
-        P[p].x = pr;
+        P[ps].x = pr;
       else if (f == 1)
-        P[p].y = pr;
+        P[ps].y = pr;
       else
-        Puz[p] = pr;
+        Gf[ps] = make_double2(pr, 0.0);
     }
-    __syncthreads();
-  }
-  // 3. forward transforms of the products
-  double2* C1 = fft_cta(P, F0, a.fp, a.tw, -1);
-  // Save the two unpacked spectra for k <= N/2 into the free buffer W... then FFT Puz.
-  const double sc = 1.0 / ((double)M * (double)N);
-  const int h = N / 2;
-  for (int k = threadIdx.x; k < Nk; k += blockDim.x) {
-    double2 c = C1[k];
-    double2 cm = C1[(M - k) % M];
-    // b: (c + conj(cm))/2 ; ux: (c - conj(cm))/(2i)
-    double2 sb = make_double2(0.5 * (c.x + cm.x), 0.5 * (c.y - cm.y));
-    double2 su = make_double2(0.5 * (c.y + cm.y), -0.5 * (c.x - cm.x));
-    double2 ob, ou;
-    if (k == 0) {
-      ob = make_double2(sb.x * sc, 0.0);
-      ou = make_double2(su.x * sc, 0.0);
-    } else if (k == h) {
-      ob = make_double2(2.0 * sb.x * sc, 0.0);
-      ou = make_double2(2.0 * su.x * sc, 0.0);
+    if (f == 2) {
+      Q = Gf;
+      // the gradient buffer G is free from here on
+      __syncthreads();
+      // 3a. forward transform of prod_b + i prod_ux into G's buffer pair
+      double2* C1 = fft_cta<true>(P, G, a.fp, tw, -1);
+      // 3b. forward transform of prod_uz, ping-ponging with U's buffer (free now);
+      // it touches neither C1 nor P's partner, so both proceed before one barrier
+      double2* C2 = fft_cta<true>(Q, U, a.fp, tw, -1);
+      const double sc = 1.0 / ((double)M * (double)N);
+      const size_t ro = (size_t)z * Nk;
+      for (int k = threadIdx.x; k < Nk; k += blockDim.x) {
+        const double2 c = C1[fidx<true>(k)];
+        const double2 cm = C1[fidx<true>((M - k) % M)];
+        // b: (c + conj(cm))/2 ; ux: (c - conj(cm))/(2i)
+        const double2 sb = make_double2(0.5 * (c.x + cm.x), 0.5 * (c.y - cm.y));
+        const double2 su = make_double2(0.5 * (c.y + cm.y), -0.5 * (c.x - cm.x));
+        const double2 c2 = C2[fidx<true>(k)];
+        double2 ob, ou, oz;
+        if (k == 0) {
+          ob = make_double2(sb.x * sc, 0.0);
+          ou = make_double2(su.x * sc, 0.0);
+          oz = make_double2(c2.x * sc, 0.0);
+        } else if (k == hN) {
+          ob = make_double2(2.0 * sb.x * sc, 0.0);
+          ou = make_double2(2.0 * su.x * sc, 0.0);
+          oz = make_double2(2.0 * c2.x * sc, 0.0);
+        } else {
+          ob = cscale(sb, sc);
+          ou = cscale(su, sc);
+          oz = cscale(c2, sc);
+        }
+        a.out[0][ro + k] = ob;
+        a.out[1][ro + k] = ou;
+        a.out[2][ro + k] = oz;
+      }
     } else {
-      ob = cscale(sb, sc);
-      ou = cscale(su, sc);
+      __syncthreads();
     }
-    a.out[0][ro + k] = ob;
-    a.out[1][ro + k] = ou;
-  }
-  __syncthreads();
-  double2* B1 = (C1 == P) ? F0 : P;
-  for (int p = threadIdx.x; p < M; p += blockDim.x) B1[p] = make_double2(Puz[p], 0.0);
-  __syncthreads();
-  double2* B2 = (B1 == P) ? F0 : P;
-  double2* C2 = fft_cta(B1, B2, a.fp, a.tw, -1);
-  for (int k = threadIdx.x; k < Nk; k += blockDim.x) {
-    double2 c = C2[k];
-    double2 o;
-    if (k == 0)
-      o = make_double2(c.x * sc, 0.0);
-    else if (k == h)
-      o = make_double2(2.0 * c.x * sc, 0.0);
-    else
-      o = cscale(c, sc);
-    a.out[2][ro + k] = o;
   }
 }
 
@@ -507,7 +577,9 @@ cudaError_t set_transform_smem_limits(int bytes) {
 }
 
 size_t xprod_smem_bytes(int M, int Nk) {
-  return (size_t)M * 4 * sizeof(double2) + (size_t)((M + 1) / 2) * sizeof(double2) + (size_t)6 * Nk * sizeof(double2);
+  (void)Nk;
+  const size_t Ms = (size_t)((M + 7) & ~7);
+  return (4 * Ms + (size_t)(M / 2)) * sizeof(double2);
 }
 
 void launch_xprod(const XProdArgs& a, cudaStream_t st) {
