@@ -58,6 +58,7 @@ struct ClassTables {
 struct FactorSet {
   double alpha = 0, beta = 0;
   DevBuf FR, BR, SI;  // solve-layout factor records (see tb_kernels.cuh)
+  DevBuf PP;          // partition transfer matrices of the solve
 };
 
 struct Tableau {
@@ -136,6 +137,7 @@ struct tb_plan {
   int graph_kind = -1;
   cudaGraphExec_t gexec = nullptr;
   int kernels_per_step = 0;
+  int tau_parts = 1;  // partitions of the tau solve (kTauParts or 1)
   // profiling: eager launches bracketed by events, accumulated per kernel name
   bool profiling = false;
   struct ProfRec {
@@ -290,6 +292,7 @@ TauArgs tau_args(tb_plan* P, FactorSet* f, const double2* rhsP) {
   a.tau = P->tau.as<double2>();
   a.rhsP = rhsP;
   a.npad = (P->lay.cls[0].n + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
+  a.PP = f ? f->PP.as<double>() : nullptr;
   a.rhs_off = P->rhs_off.as<int>();
   a.err_mode = P->err_mode.as<int>();
   return a;
@@ -309,6 +312,8 @@ FactorSet* get_factors(tb_plan* P, double alpha, double beta) {
   fs->FR.alloc(groups * n * 2 * kFwdRec * kSolveModes * sizeof(double));
   fs->BR.alloc(groups * n * 2 * kBwdRec * kSolveModes * sizeof(double));
   fs->SI.alloc(groups * 2 * 16 * kSolveModes * sizeof(double));
+  const size_t npp = tau_transfer_doubles(Nk, P->tau_parts);
+  if (npp) fs->PP.alloc(npp * sizeof(double));
   TB_CUDA_TRY(cudaMemsetAsync(fs->FR.p, 0, fs->FR.bytes, P->st));
   TB_CUDA_TRY(cudaMemsetAsync(fs->BR.p, 0, fs->BR.bytes, P->st));
   TB_CUDA_TRY(cudaMemsetAsync(fs->SI.p, 0, fs->SI.bytes, P->st));
@@ -319,7 +324,7 @@ FactorSet* get_factors(tb_plan* P, double alpha, double beta) {
   TB_CUDA_TRY(cudaMemcpyAsync(P->err_mode.p, &neg, sizeof(int), cudaMemcpyHostToDevice, P->st));
   TauArgs a = tau_args(P, fs.get(), nullptr);
   a.scratch = scratch.as<double>();
-  launch_tau_factor(a, P->st);
+  launch_tau_factor(a, P->tau_parts, P->st);
   check_launch("tau factor");
   int bad = 0;
   TB_CUDA_TRY(cudaMemcpyAsync(&bad, P->err_mode.p, sizeof(int), cudaMemcpyDeviceToHost, P->st));
@@ -403,7 +408,7 @@ void enqueue_rk_step(tb_plan* P, double dt) {
       }
       timed(P, "stage_lincomb", [&] { launch_lincomb(lc, P->LXP[i].as<double2>(), cnt, P->st); });
       TauArgs a = tau_args(P, fs, P->LXP[i].as<double2>());
-      timed(P, "tau_solve", [&] { launch_tau_solve(a, P->st); });
+      timed(P, "tau_solve", [&] { launch_tau_solve(a, P->tau_parts, P->st); });
       timed(P, "lx_finalize", [&] {
         launch_lx_finalize(P->LXP[i].as<double2>(), X, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, P->k0, P->s,
                            P->d.kappa, P->d.nu, beta, P->st);
@@ -476,7 +481,7 @@ void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
   }
   timed(P, "stage_lincomb", [&] { launch_lincomb(lc, P->Rsb.as<double2>(), cnt, P->st); });
   TauArgs a = tau_args(P, fs, P->Rsb.as<double2>());
-  timed(P, "tau_solve", [&] { launch_tau_solve(a, P->st); });
+  timed(P, "tau_solve", [&] { launch_tau_solve(a, P->tau_parts, P->st); });
   TB_CUDA_TRY(cudaMemcpyAsync(P->Fprev.p, Fcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
   TB_CUDA_TRY(cudaMemcpyAsync(P->MXprev.p, MXcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
   P->kernels_per_step = 3 + 1 + 1 + 1;
@@ -673,16 +678,28 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
       upload(T.c1_nz, L.c1_nz);
     }
     TB_REQUIRE(P->lay.cls[0].n == P->lay.cls[1].n, TB_ENOTSUPPORTED, "parity classes of unequal size");
-    TB_REQUIRE(tau_solve_smem_bytes((P->lay.cls[0].n + kTauRowPad - 1) / kTauRowPad * kTauRowPad) <= 227 * 1024,
-               TB_ENOTSUPPORTED, "Nz too large for the staged tau solve");
+    {
+      // partitioned solve (kTauParts warps per mode group) when its shared
+      // memory fits, else one warp per group
+      const int npad = (P->lay.cls[0].n + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
+      P->tau_parts = tau_solve_smem_bytes(npad, kTauParts) <= 227 * 1024 ? kTauParts : 1;
+      TB_REQUIRE(tau_solve_smem_bytes(npad, P->tau_parts) <= 227 * 1024, TB_ENOTSUPPORTED,
+                 "Nz too large for the staged tau solve");
+    }
     TB_REQUIRE(rk_final_smem_bytes(P->Nz) <= 227 * 1024, TB_ENOTSUPPORTED, "Nz too large for the final RK update");
     P->err_mode.alloc(sizeof(int));
     {
+      // per (band row, class): 2 * (element offset of the row's right-hand side
+      // in a stage vector) + 1 when it is a u_x momentum row (scaled by -i on
+      // load); -1 for the padding rows
       const int n = P->lay.cls[0].n;
-      std::vector<int> ro((size_t)2 * n);
+      const int npad = (n + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
+      std::vector<int> ro((size_t)2 * npad, -1);
       for (int j = 0; j < n; ++j)
-        for (int cc = 0; cc < 2; ++cc)
-          ro[2 * j + cc] = (P->lay.cls[cc].row_eq[j] * P->Nz + P->lay.cls[cc].row_k[j]) * P->Nk;
+        for (int cc = 0; cc < 2; ++cc) {
+          const int eq = P->lay.cls[cc].row_eq[j];
+          ro[2 * j + cc] = 2 * (eq * P->Nz + P->lay.cls[cc].row_k[j]) * P->Nk + (eq == EQ_MX ? 1 : 0);
+        }
       upload(P->rhs_off, ro);
     }
     // state and work arrays

@@ -63,11 +63,14 @@ constexpr int kTauKL = 4, kTauKU = 8;
 constexpr int kSolveModes = 4;
 constexpr int kFwdRec = 1 + kTauKL + 4 + 1;  // pivot, multipliers, border, pad to 16 B
 constexpr int kBwdRec = 1 + kTauKL + kTauKU + 4 + 1;
-// Register windows of the solve sweeps; band rows are padded to a multiple of
-// their least common multiple (kTauRowPad) with identity rows.
+// Register windows of the solve sweeps.  The solve splits the band rows into
+// kTauParts partitions (one warp each), each a whole number of backward
+// windows, so rows are padded with identity rows to a multiple of
+// kTauParts * kBwdWin (kTauRowPad).
 constexpr int kFwdWin = kTauKL + 2;
 constexpr int kBwdWin = kTauKL + kTauKU;
-constexpr int kTauRowPad = 12;
+constexpr int kTauParts = 4;
+constexpr int kTauRowPad = kTauParts * kBwdWin;
 struct ClassDev {
   int n, nb, kl, ku;
   const short* row_eq;
@@ -102,15 +105,21 @@ struct TauArgs {
   double2* tau;
   // P-space right-hand side (cont, b, mx, mz) x Nz x Nk
   const double2* rhsP;
-  // element offset of band row j's right-hand side in rhsP, [row][class]
+  // [row][class] over npad rows: 2 * (element offset of band row j's right-hand
+  // side in rhsP) + 1 for a u_x momentum row, -1 for none
   const int* rhs_off;
+  // partition transfer matrices of the solve (Phi 4x4, Psi 12x12 per
+  // partition 1..kTauParts-2, class and mode), written by the factorisation
+  double* PP;
   double* scratch;     // factor workspace
   int* err_mode;       // first singular mode, or -1
 };
-void launch_tau_factor(const TauArgs& a, cudaStream_t st);
-void launch_tau_solve(const TauArgs& a, cudaStream_t st);
+// parts: kTauParts (partitioned solve, needs a.PP) or 1 (one warp per group)
+void launch_tau_factor(const TauArgs& a, int parts, cudaStream_t st);
+void launch_tau_solve(const TauArgs& a, int parts, cudaStream_t st);
 cudaError_t set_tau_smem_limits(int bytes);
-size_t tau_solve_smem_bytes(int npad);
+size_t tau_solve_smem_bytes(int npad, int parts);
+size_t tau_transfer_doubles(int Nk, int parts);
 
 struct LinComb {
   const double2* in[12];

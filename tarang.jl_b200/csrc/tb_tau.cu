@@ -202,18 +202,37 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
 }
 
 // ---------------------------------------------------------------------------
-// Solve: one warp per group of kSolveModes Fourier modes.  Lane (c, part, mm)
-// runs the forward and backward sweeps of parity class c for mode
-// g*kSolveModes + mm on the real (part 0) or imaginary (part 1) column.  The
-// factor rows of the group are contiguous records that the whole warp streams
-// into a shared-memory ring with cp.async, kRowsPerStage rows per stage and
-// kStages stages deep; each lane then pulls its own records of a window of rows
-// into registers with 16-byte loads before the window's arithmetic, so the
-// sequential sweeps wait on no shared-memory load.  The forward sweep's
-// intermediate y stays in shared memory for the backward sweep.
+// Solve: one CTA of P warps per group of kSolveModes Fourier modes.  Lane
+// (c, part, mm) of a warp runs the sweeps of parity class c for mode
+// g*kSolveModes + mm on the real (part 0) or imaginary (part 1) column; lanes
+// NL..31 mirror lanes 0..NL-1 (same arithmetic, so the unrolled sweeps stay
+// branch free) and only the owner lanes store.
+//
+// The npad band rows are split into P partitions of Lp = npad/P rows, warp w
+// owning rows [w Lp, (w+1) Lp).  Both triangular sweeps are linear
+// recurrences whose state crossing a partition boundary is small: the 4
+// pending entries of the forward window, the 12 latest unknowns of the
+// backward window.  So
+//   F1  every warp sweeps its rows forward from the raw right-hand side
+//       (exact for warp 0) and publishes its exit window;
+//   F2  warp w >= 1 composes the boundary corrections of the partitions above
+//       it with the transfer matrices Phi (4x4, from the factors);
+//   F3  warp w >= 1 re-runs its rows from the corrected window;
+//   B1  every warp sweeps its rows backward from a zero window (exact for the
+//       last warp) and publishes its top 12 unknowns;
+//   B2  warp w < P-1 composes the true incoming window with Psi (12x12);
+//   B3  warp w < P-1 re-runs its rows from that window, storing X.
+// Each sequential chain is 4 Lp = npad rows long instead of 2 npad.  The
+// factor records of a warp's rows stream through its own shared-memory ring
+// (cp.async, kPartStages stages of kPartRows rows); each lane pulls its
+// records of a stage into registers with 16-byte loads before the stage's
+// arithmetic.  The forward sweep's y stays in shared memory for the backward
+// sweep of the same warp.
 // ---------------------------------------------------------------------------
-constexpr int kRowsPerStage = 12;  // a multiple of the forward and backward window lengths
-constexpr int kStages = 6;
+constexpr int kPartRows = 6;    // rows per ring stage (the forward window)
+constexpr int kPartStages = 4;  // ring depth
+constexpr int kXch = 20;        // exchange doubles per (warp, lane): D(4) Z(4) Xhat(12)
+constexpr int kTransfer = 16 + 144;  // Phi (4x4) and Psi (12x12) per (partition, class, mode)
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -226,9 +245,18 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-template <int KL, int KU>
-__global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
+template <int P>
+__host__ __device__ constexpr size_t part_stage_doubles() {
+  constexpr size_t MP = kSolveModes;
+  constexpr size_t F = kPartRows * (2 * MP * kFwdRec + 2 * 2 * MP);
+  constexpr size_t B = kPartRows * (2 * MP * kBwdRec);
+  return F > B ? F : B;
+}
+
+template <int KL, int KU, int P>
+__global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   static_assert(KL + 2 == kFwdWin && KL + KU == kBwdWin, "window sizes follow the band shape");
+  static_assert(kFwdWin == kPartRows && kBwdWin == 2 * kPartRows, "one forward window per stage, two stages per backward block");
   static_assert(kFwdRec == KL + NBMAX + 2 && kFwdRec % 2 == 0, "forward record: pivot, l, border, pad");
   static_assert(kBwdRec == KL + KU + NBMAX + 2 && kBwdRec % 2 == 0, "backward record: 1/d, u, border, code");
   constexpr int MP = kSolveModes;
@@ -237,127 +265,236 @@ __global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
   constexpr int BREC = 2 * MP * kBwdRec;  // doubles per backward row
   constexpr int RREC = 2 * MP;            // double2 rhs entries per row (class, mode)
   constexpr int FV = kFwdRec / 2, BV = kBwdRec / 2;  // 16-byte words per record
-  constexpr int R = kRowsPerStage;
-  constexpr int NL = 4 * MP;              // distinct lanes; lanes NL..31 mirror lanes 0..NL-1
-  constexpr int BSUB = 4;                 // backward rows whose records are held in registers at once
+  constexpr int R = kPartRows, NS = kPartStages;
+  constexpr int NL = 4 * MP;  // distinct lanes
+  constexpr int BSUB = 3;     // backward rows whose records are held in registers at once
+  constexpr int STAGE = (int)part_stage_doubles<P>();
   static_assert(NL <= 32 && 32 % NL == 0, "lane layout");
-  static_assert(kBwdWin % BSUB == 0, "backward sub-blocks");
+  static_assert(R % BSUB == 0, "backward sub-blocks");
   extern __shared__ __align__(16) double smem[];
   const int np = a.npad;
   const int Nk = a.Nk;
   const int g = blockIdx.x;
-  const int lane = threadIdx.x;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int Lp = np / P, row0 = warp * Lp;
+  const int nst = Lp / R;  // ring stages of this warp's rows
   const int ln = lane % NL;
-  // ln = c*2*MP + part*MP + mm : class c, real (part 0) / imaginary (part 1) column, mode mm.
-  // Mirror lanes repeat the same arithmetic (so the unrolled sweeps stay branch free) and
-  // only the owner lanes store.
   const int c = ln / (2 * MP), part = (ln / MP) & 1, mm = ln % MP;
-  const int slot = c * MP + mm;  // this lane's record within a row
+  const int slot = c * MP + mm;
   const bool owner = lane < NL;
   const int m = g * MP + mm;
   const bool live = owner && m < Nk;
-  constexpr int FSTAGE = R * (FREC + 2 * RREC);
-  constexpr int BSTAGE = R * BREC;
-  constexpr int STAGE = FSTAGE > BSTAGE ? FSTAGE : BSTAGE;
-  double* ring = smem;
-  double* ysave = smem + (size_t)kStages * STAGE;                  // [row][ln]
-  int* rofs = reinterpret_cast<int*>(ysave + (size_t)np * NL);  // [row][class] rhs offset, -1: none
-  unsigned char* rrot = reinterpret_cast<unsigned char*>(rofs + 2 * np);  // [row][class] 1: u_x momentum row
-  for (int q = lane; q < 2 * np; q += 32) {
-    const int row = q / 2, cc = q % 2;
-    const bool in = row < a.cls[cc].n;
-    rofs[q] = (q < 2 * a.cls[0].n) ? a.rhs_off[q] : -1;
-    rrot[q] = (in && a.cls[cc].row_eq[row] == EQ_MX) ? 1 : 0;
-  }
-  __syncwarp();
+  double* ring = smem + (size_t)warp * NS * STAGE;
+  double* ysave = smem + (size_t)P * NS * STAGE;  // [row][ln]
+  double* xch = ysave + (size_t)np * NL;          // [warp][ln][kXch]
+  int* rofs = reinterpret_cast<int*>(xch + (size_t)P * NL * kXch);
+  // [row][class] right-hand-side code: 2 * element offset + (1 for a u_x momentum
+  // row, scaled by -i on load), -1 for none
+  for (int q = threadIdx.x; q < np / 2; q += 32 * P) cp_async16(rofs + 4 * q, a.rhs_off + 4 * q, true);
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
   const double* FRg = a.cls[0].FR + (size_t)g * np * FREC;
   const double* BRg = a.cls[0].BR + (size_t)g * np * BREC;
-  const int nstage = np / R;
+  double* Xd = reinterpret_cast<double*>(a.X);
+  double* Td = reinterpret_cast<double*>(a.tau);
+  const size_t xplanes = (size_t)4 * a.Nz * Nk;
 
-  // ---- forward sweep: y = L^-1 P r (rows 0..np-1), boundary rows accumulate z ----
-  auto issue_fwd = [&](int s) {
-    if (s < nstage) {
-      double* dst = ring + (size_t)(s % kStages) * STAGE;
-      const int r0 = s * R;
+  // ---- forward sweep over this warp's rows: y = L^-1 P r, boundary rows accumulate z ----
+  double y[kFwdWin];
+  double z[NBMAX];
+  auto issue_fwd = [&](int s) {  // local stage s: rows row0 + s R ..; stage nst is the first of the next warp
+    const int r0 = row0 + s * R;
+    if (s <= nst && r0 < np) {
+      double* dst = ring + (size_t)(s % NS) * STAGE;
       for (int q = lane; q < R * FREC / 2; q += 32) cp_async16(dst + 2 * q, FRg + (size_t)r0 * FREC + 2 * q, true);
       double2* rdst = reinterpret_cast<double2*>(dst + R * FREC);
       for (int q = lane; q < R * RREC; q += 32) {
         const int r = q / RREC, cc = (q / MP) % 2, md = q % MP;
         const int mq = g * MP + md;
-        const int off = rofs[2 * (r0 + r) + cc];
-        const bool ok = off >= 0 && mq < Nk;
-        cp_async16(rdst + q, a.rhsP + (ok ? (size_t)off + mq : 0), ok);
+        const int code = rofs[2 * (r0 + r) + cc];
+        const bool ok = code >= 0 && mq < Nk;
+        cp_async16(rdst + q, a.rhsP + (ok ? (size_t)(code >> 1) + mq : 0), ok);
       }
     }
     cp_async_commit();
   };
-  for (int s = 0; s < kStages - 1; ++s) issue_fwd(s);
-  // right-hand side of row j (j < np) for this lane: u_x momentum rows are
-  // scaled by -i, i.e. (re, im) -> (im, -re)
-  auto rhs_row = [&](int j) -> double {
-    const int s = j / R, r = j % R;
-    const double* rb = ring + (size_t)(s % kStages) * STAGE + R * FREC + (size_t)(r * RREC + slot) * 2;
-    const int rot = rrot[2 * j + c];
+  // right-hand side of row r0 + u of local stage s for this lane (0 past the last row);
+  // u_x momentum rows are scaled by -i, i.e. (re, im) -> (im, -re)
+  auto rhs_at = [&](int s, int u) -> double {
+    const int j = row0 + s * R + u;
+    if (j >= np) return 0.0;
+    const double* rb = ring + (size_t)(s % NS) * STAGE + R * FREC + (size_t)(u * RREC + slot) * 2;
+    const int rot = rofs[2 * j + c] & 1;
     const double v = rb[part ^ rot];
     return (rot & part) ? -v : v;
   };
-  double y[kFwdWin];
-  double z[NBMAX];
-#pragma unroll
-  for (int b = 0; b < NBMAX; ++b) z[b] = (part == 0 && m == 0 && b < a.cls[c].nb) ? a.beta * a.cls[c].bc_rhs[b] : 0.0;
-  for (int j0 = 0; j0 < np; j0 += kFwdWin) {
-    const int s = j0 / R;
-    if (j0 % R == 0) {
-      issue_fwd(s + kStages - 1);
-      cp_async_wait<kStages - 2>();  // stages s and s+1 are resident
+  // d0..d3: correction of the first 4 entries of the starting window
+  auto fwd_sweep = [&](double d0, double d1, double d2, double d3) {
+    for (int s = 0; s < NS - 1; ++s) issue_fwd(s);
+    for (int s = 0; s < nst; ++s) {
+      issue_fwd(s + NS - 1);        // refills the slot of stage s-1
+      cp_async_wait<NS - 2>();      // stages s and s+1 are resident
       __syncwarp();
       if (s == 0) {
 #pragma unroll
-        for (int t = 0; t < kFwdWin; ++t) y[t] = rhs_row(t);
+        for (int t = 0; t < kFwdWin; ++t)
+          y[t] = rhs_at(0, t) + (t == 0 ? d0 : t == 1 ? d1 : t == 2 ? d2 : t == 3 ? d3 : 0.0);
+      }
+      const double2* st =
+          reinterpret_cast<const double2*>(ring + (size_t)(s % NS) * STAGE + (size_t)slot * kFwdRec);
+      double2 rv[kFwdWin][FV];
+#pragma unroll
+      for (int u = 0; u < kFwdWin; ++u)
+#pragma unroll
+        for (int v = 0; v < FV; ++v) rv[u][v] = st[u * (FREC / 2) + v];
+      double incoming[kFwdWin];
+#pragma unroll
+      for (int u = 0; u < kFwdWin; ++u) incoming[u] = rhs_at(s + 1, u);
+      double* ys = ysave + (size_t)(row0 + s * R) * NL + ln;
+#pragma unroll
+      for (int u = 0; u < kFwdWin; ++u) {
+        auto rec = [&](int k) -> double { return (k & 1) ? rv[u][k >> 1].y : rv[u][k >> 1].x; };
+        const int p = __double2loint(rv[u][0].x);
+        double yj = y[u];
+#pragma unroll
+        for (int t = 1; t <= KL; ++t) {
+          const bool sw = (t == p);
+          const double yt = y[(u + t) % kFwdWin];
+          y[(u + t) % kFwdWin] = sw ? yj : yt;
+          yj = sw ? yt : yj;
+        }
+        ys[u * NL] = yj;
+#pragma unroll
+        for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-rec(t), yj, y[(u + t) % kFwdWin]);
+#pragma unroll
+        for (int b = 0; b < NBMAX; ++b) z[b] = fma(-rec(1 + KL + b), yj, z[b]);
+        y[u] = incoming[u];
+      }
+      __syncwarp();  // the slot of stage s is refilled next
+    }
+    cp_async_wait<0>();
+    __syncwarp();
+  };
+
+  // ---- backward sweep over this warp's rows: x = U^-1 (y - B x1) ----
+  double xw[kBwdWin];  // x_j lives in slot j % kBwdWin
+  double x1[NBMAX];
+  auto issue_bwd = [&](int s) {  // local stage s from the bottom: rows row0 + Lp - (s+1) R ..
+    if (s < nst) {
+      double* dst = ring + (size_t)(s % NS) * STAGE;
+      const int lo = row0 + Lp - (s + 1) * R;
+      for (int q = lane; q < R * BREC / 2; q += 32) cp_async16(dst + 2 * q, BRg + (size_t)lo * BREC + 2 * q, true);
+    }
+    cp_async_commit();
+  };
+  auto bwd_sweep = [&](bool store) {
+    for (int s = 0; s < NS - 1; ++s) issue_bwd(s);
+    for (int s0 = 0; s0 < nst; s0 += 2) {
+      const int q0 = row0 + Lp - (s0 + 2) * R;  // block rows q0 .. q0 + kBwdWin - 1, q0 % kBwdWin == 0
+#pragma unroll
+      for (int hs = 0; hs < 2; ++hs) {
+        const int s = s0 + hs;
+        issue_bwd(s + NS - 1);
+        cp_async_wait<NS - 1>();  // stage s is resident
+        __syncwarp();
+        const double2* st =
+            reinterpret_cast<const double2*>(ring + (size_t)(s % NS) * STAGE + (size_t)slot * kBwdRec);
+#pragma unroll
+        for (int h = 0; h < R / BSUB; ++h) {
+          // rows q0 + kBwdWin - 1 - u for u = hs R + h BSUB + w; stage row index R - 1 - (h BSUB + w)
+          double2 rv[BSUB][BV];
+#pragma unroll
+          for (int w = 0; w < BSUB; ++w)
+#pragma unroll
+            for (int v = 0; v < BV; ++v) rv[w][v] = st[(R - 1 - (h * BSUB + w)) * (BREC / 2) + v];
+#pragma unroll
+          for (int w = 0; w < BSUB; ++w) {
+            const int u = hs * R + h * BSUB + w;
+            const int j = q0 + kBwdWin - 1 - u;  // j % kBwdWin == kBwdWin-1-u
+            auto rec = [&](int k) -> double { return (k & 1) ? rv[w][k >> 1].y : rv[w][k >> 1].x; };
+            double acc0 = ysave[(size_t)j * NL + ln];
+            double acc1 = 0.0, acc2 = 0.0;
+#pragma unroll
+            for (int b = 0; b < NBMAX; ++b) acc1 = fma(-rec(W1 + b), x1[b], acc1);
+#pragma unroll
+            for (int t = kBwdWin; t >= 2; --t) {
+              const int sl = (kBwdWin - 1 - u + t) % kBwdWin;
+              if (t % 3 == 0)
+                acc0 = fma(-rec(t), xw[sl], acc0);
+              else if (t % 3 == 1)
+                acc1 = fma(-rec(t), xw[sl], acc1);
+              else
+                acc2 = fma(-rec(t), xw[sl], acc2);
+            }
+            const double sacc = fma(-rec(1), xw[(kBwdWin - u) % kBwdWin], acc0 + (acc1 + acc2));
+            const double xj = sacc * rec(0);
+            xw[(kBwdWin - 1 - u) % kBwdWin] = xj;
+            // store, undoing the i-scaling of u_x and its taus: ux = i v gives
+            // re(ux) = -v_im (from the part-1 lane), im(ux) = v_re (from the part-0 lane)
+            const long long code = __double_as_longlong(rv[w][BV - 1].y);
+            const bool rl = code & 1;
+            const size_t off = (size_t)(code >> 1);
+            double* base = off < xplanes ? Xd + 2 * (off + m) : Td + 2 * (off - xplanes + m);
+            if (store && live && code >= 0) base[rl ? 1 - part : part] = (rl && part) ? -xj : xj;
+          }
+        }
+        __syncwarp();  // the slot of stage s is refilled next
       }
     }
-    // this lane's records of rows j0 .. j0+kFwdWin-1, loaded up front
-    const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % kStages) * STAGE +
-                                                         (size_t)(j0 - s * R) * FREC + (size_t)slot * kFwdRec);
-    double2 rv[kFwdWin][FV];
+    cp_async_wait<0>();
+    __syncwarp();
+  };
+
+  // ---- forward: F1 ----
 #pragma unroll
-    for (int u = 0; u < kFwdWin; ++u)
+  for (int b = 0; b < NBMAX; ++b)
+    z[b] = (warp == 0 && part == 0 && m == 0 && b < a.cls[c].nb) ? a.beta * a.cls[c].bc_rhs[b] : 0.0;
+  fwd_sweep(0.0, 0.0, 0.0, 0.0);
+  double* myx = xch + ((size_t)warp * NL + ln) * kXch;
+  if constexpr (P > 1) {
+    // exit window minus the raw right-hand side of the next warp's first rows
+    // (the ring still holds that stage)
 #pragma unroll
-      for (int v = 0; v < FV; ++v) rv[u][v] = st[u * (FREC / 2) + v];
-    // the right-hand sides entering the window are rows j0+kFwdWin .. j0+2 kFwdWin-1,
-    // resident in stage s or s+1 (or past the end)
-    double incoming[kFwdWin];
+    for (int t = 0; t < 4; ++t) myx[t] = y[t] - rhs_at(nst, t);
 #pragma unroll
-    for (int u = 0; u < kFwdWin; ++u) {
-      const int jn = j0 + kFwdWin + u;
-      incoming[u] = (jn < np) ? rhs_row(jn < np ? jn : 0) : 0.0;
-    }
+    for (int b = 0; b < NBMAX; ++b) myx[4 + b] = z[b];
+    __syncthreads();
+    // ---- F2, F3 ----
+    if (warp > 0) {
+      double d[4];
 #pragma unroll
-    for (int u = 0; u < kFwdWin; ++u) {
-      auto rec = [&](int k) -> double { return (k & 1) ? rv[u][k >> 1].y : rv[u][k >> 1].x; };
-      const int p = __double2loint(rv[u][0].x);
-      double yj = y[u];
+      for (int t = 0; t < 4; ++t) d[t] = xch[(size_t)ln * kXch + t];  // delta_1 = D_0
+      for (int k = 1; k < warp; ++k) {
+        const double* phi = a.PP + ((((size_t)g * (P - 2) + (k - 1)) * 2 + c) * MP + mm) * kTransfer;
+        const double* Dk = xch + ((size_t)k * NL + ln) * kXch;
+        double nd[4];
 #pragma unroll
-      for (int t = 1; t <= KL; ++t) {
-        const bool sw = (t == p);
-        const double yt = y[(u + t) % kFwdWin];
-        y[(u + t) % kFwdWin] = sw ? yj : yt;
-        yj = sw ? yt : yj;
+        for (int o = 0; o < 4; ++o) {
+          double acc = Dk[o];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc = fma(phi[o * 4 + i], d[i], acc);
+          nd[o] = acc;
+        }
+#pragma unroll
+        for (int o = 0; o < 4; ++o) d[o] = nd[o];
       }
-      ysave[(size_t)(j0 + u) * NL + ln] = yj;
 #pragma unroll
-      for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-rec(t), yj, y[(u + t) % kFwdWin]);
+      for (int b = 0; b < NBMAX; ++b) z[b] = 0.0;
+      fwd_sweep(d[0], d[1], d[2], d[3]);
 #pragma unroll
-      for (int b = 0; b < NBMAX; ++b) z[b] = fma(-rec(1 + KL + b), yj, z[b]);
-      y[u] = incoming[u];
+      for (int b = 0; b < NBMAX; ++b) myx[4 + b] = z[b];
     }
-    if ((j0 + kFwdWin) % R == 0) __syncwarp();  // the ring slot of stage s may be refilled next
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < NBMAX; ++b) {
+      double acc = 0.0;
+      for (int k = 0; k < P; ++k) acc += xch[((size_t)k * NL + ln) * kXch + 4 + b];
+      z[b] = acc;
+    }
   }
-  cp_async_wait<0>();
-  __syncwarp();
 
   // ---- border unknowns from the Schur complement ----
-  double x1[NBMAX];
   {
     const double* si = a.cls[0].SI + ((size_t)g * 2 + c) * NBMAX * NBMAX * MP + mm;
 #pragma unroll
@@ -369,87 +506,105 @@ __global__ void __launch_bounds__(32) k_tau_solve(TauArgs a) {
     }
   }
 
-  // ---- backward sweep: x = U^-1 (y - B x1), rows np-1..0 ----
-  auto issue_bwd = [&](int s) {
-    if (s < nstage) {
-      double* dst = ring + (size_t)(s % kStages) * STAGE;
-      const int lo = np - (s + 1) * R;
-      for (int q = lane; q < R * BREC / 2; q += 32) cp_async16(dst + 2 * q, BRg + (size_t)lo * BREC + 2 * q, true);
-    }
-    cp_async_commit();
-  };
-  for (int s = 0; s < kStages - 1; ++s) issue_bwd(s);
-  double xw[kBwdWin];  // x_{j+t} lives in slot (j+t) % kBwdWin
+  // ---- backward: B1 ----
 #pragma unroll
   for (int t = 0; t < kBwdWin; ++t) xw[t] = 0.0;
-  const size_t xplanes = (size_t)4 * a.Nz * Nk;
-  double* Xd = reinterpret_cast<double*>(a.X);
-  double* Td = reinterpret_cast<double*>(a.tau);
-  static_assert(kBwdWin == R, "one backward block per stage");
-  for (int s = 0; s < nstage; ++s) {
-    issue_bwd(s + kStages - 1);
-    cp_async_wait<kStages - 1>();
-    __syncwarp();
-    const int q0 = np - (s + 1) * R;  // rows q0+R-1 .. q0, q0 % kBwdWin == 0
-    const double2* st =
-        reinterpret_cast<const double2*>(ring + (size_t)(s % kStages) * STAGE + (size_t)slot * kBwdRec);
+  bwd_sweep(warp == P - 1);
+  if constexpr (P > 1) {
 #pragma unroll
-    for (int h = 0; h < kBwdWin / BSUB; ++h) {
-      // records of rows q0+kBwdWin-1-u for u = h*BSUB .. h*BSUB+BSUB-1
-      double2 rv[BSUB][BV];
+    for (int t = 0; t < kBwdWin; ++t) myx[8 + t] = xw[t];
+    __syncthreads();
+    // ---- B2, B3 ----
+    if (warp < P - 1) {
+      double T[kBwdWin];
+      const double* Xl = xch + ((size_t)(P - 1) * NL + ln) * kXch + 8;
 #pragma unroll
-      for (int w = 0; w < BSUB; ++w)
+      for (int t = 0; t < kBwdWin; ++t) T[t] = Xl[t];
+      for (int k = P - 2; k > warp; --k) {
+        const double* psi = a.PP + ((((size_t)g * (P - 2) + (k - 1)) * 2 + c) * MP + mm) * kTransfer + 16;
+        const double* Xk = xch + ((size_t)k * NL + ln) * kXch + 8;
+        double nt[kBwdWin];
 #pragma unroll
-        for (int v = 0; v < BV; ++v) rv[w][v] = st[(kBwdWin - 1 - (h * BSUB + w)) * (BREC / 2) + v];
-      double xs[BSUB];
+        for (int o = 0; o < kBwdWin; ++o) {
+          double acc = Xk[o];
 #pragma unroll
-      for (int w = 0; w < BSUB; ++w) {
-        const int u = h * BSUB + w;
-        const int j = q0 + kBwdWin - 1 - u;  // j % kBwdWin == kBwdWin-1-u
-        auto rec = [&](int k) -> double { return (k & 1) ? rv[w][k >> 1].y : rv[w][k >> 1].x; };
-        double acc0 = ysave[(size_t)j * NL + ln];
-        double acc1 = 0.0, acc2 = 0.0;
-#pragma unroll
-        for (int b = 0; b < NBMAX; ++b) acc1 = fma(-rec(W1 + b), x1[b], acc1);
-#pragma unroll
-        for (int t = kBwdWin; t >= 2; --t) {
-          const int sl = (kBwdWin - 1 - u + t) % kBwdWin;
-          if (t % 3 == 0)
-            acc0 = fma(-rec(t), xw[sl], acc0);
-          else if (t % 3 == 1)
-            acc1 = fma(-rec(t), xw[sl], acc1);
-          else
-            acc2 = fma(-rec(t), xw[sl], acc2);
+          for (int i = 0; i < kBwdWin; ++i) acc = fma(psi[o * kBwdWin + i], T[i], acc);
+          nt[o] = acc;
         }
-        const double sacc = fma(-rec(1), xw[(kBwdWin - u) % kBwdWin], acc0 + (acc1 + acc2));
-        const double xj = sacc * rec(0);
-        xw[(kBwdWin - 1 - u) % kBwdWin] = xj;
-        xs[w] = xj;
-      }
-      // stores, undoing the i-scaling of u_x and its taus (ux = i vx: re = -vx_im, im = vx_re)
 #pragma unroll
-      for (int w = 0; w < BSUB; ++w) {
-        const double partner = __shfl_xor_sync(0xffffffffu, xs[w], MP);
-        const long long code = __double_as_longlong(rv[w][BV - 1].y);
-        const size_t off = (size_t)(code >> 1);
-        const double v = (code & 1) ? (part ? partner : -partner) : xs[w];
-        double* dst = off < xplanes ? Xd + 2 * (off + m) : Td + 2 * (off - xplanes + m);
-        if (live && code >= 0) dst[part] = v;
+        for (int o = 0; o < kBwdWin; ++o) T[o] = nt[o];
+      }
+#pragma unroll
+      for (int t = 0; t < kBwdWin; ++t) xw[t] = T[t];
+      bwd_sweep(true);
+    }
+  }
+  // border unknowns
+  if (warp == 0) {
+#pragma unroll
+    for (int b = 0; b < NBMAX; ++b) {
+      if (live && b < a.cls[c].nb) {
+        const int unk = a.cls[c].left_unk[b];
+        const int k = a.cls[c].left_k[b];
+        const bool rl = realified(unk);
+        double* dst = unk < 4 ? Xd + 2 * (((size_t)unk * a.Nz + k) * Nk + m) : Td + 2 * ((size_t)(unk - UK_TAU0) * Nk + m);
+        dst[rl ? 1 - part : part] = (rl && part) ? -x1[b] : x1[b];
       }
     }
-    __syncwarp();
   }
-  cp_async_wait<0>();
-  // border unknowns
-#pragma unroll
-  for (int b = 0; b < NBMAX; ++b) {
-    const double partner = __shfl_xor_sync(0xffffffffu, x1[b], MP);
-    if (live && b < a.cls[c].nb) {
-      const int unk = a.cls[c].left_unk[b];
-      const int k = a.cls[c].left_k[b];
-      const double v = realified(unk) ? (part ? partner : -partner) : x1[b];
-      double* dst = unk < 4 ? Xd + 2 * (((size_t)unk * a.Nz + k) * Nk + m) : Td + 2 * ((size_t)(unk - UK_TAU0) * Nk + m);
-      dst[part] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Partition transfer matrices of the solve, one thread per (mode, class),
+// from the factor records: for partition k = 1..P-2 (rows [k Lp, (k+1) Lp))
+//   Phi_k[o][i] = exit pending entry o of the forward window after the rows of
+//                 partition k, started from unit pending entry i and a zero
+//                 right-hand side;
+//   Psi_k[o][i] = unknown of row k Lp + o after the backward sweep of the rows
+//                 of partition k, started from unit window entry i (row
+//                 (k+1) Lp + i) with zero y and border unknowns.
+// The arithmetic is that of the sweeps in k_tau_solve.
+// ---------------------------------------------------------------------------
+template <int KL, int KU, int P>
+__global__ void __launch_bounds__(64) k_tau_transfer(TauArgs a) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (m >= a.Nk) return;
+  const int np = a.npad, Lp = np / P;
+  const int g = m / kSolveModes, mm = m % kSolveModes;
+  for (int k = 1; k <= P - 2; ++k) {
+    double* out = a.PP + ((((size_t)g * (P - 2) + (k - 1)) * 2 + c) * kSolveModes + mm) * kTransfer;
+    const int r0 = k * Lp, r1 = (k + 1) * Lp;
+    for (int i = 0; i < 4; ++i) {
+      double y[kFwdWin];
+      for (int t = 0; t < kFwdWin; ++t) y[t] = (t == i) ? 1.0 : 0.0;
+      for (int j = r0; j < r1; ++j) {
+        const double* fr = fwd_record(a.cls[0].FR, np, m, j, c);
+        const int u = (j - r0) % kFwdWin;
+        const int p = __double2loint(fr[0]);
+        double yj = y[u];
+        for (int t = 1; t <= KL; ++t) {
+          if (t == p) {
+            const double yt = y[(u + t) % kFwdWin];
+            y[(u + t) % kFwdWin] = yj;
+            yj = yt;
+          }
+        }
+        for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-fr[t], yj, y[(u + t) % kFwdWin]);
+        y[u] = 0.0;
+      }
+      for (int o = 0; o < 4; ++o) out[o * 4 + i] = y[o];
+    }
+    for (int i = 0; i < kBwdWin; ++i) {
+      double xw[kBwdWin];
+      for (int t = 0; t < kBwdWin; ++t) xw[t] = (t == i) ? 1.0 : 0.0;
+      for (int j = r1 - 1; j >= r0; --j) {
+        const double* br = bwd_record(a.cls[0].BR, np, m, j, c);
+        double acc = 0.0;
+        for (int t = 1; t <= KL + KU; ++t) acc = fma(-br[t], xw[(j + t) % kBwdWin], acc);
+        xw[j % kBwdWin] = acc * br[0];
+      }
+      for (int o = 0; o < kBwdWin; ++o) out[16 + o * kBwdWin + i] = xw[o];
     }
   }
 }
@@ -470,33 +625,36 @@ __global__ void k_lincomb(LinComb lc, double2* __restrict__ out, long long count
 
 __device__ __forceinline__ double2 proj(double2 v, bool p) { return p ? make_double2(v.x, 0.0) : v; }
 
-__global__ void k_mass_apply(const double2* __restrict__ X, double2* __restrict__ MX, const double* __restrict__ s3,
-                             int Nz, int Nk, int Nx, int project) {
-  const long long total = (long long)Nz * Nk;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(i / Nk), m = (int)(i % Nk);
-    const bool pj = project && (m == 0 || 2 * m == Nx);
-    const double s0 = s3[3 * k], s1 = s3[3 * k + 1], s2 = s3[3 * k + 2];
-    MX[i] = make_double2(0.0, 0.0);
-    for (int f = 0; f < 3; ++f) {
-      const double2* Xf = X + (size_t)f * Nz * Nk;
-      double2 acc = make_double2(0.0, 0.0);
-      acc = cfma(s0, proj(Xf[(size_t)k * Nk + m], pj), acc);
-      if (k + 2 < Nz) acc = cfma(s1, proj(Xf[(size_t)(k + 2) * Nk + m], pj), acc);
-      if (k + 4 < Nz) acc = cfma(s2, proj(Xf[(size_t)(k + 4) * Nk + m], pj), acc);
-      MX[(size_t)(1 + f) * Nz * Nk + i] = acc;
-    }
+// One thread per (row k, mode m): grid (ceil(Nk / 128), Nz).
+__global__ void __launch_bounds__(128) k_mass_apply(const double2* __restrict__ X, double2* __restrict__ MX,
+                                                    const double* __restrict__ s3, int Nz, int Nk, int Nx,
+                                                    int project) {
+  const int k = blockIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= Nk) return;
+  const size_t i = (size_t)k * Nk + m;
+  const bool pj = project && (m == 0 || 2 * m == Nx);
+  const double s0 = s3[3 * k], s1 = s3[3 * k + 1], s2 = s3[3 * k + 2];
+  MX[i] = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    const double2* Xf = X + (size_t)f * Nz * Nk;
+    double2 acc = make_double2(0.0, 0.0);
+    acc = cfma(s0, proj(Xf[i], pj), acc);
+    if (k + 2 < Nz) acc = cfma(s1, proj(Xf[i + 2 * (size_t)Nk], pj), acc);
+    if (k + 4 < Nz) acc = cfma(s2, proj(Xf[i + 4 * (size_t)Nk], pj), acc);
+    MX[(size_t)(1 + f) * Nz * Nk + i] = acc;
   }
 }
 
-__global__ void k_lx_finalize(double2* __restrict__ LX, const double2* __restrict__ X, const double* __restrict__ s3,
-                              int Nz, int Nk, int Nx, double k0, double s, double kappa, double nu, double beta) {
-  const long long total = (long long)Nz * Nk;
+// One thread per (row k, mode m): grid (ceil(Nk / 128), Nz).
+__global__ void __launch_bounds__(128) k_lx_finalize(double2* __restrict__ LX, const double2* __restrict__ X,
+                                                     const double* __restrict__ s3, int Nz, int Nk, int Nx, double k0,
+                                                     double s, double kappa, double nu, double beta) {
   const double ib = 1.0 / beta;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(i / Nk), m = (int)(i % Nk);
+  {
+    const int k = blockIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= Nk) return;
+    const size_t i = (size_t)k * Nk + m;
     const double s0 = s3[3 * k], s1 = s3[3 * k + 1], s2 = s3[3 * k + 2];
     auto xf = [&](int f, int kk) -> double2 {
       return (kk < Nz) ? X[((size_t)f * Nz + kk) * Nk + m] : make_double2(0.0, 0.0);
@@ -542,22 +700,23 @@ __global__ void k_lx_finalize(double2* __restrict__ LX, const double2* __restric
 // Final RK update X_f = S^{-1} y for f = b, ux, uz, where y is the stage
 // combination of the b / u_x / u_z equation rows (C^(2) space).  S is upper
 // triangular with offsets 0, +2, +4, so each (field, parity, mode) column is a
-// short backward recurrence.  A CTA owns 32 modes of one (field, parity): its
-// 256 threads form y for all rows into shared memory (independent, coalesced
-// loads) together with the S entries of those rows and the reciprocal
-// diagonal, warp 0 runs the 32 recurrences out of shared memory, and all
-// threads write X back.
+// short backward recurrence.  A CTA owns kFinalModes modes of one (field,
+// parity): its 256 threads form y for all rows into shared memory (every
+// input of a row in flight at once), together with the S entries of those
+// rows and the reciprocal diagonal; the first kFinalModes threads run the
+// recurrences out of shared memory, and all threads write X back.
+constexpr int kFinalModes = 8;
 template <int N>
 __global__ void __launch_bounds__(256) k_rk_final(LinComb lc, double2* __restrict__ X, const double* __restrict__ s3,
                                                   int Nz, int Nk) {
-  extern __shared__ double2 ys[];  // [rows of this parity][32], then 3 doubles per row
+  extern __shared__ double2 ys[];  // [rows of this parity][kFinalModes], then 3 doubles per row
+  constexpr int MB = kFinalModes, RG = 256 / MB;  // modes per CTA, row groups
   const int f = blockIdx.y >> 1, par = blockIdx.y & 1;
-  const int m0 = blockIdx.x * 32;
-  const int mm = threadIdx.x % 32, ks = threadIdx.x / 32;
-  const int m = m0 + mm;
+  const int mm = threadIdx.x % MB, ks = threadIdx.x / MB;
+  const int m = blockIdx.x * MB + mm;
   const size_t plane = (size_t)Nz * Nk;
   const int K = (Nz - par + 1) / 2;  // rows k = par + 2 ri
-  double* sk = reinterpret_cast<double*>(ys + (size_t)K * 32);  // [ri][3]: 1/S_kk, S_k,k+2, S_k,k+4
+  double* sk = reinterpret_cast<double*>(ys + (size_t)K * MB);  // [ri][3]: 1/S_kk, S_k,k+2, S_k,k+4
   for (int q = threadIdx.x; q < K; q += blockDim.x) {
     const int k = par + 2 * q;
     sk[3 * q] = 1.0 / s3[3 * k];
@@ -566,8 +725,8 @@ __global__ void __launch_bounds__(256) k_rk_final(LinComb lc, double2* __restric
   }
   const size_t base = (size_t)(1 + f) * plane;  // equation rows b, mx, mz follow continuity
   const int mc = m < Nk ? m : Nk - 1;           // clamped column: loads stay in bounds
-  for (int r0 = ks; r0 < K; r0 += 16) {
-    const int r1 = (r0 + 8 < K) ? r0 + 8 : r0;
+  for (int r0 = ks; r0 < K; r0 += 2 * RG) {
+    const int r1 = (r0 + RG < K) ? r0 + RG : r0;
     const size_t e0 = base + (size_t)(par + 2 * r0) * Nk + mc;
     const size_t e1 = base + (size_t)(par + 2 * r1) * Nk + mc;
     double2 v0[N], v1[N];
@@ -582,49 +741,51 @@ __global__ void __launch_bounds__(256) k_rk_final(LinComb lc, double2* __restric
       a0 = cfma(lc.w[t], v0[t], a0);
       a1 = cfma(lc.w[t], v1[t], a1);
     }
-    ys[r0 * 32 + mm] = a0;
-    if (r0 + 8 < K) ys[(r0 + 8) * 32 + mm] = a1;
+    ys[r0 * MB + mm] = a0;
+    if (r0 + RG < K) ys[(r0 + RG) * MB + mm] = a1;
   }
   __syncthreads();
-  if (ks == 0) {
+  if (threadIdx.x < MB) {
     double2 x2 = make_double2(0.0, 0.0), x4 = make_double2(0.0, 0.0);
     for (int ri = K - 1; ri >= 0; --ri) {
-      double2 y = ys[ri * 32 + mm];
+      double2 y = ys[ri * MB + mm];
       y = cfma(-sk[3 * ri + 1], x2, y);
       y = cfma(-sk[3 * ri + 2], x4, y);
       const double inv = sk[3 * ri];
       const double2 x = make_double2(y.x * inv, y.y * inv);
-      ys[ri * 32 + mm] = x;
+      ys[ri * MB + mm] = x;
       x4 = x2;
       x2 = x;
     }
   }
   __syncthreads();
   if (m < Nk)
-    for (int ri = ks; ri < K; ri += 8) X[(size_t)f * plane + (size_t)(par + 2 * ri) * Nk + m] = ys[ri * 32 + mm];
+    for (int ri = ks; ri < K; ri += RG) X[(size_t)f * plane + (size_t)(par + 2 * ri) * Nk + m] = ys[ri * MB + mm];
 }
 
 template <int KL, int KU>
-void factor_impl(const TauArgs& a, cudaStream_t st) {
+void factor_impl(const TauArgs& a, int parts, cudaStream_t st) {
   int nmax = a.cls[0].n > a.cls[1].n ? a.cls[0].n : a.cls[1].n;
   dim3 grid((a.Nk + 63) / 64, 2);
   k_tau_factor<KL, KU><<<grid, 64, 0, st>>>(a, nmax);
+  if (parts == kTauParts && kTauParts > 2) k_tau_transfer<KL, KU, kTauParts><<<grid, 64, 0, st>>>(a);
 }
 
+template <int P>
 size_t solve_smem_bytes(int npad) {
-  constexpr int MP = kSolveModes;
-  const size_t FREC = 2 * kFwdRec * MP, BREC = 2 * kBwdRec * MP, RREC = 2 * MP;
-  const size_t FSTAGE = kRowsPerStage * (FREC + 2 * RREC), BSTAGE = kRowsPerStage * BREC;
-  const size_t STAGE = FSTAGE > BSTAGE ? FSTAGE : BSTAGE;
-  return (kStages * STAGE) * sizeof(double) + (size_t)npad * 4 * MP * sizeof(double) + (size_t)npad * 2 * sizeof(int) +
-         (size_t)npad * 2;
+  constexpr size_t NL = 4 * kSolveModes;
+  return ((size_t)P * kPartStages * part_stage_doubles<P>() + (size_t)npad * NL + (size_t)P * NL * kXch) *
+             sizeof(double) +
+         (size_t)npad * 2 * sizeof(int);
 }
 
 template <int KL, int KU>
-void solve_impl(const TauArgs& a, cudaStream_t st) {
+void solve_impl(const TauArgs& a, int parts, cudaStream_t st) {
   const int groups = (a.Nk + kSolveModes - 1) / kSolveModes;
-  const size_t smem = solve_smem_bytes(a.npad);
-  k_tau_solve<KL, KU><<<groups, 32, smem, st>>>(a);
+  if (parts == kTauParts)
+    k_tau_solve<KL, KU, kTauParts><<<groups, 32 * kTauParts, solve_smem_bytes<kTauParts>(a.npad), st>>>(a);
+  else
+    k_tau_solve<KL, KU, 1><<<groups, 32, solve_smem_bytes<1>(a.npad), st>>>(a);
 }
 
 }  // namespace
@@ -632,7 +793,9 @@ void solve_impl(const TauArgs& a, cudaStream_t st) {
 size_t tau_factor_scratch_doubles(int nmax, int Nk);
 
 cudaError_t set_tau_smem_limits(int bytes) {
-  cudaError_t e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU, kTauParts>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
   const void* fns[] = {(const void*)k_rk_final<1>,  (const void*)k_rk_final<2>,  (const void*)k_rk_final<3>,
                        (const void*)k_rk_final<4>,  (const void*)k_rk_final<5>,  (const void*)k_rk_final<6>,
@@ -645,12 +808,20 @@ cudaError_t set_tau_smem_limits(int bytes) {
   return cudaSuccess;
 }
 
-size_t tau_solve_smem_bytes(int n) { return solve_smem_bytes(n); }
+size_t tau_solve_smem_bytes(int npad, int parts) {
+  return parts == kTauParts ? solve_smem_bytes<kTauParts>(npad) : solve_smem_bytes<1>(npad);
+}
+
+size_t tau_transfer_doubles(int Nk, int parts) {
+  if (parts <= 2) return 0;
+  const size_t groups = (size_t)(Nk + kSolveModes - 1) / kSolveModes;
+  return groups * (size_t)(parts - 2) * 2 * kSolveModes * kTransfer;
+}
 
 // Supported band shape: the RBC layout gives kl = 4, ku = 8 for every Nz >= 8
 // (narrower layouts are zero-padded to it by the plan).
-void launch_tau_factor(const TauArgs& a, cudaStream_t st) { factor_impl<kTauKL, kTauKU>(a, st); }
-void launch_tau_solve(const TauArgs& a, cudaStream_t st) { solve_impl<kTauKL, kTauKU>(a, st); }
+void launch_tau_factor(const TauArgs& a, int parts, cudaStream_t st) { factor_impl<kTauKL, kTauKU>(a, parts, st); }
+void launch_tau_solve(const TauArgs& a, int parts, cudaStream_t st) { solve_impl<kTauKL, kTauKU>(a, parts, st); }
 
 size_t tau_factor_scratch_doubles(int nmax, int Nk) {
   const int KL = kTauKL, KU = kTauKU, WW = 2 * KL + KU + 1;
@@ -677,23 +848,19 @@ void launch_lincomb(const LinComb& lc, double2* out, long long count, cudaStream
 
 void launch_mass_apply(const double2* X, double2* MX, const double* s3, int Nz, int Nk, int Nx, int project,
                        cudaStream_t st) {
-  long long total = (long long)Nz * Nk;
-  int blocks = (int)((total + 255) / 256);
-  if (blocks > 148 * 16) blocks = 148 * 16;
-  k_mass_apply<<<blocks, 256, 0, st>>>(X, MX, s3, Nz, Nk, Nx, project);
+  dim3 grid((Nk + 127) / 128, Nz);
+  k_mass_apply<<<grid, 128, 0, st>>>(X, MX, s3, Nz, Nk, Nx, project);
 }
 
 void launch_lx_finalize(double2* LX, const double2* X, const double* s3, int Nz, int Nk, int Nx, double k0,
                         double s, double kappa, double nu, double beta, cudaStream_t st) {
-  long long total = (long long)Nz * Nk;
-  int blocks = (int)((total + 255) / 256);
-  if (blocks > 148 * 16) blocks = 148 * 16;
-  k_lx_finalize<<<blocks, 256, 0, st>>>(LX, X, s3, Nz, Nk, Nx, k0, s, kappa, nu, beta);
+  dim3 grid((Nk + 127) / 128, Nz);
+  k_lx_finalize<<<grid, 128, 0, st>>>(LX, X, s3, Nz, Nk, Nx, k0, s, kappa, nu, beta);
 }
 
 void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* s3, int Nz, int Nk,
                      cudaStream_t st) {
-  dim3 grid((Nk + 31) / 32, 6);
+  dim3 grid((Nk + kFinalModes - 1) / kFinalModes, 6);
   const size_t smem = rk_final_smem_bytes(Nz);
 #define TB_RKFINAL_CASE(N) \
   case N:                   \
@@ -712,7 +879,7 @@ void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* 
 
 size_t rk_final_smem_bytes(int Nz) {
   const size_t K = (size_t)(Nz + 1) / 2;
-  return K * 32 * sizeof(double2) + K * 3 * sizeof(double);
+  return K * kFinalModes * sizeof(double2) + K * 3 * sizeof(double);
 }
 
 }  // namespace tb
