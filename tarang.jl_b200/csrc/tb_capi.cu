@@ -45,6 +45,16 @@ struct DevBuf {
   }
 };
 
+// Non-owning window into a DevBuf.
+struct DevView {
+  void* p = nullptr;
+  size_t bytes = 0;
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
 template <class T>
 void upload(DevBuf& d, const std::vector<T>& h) {
   d.alloc(h.size() * sizeof(T));
@@ -59,6 +69,7 @@ struct FactorSet {
   double alpha = 0, beta = 0;
   DevBuf FR, BR, SI;  // solve-layout factor records (see tb_kernels.cuh)
   DevBuf PP;          // partition transfer matrices of the solve
+  DevBuf HR;          // per-row backward responses of the partitioned solve
 };
 
 struct Tableau {
@@ -117,7 +128,10 @@ struct tb_plan {
   float last_ms = 0.f;
   size_t plane = 0;  // Nz * Nk complex entries
   // state and work arrays
-  DevBuf X, tau, G, H, MX0, FP[4], LXP[4], Fprev, MXprev, Rsb, tmpgrid;
+  // X holds the 4 state planes followed by the 7 tau rows (tau views its tail),
+  // so one 32-bit element offset from X addresses every unknown of the solve
+  DevBuf X, G, H, MX0, FP[4], LXP[4], Fprev, MXprev, Rsb, tmpgrid;
+  DevView tau;
   // transform constants
   DevBuf bwd, fwd, s3, twM, twN;
   // parity halves of the Chebyshev matrices (H = ceil(Nz/2) rows/cols)
@@ -293,6 +307,7 @@ TauArgs tau_args(tb_plan* P, FactorSet* f, const double2* rhsP) {
   a.rhsP = rhsP;
   a.npad = (P->lay.cls[0].n + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
   a.PP = f ? f->PP.as<double>() : nullptr;
+  a.HR = f ? f->HR.as<double>() : nullptr;
   a.rhs_off = P->rhs_off.as<int>();
   a.err_mode = P->err_mode.as<int>();
   return a;
@@ -314,6 +329,8 @@ FactorSet* get_factors(tb_plan* P, double alpha, double beta) {
   fs->SI.alloc(groups * 2 * 16 * kSolveModes * sizeof(double));
   const size_t npp = tau_transfer_doubles(Nk, P->tau_parts);
   if (npp) fs->PP.alloc(npp * sizeof(double));
+  const size_t nhr = tau_response_doubles(Nk, (int)n, P->tau_parts);
+  if (nhr) fs->HR.alloc(nhr * sizeof(double));
   TB_CUDA_TRY(cudaMemsetAsync(fs->FR.p, 0, fs->FR.bytes, P->st));
   TB_CUDA_TRY(cudaMemsetAsync(fs->BR.p, 0, fs->BR.bytes, P->st));
   TB_CUDA_TRY(cudaMemsetAsync(fs->SI.p, 0, fs->SI.bytes, P->st));
@@ -704,8 +721,9 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
     }
     // state and work arrays
     const size_t pb = P->plane * sizeof(double2);
-    P->X.alloc(4 * pb);
-    P->tau.alloc(7 * P->Nk * sizeof(double2));
+    P->X.alloc(4 * pb + 7 * P->Nk * sizeof(double2));
+    P->tau.p = static_cast<char*>(P->X.p) + 4 * pb;
+    P->tau.bytes = 7 * P->Nk * sizeof(double2);
     P->G.alloc(12 * (size_t)((P->Nz + 1) / 2) * P->Nk * sizeof(double2));
     P->H.alloc(3 * pb);
     P->MX0.alloc(4 * pb);

@@ -58,11 +58,17 @@ constexpr int kTauKL = 4, kTauKU = 8;
 // The solve streams per-row factor records of kSolveModes consecutive Fourier
 // modes: forward record = pivot offset, kTauKL multipliers, 4 boundary-row
 // multipliers; backward record = 1/diag, kTauKL+kTauKU U entries, 4 border
-// entries and the encoded store target of the band column (one contiguous
-// record per mode, an even number of doubles so a lane reads it 16 bytes at a time).
+// entries, the encoded store target of the band column and the 4 responses of
+// the row's y to its partition's starting window (one contiguous record per
+// mode, an even number of doubles so a lane reads it 16 bytes at a time).
 constexpr int kSolveModes = 4;
 constexpr int kFwdRec = 1 + kTauKL + 4 + 1;  // pivot, multipliers, border, pad to 16 B
-constexpr int kBwdRec = 1 + kTauKL + kTauKU + 4 + 1;
+// backward: 1/diag, U entries, border, store code, 4 forward responses G
+constexpr int kBwdCode = 1 + kTauKL + kTauKU + 4;
+constexpr int kBwdG = kBwdCode + 1;
+constexpr int kBwdRec = kBwdG + 4;
+// per-row backward responses H of the partitioned solve: 12 entries, store code, pad
+constexpr int kHRec = kTauKL + kTauKU + 2;
 // Register windows of the solve sweeps.  The solve splits the band rows into
 // kTauParts partitions (one warp each), each a whole number of backward
 // windows, so rows are padded with identity rows to a multiple of
@@ -100,7 +106,7 @@ struct TauArgs {
   int npad;            // band rows padded to a multiple of kTauRowPad
   double k0;           // 2 pi / Lx
   double alpha, beta;  // LHS = alpha M + beta L
-  // state (T space): X[4][Nz][Nk] (b, ux, uz, p), tau[7][Nk]
+  // state (T space): X[4][Nz][Nk] (b, ux, uz, p) directly followed by tau[7][Nk]
   double2* X;
   double2* tau;
   // P-space right-hand side (cont, b, mx, mz) x Nz x Nk
@@ -108,9 +114,11 @@ struct TauArgs {
   // [row][class] over npad rows: 2 * (element offset of band row j's right-hand
   // side in rhsP) + 1 for a u_x momentum row, -1 for none
   const int* rhs_off;
-  // partition transfer matrices of the solve (Phi 4x4, Psi 12x12 per
-  // partition 1..kTauParts-2, class and mode), written by the factorisation
+  // partition responses of the solve, written by the factorisation:
+  // PP[group][partition][class][mode] = Phi (4x4), Psi (12x12), Gz (4x4);
+  // HR[group][row][class][mode][kHRec] = H (12), store code, pad
   double* PP;
+  double* HR;
   double* scratch;     // factor workspace
   int* err_mode;       // first singular mode, or -1
 };
@@ -120,6 +128,7 @@ void launch_tau_solve(const TauArgs& a, int parts, cudaStream_t st);
 cudaError_t set_tau_smem_limits(int bytes);
 size_t tau_solve_smem_bytes(int npad, int parts);
 size_t tau_transfer_doubles(int Nk, int parts);
+size_t tau_response_doubles(int Nk, int npad, int parts);
 
 struct LinComb {
   const double2* in[12];

@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
       // array, encoded as offset*2 + (1 if the unknown is scaled by i), bit-cast
       const int unk = C.col_unk[j], kk = C.col_k[j];
       const long long off = unk < 4 ? ((long long)unk * a.Nz + kk) * Nk : (long long)4 * a.Nz * Nk + (long long)(unk - UK_TAU0) * Nk;
-      br[W1 + NBMAX] = __longlong_as_double(2 * off + (realified(unk) ? 1 : 0));
+      br[kBwdCode] = __longlong_as_double(2 * off + (realified(unk) ? 1 : 0));
     }
   }
   // padding rows n..npad-1: identity rows with no right-hand side and no store
@@ -155,8 +155,8 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
     double* br = bwd_record(C.BR, a.npad, m, j, c);
     for (int t = 0; t < kFwdRec; ++t) fr[t] = 0.0;
     br[0] = 1.0;
-    for (int t = 1; t < kBwdRec - 1; ++t) br[t] = 0.0;
-    br[kBwdRec - 1] = __longlong_as_double(-1LL);
+    for (int t = 1; t < kBwdCode; ++t) br[t] = 0.0;
+    br[kBwdCode] = __longlong_as_double(-1LL);
   }
   // invert the nb x nb Schur complement (Gauss-Jordan, partial pivoting)
   double Aug[NBMAX][2 * NBMAX];
@@ -211,28 +211,32 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
 // The npad band rows are split into P partitions of Lp = npad/P rows, warp w
 // owning rows [w Lp, (w+1) Lp).  Both triangular sweeps are linear
 // recurrences whose state crossing a partition boundary is small: the 4
-// pending entries of the forward window, the 12 latest unknowns of the
-// backward window.  So
-//   F1  every warp sweeps its rows forward from the raw right-hand side
-//       (exact for warp 0) and publishes its exit window;
-//   F2  warp w >= 1 composes the boundary corrections of the partitions above
-//       it with the transfer matrices Phi (4x4, from the factors);
-//   F3  warp w >= 1 re-runs its rows from the corrected window;
-//   B1  every warp sweeps its rows backward from a zero window (exact for the
-//       last warp) and publishes its top 12 unknowns;
-//   B2  warp w < P-1 composes the true incoming window with Psi (12x12);
-//   B3  warp w < P-1 re-runs its rows from that window, storing X.
-// Each sequential chain is 4 Lp = npad rows long instead of 2 npad.  The
-// factor records of a warp's rows stream through its own shared-memory ring
-// (cp.async, kPartStages stages of kPartRows rows); each lane pulls its
-// records of a stage into registers with 16-byte loads before the stage's
-// arithmetic.  The forward sweep's y stays in shared memory for the backward
-// sweep of the same warp.
+// pending entries of the forward window and the 12 latest unknowns of the
+// backward window.  Every warp sweeps its own rows from a guessed boundary
+// state (the raw right-hand side forward, zeros backward), which is exact for
+// the first (forward) and last (backward) warp, and the error of the guess is
+// removed with responses precomputed by the factorisation:
+//   F1  forward sweep of every partition; publish the exit window;
+//   F2  warp w >= 1 composes its true starting window with the 4x4 transfer
+//       matrices Phi of the partitions above it; the border accumulators get
+//       the 4x4 response Gz, and each y of the partition the 4-vector
+//       response G (held in the backward record, applied when y is read);
+//   B1  backward sweep of every partition from a zero window (the last warp
+//       stores X; the others keep their unknowns in shared memory);
+//   B2  warp w < P-1 composes its true incoming window with the 12x12
+//       transfer matrices Psi of the partitions below it;
+//   B3  warp w < P-1 adds the 12-vector response H of each of its unknowns
+//       (one streamed pass, no recurrence) and stores X.
+// Each sequential chain is 2 Lp rows long.  Factor records stream through a
+// per-warp shared-memory ring (cp.async, kPartStages stages of kPartRows
+// rows); each lane pulls its records of a stage into registers with 16-byte
+// loads before the stage's arithmetic.
 // ---------------------------------------------------------------------------
 constexpr int kPartRows = 6;    // rows per ring stage (the forward window)
 constexpr int kPartStages = 4;  // ring depth
 constexpr int kXch = 20;        // exchange doubles per (warp, lane): D(4) Z(4) Xhat(12)
-constexpr int kTransfer = 16 + 144;  // Phi (4x4) and Psi (12x12) per (partition, class, mode)
+// per (partition, class, mode): Phi (4x4), Psi (12x12), Gz (4x4)
+constexpr int kTrPhi = 0, kTrPsi = 16, kTrGz = 160, kTransfer = 176;
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -245,12 +249,23 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-template <int P>
 __host__ __device__ constexpr size_t part_stage_doubles() {
   constexpr size_t MP = kSolveModes;
   constexpr size_t F = kPartRows * (2 * MP * kFwdRec + 2 * 2 * MP);
   constexpr size_t B = kPartRows * (2 * MP * kBwdRec);
-  return F > B ? F : B;
+  constexpr size_t H = kPartRows * (2 * MP * kHRec);
+  return F > B ? (F > H ? F : H) : (B > H ? B : H);
+}
+
+// X (4 planes) and tau (7 x Nk) are one allocation, so a 32-bit element
+// offset from X addresses both; code = 2 * offset + (1 if the unknown is i
+// times the solved real-ified column), -1 for no store.  u_x = i v gives
+// re(u_x) = -v_im (part-1 lane) and im(u_x) = v_re (part-0 lane).
+__device__ __forceinline__ void store_unknown(double* Xd, int code, int m, int part, double x, bool on) {
+  if (on && code >= 0) {
+    const int rl = code & 1;
+    Xd[2 * ((size_t)(code >> 1) + m) + (part ^ rl)] = (rl & part) ? -x : x;
+  }
 }
 
 template <int KL, int KU, int P>
@@ -258,17 +273,20 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   static_assert(KL + 2 == kFwdWin && KL + KU == kBwdWin, "window sizes follow the band shape");
   static_assert(kFwdWin == kPartRows && kBwdWin == 2 * kPartRows, "one forward window per stage, two stages per backward block");
   static_assert(kFwdRec == KL + NBMAX + 2 && kFwdRec % 2 == 0, "forward record: pivot, l, border, pad");
-  static_assert(kBwdRec == KL + KU + NBMAX + 2 && kBwdRec % 2 == 0, "backward record: 1/d, u, border, code");
+  static_assert(kBwdCode == KL + KU + 1 + NBMAX && kBwdG == kBwdCode + 1 && kBwdRec == kBwdG + 4 && kBwdRec % 2 == 0,
+                "backward record: 1/d, u, border, code, G");
+  static_assert(kHRec == kBwdWin + 2, "H record: 12 responses, code, pad");
   constexpr int MP = kSolveModes;
   constexpr int W1 = KL + KU + 1;
   constexpr int FREC = 2 * MP * kFwdRec;  // doubles per forward row (both classes)
   constexpr int BREC = 2 * MP * kBwdRec;  // doubles per backward row
+  constexpr int HREC = 2 * MP * kHRec;    // doubles per H row
   constexpr int RREC = 2 * MP;            // double2 rhs entries per row (class, mode)
-  constexpr int FV = kFwdRec / 2, BV = kBwdRec / 2;  // 16-byte words per record
+  constexpr int FV = kFwdRec / 2, BV = kBwdRec / 2, HV = kHRec / 2;  // 16-byte words per record
   constexpr int R = kPartRows, NS = kPartStages;
   constexpr int NL = 4 * MP;  // distinct lanes
   constexpr int BSUB = 3;     // backward rows whose records are held in registers at once
-  constexpr int STAGE = (int)part_stage_doubles<P>();
+  constexpr int STAGE = (int)part_stage_doubles();
   static_assert(NL <= 32 && 32 % NL == 0, "lane layout");
   static_assert(R % BSUB == 0, "backward sub-blocks");
   extern __shared__ __align__(16) double smem[];
@@ -285,7 +303,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   const int m = g * MP + mm;
   const bool live = owner && m < Nk;
   double* ring = smem + (size_t)warp * NS * STAGE;
-  double* ysave = smem + (size_t)P * NS * STAGE;  // [row][ln]
+  double* ysave = smem + (size_t)P * NS * STAGE;  // [row][ln]: y, then (rows of warps < P-1) particular x
   double* xch = ysave + (size_t)np * NL;          // [warp][ln][kXch]
   int* rofs = reinterpret_cast<int*>(xch + (size_t)P * NL * kXch);
   // [row][class] right-hand-side code: 2 * element offset + (1 for a u_x momentum
@@ -296,11 +314,12 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   __syncthreads();
   const double* FRg = a.cls[0].FR + (size_t)g * np * FREC;
   const double* BRg = a.cls[0].BR + (size_t)g * np * BREC;
+  const double* HRg = a.HR + (size_t)g * np * HREC;
+  const double* trg = a.PP + (((size_t)g * P * 2 + c) * MP + mm) * kTransfer;  // partition k: + k 2 MP kTransfer
+  constexpr size_t TRK = (size_t)2 * MP * kTransfer;
   double* Xd = reinterpret_cast<double*>(a.X);
-  double* Td = reinterpret_cast<double*>(a.tau);
-  const size_t xplanes = (size_t)4 * a.Nz * Nk;
 
-  // ---- forward sweep over this warp's rows: y = L^-1 P r, boundary rows accumulate z ----
+  // ---- F1: forward sweep over this warp's rows: y = L^-1 P r, boundary rows accumulate z ----
   double y[kFwdWin];
   double z[NBMAX];
   auto issue_fwd = [&](int s) {  // local stage s: rows row0 + s R ..; stage nst is the first of the next warp
@@ -329,144 +348,66 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
     const double v = rb[part ^ rot];
     return (rot & part) ? -v : v;
   };
-  // d0..d3: correction of the first 4 entries of the starting window
-  auto fwd_sweep = [&](double d0, double d1, double d2, double d3) {
-    for (int s = 0; s < NS - 1; ++s) issue_fwd(s);
-    for (int s = 0; s < nst; ++s) {
-      issue_fwd(s + NS - 1);        // refills the slot of stage s-1
-      cp_async_wait<NS - 2>();      // stages s and s+1 are resident
-      __syncwarp();
-      if (s == 0) {
-#pragma unroll
-        for (int t = 0; t < kFwdWin; ++t)
-          y[t] = rhs_at(0, t) + (t == 0 ? d0 : t == 1 ? d1 : t == 2 ? d2 : t == 3 ? d3 : 0.0);
-      }
-      const double2* st =
-          reinterpret_cast<const double2*>(ring + (size_t)(s % NS) * STAGE + (size_t)slot * kFwdRec);
-      double2 rv[kFwdWin][FV];
-#pragma unroll
-      for (int u = 0; u < kFwdWin; ++u)
-#pragma unroll
-        for (int v = 0; v < FV; ++v) rv[u][v] = st[u * (FREC / 2) + v];
-      double incoming[kFwdWin];
-#pragma unroll
-      for (int u = 0; u < kFwdWin; ++u) incoming[u] = rhs_at(s + 1, u);
-      double* ys = ysave + (size_t)(row0 + s * R) * NL + ln;
-#pragma unroll
-      for (int u = 0; u < kFwdWin; ++u) {
-        auto rec = [&](int k) -> double { return (k & 1) ? rv[u][k >> 1].y : rv[u][k >> 1].x; };
-        const int p = __double2loint(rv[u][0].x);
-        double yj = y[u];
-#pragma unroll
-        for (int t = 1; t <= KL; ++t) {
-          const bool sw = (t == p);
-          const double yt = y[(u + t) % kFwdWin];
-          y[(u + t) % kFwdWin] = sw ? yj : yt;
-          yj = sw ? yt : yj;
-        }
-        ys[u * NL] = yj;
-#pragma unroll
-        for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-rec(t), yj, y[(u + t) % kFwdWin]);
-#pragma unroll
-        for (int b = 0; b < NBMAX; ++b) z[b] = fma(-rec(1 + KL + b), yj, z[b]);
-        y[u] = incoming[u];
-      }
-      __syncwarp();  // the slot of stage s is refilled next
-    }
-    cp_async_wait<0>();
-    __syncwarp();
-  };
-
-  // ---- backward sweep over this warp's rows: x = U^-1 (y - B x1) ----
-  double xw[kBwdWin];  // x_j lives in slot j % kBwdWin
-  double x1[NBMAX];
-  auto issue_bwd = [&](int s) {  // local stage s from the bottom: rows row0 + Lp - (s+1) R ..
-    if (s < nst) {
-      double* dst = ring + (size_t)(s % NS) * STAGE;
-      const int lo = row0 + Lp - (s + 1) * R;
-      for (int q = lane; q < R * BREC / 2; q += 32) cp_async16(dst + 2 * q, BRg + (size_t)lo * BREC + 2 * q, true);
-    }
-    cp_async_commit();
-  };
-  auto bwd_sweep = [&](bool store) {
-    for (int s = 0; s < NS - 1; ++s) issue_bwd(s);
-    for (int s0 = 0; s0 < nst; s0 += 2) {
-      const int q0 = row0 + Lp - (s0 + 2) * R;  // block rows q0 .. q0 + kBwdWin - 1, q0 % kBwdWin == 0
-#pragma unroll
-      for (int hs = 0; hs < 2; ++hs) {
-        const int s = s0 + hs;
-        issue_bwd(s + NS - 1);
-        cp_async_wait<NS - 1>();  // stage s is resident
-        __syncwarp();
-        const double2* st =
-            reinterpret_cast<const double2*>(ring + (size_t)(s % NS) * STAGE + (size_t)slot * kBwdRec);
-#pragma unroll
-        for (int h = 0; h < R / BSUB; ++h) {
-          // rows q0 + kBwdWin - 1 - u for u = hs R + h BSUB + w; stage row index R - 1 - (h BSUB + w)
-          double2 rv[BSUB][BV];
-#pragma unroll
-          for (int w = 0; w < BSUB; ++w)
-#pragma unroll
-            for (int v = 0; v < BV; ++v) rv[w][v] = st[(R - 1 - (h * BSUB + w)) * (BREC / 2) + v];
-#pragma unroll
-          for (int w = 0; w < BSUB; ++w) {
-            const int u = hs * R + h * BSUB + w;
-            const int j = q0 + kBwdWin - 1 - u;  // j % kBwdWin == kBwdWin-1-u
-            auto rec = [&](int k) -> double { return (k & 1) ? rv[w][k >> 1].y : rv[w][k >> 1].x; };
-            double acc0 = ysave[(size_t)j * NL + ln];
-            double acc1 = 0.0, acc2 = 0.0;
-#pragma unroll
-            for (int b = 0; b < NBMAX; ++b) acc1 = fma(-rec(W1 + b), x1[b], acc1);
-#pragma unroll
-            for (int t = kBwdWin; t >= 2; --t) {
-              const int sl = (kBwdWin - 1 - u + t) % kBwdWin;
-              if (t % 3 == 0)
-                acc0 = fma(-rec(t), xw[sl], acc0);
-              else if (t % 3 == 1)
-                acc1 = fma(-rec(t), xw[sl], acc1);
-              else
-                acc2 = fma(-rec(t), xw[sl], acc2);
-            }
-            const double sacc = fma(-rec(1), xw[(kBwdWin - u) % kBwdWin], acc0 + (acc1 + acc2));
-            const double xj = sacc * rec(0);
-            xw[(kBwdWin - 1 - u) % kBwdWin] = xj;
-            // store, undoing the i-scaling of u_x and its taus: ux = i v gives
-            // re(ux) = -v_im (from the part-1 lane), im(ux) = v_re (from the part-0 lane)
-            const long long code = __double_as_longlong(rv[w][BV - 1].y);
-            const bool rl = code & 1;
-            const size_t off = (size_t)(code >> 1);
-            double* base = off < xplanes ? Xd + 2 * (off + m) : Td + 2 * (off - xplanes + m);
-            if (store && live && code >= 0) base[rl ? 1 - part : part] = (rl && part) ? -xj : xj;
-          }
-        }
-        __syncwarp();  // the slot of stage s is refilled next
-      }
-    }
-    cp_async_wait<0>();
-    __syncwarp();
-  };
-
-  // ---- forward: F1 ----
 #pragma unroll
   for (int b = 0; b < NBMAX; ++b)
     z[b] = (warp == 0 && part == 0 && m == 0 && b < a.cls[c].nb) ? a.beta * a.cls[c].bc_rhs[b] : 0.0;
-  fwd_sweep(0.0, 0.0, 0.0, 0.0);
+  for (int s = 0; s < NS - 1; ++s) issue_fwd(s);
+  for (int s = 0; s < nst; ++s) {
+    issue_fwd(s + NS - 1);    // refills the slot of stage s-1
+    cp_async_wait<NS - 2>();  // stages s and s+1 are resident
+    __syncwarp();
+    if (s == 0) {
+#pragma unroll
+      for (int t = 0; t < kFwdWin; ++t) y[t] = rhs_at(0, t);
+    }
+    const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NS) * STAGE + (size_t)slot * kFwdRec);
+    double2 rv[kFwdWin][FV];
+#pragma unroll
+    for (int u = 0; u < kFwdWin; ++u)
+#pragma unroll
+      for (int v = 0; v < FV; ++v) rv[u][v] = st[u * (FREC / 2) + v];
+    double incoming[kFwdWin];
+#pragma unroll
+    for (int u = 0; u < kFwdWin; ++u) incoming[u] = rhs_at(s + 1, u);
+    double* ys = ysave + (size_t)(row0 + s * R) * NL + ln;
+#pragma unroll
+    for (int u = 0; u < kFwdWin; ++u) {
+      auto rec = [&](int k) -> double { return (k & 1) ? rv[u][k >> 1].y : rv[u][k >> 1].x; };
+      const int p = __double2loint(rv[u][0].x);
+      double yj = y[u];
+#pragma unroll
+      for (int t = 1; t <= KL; ++t) {
+        const bool sw = (t == p);
+        const double yt = y[(u + t) % kFwdWin];
+        y[(u + t) % kFwdWin] = sw ? yj : yt;
+        yj = sw ? yt : yj;
+      }
+      ys[u * NL] = yj;
+#pragma unroll
+      for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-rec(t), yj, y[(u + t) % kFwdWin]);
+#pragma unroll
+      for (int b = 0; b < NBMAX; ++b) z[b] = fma(-rec(1 + KL + b), yj, z[b]);
+      y[u] = incoming[u];
+    }
+    __syncwarp();  // the slot of stage s is refilled next
+  }
   double* myx = xch + ((size_t)warp * NL + ln) * kXch;
+  // exit window minus the raw right-hand side of the next warp's first rows (the
+  // ring still holds that stage)
+#pragma unroll
+  for (int t = 0; t < 4; ++t) myx[t] = y[t] - rhs_at(nst, t);
+  cp_async_wait<0>();
+  __syncwarp();
+
+  // ---- F2: true starting window of this partition, border accumulators ----
+  double d[4] = {0.0, 0.0, 0.0, 0.0};  // starting-window correction (0 for warp 0)
   if constexpr (P > 1) {
-    // exit window minus the raw right-hand side of the next warp's first rows
-    // (the ring still holds that stage)
-#pragma unroll
-    for (int t = 0; t < 4; ++t) myx[t] = y[t] - rhs_at(nst, t);
-#pragma unroll
-    for (int b = 0; b < NBMAX; ++b) myx[4 + b] = z[b];
     __syncthreads();
-    // ---- F2, F3 ----
     if (warp > 0) {
-      double d[4];
 #pragma unroll
       for (int t = 0; t < 4; ++t) d[t] = xch[(size_t)ln * kXch + t];  // delta_1 = D_0
       for (int k = 1; k < warp; ++k) {
-        const double* phi = a.PP + ((((size_t)g * (P - 2) + (k - 1)) * 2 + c) * MP + mm) * kTransfer;
+        const double* phi = trg + k * TRK + kTrPhi;
         const double* Dk = xch + ((size_t)k * NL + ln) * kXch;
         double nd[4];
 #pragma unroll
@@ -479,12 +420,14 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 #pragma unroll
         for (int o = 0; o < 4; ++o) d[o] = nd[o];
       }
+      const double* gz = trg + warp * TRK + kTrGz;
 #pragma unroll
-      for (int b = 0; b < NBMAX; ++b) z[b] = 0.0;
-      fwd_sweep(d[0], d[1], d[2], d[3]);
+      for (int b = 0; b < NBMAX; ++b)
 #pragma unroll
-      for (int b = 0; b < NBMAX; ++b) myx[4 + b] = z[b];
+        for (int i = 0; i < 4; ++i) z[b] = fma(gz[b * 4 + i], d[i], z[b]);
     }
+#pragma unroll
+    for (int b = 0; b < NBMAX; ++b) myx[4 + b] = z[b];
     __syncthreads();
 #pragma unroll
     for (int b = 0; b < NBMAX; ++b) {
@@ -495,6 +438,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   }
 
   // ---- border unknowns from the Schur complement ----
+  double x1[NBMAX];
   {
     const double* si = a.cls[0].SI + ((size_t)g * 2 + c) * NBMAX * NBMAX * MP + mm;
 #pragma unroll
@@ -506,22 +450,87 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
     }
   }
 
-  // ---- backward: B1 ----
+  // ---- B1: backward sweep over this warp's rows, x = U^-1 (y - B x1), from a zero window ----
+  const bool last = (warp == P - 1);
+  double xw[kBwdWin];  // x_j lives in slot j % kBwdWin
 #pragma unroll
   for (int t = 0; t < kBwdWin; ++t) xw[t] = 0.0;
-  bwd_sweep(warp == P - 1);
-  if constexpr (P > 1) {
+  auto issue_bwd = [&](int s) {  // local stage s from the bottom: rows row0 + Lp - (s+1) R ..
+    if (s < nst) {
+      double* dst = ring + (size_t)(s % NS) * STAGE;
+      const int lo = row0 + Lp - (s + 1) * R;
+      for (int q = lane; q < R * BREC / 2; q += 32) cp_async16(dst + 2 * q, BRg + (size_t)lo * BREC + 2 * q, true);
+    }
+    cp_async_commit();
+  };
+  for (int s = 0; s < NS - 1; ++s) issue_bwd(s);
+  for (int s0 = 0; s0 < nst; s0 += 2) {
+    const int q0 = row0 + Lp - (s0 + 2) * R;  // block rows q0 .. q0 + kBwdWin - 1, q0 % kBwdWin == 0
 #pragma unroll
-    for (int t = 0; t < kBwdWin; ++t) myx[8 + t] = xw[t];
+    for (int hs = 0; hs < 2; ++hs) {
+      const int s = s0 + hs;
+      issue_bwd(s + NS - 1);
+      cp_async_wait<NS - 1>();  // stage s is resident
+      __syncwarp();
+      const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NS) * STAGE + (size_t)slot * kBwdRec);
+#pragma unroll
+      for (int h = 0; h < R / BSUB; ++h) {
+        // rows q0 + kBwdWin - 1 - u for u = hs R + h BSUB + w; stage row index R - 1 - (h BSUB + w)
+        double2 rv[BSUB][BV];
+#pragma unroll
+        for (int w = 0; w < BSUB; ++w)
+#pragma unroll
+          for (int v = 0; v < BV; ++v) rv[w][v] = st[(R - 1 - (h * BSUB + w)) * (BREC / 2) + v];
+#pragma unroll
+        for (int w = 0; w < BSUB; ++w) {
+          const int u = hs * R + h * BSUB + w;
+          const int j = q0 + kBwdWin - 1 - u;  // j % kBwdWin == kBwdWin-1-u
+          auto rec = [&](int k) -> double { return (k & 1) ? rv[w][k >> 1].y : rv[w][k >> 1].x; };
+          double* yx = ysave + (size_t)j * NL + ln;
+          double acc0 = *yx;
+          double acc1 = 0.0, acc2 = 0.0;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc2 = fma(rec(kBwdG + i), d[i], acc2);  // y correction G d
+#pragma unroll
+          for (int b = 0; b < NBMAX; ++b) acc1 = fma(-rec(W1 + b), x1[b], acc1);
+#pragma unroll
+          for (int t = kBwdWin; t >= 2; --t) {
+            const int sl = (kBwdWin - 1 - u + t) % kBwdWin;
+            if (t % 3 == 0)
+              acc0 = fma(-rec(t), xw[sl], acc0);
+            else if (t % 3 == 1)
+              acc1 = fma(-rec(t), xw[sl], acc1);
+            else
+              acc2 = fma(-rec(t), xw[sl], acc2);
+          }
+          const double sacc = fma(-rec(1), xw[(kBwdWin - u) % kBwdWin], acc0 + (acc1 + acc2));
+          const double xj = sacc * rec(0);
+          xw[(kBwdWin - 1 - u) % kBwdWin] = xj;
+          if (last)
+            store_unknown(Xd, __double2loint(rec(kBwdCode)), m, part, xj, live);
+          else
+            *yx = xj;  // particular unknown, completed in B3
+        }
+      }
+      __syncwarp();  // the slot of stage s is refilled next
+    }
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+
+  if constexpr (P > 1) {
+    // ---- B2: true incoming window of this partition ----
+    double* myxh = myx + 8;
+#pragma unroll
+    for (int t = 0; t < kBwdWin; ++t) myxh[t] = xw[t];
     __syncthreads();
-    // ---- B2, B3 ----
-    if (warp < P - 1) {
+    if (!last) {
       double T[kBwdWin];
       const double* Xl = xch + ((size_t)(P - 1) * NL + ln) * kXch + 8;
 #pragma unroll
       for (int t = 0; t < kBwdWin; ++t) T[t] = Xl[t];
       for (int k = P - 2; k > warp; --k) {
-        const double* psi = a.PP + ((((size_t)g * (P - 2) + (k - 1)) * 2 + c) * MP + mm) * kTransfer + 16;
+        const double* psi = trg + k * TRK + kTrPsi;
         const double* Xk = xch + ((size_t)k * NL + ln) * kXch + 8;
         double nt[kBwdWin];
 #pragma unroll
@@ -534,9 +543,38 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 #pragma unroll
         for (int o = 0; o < kBwdWin; ++o) T[o] = nt[o];
       }
+      // ---- B3: x_j += H_j . T over the rows of this partition ----
+      auto issue_h = [&](int s) {
+        if (s < nst) {
+          double* dst = ring + (size_t)(s % NS) * STAGE;
+          const int lo = row0 + s * R;
+          for (int q = lane; q < R * HREC / 2; q += 32) cp_async16(dst + 2 * q, HRg + (size_t)lo * HREC + 2 * q, true);
+        }
+        cp_async_commit();
+      };
+      for (int s = 0; s < NS - 1; ++s) issue_h(s);
+      for (int s = 0; s < nst; ++s) {
+        issue_h(s + NS - 1);
+        cp_async_wait<NS - 1>();
+        __syncwarp();
+        const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NS) * STAGE + (size_t)slot * kHRec);
 #pragma unroll
-      for (int t = 0; t < kBwdWin; ++t) xw[t] = T[t];
-      bwd_sweep(true);
+        for (int u = 0; u < R; ++u) {
+          double2 hv[HV];
+#pragma unroll
+          for (int v = 0; v < HV; ++v) hv[v] = st[u * (HREC / 2) + v];
+          const int j = row0 + s * R + u;
+          double acc0 = ysave[(size_t)j * NL + ln], acc1 = 0.0;
+#pragma unroll
+          for (int i = 0; i < kBwdWin; i += 2) {
+            acc0 = fma(hv[i / 2].x, T[i], acc0);
+            acc1 = fma(hv[i / 2].y, T[i + 1], acc1);
+          }
+          store_unknown(Xd, __double2loint(hv[HV - 1].x), m, part, acc0 + acc1, live);
+        }
+        __syncwarp();
+      }
+      cp_async_wait<0>();
     }
   }
   // border unknowns
@@ -546,24 +584,23 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
       if (live && b < a.cls[c].nb) {
         const int unk = a.cls[c].left_unk[b];
         const int k = a.cls[c].left_k[b];
-        const bool rl = realified(unk);
-        double* dst = unk < 4 ? Xd + 2 * (((size_t)unk * a.Nz + k) * Nk + m) : Td + 2 * ((size_t)(unk - UK_TAU0) * Nk + m);
-        dst[rl ? 1 - part : part] = (rl && part) ? -x1[b] : x1[b];
+        const int off = unk < 4 ? (unk * a.Nz + k) * Nk : 4 * a.Nz * Nk + (unk - UK_TAU0) * Nk;
+        store_unknown(Xd, 2 * off + (realified(unk) ? 1 : 0), m, part, x1[b], true);
       }
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// Partition transfer matrices of the solve, one thread per (mode, class),
-// from the factor records: for partition k = 1..P-2 (rows [k Lp, (k+1) Lp))
-//   Phi_k[o][i] = exit pending entry o of the forward window after the rows of
-//                 partition k, started from unit pending entry i and a zero
-//                 right-hand side;
-//   Psi_k[o][i] = unknown of row k Lp + o after the backward sweep of the rows
-//                 of partition k, started from unit window entry i (row
-//                 (k+1) Lp + i) with zero y and border unknowns.
-// The arithmetic is that of the sweeps in k_tau_solve.
+// Partition responses of the solve, one thread per (mode, class), from the
+// factor records (the arithmetic of the sweeps in k_tau_solve).  Partition k
+// owns rows [k Lp, (k+1) Lp).  For k >= 1 (forward, started from unit pending
+// entry i of the window and a zero right-hand side):
+//   G of row j (backward record slots kBwdG..) = y_j,
+//   Phi_k[o][i] = exit pending entry o,  Gz_k[b][i] = border accumulator b.
+// For k <= P-2 (backward from unit window entry i, row (k+1) Lp + i, with zero
+// y and border unknowns):
+//   H of row j (H record) = x_j,  Psi_k[o][i] = x of row k Lp + o.
 // ---------------------------------------------------------------------------
 template <int KL, int KU, int P>
 __global__ void __launch_bounds__(64) k_tau_transfer(TauArgs a) {
@@ -572,39 +609,52 @@ __global__ void __launch_bounds__(64) k_tau_transfer(TauArgs a) {
   if (m >= a.Nk) return;
   const int np = a.npad, Lp = np / P;
   const int g = m / kSolveModes, mm = m % kSolveModes;
-  for (int k = 1; k <= P - 2; ++k) {
-    double* out = a.PP + ((((size_t)g * (P - 2) + (k - 1)) * 2 + c) * kSolveModes + mm) * kTransfer;
+  for (int k = 0; k < P; ++k) {
+    double* tr = a.PP + ((((size_t)g * P + k) * 2 + c) * kSolveModes + mm) * kTransfer;
     const int r0 = k * Lp, r1 = (k + 1) * Lp;
-    for (int i = 0; i < 4; ++i) {
-      double y[kFwdWin];
-      for (int t = 0; t < kFwdWin; ++t) y[t] = (t == i) ? 1.0 : 0.0;
-      for (int j = r0; j < r1; ++j) {
-        const double* fr = fwd_record(a.cls[0].FR, np, m, j, c);
-        const int u = (j - r0) % kFwdWin;
-        const int p = __double2loint(fr[0]);
-        double yj = y[u];
-        for (int t = 1; t <= KL; ++t) {
-          if (t == p) {
-            const double yt = y[(u + t) % kFwdWin];
-            y[(u + t) % kFwdWin] = yj;
-            yj = yt;
+    if (k >= 1) {
+      for (int i = 0; i < 4; ++i) {
+        double y[kFwdWin], z[NBMAX] = {0.0, 0.0, 0.0, 0.0};
+        for (int t = 0; t < kFwdWin; ++t) y[t] = (t == i) ? 1.0 : 0.0;
+        for (int j = r0; j < r1; ++j) {
+          const double* fr = fwd_record(a.cls[0].FR, np, m, j, c);
+          const int u = (j - r0) % kFwdWin;
+          const int p = __double2loint(fr[0]);
+          double yj = y[u];
+          for (int t = 1; t <= KL; ++t) {
+            if (t == p) {
+              const double yt = y[(u + t) % kFwdWin];
+              y[(u + t) % kFwdWin] = yj;
+              yj = yt;
+            }
+          }
+          bwd_record(a.cls[0].BR, np, m, j, c)[kBwdG + i] = yj;
+          for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-fr[t], yj, y[(u + t) % kFwdWin]);
+          for (int b = 0; b < NBMAX; ++b) z[b] = fma(-fr[1 + KL + b], yj, z[b]);
+          y[u] = 0.0;
+        }
+        for (int o = 0; o < 4; ++o) tr[kTrPhi + o * 4 + i] = y[o];
+        for (int b = 0; b < NBMAX; ++b) tr[kTrGz + b * 4 + i] = z[b];
+      }
+    }
+    if (k <= P - 2) {
+      for (int i = 0; i < kBwdWin; ++i) {
+        double xw[kBwdWin];
+        for (int t = 0; t < kBwdWin; ++t) xw[t] = (t == i) ? 1.0 : 0.0;
+        for (int j = r1 - 1; j >= r0; --j) {
+          const double* br = bwd_record(a.cls[0].BR, np, m, j, c);
+          double acc = 0.0;
+          for (int t = 1; t <= KL + KU; ++t) acc = fma(-br[t], xw[(j + t) % kBwdWin], acc);
+          xw[j % kBwdWin] = acc * br[0];
+          double* hr = a.HR + ((((size_t)g * np + j) * 2 + c) * kSolveModes + mm) * kHRec;
+          hr[i] = xw[j % kBwdWin];
+          if (i == 0) {
+            hr[kBwdWin] = br[kBwdCode];
+            hr[kBwdWin + 1] = 0.0;
           }
         }
-        for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-fr[t], yj, y[(u + t) % kFwdWin]);
-        y[u] = 0.0;
+        for (int o = 0; o < kBwdWin; ++o) tr[kTrPsi + o * kBwdWin + i] = xw[o];
       }
-      for (int o = 0; o < 4; ++o) out[o * 4 + i] = y[o];
-    }
-    for (int i = 0; i < kBwdWin; ++i) {
-      double xw[kBwdWin];
-      for (int t = 0; t < kBwdWin; ++t) xw[t] = (t == i) ? 1.0 : 0.0;
-      for (int j = r1 - 1; j >= r0; --j) {
-        const double* br = bwd_record(a.cls[0].BR, np, m, j, c);
-        double acc = 0.0;
-        for (int t = 1; t <= KL + KU; ++t) acc = fma(-br[t], xw[(j + t) % kBwdWin], acc);
-        xw[j % kBwdWin] = acc * br[0];
-      }
-      for (int o = 0; o < kBwdWin; ++o) out[16 + o * kBwdWin + i] = xw[o];
     }
   }
 }
@@ -768,13 +818,13 @@ void factor_impl(const TauArgs& a, int parts, cudaStream_t st) {
   int nmax = a.cls[0].n > a.cls[1].n ? a.cls[0].n : a.cls[1].n;
   dim3 grid((a.Nk + 63) / 64, 2);
   k_tau_factor<KL, KU><<<grid, 64, 0, st>>>(a, nmax);
-  if (parts == kTauParts && kTauParts > 2) k_tau_transfer<KL, KU, kTauParts><<<grid, 64, 0, st>>>(a);
+  if (parts == kTauParts && kTauParts > 1) k_tau_transfer<KL, KU, kTauParts><<<grid, 64, 0, st>>>(a);
 }
 
 template <int P>
 size_t solve_smem_bytes(int npad) {
   constexpr size_t NL = 4 * kSolveModes;
-  return ((size_t)P * kPartStages * part_stage_doubles<P>() + (size_t)npad * NL + (size_t)P * NL * kXch) *
+  return ((size_t)P * kPartStages * part_stage_doubles() + (size_t)npad * NL + (size_t)P * NL * kXch) *
              sizeof(double) +
          (size_t)npad * 2 * sizeof(int);
 }
@@ -813,9 +863,15 @@ size_t tau_solve_smem_bytes(int npad, int parts) {
 }
 
 size_t tau_transfer_doubles(int Nk, int parts) {
-  if (parts <= 2) return 0;
+  if (parts <= 1) return 0;
   const size_t groups = (size_t)(Nk + kSolveModes - 1) / kSolveModes;
-  return groups * (size_t)(parts - 2) * 2 * kSolveModes * kTransfer;
+  return groups * (size_t)parts * 2 * kSolveModes * kTransfer;
+}
+
+size_t tau_response_doubles(int Nk, int npad, int parts) {
+  if (parts <= 1) return 0;
+  const size_t groups = (size_t)(Nk + kSolveModes - 1) / kSolveModes;
+  return groups * (size_t)npad * 2 * kSolveModes * kHRec;
 }
 
 // Supported band shape: the RBC layout gives kl = 4, ku = 8 for every Nz >= 8
