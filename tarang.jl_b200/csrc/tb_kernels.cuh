@@ -62,7 +62,9 @@ constexpr int kTauKL = 4, kTauKU = 8;
 // the row's y to its partition's starting window (one contiguous record per
 // mode, an even number of doubles so a lane reads it 16 bytes at a time).
 constexpr int kSolveModes = 4;
-constexpr int kFwdRec = 1 + kTauKL + 4 + 1;  // pivot, multipliers, border, pad to 16 B
+// forward: pivot, multipliers, border, rotation flag of the row entering the window
+constexpr int kFwdRec = 1 + kTauKL + 4 + 1;
+constexpr int kFwdRot = kFwdRec - 1;
 // backward: 1/diag, U entries, border, store code, 4 forward responses G
 constexpr int kBwdCode = 1 + kTauKL + kTauKU + 4;
 constexpr int kBwdG = kBwdCode + 1;

@@ -137,7 +137,12 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
       fr[1 + KL + q] = cq;
     }
     for (int q = nb; q < NBMAX; ++q) fr[1 + KL + q] = 0.0;
-    for (int q = 1 + KL + NBMAX; q < kFwdRec; ++q) fr[q] = 0.0;
+    // last slot: 1 when the right-hand side of row j + kFwdWin (the row entering
+    // the forward window at this row) is a u_x momentum row, scaled by -i on load
+    {
+      const int jn = j + kFwdWin;
+      fr[kFwdRot] = __longlong_as_double((jn < n && C.row_eq[jn] == EQ_MX) ? 1LL : 0LL);
+    }
     br[0] = dinv;
     for (int t = 1; t < W1; ++t) br[t] = (j + t < n) ? W[(size_t)j * WW + KL + t] : 0.0;
     for (int b = 0; b < NBMAX; ++b) br[W1 + b] = (b < nb) ? Bd[(size_t)j * NBMAX + b] : 0.0;
@@ -272,7 +277,8 @@ template <int KL, int KU, int P>
 __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   static_assert(KL + 2 == kFwdWin && KL + KU == kBwdWin, "window sizes follow the band shape");
   static_assert(kFwdWin == kPartRows && kBwdWin == 2 * kPartRows, "one forward window per stage, two stages per backward block");
-  static_assert(kFwdRec == KL + NBMAX + 2 && kFwdRec % 2 == 0, "forward record: pivot, l, border, pad");
+  static_assert(kFwdRec == KL + NBMAX + 2 && kFwdRot == kFwdRec - 1 && kFwdRec % 2 == 0,
+                "forward record: pivot, l, border, rotation flag of the entering row");
   static_assert(kBwdCode == KL + KU + 1 + NBMAX && kBwdG == kBwdCode + 1 && kBwdRec == kBwdG + 4 && kBwdRec % 2 == 0,
                 "backward record: 1/d, u, border, code, G");
   static_assert(kHRec == kBwdWin + 2, "H record: 12 responses, code, pad");
@@ -324,14 +330,16 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   double z[NBMAX];
   auto issue_fwd = [&](int s) {  // local stage s: rows row0 + s R ..; stage nst is the first of the next warp
     const int r0 = row0 + s * R;
-    if (s <= nst && r0 < np) {
+    if (s <= nst) {
       double* dst = ring + (size_t)(s % NS) * STAGE;
-      for (int q = lane; q < R * FREC / 2; q += 32) cp_async16(dst + 2 * q, FRg + (size_t)r0 * FREC + 2 * q, true);
+      if (r0 < np)
+        for (int q = lane; q < R * FREC / 2; q += 32) cp_async16(dst + 2 * q, FRg + (size_t)r0 * FREC + 2 * q, true);
+      // right-hand sides (zero-filled past the last row)
       double2* rdst = reinterpret_cast<double2*>(dst + R * FREC);
       for (int q = lane; q < R * RREC; q += 32) {
         const int r = q / RREC, cc = (q / MP) % 2, md = q % MP;
         const int mq = g * MP + md;
-        const int code = rofs[2 * (r0 + r) + cc];
+        const int code = (r0 + r < np) ? rofs[2 * (r0 + r) + cc] : -1;
         const bool ok = code >= 0 && mq < Nk;
         cp_async16(rdst + q, a.rhsP + (ok ? (size_t)(code >> 1) + mq : 0), ok);
       }
@@ -366,9 +374,18 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
     for (int u = 0; u < kFwdWin; ++u)
 #pragma unroll
       for (int v = 0; v < FV; ++v) rv[u][v] = st[u * (FREC / 2) + v];
+    // right-hand sides of the rows entering the window (stage s+1, zero-filled
+    // past the last row), -i applied to u_x momentum rows by the record's flag
     double incoming[kFwdWin];
+    {
+      const double* rb = ring + (size_t)((s + 1) % NS) * STAGE + R * FREC + (size_t)slot * 2;
 #pragma unroll
-    for (int u = 0; u < kFwdWin; ++u) incoming[u] = rhs_at(s + 1, u);
+      for (int u = 0; u < kFwdWin; ++u) {
+        const int rot = __double2loint(rv[u][FV - 1].y);
+        const double v = rb[u * RREC * 2 + (part ^ rot)];
+        incoming[u] = (rot & part) ? -v : v;
+      }
+    }
     double* ys = ysave + (size_t)(row0 + s * R) * NL + ln;
 #pragma unroll
     for (int u = 0; u < kFwdWin; ++u) {
@@ -398,16 +415,37 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   for (int t = 0; t < 4; ++t) myx[t] = y[t] - rhs_at(nst, t);
   cp_async_wait<0>();
   __syncwarp();
+  // The ring is free: stage the Schur inverse of the group and this warp's
+  // forward transfer data (Phi_k for k < warp, Gz_warp) while the other warps
+  // finish their sweeps.
+  constexpr int TRF = 32;  // Phi (16) + Gz (16) per (partition, record slot)
+  double* sSI = ring;                         // [class][4][4][mode], 2*16*MP doubles
+  double* sTR = ring + 2 * NBMAX * NBMAX * MP;  // [k-1][slot][TRF]
+  {
+    const double* SIg = a.cls[0].SI + (size_t)g * 2 * NBMAX * NBMAX * MP;
+    for (int q = lane; q < NBMAX * NBMAX * MP; q += 32) cp_async16(sSI + 2 * q, SIg + 2 * q, true);
+    if (P > 1 && warp > 0) {
+      for (int q = lane; q < warp * 2 * MP * (TRF / 2); q += 32) {
+        const int k = 1 + q / (2 * MP * (TRF / 2)), rs = (q / (TRF / 2)) % (2 * MP), h = q % (TRF / 2);
+        const double* rec = a.PP + (((size_t)g * P + k) * 2 * MP + rs) * kTransfer;
+        const double* src = (h < 8) ? rec + kTrPhi + 2 * h : rec + kTrGz + 2 * (h - 8);
+        cp_async16(sTR + ((size_t)(k - 1) * 2 * MP + rs) * TRF + 2 * h, src, true);
+      }
+    }
+    cp_async_commit();
+  }
 
   // ---- F2: true starting window of this partition, border accumulators ----
   double d[4] = {0.0, 0.0, 0.0, 0.0};  // starting-window correction (0 for warp 0)
   if constexpr (P > 1) {
     __syncthreads();
+    cp_async_wait<0>();
+    __syncwarp();
     if (warp > 0) {
 #pragma unroll
       for (int t = 0; t < 4; ++t) d[t] = xch[(size_t)ln * kXch + t];  // delta_1 = D_0
       for (int k = 1; k < warp; ++k) {
-        const double* phi = trg + k * TRK + kTrPhi;
+        const double* phi = sTR + ((size_t)(k - 1) * 2 * MP + slot) * TRF;
         const double* Dk = xch + ((size_t)k * NL + ln) * kXch;
         double nd[4];
 #pragma unroll
@@ -420,7 +458,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 #pragma unroll
         for (int o = 0; o < 4; ++o) d[o] = nd[o];
       }
-      const double* gz = trg + warp * TRK + kTrGz;
+      const double* gz = sTR + ((size_t)(warp - 1) * 2 * MP + slot) * TRF + 16;
 #pragma unroll
       for (int b = 0; b < NBMAX; ++b)
 #pragma unroll
@@ -435,12 +473,15 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
       for (int k = 0; k < P; ++k) acc += xch[((size_t)k * NL + ln) * kXch + 4 + b];
       z[b] = acc;
     }
+  } else {
+    cp_async_wait<0>();
+    __syncwarp();
   }
 
   // ---- border unknowns from the Schur complement ----
   double x1[NBMAX];
   {
-    const double* si = a.cls[0].SI + ((size_t)g * 2 + c) * NBMAX * NBMAX * MP + mm;
+    const double* si = sSI + (size_t)c * NBMAX * NBMAX * MP + mm;
 #pragma unroll
     for (int q = 0; q < NBMAX; ++q) {
       double acc = 0.0;
@@ -449,9 +490,10 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
       x1[q] = acc;
     }
   }
+  __syncwarp();  // the ring is reused by B1
 
   // ---- B1: backward sweep over this warp's rows, x = U^-1 (y - B x1), from a zero window ----
-  const bool last = (warp == P - 1);
+  // (the particular unknowns replace y in shared memory; B3 completes and stores them)
   double xw[kBwdWin];  // x_j lives in slot j % kBwdWin
 #pragma unroll
   for (int t = 0; t < kBwdWin; ++t) xw[t] = 0.0;
@@ -506,10 +548,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
           const double sacc = fma(-rec(1), xw[(kBwdWin - u) % kBwdWin], acc0 + (acc1 + acc2));
           const double xj = sacc * rec(0);
           xw[(kBwdWin - 1 - u) % kBwdWin] = xj;
-          if (last)
-            store_unknown(Xd, __double2loint(rec(kBwdCode)), m, part, xj, live);
-          else
-            *yx = xj;  // particular unknown, completed in B3
+          *yx = xj;
         }
       }
       __syncwarp();  // the slot of stage s is refilled next
@@ -518,19 +557,33 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   cp_async_wait<0>();
   __syncwarp();
 
+  // ---- B2: true incoming window T of this partition (zero for the last) ----
+  const bool last = (warp == P - 1);
+  double T[kBwdWin];
+#pragma unroll
+  for (int t = 0; t < kBwdWin; ++t) T[t] = 0.0;
   if constexpr (P > 1) {
-    // ---- B2: true incoming window of this partition ----
+    // stage Psi_k, k = warp+1 .. P-2, in the ring while the other warps finish B1
+    double* sPsi = ring;  // [k-warp-1][slot][144]
+    const int npsi = (P - 2 - warp) > 0 ? (P - 2 - warp) : 0;
+    for (int q = lane; q < npsi * 2 * MP * 72; q += 32) {
+      const int kk = q / (2 * MP * 72), rs = (q / 72) % (2 * MP), h = q % 72;
+      const double* rec = a.PP + (((size_t)g * P + warp + 1 + kk) * 2 * MP + rs) * kTransfer + kTrPsi;
+      cp_async16(sPsi + ((size_t)kk * 2 * MP + rs) * 144 + 2 * h, rec + 2 * h, true);
+    }
+    cp_async_commit();
     double* myxh = myx + 8;
 #pragma unroll
     for (int t = 0; t < kBwdWin; ++t) myxh[t] = xw[t];
     __syncthreads();
+    cp_async_wait<0>();
+    __syncwarp();
     if (!last) {
-      double T[kBwdWin];
       const double* Xl = xch + ((size_t)(P - 1) * NL + ln) * kXch + 8;
 #pragma unroll
       for (int t = 0; t < kBwdWin; ++t) T[t] = Xl[t];
       for (int k = P - 2; k > warp; --k) {
-        const double* psi = trg + k * TRK + kTrPsi;
+        const double* psi = sPsi + ((size_t)(k - warp - 1) * 2 * MP + slot) * 144;
         const double* Xk = xch + ((size_t)k * NL + ln) * kXch + 8;
         double nt[kBwdWin];
 #pragma unroll
@@ -543,39 +596,50 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 #pragma unroll
         for (int o = 0; o < kBwdWin; ++o) T[o] = nt[o];
       }
-      // ---- B3: x_j += H_j . T over the rows of this partition ----
-      auto issue_h = [&](int s) {
-        if (s < nst) {
-          double* dst = ring + (size_t)(s % NS) * STAGE;
-          const int lo = row0 + s * R;
-          for (int q = lane; q < R * HREC / 2; q += 32) cp_async16(dst + 2 * q, HRg + (size_t)lo * HREC + 2 * q, true);
-        }
-        cp_async_commit();
-      };
-      for (int s = 0; s < NS - 1; ++s) issue_h(s);
-      for (int s = 0; s < nst; ++s) {
-        issue_h(s + NS - 1);
-        cp_async_wait<NS - 1>();
-        __syncwarp();
-        const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NS) * STAGE + (size_t)slot * kHRec);
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-          double2 hv[HV];
-#pragma unroll
-          for (int v = 0; v < HV; ++v) hv[v] = st[u * (HREC / 2) + v];
-          const int j = row0 + s * R + u;
-          double acc0 = ysave[(size_t)j * NL + ln], acc1 = 0.0;
-#pragma unroll
-          for (int i = 0; i < kBwdWin; i += 2) {
-            acc0 = fma(hv[i / 2].x, T[i], acc0);
-            acc1 = fma(hv[i / 2].y, T[i + 1], acc1);
-          }
-          store_unknown(Xd, __double2loint(hv[HV - 1].x), m, part, acc0 + acc1, live);
-        }
-        __syncwarp();
-      }
-      cp_async_wait<0>();
     }
+    __syncwarp();  // the ring is reused by B3
+  }
+
+  // ---- B3: x_j = particular + H_j . T over the rows of this partition, stored to X ----
+  {
+    constexpr int NS3 = 6;            // H ring: NS3 slots of R rows
+    constexpr int SLOT3 = R * HREC;
+    static_assert(NS3 * SLOT3 <= NS * STAGE, "H ring fits the warp's ring");
+    static_assert(R % 2 == 0 && 32 == 2 * NL, "B3 splits the rows of a stage between the two lane halves");
+    const int half = lane / NL;
+    auto issue_h = [&](int s) {
+      if (s < nst) {
+        double* dst = ring + (size_t)(s % NS3) * SLOT3;
+        const int lo = row0 + s * R;
+        for (int q = lane; q < R * HREC / 2; q += 32) cp_async16(dst + 2 * q, HRg + (size_t)lo * HREC + 2 * q, true);
+      }
+      cp_async_commit();
+    };
+    for (int s = 0; s < NS3 - 1; ++s) issue_h(s);
+    for (int s = 0; s < nst; ++s) {
+      issue_h(s + NS3 - 1);
+      cp_async_wait<NS3 - 1>();
+      __syncwarp();
+      const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NS3) * SLOT3 + (size_t)slot * kHRec);
+      // no recurrence here: the two lane halves take alternate rows
+#pragma unroll
+      for (int q = 0; q < R / 2; ++q) {
+        const int u = 2 * q + half;
+        double2 hv[HV];
+#pragma unroll
+        for (int v = 0; v < HV; ++v) hv[v] = st[u * (HREC / 2) + v];
+        const int j = row0 + s * R + u;
+        double acc0 = ysave[(size_t)j * NL + ln], acc1 = 0.0;
+#pragma unroll
+        for (int i = 0; i < kBwdWin; i += 2) {
+          acc0 = fma(hv[i / 2].x, T[i], acc0);
+          acc1 = fma(hv[i / 2].y, T[i + 1], acc1);
+        }
+        store_unknown(Xd, __double2loint(hv[HV - 1].x), m, part, acc0 + acc1, m < Nk);
+      }
+      __syncwarp();
+    }
+    cp_async_wait<0>();
   }
   // border unknowns
   if (warp == 0) {
@@ -610,7 +674,8 @@ __global__ void __launch_bounds__(64) k_tau_transfer(TauArgs a) {
   const int np = a.npad, Lp = np / P;
   const int g = m / kSolveModes, mm = m % kSolveModes;
   for (int k = 0; k < P; ++k) {
-    double* tr = a.PP + ((((size_t)g * P + k) * 2 + c) * kSolveModes + mm) * kTransfer;
+    // Phi, Gz, Psi exist only for P > 1 (a.PP is null otherwise)
+    double* tr = P > 1 ? a.PP + ((((size_t)g * P + k) * 2 + c) * kSolveModes + mm) * kTransfer : nullptr;
     const int r0 = k * Lp, r1 = (k + 1) * Lp;
     if (k >= 1) {
       for (int i = 0; i < 4; ++i) {
@@ -637,7 +702,15 @@ __global__ void __launch_bounds__(64) k_tau_transfer(TauArgs a) {
         for (int b = 0; b < NBMAX; ++b) tr[kTrGz + b * 4 + i] = z[b];
       }
     }
-    if (k <= P - 2) {
+    if (k == P - 1) {
+      // the last partition's unknowns need no correction: zero H, store codes only
+      for (int j = r0; j < r1; ++j) {
+        double* hr = a.HR + ((((size_t)g * np + j) * 2 + c) * kSolveModes + mm) * kHRec;
+        for (int i = 0; i < kBwdWin; ++i) hr[i] = 0.0;
+        hr[kBwdWin] = bwd_record(a.cls[0].BR, np, m, j, c)[kBwdCode];
+        hr[kBwdWin + 1] = 0.0;
+      }
+    } else {
       for (int i = 0; i < kBwdWin; ++i) {
         double xw[kBwdWin];
         for (int t = 0; t < kBwdWin; ++t) xw[t] = (t == i) ? 1.0 : 0.0;
@@ -818,7 +891,10 @@ void factor_impl(const TauArgs& a, int parts, cudaStream_t st) {
   int nmax = a.cls[0].n > a.cls[1].n ? a.cls[0].n : a.cls[1].n;
   dim3 grid((a.Nk + 63) / 64, 2);
   k_tau_factor<KL, KU><<<grid, 64, 0, st>>>(a, nmax);
-  if (parts == kTauParts && kTauParts > 1) k_tau_transfer<KL, KU, kTauParts><<<grid, 64, 0, st>>>(a);
+  if (parts == kTauParts)
+    k_tau_transfer<KL, KU, kTauParts><<<grid, 64, 0, st>>>(a);
+  else
+    k_tau_transfer<KL, KU, 1><<<grid, 64, 0, st>>>(a);
 }
 
 template <int P>
@@ -869,7 +945,7 @@ size_t tau_transfer_doubles(int Nk, int parts) {
 }
 
 size_t tau_response_doubles(int Nk, int npad, int parts) {
-  if (parts <= 1) return 0;
+  (void)parts;
   const size_t groups = (size_t)(Nk + kSolveModes - 1) / kSolveModes;
   return groups * (size_t)npad * 2 * kSolveModes * kHRec;
 }
