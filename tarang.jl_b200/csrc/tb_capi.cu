@@ -133,7 +133,7 @@ struct tb_plan {
   DevBuf X, G, H, MX0, FP[4], LXP[4], Fprev, MXprev, Rsb, tmpgrid;
   DevView tau;
   // transform constants
-  DevBuf bwd, fwd, s3, twM, twN;
+  DevBuf bwd, fwd, s3, twM, twN, ptwM;
   // parity halves of the Chebyshev matrices (H = ceil(Nz/2) rows/cols)
   DevBuf bEv, bOv, bEd, bOd, fE, fO, sfE, sfO;
   int Hz = 0, Ke = 0, Ko = 0;  // Hz = ceil(Nz/2)
@@ -252,6 +252,24 @@ void collect_profile(tb_plan* P) {
 }
 
 inline int pad16k(int k) { return (k + 15) / 16 * 16; }
+
+// Per-pass twiddle tables of a Stockham plan: pass s (stride Ns, radix R)
+// contributes exp(-2 pi i j n/(Ns R) / n) for j < Ns, passes concatenated.
+std::vector<double2> pass_twiddles(const FftPlan& fp) {
+  std::vector<double2> t;
+  const long double pi = 3.141592653589793238462643383279502884L;
+  int Ns = 1;
+  for (int s = 0; s < fp.nstages; ++s) {
+    const int R = fp.radix[s];
+    const int tstride = fp.n / (Ns * R);
+    for (int j = 0; j < Ns; ++j) {
+      long double a = -2.0L * pi * (long double)(j * tstride) / (long double)fp.n;
+      t.push_back(make_double2((double)cosl(a), (double)sinl(a)));
+    }
+    Ns *= R;
+  }
+  return t;
+}
 
 std::vector<double2> twiddles(int n) {
   std::vector<double2> t(n);
@@ -378,7 +396,8 @@ void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
     xa.od[f] = gp(f, 3);
     xa.out[f] = P->H.as<double2>() + (size_t)f * P->plane;
   }
-  xa.tw = P->twM.as<double2>();
+  xa.ptw = P->ptwM.as<double2>();
+  xa.nptw = (int)(P->ptwM.bytes / sizeof(double2));
   xa.fp = P->fpM;
   xa.Nx = P->Nx;
   xa.Nk = P->Nk;
@@ -621,7 +640,8 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
     P->plane = (size_t)P->Nz * P->Nk;
     TB_REQUIRE(make_fft_plan(P->M, &P->fpM) && make_fft_plan(P->Nx, &P->fpN), TB_ENOTSUPPORTED,
                "Nx must be of the form 2^a 3^b");
-    TB_REQUIRE(xprod_smem_bytes(P->M, P->Nk) <= 227 * 1024, TB_ENOTSUPPORTED, "Nx too large for the fused x kernel");
+    TB_REQUIRE(xprod_smem_bytes(P->M, P->Nk, (int)pass_twiddles(P->fpM).size()) <= 227 * 1024, TB_ENOTSUPPORTED,
+               "Nx too large for the fused x kernel");
     TB_CUDA_TRY(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
     TB_CUDA_TRY(cudaEventCreate(&P->ev0));
     TB_CUDA_TRY(cudaEventCreate(&P->ev1));
@@ -662,6 +682,7 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
     upload(P->bwd, bwdp);
     upload(P->s3, cm.s3);
     upload(P->twM, twiddles(P->M));
+    upload(P->ptwM, pass_twiddles(P->fpM));
     upload(P->twN, twiddles(P->Nx));
     // tau layout
     P->lay = build_rbc_layout(P->Nz, desc->Lx, desc->Lz, desc->kappa, desc->nu, (double)desc->Nx,

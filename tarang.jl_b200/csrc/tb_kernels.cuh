@@ -29,13 +29,14 @@ struct XProdArgs {
   const double2* ed[3];
   const double2* od[3];
   double2* out[3];       // mixed-space products -(u.grad f) (Nz x Nk complex)
-  const double2* tw;     // exp(-2 pi i t / M), t < M
+  const double2* ptw;    // per-pass twiddle tables of the length-M plan (pass_twiddle_count entries)
+  int nptw;
   FftPlan fp;            // length M plan
   int Nx, Nk, M, Nz;
   double k0;             // 2 pi / Lx
 };
 void launch_xprod(const XProdArgs& a, cudaStream_t st);
-size_t xprod_smem_bytes(int M, int Nk);
+size_t xprod_smem_bytes(int M, int Nk, int nptw);
 // Raise the dynamic shared-memory limit of the transform kernels (once per plan).
 cudaError_t set_transform_smem_limits(int bytes);
 // Scratch (doubles) the factorisation needs for nmax band rows and Nk modes.

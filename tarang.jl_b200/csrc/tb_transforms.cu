@@ -49,7 +49,13 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
+// SPLITK = false: CTA tile 64 x 64, warp (wm, wn) owns rows wm*32.., cols wn*32..
+// SPLITK = true:  CTA tile 32 x 64 (twice the CTAs for short M), warp (wk, wn)
+//                 owns cols wn*32.. and the k-steps ks = 2 wk, 2 wk + 1 of every
+//                 16-deep slice; the two k halves are summed through shared memory.
+template <bool SPLITK>
 __global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ldb, int ldc, int Nrows) {
+  constexpr int TM = SPLITK ? GBM / 2 : GBM;  // CTA tile rows
   extern __shared__ __align__(16) double gsm[];
   double (*As)[GBM * ASTR] = reinterpret_cast<double (*)[GBM * ASTR]>(gsm);
   double (*Bs)[GBK * BSTR] = reinterpret_cast<double (*)[GBK * BSTR]>(gsm + 2 * GBM * ASTR);
@@ -58,19 +64,19 @@ __global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ld
   const double* __restrict__ A = it.A;
   const double* __restrict__ B = it.B;
   const int Mo = it.M, K = it.K, Kp = it.Kpad, mode = it.mode, par = it.par;
-  const int row0 = blockIdx.y * GBM, col0 = blockIdx.x * GBN;
+  const int row0 = blockIdx.y * TM, col0 = blockIdx.x * GBN;
   if (row0 >= Mo) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 1, wn = warp & 1;
+  const int wm = SPLITK ? 0 : (warp >> 1), wk = SPLITK ? (warp >> 1) : 0, wn = warp & 1;
   const int gid = lane >> 2, tig = lane & 3;
   const bool mirror = mode == GEMM_MIRROR;
   const int ntiles = (K + GBK - 1) / GBK;
 
   auto load_tile = [&](int t, int buf) {
     const int k0 = t * GBK;
-    // A: 64 rows x 16 doubles = 512 chunks of 16 B, 4 per thread
+    // A: TM rows x 16 doubles = TM*8 chunks of 16 B
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < TM * 8 / GTH; ++q) {
       const int ch = tid + q * GTH;
       const int r = ch >> 3, kc = (ch & 7) * 2;
       const int gr = row0 + r;
@@ -118,7 +124,8 @@ __global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ld
     const double* bs = Bs[buf];
     const double* bm = Bm[buf];
 #pragma unroll
-    for (int ks = 0; ks < GBK / 4; ++ks) {
+    for (int kq = 0; kq < (SPLITK ? GBK / 8 : GBK / 4); ++kq) {
+      const int ks = SPLITK ? 2 * wk + kq : kq;
       const int kk = ks * 4 + tig;
       double a[4], b[4];
 #pragma unroll
@@ -141,6 +148,28 @@ __global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ld
     __syncthreads();
   }
   g_wait0();
+  if constexpr (SPLITK) {
+    // the upper k half hands its partial tile to the lower half (buffers are free)
+    double* red = gsm + (size_t)wn * 32 * 32;
+    if (wk == 1) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          red[((i * 4 + j) * 2 + 0) * 32 + lane] = acc[i][j][0];
+          red[((i * 4 + j) * 2 + 1) * 32 + lane] = acc[i][j][1];
+        }
+    }
+    __syncthreads();
+    if (wk == 1) return;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        acc[i][j][0] += red[((i * 4 + j) * 2 + 0) * 32 + lane];
+        acc[i][j][1] += red[((i * 4 + j) * 2 + 1) * 32 + lane];
+      }
+  }
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int gr = row0 + wm * 32 + i * 8 + gid;
@@ -163,8 +192,16 @@ __global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ld
 void launch_gemm_f64(const GemmBatch& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, cudaStream_t st) {
   int mmax = 0;
   for (int b = 0; b < nbatch; ++b) mmax = bt.item[b].M > mmax ? bt.item[b].M : mmax;
-  dim3 grid((ncol + GBN - 1) / GBN, (mmax + GBM - 1) / GBM, nbatch);
-  k_gemm_f64<<<grid, GTH, kGemmSmem, st>>>(bt, ncol, ldb, ldc, Nrows);
+  const int ncx = (ncol + GBN - 1) / GBN;
+  const long long ctas = (long long)ncx * ((mmax + GBM - 1) / GBM) * nbatch;
+  if (ctas < 2LL * 148) {
+    // too few 64-row tiles to fill the SMs: halve the tile rows and split K inside the CTA
+    dim3 grid(ncx, (mmax + GBM / 2 - 1) / (GBM / 2), nbatch);
+    k_gemm_f64<true><<<grid, GTH, kGemmSmem, st>>>(bt, ncol, ldb, ldc, Nrows);
+  } else {
+    dim3 grid(ncx, (mmax + GBM - 1) / GBM, nbatch);
+    k_gemm_f64<false><<<grid, GTH, kGemmSmem, st>>>(bt, ncol, ldb, ldc, Nrows);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -319,6 +356,77 @@ __device__ double2* fft_cta(double2* a, double2* b, const FftPlan& fp, const dou
   return in;
 }
 
+// Stockham pass as fft_pass, with the twiddles of this pass from its own table
+// pt[j] = exp(-2 pi i j tstride / n), j < Ns (consecutive threads read
+// consecutive entries: no bank conflicts); w^r for r > 1 by products of w.
+template <int R, bool SW>
+__device__ __forceinline__ void fft_pass_pt(const double2* __restrict__ in, double2* __restrict__ out, int n, int Ns,
+                                            const double2* __restrict__ pt, int sign) {
+  const int nR = n / R;
+  for (int idx = threadIdx.x; idx < nR; idx += blockDim.x) {
+    const int j = idx % Ns, k = idx / Ns;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = in[fidx<SW>(idx + r * nR)];
+    if (Ns > 1) {
+      double2 w1 = pt[j];
+      if (sign > 0) w1.y = -w1.y;
+      if constexpr (R == 8) {
+        const double2 w2 = cmul(w1, w1), w4 = cmul(w2, w2), w3 = cmul(w1, w2);
+        v[1] = cmul(v[1], w1);
+        v[2] = cmul(v[2], w2);
+        v[3] = cmul(v[3], w3);
+        v[4] = cmul(v[4], w4);
+        v[5] = cmul(v[5], cmul(w1, w4));
+        v[6] = cmul(v[6], cmul(w2, w4));
+        v[7] = cmul(v[7], cmul(w3, w4));
+      } else if constexpr (R == 4) {
+        const double2 w2 = cmul(w1, w1);
+        v[1] = cmul(v[1], w1);
+        v[2] = cmul(v[2], w2);
+        v[3] = cmul(v[3], cmul(w1, w2));
+      } else if constexpr (R == 3) {
+        v[1] = cmul(v[1], w1);
+        v[2] = cmul(v[2], cmul(w1, w1));
+      } else {
+        v[1] = cmul(v[1], w1);
+      }
+    }
+    dft_small<R>(v, sign);
+    const int ob = k * Ns * R + j;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out[fidx<SW>(ob + r * Ns)] = v[r];
+  }
+}
+
+// fft_cta with per-pass twiddle tables: pass s reads pt + (sum of Ns of the
+// passes before it), the layout written by pass_twiddles() on the host.
+template <bool SW>
+__device__ double2* fft_cta_pt(double2* a, double2* b, const FftPlan& fp, const double2* __restrict__ pt, int sign) {
+  const int n = fp.n;
+  int Ns = 1;
+  double2* in = a;
+  double2* out = b;
+  for (int s = 0; s < fp.nstages; ++s) {
+    const int R = fp.radix[s];
+    if (R == 8)
+      fft_pass_pt<8, SW>(in, out, n, Ns, pt, sign);
+    else if (R == 4)
+      fft_pass_pt<4, SW>(in, out, n, Ns, pt, sign);
+    else if (R == 2)
+      fft_pass_pt<2, SW>(in, out, n, Ns, pt, sign);
+    else
+      fft_pass_pt<3, SW>(in, out, n, Ns, pt, sign);
+    __syncthreads();
+    double2* t = in;
+    in = out;
+    out = t;
+    pt += Ns;
+    Ns *= R;
+  }
+  return in;
+}
+
 // Half-spectrum entry H_k of a row whose unnormalised rfft bins are g (length
 // Nk = N/2+1), as an operand of the padded product: DC and Nyquist are real
 // (irfft ignores their imaginary parts) and the Nyquist bin is split in half.
@@ -353,9 +461,9 @@ __global__ void __launch_bounds__(256, 2) k_xprod(XProdArgs a) {
   double2* S1 = sm + Ms;
   double2* S2 = sm + 2 * Ms;
   double2* S3 = sm + 3 * Ms;
-  double2* tw = sm + 4 * Ms;  // exp(-2 pi i t / M), t < M/2
-  const int half = M / 2, hN = N / 2;
-  for (int t = threadIdx.x; t < half; t += blockDim.x) tw[t] = a.tw[t];
+  double2* tw = sm + 4 * Ms;  // per-pass twiddle tables of the length-M plan
+  const int hN = N / 2;
+  for (int t = threadIdx.x; t < a.nptw; t += blockDim.x) tw[t] = a.ptw[t];
   // Grid row z from the even/odd Chebyshev half planes: rows z < H are E + O,
   // mirrored rows N-1-z are E - O for values and -E + O for z-derivatives.
   const int z = blockIdx.x;
@@ -388,7 +496,7 @@ __global__ void __launch_bounds__(256, 2) k_xprod(XProdArgs a) {
   for (int q = threadIdx.x; q <= hN; q += blockDim.x) put2(S0, q, hbin(value(1, q), q), hbin(value(2, q), q));
   zero_gap(S0);
   __syncthreads();
-  double2* U = fft_cta<true>(S0, S1, a.fp, tw, +1);
+  double2* U = fft_cta_pt<true>(S0, S1, a.fp, tw, +1);
   double2* P = (U == S0) ? S1 : S0;  // prod_b + i prod_ux
   double2* Q = nullptr;              // prod_uz (real parts)
   // 2. gradients of each field and the advection products
@@ -404,7 +512,7 @@ __global__ void __launch_bounds__(256, 2) k_xprod(XProdArgs a) {
     }
     zero_gap(S2);
     __syncthreads();
-    double2* G = fft_cta<true>(S2, S3, a.fp, tw, +1);
+    double2* G = fft_cta_pt<true>(S2, S3, a.fp, tw, +1);
     double2* Gf = (G == S2) ? S3 : S2;  // the pass buffer left free
     for (int p = threadIdx.x; p < M; p += blockDim.x) {
       const int ps = fidx<true>(p);
@@ -422,10 +530,10 @@ __global__ void __launch_bounds__(256, 2) k_xprod(XProdArgs a) {
       // the gradient buffer G is free from here on
       __syncthreads();
       // 3a. forward transform of prod_b + i prod_ux into G's buffer pair
-      double2* C1 = fft_cta<true>(P, G, a.fp, tw, -1);
+      double2* C1 = fft_cta_pt<true>(P, G, a.fp, tw, -1);
       // 3b. forward transform of prod_uz, ping-ponging with U's buffer (free now);
       // it touches neither C1 nor P's partner, so both proceed before one barrier
-      double2* C2 = fft_cta<true>(Q, U, a.fp, tw, -1);
+      double2* C2 = fft_cta_pt<true>(Q, U, a.fp, tw, -1);
       const double sc = 1.0 / ((double)M * (double)N);
       const size_t ro = (size_t)z * Nk;
       for (int k = threadIdx.x; k < Nk; k += blockDim.x) {
@@ -568,7 +676,11 @@ __global__ void __launch_bounds__(256) k_x_dealias_mul(const double* __restrict_
 
 cudaError_t set_transform_smem_limits(int bytes) {
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem)) != cudaSuccess)
+  if ((e = cudaFuncSetAttribute(k_gemm_f64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem)) !=
+      cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(k_gemm_f64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem)) !=
+      cudaSuccess)
     return e;
   if ((e = cudaFuncSetAttribute(k_xprod, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_x_rfft, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
@@ -576,14 +688,14 @@ cudaError_t set_transform_smem_limits(int bytes) {
   return cudaFuncSetAttribute(k_x_dealias_mul, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-size_t xprod_smem_bytes(int M, int Nk) {
+size_t xprod_smem_bytes(int M, int Nk, int nptw) {
   (void)Nk;
   const size_t Ms = (size_t)((M + 7) & ~7);
-  return (4 * Ms + (size_t)(M / 2)) * sizeof(double2);
+  return (4 * Ms + (size_t)nptw) * sizeof(double2);
 }
 
 void launch_xprod(const XProdArgs& a, cudaStream_t st) {
-  size_t smem = xprod_smem_bytes(a.M, a.Nk);
+  size_t smem = xprod_smem_bytes(a.M, a.Nk, a.nptw);
   k_xprod<<<a.Nz, 256, smem, st>>>(a);
 }
 
