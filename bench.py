@@ -182,10 +182,12 @@ def kernel_work(name: str, cfg, scheme: str):
         # reads 12 half planes (values, z-derivatives; even/odd) and writes 3 planes
         return "bytes", 9.0 * plane
     if name == "tau_solve":
-        # streamed factor records (forward 9 + backward 18 doubles per row, class, mode,
-        # rows padded to a multiple of 12) + Schur inverses; rhs read (4 planes);
-        # unknowns written (4 planes + taus)
-        npad = (n + 11) // 12 * 12
+        # the banded LU factors themselves (forward 9 + backward 18 doubles per band row,
+        # class and mode: pivot, 4 multipliers, 4 border multipliers; 1/diag, 12 U
+        # entries, 4 border entries, store target; rows padded to a multiple of 48)
+        # + Schur inverses; rhs read (4 planes); unknowns written (4 planes + taus).
+        # The partitioned solve's extra response records are not algorithmic bytes.
+        npad = (n + 47) // 48 * 48
         groups = (nk + 3) // 4
         fac = groups * 4 * (npad * 2 * (9 + 18) * 8 + 2 * 16 * 8)
         return "bytes", fac + 4.0 * plane + 4.0 * plane + 7 * nk * 16
