@@ -182,6 +182,39 @@ tb_status tb_batched_lu_factor(tb_context* ctx, int n, int batch, double* A, int
 tb_status tb_batched_lu_solve(tb_context* ctx, int n, int batch, const double* A, const int* piv,
                               double* B /* n x batch complex, overwritten by X */);
 
+/* -------------------------------------------------------------------------
+ * Asynchronous stepping.  The reference's step!/run! (solver_stepping.jl:24-38,
+ * 115-205) return when the step is done; these calls let a caller (or the
+ * ensemble runner and the request server below) keep several plans in flight.
+ * tb_step_async enqueues nsteps steps on the plan's stream, as CUDA graphs of
+ * up to graph_steps steps each, and returns; tb_plan_query reports whether the
+ * plan's stream is idle, tb_plan_wait waits for it.  tb_plan_device_bytes:
+ * device memory the plan holds (state, work arrays, constants, factors).
+ * ---------------------------------------------------------------------- */
+tb_status tb_step_async(tb_plan* plan, double dt, int nsteps, int graph_steps);
+tb_status tb_plan_query(tb_plan* plan, int* idle);
+tb_status tb_plan_wait(tb_plan* plan);
+tb_status tb_plan_device_bytes(const tb_plan* plan, size_t* bytes);
+
+/* -------------------------------------------------------------------------
+ * Ensembles: many independent plans (uneven sizes, own parameters and dt)
+ * stepped together.  Counterpart of the reference's batched ensemble path
+ * (mode_batch.jl:23-668, step_subproblem_rk_batched.jl:838-1006), which steps
+ * instances in turn.  Members are borrowed plans of one context; a run steps
+ * every member nsteps at its own dt (dt[i]), spreading the members' step graphs
+ * over worker streams.  tb_ensemble_tune times candidate (streams, steps per
+ * graph) settings on the members from a snapshot of their state, restores the
+ * state and keeps the fastest setting.  member_ms[i]: time from the run's start
+ * until member i finished (device clock); total_ms: the run.
+ * ---------------------------------------------------------------------- */
+typedef struct tb_ensemble tb_ensemble;
+tb_status tb_ensemble_create(tb_context* ctx, int n, tb_plan* const* members, tb_ensemble** out);
+tb_status tb_ensemble_destroy(tb_ensemble* ens);
+tb_status tb_ensemble_tune(tb_ensemble* ens, const double* dt, int trial_steps, int* streams, int* graph_steps);
+tb_status tb_ensemble_set_config(tb_ensemble* ens, int streams, int graph_steps);
+tb_status tb_ensemble_config(const tb_ensemble* ens, int* streams, int* graph_steps);
+tb_status tb_ensemble_run(tb_ensemble* ens, const double* dt, int nsteps, float* member_ms, float* total_ms);
+
 #ifdef __cplusplus
 }
 #endif

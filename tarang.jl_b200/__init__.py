@@ -18,6 +18,7 @@ from .api import (  # noqa: F401
     ChannelDomain,
     ChebyshevT,
     Domain,
+    Ensemble,
     InitialValueSolver,
     Plan,
     RealFourier,

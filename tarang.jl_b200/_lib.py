@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import POINTER, Structure, c_char_p, c_double, c_float, c_int, c_longlong, c_void_p
+from ctypes import POINTER, Structure, c_char_p, c_double, c_float, c_int, c_longlong, c_size_t, c_void_p
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtarang_b200.so")
@@ -77,6 +77,16 @@ SIGNATURES = {
     "tb_rhs_advection": (c_int, [c_void_p, c_void_p, c_void_p]),
     "tb_batched_lu_factor": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, POINTER(c_int)]),
     "tb_batched_lu_solve": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "tb_step_async": (c_int, [c_void_p, c_double, c_int, c_int]),
+    "tb_plan_query": (c_int, [c_void_p, POINTER(c_int)]),
+    "tb_plan_wait": (c_int, [c_void_p]),
+    "tb_plan_device_bytes": (c_int, [c_void_p, POINTER(c_size_t)]),
+    "tb_ensemble_create": (c_int, [c_void_p, c_int, c_void_p, POINTER(c_void_p)]),
+    "tb_ensemble_destroy": (c_int, [c_void_p]),
+    "tb_ensemble_tune": (c_int, [c_void_p, c_void_p, c_int, POINTER(c_int), POINTER(c_int)]),
+    "tb_ensemble_set_config": (c_int, [c_void_p, c_int, c_int]),
+    "tb_ensemble_config": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
+    "tb_ensemble_run": (c_int, [c_void_p, c_void_p, c_int, c_void_p, POINTER(c_float)]),
 }
 
 

@@ -20,7 +20,7 @@ from __future__ import annotations
 import ctypes
 import math
 import re
-from ctypes import byref, c_double, c_float, c_int, c_longlong, c_void_p
+from ctypes import byref, c_double, c_float, c_int, c_longlong, c_size_t, c_void_p
 from typing import Dict, List, Optional, Sequence
 
 import numpy as np
@@ -160,6 +160,28 @@ class Plan:
     def step(self, dt: float, nsteps: int = 1) -> None:
         check(lib.tb_step(self.ptr, float(dt), int(nsteps)), self.ctx)
 
+    def sim_time(self) -> float:
+        t, it = c_double(), c_longlong()
+        check(lib.tb_sim_time(self.ptr, byref(t), byref(it)), self.ctx)
+        return t.value
+
+    # asynchronous stepping (several plans in flight)
+    def step_async(self, dt: float, nsteps: int = 1, graph_steps: int = 1) -> None:
+        check(lib.tb_step_async(self.ptr, float(dt), int(nsteps), int(graph_steps)), self.ctx)
+
+    def idle(self) -> bool:
+        v = c_int()
+        check(lib.tb_plan_query(self.ptr, byref(v)), self.ctx)
+        return bool(v.value)
+
+    def wait(self) -> None:
+        check(lib.tb_plan_wait(self.ptr), self.ctx)
+
+    def device_bytes(self) -> int:
+        v = c_size_t()
+        check(lib.tb_plan_device_bytes(self.ptr, byref(v)), self.ctx)
+        return int(v.value)
+
     def last_step_ms(self) -> float:
         ms = c_float()
         check(lib.tb_last_step_ms(self.ptr, byref(ms)), self.ctx)
@@ -231,6 +253,60 @@ class Plan:
 # ---------------------------------------------------------------------------
 # Fields
 # ---------------------------------------------------------------------------
+
+
+class Ensemble:
+    """Independent plans (uneven sizes, own parameters and dt) stepped together.
+
+    Counterpart of the reference's batched ensemble path
+    (src/core/timesteppers/mode_batch.jl:23-668): ``run`` steps every member
+    ``nsteps`` at its own dt and returns the per-member completion times (ms
+    from the run's start, device clock) and the run's total; ``tune`` picks the
+    worker-stream count and steps per graph by timing them on the members
+    (their state is restored afterwards).
+    """
+
+    def __init__(self, plans: Sequence[Plan]):
+        if not plans:
+            raise ValueError("empty ensemble")
+        self.plans = list(plans)
+        self.ctx = self.plans[0].ctx
+        arr = (c_void_p * len(self.plans))(*[p.ptr.value for p in self.plans])
+        self.ptr = c_void_p()
+        check(lib.tb_ensemble_create(self.ctx, len(self.plans), arr, byref(self.ptr)), self.ctx)
+
+    def __del__(self):
+        ptr = getattr(self, "ptr", None)
+        if ptr:
+            lib.tb_ensemble_destroy(ptr)
+            self.ptr = None
+
+    def _dts(self, dt) -> np.ndarray:
+        d = np.broadcast_to(np.asarray(dt, dtype=np.float64), (len(self.plans),))
+        return np.ascontiguousarray(d)
+
+    def tune(self, dt, trial_steps: int = 8):
+        d = self._dts(dt)
+        s, g = c_int(), c_int()
+        check(lib.tb_ensemble_tune(self.ptr, d.ctypes.data_as(c_void_p), int(trial_steps), byref(s), byref(g)),
+              self.ctx)
+        return s.value, g.value
+
+    def set_config(self, streams: int, graph_steps: int) -> None:
+        check(lib.tb_ensemble_set_config(self.ptr, int(streams), int(graph_steps)), self.ctx)
+
+    def config(self):
+        s, g = c_int(), c_int()
+        check(lib.tb_ensemble_config(self.ptr, byref(s), byref(g)), self.ctx)
+        return s.value, g.value
+
+    def run(self, dt, nsteps: int):
+        d = self._dts(dt)
+        ms = np.zeros(len(self.plans), dtype=np.float32)
+        tot = c_float()
+        check(lib.tb_ensemble_run(self.ptr, d.ctypes.data_as(c_void_p), int(nsteps), ms.ctypes.data_as(c_void_p),
+                                  byref(tot)), self.ctx)
+        return ms, tot.value
 
 
 class ScalarField:

@@ -14,69 +14,11 @@
 
 #include "tb_internal.h"
 #include "tb_kernels.cuh"
+#include "tb_plan.h"
 
 using namespace tb;
 
-namespace {
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  DevBuf() = default;
-  DevBuf(const DevBuf&) = delete;
-  DevBuf& operator=(const DevBuf&) = delete;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
-  void alloc(size_t b) {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = b;
-    if (b == 0) return;
-    cudaError_t e = cudaMalloc(&p, b);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      throw Error{TB_ENOMEM, std::string("cudaMalloc(") + std::to_string(b) + "): " + cudaGetErrorString(e)};
-    }
-  }
-  template <class T>
-  T* as() const {
-    return static_cast<T*>(p);
-  }
-};
-
-// Non-owning window into a DevBuf.
-struct DevView {
-  void* p = nullptr;
-  size_t bytes = 0;
-  template <class T>
-  T* as() const {
-    return static_cast<T*>(p);
-  }
-};
-
-template <class T>
-void upload(DevBuf& d, const std::vector<T>& h) {
-  d.alloc(h.size() * sizeof(T));
-  if (!h.empty()) TB_CUDA_TRY(cudaMemcpy(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
-}
-
-struct ClassTables {
-  DevBuf row_eq, row_k, col_unk, col_k, left_unk, left_k, bc_rhs, band, bord, c2_z, c2_nz, c1_z, c1_nz;
-};
-
-struct FactorSet {
-  double alpha = 0, beta = 0;
-  DevBuf FR, BR, SI;  // solve-layout factor records (see tb_kernels.cuh)
-  DevBuf PP;          // partition transfer matrices of the solve
-  DevBuf HR;          // per-row backward responses of the partitioned solve
-};
-
-struct Tableau {
-  int s;
-  double AE[4][4], AI[4][4], bE[4], bI[4];
-};
-
+namespace tb {
 Tableau tableau(int ts) {
   Tableau t{};
   if (ts == TB_RK222) {
@@ -116,66 +58,8 @@ Tableau tableau(int ts) {
   return t;
 }
 
-}  // namespace
+}  // namespace tb
 
-struct tb_plan {
-  tb_context* ctx = nullptr;
-  tb_problem_desc d{};
-  int Nx = 0, Nz = 0, Nk = 0, M = 0;
-  double k0 = 0, s = 0;
-  cudaStream_t st = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  float last_ms = 0.f;
-  size_t plane = 0;  // Nz * Nk complex entries
-  // state and work arrays
-  // X holds the 4 state planes followed by the 7 tau rows (tau views its tail),
-  // so one 32-bit element offset from X addresses every unknown of the solve
-  DevBuf X, G, H, MX0, FP[4], LXP[4], Fprev, MXprev, Rsb, tmpgrid;
-  DevView tau;
-  // transform constants
-  DevBuf bwd, fwd, s3, twM, twN, ptwM;
-  // parity halves of the Chebyshev matrices (H = ceil(Nz/2) rows/cols)
-  DevBuf bEv, bOv, bEd, bOd, fE, fO, sfE, sfO;
-  int Hz = 0, Ke = 0, Ko = 0;  // Hz = ceil(Nz/2)
-  FftPlan fpM{}, fpN{};
-  // tau layout
-  TauLayout lay;
-  ClassTables ct[2];
-  std::vector<std::unique_ptr<FactorSet>> factors;
-  DevBuf err_mode, rhs_off;
-  // stepping state
-  double sim_time = 0.0;
-  long long iteration = 0;
-  int ms_history = 0;  // SBDF: number of stored history levels
-  double graph_dt = -1.0;
-  int graph_kind = -1;
-  cudaGraphExec_t gexec = nullptr;
-  int kernels_per_step = 0;
-  int tau_parts = 1;  // partitions of the tau solve (kTauParts or 1)
-  // profiling: eager launches bracketed by events, accumulated per kernel name
-  bool profiling = false;
-  struct ProfRec {
-    std::string name;
-    cudaEvent_t a, b;
-  };
-  std::vector<ProfRec> pending;
-  std::vector<cudaEvent_t> event_pool;
-  std::map<std::string, std::pair<double, long long>> prof;  // name -> (ms, launches)
-
-  ~tb_plan() {
-    for (auto e : event_pool) cudaEventDestroy(e);
-    for (auto& r : pending) {
-      cudaEventDestroy(r.a);
-      cudaEventDestroy(r.b);
-    }
-    if (gexec) cudaGraphExecDestroy(gexec);
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
-    if (st) cudaStreamDestroy(st);
-  }
-
-  double2* Xp(int f) const { return X.as<double2>() + (size_t)f * plane; }
-};
 
 namespace {
 
@@ -192,6 +76,12 @@ tb_status fail(tb_context* ctx, const Error& e) {
   g_err = e.msg;
   return e.code;
 }
+
+}  // namespace
+
+void tb::record_error(tb_context* ctx, const Error& e) { fail(ctx, e); }
+
+namespace {
 
 template <class F>
 tb_status guard(tb_context* ctx, F&& fn) {
@@ -531,27 +421,150 @@ void drop_graph(tb_plan* P) {
 }
 
 // Capture one step of `kind` (0 = RK, 1 = SBDF1, 2 = SBDF2) for dt.
-void capture_step(tb_plan* P, double dt, int kind) {
-  drop_graph(P);
+// Captures `steps` consecutive steps of one kind (the plan's stream must be idle).
+cudaGraphExec_t capture_steps(tb_plan* P, double dt, int kind, int steps) {
   cudaGraph_t g = nullptr;
   TB_CUDA_TRY(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeThreadLocal));
   try {
-    if (kind == 0)
-      enqueue_rk_step(P, dt);
-    else
-      enqueue_sbdf_step(P, dt, kind);
+    for (int i = 0; i < steps; ++i) {
+      if (kind == 0)
+        enqueue_rk_step(P, dt);
+      else
+        enqueue_sbdf_step(P, dt, kind);
+    }
   } catch (...) {
     cudaStreamEndCapture(P->st, &g);
     if (g) cudaGraphDestroy(g);
     throw;
   }
   TB_CUDA_TRY(cudaStreamEndCapture(P->st, &g));
-  cudaError_t e = cudaGraphInstantiate(&P->gexec, g, 0);
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) throw Error{TB_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+  return exec;
+}
+
+void capture_step(tb_plan* P, double dt, int kind) {
+  drop_graph(P);
+  P->gexec = capture_steps(P, dt, kind, 1);
   P->graph_dt = dt;
   P->graph_kind = kind;
 }
+
+// Factors for the next step of the given kind (built once per dt).
+void prepare_kind(tb_plan* P, double dt, int kind) {
+  if (kind == 0) {
+    const Tableau T = tableau(P->d.timestepper);
+    get_factors(P, 1.0, dt * T.AI[1][1]);
+  } else {
+    get_factors(P, sbdf_coefs(kind, dt).a0, 1.0);
+  }
+}
+
+void advance_counters(tb_plan* P, double dt, int kind, int steps) {
+  P->sim_time += dt * steps;
+  P->iteration += steps;
+  if (kind != 0) P->ms_history = 1;
+}
+
+}  // namespace
+
+int tb::plan_next_kind(const tb_plan* P) {
+  const int ts = P->d.timestepper;
+  if (ts == TB_SBDF1) return 1;
+  if (ts == TB_SBDF2) return (P->ms_history >= 1) ? 2 : 1;
+  return 0;
+}
+
+void tb::plan_launch_steps(tb_plan* P, double dt, int nsteps, cudaStream_t s, int graph_steps) {
+  if (!s) s = P->st;
+  if (graph_steps < 1) graph_steps = 1;
+  int left = nsteps;
+  while (left > 0) {
+    const int kind = plan_next_kind(P);
+    // SBDF2's first step is SBDF1 and stands alone; every other step repeats
+    const bool uniform = !(P->d.timestepper == TB_SBDF2 && kind == 1);
+    const int chunk = uniform ? std::min(left, graph_steps) : 1;
+    prepare_kind(P, dt, kind);
+    if (P->profiling) {
+      if (s != P->st) throw Error{TB_EINVAL, "profiled steps run on the plan's own stream"};
+      for (int i = 0; i < chunk; ++i) {
+        if (kind == 0)
+          enqueue_rk_step(P, dt);
+        else
+          enqueue_sbdf_step(P, dt, kind);
+      }
+      check_launch("profiled step");
+    } else if (chunk == 1) {
+      if (!(P->gexec && P->graph_dt == dt && P->graph_kind == kind)) {
+        TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+        capture_step(P, dt, kind);
+      }
+      TB_CUDA_TRY(cudaGraphLaunch(P->gexec, s));
+    } else {
+      StepGraph& mg = P->multi;
+      if (!(mg.exec && mg.dt == dt && mg.kind == kind && mg.steps == chunk)) {
+        if (mg.exec) cudaGraphExecDestroy(mg.exec);
+        mg.exec = nullptr;
+        TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+        mg.exec = capture_steps(P, dt, kind, chunk);
+        mg.dt = dt;
+        mg.kind = kind;
+        mg.steps = chunk;
+      }
+      TB_CUDA_TRY(cudaGraphLaunch(mg.exec, s));
+    }
+    advance_counters(P, dt, kind, chunk);
+    left -= chunk;
+  }
+}
+
+size_t tb::plan_device_bytes(const tb_plan* P) {
+  size_t b = 0;
+  const DevBuf* bufs[] = {&P->X,   &P->G,   &P->H,    &P->MX0,  &P->Fprev, &P->MXprev, &P->Rsb, &P->tmpgrid,
+                          &P->bwd, &P->fwd, &P->s3,   &P->twM,  &P->twN,   &P->ptwM,   &P->bEv, &P->bOv,
+                          &P->bEd, &P->bOd, &P->fE,   &P->fO,   &P->sfE,   &P->sfO,    &P->err_mode, &P->rhs_off};
+  for (const DevBuf* d : bufs) b += d->bytes;
+  for (int i = 0; i < 4; ++i) b += P->FP[i].bytes + P->LXP[i].bytes;
+  for (int c = 0; c < 2; ++c) {
+    const ClassTables& t = P->ct[c];
+    const DevBuf* tb_[] = {&t.row_eq, &t.row_k, &t.col_unk, &t.col_k, &t.left_unk, &t.left_k, &t.bc_rhs,
+                           &t.band,   &t.bord,  &t.c2_z,    &t.c2_nz, &t.c1_z,     &t.c1_nz};
+    for (const DevBuf* d : tb_) b += d->bytes;
+  }
+  for (const auto& f : P->factors) b += f->FR.bytes + f->BR.bytes + f->SI.bytes + f->PP.bytes + f->HR.bytes;
+  return b;
+}
+
+void tb::plan_snapshot(tb_plan* P, PlanSnapshot* snap) {
+  snap->X.alloc(P->X.bytes);
+  TB_CUDA_TRY(cudaMemcpyAsync(snap->X.p, P->X.p, P->X.bytes, cudaMemcpyDeviceToDevice, P->st));
+  if (P->Fprev.bytes) {
+    snap->Fprev.alloc(P->Fprev.bytes);
+    snap->MXprev.alloc(P->MXprev.bytes);
+    TB_CUDA_TRY(cudaMemcpyAsync(snap->Fprev.p, P->Fprev.p, P->Fprev.bytes, cudaMemcpyDeviceToDevice, P->st));
+    TB_CUDA_TRY(cudaMemcpyAsync(snap->MXprev.p, P->MXprev.p, P->MXprev.bytes, cudaMemcpyDeviceToDevice, P->st));
+  }
+  snap->sim_time = P->sim_time;
+  snap->iteration = P->iteration;
+  snap->ms_history = P->ms_history;
+  TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+}
+
+void tb::plan_restore(tb_plan* P, const PlanSnapshot& snap) {
+  TB_CUDA_TRY(cudaMemcpyAsync(P->X.p, snap.X.p, P->X.bytes, cudaMemcpyDeviceToDevice, P->st));
+  if (snap.Fprev.bytes) {
+    TB_CUDA_TRY(cudaMemcpyAsync(P->Fprev.p, snap.Fprev.p, P->Fprev.bytes, cudaMemcpyDeviceToDevice, P->st));
+    TB_CUDA_TRY(cudaMemcpyAsync(P->MXprev.p, snap.MXprev.p, P->MXprev.bytes, cudaMemcpyDeviceToDevice, P->st));
+  }
+  P->sim_time = snap.sim_time;
+  P->iteration = snap.iteration;
+  P->ms_history = snap.ms_history;
+  TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+}
+
+namespace {
 
 void validate_desc(const tb_problem_desc* d) {
   TB_REQUIRE(d != nullptr, TB_EINVAL, "null problem descriptor");
@@ -815,38 +828,56 @@ tb_status tb_step(tb_plan* P, double dt, int nsteps) {
     TB_REQUIRE(dt > 0 && std::isfinite(dt), TB_EINVAL, "dt must be positive and finite");
     TB_REQUIRE(nsteps >= 0, TB_EINVAL, "nsteps must be >= 0");
     TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
-    const int ts = P->d.timestepper;
     TB_CUDA_TRY(cudaEventRecord(P->ev0, P->st));
-    for (int i = 0; i < nsteps; ++i) {
-      int kind = 0;
-      if (ts == TB_SBDF1) kind = 1;
-      if (ts == TB_SBDF2) kind = (P->ms_history >= 1) ? 2 : 1;
-      if (kind == 0) {
-        const Tableau T = tableau(ts);
-        get_factors(P, 1.0, dt * T.AI[1][1]);
-      } else {
-        get_factors(P, sbdf_coefs(kind, dt).a0, 1.0);
-      }
-      if (P->profiling) {
-        if (kind == 0)
-          enqueue_rk_step(P, dt);
-        else
-          enqueue_sbdf_step(P, dt, kind);
-        check_launch("profiled step");
-      } else {
-        if (!(P->gexec && P->graph_dt == dt && P->graph_kind == kind)) capture_step(P, dt, kind);
-        TB_CUDA_TRY(cudaGraphLaunch(P->gexec, P->st));
-      }
-      P->sim_time += dt;
-      P->iteration += 1;
-      if (kind != 0) P->ms_history = 1;
-    }
+    plan_launch_steps(P, dt, nsteps, P->st, 1);
     TB_CUDA_TRY(cudaEventRecord(P->ev1, P->st));
     TB_CUDA_TRY(cudaEventSynchronize(P->ev1));
     TB_CUDA_TRY(cudaEventElapsedTime(&P->last_ms, P->ev0, P->ev1));
     TB_CUDA_TRY(cudaGetLastError());
     if (P->profiling) collect_profile(P);
   });
+}
+
+tb_status tb_step_async(tb_plan* P, double dt, int nsteps, int graph_steps) {
+  if (!P) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_REQUIRE(dt > 0 && std::isfinite(dt), TB_EINVAL, "dt must be positive and finite");
+    TB_REQUIRE(nsteps >= 0 && graph_steps >= 1, TB_EINVAL, "nsteps must be >= 0 and graph_steps >= 1");
+    TB_REQUIRE(!P->profiling, TB_ESTATE, "profiling runs through tb_step");
+    TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
+    plan_launch_steps(P, dt, nsteps, P->st, graph_steps);
+    check_launch("asynchronous steps");
+  });
+}
+
+tb_status tb_plan_query(tb_plan* P, int* idle) {
+  if (!P || !idle) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
+    const cudaError_t e = cudaStreamQuery(P->st);
+    if (e == cudaSuccess) {
+      *idle = 1;
+    } else if (e == cudaErrorNotReady) {
+      cudaGetLastError();
+      *idle = 0;
+    } else {
+      throw Error{TB_ECUDA, std::string("plan stream: ") + cudaGetErrorString(e)};
+    }
+  });
+}
+
+tb_status tb_plan_wait(tb_plan* P) {
+  if (!P) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  });
+}
+
+tb_status tb_plan_device_bytes(const tb_plan* P, size_t* bytes) {
+  if (!P || !bytes) return TB_EINVAL;
+  *bytes = plan_device_bytes(P);
+  return TB_OK;
 }
 
 tb_status tb_sim_time(const tb_plan* P, double* t, long long* it) {

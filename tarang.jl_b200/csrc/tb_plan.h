@@ -1,0 +1,193 @@
+// Plan object of the C ABI and the internal driver entry points shared by the
+// C ABI (tb_capi.cu), the ensemble runner (tb_ensemble.cu) and the request
+// server (tb_server.cu).  Not part of the public interface.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "tb_internal.h"
+#include "tb_kernels.cuh"
+
+namespace tb {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  void alloc(size_t b) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = b;
+    if (b == 0) return;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      throw Error{TB_ENOMEM, std::string("cudaMalloc(") + std::to_string(b) + "): " + cudaGetErrorString(e)};
+    }
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// Non-owning window into a DevBuf.
+struct DevView {
+  void* p = nullptr;
+  size_t bytes = 0;
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+template <class T>
+void upload(DevBuf& d, const std::vector<T>& h) {
+  d.alloc(h.size() * sizeof(T));
+  if (!h.empty()) TB_CUDA_TRY(cudaMemcpy(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+}
+
+struct ClassTables {
+  DevBuf row_eq, row_k, col_unk, col_k, left_unk, left_k, bc_rhs, band, bord, c2_z, c2_nz, c1_z, c1_nz;
+};
+
+struct FactorSet {
+  double alpha = 0, beta = 0;
+  DevBuf FR, BR, SI;  // solve-layout factor records (see tb_kernels.cuh)
+  DevBuf PP;          // partition transfer matrices of the solve
+  DevBuf HR;          // per-row backward responses of the partitioned solve
+};
+
+struct Tableau {
+  int s;
+  double AE[4][4], AI[4][4], bE[4], bI[4];
+};
+
+Tableau tableau(int ts);
+
+// Graph of `steps` consecutive steps of one kind at one dt.
+struct StepGraph {
+  double dt = -1.0;
+  int kind = -1, steps = 0;
+  cudaGraphExec_t exec = nullptr;
+};
+
+}  // namespace tb
+
+struct tb_plan {
+  using DevBuf = tb::DevBuf;
+  using DevView = tb::DevView;
+  using ClassTables = tb::ClassTables;
+  using FactorSet = tb::FactorSet;
+  using TauLayout = tb::TauLayout;
+  using FftPlan = tb::FftPlan;
+  tb_context* ctx = nullptr;
+  tb_problem_desc d{};
+  int Nx = 0, Nz = 0, Nk = 0, M = 0;
+  double k0 = 0, s = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  size_t plane = 0;  // Nz * Nk complex entries
+  // state and work arrays
+  // X holds the 4 state planes followed by the 7 tau rows (tau views its tail),
+  // so one 32-bit element offset from X addresses every unknown of the solve
+  DevBuf X, G, H, MX0, FP[4], LXP[4], Fprev, MXprev, Rsb, tmpgrid;
+  DevView tau;
+  // transform constants
+  DevBuf bwd, fwd, s3, twM, twN, ptwM;
+  // parity halves of the Chebyshev matrices (H = ceil(Nz/2) rows/cols)
+  DevBuf bEv, bOv, bEd, bOd, fE, fO, sfE, sfO;
+  int Hz = 0, Ke = 0, Ko = 0;  // Hz = ceil(Nz/2)
+  FftPlan fpM{}, fpN{};
+  // tau layout
+  TauLayout lay;
+  ClassTables ct[2];
+  std::vector<std::unique_ptr<FactorSet>> factors;
+  DevBuf err_mode, rhs_off;
+  // stepping state
+  double sim_time = 0.0;
+  long long iteration = 0;
+  int ms_history = 0;  // SBDF: number of stored history levels
+  double graph_dt = -1.0;
+  int graph_kind = -1;
+  cudaGraphExec_t gexec = nullptr;
+  tb::StepGraph multi;  // graph of several steps (asynchronous / batched stepping)
+  int kernels_per_step = 0;
+  int tau_parts = 1;  // partitions of the tau solve (kTauParts or 1)
+  // profiling: eager launches bracketed by events, accumulated per kernel name
+  bool profiling = false;
+  struct ProfRec {
+    std::string name;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfRec> pending;
+  std::vector<cudaEvent_t> event_pool;
+  std::map<std::string, std::pair<double, long long>> prof;  // name -> (ms, launches)
+
+  ~tb_plan() {
+    for (auto e : event_pool) cudaEventDestroy(e);
+    for (auto& r : pending) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (multi.exec) cudaGraphExecDestroy(multi.exec);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  double2* Xp(int f) const { return X.as<double2>() + (size_t)f * plane; }
+};
+
+namespace tb {
+
+// Device bytes the plan holds (state, work arrays, constants, factors).
+size_t plan_device_bytes(const tb_plan* P);
+// Kind of the next step: 0 RK, 1 SBDF1, 2 SBDF2.
+int plan_next_kind(const tb_plan* P);
+// Enqueue nsteps steps on stream s (the plan's own stream if s is null), using
+// cached CUDA graphs of up to graph_steps steps; factors and graphs are built
+// on first use of a (dt, kind).  Returns without waiting for the GPU.
+void plan_launch_steps(tb_plan* P, double dt, int nsteps, cudaStream_t s, int graph_steps);
+// Snapshot / restore of the stepping state (X, history, counters) in device scratch.
+struct PlanSnapshot {
+  DevBuf X, Fprev, MXprev;
+  double sim_time = 0.0;
+  long long iteration = 0;
+  int ms_history = 0;
+};
+void plan_snapshot(tb_plan* P, PlanSnapshot* snap);
+void plan_restore(tb_plan* P, const PlanSnapshot& snap);
+
+// Error plumbing shared by the C ABI translation units.
+void record_error(tb_context* ctx, const Error& e);
+template <class F>
+tb_status guarded(tb_context* ctx, F&& fn) {
+  try {
+    fn();
+    return TB_OK;
+  } catch (const Error& e) {
+    record_error(ctx, e);
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    record_error(ctx, Error{TB_ENOMEM, "host allocation failed"});
+    return TB_ENOMEM;
+  } catch (...) {
+    record_error(ctx, Error{TB_EINVAL, "unexpected internal error"});
+    return TB_EINVAL;
+  }
+}
+
+}  // namespace tb
