@@ -40,7 +40,7 @@ struct tb_ensemble {
 
 namespace {
 
-constexpr int kMaxWorkerStreams = 16;
+constexpr int kMaxWorkerStreams = 32;
 
 void ensure_streams(tb_ensemble* E, int n) {
   while ((int)E->ws.size() < n) {
@@ -162,7 +162,7 @@ tb_status tb_ensemble_tune(tb_ensemble* E, const double* dt, int trial_steps, in
     // warm-up: factors and graphs of every member at this dt
     run(E, dt, std::min(trial_steps, 2), std::min(n, 8), 1, nullptr, nullptr);
     restore();
-    const int cand_s[] = {1, 2, 4, 8, 16};
+    const int cand_s[] = {1, 2, 4, 8, 16, 32};
     const int cand_g[] = {1, 4, 16};
     float best = 1e30f;
     int bs = E->streams, bg = E->graph_steps;

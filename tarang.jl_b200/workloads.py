@@ -107,3 +107,24 @@ def step_model_bytes(cfg: RBCConfig, scheme: str) -> float:
             total += 2 * V + Phi
     total += V + sum(V * (bE[j] + bI[j]) for j in range(s)) + 2 * V
     return total
+
+
+# ---------------------------------------------------------------------------
+# Batched ensemble: independent 2D RBC instances of uneven size.
+# ---------------------------------------------------------------------------
+ENSEMBLE_SIZES = ((128, 32), (256, 64), (384, 96), (512, 128))
+
+
+def ensemble_members(n: int = 64, seed: int = 7, dt: float = 0.02, scheme: str = "RK222"):
+    """Ensemble configuration: (Nx, Nz) drawn by seed from ENSEMBLE_SIZES, Ra
+    log-uniform in [1e5, 1e8], Pr uniform in [0.7, 7]; member k gets noise seed
+    1000 + k.  One dt for all members (free-fall units, well inside the
+    advective limit of the first 100 steps from rest)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        Nx, Nz = ENSEMBLE_SIZES[int(rng.integers(len(ENSEMBLE_SIZES)))]
+        Ra = float(10.0 ** rng.uniform(5.0, 8.0))
+        Pr = float(rng.uniform(0.7, 7.0))
+        out.append(RBCConfig(Nx=Nx, Nz=Nz, Ra=Ra, Pr=Pr, dt=dt, scheme=scheme, seed=1000 + k))
+    return out
