@@ -48,8 +48,12 @@ enum { TB_RK222 = 0, TB_RK443 = 1, TB_SBDF1 = 2, TB_SBDF2 = 3 };
 
 /* Equation programs.  TB_PROGRAM_RBC is the Boussinesq system of
  * test/test_subproblem_rk.jl:50-57 (first-order tau formulation with
- * lift(., -1) on the last ChebyshevT mode). */
-enum { TB_PROGRAM_RBC = 0 };
+ * lift(., -1) on the last ChebyshevT mode).  TB_PROGRAM_TURB2D is the doubly
+ * periodic vorticity-streamfunction system of
+ * examples/2d_decaying_turbulence_gpu.jl (dq/dt - nu Lap q = -u.grad q,
+ * Lap psi = q with zero-mean gauge, u = skew(grad psi)) stepped with
+ * DiagonalIMEX_SBDF2 in FP32 (uses Nx, Ny, Lx, Ly, nu). */
+enum { TB_PROGRAM_RBC = 0, TB_PROGRAM_TURB2D = 1 };
 
 /* Arithmetic of the step. */
 enum { TB_PREC_F64 = 0, TB_PREC_MIXED = 1 };
@@ -67,7 +71,7 @@ typedef struct tb_problem_desc {
   double dealias;    /* 3/2 padding factor along Fourier axes                    */
   int precision;     /* TB_PREC_*                                                */
   int timestepper;   /* TB_RK222 ...                                             */
-  int program;       /* TB_PROGRAM_RBC                                           */
+  int program;       /* TB_PROGRAM_RBC or TB_PROGRAM_TURB2D                      */
   double kappa, nu;  /* b diffusivity, kinematic viscosity                       */
   double b_bottom;   /* value of b at z = 0   (BC "b(z=0) = ...")               */
   double b_top;      /* value of b at z = Lz  (BC "b(z=Lz) = ...")              */
@@ -214,6 +218,60 @@ tb_status tb_ensemble_tune(tb_ensemble* ens, const double* dt, int trial_steps, 
 tb_status tb_ensemble_set_config(tb_ensemble* ens, int streams, int graph_steps);
 tb_status tb_ensemble_config(const tb_ensemble* ens, int* streams, int* graph_steps);
 tb_status tb_ensemble_run(tb_ensemble* ens, const double* dt, int nsteps, float* member_ms, float* total_ms);
+
+/* -------------------------------------------------------------------------
+ * 2D decaying turbulence, FP32.  Replaces the reference's DiagonalIMEX_SBDF2
+ * step for a doubly periodic RealFourier x RealFourier problem
+ * (src/core/timesteppers/step_diagonal_imex.jl:329-388, 674-689) with the
+ * spectral Poisson and velocity refresh (state_utils.jl:1059-1104) and the
+ * 3/2-padded products with symmetric Nyquist split/fold
+ * (nonlinear_padding.jl:182-443).  q0_spec: initial vorticity coefficients,
+ * complex128 (Nx/2+1, Ny), x fastest, unnormalised rfft along x and fft along
+ * y (the reference's coefficient layout).  Nx, Ny even, 2^a 3^b, <= 2048.
+ * ---------------------------------------------------------------------- */
+typedef struct tb_turb tb_turb;
+tb_status tb_turb_create(tb_context* ctx, const tb_problem_desc* desc, const double* q0_spec, tb_turb** out);
+tb_status tb_turb_destroy(tb_turb* turb);
+tb_status tb_turb_step(tb_turb* turb, double dt, int nsteps);
+tb_status tb_turb_get_vorticity(tb_turb* turb, double* q_spec_host);
+
+/* -------------------------------------------------------------------------
+ * Request server (continuous batching).  No counterpart in the reference,
+ * which runs one solver per process.  A worker thread admits requests in
+ * arrival order while their estimated device bytes fit the budget and a run
+ * slot is free, gives each its own plan and stream, and keeps every running
+ * request's next chunk of steps in flight, so requests of different programs
+ * and sizes overlap on the device and new ones join as memory frees up.
+ * init_grid: RBC - the initial buoyancy on the (Nz, Nx) grid (x fastest,
+ * real); TURB2D - the initial vorticity coefficients as for tb_turb_create.
+ * Results: RBC fields 0..2 = b, u_x, u_z coefficients (Nx/2+1, Nz) complex128;
+ * TURB2D field 0 = vorticity coefficients (Nx/2+1, Ny) complex128.
+ * Time to solution = completion - submission (host clock, ms).
+ * ---------------------------------------------------------------------- */
+enum { TB_REQ_QUEUED = 0, TB_REQ_RUNNING = 1, TB_REQ_DONE = 2, TB_REQ_FAILED = 3 };
+typedef struct tb_request {
+  tb_problem_desc desc;
+  double dt;
+  int nsteps;
+  const double* init_grid;
+} tb_request;
+typedef struct tb_server_stats {
+  long long submitted, completed, failed, running, queued;
+  double elapsed_ms;   /* first submission to last completion            */
+  double solves_per_s; /* completed requests per second of elapsed time  */
+  double steps_per_s;  /* completed request steps per second             */
+  double p50_ms, p99_ms, mean_wait_ms;
+  size_t peak_bytes, budget_bytes;
+  int peak_running;
+} tb_server_stats;
+typedef struct tb_server tb_server;
+tb_status tb_server_create(tb_context* ctx, size_t budget_bytes, int max_running, int chunk_steps, tb_server** out);
+tb_status tb_server_submit(tb_server* srv, const tb_request* req, long long* id);
+tb_status tb_server_poll(tb_server* srv, long long id, int* state, double* tts_ms);
+tb_status tb_server_result(tb_server* srv, long long id, int field, double* host_out, size_t* ndoubles);
+tb_status tb_server_wait_all(tb_server* srv);
+tb_status tb_server_get_stats(tb_server* srv, tb_server_stats* out);
+tb_status tb_server_destroy(tb_server* srv);
 
 #ifdef __cplusplus
 }

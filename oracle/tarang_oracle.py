@@ -617,3 +617,150 @@ def run_rbc(p: RBCParams, scheme: str, dt: float, nsteps: int, seed: int = 42) -
     for _ in range(nsteps):
         sim.step(dt, scheme)
     return sim
+
+
+# ---------------------------------------------------------------------------
+# 2D doubly periodic decaying turbulence (vorticity form), DiagonalIMEX_SBDF2
+# (examples/2d_decaying_turbulence_gpu.jl).  Layout: a grid field of logical
+# size (Nx, Ny) is an array of shape (Ny, Nx); coefficients (Nx/2+1, Ny) are
+# shape (Ny, Nx/2+1): rfft along x, fft along y, unnormalised.
+# ---------------------------------------------------------------------------
+def turb_wavenumbers(Nx: int, Ny: int, Lx: float, Ly: float):
+    """kx: rfft layout 0..Nx/2 (basis_wavenumbers.jl:68-79); ky: fft order with
+    -Ny/2 at the Nyquist index (basis_wavenumbers.jl:95-108)."""
+    kx = 2 * np.pi / Lx * np.arange(Nx // 2 + 1)
+    ky = 2 * np.pi / Ly * np.concatenate([np.arange(Ny // 2), np.arange(-(Ny // 2), 0)])
+    return kx[None, :], ky[:, None]
+
+
+def turb_forward(g: np.ndarray) -> np.ndarray:
+    """Grid (Ny, Nx) real -> coefficients: rfft along x then fft along y."""
+    return np.fft.fft(np.fft.rfft(g, axis=1), axis=0)
+
+
+def turb_backward(c: np.ndarray, Nx: int) -> np.ndarray:
+    """Coefficients -> grid: ifft along y, irfft along x (Im of DC and Nyquist dropped)."""
+    return np.fft.irfft(np.fft.ifft(c, axis=0), n=Nx, axis=1)
+
+
+def _pad_full(A: np.ndarray, M: Tuple[int, int]) -> np.ndarray:
+    """Zero-pad a full complex spectrum with the even-N Nyquist split X/2 at
+    +-N/2, axis x first then y (nonlinear_padding.jl:164-262)."""
+    Ny, Nx = A.shape
+    My, Mx = M
+    P = np.zeros((My, Mx), dtype=complex)
+
+    def ranges(N, Mn):
+        h = N // 2
+        pos = (slice(0, h + 1), slice(0, h + 1))
+        nneg = N - h - 1
+        neg = (slice(N - nneg, N), slice(Mn - nneg, Mn)) if nneg > 0 else None
+        return pos, neg
+
+    (py, pyp), ny_ = ranges(Ny, My)
+    (px, pxp), nx_ = ranges(Nx, Mx)
+    P[pyp, pxp] = A[py, px]
+    if ny_:
+        P[ny_[1], pxp] = A[ny_[0], px]
+    if nx_:
+        P[pyp, nx_[1]] = A[py, nx_[0]]
+    if ny_ and nx_:
+        P[ny_[1], nx_[1]] = A[ny_[0], nx_[0]]
+    for axis, N, Mn in ((1, Nx, Mx), (0, Ny, My)):
+        if N % 2 == 0 and Mn > N:
+            nyq, mir = N // 2, Mn - N // 2
+            if axis == 1:
+                P[:, nyq] *= 0.5
+                P[:, mir] = P[:, nyq]
+            else:
+                P[nyq, :] *= 0.5
+                P[mir, :] = P[nyq, :]
+    return P
+
+
+def _truncate_full(P: np.ndarray, N: Tuple[int, int]) -> np.ndarray:
+    """Fold the -N/2 images into +N/2 (x then y) and truncate
+    (nonlinear_padding.jl:208-346)."""
+    P = P.copy()
+    My, Mx = P.shape
+    Ny, Nx = N
+    for axis, n, Mn in ((1, Nx, Mx), (0, Ny, My)):
+        if n % 2 == 0 and Mn > n:
+            nyq, mir = n // 2, Mn - n // 2
+            if axis == 1:
+                P[:, nyq] += P[:, mir]
+            else:
+                P[nyq, :] += P[mir, :]
+    out = np.zeros((Ny, Nx), dtype=complex)
+    hy, hx = Ny // 2, Nx // 2
+    ny_, nx_ = Ny - hy - 1, Nx - hx - 1
+    out[: hy + 1, : hx + 1] = P[: hy + 1, : hx + 1]
+    if ny_:
+        out[Ny - ny_:, : hx + 1] = P[My - ny_:, : hx + 1]
+    if nx_:
+        out[: hy + 1, Nx - nx_:] = P[: hy + 1, Mx - nx_:]
+    if ny_ and nx_:
+        out[Ny - ny_:, Nx - nx_:] = P[My - ny_:, Mx - nx_:]
+    return out
+
+
+def padded_multiply_2d(a: np.ndarray, b: np.ndarray, factor: float = 1.5) -> np.ndarray:
+    """evaluate_padded_multiply for two real grid fields on a doubly periodic
+    grid (nonlinear_padding.jl:359-443): fftn, pad with Nyquist split, ifftn
+    (1/M), product, fftn, fold + truncate, ifftn (1/N), real part, times M/N
+    per axis."""
+    Ny, Nx = a.shape
+    My, Mx = padded_length(Ny, factor), padded_length(Nx, factor)
+    Pa = np.fft.ifftn(_pad_full(np.fft.fftn(a), (My, Mx)))
+    Pb = np.fft.ifftn(_pad_full(np.fft.fftn(b), (My, Mx)))
+    R = _truncate_full(np.fft.fftn(Pa * Pb), (Ny, Nx))
+    return np.real(np.fft.ifftn(R)) * (Mx / Nx) * (My / Ny)
+
+
+def turb_rhs(q: np.ndarray, Nx: int, Lx: float, Ly: float) -> np.ndarray:
+    """F = -u.grad(q) in coefficients: psi = -q/k^2 (k=0 gauge 0,
+    state_utils.jl:1059-1075), u = (-d_y psi, d_x psi) (:1077-1104), derivative
+    multipliers i k (lazy_rhs.jl:1190-1238), dealiased products."""
+    Ny = q.shape[0]
+    kx, ky = turb_wavenumbers(Nx, Ny, Lx, Ly)
+    k2 = kx ** 2 + ky ** 2
+    psi = np.where(k2 > 1e-12, -q / np.where(k2 > 1e-12, k2, 1.0), 0.0)
+    u = turb_backward(-1j * ky * psi, Nx)
+    v = turb_backward(1j * kx * psi, Nx)
+    qx = turb_backward(1j * kx * q, Nx)
+    qy = turb_backward(1j * ky * q, Nx)
+    F = -(padded_multiply_2d(u, qx) + padded_multiply_2d(v, qy))
+    return turb_forward(F)
+
+
+def run_turb(q0: np.ndarray, Nx: int, Lx: float, Ly: float, nu: float, dt: float, nsteps: int) -> np.ndarray:
+    """DiagonalIMEX_SBDF2 with constant dt (step_diagonal_imex.jl:329-388,
+    674-689), L^ = nu k^2: SBDF1 startup, then
+    q_{n+1} = (2 q_n - q_{n-1}/2 + dt (2 F_n - F_{n-1})) / (3/2 + dt L^)."""
+    Ny = q0.shape[0]
+    kx, ky = turb_wavenumbers(Nx, Ny, Lx, Ly)
+    L = nu * (kx ** 2 + ky ** 2)
+    q, qm, Fm = q0.copy(), None, None
+    for n in range(nsteps):
+        Fn = turb_rhs(q, Nx, Lx, Ly)
+        if n == 0:
+            qn = (q + dt * Fn) / (1.0 + dt * L)
+        else:
+            qn = (2.0 * q - 0.5 * qm + dt * (2.0 * Fn - Fm)) / (1.5 + dt * L)
+        qm, q, Fm = q, qn, Fn
+    return q
+
+
+def turb_initial_spec(Nx: int, Ny: int, seed: int, kmin: float = 1.0, kmax: Optional[float] = None,
+                      amp: float = 10.0) -> np.ndarray:
+    """Seeded initial vorticity with a k^-3 energy spectrum (|q^| ~ 1/k per mode
+    for kmin <= |k| <= kmax, random phases), scaled to max |q| = amp on the grid."""
+    kmax = kmax if kmax is not None else min(Nx, Ny) / 3.0
+    rng = np.random.default_rng(seed)
+    kx, ky = turb_wavenumbers(Nx, Ny, 2 * np.pi, 2 * np.pi)
+    k = np.sqrt(kx ** 2 + ky ** 2)
+    mag = np.where((k >= kmin) & (k <= kmax), 1.0 / np.maximum(k, 1e-30), 0.0)
+    phase = rng.uniform(0.0, 2 * np.pi, size=mag.shape)
+    g = turb_backward(mag * np.exp(1j * phase), Nx)
+    g *= amp / np.abs(g).max()
+    return turb_forward(g)

@@ -21,6 +21,10 @@ from .api import (  # noqa: F401
     Ensemble,
     InitialValueSolver,
     Plan,
+    Server,
+    Turb2D,
+    rbc_desc,
+    turb_desc,
     RealFourier,
     ScalarField,
     VectorField,

@@ -17,6 +17,8 @@ TB_OK, TB_EINVAL, TB_ENOMEM, TB_ESINGULAR, TB_ETIMEOUT, TB_ECUDA, TB_ENOTSUPPORT
 TB_HOST, TB_DEVICE = 0, 1
 TB_RK222, TB_RK443, TB_SBDF1, TB_SBDF2 = 0, 1, 2, 3
 TB_PROGRAM_RBC = 0
+TB_PROGRAM_TURB2D = 1
+TB_REQ_QUEUED, TB_REQ_RUNNING, TB_REQ_DONE, TB_REQ_FAILED = 0, 1, 2, 3
 TB_PREC_F64, TB_PREC_MIXED = 0, 1
 TB_FIELD_B, TB_FIELD_UX, TB_FIELD_UZ, TB_FIELD_P, TB_FIELD_TAU = range(5)
 
@@ -38,6 +40,19 @@ class tb_problem_desc(Structure):
         ("nu", c_double),
         ("b_bottom", c_double),
         ("b_top", c_double),
+    ]
+
+
+class tb_request(Structure):
+    _fields_ = [("desc", tb_problem_desc), ("dt", c_double), ("nsteps", c_int), ("init_grid", c_void_p)]
+
+
+class tb_server_stats(Structure):
+    _fields_ = [
+        ("submitted", c_longlong), ("completed", c_longlong), ("failed", c_longlong), ("running", c_longlong),
+        ("queued", c_longlong), ("elapsed_ms", c_double), ("solves_per_s", c_double), ("steps_per_s", c_double),
+        ("p50_ms", c_double), ("p99_ms", c_double), ("mean_wait_ms", c_double), ("peak_bytes", c_size_t),
+        ("budget_bytes", c_size_t), ("peak_running", c_int),
     ]
 
 
@@ -87,6 +102,17 @@ SIGNATURES = {
     "tb_ensemble_set_config": (c_int, [c_void_p, c_int, c_int]),
     "tb_ensemble_config": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
     "tb_ensemble_run": (c_int, [c_void_p, c_void_p, c_int, c_void_p, POINTER(c_float)]),
+    "tb_turb_create": (c_int, [c_void_p, POINTER(tb_problem_desc), c_void_p, POINTER(c_void_p)]),
+    "tb_turb_destroy": (c_int, [c_void_p]),
+    "tb_turb_step": (c_int, [c_void_p, c_double, c_int]),
+    "tb_turb_get_vorticity": (c_int, [c_void_p, c_void_p]),
+    "tb_server_create": (c_int, [c_void_p, c_size_t, c_int, c_int, POINTER(c_void_p)]),
+    "tb_server_submit": (c_int, [c_void_p, POINTER(tb_request), POINTER(c_longlong)]),
+    "tb_server_poll": (c_int, [c_void_p, c_longlong, POINTER(c_int), POINTER(c_double)]),
+    "tb_server_result": (c_int, [c_void_p, c_longlong, c_int, c_void_p, POINTER(c_size_t)]),
+    "tb_server_wait_all": (c_int, [c_void_p]),
+    "tb_server_get_stats": (c_int, [c_void_p, POINTER(tb_server_stats)]),
+    "tb_server_destroy": (c_int, [c_void_p]),
 }
 
 

@@ -309,6 +309,124 @@ class Ensemble:
         return ms, tot.value
 
 
+class Turb2D:
+    """Doubly periodic 2D decaying turbulence in FP32 (DiagonalIMEX_SBDF2), the
+    reference's examples/2d_decaying_turbulence_gpu.jl on the C ABI.
+    Coefficients are complex (Ny, Nx/2+1) arrays (rfft along x, fft along y)."""
+
+    def __init__(self, Nx: int, Ny: int, nu: float, q0_spec: np.ndarray, Lx: float = 2 * math.pi,
+                 Ly: float = 2 * math.pi, device: int = 0):
+        self.Nx, self.Ny = int(Nx), int(Ny)
+        self.ctx = _context(device)
+        d = turb_desc(Nx, Ny, nu, Lx, Ly)
+        q = np.ascontiguousarray(q0_spec, dtype=np.complex128)
+        assert q.shape == (self.Ny, self.Nx // 2 + 1)
+        self.ptr = c_void_p()
+        check(lib.tb_turb_create(self.ctx, byref(d), q.ctypes.data_as(c_void_p), byref(self.ptr)), self.ctx)
+
+    def __del__(self):
+        ptr = getattr(self, "ptr", None)
+        if ptr:
+            lib.tb_turb_destroy(ptr)
+            self.ptr = None
+
+    def step(self, dt: float, nsteps: int = 1) -> None:
+        check(lib.tb_turb_step(self.ptr, float(dt), int(nsteps)), self.ctx)
+
+    def vorticity(self) -> np.ndarray:
+        out = np.zeros((self.Ny, self.Nx // 2 + 1), dtype=np.complex128)
+        check(lib.tb_turb_get_vorticity(self.ptr, out.ctypes.data_as(c_void_p)), self.ctx)
+        return out
+
+
+def turb_desc(Nx: int, Ny: int, nu: float, Lx: float = 2 * math.pi, Ly: float = 2 * math.pi):
+    d = L.tb_problem_desc()
+    d.ndim, d.Nx, d.Ny, d.Nz = 2, int(Nx), int(Ny), 1
+    d.Lx, d.Ly, d.Lz, d.dealias = float(Lx), float(Ly), 1.0, 1.5
+    d.precision, d.timestepper, d.program = 0, L.TB_SBDF2, L.TB_PROGRAM_TURB2D
+    d.kappa, d.nu, d.b_bottom, d.b_top = 0.0, float(nu), 0.0, 0.0
+    return d
+
+
+def rbc_desc(Nx: int, Nz: int, kappa: float, nu: float, timestepper: int = 0, Lx: float = 4.0, Lz: float = 1.0,
+             b_bottom: Optional[float] = None, b_top: float = 0.0):
+    d = L.tb_problem_desc()
+    d.ndim, d.Nx, d.Ny, d.Nz = 2, int(Nx), 1, int(Nz)
+    d.Lx, d.Ly, d.Lz, d.dealias = float(Lx), 1.0, float(Lz), 1.5
+    d.precision, d.timestepper, d.program = L.TB_PREC_F64, int(timestepper), L.TB_PROGRAM_RBC
+    d.kappa, d.nu = float(kappa), float(nu)
+    d.b_bottom, d.b_top = float(Lz if b_bottom is None else b_bottom), float(b_top)
+    return d
+
+
+class Server:
+    """Request server with continuous batching (tb_server_* in the C ABI).
+
+    ``submit`` takes a problem descriptor (``rbc_desc`` / ``turb_desc``), dt,
+    the step count and the initial data (RBC: buoyancy grid (Nz, Nx); TURB2D:
+    vorticity coefficients (Ny, Nx/2+1) complex) and returns an id; results
+    come back as coefficient arrays once the request is done."""
+
+    def __init__(self, budget_bytes: int, max_running: int = 16, chunk_steps: int = 10, device: int = 0):
+        self.ctx = _context(device)
+        self.ptr = c_void_p()
+        self._keep = {}
+        self._shape = {}
+        check(lib.tb_server_create(self.ctx, int(budget_bytes), int(max_running), int(chunk_steps),
+                                   byref(self.ptr)), self.ctx)
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        ptr = getattr(self, "ptr", None)
+        if ptr:
+            lib.tb_server_destroy(ptr)
+            self.ptr = None
+
+    def submit(self, desc, dt: float, nsteps: int, init: np.ndarray) -> int:
+        if desc.program == L.TB_PROGRAM_TURB2D:
+            data = np.ascontiguousarray(init, dtype=np.complex128)
+            shape = (desc.Ny, desc.Nx // 2 + 1)
+            assert data.shape == shape
+            nf = 1
+        else:
+            data = np.ascontiguousarray(init, dtype=np.float64)
+            assert data.shape == (desc.Nz, desc.Nx)
+            shape = (desc.Nz, desc.Nx // 2 + 1)
+            nf = 3
+        r = L.tb_request()
+        r.desc, r.dt, r.nsteps = desc, float(dt), int(nsteps)
+        r.init_grid = data.ctypes.data_as(c_void_p)
+        rid = c_longlong()
+        check(lib.tb_server_submit(self.ptr, byref(r), byref(rid)), self.ctx)
+        self._shape[rid.value] = (shape, nf)
+        return rid.value
+
+    def poll(self, rid: int):
+        st, t = c_int(), c_double()
+        check(lib.tb_server_poll(self.ptr, int(rid), byref(st), byref(t)), self.ctx)
+        return st.value, t.value
+
+    def result(self, rid: int):
+        shape, nf = self._shape[rid]
+        out = []
+        for f in range(nf):
+            a = np.zeros(shape, dtype=np.complex128)
+            n = c_size_t()
+            check(lib.tb_server_result(self.ptr, int(rid), f, a.ctypes.data_as(c_void_p), byref(n)), self.ctx)
+            out.append(a)
+        return out
+
+    def wait_all(self) -> None:
+        check(lib.tb_server_wait_all(self.ptr), self.ctx)
+
+    def stats(self) -> Dict[str, float]:
+        st = L.tb_server_stats()
+        check(lib.tb_server_get_stats(self.ptr, byref(st)), self.ctx)
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+
 class ScalarField:
     """A scalar field on a domain (or a tau field with ``bases=(xbasis,)`` / ``()``).
 

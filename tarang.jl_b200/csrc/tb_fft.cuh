@@ -1,0 +1,191 @@
+// Stockham FFT building blocks in shared memory, generic over the complex
+// type (float2 for the FP32 programs, double2).  Same formulation as the
+// double-only transforms of the Chebyshev programs: radix 8/4/2/3 passes,
+// natural-order output, XOR-swizzled buffers, per-pass twiddle tables
+// pt[j] = exp(-2 pi i j n/(Ns R) / n) for j < Ns.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "tb_internal.h"
+
+namespace tb {
+namespace fftg {
+
+template <class C>
+struct Real;
+template <>
+struct Real<float2> {
+  using type = float;
+};
+template <>
+struct Real<double2> {
+  using type = double;
+};
+
+template <class C>
+__device__ __forceinline__ C mk(typename Real<C>::type x, typename Real<C>::type y) {
+  C c;
+  c.x = x;
+  c.y = y;
+  return c;
+}
+template <class C>
+__device__ __forceinline__ C add(C a, C b) {
+  return mk<C>(a.x + b.x, a.y + b.y);
+}
+template <class C>
+__device__ __forceinline__ C sub(C a, C b) {
+  return mk<C>(a.x - b.x, a.y - b.y);
+}
+template <class C>
+__device__ __forceinline__ C mul(C a, C b) {
+  return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <class C>
+__device__ __forceinline__ C scale(C a, typename Real<C>::type s) {
+  return mk<C>(a.x * s, a.y * s);
+}
+template <class C>
+__device__ __forceinline__ C conjg(C a) {
+  return mk<C>(a.x, -a.y);
+}
+// multiply by exp(sign i pi/2)
+template <class C>
+__device__ __forceinline__ C rot4(C d, int sign) {
+  return (sign < 0) ? mk<C>(d.y, -d.x) : mk<C>(-d.y, d.x);
+}
+
+template <bool SW>
+__device__ __forceinline__ int fidx(int i) {
+  return SW ? (i ^ ((i >> 3) & 7)) : i;
+}
+
+template <class C>
+__device__ __forceinline__ void dft4(C& x0, C& x1, C& x2, C& x3, int sign) {
+  const C t0 = add(x0, x2), t1 = sub(x0, x2), t2 = add(x1, x3), t3 = rot4(sub(x1, x3), sign);
+  x0 = add(t0, t2);
+  x1 = add(t1, t3);
+  x2 = sub(t0, t2);
+  x3 = sub(t1, t3);
+}
+
+template <int R, class C>
+__device__ __forceinline__ void dft_small(C (&v)[R], int sign) {
+  using T = typename Real<C>::type;
+  if constexpr (R == 2) {
+    const C a = v[0], b = v[1];
+    v[0] = add(a, b);
+    v[1] = sub(a, b);
+  } else if constexpr (R == 3) {
+    const T h = (T)0.86602540378443864676372317075294;  // sqrt(3)/2
+    const C sm = add(v[1], v[2]), df = sub(v[1], v[2]);
+    const C base = mk<C>(v[0].x - (T)0.5 * sm.x, v[0].y - (T)0.5 * sm.y);
+    const C rot = mk<C>(-(T)sign * h * df.y, (T)sign * h * df.x);
+    v[0] = add(v[0], sm);
+    v[1] = add(base, rot);
+    v[2] = sub(base, rot);
+  } else if constexpr (R == 4) {
+    dft4(v[0], v[1], v[2], v[3], sign);
+  } else {
+    const T r = (T)0.70710678118654752440084436210485;
+    const T s = (T)sign;
+    C a[4], b[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      a[n] = add(v[n], v[n + 4]);
+      b[n] = sub(v[n], v[n + 4]);
+    }
+    b[1] = mk<C>(r * (b[1].x - s * b[1].y), r * (b[1].y + s * b[1].x));
+    b[2] = rot4(b[2], sign);
+    b[3] = mk<C>(r * (-b[3].x - s * b[3].y), r * (-b[3].y + s * b[3].x));
+    dft4(a[0], a[1], a[2], a[3], sign);
+    dft4(b[0], b[1], b[2], b[3], sign);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[2 * k] = a[k];
+      v[2 * k + 1] = b[k];
+    }
+  }
+}
+
+template <int R, bool SW, class C>
+__device__ __forceinline__ void pass(const C* __restrict__ in, C* __restrict__ out, int n, int Ns,
+                                     const C* __restrict__ pt, int sign) {
+  const int nR = n / R;
+  for (int idx = threadIdx.x; idx < nR; idx += blockDim.x) {
+    const int j = idx % Ns, k = idx / Ns;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = in[fidx<SW>(idx + r * nR)];
+    if (Ns > 1) {
+      C w1 = pt[j];
+      if (sign > 0) w1.y = -w1.y;
+      if constexpr (R == 8) {
+        const C w2 = mul(w1, w1), w4 = mul(w2, w2), w3 = mul(w1, w2);
+        v[1] = mul(v[1], w1);
+        v[2] = mul(v[2], w2);
+        v[3] = mul(v[3], w3);
+        v[4] = mul(v[4], w4);
+        v[5] = mul(v[5], mul(w1, w4));
+        v[6] = mul(v[6], mul(w2, w4));
+        v[7] = mul(v[7], mul(w3, w4));
+      } else if constexpr (R == 4) {
+        const C w2 = mul(w1, w1);
+        v[1] = mul(v[1], w1);
+        v[2] = mul(v[2], w2);
+        v[3] = mul(v[3], mul(w1, w2));
+      } else if constexpr (R == 3) {
+        v[1] = mul(v[1], w1);
+        v[2] = mul(v[2], mul(w1, w1));
+      } else {
+        v[1] = mul(v[1], w1);
+      }
+    }
+    dft_small<R>(v, sign);
+    const int ob = k * Ns * R + j;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out[fidx<SW>(ob + r * Ns)] = v[r];
+  }
+}
+
+// Whole-CTA FFT of length fp.n between buffers a and b; returns the buffer
+// holding the result.  sign -1 forward, +1 inverse, both unnormalised.
+template <bool SW, class C>
+__device__ C* fft(C* a, C* b, const FftPlan& fp, const C* __restrict__ pt, int sign) {
+  const int n = fp.n;
+  int Ns = 1;
+  C* in = a;
+  C* out = b;
+  for (int s = 0; s < fp.nstages; ++s) {
+    const int R = fp.radix[s];
+    if (R == 8)
+      pass<8, SW>(in, out, n, Ns, pt, sign);
+    else if (R == 4)
+      pass<4, SW>(in, out, n, Ns, pt, sign);
+    else if (R == 2)
+      pass<2, SW>(in, out, n, Ns, pt, sign);
+    else
+      pass<3, SW>(in, out, n, Ns, pt, sign);
+    __syncthreads();
+    C* t = in;
+    in = out;
+    out = t;
+    pt += Ns;
+    Ns *= R;
+  }
+  return in;
+}
+
+// Number of per-pass twiddle entries of a plan (sum of the passes' Ns).
+__host__ __device__ inline int pass_twiddle_count(const FftPlan& fp) {
+  int c = 0, Ns = 1;
+  for (int s = 0; s < fp.nstages; ++s) {
+    c += Ns;
+    Ns *= fp.radix[s];
+  }
+  return c;
+}
+
+}  // namespace fftg
+}  // namespace tb

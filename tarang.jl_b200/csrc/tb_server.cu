@@ -1,0 +1,410 @@
+// Request server: runs of different programs and sizes admitted by device-memory
+// budget and stepped side by side (continuous batching).
+//
+// The reference runs one solver per process (solver_stepping.jl:115-205); the
+// serving pattern is new here.  A worker thread owns all GPU work:
+//   - admission, in arrival order: the next queued request starts when its
+//     estimated device bytes fit the remaining budget and a run slot is free;
+//     it gets its own plan and stream;
+//   - progress: every running request whose previous chunk has finished gets
+//     its next chunk of steps (one CUDA graph launch on its own stream), so
+//     the chunks of all running requests overlap on the device and a request
+//     that arrives while others run joins as soon as memory frees up;
+//   - completion: the final state is copied to host memory, the plan and its
+//     device memory are released, and the time from submission is recorded.
+// Each request's arithmetic is exactly what it would be alone (its own plan,
+// its own graphs); only the interleaving on the device differs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "tb_plan.h"
+#include "tb_turb.h"
+
+using namespace tb;
+
+namespace {
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+// One admitted run on the device.
+struct Job {
+  virtual ~Job() = default;
+  virtual cudaStream_t stream() const = 0;
+  virtual void launch(double dt, int steps) = 0;
+  virtual size_t device_bytes() const = 0;
+  virtual int nfields() const = 0;
+  virtual size_t field_doubles(int field) const = 0;
+  virtual void fetch(int field, double* host) = 0;
+};
+
+struct RbcJob : Job {
+  tb_plan* P = nullptr;
+  ~RbcJob() override {
+    if (P) tb_plan_destroy(P);
+  }
+  cudaStream_t stream() const override { return P->st; }
+  void launch(double dt, int steps) override { plan_launch_steps(P, dt, steps, P->st, steps); }
+  size_t device_bytes() const override { return plan_device_bytes(P); }
+  int nfields() const override { return 3; }  // b, u_x, u_z coefficients
+  size_t field_doubles(int) const override { return 2 * P->plane; }
+  void fetch(int field, double* host) override {
+    TB_CUDA_TRY(cudaMemcpyAsync(host, P->Xp(field), P->plane * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  }
+};
+
+struct TurbJob : Job {
+  tb_turb* T = nullptr;
+  ~TurbJob() override {
+    if (T) turb_destroy(T);
+  }
+  cudaStream_t stream() const override { return turb_stream(T); }
+  void launch(double dt, int steps) override { turb_launch_steps(T, dt, steps); }
+  size_t device_bytes() const override { return turb_device_bytes(T); }
+  int nfields() const override { return 1; }  // vorticity coefficients
+  size_t field_doubles(int) const override { return turb_field_doubles(T); }
+  void fetch(int, double* host) override { turb_fetch(T, host); }
+};
+
+// Device bytes a run of this size will hold (plan, factors, graphs' scratch).
+size_t estimate_bytes(const tb_problem_desc& d) {
+  if (d.program == TB_PROGRAM_TURB2D) return turb_estimate_bytes(d.Nx, d.Ny);
+  const size_t nk = d.Nx / 2 + 1, plane = (size_t)d.Nz * nk * 16;
+  const size_t npad = ((size_t)2 * d.Nz + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
+  const size_t groups = (nk + kSolveModes - 1) / kSolveModes;
+  const size_t rec = groups * npad * 2 * kSolveModes * (kFwdRec + kBwdRec + kHRec) * 8;
+  const size_t work = plane * (4 + 6 + 3 + 4 + 4 * 4 * 2 + 3 * 4 + 1) + (size_t)d.Nz * d.Nz * 8 * 8;
+  return rec + work + (16u << 20);
+}
+
+struct Request {
+  long long id = 0;
+  tb_problem_desc desc{};
+  double dt = 0;
+  int nsteps = 0, left = 0;
+  std::vector<double> init;
+  double t_submit = 0, t_start = 0, t_done = 0;
+  int state = TB_REQ_QUEUED;
+  std::string error;
+  size_t bytes = 0;
+  std::unique_ptr<Job> job;
+  cudaEvent_t ev = nullptr;
+  bool chunk_pending = false;
+  std::vector<std::vector<double>> result;
+};
+
+}  // namespace
+
+struct tb_server {
+  tb_context* ctx = nullptr;
+  size_t budget = 0;
+  int max_running = 1, chunk = 1;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<Request*> queue;
+  std::vector<Request*> running;
+  std::map<long long, std::unique_ptr<Request>> all;
+  long long next_id = 1;
+  bool stop = false;
+  std::thread worker;
+  // statistics
+  size_t used = 0, peak = 0;
+  int peak_running = 0;
+  long long completed = 0, failed = 0, steps_done = 0;
+  double first_submit = -1, last_done = 0;
+  std::vector<double> tts, waits;
+
+  void loop();
+  void admit();
+  void progress();
+  void fail_admitted(Request* r, const std::string& msg);
+  void fail_running(Request* r, const std::string& msg);
+};
+
+namespace {
+
+std::unique_ptr<Job> make_job(tb_context* ctx, const Request& r) {
+  if (r.desc.program == TB_PROGRAM_TURB2D) {
+    auto j = std::make_unique<TurbJob>();
+    j->T = turb_create(ctx, r.desc, r.init.data());
+    return j;
+  }
+  auto j = std::make_unique<RbcJob>();
+  tb_status st = tb_plan_create(ctx, &r.desc, &j->P);
+  if (st != TB_OK) throw Error{st, ctx->last_error};
+  tb_plan* P = j->P;
+  // initial state: b from the grid field, u = 0
+  DevBuf grid, coeff;
+  grid.alloc(r.init.size() * sizeof(double));
+  coeff.alloc(P->plane * sizeof(double2));
+  TB_CUDA_TRY(cudaMemcpy(grid.p, r.init.data(), grid.bytes, cudaMemcpyHostToDevice));
+  st = tb_transform_forward(P, grid.as<double>(), coeff.as<double>(), 1);
+  if (st != TB_OK) throw Error{st, ctx->last_error};
+  TB_CUDA_TRY(cudaMemsetAsync(P->X.p, 0, P->X.bytes, P->st));
+  TB_CUDA_TRY(cudaMemcpyAsync(P->Xp(0), coeff.p, coeff.bytes, cudaMemcpyDeviceToDevice, P->st));
+  TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  return j;
+}
+
+}  // namespace
+
+void tb_server::admit() {
+  while (true) {
+    Request* r = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (queue.empty() || (int)running.size() >= max_running) return;
+      Request* h = queue.front();
+      if (h->bytes > budget) {  // can never fit
+        queue.pop_front();
+        h->state = TB_REQ_FAILED;
+        h->error = "request needs more device memory than the server budget";
+        ++failed;
+        cv.notify_all();
+        continue;
+      }
+      if (used + h->bytes > budget) return;  // wait for memory to free up (arrival order)
+      queue.pop_front();
+      r = h;
+      used += r->bytes;
+      peak = std::max(peak, used);
+    }
+    try {
+      r->t_start = now_ms();
+      r->job = make_job(ctx, *r);
+      TB_CUDA_TRY(cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming));
+      std::lock_guard<std::mutex> lk(mu);
+      r->state = TB_REQ_RUNNING;
+      running.push_back(r);
+      peak_running = std::max(peak_running, (int)running.size());
+    } catch (const Error& e) {
+      fail_admitted(r, e.msg);
+    } catch (const std::exception& e) {
+      fail_admitted(r, e.what());
+    }
+  }
+}
+
+void tb_server::fail_admitted(Request* r, const std::string& msg) {
+  r->job.reset();
+  std::lock_guard<std::mutex> lk(mu);
+  used -= r->bytes;
+  r->state = TB_REQ_FAILED;
+  r->error = msg;
+  ++failed;
+  cv.notify_all();
+}
+
+void tb_server::progress() {
+  std::vector<Request*> act;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    act = running;
+  }
+  for (Request* r : act) {
+    try {
+      if (r->chunk_pending) {
+        const cudaError_t e = cudaEventQuery(r->ev);
+        if (e == cudaErrorNotReady) {
+          cudaGetLastError();
+          continue;
+        }
+        if (e != cudaSuccess) throw Error{TB_ECUDA, std::string("request stream: ") + cudaGetErrorString(e)};
+        r->chunk_pending = false;
+      }
+      if (r->left > 0) {
+        const int c = std::min(r->left, chunk);
+        r->job->launch(r->dt, c);
+        TB_CUDA_TRY(cudaEventRecord(r->ev, r->job->stream()));
+        r->left -= c;
+        r->chunk_pending = true;
+        continue;
+      }
+      // finished: result to host, device memory back to the pool
+      r->result.resize(r->job->nfields());
+      for (int f = 0; f < r->job->nfields(); ++f) {
+        r->result[f].resize(r->job->field_doubles(f));
+        r->job->fetch(f, r->result[f].data());
+      }
+      r->job.reset();
+      cudaEventDestroy(r->ev);
+      r->ev = nullptr;
+      std::lock_guard<std::mutex> lk(mu);
+      r->t_done = now_ms();
+      r->state = TB_REQ_DONE;
+      running.erase(std::find(running.begin(), running.end(), r));
+      used -= r->bytes;
+      ++completed;
+      steps_done += r->nsteps;
+      last_done = r->t_done;
+      tts.push_back(r->t_done - r->t_submit);
+      waits.push_back(r->t_start - r->t_submit);
+      cv.notify_all();
+    } catch (const Error& e) {
+      fail_running(r, e.msg);
+    } catch (const std::exception& e) {
+      fail_running(r, e.what());
+    }
+  }
+}
+
+void tb_server::fail_running(Request* r, const std::string& msg) {
+  r->job.reset();
+  if (r->ev) cudaEventDestroy(r->ev);
+  r->ev = nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  r->state = TB_REQ_FAILED;
+  r->error = msg;
+  running.erase(std::find(running.begin(), running.end(), r));
+  used -= r->bytes;
+  ++failed;
+  cv.notify_all();
+}
+
+void tb_server::loop() {
+  cudaSetDevice(ctx->device);
+  while (true) {
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      if (stop && queue.empty() && running.empty()) return;
+      if (queue.empty() && running.empty()) {
+        cv.wait_for(lk, std::chrono::milliseconds(2));
+        continue;
+      }
+    }
+    admit();
+    progress();
+    std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+}
+
+extern "C" {
+
+tb_status tb_server_create(tb_context* ctx, size_t budget_bytes, int max_running, int chunk_steps, tb_server** out) {
+  if (!ctx || !out || budget_bytes == 0 || max_running < 1 || chunk_steps < 1) return TB_EINVAL;
+  *out = nullptr;
+  return guarded(ctx, [&] {
+    auto S = std::make_unique<tb_server>();
+    S->ctx = ctx;
+    S->budget = budget_bytes;
+    S->max_running = max_running;
+    S->chunk = chunk_steps;
+    tb_server* raw = S.get();
+    S->worker = std::thread([raw] { raw->loop(); });
+    *out = S.release();
+  });
+}
+
+tb_status tb_server_submit(tb_server* S, const tb_request* req, long long* id) {
+  if (!S || !req || !id || !req->init_grid || req->nsteps < 0 || !(req->dt > 0)) return TB_EINVAL;
+  return guarded(S->ctx, [&] {
+    const tb_problem_desc& d = req->desc;
+    TB_REQUIRE(d.program == TB_PROGRAM_RBC || d.program == TB_PROGRAM_TURB2D, TB_ENOTSUPPORTED, "unknown program");
+    auto r = std::make_unique<Request>();
+    r->desc = d;
+    r->dt = req->dt;
+    r->nsteps = r->left = req->nsteps;
+    // RBC: real grid (Nz, Nx); TURB2D: complex coefficients (Ny, Nx/2+1)
+    const size_t ng = d.program == TB_PROGRAM_TURB2D ? (size_t)2 * d.Ny * (d.Nx / 2 + 1) : (size_t)d.Nx * d.Nz;
+    TB_REQUIRE(d.Nx > 0 && (d.program == TB_PROGRAM_TURB2D ? d.Ny > 0 : d.Nz > 0), TB_EINVAL, "bad sizes");
+    r->init.assign(req->init_grid, req->init_grid + ng);
+    r->bytes = estimate_bytes(d);
+    std::lock_guard<std::mutex> lk(S->mu);
+    r->id = S->next_id++;
+    r->t_submit = now_ms();
+    if (S->first_submit < 0) S->first_submit = r->t_submit;
+    *id = r->id;
+    S->queue.push_back(r.get());
+    S->all[r->id] = std::move(r);
+    S->cv.notify_all();
+  });
+}
+
+tb_status tb_server_poll(tb_server* S, long long id, int* state, double* tts_ms) {
+  if (!S || !state) return TB_EINVAL;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->all.find(id);
+  if (it == S->all.end()) return TB_EINVAL;
+  *state = it->second->state;
+  if (tts_ms) *tts_ms = it->second->state == TB_REQ_DONE ? it->second->t_done - it->second->t_submit : -1.0;
+  if (it->second->state == TB_REQ_FAILED) S->ctx->last_error = it->second->error;
+  return TB_OK;
+}
+
+tb_status tb_server_result(tb_server* S, long long id, int field, double* host_out, size_t* ndoubles) {
+  if (!S) return TB_EINVAL;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->all.find(id);
+  if (it == S->all.end() || it->second->state != TB_REQ_DONE) return TB_ESTATE;
+  const Request& r = *it->second;
+  if (field < 0 || field >= (int)r.result.size()) return TB_EINVAL;
+  if (ndoubles) *ndoubles = r.result[field].size();
+  if (host_out) std::copy(r.result[field].begin(), r.result[field].end(), host_out);
+  return TB_OK;
+}
+
+tb_status tb_server_wait_all(tb_server* S) {
+  if (!S) return TB_EINVAL;
+  std::unique_lock<std::mutex> lk(S->mu);
+  S->cv.wait(lk, [&] { return S->queue.empty() && S->running.empty(); });
+  return TB_OK;
+}
+
+static double percentile(std::vector<double> v, double q) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const double pos = q * (v.size() - 1);
+  const size_t i = (size_t)pos;
+  const double f = pos - i;
+  return i + 1 < v.size() ? v[i] * (1 - f) + v[i + 1] * f : v[i];
+}
+
+tb_status tb_server_get_stats(tb_server* S, tb_server_stats* out) {
+  if (!S || !out) return TB_EINVAL;
+  std::lock_guard<std::mutex> lk(S->mu);
+  tb_server_stats st{};
+  st.submitted = (long long)S->all.size();
+  st.completed = S->completed;
+  st.failed = S->failed;
+  st.running = (long long)S->running.size();
+  st.queued = (long long)S->queue.size();
+  st.elapsed_ms = S->first_submit >= 0 ? S->last_done - S->first_submit : 0.0;
+  st.solves_per_s = st.elapsed_ms > 0 ? S->completed / (st.elapsed_ms / 1e3) : 0.0;
+  st.steps_per_s = st.elapsed_ms > 0 ? S->steps_done / (st.elapsed_ms / 1e3) : 0.0;
+  st.p50_ms = percentile(S->tts, 0.50);
+  st.p99_ms = percentile(S->tts, 0.99);
+  double w = 0;
+  for (double x : S->waits) w += x;
+  st.mean_wait_ms = S->waits.empty() ? 0.0 : w / S->waits.size();
+  st.peak_bytes = S->peak;
+  st.budget_bytes = S->budget;
+  st.peak_running = S->peak_running;
+  *out = st;
+  return TB_OK;
+}
+
+tb_status tb_server_destroy(tb_server* S) {
+  if (!S) return TB_EINVAL;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+    S->cv.notify_all();
+  }
+  if (S->worker.joinable()) S->worker.join();
+  delete S;
+  return TB_OK;
+}
+
+}  // extern "C"

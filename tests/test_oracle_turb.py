@@ -1,0 +1,72 @@
+"""Known answers of the oracle's doubly periodic turbulence restatement
+(examples/2d_decaying_turbulence_gpu.jl; nonlinear_padding.jl;
+step_diagonal_imex.jl).  CPU only."""
+import numpy as np
+
+from oracle.tarang_oracle import (
+    padded_multiply_2d,
+    run_turb,
+    turb_backward,
+    turb_forward,
+    turb_initial_spec,
+    turb_rhs,
+    turb_wavenumbers,
+)
+
+
+def grid(Nx, Ny):
+    x = np.arange(Nx) * 2 * np.pi / Nx
+    y = np.arange(Ny) * 2 * np.pi / Ny
+    return np.meshgrid(x, y)
+
+
+def test_transform_round_trip():
+    rng = np.random.default_rng(0)
+    g = rng.standard_normal((12, 16))
+    assert np.abs(turb_backward(turb_forward(g), 16) - g).max() < 1e-13
+
+
+def test_resolved_product_is_pointwise():
+    X, Y = grid(16, 12)
+    a = np.cos(2 * X) * np.sin(Y)
+    b = np.sin(3 * X + 1) * np.cos(2 * Y)
+    assert np.abs(padded_multiply_2d(a, b) - a * b).max() < 1e-13
+
+
+def test_nyquist_modes_keep_full_amplitude():
+    # the reason for the symmetric split/fold (nonlinear_padding.jl:182-190):
+    # a Nyquist mode times 1 comes back at full amplitude along either axis
+    X, Y = grid(16, 12)
+    for a in (np.cos(8 * X) * np.cos(2 * Y), np.cos(2 * X) * np.cos(6 * Y), np.cos(8 * X) * np.cos(6 * Y)):
+        assert np.abs(padded_multiply_2d(a, np.ones_like(a)) - a).max() < 1e-13
+
+
+def test_single_mode_is_steady_under_advection():
+    # psi ~ q for a single wavenumber shell: u.grad q = 0
+    Nx, Ny = 32, 32
+    X, Y = grid(Nx, Ny)
+    q = turb_forward(np.cos(3 * X + 4 * Y))
+    F = turb_rhs(q, Nx, 2 * np.pi, 2 * np.pi)
+    assert np.abs(F).max() < 1e-10 * np.abs(q).max()
+
+
+def test_sbdf_startup_and_viscous_decay():
+    Nx, Ny, nu, dt = 16, 16, 0.05, 0.1
+    X, Y = grid(Nx, Ny)
+    q0 = turb_forward(np.cos(2 * X + Y))
+    k2 = 5.0
+    q1 = run_turb(q0, Nx, 2 * np.pi, 2 * np.pi, nu, dt, 1)
+    assert np.abs(q1 - q0 / (1 + dt * nu * k2)).max() < 1e-12 * np.abs(q0).max()
+    # SBDF2: q_{n+1} (3/2 + dt L) = 2 q_n - q_{n-1}/2 for a steady mode
+    q2 = run_turb(q0, Nx, 2 * np.pi, 2 * np.pi, nu, dt, 2)
+    want = (2 * q1 - 0.5 * q0) / (1.5 + dt * nu * k2)
+    assert np.abs(q2 - want).max() < 1e-12 * np.abs(q0).max()
+
+
+def test_initial_spectrum_is_seeded_and_scaled():
+    a = turb_initial_spec(32, 32, 3)
+    b = turb_initial_spec(32, 32, 3)
+    assert np.array_equal(a, b)
+    assert abs(np.abs(turb_backward(a, 32)).max() - 10.0) < 1e-12
+    kx, ky = turb_wavenumbers(32, 32, 2 * np.pi, 2 * np.pi)
+    assert np.abs(a[np.sqrt(kx ** 2 + ky ** 2) > 32 / 3.0 + 1e-9]).max() < 1e-9
