@@ -45,9 +45,12 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["rbc", "ensemble"], default="rbc",
-                    help="rbc: the single-instance step (headline); ensemble: the batched ensemble alone")
+    ap.add_argument("--workload", choices=["rbc", "ensemble", "serving"], default="rbc",
+                    help="rbc: the single-instance step (headline); ensemble / serving: that workload alone")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble summary in the rbc line")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving summary in the rbc line")
+    ap.add_argument("--serve-requests", type=int, default=60)
+    ap.add_argument("--serve-budget-gb", type=float, default=40.0)
     ap.add_argument("--ensemble-size", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=100)
     return ap.parse_args()
@@ -429,6 +432,11 @@ def run_ours(args, cfg, scheme, dist):
                 out["ensemble"] = run_ensemble(args, dev)
             except Exception as exc:  # reported, never fatal to the headline line
                 out["ensemble"] = {"error": f"{type(exc).__name__}: {exc}"}
+        if dist.world == 1 and not args.no_serving:
+            try:
+                out["serving"] = run_serving(args, dev)
+            except Exception as exc:  # reported, never fatal to the headline line
+                out["serving"] = {"error": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(out), flush=True)
 
 
@@ -510,6 +518,85 @@ def run_ensemble(args, dev):
     }
 
 
+def run_serving(args, dev):
+    """Serving mix: seeded Poisson arrivals (20/s) of RBC channel runs and FP32
+    decaying turbulence, 50-500 steps each, admitted by HBM budget.  Replayed
+    through the request server (continuous batching) and through the plain GPU
+    form (one request at a time); also the saturated throughput with every
+    request queued at once."""
+    import numpy as np
+
+    from __graft_entry__ import load_package
+
+    tb = load_package()
+    from tarang_b200 import workloads as W
+
+    reqs = W.serving_requests(args.serve_requests)
+    prepared = []
+    for r in reqs:
+        if r.kind == "rbc":
+            c = r.rbc
+            prepared.append((tb.rbc_desc(c.Nx, c.Nz, c.kappa, c.nu, 0, Lx=c.Lx, Lz=c.Lz), r.dt, r.nsteps,
+                             W.rbc_initial_grid(c)))
+        else:
+            prepared.append((tb.turb_desc(r.N, r.N, r.nu), r.dt, r.nsteps, W.turb_initial_spec(r.N, r.seed)))
+    budget = int(args.serve_budget_gb * (1 << 30))
+
+    def replay(max_running, timed_arrivals, chunk=10, subset=None):
+        srv = tb.Server(budget_bytes=budget, max_running=max_running, chunk_steps=chunk, device=dev)
+        t0 = time.perf_counter()
+        ids = []
+        for k, (r, (d, dt, n, init)) in enumerate(zip(reqs, prepared)):
+            if subset is not None and k not in subset:
+                continue
+            if timed_arrivals:
+                wait = r.arrival_s - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+            ids.append(srv.submit(d, dt, n, init))
+        srv.wait_all()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        ok = all(srv.poll(i)[0] == tb._lib.TB_REQ_DONE for i in ids)
+        srv.close()
+        return {"solves_per_s": st["solves_per_s"], "steps_per_s": st["steps_per_s"],
+                "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_queue_wait_ms": st["mean_wait_ms"],
+                "peak_running": st["peak_running"], "peak_budgeted_bytes": st["peak_bytes"],
+                "completed": st["completed"], "failed": st["failed"], "wall_s": wall, "all_done": ok}
+
+    # warm-up: one request of every kind and size (kernel loading, first-use costs)
+    seen, warm = set(), []
+    for k, r in enumerate(reqs):
+        key = (r.kind, r.rbc.Nx if r.rbc else r.N)
+        if key not in seen:
+            seen.add(key)
+            warm.append(k)
+    replay(8, False, subset=set(warm))
+    # continuous batching: up to 16 requests in flight, chunks of 10 steps;
+    # plain GPU form: one request at a time, chunks of 50 steps
+    served = replay(16, True)
+    plain = replay(1, True, chunk=50)
+    sat = replay(16, False)
+    sat_plain = replay(1, False, chunk=50)
+    kinds = {"rbc": sum(r.kind == "rbc" for r in reqs), "turb": sum(r.kind == "turb" for r in reqs)}
+    return {
+        "metric": "serving solves/s and time to solution (Poisson 20/s replay)",
+        "value": served["solves_per_s"],
+        "unit": "requests/s",
+        "requests": len(reqs),
+        "mix": kinds,
+        "hbm_budget_bytes": budget,
+        "replay": served,
+        "plain_gpu_replay": plain,
+        "saturated": sat,
+        "plain_gpu_saturated": sat_plain,
+        "saturated_speedup_vs_plain_gpu": sat["solves_per_s"] / max(sat_plain["solves_per_s"], 1e-30),
+        "dtype": {"rbc": "f64", "turbulence": "f32"},
+        "data": "synthetic: seeded arrivals (seed 11), sizes and parameters; RBC noise seed 5000+k, "
+                "turbulence k^-3 spectrum seed 7000+k",
+    }
+
+
 _FP64_PEAK = None
 
 
@@ -561,6 +648,9 @@ def main():
         elif args.workload == "ensemble":
             if dist.rank == 0:
                 print(json.dumps(run_ensemble(args, dist.local)), flush=True)
+        elif args.workload == "serving":
+            if dist.rank == 0:
+                print(json.dumps(run_serving(args, dist.local)), flush=True)
         else:
             run_ours(args, cfg, scheme, dist)
     finally:

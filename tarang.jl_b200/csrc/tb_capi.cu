@@ -496,12 +496,14 @@ void tb::plan_launch_steps(tb_plan* P, double dt, int nsteps, cudaStream_t s, in
           enqueue_sbdf_step(P, dt, kind);
       }
       check_launch("profiled step");
-    } else if (chunk == 1) {
+    } else if (chunk < graph_steps || chunk == 1) {
+      // single steps (also for a partial last chunk, so the graph of
+      // graph_steps steps is kept)
       if (!(P->gexec && P->graph_dt == dt && P->graph_kind == kind)) {
         TB_CUDA_TRY(cudaStreamSynchronize(P->st));
         capture_step(P, dt, kind);
       }
-      TB_CUDA_TRY(cudaGraphLaunch(P->gexec, s));
+      for (int i = 0; i < chunk; ++i) TB_CUDA_TRY(cudaGraphLaunch(P->gexec, s));
     } else {
       StepGraph& mg = P->multi;
       if (!(mg.exec && mg.dt == dt && mg.kind == kind && mg.steps == chunk)) {
@@ -517,6 +519,25 @@ void tb::plan_launch_steps(tb_plan* P, double dt, int nsteps, cudaStream_t s, in
     }
     advance_counters(P, dt, kind, chunk);
     left -= chunk;
+  }
+}
+
+void tb::plan_prepare(tb_plan* P, double dt, int graph_steps) {
+  TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
+  const int kind = plan_next_kind(P);
+  prepare_kind(P, dt, kind);
+  TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  if (!(P->gexec && P->graph_dt == dt && P->graph_kind == kind)) capture_step(P, dt, kind);
+  const bool uniform = !(P->d.timestepper == TB_SBDF2 && kind == 1);
+  if (uniform && graph_steps > 1) {
+    StepGraph& mg = P->multi;
+    if (!(mg.exec && mg.dt == dt && mg.kind == kind && mg.steps == graph_steps)) {
+      if (mg.exec) cudaGraphExecDestroy(mg.exec);
+      mg.exec = capture_steps(P, dt, kind, graph_steps);
+      mg.dt = dt;
+      mg.kind = kind;
+      mg.steps = graph_steps;
+    }
   }
 }
 

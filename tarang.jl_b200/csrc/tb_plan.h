@@ -161,6 +161,9 @@ int plan_next_kind(const tb_plan* P);
 // cached CUDA graphs of up to graph_steps steps; factors and graphs are built
 // on first use of a (dt, kind).  Returns without waiting for the GPU.
 void plan_launch_steps(tb_plan* P, double dt, int nsteps, cudaStream_t s, int graph_steps);
+// Factors and step graphs for the next steps at dt, built ahead of the first
+// launch (so that a caller can overlap this host work with other plans' steps).
+void plan_prepare(tb_plan* P, double dt, int graph_steps);
 // Snapshot / restore of the stepping state (X, history, counters) in device scratch.
 struct PlanSnapshot {
   DevBuf X, Fprev, MXprev;

@@ -33,6 +33,8 @@ using namespace tb;
 
 namespace {
 
+constexpr int kSetupThreads = 4;  // host threads building admitted requests' plans
+
 double now_ms() {
   using namespace std::chrono;
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
@@ -47,6 +49,8 @@ struct Job {
   virtual int nfields() const = 0;
   virtual size_t field_doubles(int field) const = 0;
   virtual void fetch(int field, double* host) = 0;
+  // factors and step graphs built before the first launch
+  virtual void prepare(double dt, int chunk) = 0;
 };
 
 struct RbcJob : Job {
@@ -63,6 +67,7 @@ struct RbcJob : Job {
     TB_CUDA_TRY(cudaMemcpyAsync(host, P->Xp(field), P->plane * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
     TB_CUDA_TRY(cudaStreamSynchronize(P->st));
   }
+  void prepare(double dt, int chunk) override { plan_prepare(P, dt, chunk); }
 };
 
 struct TurbJob : Job {
@@ -76,6 +81,7 @@ struct TurbJob : Job {
   int nfields() const override { return 1; }  // vorticity coefficients
   size_t field_doubles(int) const override { return turb_field_doubles(T); }
   void fetch(int, double* host) override { turb_fetch(T, host); }
+  void prepare(double dt, int) override { turb_prepare(T, dt); }
 };
 
 // Device bytes a run of this size will hold (plan, factors, graphs' scratch).
@@ -113,8 +119,17 @@ struct tb_server {
   int max_running = 1, chunk = 1;
   std::mutex mu;
   std::condition_variable cv;
-  std::deque<Request*> queue;
+  std::deque<Request*> queue;     // submitted, not admitted
+  std::deque<Request*> setupq;    // admitted, waiting for a setup thread
+  int setting_up = 0;             // admitted, plan being built
   std::vector<Request*> running;
+  std::condition_variable setup_cv;
+  std::vector<std::thread> setup_workers;
+  // Finished jobs keep their device memory until the budget needs it or the
+  // server is idle: cudaFree waits for the whole device, so releasing memory
+  // while other requests run would stall them all.
+  std::vector<std::unique_ptr<Job>> zombies;
+  size_t zombie_bytes = 0;
   std::map<long long, std::unique_ptr<Request>> all;
   long long next_id = 1;
   bool stop = false;
@@ -127,8 +142,11 @@ struct tb_server {
   std::vector<double> tts, waits;
 
   void loop();
+  void setup_loop();
   void admit();
   void progress();
+  bool idle_locked() const { return queue.empty() && setupq.empty() && setting_up == 0 && running.empty(); }
+  void release_zombies();
   void fail_admitted(Request* r, const std::string& msg);
   void fail_running(Request* r, const std::string& msg);
 };
@@ -160,38 +178,74 @@ std::unique_ptr<Job> make_job(tb_context* ctx, const Request& r) {
 
 }  // namespace
 
+// Admission: in arrival order, while the head's estimated bytes fit the
+// remaining budget and a run slot is free; the plan is built by a setup
+// thread so that host-side construction overlaps the steps of running requests.
 void tb_server::admit() {
+  std::lock_guard<std::mutex> lk(mu);
+  while (!queue.empty() && (int)running.size() + setting_up + (int)setupq.size() < max_running) {
+    Request* h = queue.front();
+    if (h->bytes > budget) {  // can never fit
+      queue.pop_front();
+      h->state = TB_REQ_FAILED;
+      h->error = "request needs more device memory than the server budget";
+      ++failed;
+      cv.notify_all();
+      continue;
+    }
+    if (used + zombie_bytes + h->bytes > budget) {
+      if (zombie_bytes == 0 || used + h->bytes > budget) return;  // wait for memory (arrival order)
+      release_zombies();  // the finished jobs' memory makes room
+      continue;
+    }
+    queue.pop_front();
+    used += h->bytes;
+    peak = std::max(peak, used);
+    setupq.push_back(h);
+    setup_cv.notify_one();
+  }
+}
+
+// (mu held)
+void tb_server::release_zombies() {
+  zombies.clear();
+  zombie_bytes = 0;
+}
+
+void tb_server::setup_loop() {
+  cudaSetDevice(ctx->device);
   while (true) {
     Request* r = nullptr;
     {
-      std::lock_guard<std::mutex> lk(mu);
-      if (queue.empty() || (int)running.size() >= max_running) return;
-      Request* h = queue.front();
-      if (h->bytes > budget) {  // can never fit
-        queue.pop_front();
-        h->state = TB_REQ_FAILED;
-        h->error = "request needs more device memory than the server budget";
-        ++failed;
-        cv.notify_all();
-        continue;
-      }
-      if (used + h->bytes > budget) return;  // wait for memory to free up (arrival order)
-      queue.pop_front();
-      r = h;
-      used += r->bytes;
-      peak = std::max(peak, used);
+      std::unique_lock<std::mutex> lk(mu);
+      // leave only when stopping with nothing left to admit, build or free
+      setup_cv.wait(lk, [&] { return !setupq.empty() || (stop && queue.empty()); });
+      if (setupq.empty()) return;
+      r = setupq.front();
+      setupq.pop_front();
+      ++setting_up;
     }
     try {
       r->t_start = now_ms();
       r->job = make_job(ctx, *r);
+      r->job->prepare(r->dt, chunk);
       TB_CUDA_TRY(cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming));
       std::lock_guard<std::mutex> lk(mu);
+      --setting_up;
       r->state = TB_REQ_RUNNING;
       running.push_back(r);
       peak_running = std::max(peak_running, (int)running.size());
     } catch (const Error& e) {
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        --setting_up;
+      }
       fail_admitted(r, e.msg);
     } catch (const std::exception& e) {
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        --setting_up;
+      }
       fail_admitted(r, e.what());
     }
   }
@@ -238,14 +292,15 @@ void tb_server::progress() {
         r->result[f].resize(r->job->field_doubles(f));
         r->job->fetch(f, r->result[f].data());
       }
-      r->job.reset();
       cudaEventDestroy(r->ev);
       r->ev = nullptr;
       std::lock_guard<std::mutex> lk(mu);
+      zombies.push_back(std::move(r->job));
+      zombie_bytes += r->bytes;
+      used -= r->bytes;
       r->t_done = now_ms();
       r->state = TB_REQ_DONE;
       running.erase(std::find(running.begin(), running.end(), r));
-      used -= r->bytes;
       ++completed;
       steps_done += r->nsteps;
       last_done = r->t_done;
@@ -278,9 +333,10 @@ void tb_server::loop() {
   while (true) {
     {
       std::unique_lock<std::mutex> lk(mu);
-      if (stop && queue.empty() && running.empty()) return;
+      if (idle_locked() && !zombies.empty()) release_zombies();  // nothing runs: free now
+      if (stop && idle_locked()) return;
       if (queue.empty() && running.empty()) {
-        cv.wait_for(lk, std::chrono::milliseconds(2));
+        cv.wait_for(lk, std::chrono::milliseconds(1));
         continue;
       }
     }
@@ -303,6 +359,7 @@ tb_status tb_server_create(tb_context* ctx, size_t budget_bytes, int max_running
     S->chunk = chunk_steps;
     tb_server* raw = S.get();
     S->worker = std::thread([raw] { raw->loop(); });
+    for (int i = 0; i < kSetupThreads; ++i) S->setup_workers.emplace_back([raw] { raw->setup_loop(); });
     *out = S.release();
   });
 }
@@ -358,7 +415,7 @@ tb_status tb_server_result(tb_server* S, long long id, int field, double* host_o
 tb_status tb_server_wait_all(tb_server* S) {
   if (!S) return TB_EINVAL;
   std::unique_lock<std::mutex> lk(S->mu);
-  S->cv.wait(lk, [&] { return S->queue.empty() && S->running.empty(); });
+  S->cv.wait(lk, [&] { return S->idle_locked(); });
   return TB_OK;
 }
 
@@ -402,7 +459,13 @@ tb_status tb_server_destroy(tb_server* S) {
     S->stop = true;
     S->cv.notify_all();
   }
-  if (S->worker.joinable()) S->worker.join();
+  if (S->worker.joinable()) S->worker.join();  // drains every admitted request first
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->setup_cv.notify_all();
+  }
+  for (auto& t : S->setup_workers)
+    if (t.joinable()) t.join();
   delete S;
   return TB_OK;
 }

@@ -52,6 +52,13 @@ __device__ __forceinline__ double* bwd_record(double* BR, int npad, int m, int j
 // eliminated alongside as a dense border and leave an nb x nb Schur
 // complement, inverted explicitly.
 // ---------------------------------------------------------------------------
+// Strided view of a thread's work array in interleaved scratch.
+struct Strided {
+  double* p;
+  size_t s;
+  __device__ __forceinline__ double& operator[](size_t i) const { return p[i * s]; }
+};
+
 template <int KL, int KU>
 __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -64,11 +71,13 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
   const int Nk = a.Nk;
   const double kx = a.k0 * m;
   const bool zmode = (m == 0);
-  const size_t per = (size_t)nmax * WW + (size_t)nmax * NBMAX + (size_t)NBMAX * nmax + NBMAX * NBMAX;
-  double* W = a.scratch + ((size_t)c * Nk + m) * per;
-  double* Bd = W + (size_t)nmax * WW;
-  double* Cr = Bd + (size_t)nmax * NBMAX;
-  double* C1 = Cr + (size_t)NBMAX * nmax;
+  // per-thread work arrays interleaved across the 2 Nk threads (element i of a
+  // thread at scratch[i * 2Nk + t]) so that a warp's accesses coalesce
+  const size_t T = (size_t)2 * Nk, t = (size_t)c * Nk + m;
+  const Strided W{a.scratch + t, T};
+  const Strided Bd{a.scratch + t + (size_t)nmax * WW * T, T};
+  const Strided Cr{a.scratch + t + ((size_t)nmax * WW + (size_t)nmax * NBMAX) * T, T};
+  const Strided C1{a.scratch + t + ((size_t)nmax * WW + 2 * (size_t)nmax * NBMAX) * T, T};
   const int cw = C.kl + C.ku + 1;
   for (int r = 0; r < n; ++r) {
     for (int d = 0; d < WW; ++d) W[(size_t)r * WW + d] = 0.0;
@@ -656,10 +665,11 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Partition responses of the solve, one thread per (mode, class), from the
-// factor records (the arithmetic of the sweeps in k_tau_solve).  Partition k
-// owns rows [k Lp, (k+1) Lp).  For k >= 1 (forward, started from unit pending
-// entry i of the window and a zero right-hand side):
+// Partition responses of the solve, one thread per (mode, class, partition,
+// unit vector), from the factor records (the arithmetic of the sweeps in
+// k_tau_solve).  Partition k owns rows [k Lp, (k+1) Lp).  For k >= 1
+// (forward, started from unit pending entry i of the window and a zero
+// right-hand side):
 //   G of row j (backward record slots kBwdG..) = y_j,
 //   Phi_k[o][i] = exit pending entry o,  Gz_k[b][i] = border accumulator b.
 // For k <= P-2 (backward from unit window entry i, row (k+1) Lp + i, with zero
@@ -667,69 +677,71 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 //   H of row j (H record) = x_j,  Psi_k[o][i] = x of row k Lp + o.
 // ---------------------------------------------------------------------------
 template <int KL, int KU, int P>
-__global__ void __launch_bounds__(64) k_tau_transfer(TauArgs a) {
+__global__ void __launch_bounds__(128) k_tau_transfer(TauArgs a) {
+  // one thread per (mode, class, partition, unit): forward unit i < 4,
+  // backward unit i - 4 < 12
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  const int c = blockIdx.y;
+  const int c = blockIdx.y & 1, k = blockIdx.y >> 1;
+  const int i = blockIdx.z;
   if (m >= a.Nk) return;
   const int np = a.npad, Lp = np / P;
   const int g = m / kSolveModes, mm = m % kSolveModes;
-  for (int k = 0; k < P; ++k) {
-    // Phi, Gz, Psi exist only for P > 1 (a.PP is null otherwise)
-    double* tr = P > 1 ? a.PP + ((((size_t)g * P + k) * 2 + c) * kSolveModes + mm) * kTransfer : nullptr;
-    const int r0 = k * Lp, r1 = (k + 1) * Lp;
-    if (k >= 1) {
-      for (int i = 0; i < 4; ++i) {
-        double y[kFwdWin], z[NBMAX] = {0.0, 0.0, 0.0, 0.0};
-        for (int t = 0; t < kFwdWin; ++t) y[t] = (t == i) ? 1.0 : 0.0;
-        for (int j = r0; j < r1; ++j) {
-          const double* fr = fwd_record(a.cls[0].FR, np, m, j, c);
-          const int u = (j - r0) % kFwdWin;
-          const int p = __double2loint(fr[0]);
-          double yj = y[u];
-          for (int t = 1; t <= KL; ++t) {
-            if (t == p) {
-              const double yt = y[(u + t) % kFwdWin];
-              y[(u + t) % kFwdWin] = yj;
-              yj = yt;
-            }
-          }
-          bwd_record(a.cls[0].BR, np, m, j, c)[kBwdG + i] = yj;
-          for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-fr[t], yj, y[(u + t) % kFwdWin]);
-          for (int b = 0; b < NBMAX; ++b) z[b] = fma(-fr[1 + KL + b], yj, z[b]);
-          y[u] = 0.0;
+  // Phi, Gz, Psi exist only for P > 1 (a.PP is null otherwise)
+  double* tr = P > 1 ? a.PP + ((((size_t)g * P + k) * 2 + c) * kSolveModes + mm) * kTransfer : nullptr;
+  const int r0 = k * Lp, r1 = (k + 1) * Lp;
+  if (i < 4) {
+    if (k < 1) return;
+    double y[kFwdWin], z[NBMAX] = {0.0, 0.0, 0.0, 0.0};
+    for (int t = 0; t < kFwdWin; ++t) y[t] = (t == i) ? 1.0 : 0.0;
+    for (int j = r0; j < r1; ++j) {
+      const double* fr = fwd_record(a.cls[0].FR, np, m, j, c);
+      const int u = (j - r0) % kFwdWin;
+      const int p = __double2loint(fr[0]);
+      double yj = y[u];
+      for (int t = 1; t <= KL; ++t) {
+        if (t == p) {
+          const double yt = y[(u + t) % kFwdWin];
+          y[(u + t) % kFwdWin] = yj;
+          yj = yt;
         }
-        for (int o = 0; o < 4; ++o) tr[kTrPhi + o * 4 + i] = y[o];
-        for (int b = 0; b < NBMAX; ++b) tr[kTrGz + b * 4 + i] = z[b];
       }
+      bwd_record(a.cls[0].BR, np, m, j, c)[kBwdG + i] = yj;
+      for (int t = 1; t <= KL; ++t) y[(u + t) % kFwdWin] = fma(-fr[t], yj, y[(u + t) % kFwdWin]);
+      for (int b = 0; b < NBMAX; ++b) z[b] = fma(-fr[1 + KL + b], yj, z[b]);
+      y[u] = 0.0;
     }
-    if (k == P - 1) {
-      // the last partition's unknowns need no correction: zero H, store codes only
-      for (int j = r0; j < r1; ++j) {
-        double* hr = a.HR + ((((size_t)g * np + j) * 2 + c) * kSolveModes + mm) * kHRec;
-        for (int i = 0; i < kBwdWin; ++i) hr[i] = 0.0;
+    for (int o = 0; o < 4; ++o) tr[kTrPhi + o * 4 + i] = y[o];
+    for (int b = 0; b < NBMAX; ++b) tr[kTrGz + b * 4 + i] = z[b];
+    return;
+  }
+  const int ib = i - 4;
+  if (k == P - 1) {
+    // the last partition's unknowns need no correction: zero H, store codes
+    for (int j = r0; j < r1; ++j) {
+      double* hr = a.HR + ((((size_t)g * np + j) * 2 + c) * kSolveModes + mm) * kHRec;
+      hr[ib] = 0.0;
+      if (ib == 0) {
         hr[kBwdWin] = bwd_record(a.cls[0].BR, np, m, j, c)[kBwdCode];
         hr[kBwdWin + 1] = 0.0;
       }
-    } else {
-      for (int i = 0; i < kBwdWin; ++i) {
-        double xw[kBwdWin];
-        for (int t = 0; t < kBwdWin; ++t) xw[t] = (t == i) ? 1.0 : 0.0;
-        for (int j = r1 - 1; j >= r0; --j) {
-          const double* br = bwd_record(a.cls[0].BR, np, m, j, c);
-          double acc = 0.0;
-          for (int t = 1; t <= KL + KU; ++t) acc = fma(-br[t], xw[(j + t) % kBwdWin], acc);
-          xw[j % kBwdWin] = acc * br[0];
-          double* hr = a.HR + ((((size_t)g * np + j) * 2 + c) * kSolveModes + mm) * kHRec;
-          hr[i] = xw[j % kBwdWin];
-          if (i == 0) {
-            hr[kBwdWin] = br[kBwdCode];
-            hr[kBwdWin + 1] = 0.0;
-          }
-        }
-        for (int o = 0; o < kBwdWin; ++o) tr[kTrPsi + o * kBwdWin + i] = xw[o];
-      }
+    }
+    return;
+  }
+  double xw[kBwdWin];
+  for (int t = 0; t < kBwdWin; ++t) xw[t] = (t == ib) ? 1.0 : 0.0;
+  for (int j = r1 - 1; j >= r0; --j) {
+    const double* br = bwd_record(a.cls[0].BR, np, m, j, c);
+    double acc = 0.0;
+    for (int t = 1; t <= KL + KU; ++t) acc = fma(-br[t], xw[(j + t) % kBwdWin], acc);
+    xw[j % kBwdWin] = acc * br[0];
+    double* hr = a.HR + ((((size_t)g * np + j) * 2 + c) * kSolveModes + mm) * kHRec;
+    hr[ib] = xw[j % kBwdWin];
+    if (ib == 0) {
+      hr[kBwdWin] = br[kBwdCode];
+      hr[kBwdWin + 1] = 0.0;
     }
   }
+  for (int o = 0; o < kBwdWin; ++o) tr[kTrPsi + o * kBwdWin + ib] = xw[o];
 }
 
 template <int N>
@@ -891,10 +903,11 @@ void factor_impl(const TauArgs& a, int parts, cudaStream_t st) {
   int nmax = a.cls[0].n > a.cls[1].n ? a.cls[0].n : a.cls[1].n;
   dim3 grid((a.Nk + 63) / 64, 2);
   k_tau_factor<KL, KU><<<grid, 64, 0, st>>>(a, nmax);
+  const int tgx = (a.Nk + 127) / 128;
   if (parts == kTauParts)
-    k_tau_transfer<KL, KU, kTauParts><<<grid, 64, 0, st>>>(a);
+    k_tau_transfer<KL, KU, kTauParts><<<dim3(tgx, 2 * kTauParts, 16), 128, 0, st>>>(a);
   else
-    k_tau_transfer<KL, KU, 1><<<grid, 64, 0, st>>>(a);
+    k_tau_transfer<KL, KU, 1><<<dim3(tgx, 2, 16), 128, 0, st>>>(a);
 }
 
 template <int P>

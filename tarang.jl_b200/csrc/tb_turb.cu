@@ -404,23 +404,27 @@ void tb::turb_destroy(tb_turb* T) { delete T; }
 
 cudaStream_t tb::turb_stream(const tb_turb* T) { return T->st; }
 
+void tb::turb_prepare(tb_turb* T, double dt) {
+  if (T->graph_dt == dt) return;
+  TB_CUDA_TRY(cudaSetDevice(T->ctx->device));
+  TB_CUDA_TRY(cudaStreamSynchronize(T->st));
+  for (auto& e : T->g)
+    if (e) cudaGraphExecDestroy(e), e = nullptr;
+  const int keep = T->cur;
+  for (int c = 0; c < 2; ++c) {
+    T->cur = c;
+    T->g[c] = capture(T, dt);
+  }
+  T->cur = keep;
+  T->graph_dt = dt;
+}
+
 void tb::turb_launch_steps(tb_turb* T, double dt, int steps) {
   for (int i = 0; i < steps; ++i) {
     if (T->iteration == 0) {
       enqueue_step(T, dt, 1);
     } else {
-      if (T->graph_dt != dt) {
-        TB_CUDA_TRY(cudaStreamSynchronize(T->st));
-        for (auto& e : T->g)
-          if (e) cudaGraphExecDestroy(e), e = nullptr;
-        const int keep = T->cur;
-        for (int c = 0; c < 2; ++c) {
-          T->cur = c;
-          T->g[c] = capture(T, dt);
-        }
-        T->cur = keep;
-        T->graph_dt = dt;
-      }
+      turb_prepare(T, dt);
       TB_CUDA_TRY(cudaGraphLaunch(T->g[T->cur], T->st));
     }
     const cudaError_t e = cudaGetLastError();

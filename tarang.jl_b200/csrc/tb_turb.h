@@ -17,6 +17,8 @@ void turb_destroy(tb_turb* T);
 cudaStream_t turb_stream(const tb_turb* T);
 // Enqueue steps on the plan's stream (returns without waiting).
 void turb_launch_steps(tb_turb* T, double dt, int steps);
+// Step graphs for dt, built ahead of the first launch.
+void turb_prepare(tb_turb* T, double dt);
 size_t turb_device_bytes(const tb_turb* T);
 size_t turb_field_doubles(const tb_turb* T);
 // Vorticity coefficients to host, complex128 (Nx/2+1, Ny), x fastest (waits).

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import math
 from dataclasses import dataclass
+from typing import Optional
 
 import numpy as np
 
@@ -128,3 +129,59 @@ def ensemble_members(n: int = 64, seed: int = 7, dt: float = 0.02, scheme: str =
         Pr = float(rng.uniform(0.7, 7.0))
         out.append(RBCConfig(Nx=Nx, Nz=Nz, Ra=Ra, Pr=Pr, dt=dt, scheme=scheme, seed=1000 + k))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Serving mix: Poisson arrivals of RBC channel runs and 2D decaying turbulence.
+# ---------------------------------------------------------------------------
+TURB_SIZES = (256, 512, 1024)
+
+
+@dataclass
+class ServeRequest:
+    kind: str          # "rbc" or "turb"
+    arrival_s: float   # arrival time from the start of the replay
+    nsteps: int
+    rbc: Optional[RBCConfig] = None
+    N: int = 0         # turbulence grid N x N
+    nu: float = 1e-4
+    dt: float = 2e-3
+    seed: int = 0
+
+
+def serving_requests(n: int = 60, seed: int = 11, rate: float = 20.0, rbc_frac: float = 0.7):
+    """Seeded Poisson arrivals (mean `rate` per second): 70 % RBC channel runs
+    with the ensemble's sizes and parameter ranges, 30 % FP32 decaying
+    turbulence N x N, N in TURB_SIZES (nu = 1e-4, dt = 2e-3, k^-3 spectrum with
+    a per-request seed); each request runs a uniform 50-500 steps."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        steps = int(rng.integers(50, 501))
+        if rng.uniform() < rbc_frac:
+            Nx, Nz = ENSEMBLE_SIZES[int(rng.integers(len(ENSEMBLE_SIZES)))]
+            Ra = float(10.0 ** rng.uniform(5.0, 8.0))
+            Pr = float(rng.uniform(0.7, 7.0))
+            cfg = RBCConfig(Nx=Nx, Nz=Nz, Ra=Ra, Pr=Pr, dt=0.02, scheme="RK222", seed=5000 + k)
+            out.append(ServeRequest("rbc", t, steps, rbc=cfg, dt=cfg.dt, seed=cfg.seed))
+        else:
+            N = TURB_SIZES[int(rng.integers(len(TURB_SIZES)))]
+            out.append(ServeRequest("turb", t, steps, N=N, seed=7000 + k))
+    return out
+
+
+def turb_initial_spec(N: int, seed: int, amp: float = 10.0) -> np.ndarray:
+    """Vorticity coefficients (N, N/2+1) with a k^-3 energy spectrum: |q^| ~ 1/k
+    per mode for 1 <= |k| <= N/3, random phases from PCG64(seed), scaled to
+    max |q| = amp on the grid (rfft along x, fft along y, unnormalised)."""
+    rng = np.random.default_rng(seed)
+    kx = np.arange(N // 2 + 1)[None, :]
+    ky = np.concatenate([np.arange(N // 2), np.arange(-(N // 2), 0)])[:, None]
+    k = np.sqrt(kx ** 2 + ky ** 2)
+    mag = np.where((k >= 1.0) & (k <= N / 3.0), 1.0 / np.maximum(k, 1e-30), 0.0)
+    phase = rng.uniform(0.0, 2 * np.pi, size=mag.shape)
+    g = np.fft.irfft(np.fft.ifft(mag * np.exp(1j * phase), axis=0), n=N, axis=1)
+    g *= amp / np.abs(g).max()
+    return np.fft.fft(np.fft.rfft(g, axis=1), axis=0)
