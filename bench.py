@@ -49,6 +49,7 @@ def parse_args():
                     help="rbc: the single-instance step (headline); ensemble / serving: that workload alone")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble summary in the rbc line")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving summary in the rbc line")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision summary in the rbc line")
     ap.add_argument("--serve-requests", type=int, default=60)
     ap.add_argument("--serve-budget-gb", type=float, default=40.0)
     ap.add_argument("--ensemble-size", type=int, default=64)
@@ -432,6 +433,11 @@ def run_ours(args, cfg, scheme, dist):
                 out["ensemble"] = run_ensemble(args, dev)
             except Exception as exc:  # reported, never fatal to the headline line
                 out["ensemble"] = {"error": f"{type(exc).__name__}: {exc}"}
+        if dist.world == 1 and not args.no_mixed:
+            try:
+                out["mixed"] = run_mixed(args, cfg, scheme, dev)
+            except Exception as exc:  # reported, never fatal to the headline line
+                out["mixed"] = {"error": f"{type(exc).__name__}: {exc}"}
         if dist.world == 1 and not args.no_serving:
             try:
                 out["serving"] = run_serving(args, dev)
@@ -515,6 +521,49 @@ def run_ensemble(args, dev):
         "speedup_vs_plain_gpu": (steps / (total / 1e3)) / (steps / plain_s),
         "finite": bool(finite),
         "data": "synthetic: sizes, Ra, Pr and noise seeded (ensemble seed 7, member noise seed 1000+k)",
+    }
+
+
+def run_mixed(args, cfg, scheme, dev):
+    """Mixed precision on the headline configuration: FP32 transforms and
+    products, FP64 tau LU, solves and stage algebra.  Steps/s (CUDA-graph
+    replay, device clock) and the relative L2 error of b, u_x, u_z after the
+    same number of steps against the Float64 form (which tracks the CPU oracle
+    to 1e-10)."""
+    import numpy as np
+    import torch
+
+    from __graft_entry__ import load_package
+
+    tb = load_package()
+    from tarang_b200 import workloads as W
+    from tarang_b200._lib import TB_PREC_MIXED
+
+    ts = {"RK222": 0, "RK443": 1, "SBDF2": 3}[scheme]
+    dom = tb.ChannelDomain(cfg.Nx, cfg.Nz, Lx=cfg.Lx, Lz=cfg.Lz, arch=tb.GPU(dev))
+    mixed = tb.Plan(dom, cfg.kappa, cfg.nu, cfg.Lz, 0.0, ts, precision=TB_PREC_MIXED)
+    full = tb.Plan(dom, cfg.kappa, cfg.nu, cfg.Lz, 0.0, ts)
+    b0 = full.forward(W.rbc_initial_grid(cfg))
+    for pl in (mixed, full):
+        pl.set_state(0, b0)
+    n = args.steps
+    mixed.step(cfg.dt, n)
+    full.step(cfg.dt, n)
+    err = {name: float(np.linalg.norm(mixed.get_state(f) - full.get_state(f)) / np.linalg.norm(full.get_state(f)))
+           for f, name in ((0, "b"), (1, "ux"), (2, "uz"))}
+    # timing: graph replay after warm-up, from the state reached above
+    mixed.step(cfg.dt, args.warmup)
+    torch.cuda.synchronize()
+    mixed.step(cfg.dt, n)
+    ms = mixed.last_step_ms()
+    return {
+        "metric": f"RBC 2D steps/s ({cfg.Nx}x{cfg.Nz}, {scheme}, FP32 transforms/products + FP64 tau LU)",
+        "value": n / (ms / 1e3),
+        "unit": "steps/s",
+        "ms_per_step": ms / n,
+        "rel_l2_vs_f64_after_steps": err,
+        "steps": n,
+        "dtype": "f32 transforms/products, f64 solves/stage algebra",
     }
 
 

@@ -262,7 +262,61 @@ FactorSet* get_factors(tb_plan* P, double alpha, double beta) {
 }
 
 // F = -(u.grad) f in C^(2) rows (sfwd) or T coefficients (fwd) for f = b, ux, uz.
+// Mixed precision: the same RHS program on FP32 data; F is written in FP64.
+void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
+  const int N = P->Nz, H = P->Hz;
+  const int ncol = 2 * P->Nk;
+  const size_t hplane = (size_t)H * P->Nk;
+  float2* X32 = P->X32.as<float2>();
+  float2* G = P->G32.as<float2>();
+  auto gp = [&](int f, int w) { return G + (size_t)(4 * f + w) * hplane; };
+  timed(P, "round_f32", [&] { launch_round_f32(Xin, X32, 3LL * (long long)P->plane, P->st); });
+  GemmBatch32 bt{};
+  int nb = 0;
+  for (int f = 0; f < 3; ++f) {
+    const float* in = reinterpret_cast<const float*>(X32 + (size_t)f * P->plane);
+    const float* Am[4] = {P->bEv32.as<float>(), P->bOv32.as<float>(), P->bEd32.as<float>(), P->bOd32.as<float>()};
+    for (int w = 0; w < 4; ++w)
+      bt.item[nb++] = GemmItem32{Am[w], in, gp(f, w), H, (w & 1) ? P->Ko : P->Ke, pad16k((w & 1) ? P->Ko : P->Ke),
+                                 GEMM_PARITY, w & 1};
+  }
+  timed(P, "z_backward_gemm", [&] { launch_gemm_f32(bt, nb, ncol, ncol, ncol, N, false, P->st); });
+  XProdArgs32 xa{};
+  for (int f = 0; f < 3; ++f) {
+    xa.ev[f] = gp(f, 0);
+    xa.ov[f] = gp(f, 1);
+    xa.ed[f] = gp(f, 2);
+    xa.od[f] = gp(f, 3);
+    xa.out[f] = P->H32.as<float2>() + (size_t)f * P->plane;
+  }
+  xa.ptw = P->ptwM32.as<float2>();
+  xa.nptw = (int)(P->ptwM32.bytes / sizeof(float2));
+  xa.fp = P->fpM;
+  xa.Nx = P->Nx;
+  xa.Nk = P->Nk;
+  xa.M = P->M;
+  xa.Nz = N;
+  xa.k0 = (float)P->k0;
+  timed(P, "x_fft_products", [&] { launch_xprod32(xa, P->st); });
+  GemmBatch32 bf{};
+  nb = 0;
+  for (int f = 0; f < 3; ++f) {
+    const float* in = reinterpret_cast<const float*>(P->H32.as<float2>() + (size_t)f * P->plane);
+    double* out = reinterpret_cast<double*>(out3 + (size_t)f * P->plane);
+    bf.item[nb++] = GemmItem32{c2rows ? P->sfE32.as<float>() : P->fE32.as<float>(), in, out, P->Ke, H, pad16k(H),
+                               GEMM_MIRROR, 0};
+    if (P->Ko > 0)
+      bf.item[nb++] = GemmItem32{c2rows ? P->sfO32.as<float>() : P->fO32.as<float>(), in, out, P->Ko, H, pad16k(H),
+                                 GEMM_MIRROR, 1};
+  }
+  timed(P, "z_forward_gemm", [&] { launch_gemm_f32(bf, nb, ncol, ncol, ncol, N, true, P->st); });
+}
+
 void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
+  if (P->mixed) {
+    enqueue_rhs_mixed(P, Xin, out3, c2rows);
+    return;
+  }
   const int N = P->Nz, H = P->Hz;
   const int ncol = 2 * P->Nk;
   const size_t hplane = (size_t)H * P->Nk;
@@ -555,6 +609,9 @@ size_t tb::plan_device_bytes(const tb_plan* P) {
     for (const DevBuf* d : tb_) b += d->bytes;
   }
   for (const auto& f : P->factors) b += f->FR.bytes + f->BR.bytes + f->SI.bytes + f->PP.bytes + f->HR.bytes;
+  const DevBuf* m32[] = {&P->X32,  &P->G32,  &P->H32,  &P->bEv32, &P->bOv32, &P->bEd32,
+                         &P->bOd32, &P->fE32, &P->fO32, &P->sfE32, &P->sfO32, &P->ptwM32};
+  for (const DevBuf* d : m32) b += d->bytes;
   return b;
 }
 
@@ -596,7 +653,7 @@ void validate_desc(const tb_problem_desc* d) {
   TB_REQUIRE(d->Lx > 0 && d->Lz > 0, TB_EINVAL, "domain lengths must be positive");
   TB_REQUIRE(std::fabs(d->dealias - 1.5) < 1e-12, TB_ENOTSUPPORTED, "only dealias = 3/2 is implemented");
   TB_REQUIRE(d->timestepper >= TB_RK222 && d->timestepper <= TB_SBDF2, TB_EINVAL, "unknown timestepper");
-  TB_REQUIRE(d->precision == TB_PREC_F64, TB_ENOTSUPPORTED, "precision mode not implemented in this build");
+  TB_REQUIRE(d->precision == TB_PREC_F64 || d->precision == TB_PREC_MIXED, TB_EINVAL, "unknown precision mode");
   TB_REQUIRE(d->kappa > 0 && d->nu > 0, TB_EINVAL, "kappa and nu must be positive");
 }
 
@@ -718,6 +775,29 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
     upload(P->twM, twiddles(P->M));
     upload(P->ptwM, pass_twiddles(P->fpM));
     upload(P->twN, twiddles(P->Nx));
+    P->mixed = desc->precision == TB_PREC_MIXED;
+    if (P->mixed) {
+      auto f32 = [](const std::vector<double>& v) {
+        std::vector<float> o(v.size());
+        for (size_t i = 0; i < v.size(); ++i) o[i] = (float)v[i];
+        return o;
+      };
+      upload(P->bEv32, f32(cols_of(cm.bwd, 0)));
+      upload(P->bOv32, f32(cols_of(cm.bwd, 1)));
+      upload(P->bEd32, f32(cols_of(cm.bwd_d, 0)));
+      upload(P->bOd32, f32(cols_of(cm.bwd_d, 1)));
+      upload(P->fE32, f32(rows_of(cm.fwd, 0)));
+      upload(P->fO32, f32(rows_of(cm.fwd, 1)));
+      upload(P->sfE32, f32(rows_of(cm.sfwd, 0)));
+      upload(P->sfO32, f32(rows_of(cm.sfwd, 1)));
+      const std::vector<double2> pt = pass_twiddles(P->fpM);
+      std::vector<float2> pt32(pt.size());
+      for (size_t i = 0; i < pt.size(); ++i) pt32[i] = make_float2((float)pt[i].x, (float)pt[i].y);
+      upload(P->ptwM32, pt32);
+      TB_REQUIRE(xprod32_smem_bytes(P->M, (int)pt32.size()) <= 227 * 1024, TB_ENOTSUPPORTED,
+                 "Nx too large for the FP32 x kernel");
+      TB_CUDA_TRY(set_mixed_smem_limits(227 * 1024));
+    }
     // tau layout
     P->lay = build_rbc_layout(P->Nz, desc->Lx, desc->Lz, desc->kappa, desc->nu, (double)desc->Nx,
                               desc->b_bottom, desc->b_top);
@@ -781,6 +861,11 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
     P->tau.bytes = 7 * P->Nk * sizeof(double2);
     P->G.alloc(12 * (size_t)((P->Nz + 1) / 2) * P->Nk * sizeof(double2));
     P->H.alloc(3 * pb);
+    if (P->mixed) {
+      P->X32.alloc(3 * P->plane * sizeof(float2));
+      P->G32.alloc(12 * (size_t)((P->Nz + 1) / 2) * P->Nk * sizeof(float2));
+      P->H32.alloc(3 * P->plane * sizeof(float2));
+    }
     P->MX0.alloc(4 * pb);
     for (int i = 0; i < 4; ++i) {
       P->FP[i].alloc(4 * pb);

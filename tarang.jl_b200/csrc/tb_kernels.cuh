@@ -21,6 +21,35 @@ struct GemmBatch {
 };
 void launch_gemm_f64(const GemmBatch& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, cudaStream_t st);
 
+// FP32 twins for the mixed-precision RHS (same row maps; C is float or double).
+struct GemmItem32 {
+  const float* A;  // M x Kpad row-major, zero padded
+  const float* B;  // input rows (ldb floats apart; ldb even)
+  void* C;         // output rows (ldc elements)
+  int M, K, Kpad, mode, par;
+};
+struct GemmBatch32 {
+  GemmItem32 item[kGemmMaxBatch];
+};
+void launch_gemm_f32(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
+                     cudaStream_t st);
+void launch_round_f32(const double2* in, float2* out, long long n, cudaStream_t st);
+struct XProdArgs32 {
+  const float2* ev[3];
+  const float2* ov[3];
+  const float2* ed[3];
+  const float2* od[3];
+  float2* out[3];
+  const float2* ptw;  // per-pass FP32 twiddles of the length-M plan
+  int nptw;
+  FftPlan fp;
+  int Nx, Nk, M, Nz;
+  float k0;
+};
+void launch_xprod32(const XProdArgs32& a, cudaStream_t st);
+size_t xprod32_smem_bytes(int M, int nptw);
+cudaError_t set_mixed_smem_limits(int bytes);
+
 struct XProdArgs {
   // mixed-space inputs as even/odd Chebyshev half planes (ceil(Nz/2) x Nk
   // complex) of the values (ev, ov) and z-derivatives (ed, od) of b, ux, uz

@@ -125,6 +125,9 @@ struct tb_plan {
   tb::StepGraph multi;  // graph of several steps (asynchronous / batched stepping)
   int kernels_per_step = 0;
   int tau_parts = 1;  // partitions of the tau solve (kTauParts or 1)
+  // mixed precision (TB_PREC_MIXED): FP32 copies for the RHS program
+  bool mixed = false;
+  DevBuf X32, G32, H32, bEv32, bOv32, bEd32, bOd32, fE32, fO32, sfE32, sfO32, ptwM32;
   // profiling: eager launches bracketed by events, accumulated per kernel name
   bool profiling = false;
   struct ProfRec {
