@@ -45,13 +45,14 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["rbc", "ensemble", "serving"], default="rbc",
+    ap.add_argument("--workload", choices=["rbc", "ensemble", "serving", "turb"], default="rbc",
                     help="rbc: the single-instance step (headline); ensemble / serving: that workload alone")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble summary in the rbc line")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving summary in the rbc line")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision summary in the rbc line")
     ap.add_argument("--serve-requests", type=int, default=60)
     ap.add_argument("--serve-budget-gb", type=float, default=40.0)
+    ap.add_argument("--turb-n", type=int, default=1024)
     ap.add_argument("--ensemble-size", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=100)
     return ap.parse_args()
@@ -567,6 +568,32 @@ def run_mixed(args, cfg, scheme, dev):
     }
 
 
+def run_turb(args, dev):
+    """One FP32 decaying-turbulence instance (N x N, DiagonalIMEX SBDF2,
+    nu = 1e-4, dt = 2e-3, k^-3 initial spectrum): steps/s on the device clock."""
+    import torch
+
+    from __graft_entry__ import load_package
+
+    tb = load_package()
+    from tarang_b200 import workloads as W
+
+    N = args.turb_n
+    t = tb.Turb2D(N, N, 1e-4, W.turb_initial_spec(N, 7000), device=dev)
+    t.step(2e-3, args.warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    t.step(2e-3, args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"metric": f"2D decaying turbulence steps/s ({N}x{N}, FP32, DiagonalIMEX SBDF2)",
+            "value": args.steps / (ms / 1e3), "unit": "steps/s", "ms_per_step": ms / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "dtype": "f32",
+            "data": "synthetic: k^-3 spectrum, random phases (seed 7000)"}
+
+
 def run_serving(args, dev):
     """Serving mix: seeded Poisson arrivals (20/s) of RBC channel runs and FP32
     decaying turbulence, 50-500 steps each, admitted by HBM budget.  Replayed
@@ -700,6 +727,9 @@ def main():
         elif args.workload == "serving":
             if dist.rank == 0:
                 print(json.dumps(run_serving(args, dist.local)), flush=True)
+        elif args.workload == "turb":
+            if dist.rank == 0:
+                print(json.dumps(run_turb(args, dist.local)), flush=True)
         else:
             run_ours(args, cfg, scheme, dist)
     finally:
