@@ -764,3 +764,367 @@ def turb_initial_spec(Nx: int, Ny: int, seed: int, kmin: float = 1.0, kmax: Opti
     g = turb_backward(mag * np.exp(1j * phase), Nx)
     g *= amp / np.abs(g).max()
     return turb_forward(g)
+
+
+# ---------------------------------------------------------------------------
+# 3D Rayleigh-Benard: RealFourier x, RealFourier y, ChebyshevT z
+# (ChannelDomain3D, src/extras/quick_domains.jl:124-143; equations of
+# examples/ivp/rotating_rayleigh_benard_3d.jl:80-104 without rotation, in the
+# free-fall scaling of test/test_subproblem_rk.jl:23-24).
+#
+# Layout: a grid field of logical size (Nx, Ny, Nz) is an array of shape
+# (Nz, Ny, Nx); coefficients (Nx/2+1, Ny, Nz) are shape (Nz, Ny, Nx/2+1): rfft
+# along x, fft along y (ky in FFT order, -Ny/2 at the Nyquist index), then the
+# ChebyshevT transform along z, all unnormalised in x and y like the 2D case.
+# ---------------------------------------------------------------------------
+
+
+def forward_3d(g: np.ndarray) -> np.ndarray:
+    """Grid (Nz, Ny, Nx) -> coefficients (Nz, Ny, Nx/2+1)."""
+    return cheb_forward(np.fft.fft(np.fft.rfft(g, axis=2), axis=1), axis=0)
+
+
+def backward_3d(c: np.ndarray, Nx: int) -> np.ndarray:
+    """Coefficients -> grid: ChebyshevT backward, ifft along y, irfft along x
+    (Im of the kx = 0 and Nyquist bins dropped at every y, as FFTW's c2r)."""
+    return np.fft.irfft(np.fft.ifft(cheb_backward(c, axis=0), axis=1), n=Nx, axis=2)
+
+
+def _pad_xy(A: np.ndarray, My: int, Mx: int) -> np.ndarray:
+    """_pad_full over the last two axes (y, x) of a stack of full spectra."""
+    Ny, Nx = A.shape[-2:]
+    P = np.zeros(A.shape[:-2] + (My, Mx), dtype=complex)
+    hy, hx = Ny // 2, Nx // 2
+    ny_, nx_ = Ny - hy - 1, Nx - hx - 1
+    P[..., : hy + 1, : hx + 1] = A[..., : hy + 1, : hx + 1]
+    if ny_:
+        P[..., My - ny_:, : hx + 1] = A[..., Ny - ny_:, : hx + 1]
+    if nx_:
+        P[..., : hy + 1, Mx - nx_:] = A[..., : hy + 1, Nx - nx_:]
+    if ny_ and nx_:
+        P[..., My - ny_:, Mx - nx_:] = A[..., Ny - ny_:, Nx - nx_:]
+    if Nx % 2 == 0 and Mx > Nx:
+        P[..., :, hx] *= 0.5
+        P[..., :, Mx - hx] = P[..., :, hx]
+    if Ny % 2 == 0 and My > Ny:
+        P[..., hy, :] *= 0.5
+        P[..., My - hy, :] = P[..., hy, :]
+    return P
+
+
+def _truncate_xy(P: np.ndarray, Ny: int, Nx: int) -> np.ndarray:
+    """_truncate_full over the last two axes: fold the -N/2 images, truncate."""
+    P = P.copy()
+    My, Mx = P.shape[-2:]
+    hy, hx = Ny // 2, Nx // 2
+    if Nx % 2 == 0 and Mx > Nx:
+        P[..., :, hx] += P[..., :, Mx - hx]
+    if Ny % 2 == 0 and My > Ny:
+        P[..., hy, :] += P[..., My - hy, :]
+    out = np.zeros(P.shape[:-2] + (Ny, Nx), dtype=complex)
+    ny_, nx_ = Ny - hy - 1, Nx - hx - 1
+    out[..., : hy + 1, : hx + 1] = P[..., : hy + 1, : hx + 1]
+    if ny_:
+        out[..., Ny - ny_:, : hx + 1] = P[..., My - ny_:, : hx + 1]
+    if nx_:
+        out[..., : hy + 1, Nx - nx_:] = P[..., : hy + 1, Mx - nx_:]
+    if ny_ and nx_:
+        out[..., Ny - ny_:, Nx - nx_:] = P[..., My - ny_:, Mx - nx_:]
+    return out
+
+
+def padded_multiply_3d(a: np.ndarray, b: np.ndarray, factor: float = 1.5) -> np.ndarray:
+    """evaluate_padded_multiply for two real grid fields (Nz, Ny, Nx): 3/2
+    padding along both Fourier axes only (nonlinear_padding.jl:86-103,
+    359-443), per z level exactly padded_multiply_2d."""
+    Ny, Nx = a.shape[-2:]
+    My, Mx = padded_length(Ny, factor), padded_length(Nx, factor)
+    ax = (-2, -1)
+    Pa = np.fft.ifftn(_pad_xy(np.fft.fftn(a, axes=ax), My, Mx), axes=ax)
+    Pb = np.fft.ifftn(_pad_xy(np.fft.fftn(b, axes=ax), My, Mx), axes=ax)
+    R = _truncate_xy(np.fft.fftn(Pa * Pb, axes=ax), Ny, Nx)
+    return np.real(np.fft.ifftn(R, axes=ax)) * (Mx / Nx) * (My / Ny)
+
+
+@dataclass
+class RBC3Params:
+    Nx: int
+    Ny: int
+    Nz: int
+    Lx: float = 4.0
+    Ly: float = 4.0
+    Lz: float = 1.0
+    Ra: float = 1e7
+    Pr: float = 1.0
+    dealias: float = 1.5
+    b_bottom: float = None
+    b_top: float = 0.0
+
+    @property
+    def kappa(self) -> float:
+        return (self.Ra * self.Pr) ** -0.5
+
+    @property
+    def nu(self) -> float:
+        return (self.Ra / self.Pr) ** -0.5
+
+    def bottom(self) -> float:
+        return self.Lz if self.b_bottom is None else self.b_bottom
+
+
+def rbc3_initial_b(p: RBC3Params, seed: int = 42, amp: float = 1e-3) -> np.ndarray:
+    """b0 = Lz - z + amp z (Lz - z) xi on the (x, y, z) grid, xi ~ N(0,1) from
+    PCG64(seed) drawn in Julia (x, y, z) order; returned as (Nz, Ny, Nx)."""
+    rng = np.random.default_rng(seed)
+    xi = rng.standard_normal((p.Nx, p.Ny, p.Nz)).transpose(2, 1, 0)
+    z = cheb_grid(p.Nz, 0.0, p.Lz)[:, None, None]
+    return (p.Lz - z) + amp * z * (p.Lz - z) * xi
+
+
+class RBC3D:
+    """Per-(kx, ky) tau system of 3D Boussinesq RBC in the reference's own
+    Cartesian form (one complex system per Fourier mode pair, as
+    build_matrices! assembles it, subproblem_matrix_build.jl:11-309) and the
+    IMEX Runge-Kutta stepper of step_subproblem_rk.jl:393-739.
+
+    Unknowns per mode: [p, b, ux, uy, uz](Nz each), then tau_p (only at
+    kx = ky = 0), tau_b1, tau_b2, tau_u1 (x, y, z), tau_u2 (x, y, z).
+    Equations: continuity, b, u_x, u_y, u_z (Nz rows each), then the wall rows
+    b, ux, uy, uz at z = 0 and at z = Lz, and integ(p) at kx = ky = 0.
+    """
+
+    TAU_NAMES = ("tau_p", "tau_b1", "tau_b2", "tau_u1x", "tau_u1y", "tau_u1z", "tau_u2x", "tau_u2y", "tau_u2z")
+
+    def __init__(self, p: RBC3Params):
+        self.p = p
+        Nx, Ny, Nz = p.Nx, p.Ny, p.Nz
+        self.Kx = Nx // 2 + 1
+        self.kx = 2 * np.pi / p.Lx * np.arange(self.Kx)
+        self.ky = 2 * np.pi / p.Ly * np.concatenate([np.arange(Ny // 2), np.arange(-(Ny // 2), 0)])
+        self.D = cheb_diff_matrix(Nz, p.Lz)
+        self.D2 = self.D @ self.D
+        self._mats: Dict[Tuple[int, int], tuple] = {}
+        self._lu: Dict[Tuple[int, int, float, float], object] = {}
+        shape = (Nz, Ny, self.Kx)
+        self.b = np.zeros(shape, complex)
+        self.ux = np.zeros(shape, complex)
+        self.uy = np.zeros(shape, complex)
+        self.uz = np.zeros(shape, complex)
+        self.pr = np.zeros(shape, complex)
+        self.tau = np.zeros((9, Ny, self.Kx), complex)
+        self.sim_time = 0.0
+        self.iteration = 0
+
+    def modes(self):
+        return [(iy, ix) for iy in range(self.p.Ny) for ix in range(self.Kx)]
+
+    def mode_matrices(self, iy: int, ix: int):
+        """Sparse M, L, BC-row list and ALG_F of Fourier mode (kx[ix], ky[iy])."""
+        key = (iy, ix)
+        if key in self._mats:
+            return self._mats[key]
+        p = self.p
+        N = p.Nz
+        kx, ky = self.kx[ix], self.ky[iy]
+        k2 = kx * kx + ky * ky
+        dc = ix == 0 and iy == 0
+        names = self.TAU_NAMES if dc else self.TAU_NAMES[1:]
+        n = 5 * N + len(names)
+        cp, cb, cux, cuy, cuz = 0, N, 2 * N, 3 * N, 4 * N
+        tcol = {nm: 5 * N + i for i, nm in enumerate(names)}
+        rc, rb, rx, ry, rz, r_bc = 0, N, 2 * N, 3 * N, 4 * N, 5 * N
+        kap, nu = p.kappa, p.nu
+        Lr, Lc, Lv = [], [], []
+        idx = np.arange(N)
+        dr, dcol = np.nonzero(self.D)
+        d2r, d2c = np.nonzero(self.D2)
+        De = self.D[:, N - 1]
+        der = np.nonzero(De)[0]
+
+        def add(r0, c0, rr, cc, vv):
+            vv = np.broadcast_to(np.asarray(vv, dtype=complex), np.shape(rr))
+            keep = np.abs(vv) >= 1e-12  # entry cutoff (subproblem_matrix_build.jl:88-100)
+            Lr.append(r0 + np.asarray(rr)[keep])
+            Lc.append(c0 + np.asarray(cc)[keep])
+            Lv.append(vv[keep])
+
+        def lap_block(r0, c0, coef):
+            add(r0, c0, idx, idx, -coef * k2 * np.ones(N))
+            add(r0, c0, d2r, d2c, coef * self.D2[d2r, d2c])
+
+        # trace(grad_u) + tau_p = 0
+        add(rc, cux, idx, idx, 1j * kx * np.ones(N))
+        add(rc, cuy, idx, idx, 1j * ky * np.ones(N))
+        add(rc, cuz, dr, dcol, self.D[dr, dcol])
+        add(rc, tcol["tau_u1z"], [N - 1], [0], [1.0])
+        if dc:
+            add(rc, tcol["tau_p"], [0], [0], [1.0])
+        # dt(b) - kappa div(grad_b) + lift(tau_b2) = -u.grad(b)
+        lap_block(rb, cb, -kap)
+        add(rb, tcol["tau_b1"], der, np.zeros_like(der), -kap * De[der])
+        add(rb, tcol["tau_b2"], [N - 1], [0], [1.0])
+        # dt(u) - nu div(grad_u) + grad(p) - b ez + lift(tau_u2) = -u.grad(u)
+        for r0, c0, t1, t2, grad in ((rx, cux, "tau_u1x", "tau_u2x", 1j * kx), (ry, cuy, "tau_u1y", "tau_u2y", 1j * ky)):
+            lap_block(r0, c0, -nu)
+            add(r0, tcol[t1], der, np.zeros_like(der), -nu * De[der])
+            add(r0, cp, idx, idx, grad * np.ones(N))
+            add(r0, tcol[t2], [N - 1], [0], [1.0])
+        lap_block(rz, cuz, -nu)
+        add(rz, tcol["tau_u1z"], der, np.zeros_like(der), -nu * De[der])
+        add(rz, cp, dr, dcol, self.D[dr, dcol])
+        add(rz, cb, idx, idx, -np.ones(N))
+        add(rz, tcol["tau_u2z"], [N - 1], [0], [1.0])
+        bot = cheb_eval_row(N, -1.0)
+        top = cheb_eval_row(N, 1.0)
+        zero = np.zeros(N, int)
+        walls = ((cb, bot), (cux, bot), (cuy, bot), (cuz, bot), (cb, top), (cux, top), (cuy, top), (cuz, top))
+        for i, (col, row) in enumerate(walls):
+            add(r_bc + i, col, zero, idx, row)
+        bc_rows = list(range(r_bc, r_bc + 8))
+        alg_f = np.zeros(n, complex)
+        if dc:
+            # a constant BC value v projects to v Nx Ny at kx = ky = 0 (subproblem_rhs.jl:99-115)
+            alg_f[r_bc + 0] = p.bottom() * p.Nx * p.Ny
+            alg_f[r_bc + 4] = p.b_top * p.Nx * p.Ny
+            add(r_bc + 8, cp, zero, idx, p.Lx * p.Ly * cheb_integ_row(N, p.Lz))
+            bc_rows.append(r_bc + 8)
+        L = sps.coo_matrix((np.concatenate(Lv), (np.concatenate(Lr), np.concatenate(Lc))), shape=(n, n)).tocsr()
+        L.sum_duplicates()
+        Mi = np.concatenate([cb + idx, cux + idx, cuy + idx, cuz + idx])
+        Mr = np.concatenate([rb + idx, rx + idx, ry + idx, rz + idx])
+        M = sps.coo_matrix((np.ones(4 * N, complex), (Mr, Mi)), shape=(n, n)).tocsr()
+        out = (M, L, np.array(bc_rows), alg_f)
+        self._mats[key] = out
+        return out
+
+    def _fields(self):
+        return (self.pr, self.b, self.ux, self.uy, self.uz)
+
+    def gather(self, iy, ix, fields, tau) -> np.ndarray:
+        taus = tau[:, iy, ix] if (ix == 0 and iy == 0) else tau[1:, iy, ix]
+        return np.concatenate([f[:, iy, ix] for f in fields] + [taus])
+
+    def scatter(self, iy, ix, x) -> None:
+        N = self.p.Nz
+        for i, f in enumerate(self._fields()):
+            f[:, iy, ix] = x[i * N : (i + 1) * N]
+        if ix == 0 and iy == 0:
+            self.tau[:, iy, ix] = x[5 * N :]
+        else:
+            self.tau[0, iy, ix] = 0.0
+            self.tau[1:, iy, ix] = x[5 * N :]
+
+    def equation_F(self, iy, ix, F) -> np.ndarray:
+        N = self.p.Nz
+        n = 5 * N + (9 if (ix == 0 and iy == 0) else 8)
+        f = np.zeros(n, complex)
+        for i, Ff in enumerate(F):
+            f[(i + 1) * N : (i + 2) * N] = Ff[:, iy, ix]
+        return f
+
+    def mass_solve(self, rhs: np.ndarray) -> np.ndarray:
+        """Min-norm solve of the 0/1 selection M: copy the b/u rows, zero p and taus."""
+        N = self.p.Nz
+        x = np.zeros_like(rhs)
+        x[N : 5 * N] = rhs[N : 5 * N]
+        return x
+
+    def _lhs_lu(self, iy, ix, alpha, beta):
+        key = (iy, ix, alpha, beta)
+        lu = self._lu.get(key)
+        if lu is None:
+            M, L, _, _ = self.mode_matrices(iy, ix)
+            try:
+                lu = spsl.splu((alpha * M + beta * L).tocsc())
+            except RuntimeError as e:
+                raise np.linalg.LinAlgError(f"singular tau matrix at mode ({ix}, {iy}): {e}")
+            self._lu[key] = lu
+        return lu
+
+    def set_b_grid(self, bg: np.ndarray) -> None:
+        self.b = forward_3d(bg)
+
+    def projected(self, c: np.ndarray) -> np.ndarray:
+        """The grid round trip of a coefficient field (Hermitian projection of
+        the kx = 0 and kx = Nx/2 planes in ky)."""
+        return forward_3d(backward_3d(c, self.p.Nx))
+
+    def rhs(self, b, ux, uy, uz):
+        """F = -(u.grad f) for f in (b, ux, uy, uz) with lazy-evaluator semantics:
+        every factor is a grid field from a coefficient round trip, each product
+        3/2-dealiased (lazy_rhs.jl:712-1336)."""
+        p = self.p
+        Nx = p.Nx
+        g = [backward_3d(c, Nx) for c in (b, ux, uy, uz)]
+        KX = (1j * self.kx)[None, None, :]
+        KY = (1j * self.ky)[None, :, None]
+
+        def dx(f):
+            return backward_3d(KX * forward_3d(f), Nx)
+
+        def dy(f):
+            return backward_3d(KY * forward_3d(f), Nx)
+
+        def dz(f):
+            return backward_3d(np.tensordot(self.D, forward_3d(f), axes=(1, 0)), Nx)
+
+        out = []
+        for fg in g:
+            t = padded_multiply_3d(g[1], dx(fg), p.dealias)
+            t = t + padded_multiply_3d(g[2], dy(fg), p.dealias)
+            t = t + padded_multiply_3d(g[3], dz(fg), p.dealias)
+            out.append(forward_3d(-t))
+        return out
+
+    def step_rk(self, dt: float, ts: dict) -> None:
+        AE, AI, bE, bI = ts["AE"], ts["AI"], ts["bE"], ts["bI"]
+        s = AE.shape[0]
+        modes = self.modes()
+        x0 = {m: self.gather(*m, self._fields(), self.tau) for m in modes}
+        MX0 = {m: self.mode_matrices(*m)[0] @ x0[m] for m in modes}
+        F, LX = [], []
+        for i in range(s):
+            a_ii = AI[i, i]
+            xs = {}
+            for m in modes:
+                M, L, bc, algf = self.mode_matrices(*m)
+                rhs = MX0[m].copy()
+                for j in range(i):
+                    if abs(dt * AE[i, j]) > 1e-14:
+                        rhs += dt * AE[i, j] * F[j][m]
+                    if abs(dt * AI[i, j]) > 1e-14:
+                        rhs -= dt * AI[i, j] * LX[j][m]
+                if abs(a_ii) < 1e-14:
+                    xs[m] = self.mass_solve(rhs)
+                else:
+                    rhs[bc] = dt * a_ii * algf[bc]
+                    xs[m] = self._lhs_lu(*m, 1.0, dt * a_ii).solve(rhs)
+            for m in modes:
+                self.scatter(*m, xs[m])
+            Fc = self.rhs(self.b, self.ux, self.uy, self.uz)
+            proj = [self.pr] + [self.projected(c) for c in (self.b, self.ux, self.uy, self.uz)]
+            F.append({m: self.equation_F(*m, Fc) for m in modes})
+            LX.append({m: self.mode_matrices(*m)[1] @ self.gather(*m, proj, self.tau) for m in modes})
+        for m in modes:
+            rhs = MX0[m].copy()
+            for j in range(s):
+                if abs(dt * bE[j]) > 1e-14:
+                    rhs += dt * bE[j] * F[j][m]
+                if abs(dt * bI[j]) > 1e-14:
+                    rhs -= dt * bI[j] * LX[j][m]
+            self.scatter(*m, self.mass_solve(rhs))
+        self.sim_time += dt
+        self.iteration += 1
+
+    def state_dict(self) -> Dict[str, np.ndarray]:
+        return dict(b=self.b.copy(), ux=self.ux.copy(), uy=self.uy.copy(), uz=self.uz.copy(), p=self.pr.copy(),
+                    tau=self.tau.copy())
+
+
+def run_rbc3(p: RBC3Params, scheme: str, dt: float, nsteps: int, seed: int = 42) -> RBC3D:
+    """Build the 3D RBC problem with the seeded initial b and advance nsteps (RK)."""
+    sim = RBC3D(p)
+    sim.set_b_grid(rbc3_initial_b(p, seed))
+    for _ in range(nsteps):
+        sim.step_rk(dt, TABLEAUS[scheme])
+    return sim
