@@ -58,16 +58,20 @@ enum { TB_PROGRAM_RBC = 0, TB_PROGRAM_TURB2D = 1 };
 /* Arithmetic of the step. */
 enum { TB_PREC_F64 = 0, TB_PREC_MIXED = 1 };
 
-/* Field selectors for tb_set_state / tb_get_state. */
+/* Field selectors for tb_set_state / tb_get_state.  3D plans (ndim 3) hold
+ * coefficient fields complex (Nx/2+1, Ny, Nz) column-major (kx fastest, ky in
+ * FFT order) and 9 taus of (Nx/2+1, Ny): tau_p, tau_b1, tau_b2, tau_u1x,
+ * tau_u1y, tau_u1z, tau_u2x, tau_u2y, tau_u2z. */
 enum {
   TB_FIELD_B = 0, TB_FIELD_UX = 1, TB_FIELD_UZ = 2, TB_FIELD_P = 3,
-  TB_FIELD_TAU = 4 /* 7 x (Nx/2+1) complex: tau_p, tau_b1, tau_b2, tau_u1x, tau_u1z, tau_u2x, tau_u2z */
+  TB_FIELD_TAU = 4, /* 2D: 7 x (Nx/2+1) complex: tau_p, tau_b1, tau_b2, tau_u1x, tau_u1z, tau_u2x, tau_u2z */
+  TB_FIELD_UY = 5   /* 3D only */
 };
 
 typedef struct tb_problem_desc {
-  int ndim;          /* 2                                                        */
+  int ndim;          /* 2, or 3 (RealFourier y, RK222 / RK443, even Nz)          */
   int Nx, Ny, Nz;    /* grid sizes (Ny ignored in 2D)                            */
-  double Lx, Ly, Lz; /* x in [0,Lx), z in [0,Lz]                                 */
+  double Lx, Ly, Lz; /* x in [0,Lx), y in [0,Ly), z in [0,Lz]                    */
   double dealias;    /* 3/2 padding factor along Fourier axes                    */
   int precision;     /* TB_PREC_*                                                */
   int timestepper;   /* TB_RK222 ...                                             */

@@ -21,9 +21,11 @@ from .api import (  # noqa: F401
     Ensemble,
     InitialValueSolver,
     Plan,
+    Plan3D,
     Server,
     Turb2D,
     rbc_desc,
+    rbc3_desc,
     turb_desc,
     RealFourier,
     ScalarField,

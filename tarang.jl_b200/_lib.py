@@ -20,7 +20,7 @@ TB_PROGRAM_RBC = 0
 TB_PROGRAM_TURB2D = 1
 TB_REQ_QUEUED, TB_REQ_RUNNING, TB_REQ_DONE, TB_REQ_FAILED = 0, 1, 2, 3
 TB_PREC_F64, TB_PREC_MIXED = 0, 1
-TB_FIELD_B, TB_FIELD_UX, TB_FIELD_UZ, TB_FIELD_P, TB_FIELD_TAU = range(5)
+TB_FIELD_B, TB_FIELD_UX, TB_FIELD_UZ, TB_FIELD_P, TB_FIELD_TAU, TB_FIELD_UY = range(6)
 
 
 class tb_problem_desc(Structure):

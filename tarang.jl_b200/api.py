@@ -250,6 +250,55 @@ class Plan:
         return o[0], o[1], o[2]
 
 
+class Plan3D(Plan):
+    """3D Rayleigh-Benard plan: RealFourier x, RealFourier y, ChebyshevT z
+    (ChannelDomain3D, src/extras/quick_domains.jl:124-143; bounds (0, Lz) in z).
+
+    Coefficient fields are complex (Nz, Ny, Nx/2+1) arrays (the reference's
+    column-major (Nx/2+1, Ny, Nz): rfft along x, fft along y in FFT order, then
+    ChebyshevT along z); taus are (9, Ny, Nx/2+1) in the order tau_p, tau_b1,
+    tau_b2, tau_u1x, tau_u1y, tau_u1z, tau_u2x, tau_u2y, tau_u2z.  Fields: TB_FIELD_B,
+    TB_FIELD_UX, TB_FIELD_UY, TB_FIELD_UZ, TB_FIELD_P, TB_FIELD_TAU.
+    """
+
+    def __init__(self, Nx: int, Ny: int, Nz: int, kappa: float, nu: float, timestepper: int = L.TB_RK222,
+                 Lx: float = 4.0, Ly: float = 4.0, Lz: float = 1.0, b_bottom: Optional[float] = None,
+                 b_top: float = 0.0, precision: int = L.TB_PREC_F64, device: int = 0):
+        self.Nx, self.Ny, self.Nz = int(Nx), int(Ny), int(Nz)
+        self.Kx = self.Nx // 2 + 1
+        self.domain = None
+        self.ctx = _context(device)
+        d = rbc3_desc(Nx, Ny, Nz, kappa, nu, timestepper, Lx, Ly, Lz, b_bottom, b_top, precision)
+        self.desc = d
+        self.ptr = c_void_p()
+        check(lib.tb_plan_create(self.ctx, byref(d), byref(self.ptr)), self.ctx)
+
+    def _shape(self, field: int):
+        return (9, self.Ny, self.Kx) if field == L.TB_FIELD_TAU else (self.Nz, self.Ny, self.Kx)
+
+    def set_state(self, field: int, arr: np.ndarray) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.complex128)
+        assert a.shape == self._shape(field), (a.shape, self._shape(field))
+        check(lib.tb_set_state(self.ptr, field, a.ctypes.data_as(c_void_p), L.TB_HOST), self.ctx)
+
+    def get_state(self, field: int) -> np.ndarray:
+        out = np.empty(self._shape(field), np.complex128)
+        check(lib.tb_get_state(self.ptr, field, out.ctypes.data_as(c_void_p), L.TB_HOST), self.ctx)
+        return out
+
+
+def rbc3_desc(Nx: int, Ny: int, Nz: int, kappa: float, nu: float, timestepper: int = 0, Lx: float = 4.0,
+              Ly: float = 4.0, Lz: float = 1.0, b_bottom: Optional[float] = None, b_top: float = 0.0,
+              precision: int = 0):
+    d = L.tb_problem_desc()
+    d.ndim, d.Nx, d.Ny, d.Nz = 3, int(Nx), int(Ny), int(Nz)
+    d.Lx, d.Ly, d.Lz, d.dealias = float(Lx), float(Ly), float(Lz), 1.5
+    d.precision, d.timestepper, d.program = int(precision), int(timestepper), L.TB_PROGRAM_RBC
+    d.kappa, d.nu = float(kappa), float(nu)
+    d.b_bottom, d.b_top = float(Lz if b_bottom is None else b_bottom), float(b_top)
+    return d
+
+
 # ---------------------------------------------------------------------------
 # Fields
 # ---------------------------------------------------------------------------

@@ -102,31 +102,6 @@ void check_launch(const char* what) {
   if (e != cudaSuccess) throw Error{TB_ECUDA, std::string(what) + ": " + cudaGetErrorString(e)};
 }
 
-cudaEvent_t take_event(tb_plan* P) {
-  if (!P->event_pool.empty()) {
-    cudaEvent_t e = P->event_pool.back();
-    P->event_pool.pop_back();
-    return e;
-  }
-  cudaEvent_t e;
-  TB_CUDA_TRY(cudaEventCreate(&e));
-  return e;
-}
-
-// Runs fn (which enqueues one kernel) and, in profiling mode, brackets it with events.
-template <class F>
-void timed(tb_plan* P, const char* name, F&& fn) {
-  if (!P->profiling) {
-    fn();
-    return;
-  }
-  cudaEvent_t a = take_event(P), b = take_event(P);
-  TB_CUDA_TRY(cudaEventRecord(a, P->st));
-  fn();
-  TB_CUDA_TRY(cudaEventRecord(b, P->st));
-  P->pending.push_back({name, a, b});
-}
-
 void collect_profile(tb_plan* P) {
   TB_CUDA_TRY(cudaStreamSynchronize(P->st));
   for (auto& r : P->pending) {
@@ -171,10 +146,10 @@ std::vector<double2> twiddles(int n) {
   return t;
 }
 
-ClassDev class_dev(tb_plan* P, int c, FactorSet* f) {
+ClassDev class_dev(tb_plan* P, int sy, int c, FactorSet* f) {
   ClassDev cd{};
-  const ClassLayout& L = P->lay.cls[c];
-  ClassTables& T = P->ct[c];
+  const ClassLayout& L = P->sys[sy].lay.cls[c];
+  ClassTables& T = P->sys[sy].ct[c];
   cd.n = L.n;
   cd.nb = L.nb;
   cd.kl = L.kl;
@@ -192,6 +167,8 @@ ClassDev class_dev(tb_plan* P, int c, FactorSet* f) {
   cd.c2_nz = T.c2_nz.as<double>();
   cd.c1_z = T.c1_z.as<double>();
   cd.c1_nz = T.c1_nz.as<double>();
+  cd.col_code = T.col_code.as<int>();
+  cd.left_code = T.left_code.as<int>();
   if (f) {
     cd.FR = f->FR.as<double>();
     cd.BR = f->BR.as<double>();
@@ -200,65 +177,70 @@ ClassDev class_dev(tb_plan* P, int c, FactorSet* f) {
   return cd;
 }
 
-TauArgs tau_args(tb_plan* P, FactorSet* f, const double2* rhsP) {
+TauArgs tau_args(tb_plan* P, int sy, FactorSet* f, const double2* rhsP) {
   TauArgs a{};
-  a.cls[0] = class_dev(P, 0, f);
-  a.cls[1] = class_dev(P, 1, f);
+  a.cls[0] = class_dev(P, sy, 0, f);
+  a.cls[1] = class_dev(P, sy, 1, f);
   a.Nz = P->Nz;
   a.Nk = P->Nk;
   a.Nx = P->Nx;
   a.k0 = P->k0;
+  a.kmag = P->kmag.as<double>();
   a.alpha = f ? f->alpha : 0.0;
   a.beta = f ? f->beta : 0.0;
   a.X = P->X.as<double2>();
   a.tau = P->tau.as<double2>();
   a.rhsP = rhsP;
-  a.npad = (P->lay.cls[0].n + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
+  a.npad = P->sys[sy].npad;
   a.PP = f ? f->PP.as<double>() : nullptr;
   a.HR = f ? f->HR.as<double>() : nullptr;
-  a.rhs_off = P->rhs_off.as<int>();
+  a.rhs_off = P->sys[sy].rhs_off.as<int>();
   a.err_mode = P->err_mode.as<int>();
   return a;
 }
 
-FactorSet* get_factors(tb_plan* P, double alpha, double beta) {
-  for (auto& f : P->factors)
+FactorSet* get_factors(tb_plan* P, int sy, double alpha, double beta) {
+  TauSystem& S = P->sys[sy];
+  for (auto& f : S.factors)
     if (f->alpha == alpha && f->beta == beta) return f.get();
   // keep at most two sets (SBDF needs the SBDF1 and SBDF2 left-hand sides)
-  if (P->factors.size() >= 2) P->factors.erase(P->factors.begin());
+  if (S.factors.size() >= 2) S.factors.erase(S.factors.begin());
   auto fs = std::make_unique<FactorSet>();
   fs->alpha = alpha;
   fs->beta = beta;
   const int Nk = P->Nk;
   const size_t groups = (size_t)(Nk + kSolveModes - 1) / kSolveModes;
-  const size_t n = (P->lay.cls[0].n + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
+  const size_t n = S.npad;
   fs->FR.alloc(groups * n * 2 * kFwdRec * kSolveModes * sizeof(double));
   fs->BR.alloc(groups * n * 2 * kBwdRec * kSolveModes * sizeof(double));
   fs->SI.alloc(groups * 2 * 16 * kSolveModes * sizeof(double));
-  const size_t npp = tau_transfer_doubles(Nk, P->tau_parts);
+  const size_t npp = tau_transfer_doubles(Nk, S.tau_parts);
   if (npp) fs->PP.alloc(npp * sizeof(double));
-  const size_t nhr = tau_response_doubles(Nk, (int)n, P->tau_parts);
+  const size_t nhr = tau_response_doubles(Nk, (int)n, S.tau_parts);
   if (nhr) fs->HR.alloc(nhr * sizeof(double));
   TB_CUDA_TRY(cudaMemsetAsync(fs->FR.p, 0, fs->FR.bytes, P->st));
   TB_CUDA_TRY(cudaMemsetAsync(fs->BR.p, 0, fs->BR.bytes, P->st));
   TB_CUDA_TRY(cudaMemsetAsync(fs->SI.p, 0, fs->SI.bytes, P->st));
-  const int nmax = std::max(P->lay.cls[0].n, P->lay.cls[1].n);
+  const int nmax = std::max(S.lay.cls[0].n, S.lay.cls[1].n);
   DevBuf scratch;
   scratch.alloc(tau_factor_scratch_doubles(nmax, Nk) * sizeof(double));
   int neg = 0x7fffffff;
   TB_CUDA_TRY(cudaMemcpyAsync(P->err_mode.p, &neg, sizeof(int), cudaMemcpyHostToDevice, P->st));
-  TauArgs a = tau_args(P, fs.get(), nullptr);
+  TauArgs a = tau_args(P, sy, fs.get(), nullptr);
   a.scratch = scratch.as<double>();
-  launch_tau_factor(a, P->tau_parts, P->st);
+  launch_tau_factor(a, S.tau_parts, P->st);
   check_launch("tau factor");
   int bad = 0;
   TB_CUDA_TRY(cudaMemcpyAsync(&bad, P->err_mode.p, sizeof(int), cudaMemcpyDeviceToHost, P->st));
   TB_CUDA_TRY(cudaStreamSynchronize(P->st));
-  if (bad != neg)
-    throw Error{TB_ESINGULAR, "singular tau system at Fourier mode " + std::to_string(bad) +
-                                  " (kx = " + std::to_string(bad * P->k0) + ")"};
-  P->factors.push_back(std::move(fs));
-  return P->factors.back().get();
+  if (bad != neg) {
+    std::string where = P->ndim == 3 ? " (kx index " + std::to_string(bad / P->Ny) + ", ky index " +
+                                           std::to_string(bad % P->Ny) + ")"
+                                     : " (kx = " + std::to_string(bad * P->k0) + ")";
+    throw Error{TB_ESINGULAR, "singular tau system at Fourier mode " + std::to_string(bad) + where};
+  }
+  S.factors.push_back(std::move(fs));
+  return S.factors.back().get();
 }
 
 // F = -(u.grad) f in C^(2) rows (sfwd) or T coefficients (fwd) for f = b, ux, uz.
@@ -366,10 +348,14 @@ void enqueue_rk_step(tb_plan* P, double dt) {
   const Tableau T = tableau(P->d.timestepper);
   const double gamma = T.AI[1][1];
   const double beta = dt * gamma;
-  FactorSet* fs = get_factors(P, 1.0, beta);  // done before capture by the caller
-  const long long cnt = 4LL * (long long)P->plane;
+  FactorSet* fs = get_factors(P, 0, 1.0, beta);  // done before capture by the caller
+  FactorSet* fs2 = P->nsys > 1 ? get_factors(P, 1, 1.0, beta) : nullptr;
+  const long long cnt = (long long)P->nplanes * (long long)P->plane;
   double2* X = P->X.as<double2>();
-  timed(P, "mass_apply", [&] { launch_mass_apply(X, P->MX0.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 0, P->st); });
+  const bool d3 = P->ndim == 3;
+  timed(P, "mass_apply", [&] {
+    launch_mass_apply(X, P->MX0.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 0, P->nf, P->st);
+  });
   int nk = 1;
   for (int i = 0; i < T.s; ++i) {
     if (i > 0) {
@@ -387,16 +373,30 @@ void enqueue_rk_step(tb_plan* P, double dt) {
         }
       }
       timed(P, "stage_lincomb", [&] { launch_lincomb(lc, P->LXP[i].as<double2>(), cnt, P->st); });
-      TauArgs a = tau_args(P, fs, P->LXP[i].as<double2>());
-      timed(P, "tau_solve", [&] { launch_tau_solve(a, P->tau_parts, P->st); });
+      TauArgs a = tau_args(P, 0, fs, P->LXP[i].as<double2>());
+      timed(P, "tau_solve", [&] { launch_tau_solve(a, P->sys[0].tau_parts, P->st); });
+      if (fs2) {
+        TauArgs a2 = tau_args(P, 1, fs2, P->LXP[i].as<double2>());
+        timed(P, "tau_solve_perp", [&] { launch_tau_solve(a2, P->sys[1].tau_parts, P->st); });
+        ++nk;
+      }
       timed(P, "lx_finalize", [&] {
-        launch_lx_finalize(P->LXP[i].as<double2>(), X, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, P->k0, P->s,
-                           P->d.kappa, P->d.nu, beta, P->st);
+        launch_lx_finalize(P->LXP[i].as<double2>(), X, P->s3.as<double>(), P->Nz, P->Nk, d3 ? 0 : P->Nx, P->k0, P->s,
+                           P->d.kappa, P->d.nu, beta, P->nf, P->st);
       });
       nk += 3;
+      if (d3) {
+        rbc3d_lx_project(P, P->LXP[i].as<double2>(), beta);
+        ++nk;
+      }
     }
-    enqueue_rhs(P, X, P->FP[i].as<double2>() + P->plane, true);
-    nk += 3;
+    if (d3) {
+      rbc3d_enqueue_rhs(P, X, P->FP[i].as<double2>() + P->plane);
+      nk += P->mixed ? 6 : 5;
+    } else {
+      enqueue_rhs(P, X, P->FP[i].as<double2>() + P->plane, true);
+      nk += P->mixed ? 4 : 3;
+    }
   }
   LinComb lc{};
   lc.in[lc.n] = P->MX0.as<double2>();
@@ -411,7 +411,9 @@ void enqueue_rk_step(tb_plan* P, double dt) {
       lc.w[lc.n++] = -dt * T.bI[j];
     }
   }
-  timed(P, "rk_final", [&] { launch_rk_final(lc, X, P->tau.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->st); });
+  timed(P, "rk_final", [&] {
+    launch_rk_final(lc, X, P->tau.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->nf, P->ntau, P->st);
+  });
   nk += 1;
   P->kernels_per_step = nk;
 }
@@ -441,13 +443,13 @@ SbdfCoefs sbdf_coefs(int order, double dt) {
 void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
   const SbdfCoefs K = sbdf_coefs(order, dt);
   const double a0 = K.a0, a1 = K.a1, a2 = K.a2, c1 = K.c1, c2 = K.c2;
-  FactorSet* fs = get_factors(P, a0, 1.0);
-  const long long cnt = 4LL * (long long)P->plane;
+  FactorSet* fs = get_factors(P, 0, a0, 1.0);
+  const long long cnt = (long long)P->nplanes * (long long)P->plane;
   double2* X = P->X.as<double2>();
   double2* Fcur = P->FP[0].as<double2>();
   double2* MXcur = P->MX0.as<double2>();
   enqueue_rhs(P, X, Fcur + P->plane, true);
-  timed(P, "mass_apply", [&] { launch_mass_apply(X, MXcur, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 1, P->st); });
+  timed(P, "mass_apply", [&] { launch_mass_apply(X, MXcur, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 1, P->nf, P->st); });
   LinComb lc{};
   lc.in[lc.n] = Fcur;
   lc.w[lc.n++] = c1;
@@ -460,8 +462,8 @@ void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
     lc.w[lc.n++] = -a2;
   }
   timed(P, "stage_lincomb", [&] { launch_lincomb(lc, P->Rsb.as<double2>(), cnt, P->st); });
-  TauArgs a = tau_args(P, fs, P->Rsb.as<double2>());
-  timed(P, "tau_solve", [&] { launch_tau_solve(a, P->tau_parts, P->st); });
+  TauArgs a = tau_args(P, 0, fs, P->Rsb.as<double2>());
+  timed(P, "tau_solve", [&] { launch_tau_solve(a, P->sys[0].tau_parts, P->st); });
   TB_CUDA_TRY(cudaMemcpyAsync(P->Fprev.p, Fcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
   TB_CUDA_TRY(cudaMemcpyAsync(P->MXprev.p, MXcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
   P->kernels_per_step = 3 + 1 + 1 + 1;
@@ -508,11 +510,13 @@ void capture_step(tb_plan* P, double dt, int kind) {
 
 // Factors for the next step of the given kind (built once per dt).
 void prepare_kind(tb_plan* P, double dt, int kind) {
-  if (kind == 0) {
-    const Tableau T = tableau(P->d.timestepper);
-    get_factors(P, 1.0, dt * T.AI[1][1]);
-  } else {
-    get_factors(P, sbdf_coefs(kind, dt).a0, 1.0);
+  for (int sy = 0; sy < P->nsys; ++sy) {
+    if (kind == 0) {
+      const Tableau T = tableau(P->d.timestepper);
+      get_factors(P, sy, 1.0, dt * T.AI[1][1]);
+    } else {
+      get_factors(P, sy, sbdf_coefs(kind, dt).a0, 1.0);
+    }
   }
 }
 
@@ -599,16 +603,21 @@ size_t tb::plan_device_bytes(const tb_plan* P) {
   size_t b = 0;
   const DevBuf* bufs[] = {&P->X,   &P->G,   &P->H,    &P->MX0,  &P->Fprev, &P->MXprev, &P->Rsb, &P->tmpgrid,
                           &P->bwd, &P->fwd, &P->s3,   &P->twM,  &P->twN,   &P->ptwM,   &P->bEv, &P->bOv,
-                          &P->bEd, &P->bOd, &P->fE,   &P->fO,   &P->sfE,   &P->sfO,    &P->err_mode, &P->rhs_off};
+                          &P->bEd, &P->bOd, &P->fE,   &P->fO,   &P->sfE,   &P->sfO,    &P->err_mode};
   for (const DevBuf* d : bufs) b += d->bytes;
   for (int i = 0; i < 4; ++i) b += P->FP[i].bytes + P->LXP[i].bytes;
-  for (int c = 0; c < 2; ++c) {
-    const ClassTables& t = P->ct[c];
-    const DevBuf* tb_[] = {&t.row_eq, &t.row_k, &t.col_unk, &t.col_k, &t.left_unk, &t.left_k, &t.bc_rhs,
-                           &t.band,   &t.bord,  &t.c2_z,    &t.c2_nz, &t.c1_z,     &t.c1_nz};
-    for (const DevBuf* d : tb_) b += d->bytes;
+  for (int sy = 0; sy < P->nsys; ++sy) {
+    const TauSystem& S = P->sys[sy];
+    b += S.rhs_off.bytes;
+    for (int c = 0; c < 2; ++c) {
+      const ClassTables& t = S.ct[c];
+      const DevBuf* tb_[] = {&t.row_eq, &t.row_k, &t.col_unk, &t.col_k, &t.left_unk, &t.left_k, &t.bc_rhs, &t.band,
+                             &t.bord,   &t.c2_z,  &t.c2_nz,   &t.c1_z,  &t.c1_nz,    &t.col_code, &t.left_code};
+      for (const DevBuf* d : tb_) b += d->bytes;
+    }
+    for (const auto& f : S.factors) b += f->FR.bytes + f->BR.bytes + f->SI.bytes + f->PP.bytes + f->HR.bytes;
   }
-  for (const auto& f : P->factors) b += f->FR.bytes + f->BR.bytes + f->SI.bytes + f->PP.bytes + f->HR.bytes;
+  b += rbc3d_device_bytes(P);
   const DevBuf* m32[] = {&P->X32,  &P->G32,  &P->H32,  &P->bEv32, &P->bOv32, &P->bEd32,
                          &P->bOd32, &P->fE32, &P->fO32, &P->sfE32, &P->sfO32, &P->ptwM32};
   for (const DevBuf* d : m32) b += d->bytes;
@@ -646,15 +655,209 @@ namespace {
 
 void validate_desc(const tb_problem_desc* d) {
   TB_REQUIRE(d != nullptr, TB_EINVAL, "null problem descriptor");
-  TB_REQUIRE(d->ndim == 2, TB_ENOTSUPPORTED, "only 2D Fourier x Chebyshev plans are implemented");
+  TB_REQUIRE(d->ndim == 2 || d->ndim == 3, TB_ENOTSUPPORTED, "ndim must be 2 or 3");
   TB_REQUIRE(d->program == TB_PROGRAM_RBC, TB_ENOTSUPPORTED, "unknown equation program");
   TB_REQUIRE(d->Nx >= 6 && d->Nx % 2 == 0, TB_EINVAL, "Nx must be even and >= 6");
+  if (d->ndim == 3) {
+    TB_REQUIRE(d->Ny >= 6 && d->Ny % 2 == 0, TB_EINVAL, "Ny must be even and >= 6");
+    TB_REQUIRE(d->Ly > 0, TB_EINVAL, "domain lengths must be positive");
+    TB_REQUIRE(d->Nz % 2 == 0, TB_ENOTSUPPORTED, "3D plans need an even Nz");
+    TB_REQUIRE(d->timestepper == TB_RK222 || d->timestepper == TB_RK443, TB_ENOTSUPPORTED,
+               "3D plans step with RK222 or RK443");
+  }
   TB_REQUIRE(d->Nz >= 8 && d->Nz <= 32767, TB_EINVAL, "Nz must be in [8, 32767]");
   TB_REQUIRE(d->Lx > 0 && d->Lz > 0, TB_EINVAL, "domain lengths must be positive");
   TB_REQUIRE(std::fabs(d->dealias - 1.5) < 1e-12, TB_ENOTSUPPORTED, "only dealias = 3/2 is implemented");
   TB_REQUIRE(d->timestepper >= TB_RK222 && d->timestepper <= TB_SBDF2, TB_EINVAL, "unknown timestepper");
   TB_REQUIRE(d->precision == TB_PREC_F64 || d->precision == TB_PREC_MIXED, TB_EINVAL, "unknown precision mode");
   TB_REQUIRE(d->kappa > 0 && d->nu > 0, TB_EINVAL, "kappa and nu must be positive");
+}
+
+// Store code of unknown (unk, k) of tau system sy: 2 * (element offset of its
+// row for mode 0 from X) + 1 when the unknown is i times the solved real column
+// (u_x / u_par and its two taus).  System 0 taus occupy tau rows 0..6, the
+// decoupled system's tau_1 / tau_2 rows 7 / 8.
+long long store_code(const tb_plan* P, int sy, int unk, int k) {
+  const long long Nk = P->Nk, taub = (long long)P->nplanes * (long long)P->plane;
+  if (sy == 0) {
+    if (unk < UK_TAU0) return 2 * ((long long)unk * P->Nz + k) * Nk + (unk == UK_UX ? 1 : 0);
+    const int t = unk - UK_TAU0;
+    return 2 * (taub + t * Nk) + ((t == 3 || t == 5) ? 1 : 0);
+  }
+  if (unk < UK_TAU0) return 2 * ((long long)4 * P->Nz + k) * Nk;
+  return 2 * (taub + (long long)(6 + unk - UK_TAU0) * Nk);
+}
+
+// Right-hand-side code of a band row: 2 * (element offset of its row in a stage
+// vector) + 1 for a u_x / u_par momentum row (scaled by -i on load).
+long long rhs_code(const tb_plan* P, int sy, int eq, int k) {
+  if (sy == 0) return 2 * ((long long)eq * P->Nz + k) * P->Nk + (eq == EQ_MX ? 1 : 0);
+  return 2 * ((long long)4 * P->Nz + k) * P->Nk;
+}
+
+void install_system(tb_plan* P, int sy, TauLayout lay) {
+  TauSystem& S = P->sys[sy];
+  auto to_int = [](long long v) {
+    TB_REQUIRE(v >= -1 && v < 0x7fffffffLL, TB_ENOTSUPPORTED, "plan too large for 32-bit solve addressing");
+    return (int)v;
+  };
+  for (int c = 0; c < 2; ++c) {
+    ClassLayout& L = lay.cls[c];
+    TB_REQUIRE(L.kl <= kTauKL && L.ku <= kTauKU && L.nb <= 4, TB_ENOTSUPPORTED, "unexpected tau band shape");
+    // pad the band template to the compiled (kTauKL, kTauKU) shape
+    const int WC = kTauKL + kTauKU + 1;
+    std::vector<Coef> band((size_t)L.n * WC, Coef{0, 0, 0, 0});
+    for (int r = 0; r < L.n; ++r)
+      for (int d = 0; d < L.kl + L.ku + 1; ++d)
+        band[(size_t)r * WC + (d - L.kl + kTauKL)] = L.band[(size_t)r * (L.kl + L.ku + 1) + d];
+    L.band = band;
+    L.kl = kTauKL;
+    L.ku = kTauKU;
+    auto to_short = [](const std::vector<int>& v) { return std::vector<short>(v.begin(), v.end()); };
+    std::vector<int> cc(L.n), lc(L.nb);
+    for (int j = 0; j < L.n; ++j) cc[j] = to_int(store_code(P, sy, L.col_unk[j], L.col_k[j]));
+    for (int b = 0; b < L.nb; ++b) lc[b] = to_int(store_code(P, sy, L.left_unk[b], L.left_k[b]));
+    ClassTables& T = S.ct[c];
+    upload(T.row_eq, to_short(L.row_eq));
+    upload(T.row_k, to_short(L.row_k));
+    upload(T.col_unk, to_short(L.col_unk));
+    upload(T.col_k, to_short(L.col_k));
+    upload(T.left_unk, to_short(L.left_unk));
+    upload(T.left_k, to_short(L.left_k));
+    upload(T.bc_rhs, L.bc_rhs);
+    upload(T.band, L.band);
+    upload(T.bord, L.bord);
+    upload(T.c2_z, L.c2_z);
+    upload(T.c2_nz, L.c2_nz);
+    upload(T.c1_z, L.c1_z);
+    upload(T.c1_nz, L.c1_nz);
+    upload(T.col_code, cc);
+    upload(T.left_code, lc);
+  }
+  TB_REQUIRE(lay.cls[0].n == lay.cls[1].n, TB_ENOTSUPPORTED, "parity classes of unequal size");
+  const int n = lay.cls[0].n;
+  S.npad = (n + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
+  // partitioned solve (kTauParts warps per mode group) when its shared memory
+  // fits and the modes alone do not fill the GPU, else one warp per group
+  const bool many_groups = (P->Nk + kSolveModes - 1) / kSolveModes >= 4 * 148;
+  S.tau_parts = (!many_groups && tau_solve_smem_bytes(S.npad, kTauParts) <= 227 * 1024) ? kTauParts : 1;
+  TB_REQUIRE(tau_solve_smem_bytes(S.npad, S.tau_parts) <= 227 * 1024, TB_ENOTSUPPORTED,
+             "Nz too large for the staged tau solve");
+  // per (band row, class) right-hand-side code, -1 for the padding rows
+  std::vector<int> ro((size_t)2 * S.npad, -1);
+  for (int j = 0; j < n; ++j)
+    for (int c = 0; c < 2; ++c) ro[2 * j + c] = to_int(rhs_code(P, sy, lay.cls[c].row_eq[j], lay.cls[c].row_k[j]));
+  upload(S.rhs_off, ro);
+  S.lay = std::move(lay);
+}
+
+// 3D state I/O through the host: public layout (kx, ky, z) kx fastest,
+// Cartesian velocity and taus <-> the plan's [plane][z][ix * Ny + iy] with
+// (u_par, u_perp) and tau rows (tau_p, b1, b2, u1par, u1z, u2par, u2z, u1perp,
+// u2perp).  Not a hot path.
+void state3d_io(tb_plan* P, int field, void* data, int where, bool set) {
+  TB_REQUIRE(field >= TB_FIELD_B && field <= TB_FIELD_UY, TB_EINVAL, "bad field selector");
+  const int Kx = P->Kx, Ny = P->Ny, Nz = P->Nz;
+  const size_t Nk = P->Nk, plane = P->plane;
+  std::vector<double2> Xh((size_t)P->X.bytes / sizeof(double2));
+  TB_CUDA_TRY(cudaMemcpyAsync(Xh.data(), P->X.p, P->X.bytes, cudaMemcpyDeviceToHost, P->st));
+  TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  const bool tau = field == TB_FIELD_TAU;
+  const size_t count = tau ? 9 * Nk : plane;
+  std::vector<double2> pub(count);
+  auto rot = [&](size_t m, double& cx, double& cy) {
+    const int ix = (int)(m / Ny), iy = (int)(m % Ny);
+    const double kx = P->k0 * ix, ky = P->k0y * (iy < Ny / 2 ? iy : iy - Ny);
+    const double kk = std::sqrt(kx * kx + ky * ky);
+    cx = kk > 0 ? kx / kk : 1.0;
+    cy = kk > 0 ? ky / kk : 0.0;
+  };
+  auto pub_index = [&](size_t m, int z) { return (size_t)(m / Ny) + (size_t)Kx * ((m % Ny) + (size_t)Ny * z); };
+  auto cx_of = [](double c, double2 a, double d, double2 b) {
+    return make_double2(c * a.x + d * b.x, c * a.y + d * b.y);
+  };
+  // internal (row, m) -> pointer into Xh for the Cartesian-independent slots
+  double2* taub = Xh.data() + (size_t)P->nplanes * plane;
+  if (set) {
+    if (where == TB_DEVICE)
+      TB_CUDA_TRY(cudaMemcpy(pub.data(), data, count * sizeof(double2), cudaMemcpyDeviceToHost));
+    else
+      std::memcpy(pub.data(), data, count * sizeof(double2));
+  }
+  if (tau) {
+    const int ord[9] = {0, 1, 2, -1, 4, -1, 6, -1, -1};  // public row -> internal row (-1 rotated)
+    for (size_t m = 0; m < Nk; ++m) {
+      double cx, cy;
+      rot(m, cx, cy);
+      const size_t pm = (m / Ny) + (size_t)Kx * (m % Ny);
+      for (int r = 0; r < 9; ++r)
+        if (ord[r] >= 0) {
+          double2& slot = taub[(size_t)ord[r] * Nk + m];
+          if (set)
+            slot = pub[(size_t)r * Nk + pm];
+          else
+            pub[(size_t)r * Nk + pm] = slot;
+        }
+      for (int w = 0; w < 2; ++w) {  // tau_u1 (public rows 3, 4), tau_u2 (6, 7)
+        const int rx = w ? 6 : 3, ry = w ? 7 : 4;
+        double2& par = taub[(size_t)(w ? 5 : 3) * Nk + m];
+        double2& perp = taub[(size_t)(w ? 8 : 7) * Nk + m];
+        if (set) {
+          const double2 ux = pub[(size_t)rx * Nk + pm], uy = pub[(size_t)ry * Nk + pm];
+          par = cx_of(cx, ux, cy, uy);
+          perp = cx_of(-cy, ux, cx, uy);
+        } else {
+          pub[(size_t)rx * Nk + pm] = cx_of(cx, par, -cy, perp);
+          pub[(size_t)ry * Nk + pm] = cx_of(cy, par, cx, perp);
+        }
+      }
+    }
+    // tau_u1z / tau_u2z sit at public rows 5 / 8, internal rows 4 / 6
+    for (size_t m = 0; m < Nk; ++m) {
+      const size_t pm = (m / Ny) + (size_t)Kx * (m % Ny);
+      double2& a = taub[4 * Nk + m];
+      double2& b = taub[6 * Nk + m];
+      if (set) {
+        a = pub[5 * Nk + pm];
+        b = pub[8 * Nk + pm];
+      } else {
+        pub[5 * Nk + pm] = a;
+        pub[8 * Nk + pm] = b;
+      }
+    }
+  } else {
+    for (int z = 0; z < Nz; ++z)
+      for (size_t m = 0; m < Nk; ++m) {
+        const size_t i = (size_t)z * Nk + m, pi = pub_index(m, z);
+        if (field == TB_FIELD_B || field == TB_FIELD_UZ || field == TB_FIELD_P) {
+          const int pl = field == TB_FIELD_B ? 0 : (field == TB_FIELD_UZ ? 2 : 3);
+          if (set)
+            Xh[pl * plane + i] = pub[pi];
+          else
+            pub[pi] = Xh[pl * plane + i];
+        } else {
+          double cx, cy;
+          rot(m, cx, cy);
+          double2& par = Xh[plane + i];
+          double2& perp = Xh[4 * plane + i];
+          double2 ux = cx_of(cx, par, -cy, perp), uy = cx_of(cy, par, cx, perp);
+          if (set) {
+            (field == TB_FIELD_UX ? ux : uy) = pub[pi];
+            par = cx_of(cx, ux, cy, uy);
+            perp = cx_of(-cy, ux, cx, uy);
+          } else {
+            pub[pi] = field == TB_FIELD_UX ? ux : uy;
+          }
+        }
+      }
+  }
+  if (set) {
+    TB_CUDA_TRY(cudaMemcpy(P->X.p, Xh.data(), P->X.bytes, cudaMemcpyHostToDevice));
+  } else if (where == TB_DEVICE) {
+    TB_CUDA_TRY(cudaMemcpy(data, pub.data(), count * sizeof(double2), cudaMemcpyHostToDevice));
+  } else {
+    std::memcpy(data, pub.data(), count * sizeof(double2));
+  }
 }
 
 }  // namespace
@@ -720,19 +923,32 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
     TB_CUDA_TRY(cudaSetDevice(ctx->device));
     P->ctx = ctx;
     P->d = *desc;
+    P->ndim = desc->ndim;
     P->Nx = desc->Nx;
     P->Nz = desc->Nz;
-    P->Nk = desc->Nx / 2 + 1;
+    P->Kx = desc->Nx / 2 + 1;
+    P->Ny = desc->ndim == 3 ? desc->Ny : 1;
+    P->Nk = P->Kx * P->Ny;
     int M = (int)std::ceil(1.5 * desc->Nx);
     if (M % 2) ++M;
     P->M = M;
     P->k0 = 2.0 * M_PI / desc->Lx;
     P->s = 2.0 / desc->Lz;
     P->plane = (size_t)P->Nz * P->Nk;
+    if (desc->ndim == 3) {
+      int My = (int)std::ceil(1.5 * desc->Ny);
+      if (My % 2) ++My;
+      P->My = My;
+      P->k0y = 2.0 * M_PI / desc->Ly;
+      P->nplanes = 5;
+      P->ntau = 9;
+      P->nf = 4;
+    }
     TB_REQUIRE(make_fft_plan(P->M, &P->fpM) && make_fft_plan(P->Nx, &P->fpN), TB_ENOTSUPPORTED,
                "Nx must be of the form 2^a 3^b");
-    TB_REQUIRE(xprod_smem_bytes(P->M, P->Nk, (int)pass_twiddles(P->fpM).size()) <= 227 * 1024, TB_ENOTSUPPORTED,
-               "Nx too large for the fused x kernel");
+    if (desc->ndim == 2)
+      TB_REQUIRE(xprod_smem_bytes(P->M, P->Nk, (int)pass_twiddles(P->fpM).size()) <= 227 * 1024, TB_ENOTSUPPORTED,
+                 "Nx too large for the fused x kernel");
     TB_CUDA_TRY(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
     TB_CUDA_TRY(cudaEventCreate(&P->ev0));
     TB_CUDA_TRY(cudaEventCreate(&P->ev1));
@@ -798,90 +1014,49 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
                  "Nx too large for the FP32 x kernel");
       TB_CUDA_TRY(set_mixed_smem_limits(227 * 1024));
     }
-    // tau layout
-    P->lay = build_rbc_layout(P->Nz, desc->Lx, desc->Lz, desc->kappa, desc->nu, (double)desc->Nx,
-                              desc->b_bottom, desc->b_top);
-    for (int c = 0; c < 2; ++c) {
-      const ClassLayout& L = P->lay.cls[c];
-      TB_REQUIRE(L.kl <= kTauKL && L.ku <= kTauKU && L.nb <= 4, TB_ENOTSUPPORTED, "unexpected tau band shape");
-      // pad the band template to the compiled (kTauKL, kTauKU) shape
-      const int WC = kTauKL + kTauKU + 1;
-      std::vector<Coef> band((size_t)L.n * WC, Coef{0, 0, 0, 0});
-      for (int r = 0; r < L.n; ++r)
-        for (int d = 0; d < L.kl + L.ku + 1; ++d)
-          band[(size_t)r * WC + (d - L.kl + kTauKL)] = L.band[(size_t)r * (L.kl + L.ku + 1) + d];
-      P->lay.cls[c].band = band;
-      P->lay.cls[c].kl = kTauKL;
-      P->lay.cls[c].ku = kTauKU;
-      auto to_short = [](const std::vector<int>& v) { return std::vector<short>(v.begin(), v.end()); };
-      ClassTables& T = P->ct[c];
-      upload(T.row_eq, to_short(L.row_eq));
-      upload(T.row_k, to_short(L.row_k));
-      upload(T.col_unk, to_short(L.col_unk));
-      upload(T.col_k, to_short(L.col_k));
-      upload(T.left_unk, to_short(L.left_unk));
-      upload(T.left_k, to_short(L.left_k));
-      upload(T.bc_rhs, L.bc_rhs);
-      upload(T.band, band);
-      upload(T.bord, L.bord);
-      upload(T.c2_z, L.c2_z);
-      upload(T.c2_nz, L.c2_nz);
-      upload(T.c1_z, L.c1_z);
-      upload(T.c1_nz, L.c1_nz);
-    }
-    TB_REQUIRE(P->lay.cls[0].n == P->lay.cls[1].n, TB_ENOTSUPPORTED, "parity classes of unequal size");
-    {
-      // partitioned solve (kTauParts warps per mode group) when its shared
-      // memory fits, else one warp per group
-      const int npad = (P->lay.cls[0].n + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
-      P->tau_parts = tau_solve_smem_bytes(npad, kTauParts) <= 227 * 1024 ? kTauParts : 1;
-      TB_REQUIRE(tau_solve_smem_bytes(npad, P->tau_parts) <= 227 * 1024, TB_ENOTSUPPORTED,
-                 "Nz too large for the staged tau solve");
-    }
+    // tau systems: the coupled Boussinesq system (with |k| per mode in 3D) and,
+    // in 3D, the decoupled cross-wavevector velocity
+    const bool d3 = P->ndim == 3;
+    install_system(P.get(), 0,
+                   build_rbc_layout(P->Nz, d3 ? desc->Lx * desc->Ly : desc->Lx, desc->Lz, desc->kappa, desc->nu,
+                                    d3 ? (double)desc->Nx * desc->Ny : (double)desc->Nx, desc->b_bottom, desc->b_top));
+    if (d3) install_system(P.get(), 1, build_helmholtz_layout(P->Nz, desc->Lz, desc->nu));
+    P->nsys = d3 ? 2 : 1;
     TB_REQUIRE(rk_final_smem_bytes(P->Nz) <= 227 * 1024, TB_ENOTSUPPORTED, "Nz too large for the final RK update");
     P->err_mode.alloc(sizeof(int));
-    {
-      // per (band row, class): 2 * (element offset of the row's right-hand side
-      // in a stage vector) + 1 when it is a u_x momentum row (scaled by -i on
-      // load); -1 for the padding rows
-      const int n = P->lay.cls[0].n;
-      const int npad = (n + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
-      std::vector<int> ro((size_t)2 * npad, -1);
-      for (int j = 0; j < n; ++j)
-        for (int cc = 0; cc < 2; ++cc) {
-          const int eq = P->lay.cls[cc].row_eq[j];
-          ro[2 * j + cc] = 2 * (eq * P->Nz + P->lay.cls[cc].row_k[j]) * P->Nk + (eq == EQ_MX ? 1 : 0);
-        }
-      upload(P->rhs_off, ro);
-    }
     // state and work arrays
     const size_t pb = P->plane * sizeof(double2);
-    P->X.alloc(4 * pb + 7 * P->Nk * sizeof(double2));
-    P->tau.p = static_cast<char*>(P->X.p) + 4 * pb;
-    P->tau.bytes = 7 * P->Nk * sizeof(double2);
-    P->G.alloc(12 * (size_t)((P->Nz + 1) / 2) * P->Nk * sizeof(double2));
-    P->H.alloc(3 * pb);
-    if (P->mixed) {
-      P->X32.alloc(3 * P->plane * sizeof(float2));
-      P->G32.alloc(12 * (size_t)((P->Nz + 1) / 2) * P->Nk * sizeof(float2));
-      P->H32.alloc(3 * P->plane * sizeof(float2));
+    P->X.alloc(P->nplanes * pb + (size_t)P->ntau * P->Nk * sizeof(double2));
+    P->tau.p = static_cast<char*>(P->X.p) + P->nplanes * pb;
+    P->tau.bytes = (size_t)P->ntau * P->Nk * sizeof(double2);
+    if (!d3) {
+      P->G.alloc(12 * (size_t)((P->Nz + 1) / 2) * P->Nk * sizeof(double2));
+      P->H.alloc(3 * pb);
+      if (P->mixed) {
+        P->X32.alloc(3 * P->plane * sizeof(float2));
+        P->G32.alloc(12 * (size_t)((P->Nz + 1) / 2) * P->Nk * sizeof(float2));
+        P->H32.alloc(3 * P->plane * sizeof(float2));
+      }
+      P->tmpgrid.alloc(P->plane * sizeof(double2));
+    } else {
+      rbc3d_setup(P.get());
     }
-    P->MX0.alloc(4 * pb);
-    for (int i = 0; i < 4; ++i) {
-      P->FP[i].alloc(4 * pb);
-      P->LXP[i].alloc(4 * pb);
+    P->MX0.alloc(P->nplanes * pb);
+    const int nst = tableau(desc->timestepper).s;
+    const int nstage = (desc->timestepper == TB_SBDF1 || desc->timestepper == TB_SBDF2) ? 1 : nst;
+    for (int i = 0; i < nstage; ++i) {
+      P->FP[i].alloc(P->nplanes * pb);
+      P->LXP[i].alloc(P->nplanes * pb);
     }
     const bool sbdf = desc->timestepper == TB_SBDF1 || desc->timestepper == TB_SBDF2;
     if (sbdf) {
-      P->Fprev.alloc(4 * pb);
-      P->MXprev.alloc(4 * pb);
-      P->Rsb.alloc(4 * pb);
+      P->Fprev.alloc(P->nplanes * pb);
+      P->MXprev.alloc(P->nplanes * pb);
+      P->Rsb.alloc(P->nplanes * pb);
     }
-    P->tmpgrid.alloc(P->plane * sizeof(double2));
     TB_CUDA_TRY(cudaMemsetAsync(P->X.p, 0, P->X.bytes, P->st));
-    TB_CUDA_TRY(cudaMemsetAsync(P->tau.p, 0, P->tau.bytes, P->st));
     TB_CUDA_TRY(cudaMemsetAsync(P->MX0.p, 0, P->MX0.bytes, P->st));
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < nstage; ++i) {
       TB_CUDA_TRY(cudaMemsetAsync(P->FP[i].p, 0, P->FP[i].bytes, P->st));
       TB_CUDA_TRY(cudaMemsetAsync(P->LXP[i].p, 0, P->LXP[i].bytes, P->st));
     }
@@ -905,6 +1080,11 @@ tb_status tb_plan_destroy(tb_plan* plan) {
 
 tb_status tb_set_state(tb_plan* P, int field, const void* data, int where) {
   if (!P || !data) return TB_EINVAL;
+  if (P->ndim == 3)
+    return guard(P->ctx, [&] {
+      state3d_io(P, field, const_cast<void*>(data), where, true);
+      P->ms_history = 0;
+    });
   return guard(P->ctx, [&] {
     TB_REQUIRE(field >= TB_FIELD_B && field <= TB_FIELD_TAU, TB_EINVAL, "bad field selector");
     void* dst = field == TB_FIELD_TAU ? P->tau.p : (void*)P->Xp(field);
@@ -918,6 +1098,7 @@ tb_status tb_set_state(tb_plan* P, int field, const void* data, int where) {
 
 tb_status tb_get_state(tb_plan* P, int field, void* data, int where) {
   if (!P || !data) return TB_EINVAL;
+  if (P->ndim == 3) return guard(P->ctx, [&] { state3d_io(P, field, data, where, false); });
   return guard(P->ctx, [&] {
     TB_REQUIRE(field >= TB_FIELD_B && field <= TB_FIELD_TAU, TB_EINVAL, "bad field selector");
     const void* src = field == TB_FIELD_TAU ? P->tau.p : (const void*)P->Xp(field);
@@ -1057,6 +1238,7 @@ tb_status tb_kernels_per_step(const tb_plan* P, int* n) {
 tb_status tb_transform_forward(tb_plan* P, const double* grid, double* coeff, int nfields) {
   if (!P || !grid || !coeff || nfields < 1) return TB_EINVAL;
   return guard(P->ctx, [&] {
+    TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "2D plans only");
     const size_t gsz = (size_t)P->Nz * P->Nx;
     for (int f = 0; f < nfields; ++f) {
       double2* mixed = P->tmpgrid.as<double2>();
@@ -1076,6 +1258,7 @@ tb_status tb_transform_forward(tb_plan* P, const double* grid, double* coeff, in
 tb_status tb_transform_backward(tb_plan* P, const double* coeff, double* grid, int nfields) {
   if (!P || !grid || !coeff || nfields < 1) return TB_EINVAL;
   return guard(P->ctx, [&] {
+    TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "2D plans only");
     const size_t gsz = (size_t)P->Nz * P->Nx;
     for (int f = 0; f < nfields; ++f) {
       double2* mixed = P->tmpgrid.as<double2>();
@@ -1093,6 +1276,7 @@ tb_status tb_transform_backward(tb_plan* P, const double* coeff, double* grid, i
 tb_status tb_dealiased_multiply(tb_plan* P, const double* a, const double* b, double* out) {
   if (!P || !a || !b || !out) return TB_EINVAL;
   return guard(P->ctx, [&] {
+    TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "2D plans only");
     launch_x_dealias_mul(a, b, out, P->Nz, P->Nx, P->M, P->fpN, P->twN.as<double2>(), P->fpM,
                          P->twM.as<double2>(), P->st);
     check_launch("dealiased multiply");
@@ -1103,6 +1287,7 @@ tb_status tb_dealiased_multiply(tb_plan* P, const double* a, const double* b, do
 tb_status tb_rhs_advection(tb_plan* P, const double* coeff_in, double* coeff_out) {
   if (!P || !coeff_in || !coeff_out) return TB_EINVAL;
   return guard(P->ctx, [&] {
+    TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "2D plans only");
     enqueue_rhs(P, reinterpret_cast<const double2*>(coeff_in), reinterpret_cast<double2*>(coeff_out), false);
     check_launch("rhs advection");
     TB_CUDA_TRY(cudaStreamSynchronize(P->st));

@@ -177,6 +177,79 @@ __device__ C* fft(C* a, C* b, const FftPlan& fp, const C* __restrict__ pt, int s
   return in;
 }
 
+// Batched form: nb transforms of length fp.n, buffer q at a + q * stride (and
+// b + q * stride), all butterflies of a pass spread over the CTA.
+template <int R, bool SW, class C>
+__device__ __forceinline__ void pass_batch(const C* __restrict__ in, C* __restrict__ out, int n, int Ns,
+                                           const C* __restrict__ pt, int sign, int nb, int stride) {
+  const int nR = n / R;
+  for (int t = threadIdx.x; t < nb * nR; t += blockDim.x) {
+    const int q = t / nR, idx = t - q * nR;
+    const int j = idx % Ns, k = idx / Ns;
+    const C* src = in + (size_t)q * stride;
+    C* dst = out + (size_t)q * stride;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[fidx<SW>(idx + r * nR)];
+    if (Ns > 1) {
+      C w1 = pt[j];
+      if (sign > 0) w1.y = -w1.y;
+      if constexpr (R == 8) {
+        const C w2 = mul(w1, w1), w4 = mul(w2, w2), w3 = mul(w1, w2);
+        v[1] = mul(v[1], w1);
+        v[2] = mul(v[2], w2);
+        v[3] = mul(v[3], w3);
+        v[4] = mul(v[4], w4);
+        v[5] = mul(v[5], mul(w1, w4));
+        v[6] = mul(v[6], mul(w2, w4));
+        v[7] = mul(v[7], mul(w3, w4));
+      } else if constexpr (R == 4) {
+        const C w2 = mul(w1, w1);
+        v[1] = mul(v[1], w1);
+        v[2] = mul(v[2], w2);
+        v[3] = mul(v[3], mul(w1, w2));
+      } else if constexpr (R == 3) {
+        v[1] = mul(v[1], w1);
+        v[2] = mul(v[2], mul(w1, w1));
+      } else {
+        v[1] = mul(v[1], w1);
+      }
+    }
+    dft_small<R>(v, sign);
+    const int ob = k * Ns * R + j;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[fidx<SW>(ob + r * Ns)] = v[r];
+  }
+}
+
+// nb CTA-wide transforms between buffer sets a and b (buffer q at + q * stride);
+// returns the set holding the results.
+template <bool SW, class C>
+__device__ C* fft_batch(C* a, C* b, int nb, int stride, const FftPlan& fp, const C* __restrict__ pt, int sign) {
+  const int n = fp.n;
+  int Ns = 1;
+  C* in = a;
+  C* out = b;
+  for (int s = 0; s < fp.nstages; ++s) {
+    const int R = fp.radix[s];
+    if (R == 8)
+      pass_batch<8, SW>(in, out, n, Ns, pt, sign, nb, stride);
+    else if (R == 4)
+      pass_batch<4, SW>(in, out, n, Ns, pt, sign, nb, stride);
+    else if (R == 2)
+      pass_batch<2, SW>(in, out, n, Ns, pt, sign, nb, stride);
+    else
+      pass_batch<3, SW>(in, out, n, Ns, pt, sign, nb, stride);
+    __syncthreads();
+    C* t = in;
+    in = out;
+    out = t;
+    pt += Ns;
+    Ns *= R;
+  }
+  return in;
+}
+
 // Number of per-pass twiddle entries of a plan (sum of the passes' Ns).
 __host__ __device__ inline int pass_twiddle_count(const FftPlan& fp) {
   int c = 0, Ns = 1;

@@ -90,6 +90,10 @@ void set_thread_error(const std::string& msg);
 TauLayout build_rbc_layout(int Nz, double Lx, double Lz, double kappa, double nu, double Nx_scale,
                            double b_bottom, double b_top);
 
+// Banded layout of the decoupled velocity component of the 3D program
+// (Helmholtz tau system with two lifts and two no-slip walls); needs even Nz.
+TauLayout build_helmholtz_layout(int Nz, double Lz, double nu);
+
 // Chebyshev transform matrices (row-major, N x N) built in extended precision.
 struct ChebMats {
   std::vector<double> bwd;     // grid_j = sum_n bwd[j][n] c_n

@@ -9,7 +9,7 @@ namespace tb {
 
 // Batched Chebyshev-direction GEMM (see tb_transforms.cu for the row maps).
 enum { GEMM_PLAIN = 0, GEMM_PARITY = 1, GEMM_MIRROR = 2 };
-constexpr int kGemmMaxBatch = 12;
+constexpr int kGemmMaxBatch = 16;
 struct GemmItem {
   const double* A;  // M x Kpad row-major, columns K..Kpad-1 zero (Kpad a multiple of 16)
   const double* B;  // input rows (ldb doubles apart; ldb even)
@@ -124,6 +124,11 @@ struct ClassDev {
   const double* c2_nz;
   const double* c1_z; // nb x nb
   const double* c1_nz;
+  // store targets (element offset of the unknown's row for mode 0, times 2,
+  // plus 1 when the unknown is i times the solved real column): band column
+  // j -> col_code[j], border unknown b -> left_code[b]
+  const int* col_code;
+  const int* left_code;
   // factors, shared by both classes (set on cls[0]):
   //   FR[group][row][class][kSolveModes][kFwdRec], BR[group][row][class][kSolveModes][kBwdRec],
   //   SI[group][class][4][4][kSolveModes]
@@ -137,6 +142,7 @@ struct TauArgs {
   int Nz, Nk, Nx;
   int npad;            // band rows padded to a multiple of kTauRowPad
   double k0;           // 2 pi / Lx
+  const double* kmag;  // per-mode horizontal wavenumber |k| (3D), or null for k0 * m
   double alpha, beta;  // LHS = alpha M + beta L
   // state (T space): X[4][Nz][Nk] (b, ux, uz, p) directly followed by tau[7][Nk]
   double2* X;
@@ -170,15 +176,19 @@ struct LinComb {
 // out[i] = sum_t w_t in_t[i] over count complex entries
 void launch_lincomb(const LinComb& lc, double2* out, long long count, cudaStream_t st);
 
-// MX[e][k][m] = S X_f (e = 1+f), cont rows zero; optional DC/Nyquist projection.
+// Velocity-like fields of a stage vector: nf = 3 (2D: b, u_x, u_z in X planes
+// 0..2, equation planes 1..3) or 4 (3D adds u_perp in X plane 4 with its
+// momentum rows in equation plane 4).
+// MX[e][k][m] = S X_f, cont rows zero; optional DC/Nyquist projection (2D).
 void launch_mass_apply(const double2* X, double2* MX, const double* s3, int Nz, int Nk, int Nx, int project,
-                       cudaStream_t st);
-// LX (in place over rhsP) = (rhsP - PM X)/beta - PL delta at the DC/Nyquist modes.
+                       int nf, cudaStream_t st);
+// LX (in place over rhsP) = (rhsP - PM X)/beta, minus PL delta at the 2D
+// DC/Nyquist modes when Nx > 0 (3D passes Nx = 0 and corrects separately).
 void launch_lx_finalize(double2* LX, const double2* X, const double* s3, int Nz, int Nk, int Nx, double k0,
-                        double s, double kappa, double nu, double beta, cudaStream_t st);
-// X_f = S^{-1} (lincomb)[1+f] for f = b, ux, uz; p and taus zeroed.
-void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* s3, int Nz, int Nk,
-                     cudaStream_t st);
+                        double s, double kappa, double nu, double beta, int nf, cudaStream_t st);
+// X_f = S^{-1} (lincomb)[eq(f)] for the nf velocity-like fields; p and the ntau taus zeroed.
+void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* s3, int Nz, int Nk, int nf,
+                     int ntau, cudaStream_t st);
 size_t rk_final_smem_bytes(int Nz);
 
 }  // namespace tb

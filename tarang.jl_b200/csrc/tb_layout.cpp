@@ -263,6 +263,81 @@ TauLayout build_rbc_layout(int N, double Lx, double Lz, double kappa, double nu,
   return out;
 }
 
+TauLayout build_helmholtz_layout(int N, double Lz, double nu) {
+  // One velocity component decoupled from the pressure (the 3D cross-wavevector
+  // component):  dt(u) - nu div(grad_u) + lift(tau_2) = F,
+  // grad_u = grad(u) + ez lift(tau_1),  u(z=0) = u(z=Lz) = 0.
+  // Unknown codes: UK_B for u, UK_TAU0 + 1 / + 2 for tau_1 / tau_2.  Class sg
+  // holds the coefficients and C^(2) rows of parity sg; its lowest coefficient
+  // u_sg is the border unknown, so the bulk block is tridiagonal with the
+  // dominant S_{k,k+2} / D2 entries on its diagonal.
+  TB_REQUIRE(N % 2 == 0, TB_ENOTSUPPORTED, "the 3D plan needs an even Nz");
+  TauLayout out;
+  out.Nz = N;
+  const double s = 2.0 / Lz;
+  for (int sg = 0; sg < 2; ++sg) {
+    ClassLayout& L = out.cls[sg];
+    const int tau = (sg == N % 2) ? UK_TAU0 + 1 : UK_TAU0 + 2;
+    for (int k = sg; k < N; k += 2) {
+      L.row_eq.push_back(EQ_B);
+      L.row_k.push_back(k);
+    }
+    for (int j = sg + 2; j < N; j += 2) {
+      L.col_unk.push_back(UK_B);
+      L.col_k.push_back(j);
+    }
+    L.col_unk.push_back(tau);
+    L.col_k.push_back(0);
+    L.left_unk.push_back(UK_B);
+    L.left_k.push_back(sg);
+    const int n = (int)L.row_eq.size();
+    TB_REQUIRE((int)L.col_unk.size() == n, TB_EINVAL, "helmholtz layout: rows != columns");
+    L.n = n;
+    L.nb = 1;
+    std::vector<Coef> dense((size_t)n * n, Coef{0, 0, 0, 0});
+    L.bord.assign((size_t)n, Coef{0, 0, 0, 0});
+    for (int r = 0; r < n; ++r) {
+      const int k = L.row_k[r];
+      for (int j = k; j < std::min(N, k + 5); ++j) {
+        const double Sv = S_at(N, k, j), D2v = D2_at(N, k, j, s);
+        const Coef c{Sv, -nu * D2v, 0, nu * Sv};
+        if (c.m == 0 && c.l0 == 0 && c.l2 == 0) continue;
+        if (j == sg) {
+          L.bord[r] = c;
+        } else {
+          const int col = (j - sg) / 2 - 1;
+          dense[(size_t)r * n + col] = c;
+        }
+      }
+      const double lift = (tau == UK_TAU0 + 1) ? -nu * SD_at(N, k, N - 1, s) : S_at(N, k, N - 1);
+      if (lift != 0) dense[(size_t)r * n + (n - 1)].l0 += lift;
+    }
+    int kl = 0, ku = 0;
+    for (int r = 0; r < n; ++r)
+      for (int c = 0; c < n; ++c) {
+        const Coef& d = dense[(size_t)r * n + c];
+        if (d.m == 0 && d.l0 == 0 && d.l1 == 0 && d.l2 == 0) continue;
+        kl = std::max(kl, r - c);
+        ku = std::max(ku, c - r);
+      }
+    L.kl = kl;
+    L.ku = ku;
+    const int w = kl + ku + 1;
+    L.band.assign((size_t)n * w, Coef{0, 0, 0, 0});
+    for (int r = 0; r < n; ++r)
+      for (int c = std::max(0, r - kl); c <= std::min(n - 1, r + ku); ++c)
+        L.band[(size_t)r * w + (c - r + kl)] = dense[(size_t)r * n + c];
+    // wall rows: u(z=Lz) +- u(z=0) = sum of the class's coefficients
+    L.c2_z.assign((size_t)n, 0.0);
+    L.c1_z.assign(1, 1.0);
+    for (int c = 0; c + 1 < n; ++c) L.c2_z[c] = 1.0;
+    L.c2_nz = L.c2_z;
+    L.c1_nz = L.c1_z;
+    L.bc_rhs.assign(1, 0.0);
+  }
+  return out;
+}
+
 ChebMats build_cheb_mats(int N, double Lz) {
   ChebMats m;
   typedef long double ld;

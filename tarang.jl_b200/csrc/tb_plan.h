@@ -59,6 +59,7 @@ void upload(DevBuf& d, const std::vector<T>& h) {
 
 struct ClassTables {
   DevBuf row_eq, row_k, col_unk, col_k, left_unk, left_k, bc_rhs, band, bord, c2_z, c2_nz, c1_z, c1_nz;
+  DevBuf col_code, left_code;  // store targets of the band columns / border unknowns
 };
 
 struct FactorSet {
@@ -66,6 +67,17 @@ struct FactorSet {
   DevBuf FR, BR, SI;  // solve-layout factor records (see tb_kernels.cuh)
   DevBuf PP;          // partition transfer matrices of the solve
   DevBuf HR;          // per-row backward responses of the partitioned solve
+};
+
+// One family of per-mode banded tau systems: the coupled Boussinesq system
+// (system 0) or, in 3D, the decoupled cross-wavevector velocity (system 1).
+struct TauSystem {
+  TauLayout lay;
+  ClassTables ct[2];
+  DevBuf rhs_off;  // [row][class] right-hand-side codes
+  std::vector<std::unique_ptr<FactorSet>> factors;
+  int tau_parts = 1;  // partitions of the solve (kTauParts or 1)
+  int npad = 0;       // band rows padded to a multiple of kTauRowPad
 };
 
 struct Tableau {
@@ -90,6 +102,7 @@ struct tb_plan {
   using ClassTables = tb::ClassTables;
   using FactorSet = tb::FactorSet;
   using TauLayout = tb::TauLayout;
+  using TauSystem = tb::TauSystem;
   using FftPlan = tb::FftPlan;
   tb_context* ctx = nullptr;
   tb_problem_desc d{};
@@ -99,22 +112,34 @@ struct tb_plan {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
   size_t plane = 0;  // Nz * Nk complex entries
+  // 3D (ndim 3): Fourier modes m = ix * Ny + iy over Kx = Nx/2+1 x-modes and Ny
+  // y-modes (ky in FFT order), Nk = Kx * Ny; the horizontal velocity is held as
+  // (u_par, u_perp) along / across the wavevector (u_par in the u_x slot)
+  int ndim = 2, Ny = 1, Kx = 0, My = 0;
+  int nplanes = 4;  // state planes before the taus: b, u_x|u_par, u_z, p (, u_perp)
+  int ntau = 7;     // tau rows
+  int nf = 3;       // velocity-like fields with a time derivative
+  double k0y = 0;
   // state and work arrays
-  // X holds the 4 state planes followed by the 7 tau rows (tau views its tail),
+  // X holds the state planes followed by the tau rows (tau views its tail),
   // so one 32-bit element offset from X addresses every unknown of the solve
   DevBuf X, G, H, MX0, FP[4], LXP[4], Fprev, MXprev, Rsb, tmpgrid;
   DevView tau;
+  // 3D RHS program (element type of the RHS precision): Cartesian copy of the
+  // state, Chebyshev half planes, y-transformed factors, x-pass products,
+  // y-forward output, per-pass twiddles of the padded x / y plans
+  DevBuf kmag, Xc, G3, mix3, pm3, H3, ptwX, ptwY;
+  FftPlan fpMy{};
   // transform constants
   DevBuf bwd, fwd, s3, twM, twN, ptwM;
   // parity halves of the Chebyshev matrices (H = ceil(Nz/2) rows/cols)
   DevBuf bEv, bOv, bEd, bOd, fE, fO, sfE, sfO;
   int Hz = 0, Ke = 0, Ko = 0;  // Hz = ceil(Nz/2)
   FftPlan fpM{}, fpN{};
-  // tau layout
-  TauLayout lay;
-  ClassTables ct[2];
-  std::vector<std::unique_ptr<FactorSet>> factors;
-  DevBuf err_mode, rhs_off;
+  // tau systems
+  TauSystem sys[2];
+  int nsys = 1;
+  DevBuf err_mode;
   // stepping state
   double sim_time = 0.0;
   long long iteration = 0;
@@ -124,7 +149,6 @@ struct tb_plan {
   cudaGraphExec_t gexec = nullptr;
   tb::StepGraph multi;  // graph of several steps (asynchronous / batched stepping)
   int kernels_per_step = 0;
-  int tau_parts = 1;  // partitions of the tau solve (kTauParts or 1)
   // mixed precision (TB_PREC_MIXED): FP32 copies for the RHS program
   bool mixed = false;
   DevBuf X32, G32, H32, bEv32, bOv32, bEd32, bOd32, fE32, fO32, sfE32, sfO32, ptwM32;
@@ -176,6 +200,40 @@ struct PlanSnapshot {
 };
 void plan_snapshot(tb_plan* P, PlanSnapshot* snap);
 void plan_restore(tb_plan* P, const PlanSnapshot& snap);
+
+// Profiling hook: runs fn (which enqueues one kernel) and, with profiling on,
+// brackets it with events collected after the step.
+inline cudaEvent_t take_event(tb_plan* P) {
+  if (!P->event_pool.empty()) {
+    cudaEvent_t e = P->event_pool.back();
+    P->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  TB_CUDA_TRY(cudaEventCreate(&e));
+  return e;
+}
+template <class F>
+void timed(tb_plan* P, const char* name, F&& fn) {
+  if (!P->profiling) {
+    fn();
+    return;
+  }
+  cudaEvent_t a = take_event(P), b = take_event(P);
+  TB_CUDA_TRY(cudaEventRecord(a, P->st));
+  fn();
+  TB_CUDA_TRY(cudaEventRecord(b, P->st));
+  P->pending.push_back({name, a, b});
+}
+
+// 3D program (tb_rbc3d.cu): constants and work arrays of a new plan, the RHS
+// F = -(u.grad) f for f = b, u_x, u_y, u_z written as the b, u_par, u_z, u_perp
+// momentum rows (C^(2) space, 4 planes from out4), and the L delta correction
+// of the stage L X for the Hermitian projection of the kx = 0 and Nyquist planes.
+void rbc3d_setup(tb_plan* P);
+void rbc3d_enqueue_rhs(tb_plan* P, const double2* Xin, double2* out4);
+void rbc3d_lx_project(tb_plan* P, double2* LX, double beta);
+size_t rbc3d_device_bytes(const tb_plan* P);
 
 // Error plumbing shared by the C ABI translation units.
 void record_error(tb_context* ctx, const Error& e);

@@ -1,0 +1,575 @@
+// 3D Rayleigh-Benard program: RealFourier x, RealFourier y, ChebyshevT z
+// (ChannelDomain3D, src/extras/quick_domains.jl:124-143), equations of
+// test/test_subproblem_rk.jl:50-57 with a 3-component velocity.
+//
+// Fourier modes m = ix * Ny + iy: kx = 2 pi/Lx ix (ix = 0..Nx/2, Nyquist
+// +Nx/2), ky = 2 pi/Ly [0..Ny/2-1, -Ny/2..-1] (basis_wavenumbers.jl:68-108).
+// The horizontal velocity is held along / across the wavevector,
+//   u_par = (kx u_x + ky u_y)/|k|,  u_perp = (-ky u_x + kx u_y)/|k|
+// (u_par = u_x, u_perp = u_y at k = 0); the momentum rows rotate the same way.
+// Then the pressure and continuity couple only (b, u_par, u_z, p), which is the
+// 2D system with kx replaced by |k|, and u_perp is a Helmholtz problem of its
+// own; both are exact row/column rotations of the reference's per-mode
+// Cartesian system (subproblem_matrix_build.jl:11-309), so the solution is
+// unchanged.
+//
+// RHS  F_f = -(u_x d_x f + u_y d_y f + u_z d_z f),  f = b, u_x, u_y, u_z,
+// following the lazy evaluator (lazy_rhs.jl:712-1336) and the 3/2 padded
+// product along both Fourier axes (nonlinear_padding.jl:86-103, 164-443):
+//   k3_prep   state -> Cartesian b, u_x, u_y, u_z (RHS precision)
+//   GEMM      Chebyshev backward: values and z-derivatives as even/odd half
+//             planes over the z grid (tensor-core DMMA in FP64, SIMT in FP32)
+//   k3_yinv   per (kx, z pair): value, d_y and d_z of each field with the grid
+//             round trip's Hermitian projection of the kx = 0 / Nyquist columns,
+//             the x Nyquist split, y padding with the Nyquist split, 12 inverse
+//             FFTs along y
+//   k3_xpass  per (y rows, z): d_x from the x bins, 15 real inverse FFTs along
+//             x (8 packed), the 4 products, 2 packed forward FFTs, x truncation
+//             with the Nyquist fold
+//   k3_yfwd   per (kx, z): 4 forward FFTs along y, Nyquist fold, truncation,
+//             scale, rotation of the momentum rows
+//   GEMM      Chebyshev forward into C^(2) rows (S fwd) of the stage vector.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "tb_fft.cuh"
+#include "tb_internal.h"
+#include "tb_kernels.cuh"
+#include "tb_plan.h"
+
+namespace tb {
+namespace {
+
+namespace F = tb::fftg;
+
+constexpr int kR3Threads = 256;
+
+struct R3Args {
+  int Nx, Ny, Nz, Kx, Mx, My, Nk, H;
+  double kx0, ky0;
+  FftPlan fpx, fpy;
+  int nptx, npty;
+};
+
+__device__ __forceinline__ int ky_index(int iy, int Ny) { return iy < Ny / 2 ? iy : iy - Ny; }
+
+// Rotation (cx, cy) = (kx, ky)/|k| of mode (ix, iy); (1, 0) at k = 0.
+__device__ __forceinline__ void rot_of(const R3Args& a, int ix, int iy, double& cx, double& cy) {
+  const double kx = a.kx0 * ix, ky = a.ky0 * ky_index(iy, a.Ny);
+  const double kk = sqrt(kx * kx + ky * ky);
+  if (kk > 0.0) {
+    cx = kx / kk;
+    cy = ky / kk;
+  } else {
+    cx = 1.0;
+    cy = 0.0;
+  }
+}
+
+// State (b, u_par, u_z, p, u_perp planes) -> Cartesian (b, u_x, u_y, u_z) in
+// the RHS precision.  Grid (ceil(Nk/256), Nz).
+template <class C>
+__global__ void __launch_bounds__(256) k3_prep(R3Args a, const double2* __restrict__ X, C* __restrict__ Xc) {
+  using T = typename F::Real<C>::type;
+  const int z = blockIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.Nk) return;
+  const size_t plane = (size_t)a.Nz * a.Nk, i = (size_t)z * a.Nk + m;
+  double cx, cy;
+  rot_of(a, m / a.Ny, m % a.Ny, cx, cy);
+  const double2 b = X[i], up = X[plane + i], uz = X[2 * plane + i], uq = X[4 * plane + i];
+  Xc[i] = F::mk<C>((T)b.x, (T)b.y);
+  Xc[plane + i] = F::mk<C>((T)(cx * up.x - cy * uq.x), (T)(cx * up.y - cy * uq.y));
+  Xc[2 * plane + i] = F::mk<C>((T)(cy * up.x + cx * uq.x), (T)(cy * up.y + cx * uq.y));
+  Xc[3 * plane + i] = F::mk<C>((T)uz.x, (T)uz.y);
+}
+
+// Per (kx column ix, z pair j / Nz-1-j).  G: 16 half planes (field f, w) at
+// G + (4 f + w) hplane, w = 0 even values, 1 odd values, 2 even d_z, 3 odd d_z,
+// element (j, m).  Output mix[z][q][ix][y], q = 3 f + kind (value, d_y, d_z).
+template <class C>
+__global__ void __launch_bounds__(kR3Threads) k3_yinv(R3Args a, const C* __restrict__ G, const C* __restrict__ pty,
+                                                       C* __restrict__ mix) {
+  using T = typename F::Real<C>::type;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  C* sm = reinterpret_cast<C*>(sm_raw);
+  const int Ny = a.Ny, My = a.My, ix = blockIdx.x, j = blockIdx.y;
+  const int Ms = (My + 7) & ~7;
+  C* stg = sm;                    // [16][Ny]
+  C* A = stg + 16 * Ny;           // [12][Ms]
+  C* B = A + 12 * Ms;             // [12][Ms]
+  C* pt = B + 12 * Ms;            // [npty]
+  const size_t hplane = (size_t)a.H * a.Nk;
+  for (int t = threadIdx.x; t < a.npty; t += blockDim.x) pt[t] = pty[t];
+  for (int t = threadIdx.x; t < 16 * Ny; t += blockDim.x) {
+    const int q = t / Ny, iy = t - q * Ny;
+    stg[t] = G[(size_t)q * hplane + (size_t)j * a.Nk + (size_t)ix * Ny + iy];
+  }
+  __syncthreads();
+  const bool edge = (ix == 0) || (2 * ix == a.Nx);  // columns whose grid round trip is Hermitian
+  const T xs = (2 * ix == a.Nx) ? (T)0.5 : (T)1.0;  // even-N Nyquist split along x
+  for (int lev = 0; lev < 2; ++lev) {
+    const int zl = lev ? a.Nz - 1 - j : j;
+    // value (kind 0, 1) or z-derivative (kind 2) of field f at grid level zl
+    auto base = [&](int f, int kind, int iy) -> C {
+      const C e = stg[(4 * f + (kind == 2 ? 2 : 0)) * Ny + iy];
+      const C o = stg[(4 * f + (kind == 2 ? 3 : 1)) * Ny + iy];
+      if (kind == 2) return lev ? F::sub(o, e) : F::add(e, o);
+      return lev ? F::sub(e, o) : F::add(e, o);
+    };
+    for (int t = threadIdx.x; t < 12 * Ms; t += blockDim.x) A[t] = F::mk<C>((T)0, (T)0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < 12 * Ny; t += blockDim.x) {
+      const int q = t / Ny, iy = t - q * Ny;
+      const int f = q / 3, kind = q - 3 * f;
+      // the factor is a derivative of the field's grid round trip, so the
+      // projection comes first (it differs from projecting i ky v at the
+      // self-paired ky = -Ny/2 mode)
+      C v = base(f, kind, iy);
+      if (edge) {
+        const C w = base(f, kind, (Ny - iy) % Ny);
+        v = F::mk<C>((T)0.5 * (v.x + w.x), (T)0.5 * (v.y - w.y));
+      }
+      if (kind == 1) {
+        const T kyv = (T)(a.ky0 * ky_index(iy, Ny));
+        v = F::mk<C>(-kyv * v.y, kyv * v.x);  // i ky v
+      }
+      v = F::scale(v, xs);
+      C* col = A + (size_t)q * Ms;
+      if (2 * iy < Ny) {
+        col[F::fidx<true>(iy)] = v;
+      } else if (2 * iy == Ny) {
+        const C h = F::scale(v, (T)0.5);
+        col[F::fidx<true>(Ny / 2)] = h;
+        col[F::fidx<true>(My - Ny / 2)] = h;
+      } else {
+        col[F::fidx<true>(My - Ny + iy)] = v;
+      }
+    }
+    __syncthreads();
+    C* R = F::fft_batch<true>(A, B, 12, Ms, a.fpy, pt, +1);
+    for (int t = threadIdx.x; t < 12 * My; t += blockDim.x) {
+      const int q = t / My, y = t - q * My;
+      mix[(((size_t)zl * 12 + q) * a.Kx + ix) * My + y] = R[(size_t)q * Ms + F::fidx<true>(y)];
+    }
+    __syncthreads();
+  }
+}
+
+// Per (RR consecutive padded y rows, z level).  mix[z][q][kx][y] ->
+// pm[z][f][kx][y] (f = b, u_x, u_y, u_z; kx < Kx, Nyquist folded).
+template <class C, int RR>
+__global__ void __launch_bounds__(kR3Threads) k3_xpass(R3Args a, const C* __restrict__ mix, const C* __restrict__ ptx,
+                                                        C* __restrict__ pm) {
+  using T = typename F::Real<C>::type;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  C* sm = reinterpret_cast<C*>(sm_raw);
+  const int Mx = a.Mx, Kx = a.Kx, My = a.My, hN = a.Nx / 2;
+  const int y0 = blockIdx.x * RR, z = blockIdx.y;
+  const int Ms = (Mx + 7) & ~7;
+  constexpr int NB = 8 * RR;
+  C* Z = sm;              // [NB][Ms]
+  C* S = Z + NB * Ms;     // [NB][Ms]
+  C* pt = S + NB * Ms;    // [nptx]
+  for (int t = threadIdx.x; t < a.nptx; t += blockDim.x) pt[t] = ptx[t];
+  const int nh = Mx / 2 + 1;
+  // half-spectrum bin k of factor idx (0 u_x, 1 u_y, 2 u_z, 3..6 d_x f, 7..10
+  // d_y f, 11..14 d_z f, 15 none) on row y0 + r; DC and Nyquist kept real
+  auto fac = [&](int idx, int r, int k) -> C {
+    if (idx >= 15 || k >= Kx) return F::mk<C>((T)0, (T)0);
+    int q;
+    bool dx = false;
+    if (idx < 3) {
+      q = 3 * (idx + 1);
+    } else if (idx < 7) {
+      q = 3 * (idx - 3);
+      dx = true;
+    } else if (idx < 11) {
+      q = 3 * (idx - 7) + 1;
+    } else {
+      q = 3 * (idx - 11) + 2;
+    }
+    if (dx && (k == 0 || k == hN)) return F::mk<C>((T)0, (T)0);
+    C v = mix[(((size_t)z * 12 + q) * Kx + k) * My + y0 + r];
+    if (k == 0 || k == hN) v.y = (T)0;
+    if (dx) {
+      const T kk = (T)(a.kx0 * k);
+      v = F::mk<C>(-kk * v.y, kk * v.x);  // i kx v
+    }
+    return v;
+  };
+  for (int t = threadIdx.x; t < RR * 8 * nh; t += blockDim.x) {
+    const int r = t % RR, rest = t / RR;
+    const int k = rest % nh, p = rest / nh;
+    const C A = fac(2 * p, r, k), B = fac(2 * p + 1, r, k);
+    C* dst = Z + (size_t)(r * 8 + p) * Ms;
+    // spectrum of a + i b: A + i B at k, conj(A) + i conj(B) at Mx - k
+    dst[F::fidx<true>(k)] = F::mk<C>(A.x - B.y, A.y + B.x);
+    if (k > 0 && k < Mx / 2) dst[F::fidx<true>(Mx - k)] = F::mk<C>(A.x + B.y, -A.y + B.x);
+  }
+  __syncthreads();
+  C* Rg = F::fft_batch<true>(Z, S, NB, Ms, a.fpx, pt, +1);
+  C* W = (Rg == Z) ? S : Z;
+  for (int t = threadIdx.x; t < RR * Mx; t += blockDim.x) {
+    const int r = t / Mx, x = t - r * Mx;
+    const int i = F::fidx<true>(x);
+    const C* g = Rg + (size_t)r * 8 * Ms;
+    const C z0 = g[i], z1 = g[Ms + i], z2 = g[2 * Ms + i], z3 = g[3 * Ms + i];
+    const C z4 = g[4 * Ms + i], z5 = g[5 * Ms + i], z6 = g[6 * Ms + i], z7 = g[7 * Ms + i];
+    const T ux = z0.x, uy = z0.y, uz = z1.x;
+    const T pb = ux * z1.y + uy * z3.y + uz * z5.y;   // d_x b, d_y b, d_z b
+    const T pu = ux * z2.x + uy * z4.x + uz * z6.x;   // d_x u_x, d_y u_x, d_z u_x
+    const T pv = ux * z2.y + uy * z4.y + uz * z6.y;   // d_x u_y, d_y u_y, d_z u_y
+    const T pw = ux * z3.x + uy * z5.x + uz * z7.x;   // d_x u_z, d_y u_z, d_z u_z
+    W[(size_t)(2 * r) * Ms + i] = F::mk<C>(pb, pu);
+    W[(size_t)(2 * r + 1) * Ms + i] = F::mk<C>(pv, pw);
+  }
+  __syncthreads();
+  C* Fq = F::fft_batch<true>(W, Rg, 2 * RR, Ms, a.fpx, pt, -1);
+  for (int t = threadIdx.x; t < RR * 2 * Kx; t += blockDim.x) {
+    const int r = t % RR, rest = t / RR;
+    const int k = rest % Kx, h = rest / Kx;
+    const C* buf = Fq + (size_t)(2 * r + h) * Ms;
+    const C c = buf[F::fidx<true>(k)], cm = buf[F::fidx<true>((Mx - k) % Mx)];
+    // first: (c + conj(cm))/2, second: (c - conj(cm))/(2i)
+    C o1 = F::mk<C>((T)0.5 * (c.x + cm.x), (T)0.5 * (c.y - cm.y));
+    C o2 = F::mk<C>((T)0.5 * (c.y + cm.y), (T)-0.5 * (c.x - cm.x));
+    if (k == 0) {
+      o1.y = (T)0;
+      o2.y = (T)0;
+    } else if (k == hN) {  // fold of the -Nx/2 image: 2 Re
+      o1 = F::mk<C>((T)2 * o1.x, (T)0);
+      o2 = F::mk<C>((T)2 * o2.x, (T)0);
+    }
+    pm[(((size_t)z * 4 + 2 * h) * Kx + k) * My + y0 + r] = o1;
+    pm[(((size_t)z * 4 + 2 * h + 1) * Kx + k) * My + y0 + r] = o2;
+  }
+}
+
+// Per (kx column ix, z level): forward FFTs along y of the 4 products, y
+// Nyquist fold and truncation, F = -P / (Nx Ny Mx My), rotation of the
+// horizontal momentum rows; out[f][z][m] for f = b, u_par, u_z, u_perp.
+template <class C>
+__global__ void __launch_bounds__(kR3Threads) k3_yfwd(R3Args a, const C* __restrict__ pm, const C* __restrict__ pty,
+                                                       C* __restrict__ out) {
+  using T = typename F::Real<C>::type;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  C* sm = reinterpret_cast<C*>(sm_raw);
+  const int Ny = a.Ny, My = a.My, ix = blockIdx.x, z = blockIdx.y;
+  const int Ms = (My + 7) & ~7;
+  C* A = sm;
+  C* B = A + 4 * Ms;
+  C* pt = B + 4 * Ms;
+  for (int t = threadIdx.x; t < a.npty; t += blockDim.x) pt[t] = pty[t];
+  for (int t = threadIdx.x; t < 4 * My; t += blockDim.x) {
+    const int f = t / My, y = t - f * My;
+    A[(size_t)f * Ms + F::fidx<true>(y)] = pm[(((size_t)z * 4 + f) * a.Kx + ix) * My + y];
+  }
+  __syncthreads();
+  const C* Q = F::fft_batch<true>(A, B, 4, Ms, a.fpy, pt, -1);
+  const double sc = -1.0 / ((double)a.Nx * (double)Ny * (double)a.Mx * (double)My);
+  const size_t plane = (size_t)a.Nz * a.Nk;
+  for (int iy = threadIdx.x; iy < Ny; iy += blockDim.x) {
+    double2 v[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      const C* col = Q + (size_t)f * Ms;
+      C r;
+      if (2 * iy < Ny) {
+        r = col[F::fidx<true>(iy)];
+      } else if (2 * iy == Ny) {
+        r = F::add(col[F::fidx<true>(Ny / 2)], col[F::fidx<true>(My - Ny / 2)]);
+      } else {
+        r = col[F::fidx<true>(My - Ny + iy)];
+      }
+      v[f] = make_double2(sc * (double)r.x, sc * (double)r.y);
+    }
+    double cx, cy;
+    rot_of(a, ix, iy, cx, cy);
+    const size_t e = (size_t)z * a.Nk + (size_t)ix * Ny + iy;
+    out[e] = F::mk<C>((T)v[0].x, (T)v[0].y);
+    out[plane + e] = F::mk<C>((T)(cx * v[1].x + cy * v[2].x), (T)(cx * v[1].y + cy * v[2].y));
+    out[2 * plane + e] = F::mk<C>((T)v[3].x, (T)v[3].y);
+    out[3 * plane + e] = F::mk<C>((T)(-cy * v[1].x + cx * v[2].x), (T)(-cy * v[1].y + cx * v[2].y));
+  }
+}
+
+// L delta for the Hermitian projection of the kx = 0 and kx = Nx/2 planes
+// (the grid round trip of the stage fields, step_subproblem_rk.jl gathers
+// through coeff_data!), subtracted from the stage L X:
+//   delta = (X(m) - conj X(m'))/2 in Cartesian components, m' = (ix, -ky),
+//   cont  i kx S d_ux + i ky S d_uy + SD d_uz
+//   b     kappa (k^2 S - D2) d_b
+//   mom   nu (k^2 S - D2) d_u  (- S d_b in z), rotated to (par, perp) rows.
+// One thread per (row k, plane, iy): grid (ceil(2 Ny / 128), Nz).
+__global__ void __launch_bounds__(128) k3_lx_project(R3Args a, double2* __restrict__ LX, const double2* __restrict__ X,
+                                                     const double* __restrict__ s3, double s, double kappa, double nu,
+                                                     double beta) {
+  const int k = blockIdx.y, t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2 * a.Ny) return;
+  const int Ny = a.Ny, Nz = a.Nz, Nk = a.Nk;
+  const int ix = (t < Ny) ? 0 : a.Kx - 1, iy = t % Ny;
+  const int iyp = (Ny - iy) % Ny;
+  const int m = ix * Ny + iy, mp = ix * Ny + iyp;
+  const size_t plane = (size_t)Nz * Nk;
+  double cx, cy, px, py;
+  rot_of(a, ix, iy, cx, cy);
+  rot_of(a, ix, iyp, px, py);
+  // Cartesian delta of field f (0 b, 1 u_x, 2 u_y, 3 u_z) at row kk
+  auto delta = [&](int f, int kk) -> double2 {
+    if (kk >= Nz) return make_double2(0.0, 0.0);
+    const size_t i = (size_t)kk * Nk + m, ip = (size_t)kk * Nk + mp;
+    double2 v, w;
+    if (f == 0) {
+      v = X[i];
+      w = X[ip];
+    } else if (f == 3) {
+      v = X[2 * plane + i];
+      w = X[2 * plane + ip];
+    } else {
+      const double2 up = X[plane + i], uq = X[4 * plane + i];
+      const double2 wp = X[plane + ip], wq = X[4 * plane + ip];
+      if (f == 1) {
+        v = make_double2(cx * up.x - cy * uq.x, cx * up.y - cy * uq.y);
+        w = make_double2(px * wp.x - py * wq.x, px * wp.y - py * wq.y);
+      } else {
+        v = make_double2(cy * up.x + cx * uq.x, cy * up.y + cx * uq.y);
+        w = make_double2(py * wp.x + px * wq.x, py * wp.y + px * wq.y);
+      }
+    }
+    return make_double2(0.5 * (v.x - w.x), 0.5 * (v.y + w.y));
+  };
+  const double s0 = s3[3 * k], s1 = s3[3 * k + 1], s2 = s3[3 * k + 2];
+  auto Sd = [&](int f) -> double2 {
+    const double2 d0 = delta(f, k), d2 = delta(f, k + 2), d4 = delta(f, k + 4);
+    return make_double2(s0 * d0.x + s1 * d2.x + s2 * d4.x, s0 * d0.y + s1 * d2.y + s2 * d4.y);
+  };
+  const double kx = a.kx0 * ix, ky = a.ky0 * ky_index(iy, Ny), k2 = kx * kx + ky * ky;
+  const double d2c = 2.0 * (k + 2) * s * s;
+  const double2 Sb = Sd(0), Sux = Sd(1), Suy = Sd(2), Suz = Sd(3);
+  const double2 Db = delta(0, k + 2), Dux = delta(1, k + 2), Duy = delta(2, k + 2), Duz = delta(3, k + 2);
+  const double2 u1 = delta(3, k + 1), u3 = delta(3, k + 3);
+  double2 L[5];
+  // continuity: i kx S d_ux + i ky S d_uy + SD d_uz
+  L[0] = make_double2(-kx * Sux.y - ky * Suy.y + s * (u1.x - u3.x), kx * Sux.x + ky * Suy.x + s * (u1.y - u3.y));
+  L[1] = make_double2(kappa * (k2 * Sb.x - d2c * Db.x), kappa * (k2 * Sb.y - d2c * Db.y));
+  const double2 mx = make_double2(nu * (k2 * Sux.x - d2c * Dux.x), nu * (k2 * Sux.y - d2c * Dux.y));
+  const double2 my = make_double2(nu * (k2 * Suy.x - d2c * Duy.x), nu * (k2 * Suy.y - d2c * Duy.y));
+  L[3] = make_double2(nu * (k2 * Suz.x - d2c * Duz.x) - Sb.x, nu * (k2 * Suz.y - d2c * Duz.y) - Sb.y);
+  L[2] = make_double2(cx * mx.x + cy * my.x, cx * mx.y + cy * my.y);
+  L[4] = make_double2(-cy * mx.x + cx * my.x, -cy * mx.y + cx * my.y);
+  (void)beta;
+  const size_t i = (size_t)k * Nk + m;
+#pragma unroll
+  for (int e = 0; e < 5; ++e) {
+    double2 r = LX[(size_t)e * plane + i];
+    r.x -= L[e].x;
+    r.y -= L[e].y;
+    LX[(size_t)e * plane + i] = r;
+  }
+}
+
+template <class C>
+std::vector<C> pass_twiddles_t(const FftPlan& fp) {
+  std::vector<C> t;
+  const long double pi = 3.141592653589793238462643383279502884L;
+  int Ns = 1;
+  for (int s = 0; s < fp.nstages; ++s) {
+    const int R = fp.radix[s];
+    const int tstride = fp.n / (Ns * R);
+    for (int j = 0; j < Ns; ++j) {
+      const long double ang = -2.0L * pi * (long double)(j * tstride) / (long double)fp.n;
+      C c;
+      c.x = (decltype(c.x))cosl(ang);
+      c.y = (decltype(c.y))sinl(ang);
+      t.push_back(c);
+    }
+    Ns *= R;
+  }
+  return t;
+}
+
+R3Args args_of(const tb_plan* P) {
+  R3Args a{};
+  a.Nx = P->Nx;
+  a.Ny = P->Ny;
+  a.Nz = P->Nz;
+  a.Kx = P->Kx;
+  a.Mx = P->M;
+  a.My = P->My;
+  a.Nk = P->Nk;
+  a.H = P->Nz / 2;
+  a.kx0 = P->k0;
+  a.ky0 = P->k0y;
+  a.fpx = P->fpM;
+  a.fpy = P->fpMy;
+  a.nptx = F::pass_twiddle_count(P->fpM);
+  a.npty = F::pass_twiddle_count(P->fpMy);
+  return a;
+}
+
+template <class C>
+size_t yinv_smem(const R3Args& a) {
+  const size_t Ms = (size_t)((a.My + 7) & ~7);
+  return (16 * (size_t)a.Ny + 24 * Ms + (size_t)a.npty) * sizeof(C);
+}
+template <class C, int RR>
+size_t xpass_smem(const R3Args& a) {
+  const size_t Ms = (size_t)((a.Mx + 7) & ~7);
+  return (16 * RR * Ms + (size_t)a.nptx) * sizeof(C);
+}
+template <class C>
+size_t yfwd_smem(const R3Args& a) {
+  const size_t Ms = (size_t)((a.My + 7) & ~7);
+  return (8 * Ms + (size_t)a.npty) * sizeof(C);
+}
+
+// Rows per x-pass CTA: 2 in FP32, 1 in FP64 (same shared memory).
+template <class C>
+struct XRows;
+template <>
+struct XRows<float2> {
+  static constexpr int value = 2;
+};
+template <>
+struct XRows<double2> {
+  static constexpr int value = 1;
+};
+
+template <class C>
+void set_limits(int bytes) {
+  constexpr int RR = XRows<C>::value;
+  TB_CUDA_TRY(cudaFuncSetAttribute(k3_yinv<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  TB_CUDA_TRY(cudaFuncSetAttribute(k3_xpass<C, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  TB_CUDA_TRY(cudaFuncSetAttribute(k3_yfwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+}
+
+inline int pad16(int k) { return (k + 15) / 16 * 16; }
+
+template <class C>
+void enqueue_rhs_t(tb_plan* P, const double2* Xin, double2* out4) {
+  constexpr int RR = XRows<C>::value;
+  const R3Args a = args_of(P);
+  const int N = P->Nz, H = N / 2;
+  const size_t plane = P->plane, hplane = (size_t)H * P->Nk;
+  const int ncol = 2 * P->Nk;
+  C* Xc = P->Xc.as<C>();
+  C* G = P->G3.as<C>();
+  timed(P, "rhs3_prep", [&] {
+    k3_prep<C><<<dim3((P->Nk + 255) / 256, N), 256, 0, P->st>>>(a, Xin, Xc);
+  });
+  constexpr bool f32 = sizeof(C) == sizeof(float2);
+  if constexpr (f32) {
+    GemmBatch32 bt{};
+    const float* Am[4] = {P->bEv32.as<float>(), P->bOv32.as<float>(), P->bEd32.as<float>(), P->bOd32.as<float>()};
+    for (int f = 0; f < 4; ++f)
+      for (int w = 0; w < 4; ++w)
+        bt.item[4 * f + w] = GemmItem32{Am[w], reinterpret_cast<const float*>(Xc + (size_t)f * plane),
+                                        G + (size_t)(4 * f + w) * hplane, H, (w & 1) ? P->Ko : P->Ke,
+                                        pad16((w & 1) ? P->Ko : P->Ke), GEMM_PARITY, w & 1};
+    timed(P, "z_backward_gemm", [&] { launch_gemm_f32(bt, 16, ncol, ncol, ncol, N, false, P->st); });
+  } else {
+    GemmBatch bt{};
+    const double* Am[4] = {P->bEv.as<double>(), P->bOv.as<double>(), P->bEd.as<double>(), P->bOd.as<double>()};
+    for (int f = 0; f < 4; ++f)
+      for (int w = 0; w < 4; ++w)
+        bt.item[4 * f + w] = GemmItem{Am[w], reinterpret_cast<const double*>(Xc + (size_t)f * plane),
+                                      reinterpret_cast<double*>(G + (size_t)(4 * f + w) * hplane), H,
+                                      (w & 1) ? P->Ko : P->Ke, pad16((w & 1) ? P->Ko : P->Ke), GEMM_PARITY, w & 1};
+    timed(P, "z_backward_gemm", [&] { launch_gemm_f64(bt, 16, ncol, ncol, ncol, N, P->st); });
+  }
+  timed(P, "rhs3_yinv", [&] {
+    k3_yinv<C><<<dim3(P->Kx, H), kR3Threads, yinv_smem<C>(a), P->st>>>(a, G, P->ptwY.as<C>(), P->mix3.as<C>());
+  });
+  timed(P, "rhs3_xpass", [&] {
+    k3_xpass<C, RR><<<dim3(P->My / RR, N), kR3Threads, xpass_smem<C, RR>(a), P->st>>>(
+        a, P->mix3.as<C>(), P->ptwX.as<C>(), P->pm3.as<C>());
+  });
+  timed(P, "rhs3_yfwd", [&] {
+    k3_yfwd<C><<<dim3(P->Kx, N), kR3Threads, yfwd_smem<C>(a), P->st>>>(a, P->pm3.as<C>(), P->ptwY.as<C>(),
+                                                                        P->H3.as<C>());
+  });
+  const C* H3 = P->H3.as<C>();
+  if constexpr (f32) {
+    GemmBatch32 bf{};
+    int nb = 0;
+    for (int f = 0; f < 4; ++f) {
+      const float* in = reinterpret_cast<const float*>(H3 + (size_t)f * plane);
+      double* out = reinterpret_cast<double*>(out4 + (size_t)f * plane);
+      bf.item[nb++] = GemmItem32{P->sfE32.as<float>(), in, out, P->Ke, H, pad16(H), GEMM_MIRROR, 0};
+      bf.item[nb++] = GemmItem32{P->sfO32.as<float>(), in, out, P->Ko, H, pad16(H), GEMM_MIRROR, 1};
+    }
+    timed(P, "z_forward_gemm", [&] { launch_gemm_f32(bf, nb, ncol, ncol, ncol, N, true, P->st); });
+  } else {
+    GemmBatch bf{};
+    int nb = 0;
+    for (int f = 0; f < 4; ++f) {
+      const double* in = reinterpret_cast<const double*>(H3 + (size_t)f * plane);
+      double* out = reinterpret_cast<double*>(out4 + (size_t)f * plane);
+      bf.item[nb++] = GemmItem{P->sfE.as<double>(), in, out, P->Ke, H, pad16(H), GEMM_MIRROR, 0};
+      bf.item[nb++] = GemmItem{P->sfO.as<double>(), in, out, P->Ko, H, pad16(H), GEMM_MIRROR, 1};
+    }
+    timed(P, "z_forward_gemm", [&] { launch_gemm_f64(bf, nb, ncol, ncol, ncol, N, P->st); });
+  }
+}
+
+template <class C>
+void setup_t(tb_plan* P) {
+  constexpr int RR = XRows<C>::value;
+  const R3Args a = args_of(P);
+  TB_REQUIRE(P->My % RR == 0, TB_ENOTSUPPORTED, "padded Ny must be a multiple of the x-pass rows");
+  const size_t lim = 227 * 1024;
+  const size_t xs = xpass_smem<C, RR>(a);
+  TB_REQUIRE(yinv_smem<C>(a) <= lim && xs <= lim && yfwd_smem<C>(a) <= lim, TB_ENOTSUPPORTED,
+             "Nx or Ny too large for the 3D transform kernels");
+  set_limits<C>((int)lim);
+  const size_t plane = P->plane, H = (size_t)P->Nz / 2;
+  P->Xc.alloc(4 * plane * sizeof(C));
+  P->G3.alloc(16 * H * P->Nk * sizeof(C));
+  const size_t slab = (size_t)P->Nz * P->Kx * P->My;
+  P->mix3.alloc(12 * slab * sizeof(C));
+  P->pm3.alloc(4 * slab * sizeof(C));
+  P->H3.alloc(4 * plane * sizeof(C));
+  upload(P->ptwX, pass_twiddles_t<C>(P->fpM));
+  upload(P->ptwY, pass_twiddles_t<C>(P->fpMy));
+}
+
+}  // namespace
+
+void rbc3d_setup(tb_plan* P) {
+  TB_REQUIRE(make_fft_plan(P->My, &P->fpMy), TB_ENOTSUPPORTED, "Ny must be of the form 2^a 3^b");
+  std::vector<double> km(P->Nk);
+  for (int ix = 0; ix < P->Kx; ++ix)
+    for (int iy = 0; iy < P->Ny; ++iy) {
+      const double kx = P->k0 * ix, ky = P->k0y * (iy < P->Ny / 2 ? iy : iy - P->Ny);
+      km[(size_t)ix * P->Ny + iy] = std::sqrt(kx * kx + ky * ky);
+    }
+  upload(P->kmag, km);
+  if (P->mixed)
+    setup_t<float2>(P);
+  else
+    setup_t<double2>(P);
+}
+
+void rbc3d_enqueue_rhs(tb_plan* P, const double2* Xin, double2* out4) {
+  if (P->mixed)
+    enqueue_rhs_t<float2>(P, Xin, out4);
+  else
+    enqueue_rhs_t<double2>(P, Xin, out4);
+}
+
+void rbc3d_lx_project(tb_plan* P, double2* LX, double beta) {
+  const R3Args a = args_of(P);
+  timed(P, "lx_project", [&] {
+    k3_lx_project<<<dim3((2 * P->Ny + 127) / 128, P->Nz), 128, 0, P->st>>>(
+        a, LX, P->X.as<double2>(), P->s3.as<double>(), P->s, P->d.kappa, P->d.nu, beta);
+  });
+}
+
+size_t rbc3d_device_bytes(const tb_plan* P) {
+  return P->kmag.bytes + P->Xc.bytes + P->G3.bytes + P->mix3.bytes + P->pm3.bytes + P->H3.bytes + P->ptwX.bytes +
+         P->ptwY.bytes;
+}
+
+}  // namespace tb

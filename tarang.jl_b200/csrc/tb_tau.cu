@@ -29,10 +29,6 @@ __device__ __forceinline__ double2 cfma(double a, double2 x, double2 acc) {
   return make_double2(fma(a, x.x, acc.x), fma(a, x.y, acc.y));
 }
 
-__device__ __forceinline__ bool realified(int unk) {
-  return unk == UK_UX || unk == UK_TAU0 + 3 || unk == UK_TAU0 + 5;
-}
-
 // Solve-layout factor records: for group g = m / kSolveModes and band row j the
 // records of both classes and the group's modes are contiguous,
 // FR[g][j][class][mode % kSolveModes][kFwdRec] (and BR likewise), so one lane
@@ -69,7 +65,7 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
   constexpr int WW = 2 * KL + KU + 1;
   constexpr int W1 = KL + KU + 1;
   const int Nk = a.Nk;
-  const double kx = a.k0 * m;
+  const double kx = a.kmag ? a.kmag[m] : a.k0 * m;
   const bool zmode = (m == 0);
   // per-thread work arrays interleaved across the 2 Nk threads (element i of a
   // thread at scratch[i * 2Nk + t]) so that a warp's accesses coalesce
@@ -155,13 +151,8 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
     br[0] = dinv;
     for (int t = 1; t < W1; ++t) br[t] = (j + t < n) ? W[(size_t)j * WW + KL + t] : 0.0;
     for (int b = 0; b < NBMAX; ++b) br[W1 + b] = (b < nb) ? Bd[(size_t)j * NBMAX + b] : 0.0;
-    {
-      // store target of this band column: element offset (per mode) into X or the tau
-      // array, encoded as offset*2 + (1 if the unknown is scaled by i), bit-cast
-      const int unk = C.col_unk[j], kk = C.col_k[j];
-      const long long off = unk < 4 ? ((long long)unk * a.Nz + kk) * Nk : (long long)4 * a.Nz * Nk + (long long)(unk - UK_TAU0) * Nk;
-      br[kBwdCode] = __longlong_as_double(2 * off + (realified(unk) ? 1 : 0));
-    }
+    // store target of this band column (element offset of its row * 2 + the i flag), bit-cast
+    br[kBwdCode] = __longlong_as_double((long long)C.col_code[j]);
   }
   // padding rows n..npad-1: identity rows with no right-hand side and no store
   for (int j = n; j < a.npad; ++j) {
@@ -271,8 +262,8 @@ __host__ __device__ constexpr size_t part_stage_doubles() {
   return F > B ? (F > H ? F : H) : (B > H ? B : H);
 }
 
-// X (4 planes) and tau (7 x Nk) are one allocation, so a 32-bit element
-// offset from X addresses both; code = 2 * offset + (1 if the unknown is i
+// X (the state planes) and the tau rows are one allocation, so a 32-bit
+// element offset from X addresses both; code = 2 * offset + (1 if the unknown is i
 // times the solved real-ified column), -1 for no store.  u_x = i v gives
 // re(u_x) = -v_im (part-1 lane) and im(u_x) = v_re (part-0 lane).
 __device__ __forceinline__ void store_unknown(double* Xd, int code, int m, int part, double x, bool on) {
@@ -654,12 +645,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   if (warp == 0) {
 #pragma unroll
     for (int b = 0; b < NBMAX; ++b) {
-      if (live && b < a.cls[c].nb) {
-        const int unk = a.cls[c].left_unk[b];
-        const int k = a.cls[c].left_k[b];
-        const int off = unk < 4 ? (unk * a.Nz + k) * Nk : 4 * a.Nz * Nk + (unk - UK_TAU0) * Nk;
-        store_unknown(Xd, 2 * off + (realified(unk) ? 1 : 0), m, part, x1[b], true);
-      }
+      if (live && b < a.cls[c].nb) store_unknown(Xd, a.cls[c].left_code[b], m, part, x1[b], true);
     }
   }
 }
@@ -760,31 +746,35 @@ __global__ void k_lincomb(LinComb lc, double2* __restrict__ out, long long count
 
 __device__ __forceinline__ double2 proj(double2 v, bool p) { return p ? make_double2(v.x, 0.0) : v; }
 
+// State plane and equation plane of velocity-like field q (b, u_x / u_par,
+// u_z, then u_perp in 3D).
+__device__ __forceinline__ int xplane_of(int q) { return q < 3 ? q : 4; }
+__device__ __forceinline__ int eplane_of(int q) { return q < 3 ? 1 + q : 4; }
+
 // One thread per (row k, mode m): grid (ceil(Nk / 128), Nz).
 __global__ void __launch_bounds__(128) k_mass_apply(const double2* __restrict__ X, double2* __restrict__ MX,
                                                     const double* __restrict__ s3, int Nz, int Nk, int Nx,
-                                                    int project) {
+                                                    int project, int nf) {
   const int k = blockIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= Nk) return;
   const size_t i = (size_t)k * Nk + m;
   const bool pj = project && (m == 0 || 2 * m == Nx);
   const double s0 = s3[3 * k], s1 = s3[3 * k + 1], s2 = s3[3 * k + 2];
   MX[i] = make_double2(0.0, 0.0);
-#pragma unroll
-  for (int f = 0; f < 3; ++f) {
-    const double2* Xf = X + (size_t)f * Nz * Nk;
+  for (int f = 0; f < nf; ++f) {
+    const double2* Xf = X + (size_t)xplane_of(f) * Nz * Nk;
     double2 acc = make_double2(0.0, 0.0);
     acc = cfma(s0, proj(Xf[i], pj), acc);
     if (k + 2 < Nz) acc = cfma(s1, proj(Xf[i + 2 * (size_t)Nk], pj), acc);
     if (k + 4 < Nz) acc = cfma(s2, proj(Xf[i + 4 * (size_t)Nk], pj), acc);
-    MX[(size_t)(1 + f) * Nz * Nk + i] = acc;
+    MX[(size_t)eplane_of(f) * Nz * Nk + i] = acc;
   }
 }
 
 // One thread per (row k, mode m): grid (ceil(Nk / 128), Nz).
 __global__ void __launch_bounds__(128) k_lx_finalize(double2* __restrict__ LX, const double2* __restrict__ X,
                                                      const double* __restrict__ s3, int Nz, int Nk, int Nx, double k0,
-                                                     double s, double kappa, double nu, double beta) {
+                                                     double s, double kappa, double nu, double beta, int nf) {
   const double ib = 1.0 / beta;
   {
     const int k = blockIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -812,7 +802,12 @@ __global__ void __launch_bounds__(128) k_lx_finalize(double2* __restrict__ LX, c
       }
       out[e] = make_double2(r.x * ib, r.y * ib);
     }
-    if (m == 0 || 2 * m == Nx) {
+    if (nf > 3) {  // u_perp rows (3D): the equation plane after the pressure
+      double2 r = LX[4 * plane + i];
+      const double2 mx = Sx(4);
+      LX[4 * plane + i] = make_double2((r.x - mx.x) * ib, (r.y - mx.y) * ib);
+    }
+    if (Nx > 0 && (m == 0 || 2 * m == Nx)) {
       // L applied to delta = i Im(X) of b, ux, uz (the part a grid round trip drops)
       const double kx = k0 * m, kx2 = kx * kx;
       auto dl = [&](int f, int kk) -> double { return (kk < Nz) ? X[((size_t)f * Nz + kk) * Nk + m].y : 0.0; };
@@ -858,7 +853,7 @@ __global__ void __launch_bounds__(256) k_rk_final(LinComb lc, double2* __restric
     sk[3 * q + 1] = s3[3 * k + 1];
     sk[3 * q + 2] = s3[3 * k + 2];
   }
-  const size_t base = (size_t)(1 + f) * plane;  // equation rows b, mx, mz follow continuity
+  const size_t base = (size_t)eplane_of(f) * plane;  // equation rows of field f
   const int mc = m < Nk ? m : Nk - 1;           // clamped column: loads stay in bounds
   for (int r0 = ks; r0 < K; r0 += 2 * RG) {
     const int r1 = (r0 + RG < K) ? r0 + RG : r0;
@@ -895,7 +890,8 @@ __global__ void __launch_bounds__(256) k_rk_final(LinComb lc, double2* __restric
   }
   __syncthreads();
   if (m < Nk)
-    for (int ri = ks; ri < K; ri += RG) X[(size_t)f * plane + (size_t)(par + 2 * ri) * Nk + m] = ys[ri * MB + mm];
+    for (int ri = ks; ri < K; ri += RG)
+      X[(size_t)xplane_of(f) * plane + (size_t)(par + 2 * ri) * Nk + m] = ys[ri * MB + mm];
 }
 
 template <int KL, int KU>
@@ -992,20 +988,20 @@ void launch_lincomb(const LinComb& lc, double2* out, long long count, cudaStream
 }
 
 void launch_mass_apply(const double2* X, double2* MX, const double* s3, int Nz, int Nk, int Nx, int project,
-                       cudaStream_t st) {
+                       int nf, cudaStream_t st) {
   dim3 grid((Nk + 127) / 128, Nz);
-  k_mass_apply<<<grid, 128, 0, st>>>(X, MX, s3, Nz, Nk, Nx, project);
+  k_mass_apply<<<grid, 128, 0, st>>>(X, MX, s3, Nz, Nk, Nx, project, nf);
 }
 
 void launch_lx_finalize(double2* LX, const double2* X, const double* s3, int Nz, int Nk, int Nx, double k0,
-                        double s, double kappa, double nu, double beta, cudaStream_t st) {
+                        double s, double kappa, double nu, double beta, int nf, cudaStream_t st) {
   dim3 grid((Nk + 127) / 128, Nz);
-  k_lx_finalize<<<grid, 128, 0, st>>>(LX, X, s3, Nz, Nk, Nx, k0, s, kappa, nu, beta);
+  k_lx_finalize<<<grid, 128, 0, st>>>(LX, X, s3, Nz, Nk, Nx, k0, s, kappa, nu, beta, nf);
 }
 
-void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* s3, int Nz, int Nk,
-                     cudaStream_t st) {
-  dim3 grid((Nk + kFinalModes - 1) / kFinalModes, 6);
+void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* s3, int Nz, int Nk, int nf,
+                     int ntau, cudaStream_t st) {
+  dim3 grid((Nk + kFinalModes - 1) / kFinalModes, 2 * nf);
   const size_t smem = rk_final_smem_bytes(Nz);
 #define TB_RKFINAL_CASE(N) \
   case N:                   \
@@ -1019,7 +1015,7 @@ void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* 
   }
 #undef TB_RKFINAL_CASE
   cudaMemsetAsync(X + (size_t)3 * Nz * Nk, 0, sizeof(double2) * (size_t)Nz * Nk, st);
-  cudaMemsetAsync(tau, 0, sizeof(double2) * 7 * (size_t)Nk, st);
+  cudaMemsetAsync(tau, 0, sizeof(double2) * (size_t)ntau * Nk, st);
 }
 
 size_t rk_final_smem_bytes(int Nz) {

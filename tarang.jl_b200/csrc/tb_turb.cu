@@ -96,9 +96,17 @@ __global__ void __launch_bounds__(kTurbThreads) k_turb_yinv(TurbArgs a, const fl
   const float kxv = a.kx0 * kx;
   const bool edge = (kx == 0) || (2 * kx == a.Nx);  // columns whose grid round trip is real
   const float xs = (2 * kx == a.Nx) ? 0.5f : 1.0f;  // even-N Nyquist split along x
+  // q^ of the grid round trip: the kx = 0 / Nyquist columns lose their
+  // non-Hermitian part before any derivative is taken
+  auto qproj = [&](int ky) -> float2 {
+    const float2 c = qs[ky];
+    if (!edge) return c;
+    const float2 w = qs[(Ny - ky) % Ny];
+    return F::mk<float2>(0.5f * (c.x + w.x), 0.5f * (c.y - w.y));
+  };
   auto factor = [&](int f, int ky) -> float2 {
     const float kyv = a.ky0 * ky_of(ky, Ny);
-    const float2 c = qs[ky];
+    const float2 c = qproj(ky);
     const float k2 = kxv * kxv + kyv * kyv;
     float2 psi = k2 > 1e-12f ? F::mk<float2>(-c.x / k2, -c.y / k2) : F::mk<float2>(0.f, 0.f);
     // i k z = (-k z.y, k z.x)
@@ -112,10 +120,6 @@ __global__ void __launch_bounds__(kTurbThreads) k_turb_yinv(TurbArgs a, const fl
     __syncthreads();
     for (int ky = threadIdx.x; ky < Ny; ky += blockDim.x) {
       float2 v = factor(f, ky);
-      if (edge) {
-        const float2 w = factor(f, (Ny - ky) % Ny);
-        v = F::mk<float2>(0.5f * (v.x + w.x), 0.5f * (v.y - w.y));
-      }
       v = F::scale(v, xs);
       if (2 * ky < Ny) {
         A[F::fidx<true>(ky)] = v;
@@ -167,11 +171,12 @@ __global__ void __launch_bounds__(kTurbThreads) k_turb_xpass(TurbArgs a, const f
   for (int t = threadIdx.x; t < a.nptx; t += blockDim.x) pt[t] = a.ptx[t];
   auto row = [&](int f) { return mixT + ((size_t)f * My + y) * Kx; };
   const float2 *ru = row(0), *rv = row(1), *rqx = row(2), *rqy = row(3);
-  // half-spectrum bin k of a factor (zero past the data, DC kept real as irfft does)
+  // half-spectrum bin k of a factor (zero past the data; DC and Nyquist kept
+  // real, as the factor's own irfft on Nx points does)
   auto bin = [&](const float2* r, int k) -> float2 {
     if (k >= Kx) return F::mk<float2>(0.f, 0.f);
     float2 v = r[k];
-    if (k == 0) v.y = 0.f;
+    if (k == 0 || 2 * k == a.Nx) v.y = 0.f;
     return v;
   };
   for (int k = threadIdx.x; k <= Mx / 2; k += blockDim.x) {

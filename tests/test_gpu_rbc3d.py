@@ -1,0 +1,73 @@
+"""3D Rayleigh-Benard (RealFourier x, RealFourier y, ChebyshevT z) through the
+C ABI against the 3D oracle: the FP64 plan to 1e-10 relative L2 of every
+field, the mixed plan (FP32 transforms and products, FP64 tau solves) to 1e-6."""
+import numpy as np
+import pytest
+
+from oracle.tarang_oracle import RBC3D, TABLEAUS, RBC3Params, forward_3d, rbc3_initial_b, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TS = {"RK222": 0, "RK443": 1}
+
+CASES = [
+    # Nx, Ny, Nz, Lx, Ly, Ra, scheme, dt, steps
+    (16, 12, 16, 4.0, 3.0, 1e5, "RK222", 0.05, 4),
+    (12, 16, 12, 3.0, 4.0, 1e6, "RK443", 0.02, 3),
+    (24, 24, 20, 4.0, 4.0, 1e7, "RK222", 0.005, 3),
+]
+
+
+def _run(tb, case, precision, seed=42):
+    Nx, Ny, Nz, Lx, Ly, Ra, scheme, dt, n = case
+    p = RBC3Params(Nx=Nx, Ny=Ny, Nz=Nz, Lx=Lx, Ly=Ly, Lz=1.0, Ra=Ra)
+    plan = tb.Plan3D(Nx, Ny, Nz, p.kappa, p.nu, TS[scheme], Lx, Ly, 1.0, precision=precision)
+    plan.set_state(tb._lib.TB_FIELD_B, forward_3d(rbc3_initial_b(p, seed, amp=1e-2)))
+    plan.step(dt, n)
+    sim = RBC3D(p)
+    sim.set_b_grid(rbc3_initial_b(p, seed, amp=1e-2))
+    for _ in range(n):
+        sim.step_rk(dt, TABLEAUS[scheme])
+    return plan, sim
+
+
+FIELDS = [("b", 0), ("ux", 1), ("uy", 5), ("uz", 2)]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_rbc3d_f64_matches_oracle(tb, case):
+    plan, sim = _run(tb, case, tb._lib.TB_PREC_F64)
+    for name, f in FIELDS:
+        got, want = plan.get_state(f), getattr(sim, name)
+        assert np.abs(want).max() > 0
+        assert rel_l2(got, want) < 1e-10, name
+    assert np.abs(plan.get_state(tb._lib.TB_FIELD_P)).max() == 0.0  # zeroed by the final mass solve
+
+
+@pytest.mark.parametrize("case", CASES[:2])
+def test_rbc3d_mixed_matches_oracle(tb, case):
+    plan, sim = _run(tb, case, tb._lib.TB_PREC_MIXED)
+    for name, f in FIELDS:
+        assert rel_l2(plan.get_state(f), getattr(sim, name)) < 1e-6, name
+
+
+def test_rbc3d_state_io_round_trip(tb):
+    Nx, Ny, Nz = 12, 24, 10
+    plan = tb.Plan3D(Nx, Ny, Nz, 1e-3, 1e-3)
+    rng = np.random.default_rng(3)
+    shape = (Nz, Ny, Nx // 2 + 1)
+    fields = {f: rng.standard_normal(shape) + 1j * rng.standard_normal(shape) for f in (0, 1, 2, 3, 5)}
+    for f, v in fields.items():
+        plan.set_state(f, v)
+    for f, v in fields.items():
+        assert np.abs(plan.get_state(f) - v).max() < 1e-13 * np.abs(v).max()
+    taus = rng.standard_normal((9, Ny, Nx // 2 + 1)) + 0j
+    plan.set_state(tb._lib.TB_FIELD_TAU, taus)
+    assert np.abs(plan.get_state(tb._lib.TB_FIELD_TAU) - taus).max() < 1e-13
+
+
+def test_rbc3d_rejects_unsupported(tb):
+    with pytest.raises(tb.TarangError):
+        tb.Plan3D(16, 12, 15, 1e-3, 1e-3)  # odd Nz
+    with pytest.raises(tb.TarangError):
+        tb.Plan3D(16, 12, 16, 1e-3, 1e-3, timestepper=3)  # SBDF2
