@@ -286,6 +286,24 @@ class Plan3D(Plan):
         check(lib.tb_get_state(self.ptr, field, out.ctypes.data_as(c_void_p), L.TB_HOST), self.ctx)
         return out
 
+    def forward(self, grid: np.ndarray) -> np.ndarray:
+        """Grid (Nz, Ny, Nx) real -> coefficients (Nz, Ny, Nx/2+1) on the device."""
+        import torch
+
+        g = torch.as_tensor(np.ascontiguousarray(grid, dtype=np.float64), device="cuda")
+        c = torch.empty(self.Nz * self.Ny * self.Kx * 2, dtype=torch.float64, device="cuda")
+        check(lib.tb_transform_forward(self.ptr, c_void_p(g.data_ptr()), c_void_p(c.data_ptr()), 1), self.ctx)
+        return c.cpu().numpy().view(np.complex128).reshape(self.Nz, self.Ny, self.Kx)
+
+    def backward(self, coeff: np.ndarray) -> np.ndarray:
+        """Coefficients (Nz, Ny, Nx/2+1) -> grid (Nz, Ny, Nx) on the device."""
+        import torch
+
+        c = torch.as_tensor(np.ascontiguousarray(coeff, dtype=np.complex128).view(np.float64), device="cuda")
+        g = torch.empty(self.Nz * self.Ny * self.Nx, dtype=torch.float64, device="cuda")
+        check(lib.tb_transform_backward(self.ptr, c_void_p(c.data_ptr()), c_void_p(g.data_ptr()), 1), self.ctx)
+        return g.cpu().numpy().reshape(self.Nz, self.Ny, self.Nx)
+
 
 def rbc3_desc(Nx: int, Ny: int, Nz: int, kappa: float, nu: float, timestepper: int = 0, Lx: float = 4.0,
               Ly: float = 4.0, Lz: float = 1.0, b_bottom: Optional[float] = None, b_top: float = 0.0,

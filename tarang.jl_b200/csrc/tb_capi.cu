@@ -751,113 +751,23 @@ void install_system(tb_plan* P, int sy, TauLayout lay) {
   S.lay = std::move(lay);
 }
 
-// 3D state I/O through the host: public layout (kx, ky, z) kx fastest,
-// Cartesian velocity and taus <-> the plan's [plane][z][ix * Ny + iy] with
-// (u_par, u_perp) and tau rows (tau_p, b1, b2, u1par, u1z, u2par, u2z, u1perp,
-// u2perp).  Not a hot path.
+// 3D state I/O: the layout change and the rotation of the horizontal velocity
+// run on the device (rbc3d_state_get / _set) through one plane of scratch.
 void state3d_io(tb_plan* P, int field, void* data, int where, bool set) {
   TB_REQUIRE(field >= TB_FIELD_B && field <= TB_FIELD_UY, TB_EINVAL, "bad field selector");
-  const int Kx = P->Kx, Ny = P->Ny, Nz = P->Nz;
-  const size_t Nk = P->Nk, plane = P->plane;
-  std::vector<double2> Xh((size_t)P->X.bytes / sizeof(double2));
-  TB_CUDA_TRY(cudaMemcpyAsync(Xh.data(), P->X.p, P->X.bytes, cudaMemcpyDeviceToHost, P->st));
+  const size_t count = field == TB_FIELD_TAU ? 9 * (size_t)P->Nk : P->plane;
+  double2* dev = where == TB_DEVICE ? static_cast<double2*>(data) : P->tmp3.as<double2>();
+  if (set) {
+    if (where != TB_DEVICE)
+      TB_CUDA_TRY(cudaMemcpyAsync(dev, data, count * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+    rbc3d_state_set(P, field, dev);
+  } else {
+    rbc3d_state_get(P, field, dev);
+    if (where != TB_DEVICE)
+      TB_CUDA_TRY(cudaMemcpyAsync(data, dev, count * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+  }
+  check_launch("3D state I/O");
   TB_CUDA_TRY(cudaStreamSynchronize(P->st));
-  const bool tau = field == TB_FIELD_TAU;
-  const size_t count = tau ? 9 * Nk : plane;
-  std::vector<double2> pub(count);
-  auto rot = [&](size_t m, double& cx, double& cy) {
-    const int ix = (int)(m / Ny), iy = (int)(m % Ny);
-    const double kx = P->k0 * ix, ky = P->k0y * (iy < Ny / 2 ? iy : iy - Ny);
-    const double kk = std::sqrt(kx * kx + ky * ky);
-    cx = kk > 0 ? kx / kk : 1.0;
-    cy = kk > 0 ? ky / kk : 0.0;
-  };
-  auto pub_index = [&](size_t m, int z) { return (size_t)(m / Ny) + (size_t)Kx * ((m % Ny) + (size_t)Ny * z); };
-  auto cx_of = [](double c, double2 a, double d, double2 b) {
-    return make_double2(c * a.x + d * b.x, c * a.y + d * b.y);
-  };
-  // internal (row, m) -> pointer into Xh for the Cartesian-independent slots
-  double2* taub = Xh.data() + (size_t)P->nplanes * plane;
-  if (set) {
-    if (where == TB_DEVICE)
-      TB_CUDA_TRY(cudaMemcpy(pub.data(), data, count * sizeof(double2), cudaMemcpyDeviceToHost));
-    else
-      std::memcpy(pub.data(), data, count * sizeof(double2));
-  }
-  if (tau) {
-    const int ord[9] = {0, 1, 2, -1, 4, -1, 6, -1, -1};  // public row -> internal row (-1 rotated)
-    for (size_t m = 0; m < Nk; ++m) {
-      double cx, cy;
-      rot(m, cx, cy);
-      const size_t pm = (m / Ny) + (size_t)Kx * (m % Ny);
-      for (int r = 0; r < 9; ++r)
-        if (ord[r] >= 0) {
-          double2& slot = taub[(size_t)ord[r] * Nk + m];
-          if (set)
-            slot = pub[(size_t)r * Nk + pm];
-          else
-            pub[(size_t)r * Nk + pm] = slot;
-        }
-      for (int w = 0; w < 2; ++w) {  // tau_u1 (public rows 3, 4), tau_u2 (6, 7)
-        const int rx = w ? 6 : 3, ry = w ? 7 : 4;
-        double2& par = taub[(size_t)(w ? 5 : 3) * Nk + m];
-        double2& perp = taub[(size_t)(w ? 8 : 7) * Nk + m];
-        if (set) {
-          const double2 ux = pub[(size_t)rx * Nk + pm], uy = pub[(size_t)ry * Nk + pm];
-          par = cx_of(cx, ux, cy, uy);
-          perp = cx_of(-cy, ux, cx, uy);
-        } else {
-          pub[(size_t)rx * Nk + pm] = cx_of(cx, par, -cy, perp);
-          pub[(size_t)ry * Nk + pm] = cx_of(cy, par, cx, perp);
-        }
-      }
-    }
-    // tau_u1z / tau_u2z sit at public rows 5 / 8, internal rows 4 / 6
-    for (size_t m = 0; m < Nk; ++m) {
-      const size_t pm = (m / Ny) + (size_t)Kx * (m % Ny);
-      double2& a = taub[4 * Nk + m];
-      double2& b = taub[6 * Nk + m];
-      if (set) {
-        a = pub[5 * Nk + pm];
-        b = pub[8 * Nk + pm];
-      } else {
-        pub[5 * Nk + pm] = a;
-        pub[8 * Nk + pm] = b;
-      }
-    }
-  } else {
-    for (int z = 0; z < Nz; ++z)
-      for (size_t m = 0; m < Nk; ++m) {
-        const size_t i = (size_t)z * Nk + m, pi = pub_index(m, z);
-        if (field == TB_FIELD_B || field == TB_FIELD_UZ || field == TB_FIELD_P) {
-          const int pl = field == TB_FIELD_B ? 0 : (field == TB_FIELD_UZ ? 2 : 3);
-          if (set)
-            Xh[pl * plane + i] = pub[pi];
-          else
-            pub[pi] = Xh[pl * plane + i];
-        } else {
-          double cx, cy;
-          rot(m, cx, cy);
-          double2& par = Xh[plane + i];
-          double2& perp = Xh[4 * plane + i];
-          double2 ux = cx_of(cx, par, -cy, perp), uy = cx_of(cy, par, cx, perp);
-          if (set) {
-            (field == TB_FIELD_UX ? ux : uy) = pub[pi];
-            par = cx_of(cx, ux, cy, uy);
-            perp = cx_of(-cy, ux, cx, uy);
-          } else {
-            pub[pi] = field == TB_FIELD_UX ? ux : uy;
-          }
-        }
-      }
-  }
-  if (set) {
-    TB_CUDA_TRY(cudaMemcpy(P->X.p, Xh.data(), P->X.bytes, cudaMemcpyHostToDevice));
-  } else if (where == TB_DEVICE) {
-    TB_CUDA_TRY(cudaMemcpy(data, pub.data(), count * sizeof(double2), cudaMemcpyHostToDevice));
-  } else {
-    std::memcpy(data, pub.data(), count * sizeof(double2));
-  }
 }
 
 }  // namespace
@@ -1237,8 +1147,15 @@ tb_status tb_kernels_per_step(const tb_plan* P, int* n) {
 
 tb_status tb_transform_forward(tb_plan* P, const double* grid, double* coeff, int nfields) {
   if (!P || !grid || !coeff || nfields < 1) return TB_EINVAL;
+  if (P->ndim == 3)
+    return guard(P->ctx, [&] {
+      const size_t g = (size_t)P->Nz * P->Ny * P->Nx;
+      for (int f = 0; f < nfields; ++f)
+        rbc3d_transform_forward(P, grid + f * g, reinterpret_cast<double2*>(coeff) + f * P->plane);
+      check_launch("transform forward");
+      TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+    });
   return guard(P->ctx, [&] {
-    TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "2D plans only");
     const size_t gsz = (size_t)P->Nz * P->Nx;
     for (int f = 0; f < nfields; ++f) {
       double2* mixed = P->tmpgrid.as<double2>();
@@ -1257,8 +1174,15 @@ tb_status tb_transform_forward(tb_plan* P, const double* grid, double* coeff, in
 
 tb_status tb_transform_backward(tb_plan* P, const double* coeff, double* grid, int nfields) {
   if (!P || !grid || !coeff || nfields < 1) return TB_EINVAL;
+  if (P->ndim == 3)
+    return guard(P->ctx, [&] {
+      const size_t g = (size_t)P->Nz * P->Ny * P->Nx;
+      for (int f = 0; f < nfields; ++f)
+        rbc3d_transform_backward(P, reinterpret_cast<const double2*>(coeff) + f * P->plane, grid + f * g);
+      check_launch("transform backward");
+      TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+    });
   return guard(P->ctx, [&] {
-    TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "2D plans only");
     const size_t gsz = (size_t)P->Nz * P->Nx;
     for (int f = 0; f < nfields; ++f) {
       double2* mixed = P->tmpgrid.as<double2>();

@@ -130,6 +130,10 @@ struct tb_plan {
   // y-forward output, per-pass twiddles of the padded x / y plans
   DevBuf kmag, Xc, G3, mix3, pm3, H3, ptwX, ptwY;
   FftPlan fpMy{};
+  // 3D field transforms and state I/O: plan and per-pass twiddles of the Ny
+  // transform, one complex plane of scratch
+  FftPlan fpNy{};
+  DevBuf ptwNy, tmp3;
   // transform constants
   DevBuf bwd, fwd, s3, twM, twN, ptwM;
   // parity halves of the Chebyshev matrices (H = ceil(Nz/2) rows/cols)
@@ -234,6 +238,14 @@ void rbc3d_setup(tb_plan* P);
 void rbc3d_enqueue_rhs(tb_plan* P, const double2* Xin, double2* out4);
 void rbc3d_lx_project(tb_plan* P, double2* LX, double beta);
 size_t rbc3d_device_bytes(const tb_plan* P);
+// 3D transforms between grid (Nz, Ny, Nx) real and coefficients (Nz, Ny, Nx/2+1)
+// complex (kx fastest), device pointers, one field.
+void rbc3d_transform_forward(tb_plan* P, const double* grid, double2* coeff);
+void rbc3d_transform_backward(tb_plan* P, const double2* coeff, double* grid);
+// State I/O between the public layout (device pointer) and the plan's planes:
+// field TB_FIELD_* (Cartesian velocity), or the 9 taus.
+void rbc3d_state_get(tb_plan* P, int field, double2* dst);
+void rbc3d_state_set(tb_plan* P, int field, const double2* src);
 
 // Error plumbing shared by the C ABI translation units.
 void record_error(tb_context* ctx, const Error& e);

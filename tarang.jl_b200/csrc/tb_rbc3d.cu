@@ -31,6 +31,7 @@
 //   GEMM      Chebyshev forward into C^(2) rows (S fwd) of the stage vector.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -370,6 +371,117 @@ __global__ void __launch_bounds__(128) k3_lx_project(R3Args a, double2* __restri
   }
 }
 
+// FFT along y of the columns of a [z][y][kx] array (length Ny, in place),
+// sign -1 forward (unnormalised) or +1 inverse (scaled by 1/Ny).  Grid (Kx, Nz).
+__global__ void __launch_bounds__(256) k3_ycols(double2* __restrict__ a, int Ny, int Kx, FftPlan fp,
+                                                const double2* __restrict__ ptw, int npt, int sign) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  double2* sm = reinterpret_cast<double2*>(sm_raw);
+  const int kx = blockIdx.x, z = blockIdx.y;
+  const int Ms = (Ny + 7) & ~7;
+  double2* A = sm;
+  double2* B = sm + Ms;
+  double2* pt = sm + 2 * Ms;
+  for (int t = threadIdx.x; t < npt; t += blockDim.x) pt[t] = ptw[t];
+  double2* col = a + (size_t)z * Ny * Kx + kx;
+  for (int y = threadIdx.x; y < Ny; y += blockDim.x) A[F::fidx<true>(y)] = col[(size_t)y * Kx];
+  __syncthreads();
+  const double2* R = F::fft<true>(A, B, fp, pt, sign);
+  const double sc = sign > 0 ? 1.0 / Ny : 1.0;
+  for (int y = threadIdx.x; y < Ny; y += blockDim.x) col[(size_t)y * Kx] = F::scale(R[F::fidx<true>(y)], sc);
+}
+
+// Public coefficient index of (z, mode m = ix Ny + iy): ix + Kx (iy + Ny z).
+__device__ __forceinline__ size_t pub_of(const R3Args& a, int z, int m) {
+  return (size_t)(m / a.Ny) + (size_t)a.Kx * ((size_t)(m % a.Ny) + (size_t)a.Ny * z);
+}
+
+// Field I/O: grid (ceil(Nk/256), Nz) over the plan's modes.
+__global__ void __launch_bounds__(256) k3_state_get(R3Args a, const double2* __restrict__ X, int field,
+                                                    double2* __restrict__ out) {
+  const int z = blockIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.Nk) return;
+  const size_t plane = (size_t)a.Nz * a.Nk, i = (size_t)z * a.Nk + m;
+  double2 v;
+  if (field == TB_FIELD_B) {
+    v = X[i];
+  } else if (field == TB_FIELD_UZ) {
+    v = X[2 * plane + i];
+  } else if (field == TB_FIELD_P) {
+    v = X[3 * plane + i];
+  } else {
+    double cx, cy;
+    rot_of(a, m / a.Ny, m % a.Ny, cx, cy);
+    const double2 up = X[plane + i], uq = X[4 * plane + i];
+    v = field == TB_FIELD_UX ? make_double2(cx * up.x - cy * uq.x, cx * up.y - cy * uq.y)
+                             : make_double2(cy * up.x + cx * uq.x, cy * up.y + cx * uq.y);
+  }
+  out[pub_of(a, z, m)] = v;
+}
+
+__global__ void __launch_bounds__(256) k3_state_set(R3Args a, double2* __restrict__ X, int field,
+                                                    const double2* __restrict__ in) {
+  const int z = blockIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.Nk) return;
+  const size_t plane = (size_t)a.Nz * a.Nk, i = (size_t)z * a.Nk + m;
+  const double2 v = in[pub_of(a, z, m)];
+  if (field == TB_FIELD_B) {
+    X[i] = v;
+  } else if (field == TB_FIELD_UZ) {
+    X[2 * plane + i] = v;
+  } else if (field == TB_FIELD_P) {
+    X[3 * plane + i] = v;
+  } else {
+    double cx, cy;
+    rot_of(a, m / a.Ny, m % a.Ny, cx, cy);
+    const double2 up = X[plane + i], uq = X[4 * plane + i];
+    double2 ux = make_double2(cx * up.x - cy * uq.x, cx * up.y - cy * uq.y);
+    double2 uy = make_double2(cy * up.x + cx * uq.x, cy * up.y + cx * uq.y);
+    if (field == TB_FIELD_UX)
+      ux = v;
+    else
+      uy = v;
+    X[plane + i] = make_double2(cx * ux.x + cy * uy.x, cx * ux.y + cy * uy.y);
+    X[4 * plane + i] = make_double2(-cy * ux.x + cx * uy.x, -cy * ux.y + cx * uy.y);
+  }
+}
+
+// Taus: public rows (tau_p, b1, b2, u1x, u1y, u1z, u2x, u2y, u2z) over (kx, ky)
+// kx fastest; plan rows (tau_p, b1, b2, u1par, u1z, u2par, u2z, u1perp, u2perp)
+// over modes.  Grid ceil(Nk/256).
+__global__ void __launch_bounds__(256) k3_tau_io(R3Args a, double2* __restrict__ tau, double2* __restrict__ pub,
+                                                 int set) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.Nk) return;
+  const size_t Nk = a.Nk, pm = (size_t)(m / a.Ny) + (size_t)a.Kx * (m % a.Ny);
+  double cx, cy;
+  rot_of(a, m / a.Ny, m % a.Ny, cx, cy);
+  const int direct_pub[5] = {0, 1, 2, 5, 8}, direct_int[5] = {0, 1, 2, 4, 6};
+  for (int r = 0; r < 5; ++r) {
+    double2* ti = tau + direct_int[r] * Nk + m;
+    double2* tp = pub + direct_pub[r] * Nk + pm;
+    if (set)
+      *ti = *tp;
+    else
+      *tp = *ti;
+  }
+  for (int w = 0; w < 2; ++w) {
+    double2* par = tau + (w ? 5 : 3) * Nk + m;
+    double2* perp = tau + (w ? 8 : 7) * Nk + m;
+    double2* px = pub + (w ? 6 : 3) * Nk + pm;
+    double2* py = pub + (w ? 7 : 4) * Nk + pm;
+    if (set) {
+      const double2 ux = *px, uy = *py;
+      *par = make_double2(cx * ux.x + cy * uy.x, cx * ux.y + cy * uy.y);
+      *perp = make_double2(-cy * ux.x + cx * uy.x, -cy * ux.y + cx * uy.y);
+    } else {
+      const double2 up = *par, uq = *perp;
+      *px = make_double2(cx * up.x - cy * uq.x, cx * up.y - cy * uq.y);
+      *py = make_double2(cy * up.x + cx * uq.x, cy * up.y + cx * uq.y);
+    }
+  }
+}
+
 template <class C>
 std::vector<C> pass_twiddles_t(const FftPlan& fp) {
   std::vector<C> t;
@@ -538,7 +650,10 @@ void setup_t(tb_plan* P) {
 }  // namespace
 
 void rbc3d_setup(tb_plan* P) {
-  TB_REQUIRE(make_fft_plan(P->My, &P->fpMy), TB_ENOTSUPPORTED, "Ny must be of the form 2^a 3^b");
+  TB_REQUIRE(make_fft_plan(P->My, &P->fpMy) && make_fft_plan(P->Ny, &P->fpNy), TB_ENOTSUPPORTED,
+             "Ny must be of the form 2^a 3^b with a padded length 3Ny/2 of the same form");
+  upload(P->ptwNy, pass_twiddles_t<double2>(P->fpNy));
+  P->tmp3.alloc(std::max(P->plane, (size_t)9 * P->Nk) * sizeof(double2));
   std::vector<double> km(P->Nk);
   for (int ix = 0; ix < P->Kx; ++ix)
     for (int iy = 0; iy < P->Ny; ++iy) {
@@ -569,7 +684,55 @@ void rbc3d_lx_project(tb_plan* P, double2* LX, double beta) {
 
 size_t rbc3d_device_bytes(const tb_plan* P) {
   return P->kmag.bytes + P->Xc.bytes + P->G3.bytes + P->mix3.bytes + P->pm3.bytes + P->H3.bytes + P->ptwX.bytes +
-         P->ptwY.bytes;
+         P->ptwY.bytes + P->ptwNy.bytes + P->tmp3.bytes;
+}
+
+namespace {
+void ycols(tb_plan* P, double2* a, int sign) {
+  const int npt = F::pass_twiddle_count(P->fpNy);
+  const size_t smem = (2 * (size_t)((P->Ny + 7) & ~7) + npt) * sizeof(double2);
+  k3_ycols<<<dim3(P->Kx, P->Nz), 256, smem, P->st>>>(a, P->Ny, P->Kx, P->fpNy, P->ptwNy.as<double2>(), npt, sign);
+}
+}  // namespace
+
+void rbc3d_transform_forward(tb_plan* P, const double* grid, double2* coeff) {
+  double2* t = P->tmp3.as<double2>();
+  launch_x_rfft(grid, t, P->Nz * P->Ny, P->Nx, P->fpN, P->twN.as<double2>(), P->st);
+  ycols(P, t, -1);
+  const int H = P->Nz / 2, ncol = 2 * P->Nk;
+  GemmBatch bt{};
+  bt.item[0] = GemmItem{P->fE.as<double>(), reinterpret_cast<const double*>(t), reinterpret_cast<double*>(coeff),
+                        P->Ke, H, pad16(H), GEMM_MIRROR, 0};
+  bt.item[1] = GemmItem{P->fO.as<double>(), reinterpret_cast<const double*>(t), reinterpret_cast<double*>(coeff),
+                        P->Ko, H, pad16(H), GEMM_MIRROR, 1};
+  launch_gemm_f64(bt, 2, ncol, ncol, ncol, P->Nz, P->st);
+}
+
+void rbc3d_transform_backward(tb_plan* P, const double2* coeff, double* grid) {
+  double2* t = P->tmp3.as<double2>();
+  const int ncol = 2 * P->Nk;
+  GemmBatch bt{};
+  bt.item[0] = GemmItem{P->bwd.as<double>(), reinterpret_cast<const double*>(coeff), reinterpret_cast<double*>(t),
+                        P->Nz, P->Nz, pad16(P->Nz), GEMM_PLAIN, 0};
+  launch_gemm_f64(bt, 1, ncol, ncol, ncol, P->Nz, P->st);
+  ycols(P, t, +1);
+  launch_x_irfft(t, grid, P->Nz * P->Ny, P->Nx, P->fpN, P->twN.as<double2>(), P->st);
+}
+
+void rbc3d_state_get(tb_plan* P, int field, double2* dst) {
+  const R3Args a = args_of(P);
+  if (field == TB_FIELD_TAU)
+    k3_tau_io<<<(P->Nk + 255) / 256, 256, 0, P->st>>>(a, P->tau.as<double2>(), dst, 0);
+  else
+    k3_state_get<<<dim3((P->Nk + 255) / 256, P->Nz), 256, 0, P->st>>>(a, P->X.as<double2>(), field, dst);
+}
+
+void rbc3d_state_set(tb_plan* P, int field, const double2* src) {
+  const R3Args a = args_of(P);
+  if (field == TB_FIELD_TAU)
+    k3_tau_io<<<(P->Nk + 255) / 256, 256, 0, P->st>>>(a, P->tau.as<double2>(), const_cast<double2*>(src), 1);
+  else
+    k3_state_set<<<dim3((P->Nk + 255) / 256, P->Nz), 256, 0, P->st>>>(a, P->X.as<double2>(), field, src);
 }
 
 }  // namespace tb

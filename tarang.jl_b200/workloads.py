@@ -110,6 +110,70 @@ def step_model_bytes(cfg: RBCConfig, scheme: str) -> float:
     return total
 
 
+@dataclass
+class RBC3Config:
+    """3D Rayleigh-Benard: RealFourier x, y x ChebyshevT z (ChannelDomain3D-style, z in [0, Lz])."""
+
+    Nx: int = 256
+    Ny: int = 256
+    Nz: int = 128
+    Lx: float = 4.0
+    Ly: float = 4.0
+    Lz: float = 1.0
+    Ra: float = 1e7
+    Pr: float = 1.0
+    dt: float = 5e-3
+    scheme: str = "RK222"
+    steps: int = 50
+    seed: int = 42
+    noise: float = 1e-3
+
+    @property
+    def kappa(self) -> float:
+        return (self.Ra * self.Pr) ** -0.5
+
+    @property
+    def nu(self) -> float:
+        return (self.Ra / self.Pr) ** -0.5
+
+
+C3 = RBC3Config()
+
+
+def rbc3_initial_grid(cfg: RBC3Config) -> np.ndarray:
+    """b0 = Lz - z + noise * z (Lz - z) xi on the (Nz, Ny, Nx) grid, xi ~ N(0,1)
+    from PCG64(seed) drawn in Julia (x, y, z) order."""
+    rng = np.random.default_rng(cfg.seed)
+    xi = rng.standard_normal((cfg.Nx, cfg.Ny, cfg.Nz)).transpose(2, 1, 0)
+    z = (cfg.Lz / 2.0 * (1.0 - np.cos(np.pi * np.arange(cfg.Nz) / (cfg.Nz - 1))))[:, None, None]
+    return (cfg.Lz - z) + cfg.noise * z * (cfg.Lz - z) * xi
+
+
+def step_model_bytes3(cfg: RBC3Config) -> float:
+    """The byte model of step_model_bytes for the 3D system: modes (Nx/2+1) Ny,
+    n = 5 Nz + 9 per mode, and the RHS reads the 4 advected fields and writes
+    4 F fields (8 C per stage)."""
+    nk = (cfg.Nx // 2 + 1) * cfg.Ny
+    n = 5 * cfg.Nz + 9
+    C = nk * cfg.Nz * 16.0
+    V = nk * n * 16.0
+    Phi = nk * n * 848.0
+    AE, AI, bE, bI = TABLEAU_PATTERNS[cfg.scheme]
+    s = len(bE)
+    total = 2 * V
+    for i in range(s):
+        total += V
+        for j in range(i):
+            total += V * (AE[i][j] + AI[i][j])
+        if AI[i][i]:
+            total += Phi
+        total += V + 8 * C
+        if any(AI[k][i] for k in range(i + 1, s)) or bI[i]:
+            total += 2 * V + Phi
+    total += V + sum(V * (bE[j] + bI[j]) for j in range(s)) + 2 * V
+    return total
+
+
 # ---------------------------------------------------------------------------
 # Batched ensemble: independent 2D RBC instances of uneven size.
 # ---------------------------------------------------------------------------

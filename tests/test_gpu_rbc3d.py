@@ -4,7 +4,7 @@ field, the mixed plan (FP32 transforms and products, FP64 tau solves) to 1e-6.""
 import numpy as np
 import pytest
 
-from oracle.tarang_oracle import RBC3D, TABLEAUS, RBC3Params, forward_3d, rbc3_initial_b, rel_l2
+from oracle.tarang_oracle import RBC3D, TABLEAUS, RBC3Params, backward_3d, forward_3d, rbc3_initial_b, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -22,7 +22,7 @@ def _run(tb, case, precision, seed=42):
     Nx, Ny, Nz, Lx, Ly, Ra, scheme, dt, n = case
     p = RBC3Params(Nx=Nx, Ny=Ny, Nz=Nz, Lx=Lx, Ly=Ly, Lz=1.0, Ra=Ra)
     plan = tb.Plan3D(Nx, Ny, Nz, p.kappa, p.nu, TS[scheme], Lx, Ly, 1.0, precision=precision)
-    plan.set_state(tb._lib.TB_FIELD_B, forward_3d(rbc3_initial_b(p, seed, amp=1e-2)))
+    plan.set_state(tb._lib.TB_FIELD_B, plan.forward(rbc3_initial_b(p, seed, amp=1e-2)))
     plan.step(dt, n)
     sim = RBC3D(p)
     sim.set_b_grid(rbc3_initial_b(p, seed, amp=1e-2))
@@ -71,3 +71,15 @@ def test_rbc3d_rejects_unsupported(tb):
         tb.Plan3D(16, 12, 15, 1e-3, 1e-3)  # odd Nz
     with pytest.raises(tb.TarangError):
         tb.Plan3D(16, 12, 16, 1e-3, 1e-3, timestepper=3)  # SBDF2
+
+
+def test_rbc3d_transforms_match_oracle(tb):
+    Nx, Ny, Nz = 24, 16, 12
+    plan = tb.Plan3D(Nx, Ny, Nz, 1e-3, 1e-3, Lx=3.0, Ly=2.0)
+    g = np.random.default_rng(4).standard_normal((Nz, Ny, Nx))
+    c = plan.forward(g)
+    assert rel_l2(c, forward_3d(g)) < 1e-13
+    assert rel_l2(plan.backward(c), g) < 1e-13
+    c2 = forward_3d(g)
+    c2[:, :, -1] += 0.5j  # non-Hermitian Nyquist content is dropped like FFTW's c2r
+    assert rel_l2(plan.backward(c2), backward_3d(c2, Nx)) < 1e-13
