@@ -52,6 +52,9 @@ def parse_args():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving summary in the rbc line")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision summary in the rbc line")
     ap.add_argument("--no-rbc3d", action="store_true", help="skip the 3D (256x256x128) summary in the rbc line")
+    ap.add_argument("--rbc3d-grid", default="256x256x128", help="Nx x Ny x Nz of the 3D workload")
+    ap.add_argument("--rbc3d-quick", action="store_true",
+                    help="3D workload without the FP64 comparison and the end-to-end run (profiling)")
     ap.add_argument("--serve-requests", type=int, default=60)
     ap.add_argument("--serve-budget-gb", type=float, default=40.0)
     ap.add_argument("--turb-n", type=int, default=1024)
@@ -668,7 +671,8 @@ def run_rbc3d(args, dev, with_cpu=True):
     from tarang_b200._lib import (TB_FIELD_B, TB_FIELD_P, TB_FIELD_UX, TB_FIELD_UY, TB_FIELD_UZ, TB_PREC_F64,
                                   TB_PREC_MIXED)
 
-    c = W.C3
+    nx, ny, nz = (int(v) for v in args.rbc3d_grid.lower().split("x"))
+    c = W.RBC3Config(Nx=nx, Ny=ny, Nz=nz) if (nx, ny, nz) != (W.C3.Nx, W.C3.Ny, W.C3.Nz) else W.C3
     torch.cuda.set_device(dev)
     grid = W.rbc3_initial_grid(c)
     t0 = time.perf_counter()
@@ -711,6 +715,9 @@ def run_rbc3d(args, dev, with_cpu=True):
                  "note": "the byte model charges the nominal bordered-banded LHS (n x 848 B per mode) on 4 reads "
                          "per step; the built real banded factors are phi_built_bytes per read"}
     step_roof["frac"] = step_roof["achieved_gbs"] / step_roof["peak_gbs"]
+    if args.rbc3d_quick:
+        return {"metric": f"RBC 3D steps/s ({c.Nx}x{c.Ny}x{c.Nz}, {c.scheme}, mixed)", "value": value,
+                "ms_per_step": ms / c.steps, "kernels": kernels, "step_roofline": step_roof}
     # error against the FP64 plan from the same initial state
     for f in (TB_FIELD_UX, TB_FIELD_UY, TB_FIELD_UZ, TB_FIELD_P):
         plan.set_state(f, np.zeros((c.Nz, c.Ny, c.Nx // 2 + 1), np.complex128))

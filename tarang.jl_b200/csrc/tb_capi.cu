@@ -196,6 +196,7 @@ TauArgs tau_args(tb_plan* P, int sy, FactorSet* f, const double2* rhsP) {
   a.HR = f ? f->HR.as<double>() : nullptr;
   a.rhs_off = P->sys[sy].rhs_off.as<int>();
   a.err_mode = P->err_mode.as<int>();
+  a.ysave = P->solve_scratch.as<double>();
   return a;
 }
 
@@ -603,7 +604,8 @@ size_t tb::plan_device_bytes(const tb_plan* P) {
   size_t b = 0;
   const DevBuf* bufs[] = {&P->X,   &P->G,   &P->H,    &P->MX0,  &P->Fprev, &P->MXprev, &P->Rsb, &P->tmpgrid,
                           &P->bwd, &P->fwd, &P->s3,   &P->twM,  &P->twN,   &P->ptwM,   &P->bEv, &P->bOv,
-                          &P->bEd, &P->bOd, &P->fE,   &P->fO,   &P->sfE,   &P->sfO,    &P->err_mode};
+                          &P->bEd, &P->bOd, &P->fE,   &P->fO,   &P->sfE,   &P->sfO,    &P->err_mode,
+                          &P->solve_scratch};
   for (const DevBuf* d : bufs) b += d->bytes;
   for (int i = 0; i < 4; ++i) b += P->FP[i].bytes + P->LXP[i].bytes;
   for (int sy = 0; sy < P->nsys; ++sy) {
@@ -743,6 +745,8 @@ void install_system(tb_plan* P, int sy, TauLayout lay) {
   S.tau_parts = (!many_groups && tau_solve_smem_bytes(S.npad, kTauParts) <= 227 * 1024) ? kTauParts : 1;
   TB_REQUIRE(tau_solve_smem_bytes(S.npad, S.tau_parts) <= 227 * 1024, TB_ENOTSUPPORTED,
              "Nz too large for the staged tau solve");
+  const size_t ys = tau_solve_scratch_doubles(P->Nk, S.npad, S.tau_parts) * sizeof(double);
+  if (ys > P->solve_scratch.bytes) P->solve_scratch.alloc(ys);
   // per (band row, class) right-hand-side code, -1 for the padding rows
   std::vector<int> ro((size_t)2 * S.npad, -1);
   for (int j = 0; j < n; ++j)

@@ -158,6 +158,7 @@ struct TauArgs {
   double* PP;
   double* HR;
   double* scratch;     // factor workspace
+  double* ysave;       // one-partition solve: [group][row][lane] y scratch (tau_solve_scratch_doubles)
   int* err_mode;       // first singular mode, or -1
 };
 // parts: kTauParts (partitioned solve, needs a.PP) or 1 (one warp per group)
@@ -167,6 +168,7 @@ cudaError_t set_tau_smem_limits(int bytes);
 size_t tau_solve_smem_bytes(int npad, int parts);
 size_t tau_transfer_doubles(int Nk, int parts);
 size_t tau_response_doubles(int Nk, int npad, int parts);
+size_t tau_solve_scratch_doubles(int Nk, int npad, int parts);
 
 struct LinComb {
   const double2* in[12];

@@ -144,6 +144,7 @@ struct tb_plan {
   TauSystem sys[2];
   int nsys = 1;
   DevBuf err_mode;
+  DevBuf solve_scratch;  // y columns of one-partition tau solves (shared by the systems)
   // stepping state
   double sim_time = 0.0;
   long long iteration = 0;

@@ -254,10 +254,13 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+// Doubles per ring stage; with one partition a backward stage also carries the
+// stage's y values (kPartRows x 4 kSolveModes), prefetched from global scratch.
+template <int P>
 __host__ __device__ constexpr size_t part_stage_doubles() {
   constexpr size_t MP = kSolveModes;
   constexpr size_t F = kPartRows * (2 * MP * kFwdRec + 2 * 2 * MP);
-  constexpr size_t B = kPartRows * (2 * MP * kBwdRec);
+  constexpr size_t B = kPartRows * (2 * MP * kBwdRec + (P == 1 ? 4 * MP : 0));
   constexpr size_t H = kPartRows * (2 * MP * kHRec);
   return F > B ? (F > H ? F : H) : (B > H ? B : H);
 }
@@ -292,7 +295,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   constexpr int R = kPartRows, NS = kPartStages;
   constexpr int NL = 4 * MP;  // distinct lanes
   constexpr int BSUB = 3;     // backward rows whose records are held in registers at once
-  constexpr int STAGE = (int)part_stage_doubles();
+  constexpr int STAGE = (int)part_stage_doubles<P>();
   static_assert(NL <= 32 && 32 % NL == 0, "lane layout");
   static_assert(R % BSUB == 0, "backward sub-blocks");
   extern __shared__ __align__(16) double smem[];
@@ -309,8 +312,12 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   const int m = g * MP + mm;
   const bool live = owner && m < Nk;
   double* ring = smem + (size_t)warp * NS * STAGE;
-  double* ysave = smem + (size_t)P * NS * STAGE;  // [row][ln]: y, then (rows of warps < P-1) particular x
-  double* xch = ysave + (size_t)np * NL;          // [warp][ln][kXch]
+  // [row][ln]: y, then (rows of warps < P-1) particular x.  With one partition
+  // the group's y column lives in global scratch (written by F1 and read back
+  // by B1 of the same CTA while it is still in L2), which halves the shared
+  // memory of a CTA and doubles the resident groups per SM.
+  double* ysave = (P == 1) ? a.ysave + (size_t)g * np * NL : smem + (size_t)P * NS * STAGE;
+  double* xch = smem + (size_t)P * NS * STAGE + (P == 1 ? 0 : (size_t)np * NL);  // [warp][ln][kXch]
   int* rofs = reinterpret_cast<int*>(xch + (size_t)P * NL * kXch);
   // [row][class] right-hand-side code: 2 * element offset + (1 for a u_x momentum
   // row, scaled by -i on load), -1 for none
@@ -414,6 +421,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 #pragma unroll
   for (int t = 0; t < 4; ++t) myx[t] = y[t] - rhs_at(nst, t);
   cp_async_wait<0>();
+  if constexpr (P == 1) __threadfence();  // y stores of all lanes reach L2 before their cp.async reloads
   __syncwarp();
   // The ring is free: stage the Schur inverse of the group and this warp's
   // forward transfer data (Phi_k for k < warp, Gz_warp) while the other warps
@@ -502,6 +510,9 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
       double* dst = ring + (size_t)(s % NS) * STAGE;
       const int lo = row0 + Lp - (s + 1) * R;
       for (int q = lane; q < R * BREC / 2; q += 32) cp_async16(dst + 2 * q, BRg + (size_t)lo * BREC + 2 * q, true);
+      if constexpr (P == 1)
+        for (int q = lane; q < R * NL / 2; q += 32)
+          cp_async16(dst + R * BREC + 2 * q, ysave + (size_t)lo * NL + 2 * q, true);
     }
     cp_async_commit();
   };
@@ -529,7 +540,11 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
           const int j = q0 + kBwdWin - 1 - u;  // j % kBwdWin == kBwdWin-1-u
           auto rec = [&](int k) -> double { return (k & 1) ? rv[w][k >> 1].y : rv[w][k >> 1].x; };
           double* yx = ysave + (size_t)j * NL + ln;
-          double acc0 = *yx;
+          double acc0;
+          if constexpr (P == 1)
+            acc0 = ring[(size_t)(s % NS) * STAGE + R * BREC + (R - 1 - (h * BSUB + w)) * NL + ln];
+          else
+            acc0 = *yx;
           double acc1 = 0.0, acc2 = 0.0;
 #pragma unroll
           for (int i = 0; i < 4; ++i) acc2 = fma(rec(kBwdG + i), d[i], acc2);  // y correction G d
@@ -548,7 +563,10 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
           const double sacc = fma(-rec(1), xw[(kBwdWin - u) % kBwdWin], acc0 + (acc1 + acc2));
           const double xj = sacc * rec(0);
           xw[(kBwdWin - 1 - u) % kBwdWin] = xj;
-          *yx = xj;
+          if constexpr (P == 1)
+            store_unknown(Xd, __double2loint(rec(kBwdCode)), m, part, xj, live);  // final: no correction
+          else
+            *yx = xj;
         }
       }
       __syncwarp();  // the slot of stage s is refilled next
@@ -601,7 +619,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   }
 
   // ---- B3: x_j = particular + H_j . T over the rows of this partition, stored to X ----
-  {
+  if constexpr (P > 1) {
     constexpr int NS3 = 6;            // H ring: NS3 slots of R rows
     constexpr int SLOT3 = R * HREC;
     static_assert(NS3 * SLOT3 <= NS * STAGE, "H ring fits the warp's ring");
@@ -899,18 +917,16 @@ void factor_impl(const TauArgs& a, int parts, cudaStream_t st) {
   int nmax = a.cls[0].n > a.cls[1].n ? a.cls[0].n : a.cls[1].n;
   dim3 grid((a.Nk + 63) / 64, 2);
   k_tau_factor<KL, KU><<<grid, 64, 0, st>>>(a, nmax);
+  // one partition: the sweeps need no transfer responses (B1 stores x directly)
   const int tgx = (a.Nk + 127) / 128;
-  if (parts == kTauParts)
-    k_tau_transfer<KL, KU, kTauParts><<<dim3(tgx, 2 * kTauParts, 16), 128, 0, st>>>(a);
-  else
-    k_tau_transfer<KL, KU, 1><<<dim3(tgx, 2, 16), 128, 0, st>>>(a);
+  if (parts == kTauParts) k_tau_transfer<KL, KU, kTauParts><<<dim3(tgx, 2 * kTauParts, 16), 128, 0, st>>>(a);
 }
 
 template <int P>
 size_t solve_smem_bytes(int npad) {
   constexpr size_t NL = 4 * kSolveModes;
-  return ((size_t)P * kPartStages * part_stage_doubles() + (size_t)npad * NL + (size_t)P * NL * kXch) *
-             sizeof(double) +
+  const size_t ys = P == 1 ? 0 : (size_t)npad * NL;  // one partition keeps y in global scratch
+  return ((size_t)P * kPartStages * part_stage_doubles<P>() + ys + (size_t)P * NL * kXch) * sizeof(double) +
          (size_t)npad * 2 * sizeof(int);
 }
 
@@ -953,8 +969,14 @@ size_t tau_transfer_doubles(int Nk, int parts) {
   return groups * (size_t)parts * 2 * kSolveModes * kTransfer;
 }
 
+size_t tau_solve_scratch_doubles(int Nk, int npad, int parts) {
+  if (parts != 1) return 0;
+  const size_t groups = (size_t)(Nk + kSolveModes - 1) / kSolveModes;
+  return groups * (size_t)npad * 4 * kSolveModes;
+}
+
 size_t tau_response_doubles(int Nk, int npad, int parts) {
-  (void)parts;
+  if (parts <= 1) return 0;
   const size_t groups = (size_t)(Nk + kSolveModes - 1) / kSolveModes;
   return groups * (size_t)npad * 2 * kSolveModes * kHRec;
 }

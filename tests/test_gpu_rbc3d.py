@@ -15,6 +15,8 @@ CASES = [
     (16, 12, 16, 4.0, 3.0, 1e5, "RK222", 0.05, 4),
     (12, 16, 12, 3.0, 4.0, 1e6, "RK443", 0.02, 3),
     (24, 24, 20, 4.0, 4.0, 1e7, "RK222", 0.005, 3),
+    # 2376 modes: enough mode groups that the tau solves run one warp per group
+    (64, 72, 8, 4.0, 4.0, 1e6, "RK222", 0.02, 2),
 ]
 
 
