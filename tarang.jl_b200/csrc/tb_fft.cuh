@@ -177,8 +177,129 @@ __device__ C* fft(C* a, C* b, const FftPlan& fp, const C* __restrict__ pt, int s
   return in;
 }
 
+// Swizzle keyed to the element size: the low bits of an index are XORed with
+// the next ones over a group of 128 bytes (8 double2 or 16 float2), so that the
+// stride-R stores of a pass and the unit-stride loads both spread over all
+// banks.  Buffers are padded to whole groups (pad_swz).
+template <class C>
+struct SwzGroup;
+template <>
+struct SwzGroup<double2> {
+  static constexpr int shift = 3;
+};
+template <>
+struct SwzGroup<float2> {
+  static constexpr int shift = 4;
+};
+template <class C>
+__host__ __device__ constexpr int pad_swz(int n) {
+  return (n + (1 << SwzGroup<C>::shift) - 1) & ~((1 << SwzGroup<C>::shift) - 1);
+}
+template <class C>
+__device__ __forceinline__ int sidx(int i) {
+  constexpr int s = SwzGroup<C>::shift;
+  return i ^ ((i >> s) & ((1 << s) - 1));
+}
+
+// Radix of stage s of the Stockham plan of length n (radices 8, then 4, 2, 3:
+// the order make_fft_plan uses), 0 past the last stage.
+__host__ __device__ constexpr int ct_radix(int n, int s) {
+  int k = 0;
+  while (n % 8 == 0) {
+    if (k == s) return 8;
+    n /= 8;
+    ++k;
+  }
+  while (n % 4 == 0) {
+    if (k == s) return 4;
+    n /= 4;
+    ++k;
+  }
+  while (n % 2 == 0) {
+    if (k == s) return 2;
+    n /= 2;
+    ++k;
+  }
+  while (n % 3 == 0) {
+    if (k == s) return 3;
+    n /= 3;
+    ++k;
+  }
+  return 0;
+}
+
+template <int R, class C>
+__device__ __forceinline__ void twiddle_apply(C (&v)[R], C w1) {
+  if constexpr (R == 8) {
+    const C w2 = mul(w1, w1), w4 = mul(w2, w2), w3 = mul(w1, w2);
+    v[1] = mul(v[1], w1);
+    v[2] = mul(v[2], w2);
+    v[3] = mul(v[3], w3);
+    v[4] = mul(v[4], w4);
+    v[5] = mul(v[5], mul(w1, w4));
+    v[6] = mul(v[6], mul(w2, w4));
+    v[7] = mul(v[7], mul(w3, w4));
+  } else if constexpr (R == 4) {
+    const C w2 = mul(w1, w1);
+    v[1] = mul(v[1], w1);
+    v[2] = mul(v[2], w2);
+    v[3] = mul(v[3], mul(w1, w2));
+  } else if constexpr (R == 3) {
+    v[1] = mul(v[1], w1);
+    v[2] = mul(v[2], mul(w1, w1));
+  } else {
+    v[1] = mul(v[1], w1);
+  }
+}
+
+// Compile-time form of pass_batch for a length-N plan (constant divisors and
+// strides, typed swizzle).
+template <int R, int NS, int N, class C>
+__device__ __forceinline__ void pass_ct(const C* __restrict__ in, C* __restrict__ out, const C* __restrict__ pt,
+                                        int sign, int nb, int stride) {
+  constexpr int nR = N / R;
+  for (int t = threadIdx.x; t < nb * nR; t += blockDim.x) {
+    const int q = t / nR, idx = t - q * nR;
+    const int j = idx % NS, k = idx / NS;
+    const C* src = in + (size_t)q * stride;
+    C* dst = out + (size_t)q * stride;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[sidx<C>(idx + r * nR)];
+    if constexpr (NS > 1) {
+      C w1 = pt[j];
+      if (sign > 0) w1.y = -w1.y;
+      twiddle_apply<R>(v, w1);
+    }
+    dft_small<R>(v, sign);
+    const int ob = k * NS * R + j;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[sidx<C>(ob + r * NS)] = v[r];
+  }
+}
+
+template <int N, int S, int NS, class C>
+__device__ __forceinline__ C* stages_ct(C* in, C* out, const C* __restrict__ pt, int sign, int nb, int stride) {
+  constexpr int R = ct_radix(N, S);
+  if constexpr (R == 0) {
+    return in;
+  } else {
+    pass_ct<R, NS, N>(in, out, pt, sign, nb, stride);
+    __syncthreads();
+    return stages_ct<N, S + 1, NS * R>(out, in, pt + NS, sign, nb, stride);
+  }
+}
+
+// nb CTA-wide length-N transforms (N a compile-time constant) between buffer
+// sets a and b; returns the set holding the results.  Same arithmetic and
+// twiddle tables as fft_batch with the runtime plan of length N.
+template <int N, class C>
+__device__ C* fft_batch_ct(C* a, C* b, int nb, int stride, const C* __restrict__ pt, int sign) {
+  return stages_ct<N, 0, 1>(a, b, pt, sign, nb, stride);
+}
+
 // Batched form: nb transforms of length fp.n, buffer q at a + q * stride (and
-// b + q * stride), all butterflies of a pass spread over the CTA.
+// b + q * stride), all butterflies of a pass spread over the CTA (typed swizzle).
 template <int R, bool SW, class C>
 __device__ __forceinline__ void pass_batch(const C* __restrict__ in, C* __restrict__ out, int n, int Ns,
                                            const C* __restrict__ pt, int sign, int nb, int stride) {
@@ -190,35 +311,16 @@ __device__ __forceinline__ void pass_batch(const C* __restrict__ in, C* __restri
     C* dst = out + (size_t)q * stride;
     C v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src[fidx<SW>(idx + r * nR)];
+    for (int r = 0; r < R; ++r) v[r] = src[SW ? sidx<C>(idx + r * nR) : idx + r * nR];
     if (Ns > 1) {
       C w1 = pt[j];
       if (sign > 0) w1.y = -w1.y;
-      if constexpr (R == 8) {
-        const C w2 = mul(w1, w1), w4 = mul(w2, w2), w3 = mul(w1, w2);
-        v[1] = mul(v[1], w1);
-        v[2] = mul(v[2], w2);
-        v[3] = mul(v[3], w3);
-        v[4] = mul(v[4], w4);
-        v[5] = mul(v[5], mul(w1, w4));
-        v[6] = mul(v[6], mul(w2, w4));
-        v[7] = mul(v[7], mul(w3, w4));
-      } else if constexpr (R == 4) {
-        const C w2 = mul(w1, w1);
-        v[1] = mul(v[1], w1);
-        v[2] = mul(v[2], w2);
-        v[3] = mul(v[3], mul(w1, w2));
-      } else if constexpr (R == 3) {
-        v[1] = mul(v[1], w1);
-        v[2] = mul(v[2], mul(w1, w1));
-      } else {
-        v[1] = mul(v[1], w1);
-      }
+      twiddle_apply<R>(v, w1);
     }
     dft_small<R>(v, sign);
     const int ob = k * Ns * R + j;
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst[fidx<SW>(ob + r * Ns)] = v[r];
+    for (int r = 0; r < R; ++r) dst[SW ? sidx<C>(ob + r * Ns) : ob + r * Ns] = v[r];
   }
 }
 

@@ -86,17 +86,28 @@ __global__ void __launch_bounds__(256) k3_prep(R3Args a, const double2* __restri
   Xc[3 * plane + i] = F::mk<C>((T)uz.x, (T)uz.y);
 }
 
+// Batched FFT of nb buffers: the compile-time plan when the length is one of the
+// specialised sizes (N > 0), else the runtime plan.
+template <int N, class C>
+__device__ __forceinline__ C* fftb(C* a, C* b, int nb, int stride, const FftPlan& fp, const C* __restrict__ pt,
+                                   int sign) {
+  if constexpr (N > 0)
+    return F::fft_batch_ct<N>(a, b, nb, stride, pt, sign);
+  else
+    return F::fft_batch<true>(a, b, nb, stride, fp, pt, sign);
+}
+
 // Per (kx column ix, z pair j / Nz-1-j).  G: 16 half planes (field f, w) at
 // G + (4 f + w) hplane, w = 0 even values, 1 odd values, 2 even d_z, 3 odd d_z,
 // element (j, m).  Output mix[z][q][ix][y], q = 3 f + kind (value, d_y, d_z).
-template <class C>
+template <class C, int MY>
 __global__ void __launch_bounds__(kR3Threads) k3_yinv(R3Args a, const C* __restrict__ G, const C* __restrict__ pty,
                                                        C* __restrict__ mix) {
   using T = typename F::Real<C>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
-  const int Ny = a.Ny, My = a.My, ix = blockIdx.x, j = blockIdx.y;
-  const int Ms = (My + 7) & ~7;
+  const int Ny = a.Ny, My = MY > 0 ? MY : a.My, ix = blockIdx.x, j = blockIdx.y;
+  const int Ms = F::pad_swz<C>(My);
   C* stg = sm;                    // [16][Ny]
   C* A = stg + 16 * Ny;           // [12][Ms]
   C* B = A + 12 * Ms;             // [12][Ms]
@@ -110,6 +121,7 @@ __global__ void __launch_bounds__(kR3Threads) k3_yinv(R3Args a, const C* __restr
   __syncthreads();
   const bool edge = (ix == 0) || (2 * ix == a.Nx);  // columns whose grid round trip is Hermitian
   const T xs = (2 * ix == a.Nx) ? (T)0.5 : (T)1.0;  // even-N Nyquist split along x
+  const int hy = Ny / 2, gap = My - Ny - 1;          // y bins hy+1 .. My-hy-1 stay zero
   for (int lev = 0; lev < 2; ++lev) {
     const int zl = lev ? a.Nz - 1 - j : j;
     // value (kind 0, 1) or z-derivative (kind 2) of field f at grid level zl
@@ -119,8 +131,10 @@ __global__ void __launch_bounds__(kR3Threads) k3_yinv(R3Args a, const C* __restr
       if (kind == 2) return lev ? F::sub(o, e) : F::add(e, o);
       return lev ? F::sub(e, o) : F::add(e, o);
     };
-    for (int t = threadIdx.x; t < 12 * Ms; t += blockDim.x) A[t] = F::mk<C>((T)0, (T)0);
-    __syncthreads();
+    for (int t = threadIdx.x; t < 12 * gap; t += blockDim.x) {
+      const int q = t / gap, y = hy + 1 + (t - q * gap);
+      A[(size_t)q * Ms + F::sidx<C>(y)] = F::mk<C>((T)0, (T)0);
+    }
     for (int t = threadIdx.x; t < 12 * Ny; t += blockDim.x) {
       const int q = t / Ny, iy = t - q * Ny;
       const int f = q / 3, kind = q - 3 * f;
@@ -138,21 +152,21 @@ __global__ void __launch_bounds__(kR3Threads) k3_yinv(R3Args a, const C* __restr
       }
       v = F::scale(v, xs);
       C* col = A + (size_t)q * Ms;
-      if (2 * iy < Ny) {
-        col[F::fidx<true>(iy)] = v;
-      } else if (2 * iy == Ny) {
+      if (iy < hy) {
+        col[F::sidx<C>(iy)] = v;
+      } else if (iy == hy) {
         const C h = F::scale(v, (T)0.5);
-        col[F::fidx<true>(Ny / 2)] = h;
-        col[F::fidx<true>(My - Ny / 2)] = h;
+        col[F::sidx<C>(hy)] = h;
+        col[F::sidx<C>(My - hy)] = h;
       } else {
-        col[F::fidx<true>(My - Ny + iy)] = v;
+        col[F::sidx<C>(My - Ny + iy)] = v;
       }
     }
     __syncthreads();
-    C* R = F::fft_batch<true>(A, B, 12, Ms, a.fpy, pt, +1);
+    C* R = fftb<MY>(A, B, 12, Ms, a.fpy, pt, +1);
     for (int t = threadIdx.x; t < 12 * My; t += blockDim.x) {
       const int q = t / My, y = t - q * My;
-      mix[(((size_t)zl * 12 + q) * a.Kx + ix) * My + y] = R[(size_t)q * Ms + F::fidx<true>(y)];
+      mix[(((size_t)zl * 12 + q) * a.Kx + ix) * My + y] = R[(size_t)q * Ms + F::sidx<C>(y)];
     }
     __syncthreads();
   }
@@ -160,61 +174,61 @@ __global__ void __launch_bounds__(kR3Threads) k3_yinv(R3Args a, const C* __restr
 
 // Per (RR consecutive padded y rows, z level).  mix[z][q][kx][y] ->
 // pm[z][f][kx][y] (f = b, u_x, u_y, u_z; kx < Kx, Nyquist folded).
-template <class C, int RR>
+// Factors on the x grid (15 real, packed in pairs a + i b): 0 u_x, 1 u_y,
+// 2 u_z, 3..6 d_x f, 7..10 d_y f, 11..14 d_z f (f = b, u_x, u_y, u_z).
+template <class C, int RR, int MX>
 __global__ void __launch_bounds__(kR3Threads) k3_xpass(R3Args a, const C* __restrict__ mix, const C* __restrict__ ptx,
                                                         C* __restrict__ pm) {
   using T = typename F::Real<C>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
-  const int Mx = a.Mx, Kx = a.Kx, My = a.My, hN = a.Nx / 2;
+  const int Mx = MX > 0 ? MX : a.Mx, Kx = a.Kx, My = a.My, hN = a.Nx / 2;
   const int y0 = blockIdx.x * RR, z = blockIdx.y;
-  const int Ms = (Mx + 7) & ~7;
+  const int Ms = F::pad_swz<C>(Mx);
   constexpr int NB = 8 * RR;
   C* Z = sm;              // [NB][Ms]
   C* S = Z + NB * Ms;     // [NB][Ms]
   C* pt = S + NB * Ms;    // [nptx]
   for (int t = threadIdx.x; t < a.nptx; t += blockDim.x) pt[t] = ptx[t];
-  const int nh = Mx / 2 + 1;
-  // half-spectrum bin k of factor idx (0 u_x, 1 u_y, 2 u_z, 3..6 d_x f, 7..10
-  // d_y f, 11..14 d_z f, 15 none) on row y0 + r; DC and Nyquist kept real
-  auto fac = [&](int idx, int r, int k) -> C {
-    if (idx >= 15 || k >= Kx) return F::mk<C>((T)0, (T)0);
-    int q;
-    bool dx = false;
-    if (idx < 3) {
-      q = 3 * (idx + 1);
-    } else if (idx < 7) {
-      q = 3 * (idx - 3);
-      dx = true;
-    } else if (idx < 11) {
-      q = 3 * (idx - 7) + 1;
-    } else {
-      q = 3 * (idx - 11) + 2;
-    }
-    if (dx && (k == 0 || k == hN)) return F::mk<C>((T)0, (T)0);
+  // 1. half spectra of the 15 factors, [r][factor][k < Kx], staged in S (DC and
+  // Nyquist kept real, as the factors' own irfft on Nx points does)
+  C* hs = S;
+  for (int t = threadIdx.x; t < 12 * Kx * RR; t += blockDim.x) {
+    const int r = t % RR, rest = t / RR;
+    const int k = rest % Kx, q = rest / Kx;
     C v = mix[(((size_t)z * 12 + q) * Kx + k) * My + y0 + r];
-    if (k == 0 || k == hN) v.y = (T)0;
-    if (dx) {
+    const bool edge = (k == 0 || k == hN);
+    if (edge) v.y = (T)0;
+    const int f = q / 3, kind = q - 3 * f;
+    C* row = hs + (size_t)r * 15 * Kx;
+    if (kind == 0) {
+      if (f > 0) row[(size_t)(f - 1) * Kx + k] = v;
       const T kk = (T)(a.kx0 * k);
-      v = F::mk<C>(-kk * v.y, kk * v.x);  // i kx v
+      row[(size_t)(3 + f) * Kx + k] = edge ? F::mk<C>((T)0, (T)0) : F::mk<C>(-kk * v.y, kk * v.x);  // i kx v
+    } else {
+      row[(size_t)((kind == 1 ? 7 : 11) + f) * Kx + k] = v;
     }
-    return v;
-  };
+  }
+  __syncthreads();
+  // 2. packed spectra: Z[p] = spectrum of factor 2p + i factor 2p+1 on Mx points
+  const int nh = Mx / 2 + 1;
   for (int t = threadIdx.x; t < RR * 8 * nh; t += blockDim.x) {
     const int r = t % RR, rest = t / RR;
     const int k = rest % nh, p = rest / nh;
-    const C A = fac(2 * p, r, k), B = fac(2 * p + 1, r, k);
+    const C* row = hs + (size_t)r * 15 * Kx;
+    const C A = k < Kx ? row[(size_t)(2 * p) * Kx + k] : F::mk<C>((T)0, (T)0);
+    const C B = (k < Kx && p < 7) ? row[(size_t)(2 * p + 1) * Kx + k] : F::mk<C>((T)0, (T)0);
     C* dst = Z + (size_t)(r * 8 + p) * Ms;
     // spectrum of a + i b: A + i B at k, conj(A) + i conj(B) at Mx - k
-    dst[F::fidx<true>(k)] = F::mk<C>(A.x - B.y, A.y + B.x);
-    if (k > 0 && k < Mx / 2) dst[F::fidx<true>(Mx - k)] = F::mk<C>(A.x + B.y, -A.y + B.x);
+    dst[F::sidx<C>(k)] = F::mk<C>(A.x - B.y, A.y + B.x);
+    if (k > 0 && k < Mx / 2) dst[F::sidx<C>(Mx - k)] = F::mk<C>(A.x + B.y, -A.y + B.x);
   }
   __syncthreads();
-  C* Rg = F::fft_batch<true>(Z, S, NB, Ms, a.fpx, pt, +1);
+  C* Rg = fftb<MX>(Z, S, NB, Ms, a.fpx, pt, +1);
   C* W = (Rg == Z) ? S : Z;
   for (int t = threadIdx.x; t < RR * Mx; t += blockDim.x) {
     const int r = t / Mx, x = t - r * Mx;
-    const int i = F::fidx<true>(x);
+    const int i = F::sidx<C>(x);
     const C* g = Rg + (size_t)r * 8 * Ms;
     const C z0 = g[i], z1 = g[Ms + i], z2 = g[2 * Ms + i], z3 = g[3 * Ms + i];
     const C z4 = g[4 * Ms + i], z5 = g[5 * Ms + i], z6 = g[6 * Ms + i], z7 = g[7 * Ms + i];
@@ -227,12 +241,12 @@ __global__ void __launch_bounds__(kR3Threads) k3_xpass(R3Args a, const C* __rest
     W[(size_t)(2 * r + 1) * Ms + i] = F::mk<C>(pv, pw);
   }
   __syncthreads();
-  C* Fq = F::fft_batch<true>(W, Rg, 2 * RR, Ms, a.fpx, pt, -1);
+  C* Fq = fftb<MX>(W, Rg, 2 * RR, Ms, a.fpx, pt, -1);
   for (int t = threadIdx.x; t < RR * 2 * Kx; t += blockDim.x) {
     const int r = t % RR, rest = t / RR;
     const int k = rest % Kx, h = rest / Kx;
     const C* buf = Fq + (size_t)(2 * r + h) * Ms;
-    const C c = buf[F::fidx<true>(k)], cm = buf[F::fidx<true>((Mx - k) % Mx)];
+    const C c = buf[F::sidx<C>(k)], cm = buf[F::sidx<C>((Mx - k) % Mx)];
     // first: (c + conj(cm))/2, second: (c - conj(cm))/(2i)
     C o1 = F::mk<C>((T)0.5 * (c.x + cm.x), (T)0.5 * (c.y - cm.y));
     C o2 = F::mk<C>((T)0.5 * (c.y + cm.y), (T)-0.5 * (c.x - cm.x));
@@ -251,24 +265,24 @@ __global__ void __launch_bounds__(kR3Threads) k3_xpass(R3Args a, const C* __rest
 // Per (kx column ix, z level): forward FFTs along y of the 4 products, y
 // Nyquist fold and truncation, F = -P / (Nx Ny Mx My), rotation of the
 // horizontal momentum rows; out[f][z][m] for f = b, u_par, u_z, u_perp.
-template <class C>
+template <class C, int MY>
 __global__ void __launch_bounds__(kR3Threads) k3_yfwd(R3Args a, const C* __restrict__ pm, const C* __restrict__ pty,
                                                        C* __restrict__ out) {
   using T = typename F::Real<C>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
-  const int Ny = a.Ny, My = a.My, ix = blockIdx.x, z = blockIdx.y;
-  const int Ms = (My + 7) & ~7;
+  const int Ny = a.Ny, My = MY > 0 ? MY : a.My, ix = blockIdx.x, z = blockIdx.y;
+  const int Ms = F::pad_swz<C>(My);
   C* A = sm;
   C* B = A + 4 * Ms;
   C* pt = B + 4 * Ms;
   for (int t = threadIdx.x; t < a.npty; t += blockDim.x) pt[t] = pty[t];
   for (int t = threadIdx.x; t < 4 * My; t += blockDim.x) {
     const int f = t / My, y = t - f * My;
-    A[(size_t)f * Ms + F::fidx<true>(y)] = pm[(((size_t)z * 4 + f) * a.Kx + ix) * My + y];
+    A[(size_t)f * Ms + F::sidx<C>(y)] = pm[(((size_t)z * 4 + f) * a.Kx + ix) * My + y];
   }
   __syncthreads();
-  const C* Q = F::fft_batch<true>(A, B, 4, Ms, a.fpy, pt, -1);
+  const C* Q = fftb<MY>(A, B, 4, Ms, a.fpy, pt, -1);
   const double sc = -1.0 / ((double)a.Nx * (double)Ny * (double)a.Mx * (double)My);
   const size_t plane = (size_t)a.Nz * a.Nk;
   for (int iy = threadIdx.x; iy < Ny; iy += blockDim.x) {
@@ -278,11 +292,11 @@ __global__ void __launch_bounds__(kR3Threads) k3_yfwd(R3Args a, const C* __restr
       const C* col = Q + (size_t)f * Ms;
       C r;
       if (2 * iy < Ny) {
-        r = col[F::fidx<true>(iy)];
+        r = col[F::sidx<C>(iy)];
       } else if (2 * iy == Ny) {
-        r = F::add(col[F::fidx<true>(Ny / 2)], col[F::fidx<true>(My - Ny / 2)]);
+        r = F::add(col[F::sidx<C>(Ny / 2)], col[F::sidx<C>(My - Ny / 2)]);
       } else {
-        r = col[F::fidx<true>(My - Ny + iy)];
+        r = col[F::sidx<C>(My - Ny + iy)];
       }
       v[f] = make_double2(sc * (double)r.x, sc * (double)r.y);
     }
@@ -523,17 +537,17 @@ R3Args args_of(const tb_plan* P) {
 
 template <class C>
 size_t yinv_smem(const R3Args& a) {
-  const size_t Ms = (size_t)((a.My + 7) & ~7);
+  const size_t Ms = (size_t)F::pad_swz<C>(a.My);
   return (16 * (size_t)a.Ny + 24 * Ms + (size_t)a.npty) * sizeof(C);
 }
 template <class C, int RR>
 size_t xpass_smem(const R3Args& a) {
-  const size_t Ms = (size_t)((a.Mx + 7) & ~7);
+  const size_t Ms = (size_t)F::pad_swz<C>(a.Mx);
   return (16 * RR * Ms + (size_t)a.nptx) * sizeof(C);
 }
 template <class C>
 size_t yfwd_smem(const R3Args& a) {
-  const size_t Ms = (size_t)((a.My + 7) & ~7);
+  const size_t Ms = (size_t)F::pad_swz<C>(a.My);
   return (8 * Ms + (size_t)a.npty) * sizeof(C);
 }
 
@@ -549,12 +563,17 @@ struct XRows<double2> {
   static constexpr int value = 1;
 };
 
+// Padded transform length with compiled plans (the 256-point grids of the 3D
+// benchmark configuration); other lengths run the runtime plan.
+constexpr int kFixedLen = 384;
+
 template <class C>
 void set_limits(int bytes) {
   constexpr int RR = XRows<C>::value;
-  TB_CUDA_TRY(cudaFuncSetAttribute(k3_yinv<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  TB_CUDA_TRY(cudaFuncSetAttribute(k3_xpass<C, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  TB_CUDA_TRY(cudaFuncSetAttribute(k3_yfwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  const void* fns[] = {(const void*)k3_yinv<C, 0>,      (const void*)k3_yinv<C, kFixedLen>,
+                       (const void*)k3_xpass<C, RR, 0>, (const void*)k3_xpass<C, RR, kFixedLen>,
+                       (const void*)k3_yfwd<C, 0>,      (const void*)k3_yfwd<C, kFixedLen>};
+  for (const void* fn : fns) TB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
 }
 
 inline int pad16(int k) { return (k + 15) / 16 * 16; }
@@ -591,16 +610,19 @@ void enqueue_rhs_t(tb_plan* P, const double2* Xin, double2* out4) {
                                       (w & 1) ? P->Ko : P->Ke, pad16((w & 1) ? P->Ko : P->Ke), GEMM_PARITY, w & 1};
     timed(P, "z_backward_gemm", [&] { launch_gemm_f64(bt, 16, ncol, ncol, ncol, N, P->st); });
   }
+  const bool fy = P->My == kFixedLen, fx = P->M == kFixedLen;
   timed(P, "rhs3_yinv", [&] {
-    k3_yinv<C><<<dim3(P->Kx, H), kR3Threads, yinv_smem<C>(a), P->st>>>(a, G, P->ptwY.as<C>(), P->mix3.as<C>());
+    auto kern = fy ? k3_yinv<C, kFixedLen> : k3_yinv<C, 0>;
+    kern<<<dim3(P->Kx, H), kR3Threads, yinv_smem<C>(a), P->st>>>(a, G, P->ptwY.as<C>(), P->mix3.as<C>());
   });
   timed(P, "rhs3_xpass", [&] {
-    k3_xpass<C, RR><<<dim3(P->My / RR, N), kR3Threads, xpass_smem<C, RR>(a), P->st>>>(
-        a, P->mix3.as<C>(), P->ptwX.as<C>(), P->pm3.as<C>());
+    auto kern = fx ? k3_xpass<C, RR, kFixedLen> : k3_xpass<C, RR, 0>;
+    kern<<<dim3(P->My / RR, N), kR3Threads, xpass_smem<C, RR>(a), P->st>>>(a, P->mix3.as<C>(), P->ptwX.as<C>(),
+                                                                            P->pm3.as<C>());
   });
   timed(P, "rhs3_yfwd", [&] {
-    k3_yfwd<C><<<dim3(P->Kx, N), kR3Threads, yfwd_smem<C>(a), P->st>>>(a, P->pm3.as<C>(), P->ptwY.as<C>(),
-                                                                        P->H3.as<C>());
+    auto kern = fy ? k3_yfwd<C, kFixedLen> : k3_yfwd<C, 0>;
+    kern<<<dim3(P->Kx, N), kR3Threads, yfwd_smem<C>(a), P->st>>>(a, P->pm3.as<C>(), P->ptwY.as<C>(), P->H3.as<C>());
   });
   const C* H3 = P->H3.as<C>();
   if constexpr (f32) {

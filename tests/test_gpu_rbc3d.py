@@ -17,6 +17,9 @@ CASES = [
     (24, 24, 20, 4.0, 4.0, 1e7, "RK222", 0.005, 3),
     # 2376 modes: enough mode groups that the tau solves run one warp per group
     (64, 72, 8, 4.0, 4.0, 1e6, "RK222", 0.02, 2),
+    # 384-point padded x / y transforms (the compiled plans of the 256-point grids)
+    (256, 8, 8, 4.0, 4.0, 1e6, "RK222", 0.01, 2),
+    (8, 256, 8, 4.0, 4.0, 1e6, "RK222", 0.01, 2),
 ]
 
 
@@ -46,7 +49,7 @@ def test_rbc3d_f64_matches_oracle(tb, case):
     assert np.abs(plan.get_state(tb._lib.TB_FIELD_P)).max() == 0.0  # zeroed by the final mass solve
 
 
-@pytest.mark.parametrize("case", CASES[:2])
+@pytest.mark.parametrize("case", CASES[:2] + CASES[-2:])
 def test_rbc3d_mixed_matches_oracle(tb, case):
     plan, sim = _run(tb, case, tb._lib.TB_PREC_MIXED)
     for name, f in FIELDS:
