@@ -102,6 +102,14 @@ class Dist:
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
+    def gather(self, obj):
+        """Every rank's obj, in rank order (host objects; statistics only)."""
+        if not self.pg:
+            return [obj]
+        out = [None] * self.world
+        self.pg.all_gather_object(out, obj)
+        return out
+
     def close(self):
         if self.pg:
             self.pg.barrier()
@@ -434,11 +442,7 @@ def run_ours(args, cfg, scheme, dist):
             "cpu_baseline": cpu,
             "finite": bool(finite),
         }
-        if dist.world == 1 and not args.no_ensemble:
-            try:
-                out["ensemble"] = run_ensemble(args, dev)
-            except Exception as exc:  # reported, never fatal to the headline line
-                out["ensemble"] = {"error": f"{type(exc).__name__}: {exc}"}
+
         if dist.world == 1 and not args.no_mixed:
             try:
                 out["mixed"] = run_mixed(args, cfg, scheme, dev)
@@ -449,18 +453,31 @@ def run_ours(args, cfg, scheme, dist):
                 out["rbc3d"] = run_rbc3d(args, dev)
             except Exception as exc:  # reported, never fatal to the headline line
                 out["rbc3d"] = {"error": f"{type(exc).__name__}: {exc}"}
-        if dist.world == 1 and not args.no_serving:
-            try:
-                out["serving"] = run_serving(args, dev)
-            except Exception as exc:  # reported, never fatal to the headline line
-                out["serving"] = {"error": f"{type(exc).__name__}: {exc}"}
+    # sharded across every rank (collective statistics: all ranks take part)
+    if not args.no_ensemble:
+        try:
+            ens_out = run_ensemble(args, dev, dist)
+        except Exception as exc:  # reported, never fatal to the headline line
+            ens_out = {"error": f"{type(exc).__name__}: {exc}"}
+    if not args.no_serving:
+        try:
+            srv_out = run_serving(args, dev, dist)
+        except Exception as exc:  # reported, never fatal to the headline line
+            srv_out = {"error": f"{type(exc).__name__}: {exc}"}
+    if dist.rank == 0:
+        if not args.no_ensemble:
+            out["ensemble"] = ens_out
+        if not args.no_serving:
+            out["serving"] = srv_out
         print(json.dumps(out), flush=True)
 
 
-def run_ensemble(args, dev):
+def run_ensemble(args, dev, dist=None):
     """Batched ensemble (independent 2D RBC instances of uneven size, RK222):
     instance steps per second of the ensemble runner against the plain GPU form
-    (the same plans stepped one after another), and time-to-solution p50/p99."""
+    (the same plans stepped one after another), and time-to-solution p50/p99.
+    Under N ranks the members are sharded by cost (shard_instances) with no
+    data-path collective; only the statistics are gathered."""
     import numpy as np
     import torch
 
@@ -470,6 +487,10 @@ def run_ensemble(args, dev):
     from tarang_b200 import workloads as W
 
     members = W.ensemble_members(args.ensemble_size)
+    world = dist.world if dist else 1
+    rank = dist.rank if dist else 0
+    shards = W.shard_instances([W.instance_cost(c) for c in members], world)
+    members = [members[i] for i in shards[rank]]
     plans, init = [], []
     for c in members:
         dom = tb.ChannelDomain(c.Nx, c.Nz, Lx=c.Lx, Lz=c.Lz, arch=tb.GPU(dev))
@@ -508,29 +529,33 @@ def run_ensemble(args, dev):
     ms, total = ens.run(dts, n)
     wall = time.perf_counter() - t0
     finite = all(np.isfinite(p.get_state(0)).all() for p in plans)
-    steps = len(plans) * n
+    part = {"steps": len(plans) * n, "total_ms": float(total), "ms": [float(v) for v in ms], "plain_s": plain_s,
+            "plain_done_ms": done, "finite": bool(finite)}
+    parts = dist.gather(part) if dist else [part]
+    agg = W.combine_ensemble(parts)
     sizes = {}
-    for c in members:
+    for c in W.ensemble_members(args.ensemble_size):
         sizes[f"{c.Nx}x{c.Nz}"] = sizes.get(f"{c.Nx}x{c.Nz}", 0) + 1
     return {
         "metric": "ensemble instance steps/s",
-        "value": steps / (total / 1e3),
+        "value": agg["value"],
         "unit": "instance-steps/s",
-        "members": len(plans),
+        "members": agg["members"],
         "steps_each": n,
         "sizes": sizes,
+        "n_gpus": world,
+        "sharding": "members assigned to ranks by cost (longest processing time first), no collective"
+                    if world > 1 else "one GPU",
         "scheme": "RK222",
         "dtype": "f64",
         "tuned": {"worker_streams": streams, "steps_per_graph": gsteps},
-        "time_to_solution_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99)),
-                                "max": float(total)},
+        "time_to_solution_ms": {"p50": agg["p50_ms"], "p99": agg["p99_ms"], "max": agg["total_ms"]},
         "wall_s": wall,
-        "plain_gpu": {"value": steps / plain_s, "unit": "instance-steps/s",
+        "plain_gpu": {"value": agg["plain_value"], "unit": "instance-steps/s",
                       "what": "the same plans stepped one after another with tb_step (host wall clock)",
-                      "time_to_solution_ms": {"p50": float(np.percentile(done, 50)),
-                                              "p99": float(np.percentile(done, 99))}},
-        "speedup_vs_plain_gpu": (steps / (total / 1e3)) / (steps / plain_s),
-        "finite": bool(finite),
+                      "time_to_solution_ms": {"p50": agg["plain_p50_ms"], "p99": agg["plain_p99_ms"]}},
+        "speedup_vs_plain_gpu": agg["value"] / agg["plain_value"],
+        "finite": all(p["finite"] for p in parts),
         "data": "synthetic: sizes, Ra, Pr and noise seeded (ensemble seed 7, member noise seed 1000+k)",
     }
 
@@ -807,12 +832,14 @@ def run_turb(args, dev):
             "data": "synthetic: k^-3 spectrum, random phases (seed 7000)"}
 
 
-def run_serving(args, dev):
+def run_serving(args, dev, dist=None):
     """Serving mix: seeded Poisson arrivals (20/s) of RBC channel runs and FP32
     decaying turbulence, 50-500 steps each, admitted by HBM budget.  Replayed
     through the request server (continuous batching) and through the plain GPU
     form (one request at a time); also the saturated throughput with every
-    request queued at once."""
+    request queued at once.  Under N ranks the requests are sharded by cost
+    (each rank serves its share at the original arrival times, no data-path
+    collective) and the statistics are gathered."""
     import numpy as np
 
     from __graft_entry__ import load_package
@@ -821,9 +848,14 @@ def run_serving(args, dev):
     from tarang_b200 import workloads as W
 
     reqs = W.serving_requests(args.serve_requests)
+    world = dist.world if dist else 1
+    rank = dist.rank if dist else 0
+    mine = set(W.shard_instances([W.instance_cost(r) for r in reqs], world)[rank])
     prepared = []
-    for r in reqs:
-        if r.kind == "rbc":
+    for k, r in enumerate(reqs):
+        if k not in mine:
+            prepared.append(None)
+        elif r.kind == "rbc":
             c = r.rbc
             prepared.append((tb.rbc_desc(c.Nx, c.Nz, c.kappa, c.nu, 0, Lx=c.Lx, Lz=c.Lz), r.dt, r.nsteps,
                              W.rbc_initial_grid(c)))
@@ -832,35 +864,47 @@ def run_serving(args, dev):
     budget = int(args.serve_budget_gb * (1 << 30))
 
     def replay(max_running, timed_arrivals, chunk=10, subset=None):
+        subset = mine if subset is None else (subset & mine)
         srv = tb.Server(budget_bytes=budget, max_running=max_running, chunk_steps=chunk, device=dev)
         t0 = time.perf_counter()
-        ids = []
-        for k, (r, (d, dt, n, init)) in enumerate(zip(reqs, prepared)):
-            if subset is not None and k not in subset:
+        ids, steps = [], 0
+        for k, r in enumerate(reqs):
+            if k not in subset:
                 continue
+            d, dt, n, init = prepared[k]
             if timed_arrivals:
                 wait = r.arrival_s - (time.perf_counter() - t0)
                 if wait > 0:
                     time.sleep(wait)
             ids.append(srv.submit(d, dt, n, init))
+            steps += n
         srv.wait_all()
         wall = time.perf_counter() - t0
         st = srv.stats()
-        ok = all(srv.poll(i)[0] == tb._lib.TB_REQ_DONE for i in ids)
+        polls = [srv.poll(i) for i in ids]
+        ok = all(p[0] == tb._lib.TB_REQ_DONE for p in polls)
         srv.close()
-        return {"solves_per_s": st["solves_per_s"], "steps_per_s": st["steps_per_s"],
-                "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_queue_wait_ms": st["mean_wait_ms"],
-                "peak_running": st["peak_running"], "peak_budgeted_bytes": st["peak_bytes"],
-                "completed": st["completed"], "failed": st["failed"], "wall_s": wall, "all_done": ok}
+        part = {"completed": int(st["completed"]), "steps": steps, "wall_s": wall,
+                "tts_ms": [float(p[1]) for p in polls], "failed": int(st["failed"]), "all_done": ok,
+                "peak_running": int(st["peak_running"]), "peak_bytes": int(st["peak_bytes"]),
+                "mean_wait_ms": float(st["mean_wait_ms"])}
+        parts = dist.gather(part) if dist else [part]
+        agg = W.combine_serving(parts)
+        return {"solves_per_s": agg["solves_per_s"], "steps_per_s": agg["steps_per_s"], "p50_ms": agg["p50_ms"],
+                "p99_ms": agg["p99_ms"], "mean_queue_wait_ms": float(np.mean([p["mean_wait_ms"] for p in parts])),
+                "peak_running": max(p["peak_running"] for p in parts),
+                "peak_budgeted_bytes": max(p["peak_bytes"] for p in parts), "completed": agg["completed"],
+                "failed": sum(p["failed"] for p in parts), "wall_s": agg["wall_s"],
+                "all_done": all(p["all_done"] for p in parts)}
 
     # warm-up: one request of every kind and size (kernel loading, first-use costs)
-    seen, warm = set(), []
+    seen, warm = set(), set()
     for k, r in enumerate(reqs):
         key = (r.kind, r.rbc.Nx if r.rbc else r.N)
-        if key not in seen:
+        if k in mine and key not in seen:
             seen.add(key)
-            warm.append(k)
-    replay(8, False, subset=set(warm))
+            warm.add(k)
+    replay(8, False, subset=warm)
     # continuous batching: up to 16 requests in flight, chunks of 10 steps;
     # plain GPU form: one request at a time, chunks of 50 steps
     served = replay(16, True)
@@ -874,6 +918,9 @@ def run_serving(args, dev):
         "unit": "requests/s",
         "requests": len(reqs),
         "mix": kinds,
+        "n_gpus": world,
+        "sharding": "requests assigned to ranks by cost, each rank replays its share at the original arrival "
+                    "times, no collective" if world > 1 else "one GPU",
         "hbm_budget_bytes": budget,
         "replay": served,
         "plain_gpu_replay": plain,
@@ -935,11 +982,13 @@ def main():
         if args.impl == "reference":
             run_reference(args, cfg, scheme, dist)
         elif args.workload == "ensemble":
+            res = run_ensemble(args, dist.local, dist)
             if dist.rank == 0:
-                print(json.dumps(run_ensemble(args, dist.local)), flush=True)
+                print(json.dumps(res), flush=True)
         elif args.workload == "serving":
+            res = run_serving(args, dist.local, dist)
             if dist.rank == 0:
-                print(json.dumps(run_serving(args, dist.local)), flush=True)
+                print(json.dumps(res), flush=True)
         elif args.workload == "rbc3d":
             if dist.rank == 0:
                 print(json.dumps(run_rbc3d(args, dist.local)), flush=True)

@@ -249,3 +249,72 @@ def turb_initial_spec(N: int, seed: int, amp: float = 10.0) -> np.ndarray:
     g = np.fft.irfft(np.fft.ifft(mag * np.exp(1j * phase), axis=0), n=N, axis=1)
     g *= amp / np.abs(g).max()
     return np.fft.fft(np.fft.rfft(g, axis=1), axis=0)
+
+
+# ---------------------------------------------------------------------------
+# Instance sharding across GPUs (independent solves, no data-path collective)
+# ---------------------------------------------------------------------------
+def instance_cost(item) -> float:
+    """Relative device work of one independent instance: the byte model of one
+    step times the steps it runs (RBCConfig members run `steps` given by the
+    caller; ServeRequest carries its own)."""
+    if isinstance(item, ServeRequest):
+        if item.kind == "rbc":
+            return step_model_bytes(item.rbc, "RK222") * item.nsteps
+        M = 3 * item.N // 2
+        return 12.0 * 8.0 * M * M * item.nsteps  # padded FP32 planes moved per step
+    return step_model_bytes(item, item.scheme)
+
+
+def shard_instances(costs, world: int):
+    """Longest-processing-time assignment of independent instances to `world`
+    ranks: instances in decreasing cost (index breaks ties) each go to the rank
+    with the least assigned cost (lowest rank breaks ties).  Deterministic, so
+    every rank computes the same partition without communicating; returns one
+    ascending index list per rank."""
+    order = sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i))
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += float(costs[i])
+    return [sorted(x) for x in out]
+
+
+def combine_ensemble(parts):
+    """Whole-job ensemble figures from per-rank parts (dicts with steps,
+    total_ms, ms (per-member completion), plain_s, plain_done_ms): instance
+    steps over the slowest rank's time, percentiles over all members."""
+    steps = sum(p["steps"] for p in parts)
+    total_ms = max(p["total_ms"] for p in parts)
+    plain_s = max(p["plain_s"] for p in parts)
+    ms = np.concatenate([np.asarray(p["ms"], dtype=np.float64) for p in parts])
+    done = np.concatenate([np.asarray(p["plain_done_ms"], dtype=np.float64) for p in parts])
+    return {
+        "value": steps / (total_ms / 1e3),
+        "plain_value": steps / plain_s,
+        "total_ms": total_ms,
+        "p50_ms": float(np.percentile(ms, 50)),
+        "p99_ms": float(np.percentile(ms, 99)),
+        "plain_p50_ms": float(np.percentile(done, 50)),
+        "plain_p99_ms": float(np.percentile(done, 99)),
+        "members": int(ms.size),
+    }
+
+
+def combine_serving(parts):
+    """Whole-job serving figures from per-rank replays (dicts with completed,
+    steps, wall_s, tts_ms list): requests and request-steps per second over the
+    slowest rank's wall time, time-to-solution percentiles over all requests."""
+    wall = max(p["wall_s"] for p in parts)
+    tts = np.concatenate([np.asarray(p["tts_ms"], dtype=np.float64) for p in parts])
+    completed = sum(p["completed"] for p in parts)
+    return {
+        "solves_per_s": completed / wall,
+        "steps_per_s": sum(p["steps"] for p in parts) / wall,
+        "p50_ms": float(np.percentile(tts, 50)) if tts.size else None,
+        "p99_ms": float(np.percentile(tts, 99)) if tts.size else None,
+        "completed": completed,
+        "wall_s": wall,
+    }

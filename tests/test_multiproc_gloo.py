@@ -50,3 +50,35 @@ def test_reference_arm_prints_once_under_two_ranks():
     assert len(lines0) == 1 and not lines1
     d = json.loads(lines0[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_instance_sharding_is_complete_disjoint_and_agreed_by_two_ranks():
+    # Each rank derives its share of the ensemble members and of the serving
+    # requests on its own (no communication), as bench.py does under torchrun;
+    # the gathered shares must cover every instance exactly once and every rank
+    # must have computed the same partition.
+    code = (
+        "import json, bench\n"
+        "from __graft_entry__ import load_package\n"
+        "load_package()\n"
+        "from tarang_b200 import workloads as W\n"
+        "d = bench.Dist()\n"
+        "mem = W.ensemble_members(64)\n"
+        "req = W.serving_requests(60)\n"
+        "sm = W.shard_instances([W.instance_cost(c) for c in mem], d.world)\n"
+        "sr = W.shard_instances([W.instance_cost(r) for r in req], d.world)\n"
+        "got = d.gather({'rank': d.rank, 'members': sm[d.rank], 'requests': sr[d.rank], 'plan': [sm, sr]})\n"
+        "print(json.dumps(got))\n"
+        "d.close()\n"
+    )
+    res = _run_two_ranks(code, 29637)
+    for rc, out, err in res:
+        assert rc == 0, err[-2000:]
+    got = json.loads(res[0][1].strip().splitlines()[-1])
+    assert got == json.loads(res[1][1].strip().splitlines()[-1])
+    assert [g["rank"] for g in got] == [0, 1]
+    assert got[0]["plan"] == got[1]["plan"]
+    for key, n in (("members", 64), ("requests", 60)):
+        allidx = sorted(got[0][key] + got[1][key])
+        assert allidx == list(range(n))
+        assert got[0][key] and got[1][key]
