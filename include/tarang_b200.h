@@ -137,6 +137,21 @@ tb_status tb_tau_layout_query(int Nz, double Lx, double Lz, int cls, int* info4)
 /* Number of kernels one step launches (for launch accounting). */
 tb_status tb_kernels_per_step(const tb_plan* plan, int* n);
 
+/* Kernel shapes of a plan (the library's own autotuning; the reference tunes
+ * FFTW plans instead, transform_fourier.jl plan cache):
+ *   tau_parts  warps per 4-mode group in the tau solves: 4 (partitioned, the
+ *              shortest latency for one plan) or 1 (no response records, the
+ *              least device work per solve);
+ *   xrows      3D only: padded y rows per x-pass CTA, 1, 2 or 4.
+ * 0 keeps a setting.  A change drops the plan's factors and step graphs; the
+ * next step rebuilds them.  tb_plan_tune times trial_steps steps of every
+ * feasible combination from the current state (the state is restored after
+ * each trial and at the end) and keeps the fastest; *tau_parts / *xrows get
+ * the choice (xrows 0 in 2D). */
+tb_status tb_plan_set_variant(tb_plan* plan, int tau_parts, int xrows);
+tb_status tb_plan_get_variant(const tb_plan* plan, int* tau_parts, int* xrows);
+tb_status tb_plan_tune(tb_plan* plan, double dt, int trial_steps, int* tau_parts, int* xrows);
+
 /* -------------------------------------------------------------------------
  * Transform backend.  Replaces Tarang._gpu_forward_transform_backend! /
  * _gpu_backward_transform_backend!(::GPU, field)
@@ -211,8 +226,9 @@ tb_status tb_plan_device_bytes(const tb_plan* plan, size_t* bytes);
  * instances in turn.  Members are borrowed plans of one context; a run steps
  * every member nsteps at its own dt (dt[i]), spreading the members' step graphs
  * over worker streams.  tb_ensemble_tune times candidate (streams, steps per
- * graph) settings on the members from a snapshot of their state, restores the
- * state and keeps the fastest setting.  member_ms[i]: time from the run's start
+ * graph, tau-solve partitions of the members) settings on the members from a
+ * snapshot of their state, restores the state and keeps the fastest setting
+ * (the partitioning is applied to the member plans: tb_plan_get_variant).  member_ms[i]: time from the run's start
  * until member i finished (device clock); total_ms: the run.
  * ---------------------------------------------------------------------- */
 typedef struct tb_ensemble tb_ensemble;

@@ -204,6 +204,22 @@ class Plan:
             out[buf.value.decode()] = (ms.value, cnt.value)
         return out
 
+    def variant(self):
+        """(tau-solve partitions, 3D x-pass rows per CTA or 0): the plan's kernel shapes."""
+        a, b = c_int(), c_int()
+        check(lib.tb_plan_get_variant(self.ptr, byref(a), byref(b)), self.ctx)
+        return a.value, b.value
+
+    def set_variant(self, tau_parts: int = 0, xrows: int = 0) -> None:
+        check(lib.tb_plan_set_variant(self.ptr, int(tau_parts), int(xrows)), self.ctx)
+
+    def tune(self, dt: float, trial_steps: int = 4):
+        """Time every feasible kernel-shape combination on trial steps from the
+        current state (restored afterwards) and keep the fastest."""
+        a, b = c_int(), c_int()
+        check(lib.tb_plan_tune(self.ptr, float(dt), int(trial_steps), byref(a), byref(b)), self.ctx)
+        return a.value, b.value
+
     def kernels_per_step(self) -> int:
         n = c_int()
         check(lib.tb_kernels_per_step(self.ptr, byref(n)), self.ctx)

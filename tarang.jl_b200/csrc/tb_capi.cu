@@ -581,6 +581,41 @@ void tb::plan_launch_steps(tb_plan* P, double dt, int nsteps, cudaStream_t s, in
   }
 }
 
+bool tb::plan_tau_parts_ok(const tb_plan* P, int parts) {
+  if (parts != 1 && parts != kTauParts) return false;
+  for (int sy = 0; sy < P->nsys; ++sy)
+    if (tau_solve_smem_bytes(P->sys[sy].npad, parts) > 227 * 1024) return false;
+  return true;
+}
+
+void tb::plan_set_variant(tb_plan* P, int tau_parts, int xrows) {
+  bool changed = false;
+  if (tau_parts > 0) {
+    TB_REQUIRE(plan_tau_parts_ok(P, tau_parts), TB_ENOTSUPPORTED, "tau solve partitions must be 1 or 4 and fit");
+    for (int sy = 0; sy < P->nsys; ++sy) {
+      TauSystem& S = P->sys[sy];
+      if (S.tau_parts == tau_parts) continue;
+      TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+      S.tau_parts = tau_parts;
+      S.factors.clear();  // record layouts differ between the two forms
+      const size_t ys = tau_solve_scratch_doubles(P->Nk, S.npad, tau_parts) * sizeof(double);
+      if (ys > P->solve_scratch.bytes) P->solve_scratch.alloc(ys);
+      changed = true;
+    }
+  }
+  if (xrows > 0 && xrows != P->xrows) {
+    TB_REQUIRE(P->ndim == 3 && rbc3d_xrows_ok(P, xrows), TB_ENOTSUPPORTED, "x-pass rows must be 1, 2 or 4 and fit");
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+    P->xrows = xrows;
+    changed = true;
+  }
+  if (changed) {
+    drop_graph(P);
+    if (P->multi.exec) cudaGraphExecDestroy(P->multi.exec);
+    P->multi = StepGraph{};
+  }
+}
+
 void tb::plan_prepare(tb_plan* P, double dt, int graph_steps) {
   TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
   const int kind = plan_next_kind(P);
@@ -1141,6 +1176,67 @@ tb_status tb_tau_layout_query(int Nz, double Lx, double Lz, int cls, int* info4)
     g_err = e.msg;
     return e.code;
   }
+}
+
+tb_status tb_plan_set_variant(tb_plan* P, int tau_parts, int xrows) {
+  if (!P) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
+    plan_set_variant(P, tau_parts, xrows);
+  });
+}
+
+tb_status tb_plan_get_variant(const tb_plan* P, int* tau_parts, int* xrows) {
+  if (!P) return TB_EINVAL;
+  if (tau_parts) *tau_parts = P->sys[0].tau_parts;
+  if (xrows) *xrows = P->ndim == 3 ? P->xrows : 0;
+  return TB_OK;
+}
+
+tb_status tb_plan_tune(tb_plan* P, double dt, int trial_steps, int* tau_parts, int* xrows) {
+  if (!P || trial_steps < 1) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_REQUIRE(dt > 0 && std::isfinite(dt), TB_EINVAL, "dt must be positive and finite");
+    TB_REQUIRE(!P->profiling, TB_ESTATE, "tuning runs without profiling");
+    TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
+    PlanSnapshot snap;
+    plan_snapshot(P, &snap);
+    std::vector<int> parts_c, rows_c;
+    for (int p : {kTauParts, 1})
+      if (plan_tau_parts_ok(P, p)) parts_c.push_back(p);
+    if (P->ndim == 3) {
+      for (int r : {1, 2, 4})
+        if (rbc3d_xrows_ok(P, r)) rows_c.push_back(r);
+    } else {
+      rows_c.push_back(0);
+    }
+    float best = 1e30f;
+    int bp = P->sys[0].tau_parts, br = P->ndim == 3 ? P->xrows : 0;
+    for (int pc : parts_c)
+      for (int rc : rows_c) {
+        plan_set_variant(P, pc, rc);
+        // first launches factor the tau systems and capture the graphs
+        plan_launch_steps(P, dt, std::min(trial_steps, 2), P->st, 1);
+        TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+        plan_restore(P, snap);
+        TB_CUDA_TRY(cudaEventRecord(P->ev0, P->st));
+        plan_launch_steps(P, dt, trial_steps, P->st, 1);
+        TB_CUDA_TRY(cudaEventRecord(P->ev1, P->st));
+        TB_CUDA_TRY(cudaEventSynchronize(P->ev1));
+        float ms = 0.f;
+        TB_CUDA_TRY(cudaEventElapsedTime(&ms, P->ev0, P->ev1));
+        plan_restore(P, snap);
+        if (ms < best) {
+          best = ms;
+          bp = pc;
+          br = rc;
+        }
+      }
+    plan_set_variant(P, bp, br);
+    plan_restore(P, snap);
+    if (tau_parts) *tau_parts = bp;
+    if (xrows) *xrows = br;
+  });
 }
 
 tb_status tb_kernels_per_step(const tb_plan* P, int* n) {

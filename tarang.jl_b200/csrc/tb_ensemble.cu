@@ -159,29 +159,43 @@ tb_status tb_ensemble_tune(tb_ensemble* E, const double* dt, int trial_steps, in
     auto restore = [&] {
       for (int i = 0; i < n; ++i) plan_restore(E->members[i], snaps[i]);
     };
-    // warm-up: factors and graphs of every member at this dt
-    run(E, dt, std::min(trial_steps, 2), std::min(n, 8), 1, nullptr, nullptr);
-    restore();
+    // tau-solve partitioning of the members: the partitioned solve has the
+    // shortest latency for one plan, the one-warp solve the least work when
+    // many plans share the GPU; both are tried when every member can run them
+    std::vector<int> cand_p;
+    for (int pc : {kTauParts, 1}) {
+      bool ok = true;
+      for (auto* m : E->members) ok = ok && plan_tau_parts_ok(m, pc);
+      if (ok) cand_p.push_back(pc);
+    }
     const int cand_s[] = {1, 2, 4, 8, 16, 32};
     const int cand_g[] = {1, 4, 16};
     float best = 1e30f;
-    int bs = E->streams, bg = E->graph_steps;
-    for (int g : cand_g) {
-      if (g > trial_steps) continue;
-      for (int s : cand_s) {
-        if (s > n || s > kMaxWorkerStreams) continue;
-        float tot = 0.f;
-        run(E, dt, trial_steps, s, g, nullptr, nullptr);  // captures this graph size
-        restore();
-        run(E, dt, trial_steps, s, g, nullptr, &tot);
-        restore();
-        if (tot < best) {
-          best = tot;
-          bs = s;
-          bg = g;
+    int bs = E->streams, bg = E->graph_steps, bp = E->members[0]->sys[0].tau_parts;
+    for (int pc : cand_p) {
+      for (auto* m : E->members) plan_set_variant(m, pc, 0);
+      // warm-up: factors and graphs of every member at this dt
+      run(E, dt, std::min(trial_steps, 2), std::min(n, 8), 1, nullptr, nullptr);
+      restore();
+      for (int g : cand_g) {
+        if (g > trial_steps) continue;
+        for (int s : cand_s) {
+          if (s > n || s > kMaxWorkerStreams) continue;
+          float tot = 0.f;
+          run(E, dt, trial_steps, s, g, nullptr, nullptr);  // captures this graph size
+          restore();
+          run(E, dt, trial_steps, s, g, nullptr, &tot);
+          restore();
+          if (tot < best) {
+            best = tot;
+            bs = s;
+            bg = g;
+            bp = pc;
+          }
         }
       }
     }
+    for (auto* m : E->members) plan_set_variant(m, bp, 0);
     E->streams = bs;
     E->graph_steps = bg;
     if (streams) *streams = bs;

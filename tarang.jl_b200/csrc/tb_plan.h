@@ -134,6 +134,7 @@ struct tb_plan {
   // transform, one complex plane of scratch
   FftPlan fpNy{};
   DevBuf ptwNy, tmp3;
+  int xrows = 1;  // padded y rows per x-pass CTA (a tuned shape)
   // transform constants
   DevBuf bwd, fwd, s3, twM, twN, ptwM;
   // parity halves of the Chebyshev matrices (H = ceil(Nz/2) rows/cols)
@@ -237,6 +238,12 @@ void timed(tb_plan* P, const char* name, F&& fn) {
 // of the stage L X for the Hermitian projection of the kx = 0 and Nyquist planes.
 void rbc3d_setup(tb_plan* P);
 void rbc3d_enqueue_rhs(tb_plan* P, const double2* Xin, double2* out4);
+bool rbc3d_xrows_ok(const tb_plan* P, int rows);
+// Tunable kernel shapes of a plan: tau-solve partitions (1 or kTauParts, for
+// every tau system) and, in 3D, x-pass rows per CTA (1, 2, 4).  Changing one
+// drops the plan's factors and step graphs (rebuilt on the next step).
+bool plan_tau_parts_ok(const tb_plan* P, int parts);
+void plan_set_variant(tb_plan* P, int tau_parts, int xrows);
 void rbc3d_lx_project(tb_plan* P, double2* LX, double beta);
 size_t rbc3d_device_bytes(const tb_plan* P);
 // 3D transforms between grid (Nz, Ny, Nx) real and coefficients (Nz, Ny, Nx/2+1)

@@ -569,18 +569,34 @@ constexpr int kFixedLen = 384;
 
 template <class C>
 void set_limits(int bytes) {
-  constexpr int RR = XRows<C>::value;
-  const void* fns[] = {(const void*)k3_yinv<C, 0>,      (const void*)k3_yinv<C, kFixedLen>,
-                       (const void*)k3_xpass<C, RR, 0>, (const void*)k3_xpass<C, RR, kFixedLen>,
-                       (const void*)k3_yfwd<C, 0>,      (const void*)k3_yfwd<C, kFixedLen>};
+  const void* fns[] = {(const void*)k3_yinv<C, 0>,         (const void*)k3_yinv<C, kFixedLen>,
+                       (const void*)k3_xpass<C, 1, 0>,    (const void*)k3_xpass<C, 1, kFixedLen>,
+                       (const void*)k3_xpass<C, 2, 0>,    (const void*)k3_xpass<C, 2, kFixedLen>,
+                       (const void*)k3_xpass<C, 4, 0>,    (const void*)k3_xpass<C, 4, kFixedLen>,
+                       (const void*)k3_yfwd<C, 0>,         (const void*)k3_yfwd<C, kFixedLen>};
   for (const void* fn : fns) TB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+}
+
+// x-pass rows per CTA that fit (shared memory, padded Ny divisible).
+template <class C>
+bool xrows_ok(const tb_plan* P, const R3Args& a, int rr) {
+  if (rr != 1 && rr != 2 && rr != 4) return false;
+  if (P->My % rr) return false;
+  const size_t Ms = (size_t)F::pad_swz<C>(a.Mx);
+  return (16 * (size_t)rr * Ms + (size_t)a.nptx) * sizeof(C) <= 227 * 1024;
+}
+
+template <class C, int RR>
+void launch_xpass(tb_plan* P, const R3Args& a, cudaStream_t st) {
+  auto kern = (P->M == kFixedLen) ? k3_xpass<C, RR, kFixedLen> : k3_xpass<C, RR, 0>;
+  kern<<<dim3(P->My / RR, P->Nz), kR3Threads, xpass_smem<C, RR>(a), st>>>(a, P->mix3.as<C>(), P->ptwX.as<C>(),
+                                                                          P->pm3.as<C>());
 }
 
 inline int pad16(int k) { return (k + 15) / 16 * 16; }
 
 template <class C>
 void enqueue_rhs_t(tb_plan* P, const double2* Xin, double2* out4) {
-  constexpr int RR = XRows<C>::value;
   const R3Args a = args_of(P);
   const int N = P->Nz, H = N / 2;
   const size_t plane = P->plane, hplane = (size_t)H * P->Nk;
@@ -615,10 +631,14 @@ void enqueue_rhs_t(tb_plan* P, const double2* Xin, double2* out4) {
     auto kern = fy ? k3_yinv<C, kFixedLen> : k3_yinv<C, 0>;
     kern<<<dim3(P->Kx, H), kR3Threads, yinv_smem<C>(a), P->st>>>(a, G, P->ptwY.as<C>(), P->mix3.as<C>());
   });
+  (void)fx;
   timed(P, "rhs3_xpass", [&] {
-    auto kern = fx ? k3_xpass<C, RR, kFixedLen> : k3_xpass<C, RR, 0>;
-    kern<<<dim3(P->My / RR, N), kR3Threads, xpass_smem<C, RR>(a), P->st>>>(a, P->mix3.as<C>(), P->ptwX.as<C>(),
-                                                                            P->pm3.as<C>());
+    if (P->xrows == 4)
+      launch_xpass<C, 4>(P, a, P->st);
+    else if (P->xrows == 2)
+      launch_xpass<C, 2>(P, a, P->st);
+    else
+      launch_xpass<C, 1>(P, a, P->st);
   });
   timed(P, "rhs3_yfwd", [&] {
     auto kern = fy ? k3_yfwd<C, kFixedLen> : k3_yfwd<C, 0>;
@@ -654,9 +674,9 @@ void setup_t(tb_plan* P) {
   const R3Args a = args_of(P);
   TB_REQUIRE(P->My % RR == 0, TB_ENOTSUPPORTED, "padded Ny must be a multiple of the x-pass rows");
   const size_t lim = 227 * 1024;
-  const size_t xs = xpass_smem<C, RR>(a);
-  TB_REQUIRE(yinv_smem<C>(a) <= lim && xs <= lim && yfwd_smem<C>(a) <= lim, TB_ENOTSUPPORTED,
+  TB_REQUIRE(yinv_smem<C>(a) <= lim && xrows_ok<C>(P, a, RR) && yfwd_smem<C>(a) <= lim, TB_ENOTSUPPORTED,
              "Nx or Ny too large for the 3D transform kernels");
+  P->xrows = RR;
   set_limits<C>((int)lim);
   const size_t plane = P->plane, H = (size_t)P->Nz / 2;
   P->Xc.alloc(4 * plane * sizeof(C));
@@ -687,6 +707,11 @@ void rbc3d_setup(tb_plan* P) {
     setup_t<float2>(P);
   else
     setup_t<double2>(P);
+}
+
+bool rbc3d_xrows_ok(const tb_plan* P, int rows) {
+  const R3Args a = args_of(P);
+  return P->mixed ? xrows_ok<float2>(P, a, rows) : xrows_ok<double2>(P, a, rows);
 }
 
 void rbc3d_enqueue_rhs(tb_plan* P, const double2* Xin, double2* out4) {

@@ -623,8 +623,8 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
     constexpr int NS3 = 6;            // H ring: NS3 slots of R rows
     constexpr int SLOT3 = R * HREC;
     static_assert(NS3 * SLOT3 <= NS * STAGE, "H ring fits the warp's ring");
-    static_assert(R % 2 == 0 && 32 == 2 * NL, "B3 splits the rows of a stage between the two lane halves");
-    const int half = lane / NL;
+    constexpr int LG = 32 / NL;  // lane groups: each takes every LG-th row of a stage
+    const int grp = lane / NL;
     auto issue_h = [&](int s) {
       if (s < nst) {
         double* dst = ring + (size_t)(s % NS3) * SLOT3;
@@ -639,10 +639,11 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
       cp_async_wait<NS3 - 1>();
       __syncwarp();
       const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NS3) * SLOT3 + (size_t)slot * kHRec);
-      // no recurrence here: the two lane halves take alternate rows
+      // no recurrence here: the lane groups take interleaved rows
 #pragma unroll
-      for (int q = 0; q < R / 2; ++q) {
-        const int u = 2 * q + half;
+      for (int q = 0; q < (R + LG - 1) / LG; ++q) {
+        const int u = q * LG + grp;
+        if (u >= R) break;
         double2 hv[HV];
 #pragma unroll
         for (int v = 0; v < HV; ++v) hv[v] = st[u * (HREC / 2) + v];

@@ -1,0 +1,77 @@
+"""Tunable kernel shapes (tau-solve partitions, 3D x-pass rows per CTA) and
+the tuners that choose them: every shape gives the same solution, and tuning
+leaves the state where it was."""
+import numpy as np
+import pytest
+
+from oracle.tarang_oracle import RBCParams, forward_2d, rbc_initial_b, rel_l2, run_rbc
+from oracle.tarang_oracle import RBC3D, TABLEAUS, RBC3Params, rbc3_initial_b
+
+pytestmark = pytest.mark.gpu
+
+
+def test_tau_partitions_give_the_oracle_solution(tb):
+    p = RBCParams(Nx=48, Nz=24, Lx=4.0, Lz=1.0, Ra=1e8)
+    sim = run_rbc(p, "RK443", 0.01, 4, seed=42)
+    for parts in (4, 1):
+        dom = tb.ChannelDomain(48, 24, Lx=4.0, Lz=1.0)
+        plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 1)
+        plan.set_variant(tau_parts=parts)
+        assert plan.variant()[0] == parts
+        plan.set_state(0, forward_2d(rbc_initial_b(p, 42)))
+        plan.step(0.01, 4)
+        for f, want in ((0, sim.b), (1, sim.ux), (2, sim.uz)):
+            assert rel_l2(plan.get_state(f), want) < 1e-10
+
+
+def test_xpass_rows_and_tau_partitions_agree_in_3d(tb):
+    p = RBC3Params(Nx=24, Ny=24, Nz=12, Lx=4.0, Ly=4.0, Ra=1e6)
+    sim = RBC3D(p)
+    sim.set_b_grid(rbc3_initial_b(p, 42, amp=1e-2))
+    for _ in range(2):
+        sim.step_rk(0.01, TABLEAUS["RK222"])
+    ref = None
+    for parts, rows in ((4, 2), (1, 1), (1, 4), (4, 1)):
+        plan = tb.Plan3D(24, 24, 12, p.kappa, p.nu, 0, 4.0, 4.0, 1.0, precision=tb._lib.TB_PREC_MIXED)
+        plan.set_variant(tau_parts=parts, xrows=rows)
+        assert plan.variant() == (parts, rows)
+        plan.set_state(0, plan.forward(rbc3_initial_b(p, 42, amp=1e-2)))
+        plan.step(0.01, 2)
+        ux = plan.get_state(1)
+        assert rel_l2(ux, sim.ux) < 1e-6
+        if ref is None:
+            ref = ux
+        else:
+            assert rel_l2(ux, ref) < 1e-12  # the same arithmetic in every shape
+
+
+def test_plan_tune_keeps_state_and_picks_a_feasible_shape(tb):
+    p = RBCParams(Nx=64, Nz=32, Lx=4.0, Lz=1.0, Ra=1e6)
+    dom = tb.ChannelDomain(64, 32, Lx=4.0, Lz=1.0)
+    plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 0)
+    plan.set_state(0, forward_2d(rbc_initial_b(p, 42)))
+    plan.step(0.02, 2)
+    before = [plan.get_state(f) for f in (0, 1, 2)]
+    parts, rows = plan.tune(0.02, trial_steps=3)
+    assert parts in (1, 4) and rows == 0 and plan.variant()[0] == parts
+    for f, b in zip((0, 1, 2), before):
+        assert np.array_equal(plan.get_state(f), b)
+    plan.step(0.02, 2)  # steps on with the chosen shape
+    assert np.isfinite(plan.get_state(2)).all()
+
+
+def test_ensemble_tune_applies_one_partitioning_to_all_members(tb):
+    plans = []
+    for Nx, Nz in ((64, 16), (96, 24), (128, 32)):
+        p = RBCParams(Nx=Nx, Nz=Nz, Ra=1e6)
+        dom = tb.ChannelDomain(Nx, Nz, Lx=4.0, Lz=1.0)
+        pl = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 0)
+        pl.set_state(0, forward_2d(rbc_initial_b(p, 7)))
+        plans.append(pl)
+    ens = tb.Ensemble(plans)
+    before = [pl.get_state(0) for pl in plans]
+    ens.tune(0.02, trial_steps=2)
+    parts = {pl.variant()[0] for pl in plans}
+    assert len(parts) == 1 and parts <= {1, 4}
+    for pl, b in zip(plans, before):
+        assert np.array_equal(pl.get_state(0), b)
