@@ -298,6 +298,82 @@ __device__ C* fft_batch_ct(C* a, C* b, int nb, int stride, const C* __restrict__
   return stages_ct<N, 0, 1>(a, b, pt, sign, nb, stride);
 }
 
+// ---------------------------------------------------------------------------
+// Length-384 transforms in two register passes (384 = 16 x 24, four-step):
+// pass 1 takes, per (transform, n2 < 24), the 16 inputs x[24 n1 + n2] into
+// registers, a 16-point DFT (4 x 4 in registers), the twiddles w^(n2 k1), and
+// stores row k1 of a [16][25] scratch; pass 2 takes, per (transform, k1 < 16),
+// scratch row k1, a 24-point DFT (8 x 3 in registers) and stores X[k1 + 16 k2].
+// Two shared-memory round trips per element instead of the four of the
+// Stockham plan (8, 8, 2, 3).  Buffers in natural order (no swizzle), at least
+// kLen384Buf elements apart.  w: exp(-2 pi i k / 384), k < 384.
+// ---------------------------------------------------------------------------
+constexpr int kLen384Buf = 400;  // 16 rows of 25 (padding spreads the row starts over the banks)
+
+template <class C>
+__device__ __forceinline__ C tw384(const C* __restrict__ w, int k, int sign) {
+  C t = w[k];
+  if (sign > 0) t.y = -t.y;
+  return t;
+}
+
+// In-register DFT of length R1 R2 (natural order in and out); internal
+// twiddles w_{R1 R2}^j = w_384^(j WS) with WS = 384 / (R1 R2).
+template <int R1, int R2, int WS, class C>
+__device__ __forceinline__ void dft_reg(C (&x)[R1 * R2], const C* __restrict__ w, int sign) {
+  C y[R1 * R2];
+#pragma unroll
+  for (int n2 = 0; n2 < R2; ++n2) {
+    C a[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) a[n1] = x[R2 * n1 + n2];
+    dft_small<R1>(a, sign);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) y[k1 * R2 + n2] = (n2 * k1 == 0) ? a[k1] : mul(a[k1], tw384(w, n2 * k1 * WS, sign));
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < R1; ++k1) {
+    C b[R2];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) b[n2] = y[k1 * R2 + n2];
+    dft_small<R2>(b, sign);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) x[k1 + R1 * k2] = b[k2];
+  }
+}
+
+// nb length-384 transforms, buffer q at a + q * stride (stride >= kLen384Buf),
+// b the scratch set; results in a (returned).  sign -1 forward, +1 inverse,
+// unnormalised.
+template <class C>
+__device__ C* fft384_batch(C* a, C* b, int nb, int stride, const C* __restrict__ w, int sign) {
+  for (int t = threadIdx.x; t < nb * 24; t += blockDim.x) {
+    const int q = t / 24, n2 = t - 24 * q;
+    const C* src = a + (size_t)q * stride;
+    C* dst = b + (size_t)q * stride;
+    C v[16];
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) v[n1] = src[24 * n1 + n2];
+    dft_reg<4, 4, 24>(v, w, sign);
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) dst[k1 * 25 + n2] = (k1 == 0 || n2 == 0) ? v[k1] : mul(v[k1], tw384(w, n2 * k1, sign));
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nb * 16; t += blockDim.x) {
+    const int q = t / 16, k1 = t - 16 * q;
+    const C* src = b + (size_t)q * stride + k1 * 25;
+    C* dst = a + (size_t)q * stride;
+    C v[24];
+#pragma unroll
+    for (int n2 = 0; n2 < 24; ++n2) v[n2] = src[n2];
+    dft_reg<8, 3, 16>(v, w, sign);
+#pragma unroll
+    for (int k2 = 0; k2 < 24; ++k2) dst[k1 + 16 * k2] = v[k2];
+  }
+  __syncthreads();
+  return a;
+}
+
 // Batched form: nb transforms of length fp.n, buffer q at a + q * stride (and
 // b + q * stride), all butterflies of a pass spread over the CTA (typed swizzle).
 template <int R, bool SW, class C>

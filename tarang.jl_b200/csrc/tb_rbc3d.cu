@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "tb_fft.cuh"
@@ -86,12 +87,33 @@ __global__ void __launch_bounds__(256) k3_prep(R3Args a, const double2* __restri
   Xc[3 * plane + i] = F::mk<C>((T)uz.x, (T)uz.y);
 }
 
-// Batched FFT of nb buffers: the compile-time plan when the length is one of the
-// specialised sizes (N > 0), else the runtime plan.
+// The FP32 kernels at the 384-point padded length run the two-pass register
+// transform (natural-order buffers, kLen384Buf apart, twiddle table w^k for
+// k < 384); other compiled lengths the Stockham plan with constant strides,
+// the rest the runtime plan (both on swizzled buffers, per-pass twiddles).
+template <class C, int M>
+constexpr bool kReg384 = std::is_same<C, float2>::value && M == 384;
+
+template <class C, int M>
+__device__ __forceinline__ int bidx(int i) {
+  if constexpr (kReg384<C, M>)
+    return i;
+  else
+    return F::sidx<C>(i);
+}
+
+template <class C, int M>
+__host__ __device__ constexpr int buf_len(int m) {
+  return kReg384<C, M> ? F::kLen384Buf : F::pad_swz<C>(m);
+}
+
+// Batched FFT of nb buffers.
 template <int N, class C>
 __device__ __forceinline__ C* fftb(C* a, C* b, int nb, int stride, const FftPlan& fp, const C* __restrict__ pt,
                                    int sign) {
-  if constexpr (N > 0)
+  if constexpr (kReg384<C, N>)
+    return F::fft384_batch(a, b, nb, stride, pt, sign);
+  else if constexpr (N > 0)
     return F::fft_batch_ct<N>(a, b, nb, stride, pt, sign);
   else
     return F::fft_batch<true>(a, b, nb, stride, fp, pt, sign);
@@ -107,7 +129,7 @@ __global__ void __launch_bounds__(kR3Threads) k3_yinv(R3Args a, const C* __restr
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
   const int Ny = a.Ny, My = MY > 0 ? MY : a.My, ix = blockIdx.x, j = blockIdx.y;
-  const int Ms = F::pad_swz<C>(My);
+  const int Ms = buf_len<C, MY>(My);
   C* stg = sm;                    // [16][Ny]
   C* A = stg + 16 * Ny;           // [12][Ms]
   C* B = A + 12 * Ms;             // [12][Ms]
@@ -133,7 +155,7 @@ __global__ void __launch_bounds__(kR3Threads) k3_yinv(R3Args a, const C* __restr
     };
     for (int t = threadIdx.x; t < 12 * gap; t += blockDim.x) {
       const int q = t / gap, y = hy + 1 + (t - q * gap);
-      A[(size_t)q * Ms + F::sidx<C>(y)] = F::mk<C>((T)0, (T)0);
+      A[(size_t)q * Ms + bidx<C, MY>(y)] = F::mk<C>((T)0, (T)0);
     }
     for (int t = threadIdx.x; t < 12 * Ny; t += blockDim.x) {
       const int q = t / Ny, iy = t - q * Ny;
@@ -153,20 +175,20 @@ __global__ void __launch_bounds__(kR3Threads) k3_yinv(R3Args a, const C* __restr
       v = F::scale(v, xs);
       C* col = A + (size_t)q * Ms;
       if (iy < hy) {
-        col[F::sidx<C>(iy)] = v;
+        col[bidx<C, MY>(iy)] = v;
       } else if (iy == hy) {
         const C h = F::scale(v, (T)0.5);
-        col[F::sidx<C>(hy)] = h;
-        col[F::sidx<C>(My - hy)] = h;
+        col[bidx<C, MY>(hy)] = h;
+        col[bidx<C, MY>(My - hy)] = h;
       } else {
-        col[F::sidx<C>(My - Ny + iy)] = v;
+        col[bidx<C, MY>(My - Ny + iy)] = v;
       }
     }
     __syncthreads();
     C* R = fftb<MY>(A, B, 12, Ms, a.fpy, pt, +1);
     for (int t = threadIdx.x; t < 12 * My; t += blockDim.x) {
       const int q = t / My, y = t - q * My;
-      mix[(((size_t)zl * 12 + q) * a.Kx + ix) * My + y] = R[(size_t)q * Ms + F::sidx<C>(y)];
+      mix[(((size_t)zl * 12 + q) * a.Kx + ix) * My + y] = R[(size_t)q * Ms + bidx<C, MY>(y)];
     }
     __syncthreads();
   }
@@ -184,7 +206,7 @@ __global__ void __launch_bounds__(kR3Threads) k3_xpass(R3Args a, const C* __rest
   C* sm = reinterpret_cast<C*>(sm_raw);
   const int Mx = MX > 0 ? MX : a.Mx, Kx = a.Kx, My = a.My, hN = a.Nx / 2;
   const int y0 = blockIdx.x * RR, z = blockIdx.y;
-  const int Ms = F::pad_swz<C>(Mx);
+  const int Ms = buf_len<C, MX>(Mx);
   constexpr int NB = 8 * RR;
   C* Z = sm;              // [NB][Ms]
   C* S = Z + NB * Ms;     // [NB][Ms]
@@ -220,15 +242,15 @@ __global__ void __launch_bounds__(kR3Threads) k3_xpass(R3Args a, const C* __rest
     const C B = (k < Kx && p < 7) ? row[(size_t)(2 * p + 1) * Kx + k] : F::mk<C>((T)0, (T)0);
     C* dst = Z + (size_t)(r * 8 + p) * Ms;
     // spectrum of a + i b: A + i B at k, conj(A) + i conj(B) at Mx - k
-    dst[F::sidx<C>(k)] = F::mk<C>(A.x - B.y, A.y + B.x);
-    if (k > 0 && k < Mx / 2) dst[F::sidx<C>(Mx - k)] = F::mk<C>(A.x + B.y, -A.y + B.x);
+    dst[bidx<C, MX>(k)] = F::mk<C>(A.x - B.y, A.y + B.x);
+    if (k > 0 && k < Mx / 2) dst[bidx<C, MX>(Mx - k)] = F::mk<C>(A.x + B.y, -A.y + B.x);
   }
   __syncthreads();
   C* Rg = fftb<MX>(Z, S, NB, Ms, a.fpx, pt, +1);
   C* W = (Rg == Z) ? S : Z;
   for (int t = threadIdx.x; t < RR * Mx; t += blockDim.x) {
     const int r = t / Mx, x = t - r * Mx;
-    const int i = F::sidx<C>(x);
+    const int i = bidx<C, MX>(x);
     const C* g = Rg + (size_t)r * 8 * Ms;
     const C z0 = g[i], z1 = g[Ms + i], z2 = g[2 * Ms + i], z3 = g[3 * Ms + i];
     const C z4 = g[4 * Ms + i], z5 = g[5 * Ms + i], z6 = g[6 * Ms + i], z7 = g[7 * Ms + i];
@@ -246,7 +268,7 @@ __global__ void __launch_bounds__(kR3Threads) k3_xpass(R3Args a, const C* __rest
     const int r = t % RR, rest = t / RR;
     const int k = rest % Kx, h = rest / Kx;
     const C* buf = Fq + (size_t)(2 * r + h) * Ms;
-    const C c = buf[F::sidx<C>(k)], cm = buf[F::sidx<C>((Mx - k) % Mx)];
+    const C c = buf[bidx<C, MX>(k)], cm = buf[bidx<C, MX>((Mx - k) % Mx)];
     // first: (c + conj(cm))/2, second: (c - conj(cm))/(2i)
     C o1 = F::mk<C>((T)0.5 * (c.x + cm.x), (T)0.5 * (c.y - cm.y));
     C o2 = F::mk<C>((T)0.5 * (c.y + cm.y), (T)-0.5 * (c.x - cm.x));
@@ -272,14 +294,14 @@ __global__ void __launch_bounds__(kR3Threads) k3_yfwd(R3Args a, const C* __restr
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
   const int Ny = a.Ny, My = MY > 0 ? MY : a.My, ix = blockIdx.x, z = blockIdx.y;
-  const int Ms = F::pad_swz<C>(My);
+  const int Ms = buf_len<C, MY>(My);
   C* A = sm;
   C* B = A + 4 * Ms;
   C* pt = B + 4 * Ms;
   for (int t = threadIdx.x; t < a.npty; t += blockDim.x) pt[t] = pty[t];
   for (int t = threadIdx.x; t < 4 * My; t += blockDim.x) {
     const int f = t / My, y = t - f * My;
-    A[(size_t)f * Ms + F::sidx<C>(y)] = pm[(((size_t)z * 4 + f) * a.Kx + ix) * My + y];
+    A[(size_t)f * Ms + bidx<C, MY>(y)] = pm[(((size_t)z * 4 + f) * a.Kx + ix) * My + y];
   }
   __syncthreads();
   const C* Q = fftb<MY>(A, B, 4, Ms, a.fpy, pt, -1);
@@ -292,11 +314,11 @@ __global__ void __launch_bounds__(kR3Threads) k3_yfwd(R3Args a, const C* __restr
       const C* col = Q + (size_t)f * Ms;
       C r;
       if (2 * iy < Ny) {
-        r = col[F::sidx<C>(iy)];
+        r = col[bidx<C, MY>(iy)];
       } else if (2 * iy == Ny) {
-        r = F::add(col[F::sidx<C>(Ny / 2)], col[F::sidx<C>(My - Ny / 2)]);
+        r = F::add(col[bidx<C, MY>(Ny / 2)], col[bidx<C, MY>(My - Ny / 2)]);
       } else {
-        r = col[F::sidx<C>(My - Ny + iy)];
+        r = col[bidx<C, MY>(My - Ny + iy)];
       }
       v[f] = make_double2(sc * (double)r.x, sc * (double)r.y);
     }
@@ -530,24 +552,31 @@ R3Args args_of(const tb_plan* P) {
   a.ky0 = P->k0y;
   a.fpx = P->fpM;
   a.fpy = P->fpMy;
-  a.nptx = F::pass_twiddle_count(P->fpM);
-  a.npty = F::pass_twiddle_count(P->fpMy);
+  // the FP32 384-point transform reads the full table exp(-2 pi i k/384)
+  a.nptx = (P->mixed && P->M == 384) ? 384 : F::pass_twiddle_count(P->fpM);
+  a.npty = (P->mixed && P->My == 384) ? 384 : F::pass_twiddle_count(P->fpMy);
   return a;
+}
+
+// Buffer length of the transform kernels for padded length m (see buf_len).
+template <class C>
+size_t buf_len_host(int m) {
+  return (std::is_same<C, float2>::value && m == 384) ? (size_t)F::kLen384Buf : (size_t)F::pad_swz<C>(m);
 }
 
 template <class C>
 size_t yinv_smem(const R3Args& a) {
-  const size_t Ms = (size_t)F::pad_swz<C>(a.My);
+  const size_t Ms = buf_len_host<C>(a.My);
   return (16 * (size_t)a.Ny + 24 * Ms + (size_t)a.npty) * sizeof(C);
 }
 template <class C, int RR>
 size_t xpass_smem(const R3Args& a) {
-  const size_t Ms = (size_t)F::pad_swz<C>(a.Mx);
+  const size_t Ms = buf_len_host<C>(a.Mx);
   return (16 * RR * Ms + (size_t)a.nptx) * sizeof(C);
 }
 template <class C>
 size_t yfwd_smem(const R3Args& a) {
-  const size_t Ms = (size_t)F::pad_swz<C>(a.My);
+  const size_t Ms = buf_len_host<C>(a.My);
   return (8 * Ms + (size_t)a.npty) * sizeof(C);
 }
 
@@ -582,7 +611,7 @@ template <class C>
 bool xrows_ok(const tb_plan* P, const R3Args& a, int rr) {
   if (rr != 1 && rr != 2 && rr != 4) return false;
   if (P->My % rr) return false;
-  const size_t Ms = (size_t)F::pad_swz<C>(a.Mx);
+  const size_t Ms = buf_len_host<C>(a.Mx);
   return (16 * (size_t)rr * Ms + (size_t)a.nptx) * sizeof(C) <= 227 * 1024;
 }
 
@@ -685,8 +714,20 @@ void setup_t(tb_plan* P) {
   P->mix3.alloc(12 * slab * sizeof(C));
   P->pm3.alloc(4 * slab * sizeof(C));
   P->H3.alloc(4 * plane * sizeof(C));
-  upload(P->ptwX, pass_twiddles_t<C>(P->fpM));
-  upload(P->ptwY, pass_twiddles_t<C>(P->fpMy));
+  auto table = [&](const FftPlan& fp) {
+    if (std::is_same<C, float2>::value && fp.n == 384) {
+      std::vector<C> t(384);
+      const long double pi = 3.141592653589793238462643383279502884L;
+      for (int k = 0; k < 384; ++k) {
+        t[k].x = (decltype(t[k].x))cosl(-2.0L * pi * k / 384.0L);
+        t[k].y = (decltype(t[k].y))sinl(-2.0L * pi * k / 384.0L);
+      }
+      return t;
+    }
+    return pass_twiddles_t<C>(fp);
+  };
+  upload(P->ptwX, table(P->fpM));
+  upload(P->ptwY, table(P->fpMy));
 }
 
 }  // namespace
