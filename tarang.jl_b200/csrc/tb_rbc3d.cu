@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kR3Threads) k3_yinv(R3Args a, const C* __restr
 // Factors on the x grid (15 real, packed in pairs a + i b): 0 u_x, 1 u_y,
 // 2 u_z, 3..6 d_x f, 7..10 d_y f, 11..14 d_z f (f = b, u_x, u_y, u_z).
 template <class C, int RR, int MX>
-__global__ void __launch_bounds__(kR3Threads) k3_xpass(R3Args a, const C* __restrict__ mix, const C* __restrict__ ptx,
+__global__ void __launch_bounds__(RR == 4 ? 2 * kR3Threads : kR3Threads) k3_xpass(R3Args a, const C* __restrict__ mix, const C* __restrict__ ptx,
                                                         C* __restrict__ pm) {
   using T = typename F::Real<C>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -615,11 +615,15 @@ bool xrows_ok(const tb_plan* P, const R3Args& a, int rr) {
   return (16 * (size_t)rr * Ms + (size_t)a.nptx) * sizeof(C) <= 227 * 1024;
 }
 
+// Four rows per CTA run with 512 threads (one CTA per SM by shared memory):
+// the staged loads then take whole 32-byte sectors (4 consecutive y of FP32
+// complex) where one or two rows take a quarter or half of each.
 template <class C, int RR>
 void launch_xpass(tb_plan* P, const R3Args& a, cudaStream_t st) {
   auto kern = (P->M == kFixedLen) ? k3_xpass<C, RR, kFixedLen> : k3_xpass<C, RR, 0>;
-  kern<<<dim3(P->My / RR, P->Nz), kR3Threads, xpass_smem<C, RR>(a), st>>>(a, P->mix3.as<C>(), P->ptwX.as<C>(),
-                                                                          P->pm3.as<C>());
+  const int threads = RR == 4 ? 2 * kR3Threads : kR3Threads;
+  kern<<<dim3(P->My / RR, P->Nz), threads, xpass_smem<C, RR>(a), st>>>(a, P->mix3.as<C>(), P->ptwX.as<C>(),
+                                                                       P->pm3.as<C>());
 }
 
 inline int pad16(int k) { return (k + 15) / 16 * 16; }
