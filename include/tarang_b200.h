@@ -137,6 +137,19 @@ tb_status tb_tau_layout_query(int Nz, double Lx, double Lz, int cls, int* info4)
 /* Number of kernels one step launches (for launch accounting). */
 tb_status tb_kernels_per_step(const tb_plan* plan, int* n);
 
+/* Dynamic wall values of b (time- and space-dependent boundary conditions
+ * b(z=0) = f(x[, y], t), b(z=Lz) = g(x[, y], t)).  Replaces the per-stage BC
+ * refresh and ALG_F re-gather of the reference (step_subproblem_rk.jl:547-560,
+ * subproblem_rhs.jl:523-607): wall 0 is z = 0, wall 1 is z = Lz; value are the
+ * coefficients of the wall profile (the unnormalised transform of its grid
+ * values: complex Nx/2+1 in 2D, (Nx/2+1, Ny) kx fastest in 3D) at the plan's
+ * current time, rate their time derivative (NULL: constant), so each stage
+ * solve sees value + rate (t_stage - now); rk stage times are t_n + c_i dt,
+ * SBDF solves t_{n+1}.  A time dependence other than linear is followed by
+ * calling this between steps.  The first call replaces the descriptor's
+ * constant b_bottom / b_top (the other wall keeps its constant until set). */
+tb_status tb_set_wall_values(tb_plan* plan, int wall, const double* value, const double* rate, int where);
+
 /* Kernel shapes of a plan (the library's own autotuning; the reference tunes
  * FFTW plans instead, transform_fourier.jl plan cache):
  *   tau_parts  warps per 4-mode group in the tau solves: 4 (partitioned, the

@@ -325,6 +325,22 @@ class RBC2D:
         self.iteration = 0
         self._ms_hist: List[Tuple[np.ndarray, np.ndarray]] = []  # SBDF (MX, F) history, newest first
         self._ms_dt_prev: Optional[float] = None
+        # dynamic wall values of b: t -> (bottom, top) coefficient arrays (Nk,),
+        # re-gathered into the BC rows at every stage time (None: constant BCs)
+        self.wall_b = None
+
+    def _stage_algf(self, m: int, algf: np.ndarray, t: float) -> np.ndarray:
+        """ALG_F at time t: the b wall rows take the wall profile's coefficients
+        (per-stage refresh of step_subproblem_rk.jl:547-560, gather_alg_F!
+        subproblem_rhs.jl:523-607)."""
+        if self.wall_b is None:
+            return algf
+        bot, top = self.wall_b(t)
+        out = algf.copy()
+        r_bc = 4 * self.p.Nz
+        out[r_bc + 0] = bot[m]
+        out[r_bc + 3] = top[m]
+        return out
 
     # -- per-mode matrices (subproblem_matrix_build.jl:11-309) --------------
     def n_unknowns(self, m: int) -> int:
@@ -533,6 +549,7 @@ class RBC2D:
                 if abs(a_ii) < 1e-14:
                     x = self.mass_solve(m, rhs)
                 else:
+                    algf = self._stage_algf(m, algf, self.sim_time + dt * ts["c"][i])
                     rhs[bc] = dt * a_ii * algf[bc]
                     x = self._lhs_lu(m, 1.0, dt * a_ii).solve(rhs)
                 xs.append(x)
@@ -578,6 +595,7 @@ class RBC2D:
             for k in range(1, len(a)):
                 if abs(a[k]) >= 1e-14 and k - 1 < len(hist):
                     rhs -= a[k] * hist[k - 1][0][m]
+            algf = self._stage_algf(m, algf, self.sim_time + dt)
             rhs[bc] = bcoef[0] * algf[bc]
             xs.append(self._lhs_lu(m, a[0], bcoef[0]).solve(rhs))
         for m in range(Nk):
@@ -914,6 +932,8 @@ class RBC3D:
         self.tau = np.zeros((9, Ny, self.Kx), complex)
         self.sim_time = 0.0
         self.iteration = 0
+        # dynamic wall values of b: t -> (bottom, top) coefficient arrays (Ny, Kx)
+        self.wall_b = None
 
     def modes(self):
         return [(iy, ix) for iy in range(self.p.Ny) for ix in range(self.Kx)]
@@ -1097,6 +1117,11 @@ class RBC3D:
                 if abs(a_ii) < 1e-14:
                     xs[m] = self.mass_solve(rhs)
                 else:
+                    if self.wall_b is not None:
+                        bot, top = self.wall_b(self.sim_time + dt * ts["c"][i])
+                        algf = algf.copy()
+                        algf[5 * self.p.Nz + 0] = bot[m]
+                        algf[5 * self.p.Nz + 4] = top[m]
                     rhs[bc] = dt * a_ii * algf[bc]
                     xs[m] = self._lhs_lu(*m, 1.0, dt * a_ii).solve(rhs)
             for m in modes:

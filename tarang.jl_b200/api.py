@@ -204,6 +204,14 @@ class Plan:
             out[buf.value.decode()] = (ms.value, cnt.value)
         return out
 
+    def set_wall_values(self, wall: int, value: np.ndarray, rate: Optional[np.ndarray] = None) -> None:
+        """b at wall 0 (z = 0) or 1 (z = Lz): coefficients of the wall profile at
+        the current time (complex Nx/2+1; (Ny, Nx/2+1) in 3D) and their rate."""
+        v = np.ascontiguousarray(value, dtype=np.complex128)
+        r = None if rate is None else np.ascontiguousarray(rate, dtype=np.complex128)
+        check(lib.tb_set_wall_values(self.ptr, int(wall), v.ctypes.data_as(c_void_p),
+                                     None if r is None else r.ctypes.data_as(c_void_p), L.TB_HOST), self.ctx)
+
     def variant(self):
         """(tau-solve partitions, 3D x-pass rows per CTA or 0): the plan's kernel shapes."""
         a, b = c_int(), c_int()

@@ -375,6 +375,13 @@ void enqueue_rk_step(tb_plan* P, double dt) {
       }
       timed(P, "stage_lincomb", [&] { launch_lincomb(lc, P->LXP[i].as<double2>(), cnt, P->st); });
       TauArgs a = tau_args(P, 0, fs, P->LXP[i].as<double2>());
+      if (P->bc_dynamic) {  // wall values at the stage time t_n + c_i dt
+        double ci = 0.0;
+        for (int j = 0; j < i; ++j) ci += T.AE[i][j];
+        a.bcdyn = P->bcdyn.as<double2>();
+        a.t_dev = P->t_dev.as<double>();
+        a.bc_toff = ci * dt;
+      }
       timed(P, "tau_solve", [&] { launch_tau_solve(a, P->sys[0].tau_parts, P->st); });
       if (fs2) {
         TauArgs a2 = tau_args(P, 1, fs2, P->LXP[i].as<double2>());
@@ -416,6 +423,10 @@ void enqueue_rk_step(tb_plan* P, double dt) {
     launch_rk_final(lc, X, P->tau.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->nf, P->ntau, P->st);
   });
   nk += 1;
+  if (P->bc_dynamic) {
+    launch_advance_time(P->t_dev.as<double>(), dt, P->st);
+    nk += 1;
+  }
   P->kernels_per_step = nk;
 }
 
@@ -464,10 +475,19 @@ void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
   }
   timed(P, "stage_lincomb", [&] { launch_lincomb(lc, P->Rsb.as<double2>(), cnt, P->st); });
   TauArgs a = tau_args(P, 0, fs, P->Rsb.as<double2>());
+  if (P->bc_dynamic) {  // wall values at t_{n+1}
+    a.bcdyn = P->bcdyn.as<double2>();
+    a.t_dev = P->t_dev.as<double>();
+    a.bc_toff = dt;
+  }
   timed(P, "tau_solve", [&] { launch_tau_solve(a, P->sys[0].tau_parts, P->st); });
   TB_CUDA_TRY(cudaMemcpyAsync(P->Fprev.p, Fcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
   TB_CUDA_TRY(cudaMemcpyAsync(P->MXprev.p, MXcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
   P->kernels_per_step = 3 + 1 + 1 + 1;
+  if (P->bc_dynamic) {
+    launch_advance_time(P->t_dev.as<double>(), dt, P->st);
+    P->kernels_per_step += 1;
+  }
 }
 
 void drop_graph(tb_plan* P) {
@@ -640,7 +660,7 @@ size_t tb::plan_device_bytes(const tb_plan* P) {
   const DevBuf* bufs[] = {&P->X,   &P->G,   &P->H,    &P->MX0,  &P->Fprev, &P->MXprev, &P->Rsb, &P->tmpgrid,
                           &P->bwd, &P->fwd, &P->s3,   &P->twM,  &P->twN,   &P->ptwM,   &P->bEv, &P->bOv,
                           &P->bEd, &P->bOd, &P->fE,   &P->fO,   &P->sfE,   &P->sfO,    &P->err_mode,
-                          &P->solve_scratch};
+                          &P->solve_scratch, &P->bcdyn,  &P->t_dev};
   for (const DevBuf* d : bufs) b += d->bytes;
   for (int i = 0; i < 4; ++i) b += P->FP[i].bytes + P->LXP[i].bytes;
   for (int sy = 0; sy < P->nsys; ++sy) {
@@ -670,6 +690,8 @@ void tb::plan_snapshot(tb_plan* P, PlanSnapshot* snap) {
     TB_CUDA_TRY(cudaMemcpyAsync(snap->Fprev.p, P->Fprev.p, P->Fprev.bytes, cudaMemcpyDeviceToDevice, P->st));
     TB_CUDA_TRY(cudaMemcpyAsync(snap->MXprev.p, P->MXprev.p, P->MXprev.bytes, cudaMemcpyDeviceToDevice, P->st));
   }
+  if (P->bc_dynamic)
+    TB_CUDA_TRY(cudaMemcpyAsync(&snap->t_dev, P->t_dev.p, sizeof(double), cudaMemcpyDeviceToHost, P->st));
   snap->sim_time = P->sim_time;
   snap->iteration = P->iteration;
   snap->ms_history = P->ms_history;
@@ -682,6 +704,8 @@ void tb::plan_restore(tb_plan* P, const PlanSnapshot& snap) {
     TB_CUDA_TRY(cudaMemcpyAsync(P->Fprev.p, snap.Fprev.p, P->Fprev.bytes, cudaMemcpyDeviceToDevice, P->st));
     TB_CUDA_TRY(cudaMemcpyAsync(P->MXprev.p, snap.MXprev.p, P->MXprev.bytes, cudaMemcpyDeviceToDevice, P->st));
   }
+  if (P->bc_dynamic)
+    TB_CUDA_TRY(cudaMemcpyAsync(P->t_dev.p, &snap.t_dev, sizeof(double), cudaMemcpyHostToDevice, P->st));
   P->sim_time = snap.sim_time;
   P->iteration = snap.iteration;
   P->ms_history = snap.ms_history;
@@ -1236,6 +1260,65 @@ tb_status tb_plan_tune(tb_plan* P, double dt, int trial_steps, int* tau_parts, i
     plan_restore(P, snap);
     if (tau_parts) *tau_parts = bp;
     if (xrows) *xrows = br;
+  });
+}
+
+tb_status tb_set_wall_values(tb_plan* P, int wall, const double* value, const double* rate, int where) {
+  if (!P || !value || (wall != 0 && wall != 1)) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_REQUIRE(P->d.program == TB_PROGRAM_RBC, TB_ENOTSUPPORTED, "wall values belong to the RBC program");
+    TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+    const size_t nm = P->Nk;
+    auto fetch = [&](const double* src, std::vector<double2>& dst) {
+      dst.assign(nm, make_double2(0.0, 0.0));
+      if (!src) return;
+      std::vector<double2> pub(nm);
+      if (where == TB_DEVICE)
+        TB_CUDA_TRY(cudaMemcpy(pub.data(), src, nm * sizeof(double2), cudaMemcpyDeviceToHost));
+      else
+        std::memcpy(pub.data(), src, nm * sizeof(double2));
+      for (size_t m = 0; m < nm; ++m) {  // public (kx fastest) -> plan mode order (ky fastest in 3D)
+        const size_t ix = m / P->Ny, iy = m % P->Ny;
+        dst[m] = pub[ix + (size_t)P->Kx * iy];
+      }
+      for (const double2& v : dst)
+        TB_REQUIRE(std::isfinite(v.x) && std::isfinite(v.y), TB_EINVAL, "wall values must be finite");
+    };
+    std::vector<double2> v0, v1;
+    fetch(value, v0);
+    fetch(rate, v1);
+    if (!P->bc_dynamic) {
+      // start from the plan's constant wall values: b at the DC mode, times the
+      // unnormalised transform of a constant (Nx, or Nx Ny)
+      const double scale = (double)P->Nx * (double)P->Ny;
+      P->bc_host.assign(4 * nm, make_double2(0.0, 0.0));
+      P->bc_host[0] = make_double2(P->d.b_bottom * scale, 0.0);
+      P->bc_host[2 * nm] = make_double2(P->d.b_top * scale, 0.0);
+      P->bcdyn.alloc(4 * nm * sizeof(double2));
+      P->t_dev.alloc(sizeof(double));
+      P->bc_tref = P->sim_time;
+      P->bc_dynamic = true;
+      drop_graph(P);  // step graphs gain the wall-time update
+      if (P->multi.exec) cudaGraphExecDestroy(P->multi.exec);
+      P->multi = StepGraph{};
+    }
+    // re-reference both walls to the current time, then replace this wall
+    const double el = P->sim_time - P->bc_tref;
+    for (int w = 0; w < 2; ++w)
+      for (size_t m = 0; m < nm; ++m) {
+        double2& a = P->bc_host[(2 * w) * nm + m];
+        const double2 r = P->bc_host[(2 * w + 1) * nm + m];
+        a = make_double2(a.x + r.x * el, a.y + r.y * el);
+      }
+    for (size_t m = 0; m < nm; ++m) {
+      P->bc_host[(2 * wall) * nm + m] = v0[m];
+      P->bc_host[(2 * wall + 1) * nm + m] = v1[m];
+    }
+    P->bc_tref = P->sim_time;
+    const double zero = 0.0;
+    TB_CUDA_TRY(cudaMemcpy(P->bcdyn.p, P->bc_host.data(), 4 * nm * sizeof(double2), cudaMemcpyHostToDevice));
+    TB_CUDA_TRY(cudaMemcpy(P->t_dev.p, &zero, sizeof(double), cudaMemcpyHostToDevice));
   });
 }
 

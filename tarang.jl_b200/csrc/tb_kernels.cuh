@@ -159,6 +159,11 @@ struct TauArgs {
   double* HR;
   double* scratch;     // factor workspace
   double* ysave;       // one-partition solve: [group][row][lane] y scratch (tau_solve_scratch_doubles)
+  // dynamic wall values of b (null: constant BCs from bc_rhs): [bottom value,
+  // bottom rate, top value, top rate][mode] at time *t_dev + bc_toff
+  const double2* bcdyn;
+  const double* t_dev;
+  double bc_toff;
   int* err_mode;       // first singular mode, or -1
 };
 // parts: kTauParts (partitioned solve, needs a.PP) or 1 (one warp per group)
@@ -177,6 +182,8 @@ struct LinComb {
 };
 // out[i] = sum_t w_t in_t[i] over count complex entries
 void launch_lincomb(const LinComb& lc, double2* out, long long count, cudaStream_t st);
+
+void launch_advance_time(double* t, double dt, cudaStream_t st);
 
 // Velocity-like fields of a stage vector: nf = 3 (2D: b, u_x, u_z in X planes
 // 0..2, equation planes 1..3) or 4 (3D adds u_perp in X plane 4 with its

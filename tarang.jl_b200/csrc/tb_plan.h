@@ -146,6 +146,13 @@ struct tb_plan {
   int nsys = 1;
   DevBuf err_mode;
   DevBuf solve_scratch;  // y columns of one-partition tau solves (shared by the systems)
+  // dynamic wall values of b (tb_set_wall_values): [bottom value, bottom rate,
+  // top value, top rate][mode] on the device, and the time since they were
+  // set (advanced on the device at the end of each step, so graphs replay)
+  bool bc_dynamic = false;
+  DevBuf bcdyn, t_dev;
+  std::vector<double2> bc_host;
+  double bc_tref = 0.0;
   // stepping state
   double sim_time = 0.0;
   long long iteration = 0;
@@ -200,6 +207,7 @@ void plan_prepare(tb_plan* P, double dt, int graph_steps);
 // Snapshot / restore of the stepping state (X, history, counters) in device scratch.
 struct PlanSnapshot {
   DevBuf X, Fprev, MXprev;
+  double t_dev = 0.0;  // time of the dynamic wall values
   double sim_time = 0.0;
   long long iteration = 0;
   int ms_history = 0;

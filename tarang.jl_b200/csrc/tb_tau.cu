@@ -366,6 +366,17 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 #pragma unroll
   for (int b = 0; b < NBMAX; ++b)
     z[b] = (warp == 0 && part == 0 && m == 0 && b < a.cls[c].nb) ? a.beta * a.cls[c].bc_rhs[b] : 0.0;
+  if (a.bcdyn != nullptr && warp == 0 && m < Nk) {
+    // dynamic wall values of b: boundary row 0 of class c is the parity-c
+    // combination of the walls, (top + bottom)/2 (c = 0) or (top - bottom)/2,
+    // with both walls at the stage time (value + rate * t)
+    const double t = *a.t_dev + a.bc_toff;
+    const double2 v0b = a.bcdyn[m], v1b = a.bcdyn[Nk + m], v0t = a.bcdyn[2 * (size_t)Nk + m],
+                  v1t = a.bcdyn[3 * (size_t)Nk + m];
+    const double bot = part ? fma(v1b.y, t, v0b.y) : fma(v1b.x, t, v0b.x);
+    const double top = part ? fma(v1t.y, t, v0t.y) : fma(v1t.x, t, v0t.x);
+    z[0] = a.beta * 0.5 * (c == 0 ? top + bot : top - bot);
+  }
   for (int s = 0; s < NS - 1; ++s) issue_fwd(s);
   for (int s = 0; s < nst; ++s) {
     issue_fwd(s + NS - 1);    // refills the slot of stage s-1
@@ -771,6 +782,9 @@ __device__ __forceinline__ int xplane_of(int q) { return q < 3 ? q : 4; }
 __device__ __forceinline__ int eplane_of(int q) { return q < 3 ? 1 + q : 4; }
 
 // One thread per (row k, mode m): grid (ceil(Nk / 128), Nz).
+// Advance the device time of dynamic wall values by dt (end of a step).
+__global__ void k_advance_time(double* t, double dt) { *t += dt; }
+
 __global__ void __launch_bounds__(128) k_mass_apply(const double2* __restrict__ X, double2* __restrict__ MX,
                                                     const double* __restrict__ s3, int Nz, int Nk, int Nx,
                                                     int project, int nf) {
@@ -1009,6 +1023,8 @@ void launch_lincomb(const LinComb& lc, double2* out, long long count, cudaStream
   }
 #undef TB_LINCOMB_CASE
 }
+
+void launch_advance_time(double* t, double dt, cudaStream_t st) { k_advance_time<<<1, 1, 0, st>>>(t, dt); }
 
 void launch_mass_apply(const double2* X, double2* MX, const double* s3, int Nz, int Nk, int Nx, int project,
                        int nf, cudaStream_t st) {
