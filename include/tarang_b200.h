@@ -150,6 +150,20 @@ tb_status tb_kernels_per_step(const tb_plan* plan, int* n);
  * constant b_bottom / b_top (the other wall keeps its constant until set). */
 tb_status tb_set_wall_values(tb_plan* plan, int wall, const double* value, const double* rate, int where);
 
+/* Checkpoints (save_state / load_state!, src/tools/solver_checkpoint.jl:88-194).
+ * tb_checkpoint_stage transforms the state to the grid on the device - fields
+ * b, u_x, (u_y,) u_z, p, each real (Nx, Nz) or (Nx, Ny, Nz) column-major,
+ * back to back - and copies them to host_grid (capacity in doubles) on a side
+ * stream: the call returns at once, the plan may step on, and
+ * tb_checkpoint_wait completes the copy (host_grid should be pinned for the
+ * copy to overlap).  clock = {sim_time, iteration, last dt}.
+ * tb_checkpoint_load sets the state from such grid fields and the clock; the
+ * taus are cleared (no later step reads them) and the multistep history
+ * restarts, as the reference drops its timestepper state on load. */
+tb_status tb_checkpoint_stage(tb_plan* plan, double* host_grid, size_t capacity, double* clock);
+tb_status tb_checkpoint_wait(tb_plan* plan);
+tb_status tb_checkpoint_load(tb_plan* plan, const double* grid, int where, const double* clock);
+
 /* Kernel shapes of a plan (the library's own autotuning; the reference tunes
  * FFTW plans instead, transform_fourier.jl plan cache):
  *   tau_parts  warps per 4-mode group in the tau solves: 4 (partitioned, the

@@ -1141,6 +1141,53 @@ class RBC3D:
         self.sim_time += dt
         self.iteration += 1
 
+    def step_sbdf(self, dt: float, order: int = 2) -> None:
+        """SBDF1/SBDF2 (step_subproblem_multistep.jl:197-405; SBDF1 start,
+        step_multistep.jl:341-356) on the 3D system; M X from the projected
+        fields as the 2D restatement."""
+        hist_prev = getattr(self, "_ms_hist", [])
+        use_order = 1 if (order == 1 or len(hist_prev) < 1) else 2
+        a, bcoef, c = sbdf_coefs(use_order, dt, getattr(self, "_ms_dt_prev", None))
+        Fc3 = self.rhs(self.b, self.ux, self.uy, self.uz)
+        proj = [self.pr] + [self.projected(cf) for cf in (self.b, self.ux, self.uy, self.uz)]
+        modes = self.modes()
+        MXc = {m: self.mode_matrices(*m)[0] @ self.gather(*m, proj, self.tau) for m in modes}
+        Fc = {m: self.equation_F(*m, Fc3) for m in modes}
+        hist = [(MXc, Fc)] + hist_prev
+        xs = {}
+        for m in modes:
+            M, L, bc, algf = self.mode_matrices(*m)
+            rhs = np.zeros(M.shape[0], complex)
+            for k in range(1, len(c)):
+                if abs(c[k]) >= 1e-14 and k - 1 < len(hist):
+                    rhs += c[k] * hist[k - 1][1][m]
+            for k in range(1, len(a)):
+                if abs(a[k]) >= 1e-14 and k - 1 < len(hist):
+                    rhs -= a[k] * hist[k - 1][0][m]
+            if self.wall_b is not None:
+                bot, top = self.wall_b(self.sim_time + dt)
+                algf = algf.copy()
+                algf[5 * self.p.Nz + 0] = bot[m]
+                algf[5 * self.p.Nz + 4] = top[m]
+            rhs[bc] = bcoef[0] * algf[bc]
+            xs[m] = self._lhs_lu(*m, a[0], bcoef[0]).solve(rhs)
+        for m in modes:
+            self.scatter(*m, xs[m])
+        self._ms_hist = hist[:1] if order == 1 else hist[:2]
+        self._ms_dt_prev = dt
+        self.sim_time += dt
+        self.iteration += 1
+
+    def step(self, dt: float, scheme: str) -> None:
+        if scheme in TABLEAUS:
+            self.step_rk(dt, TABLEAUS[scheme])
+        elif scheme == "SBDF1":
+            self.step_sbdf(dt, 1)
+        elif scheme == "SBDF2":
+            self.step_sbdf(dt, 2)
+        else:
+            raise ValueError(scheme)
+
     def state_dict(self) -> Dict[str, np.ndarray]:
         return dict(b=self.b.copy(), ux=self.ux.copy(), uy=self.uy.copy(), uz=self.uz.copy(), p=self.pr.copy(),
                     tau=self.tau.copy())

@@ -86,6 +86,9 @@ SIGNATURES = {
     "tb_kernels_per_step": (c_int, [c_void_p, POINTER(c_int)]),
     "tb_plan_set_variant": (c_int, [c_void_p, c_int, c_int]),
     "tb_set_wall_values": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int]),
+    "tb_checkpoint_stage": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
+    "tb_checkpoint_wait": (c_int, [c_void_p]),
+    "tb_checkpoint_load": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "tb_plan_get_variant": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
     "tb_plan_tune": (c_int, [c_void_p, c_double, c_int, POINTER(c_int), POINTER(c_int)]),
     "tb_tau_layout_query": (c_int, [c_int, c_double, c_double, c_int, POINTER(c_int)]),

@@ -212,6 +212,18 @@ class Plan:
         check(lib.tb_set_wall_values(self.ptr, int(wall), v.ctypes.data_as(c_void_p),
                                      None if r is None else r.ctypes.data_as(c_void_p), L.TB_HOST), self.ctx)
 
+    def save_state(self, path: str) -> None:
+        """Grid-space NetCDF checkpoint of the state and clock (solver_checkpoint.jl:88-125)."""
+        from .checkpoint import save_state
+
+        save_state(self, path)
+
+    def load_state(self, path: str) -> None:
+        """Restore the state and clock from a checkpoint (solver_checkpoint.jl:146-194)."""
+        from .checkpoint import load_state
+
+        load_state(self, path)
+
     def variant(self):
         """(tau-solve partitions, 3D x-pass rows per CTA or 0): the plan's kernel shapes."""
         a, b = c_int(), c_int()

@@ -456,12 +456,26 @@ void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
   const SbdfCoefs K = sbdf_coefs(order, dt);
   const double a0 = K.a0, a1 = K.a1, a2 = K.a2, c1 = K.c1, c2 = K.c2;
   FactorSet* fs = get_factors(P, 0, a0, 1.0);
+  FactorSet* fs2 = P->nsys > 1 ? get_factors(P, 1, a0, 1.0) : nullptr;
   const long long cnt = (long long)P->nplanes * (long long)P->plane;
   double2* X = P->X.as<double2>();
   double2* Fcur = P->FP[0].as<double2>();
   double2* MXcur = P->MX0.as<double2>();
-  enqueue_rhs(P, X, Fcur + P->plane, true);
-  timed(P, "mass_apply", [&] { launch_mass_apply(X, MXcur, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 1, P->nf, P->st); });
+  const bool d3 = P->ndim == 3;
+  int extra = 0;
+  if (d3)
+    rbc3d_enqueue_rhs(P, X, Fcur + P->plane);
+  else
+    enqueue_rhs(P, X, Fcur + P->plane, true);
+  // M X of the projected fields: 2D drops Im at the DC / Nyquist modes; 3D
+  // subtracts M delta on the kx = 0 / Nyquist planes
+  timed(P, "mass_apply", [&] {
+    launch_mass_apply(X, MXcur, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, d3 ? 0 : 1, P->nf, P->st);
+  });
+  if (d3) {
+    rbc3d_mx_project(P, MXcur);
+    ++extra;
+  }
   LinComb lc{};
   lc.in[lc.n] = Fcur;
   lc.w[lc.n++] = c1;
@@ -481,9 +495,14 @@ void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
     a.bc_toff = dt;
   }
   timed(P, "tau_solve", [&] { launch_tau_solve(a, P->sys[0].tau_parts, P->st); });
+  if (fs2) {
+    TauArgs a2 = tau_args(P, 1, fs2, P->Rsb.as<double2>());
+    timed(P, "tau_solve_perp", [&] { launch_tau_solve(a2, P->sys[1].tau_parts, P->st); });
+    ++extra;
+  }
   TB_CUDA_TRY(cudaMemcpyAsync(P->Fprev.p, Fcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
   TB_CUDA_TRY(cudaMemcpyAsync(P->MXprev.p, MXcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
-  P->kernels_per_step = 3 + 1 + 1 + 1;
+  P->kernels_per_step = (d3 ? (P->mixed ? 6 : 5) : (P->mixed ? 4 : 3)) + 1 + 1 + 1 + extra;
   if (P->bc_dynamic) {
     launch_advance_time(P->t_dev.as<double>(), dt, P->st);
     P->kernels_per_step += 1;
@@ -542,6 +561,7 @@ void prepare_kind(tb_plan* P, double dt, int kind) {
 }
 
 void advance_counters(tb_plan* P, double dt, int kind, int steps) {
+  P->last_dt = dt;
   P->sim_time += dt * steps;
   P->iteration += steps;
   if (kind != 0) P->ms_history = 1;
@@ -723,8 +743,7 @@ void validate_desc(const tb_problem_desc* d) {
     TB_REQUIRE(d->Ny >= 6 && d->Ny % 2 == 0, TB_EINVAL, "Ny must be even and >= 6");
     TB_REQUIRE(d->Ly > 0, TB_EINVAL, "domain lengths must be positive");
     TB_REQUIRE(d->Nz % 2 == 0, TB_ENOTSUPPORTED, "3D plans need an even Nz");
-    TB_REQUIRE(d->timestepper == TB_RK222 || d->timestepper == TB_RK443, TB_ENOTSUPPORTED,
-               "3D plans step with RK222 or RK443");
+
   }
   TB_REQUIRE(d->Nz >= 8 && d->Nz <= 32767, TB_EINVAL, "Nz must be in [8, 32767]");
   TB_REQUIRE(d->Lx > 0 && d->Lz > 0, TB_EINVAL, "domain lengths must be positive");
@@ -1319,6 +1338,127 @@ tb_status tb_set_wall_values(tb_plan* P, int wall, const double* value, const do
     const double zero = 0.0;
     TB_CUDA_TRY(cudaMemcpy(P->bcdyn.p, P->bc_host.data(), 4 * nm * sizeof(double2), cudaMemcpyHostToDevice));
     TB_CUDA_TRY(cudaMemcpy(P->t_dev.p, &zero, sizeof(double), cudaMemcpyHostToDevice));
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// Grid fields of a checkpoint, in order: b, u_x, (u_y), u_z, p.
+int checkpoint_fields(const tb_plan* P) { return P->ndim == 3 ? 5 : 4; }
+size_t grid_points(const tb_plan* P) { return (size_t)P->Nz * P->Ny * P->Nx; }
+
+// 2D: coefficient plane (Nz, Nx/2+1) -> grid (Nz, Nx) on the plan's stream.
+void grid_of_plane_2d(tb_plan* P, const double2* coeff, double* grid) {
+  double2* mixed = P->tmpgrid.as<double2>();
+  GemmBatch bt{};
+  bt.item[0] = GemmItem{P->bwd.as<double>(), reinterpret_cast<const double*>(coeff), reinterpret_cast<double*>(mixed),
+                        P->Nz, P->Nz, pad16k(P->Nz), GEMM_PLAIN, 0};
+  launch_gemm_f64(bt, 1, 2 * P->Nk, 2 * P->Nk, 2 * P->Nk, P->Nz, P->st);
+  launch_x_irfft(mixed, grid, P->Nz, P->Nx, P->fpN, P->twN.as<double2>(), P->st);
+}
+
+void plane_of_grid_2d(tb_plan* P, const double* grid, double2* coeff) {
+  double2* mixed = P->tmpgrid.as<double2>();
+  launch_x_rfft(grid, mixed, P->Nz, P->Nx, P->fpN, P->twN.as<double2>(), P->st);
+  GemmBatch bt{};
+  bt.item[0] = GemmItem{P->fE.as<double>(), reinterpret_cast<const double*>(mixed), reinterpret_cast<double*>(coeff),
+                        P->Ke, P->Hz, pad16k(P->Hz), GEMM_MIRROR, 0};
+  bt.item[1] = GemmItem{P->fO.as<double>(), reinterpret_cast<const double*>(mixed), reinterpret_cast<double*>(coeff),
+                        P->Ko, P->Hz, pad16k(P->Hz), GEMM_MIRROR, 1};
+  launch_gemm_f64(bt, P->Ko > 0 ? 2 : 1, 2 * P->Nk, 2 * P->Nk, 2 * P->Nk, P->Nz, P->st);
+}
+
+}  // namespace
+
+extern "C" {
+
+tb_status tb_checkpoint_stage(tb_plan* P, double* host_grid, size_t capacity, double* clock3) {
+  if (!P || !host_grid) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_REQUIRE(P->d.program == TB_PROGRAM_RBC, TB_ENOTSUPPORTED, "checkpoints of RBC plans");
+    const int nf = checkpoint_fields(P);
+    const size_t g = grid_points(P);
+    TB_REQUIRE(capacity >= (size_t)nf * g, TB_EINVAL, "host buffer smaller than the checkpoint's grid fields");
+    TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
+    if (!P->io_st) {
+      TB_CUDA_TRY(cudaStreamCreateWithFlags(&P->io_st, cudaStreamNonBlocking));
+      TB_CUDA_TRY(cudaEventCreateWithFlags(&P->io_ready, cudaEventDisableTiming));
+      TB_CUDA_TRY(cudaEventCreateWithFlags(&P->io_done, cudaEventDisableTiming));
+      TB_CUDA_TRY(cudaEventRecord(P->io_done, P->io_st));
+    }
+    if (P->stage_grid.bytes < (size_t)nf * g * sizeof(double)) {
+      TB_CUDA_TRY(cudaStreamSynchronize(P->io_st));
+      P->stage_grid.alloc((size_t)nf * g * sizeof(double));
+    }
+    double* stage = P->stage_grid.as<double>();
+    // the previous checkpoint's copy must have left the staging buffer
+    TB_CUDA_TRY(cudaStreamWaitEvent(P->st, P->io_done, 0));
+    if (P->ndim == 3) {
+      const int fields[5] = {TB_FIELD_B, TB_FIELD_UX, TB_FIELD_UY, TB_FIELD_UZ, TB_FIELD_P};
+      for (int f = 0; f < nf; ++f) {
+        rbc3d_state_get(P, fields[f], P->tmp3.as<double2>());
+        rbc3d_transform_backward(P, P->tmp3.as<double2>(), stage + f * g);
+      }
+    } else {
+      const int planes[4] = {0, 1, 2, 3};  // b, u_x, u_z, p
+      for (int f = 0; f < nf; ++f) grid_of_plane_2d(P, P->Xp(planes[f]), stage + f * g);
+    }
+    check_launch("checkpoint staging");
+    TB_CUDA_TRY(cudaEventRecord(P->io_ready, P->st));
+    TB_CUDA_TRY(cudaStreamWaitEvent(P->io_st, P->io_ready, 0));
+    TB_CUDA_TRY(cudaMemcpyAsync(host_grid, stage, (size_t)nf * g * sizeof(double), cudaMemcpyDeviceToHost,
+                                P->io_st));
+    TB_CUDA_TRY(cudaEventRecord(P->io_done, P->io_st));
+    if (clock3) {
+      clock3[0] = P->sim_time;
+      clock3[1] = (double)P->iteration;
+      clock3[2] = P->last_dt;
+    }
+  });
+}
+
+tb_status tb_checkpoint_wait(tb_plan* P) {
+  if (!P) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    if (P->io_st) TB_CUDA_TRY(cudaStreamSynchronize(P->io_st));
+  });
+}
+
+tb_status tb_checkpoint_load(tb_plan* P, const double* grid, int where, const double* clock3) {
+  if (!P || !grid || !clock3) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_REQUIRE(P->d.program == TB_PROGRAM_RBC, TB_ENOTSUPPORTED, "checkpoints of RBC plans");
+    TB_REQUIRE(std::isfinite(clock3[0]) && clock3[1] >= 0, TB_EINVAL, "checkpoint clock must be finite");
+    TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
+    const int nf = checkpoint_fields(P);
+    const size_t g = grid_points(P);
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+    if (P->stage_grid.bytes < (size_t)nf * g * sizeof(double)) P->stage_grid.alloc((size_t)nf * g * sizeof(double));
+    if (P->io_st) TB_CUDA_TRY(cudaStreamSynchronize(P->io_st));
+    double* stage = P->stage_grid.as<double>();
+    TB_CUDA_TRY(cudaMemcpy(stage, grid, (size_t)nf * g * sizeof(double),
+                           where == TB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+    // the taus and pressure history never enter a later step through M X, and
+    // the multistep history restarts (the reference drops its timestepper state)
+    TB_CUDA_TRY(cudaMemsetAsync(P->tau.p, 0, P->tau.bytes, P->st));
+    if (P->ndim == 3) {
+      const int fields[5] = {TB_FIELD_B, TB_FIELD_UX, TB_FIELD_UY, TB_FIELD_UZ, TB_FIELD_P};
+      TB_CUDA_TRY(cudaMemsetAsync(P->X.p, 0, (size_t)P->nplanes * P->plane * sizeof(double2), P->st));
+      for (int f = 0; f < nf; ++f) {
+        rbc3d_transform_forward(P, stage + f * g, P->tmp3.as<double2>());
+        rbc3d_state_set(P, fields[f], P->tmp3.as<double2>());
+      }
+    } else {
+      for (int f = 0; f < nf; ++f) plane_of_grid_2d(P, stage + f * g, P->Xp(f));
+    }
+    check_launch("checkpoint load");
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+    P->sim_time = clock3[0];
+    P->iteration = (long long)clock3[1];
+    P->last_dt = clock3[2];
+    P->ms_history = 0;
   });
 }
 

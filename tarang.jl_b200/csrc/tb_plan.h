@@ -153,7 +153,13 @@ struct tb_plan {
   DevBuf bcdyn, t_dev;
   std::vector<double2> bc_host;
   double bc_tref = 0.0;
+  // checkpoint staging: grid copies of the fields on the device, copied to the
+  // caller's host buffer on a side stream while the plan steps on
+  DevBuf stage_grid;
+  cudaStream_t io_st = nullptr;
+  cudaEvent_t io_ready = nullptr, io_done = nullptr;
   // stepping state
+  double last_dt = 0.0;
   double sim_time = 0.0;
   long long iteration = 0;
   int ms_history = 0;  // SBDF: number of stored history levels
@@ -183,6 +189,12 @@ struct tb_plan {
     }
     if (gexec) cudaGraphExecDestroy(gexec);
     if (multi.exec) cudaGraphExecDestroy(multi.exec);
+    if (io_st) {
+      cudaStreamSynchronize(io_st);
+      cudaStreamDestroy(io_st);
+    }
+    if (io_ready) cudaEventDestroy(io_ready);
+    if (io_done) cudaEventDestroy(io_done);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (st) cudaStreamDestroy(st);
@@ -253,6 +265,7 @@ bool rbc3d_xrows_ok(const tb_plan* P, int rows);
 bool plan_tau_parts_ok(const tb_plan* P, int parts);
 void plan_set_variant(tb_plan* P, int tau_parts, int xrows);
 void rbc3d_lx_project(tb_plan* P, double2* LX, double beta);
+void rbc3d_mx_project(tb_plan* P, double2* MX);
 size_t rbc3d_device_bytes(const tb_plan* P);
 // 3D transforms between grid (Nz, Ny, Nx) real and coefficients (Nz, Ny, Nx/2+1)
 // complex (kx fastest), device pointers, one field.

@@ -340,6 +340,9 @@ __global__ void __launch_bounds__(kR3Threads) k3_yfwd(R3Args a, const C* __restr
 //   b     kappa (k^2 S - D2) d_b
 //   mom   nu (k^2 S - D2) d_u  (- S d_b in z), rotated to (par, perp) rows.
 // One thread per (row k, plane, iy): grid (ceil(2 Ny / 128), Nz).
+// MASS: the same projection for M X of the multistep history (M delta: S d_b,
+// S d_u rotated; continuity rows 0).
+template <bool MASS>
 __global__ void __launch_bounds__(128) k3_lx_project(R3Args a, double2* __restrict__ LX, const double2* __restrict__ X,
                                                      const double* __restrict__ s3, double s, double kappa, double nu,
                                                      double beta) {
@@ -388,12 +391,21 @@ __global__ void __launch_bounds__(128) k3_lx_project(R3Args a, double2* __restri
   const double2 Db = delta(0, k + 2), Dux = delta(1, k + 2), Duy = delta(2, k + 2), Duz = delta(3, k + 2);
   const double2 u1 = delta(3, k + 1), u3 = delta(3, k + 3);
   double2 L[5];
-  // continuity: i kx S d_ux + i ky S d_uy + SD d_uz
-  L[0] = make_double2(-kx * Sux.y - ky * Suy.y + s * (u1.x - u3.x), kx * Sux.x + ky * Suy.x + s * (u1.y - u3.y));
-  L[1] = make_double2(kappa * (k2 * Sb.x - d2c * Db.x), kappa * (k2 * Sb.y - d2c * Db.y));
-  const double2 mx = make_double2(nu * (k2 * Sux.x - d2c * Dux.x), nu * (k2 * Sux.y - d2c * Dux.y));
-  const double2 my = make_double2(nu * (k2 * Suy.x - d2c * Duy.x), nu * (k2 * Suy.y - d2c * Duy.y));
-  L[3] = make_double2(nu * (k2 * Suz.x - d2c * Duz.x) - Sb.x, nu * (k2 * Suz.y - d2c * Duz.y) - Sb.y);
+  double2 mx, my;
+  if constexpr (MASS) {
+    L[0] = make_double2(0.0, 0.0);
+    L[1] = Sb;
+    mx = Sux;
+    my = Suy;
+    L[3] = Suz;
+  } else {
+    // continuity: i kx S d_ux + i ky S d_uy + SD d_uz
+    L[0] = make_double2(-kx * Sux.y - ky * Suy.y + s * (u1.x - u3.x), kx * Sux.x + ky * Suy.x + s * (u1.y - u3.y));
+    L[1] = make_double2(kappa * (k2 * Sb.x - d2c * Db.x), kappa * (k2 * Sb.y - d2c * Db.y));
+    mx = make_double2(nu * (k2 * Sux.x - d2c * Dux.x), nu * (k2 * Sux.y - d2c * Dux.y));
+    my = make_double2(nu * (k2 * Suy.x - d2c * Duy.x), nu * (k2 * Suy.y - d2c * Duy.y));
+    L[3] = make_double2(nu * (k2 * Suz.x - d2c * Duz.x) - Sb.x, nu * (k2 * Suz.y - d2c * Duz.y) - Sb.y);
+  }
   L[2] = make_double2(cx * mx.x + cy * my.x, cx * mx.y + cy * my.y);
   L[4] = make_double2(-cy * mx.x + cx * my.x, -cy * mx.y + cx * my.y);
   (void)beta;
@@ -769,8 +781,16 @@ void rbc3d_enqueue_rhs(tb_plan* P, const double2* Xin, double2* out4) {
 void rbc3d_lx_project(tb_plan* P, double2* LX, double beta) {
   const R3Args a = args_of(P);
   timed(P, "lx_project", [&] {
-    k3_lx_project<<<dim3((2 * P->Ny + 127) / 128, P->Nz), 128, 0, P->st>>>(
+    k3_lx_project<false><<<dim3((2 * P->Ny + 127) / 128, P->Nz), 128, 0, P->st>>>(
         a, LX, P->X.as<double2>(), P->s3.as<double>(), P->s, P->d.kappa, P->d.nu, beta);
+  });
+}
+
+void rbc3d_mx_project(tb_plan* P, double2* MX) {
+  const R3Args a = args_of(P);
+  timed(P, "mx_project", [&] {
+    k3_lx_project<true><<<dim3((2 * P->Ny + 127) / 128, P->Nz), 128, 0, P->st>>>(
+        a, MX, P->X.as<double2>(), P->s3.as<double>(), P->s, P->d.kappa, P->d.nu, 1.0);
   });
 }
 

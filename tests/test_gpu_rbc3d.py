@@ -75,7 +75,7 @@ def test_rbc3d_rejects_unsupported(tb):
     with pytest.raises(tb.TarangError):
         tb.Plan3D(16, 12, 15, 1e-3, 1e-3)  # odd Nz
     with pytest.raises(tb.TarangError):
-        tb.Plan3D(16, 12, 16, 1e-3, 1e-3, timestepper=3)  # SBDF2
+        tb.Plan3D(16, 18, 16, 1e-3, 1e-3)  # padded Ny = 28 is not 2^a 3^b
 
 
 def test_rbc3d_transforms_match_oracle(tb):
@@ -88,3 +88,17 @@ def test_rbc3d_transforms_match_oracle(tb):
     c2 = forward_3d(g)
     c2[:, :, -1] += 0.5j  # non-Hermitian Nyquist content is dropped like FFTW's c2r
     assert rel_l2(plan.backward(c2), backward_3d(c2, Nx)) < 1e-13
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-10), (1, 1e-6)])
+def test_rbc3d_sbdf2_matches_oracle(tb, precision, tol):
+    p = RBC3Params(Nx=16, Ny=12, Nz=12, Lx=4.0, Ly=3.0, Ra=1e6)
+    sim = RBC3D(p)
+    sim.set_b_grid(rbc3_initial_b(p, 42, amp=1e-2))
+    for _ in range(4):
+        sim.step(0.02, "SBDF2")
+    plan = tb.Plan3D(16, 12, 12, p.kappa, p.nu, 3, 4.0, 3.0, 1.0, precision=precision)
+    plan.set_state(0, plan.forward(rbc3_initial_b(p, 42, amp=1e-2)))
+    plan.step(0.02, 4)
+    for name, f in FIELDS:
+        assert rel_l2(plan.get_state(f), getattr(sim, name)) < tol, name

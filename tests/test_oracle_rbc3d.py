@@ -112,3 +112,18 @@ def test_stage_solution_satisfies_walls():
     for f in range(1, 5):  # b, ux, uy, uz vanish at both walls at kx != 0
         c = x[f * N : (f + 1) * N]
         assert abs(np.sum(c)) < 1e-9 and abs(np.sum(c * (-1.0) ** np.arange(N))) < 1e-9
+
+
+def test_y_invariant_sbdf2_follows_the_2d_problem():
+    p2 = RBCParams(Nx=16, Nz=12, Lx=4.0, Lz=1.0, Ra=1e6)
+    p3 = RBC3Params(Nx=16, Ny=6, Nz=12, Lx=4.0, Ly=3.0, Lz=1.0, Ra=1e6)
+    b2 = rbc_initial_b(p2, 3)
+    s2 = RBC2D(p2)
+    s2.set_b_grid(b2)
+    s3 = RBC3D(p3)
+    s3.set_b_grid(np.repeat(b2[:, None, :], p3.Ny, axis=1))
+    for _ in range(4):
+        s2.step(0.02, "SBDF2")
+        s3.step(0.02, "SBDF2")
+    for a2, a3 in ((s2.b, s3.b), (s2.ux, s3.ux), (s2.uz, s3.uz)):
+        assert rel_l2(a3[:, 0, :] / p3.Ny, a2) < 1e-11
