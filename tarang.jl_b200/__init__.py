@@ -16,6 +16,7 @@ from .api import (  # noqa: F401
     SBDF1,
     SBDF2,
     ChannelDomain,
+    ChannelDomain3D,
     ChebyshevT,
     Domain,
     Ensemble,

@@ -73,17 +73,31 @@ class ChebyshevT(RealFourier):
 
 
 class Domain:
+    """RealFourier x (, RealFourier y) x ChebyshevT z."""
+
     def __init__(self, bases: Sequence, arch=None):
         self.bases = tuple(bases)
         self.arch = arch if arch is not None else GPU()
         if isinstance(self.arch, CPU):
             raise NotImplementedError("the B200 library serves arch=GPU() only")
-        self.xbasis, self.zbasis = self.bases
+        if len(self.bases) == 3:
+            self.xbasis, self.ybasis, self.zbasis = self.bases
+        else:
+            self.xbasis, self.zbasis = self.bases
+            self.ybasis = None
         self._tplan = None
+
+    @property
+    def ndim(self) -> int:
+        return 3 if self.ybasis is not None else 2
 
     @property
     def Nx(self) -> int:
         return self.xbasis.size
+
+    @property
+    def Ny(self) -> int:
+        return self.ybasis.size if self.ybasis is not None else 1
 
     @property
     def Nz(self) -> int:
@@ -93,17 +107,31 @@ class Domain:
     def Nk(self) -> int:
         return self.Nx // 2 + 1
 
+    def coeff_shape(self):
+        """Coefficient layout of a field: (Nz, Nx/2+1) or (Nz, Ny, Nx/2+1)."""
+        return (self.Nz, self.Ny, self.Nk) if self.ndim == 3 else (self.Nz, self.Nk)
+
+    def grid_shape(self):
+        return (self.Nz, self.Ny, self.Nx) if self.ndim == 3 else (self.Nz, self.Nx)
+
     def grids(self):
-        """(x, z) grids: x_j = j Lx/Nx, z_j = Lz/2 (1 - cos(pi j/(Nz-1))) (basis_interface.jl:81-121)."""
+        """(x, [y,] z) grids: x_j = j Lx/Nx, z_j = a + (b-a)/2 (1 - cos(pi j/(Nz-1))) (basis_interface.jl:81-121)."""
         x = self.xbasis.bounds[0] + np.arange(self.Nx) * self.xbasis.length / self.Nx
         a, b = self.zbasis.bounds
         z = (b - a) / 2 * (-np.cos(np.pi * np.arange(self.Nz) / (self.Nz - 1))) + (b + a) / 2
+        if self.ndim == 3:
+            y = self.ybasis.bounds[0] + np.arange(self.Ny) * self.ybasis.length / self.Ny
+            return x, y, z
         return x, z
 
     def transform_plan(self) -> "Plan":
         """A plan used only for field transforms (physics parameters unused)."""
         if self._tplan is None:
-            self._tplan = Plan(self, kappa=1.0, nu=1.0, b_bottom=0.0, b_top=0.0, timestepper=L.TB_RK222)
+            if self.ndim == 3:
+                self._tplan = Plan3D(self.Nx, self.Ny, self.Nz, 1.0, 1.0, L.TB_RK222, self.xbasis.length,
+                                     self.ybasis.length, self.zbasis.length, device=self.arch.device)
+            else:
+                self._tplan = Plan(self, kappa=1.0, nu=1.0, b_bottom=0.0, b_top=0.0, timestepper=L.TB_RK222)
         return self._tplan
 
 
@@ -113,6 +141,17 @@ def ChannelDomain(Nx: int, Nz: int, Lx: float = 2 * math.pi, Lz: float = 2.0, dt
     if dtype not in (np.float64, float):
         raise NotImplementedError("the FP64 path stores Float64 fields")
     return Domain((RealFourier("x", Nx, (0.0, Lx), dealias), ChebyshevT("z", Nz, (0.0, Lz), dealias)), arch)
+
+
+def ChannelDomain3D(Nx: int, Ny: int, Nz: int, Lx: float = 4 * math.pi, Ly: float = 2 * math.pi, Lz: float = 2.0,
+                    dtype=np.float64, arch=None, dealias: float = 1.5, zbounds=None) -> Domain:
+    """RealFourier x, y x ChebyshevT z (quick_domains.jl:124-143: z in (-1, 1)
+    by default there; zbounds overrides, e.g. (0, Lz))."""
+    if dtype not in (np.float64, float):
+        raise NotImplementedError("the FP64 path stores Float64 fields")
+    zb = (-1.0, 1.0) if zbounds is None else tuple(map(float, zbounds))
+    return Domain((RealFourier("x", Nx, (0.0, Lx), dealias), RealFourier("y", Ny, (0.0, Ly), dealias),
+                   ChebyshevT("z", Nz, zb, dealias)), arch)
 
 
 # ---------------------------------------------------------------------------
@@ -541,8 +580,12 @@ class ScalarField:
         self.domain = domain
         self.name = name
         self.bases = domain.bases if bases is None else tuple(bases)
-        self._coeff = np.zeros((domain.Nz, domain.Nk), np.complex128) if len(self.bases) == 2 else np.zeros(
-            domain.Nk, np.complex128)
+        full = len(self.bases) == len(domain.bases)
+        if full:
+            shape = domain.coeff_shape()
+        else:  # a tau field on the Fourier bases
+            shape = (domain.Ny, domain.Nk) if domain.ndim == 3 else (domain.Nk,)
+        self._coeff = np.zeros(shape, np.complex128)
         self._solver = None
         self._slot = None  # (field selector, row) inside the solver's plan
 
@@ -567,7 +610,7 @@ class ScalarField:
         if layout == "c":
             return self._coeff.copy()
         if layout == "g":
-            if len(self.bases) != 2:
+            if len(self.bases) != len(self.domain.bases):
                 raise NotImplementedError("grid view of tau fields")
             return self.domain.transform_plan().backward(self._coeff)
         raise KeyError(layout)
@@ -576,7 +619,7 @@ class ScalarField:
         if layout == "c":
             self._coeff = np.array(value, dtype=np.complex128).reshape(self._coeff.shape)
         elif layout == "g":
-            g = np.broadcast_to(np.asarray(value, dtype=np.float64), (self.domain.Nz, self.domain.Nx))
+            g = np.broadcast_to(np.asarray(value, dtype=np.float64), self.domain.grid_shape())
             self._coeff = self.domain.transform_plan().forward(np.ascontiguousarray(g))
         else:
             raise KeyError(layout)
@@ -587,12 +630,13 @@ class VectorField:
     def __init__(self, domain: Domain, name: str, bases: Optional[tuple] = None):
         self.domain = domain
         self.name = name
-        self.components = [ScalarField(domain, f"{name}_{c}", bases) for c in ("x", "z")]
+        comps = ("x", "y", "z") if domain.ndim == 3 else ("x", "z")
+        self.components = [ScalarField(domain, f"{name}_{c}", bases) for c in comps]
 
 
 def unit_vector_fields(domain: Domain):
-    """Constant unit vectors (ex, ez); used only as tokens in equation strings."""
-    return ("ex", "ez")
+    """Constant unit vectors ((ex, [ey,] ez)); used only as tokens in equation strings."""
+    return ("ex", "ey", "ez") if domain.ndim == 3 else ("ex", "ez")
 
 
 # ---------------------------------------------------------------------------
@@ -723,17 +767,24 @@ class InitialValueSolver:
                 domain = v.domain
             else:
                 fields[v.name] = v
-                if len(v.bases) == 2:
+                if len(v.bases) == len(v.domain.bases):
                     domain = v.domain
         self.domain = domain
         self.problem = problem
         self.timestepper = timestepper
         self.dt = dt
-        self.plan = Plan(domain, spec["kappa"], spec["nu"], spec["b_bottom"], spec["b_top"], _TS_IDS[timestepper.name])
+        ts = _TS_IDS[timestepper.name]
+        if domain.ndim == 3:
+            self.plan = Plan3D(domain.Nx, domain.Ny, domain.Nz, spec["kappa"], spec["nu"], ts, domain.xbasis.length,
+                               domain.ybasis.length, domain.zbasis.length, spec["b_bottom"], spec["b_top"],
+                               device=domain.arch.device)
+        else:
+            self.plan = Plan(domain, spec["kappa"], spec["nu"], spec["b_bottom"], spec["b_top"], ts)
         names = spec["names"]
         b, u, p = fields[names["b"]], fields[names["u"]], fields[names["p"]]
-        binds = [(b, (L.TB_FIELD_B, None)), (u.components[0], (L.TB_FIELD_UX, None)),
-                 (u.components[1], (L.TB_FIELD_UZ, None)), (p, (L.TB_FIELD_P, None))]
+        ucomp = ([L.TB_FIELD_UX, L.TB_FIELD_UY, L.TB_FIELD_UZ] if domain.ndim == 3 else [L.TB_FIELD_UX, L.TB_FIELD_UZ])
+        binds = [(b, (L.TB_FIELD_B, None))] + [(c, (sel, None)) for c, sel in zip(u.components, ucomp)] + \
+                [(p, (L.TB_FIELD_P, None))]
         for f, slot in binds:
             f._solver, f._slot = self, slot
             f._push()

@@ -102,3 +102,42 @@ def test_rbc3d_sbdf2_matches_oracle(tb, precision, tol):
     plan.step(0.02, 4)
     for name, f in FIELDS:
         assert rel_l2(plan.get_state(f), getattr(sim, name)) < tol, name
+
+
+def test_reference_style_3d_script(tb):
+    # the 3D channel written against the mirror API as in the reference's
+    # examples/ivp/rotating_rayleigh_benard_3d.jl (without rotation), against the oracle
+    Lx, Ly, Lz, Nx, Ny, Nz, Ra = 4.0, 3.0, 1.0, 16, 12, 12, 1e5
+    kappa, nu = Ra ** -0.5, Ra ** -0.5
+    domain = tb.ChannelDomain3D(Nx, Ny, Nz, Lx=Lx, Ly=Ly, Lz=Lz, zbounds=(0.0, Lz))
+    p = tb.ScalarField(domain, "p")
+    b = tb.ScalarField(domain, "b")
+    u = tb.VectorField(domain, "u")
+    xy = (domain.xbasis, domain.ybasis)
+    taus = [tb.ScalarField(domain, "tau_p", ()), tb.ScalarField(domain, "tau_b1", xy),
+            tb.ScalarField(domain, "tau_b2", xy), tb.VectorField(domain, "tau_u1", xy),
+            tb.VectorField(domain, "tau_u2", xy)]
+    assert taus[1]["c"].shape == (Ny, Nx // 2 + 1) and len(u.components) == 3
+    problem = tb.IVP([p, b, u] + taus)
+    tb.add_parameters(problem, kappa=kappa, nu=nu, Lz=Lz)
+    tb.add_equation(problem, "trace(grad_u) + tau_p = 0")
+    tb.add_equation(problem, "∂t(b) - kappa*div(grad_b) + τ_lift(tau_b2) = -u⋅∇(b)")
+    tb.add_equation(problem, "∂t(u) - nu*div(grad_u) + ∇(p) - b*ez + τ_lift(tau_u2) = -u⋅∇(u)")
+    tb.add_bc(problem, "b(z=0) = Lz")
+    tb.add_bc(problem, "u(z=0) = 0")
+    tb.add_bc(problem, "b(z=Lz) = 0")
+    tb.add_bc(problem, "u(z=Lz) = 0")
+    tb.add_bc(problem, "integ(p) = 0")
+    solver = tb.InitialValueSolver(problem, tb.RK222(), dt=0.02)
+    rp = RBC3Params(Nx=Nx, Ny=Ny, Nz=Nz, Lx=Lx, Ly=Ly, Lz=Lz, Ra=Ra)
+    b["g"] = rbc3_initial_b(rp, 42, amp=1e-2)
+    tb.run(solver, stop_iteration=3)
+    sim = RBC3D(rp)
+    sim.set_b_grid(rbc3_initial_b(rp, 42, amp=1e-2))
+    for _ in range(3):
+        sim.step_rk(0.02, TABLEAUS["RK222"])
+    assert solver.iteration == 3
+    assert rel_l2(b["c"], sim.b) < 1e-10
+    for comp, want in zip(u.components, (sim.ux, sim.uy, sim.uz)):
+        assert rel_l2(comp["c"], want) < 1e-10
+    assert b["g"].shape == (Nz, Ny, Nx)
