@@ -528,6 +528,7 @@ def run_ensemble(args, dev, dist=None):
     ens = tb.Ensemble(plans)
     streams, gsteps = ens.tune(dts, trial_steps=8)
     tuned_parts = plans[0].variant()[0]
+    tuned_fused, tuned_groups = ens.form()
     reset()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -553,7 +554,8 @@ def run_ensemble(args, dev, dist=None):
                     if world > 1 else "one GPU",
         "scheme": "RK222",
         "dtype": "f64",
-        "tuned": {"worker_streams": streams, "steps_per_graph": gsteps, "tau_solve_partitions": tuned_parts},
+        "tuned": {"worker_streams": streams, "steps_per_graph": gsteps, "tau_solve_partitions": tuned_parts,
+                  "fused_form": tuned_fused, "stacked_group_plans": tuned_groups},
         "time_to_solution_ms": {"p50": agg["p50_ms"], "p99": agg["p99_ms"], "max": agg["total_ms"]},
         "wall_s": wall,
         "plain_gpu": {"value": agg["plain_value"], "unit": "instance-steps/s",

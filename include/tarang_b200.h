@@ -264,6 +264,14 @@ tb_status tb_ensemble_destroy(tb_ensemble* ens);
 tb_status tb_ensemble_tune(tb_ensemble* ens, const double* dt, int trial_steps, int* streams, int* graph_steps);
 tb_status tb_ensemble_set_config(tb_ensemble* ens, int streams, int graph_steps);
 tb_status tb_ensemble_config(const tb_ensemble* ens, int* streams, int* graph_steps);
+/* Form of a run: 0 per member (each member's step graphs on worker streams),
+ * 1 fused: members of one shape (Nx, Nz, domain, walls, RK222/RK443, FP64)
+ * at one dt are stacked along the mode axis into one plan per shape, so each
+ * kernel of a step covers the whole group in one launch (state gathered into
+ * and scattered from the group plan around a run); other members step per
+ * member.  tb_ensemble_tune chooses the form; groups reports the stacked plans. */
+tb_status tb_ensemble_set_form(tb_ensemble* ens, int fused);
+tb_status tb_ensemble_get_form(const tb_ensemble* ens, int* fused, int* groups);
 tb_status tb_ensemble_run(tb_ensemble* ens, const double* dt, int nsteps, float* member_ms, float* total_ms);
 
 /* -------------------------------------------------------------------------

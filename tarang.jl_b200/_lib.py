@@ -108,6 +108,8 @@ SIGNATURES = {
     "tb_ensemble_tune": (c_int, [c_void_p, c_void_p, c_int, POINTER(c_int), POINTER(c_int)]),
     "tb_ensemble_set_config": (c_int, [c_void_p, c_int, c_int]),
     "tb_ensemble_config": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
+    "tb_ensemble_set_form": (c_int, [c_void_p, c_int]),
+    "tb_ensemble_get_form": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
     "tb_ensemble_run": (c_int, [c_void_p, c_void_p, c_int, c_void_p, POINTER(c_float)]),
     "tb_turb_create": (c_int, [c_void_p, POINTER(tb_problem_desc), c_void_p, POINTER(c_void_p)]),
     "tb_turb_destroy": (c_int, [c_void_p]),

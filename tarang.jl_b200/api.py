@@ -442,6 +442,16 @@ class Ensemble:
         check(lib.tb_ensemble_config(self.ptr, byref(s), byref(g)), self.ctx)
         return s.value, g.value
 
+    def set_form(self, fused: bool) -> None:
+        """Fused: same-shape members stepped as one stacked plan per shape."""
+        check(lib.tb_ensemble_set_form(self.ptr, 1 if fused else 0), self.ctx)
+
+    def form(self):
+        """(fused, number of stacked group plans)."""
+        f, g = c_int(), c_int()
+        check(lib.tb_ensemble_get_form(self.ptr, byref(f), byref(g)), self.ctx)
+        return bool(f.value), g.value
+
     def run(self, dt, nsteps: int):
         d = self._dts(dt)
         ms = np.zeros(len(self.plans), dtype=np.float32)

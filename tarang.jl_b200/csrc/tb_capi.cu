@@ -197,6 +197,8 @@ TauArgs tau_args(tb_plan* P, int sy, FactorSet* f, const double2* rhsP) {
   a.rhs_off = P->sys[sy].rhs_off.as<int>();
   a.err_mode = P->err_mode.as<int>();
   a.ysave = P->solve_scratch.as<double>();
+  a.Nkm = P->Nkm;
+  a.mode0 = 0;
   return a;
 }
 
@@ -224,12 +226,22 @@ FactorSet* get_factors(tb_plan* P, int sy, double alpha, double beta) {
   TB_CUDA_TRY(cudaMemsetAsync(fs->SI.p, 0, fs->SI.bytes, P->st));
   const int nmax = std::max(S.lay.cls[0].n, S.lay.cls[1].n);
   DevBuf scratch;
-  scratch.alloc(tau_factor_scratch_doubles(nmax, Nk) * sizeof(double));
+  scratch.alloc(tau_factor_scratch_doubles(nmax, P->Nkm) * sizeof(double));
   int neg = 0x7fffffff;
   TB_CUDA_TRY(cudaMemcpyAsync(P->err_mode.p, &neg, sizeof(int), cudaMemcpyHostToDevice, P->st));
   TauArgs a = tau_args(P, sy, fs.get(), nullptr);
   a.scratch = scratch.as<double>();
-  launch_tau_factor(a, S.tau_parts, P->st);
+  for (int b = 0; b < P->B; ++b) {  // one factor launch per stacked instance (its own kappa, nu)
+    TauArgs ab = a;
+    ab.mode0 = b * P->Nkm;
+    if (P->B > 1)
+      for (int c = 0; c < 2; ++c) {
+        ab.cls[c].band = S.mband[2 * b + c].as<Coef>();
+        ab.cls[c].bord = S.mbord[2 * b + c].as<Coef>();
+      }
+    launch_tau_factor(ab, S.tau_parts, P->st);
+  }
+  launch_tau_transfer(a, S.tau_parts, P->st);
   check_launch("tau factor");
   int bad = 0;
   TB_CUDA_TRY(cudaMemcpyAsync(&bad, P->err_mode.p, sizeof(int), cudaMemcpyDeviceToHost, P->st));
@@ -327,7 +339,9 @@ void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
   xa.nptw = (int)(P->ptwM.bytes / sizeof(double2));
   xa.fp = P->fpM;
   xa.Nx = P->Nx;
-  xa.Nk = P->Nk;
+  xa.Nk = P->Nkm;
+  xa.ld = P->Nk;
+  xa.instances = P->B;
   xa.M = P->M;
   xa.Nz = N;
   xa.k0 = P->k0;
@@ -355,7 +369,7 @@ void enqueue_rk_step(tb_plan* P, double dt) {
   double2* X = P->X.as<double2>();
   const bool d3 = P->ndim == 3;
   timed(P, "mass_apply", [&] {
-    launch_mass_apply(X, P->MX0.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 0, P->nf, P->st);
+    launch_mass_apply(X, P->MX0.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 0, P->nf, P->st, P->Nkm);
   });
   int nk = 1;
   for (int i = 0; i < T.s; ++i) {
@@ -390,7 +404,8 @@ void enqueue_rk_step(tb_plan* P, double dt) {
       }
       timed(P, "lx_finalize", [&] {
         launch_lx_finalize(P->LXP[i].as<double2>(), X, P->s3.as<double>(), P->Nz, P->Nk, d3 ? 0 : P->Nx, P->k0, P->s,
-                           P->d.kappa, P->d.nu, beta, P->nf, P->st);
+                           P->d.kappa, P->d.nu, beta, P->nf, P->st, P->Nkm, P->kappa_m.as<double>(),
+                           P->nu_m.as<double>());
       });
       nk += 3;
       if (d3) {
@@ -470,7 +485,7 @@ void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
   // M X of the projected fields: 2D drops Im at the DC / Nyquist modes; 3D
   // subtracts M delta on the kx = 0 / Nyquist planes
   timed(P, "mass_apply", [&] {
-    launch_mass_apply(X, MXcur, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, d3 ? 0 : 1, P->nf, P->st);
+    launch_mass_apply(X, MXcur, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, d3 ? 0 : 1, P->nf, P->st, P->Nkm);
   });
   if (d3) {
     rbc3d_mx_project(P, MXcur);
@@ -694,7 +709,9 @@ size_t tb::plan_device_bytes(const tb_plan* P) {
     }
     for (const auto& f : S.factors) b += f->FR.bytes + f->BR.bytes + f->SI.bytes + f->PP.bytes + f->HR.bytes;
   }
-  b += rbc3d_device_bytes(P);
+  b += rbc3d_device_bytes(P) + P->kappa_m.bytes + P->nu_m.bytes;
+  for (const DevBuf& d : P->sys[0].mband) b += d.bytes;
+  for (const DevBuf& d : P->sys[0].mbord) b += d.bytes;
   const DevBuf* m32[] = {&P->X32,  &P->G32,  &P->H32,  &P->bEv32, &P->bOv32, &P->bEd32,
                          &P->bOd32, &P->fE32, &P->fO32, &P->sfE32, &P->sfO32, &P->ptwM32};
   for (const DevBuf* d : m32) b += d->bytes;
@@ -775,6 +792,20 @@ long long rhs_code(const tb_plan* P, int sy, int eq, int k) {
   return 2 * ((long long)4 * P->Nz + k) * P->Nk;
 }
 
+// Pad a class's band template to the compiled (kTauKL, kTauKU) shape.
+void pad_band(ClassLayout& L) {
+  TB_REQUIRE(L.kl <= kTauKL && L.ku <= kTauKU && L.nb <= 4, TB_ENOTSUPPORTED, "unexpected tau band shape");
+  if (L.kl == kTauKL && L.ku == kTauKU) return;
+  const int WC = kTauKL + kTauKU + 1;
+  std::vector<Coef> band((size_t)L.n * WC, Coef{0, 0, 0, 0});
+  for (int r = 0; r < L.n; ++r)
+    for (int d = 0; d < L.kl + L.ku + 1; ++d)
+      band[(size_t)r * WC + (d - L.kl + kTauKL)] = L.band[(size_t)r * (L.kl + L.ku + 1) + d];
+  L.band = band;
+  L.kl = kTauKL;
+  L.ku = kTauKU;
+}
+
 void install_system(tb_plan* P, int sy, TauLayout lay) {
   TauSystem& S = P->sys[sy];
   auto to_int = [](long long v) {
@@ -783,16 +814,7 @@ void install_system(tb_plan* P, int sy, TauLayout lay) {
   };
   for (int c = 0; c < 2; ++c) {
     ClassLayout& L = lay.cls[c];
-    TB_REQUIRE(L.kl <= kTauKL && L.ku <= kTauKU && L.nb <= 4, TB_ENOTSUPPORTED, "unexpected tau band shape");
-    // pad the band template to the compiled (kTauKL, kTauKU) shape
-    const int WC = kTauKL + kTauKU + 1;
-    std::vector<Coef> band((size_t)L.n * WC, Coef{0, 0, 0, 0});
-    for (int r = 0; r < L.n; ++r)
-      for (int d = 0; d < L.kl + L.ku + 1; ++d)
-        band[(size_t)r * WC + (d - L.kl + kTauKL)] = L.band[(size_t)r * (L.kl + L.ku + 1) + d];
-    L.band = band;
-    L.kl = kTauKL;
-    L.ku = kTauKU;
+    pad_band(L);
     auto to_short = [](const std::vector<int>& v) { return std::vector<short>(v.begin(), v.end()); };
     std::vector<int> cc(L.n), lc(L.nb);
     for (int j = 0; j < L.n; ++j) cc[j] = to_int(store_code(P, sy, L.col_unk[j], L.col_k[j]));
@@ -905,12 +927,18 @@ tb_status tb_context_destroy(tb_context* ctx) {
 
 const char* tb_last_error(const tb_context* ctx) { return ctx ? ctx->last_error.c_str() : g_err.c_str(); }
 
-tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan** out) {
-  if (!ctx || !out) return TB_EINVAL;
-  *out = nullptr;
-  std::unique_ptr<tb_plan> P(new (std::nothrow) tb_plan());
-  if (!P) return TB_ENOMEM;
-  tb_status s = guard(ctx, [&] {
+}  // extern "C"
+
+void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, int B) {
+  const tb_problem_desc* desc = descs;
+  TB_REQUIRE(B >= 1, TB_EINVAL, "no instances");
+  for (int b = 1; b < B; ++b)
+    TB_REQUIRE(descs[b].ndim == 2 && descs[0].ndim == 2 && descs[b].Nx == descs[0].Nx && descs[b].Nz == descs[0].Nz &&
+                   descs[b].Lx == descs[0].Lx && descs[b].Lz == descs[0].Lz &&
+                   descs[b].timestepper == descs[0].timestepper && descs[b].precision == TB_PREC_F64 &&
+                   descs[0].precision == TB_PREC_F64 && descs[b].b_bottom == descs[0].b_bottom &&
+                   descs[b].b_top == descs[0].b_top,
+               TB_EINVAL, "stacked instances must share the 2D shape, walls and stepper (FP64)");
     validate_desc(desc);
     TB_CUDA_TRY(cudaSetDevice(ctx->device));
     P->ctx = ctx;
@@ -920,7 +948,9 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
     P->Nz = desc->Nz;
     P->Kx = desc->Nx / 2 + 1;
     P->Ny = desc->ndim == 3 ? desc->Ny : 1;
-    P->Nk = P->Kx * P->Ny;
+    P->B = B;
+    P->Nkm = P->Kx * P->Ny;
+    P->Nk = P->Nkm * B;
     int M = (int)std::ceil(1.5 * desc->Nx);
     if (M % 2) ++M;
     P->M = M;
@@ -1009,10 +1039,29 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
     // tau systems: the coupled Boussinesq system (with |k| per mode in 3D) and,
     // in 3D, the decoupled cross-wavevector velocity
     const bool d3 = P->ndim == 3;
-    install_system(P.get(), 0,
+    install_system(P, 0,
                    build_rbc_layout(P->Nz, d3 ? desc->Lx * desc->Ly : desc->Lx, desc->Lz, desc->kappa, desc->nu,
                                     d3 ? (double)desc->Nx * desc->Ny : (double)desc->Nx, desc->b_bottom, desc->b_top));
-    if (d3) install_system(P.get(), 1, build_helmholtz_layout(P->Nz, desc->Lz, desc->nu));
+    if (B > 1) {
+      // instances differ only in kappa / nu: their band and border coefficients
+      P->sys[0].mband = std::vector<DevBuf>(2 * B);
+      P->sys[0].mbord = std::vector<DevBuf>(2 * B);
+      std::vector<double> km(B), nm(B);
+      for (int b = 0; b < B; ++b) {
+        TauLayout lb = build_rbc_layout(P->Nz, descs[b].Lx, descs[b].Lz, descs[b].kappa, descs[b].nu,
+                                        (double)descs[b].Nx, descs[b].b_bottom, descs[b].b_top);
+        for (int c = 0; c < 2; ++c) {
+          pad_band(lb.cls[c]);
+          upload(P->sys[0].mband[2 * b + c], lb.cls[c].band);
+          upload(P->sys[0].mbord[2 * b + c], lb.cls[c].bord);
+        }
+        km[b] = descs[b].kappa;
+        nm[b] = descs[b].nu;
+      }
+      upload(P->kappa_m, km);
+      upload(P->nu_m, nm);
+    }
+    if (d3) install_system(P, 1, build_helmholtz_layout(P->Nz, desc->Lz, desc->nu));
     P->nsys = d3 ? 2 : 1;
     TB_REQUIRE(rk_final_smem_bytes(P->Nz) <= 227 * 1024, TB_ENOTSUPPORTED, "Nz too large for the final RK update");
     P->err_mode.alloc(sizeof(int));
@@ -1031,7 +1080,7 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
       }
       P->tmpgrid.alloc(P->plane * sizeof(double2));
     } else {
-      rbc3d_setup(P.get());
+      rbc3d_setup(P);
     }
     P->MX0.alloc(P->nplanes * pb);
     const int nst = tableau(desc->timestepper).s;
@@ -1057,7 +1106,16 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
       TB_CUDA_TRY(cudaMemsetAsync(P->MXprev.p, 0, P->MXprev.bytes, P->st));
     }
     TB_CUDA_TRY(cudaStreamSynchronize(P->st));
-  });
+}
+
+extern "C" {
+
+tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan** out) {
+  if (!ctx || !out) return TB_EINVAL;
+  *out = nullptr;
+  std::unique_ptr<tb_plan> P(new (std::nothrow) tb_plan());
+  if (!P) return TB_ENOMEM;
+  tb_status s = guard(ctx, [&] { build_plan(P.get(), ctx, desc, 1); });
   if (s != TB_OK) return s;
   *out = P.release();
   return TB_OK;

@@ -10,6 +10,15 @@
 // graph launch covers (launch overhead against scheduling granularity).  The
 // tuner times candidate settings on the ensemble itself (from a snapshot that
 // is restored afterwards) and keeps the fastest.
+//
+// Fused form: members of one shape (Nx, Nz, domain, walls, RK stepper, FP64)
+// that step at the same dt are stacked along the mode axis into one plan
+// (build_plan with B instances): every kernel of a step then covers the whole
+// group in one launch - the tau solves over all the group's mode groups, the
+// transforms over all its columns - under one CUDA graph per group.  A run
+// gathers the members' states into the group plan, steps it, and scatters
+// the states back (one strided device copy per member each way).  The tuner
+// tries the fused form against the per-member form.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,16 +31,25 @@
 using namespace tb;
 
 struct tb_ensemble {
+  struct Group {
+    std::vector<int> idx;            // member indices (ascending)
+    std::unique_ptr<tb_plan> plan;   // the members stacked along the mode axis
+  };
   tb_context* ctx = nullptr;
   std::vector<tb_plan*> members;  // borrowed
   std::vector<double> work;       // relative cost of one step of each member
   int streams = 1;
   int graph_steps = 1;
+  bool fused = false;             // step same-shape members as stacked plans
+  std::vector<Group> groups;      // built on the first fused run
+  bool grouped = false;
   std::vector<cudaStream_t> ws;
   std::vector<cudaEvent_t> done;
   cudaEvent_t start = nullptr;
 
   ~tb_ensemble() {
+    for (auto s : ws) cudaStreamSynchronize(s);
+    groups.clear();
     for (auto s : ws) cudaStreamDestroy(s);
     for (auto e : done) cudaEventDestroy(e);
     if (start) cudaEventDestroy(start);
@@ -50,9 +68,135 @@ void ensure_streams(tb_ensemble* E, int n) {
   }
 }
 
+bool fusible(const tb_plan* P) {
+  return P->ndim == 2 && P->B == 1 && !P->mixed && !P->bc_dynamic && P->d.program == TB_PROGRAM_RBC &&
+         (P->d.timestepper == TB_RK222 || P->d.timestepper == TB_RK443);
+}
+
+bool same_shape(const tb_plan* a, const tb_plan* b) {
+  const tb_problem_desc &x = a->d, &y = b->d;
+  return x.Nx == y.Nx && x.Nz == y.Nz && x.Lx == y.Lx && x.Lz == y.Lz && x.timestepper == y.timestepper &&
+         x.b_bottom == y.b_bottom && x.b_top == y.b_top;
+}
+
+// Groups of at least two same-shape fusible members, each as a stacked plan.
+void build_groups(tb_ensemble* E) {
+  if (E->grouped) return;
+  const int n = (int)E->members.size();
+  std::vector<bool> taken(n, false);
+  for (int i = 0; i < n; ++i) {
+    if (taken[i] || !fusible(E->members[i])) continue;
+    tb_ensemble::Group G;
+    for (int j = i; j < n; ++j)
+      if (!taken[j] && fusible(E->members[j]) && same_shape(E->members[i], E->members[j])) G.idx.push_back(j);
+    if (G.idx.size() < 2) continue;
+    std::vector<tb_problem_desc> descs;
+    for (int j : G.idx) {
+      taken[j] = true;
+      descs.push_back(E->members[j]->d);
+    }
+    G.plan = std::make_unique<tb_plan>();
+    build_plan(G.plan.get(), E->ctx, descs.data(), (int)descs.size());
+    E->groups.push_back(std::move(G));
+  }
+  E->grouped = true;
+}
+
+// Copy the members' state rows (state planes and tau rows, Nkm modes each)
+// into / out of their columns of the group plan.
+void move_states(tb_ensemble* E, tb_ensemble::Group& G, cudaStream_t s, bool gather) {
+  tb_plan* Q = G.plan.get();
+  const size_t w = (size_t)Q->Nkm * sizeof(double2), ldq = (size_t)Q->Nk * sizeof(double2);
+  const size_t rows = (size_t)Q->nplanes * Q->Nz + Q->ntau;
+  for (size_t k = 0; k < G.idx.size(); ++k) {
+    tb_plan* M = E->members[G.idx[k]];
+    char* q = static_cast<char*>(Q->X.p) + k * w;
+    if (gather)
+      TB_CUDA_TRY(cudaMemcpy2DAsync(q, ldq, M->X.p, w, w, rows, cudaMemcpyDeviceToDevice, s));
+    else
+      TB_CUDA_TRY(cudaMemcpy2DAsync(M->X.p, w, q, ldq, w, rows, cudaMemcpyDeviceToDevice, s));
+  }
+}
+
+// Fused run: each group (members at one dt) as its stacked plan on its own
+// worker stream; members left over (other shapes, lone shapes, differing dt)
+// step per member on the streams after the groups.
+void run_fused(tb_ensemble* E, const double* dt, int nsteps, int streams, int gsteps, float* member_ms,
+               float* total_ms) {
+  build_groups(E);
+  const int n = (int)E->members.size();
+  std::vector<int> gi(n, -1);
+  std::vector<tb_ensemble::Group*> live;
+  for (auto& G : E->groups) {
+    bool same_dt = true;
+    for (int j : G.idx) same_dt = same_dt && dt[j] == dt[G.idx[0]];
+    if (!same_dt) continue;
+    for (int j : G.idx) gi[j] = (int)live.size();
+    live.push_back(&G);
+  }
+  std::vector<int> singles;
+  for (int i = 0; i < n; ++i)
+    if (gi[i] < 0) singles.push_back(i);
+  streams = std::max(1, std::min(std::max(streams, (int)live.size()), kMaxWorkerStreams));
+  ensure_streams(E, streams);
+  for (tb_plan* P : E->members) TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  std::vector<cudaEvent_t> gdone(live.size());
+  for (auto& e : gdone) TB_CUDA_TRY(cudaEventCreateWithFlags(&e, 0));
+  TB_CUDA_TRY(cudaEventRecord(E->start, E->ws[0]));
+  for (int s = 1; s < streams; ++s) TB_CUDA_TRY(cudaStreamWaitEvent(E->ws[s], E->start, 0));
+  for (size_t g = 0; g < live.size(); ++g) {
+    cudaStream_t s = E->ws[g % streams];
+    tb_plan* Q = live[g]->plan.get();
+    move_states(E, *live[g], s, true);
+    plan_launch_steps(Q, dt[live[g]->idx[0]], nsteps, s, gsteps);
+    move_states(E, *live[g], s, false);
+    TB_CUDA_TRY(cudaEventRecord(gdone[g], s));
+  }
+  // the lone members on the streams after the groups' (round-robin, as run)
+  std::vector<int> left(n, nsteps);
+  const int s0 = live.empty() ? 0 : (int)(live.size() % streams);
+  bool any = !singles.empty();
+  while (any) {
+    any = false;
+    for (size_t k = 0; k < singles.size(); ++k) {
+      const int i = singles[k];
+      if (left[i] <= 0) continue;
+      const int s = (s0 + (int)k) % streams;
+      const int chunk = std::min(left[i], gsteps);
+      plan_launch_steps(E->members[i], dt[i], chunk, E->ws[s], gsteps);
+      left[i] -= chunk;
+      if (left[i] == 0) TB_CUDA_TRY(cudaEventRecord(E->done[i], E->ws[s]));
+      any = true;
+    }
+  }
+  for (int s = 0; s < streams; ++s) TB_CUDA_TRY(cudaStreamSynchronize(E->ws[s]));
+  TB_CUDA_TRY(cudaGetLastError());
+  // members' counters follow their group plan's steps
+  for (size_t g = 0; g < live.size(); ++g)
+    for (int j : live[g]->idx) {
+      tb_plan* M = E->members[j];
+      M->sim_time += dt[j] * nsteps;
+      M->iteration += nsteps;
+      M->last_dt = dt[j];
+    }
+  float tmax = 0.f;
+  for (int i = 0; i < n; ++i) {
+    float ms = 0.f;
+    if (nsteps > 0) TB_CUDA_TRY(cudaEventElapsedTime(&ms, E->start, gi[i] >= 0 ? gdone[gi[i]] : E->done[i]));
+    if (member_ms) member_ms[i] = ms;
+    tmax = std::max(tmax, ms);
+  }
+  for (auto& e : gdone) cudaEventDestroy(e);
+  if (total_ms) *total_ms = tmax;
+}
+
 // One run of every member for nsteps on `streams` worker streams, graphs of
 // `gsteps` steps; per-member completion times (ms from the common start).
 void run(tb_ensemble* E, const double* dt, int nsteps, int streams, int gsteps, float* member_ms, float* total_ms) {
+  if (E->fused) {
+    run_fused(E, dt, nsteps, streams, gsteps, member_ms, total_ms);
+    return;
+  }
   const int n = (int)E->members.size();
   streams = std::max(1, std::min(streams, std::min(n, kMaxWorkerStreams)));
   ensure_streams(E, streams);
@@ -143,6 +287,19 @@ tb_status tb_ensemble_set_config(tb_ensemble* E, int streams, int graph_steps) {
   return TB_OK;
 }
 
+tb_status tb_ensemble_set_form(tb_ensemble* E, int fused) {
+  if (!E) return TB_EINVAL;
+  E->fused = fused != 0;
+  return TB_OK;
+}
+
+tb_status tb_ensemble_get_form(const tb_ensemble* E, int* fused, int* groups) {
+  if (!E) return TB_EINVAL;
+  if (fused) *fused = E->fused ? 1 : 0;
+  if (groups) *groups = (int)E->groups.size();
+  return TB_OK;
+}
+
 tb_status tb_ensemble_config(const tb_ensemble* E, int* streams, int* graph_steps) {
   if (!E) return TB_EINVAL;
   if (streams) *streams = E->streams;
@@ -162,40 +319,61 @@ tb_status tb_ensemble_tune(tb_ensemble* E, const double* dt, int trial_steps, in
     // tau-solve partitioning of the members: the partitioned solve has the
     // shortest latency for one plan, the one-warp solve the least work when
     // many plans share the GPU; both are tried when every member can run them
-    std::vector<int> cand_p;
-    for (int pc : {kTauParts, 1}) {
-      bool ok = true;
-      for (auto* m : E->members) ok = ok && plan_tau_parts_ok(m, pc);
-      if (ok) cand_p.push_back(pc);
-    }
+    // forms: per member, and fused (same-shape members stacked) when some
+    // shape has two or more fusible members
+    std::vector<bool> cand_f = {false};
+    for (int i = 0; i < n && cand_f.size() == 1; ++i)
+      for (int j = i + 1; j < n; ++j)
+        if (fusible(E->members[i]) && fusible(E->members[j]) && same_shape(E->members[i], E->members[j])) {
+          cand_f.push_back(true);
+          break;
+        }
     const int cand_s[] = {1, 2, 4, 8, 16, 32};
     const int cand_g[] = {1, 4, 16};
     float best = 1e30f;
     int bs = E->streams, bg = E->graph_steps, bp = E->members[0]->sys[0].tau_parts;
-    for (int pc : cand_p) {
-      for (auto* m : E->members) plan_set_variant(m, pc, 0);
-      // warm-up: factors and graphs of every member at this dt
-      run(E, dt, std::min(trial_steps, 2), std::min(n, 8), 1, nullptr, nullptr);
-      restore();
-      for (int g : cand_g) {
-        if (g > trial_steps) continue;
-        for (int s : cand_s) {
-          if (s > n || s > kMaxWorkerStreams) continue;
-          float tot = 0.f;
-          run(E, dt, trial_steps, s, g, nullptr, nullptr);  // captures this graph size
-          restore();
-          run(E, dt, trial_steps, s, g, nullptr, &tot);
-          restore();
-          if (tot < best) {
-            best = tot;
-            bs = s;
-            bg = g;
-            bp = pc;
+    bool bf = E->fused;
+    for (bool fz : cand_f) {
+      E->fused = fz;
+      if (fz) build_groups(E);
+      std::vector<tb_plan*> shaped(E->members.begin(), E->members.end());
+      if (fz)
+        for (auto& G : E->groups) shaped.push_back(G.plan.get());
+      std::vector<int> cand_p;
+      for (int pc : {kTauParts, 1}) {
+        bool ok = true;
+        for (auto* m : shaped) ok = ok && plan_tau_parts_ok(m, pc);
+        if (ok) cand_p.push_back(pc);
+      }
+      for (int pc : cand_p) {
+        for (auto* m : shaped) plan_set_variant(m, pc, 0);
+        // warm-up: factors and graphs of every member / group at this dt
+        run(E, dt, std::min(trial_steps, 2), std::min(n, 8), 1, nullptr, nullptr);
+        restore();
+        for (int g : cand_g) {
+          if (g > trial_steps) continue;
+          for (int s : cand_s) {
+            if (s > n || s > kMaxWorkerStreams) continue;
+            float tot = 0.f;
+            run(E, dt, trial_steps, s, g, nullptr, nullptr);  // captures this graph size
+            restore();
+            run(E, dt, trial_steps, s, g, nullptr, &tot);
+            restore();
+            if (tot < best) {
+              best = tot;
+              bs = s;
+              bg = g;
+              bp = pc;
+              bf = fz;
+            }
           }
         }
       }
     }
+    E->fused = bf;
     for (auto* m : E->members) plan_set_variant(m, bp, 0);
+    if (bf)
+      for (auto& G : E->groups) plan_set_variant(G.plan.get(), bp, 0);
     E->streams = bs;
     E->graph_steps = bg;
     if (streams) *streams = bs;

@@ -63,6 +63,8 @@ struct XProdArgs {
   FftPlan fp;            // length M plan
   int Nx, Nk, M, Nz;
   double k0;             // 2 pi / Lx
+  int ld;                // row stride of the planes (Nk, or instances x Nk in a batched plan)
+  int instances;         // instances stacked along the mode axis (grid.y)
 };
 void launch_xprod(const XProdArgs& a, cudaStream_t st);
 size_t xprod_smem_bytes(int M, int Nk, int nptw);
@@ -159,6 +161,10 @@ struct TauArgs {
   double* HR;
   double* scratch;     // factor workspace
   double* ysave;       // one-partition solve: [group][row][lane] y scratch (tau_solve_scratch_doubles)
+  // modes per instance (batched plans stack instances along the mode axis:
+  // mode m belongs to instance m / Nkm, its own mode m % Nkm); the
+  // factorisation runs per instance on modes mode0 .. mode0 + Nkm - 1
+  int Nkm, mode0;
   // dynamic wall values of b (null: constant BCs from bc_rhs): [bottom value,
   // bottom rate, top value, top rate][mode] at time *t_dev + bc_toff
   const double2* bcdyn;
@@ -166,8 +172,11 @@ struct TauArgs {
   double bc_toff;
   int* err_mode;       // first singular mode, or -1
 };
-// parts: kTauParts (partitioned solve, needs a.PP) or 1 (one warp per group)
+// parts: kTauParts (partitioned solve, needs a.PP) or 1 (one warp per group).
+// launch_tau_factor factors modes a.mode0 .. a.mode0 + a.Nkm - 1; the
+// partition responses (launch_tau_transfer) are then computed for all modes.
 void launch_tau_factor(const TauArgs& a, int parts, cudaStream_t st);
+void launch_tau_transfer(const TauArgs& a, int parts, cudaStream_t st);
 void launch_tau_solve(const TauArgs& a, int parts, cudaStream_t st);
 cudaError_t set_tau_smem_limits(int bytes);
 size_t tau_solve_smem_bytes(int npad, int parts);
@@ -190,11 +199,13 @@ void launch_advance_time(double* t, double dt, cudaStream_t st);
 // momentum rows in equation plane 4).
 // MX[e][k][m] = S X_f, cont rows zero; optional DC/Nyquist projection (2D).
 void launch_mass_apply(const double2* X, double2* MX, const double* s3, int Nz, int Nk, int Nx, int project,
-                       int nf, cudaStream_t st);
+                       int nf, cudaStream_t st, int Nkm = 0);
 // LX (in place over rhsP) = (rhsP - PM X)/beta, minus PL delta at the 2D
 // DC/Nyquist modes when Nx > 0 (3D passes Nx = 0 and corrects separately).
+// Batched plans: Nkm modes per instance, per-instance kappa / nu (null: the scalars).
 void launch_lx_finalize(double2* LX, const double2* X, const double* s3, int Nz, int Nk, int Nx, double k0,
-                        double s, double kappa, double nu, double beta, int nf, cudaStream_t st);
+                        double s, double kappa, double nu, double beta, int nf, cudaStream_t st, int Nkm = 0,
+                        const double* kappa_m = nullptr, const double* nu_m = nullptr);
 // X_f = S^{-1} (lincomb)[eq(f)] for the nf velocity-like fields; p and the ntau taus zeroed.
 void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* s3, int Nz, int Nk, int nf,
                      int ntau, cudaStream_t st);

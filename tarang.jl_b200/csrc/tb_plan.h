@@ -75,6 +75,7 @@ struct TauSystem {
   TauLayout lay;
   ClassTables ct[2];
   DevBuf rhs_off;  // [row][class] right-hand-side codes
+  std::vector<DevBuf> mband, mbord;  // stacked instances: band / border coefficients [instance][class]
   std::vector<std::unique_ptr<FactorSet>> factors;
   int tau_parts = 1;  // partitions of the solve (kTauParts or 1)
   int npad = 0;       // band rows padded to a multiple of kTauRowPad
@@ -116,6 +117,11 @@ struct tb_plan {
   // y-modes (ky in FFT order), Nk = Kx * Ny; the horizontal velocity is held as
   // (u_par, u_perp) along / across the wavevector (u_par in the u_x slot)
   int ndim = 2, Ny = 1, Kx = 0, My = 0;
+  // stacked instances (the fused ensemble form): B plans of one shape share the
+  // mode axis, instance b owning modes b Nkm .. (b+1) Nkm - 1 of Nk = B Nkm;
+  // their kappa / nu per instance (B = 1: a single plan, Nkm = Nk)
+  int B = 1, Nkm = 0;
+  DevBuf kappa_m, nu_m;
   int nplanes = 4;  // state planes before the taus: b, u_x|u_par, u_z, p (, u_perp)
   int ntau = 7;     // tau rows
   int nf = 3;       // velocity-like fields with a time derivative
@@ -204,6 +210,10 @@ struct tb_plan {
 };
 
 namespace tb {
+
+// Build a plan (tb_plan_create) or, for B > 1, one plan of B stacked 2D
+// instances of one shape (descs[0..B-1], differing only in kappa / nu).
+void build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, int B);
 
 // Device bytes the plan holds (state, work arrays, constants, factors).
 size_t plan_device_bytes(const tb_plan* P);

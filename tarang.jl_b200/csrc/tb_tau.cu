@@ -57,19 +57,19 @@ struct Strided {
 
 template <int KL, int KU>
 __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ml = blockIdx.x * blockDim.x + threadIdx.x;  // mode within this instance
   const int c = blockIdx.y;
-  if (m >= a.Nk) return;
+  if (ml >= a.Nkm) return;
+  const int m = a.mode0 + ml;
   const ClassDev& C = a.cls[c];
   const int n = C.n, nb = C.nb;
   constexpr int WW = 2 * KL + KU + 1;
   constexpr int W1 = KL + KU + 1;
-  const int Nk = a.Nk;
-  const double kx = a.kmag ? a.kmag[m] : a.k0 * m;
-  const bool zmode = (m == 0);
-  // per-thread work arrays interleaved across the 2 Nk threads (element i of a
-  // thread at scratch[i * 2Nk + t]) so that a warp's accesses coalesce
-  const size_t T = (size_t)2 * Nk, t = (size_t)c * Nk + m;
+  const double kx = a.kmag ? a.kmag[m] : a.k0 * ml;
+  const bool zmode = (ml == 0);
+  // per-thread work arrays interleaved across the 2 Nkm threads (element i of
+  // a thread at scratch[i * 2Nkm + t]) so that a warp's accesses coalesce
+  const size_t T = (size_t)2 * a.Nkm, t = (size_t)c * a.Nkm + ml;
   const Strided W{a.scratch + t, T};
   const Strided Bd{a.scratch + t + (size_t)nmax * WW * T, T};
   const Strided Cr{a.scratch + t + ((size_t)nmax * WW + (size_t)nmax * NBMAX) * T, T};
@@ -365,7 +365,8 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   };
 #pragma unroll
   for (int b = 0; b < NBMAX; ++b)
-    z[b] = (warp == 0 && part == 0 && m == 0 && b < a.cls[c].nb) ? a.beta * a.cls[c].bc_rhs[b] : 0.0;
+    z[b] = (warp == 0 && part == 0 && m < Nk && m % a.Nkm == 0 && b < a.cls[c].nb) ? a.beta * a.cls[c].bc_rhs[b]
+                                                                                   : 0.0;
   if (a.bcdyn != nullptr && warp == 0 && m < Nk) {
     // dynamic wall values of b: boundary row 0 of class c is the parity-c
     // combination of the walls, (top + bottom)/2 (c = 0) or (top - bottom)/2,
@@ -787,11 +788,12 @@ __global__ void k_advance_time(double* t, double dt) { *t += dt; }
 
 __global__ void __launch_bounds__(128) k_mass_apply(const double2* __restrict__ X, double2* __restrict__ MX,
                                                     const double* __restrict__ s3, int Nz, int Nk, int Nx,
-                                                    int project, int nf) {
+                                                    int project, int nf, int Nkm) {
   const int k = blockIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= Nk) return;
   const size_t i = (size_t)k * Nk + m;
-  const bool pj = project && (m == 0 || 2 * m == Nx);
+  const int ml = m % Nkm;  // mode within its instance
+  const bool pj = project && (ml == 0 || 2 * ml == Nx);
   const double s0 = s3[3 * k], s1 = s3[3 * k + 1], s2 = s3[3 * k + 2];
   MX[i] = make_double2(0.0, 0.0);
   for (int f = 0; f < nf; ++f) {
@@ -807,7 +809,9 @@ __global__ void __launch_bounds__(128) k_mass_apply(const double2* __restrict__ 
 // One thread per (row k, mode m): grid (ceil(Nk / 128), Nz).
 __global__ void __launch_bounds__(128) k_lx_finalize(double2* __restrict__ LX, const double2* __restrict__ X,
                                                      const double* __restrict__ s3, int Nz, int Nk, int Nx, double k0,
-                                                     double s, double kappa, double nu, double beta, int nf) {
+                                                     double s, double kappa, double nu, double beta, int nf, int Nkm,
+                                                     const double* __restrict__ kappa_m,
+                                                     const double* __restrict__ nu_m) {
   const double ib = 1.0 / beta;
   {
     const int k = blockIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -840,9 +844,14 @@ __global__ void __launch_bounds__(128) k_lx_finalize(double2* __restrict__ LX, c
       const double2 mx = Sx(4);
       LX[4 * plane + i] = make_double2((r.x - mx.x) * ib, (r.y - mx.y) * ib);
     }
-    if (Nx > 0 && (m == 0 || 2 * m == Nx)) {
+    const int ml = m % Nkm;  // mode within its instance
+    if (Nx > 0 && (ml == 0 || 2 * ml == Nx)) {
       // L applied to delta = i Im(X) of b, ux, uz (the part a grid round trip drops)
-      const double kx = k0 * m, kx2 = kx * kx;
+      const double kx = k0 * ml, kx2 = kx * kx;
+      if (kappa_m) {
+        kappa = kappa_m[m / Nkm];
+        nu = nu_m[m / Nkm];
+      }
       auto dl = [&](int f, int kk) -> double { return (kk < Nz) ? X[((size_t)f * Nz + kk) * Nk + m].y : 0.0; };
       auto Sd = [&](int f) -> double { return s0 * dl(f, k) + s1 * dl(f, k + 2) + s2 * dl(f, k + 4); };
       const double d2 = 2.0 * (k + 2) * s * s;
@@ -929,9 +938,14 @@ __global__ void __launch_bounds__(256) k_rk_final(LinComb lc, double2* __restric
 
 template <int KL, int KU>
 void factor_impl(const TauArgs& a, int parts, cudaStream_t st) {
+  (void)parts;
   int nmax = a.cls[0].n > a.cls[1].n ? a.cls[0].n : a.cls[1].n;
-  dim3 grid((a.Nk + 63) / 64, 2);
+  dim3 grid((a.Nkm + 63) / 64, 2);
   k_tau_factor<KL, KU><<<grid, 64, 0, st>>>(a, nmax);
+}
+
+template <int KL, int KU>
+void transfer_impl(const TauArgs& a, int parts, cudaStream_t st) {
   // one partition: the sweeps need no transfer responses (B1 stores x directly)
   const int tgx = (a.Nk + 127) / 128;
   if (parts == kTauParts) k_tau_transfer<KL, KU, kTauParts><<<dim3(tgx, 2 * kTauParts, 16), 128, 0, st>>>(a);
@@ -999,6 +1013,9 @@ size_t tau_response_doubles(int Nk, int npad, int parts) {
 // Supported band shape: the RBC layout gives kl = 4, ku = 8 for every Nz >= 8
 // (narrower layouts are zero-padded to it by the plan).
 void launch_tau_factor(const TauArgs& a, int parts, cudaStream_t st) { factor_impl<kTauKL, kTauKU>(a, parts, st); }
+void launch_tau_transfer(const TauArgs& a, int parts, cudaStream_t st) {
+  transfer_impl<kTauKL, kTauKU>(a, parts, st);
+}
 void launch_tau_solve(const TauArgs& a, int parts, cudaStream_t st) { solve_impl<kTauKL, kTauKU>(a, parts, st); }
 
 size_t tau_factor_scratch_doubles(int nmax, int Nk) {
@@ -1027,15 +1044,17 @@ void launch_lincomb(const LinComb& lc, double2* out, long long count, cudaStream
 void launch_advance_time(double* t, double dt, cudaStream_t st) { k_advance_time<<<1, 1, 0, st>>>(t, dt); }
 
 void launch_mass_apply(const double2* X, double2* MX, const double* s3, int Nz, int Nk, int Nx, int project,
-                       int nf, cudaStream_t st) {
+                       int nf, cudaStream_t st, int Nkm) {
   dim3 grid((Nk + 127) / 128, Nz);
-  k_mass_apply<<<grid, 128, 0, st>>>(X, MX, s3, Nz, Nk, Nx, project, nf);
+  k_mass_apply<<<grid, 128, 0, st>>>(X, MX, s3, Nz, Nk, Nx, project, nf, Nkm > 0 ? Nkm : Nk);
 }
 
 void launch_lx_finalize(double2* LX, const double2* X, const double* s3, int Nz, int Nk, int Nx, double k0,
-                        double s, double kappa, double nu, double beta, int nf, cudaStream_t st) {
+                        double s, double kappa, double nu, double beta, int nf, cudaStream_t st, int Nkm,
+                        const double* kappa_m, const double* nu_m) {
   dim3 grid((Nk + 127) / 128, Nz);
-  k_lx_finalize<<<grid, 128, 0, st>>>(LX, X, s3, Nz, Nk, Nx, k0, s, kappa, nu, beta, nf);
+  k_lx_finalize<<<grid, 128, 0, st>>>(LX, X, s3, Nz, Nk, Nx, k0, s, kappa, nu, beta, nf, Nkm > 0 ? Nkm : Nk, kappa_m,
+                                      nu_m);
 }
 
 void launch_rk_final(const LinComb& lc, double2* X, double2* tau, const double* s3, int Nz, int Nk, int nf,

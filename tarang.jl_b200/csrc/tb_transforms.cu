@@ -469,7 +469,9 @@ __global__ void __launch_bounds__(256, 2) k_xprod(XProdArgs a) {
   const int z = blockIdx.x;
   const int zm = a.Nz - 1 - z;
   const bool lower = z <= zm;
-  const size_t rr = (size_t)(lower ? z : zm) * Nk;
+  // instance blockIdx.y of a batched plan: its Nk modes start at column y * Nk
+  const size_t ld = a.ld > 0 ? (size_t)a.ld : (size_t)Nk, col0 = (size_t)blockIdx.y * Nk;
+  const size_t rr = (size_t)(lower ? z : zm) * ld + col0;
   auto value = [&](int f, int q) -> double2 {
     const double2 e = a.ev[f][rr + q], o = a.ov[f][rr + q];
     return lower ? make_double2(e.x + o.x, e.y + o.y) : make_double2(e.x - o.x, e.y - o.y);
@@ -535,7 +537,7 @@ __global__ void __launch_bounds__(256, 2) k_xprod(XProdArgs a) {
       // it touches neither C1 nor P's partner, so both proceed before one barrier
       double2* C2 = fft_cta_pt<true>(Q, U, a.fp, tw, -1);
       const double sc = 1.0 / ((double)M * (double)N);
-      const size_t ro = (size_t)z * Nk;
+      const size_t ro = (size_t)z * ld + col0;
       for (int k = threadIdx.x; k < Nk; k += blockDim.x) {
         const double2 c = C1[fidx<true>(k)];
         const double2 cm = C1[fidx<true>((M - k) % M)];
@@ -696,7 +698,7 @@ size_t xprod_smem_bytes(int M, int Nk, int nptw) {
 
 void launch_xprod(const XProdArgs& a, cudaStream_t st) {
   size_t smem = xprod_smem_bytes(a.M, a.Nk, a.nptw);
-  k_xprod<<<a.Nz, 256, smem, st>>>(a);
+  k_xprod<<<dim3(a.Nz, a.instances > 0 ? a.instances : 1), 256, smem, st>>>(a);
 }
 
 void launch_x_rfft(const double* grid, double2* spec, int nrows, int Nx, const FftPlan& fp, const double2* tw,

@@ -95,3 +95,60 @@ def test_async_steps_equal_sync_steps(tb):
     for x, y in zip(states(a), states(b)):
         assert np.array_equal(x, y)
     assert b.device_bytes() > 0
+
+
+# same shapes with different Ra / Pr (fusible groups), plus lone shapes
+FUSED = [
+    (32, 16, 2e6, "RK222", 0.05),
+    (64, 24, 1e7, "RK443", 0.01),
+    (32, 16, 1e5, "RK222", 0.05),
+    (64, 24, 3e6, "RK443", 0.01),
+    (32, 16, 5e6, "RK222", 0.05),
+    (48, 17, 1e6, "RK222", 0.05),   # lone shape: steps per member
+    (64, 24, 1e8, "RK443", 0.01),
+]
+
+
+def test_fused_form_matches_solo_runs_and_oracle(tb):
+    nsteps = 5
+    solo = []
+    for k, spec in enumerate(FUSED):
+        _, plan = build(tb, spec, 70 + k)
+        plan.step(spec[4], nsteps)
+        solo.append(states(plan))
+    pairs = [build(tb, spec, 70 + k) for k, spec in enumerate(FUSED)]
+    plans = [pl for _, pl in pairs]
+    ens = tb.Ensemble(plans)
+    ens.set_form(True)
+    ens.set_config(2, 2)
+    ms, total = ens.run([s[4] for s in FUSED], nsteps)
+    fused, groups = ens.form()
+    assert fused and groups == 2
+    for k, plan in enumerate(plans):
+        for a, b in zip(states(plan), solo[k]):
+            assert rel_l2(a, b) < 1e-12, f"member {k}"
+        assert abs(plan.sim_time() - nsteps * FUSED[k][4]) < 1e-12
+    # and the stacked plans hold each member's own kappa / nu
+    for k in (0, 1, 3):
+        p, _ = pairs[k]
+        ref = run_rbc(p, FUSED[k][3], FUSED[k][4], nsteps, seed=70 + k)
+        assert rel_l2(plans[k].get_state(0), ref.b) < 1e-10
+        assert rel_l2(plans[k].get_state(2), ref.uz) < 1e-10
+    # a second run continues from the scattered states
+    ens.run([s[4] for s in FUSED], 2)
+    _, again = build(tb, FUSED[2], 72)
+    again.step(FUSED[2][4], nsteps + 2)
+    assert rel_l2(plans[2].get_state(0), again.get_state(0)) < 1e-12
+
+
+def test_tuner_may_choose_the_fused_form(tb):
+    plans = [build(tb, spec, 90 + k)[1] for k, spec in enumerate(FUSED)]
+    before = [pl.get_state(0) for pl in plans]
+    ens = tb.Ensemble(plans)
+    ens.tune([s[4] for s in FUSED], trial_steps=2)
+    fused, groups = ens.form()
+    assert groups in (0, 2)
+    for pl, b in zip(plans, before):
+        assert np.array_equal(pl.get_state(0), b)
+    ens.run([s[4] for s in FUSED], 2)
+    assert all(np.isfinite(pl.get_state(0)).all() for pl in plans)
