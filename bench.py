@@ -12,7 +12,7 @@ device time is the max over ranks.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints one JSON line (rank 0).  `--impl reference` times the CPU restatement of
-the reference's algorithm (oracle/, NumPy + SciPy SuperLU, single thread) on the
+the reference's algorithm (oracle/, NumPy + SciPy SuperLU, all host threads) on the
 same workload.
 """
 from __future__ import annotations
@@ -230,13 +230,22 @@ def kernel_work(name: str, cfg, scheme: str):
     return "bytes", None
 
 
+def host_threads() -> int:
+    """Host cores this process may run on (the CPU legs use all of them)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 # ---------------------------------------------------------------------------
 def run_reference(args, cfg, scheme, dist):
     """CPU restatement of the reference's algorithm, timed on the host cores."""
     if dist.rank != 0:
         return
-    from oracle.tarang_oracle import RBCParams, run_rbc, rbc_initial_b, RBC2D
+    from oracle.tarang_oracle import RBCParams, run_rbc, rbc_initial_b, RBC2D, set_threads
 
+    threads = set_threads(host_threads())
     p = RBCParams(Nx=cfg.Nx, Nz=cfg.Nz, Lx=cfg.Lx, Lz=cfg.Lz, Ra=cfg.Ra, Pr=cfg.Pr)
     sim = RBC2D(p)
     sim.set_b_grid(rbc_initial_b(p, cfg.seed))
@@ -265,11 +274,12 @@ def run_reference(args, cfg, scheme, dist):
         "cpu_baseline": {
             "value": v,
             "unit": "steps/s",
-            "cores": 1,
+            "cores": threads,
             "kind": "port",
             "sample": f"{args.steps} steps after {args.warmup} warm-up steps (the first factors the tau LHS) "
                       f"of the full {cfg.Nx}x{cfg.Nz} problem; NumPy/SciPy restatement (SuperLU per mode), "
-                      "single thread; Julia is absent so the reference itself cannot run",
+                      f"{threads} host threads (pocketfft workers, per-mode solves on a thread pool); "
+                      "Julia is absent so the reference itself cannot run",
         },
         "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -295,8 +305,9 @@ def workload_config(cfg, scheme, args):
 
 
 def cpu_baseline(cfg, scheme, nsteps):
-    from oracle.tarang_oracle import RBCParams, RBC2D, rbc_initial_b
+    from oracle.tarang_oracle import RBCParams, RBC2D, rbc_initial_b, set_threads
 
+    threads = set_threads(host_threads())
     p = RBCParams(Nx=cfg.Nx, Nz=cfg.Nz, Lx=cfg.Lx, Lz=cfg.Lz, Ra=cfg.Ra, Pr=cfg.Pr)
     sim = RBC2D(p)
     sim.set_b_grid(rbc_initial_b(p, cfg.seed))
@@ -308,10 +319,11 @@ def cpu_baseline(cfg, scheme, nsteps):
     return {
         "value": nsteps / el,
         "unit": "steps/s",
-        "cores": 1,
+        "cores": threads,
         "kind": "port",
         "sample": f"{nsteps} steps of the full {cfg.Nx}x{cfg.Nz} {scheme} problem after one warm-up step; "
-                  "NumPy/SciPy restatement of the reference CPU path (SuperLU per Fourier mode), single thread",
+                  "NumPy/SciPy restatement of the reference CPU path (SuperLU per Fourier mode), "
+                  f"{threads} host threads (pocketfft workers, per-mode solves on a thread pool)",
     }
 
 
@@ -644,8 +656,9 @@ def cpu_baseline_3d(c, nz_sample: int = 16, mode_sample: int = 48):
     on a spread sample of Fourier modes (scaled to all modes)."""
     import numpy as np
 
-    from oracle.tarang_oracle import RBC3D, RBC3Params, rbc3_initial_b
+    from oracle.tarang_oracle import RBC3D, RBC3Params, _pmap, rbc3_initial_b, set_threads
 
+    threads = set_threads(host_threads())
     ps = RBC3Params(Nx=c.Nx, Ny=c.Ny, Nz=nz_sample, Lx=c.Lx, Ly=c.Ly, Lz=c.Lz, Ra=c.Ra, Pr=c.Pr)
     sim = RBC3D(ps)
     sim.set_b_grid(rbc3_initial_b(ps, c.seed, c.noise))
@@ -658,30 +671,33 @@ def cpu_baseline_3d(c, nz_sample: int = 16, mode_sample: int = 48):
     simf = RBC3D(pf)
     nk = (c.Nx // 2 + 1) * c.Ny
     beta = c.dt * (1.0 - 1.0 / math.sqrt(2.0))
-    picks = [(int(i) % c.Ny, (int(i) // c.Ny) % (c.Nx // 2 + 1)) for i in np.linspace(0, nk - 1, mode_sample)]
-    t_fac = t_sol = 0.0
-    for iy, ix in picks:
-        M, L, bc, af = simf.mode_matrices(iy, ix)
-        t0 = time.perf_counter()
-        lu = simf._lhs_lu(iy, ix, 1.0, beta)
-        t1 = time.perf_counter()
-        rhs = rng.standard_normal(M.shape[0]) + 0j
-        x = lu.solve(rhs)
-        _ = L @ x
-        t_sol += time.perf_counter() - t1
-        t_fac += t1 - t0
-    t_sol_all = t_sol * nk / mode_sample
+    nsample = max(mode_sample, 4 * threads)
+    picks = [(int(i) % c.Ny, (int(i) // c.Ny) % (c.Nx // 2 + 1)) for i in np.linspace(0, nk - 1, nsample)]
+    rhs = {m: rng.standard_normal(simf.mode_matrices(*m)[0].shape[0]) + 0j for m in picks}
+    t0 = time.perf_counter()
+    lus = dict(zip(picks, _pmap(lambda m: simf._lhs_lu(*m, 1.0, beta), picks)))
+    t_fac = time.perf_counter() - t0
+
+    def solve(m):
+        x = lus[m].solve(rhs[m])
+        return simf.mode_matrices(*m)[1] @ x
+
+    t0 = time.perf_counter()
+    _pmap(solve, picks)
+    t_sol = time.perf_counter() - t0
+    t_sol_all = t_sol * nk / nsample
     step_s = 2 * t_rhs + 2 * t_sol_all
     return {
         "value": 1.0 / step_s,
         "unit": "steps/s",
-        "cores": 1,
+        "cores": threads,
         "kind": "port",
         "sample": f"one RHS evaluation on a {c.Nx}x{c.Ny}x{nz_sample} slab (scaled by {c.Nz}/{nz_sample}) and the "
-                  f"per-mode SuperLU solve + L x of {mode_sample} of the {nk} Fourier modes at full n = "
+                  f"per-mode SuperLU solve + L x of {nsample} of the {nk} Fourier modes at full n = "
                   f"{5 * c.Nz + 9} (scaled to all modes), combined for one RK222 step (2 RHS, 2 solve passes); "
-                  f"the one-time factorisation ({t_fac * nk / mode_sample:.0f} s for all modes) is excluded; "
-                  "NumPy/SciPy restatement, single thread",
+                  f"the one-time factorisation ({t_fac * nk / nsample:.0f} s for all modes) is excluded; "
+                  f"NumPy/SciPy restatement, {threads} host threads (pocketfft workers, per-mode solves "
+                  "on a thread pool)",
         "rhs_s": t_rhs,
         "solves_s": t_sol_all,
     }

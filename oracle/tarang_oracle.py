@@ -31,6 +31,62 @@ import scipy.sparse as sps
 import scipy.sparse.linalg as spsl
 
 # ---------------------------------------------------------------------------
+# Host threads.  The reference runs FFTW with TARANG_FFTW_THREADS threads and
+# Julia tasks (src/core/runtime/runtime_init.jl:24-57); here pocketfft takes
+# ``workers`` threads and the per-mode loops (independent sparse solves and
+# mat-vecs, which release the GIL inside SuperLU) run on a thread pool.  The
+# arithmetic of every mode is the same whatever the thread count.
+# ---------------------------------------------------------------------------
+_WORKERS = 1
+_POOL = None
+
+
+def set_threads(n: int) -> int:
+    """Use n host threads for FFTs and per-mode loops (1 = serial); returns n."""
+    global _WORKERS, _POOL
+    n = max(1, int(n))
+    if _POOL is not None:
+        _POOL.shutdown(wait=True)
+        _POOL = None
+    _WORKERS = n
+    if n > 1:
+        from concurrent.futures import ThreadPoolExecutor
+
+        _POOL = ThreadPoolExecutor(max_workers=n)
+    return n
+
+
+def get_threads() -> int:
+    return _WORKERS
+
+
+def _pmap(fn, items) -> list:
+    """[fn(x) for x in items], on the thread pool when one is set."""
+    items = list(items)
+    if _POOL is None or len(items) < 2:
+        return [fn(x) for x in items]
+    nchunk = min(len(items), 4 * _WORKERS)
+    bounds = [len(items) * i // nchunk for i in range(nchunk + 1)]
+    parts = _POOL.map(lambda i: [fn(x) for x in items[bounds[i] : bounds[i + 1]]], range(nchunk))
+    return [y for part in parts for y in part]
+
+
+class _FFTThreads:
+    """scipy.fft with the current worker count (same pocketfft arithmetic)."""
+
+    def __getattr__(self, name):
+        f = getattr(sfft, name)
+
+        def call(*args, **kw):
+            kw.setdefault("workers", _WORKERS)
+            return f(*args, **kw)
+
+        return call
+
+
+_fx = _FFTThreads()
+
+# ---------------------------------------------------------------------------
 # Grids and wavenumbers
 # ---------------------------------------------------------------------------
 
@@ -67,8 +123,8 @@ def cheb_forward(g: np.ndarray, axis: int = 0) -> np.ndarray:
     map is real-linear).
     """
     N = g.shape[axis]
-    out = sfft.dct(np.real(g), type=1, axis=axis) + (
-        1j * sfft.dct(np.imag(g), type=1, axis=axis) if np.iscomplexobj(g) else 0.0
+    out = sfft.dct(np.real(g), type=1, axis=axis, workers=_WORKERS) + (
+        1j * sfft.dct(np.imag(g), type=1, axis=axis, workers=_WORKERS) if np.iscomplexobj(g) else 0.0
     )
     out = np.asarray(out) / (N - 1)
     sl = [slice(None)] * out.ndim
@@ -92,8 +148,8 @@ def cheb_backward(c: np.ndarray, axis: int = 0) -> np.ndarray:
     s[tuple(sl)] *= 2.0
     sl[axis] = N - 1
     s[tuple(sl)] *= 2.0
-    out = sfft.dct(np.real(s), type=1, axis=axis) + (
-        1j * sfft.dct(np.imag(s), type=1, axis=axis) if np.iscomplexobj(s) else 0.0
+    out = sfft.dct(np.real(s), type=1, axis=axis, workers=_WORKERS) + (
+        1j * sfft.dct(np.imag(s), type=1, axis=axis, workers=_WORKERS) if np.iscomplexobj(s) else 0.0
     )
     return np.asarray(out) / 2.0
 
@@ -104,14 +160,14 @@ def forward_2d(g: np.ndarray) -> np.ndarray:
     RealFourier first (unnormalised rfft, transform_fourier.jl:7-31), then
     ChebyshevT along z (the reference's forward order, mixed_transforms.jl:229-330).
     """
-    return cheb_forward(np.fft.rfft(g, axis=1), axis=0)
+    return cheb_forward(_fx.rfft(g, axis=1), axis=0)
 
 
 def backward_2d(c: np.ndarray, Nx: int) -> np.ndarray:
     """Coefficients (Nz, Nk) -> grid (Nz, Nx).  irfft divides by N and, like
     FFTW's c2r, ignores the imaginary parts of the DC and Nyquist bins
     (transform_fourier.jl:287-313)."""
-    return np.fft.irfft(cheb_backward(c, axis=0), n=Nx, axis=1)
+    return _fx.irfft(cheb_backward(c, axis=0), n=Nx, axis=1)
 
 
 # ---------------------------------------------------------------------------
@@ -182,7 +238,7 @@ def padded_multiply(a: np.ndarray, b: np.ndarray, factor: float = 1.5) -> np.nda
     n_neg = N - Nh - 1
 
     def pad(x):
-        s = np.fft.fft(x.astype(complex), axis=1)
+        s = _fx.fft(x.astype(complex), axis=1)
         p = np.zeros((x.shape[0], M), dtype=complex)
         p[:, : Nh + 1] = s[:, : Nh + 1]
         if n_neg > 0:
@@ -190,17 +246,17 @@ def padded_multiply(a: np.ndarray, b: np.ndarray, factor: float = 1.5) -> np.nda
         if N % 2 == 0 and M > N:
             p[:, Nh] *= 0.5
             p[:, M - Nh] = p[:, Nh]
-        return np.fft.ifft(p, axis=1)
+        return _fx.ifft(p, axis=1)
 
     prod = pad(a) * pad(b)
-    P = np.fft.fft(prod, axis=1)
+    P = _fx.fft(prod, axis=1)
     if N % 2 == 0 and M > N:
         P[:, Nh] += P[:, M - Nh]
     R = np.zeros((a.shape[0], N), dtype=complex)
     R[:, : Nh + 1] = P[:, : Nh + 1]
     if n_neg > 0:
         R[:, N - n_neg :] = P[:, M - n_neg :]
-    r = np.fft.ifft(R, axis=1)
+    r = _fx.ifft(R, axis=1)
     return np.real(r) * (M / N)
 
 
@@ -532,13 +588,13 @@ class RBC2D:
         s = ts["AE"].shape[0]
         AE, AI, bE, bI = ts["AE"], ts["AI"], ts["bE"], ts["bI"]
         x0 = [self.gather(m, *self.fields()) for m in range(Nk)]
-        MX0 = [self.mode_matrices(m)[0] @ x0[m] for m in range(Nk)]
+        MX0 = _pmap(lambda m: self.mode_matrices(m)[0] @ x0[m], range(Nk))
         F: List[List[np.ndarray]] = []
         LX: List[List[np.ndarray]] = []
         for i in range(s):
             a_ii = AI[i, i]
-            xs = []
-            for m in range(Nk):
+
+            def stage_solve(m):
                 M, L, bc, algf = self.mode_matrices(m)
                 rhs = MX0[m].copy()
                 for j in range(i):
@@ -547,28 +603,32 @@ class RBC2D:
                     if abs(dt * AI[i, j]) > 1e-14:
                         rhs -= dt * AI[i, j] * LX[j][m]
                 if abs(a_ii) < 1e-14:
-                    x = self.mass_solve(m, rhs)
-                else:
-                    algf = self._stage_algf(m, algf, self.sim_time + dt * ts["c"][i])
-                    rhs[bc] = dt * a_ii * algf[bc]
-                    x = self._lhs_lu(m, 1.0, dt * a_ii).solve(rhs)
-                xs.append(x)
+                    return self.mass_solve(m, rhs)
+                algf = self._stage_algf(m, algf, self.sim_time + dt * ts["c"][i])
+                rhs[bc] = dt * a_ii * algf[bc]
+                return self._lhs_lu(m, 1.0, dt * a_ii).solve(rhs)
+
+            xs = _pmap(stage_solve, range(Nk))
             for m in range(Nk):
                 self.scatter(m, xs[m], *self.fields())
             Fb, Fux, Fuz = self.rhs(self.b, self.ux, self.uz)
             pb, pux, puz = (self.projected(c) for c in (self.b, self.ux, self.uz))
-            F.append([self.equation_F(m, Fb, Fux, Fuz) for m in range(Nk)])
-            LX.append(
-                [self.mode_matrices(m)[1] @ self.gather(m, pb, pux, puz, self.pr, self.tau) for m in range(Nk)]
-            )
-        for m in range(Nk):
+            F.append(_pmap(lambda m: self.equation_F(m, Fb, Fux, Fuz), range(Nk)))
+            LX.append(_pmap(lambda m: self.mode_matrices(m)[1] @ self.gather(m, pb, pux, puz, self.pr, self.tau),
+                            range(Nk)))
+
+        def final(m):
             rhs = MX0[m].copy()
             for j in range(s):
                 if abs(dt * bE[j]) > 1e-14:
                     rhs += dt * bE[j] * F[j][m]
                 if abs(dt * bI[j]) > 1e-14:
                     rhs -= dt * bI[j] * LX[j][m]
-            self.scatter(m, self.mass_solve(m, rhs), *self.fields())
+            return self.mass_solve(m, rhs)
+
+        xs = _pmap(final, range(Nk))
+        for m in range(Nk):
+            self.scatter(m, xs[m], *self.fields())
         self.sim_time += dt
         self.iteration += 1
 
@@ -579,14 +639,11 @@ class RBC2D:
         a, bcoef, c = sbdf_coefs(use_order, dt, self._ms_dt_prev)
         Fb, Fux, Fuz = self.rhs(self.b, self.ux, self.uz)
         pb, pux, puz = (self.projected(cf) for cf in (self.b, self.ux, self.uz))
-        MXc, Fc = [], []
-        for m in range(Nk):
-            M = self.mode_matrices(m)[0]
-            MXc.append(M @ self.gather(m, pb, pux, puz, self.pr, self.tau))
-            Fc.append(self.equation_F(m, Fb, Fux, Fuz))
+        MXc = _pmap(lambda m: self.mode_matrices(m)[0] @ self.gather(m, pb, pux, puz, self.pr, self.tau), range(Nk))
+        Fc = _pmap(lambda m: self.equation_F(m, Fb, Fux, Fuz), range(Nk))
         hist = [(MXc, Fc)] + self._ms_hist
-        xs = []
-        for m in range(Nk):
+
+        def solve(m):
             M, L, bc, algf = self.mode_matrices(m)
             rhs = np.zeros(self.n_unknowns(m), complex)
             for k in range(1, len(c)):
@@ -597,7 +654,9 @@ class RBC2D:
                     rhs -= a[k] * hist[k - 1][0][m]
             algf = self._stage_algf(m, algf, self.sim_time + dt)
             rhs[bc] = bcoef[0] * algf[bc]
-            xs.append(self._lhs_lu(m, a[0], bcoef[0]).solve(rhs))
+            return self._lhs_lu(m, a[0], bcoef[0]).solve(rhs)
+
+        xs = _pmap(solve, range(Nk))
         for m in range(Nk):
             self.scatter(m, xs[m], *self.fields())
         self._ms_hist = hist[:1] if order == 1 else hist[:2]
@@ -653,12 +712,12 @@ def turb_wavenumbers(Nx: int, Ny: int, Lx: float, Ly: float):
 
 def turb_forward(g: np.ndarray) -> np.ndarray:
     """Grid (Ny, Nx) real -> coefficients: rfft along x then fft along y."""
-    return np.fft.fft(np.fft.rfft(g, axis=1), axis=0)
+    return _fx.fft(_fx.rfft(g, axis=1), axis=0)
 
 
 def turb_backward(c: np.ndarray, Nx: int) -> np.ndarray:
     """Coefficients -> grid: ifft along y, irfft along x (Im of DC and Nyquist dropped)."""
-    return np.fft.irfft(np.fft.ifft(c, axis=0), n=Nx, axis=1)
+    return _fx.irfft(_fx.ifft(c, axis=0), n=Nx, axis=1)
 
 
 def _pad_full(A: np.ndarray, M: Tuple[int, int]) -> np.ndarray:
@@ -729,10 +788,10 @@ def padded_multiply_2d(a: np.ndarray, b: np.ndarray, factor: float = 1.5) -> np.
     per axis."""
     Ny, Nx = a.shape
     My, Mx = padded_length(Ny, factor), padded_length(Nx, factor)
-    Pa = np.fft.ifftn(_pad_full(np.fft.fftn(a), (My, Mx)))
-    Pb = np.fft.ifftn(_pad_full(np.fft.fftn(b), (My, Mx)))
-    R = _truncate_full(np.fft.fftn(Pa * Pb), (Ny, Nx))
-    return np.real(np.fft.ifftn(R)) * (Mx / Nx) * (My / Ny)
+    Pa = _fx.ifftn(_pad_full(_fx.fftn(a), (My, Mx)))
+    Pb = _fx.ifftn(_pad_full(_fx.fftn(b), (My, Mx)))
+    R = _truncate_full(_fx.fftn(Pa * Pb), (Ny, Nx))
+    return np.real(_fx.ifftn(R)) * (Mx / Nx) * (My / Ny)
 
 
 def turb_rhs(q: np.ndarray, Nx: int, Lx: float, Ly: float) -> np.ndarray:
@@ -799,13 +858,13 @@ def turb_initial_spec(Nx: int, Ny: int, seed: int, kmin: float = 1.0, kmax: Opti
 
 def forward_3d(g: np.ndarray) -> np.ndarray:
     """Grid (Nz, Ny, Nx) -> coefficients (Nz, Ny, Nx/2+1)."""
-    return cheb_forward(np.fft.fft(np.fft.rfft(g, axis=2), axis=1), axis=0)
+    return cheb_forward(_fx.fft(_fx.rfft(g, axis=2), axis=1), axis=0)
 
 
 def backward_3d(c: np.ndarray, Nx: int) -> np.ndarray:
     """Coefficients -> grid: ChebyshevT backward, ifft along y, irfft along x
     (Im of the kx = 0 and Nyquist bins dropped at every y, as FFTW's c2r)."""
-    return np.fft.irfft(np.fft.ifft(cheb_backward(c, axis=0), axis=1), n=Nx, axis=2)
+    return _fx.irfft(_fx.ifft(cheb_backward(c, axis=0), axis=1), n=Nx, axis=2)
 
 
 def _pad_xy(A: np.ndarray, My: int, Mx: int) -> np.ndarray:
@@ -858,10 +917,10 @@ def padded_multiply_3d(a: np.ndarray, b: np.ndarray, factor: float = 1.5) -> np.
     Ny, Nx = a.shape[-2:]
     My, Mx = padded_length(Ny, factor), padded_length(Nx, factor)
     ax = (-2, -1)
-    Pa = np.fft.ifftn(_pad_xy(np.fft.fftn(a, axes=ax), My, Mx), axes=ax)
-    Pb = np.fft.ifftn(_pad_xy(np.fft.fftn(b, axes=ax), My, Mx), axes=ax)
-    R = _truncate_xy(np.fft.fftn(Pa * Pb, axes=ax), Ny, Nx)
-    return np.real(np.fft.ifftn(R, axes=ax)) * (Mx / Nx) * (My / Ny)
+    Pa = _fx.ifftn(_pad_xy(_fx.fftn(a, axes=ax), My, Mx), axes=ax)
+    Pb = _fx.ifftn(_pad_xy(_fx.fftn(b, axes=ax), My, Mx), axes=ax)
+    R = _truncate_xy(_fx.fftn(Pa * Pb, axes=ax), Ny, Nx)
+    return np.real(_fx.ifftn(R, axes=ax)) * (Mx / Nx) * (My / Ny)
 
 
 @dataclass
@@ -1100,13 +1159,20 @@ class RBC3D:
         AE, AI, bE, bI = ts["AE"], ts["AI"], ts["bE"], ts["bI"]
         s = AE.shape[0]
         modes = self.modes()
+
+        def mapped(fn):
+            return dict(zip(modes, _pmap(fn, modes)))
+
         x0 = {m: self.gather(*m, self._fields(), self.tau) for m in modes}
-        MX0 = {m: self.mode_matrices(*m)[0] @ x0[m] for m in modes}
+        MX0 = mapped(lambda m: self.mode_matrices(*m)[0] @ x0[m])
         F, LX = [], []
         for i in range(s):
             a_ii = AI[i, i]
-            xs = {}
-            for m in modes:
+            walls = None
+            if abs(a_ii) >= 1e-14 and self.wall_b is not None:
+                walls = self.wall_b(self.sim_time + dt * ts["c"][i])
+
+            def stage_solve(m):
                 M, L, bc, algf = self.mode_matrices(*m)
                 rhs = MX0[m].copy()
                 for j in range(i):
@@ -1115,29 +1181,35 @@ class RBC3D:
                     if abs(dt * AI[i, j]) > 1e-14:
                         rhs -= dt * AI[i, j] * LX[j][m]
                 if abs(a_ii) < 1e-14:
-                    xs[m] = self.mass_solve(rhs)
-                else:
-                    if self.wall_b is not None:
-                        bot, top = self.wall_b(self.sim_time + dt * ts["c"][i])
-                        algf = algf.copy()
-                        algf[5 * self.p.Nz + 0] = bot[m]
-                        algf[5 * self.p.Nz + 4] = top[m]
-                    rhs[bc] = dt * a_ii * algf[bc]
-                    xs[m] = self._lhs_lu(*m, 1.0, dt * a_ii).solve(rhs)
+                    return self.mass_solve(rhs)
+                if walls is not None:
+                    bot, top = walls
+                    algf = algf.copy()
+                    algf[5 * self.p.Nz + 0] = bot[m]
+                    algf[5 * self.p.Nz + 4] = top[m]
+                rhs[bc] = dt * a_ii * algf[bc]
+                return self._lhs_lu(*m, 1.0, dt * a_ii).solve(rhs)
+
+            xs = mapped(stage_solve)
             for m in modes:
                 self.scatter(*m, xs[m])
             Fc = self.rhs(self.b, self.ux, self.uy, self.uz)
             proj = [self.pr] + [self.projected(c) for c in (self.b, self.ux, self.uy, self.uz)]
-            F.append({m: self.equation_F(*m, Fc) for m in modes})
-            LX.append({m: self.mode_matrices(*m)[1] @ self.gather(*m, proj, self.tau) for m in modes})
-        for m in modes:
+            F.append(mapped(lambda m: self.equation_F(*m, Fc)))
+            LX.append(mapped(lambda m: self.mode_matrices(*m)[1] @ self.gather(*m, proj, self.tau)))
+
+        def final(m):
             rhs = MX0[m].copy()
             for j in range(s):
                 if abs(dt * bE[j]) > 1e-14:
                     rhs += dt * bE[j] * F[j][m]
                 if abs(dt * bI[j]) > 1e-14:
                     rhs -= dt * bI[j] * LX[j][m]
-            self.scatter(*m, self.mass_solve(rhs))
+            return self.mass_solve(rhs)
+
+        xs = mapped(final)
+        for m in modes:
+            self.scatter(*m, xs[m])
         self.sim_time += dt
         self.iteration += 1
 
@@ -1151,11 +1223,15 @@ class RBC3D:
         Fc3 = self.rhs(self.b, self.ux, self.uy, self.uz)
         proj = [self.pr] + [self.projected(cf) for cf in (self.b, self.ux, self.uy, self.uz)]
         modes = self.modes()
-        MXc = {m: self.mode_matrices(*m)[0] @ self.gather(*m, proj, self.tau) for m in modes}
-        Fc = {m: self.equation_F(*m, Fc3) for m in modes}
+        def mapped(fn):
+            return dict(zip(modes, _pmap(fn, modes)))
+
+        MXc = mapped(lambda m: self.mode_matrices(*m)[0] @ self.gather(*m, proj, self.tau))
+        Fc = mapped(lambda m: self.equation_F(*m, Fc3))
         hist = [(MXc, Fc)] + hist_prev
-        xs = {}
-        for m in modes:
+        walls = self.wall_b(self.sim_time + dt) if self.wall_b is not None else None
+
+        def solve(m):
             M, L, bc, algf = self.mode_matrices(*m)
             rhs = np.zeros(M.shape[0], complex)
             for k in range(1, len(c)):
@@ -1164,13 +1240,15 @@ class RBC3D:
             for k in range(1, len(a)):
                 if abs(a[k]) >= 1e-14 and k - 1 < len(hist):
                     rhs -= a[k] * hist[k - 1][0][m]
-            if self.wall_b is not None:
-                bot, top = self.wall_b(self.sim_time + dt)
+            if walls is not None:
+                bot, top = walls
                 algf = algf.copy()
                 algf[5 * self.p.Nz + 0] = bot[m]
                 algf[5 * self.p.Nz + 4] = top[m]
             rhs[bc] = bcoef[0] * algf[bc]
-            xs[m] = self._lhs_lu(*m, a[0], bcoef[0]).solve(rhs)
+            return self._lhs_lu(*m, a[0], bcoef[0]).solve(rhs)
+
+        xs = mapped(solve)
         for m in modes:
             self.scatter(*m, xs[m])
         self._ms_hist = hist[:1] if order == 1 else hist[:2]
