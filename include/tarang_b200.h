@@ -318,6 +318,7 @@ typedef struct tb_server_stats {
   double p50_ms, p99_ms, mean_wait_ms;
   size_t peak_bytes, budget_bytes;
   int peak_running;
+  double mean_setup_ms; /* admission to ready: plan build, factors, graph capture */
 } tb_server_stats;
 typedef struct tb_server tb_server;
 tb_status tb_server_create(tb_context* ctx, size_t budget_bytes, int max_running, int chunk_steps, tb_server** out);

@@ -52,7 +52,7 @@ class tb_server_stats(Structure):
         ("submitted", c_longlong), ("completed", c_longlong), ("failed", c_longlong), ("running", c_longlong),
         ("queued", c_longlong), ("elapsed_ms", c_double), ("solves_per_s", c_double), ("steps_per_s", c_double),
         ("p50_ms", c_double), ("p99_ms", c_double), ("mean_wait_ms", c_double), ("peak_bytes", c_size_t),
-        ("budget_bytes", c_size_t), ("peak_running", c_int),
+        ("budget_bytes", c_size_t), ("peak_running", c_int), ("mean_setup_ms", c_double),
     ]
 
 

@@ -225,8 +225,8 @@ FactorSet* get_factors(tb_plan* P, int sy, double alpha, double beta) {
   TB_CUDA_TRY(cudaMemsetAsync(fs->BR.p, 0, fs->BR.bytes, P->st));
   TB_CUDA_TRY(cudaMemsetAsync(fs->SI.p, 0, fs->SI.bytes, P->st));
   const int nmax = std::max(S.lay.cls[0].n, S.lay.cls[1].n);
-  DevBuf scratch;
-  scratch.alloc(tau_factor_scratch_doubles(nmax, P->Nkm) * sizeof(double));
+  StreamBuf scratch;  // released in stream order: no device-wide wait
+  scratch.alloc(tau_factor_scratch_doubles(nmax, P->Nkm) * sizeof(double), P->st);
   int neg = 0x7fffffff;
   TB_CUDA_TRY(cudaMemcpyAsync(P->err_mode.p, &neg, sizeof(int), cudaMemcpyHostToDevice, P->st));
   TauArgs a = tau_args(P, sy, fs.get(), nullptr);
@@ -916,6 +916,14 @@ tb_status tb_context_create(int device, tb_context** out) {
   tb_context* c = new (std::nothrow) tb_context();
   if (!c) return TB_ENOMEM;
   c->device = device;
+  // Stream-ordered scratch (factorisation work arrays, staging of initial
+  // states) returns to the device's default pool; keep up to 256 MB of it
+  // mapped so that a later plan reuses it without a new mapping.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    unsigned long long keep = 256ull << 20;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   *out = c;
   return TB_OK;
 }

@@ -41,6 +41,38 @@ struct DevBuf {
   }
 };
 
+// Stream-ordered scratch: allocated from the device's memory pool in the order
+// of one stream and released in that order, so that dropping it does not wait
+// for the whole device the way cudaFree does (a request server builds plans
+// while other requests' steps run).
+struct StreamBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaStream_t st = nullptr;
+  StreamBuf() = default;
+  StreamBuf(const StreamBuf&) = delete;
+  StreamBuf& operator=(const StreamBuf&) = delete;
+  ~StreamBuf() {
+    if (p) cudaFreeAsync(p, st);
+  }
+  void alloc(size_t b, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+    bytes = b;
+    st = s;
+    if (b == 0) return;
+    cudaError_t e = cudaMallocAsync(&p, b, s);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      throw Error{TB_ENOMEM, std::string("cudaMallocAsync(") + std::to_string(b) + "): " + cudaGetErrorString(e)};
+    }
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
 // Non-owning window into a DevBuf.
 struct DevView {
   void* p = nullptr;

@@ -33,7 +33,12 @@ using namespace tb;
 
 namespace {
 
-constexpr int kSetupThreads = 4;  // host threads building admitted requests' plans
+// Host threads building admitted requests' plans: half the host's hardware
+// threads, 4 to 16 (plan construction is host work that overlaps the steps).
+int setup_threads() {
+  const unsigned hw = std::thread::hardware_concurrency();
+  return (int)std::max(4u, std::min(16u, hw / 2));
+}
 
 double now_ms() {
   using namespace std::chrono;
@@ -101,7 +106,7 @@ struct Request {
   double dt = 0;
   int nsteps = 0, left = 0;
   std::vector<double> init;
-  double t_submit = 0, t_start = 0, t_done = 0;
+  double t_submit = 0, t_start = 0, t_ready = 0, t_done = 0;
   int state = TB_REQ_QUEUED;
   std::string error;
   size_t bytes = 0;
@@ -139,7 +144,7 @@ struct tb_server {
   int peak_running = 0;
   long long completed = 0, failed = 0, steps_done = 0;
   double first_submit = -1, last_done = 0;
-  std::vector<double> tts, waits;
+  std::vector<double> tts, waits, setups;
 
   void loop();
   void setup_loop();
@@ -164,10 +169,10 @@ std::unique_ptr<Job> make_job(tb_context* ctx, const Request& r) {
   if (st != TB_OK) throw Error{st, ctx->last_error};
   tb_plan* P = j->P;
   // initial state: b from the grid field, u = 0
-  DevBuf grid, coeff;
-  grid.alloc(r.init.size() * sizeof(double));
-  coeff.alloc(P->plane * sizeof(double2));
-  TB_CUDA_TRY(cudaMemcpy(grid.p, r.init.data(), grid.bytes, cudaMemcpyHostToDevice));
+  StreamBuf grid, coeff;  // staging released in stream order: no device-wide wait
+  grid.alloc(r.init.size() * sizeof(double), P->st);
+  coeff.alloc(P->plane * sizeof(double2), P->st);
+  TB_CUDA_TRY(cudaMemcpyAsync(grid.p, r.init.data(), grid.bytes, cudaMemcpyHostToDevice, P->st));
   st = tb_transform_forward(P, grid.as<double>(), coeff.as<double>(), 1);
   if (st != TB_OK) throw Error{st, ctx->last_error};
   TB_CUDA_TRY(cudaMemsetAsync(P->X.p, 0, P->X.bytes, P->st));
@@ -230,7 +235,9 @@ void tb_server::setup_loop() {
       r->job = make_job(ctx, *r);
       r->job->prepare(r->dt, chunk);
       TB_CUDA_TRY(cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming));
+      r->t_ready = now_ms();
       std::lock_guard<std::mutex> lk(mu);
+      setups.push_back(r->t_ready - r->t_start);
       --setting_up;
       r->state = TB_REQ_RUNNING;
       running.push_back(r);
@@ -359,7 +366,7 @@ tb_status tb_server_create(tb_context* ctx, size_t budget_bytes, int max_running
     S->chunk = chunk_steps;
     tb_server* raw = S.get();
     S->worker = std::thread([raw] { raw->loop(); });
-    for (int i = 0; i < kSetupThreads; ++i) S->setup_workers.emplace_back([raw] { raw->setup_loop(); });
+    for (int i = 0, n = setup_threads(); i < n; ++i) S->setup_workers.emplace_back([raw] { raw->setup_loop(); });
     *out = S.release();
   });
 }
@@ -448,6 +455,9 @@ tb_status tb_server_get_stats(tb_server* S, tb_server_stats* out) {
   st.peak_bytes = S->peak;
   st.budget_bytes = S->budget;
   st.peak_running = S->peak_running;
+  double su = 0;
+  for (double x : S->setups) su += x;
+  st.mean_setup_ms = S->setups.empty() ? 0.0 : su / S->setups.size();
   *out = st;
   return TB_OK;
 }
