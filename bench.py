@@ -477,6 +477,11 @@ def run_ours(args, cfg, scheme, dist):
                 out["mixed"] = run_mixed(args, cfg, scheme, dev)
             except Exception as exc:  # reported, never fatal to the headline line
                 out["mixed"] = {"error": f"{type(exc).__name__}: {exc}"}
+        if dist.world == 1 and not args.no_mixed and scheme != "SBDF2":
+            try:
+                out["sbdf2"] = run_sbdf2(args, cfg, dev)
+            except Exception as exc:  # reported, never fatal to the headline line
+                out["sbdf2"] = {"error": f"{type(exc).__name__}: {exc}"}
         if dist.world == 1 and not args.no_rbc3d:
             try:
                 out["rbc3d"] = run_rbc3d(args, dev)
@@ -632,6 +637,53 @@ def run_mixed(args, cfg, scheme, dev):
         "rel_l2_vs_f64_after_steps": err,
         "steps": n,
         "dtype": "f32 transforms/products, f64 solves/stage algebra",
+    }
+
+
+def run_sbdf2(args, cfg, dev):
+    """SBDF2 on the headline grid (the multistep half of the 1024x256
+    benchmark): Float64 and mixed steps/s on the device clock (graph replay
+    after warm-up), the step byte model's HBM fraction, and the mixed form's
+    relative L2 error against Float64 after the same steps."""
+    import numpy as np
+    import torch
+
+    from __graft_entry__ import load_package
+
+    tb = load_package()
+    from tarang_b200 import workloads as W
+    from tarang_b200._lib import TB_PREC_MIXED, TB_SBDF2
+
+    dom = tb.ChannelDomain(cfg.Nx, cfg.Nz, Lx=cfg.Lx, Lz=cfg.Lz, arch=tb.GPU(dev))
+    full = tb.Plan(dom, cfg.kappa, cfg.nu, cfg.Lz, 0.0, TB_SBDF2)
+    mixed = tb.Plan(dom, cfg.kappa, cfg.nu, cfg.Lz, 0.0, TB_SBDF2, precision=TB_PREC_MIXED)
+    b0 = full.forward(W.rbc_initial_grid(cfg))
+    n = args.steps
+    for pl in (full, mixed):
+        pl.set_state(0, b0)
+        pl.step(cfg.dt, n)
+    err = {nm: float(np.linalg.norm(mixed.get_state(f) - full.get_state(f)) / np.linalg.norm(full.get_state(f)))
+           for f, nm in ((0, "b"), (1, "ux"), (2, "uz"))}
+    peaks, _ = measured_peaks()
+    model = W.step_model_bytes(cfg, "SBDF2")
+    out = {}
+    for name, pl in (("f64", full), ("mixed", mixed)):
+        pl.step(cfg.dt, args.warmup)
+        torch.cuda.synchronize()
+        pl.step(cfg.dt, n)
+        ms = pl.last_step_ms() / n
+        out[name] = {"value": 1e3 / ms, "ms_per_step": ms,
+                     "step_roofline_frac": model / (ms * 1e-3) / (peaks["hbm_gbs"] * 1e9)}
+    return {
+        "metric": f"RBC 2D steps/s ({cfg.Nx}x{cfg.Nz}, SBDF2)",
+        "unit": "steps/s",
+        "value": out["f64"]["value"],
+        "f64": out["f64"],
+        "mixed": out["mixed"],
+        "mixed_rel_l2_vs_f64_after_steps": err,
+        "bytes_per_step_model": model,
+        "steps": n,
+        "dtype": "f64; mixed: f32 transforms/products, f64 solves/stage algebra",
     }
 
 

@@ -239,7 +239,9 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
 // ---------------------------------------------------------------------------
 constexpr int kPartRows = 6;    // rows per ring stage (the forward window)
 constexpr int kPartStages = 4;  // ring depth
-constexpr int kXch = 20;        // exchange doubles per (warp, lane): D(4) Z(4) Xhat(12)
+// exchange doubles per (warp, lane): D(4) Z(4) Xhat(12), padded to 21 so that
+// the 16 lanes of a warp read distinct banks
+constexpr int kXch = 21;
 // per (partition, class, mode): Phi (4x4), Psi (12x12), Gz (4x4)
 constexpr int kTrPhi = 0, kTrPsi = 16, kTrGz = 160, kTransfer = 176;
 
@@ -439,8 +441,12 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   // forward transfer data (Phi_k for k < warp, Gz_warp) while the other warps
   // finish their sweeps.
   constexpr int TRF = 32;  // Phi (16) + Gz (16) per (partition, record slot)
+  // shared-memory stride of a staged (partition, slot) record: 34 doubles, so
+  // that the 8 slots a warp reads at once fall in distinct banks
+  constexpr int TRS = TRF + 2;
+  static_assert(2 * NBMAX * NBMAX * MP + (P - 1) * 2 * MP * TRS <= NS * STAGE, "Schur inverse and Phi fit the ring");
   double* sSI = ring;                         // [class][4][4][mode], 2*16*MP doubles
-  double* sTR = ring + 2 * NBMAX * NBMAX * MP;  // [k-1][slot][TRF]
+  double* sTR = ring + 2 * NBMAX * NBMAX * MP;  // [k-1][slot][TRS]
   {
     const double* SIg = a.cls[0].SI + (size_t)g * 2 * NBMAX * NBMAX * MP;
     for (int q = lane; q < NBMAX * NBMAX * MP; q += 32) cp_async16(sSI + 2 * q, SIg + 2 * q, true);
@@ -449,7 +455,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
         const int k = 1 + q / (2 * MP * (TRF / 2)), rs = (q / (TRF / 2)) % (2 * MP), h = q % (TRF / 2);
         const double* rec = a.PP + (((size_t)g * P + k) * 2 * MP + rs) * kTransfer;
         const double* src = (h < 8) ? rec + kTrPhi + 2 * h : rec + kTrGz + 2 * (h - 8);
-        cp_async16(sTR + ((size_t)(k - 1) * 2 * MP + rs) * TRF + 2 * h, src, true);
+        cp_async16(sTR + ((size_t)(k - 1) * 2 * MP + rs) * TRS + 2 * h, src, true);
       }
     }
     cp_async_commit();
@@ -465,7 +471,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 #pragma unroll
       for (int t = 0; t < 4; ++t) d[t] = xch[(size_t)ln * kXch + t];  // delta_1 = D_0
       for (int k = 1; k < warp; ++k) {
-        const double* phi = sTR + ((size_t)(k - 1) * 2 * MP + slot) * TRF;
+        const double* phi = sTR + ((size_t)(k - 1) * 2 * MP + slot) * TRS;
         const double* Dk = xch + ((size_t)k * NL + ln) * kXch;
         double nd[4];
 #pragma unroll
@@ -478,7 +484,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 #pragma unroll
         for (int o = 0; o < 4; ++o) d[o] = nd[o];
       }
-      const double* gz = sTR + ((size_t)(warp - 1) * 2 * MP + slot) * TRF + 16;
+      const double* gz = sTR + ((size_t)(warp - 1) * 2 * MP + slot) * TRS + 16;
 #pragma unroll
       for (int b = 0; b < NBMAX; ++b)
 #pragma unroll
@@ -594,12 +600,16 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   for (int t = 0; t < kBwdWin; ++t) T[t] = 0.0;
   if constexpr (P > 1) {
     // stage Psi_k, k = warp+1 .. P-2, in the ring while the other warps finish B1
-    double* sPsi = ring;  // [k-warp-1][slot][144]
+    // [k-warp-1][slot][PS]; the stride PS = 146 doubles puts the 8 slots a
+    // warp reads at once in distinct banks
+    constexpr int PS = kBwdWin * kBwdWin + 2;
+    static_assert((P > 2 ? P - 2 : 0) * 2 * MP * PS <= NS * STAGE, "Psi fits the ring");
+    double* sPsi = ring;
     const int npsi = (P - 2 - warp) > 0 ? (P - 2 - warp) : 0;
     for (int q = lane; q < npsi * 2 * MP * 72; q += 32) {
       const int kk = q / (2 * MP * 72), rs = (q / 72) % (2 * MP), h = q % 72;
       const double* rec = a.PP + (((size_t)g * P + warp + 1 + kk) * 2 * MP + rs) * kTransfer + kTrPsi;
-      cp_async16(sPsi + ((size_t)kk * 2 * MP + rs) * 144 + 2 * h, rec + 2 * h, true);
+      cp_async16(sPsi + ((size_t)kk * 2 * MP + rs) * PS + 2 * h, rec + 2 * h, true);
     }
     cp_async_commit();
     double* myxh = myx + 8;
@@ -613,7 +623,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 #pragma unroll
       for (int t = 0; t < kBwdWin; ++t) T[t] = Xl[t];
       for (int k = P - 2; k > warp; --k) {
-        const double* psi = sPsi + ((size_t)(k - warp - 1) * 2 * MP + slot) * 144;
+        const double* psi = sPsi + ((size_t)(k - warp - 1) * 2 * MP + slot) * PS;
         const double* Xk = xch + ((size_t)k * NL + ln) * kXch + 8;
         double nt[kBwdWin];
 #pragma unroll
