@@ -428,17 +428,15 @@ def run_ours(args, cfg, scheme, dist):
     dist.barrier()
     t0 = time.perf_counter()
     for _ in range(ne):
-        for f, a in host.items():
-            plan.set_state(f, a)
+        plan.set_states(host)
         plan.step(cfg.dt, 1)
-        for f in host:
-            tb.lib.tb_get_state(plan.ptr, f, host[f].ctypes.data_as(__import__("ctypes").c_void_p), 0)
+        plan.get_states(host)
     e2e_el = dist.max(time.perf_counter() - t0)
     sbytes = W.state_bytes(cfg)
     e2e = {"value": dist.world * ne / e2e_el, "unit": "steps/s", "h2d_bytes_per_step": sbytes,
            "d2h_bytes_per_step": sbytes, "steps": ne,
-           "what": "per step: tb_set_state of b,ux,uz,p,taus from pinned host memory, tb_step(1), "
-                   "tb_get_state of all fields to host"}
+           "what": "per step: tb_set_states of b,ux,uz,p,taus from pinned host memory, tb_step(1), "
+                   "tb_get_states of all fields to pinned host memory (one wait per call)"}
 
     finite = all(np.isfinite(plan.get_state(f)).all() for f in (TB_FIELD_B, TB_FIELD_UZ))
     cpu = None

@@ -105,6 +105,14 @@ tb_status tb_plan_destroy(tb_plan* plan);
  * where = TB_HOST or TB_DEVICE.  Replaces get_coeff_data/set on state fields. */
 tb_status tb_set_state(tb_plan* plan, int field, const void* data, int where);
 tb_status tb_get_state(tb_plan* plan, int field, void* data, int where);
+/* Several fields in one call: data[i] holds field fields[i] (2D plans).  The
+ * copies are queued back to back on the plan's stream and the call returns
+ * once all of them are done (one wait instead of one per field), so a caller
+ * that moves the whole state every step (b, u_x, u_z, p, taus) pays one
+ * host/device round trip each way.  Same layouts and ownership as
+ * tb_set_state / tb_get_state; a bad selector fails before any copy. */
+tb_status tb_set_states(tb_plan* plan, int nfields, const int* fields, const void* const* data, int where);
+tb_status tb_get_states(tb_plan* plan, int nfields, const int* fields, void* const* data, int where);
 
 /* Advance nsteps steps of size dt.  Replaces step!(solver, dt)
  * (src/core/solvers/solver_stepping.jl:24-38) through

@@ -75,6 +75,8 @@ SIGNATURES = {
     "tb_plan_destroy": (c_int, [c_void_p]),
     "tb_set_state": (c_int, [c_void_p, c_int, c_void_p, c_int]),
     "tb_get_state": (c_int, [c_void_p, c_int, c_void_p, c_int]),
+    "tb_set_states": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int]),
+    "tb_get_states": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int]),
     "tb_step": (c_int, [c_void_p, c_double, c_int]),
     "tb_sim_time": (c_int, [c_void_p, POINTER(c_double), POINTER(c_longlong)]),
     "tb_synchronize": (c_int, [c_void_p]),

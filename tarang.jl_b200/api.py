@@ -196,6 +196,38 @@ class Plan:
         check(lib.tb_get_state(self.ptr, field, out.ctypes.data_as(c_void_p), L.TB_HOST), self.ctx)
         return out
 
+    def _field_shape(self, field: int):
+        return (7, self.domain.Nk) if field == L.TB_FIELD_TAU else (self.domain.Nz, self.domain.Nk)
+
+    def _field_arrays(self, arrays: Dict[int, np.ndarray], writable: bool):
+        fields = list(arrays)
+        arrs = []
+        for f in fields:
+            a = arrays[f]
+            if writable:
+                if a.dtype != np.complex128 or not a.flags.c_contiguous or not a.flags.writeable:
+                    raise ValueError("output buffers must be writable C-contiguous complex128 arrays")
+            else:
+                a = np.ascontiguousarray(a, dtype=np.complex128)
+            if a.shape != self._field_shape(f):
+                raise ValueError(f"field {f}: shape {a.shape}, expected {self._field_shape(f)}")
+            arrs.append(a)
+        fa = (c_int * len(fields))(*fields)
+        pa = (c_void_p * len(fields))(*[a.ctypes.data for a in arrs])
+        return fields, arrs, fa, pa
+
+    def set_states(self, arrays: Dict[int, np.ndarray]) -> None:
+        """Several fields from host arrays in one call (one wait for all copies)."""
+        fields, arrs, fa, pa = self._field_arrays(arrays, False)
+        check(lib.tb_set_states(self.ptr, len(fields), fa, pa, L.TB_HOST), self.ctx)
+
+    def get_states(self, out: Dict[int, np.ndarray]) -> Dict[int, np.ndarray]:
+        """Fill out[field] (C-contiguous complex128 of the field's shape, e.g.
+        pinned host memory) for every field in one call; returns out."""
+        fields, arrs, fa, pa = self._field_arrays(out, True)
+        check(lib.tb_get_states(self.ptr, len(fields), fa, pa, L.TB_HOST), self.ctx)
+        return out
+
     def step(self, dt: float, nsteps: int = 1) -> None:
         check(lib.tb_step(self.ptr, float(dt), int(nsteps)), self.ctx)
 

@@ -1167,6 +1167,45 @@ tb_status tb_get_state(tb_plan* P, int field, void* data, int where) {
   });
 }
 
+tb_status tb_set_states(tb_plan* P, int nfields, const int* fields, const void* const* data, int where) {
+  if (!P || nfields < 0 || (nfields > 0 && (!fields || !data))) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "multi-field state I/O is for 2D plans (use tb_set_state in 3D)");
+    for (int i = 0; i < nfields; ++i) {
+      TB_REQUIRE(fields[i] >= TB_FIELD_B && fields[i] <= TB_FIELD_TAU, TB_EINVAL, "bad field selector");
+      TB_REQUIRE(data[i] != nullptr, TB_EINVAL, "null field buffer");
+    }
+    for (int i = 0; i < nfields; ++i) {
+      const int f = fields[i];
+      void* dst = f == TB_FIELD_TAU ? P->tau.p : (void*)P->Xp(f);
+      const size_t bytes = f == TB_FIELD_TAU ? P->tau.bytes : P->plane * sizeof(double2);
+      TB_CUDA_TRY(cudaMemcpyAsync(dst, data[i], bytes,
+                                  where == TB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, P->st));
+    }
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+    P->ms_history = 0;  // a new state restarts multistep history
+  });
+}
+
+tb_status tb_get_states(tb_plan* P, int nfields, const int* fields, void* const* data, int where) {
+  if (!P || nfields < 0 || (nfields > 0 && (!fields || !data))) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "multi-field state I/O is for 2D plans (use tb_get_state in 3D)");
+    for (int i = 0; i < nfields; ++i) {
+      TB_REQUIRE(fields[i] >= TB_FIELD_B && fields[i] <= TB_FIELD_TAU, TB_EINVAL, "bad field selector");
+      TB_REQUIRE(data[i] != nullptr, TB_EINVAL, "null field buffer");
+    }
+    for (int i = 0; i < nfields; ++i) {
+      const int f = fields[i];
+      const void* src = f == TB_FIELD_TAU ? P->tau.p : (const void*)P->Xp(f);
+      const size_t bytes = f == TB_FIELD_TAU ? P->tau.bytes : P->plane * sizeof(double2);
+      TB_CUDA_TRY(cudaMemcpyAsync(data[i], src, bytes,
+                                  where == TB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, P->st));
+    }
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  });
+}
+
 tb_status tb_step(tb_plan* P, double dt, int nsteps) {
   if (!P) return TB_EINVAL;
   return guard(P->ctx, [&] {

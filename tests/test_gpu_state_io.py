@@ -1,0 +1,57 @@
+"""Multi-field state I/O (tb_set_states / tb_get_states): the same data and the
+same steps as the per-field calls, one wait per call."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle.tarang_oracle import RBCParams, forward_2d, rbc_initial_b
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = (0, 1, 2, 3, 4)  # b, ux, uz, p, taus
+
+
+def _plan(tb, p):
+    dom = tb.ChannelDomain(p.Nx, p.Nz, Lx=4.0, Lz=1.0)
+    plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 1)
+    plan.set_state(0, forward_2d(rbc_initial_b(p, 42)))
+    plan.step(0.01, 3)
+    return plan
+
+
+def test_states_round_trip_and_step_like_single_fields(tb):
+    p = RBCParams(Nx=64, Nz=32, Lx=4.0, Lz=1.0, Ra=1e7)
+    a, b = _plan(tb, p), _plan(tb, p)
+    got = {f: np.empty(a._field_shape(f), np.complex128) for f in FIELDS}
+    a.get_states(got)
+    for f in FIELDS:
+        assert np.array_equal(got[f], a.get_state(f))
+    # perturb, load through both routes, step both: bitwise the same states
+    rng = np.random.default_rng(3)
+    new = {f: got[f] * (1 + 1e-3 * rng.standard_normal(got[f].shape)) for f in FIELDS}
+    a.set_states(new)
+    for f in FIELDS:
+        b.set_state(f, new[f])
+    a.step(0.01, 2)
+    b.step(0.01, 2)
+    out = {f: np.empty(a._field_shape(f), np.complex128) for f in FIELDS}
+    a.get_states(out)
+    for f in FIELDS:
+        assert np.array_equal(out[f], b.get_state(f))
+
+
+def test_states_reject_bad_selectors_and_shapes(tb):
+    p = RBCParams(Nx=32, Nz=16, Lx=4.0, Lz=1.0, Ra=1e6)
+    plan = _plan(tb, p)
+    before = plan.get_state(0)
+    buf = np.zeros_like(before)
+    fields = (ctypes.c_int * 2)(0, 9)
+    ptrs = (ctypes.c_void_p * 2)(buf.ctypes.data, buf.ctypes.data)
+    st = tb.lib.tb_set_states(plan.ptr, 2, fields, ptrs, 0)
+    assert st == tb._lib.TB_EINVAL
+    assert np.array_equal(plan.get_state(0), before)  # nothing was copied
+    with pytest.raises(ValueError):
+        plan.set_states({0: np.zeros((3, 3), np.complex128)})
+    with pytest.raises(ValueError):
+        plan.get_states({0: np.zeros(before.shape, np.complex64)})
