@@ -176,20 +176,52 @@ __global__ void __launch_bounds__(256, 2) k_xprod32(XProdArgs32 a) {
   auto zero_gap = [&](float2* dst) {
     for (int k = hN + 1 + threadIdx.x; k < M - hN; k += blockDim.x) dst[F::fidx<true>(k)] = make_float2(0.f, 0.f);
   };
-  for (int q = threadIdx.x; q <= hN; q += blockDim.x) put2(S0, q, hbin(value(1, q), q), hbin(value(2, q), q));
+  // inputs in batches of QB bins per thread, every load issued before the
+  // first is used (one wait for memory per batch)
+  constexpr int QB = 3;
+  for (int q0 = threadIdx.x; q0 <= hN; q0 += QB * blockDim.x) {
+    float2 vx[QB], vz[QB];
+#pragma unroll
+    for (int i = 0; i < QB; ++i) {
+      const int q = q0 + i * blockDim.x;
+      if (q <= hN) {
+        vx[i] = value(1, q);
+        vz[i] = value(2, q);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < QB; ++i) {
+      const int q = q0 + i * blockDim.x;
+      if (q <= hN) put2(S0, q, hbin(vx[i], q), hbin(vz[i], q));
+    }
+  }
   zero_gap(S0);
   __syncthreads();
   float2* U = F::fft<true>(S0, S1, a.fp, tw, +1);
   float2* P = (U == S0) ? S1 : S0;
   for (int f = 0; f < 3; ++f) {
-    for (int q = threadIdx.x; q <= hN; q += blockDim.x) {
-      float2 Ax = make_float2(0.f, 0.f);
-      if (q > 0 && q < hN) {
-        const float kk = a.k0 * q;
-        const float2 g = value(f, q);
-        Ax = make_float2(-kk * g.y, kk * g.x);
+    for (int q0 = threadIdx.x; q0 <= hN; q0 += QB * blockDim.x) {
+      float2 gv[QB], dv[QB];
+#pragma unroll
+      for (int i = 0; i < QB; ++i) {
+        const int q = q0 + i * blockDim.x;
+        if (q <= hN) {
+          gv[i] = value(f, q);
+          dv[i] = deriv(f, q);
+        }
       }
-      put2(S2, q, Ax, hbin(deriv(f, q), q));
+#pragma unroll
+      for (int i = 0; i < QB; ++i) {
+        const int q = q0 + i * blockDim.x;
+        if (q <= hN) {
+          float2 Ax = make_float2(0.f, 0.f);
+          if (q > 0 && q < hN) {
+            const float kk = a.k0 * q;
+            Ax = make_float2(-kk * gv[i].y, kk * gv[i].x);
+          }
+          put2(S2, q, Ax, hbin(dv[i], q));
+        }
+      }
     }
     zero_gap(S2);
     __syncthreads();

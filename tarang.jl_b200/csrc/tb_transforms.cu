@@ -494,8 +494,27 @@ __global__ void __launch_bounds__(256, 2) k_xprod(XProdArgs a) {
   auto zero_gap = [&](double2* dst) {  // bins N/2 < k < M - N/2 are zero
     for (int k = hN + 1 + threadIdx.x; k < M - hN; k += blockDim.x) dst[fidx<true>(k)] = make_double2(0.0, 0.0);
   };
+  // Inputs are read in batches of QB bins per thread with every load issued
+  // before the first is used, so a thread waits for memory once per batch
+  // rather than once per bin.
+  constexpr int QB = 3;
   // 1. velocity spectrum
-  for (int q = threadIdx.x; q <= hN; q += blockDim.x) put2(S0, q, hbin(value(1, q), q), hbin(value(2, q), q));
+  for (int q0 = threadIdx.x; q0 <= hN; q0 += QB * blockDim.x) {
+    double2 vx[QB], vz[QB];
+#pragma unroll
+    for (int i = 0; i < QB; ++i) {
+      const int q = q0 + i * blockDim.x;
+      if (q <= hN) {
+        vx[i] = value(1, q);
+        vz[i] = value(2, q);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < QB; ++i) {
+      const int q = q0 + i * blockDim.x;
+      if (q <= hN) put2(S0, q, hbin(vx[i], q), hbin(vz[i], q));
+    }
+  }
   zero_gap(S0);
   __syncthreads();
   double2* U = fft_cta_pt<true>(S0, S1, a.fp, tw, +1);
@@ -503,14 +522,28 @@ __global__ void __launch_bounds__(256, 2) k_xprod(XProdArgs a) {
   double2* Q = nullptr;              // prod_uz (real parts)
   // 2. gradients of each field and the advection products
   for (int f = 0; f < 3; ++f) {
-    for (int q = threadIdx.x; q <= hN; q += blockDim.x) {
-      double2 Ax = make_double2(0.0, 0.0);
-      if (q > 0 && q < hN) {
-        const double kk = a.k0 * q;
-        const double2 g = value(f, q);
-        Ax = make_double2(-kk * g.y, kk * g.x);  // i k g
+    for (int q0 = threadIdx.x; q0 <= hN; q0 += QB * blockDim.x) {
+      double2 gv[QB], dv[QB];
+#pragma unroll
+      for (int i = 0; i < QB; ++i) {
+        const int q = q0 + i * blockDim.x;
+        if (q <= hN) {
+          gv[i] = value(f, q);
+          dv[i] = deriv(f, q);
+        }
       }
-      put2(S2, q, Ax, hbin(deriv(f, q), q));
+#pragma unroll
+      for (int i = 0; i < QB; ++i) {
+        const int q = q0 + i * blockDim.x;
+        if (q <= hN) {
+          double2 Ax = make_double2(0.0, 0.0);
+          if (q > 0 && q < hN) {
+            const double kk = a.k0 * q;
+            Ax = make_double2(-kk * gv[i].y, kk * gv[i].x);  // i k g
+          }
+          put2(S2, q, Ax, hbin(dv[i], q));
+        }
+      }
     }
     zero_gap(S2);
     __syncthreads();
