@@ -418,10 +418,13 @@ def run_ours(args, cfg, scheme, dist):
 
     # end to end through the C ABI with host buffers: per step, upload the state
     # from pinned host memory, one step, download the state
+    # one pinned host buffer holding b, u_x, u_z, p and the taus back to back
+    # (the device order), so each direction is one copy
     nk = cfg.Nx // 2 + 1
-    host = {f: torch.empty((cfg.Nz, nk), dtype=torch.complex128, pin_memory=True).numpy()
+    pinned = torch.empty((4 * cfg.Nz + 7) * nk, dtype=torch.complex128, pin_memory=True).numpy()
+    host = {f: pinned[f * cfg.Nz * nk:(f + 1) * cfg.Nz * nk].reshape(cfg.Nz, nk)
             for f in (TB_FIELD_B, TB_FIELD_UX, TB_FIELD_UZ, TB_FIELD_P)}
-    host[TB_FIELD_TAU] = torch.empty((7, nk), dtype=torch.complex128, pin_memory=True).numpy()
+    host[TB_FIELD_TAU] = pinned[4 * cfg.Nz * nk:].reshape(7, nk)
     for f in host:
         host[f][...] = plan.get_state(f)
     ne = args.e2e_steps
@@ -435,8 +438,8 @@ def run_ours(args, cfg, scheme, dist):
     sbytes = W.state_bytes(cfg)
     e2e = {"value": dist.world * ne / e2e_el, "unit": "steps/s", "h2d_bytes_per_step": sbytes,
            "d2h_bytes_per_step": sbytes, "steps": ne,
-           "what": "per step: tb_set_states of b,ux,uz,p,taus from pinned host memory, tb_step(1), "
-                   "tb_get_states of all fields to pinned host memory (one wait per call)"}
+           "what": "per step: tb_set_states of b,ux,uz,p,taus from one pinned host buffer, tb_step(1), "
+                   "tb_get_states of all fields back into it (one copy and one wait per call)"}
 
     finite = all(np.isfinite(plan.get_state(f)).all() for f in (TB_FIELD_B, TB_FIELD_UZ))
     cpu = None
@@ -1000,8 +1003,20 @@ def run_serving(args, dev, dist=None):
     # plain GPU form: one request at a time, chunks of 50 steps
     served = replay(16, True)
     plain = replay(1, True, chunk=50)
-    sat = replay(16, False)
-    sat_plain = replay(1, False, chunk=50)
+    # saturated capacity: the host-side plan setup and the shared device make
+    # single replays vary by up to 2x, so each form is replayed three times
+    # (alternating) and the median run by solves/s is reported
+    sat_runs, plain_runs = [], []
+    for _ in range(3):
+        sat_runs.append(replay(16, False))
+        plain_runs.append(replay(1, False, chunk=50))
+
+    def median_run(runs):
+        return sorted(runs, key=lambda r: r["solves_per_s"])[len(runs) // 2]
+
+    sat, sat_plain = median_run(sat_runs), median_run(plain_runs)
+    sat = dict(sat, runs_solves_per_s=[r["solves_per_s"] for r in sat_runs])
+    sat_plain = dict(sat_plain, runs_solves_per_s=[r["solves_per_s"] for r in plain_runs])
     kinds = {"rbc": sum(r.kind == "rbc" for r in reqs), "turb": sum(r.kind == "turb" for r in reqs)}
     return {
         "metric": "serving solves/s and time to solution (Poisson 20/s replay)",

@@ -109,7 +109,9 @@ tb_status tb_get_state(tb_plan* plan, int field, void* data, int where);
  * copies are queued back to back on the plan's stream and the call returns
  * once all of them are done (one wait instead of one per field), so a caller
  * that moves the whole state every step (b, u_x, u_z, p, taus) pays one
- * host/device round trip each way.  Same layouts and ownership as
+ * host/device round trip each way.  Fields adjacent in the device state
+ * (b, u_x, u_z, p, taus in that order) whose buffers are also adjacent in the
+ * caller's memory go as one copy.  Same layouts and ownership as
  * tb_set_state / tb_get_state; a bad selector fails before any copy. */
 tb_status tb_set_states(tb_plan* plan, int nfields, const int* fields, const void* const* data, int where);
 tb_status tb_get_states(tb_plan* plan, int nfields, const int* fields, void* const* data, int where);

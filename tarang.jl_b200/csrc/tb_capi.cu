@@ -1167,43 +1167,54 @@ tb_status tb_get_state(tb_plan* P, int field, void* data, int where) {
   });
 }
 
+}  // extern "C"
+
+namespace {
+// Copies of several 2D state fields on the plan's stream, one wait.  Fields
+// that are neighbours in the device state (b, u_x, u_z, p, then the taus, one
+// allocation) and whose caller buffers are neighbours too go as one copy.
+void copy_state_fields(tb_plan* P, int nfields, const int* fields, void* const* data, int where, bool to_device) {
+  TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "multi-field state I/O is for 2D plans (use the single-field call in 3D)");
+  for (int i = 0; i < nfields; ++i) {
+    TB_REQUIRE(fields[i] >= TB_FIELD_B && fields[i] <= TB_FIELD_TAU, TB_EINVAL, "bad field selector");
+    TB_REQUIRE(data[i] != nullptr, TB_EINVAL, "null field buffer");
+  }
+  auto dev = [&](int f) -> char* { return static_cast<char*>(f == TB_FIELD_TAU ? P->tau.p : (void*)P->Xp(f)); };
+  auto len = [&](int f) -> size_t { return f == TB_FIELD_TAU ? P->tau.bytes : P->plane * sizeof(double2); };
+  const cudaMemcpyKind kind = where == TB_DEVICE ? cudaMemcpyDeviceToDevice
+                                                 : (to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost);
+  for (int i = 0; i < nfields;) {
+    char* d0 = dev(fields[i]);
+    char* h0 = static_cast<char*>(data[i]);
+    size_t bytes = len(fields[i]);
+    int k = i + 1;
+    while (k < nfields && dev(fields[k]) == d0 + bytes && static_cast<char*>(data[k]) == h0 + bytes) {
+      bytes += len(fields[k]);
+      ++k;
+    }
+    if (to_device)
+      TB_CUDA_TRY(cudaMemcpyAsync(d0, h0, bytes, kind, P->st));
+    else
+      TB_CUDA_TRY(cudaMemcpyAsync(h0, d0, bytes, kind, P->st));
+    i = k;
+  }
+  TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+}
+}  // namespace
+
+extern "C" {
+
 tb_status tb_set_states(tb_plan* P, int nfields, const int* fields, const void* const* data, int where) {
   if (!P || nfields < 0 || (nfields > 0 && (!fields || !data))) return TB_EINVAL;
   return guard(P->ctx, [&] {
-    TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "multi-field state I/O is for 2D plans (use tb_set_state in 3D)");
-    for (int i = 0; i < nfields; ++i) {
-      TB_REQUIRE(fields[i] >= TB_FIELD_B && fields[i] <= TB_FIELD_TAU, TB_EINVAL, "bad field selector");
-      TB_REQUIRE(data[i] != nullptr, TB_EINVAL, "null field buffer");
-    }
-    for (int i = 0; i < nfields; ++i) {
-      const int f = fields[i];
-      void* dst = f == TB_FIELD_TAU ? P->tau.p : (void*)P->Xp(f);
-      const size_t bytes = f == TB_FIELD_TAU ? P->tau.bytes : P->plane * sizeof(double2);
-      TB_CUDA_TRY(cudaMemcpyAsync(dst, data[i], bytes,
-                                  where == TB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, P->st));
-    }
-    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+    copy_state_fields(P, nfields, fields, const_cast<void* const*>(data), where, true);
     P->ms_history = 0;  // a new state restarts multistep history
   });
 }
 
 tb_status tb_get_states(tb_plan* P, int nfields, const int* fields, void* const* data, int where) {
   if (!P || nfields < 0 || (nfields > 0 && (!fields || !data))) return TB_EINVAL;
-  return guard(P->ctx, [&] {
-    TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "multi-field state I/O is for 2D plans (use tb_get_state in 3D)");
-    for (int i = 0; i < nfields; ++i) {
-      TB_REQUIRE(fields[i] >= TB_FIELD_B && fields[i] <= TB_FIELD_TAU, TB_EINVAL, "bad field selector");
-      TB_REQUIRE(data[i] != nullptr, TB_EINVAL, "null field buffer");
-    }
-    for (int i = 0; i < nfields; ++i) {
-      const int f = fields[i];
-      const void* src = f == TB_FIELD_TAU ? P->tau.p : (const void*)P->Xp(f);
-      const size_t bytes = f == TB_FIELD_TAU ? P->tau.bytes : P->plane * sizeof(double2);
-      TB_CUDA_TRY(cudaMemcpyAsync(data[i], src, bytes,
-                                  where == TB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, P->st));
-    }
-    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
-  });
+  return guard(P->ctx, [&] { copy_state_fields(P, nfields, fields, data, where, false); });
 }
 
 tb_status tb_step(tb_plan* P, double dt, int nsteps) {

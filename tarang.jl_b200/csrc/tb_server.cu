@@ -168,6 +168,11 @@ std::unique_ptr<Job> make_job(tb_context* ctx, const Request& r) {
   tb_status st = tb_plan_create(ctx, &r.desc, &j->P);
   if (st != TB_OK) throw Error{st, ctx->last_error};
   tb_plan* P = j->P;
+  // Many requests share the device here, so the tau solves take the one-warp
+  // form: its blocks need a fifth of the shared memory of the partitioned
+  // form's, so several requests' solves share an SM instead of queueing for
+  // whole SMs (the throughput choice the ensemble tuner also makes).
+  if (plan_tau_parts_ok(P, 1)) plan_set_variant(P, 1, 0);
   // initial state: b from the grid field, u = 0
   StreamBuf grid, coeff;  // staging released in stream order: no device-wide wait
   grid.alloc(r.init.size() * sizeof(double), P->st);

@@ -55,3 +55,25 @@ def test_states_reject_bad_selectors_and_shapes(tb):
         plan.set_states({0: np.zeros((3, 3), np.complex128)})
     with pytest.raises(ValueError):
         plan.get_states({0: np.zeros(before.shape, np.complex64)})
+
+
+def test_states_through_one_contiguous_buffer(tb):
+    # adjacent host views in the device order go as one copy per direction
+    p = RBCParams(Nx=64, Nz=32, Lx=4.0, Lz=1.0, Ra=1e7)
+    a, b = _plan(tb, p), _plan(tb, p)
+    Nz, nk = p.Nz, p.Nx // 2 + 1
+    buf = np.empty((4 * Nz + 7) * nk, np.complex128)
+    views = {f: buf[f * Nz * nk:(f + 1) * Nz * nk].reshape(Nz, nk) for f in (0, 1, 2, 3)}
+    views[4] = buf[4 * Nz * nk:].reshape(7, nk)
+    a.get_states(views)
+    for f in FIELDS:
+        assert np.array_equal(views[f], a.get_state(f))
+    buf *= 1.0 + 1e-3 * np.cos(np.arange(buf.size))
+    a.set_states(views)
+    for f in FIELDS:
+        b.set_state(f, views[f])
+    a.step(0.01, 2)
+    b.step(0.01, 2)
+    a.get_states(views)
+    for f in FIELDS:
+        assert np.array_equal(views[f], b.get_state(f))
