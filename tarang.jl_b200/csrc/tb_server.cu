@@ -6,9 +6,10 @@
 //   - admission, in arrival order: the next queued request starts when its
 //     estimated device bytes fit the remaining budget and a run slot is free;
 //     it gets its own plan and stream;
-//   - progress: every running request whose previous chunk has finished gets
-//     its next chunk of steps (one CUDA graph launch on its own stream), so
-//     the chunks of all running requests overlap on the device and a request
+//   - progress: every running request keeps two chunks of steps (one CUDA
+//     graph launch each) queued on its own stream, the next behind the
+//     running one, so the chunks of all running requests overlap on the
+//     device, no stream waits for this loop to come round, and a request
 //     that arrives while others run joins as soon as memory frees up;
 //   - completion: the final state is copied to host memory, the plan and its
 //     device memory are released, and the time from submission is recorded.
@@ -35,6 +36,8 @@ namespace {
 
 // Host threads building admitted requests' plans: half the host's hardware
 // threads, 4 to 16 (plan construction is host work that overlaps the steps).
+constexpr int kChunksAhead = 2;  // graph launches queued per running request
+
 int setup_threads() {
   const unsigned hw = std::thread::hardware_concurrency();
   return (int)std::max(4u, std::min(16u, hw / 2));
@@ -111,8 +114,10 @@ struct Request {
   std::string error;
   size_t bytes = 0;
   std::unique_ptr<Job> job;
-  cudaEvent_t ev = nullptr;
-  bool chunk_pending = false;
+  // chunks in flight on the request's stream: up to kChunksAhead, each
+  // followed by an event (ev[head] marks the oldest)
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  int inflight = 0, head = 0;
   std::vector<std::vector<double>> result;
 };
 
@@ -239,7 +244,7 @@ void tb_server::setup_loop() {
       r->t_start = now_ms();
       r->job = make_job(ctx, *r);
       r->job->prepare(r->dt, chunk);
-      TB_CUDA_TRY(cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming));
+      for (auto& e : r->ev) TB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       r->t_ready = now_ms();
       std::lock_guard<std::mutex> lk(mu);
       setups.push_back(r->t_ready - r->t_start);
@@ -265,6 +270,10 @@ void tb_server::setup_loop() {
 
 void tb_server::fail_admitted(Request* r, const std::string& msg) {
   r->job.reset();
+  for (auto& e : r->ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
   std::lock_guard<std::mutex> lk(mu);
   used -= r->bytes;
   r->state = TB_REQ_FAILED;
@@ -281,31 +290,37 @@ void tb_server::progress() {
   }
   for (Request* r : act) {
     try {
-      if (r->chunk_pending) {
-        const cudaError_t e = cudaEventQuery(r->ev);
+      // retire the chunks that have finished, oldest first
+      while (r->inflight > 0) {
+        const cudaError_t e = cudaEventQuery(r->ev[r->head]);
         if (e == cudaErrorNotReady) {
           cudaGetLastError();
-          continue;
+          break;
         }
         if (e != cudaSuccess) throw Error{TB_ECUDA, std::string("request stream: ") + cudaGetErrorString(e)};
-        r->chunk_pending = false;
+        r->head ^= 1;
+        --r->inflight;
       }
-      if (r->left > 0) {
+      // keep the next chunk queued behind the running one, so the stream
+      // never waits for this loop to come round
+      while (r->left > 0 && r->inflight < kChunksAhead) {
         const int c = std::min(r->left, chunk);
         r->job->launch(r->dt, c);
-        TB_CUDA_TRY(cudaEventRecord(r->ev, r->job->stream()));
+        TB_CUDA_TRY(cudaEventRecord(r->ev[(r->head + r->inflight) & 1], r->job->stream()));
         r->left -= c;
-        r->chunk_pending = true;
-        continue;
+        ++r->inflight;
       }
+      if (r->left > 0 || r->inflight > 0) continue;
       // finished: result to host, device memory back to the pool
       r->result.resize(r->job->nfields());
       for (int f = 0; f < r->job->nfields(); ++f) {
         r->result[f].resize(r->job->field_doubles(f));
         r->job->fetch(f, r->result[f].data());
       }
-      cudaEventDestroy(r->ev);
-      r->ev = nullptr;
+      for (auto& e : r->ev) {
+        cudaEventDestroy(e);
+        e = nullptr;
+      }
       std::lock_guard<std::mutex> lk(mu);
       zombies.push_back(std::move(r->job));
       zombie_bytes += r->bytes;
@@ -329,8 +344,10 @@ void tb_server::progress() {
 
 void tb_server::fail_running(Request* r, const std::string& msg) {
   r->job.reset();
-  if (r->ev) cudaEventDestroy(r->ev);
-  r->ev = nullptr;
+  for (auto& e : r->ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
   std::lock_guard<std::mutex> lk(mu);
   r->state = TB_REQ_FAILED;
   r->error = msg;
