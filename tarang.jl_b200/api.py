@@ -187,12 +187,15 @@ class Plan:
 
     # state I/O (host numpy, coefficient layout (Nz, Nk) complex128)
     def set_state(self, field: int, arr: np.ndarray) -> None:
+        # the C call reads the field's whole extent from the pointer, so the
+        # host array must have exactly the field's shape
         a = np.ascontiguousarray(arr, dtype=np.complex128)
+        if a.shape != self._field_shape(field):
+            raise ValueError(f"field {field}: shape {a.shape}, expected {self._field_shape(field)}")
         check(lib.tb_set_state(self.ptr, field, a.ctypes.data_as(c_void_p), L.TB_HOST), self.ctx)
 
     def get_state(self, field: int) -> np.ndarray:
-        shape = (7, self.domain.Nk) if field == L.TB_FIELD_TAU else (self.domain.Nz, self.domain.Nk)
-        out = np.empty(shape, np.complex128)
+        out = np.empty(self._field_shape(field), np.complex128)
         check(lib.tb_get_state(self.ptr, field, out.ctypes.data_as(c_void_p), L.TB_HOST), self.ctx)
         return out
 
@@ -385,7 +388,8 @@ class Plan3D(Plan):
 
     def set_state(self, field: int, arr: np.ndarray) -> None:
         a = np.ascontiguousarray(arr, dtype=np.complex128)
-        assert a.shape == self._shape(field), (a.shape, self._shape(field))
+        if a.shape != self._shape(field):
+            raise ValueError(f"field {field}: shape {a.shape}, expected {self._shape(field)}")
         check(lib.tb_set_state(self.ptr, field, a.ctypes.data_as(c_void_p), L.TB_HOST), self.ctx)
 
     def get_state(self, field: int) -> np.ndarray:

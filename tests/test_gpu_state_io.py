@@ -54,6 +54,9 @@ def test_states_reject_bad_selectors_and_shapes(tb):
     with pytest.raises(ValueError):
         plan.set_states({0: np.zeros((3, 3), np.complex128)})
     with pytest.raises(ValueError):
+        plan.set_state(0, np.zeros((3, 3), np.complex128))  # would read past the array
+    assert np.array_equal(plan.get_state(0), before)
+    with pytest.raises(ValueError):
         plan.get_states({0: np.zeros(before.shape, np.complex64)})
 
 
