@@ -67,13 +67,13 @@ def parse_args():
 # distributed plumbing (replicas only; used for the barrier and the max)
 # ---------------------------------------------------------------------------
 class Dist:
-    def __init__(self):
+    def __init__(self, collectives: bool = True):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
         self.backend = None
-        if self.world > 1:
+        if self.world > 1 and collectives:
             import datetime
 
             import torch
@@ -1068,7 +1068,10 @@ def fp64_peak_tflops():
 
 def main():
     args = parse_args()
-    dist = Dist()
+    # The CPU reference leg runs on rank 0 alone and needs no collectives: the
+    # other ranks leave at once instead of waiting in a barrier for the
+    # minutes of host work on rank 0.
+    dist = Dist(collectives=args.impl != "reference")
     if args.gpus is None:
         args.gpus = dist.world
     sys.path.insert(0, os.path.join(ROOT, "tarang.jl_b200"))

@@ -37,17 +37,23 @@ def test_dist_barrier_and_max_over_ranks():
 
 
 def test_reference_arm_prints_once_under_two_ranks():
+    # rank 0 alone runs the CPU leg; the other rank leaves at once (no process
+    # group, so it never waits in a barrier for rank 0's minutes of host work)
     code = (
-        "import sys\n"
+        "import sys, time\n"
         "sys.argv = ['bench.py', '--impl', 'reference', '--config', 'c1', '--steps', '1', '--warmup', '0']\n"
         "import bench\n"
+        "t0 = time.perf_counter()\n"
         "bench.main()\n"
+        "print('ELAPSED', time.perf_counter() - t0)\n"
     )
     res = _run_two_ranks(code, 29623)
     assert all(rc == 0 for rc, _, _ in res), [e[-2000:] for _, _, e in res]
     lines0 = [l for l in res[0][1].splitlines() if l.startswith("{")]
     lines1 = [l for l in res[1][1].splitlines() if l.startswith("{")]
     assert len(lines0) == 1 and not lines1
+    el = [float(next(l for l in out.splitlines() if l.startswith("ELAPSED")).split()[1]) for _, out, _ in res]
+    assert el[1] < 0.5 * el[0], el
     d = json.loads(lines0[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0
 
