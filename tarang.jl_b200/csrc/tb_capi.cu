@@ -68,11 +68,15 @@ thread_local std::string g_err;
 }  // namespace
 
 void tb::set_thread_error(const std::string& msg) { g_err = msg; }
+void tb::set_context_error(tb_context* ctx, const std::string& msg) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->last_error = msg;
+}
 
 namespace {
 
 tb_status fail(tb_context* ctx, const Error& e) {
-  if (ctx) ctx->last_error = e.msg;
+  if (ctx) set_context_error(ctx, e.msg);
   g_err = e.msg;
   return e.code;
 }
@@ -933,7 +937,15 @@ tb_status tb_context_destroy(tb_context* ctx) {
   return TB_OK;
 }
 
-const char* tb_last_error(const tb_context* ctx) { return ctx ? ctx->last_error.c_str() : g_err.c_str(); }
+const char* tb_last_error(const tb_context* ctx) {
+  if (!ctx) return g_err.c_str();
+  // a per-thread copy, so another thread's failure cannot move the string
+  // under the caller
+  thread_local std::string copy;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  copy = ctx->last_error;
+  return copy.c_str();
+}
 
 }  // extern "C"
 

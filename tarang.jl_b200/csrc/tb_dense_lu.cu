@@ -145,12 +145,12 @@ tb_status tb_batched_lu_factor(tb_context* ctx, int n, int batch, double* A, int
   if (e == cudaSuccess) e = cudaMemcpy(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost);
   cudaFree(dbad);
   if (e != cudaSuccess) {
-    ctx->last_error = std::string("batched LU factor: ") + cudaGetErrorString(e);
+    tb::set_context_error(ctx, std::string("batched LU factor: ") + cudaGetErrorString(e));
     return TB_ECUDA;
   }
   if (bad != init) {
     if (bad_slice) *bad_slice = bad;
-    ctx->last_error = "singular matrix in batched LU at slice " + std::to_string(bad);
+    tb::set_context_error(ctx, "singular matrix in batched LU at slice " + std::to_string(bad));
     return TB_ESINGULAR;
   }
   if (bad_slice) *bad_slice = -1;
@@ -163,7 +163,7 @@ tb_status tb_batched_lu_solve(tb_context* ctx, int n, int batch, const double* A
   cudaError_t e = cudaDeviceSynchronize();
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
-    ctx->last_error = std::string("batched LU solve: ") + cudaGetErrorString(e);
+    tb::set_context_error(ctx, std::string("batched LU solve: ") + cudaGetErrorString(e));
     return TB_ECUDA;
   }
   return TB_OK;

@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -13,7 +14,10 @@
 
 struct tb_context {
   int device = 0;
+  // message of the context's last failure; written under mu (several threads
+  // may use plans of one context), read through tb_last_error
   std::string last_error;
+  mutable std::mutex mu;
 };
 
 namespace tb {
@@ -83,6 +87,8 @@ struct TauLayout {
   ClassLayout cls[2];
 };
 
+// Records the message of a failure in the context (under its mutex).
+void set_context_error(tb_context* ctx, const std::string& msg);
 // Records a message for tb_last_error(NULL) on the calling thread.
 void set_thread_error(const std::string& msg);
 

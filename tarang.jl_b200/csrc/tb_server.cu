@@ -171,7 +171,7 @@ std::unique_ptr<Job> make_job(tb_context* ctx, const Request& r) {
   }
   auto j = std::make_unique<RbcJob>();
   tb_status st = tb_plan_create(ctx, &r.desc, &j->P);
-  if (st != TB_OK) throw Error{st, ctx->last_error};
+  if (st != TB_OK) throw Error{st, tb_last_error(nullptr)};  // this thread's message
   tb_plan* P = j->P;
   // Many requests share the device here, so the tau solves take the one-warp
   // form: its blocks need a fifth of the shared memory of the partitioned
@@ -184,7 +184,7 @@ std::unique_ptr<Job> make_job(tb_context* ctx, const Request& r) {
   coeff.alloc(P->plane * sizeof(double2), P->st);
   TB_CUDA_TRY(cudaMemcpyAsync(grid.p, r.init.data(), grid.bytes, cudaMemcpyHostToDevice, P->st));
   st = tb_transform_forward(P, grid.as<double>(), coeff.as<double>(), 1);
-  if (st != TB_OK) throw Error{st, ctx->last_error};
+  if (st != TB_OK) throw Error{st, tb_last_error(nullptr)};  // this thread's message
   TB_CUDA_TRY(cudaMemsetAsync(P->X.p, 0, P->X.bytes, P->st));
   TB_CUDA_TRY(cudaMemcpyAsync(P->Xp(0), coeff.p, coeff.bytes, cudaMemcpyDeviceToDevice, P->st));
   TB_CUDA_TRY(cudaStreamSynchronize(P->st));
@@ -425,7 +425,7 @@ tb_status tb_server_poll(tb_server* S, long long id, int* state, double* tts_ms)
   if (it == S->all.end()) return TB_EINVAL;
   *state = it->second->state;
   if (tts_ms) *tts_ms = it->second->state == TB_REQ_DONE ? it->second->t_done - it->second->t_submit : -1.0;
-  if (it->second->state == TB_REQ_FAILED) S->ctx->last_error = it->second->error;
+  if (it->second->state == TB_REQ_FAILED) set_context_error(S->ctx, it->second->error);
   return TB_OK;
 }
 
