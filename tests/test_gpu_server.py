@@ -78,3 +78,27 @@ def test_admission_respects_budget(tb):
     assert s.poll(bid)[0] == tb._lib.TB_REQ_FAILED
     s.close()
     del rid, ids
+
+
+def test_failing_requests_do_not_disturb_the_others(tb):
+    # kappa = 0 passes submission and fails in the plan build on a setup
+    # thread; those requests end FAILED with the build's message while the
+    # valid ones, built concurrently on other setup threads, complete
+    good, bad = [], []
+    s = tb.Server(budget_bytes=1 << 30, max_running=8, chunk_steps=3)
+    for k in range(6):
+        p, d, b0 = rbc_req(tb, 32, 16, 1e6, 300 + k)
+        if k % 2:
+            d.kappa = 0.0
+            bad.append(s.submit(d, 0.02, 6, b0))
+        else:
+            good.append(s.submit(d, 0.02, 6, b0))
+    s.wait_all()
+    for rid in good:
+        assert s.poll(rid)[0] == tb._lib.TB_REQ_DONE
+    for rid in bad:
+        assert s.poll(rid)[0] == tb._lib.TB_REQ_FAILED
+        assert b"kappa and nu must be positive" in tb.lib.tb_last_error(s.ctx)
+    st = s.stats()
+    assert st["completed"] == len(good) and st["failed"] == len(bad)
+    s.close()
