@@ -286,8 +286,10 @@ tb_status tb_ensemble_run(tb_ensemble* ens, const double* dt, int nsteps, float*
 
 /* -------------------------------------------------------------------------
  * 2D decaying turbulence, FP32.  Replaces the reference's DiagonalIMEX_SBDF2
- * step for a doubly periodic RealFourier x RealFourier problem
- * (src/core/timesteppers/step_diagonal_imex.jl:329-388, 674-689) with the
+ * step (desc->timestepper TB_SBDF2; src/core/timesteppers/
+ * step_diagonal_imex.jl:329-388, 674-689) or DiagonalIMEX_RK222 / RK443 step
+ * (TB_RK222 / TB_RK443; _step_diagonal_imex_rk_impl!, :183-296, with the full
+ * ESDIRK tableau) for a doubly periodic RealFourier x RealFourier problem, with the
  * spectral Poisson and velocity refresh (state_utils.jl:1059-1104) and the
  * 3/2-padded products with symmetric Nyquist split/fold
  * (nonlinear_padding.jl:182-443).  q0_spec: initial vorticity coefficients,

@@ -828,6 +828,54 @@ def run_turb(q0: np.ndarray, Nx: int, Lx: float, Ly: float, nu: float, dt: float
     return q
 
 
+def turb_step_rk(q: np.ndarray, Nx: int, Lx: float, Ly: float, nu: float, dt: float, ts: dict) -> np.ndarray:
+    """One DiagonalIMEX_RK222 / RK443 step (_step_diagonal_imex_rk_impl!,
+    step_diagonal_imex.jl:183-296; tableaus types.jl:511-620, the same numbers
+    as the subproblem RK222 / RK443) with L^ = nu k^2:
+      Y_s = q_n + dt sum_{j<s} (AE_sj F_j - AI_sj L^ Y_j),  Y_s /= 1 + dt AI_ss L^
+      F_s = RHS(Y_s)
+      q_{n+1} = q_n + dt sum_s (bE_s F_s - bI_s L^ Y_s).
+    Stage states stay in coefficients (no grid round trip between stages); the
+    RHS does its own, as in the reference's evaluate_rhs."""
+    Ny = q.shape[0]
+    kx, ky = turb_wavenumbers(Nx, Ny, Lx, Ly)
+    L = nu * (kx ** 2 + ky ** 2)
+    AE, AI, bE, bI = ts["AE"], ts["AI"], ts["bE"], ts["bI"]
+    s = AE.shape[0]
+    Y: List[np.ndarray] = []
+    F: List[Optional[np.ndarray]] = []
+    for i in range(s):
+        y = q.copy()
+        for j in range(i):
+            if abs(AE[i, j]) > 1e-14:
+                y += dt * AE[i, j] * F[j]
+            if abs(AI[i, j]) > 1e-14:
+                y -= dt * AI[i, j] * L * Y[j]
+        if abs(AI[i, i]) > 1e-14:
+            y = y / (1.0 + dt * AI[i, i] * L)
+        Y.append(y)
+        # F_s enters a later stage or the update only where its weight is
+        # nonzero (the first stage's never is in these tableaus)
+        used = abs(bE[i]) > 1e-14 or any(abs(AE[k, i]) > 1e-14 for k in range(i + 1, s))
+        F.append(turb_rhs(y, Nx, Lx, Ly) if used else None)
+    out = q.copy()
+    for i in range(s):
+        if abs(bE[i]) > 1e-14:
+            out += dt * bE[i] * F[i]
+        if abs(bI[i]) > 1e-14:
+            out -= dt * bI[i] * L * Y[i]
+    return out
+
+
+def run_turb_rk(q0: np.ndarray, Nx: int, Lx: float, Ly: float, nu: float, dt: float, nsteps: int,
+                scheme: str = "RK222") -> np.ndarray:
+    """nsteps DiagonalIMEX_RK222 / RK443 steps of constant dt."""
+    q = q0.copy()
+    for _ in range(nsteps):
+        q = turb_step_rk(q, Nx, Lx, Ly, nu, dt, TABLEAUS[scheme])
+    return q
+
+
 def turb_initial_spec(Nx: int, Ny: int, seed: int, kmin: float = 1.0, kmax: Optional[float] = None,
                       amp: float = 10.0) -> np.ndarray:
     """Seeded initial vorticity with a k^-3 energy spectrum (|q^| ~ 1/k per mode

@@ -498,15 +498,17 @@ class Ensemble:
 
 
 class Turb2D:
-    """Doubly periodic 2D decaying turbulence in FP32 (DiagonalIMEX_SBDF2), the
-    reference's examples/2d_decaying_turbulence_gpu.jl on the C ABI.
-    Coefficients are complex (Ny, Nx/2+1) arrays (rfft along x, fft along y)."""
+    """Doubly periodic 2D decaying turbulence in FP32 (DiagonalIMEX_SBDF2 by
+    default, or DiagonalIMEX_RK222 / RK443 with timestepper=TB_RK222 /
+    TB_RK443), the reference's examples/2d_decaying_turbulence_gpu.jl on the C
+    ABI.  Coefficients are complex (Ny, Nx/2+1) arrays (rfft along x, fft
+    along y)."""
 
     def __init__(self, Nx: int, Ny: int, nu: float, q0_spec: np.ndarray, Lx: float = 2 * math.pi,
-                 Ly: float = 2 * math.pi, device: int = 0):
+                 Ly: float = 2 * math.pi, device: int = 0, timestepper: int = L.TB_SBDF2):
         self.Nx, self.Ny = int(Nx), int(Ny)
         self.ctx = _context(device)
-        d = turb_desc(Nx, Ny, nu, Lx, Ly)
+        d = turb_desc(Nx, Ny, nu, Lx, Ly, timestepper)
         q = np.ascontiguousarray(q0_spec, dtype=np.complex128)
         assert q.shape == (self.Ny, self.Nx // 2 + 1)
         self.ptr = c_void_p()
@@ -527,11 +529,15 @@ class Turb2D:
         return out
 
 
-def turb_desc(Nx: int, Ny: int, nu: float, Lx: float = 2 * math.pi, Ly: float = 2 * math.pi):
+def turb_desc(Nx: int, Ny: int, nu: float, Lx: float = 2 * math.pi, Ly: float = 2 * math.pi,
+              timestepper: int = L.TB_SBDF2):
+    """Descriptor of the doubly periodic vorticity problem; timestepper
+    TB_SBDF2 (DiagonalIMEX_SBDF2), TB_RK222 or TB_RK443 (DiagonalIMEX_RK222 /
+    RK443)."""
     d = L.tb_problem_desc()
     d.ndim, d.Nx, d.Ny, d.Nz = 2, int(Nx), int(Ny), 1
     d.Lx, d.Ly, d.Lz, d.dealias = float(Lx), float(Ly), 1.0, 1.5
-    d.precision, d.timestepper, d.program = 0, L.TB_SBDF2, L.TB_PROGRAM_TURB2D
+    d.precision, d.timestepper, d.program = 0, int(timestepper), L.TB_PROGRAM_TURB2D
     d.kappa, d.nu, d.b_bottom, d.b_top = 0.0, float(nu), 0.0, 0.0
     return d
 

@@ -94,7 +94,7 @@ struct TurbJob : Job {
 
 // Device bytes a run of this size will hold (plan, factors, graphs' scratch).
 size_t estimate_bytes(const tb_problem_desc& d) {
-  if (d.program == TB_PROGRAM_TURB2D) return turb_estimate_bytes(d.Nx, d.Ny);
+  if (d.program == TB_PROGRAM_TURB2D) return turb_estimate_bytes(d.Nx, d.Ny, d.timestepper);
   const size_t nk = d.Nx / 2 + 1, plane = (size_t)d.Nz * nk * 16;
   const size_t npad = ((size_t)2 * d.Nz + kTauRowPad - 1) / kTauRowPad * kTauRowPad;
   const size_t groups = (nk + kSolveModes - 1) / kSolveModes;

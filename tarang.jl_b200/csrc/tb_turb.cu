@@ -16,9 +16,14 @@
 //   3/2 padding in x and y with the even-N Nyquist split X/2 at +-N/2, product
 //   on the padded grid, forward transform, fold of the -N/2 images into +N/2
 //   and truncation                                nonlinear_padding.jl:182-443
-// The step (step_diagonal_imex.jl:674-689, constant dt, L^ = nu k^2):
+// DiagonalIMEX_SBDF2 (step_diagonal_imex.jl:674-689, constant dt, L^ = nu k^2):
 //   first step  q1 = (q0 + dt F0) / (1 + dt L^)
 //   then        q_{n+1} = (2 q_n - q_{n-1}/2 + dt (2 F_n - F_{n-1})) / (3/2 + dt L^)
+// DiagonalIMEX_RK222 / RK443 (_step_diagonal_imex_rk_impl!,
+// step_diagonal_imex.jl:183-296; the full ESDIRK tableau, types.jl:511-620):
+//   Y_s = q_n + dt sum_{j<s} (AE_sj F_j - AI_sj L^ Y_j),  Y_s /= 1 + dt AI_ss L^
+//   F_s = RHS(Y_s);  q_{n+1} = q_n + dt sum_s (bE_s F_s - bI_s L^ Y_s)
+// (a stage RHS whose weights are all zero, the first stage's, is skipped).
 //
 // Kernels per step: k_turb_yinv (per kx column: derived fields, projection,
 // y padding, 4 inverse FFTs along y), transpose, k_turb_xpass (per padded y
@@ -51,6 +56,12 @@ struct tb_turb {
   DevBuf mix, mixT;        // 4 x [Kx][My] and 4 x [My][Kx]
   DevBuf pm, pmT;          // [My][Kx] and [Kx][My]
   DevBuf ptx, pty;         // per-pass twiddles (FP32) of the Mx and My plans
+  // DiagonalIMEX RK (rk true): tableau and per-stage states / right-hand sides
+  bool rk = false;
+  int stages = 0;
+  double AE[4][4] = {}, AI[4][4] = {}, bE[4] = {}, bI[4] = {};
+  bool f_used[4] = {};
+  DevBuf Ys[4], Fs[4];     // Y_s (s >= 1; Y_0 is q_n) and F_s where used
   int cur = 0;             // Q[cur] holds q_n
   long long iteration = 0;
   double graph_dt = -1.0;
@@ -77,6 +88,42 @@ struct TurbArgs {
 };
 
 __device__ __forceinline__ float ky_of(int ky, int Ny) { return (float)(ky < Ny / 2 ? ky : ky - Ny); }
+
+// Stage combination of the diagonal IMEX RK step over [kx][ky]:
+//   out = (base + sum_t w_t (L^ if isL_t) src_t) / (1 + dgam L^),  L^ = nu k^2.
+constexpr int kCombMax = 8;
+struct TurbComb {
+  const float2* base;
+  const float2* src[kCombMax];
+  float w[kCombMax];
+  int isL[kCombMax];
+  int n;
+  float dgam;
+  float2* out;
+};
+
+__global__ void __launch_bounds__(256) k_turb_combine(TurbArgs a, TurbComb c) {
+  const size_t total = (size_t)a.Kx * a.Ny;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int kx = (int)(e / a.Ny), ky = (int)(e % a.Ny);
+    const float kxv = a.kx0 * kx, kyv = a.ky0 * ky_of(ky, a.Ny);
+    const float L = a.nu * (kxv * kxv + kyv * kyv);
+    float2 acc = c.base[e];
+#pragma unroll
+    for (int t = 0; t < kCombMax; ++t) {
+      if (t < c.n) {
+        const float2 v = c.src[t][e];
+        const float wt = c.isL[t] ? c.w[t] * L : c.w[t];
+        acc = F::mk<float2>(fmaf(wt, v.x, acc.x), fmaf(wt, v.y, acc.y));
+      }
+    }
+    if (c.dgam != 0.f) {
+      const float den = 1.0f / (1.0f + c.dgam * L);
+      acc = F::mk<float2>(acc.x * den, acc.y * den);
+    }
+    c.out[e] = acc;
+  }
+}
 
 // Per kx column: the four factors u, v, d_x q, d_y q of the products, with the
 // grid round trip's projection, the x Nyquist split and the y padding, inverse
@@ -207,7 +254,8 @@ __global__ void __launch_bounds__(kTurbThreads) k_turb_xpass(TurbArgs a, const f
 // Per kx column: forward FFT along y, the Nyquist folds and truncation to Ny,
 // F = -(...) / (Nx Ny Mx My), and the SBDF1 / SBDF2 update in place.
 //   qn: q_n [Kx][Ny];  qo: q_{n-1} on entry, q_{n+1} on exit;  Fp: F_{n-1} on
-//   entry, F_n on exit.  first: SBDF1 startup (q_{n+1} written to qo).
+//   entry, F_n on exit.  first: 1 SBDF1 startup (q_{n+1} written to qo),
+//   0 SBDF2, 2 the right-hand side alone (Fp = F; qn and qo untouched).
 __global__ void __launch_bounds__(kTurbThreads) k_turb_yfwd(TurbArgs a, const float2* __restrict__ pmT,
                                                             const float2* __restrict__ qn, float2* __restrict__ qo,
                                                             float2* __restrict__ Fp, float dt, int first) {
@@ -244,9 +292,13 @@ __global__ void __launch_bounds__(kTurbThreads) k_turb_yfwd(TurbArgs a, const fl
       r = qf(My - Ny + ky);
     }
     const float2 Fn = F::scale(r, sc);
+    const size_t e = (size_t)kx * Ny + ky;
+    if (first == 2) {
+      Fp[e] = Fn;
+      continue;
+    }
     const float kyv = a.ky0 * ky_of(ky, Ny);
     const float L = a.nu * (kxv * kxv + kyv * kyv);
-    const size_t e = (size_t)kx * Ny + ky;
     const float2 q0 = qn[e];
     float2 q1;
     if (first) {
@@ -295,20 +347,74 @@ TurbArgs args_of(const tb_turb* T) {
   return a;
 }
 
-void enqueue_step(tb_turb* T, double dt, int first) {
+// The RHS chain on q, ending in k_turb_yfwd with mode first (see there).
+void enqueue_rhs(tb_turb* T, const float2* q, float2* qo, float2* Fp, double dt, int first) {
   const TurbArgs a = args_of(T);
-  float2* qn = T->Q[T->cur].as<float2>();
-  float2* qo = T->Q[1 - T->cur].as<float2>();
   float2* mix = T->mix.as<float2>();
   float2* mixT = T->mixT.as<float2>();
-  k_turb_yinv<<<T->Kx, kTurbThreads, yinv_smem(T), T->st>>>(a, qn, mix);
+  k_turb_yinv<<<T->Kx, kTurbThreads, yinv_smem(T), T->st>>>(a, q, mix);
   dim3 tb(32, 8);
   k_transpose_c64<<<dim3((T->My + 31) / 32, (T->Kx + 31) / 32, 4), tb, 0, T->st>>>(mix, mixT, T->Kx, T->My);
   k_turb_xpass<<<T->My, kTurbThreads, xpass_smem(T), T->st>>>(a, mixT, T->pm.as<float2>());
   k_transpose_c64<<<dim3((T->Kx + 31) / 32, (T->My + 31) / 32, 1), tb, 0, T->st>>>(T->pm.as<float2>(),
                                                                                    T->pmT.as<float2>(), T->My, T->Kx);
-  k_turb_yfwd<<<T->Kx, kTurbThreads, yfwd_smem(T), T->st>>>(a, T->pmT.as<float2>(), qn, qo, T->Fb.as<float2>(),
-                                                             (float)dt, first);
+  k_turb_yfwd<<<T->Kx, kTurbThreads, yfwd_smem(T), T->st>>>(a, T->pmT.as<float2>(), q, qo, Fp, (float)dt, first);
+}
+
+void launch_combine(tb_turb* T, const TurbComb& c) {
+  const size_t total = (size_t)T->Kx * T->Ny;
+  int blocks = (int)((total + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  k_turb_combine<<<blocks, 256, 0, T->st>>>(args_of(T), c);
+}
+
+// One DiagonalIMEX RK step from Q[cur] into Q[1 - cur].
+void enqueue_rk_step(tb_turb* T, double dt) {
+  float2* qn = T->Q[T->cur].as<float2>();
+  float2* qo = T->Q[1 - T->cur].as<float2>();
+  const float2* Y[4] = {qn, nullptr, nullptr, nullptr};
+  auto add = [&](TurbComb& c, const float2* src, double w, int isL) {
+    if (c.n >= kCombMax) throw Error{TB_EINVAL, "too many stage terms"};
+    c.src[c.n] = src;
+    c.w[c.n] = (float)w;
+    c.isL[c.n] = isL;
+    ++c.n;
+  };
+  const int s = T->stages;
+  for (int i = 0; i < s; ++i) {
+    if (i > 0) {
+      TurbComb c{};
+      c.base = qn;
+      for (int j = 0; j < i; ++j) {
+        if (std::fabs(T->AE[i][j]) > 1e-14) add(c, T->Fs[j].as<float2>(), dt * T->AE[i][j], 0);
+        if (std::fabs(T->AI[i][j]) > 1e-14) add(c, Y[j], -dt * T->AI[i][j], 1);
+      }
+      c.dgam = std::fabs(T->AI[i][i]) > 1e-14 ? (float)(dt * T->AI[i][i]) : 0.f;
+      c.out = T->Ys[i].as<float2>();
+      launch_combine(T, c);
+      Y[i] = T->Ys[i].as<float2>();
+    }
+    if (T->f_used[i]) enqueue_rhs(T, Y[i], nullptr, T->Fs[i].as<float2>(), dt, 2);
+  }
+  TurbComb c{};
+  c.base = qn;
+  for (int i = 0; i < s; ++i) {
+    if (std::fabs(T->bE[i]) > 1e-14) add(c, T->Fs[i].as<float2>(), dt * T->bE[i], 0);
+    if (std::fabs(T->bI[i]) > 1e-14) add(c, Y[i], -dt * T->bI[i], 1);
+  }
+  c.dgam = 0.f;
+  c.out = qo;
+  launch_combine(T, c);
+}
+
+void enqueue_step(tb_turb* T, double dt, int first) {
+  if (T->rk) {
+    enqueue_rk_step(T, dt);
+    return;
+  }
+  float2* qn = T->Q[T->cur].as<float2>();
+  float2* qo = T->Q[1 - T->cur].as<float2>();
+  enqueue_rhs(T, qn, qo, T->Fb.as<float2>(), dt, first);
 }
 
 std::vector<float2> pass_twiddles_f(const FftPlan& fp) {
@@ -346,10 +452,13 @@ cudaGraphExec_t capture(tb_turb* T, double dt) {
 
 }  // namespace
 
-size_t tb::turb_estimate_bytes(int Nx, int Ny) {
+size_t tb::turb_estimate_bytes(int Nx, int Ny, int timestepper) {
   const size_t Kx = Nx / 2 + 1, Mx = padded_len(Nx), My = padded_len(Ny);
   (void)Mx;
-  return sizeof(float2) * (3 * Kx * Ny + 8 * Kx * My + 2 * Kx * My) + (4u << 20);
+  // SBDF2: q_n, q_{n-1}, F_{n-1}; RK: q_n, q_{n+1} and up to 3 stage states
+  // and 3 stage right-hand sides (4 stages, the first state and RHS not kept)
+  const size_t specs = timestepper == TB_SBDF2 ? 3 : (timestepper == TB_RK222 ? 6 : 8);
+  return sizeof(float2) * (specs * Kx * Ny + 8 * Kx * My + 2 * Kx * My) + (4u << 20);
 }
 
 tb_turb* tb::turb_create(tb_context* ctx, const tb_problem_desc& d, const double* q0) {
@@ -359,7 +468,28 @@ tb_turb* tb::turb_create(tb_context* ctx, const tb_problem_desc& d, const double
   TB_REQUIRE(d.Lx > 0 && d.Ly > 0 && d.nu >= 0, TB_EINVAL, "bad lengths or viscosity");
   TB_REQUIRE(std::fabs(d.dealias - 1.5) < 1e-12, TB_ENOTSUPPORTED, "only dealias = 3/2 is implemented");
   TB_REQUIRE(q0 != nullptr, TB_EINVAL, "null initial vorticity");
+  TB_REQUIRE(d.timestepper == TB_SBDF2 || d.timestepper == TB_RK222 || d.timestepper == TB_RK443, TB_ENOTSUPPORTED,
+             "turbulence steps: DiagonalIMEX SBDF2, RK222 or RK443");
   auto T = std::make_unique<tb_turb>();
+  if (d.timestepper != TB_SBDF2) {
+    const Tableau tb_ = tableau(d.timestepper);
+    T->rk = true;
+    T->stages = tb_.s;
+    for (int i = 0; i < tb_.s; ++i) {
+      T->bE[i] = tb_.bE[i];
+      T->bI[i] = tb_.bI[i];
+      for (int j = 0; j < tb_.s; ++j) {
+        T->AE[i][j] = tb_.AE[i][j];
+        T->AI[i][j] = tb_.AI[i][j];
+      }
+    }
+    // F_s is computed only where a later stage or the update weighs it
+    for (int i = 0; i < tb_.s; ++i) {
+      bool used = std::fabs(tb_.bE[i]) > 1e-14;
+      for (int k = i + 1; k < tb_.s; ++k) used = used || std::fabs(tb_.AE[k][i]) > 1e-14;
+      T->f_used[i] = used;
+    }
+  }
   T->ctx = ctx;
   T->Nx = d.Nx;
   T->Ny = d.Ny;
@@ -375,7 +505,13 @@ tb_turb* tb::turb_create(tb_context* ctx, const tb_problem_desc& d, const double
   TB_CUDA_TRY(cudaStreamCreateWithFlags(&T->st, cudaStreamNonBlocking));
   const size_t spec = (size_t)T->Kx * T->Ny * sizeof(float2);
   for (auto& b : T->Q) b.alloc(spec);
-  T->Fb.alloc(spec);
+  if (T->rk) {
+    for (int i = 1; i < T->stages; ++i) T->Ys[i].alloc(spec);
+    for (int i = 0; i < T->stages; ++i)
+      if (T->f_used[i]) T->Fs[i].alloc(spec);
+  } else {
+    T->Fb.alloc(spec);
+  }
   T->mix.alloc(4 * (size_t)T->Kx * T->My * sizeof(float2));
   T->mixT.alloc(T->mix.bytes);
   T->pm.alloc((size_t)T->Kx * T->My * sizeof(float2));
@@ -400,7 +536,7 @@ tb_turb* tb::turb_create(tb_context* ctx, const tb_problem_desc& d, const double
   // ordered after the initialisation
   TB_CUDA_TRY(cudaMemcpyAsync(T->Q[0].p, h.data(), spec, cudaMemcpyHostToDevice, T->st));
   TB_CUDA_TRY(cudaMemsetAsync(T->Q[1].p, 0, spec, T->st));
-  TB_CUDA_TRY(cudaMemsetAsync(T->Fb.p, 0, spec, T->st));
+  if (T->Fb.p) TB_CUDA_TRY(cudaMemsetAsync(T->Fb.p, 0, spec, T->st));
   TB_CUDA_TRY(cudaStreamSynchronize(T->st));
   return T.release();
 }
@@ -440,8 +576,10 @@ void tb::turb_launch_steps(tb_turb* T, double dt, int steps) {
 }
 
 size_t tb::turb_device_bytes(const tb_turb* T) {
-  return T->Q[0].bytes + T->Q[1].bytes + T->Fb.bytes + T->mix.bytes + T->mixT.bytes + T->pm.bytes + T->pmT.bytes +
-         T->ptx.bytes + T->pty.bytes;
+  size_t b = T->Q[0].bytes + T->Q[1].bytes + T->Fb.bytes + T->mix.bytes + T->mixT.bytes + T->pm.bytes +
+             T->pmT.bytes + T->ptx.bytes + T->pty.bytes;
+  for (int i = 0; i < 4; ++i) b += T->Ys[i].bytes + T->Fs[i].bytes;
+  return b;
 }
 
 size_t tb::turb_field_doubles(const tb_turb* T) { return 2 * (size_t)T->Kx * T->Ny; }

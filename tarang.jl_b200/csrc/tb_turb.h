@@ -23,6 +23,6 @@ size_t turb_device_bytes(const tb_turb* T);
 size_t turb_field_doubles(const tb_turb* T);
 // Vorticity coefficients to host, complex128 (Nx/2+1, Ny), x fastest (waits).
 void turb_fetch(tb_turb* T, double* host);
-size_t turb_estimate_bytes(int Nx, int Ny);
+size_t turb_estimate_bytes(int Nx, int Ny, int timestepper);
 
 }  // namespace tb

@@ -24,6 +24,9 @@ def test_results_same_alone_and_in_mix(tb):
         reqs.append(("rbc", d, 0.02, 12 + 3 * k, b0))
     for k, (N, M) in enumerate([(32, 32), (64, 48)]):
         reqs.append(("turb", tb.turb_desc(N, M, 1e-3), 2e-3, 10 + k, turb_initial_spec(N, M, seed=200 + k)))
+    # a DiagonalIMEX RK443 turbulence request beside the SBDF2 ones
+    reqs.append(("turb", tb.turb_desc(32, 32, 1e-3, timestepper=tb._lib.TB_RK443), 2e-3, 7,
+                 turb_initial_spec(32, 32, seed=210)))
     alone = []
     for _, d, dt, n, init in reqs:
         s = tb.Server(budget_bytes=1 << 30, max_running=1, chunk_steps=4)

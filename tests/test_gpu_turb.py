@@ -41,3 +41,34 @@ def test_turbulence_single_mode_decays_exactly(tb):
     t = tb.Turb2D(Nx, Ny, nu, q0)
     t.step(dt, 1)
     assert np.abs(t.vorticity() - q0 / (1 + dt * nu * 5.0)).max() < 1e-5 * np.abs(q0).max()
+
+
+@pytest.mark.parametrize("scheme", ["RK222", "RK443"])
+@pytest.mark.parametrize("Nx,Ny", [(32, 32), (48, 32)])
+def test_diagonal_rk_matches_oracle(tb, scheme, Nx, Ny):
+    from oracle.tarang_oracle import run_turb_rk
+
+    ts = {"RK222": tb._lib.TB_RK222, "RK443": tb._lib.TB_RK443}[scheme]
+    q0 = turb_initial_spec(Nx, Ny, seed=13)
+    nu, dt, n = 1e-3, 2e-3, 6
+    want = run_turb_rk(q0, Nx, 2 * np.pi, 2 * np.pi, nu, dt, n, scheme)
+    t = tb.Turb2D(Nx, Ny, nu, q0, timestepper=ts)
+    t.step(dt, n)
+    assert rel_l2(t.vorticity(), want) < 1e-4
+
+
+def test_diagonal_rk_stiff_single_mode(tb):
+    # dt nu k^2 = 50: the oracle's L-stable RK443 damps the mode; FP32 follows
+    from oracle.tarang_oracle import run_turb_rk
+
+    Nx = Ny = 16
+    x = np.arange(Nx) * 2 * np.pi / Nx
+    X, Y = np.meshgrid(x, x)
+    q0 = turb_forward(np.cos(2 * X + Y))
+    nu, dt = 10.0, 1.0
+    want = run_turb_rk(q0, Nx, 2 * np.pi, 2 * np.pi, nu, dt, 2, "RK443")
+    t = tb.Turb2D(Nx, Ny, nu, q0, timestepper=tb._lib.TB_RK443)
+    t.step(dt, 2)
+    got = t.vorticity()
+    assert np.abs(got - want).max() < 1e-5 * np.abs(q0).max()
+    assert np.abs(got).max() < 1e-2 * np.abs(q0).max()

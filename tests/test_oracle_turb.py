@@ -2,9 +2,11 @@
 (examples/2d_decaying_turbulence_gpu.jl; nonlinear_padding.jl;
 step_diagonal_imex.jl).  CPU only."""
 import numpy as np
+import pytest
 
 from oracle.tarang_oracle import (
     padded_multiply_2d,
+    rel_l2,
     run_turb,
     turb_backward,
     turb_forward,
@@ -70,3 +72,48 @@ def test_initial_spectrum_is_seeded_and_scaled():
     assert abs(np.abs(turb_backward(a, 32)).max() - 10.0) < 1e-12
     kx, ky = turb_wavenumbers(32, 32, 2 * np.pi, 2 * np.pi)
     assert np.abs(a[np.sqrt(kx ** 2 + ky ** 2) > 32 / 3.0 + 1e-9]).max() < 1e-9
+
+
+@pytest.mark.parametrize("scheme,order", [("RK222", 2), ("RK443", 3)])
+def test_diagonal_rk_order_on_viscous_decay(scheme, order):
+    # a single mode is steady under advection, so q(t) = q0 exp(-nu k^2 t)
+    # exactly: the step error falls as dt^order
+    from oracle.tarang_oracle import run_turb_rk
+
+    Nx = Ny = 16
+    x = np.arange(Nx) * 2 * np.pi / Nx
+    X, Y = np.meshgrid(x, x)
+    q0 = turb_forward(np.cos(2 * X + Y))
+    nu, T = 0.2, 0.5
+    exact = q0 * np.exp(-nu * 5.0 * T)
+    errs = []
+    for n in (8, 16, 32):
+        q = run_turb_rk(q0, Nx, 2 * np.pi, 2 * np.pi, nu, T / n, n, scheme)
+        errs.append(np.abs(q - exact).max())
+    rates = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
+    assert min(rates) > order - 0.3, (errs, rates)
+
+
+def test_diagonal_rk_is_l_stable_in_the_stiff_limit():
+    # dt nu k^2 = 1e4: an L-stable step damps the mode (the ESDIRK tableau with
+    # its off-diagonal terms; without them |R| -> |1 - 1/gamma| > 1)
+    from oracle.tarang_oracle import turb_step_rk, TABLEAUS
+
+    Nx = Ny = 16
+    x = np.arange(Nx) * 2 * np.pi / Nx
+    X, Y = np.meshgrid(x, x)
+    q0 = turb_forward(np.cos(2 * X + Y))
+    for scheme in ("RK222", "RK443"):
+        q = turb_step_rk(q0, Nx, 2 * np.pi, 2 * np.pi, 1e4 / 5.0, 1.0, TABLEAUS[scheme])
+        assert np.abs(q).max() < 1e-2 * np.abs(q0).max(), scheme
+
+
+def test_diagonal_rk_and_sbdf2_agree_as_dt_shrinks():
+    from oracle.tarang_oracle import run_turb_rk
+
+    Nx = Ny = 32
+    q0 = turb_initial_spec(Nx, Ny, seed=3)
+    nu, T = 1e-3, 0.02
+    a = run_turb_rk(q0, Nx, 2 * np.pi, 2 * np.pi, nu, T / 8, 8, "RK443")
+    b = run_turb(q0, Nx, 2 * np.pi, 2 * np.pi, nu, T / 64, 64)
+    assert rel_l2(a, b) < 1e-4
