@@ -302,6 +302,22 @@ tb_status tb_turb_destroy(tb_turb* turb);
 tb_status tb_turb_step(tb_turb* turb, double dt, int nsteps);
 tb_status tb_turb_get_vorticity(tb_turb* turb, double* q_spec_host);
 
+/* Doubly periodic transforms in FP64 for a PeriodicDomain (RealFourier x,
+ * RealFourier y; src/extras/quick_domains.jl:33-58), the grid <-> coefficient
+ * conversion of field["g"] (transform_fourier.jl:473-590): forward
+ * c = fft_y(rfft_x(g)) unnormalised, backward g = irfft_x(ifft_y(c)) with
+ * 1/(Nx Ny), ignoring Im of the kx = 0 and Nyquist bins.  grid (Ny, Nx) real,
+ * x fastest; coeff (Ny, Nx/2+1) complex128, kx fastest, ky in FFT order.
+ * where = TB_HOST or TB_DEVICE.  Nx, Ny even, 2^a 3^b, <= 2048. */
+typedef struct tb_periodic tb_periodic;
+tb_status tb_periodic_create(tb_context* ctx, int Nx, int Ny, tb_periodic** out);
+tb_status tb_periodic_destroy(tb_periodic* p);
+tb_status tb_periodic_forward(tb_periodic* p, const double* grid, double* coeff, int where);
+tb_status tb_periodic_backward(tb_periodic* p, const double* coeff, double* grid, int where);
+/* Replace the vorticity (same layout as tb_turb_create's q0_spec); the next
+ * step starts afresh (SBDF2: with its SBDF1 step). */
+tb_status tb_turb_set_vorticity(tb_turb* turb, const double* q_spec_host);
+
 /* -------------------------------------------------------------------------
  * Request server (continuous batching).  No counterpart in the reference,
  * which runs one solver per process.  A worker thread admits requests in

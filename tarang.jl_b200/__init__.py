@@ -15,6 +15,11 @@ from .api import (  # noqa: F401
     RK443,
     SBDF1,
     SBDF2,
+    DiagonalIMEX_RK222,
+    DiagonalIMEX_RK443,
+    DiagonalIMEX_SBDF2,
+    PeriodicDomain,
+    PeriodicTransform,
     ChannelDomain,
     ChannelDomain3D,
     ChebyshevT,

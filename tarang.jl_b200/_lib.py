@@ -76,6 +76,11 @@ SIGNATURES = {
     "tb_set_state": (c_int, [c_void_p, c_int, c_void_p, c_int]),
     "tb_get_state": (c_int, [c_void_p, c_int, c_void_p, c_int]),
     "tb_set_states": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int]),
+    "tb_periodic_create": (c_int, [c_void_p, c_int, c_int, POINTER(c_void_p)]),
+    "tb_periodic_destroy": (c_int, [c_void_p]),
+    "tb_periodic_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "tb_periodic_backward": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "tb_turb_set_vorticity": (c_int, [c_void_p, c_void_p]),
     "tb_get_states": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int]),
     "tb_step": (c_int, [c_void_p, c_double, c_int]),
     "tb_sim_time": (c_int, [c_void_p, POINTER(c_double), POINTER(c_longlong)]),

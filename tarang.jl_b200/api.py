@@ -73,14 +73,20 @@ class ChebyshevT(RealFourier):
 
 
 class Domain:
-    """RealFourier x (, RealFourier y) x ChebyshevT z."""
+    """RealFourier x (, RealFourier y) x ChebyshevT z, or the doubly periodic
+    RealFourier x RealFourier y of a PeriodicDomain."""
 
     def __init__(self, bases: Sequence, arch=None):
         self.bases = tuple(bases)
         self.arch = arch if arch is not None else GPU()
         if isinstance(self.arch, CPU):
             raise NotImplementedError("the B200 library serves arch=GPU() only")
-        if len(self.bases) == 3:
+        # doubly periodic: two RealFourier bases, no ChebyshevT direction
+        self.periodic = len(self.bases) == 2 and not any(isinstance(b, ChebyshevT) for b in self.bases)
+        if self.periodic:
+            self.xbasis, self.ybasis = self.bases
+            self.zbasis = None
+        elif len(self.bases) == 3:
             self.xbasis, self.ybasis, self.zbasis = self.bases
         else:
             self.xbasis, self.zbasis = self.bases
@@ -89,6 +95,8 @@ class Domain:
 
     @property
     def ndim(self) -> int:
+        if self.periodic:
+            return 2
         return 3 if self.ybasis is not None else 2
 
     @property
@@ -101,22 +109,29 @@ class Domain:
 
     @property
     def Nz(self) -> int:
-        return self.zbasis.size
+        return self.zbasis.size if self.zbasis is not None else 1
 
     @property
     def Nk(self) -> int:
         return self.Nx // 2 + 1
 
     def coeff_shape(self):
-        """Coefficient layout of a field: (Nz, Nx/2+1) or (Nz, Ny, Nx/2+1)."""
+        """Coefficient layout of a field: (Nz, Nx/2+1), (Nz, Ny, Nx/2+1), or
+        (Ny, Nx/2+1) on a periodic domain (rfft along x, fft along y)."""
+        if self.periodic:
+            return (self.Ny, self.Nk)
         return (self.Nz, self.Ny, self.Nk) if self.ndim == 3 else (self.Nz, self.Nk)
 
     def grid_shape(self):
+        if self.periodic:
+            return (self.Ny, self.Nx)
         return (self.Nz, self.Ny, self.Nx) if self.ndim == 3 else (self.Nz, self.Nx)
 
     def grids(self):
         """(x, [y,] z) grids: x_j = j Lx/Nx, z_j = a + (b-a)/2 (1 - cos(pi j/(Nz-1))) (basis_interface.jl:81-121)."""
         x = self.xbasis.bounds[0] + np.arange(self.Nx) * self.xbasis.length / self.Nx
+        if self.periodic:
+            return x, self.ybasis.bounds[0] + np.arange(self.Ny) * self.ybasis.length / self.Ny
         a, b = self.zbasis.bounds
         z = (b - a) / 2 * (-np.cos(np.pi * np.arange(self.Nz) / (self.Nz - 1))) + (b + a) / 2
         if self.ndim == 3:
@@ -127,12 +142,64 @@ class Domain:
     def transform_plan(self) -> "Plan":
         """A plan used only for field transforms (physics parameters unused)."""
         if self._tplan is None:
-            if self.ndim == 3:
+            if self.periodic:
+                self._tplan = PeriodicTransform(self.Nx, self.Ny, device=self.arch.device)
+            elif self.ndim == 3:
                 self._tplan = Plan3D(self.Nx, self.Ny, self.Nz, 1.0, 1.0, L.TB_RK222, self.xbasis.length,
                                      self.ybasis.length, self.zbasis.length, device=self.arch.device)
             else:
                 self._tplan = Plan(self, kappa=1.0, nu=1.0, b_bottom=0.0, b_top=0.0, timestepper=L.TB_RK222)
         return self._tplan
+
+
+class PeriodicTransform:
+    """FP64 grid <-> coefficient transforms of a doubly periodic domain on the
+    device (tb_periodic_*): coefficients (Ny, Nx/2+1) = fft_y(rfft_x(grid)),
+    unnormalised; backward with 1/(Nx Ny)."""
+
+    def __init__(self, Nx: int, Ny: int, device: int = 0):
+        self.Nx, self.Ny = int(Nx), int(Ny)
+        self.ctx = _context(device)
+        self.ptr = c_void_p()
+        check(lib.tb_periodic_create(self.ctx, self.Nx, self.Ny, byref(self.ptr)), self.ctx)
+
+    def __del__(self):
+        ptr = getattr(self, "ptr", None)
+        if ptr:
+            lib.tb_periodic_destroy(ptr)
+            self.ptr = None
+
+    def forward(self, grid: np.ndarray) -> np.ndarray:
+        g = np.ascontiguousarray(grid, dtype=np.float64)
+        if g.shape != (self.Ny, self.Nx):
+            raise ValueError(f"grid shape {g.shape}, expected {(self.Ny, self.Nx)}")
+        out = np.empty((self.Ny, self.Nx // 2 + 1), np.complex128)
+        check(lib.tb_periodic_forward(self.ptr, g.ctypes.data_as(c_void_p), out.ctypes.data_as(c_void_p),
+                                      L.TB_HOST), self.ctx)
+        return out
+
+    def backward(self, coeff: np.ndarray) -> np.ndarray:
+        c = np.ascontiguousarray(coeff, dtype=np.complex128)
+        if c.shape != (self.Ny, self.Nx // 2 + 1):
+            raise ValueError(f"coefficient shape {c.shape}, expected {(self.Ny, self.Nx // 2 + 1)}")
+        out = np.empty((self.Ny, self.Nx), np.float64)
+        check(lib.tb_periodic_backward(self.ptr, c.ctypes.data_as(c_void_p), out.ctypes.data_as(c_void_p),
+                                       L.TB_HOST), self.ctx)
+        return out
+
+
+def PeriodicDomain(*N: int, L: Optional[Sequence[float]] = None, dtype=np.float64, device=None, arch=None,
+                   dealias: float = 1.5) -> Domain:
+    """RealFourier x RealFourier on [0, Lx) x [0, Ly), default 2 pi each
+    (quick_domains.jl:33-58); the 2D form the library steps (decaying
+    turbulence)."""
+    if len(N) != 2:
+        raise NotImplementedError("the B200 library steps 2D periodic domains")
+    Ls = (2 * math.pi, 2 * math.pi) if L is None else tuple(L)
+    arch = device if device is not None else arch
+    xb = RealFourier("x", size=N[0], bounds=(0.0, Ls[0]), dealias=dealias)
+    yb = RealFourier("y", size=N[1], bounds=(0.0, Ls[1]), dealias=dealias)
+    return Domain((xb, yb), arch=arch)
 
 
 def ChannelDomain(Nx: int, Nz: int, Lx: float = 2 * math.pi, Lz: float = 2.0, dtype=np.float64, arch=None,
@@ -523,6 +590,13 @@ class Turb2D:
     def step(self, dt: float, nsteps: int = 1) -> None:
         check(lib.tb_turb_step(self.ptr, float(dt), int(nsteps)), self.ctx)
 
+    def set_vorticity(self, q_spec: np.ndarray) -> None:
+        """Replace q (complex (Ny, Nx/2+1)); the step history restarts."""
+        q = np.ascontiguousarray(q_spec, dtype=np.complex128)
+        if q.shape != (self.Ny, self.Nx // 2 + 1):
+            raise ValueError(f"vorticity shape {q.shape}, expected {(self.Ny, self.Nx // 2 + 1)}")
+        check(lib.tb_turb_set_vorticity(self.ptr, q.ctypes.data_as(c_void_p)), self.ctx)
+
     def vorticity(self) -> np.ndarray:
         out = np.zeros((self.Ny, self.Nx // 2 + 1), dtype=np.complex128)
         check(lib.tb_turb_get_vorticity(self.ptr, out.ctypes.data_as(c_void_p)), self.ctx)
@@ -635,6 +709,8 @@ class ScalarField:
         full = len(self.bases) == len(domain.bases)
         if full:
             shape = domain.coeff_shape()
+        elif not self.bases:  # a constant (gauge multiplier)
+            shape = ()
         else:  # a tau field on the Fourier bases
             shape = (domain.Ny, domain.Nk) if domain.ndim == 3 else (domain.Nk,)
         self._coeff = np.zeros(shape, np.complex128)
@@ -643,19 +719,11 @@ class ScalarField:
 
     def _pull(self) -> None:
         if self._solver is not None:
-            sel, row = self._slot
-            data = self._solver.plan.get_state(sel)
-            self._coeff = data if row is None else data[row].copy()
+            self._coeff = self._solver._read(self._slot)
 
     def _push(self) -> None:
         if self._solver is not None:
-            sel, row = self._slot
-            if row is None:
-                self._solver.plan.set_state(sel, self._coeff)
-            else:
-                taus = self._solver.plan.get_state(sel)
-                taus[row] = self._coeff
-                self._solver.plan.set_state(sel, taus)
+            self._solver._write(self._slot, self._coeff)
 
     def __getitem__(self, layout: str) -> np.ndarray:
         self._pull()
@@ -682,7 +750,7 @@ class VectorField:
     def __init__(self, domain: Domain, name: str, bases: Optional[tuple] = None):
         self.domain = domain
         self.name = name
-        comps = ("x", "y", "z") if domain.ndim == 3 else ("x", "z")
+        comps = ("x", "y") if domain.periodic else (("x", "y", "z") if domain.ndim == 3 else ("x", "z"))
         self.components = [ScalarField(domain, f"{name}_{c}", bases) for c in comps]
 
 
@@ -737,6 +805,22 @@ class SBDF1(_TS):
 
 class SBDF2(_TS):
     name = "SBDF2"
+
+
+class DiagonalIMEX_RK222(_TS):
+    """Diagonal implicit treatment per Fourier mode (pure Fourier problems)."""
+    name = "DiagonalIMEX_RK222"
+
+
+class DiagonalIMEX_RK443(_TS):
+    name = "DiagonalIMEX_RK443"
+
+
+class DiagonalIMEX_SBDF2(_TS):
+    name = "DiagonalIMEX_SBDF2"
+
+
+_DIAG_TS = {"DiagonalIMEX_RK222": L.TB_RK222, "DiagonalIMEX_RK443": L.TB_RK443, "DiagonalIMEX_SBDF2": L.TB_SBDF2}
 
 
 def _norm(s: str) -> str:
@@ -806,10 +890,50 @@ def _match_boussinesq(problem: IVP):
                 names=dict(b=bname, u=uname, p=pname))
 
 
+def _match_vorticity(problem: IVP):
+    """Recognise the 2D vorticity system of examples/2d_decaying_turbulence_gpu.jl:
+    dt(q) - nu*Δ(q) = -u⋅∇(q),  Δ(psi) + tau_psi - q = 0,  u - skew(grad(psi)) = 0,
+    integ(psi) = 0."""
+    P = problem.parameters
+    trans = poisson = vel = None
+    for e in (_norm(e) for e in problem.equations):
+        m = re.fullmatch(r"dt\((\w+)\)-(\w+)\*Δ\(\1\)=-(\w+)⋅∇\(\1\)", e)
+        if m:
+            trans = m
+            continue
+        m = re.fullmatch(r"Δ\((\w+)\)\+(\w+)-(\w+)=0", e)
+        if m:
+            poisson = m
+            continue
+        m = re.fullmatch(r"(\w+)-skew\(grad\((\w+)\)\)=0", e)
+        if m:
+            vel = m
+            continue
+        raise NotImplementedError(f"equation not in the supported vorticity program: {e!r}")
+    if not (trans and poisson and vel):
+        raise NotImplementedError("the B200 path implements the full vorticity system (q, psi, u)")
+    qname, nuname, uname = trans.group(1), trans.group(2), trans.group(3)
+    psiname, tauname = poisson.group(1), poisson.group(2)
+    if poisson.group(3) != qname or vel.group(1) != uname or vel.group(2) != psiname:
+        raise NotImplementedError("inconsistent field names in the vorticity system")
+    bcs = [_norm(b) for b in problem.bcs]
+    if bcs != [f"integ({psiname})=0"]:
+        raise NotImplementedError("expected the single gauge condition integ(psi) = 0")
+    return dict(nu=_value(nuname, P), names=dict(q=qname, psi=psiname, u=uname, tau=tauname))
+
+
 class InitialValueSolver:
     """Builds the library plan for the problem and binds its fields to the plan's state."""
 
     def __init__(self, problem: IVP, timestepper: _TS, dt: Optional[float] = None):
+        for v in problem.variables:
+            dom = v.domain
+            if getattr(dom, "periodic", False):
+                self._init_periodic(problem, timestepper, dt, dom)
+                return
+        self.periodic = False
+        if timestepper.name not in _TS_IDS:
+            raise NotImplementedError(f"{timestepper!r} on a ChebyshevT problem (use RK222/RK443/SBDF1/SBDF2)")
         spec = _match_boussinesq(problem)
         fields = {}
         domain = None
@@ -843,11 +967,75 @@ class InitialValueSolver:
         self.sim_time = 0.0
         self.iteration = 0
 
+    def _init_periodic(self, problem: IVP, timestepper: _TS, dt: Optional[float], domain: Domain) -> None:
+        """The doubly periodic vorticity problem on the FP32 turbulence program;
+        psi and u are derived from q on every read (psi^ = -q^/k^2, 0 at k = 0;
+        u = skew(grad psi) = (-d_y psi, d_x psi))."""
+        if timestepper.name not in _DIAG_TS:
+            raise NotImplementedError(f"{timestepper!r} on a periodic problem (use DiagonalIMEX_SBDF2/RK222/RK443)")
+        spec = _match_vorticity(problem)
+        fields = {v.name: v for v in problem.variables}
+        self.periodic = True
+        self.domain, self.problem, self.timestepper, self.dt = domain, problem, timestepper, dt
+        names = spec["names"]
+        q = fields[names["q"]]
+        self.plan = Turb2D(domain.Nx, domain.Ny, spec["nu"], q._coeff, domain.xbasis.length, domain.ybasis.length,
+                           device=domain.arch.device, timestepper=_DIAG_TS[timestepper.name])
+        kx = 2 * np.pi / domain.xbasis.length * np.arange(domain.Nk)
+        ky = 2 * np.pi / domain.ybasis.length * np.concatenate(
+            [np.arange(domain.Ny // 2), np.arange(-(domain.Ny // 2), 0)])
+        self._kx, self._ky = kx[None, :], ky[:, None]
+        u = fields[names["u"]]
+        binds = [(q, "q"), (fields[names["psi"]], "psi"), (u.components[0], "ux"), (u.components[1], "uy"),
+                 (fields[names["tau"]], "tau")]
+        for f, slot in binds:
+            f._solver, f._slot = self, slot
+        self.sim_time = 0.0
+        self.iteration = 0
+
+    def _psi(self) -> np.ndarray:
+        q = self.plan.vorticity()
+        k2 = self._kx ** 2 + self._ky ** 2
+        return np.where(k2 > 1e-12, -q / np.where(k2 > 1e-12, k2, 1.0), 0.0)
+
+    def _read(self, slot):
+        if not self.periodic:
+            sel, row = slot
+            data = self.plan.get_state(sel)
+            return data if row is None else data[row].copy()
+        if slot == "q":
+            return self.plan.vorticity()
+        if slot == "psi":
+            return self._psi()
+        if slot == "ux":
+            return -1j * self._ky * self._psi()
+        if slot == "uy":
+            return 1j * self._kx * self._psi()
+        return np.zeros((), np.complex128)  # the gauge multiplier vanishes at the solution
+
+    def _write(self, slot, coeff: np.ndarray) -> None:
+        if not self.periodic:
+            sel, row = slot
+            if row is None:
+                self.plan.set_state(sel, coeff)
+            else:
+                taus = self.plan.get_state(sel)
+                taus[row] = coeff
+                self.plan.set_state(sel, taus)
+            return
+        if slot != "q":
+            raise NotImplementedError("psi and u follow from q on a periodic problem; set q")
+        self.plan.set_vorticity(coeff)
+
     def step(self, dt: Optional[float] = None, nsteps: int = 1) -> None:
         dt = self.dt if dt is None else dt
         if dt is None:
             raise ValueError("dt not given")
         self.plan.step(dt, nsteps)
+        if self.periodic:
+            self.sim_time += nsteps * dt
+            self.iteration += nsteps
+            return
         t, it = c_double(), c_longlong()
         check(lib.tb_sim_time(self.plan.ptr, byref(t), byref(it)), self.plan.ctx)
         self.sim_time, self.iteration = t.value, it.value
@@ -859,8 +1047,10 @@ def step(solver: InitialValueSolver, dt: Optional[float] = None) -> None:
 
 
 def run(solver: InitialValueSolver, stop_time: Optional[float] = None, stop_iteration: Optional[int] = None,
-        log_interval: int = 0, dt: Optional[float] = None) -> None:
-    """run!(solver; stop_time, stop_iteration) (solver_stepping.jl:115-205), fixed dt."""
+        log_interval: int = 0, dt: Optional[float] = None, callbacks: Sequence = ()) -> None:
+    """run!(solver; stop_time, stop_iteration, callbacks) (solver_stepping.jl:115-205),
+    fixed dt; callbacks are (interval, fn) pairs, fn(solver) called every
+    interval iterations (the reference's ``interval => fn``)."""
     dt = solver.dt if dt is None else dt
     if dt is None:
         raise ValueError("dt not given")
@@ -872,5 +1062,15 @@ def run(solver: InitialValueSolver, stop_time: Optional[float] = None, stop_iter
         n = nt if n is None else min(n, nt)
     if n is None:
         raise ValueError("give stop_time or stop_iteration")
-    if n > 0:
-        solver.step(dt, n)
+    cbs = [(int(k), fn) for k, fn in callbacks]
+    if any(k < 1 for k, _ in cbs):
+        raise ValueError("callback intervals must be >= 1")
+    end = solver.iteration + max(n, 0)
+    while solver.iteration < end:
+        nxt = end
+        for k, _ in cbs:
+            nxt = min(nxt, (solver.iteration // k + 1) * k)
+        solver.step(dt, nxt - solver.iteration)
+        for k, fn in cbs:
+            if solver.iteration % k == 0:
+                fn(solver)

@@ -588,6 +588,11 @@ void advance_counters(tb_plan* P, double dt, int kind, int steps) {
 
 }  // namespace
 
+namespace tb {
+std::vector<double2> host_twiddles(int n) { return twiddles(n); }
+std::vector<double2> host_pass_twiddles(const FftPlan& fp) { return pass_twiddles(fp); }
+}  // namespace tb
+
 int tb::plan_next_kind(const tb_plan* P) {
   const int ts = P->d.timestepper;
   if (ts == TB_SBDF1) return 1;

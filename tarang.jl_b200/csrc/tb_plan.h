@@ -120,6 +120,14 @@ struct Tableau {
 
 Tableau tableau(int ts);
 
+// Host twiddle tables: exp(-2 pi i k/n), k < n (row FFT kernels), and the
+// per-pass tables of a Stockham plan (CTA FFTs with per-pass twiddles).
+std::vector<double2> host_twiddles(int n);
+std::vector<double2> host_pass_twiddles(const FftPlan& fp);
+// FFT along y of each kx column of a [y][kx] array (length Ny, in place):
+// sign -1 forward (unnormalised), +1 inverse (scaled by 1/Ny).
+void periodic_ycols(double2* a, int Ny, int Kx, const FftPlan& fp, const double2* ptw, int sign, cudaStream_t st);
+
 // Graph of `steps` consecutive steps of one kind at one dt.
 struct StepGraph {
   double dt = -1.0;

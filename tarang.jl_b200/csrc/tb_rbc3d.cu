@@ -807,6 +807,13 @@ void ycols(tb_plan* P, double2* a, int sign) {
 }
 }  // namespace
 
+void periodic_ycols(double2* a, int Ny, int Kx, const FftPlan& fp, const double2* ptw, int sign, cudaStream_t st) {
+  const int npt = F::pass_twiddle_count(fp);
+  const size_t smem = (2 * (size_t)((Ny + 7) & ~7) + npt) * sizeof(double2);
+  TB_CUDA_TRY(cudaFuncSetAttribute(k3_ycols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k3_ycols<<<dim3(Kx, 1), 256, smem, st>>>(a, Ny, Kx, fp, ptw, npt, sign);
+}
+
 void rbc3d_transform_forward(tb_plan* P, const double* grid, double2* coeff) {
   double2* t = P->tmp3.as<double2>();
   launch_x_rfft(grid, t, P->Nz * P->Ny, P->Nx, P->fpN, P->twN.as<double2>(), P->st);

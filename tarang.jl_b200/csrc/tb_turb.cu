@@ -525,20 +525,28 @@ tb_turb* tb::turb_create(tb_context* ctx, const tb_problem_desc& d, const double
   TB_CUDA_TRY(cudaFuncSetAttribute(k_turb_yinv, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
   TB_CUDA_TRY(cudaFuncSetAttribute(k_turb_xpass, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
   TB_CUDA_TRY(cudaFuncSetAttribute(k_turb_yfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-  // initial coefficients: reference layout (Kx, Ny) x fastest -> device [kx][ky]
+  turb_set(T.get(), q0);
+  return T.release();
+}
+
+// Vorticity coefficients from the reference layout (Kx, Ny), x fastest, into
+// Q[0] = q_n (device [kx][ky]); the step history restarts.  Everything runs on
+// the plan's own (non-blocking) stream, so the next step is ordered after it.
+void tb::turb_set(tb_turb* T, const double* q0) {
+  const size_t spec = (size_t)T->Kx * T->Ny * sizeof(float2);
   std::vector<float2> h((size_t)T->Kx * T->Ny);
   for (int ky = 0; ky < T->Ny; ++ky)
     for (int kx = 0; kx < T->Kx; ++kx) {
       const size_t s = (size_t)ky * T->Kx + kx;
       h[(size_t)kx * T->Ny + ky] = make_float2((float)q0[2 * s], (float)q0[2 * s + 1]);
     }
-  // everything on the plan's own (non-blocking) stream, so the first step is
-  // ordered after the initialisation
+  TB_CUDA_TRY(cudaStreamSynchronize(T->st));  // no step still reads the buffers
   TB_CUDA_TRY(cudaMemcpyAsync(T->Q[0].p, h.data(), spec, cudaMemcpyHostToDevice, T->st));
   TB_CUDA_TRY(cudaMemsetAsync(T->Q[1].p, 0, spec, T->st));
   if (T->Fb.p) TB_CUDA_TRY(cudaMemsetAsync(T->Fb.p, 0, spec, T->st));
   TB_CUDA_TRY(cudaStreamSynchronize(T->st));
-  return T.release();
+  T->cur = 0;
+  T->iteration = 0;
 }
 
 void tb::turb_destroy(tb_turb* T) { delete T; }
@@ -619,6 +627,14 @@ tb_status tb_turb_step(tb_turb* T, double dt, int nsteps) {
     TB_CUDA_TRY(cudaSetDevice(T->ctx->device));
     turb_launch_steps(T, dt, nsteps);
     TB_CUDA_TRY(cudaStreamSynchronize(T->st));
+  });
+}
+
+tb_status tb_turb_set_vorticity(tb_turb* T, const double* host) {
+  if (!T || !host) return TB_EINVAL;
+  return guarded(T->ctx, [&] {
+    TB_CUDA_TRY(cudaSetDevice(T->ctx->device));
+    turb_set(T, host);
   });
 }
 

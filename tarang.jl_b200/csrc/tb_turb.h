@@ -14,6 +14,8 @@ namespace tb {
 // (Nx/2+1, Ny) with x fastest (rfft along x, fft along y, unnormalised).
 tb_turb* turb_create(tb_context* ctx, const tb_problem_desc& d, const double* q0_spec);
 void turb_destroy(tb_turb* T);
+// Replace q_n (layout of q0_spec); the step history restarts.
+void turb_set(tb_turb* T, const double* q0_spec);
 cudaStream_t turb_stream(const tb_turb* T);
 // Enqueue steps on the plan's stream (returns without waiting).
 void turb_launch_steps(tb_turb* T, double dt, int steps);
