@@ -810,7 +810,9 @@ void ycols(tb_plan* P, double2* a, int sign) {
 void periodic_ycols(double2* a, int Ny, int Kx, const FftPlan& fp, const double2* ptw, int sign, cudaStream_t st) {
   const int npt = F::pass_twiddle_count(fp);
   const size_t smem = (2 * (size_t)((Ny + 7) & ~7) + npt) * sizeof(double2);
-  TB_CUDA_TRY(cudaFuncSetAttribute(k3_ycols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // the opt-in limit, never the launch's own size: the attribute is per
+  // kernel and process-wide, and the 3D path launches k3_ycols too
+  TB_CUDA_TRY(cudaFuncSetAttribute(k3_ycols, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
   k3_ycols<<<dim3(Kx, 1), 256, smem, st>>>(a, Ny, Kx, fp, ptw, npt, sign);
 }
 
