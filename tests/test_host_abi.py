@@ -94,6 +94,46 @@ def test_equation_recogniser_refuses_other_systems(tb):
         tb.api._match_boussinesq(problem)
 
 
+def _vorticity_problem(tb, nu_eq="∂t(q) - nu*Δ(q) = -u⋅∇(q)", bcs=("integ(psi) = 0",)):
+    dom = tb.PeriodicDomain(16, 16)
+    q, psi = tb.ScalarField(dom, "q"), tb.ScalarField(dom, "psi")
+    u = tb.VectorField(dom, "u")
+    tau = tb.ScalarField(dom, "tau_psi", bases=())
+    problem = tb.IVP([q, psi, u, tau])
+    tb.add_parameters(problem, nu=1e-4)
+    tb.add_equation(problem, nu_eq)
+    tb.add_equation(problem, "Δ(psi) + tau_psi - q = 0")
+    tb.add_equation(problem, "u - skew(grad(psi)) = 0")
+    for bc in bcs:
+        tb.add_bc(problem, bc)
+    return problem, dom, u, tau
+
+
+def test_vorticity_recogniser_reads_the_reference_example_strings(tb):
+    # the equations of examples/2d_decaying_turbulence_gpu.jl, on a domain
+    # whose field shapes follow the periodic coefficient layout
+    problem, dom, u, tau = _vorticity_problem(tb)
+    spec = tb.api._match_vorticity(problem)
+    assert spec["nu"] == 1e-4
+    assert spec["names"] == {"q": "q", "psi": "psi", "u": "u", "tau": "tau_psi"}
+    assert dom.periodic and dom.coeff_shape() == (16, 9) and dom.grid_shape() == (16, 16)
+    assert [c.name for c in u.components] == ["u_x", "u_y"] and tau._coeff.shape == ()
+
+
+def test_vorticity_recogniser_refuses_other_systems(tb):
+    with pytest.raises(NotImplementedError):
+        tb.api._match_vorticity(_vorticity_problem(tb, nu_eq="∂t(q) - nu*Δ(Δ(q)) = -u⋅∇(q)")[0])
+    with pytest.raises(NotImplementedError):
+        tb.api._match_vorticity(_vorticity_problem(tb, bcs=())[0])
+
+
+def test_periodic_solver_needs_a_diagonal_stepper(tb):
+    # a ChebyshevT stepper on a periodic problem is refused before any GPU work
+    problem = _vorticity_problem(tb)[0]
+    with pytest.raises(NotImplementedError):
+        tb.InitialValueSolver(problem, tb.RK222(), dt=1e-3)
+
+
 def test_cpu_architecture_is_refused(tb):
     with pytest.raises(NotImplementedError):
         tb.ChannelDomain(16, 8, arch=tb.CPU())
