@@ -228,13 +228,9 @@ FactorSet* get_factors(tb_plan* P, int sy, double alpha, double beta) {
   TB_CUDA_TRY(cudaMemsetAsync(fs->FR.p, 0, fs->FR.bytes, P->st));
   TB_CUDA_TRY(cudaMemsetAsync(fs->BR.p, 0, fs->BR.bytes, P->st));
   TB_CUDA_TRY(cudaMemsetAsync(fs->SI.p, 0, fs->SI.bytes, P->st));
-  const int nmax = std::max(S.lay.cls[0].n, S.lay.cls[1].n);
-  StreamBuf scratch;  // released in stream order: no device-wide wait
-  scratch.alloc(tau_factor_scratch_doubles(nmax, P->Nkm) * sizeof(double), P->st);
   int neg = 0x7fffffff;
   TB_CUDA_TRY(cudaMemcpyAsync(P->err_mode.p, &neg, sizeof(int), cudaMemcpyHostToDevice, P->st));
   TauArgs a = tau_args(P, sy, fs.get(), nullptr);
-  a.scratch = scratch.as<double>();
   for (int b = 0; b < P->B; ++b) {  // one factor launch per stacked instance (its own kappa, nu)
     TauArgs ab = a;
     ab.mode0 = b * P->Nkm;

@@ -71,7 +71,6 @@ size_t xprod_smem_bytes(int M, int Nk, int nptw);
 // Raise the dynamic shared-memory limit of the transform kernels (once per plan).
 cudaError_t set_transform_smem_limits(int bytes);
 // Scratch (doubles) the factorisation needs for nmax band rows and Nk modes.
-size_t tau_factor_scratch_doubles(int nmax, int Nk);
 
 // Standalone x transforms on rows: forward rfft (grid rows -> half spectra) and
 // backward irfft (half spectra -> grid rows), unnormalised / 1/N like FFTW.
@@ -159,7 +158,6 @@ struct TauArgs {
   // HR[group][row][class][mode][kHRec] = H (12), store code, pad
   double* PP;
   double* HR;
-  double* scratch;     // factor workspace
   double* ysave;       // one-partition solve: [group][row][lane] y scratch (tau_solve_scratch_doubles)
   // modes per instance (batched plans stack instances along the mode axis:
   // mode m belongs to instance m / Nkm, its own mode m % Nkm); the

@@ -48,15 +48,20 @@ __device__ __forceinline__ double* bwd_record(double* BR, int npad, int m, int j
 // eliminated alongside as a dense border and leave an nb x nb Schur
 // complement, inverted explicitly.
 // ---------------------------------------------------------------------------
-// Strided view of a thread's work array in interleaved scratch.
-struct Strided {
-  double* p;
-  size_t s;
-  __device__ __forceinline__ double& operator[](size_t i) const { return p[i * s]; }
-};
+
+constexpr int kFactorThreads = 32;  // systems per CTA of the factorisation
+
+// Shared memory of the factorisation window per CTA: rows (KL+1) x (band
+// slots + border), boundary-row columns NBMAX x (KL+KU+1), the NBMAX^2
+// border block, each for every thread.
+template <int KL, int KU>
+__host__ __device__ constexpr size_t factor_smem_bytes() {
+  return (size_t)((KL + 1) * ((2 * KL + KU + 1) + NBMAX) + NBMAX * (KL + KU + 1) + NBMAX * NBMAX) *
+         kFactorThreads * sizeof(double);
+}
 
 template <int KL, int KU>
-__global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
+__global__ void __launch_bounds__(kFactorThreads) k_tau_factor(TauArgs a) {
   const int ml = blockIdx.x * blockDim.x + threadIdx.x;  // mode within this instance
   const int c = blockIdx.y;
   if (ml >= a.Nkm) return;
@@ -67,35 +72,52 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
   constexpr int W1 = KL + KU + 1;
   const double kx = a.kmag ? a.kmag[m] : a.k0 * ml;
   const bool zmode = (ml == 0);
-  // per-thread work arrays interleaved across the 2 Nkm threads (element i of
-  // a thread at scratch[i * 2Nkm + t]) so that a warp's accesses coalesce
-  const size_t T = (size_t)2 * a.Nkm, t = (size_t)c * a.Nkm + ml;
-  const Strided W{a.scratch + t, T};
-  const Strided Bd{a.scratch + t + (size_t)nmax * WW * T, T};
-  const Strided Cr{a.scratch + t + ((size_t)nmax * WW + (size_t)nmax * NBMAX) * T, T};
-  const Strided C1{a.scratch + t + ((size_t)nmax * WW + 2 * (size_t)nmax * NBMAX) * T, T};
+  // Sliding window of the elimination in shared memory, element-major across
+  // the CTA's threads (element e of thread t at [e][t], conflict-free): at
+  // step j only rows j..j+KL and columns j..j+KL+KU of the boundary rows are
+  // live, so a row enters (its coefficients evaluated from the band tables
+  // and |k|) when step j = row - KL first updates it, and a boundary-row
+  // column when step j = column - KL - KU does.  Ring slots: row i at
+  // i % (KL+1), boundary column c at c % (KL+KU+1).
+  constexpr int RR = KL + 1, CW = KL + KU + 1;
+  extern __shared__ double fsm[];
+  const int BS = blockDim.x, tid = threadIdx.x;
+  auto Wr = [&](int i, int d) -> double& { return fsm[((size_t)(i % RR) * WW + d) * BS + tid]; };
+  auto Bd = [&](int i, int b) -> double& { return fsm[((size_t)RR * WW + (i % RR) * NBMAX + b) * BS + tid]; };
+  auto Cr = [&](int q, int col) -> double& {
+    return fsm[((size_t)RR * (WW + NBMAX) + q * CW + col % CW) * BS + tid];
+  };
+  auto C1 = [&](int q, int b) -> double& {
+    return fsm[((size_t)RR * (WW + NBMAX) + NBMAX * CW + q * NBMAX + b) * BS + tid];
+  };
   const int cw = C.kl + C.ku + 1;
-  for (int r = 0; r < n; ++r) {
-    for (int d = 0; d < WW; ++d) W[(size_t)r * WW + d] = 0.0;
+  auto init_row = [&](int r) {
+    for (int d = 0; d < WW; ++d) Wr(r, d) = 0.0;
     for (int d = 0; d < cw; ++d) {
       int col = r + d - C.kl;
       if (col < 0 || col >= n) continue;
-      W[(size_t)r * WW + (col - r + KL)] = coef_val(C.band[(size_t)r * cw + d], a.alpha, a.beta, kx);
+      Wr(r, col - r + KL) = coef_val(C.band[(size_t)r * cw + d], a.alpha, a.beta, kx);
     }
-    for (int b = 0; b < nb; ++b) Bd[(size_t)r * NBMAX + b] = coef_val(C.bord[(size_t)r * nb + b], a.alpha, a.beta, kx);
-  }
-  for (int q = 0; q < nb; ++q) {
-    for (int col = 0; col < n; ++col)
-      Cr[(size_t)q * nmax + col] = a.beta * (zmode ? C.c2_z : C.c2_nz)[(size_t)q * n + col];
-    for (int b = 0; b < nb; ++b) C1[q * NBMAX + b] = a.beta * (zmode ? C.c1_z : C.c1_nz)[q * nb + b];
-  }
+    for (int b = 0; b < nb; ++b) Bd(r, b) = coef_val(C.bord[(size_t)r * nb + b], a.alpha, a.beta, kx);
+  };
+  auto init_col = [&](int col) {
+    for (int q = 0; q < nb; ++q) Cr(q, col) = a.beta * (zmode ? C.c2_z : C.c2_nz)[(size_t)q * n + col];
+  };
+  for (int r = 0; r <= KL && r < n; ++r) init_row(r);
+  for (int col = 0; col < CW && col < n; ++col) init_col(col);
+  for (int q = 0; q < nb; ++q)
+    for (int b = 0; b < nb; ++b) C1(q, b) = a.beta * (zmode ? C.c1_z : C.c1_nz)[q * nb + b];
   for (int j = 0; j < n; ++j) {
+    // rows / columns entering the window at this step (their slots held row /
+    // column j-1, finished at the previous step)
+    if (j >= 1 && j + KL < n) init_row(j + KL);
+    if (j >= 1 && j + CW - 1 < n) init_col(j + CW - 1);
     const int ilast = min(j + KL, n - 1);
     const int clast = min(j + KL + KU, n - 1);
     int p = j;
-    double best = fabs(W[(size_t)j * WW + KL]);
+    double best = fabs(Wr(j, KL));
     for (int i = j + 1; i <= ilast; ++i) {
-      double v = fabs(W[(size_t)i * WW + (j - i + KL)]);
+      double v = fabs(Wr(i, j - i + KL));
       if (v > best) {
         best = v;
         p = i;
@@ -107,38 +129,37 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
     }
     if (p != j) {
       for (int cc = j; cc <= clast; ++cc) {
-        double t = W[(size_t)j * WW + (cc - j + KL)];
-        W[(size_t)j * WW + (cc - j + KL)] = W[(size_t)p * WW + (cc - p + KL)];
-        W[(size_t)p * WW + (cc - p + KL)] = t;
+        double t = Wr(j, cc - j + KL);
+        Wr(j, cc - j + KL) = Wr(p, cc - p + KL);
+        Wr(p, cc - p + KL) = t;
       }
       for (int b = 0; b < nb; ++b) {
-        double t = Bd[(size_t)j * NBMAX + b];
-        Bd[(size_t)j * NBMAX + b] = Bd[(size_t)p * NBMAX + b];
-        Bd[(size_t)p * NBMAX + b] = t;
+        double t = Bd(j, b);
+        Bd(j, b) = Bd(p, b);
+        Bd(p, b) = t;
       }
     }
     double* fr = fwd_record(C.FR, a.npad, m, j, c);
     double* br = bwd_record(C.BR, a.npad, m, j, c);
     // pivot offset p - j in 0..KL, stored as the integer bits of the slot
     fr[0] = __longlong_as_double((long long)(p - j));
-    const double dinv = 1.0 / W[(size_t)j * WW + KL];
+    const double dinv = 1.0 / Wr(j, KL);
     for (int t = 0; t < KL; ++t) {
       const int i = j + 1 + t;
       double l = 0.0;
       if (i <= ilast) {
-        l = W[(size_t)i * WW + (j - i + KL)] * dinv;
-        W[(size_t)i * WW + (j - i + KL)] = 0.0;
-        for (int cc = j + 1; cc <= clast; ++cc)
-          W[(size_t)i * WW + (cc - i + KL)] -= l * W[(size_t)j * WW + (cc - j + KL)];
-        for (int b = 0; b < nb; ++b) Bd[(size_t)i * NBMAX + b] -= l * Bd[(size_t)j * NBMAX + b];
+        l = Wr(i, j - i + KL) * dinv;
+        Wr(i, j - i + KL) = 0.0;
+        for (int cc = j + 1; cc <= clast; ++cc) Wr(i, cc - i + KL) -= l * Wr(j, cc - j + KL);
+        for (int b = 0; b < nb; ++b) Bd(i, b) -= l * Bd(j, b);
       }
       fr[1 + t] = l;
     }
     for (int q = 0; q < nb; ++q) {
-      const double cq = Cr[(size_t)q * nmax + j] * dinv;
-      Cr[(size_t)q * nmax + j] = 0.0;
-      for (int cc = j + 1; cc <= clast; ++cc) Cr[(size_t)q * nmax + cc] -= cq * W[(size_t)j * WW + (cc - j + KL)];
-      for (int b = 0; b < nb; ++b) C1[q * NBMAX + b] -= cq * Bd[(size_t)j * NBMAX + b];
+      const double cq = Cr(q, j) * dinv;
+      Cr(q, j) = 0.0;
+      for (int cc = j + 1; cc <= clast; ++cc) Cr(q, cc) -= cq * Wr(j, cc - j + KL);
+      for (int b = 0; b < nb; ++b) C1(q, b) -= cq * Bd(j, b);
       fr[1 + KL + q] = cq;
     }
     for (int q = nb; q < NBMAX; ++q) fr[1 + KL + q] = 0.0;
@@ -149,8 +170,8 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
       fr[kFwdRot] = __longlong_as_double((jn < n && C.row_eq[jn] == EQ_MX) ? 1LL : 0LL);
     }
     br[0] = dinv;
-    for (int t = 1; t < W1; ++t) br[t] = (j + t < n) ? W[(size_t)j * WW + KL + t] : 0.0;
-    for (int b = 0; b < NBMAX; ++b) br[W1 + b] = (b < nb) ? Bd[(size_t)j * NBMAX + b] : 0.0;
+    for (int t = 1; t < W1; ++t) br[t] = (j + t < n) ? Wr(j, KL + t) : 0.0;
+    for (int b = 0; b < NBMAX; ++b) br[W1 + b] = (b < nb) ? Bd(j, b) : 0.0;
     // store target of this band column (element offset of its row * 2 + the i flag), bit-cast
     br[kBwdCode] = __longlong_as_double((long long)C.col_code[j]);
   }
@@ -168,7 +189,7 @@ __global__ void __launch_bounds__(64) k_tau_factor(TauArgs a, int nmax) {
   for (int q = 0; q < NBMAX; ++q)
     for (int b = 0; b < 2 * NBMAX; ++b) Aug[q][b] = 0.0;
   for (int q = 0; q < nb; ++q) {
-    for (int b = 0; b < nb; ++b) Aug[q][b] = C1[q * NBMAX + b];
+    for (int b = 0; b < nb; ++b) Aug[q][b] = C1(q, b);
     Aug[q][NBMAX + q] = 1.0;
   }
   double scale = 0.0;
@@ -949,9 +970,8 @@ __global__ void __launch_bounds__(256) k_rk_final(LinComb lc, double2* __restric
 template <int KL, int KU>
 void factor_impl(const TauArgs& a, int parts, cudaStream_t st) {
   (void)parts;
-  int nmax = a.cls[0].n > a.cls[1].n ? a.cls[0].n : a.cls[1].n;
-  dim3 grid((a.Nkm + 63) / 64, 2);
-  k_tau_factor<KL, KU><<<grid, 64, 0, st>>>(a, nmax);
+  dim3 grid((a.Nkm + kFactorThreads - 1) / kFactorThreads, 2);
+  k_tau_factor<KL, KU><<<grid, kFactorThreads, factor_smem_bytes<KL, KU>(), st>>>(a);
 }
 
 template <int KL, int KU>
@@ -980,7 +1000,6 @@ void solve_impl(const TauArgs& a, int parts, cudaStream_t st) {
 
 }  // namespace
 
-size_t tau_factor_scratch_doubles(int nmax, int Nk);
 
 cudaError_t set_tau_smem_limits(int bytes) {
   cudaError_t e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -1028,11 +1047,6 @@ void launch_tau_transfer(const TauArgs& a, int parts, cudaStream_t st) {
 }
 void launch_tau_solve(const TauArgs& a, int parts, cudaStream_t st) { solve_impl<kTauKL, kTauKU>(a, parts, st); }
 
-size_t tau_factor_scratch_doubles(int nmax, int Nk) {
-  const int KL = kTauKL, KU = kTauKU, WW = 2 * KL + KU + 1;
-  const size_t per = (size_t)nmax * WW + (size_t)nmax * NBMAX + (size_t)NBMAX * nmax + NBMAX * NBMAX;
-  return per * 2 * (size_t)Nk;
-}
 
 void launch_lincomb(const LinComb& lc, double2* out, long long count, cudaStream_t st) {
   int blocks = (int)((count + 255) / 256);
