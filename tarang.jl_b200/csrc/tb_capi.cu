@@ -210,21 +210,31 @@ FactorSet* get_factors(tb_plan* P, int sy, double alpha, double beta) {
   TauSystem& S = P->sys[sy];
   for (auto& f : S.factors)
     if (f->alpha == alpha && f->beta == beta) return f.get();
-  // keep at most two sets (SBDF needs the SBDF1 and SBDF2 left-hand sides)
-  if (S.factors.size() >= 2) S.factors.erase(S.factors.begin());
-  auto fs = std::make_unique<FactorSet>();
+  // keep at most two sets (SBDF needs the SBDF1 and SBDF2 left-hand sides);
+  // a new (alpha, beta) takes over the oldest set's device buffers, so a dt
+  // change frees and allocates nothing (cudaFree would wait for the whole
+  // device).  Graphs that read the old set are tied to its dt and are
+  // recaptured before their next launch.
+  std::unique_ptr<FactorSet> fs;
+  if (S.factors.size() >= 2) {
+    fs = std::move(S.factors.front());
+    S.factors.erase(S.factors.begin());
+  } else {
+    fs = std::make_unique<FactorSet>();
+  }
   fs->alpha = alpha;
   fs->beta = beta;
   const int Nk = P->Nk;
   const size_t groups = (size_t)(Nk + kSolveModes - 1) / kSolveModes;
   const size_t n = S.npad;
-  fs->FR.alloc(groups * n * 2 * kFwdRec * kSolveModes * sizeof(double));
-  fs->BR.alloc(groups * n * 2 * kBwdRec * kSolveModes * sizeof(double));
-  fs->SI.alloc(groups * 2 * 16 * kSolveModes * sizeof(double));
-  const size_t npp = tau_transfer_doubles(Nk, S.tau_parts);
-  if (npp) fs->PP.alloc(npp * sizeof(double));
-  const size_t nhr = tau_response_doubles(Nk, (int)n, S.tau_parts);
-  if (nhr) fs->HR.alloc(nhr * sizeof(double));
+  auto fit = [](DevBuf& b, size_t bytes) {
+    if (b.bytes != bytes) b.alloc(bytes);
+  };
+  fit(fs->FR, groups * n * 2 * kFwdRec * kSolveModes * sizeof(double));
+  fit(fs->BR, groups * n * 2 * kBwdRec * kSolveModes * sizeof(double));
+  fit(fs->SI, groups * 2 * 16 * kSolveModes * sizeof(double));
+  fit(fs->PP, tau_transfer_doubles(Nk, S.tau_parts) * sizeof(double));
+  fit(fs->HR, tau_response_doubles(Nk, (int)n, S.tau_parts) * sizeof(double));
   TB_CUDA_TRY(cudaMemsetAsync(fs->FR.p, 0, fs->FR.bytes, P->st));
   TB_CUDA_TRY(cudaMemsetAsync(fs->BR.p, 0, fs->BR.bytes, P->st));
   TB_CUDA_TRY(cudaMemsetAsync(fs->SI.p, 0, fs->SI.bytes, P->st));
