@@ -577,7 +577,8 @@ class Turb2D:
         self.ctx = _context(device)
         d = turb_desc(Nx, Ny, nu, Lx, Ly, timestepper)
         q = np.ascontiguousarray(q0_spec, dtype=np.complex128)
-        assert q.shape == (self.Ny, self.Nx // 2 + 1)
+        if q.shape != (self.Ny, self.Nx // 2 + 1):
+            raise ValueError(f"vorticity shape {q.shape}, expected {(self.Ny, self.Nx // 2 + 1)}")
         self.ptr = c_void_p()
         check(lib.tb_turb_create(self.ctx, byref(d), q.ctypes.data_as(c_void_p), byref(self.ptr)), self.ctx)
 
@@ -656,11 +657,13 @@ class Server:
         if desc.program == L.TB_PROGRAM_TURB2D:
             data = np.ascontiguousarray(init, dtype=np.complex128)
             shape = (desc.Ny, desc.Nx // 2 + 1)
-            assert data.shape == shape
+            if data.shape != shape:
+                raise ValueError(f"initial vorticity shape {data.shape}, expected {shape}")
             nf = 1
         else:
             data = np.ascontiguousarray(init, dtype=np.float64)
-            assert data.shape == (desc.Nz, desc.Nx)
+            if data.shape != (desc.Nz, desc.Nx):
+                raise ValueError(f"initial grid shape {data.shape}, expected {(desc.Nz, desc.Nx)}")
             shape = (desc.Nz, desc.Nx // 2 + 1)
             nf = 3
         r = L.tb_request()
