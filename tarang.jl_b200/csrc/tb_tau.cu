@@ -43,140 +43,192 @@ __device__ __forceinline__ double* bwd_record(double* BR, int npad, int m, int j
 }
 
 // ---------------------------------------------------------------------------
-// Factorisation: one thread per (mode, class).  Banded LU with partial
-// pivoting restricted to the band of the bulk rows; the boundary rows are
-// eliminated alongside as a dense border and leave an nb x nb Schur
-// complement, inverted explicitly.
+// Factorisation: one warp per (mode, class).  Banded LU with partial pivoting
+// restricted to the band of the bulk rows; the boundary rows are eliminated
+// alongside as a dense border and leave an nb x nb Schur complement, inverted
+// explicitly.
+//
+// Only a window of the elimination is live at step j: rows j..j+KL of the
+// band and columns j..j+KL+KU of the boundary rows.  The window sits in the
+// warp's shared memory; a row enters (its coefficients evaluated from the
+// band tables and |k|) when step j = row - KL first updates it, a boundary-
+// row column when step j = column - KL - KU does (ring slots: row i at
+// i % (KL+1), column c at c % (KL+KU+1)).  At each step the lanes take the
+// columns: lane t < KL+KU updates column j+1+t of the KL rows below and of
+// the boundary rows, lanes KL+KU.. the border entries.  Every element gets the
+// same operations in the same order as a sequential elimination, so the
+// factors do not depend on the lane split; the pivot scan (KL+1 candidates)
+// and the Schur inverse run on lane 0.
 // ---------------------------------------------------------------------------
+constexpr int kFactorWarps = 4;  // systems (warps) per CTA of the factorisation
 
-constexpr int kFactorThreads = 32;  // systems per CTA of the factorisation
-
-// Shared memory of the factorisation window per CTA: rows (KL+1) x (band
-// slots + border), boundary-row columns NBMAX x (KL+KU+1), the NBMAX^2
-// border block, each for every thread.
+// Window doubles per system: rows (KL+1) x (band slots + border), boundary-row
+// columns NBMAX x (KL+KU+1), the NBMAX^2 border block.
+template <int KL, int KU>
+__host__ __device__ constexpr int factor_window_doubles() {
+  return (KL + 1) * ((2 * KL + KU + 1) + NBMAX) + NBMAX * (KL + KU + 1) + NBMAX * NBMAX;
+}
 template <int KL, int KU>
 __host__ __device__ constexpr size_t factor_smem_bytes() {
-  return (size_t)((KL + 1) * ((2 * KL + KU + 1) + NBMAX) + NBMAX * (KL + KU + 1) + NBMAX * NBMAX) *
-         kFactorThreads * sizeof(double);
+  return (size_t)factor_window_doubles<KL, KU>() * kFactorWarps * sizeof(double);
 }
 
 template <int KL, int KU>
-__global__ void __launch_bounds__(kFactorThreads) k_tau_factor(TauArgs a) {
-  const int ml = blockIdx.x * blockDim.x + threadIdx.x;  // mode within this instance
+__global__ void __launch_bounds__(32 * kFactorWarps) k_tau_factor(TauArgs a) {
+  static_assert(KL + KU + NBMAX <= 32 && kFwdRec <= 32 && kBwdCode < 32, "one lane per column and record slot");
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int ml = blockIdx.x * kFactorWarps + warp;  // mode within this instance
   const int c = blockIdx.y;
-  if (ml >= a.Nkm) return;
+  if (ml >= a.Nkm) return;  // whole warps leave together
   const int m = a.mode0 + ml;
   const ClassDev& C = a.cls[c];
   const int n = C.n, nb = C.nb;
   constexpr int WW = 2 * KL + KU + 1;
   constexpr int W1 = KL + KU + 1;
+  constexpr int RR = KL + 1, CW = KL + KU + 1;
   const double kx = a.kmag ? a.kmag[m] : a.k0 * ml;
   const bool zmode = (ml == 0);
-  // Sliding window of the elimination in shared memory, element-major across
-  // the CTA's threads (element e of thread t at [e][t], conflict-free): at
-  // step j only rows j..j+KL and columns j..j+KL+KU of the boundary rows are
-  // live, so a row enters (its coefficients evaluated from the band tables
-  // and |k|) when step j = row - KL first updates it, and a boundary-row
-  // column when step j = column - KL - KU does.  Ring slots: row i at
-  // i % (KL+1), boundary column c at c % (KL+KU+1).
-  constexpr int RR = KL + 1, CW = KL + KU + 1;
   extern __shared__ double fsm[];
-  const int BS = blockDim.x, tid = threadIdx.x;
-  auto Wr = [&](int i, int d) -> double& { return fsm[((size_t)(i % RR) * WW + d) * BS + tid]; };
-  auto Bd = [&](int i, int b) -> double& { return fsm[((size_t)RR * WW + (i % RR) * NBMAX + b) * BS + tid]; };
-  auto Cr = [&](int q, int col) -> double& {
-    return fsm[((size_t)RR * (WW + NBMAX) + q * CW + col % CW) * BS + tid];
-  };
-  auto C1 = [&](int q, int b) -> double& {
-    return fsm[((size_t)RR * (WW + NBMAX) + NBMAX * CW + q * NBMAX + b) * BS + tid];
-  };
+  double* win = fsm + (size_t)warp * factor_window_doubles<KL, KU>();
+  auto Wr = [&](int i, int d) -> double& { return win[(i % RR) * WW + d]; };
+  auto Bd = [&](int i, int b) -> double& { return win[RR * WW + (i % RR) * NBMAX + b]; };
+  auto Cr = [&](int q, int col) -> double& { return win[RR * (WW + NBMAX) + q * CW + col % CW]; };
+  auto C1 = [&](int q, int b) -> double& { return win[RR * (WW + NBMAX) + NBMAX * CW + q * NBMAX + b]; };
   const int cw = C.kl + C.ku + 1;
+  // row r enters: lane s < WW fills band slot s, lanes < nb the border
   auto init_row = [&](int r) {
-    for (int d = 0; d < WW; ++d) Wr(r, d) = 0.0;
-    for (int d = 0; d < cw; ++d) {
-      int col = r + d - C.kl;
-      if (col < 0 || col >= n) continue;
-      Wr(r, col - r + KL) = coef_val(C.band[(size_t)r * cw + d], a.alpha, a.beta, kx);
+    if (lane < WW) {
+      double v = 0.0;
+      const int d = lane + C.kl - KL;  // band-table entry of slot lane
+      const int col = r + lane - KL;
+      if (d >= 0 && d < cw && col >= 0 && col < n) v = coef_val(C.band[(size_t)r * cw + d], a.alpha, a.beta, kx);
+      Wr(r, lane) = v;
     }
-    for (int b = 0; b < nb; ++b) Bd(r, b) = coef_val(C.bord[(size_t)r * nb + b], a.alpha, a.beta, kx);
+    if (lane < nb) Bd(r, lane) = coef_val(C.bord[(size_t)r * nb + lane], a.alpha, a.beta, kx);
   };
   auto init_col = [&](int col) {
-    for (int q = 0; q < nb; ++q) Cr(q, col) = a.beta * (zmode ? C.c2_z : C.c2_nz)[(size_t)q * n + col];
+    if (lane < nb) Cr(lane, col) = a.beta * (zmode ? C.c2_z : C.c2_nz)[(size_t)lane * n + col];
   };
   for (int r = 0; r <= KL && r < n; ++r) init_row(r);
   for (int col = 0; col < CW && col < n; ++col) init_col(col);
-  for (int q = 0; q < nb; ++q)
-    for (int b = 0; b < nb; ++b) C1(q, b) = a.beta * (zmode ? C.c1_z : C.c1_nz)[q * nb + b];
+  if (lane < nb * nb) {
+    const int q = lane / nb, b = lane % nb;
+    C1(q, b) = a.beta * (zmode ? C.c1_z : C.c1_nz)[q * nb + b];
+  }
+  __syncwarp();
   for (int j = 0; j < n; ++j) {
     // rows / columns entering the window at this step (their slots held row /
     // column j-1, finished at the previous step)
     if (j >= 1 && j + KL < n) init_row(j + KL);
     if (j >= 1 && j + CW - 1 < n) init_col(j + CW - 1);
+    __syncwarp();
     const int ilast = min(j + KL, n - 1);
     const int clast = min(j + KL + KU, n - 1);
+    // pivot: the first largest |entry| of column j among rows j..ilast
     int p = j;
-    double best = fabs(Wr(j, KL));
-    for (int i = j + 1; i <= ilast; ++i) {
-      double v = fabs(Wr(i, j - i + KL));
-      if (v > best) {
-        best = v;
-        p = i;
+    bool bad = false;
+    if (lane == 0) {
+      double best = fabs(Wr(j, KL));
+      for (int i = j + 1; i <= ilast; ++i) {
+        double v = fabs(Wr(i, j - i + KL));
+        if (v > best) {
+          best = v;
+          p = i;
+        }
       }
+      bad = !(best > 0.0) || !isfinite(best);
     }
-    if (!(best > 0.0) || !isfinite(best)) {
-      atomicMin(a.err_mode, m);
+    p = __shfl_sync(0xffffffffu, p, 0);
+    if (__shfl_sync(0xffffffffu, (int)bad, 0)) {
+      if (lane == 0) atomicMin(a.err_mode, m);
       return;
     }
     if (p != j) {
-      for (int cc = j; cc <= clast; ++cc) {
+      const int cc = j + lane;
+      if (cc <= clast) {
         double t = Wr(j, cc - j + KL);
         Wr(j, cc - j + KL) = Wr(p, cc - p + KL);
         Wr(p, cc - p + KL) = t;
       }
-      for (int b = 0; b < nb; ++b) {
-        double t = Bd(j, b);
-        Bd(j, b) = Bd(p, b);
-        Bd(p, b) = t;
+      if (lane < nb) {
+        double t = Bd(j, lane);
+        Bd(j, lane) = Bd(p, lane);
+        Bd(p, lane) = t;
       }
+      __syncwarp();
     }
-    double* fr = fwd_record(C.FR, a.npad, m, j, c);
-    double* br = bwd_record(C.BR, a.npad, m, j, c);
-    // pivot offset p - j in 0..KL, stored as the integer bits of the slot
-    fr[0] = __longlong_as_double((long long)(p - j));
     const double dinv = 1.0 / Wr(j, KL);
+    // multipliers of the rows below and of the boundary rows, read by every
+    // lane before lane 0 clears their column-j entries
+    double l[KL], cqv[NBMAX];
+#pragma unroll
     for (int t = 0; t < KL; ++t) {
       const int i = j + 1 + t;
-      double l = 0.0;
-      if (i <= ilast) {
-        l = Wr(i, j - i + KL) * dinv;
-        Wr(i, j - i + KL) = 0.0;
-        for (int cc = j + 1; cc <= clast; ++cc) Wr(i, cc - i + KL) -= l * Wr(j, cc - j + KL);
-        for (int b = 0; b < nb; ++b) Bd(i, b) -= l * Bd(j, b);
+      l[t] = (i <= ilast) ? Wr(i, j - i + KL) * dinv : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < NBMAX; ++q) cqv[q] = (q < nb) ? Cr(q, j) * dinv : 0.0;
+    __syncwarp();
+    if (lane == 0) {
+      for (int t = 0; t < KL; ++t)
+        if (j + 1 + t <= ilast) Wr(j + 1 + t, j - (j + 1 + t) + KL) = 0.0;
+      for (int q = 0; q < nb; ++q) Cr(q, j) = 0.0;
+    }
+    if (lane < KL + KU) {
+      const int cc = j + 1 + lane;
+      if (cc <= clast) {
+        const double wj = Wr(j, cc - j + KL);
+#pragma unroll
+        for (int t = 0; t < KL; ++t) {
+          const int i = j + 1 + t;
+          if (i <= ilast) Wr(i, cc - i + KL) -= l[t] * wj;
+        }
+#pragma unroll
+        for (int q = 0; q < NBMAX; ++q)
+          if (q < nb) Cr(q, cc) -= cqv[q] * wj;
       }
-      fr[1 + t] = l;
+    } else if (lane - (KL + KU) < nb) {
+      const int b = lane - (KL + KU);
+      const double bj = Bd(j, b);
+#pragma unroll
+      for (int t = 0; t < KL; ++t) {
+        const int i = j + 1 + t;
+        if (i <= ilast) Bd(i, b) -= l[t] * bj;
+      }
+#pragma unroll
+      for (int q = 0; q < NBMAX; ++q)
+        if (q < nb) C1(q, b) -= cqv[q] * bj;
     }
-    for (int q = 0; q < nb; ++q) {
-      const double cq = Cr(q, j) * dinv;
-      Cr(q, j) = 0.0;
-      for (int cc = j + 1; cc <= clast; ++cc) Cr(q, cc) -= cq * Wr(j, cc - j + KL);
-      for (int b = 0; b < nb; ++b) C1(q, b) -= cq * Bd(j, b);
-      fr[1 + KL + q] = cq;
-    }
-    for (int q = nb; q < NBMAX; ++q) fr[1 + KL + q] = 0.0;
-    // last slot: 1 when the right-hand side of row j + kFwdWin (the row entering
-    // the forward window at this row) is a u_x momentum row, scaled by -i on load
-    {
+    // records of row j (row j itself is final after the swap)
+    double* fr = fwd_record(C.FR, a.npad, m, j, c);
+    double* br = bwd_record(C.BR, a.npad, m, j, c);
+    if (lane == 0) {
+      fr[0] = __longlong_as_double((long long)(p - j));  // pivot offset, integer bits
+    } else if (lane <= KL) {
+      fr[lane] = l[lane - 1];
+    } else if (lane <= KL + NBMAX) {
+      fr[lane] = cqv[lane - 1 - KL];  // 0 past nb
+    } else if (lane == kFwdRot) {
+      // 1 when the right-hand side of row j + kFwdWin (the row entering the
+      // forward window at this row) is a u_x momentum row, scaled by -i on load
       const int jn = j + kFwdWin;
       fr[kFwdRot] = __longlong_as_double((jn < n && C.row_eq[jn] == EQ_MX) ? 1LL : 0LL);
     }
-    br[0] = dinv;
-    for (int t = 1; t < W1; ++t) br[t] = (j + t < n) ? Wr(j, KL + t) : 0.0;
-    for (int b = 0; b < NBMAX; ++b) br[W1 + b] = (b < nb) ? Bd(j, b) : 0.0;
-    // store target of this band column (element offset of its row * 2 + the i flag), bit-cast
-    br[kBwdCode] = __longlong_as_double((long long)C.col_code[j]);
+    if (lane == 0) {
+      br[0] = dinv;
+    } else if (lane < W1) {
+      br[lane] = (j + lane < n) ? Wr(j, KL + lane) : 0.0;
+    } else if (lane < W1 + NBMAX) {
+      const int b = lane - W1;
+      br[lane] = (b < nb) ? Bd(j, b) : 0.0;
+    } else if (lane == kBwdCode) {
+      // store target of this band column (element offset of its row * 2 + the i flag), bit-cast
+      br[kBwdCode] = __longlong_as_double((long long)C.col_code[j]);
+    }
+    __syncwarp();  // row j's slot is refilled at the next step
   }
   // padding rows n..npad-1: identity rows with no right-hand side and no store
-  for (int j = n; j < a.npad; ++j) {
+  for (int j = n + lane; j < a.npad; j += 32) {
     double* fr = fwd_record(C.FR, a.npad, m, j, c);
     double* br = bwd_record(C.BR, a.npad, m, j, c);
     for (int t = 0; t < kFwdRec; ++t) fr[t] = 0.0;
@@ -184,6 +236,7 @@ __global__ void __launch_bounds__(kFactorThreads) k_tau_factor(TauArgs a) {
     for (int t = 1; t < kBwdCode; ++t) br[t] = 0.0;
     br[kBwdCode] = __longlong_as_double(-1LL);
   }
+  if (lane != 0) return;
   // invert the nb x nb Schur complement (Gauss-Jordan, partial pivoting)
   double Aug[NBMAX][2 * NBMAX];
   for (int q = 0; q < NBMAX; ++q)
@@ -970,8 +1023,8 @@ __global__ void __launch_bounds__(256) k_rk_final(LinComb lc, double2* __restric
 template <int KL, int KU>
 void factor_impl(const TauArgs& a, int parts, cudaStream_t st) {
   (void)parts;
-  dim3 grid((a.Nkm + kFactorThreads - 1) / kFactorThreads, 2);
-  k_tau_factor<KL, KU><<<grid, kFactorThreads, factor_smem_bytes<KL, KU>(), st>>>(a);
+  dim3 grid((a.Nkm + kFactorWarps - 1) / kFactorWarps, 2);
+  k_tau_factor<KL, KU><<<grid, 32 * kFactorWarps, factor_smem_bytes<KL, KU>(), st>>>(a);
 }
 
 template <int KL, int KU>
