@@ -72,3 +72,32 @@ def test_diagonal_rk_stiff_single_mode(tb):
     got = t.vorticity()
     assert np.abs(got - want).max() < 1e-5 * np.abs(q0).max()
     assert np.abs(got).max() < 1e-2 * np.abs(q0).max()
+
+
+@pytest.mark.parametrize("scheme", ["RK222", "RK443", "SBDF2"])
+def test_reference_pin_viscous_rate(tb, scheme):
+    # the reference's known answer (test/test_diagonal_imex.jl:208-275): cos(2x),
+    # nu = 0.5, dt = 0.005, 200 steps decays to exp(-2) (its bar: rtol 0.05)
+    ts = {"RK222": tb._lib.TB_RK222, "RK443": tb._lib.TB_RK443, "SBDF2": tb._lib.TB_SBDF2}[scheme]
+    N = 16
+    x = np.arange(N) * 2 * np.pi / N
+    X, _ = np.meshgrid(x, x)
+    q0 = turb_forward(np.cos(2 * X))
+    t = tb.Turb2D(N, N, 0.5, q0, timestepper=ts)
+    t.step(0.005, 200)
+    ratio = np.abs(t.vorticity()).max() / np.abs(q0).max()
+    assert abs(ratio - np.exp(-2.0)) < 1e-3 * np.exp(-2.0)
+
+
+@pytest.mark.parametrize("scheme", ["RK222", "RK443"])
+def test_reference_pin_stiff_mode_is_damped(tb, scheme):
+    # test/test_diagonal_imex.jl:278-308: cos(6x), nu = 1, dt = 0.25, 20 steps
+    ts = {"RK222": tb._lib.TB_RK222, "RK443": tb._lib.TB_RK443}[scheme]
+    N = 16
+    x = np.arange(N) * 2 * np.pi / N
+    X, _ = np.meshgrid(x, x)
+    q0 = turb_forward(np.cos(6 * X))
+    t = tb.Turb2D(N, N, 1.0, q0, timestepper=ts)
+    t.step(0.25, 20)
+    g = np.abs(t.vorticity()).max() / np.abs(q0).max()
+    assert np.isfinite(g) and g < 1e-2

@@ -117,3 +117,43 @@ def test_diagonal_rk_and_sbdf2_agree_as_dt_shrinks():
     a = run_turb_rk(q0, Nx, 2 * np.pi, 2 * np.pi, nu, T / 8, 8, "RK443")
     b = run_turb(q0, Nx, 2 * np.pi, 2 * np.pi, nu, T / 64, 64)
     assert rel_l2(a, b) < 1e-4
+
+
+# The reference's own known answers for the diagonal IMEX steppers
+# (test/test_diagonal_imex.jl:208-308).  A single Fourier mode is steady under
+# the advection, so the vorticity problem reduces to their viscous decay.
+def _mode(N, k):
+    x = np.arange(N) * 2 * np.pi / N
+    X, _ = np.meshgrid(x, x)
+    return turb_forward(np.cos(k * X))
+
+
+@pytest.mark.parametrize("scheme", ["RK222", "RK443", "SBDF2"])
+def test_reference_pin_viscous_rate(scheme):
+    # cos(2x), nu = 0.5, dt = 0.005, 200 steps: amplitude exp(-nu k^2 T) =
+    # exp(-2) within the reference's rtol 0.05 (and far closer here)
+    from oracle.tarang_oracle import run_turb_rk
+
+    N = 16
+    q0 = _mode(N, 2)
+    if scheme == "SBDF2":
+        q = run_turb(q0, N, 2 * np.pi, 2 * np.pi, 0.5, 0.005, 200)
+    else:
+        q = run_turb_rk(q0, N, 2 * np.pi, 2 * np.pi, 0.5, 0.005, 200, scheme)
+    ratio = np.abs(turb_backward(q, N)).max() / np.abs(turb_backward(q0, N)).max()
+    assert abs(ratio - np.exp(-2.0)) < 0.05 * np.exp(-2.0)
+    assert abs(ratio - np.exp(-2.0)) < 1e-3 * np.exp(-2.0)
+
+
+@pytest.mark.parametrize("scheme", ["RK222", "RK443"])
+def test_reference_pin_stiff_mode_is_damped(scheme):
+    # cos(6x), nu = 1, dt = 0.25 (dt nu k^2 = 9), 20 steps: finite, below the
+    # start and below 1e-2 (the full ESDIRK tableau; a diagonal-only update
+    # would grow ~2000x)
+    from oracle.tarang_oracle import run_turb_rk
+
+    N = 16
+    q0 = _mode(N, 6)
+    q = run_turb_rk(q0, N, 2 * np.pi, 2 * np.pi, 1.0, 0.25, 20, scheme)
+    g, g0 = np.abs(turb_backward(q, N)).max(), np.abs(turb_backward(q0, N)).max()
+    assert np.isfinite(g) and g < g0 and g < 1e-2
