@@ -201,3 +201,20 @@ def test_timestepper_order_on_exact_diffusion(scheme, order):
     e2 = _diffusion_error(scheme, 0.05)
     rate = np.log2(e1 / e2)
     assert rate > order - 0.3, (scheme, e1, e2, rate)
+
+
+def test_reference_pin_variable_step_sbdf_coefficients():
+    # test/test_timestepper_boundaries.jl "Variable timestep coefficient
+    # builders": dt = 0.02 after dt_prev = 0.01 (w1 = 2)
+    from oracle.tarang_oracle import sbdf_coefs
+
+    dt, dt_prev = 0.02, 0.01
+    w1 = dt / dt_prev
+    a, b, c = sbdf_coefs(2, dt, dt_prev)
+    assert abs(a[0] - (1.0 + 2.0 * w1) / ((1.0 + w1) * dt)) < 1e-14
+    assert abs(a[1] - (-(1.0 + w1) / dt)) < 1e-14
+    assert abs(a[2] - w1 ** 2 / ((1.0 + w1) * dt)) < 1e-14
+    assert tuple(b) == (1.0,) and tuple(c) == (0.0, 1.0 + w1, -w1)
+    # the SBDF1 startup: (1/dt, -1/dt), (1,), (0, 1)
+    a1, b1, c1 = sbdf_coefs(1, dt)
+    assert tuple(a1) == (1.0 / dt, -1.0 / dt) and tuple(b1) == (1.0,) and tuple(c1) == (0.0, 1.0)
