@@ -10,6 +10,8 @@ Each case restates an analytic check from the reference test suite or docs:
   - RBC builds and steps finitely                        test/test_subproblem_rk.jl:19-110
   - min-norm mass solve = least squares                  test/test_batched_mass_solve.jl:169-220
   - time-stepper order on an exact linear solution      test/test_timestepper_boundaries.jl:78-176
+  - variable-step SBDF2 / SBDF1 coefficient values       test/test_timestepper_boundaries.jl:78-176
+  - DCT-I convention and the RF x Cheb forward chain     test/test_gpu_dct1_kernels_cpu.jl:35-214
 """
 import numpy as np
 import numpy.polynomial.chebyshev as npc
@@ -218,3 +220,55 @@ def test_reference_pin_variable_step_sbdf_coefficients():
     # the SBDF1 startup: (1/dt, -1/dt), (1,), (0, 1)
     a1, b1, c1 = sbdf_coefs(1, dt)
     assert tuple(a1) == (1.0 / dt, -1.0 / dt) and tuple(b1) == (1.0,) and tuple(c1) == (0.0, 1.0)
+
+
+def _redft00(x):
+    # FFTW's REDFT00 written out: Y_k = x_0 + (-1)^k x_{n-1}
+    #                                   + 2 sum_{j=1}^{n-2} x_j cos(pi j k/(n-1))
+    n = x.shape[0]
+    j = np.arange(n)
+    C = 2.0 * np.cos(np.pi * np.outer(j, j) / (n - 1))
+    C[:, 0] = 1.0
+    C[:, -1] = (-1.0) ** j
+    return C @ x
+
+
+@pytest.mark.parametrize("n", [9, 16])
+def test_reference_pin_dct1_convention(n):
+    # test/test_gpu_dct1_kernels_cpu.jl:35-50,88-106: forward = REDFT00/(n-1),
+    # endpoints halved, odd coefficients negated; backward undoes it
+    from oracle.tarang_oracle import cheb_backward, cheb_forward
+
+    rng = np.random.default_rng(n)
+    mat = rng.standard_normal((n, 5))
+    sign = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)[:, None]
+    want = _redft00(mat) / (n - 1)
+    want[0] /= 2
+    want[-1] /= 2
+    want *= sign
+    fwd = cheb_forward(mat)
+    assert np.abs(fwd - want).max() < 1e-13
+    y = fwd * sign
+    y[0] *= 2
+    y[-1] *= 2
+    assert np.abs(cheb_backward(fwd) - _redft00(y) / 2).max() < 1e-12
+    assert np.abs(cheb_backward(fwd) - mat).max() < 1e-12
+
+
+def test_reference_pin_fourier_chebyshev_forward_chain():
+    # test/test_gpu_dct1_kernels_cpu.jl:187-214: the 2D RealFourier x
+    # ChebyshevT forward is the unnormalised rfft along x, then the DCT-I
+    # convention along z (16 x 9 grid); both stages written out as matrices
+    from oracle.tarang_oracle import forward_2d
+
+    Nx, Nz = 16, 9
+    g = np.random.default_rng(9).standard_normal((Nz, Nx))
+    k = np.arange(Nx // 2 + 1)
+    F = np.exp(-2j * np.pi * np.outer(np.arange(Nx), k) / Nx)
+    spec = g @ F
+    sign = np.where(np.arange(Nz) % 2 == 0, 1.0, -1.0)[:, None]
+    want = _redft00(spec) / (Nz - 1)
+    want[0] /= 2
+    want[-1] /= 2
+    want *= sign
+    assert np.abs(forward_2d(g) - want).max() < 1e-12
