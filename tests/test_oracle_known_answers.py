@@ -12,6 +12,8 @@ Each case restates an analytic check from the reference test suite or docs:
   - time-stepper order on an exact linear solution      test/test_timestepper_boundaries.jl:78-176
   - variable-step SBDF2 / SBDF1 coefficient values       test/test_timestepper_boundaries.jl:78-176
   - DCT-I convention and the RF x Cheb forward chain     test/test_gpu_dct1_kernels_cpu.jl:35-214
+and writes the periodic and 3D transform conventions out as DFT sums
+(src/core/transforms/transform_fourier.jl:473-590).
 """
 import numpy as np
 import numpy.polynomial.chebyshev as npc
@@ -272,3 +274,41 @@ def test_reference_pin_fourier_chebyshev_forward_chain():
     want[-1] /= 2
     want *= sign
     assert np.abs(forward_2d(g) - want).max() < 1e-12
+
+
+def _c2r(h, Nx):
+    # FFTW's c2r along the last axis, written out: the imaginary parts of the
+    # kx = 0 and Nyquist bins do not enter (transform_fourier.jl:553-575)
+    x = np.arange(Nx)
+    k = np.arange(1, Nx // 2)
+    E = np.exp(2j * np.pi * np.outer(k, x) / Nx)
+    g = h[..., :1].real + h[..., Nx // 2:Nx // 2 + 1].real * (-1.0) ** x
+    return (g + 2.0 * np.real(h[..., 1:Nx // 2] @ E)) / Nx
+
+
+def test_periodic_and_3d_transforms_written_out():
+    # the doubly periodic (rfft x, fft y) and the 3D channel (rfft x, fft y,
+    # DCT-I z) conventions as explicit DFT sums (transform_fourier.jl:473-590)
+    from oracle.tarang_oracle import backward_3d, cheb_backward, forward_3d, turb_backward, turb_forward
+
+    rng = np.random.default_rng(11)
+    Nx, Ny, Nz = 12, 8, 9
+    Fx = np.exp(-2j * np.pi * np.outer(np.arange(Nx), np.arange(Nx // 2 + 1)) / Nx)
+    Fy = np.exp(-2j * np.pi * np.outer(np.arange(Ny), np.arange(Ny)) / Ny)
+    g2 = rng.standard_normal((Ny, Nx))
+    assert np.abs(turb_forward(g2) - Fy.T @ (g2 @ Fx)).max() < 1e-12
+    c2 = rng.standard_normal((Ny, Nx // 2 + 1)) + 1j * rng.standard_normal((Ny, Nx // 2 + 1))
+    assert np.abs(turb_backward(c2, Nx) - _c2r(np.conj(Fy) @ c2 / Ny, Nx)).max() < 1e-12
+
+    g3 = rng.standard_normal((Nz, Ny, Nx))
+    spec = np.einsum("yq,zqk->zyk", Fy.T, g3 @ Fx)
+    sign = np.where(np.arange(Nz) % 2 == 0, 1.0, -1.0)[:, None, None]
+    want = np.tensordot(_redft00(np.eye(Nz)), spec, axes=(1, 0)) / (Nz - 1)
+    want[0] /= 2
+    want[-1] /= 2
+    want *= sign
+    assert np.abs(forward_3d(g3) - want).max() < 1e-11
+    assert np.abs(backward_3d(forward_3d(g3), Nx) - g3).max() < 1e-12
+    c3 = rng.standard_normal(want.shape) + 1j * rng.standard_normal(want.shape)
+    h = np.einsum("yq,zqk->zyk", np.conj(Fy) / Ny, cheb_backward(c3, axis=0))
+    assert np.abs(backward_3d(c3, Nx) - _c2r(h, Nx)).max() < 1e-12
