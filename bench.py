@@ -44,7 +44,8 @@ def parse_args():
     ap.add_argument("--scheme", choices=["RK443", "RK222", "SBDF2"], default="RK443")
     ap.add_argument("--config", choices=["c2", "c1"], default="c2")
     ap.add_argument("--e2e-steps", type=int, default=20)
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=10,
+                    help="timed steps of the CPU baseline leg (about 1 s each on 16 host threads)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["rbc", "ensemble", "serving", "turb", "rbc3d"], default="rbc",
                     help="rbc: the single-instance step (headline); ensemble / serving: that workload alone")
