@@ -41,7 +41,7 @@ def test_reference_arm_prints_once_under_two_ranks():
     # group, so it never waits in a barrier for rank 0's minutes of host work)
     code = (
         "import sys, time\n"
-        "sys.argv = ['bench.py', '--impl', 'reference', '--config', 'c1', '--steps', '1', '--warmup', '0']\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--config', 'c1', '--steps', '1', '--warmup', '3']\n"
         "import bench\n"
         "t0 = time.perf_counter()\n"
         "bench.main()\n"
@@ -56,6 +56,7 @@ def test_reference_arm_prints_once_under_two_ranks():
     assert el[1] < 0.5 * el[0], el
     d = json.loads(lines0[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["warmup"] == 3 and d["steps"] == 1 and d["cpu_baseline"]["kind"] == "port"
 
 
 def test_instance_sharding_is_complete_disjoint_and_agreed_by_two_ranks():
