@@ -12,6 +12,7 @@ Each case restates an analytic check from the reference test suite or docs:
   - time-stepper order on an exact linear solution      test/test_timestepper_boundaries.jl:78-176
   - variable-step SBDF2 / SBDF1 coefficient values       test/test_timestepper_boundaries.jl:78-176
   - DCT-I convention and the RF x Cheb forward chain     test/test_gpu_dct1_kernels_cpu.jl:35-214
+  - T-basis derivative recurrence (orders 1 and 2)       test/test_gpu_dct1_kernels_cpu.jl:164-180
 and writes the periodic and 3D transform conventions out as DFT sums
 (src/core/transforms/transform_fourier.jl:473-590).
 """
@@ -312,3 +313,21 @@ def test_periodic_and_3d_transforms_written_out():
     c3 = rng.standard_normal(want.shape) + 1j * rng.standard_normal(want.shape)
     h = np.einsum("yq,zqk->zyk", np.conj(Fy) / Ny, cheb_backward(c3, axis=0))
     assert np.abs(backward_3d(c3, Nx) - _c2r(h, Nx)).max() < 1e-12
+
+
+@pytest.mark.parametrize("n", [9, 17])
+def test_reference_pin_chebyshev_derivative_recurrence(n):
+    # test/test_gpu_dct1_kernels_cpu.jl:164-180: the T-basis derivative with
+    # scale 2/3.7, and order 2 as the first-derivative pass applied twice.
+    # Backward recurrence d_{k-1} = d_{k+1} + 2 k c_k, d_0 halved.
+    scale = 2.0 / 3.7
+    c = np.random.default_rng(n).standard_normal((n, 4))
+    d = np.zeros_like(c)
+    for k in range(n - 1, 0, -1):
+        d[k - 1] = (d[k + 1] if k + 1 < n else 0.0) + 2.0 * k * c[k]
+    d[0] /= 2.0
+    d *= scale
+    D = cheb_diff_matrix(n, 3.7)
+    assert np.abs(D @ c - d).max() < 1e-11
+    assert np.abs(D @ (D @ c) - D @ d).max() < 1e-9
+    assert np.abs(npc.chebder(c, scl=scale) - (D @ c)[:-1]).max() < 1e-11
