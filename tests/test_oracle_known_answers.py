@@ -13,6 +13,7 @@ Each case restates an analytic check from the reference test suite or docs:
   - variable-step SBDF2 / SBDF1 coefficient values       test/test_timestepper_boundaries.jl:78-176
   - DCT-I convention and the RF x Cheb forward chain     test/test_gpu_dct1_kernels_cpu.jl:35-214
   - T-basis derivative recurrence (orders 1 and 2)       test/test_gpu_dct1_kernels_cpu.jl:164-180
+  - rfft / fft wavenumber orders and length scaling      test/test_basis_wavenumbers.jl:36-69
 and writes the periodic and 3D transform conventions out as DFT sums
 (src/core/transforms/transform_fourier.jl:473-590).
 """
@@ -331,3 +332,17 @@ def test_reference_pin_chebyshev_derivative_recurrence(n):
     assert np.abs(D @ c - d).max() < 1e-11
     assert np.abs(D @ (D @ c) - D @ d).max() < 1e-9
     assert np.abs(npc.chebder(c, scl=scale) - (D @ c)[:-1]).max() < 1e-11
+
+
+def test_reference_pin_wavenumbers():
+    # test/test_basis_wavenumbers.jl:36-69: rfft layout 0..N/2 (N = 7 gives
+    # 0..3), the length scaling 2 pi / L, and the full fft order of the y axis
+    # with -N/2 at the Nyquist index
+    from oracle.tarang_oracle import turb_wavenumbers, wavenumbers_rfft
+
+    assert np.allclose(wavenumbers_rfft(8, 2 * np.pi), [0, 1, 2, 3, 4])
+    assert np.allclose(wavenumbers_rfft(7, 2 * np.pi), [0, 1, 2, 3])
+    assert np.allclose(wavenumbers_rfft(8, 4 * np.pi), 0.5 * np.arange(5))
+    kx, ky = turb_wavenumbers(16, 8, 2 * np.pi, 2 * np.pi)
+    assert np.allclose(ky.ravel(), [0, 1, 2, 3, -4, -3, -2, -1])
+    assert np.allclose(kx.ravel(), np.arange(9)) and kx.ravel()[-1] == 8.0
