@@ -27,6 +27,9 @@ from oracle.tarang_oracle import (  # noqa: E402
     padded_multiply,
     rbc_initial_b,
     run_rbc,
+    run_turb,
+    run_turb_rk,
+    turb_initial_spec,
 )
 
 CASES = [
@@ -36,6 +39,21 @@ CASES = [
     ("rbc_sbdf2_32x16", 32, 16, 1e8, "SBDF2", 0.01, 6),
     ("rbc_rk222_64x17", 64, 17, 1e6, "RK222", 0.05, 5),
 ]
+
+TURB_CASES = [
+    # name, N, scheme, nu, dt, nsteps, seed (doubly periodic vorticity, 2 pi box)
+    ("turb_sbdf2_32", 32, "SBDF2", 1e-3, 2e-3, 6, 21),
+    ("turb_rk443_32", 32, "RK443", 1e-3, 2e-3, 6, 21),
+]
+
+
+def make_turb_fixture(path: str, N, scheme, nu, dt, nsteps, seed) -> None:
+    q0 = turb_initial_spec(N, N, seed=seed)
+    if scheme == "SBDF2":
+        q = run_turb(q0, N, 2 * np.pi, 2 * np.pi, nu, dt, nsteps)
+    else:
+        q = run_turb_rk(q0, N, 2 * np.pi, 2 * np.pi, nu, dt, nsteps, scheme)
+    np.savez_compressed(path, N=N, scheme=scheme, nu=nu, dt=dt, nsteps=nsteps, seed=seed, q0=q0, q=q)
 
 
 def make_transform_fixture(path: str) -> None:
@@ -79,6 +97,8 @@ def main() -> None:
     make_transform_fixture(os.path.join(HERE, "transforms.npz"))
     for name, Nx, Nz, Ra, scheme, dt, ns in CASES:
         make_step_fixture(os.path.join(HERE, f"{name}.npz"), Nx, Nz, Ra, scheme, dt, ns)
+    for name, *case in TURB_CASES:
+        make_turb_fixture(os.path.join(HERE, f"{name}.npz"), *case)
     print("wrote fixtures to", HERE)
 
 

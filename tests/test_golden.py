@@ -38,3 +38,16 @@ def test_step_fixture(golden_dir, name):
     sim = run_rbc(p, str(d["scheme"]), float(d["dt"]), int(d["nsteps"]), seed=42)
     for f, arr in (("b", sim.b), ("ux", sim.ux), ("uz", sim.uz)):
         assert rel_l2(arr, d[f]) < 1e-12, f
+
+
+@pytest.mark.parametrize("name", ["turb_sbdf2_32", "turb_rk443_32"])
+def test_turbulence_fixture(golden_dir, name):
+    from oracle.tarang_oracle import run_turb, run_turb_rk, turb_initial_spec
+
+    d = np.load(os.path.join(golden_dir, f"{name}.npz"))
+    N, scheme, seed = int(d["N"]), str(d["scheme"]), int(d["seed"])
+    q0 = turb_initial_spec(N, N, seed=seed)
+    assert rel_l2(q0, d["q0"]) < 1e-15
+    args = (q0, N, 2 * np.pi, 2 * np.pi, float(d["nu"]), float(d["dt"]), int(d["nsteps"]))
+    q = run_turb(*args) if scheme == "SBDF2" else run_turb_rk(*args, scheme)
+    assert rel_l2(q, d["q"]) < 1e-12
