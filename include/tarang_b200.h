@@ -219,7 +219,10 @@ tb_status tb_dealiased_multiply(tb_plan* plan, const double* a_grid, const doubl
  * held until exit), so Nx <= 2048 (else TB_ENOTSUPPORTED).  Calls share that
  * array: calls that overlap on the GPU race.  The first call on a device
  * resolves the array's address (once per device); make it before any stream
- * capture.  Runs on the legacy default stream and returns when done. */
+ * capture.  Runs on the legacy default stream, which does not wait for
+ * non-blocking streams (CUDA.jl task streams, torch side streams): synchronise
+ * the stream that wrote a_grid and b_grid before calling.  Returns when
+ * out_grid is written. */
 tb_status tb_dealiased_multiply_noalloc(int device, int Nx, int Nz, const double* a_grid, const double* b_grid,
                                         double* out_grid);
 

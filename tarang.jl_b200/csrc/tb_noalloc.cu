@@ -16,7 +16,11 @@
 //     that overlap on the GPU (from several host threads or streams) race;
 //   * the first call on a device resolves the array's device address with
 //     that device current (once per device); make that first call before any
-//     stream capture.
+//     stream capture;
+//   * the kernels run on the legacy default stream, which does not wait for
+//     work on non-blocking streams (CUDA.jl task streams, a framework's side
+//     streams): the caller synchronises the stream that wrote a_grid and
+//     b_grid before the call.  The call returns when out_grid is written.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -74,8 +78,18 @@ extern "C" {
 
 tb_status tb_dealiased_multiply_noalloc(int device, int Nx, int Nz, const double* a_grid, const double* b_grid,
                                         double* out_grid) {
-  if (!a_grid || !b_grid || !out_grid || Nz < 1) return TB_EINVAL;
-  if (device < 0 || device >= kMaxDevices) return TB_EINVAL;
+  if (!a_grid || !b_grid || !out_grid) {
+    tb::set_thread_error("a_grid, b_grid and out_grid must be non-null device pointers");
+    return TB_EINVAL;
+  }
+  if (Nz < 1) {
+    tb::set_thread_error("Nz must be >= 1");
+    return TB_EINVAL;
+  }
+  if (device < 0 || device >= kMaxDevices) {
+    tb::set_thread_error("device index out of range");
+    return TB_EINVAL;
+  }
   if (Nx < 6 || Nx % 2) {
     tb::set_thread_error("Nx must be even and >= 6");
     return TB_EINVAL;

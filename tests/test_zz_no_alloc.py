@@ -1,4 +1,5 @@
-"""The allocation-free dealiased product, checked against the plan entry point.
+"""The allocation-free dealiased product, checked against the plan entry point
+and the oracle's padded product.
 
 tb_dealiased_multiply_noalloc serves callers that cannot let a library call
 cudaMalloc (a host runtime that owns the device memory pool, or a process with
@@ -34,15 +35,23 @@ def _noalloc_product(tb, Nx, Nz, a, b):
     return out.cpu().numpy()
 
 
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
 def test_noalloc_product_matches_plan_entry_point_on_two_calls(tb):
+    from oracle.tarang_oracle import padded_multiply
+
     rng = np.random.default_rng(11)
-    # two calls in a row with different sizes: the second rewrites the shared twiddles
-    for Nx, Nz in ((256, 64), (96, 17)):
+    # calls in a row with different sizes: each rewrites the shared twiddles.
+    # Nx = 2048 (padded length 3072) fills the static array exactly.
+    for Nx, Nz in ((256, 64), (96, 17), (2048, 4), (256, 64)):
         a = rng.standard_normal((Nz, Nx))
         b = rng.standard_normal((Nz, Nx))
         want = _plan_product(tb, Nx, Nz, a, b)
         got = _noalloc_product(tb, Nx, Nz, a, b)
-        assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-12
+        assert _rel(got, want) < 1e-12, (Nx, Nz)
+        assert _rel(got, padded_multiply(a, b)) < 1e-12, (Nx, Nz)
 
 
 def test_noalloc_product_rejects_sizes_beyond_its_array(tb):
@@ -54,3 +63,5 @@ def test_noalloc_product_rejects_sizes_beyond_its_array(tb):
     assert b"2048" in tb.lib.tb_last_error(None)
     assert tb.lib.tb_dealiased_multiply_noalloc(0, 14, 2, p, p, p) == 6  # 14 = 2 x 7: no radix-2/3 FFT
     assert tb.lib.tb_dealiased_multiply_noalloc(0, 15, 2, p, p, p) == 1  # odd Nx
+    assert tb.lib.tb_dealiased_multiply_noalloc(0, 64, 2, p, None, p) == 1  # null buffer
+    assert b"null" in tb.lib.tb_last_error(None)
