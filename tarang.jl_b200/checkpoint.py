@@ -41,7 +41,10 @@ def write_checkpoint(path: str, fields: Dict[str, np.ndarray], clock: Sequence[f
             v = f.createVariable(name, "d", dims)
             v[...] = np.asarray(arr, dtype=np.float64)
         f.sim_time = np.array([clock[0]], dtype=np.float64)  # double attributes, not float32
-        f.iteration = np.array([int(clock[1])], dtype=np.int32)
+        # the reference writes the iteration as a Julia Int (64-bit); classic
+        # NetCDF has no 64-bit integer, and a double holds every count up to
+        # 2^53 exactly, where a 32-bit int would wrap at 2^31
+        f.iteration = np.array([float(int(clock[1]))], dtype=np.float64)
         f.dt = np.array([clock[2]], dtype=np.float64)
     os.replace(tmp, path)
 

@@ -21,6 +21,16 @@ def test_round_trip_2d_and_3d(tmp_path):
         assert list(clock) == [1.25, 40.0, 0.01]
 
 
+def test_iteration_beyond_int32_survives(tmp_path):
+    # the reference stores the iteration as a 64-bit Int
+    names = ck.field_names(2)
+    fields = {n: np.zeros((2, 4)) for n in names}
+    path = str(tmp_path / "big.nc")
+    ck.write_checkpoint(path, fields, (3.0, 2**31 + 7, 0.5))
+    _, clock = ck.read_checkpoint(path, names)
+    assert int(clock[1]) == 2**31 + 7
+
+
 def test_missing_clock_is_refused(tmp_path):
     from scipy.io import netcdf_file
 
