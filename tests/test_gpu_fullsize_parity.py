@@ -1,0 +1,83 @@
+"""Parity at the benchmark sizes over many steps, against stored oracle runs.
+
+The Float64 bar is 1e-10 relative L2 of every field after 100 steps; the mixed
+form (FP32 transforms and products, FP64 tau solves) is held to 1e-6 against the
+same Float64 oracle runs.  The fixtures (tests/golden/make_golden.py --large)
+are the oracle's state after:
+  * 100 steps of the 2D benchmark grid, ChannelDomain(1024, 256), Lx 4, Lz 1,
+    Ra 1e8, Pr 1, dt 0.01, seeded noise (seed 42), RK443 and SBDF2;
+  * 20 steps of a 64x64x32 3D channel (Lx = Ly = 4, Lz 1) with the 3D
+    benchmark's parameters: Ra 1e7, Pr 1, dt 5e-3, RK222, seed 42.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle.tarang_oracle import RBC3Params, RBCParams, forward_2d, rbc3_initial_b, rbc_initial_b, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TS = {"RK222": 0, "RK443": 1, "SBDF1": 2, "SBDF2": 3}
+F64_BAR = 1e-10
+MIXED_BAR = 1e-6
+
+
+def _fixture(golden_dir, name):
+    path = os.path.join(golden_dir, f"{name}.npz")
+    if not os.path.exists(path):
+        pytest.fail(f"missing fixture {path}: run python tests/golden/make_golden.py --large")
+    return np.load(path)
+
+
+def _run_2d(tb, d, precision):
+    Nx, Nz = int(d["Nx"]), int(d["Nz"])
+    p = RBCParams(Nx=Nx, Nz=Nz, Lx=4.0, Lz=1.0, Ra=float(d["Ra"]), Pr=1.0)
+    dom = tb.ChannelDomain(Nx, Nz, Lx=4.0, Lz=1.0)
+    plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, TS[str(d["scheme"])], precision=precision)
+    plan.set_state(0, forward_2d(rbc_initial_b(p, 42)))
+    plan.step(float(d["dt"]), int(d["nsteps"]))
+    return plan
+
+
+@pytest.mark.parametrize("name", ["rbc_c2_rk443_1024x256", "rbc_c2_sbdf2_1024x256"])
+def test_c2_100_steps_f64_every_field(tb, golden_dir, name):
+    d = _fixture(golden_dir, name)
+    plan = _run_2d(tb, d, tb._lib.TB_PREC_F64)
+    for sel, f in ((0, "b"), (1, "ux"), (2, "uz")):
+        err = rel_l2(plan.get_state(sel), d[f])
+        assert err < F64_BAR, (f, err)
+    pr = plan.get_state(3)
+    if str(d["scheme"]) == "SBDF2":
+        err = rel_l2(pr, d["p"])
+        assert err < F64_BAR, ("p", err)
+    else:
+        # the RK final update is the reference's min-norm mass solve, which
+        # zeroes the pressure
+        assert np.abs(pr).max() == 0.0 and np.abs(d["p"]).max() == 0.0
+
+
+@pytest.mark.parametrize("name", ["rbc_c2_rk443_1024x256", "rbc_c2_sbdf2_1024x256"])
+def test_c2_100_steps_mixed_against_f64_oracle(tb, golden_dir, name):
+    d = _fixture(golden_dir, name)
+    plan = _run_2d(tb, d, tb._lib.TB_PREC_MIXED)
+    for sel, f in ((0, "b"), (1, "ux"), (2, "uz")):
+        err = rel_l2(plan.get_state(sel), d[f])
+        assert err < MIXED_BAR, (f, err)
+    if str(d["scheme"]) == "SBDF2":
+        err = rel_l2(plan.get_state(3), d["p"])
+        assert err < MIXED_BAR, ("p", err)
+
+
+@pytest.mark.parametrize("precision,bar", [("F64", F64_BAR), ("MIXED", MIXED_BAR)])
+def test_3d_20_steps_against_oracle(tb, golden_dir, precision, bar):
+    d = _fixture(golden_dir, "rbc3_rk222_64x64x32")
+    Nx, Ny, Nz = int(d["Nx"]), int(d["Ny"]), int(d["Nz"])
+    p = RBC3Params(Nx=Nx, Ny=Ny, Nz=Nz, Ra=float(d["Ra"]))
+    plan = tb.Plan3D(Nx, Ny, Nz, p.kappa, p.nu, TS[str(d["scheme"])], p.Lx, p.Ly, p.Lz,
+                     precision=getattr(tb._lib, f"TB_PREC_{precision}"))
+    plan.set_state(tb._lib.TB_FIELD_B, plan.forward(rbc3_initial_b(p, 42)))
+    plan.step(float(d["dt"]), int(d["nsteps"]))
+    for name, f in (("b", 0), ("ux", 1), ("uy", 5), ("uz", 2)):
+        err = rel_l2(plan.get_state(f), d[name])
+        assert err < bar, (name, err)
