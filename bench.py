@@ -243,6 +243,37 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+def host_info(threads: int) -> dict:
+    """The host the CPU legs run on: CPU model, core count, thread settings,
+    and whether the reference itself (Julia + the Tarang.jl sources) could run
+    here instead of the restatement."""
+    import shutil
+
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    julia = shutil.which("julia")
+    return {
+        "cpu_model": model,
+        "nproc": os.cpu_count(),
+        "threads_used": threads,
+        "thread_settings": {"pocketfft_workers": threads, "per_mode_pool_threads": threads,
+                            **{k: os.environ.get(k) for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS",
+                                                              "MKL_NUM_THREADS")}},
+        "julia": julia,
+        "reference_runnable": False,
+        "why_restatement": ("julia found at " + julia + " but the Tarang.jl sources and their FFTW/SuiteSparse "
+                            "dependencies are not installed on this host") if julia else
+                           "no julia executable on this host (probed with shutil.which at run time)",
+    }
+
+
 # ---------------------------------------------------------------------------
 def run_reference(args, cfg, scheme, dist):
     """CPU restatement of the reference's algorithm, timed on the host cores."""
@@ -298,8 +329,8 @@ def run_reference(args, cfg, scheme, dist):
             "sample": f"{nsteps} steps (of --steps {args.steps}, capped at {REF_SAMPLE_S:.0f} s) after {nwarm} "
                       "warm-up steps (the first factors the tau LHS) "
                       f"of the full {cfg.Nx}x{cfg.Nz} problem; NumPy/SciPy restatement (SuperLU per mode), "
-                      f"{threads} host threads (pocketfft workers, per-mode solves on a thread pool); "
-                      "Julia is absent so the reference itself cannot run",
+                      f"{threads} host threads (pocketfft workers, per-mode solves on a thread pool)",
+            "host": host_info(threads),
         },
         "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -345,6 +376,7 @@ def cpu_baseline(cfg, scheme, nsteps):
         "sample": f"{nsteps} steps of the full {cfg.Nx}x{cfg.Nz} {scheme} problem after 3 warm-up steps; "
                   "NumPy/SciPy restatement of the reference CPU path (SuperLU per Fourier mode), "
                   f"{threads} host threads (pocketfft workers, per-mode solves on a thread pool)",
+        "host": host_info(threads),
     }
 
 
@@ -411,18 +443,28 @@ def run_ours(args, cfg, scheme, dist):
                     "flops_per_launch": work, "peak_source": "cuBLAS FP64 GEMM (torch.matmul float64) measured in bench"}
         roof["avg_launch_ms"] = avg_ms
         roof["peak_source"] = roof.get("peak_source", f"MEASURED_PEAKS.json ({peak_src})")
-        # DRAM traffic per launch from the committed ncu capture of this workload
-        tpath = os.path.join(ROOT, "profiles", f"traffic_{cfg.Nx}x{cfg.Nz}_{scheme.lower()}.json")
-        if os.path.exists(tpath):
-            with open(tpath) as f:
-                tr = json.load(f)
-            if top in tr:
-                roof["traffic"] = tr[top]
-                roof["traffic_source"] = tpath.replace(ROOT + os.sep, "")
+    # DRAM traffic per launch (average over a step's launches of each kernel
+    # name) from the committed ncu capture of this workload
+    tpath = os.path.join(ROOT, "profiles", f"traffic_{cfg.Nx}x{cfg.Nz}_{scheme.lower()}.json")
+    tr = {}
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tr = {k: v for k, v in json.load(f).items() if not k.startswith("_")}
+    if roof is not None and top in tr:
+        roof["traffic"] = tr[top]
+        roof["traffic_source"] = tpath.replace(ROOT + os.sep, "")
     model = W.step_model_bytes(cfg, scheme)
-    step_roof = {"bytes_per_step_model": model, "achieved_gbs": model / (ms / args.steps / 1e3) / 1e9,
+    step_s = ms / args.steps / 1e3
+    step_roof = {"bytes_per_step_model": model, "achieved_gbs": model / step_s / 1e9,
                  "peak_gbs": peaks.get("hbm_gbs")}
     step_roof["frac"] = step_roof["achieved_gbs"] / step_roof["peak_gbs"]
+    if tr and all(k in tr for k in prof):
+        # what the step really moves: measured DRAM bytes of every kernel
+        # launch of one step (ncu), over the device time of a step
+        meas = sum(tr[k] * prof[k][1] / nprof for k in prof)
+        step_roof["measured_dram_bytes_per_step"] = meas
+        step_roof["measured_frac"] = meas / step_s / (step_roof["peak_gbs"] * 1e9)
+        step_roof["measured_source"] = tpath.replace(ROOT + os.sep, "")
 
     # end to end through the C ABI with host buffers: per step, upload the state
     # from pinned host memory, one step, download the state
@@ -517,7 +559,42 @@ def run_ours(args, cfg, scheme, dist):
             out["ensemble"] = ens_out
         if not args.no_serving:
             out["serving"] = srv_out
+        out["summary"] = summarize(out)  # last key: compact, so a truncated tail still carries it
         print(json.dumps(out), flush=True)
+
+
+def summarize(out: dict) -> dict:
+    """The headline and every secondary workload's main numbers, rounded."""
+
+    def g(d, *keys):
+        for k in keys:
+            if not isinstance(d, dict) or k not in d or d[k] is None:
+                return None
+            d = d[k]
+        return round(d, 4) if isinstance(d, float) else d
+
+    s = {"steps_per_s": g(out, "value"), "e2e_steps_per_s": g(out, "e2e", "value"),
+         "tau_solve_frac": g(out, "roofline", "frac"), "step_model_frac": g(out, "step_roofline", "frac"),
+         "step_measured_frac": g(out, "step_roofline", "measured_frac")}
+    if "mixed" in out:
+        errs = g(out, "mixed", "rel_l2_vs_f64_after_steps") or {}
+        s["mixed"] = {"steps_per_s": g(out, "mixed", "value"), "max_rel_l2_vs_f64": max(errs.values()) if errs else None}
+    if "c1" in out:
+        s["c1_steps_per_s"] = g(out, "c1", "value")
+    if "sbdf2" in out:
+        s["sbdf2"] = {"f64": g(out, "sbdf2", "f64", "value"), "mixed": g(out, "sbdf2", "mixed", "value")}
+    if "rbc3d" in out:
+        s["rbc3d"] = {"mixed": g(out, "rbc3d", "value"), "f64": g(out, "rbc3d", "f64_plan_steps_per_s")}
+    if "ensemble" in out:
+        s["ensemble"] = {"fused": g(out, "ensemble", "value"),
+                         "per_member_streams": g(out, "ensemble", "per_member_streams", "value"),
+                         "plain_gpu": g(out, "ensemble", "plain_gpu", "value")}
+    if "serving" in out:
+        s["serving"] = {"saturated": g(out, "serving", "saturated", "solves_per_s"),
+                        "plain_saturated": g(out, "serving", "plain_gpu_saturated", "solves_per_s"),
+                        "replay_p50_ms": g(out, "serving", "replay", "p50_ms"),
+                        "replay_p99_ms": g(out, "serving", "replay", "p99_ms")}
+    return s
 
 
 def run_ensemble(args, dev, dist=None):
@@ -579,8 +656,18 @@ def run_ensemble(args, dev, dist=None):
     ms, total = ens.run(dts, n)
     wall = time.perf_counter() - t0
     finite = all(np.isfinite(p.get_state(0)).all() for p in plans)
+    # the stronger GPU comparator: every member its own plan, graphs launched
+    # on the tuned worker streams (the ensemble runner's per-member form)
+    stream_total = None
+    if tuned_fused:
+        ens.set_form(False)
+        reset()
+        torch.cuda.synchronize()
+        _, stream_total = ens.run(dts, n)
+        ens.set_form(True)
     part = {"steps": len(plans) * n, "total_ms": float(total), "ms": [float(v) for v in ms], "plain_s": plain_s,
-            "plain_done_ms": done, "finite": bool(finite)}
+            "plain_done_ms": done, "finite": bool(finite),
+            "streams_total_ms": None if stream_total is None else float(stream_total)}
     parts = dist.gather(part) if dist else [part]
     agg = W.combine_ensemble(parts)
     sizes = {}
@@ -606,6 +693,11 @@ def run_ensemble(args, dev, dist=None):
                       "what": "the same plans stepped one after another with tb_step (host wall clock)",
                       "time_to_solution_ms": {"p50": agg["plain_p50_ms"], "p99": agg["plain_p99_ms"]}},
         "speedup_vs_plain_gpu": agg["value"] / agg["plain_value"],
+        "per_member_streams": None if any(p["streams_total_ms"] is None for p in parts) else {
+            "value": sum(p["steps"] for p in parts) / (max(p["streams_total_ms"] for p in parts) / 1e3),
+            "unit": "instance-steps/s",
+            "what": "the same members as separate plans, step graphs launched on the tuned worker streams "
+                    "(device clock)"},
         "finite": all(p["finite"] for p in parts),
         "data": "synthetic: sizes, Ra, Pr and noise seeded (ensemble seed 7, member noise seed 1000+k)",
     }
