@@ -1203,10 +1203,16 @@ class RBC3D:
             out.append(forward_3d(-t))
         return out
 
-    def step_rk(self, dt: float, ts: dict) -> None:
+    def step_rk(self, dt: float, ts: dict, modes=None, rhs_fn=None, proj_fn=None) -> None:
+        """One IMEX RK step.  `modes` restricts the per-mode work to a subset
+        (a rank of a mode-sharded step), `rhs_fn()` then supplies F for those
+        modes and `proj_fn(c)` the grid round trip of a field on them; by
+        default every mode, RBC3D.rhs and RBC3D.projected."""
         AE, AI, bE, bI = ts["AE"], ts["AI"], ts["bE"], ts["bI"]
         s = AE.shape[0]
-        modes = self.modes()
+        modes = self.modes() if modes is None else modes
+        rhs_fn = rhs_fn or (lambda: self.rhs(self.b, self.ux, self.uy, self.uz))
+        proj_fn = proj_fn or self.projected
 
         def mapped(fn):
             return dict(zip(modes, _pmap(fn, modes)))
@@ -1241,8 +1247,8 @@ class RBC3D:
             xs = mapped(stage_solve)
             for m in modes:
                 self.scatter(*m, xs[m])
-            Fc = self.rhs(self.b, self.ux, self.uy, self.uz)
-            proj = [self.pr] + [self.projected(c) for c in (self.b, self.ux, self.uy, self.uz)]
+            Fc = rhs_fn()
+            proj = [self.pr] + [proj_fn(c) for c in (self.b, self.ux, self.uy, self.uz)]
             F.append(mapped(lambda m: self.equation_F(*m, Fc)))
             LX.append(mapped(lambda m: self.mode_matrices(*m)[1] @ self.gather(*m, proj, self.tau)))
 
@@ -1317,6 +1323,120 @@ class RBC3D:
     def state_dict(self) -> Dict[str, np.ndarray]:
         return dict(b=self.b.copy(), ux=self.ux.copy(), uy=self.uy.copy(), uz=self.uz.copy(), p=self.pr.copy(),
                     tau=self.tau.copy())
+
+
+# ---------------------------------------------------------------------------
+# The 3D RHS in pencil form: the CPU stand-in for the per-rank kernels of a
+# mode-sharded step (a rank owns a kx range, all ky and z).  The same
+# arithmetic as RBC3D.rhs (lazy_rhs.jl:712-1336 with padded_multiply_3d,
+# nonlinear_padding.jl:86-103, 182-443) reordered by axis, as the reference's
+# pencil transposes reorder it (subproblem_io.jl:100-330): the z and y work
+# per kx column, the x work per padded y row.
+# ---------------------------------------------------------------------------
+def _y_pad(S: np.ndarray, My: int) -> np.ndarray:
+    """Zero-pad a full y spectrum (axis -2, FFT order) to My rows with the
+    even-Ny Nyquist split X/2 at +-Ny/2 (_pad_full's y part)."""
+    Ny = S.shape[-2]
+    hy, nneg = Ny // 2, Ny - Ny // 2 - 1
+    P = np.zeros(S.shape[:-2] + (My, S.shape[-1]), dtype=complex)
+    P[..., : hy + 1, :] = S[..., : hy + 1, :]
+    if nneg:
+        P[..., My - nneg:, :] = S[..., Ny - nneg:, :]
+    if Ny % 2 == 0 and My > Ny:
+        P[..., hy, :] *= 0.5
+        P[..., My - hy, :] = P[..., hy, :]
+    return P
+
+
+def _y_truncate(P: np.ndarray, Ny: int) -> np.ndarray:
+    """Fold the -Ny/2 image into +Ny/2 and truncate (_truncate_full's y part)."""
+    My = P.shape[-2]
+    P = P.copy()
+    hy, nneg = Ny // 2, Ny - Ny // 2 - 1
+    if Ny % 2 == 0 and My > Ny:
+        P[..., hy, :] += P[..., My - hy, :]
+    out = np.zeros(P.shape[:-2] + (Ny, P.shape[-1]), dtype=complex)
+    out[..., : hy + 1, :] = P[..., : hy + 1, :]
+    if nneg:
+        out[..., Ny - nneg:, :] = P[..., My - nneg:, :]
+    return out
+
+
+def rhs3_stage_modes(sim: "RBC3D", coeffs: Sequence[np.ndarray], kx_lo: int) -> np.ndarray:
+    """Coefficients (b, ux, uy, uz), each (Nz, Ny, Kx_r) for kx indices kx_lo..,
+    -> 12 arrays [field][value, d/dy, d/dz] on (z grid, padded y grid, kx):
+    the grid round trip's projection of the kx = 0 and kx = Nx/2 planes (Im
+    dropped after the inverse y transform, as FFTW's c2r drops it), z
+    derivative in coefficient space, Chebyshev backward, y padding, inverse y
+    transform (1/My)."""
+    p = sim.p
+    Ny = p.Ny
+    My = padded_length(Ny, p.dealias)
+    Kr = coeffs[0].shape[-1]
+    ix = kx_lo + np.arange(Kr)
+    edge = (ix == 0) | (ix == p.Nx // 2)
+    KY = (1j * sim.ky)[None, :, None]
+    out = []
+    for c in coeffs:
+        # projection: the kx = 0 / Nyquist planes of c through the y round trip with Im dropped
+        t = _fx.ifft(cheb_backward(c, axis=0), axis=1)
+        t[..., edge] = np.real(t[..., edge])
+        pc = cheb_forward(_fx.fft(t, axis=1), axis=0)
+        for S in (pc, KY * pc, np.tensordot(sim.D, pc, axes=(1, 0))):
+            g = _fx.ifft(cheb_backward(S, axis=0), axis=1)  # (z, y, kx): Ny-point inverse (1/Ny)
+            g[..., edge] = np.real(g[..., edge])
+            out.append(_fx.ifft(_y_pad(_fx.fft(g, axis=1), My), axis=1))  # My-point inverse (1/My)
+    return np.stack(out)
+
+
+def rhs3_stage_rows(sim: "RBC3D", rows: np.ndarray) -> np.ndarray:
+    """12 arrays (z, y rows, Kx) -> the 4 products -(u.grad f) for f = b, ux,
+    uy, uz on these rows, forward x transform, x Nyquist fold and truncation:
+    (4, z, y rows, Kx).  d/dx from the kx bins (Im dropped at kx = 0 and Nx/2,
+    as the grid round trip does), x padding with the Nyquist split, inverse
+    real x transform on Mx points (1/Mx)."""
+    p = sim.p
+    Nx = p.Nx
+    Mx = padded_length(Nx, p.dealias)
+    hx = Nx // 2
+    KX = 1j * sim.kx
+
+    def x_grid(X):
+        H = np.zeros(X.shape[:-1] + (Mx // 2 + 1,), dtype=complex)
+        H[..., :hx] = X[..., :hx]
+        if Nx % 2 == 0 and Mx > Nx:
+            H[..., hx] = 0.5 * X[..., hx]
+        else:
+            H[..., hx] = X[..., hx]
+        return _fx.irfft(H, n=Mx, axis=-1)
+
+    f = rows.reshape((4, 3) + rows.shape[1:])
+    grids = {}
+    for i in range(4):
+        val, dy, dz = f[i]
+        dxs = KX * val
+        dxs[..., 0] = np.real(dxs[..., 0])
+        dxs[..., hx] = np.real(dxs[..., hx])
+        grids[i] = (x_grid(val), x_grid(dxs), x_grid(dy), x_grid(dz))
+    u, v, w = grids[1][0], grids[2][0], grids[3][0]
+    out = []
+    for i in range(4):
+        _, gx, gy, gz = grids[i]
+        X = _fx.rfft(-(u * gx + v * gy + w * gz), axis=-1)[..., : hx + 1]
+        if Nx % 2 == 0 and Mx > Nx:
+            X[..., hx] = 2.0 * np.real(X[..., hx])
+        out.append(X)
+    return np.stack(out)
+
+
+def rhs3_stage_back(sim: "RBC3D", back: np.ndarray) -> List[np.ndarray]:
+    """4 arrays (z, padded y, Kx_r) -> the F coefficients (Nz, Ny, Kx_r): forward
+    y transform, y Nyquist fold and truncation, the 3/2 rule's (Mx/Nx)(My/Ny)
+    scaling, Chebyshev forward."""
+    p = sim.p
+    My, Mx = padded_length(p.Ny, p.dealias), padded_length(p.Nx, p.dealias)
+    scale = (Mx / p.Nx) * (My / p.Ny)
+    return [cheb_forward(_y_truncate(_fx.fft(b, axis=1), p.Ny) * scale, axis=0) for b in back]
 
 
 def run_rbc3(p: RBC3Params, scheme: str, dt: float, nsteps: int, seed: int = 42) -> RBC3D:
