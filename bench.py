@@ -44,6 +44,8 @@ def parse_args():
     ap.add_argument("--scheme", choices=["RK443", "RK222", "SBDF2"], default="RK443")
     ap.add_argument("--config", choices=["c2", "c1"], default="c2")
     ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--tau-parts", type=int, default=0, choices=[0, 1, 4, 8],
+                    help="tau-solve partitions of the headline plan (0: chosen by the plan's tuner)")
     ap.add_argument("--cpu-steps", type=int, default=10,
                     help="timed steps of the CPU baseline leg (about 1 s each on 16 host threads)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -400,8 +402,10 @@ def run_ours(args, cfg, scheme, dist):
 
     # warm-up (the first call factors the tau systems and captures the step graph),
     # then the plan's kernel shapes are tuned on a few steps (state restored)
+    if args.tau_parts:
+        plan.set_variant(tau_parts=args.tau_parts)
     plan.step(cfg.dt, args.warmup)
-    tuned = plan.tune(cfg.dt, trial_steps=3)
+    tuned = (args.tau_parts, 0) if args.tau_parts else plan.tune(cfg.dt, trial_steps=3)
     plan.step(cfg.dt, 1)
 
     # timed region: K graph replays, device time from CUDA events on the plan's stream
@@ -514,7 +518,7 @@ def run_ours(args, cfg, scheme, dist):
             "e2e": e2e,
             "gpu_launches": kps * args.steps,
             "kernels_per_step": kps,
-            "tuned": {"tau_solve_partitions": tuned[0]},
+            "tuned": {"tau_solve_partitions": tuned[0], "x_products_form": tuned[1]},
             "roofline": roof,
             "step_roofline": step_roof,
             "kernel_shares": {k: round(v, 4) for k, v in sorted(shares.items(), key=lambda x: -x[1])},
@@ -543,6 +547,11 @@ def run_ours(args, cfg, scheme, dist):
                 out["rbc3d"] = run_rbc3d(args, dev)
             except Exception as exc:  # reported, never fatal to the headline line
                 out["rbc3d"] = {"error": f"{type(exc).__name__}: {exc}"}
+        if dist.world == 1 and not args.no_mixed:
+            try:
+                out["dense_lu"] = run_dense_lu(dev)
+            except Exception as exc:  # reported, never fatal to the headline line
+                out["dense_lu"] = {"error": f"{type(exc).__name__}: {exc}"}
     # sharded across every rank (collective statistics: all ranks take part)
     if not args.no_ensemble:
         try:
@@ -581,6 +590,8 @@ def summarize(out: dict) -> dict:
         s["mixed"] = {"steps_per_s": g(out, "mixed", "value"), "max_rel_l2_vs_f64": max(errs.values()) if errs else None}
     if "c1" in out:
         s["c1_steps_per_s"] = g(out, "c1", "value")
+    if "dense_lu" in out:
+        s["dense_lu_ms"] = {"ours": g(out, "dense_lu", "ours_ms"), "vendor": g(out, "dense_lu", "vendor_ms")}
     if "sbdf2" in out:
         s["sbdf2"] = {"f64": g(out, "sbdf2", "f64", "value"), "mixed": g(out, "sbdf2", "mixed", "value")}
     if "rbc3d" in out:
@@ -730,7 +741,9 @@ def run_mixed(args, cfg, scheme, dev):
     full.step(cfg.dt, n)
     err = {name: float(np.linalg.norm(mixed.get_state(f) - full.get_state(f)) / np.linalg.norm(full.get_state(f)))
            for f, name in ((0, "b"), (1, "ux"), (2, "uz"))}
-    # timing: graph replay after warm-up, from the state reached above
+    # timing: graph replay after warm-up, from the state reached above, with
+    # the kernel shapes the plan's tuner picks (state restored by the tuner)
+    tuned = mixed.tune(cfg.dt, trial_steps=3)
     mixed.step(cfg.dt, args.warmup)
     torch.cuda.synchronize()
     mixed.step(cfg.dt, n)
@@ -742,6 +755,8 @@ def run_mixed(args, cfg, scheme, dev):
         "ms_per_step": ms / n,
         "rel_l2_vs_f64_after_steps": err,
         "steps": n,
+        "tuned": {"tau_solve_partitions": tuned[0], "x_products_form": tuned[1],
+                  "tensor_core_gemms": mixed.gemm_path()},
         "dtype": "f32 transforms/products, f64 solves/stage algebra",
     }
 
@@ -774,11 +789,12 @@ def run_sbdf2(args, cfg, dev):
     model = W.step_model_bytes(cfg, "SBDF2")
     out = {}
     for name, pl in (("f64", full), ("mixed", mixed)):
+        tuned = pl.tune(cfg.dt, trial_steps=3)
         pl.step(cfg.dt, args.warmup)
         torch.cuda.synchronize()
         pl.step(cfg.dt, n)
         ms = pl.last_step_ms() / n
-        out[name] = {"value": 1e3 / ms, "ms_per_step": ms,
+        out[name] = {"value": 1e3 / ms, "ms_per_step": ms, "tuned": list(tuned),
                      "step_roofline_frac": model / (ms * 1e-3) / (peaks["hbm_gbs"] * 1e9)}
     return {
         "metric": f"RBC 2D steps/s ({cfg.Nx}x{cfg.Nz}, SBDF2)",
@@ -812,6 +828,7 @@ def run_c1(args, dev):
     b0 = pl.forward(W.rbc_initial_grid(c))
     pl.set_state(0, b0)
     pl.step(c.dt, max(args.warmup, 3))
+    tuned = pl.tune(c.dt, trial_steps=3)
     pl.set_state(0, b0)
     for f in (1, 2, 3):
         pl.set_state(f, np.zeros_like(b0))
@@ -829,9 +846,72 @@ def run_c1(args, dev):
         "steps": n,
         "bytes_per_step_model": model,
         "step_roofline_frac": model / (ms * 1e-3) / (peaks["hbm_gbs"] * 1e9),
+        "tuned": list(tuned),
         "note": "the working set (~0.01 GB) stays in the 126 MB L2, so the HBM fraction is not a bound here; "
                 "the step is launch- and latency-bound",
     }
+
+
+def run_dense_lu(dev, n: int = 263, batch: int = 129, reps: int = 5):
+    """BatchedDenseLU at the small configuration's size (129 Fourier modes,
+    n = 4 Nz + 7 = 263 at Nz = 64): the library's batched complex LU
+    (tb_batched_lu_factor, the drop-in for batched_factor! whose CUDA method
+    calls getrf strided-batched) against torch.linalg.lu_factor on the same
+    slices (the vendor batched getrf), device time of the factorisation, and
+    the relative residual of a solve with each."""
+    import ctypes
+
+    import torch
+
+    from __graft_entry__ import load_package
+
+    tb = load_package()
+    g = torch.Generator(device="cpu").manual_seed(3)
+    A0 = (torch.randn(batch, n, n, dtype=torch.complex128, generator=g)
+          + n * torch.eye(n, dtype=torch.complex128)).to(dev)
+    b = torch.randn(batch, n, dtype=torch.complex128, generator=g).to(dev)
+    ctx = tb.api._context(dev)
+
+    def ours():
+        A = A0.transpose(1, 2).contiguous()  # column-major slices
+        piv = torch.empty(batch, n, dtype=torch.int32, device=dev)
+        bad = ctypes.c_int(-1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = tb.lib.tb_batched_lu_factor(ctx, n, batch, ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(piv.data_ptr()),
+                                         ctypes.byref(bad))
+        e1.record()
+        torch.cuda.synchronize()
+        assert st == 0, st
+        return e0.elapsed_time(e1), A, piv
+
+    def vendor():
+        A = A0.clone()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        LU, pv = torch.linalg.lu_factor(A)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), LU, pv
+
+    ours()
+    vendor()
+    t_ours = min(ours()[0] for _ in range(reps))
+    t_vendor = min(vendor()[0] for _ in range(reps))
+    _, A, piv = ours()
+    x = b.clone().contiguous()
+    st = tb.lib.tb_batched_lu_solve(ctx, n, batch, ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(piv.data_ptr()),
+                                    ctypes.c_void_p(x.data_ptr()))
+    assert st == 0, st
+    res = float((torch.linalg.norm(torch.einsum("bij,bj->bi", A0, x) - b) / torch.linalg.norm(b)).item())
+    _, LU, pv = vendor()
+    xv = torch.linalg.lu_solve(LU, pv, b.unsqueeze(-1)).squeeze(-1)
+    resv = float((torch.linalg.norm(torch.einsum("bij,bj->bi", A0, xv) - b) / torch.linalg.norm(b)).item())
+    return {"what": f"batched complex LU factorisation, {batch} slices of {n} x {n}",
+            "ours_ms": t_ours, "vendor_ms": t_vendor, "vendor": "torch.linalg.lu_factor (batched getrf)",
+            "ours_rel_residual": res, "vendor_rel_residual": resv}
 
 
 def kernel_work3(name: str, c, npad_main: int, npad_perp: int):

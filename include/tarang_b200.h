@@ -42,6 +42,13 @@ typedef struct tb_plan tb_plan;
 
 /* Where a host-visible pointer lives. */
 enum { TB_HOST = 0, TB_DEVICE = 1 };
+/* OR'ed into `where` of tb_set_state / tb_set_states: the write keeps the
+ * multistep (SBDF) history.  For a caller that mirrors the plan's state in its
+ * own field arrays and writes them back before every step (the Julia
+ * extension's per-step sync): the reference keeps its history across writes
+ * into a live state field (timestepper_data, src/core/timesteppers/state.jl:47-91),
+ * and a plain write restarts the history at SBDF1. */
+enum { TB_KEEP_HISTORY = 0x10 };
 
 /* Time steppers (src/core/timesteppers/types.jl:49-167, 217). */
 enum { TB_RK222 = 0, TB_RK443 = 1, TB_SBDF1 = 2, TB_SBDF2 = 3 };
@@ -102,7 +109,9 @@ tb_status tb_plan_create(tb_context* ctx, const tb_problem_desc* desc, tb_plan**
 tb_status tb_plan_destroy(tb_plan* plan);
 
 /* Coefficient-space state I/O (the fields' coefficient layout, :c).
- * where = TB_HOST or TB_DEVICE.  Replaces get_coeff_data/set on state fields. */
+ * where = TB_HOST or TB_DEVICE.  Replaces get_coeff_data/set on state fields.
+ * A set restarts the multistep history unless TB_KEEP_HISTORY is OR'ed into
+ * where. */
 tb_status tb_set_state(tb_plan* plan, int field, const void* data, int where);
 tb_status tb_get_state(tb_plan* plan, int field, void* data, int where);
 /* Several fields in one call: data[i] holds field fields[i] (2D plans).  The
@@ -176,18 +185,30 @@ tb_status tb_checkpoint_load(tb_plan* plan, const double* grid, int where, const
 
 /* Kernel shapes of a plan (the library's own autotuning; the reference tunes
  * FFTW plans instead, transform_fourier.jl plan cache):
- *   tau_parts  warps per 4-mode group in the tau solves: 4 (partitioned, the
- *              shortest latency for one plan) or 1 (no response records, the
- *              least device work per solve);
- *   xrows      3D only: padded y rows per x-pass CTA, 1, 2 or 4.
+ *   tau_parts  row partitions of each 4-mode group's tau solves: 8 (one per
+ *              half-warp, four warps) or 4 (one per warp) - partitioned, the
+ *              shortest latency for one plan - or 1 (no response records, the
+ *              least device work per solve; needs npad/12 >= parts);
+ *   xrows      3D: padded y rows per x-pass CTA, 1, 2 or 4; 2D (Float64
+ *              plans): the x-products kernel, 1 = the three gradient
+ *              transforms one after another, 2 = all inverse and forward
+ *              transforms of a row batched through shared passes.
  * 0 keeps a setting.  A change drops the plan's factors and step graphs; the
  * next step rebuilds them.  tb_plan_tune times trial_steps steps of every
  * feasible combination from the current state (the state is restored after
  * each trial and at the end) and keeps the fastest; *tau_parts / *xrows get
- * the choice (xrows 0 in 2D). */
+ * the choice. */
 tb_status tb_plan_set_variant(tb_plan* plan, int tau_parts, int xrows);
 tb_status tb_plan_get_variant(const tb_plan* plan, int* tau_parts, int* xrows);
 tb_status tb_plan_tune(tb_plan* plan, double dt, int trial_steps, int* tau_parts, int* xrows);
+/* FP32 Chebyshev transform GEMMs of a mixed-precision plan: tensor_cores = 1
+ * (the default) runs them on the tcgen05 tensor cores in TF32 with three
+ * products per term (FP32 accuracy) wherever Nz <= 256, 0 on the SIMT FP32
+ * kernel.  No counterpart in the reference, whose GPU Chebyshev transforms are
+ * cuFFT DCT-Is (ext/cuda/cheb_deriv.jl:503-596).  A change drops the plan's
+ * step graphs. */
+tb_status tb_plan_set_gemm_path(tb_plan* plan, int tensor_cores);
+tb_status tb_plan_get_gemm_path(const tb_plan* plan, int* tensor_cores);
 
 /* -------------------------------------------------------------------------
  * Transform backend.  Replaces Tarang._gpu_forward_transform_backend! /

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "libtarang_b200.so")
 
 TB_OK, TB_EINVAL, TB_ENOMEM, TB_ESINGULAR, TB_ETIMEOUT, TB_ECUDA, TB_ENOTSUPPORTED, TB_EBUDGET, TB_ESTATE = range(9)
 TB_HOST, TB_DEVICE = 0, 1
+TB_KEEP_HISTORY = 0x10
 TB_RK222, TB_RK443, TB_SBDF1, TB_SBDF2 = 0, 1, 2, 3
 TB_PROGRAM_RBC = 0
 TB_PROGRAM_TURB2D = 1
@@ -97,6 +98,8 @@ SIGNATURES = {
     "tb_checkpoint_wait": (c_int, [c_void_p]),
     "tb_checkpoint_load": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "tb_plan_get_variant": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
+    "tb_plan_set_gemm_path": (c_int, [c_void_p, c_int]),
+    "tb_plan_get_gemm_path": (c_int, [c_void_p, POINTER(c_int)]),
     "tb_plan_tune": (c_int, [c_void_p, c_double, c_int, POINTER(c_int), POINTER(c_int)]),
     "tb_tau_layout_query": (c_int, [c_int, c_double, c_double, c_int, POINTER(c_int)]),
     "tb_transform_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),

@@ -374,6 +374,16 @@ class Plan:
     def set_variant(self, tau_parts: int = 0, xrows: int = 0) -> None:
         check(lib.tb_plan_set_variant(self.ptr, int(tau_parts), int(xrows)), self.ctx)
 
+    def set_gemm_path(self, tensor_cores: bool) -> None:
+        """Mixed precision: FP32 transform GEMMs on the tcgen05 tensor cores
+        (True, the default) or on the SIMT FP32 kernel (False)."""
+        check(lib.tb_plan_set_gemm_path(self.ptr, 1 if tensor_cores else 0), self.ctx)
+
+    def gemm_path(self) -> bool:
+        v = c_int()
+        check(lib.tb_plan_get_gemm_path(self.ptr, byref(v)), self.ctx)
+        return bool(v.value)
+
     def tune(self, dt: float, trial_steps: int = 4):
         """Time every feasible kernel-shape combination on trial steps from the
         current state (restored afterwards) and keep the fastest."""

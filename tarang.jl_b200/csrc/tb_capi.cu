@@ -206,6 +206,17 @@ TauArgs tau_args(tb_plan* P, int sy, FactorSet* f, const double2* rhsP) {
   return a;
 }
 
+void drop_graph(tb_plan* P);
+
+// Destroys both cached step graphs (the single-step one and the multi-step
+// one); the next launch recaptures.  A graph still executing is released by
+// CUDA when it completes.
+void drop_step_graphs(tb_plan* P) {
+  drop_graph(P);
+  if (P->multi.exec) cudaGraphExecDestroy(P->multi.exec);
+  P->multi = StepGraph{};
+}
+
 FactorSet* get_factors(tb_plan* P, int sy, double alpha, double beta) {
   TauSystem& S = P->sys[sy];
   for (auto& f : S.factors)
@@ -213,12 +224,15 @@ FactorSet* get_factors(tb_plan* P, int sy, double alpha, double beta) {
   // keep at most two sets (SBDF needs the SBDF1 and SBDF2 left-hand sides);
   // a new (alpha, beta) takes over the oldest set's device buffers, so a dt
   // change frees and allocates nothing (cudaFree would wait for the whole
-  // device).  Graphs that read the old set are tied to its dt and are
-  // recaptured before their next launch.
+  // device).  A captured graph bakes in the device pointers of the set it was
+  // captured against, and its cache key (dt, kind, steps) cannot tell that
+  // those buffers now hold another dt's factors, so every cached step graph
+  // is dropped here and the caller recaptures before its next launch.
   std::unique_ptr<FactorSet> fs;
   if (S.factors.size() >= 2) {
     fs = std::move(S.factors.front());
     S.factors.erase(S.factors.begin());
+    drop_step_graphs(P);
   } else {
     fs = std::make_unique<FactorSet>();
   }
@@ -285,7 +299,7 @@ void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2row
       bt.item[nb++] = GemmItem32{Am[w], in, gp(f, w), H, (w & 1) ? P->Ko : P->Ke, pad16k((w & 1) ? P->Ko : P->Ke),
                                  GEMM_PARITY, w & 1};
   }
-  timed(P, "z_backward_gemm", [&] { launch_gemm_f32(bt, nb, ncol, ncol, ncol, N, false, P->st); });
+  timed(P, "z_backward_gemm", [&] { launch_gemm_f32_path(bt, nb, ncol, ncol, ncol, N, false, P->st, P->tc32); });
   XProdArgs32 xa{};
   for (int f = 0; f < 3; ++f) {
     xa.ev[f] = gp(f, 0);
@@ -302,7 +316,12 @@ void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2row
   xa.M = P->M;
   xa.Nz = N;
   xa.k0 = (float)P->k0;
-  timed(P, "x_fft_products", [&] { launch_xprod32(xa, P->st); });
+  timed(P, "x_fft_products", [&] {
+    if (P->xrows == 2)
+      launch_xprod32_b(xa, P->st);  // transforms batched through shared passes
+    else
+      launch_xprod32(xa, P->st);
+  });
   GemmBatch32 bf{};
   nb = 0;
   for (int f = 0; f < 3; ++f) {
@@ -314,7 +333,7 @@ void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2row
       bf.item[nb++] = GemmItem32{c2rows ? P->sfO32.as<float>() : P->fO32.as<float>(), in, out, P->Ko, H, pad16k(H),
                                  GEMM_MIRROR, 1};
   }
-  timed(P, "z_forward_gemm", [&] { launch_gemm_f32(bf, nb, ncol, ncol, ncol, N, true, P->st); });
+  timed(P, "z_forward_gemm", [&] { launch_gemm_f32_path(bf, nb, ncol, ncol, ncol, N, true, P->st, P->tc32); });
 }
 
 void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
@@ -355,7 +374,12 @@ void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
   xa.M = P->M;
   xa.Nz = N;
   xa.k0 = P->k0;
-  timed(P, "x_fft_products", [&] { launch_xprod(xa, P->st); });
+  timed(P, "x_fft_products", [&] {
+    if (P->xrows == 2)
+      launch_xprod_b(xa, P->st);  // transforms batched through shared passes
+    else
+      launch_xprod(xa, P->st);
+  });
   GemmBatch bf{};
   nb = 0;
   for (int f = 0; f < 3; ++f) {
@@ -651,17 +675,27 @@ void tb::plan_launch_steps(tb_plan* P, double dt, int nsteps, cudaStream_t s, in
   }
 }
 
+// The batched 2D x-products kernel fits shared memory (F64 or the FP32 form of
+// a mixed plan); single-instance FP32 plans only (the FP32 kernel has no
+// stacked-instance form).
+static bool xprod2d_batched_fits(const tb_plan* P) {
+  if (P->mixed) return P->B <= 1 && xprod32_b_fits(P->M, (int)(P->ptwM32.bytes / sizeof(float2)));
+  return xprod_b_fits(P->M, (int)(P->ptwM.bytes / sizeof(double2)));
+}
+
 bool tb::plan_tau_parts_ok(const tb_plan* P, int parts) {
-  if (parts != 1 && parts != kTauParts) return false;
-  for (int sy = 0; sy < P->nsys; ++sy)
+  if (parts != 1 && parts != kTauParts && parts != kTauParts8) return false;
+  for (int sy = 0; sy < P->nsys; ++sy) {
     if (tau_solve_smem_bytes(P->sys[sy].npad, parts) > 227 * 1024) return false;
+    if (P->sys[sy].npad / kBwdWin < parts) return false;  // every partition at least one window
+  }
   return true;
 }
 
 void tb::plan_set_variant(tb_plan* P, int tau_parts, int xrows) {
   bool changed = false;
   if (tau_parts > 0) {
-    TB_REQUIRE(plan_tau_parts_ok(P, tau_parts), TB_ENOTSUPPORTED, "tau solve partitions must be 1 or 4 and fit");
+    TB_REQUIRE(plan_tau_parts_ok(P, tau_parts), TB_ENOTSUPPORTED, "tau solve partitions must be 1, 4 or 8 and fit");
     for (int sy = 0; sy < P->nsys; ++sy) {
       TauSystem& S = P->sys[sy];
       if (S.tau_parts == tau_parts) continue;
@@ -674,16 +708,16 @@ void tb::plan_set_variant(tb_plan* P, int tau_parts, int xrows) {
     }
   }
   if (xrows > 0 && xrows != P->xrows) {
-    TB_REQUIRE(P->ndim == 3 && rbc3d_xrows_ok(P, xrows), TB_ENOTSUPPORTED, "x-pass rows must be 1, 2 or 4 and fit");
+    if (P->ndim == 3)
+      TB_REQUIRE(rbc3d_xrows_ok(P, xrows), TB_ENOTSUPPORTED, "x-pass rows must be 1, 2 or 4 and fit");
+    else
+      TB_REQUIRE(xrows == 1 || (xrows == 2 && xprod2d_batched_fits(P)), TB_ENOTSUPPORTED,
+                 "2D x-products form must be 1 (per field) or 2 (batched) and fit");
     TB_CUDA_TRY(cudaStreamSynchronize(P->st));
     P->xrows = xrows;
     changed = true;
   }
-  if (changed) {
-    drop_graph(P);
-    if (P->multi.exec) cudaGraphExecDestroy(P->multi.exec);
-    P->multi = StepGraph{};
-  }
+  if (changed) drop_step_graphs(P);
 }
 
 void tb::plan_prepare(tb_plan* P, double dt, int graph_steps) {
@@ -1007,6 +1041,7 @@ void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, i
     TB_CUDA_TRY(cudaEventCreate(&P->ev1));
     TB_CUDA_TRY(set_transform_smem_limits(227 * 1024));
     TB_CUDA_TRY(set_tau_smem_limits(227 * 1024));
+    TB_CUDA_TRY(set_tc32_smem_limits());
     // transforms
     ChebMats cm = build_cheb_mats(P->Nz, desc->Lz);
     const int N = P->Nz;
@@ -1161,10 +1196,12 @@ tb_status tb_plan_destroy(tb_plan* plan) {
 
 tb_status tb_set_state(tb_plan* P, int field, const void* data, int where) {
   if (!P || !data) return TB_EINVAL;
+  const bool keep = (where & TB_KEEP_HISTORY) != 0;
+  where &= ~TB_KEEP_HISTORY;
   if (P->ndim == 3)
     return guard(P->ctx, [&] {
       state3d_io(P, field, const_cast<void*>(data), where, true);
-      P->ms_history = 0;
+      if (!keep) P->ms_history = 0;
     });
   return guard(P->ctx, [&] {
     TB_REQUIRE(field >= TB_FIELD_B && field <= TB_FIELD_TAU, TB_EINVAL, "bad field selector");
@@ -1173,7 +1210,7 @@ tb_status tb_set_state(tb_plan* P, int field, const void* data, int where) {
     TB_CUDA_TRY(cudaMemcpyAsync(dst, data, bytes, where == TB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                 P->st));
     TB_CUDA_TRY(cudaStreamSynchronize(P->st));
-    P->ms_history = 0;  // a new state restarts multistep history
+    if (!keep) P->ms_history = 0;  // a new state restarts multistep history
   });
 }
 
@@ -1229,9 +1266,11 @@ extern "C" {
 
 tb_status tb_set_states(tb_plan* P, int nfields, const int* fields, const void* const* data, int where) {
   if (!P || nfields < 0 || (nfields > 0 && (!fields || !data))) return TB_EINVAL;
+  const bool keep = (where & TB_KEEP_HISTORY) != 0;
+  where &= ~TB_KEEP_HISTORY;
   return guard(P->ctx, [&] {
     copy_state_fields(P, nfields, fields, const_cast<void* const*>(data), where, true);
-    P->ms_history = 0;  // a new state restarts multistep history
+    if (!keep) P->ms_history = 0;  // a new state restarts multistep history
   });
 }
 
@@ -1252,6 +1291,8 @@ tb_status tb_step(tb_plan* P, double dt, int nsteps) {
     TB_CUDA_TRY(cudaEventSynchronize(P->ev1));
     TB_CUDA_TRY(cudaEventElapsedTime(&P->last_ms, P->ev0, P->ev1));
     TB_CUDA_TRY(cudaGetLastError());
+    if (P->mixed && P->tc32 && tc32_status() == 1)
+      throw Error{TB_ETIMEOUT, "a tensor-core transform GEMM gave up waiting for its MMAs (results not stored)"};
     if (P->profiling) collect_profile(P);
   });
 }
@@ -1368,10 +1409,28 @@ tb_status tb_plan_set_variant(tb_plan* P, int tau_parts, int xrows) {
   });
 }
 
+tb_status tb_plan_set_gemm_path(tb_plan* P, int tensor_cores) {
+  if (!P || (tensor_cores != 0 && tensor_cores != 1)) return TB_EINVAL;
+  return guard(P->ctx, [&] {
+    TB_CUDA_TRY(cudaSetDevice(P->ctx->device));
+    if (P->tc32 != (tensor_cores == 1)) {
+      TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+      P->tc32 = tensor_cores == 1;
+      drop_step_graphs(P);  // the captured steps launch the other kernel
+    }
+  });
+}
+
+tb_status tb_plan_get_gemm_path(const tb_plan* P, int* tensor_cores) {
+  if (!P || !tensor_cores) return TB_EINVAL;
+  *tensor_cores = P->tc32 ? 1 : 0;
+  return TB_OK;
+}
+
 tb_status tb_plan_get_variant(const tb_plan* P, int* tau_parts, int* xrows) {
   if (!P) return TB_EINVAL;
   if (tau_parts) *tau_parts = P->sys[0].tau_parts;
-  if (xrows) *xrows = P->ndim == 3 ? P->xrows : 0;
+  if (xrows) *xrows = P->xrows;
   return TB_OK;
 }
 
@@ -1384,16 +1443,17 @@ tb_status tb_plan_tune(tb_plan* P, double dt, int trial_steps, int* tau_parts, i
     PlanSnapshot snap;
     plan_snapshot(P, &snap);
     std::vector<int> parts_c, rows_c;
-    for (int p : {kTauParts, 1})
+    for (int p : {kTauParts8, kTauParts, 1})
       if (plan_tau_parts_ok(P, p)) parts_c.push_back(p);
     if (P->ndim == 3) {
       for (int r : {1, 2, 4})
         if (rbc3d_xrows_ok(P, r)) rows_c.push_back(r);
     } else {
-      rows_c.push_back(0);
+      rows_c.push_back(1);  // per-field x products
+      if (xprod2d_batched_fits(P)) rows_c.push_back(2);  // batched
     }
     float best = 1e30f;
-    int bp = P->sys[0].tau_parts, br = P->ndim == 3 ? P->xrows : 0;
+    int bp = P->sys[0].tau_parts, br = P->xrows;
     for (int pc : parts_c)
       for (int rc : rows_c) {
         plan_set_variant(P, pc, rc);
@@ -1457,9 +1517,7 @@ tb_status tb_set_wall_values(tb_plan* P, int wall, const double* value, const do
       P->t_dev.alloc(sizeof(double));
       P->bc_tref = P->sim_time;
       P->bc_dynamic = true;
-      drop_graph(P);  // step graphs gain the wall-time update
-      if (P->multi.exec) cudaGraphExecDestroy(P->multi.exec);
-      P->multi = StepGraph{};
+      drop_step_graphs(P);  // step graphs gain the wall-time update
     }
     // re-reference both walls to the current time, then replace this wall
     const double el = P->sim_time - P->bc_tref;

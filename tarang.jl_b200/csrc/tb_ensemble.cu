@@ -340,7 +340,7 @@ tb_status tb_ensemble_tune(tb_ensemble* E, const double* dt, int trial_steps, in
       if (fz)
         for (auto& G : E->groups) shaped.push_back(G.plan.get());
       std::vector<int> cand_p;
-      for (int pc : {kTauParts, 1}) {
+      for (int pc : {kTauParts8, kTauParts, 1}) {
         bool ok = true;
         for (auto* m : shaped) ok = ok && plan_tau_parts_ok(m, pc);
         if (ok) cand_p.push_back(pc);

@@ -177,6 +177,79 @@ __device__ C* fft(C* a, C* b, const FftPlan& fp, const C* __restrict__ pt, int s
   return in;
 }
 
+// One Stockham pass over NA arrays stored Ms apart (the arrays share the
+// pass's barrier); pass<R, SW> arithmetic for each array.
+template <int R, bool SW, class C>
+__device__ __forceinline__ void pass_multi(const C* __restrict__ in, C* __restrict__ out, int NA, int Ms, int n,
+                                           int Ns, const C* __restrict__ pt, int sign) {
+  const int nR = n / R, total = NA * nR;
+  for (int item = threadIdx.x; item < total; item += blockDim.x) {
+    const int arr = item / nR, idx = item - arr * nR;
+    const C* ia = in + (size_t)arr * Ms;
+    C* oa = out + (size_t)arr * Ms;
+    const int j = idx % Ns, k = idx / Ns;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = ia[fidx<SW>(idx + r * nR)];
+    if (Ns > 1) {
+      C w1 = pt[j];
+      if (sign > 0) w1.y = -w1.y;
+      if constexpr (R == 8) {
+        const C w2 = mul(w1, w1), w4 = mul(w2, w2), w3 = mul(w1, w2);
+        v[1] = mul(v[1], w1);
+        v[2] = mul(v[2], w2);
+        v[3] = mul(v[3], w3);
+        v[4] = mul(v[4], w4);
+        v[5] = mul(v[5], mul(w1, w4));
+        v[6] = mul(v[6], mul(w2, w4));
+        v[7] = mul(v[7], mul(w3, w4));
+      } else if constexpr (R == 4) {
+        const C w2 = mul(w1, w1);
+        v[1] = mul(v[1], w1);
+        v[2] = mul(v[2], w2);
+        v[3] = mul(v[3], mul(w1, w2));
+      } else if constexpr (R == 3) {
+        v[1] = mul(v[1], w1);
+        v[2] = mul(v[2], mul(w1, w1));
+      } else {
+        v[1] = mul(v[1], w1);
+      }
+    }
+    dft_small<R>(v, sign);
+    const int ob = k * Ns * R + j;
+#pragma unroll
+    for (int r = 0; r < R; ++r) oa[fidx<SW>(ob + r * Ns)] = v[r];
+  }
+}
+
+// NA whole-CTA FFTs of length fp.n at a + arr Ms, ping-ponging with b; returns
+// the block holding the results.
+template <bool SW, class C>
+__device__ C* fft_multi(C* a, C* b, int NA, int Ms, const FftPlan& fp, const C* __restrict__ pt, int sign) {
+  const int n = fp.n;
+  int Ns = 1;
+  C* in = a;
+  C* out = b;
+  for (int s = 0; s < fp.nstages; ++s) {
+    const int R = fp.radix[s];
+    if (R == 8)
+      pass_multi<8, SW>(in, out, NA, Ms, n, Ns, pt, sign);
+    else if (R == 4)
+      pass_multi<4, SW>(in, out, NA, Ms, n, Ns, pt, sign);
+    else if (R == 2)
+      pass_multi<2, SW>(in, out, NA, Ms, n, Ns, pt, sign);
+    else
+      pass_multi<3, SW>(in, out, NA, Ms, n, Ns, pt, sign);
+    __syncthreads();
+    C* t = in;
+    in = out;
+    out = t;
+    pt += Ns;
+    Ns *= R;
+  }
+  return in;
+}
+
 // Swizzle keyed to the element size: the low bits of an index are XORed with
 // the next ones over a group of 128 bytes (8 double2 or 16 float2), so that the
 // stride-R stores of a pass and the unit-stride loads both spread over all

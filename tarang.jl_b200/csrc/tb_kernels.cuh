@@ -33,6 +33,21 @@ struct GemmBatch32 {
 };
 void launch_gemm_f32(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
                      cudaStream_t st);
+// The same GEMMs on the tcgen05 tensor cores (TF32, three products per term;
+// tb_tc32.cu) for items with M <= 128 and K <= 128.
+bool gemm_tc32_supported(const GemmBatch32& bt, int nbatch);
+void launch_gemm_tc32(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
+                      cudaStream_t st);
+cudaError_t set_tc32_smem_limits();
+int tc32_status();  // 1 once a tensor-core GEMM's bounded wait gave up, -1 if unreadable
+// tensor cores when asked for and the shapes fit, else the SIMT kernel
+inline void launch_gemm_f32_path(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows,
+                                 bool out_f64, cudaStream_t st, bool tensor_cores) {
+  if (tensor_cores && gemm_tc32_supported(bt, nbatch))
+    launch_gemm_tc32(bt, nbatch, ncol, ldb, ldc, Nrows, out_f64, st);
+  else
+    launch_gemm_f32(bt, nbatch, ncol, ldb, ldc, Nrows, out_f64, st);
+}
 void launch_round_f32(const double2* in, float2* out, long long n, cudaStream_t st);
 struct XProdArgs32 {
   const float2* ev[3];
@@ -47,6 +62,8 @@ struct XProdArgs32 {
   float k0;
 };
 void launch_xprod32(const XProdArgs32& a, cudaStream_t st);
+void launch_xprod32_b(const XProdArgs32& a, cudaStream_t st);  // transforms batched (as launch_xprod_b)
+bool xprod32_b_fits(int M, int nptw);
 size_t xprod32_smem_bytes(int M, int nptw);
 cudaError_t set_mixed_smem_limits(int bytes);
 
@@ -68,6 +85,10 @@ struct XProdArgs {
 };
 void launch_xprod(const XProdArgs& a, cudaStream_t st);
 size_t xprod_smem_bytes(int M, int Nk, int nptw);
+// The same products with the inverse and forward transforms batched through
+// shared passes (two 4-array blocks of shared memory).
+void launch_xprod_b(const XProdArgs& a, cudaStream_t st);
+bool xprod_b_fits(int M, int nptw);
 // Raise the dynamic shared-memory limit of the transform kernels (once per plan).
 cudaError_t set_transform_smem_limits(int bytes);
 // Scratch (doubles) the factorisation needs for nmax band rows and Nk modes.
@@ -103,13 +124,29 @@ constexpr int kBwdRec = kBwdG + 4;
 // per-row backward responses H of the partitioned solve: 12 entries, store code, pad
 constexpr int kHRec = kTauKL + kTauKU + 2;
 // Register windows of the solve sweeps.  The solve splits the band rows into
-// kTauParts partitions (one warp each), each a whole number of backward
-// windows, so rows are padded with identity rows to a multiple of
-// kTauParts * kBwdWin (kTauRowPad).
+// partitions (one warp each), each a whole number of backward windows; rows
+// are padded with identity rows to a multiple of kTauParts * kBwdWin
+// (kTauRowPad), so kTauParts partitions are equal.  kTauParts8 partitions
+// take the same rows, as evenly as whole windows go (tau_part_row0).
 constexpr int kFwdWin = kTauKL + 2;
 constexpr int kBwdWin = kTauKL + kTauKU;
 constexpr int kTauParts = 4;
+constexpr int kTauParts8 = 8;
 constexpr int kTauRowPad = kTauParts * kBwdWin;
+// First band row of partition k (0 <= k <= P) of a P-partition solve over
+// np rows (np a multiple of kBwdWin): windows spread as evenly as they go.
+// With two partitions per warp (ppw = 2, np a multiple of 2 kBwdWin) the two
+// partitions of a warp get equal row counts, so the warp's halves sweep in
+// step: warp w takes pairs of windows spread as evenly as they go.
+__host__ __device__ inline int tau_part_row0(int np, int P, int k, int ppw = 1) {
+  if (ppw == 1) return kBwdWin * (int)(((long long)k * (np / kBwdWin)) / P);
+  const int nw = P / 2, pairs = np / (2 * kBwdWin);
+  const int w = k / 2, h = k % 2;
+  const int b0 = (int)(((long long)w * pairs) / nw), b1 = (int)(((long long)(w + 1) * pairs) / nw);
+  return 2 * kBwdWin * b0 + h * kBwdWin * (b1 - b0);
+}
+// Partitions per warp of the 8-partition solve (two: each half-warp sweeps one).
+constexpr int kTau8PerWarp = 2;
 struct ClassDev {
   int n, nb, kl, ku;
   const short* row_eq;
@@ -170,7 +207,8 @@ struct TauArgs {
   double bc_toff;
   int* err_mode;       // first singular mode, or -1
 };
-// parts: kTauParts (partitioned solve, needs a.PP) or 1 (one warp per group).
+// parts: kTauParts or kTauParts8 (partitioned solve, needs a.PP) or 1 (one
+// warp per group).
 // launch_tau_factor factors modes a.mode0 .. a.mode0 + a.Nkm - 1; the
 // partition responses (launch_tau_transfer) are then computed for all modes.
 void launch_tau_factor(const TauArgs& a, int parts, cudaStream_t st);

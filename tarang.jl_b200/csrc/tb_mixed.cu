@@ -272,6 +272,101 @@ __global__ void __launch_bounds__(256, 2) k_xprod32(XProdArgs32 a) {
   }
 }
 
+// k_xprod32 with the transforms batched (as k_xprod_b): the velocity and the
+// three gradient spectra from one read of the inputs, one set of inverse
+// passes for the four, the three products at once, one set of forward passes
+// for the two product spectra.
+template <int NT>
+__global__ void __launch_bounds__(NT, NT == 256 ? 2 : 1) k_xprod32_b(XProdArgs32 a) {
+  extern __shared__ float2 sm32b[];
+  const int M = a.M, N = a.Nx, Nk = a.Nk;
+  const int Ms = (M + 7) & ~7;
+  float2* A = sm32b;
+  float2* Bk = sm32b + 4 * Ms;
+  float2* tw = sm32b + 8 * Ms;
+  const int hN = N / 2;
+  for (int t = threadIdx.x; t < a.nptw; t += blockDim.x) tw[t] = a.ptw[t];
+  const int z = blockIdx.x;
+  const int zm = a.Nz - 1 - z;
+  const bool lower = z <= zm;
+  const size_t rr = (size_t)(lower ? z : zm) * Nk;
+  auto hbin = [&](float2 v, int q) -> float2 {
+    if (q == 0) return make_float2(v.x, 0.f);
+    if (q == hN) return make_float2(0.5f * v.x, 0.f);
+    return v;
+  };
+  auto put2 = [&](float2* dst, int q, float2 P, float2 Q) {
+    dst[F::fidx<true>(q)] = make_float2(P.x - Q.y, P.y + Q.x);
+    if (q > 0) dst[F::fidx<true>(M - q)] = make_float2(P.x + Q.y, -P.y + Q.x);
+  };
+  for (int q = threadIdx.x; q <= hN; q += blockDim.x) {
+    float2 g[3], d[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const float2 e = a.ev[f][rr + q], o = a.ov[f][rr + q];
+      const float2 ed = a.ed[f][rr + q], od = a.od[f][rr + q];
+      g[f] = lower ? make_float2(e.x + o.x, e.y + o.y) : make_float2(e.x - o.x, e.y - o.y);
+      d[f] = lower ? make_float2(ed.x + od.x, ed.y + od.y) : make_float2(od.x - ed.x, od.y - ed.y);
+    }
+    put2(A, q, hbin(g[1], q), hbin(g[2], q));
+    const float kk = a.k0 * q;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      float2 Ax = make_float2(0.f, 0.f);
+      if (q > 0 && q < hN) Ax = make_float2(-kk * g[f].y, kk * g[f].x);
+      put2(A + (size_t)(1 + f) * Ms, q, Ax, hbin(d[f], q));
+    }
+  }
+  for (int k = hN + 1 + threadIdx.x; k < M - hN; k += blockDim.x)
+#pragma unroll
+    for (int arr = 0; arr < 4; ++arr) A[(size_t)arr * Ms + F::fidx<true>(k)] = make_float2(0.f, 0.f);
+  __syncthreads();
+  float2* Rb = F::fft_multi<true>(A, Bk, 4, Ms, a.fp, tw, +1);
+  float2* Fb = (Rb == A) ? Bk : A;
+  for (int p = threadIdx.x; p < M; p += blockDim.x) {
+    const int ps = F::fidx<true>(p);
+    const float2 u = Rb[ps];
+    float pr[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const float2 gg = Rb[(size_t)(1 + f) * Ms + ps];
+      pr[f] = -(u.x * gg.x + u.y * gg.y);
+    }
+    Fb[ps] = make_float2(pr[0], pr[1]);
+    Fb[(size_t)Ms + ps] = make_float2(pr[2], 0.f);
+  }
+  __syncthreads();
+  float2* Cb = F::fft_multi<true>(Fb, Rb, 2, Ms, a.fp, tw, -1);
+  const float2* C1 = Cb;
+  const float2* C2 = Cb + Ms;
+  const float sc = 1.0f / ((float)M * (float)N);
+  const size_t ro = (size_t)z * Nk;
+  for (int k = threadIdx.x; k < Nk; k += blockDim.x) {
+    const float2 c = C1[F::fidx<true>(k)];
+    const float2 cm = C1[F::fidx<true>((M - k) % M)];
+    const float2 sb = make_float2(0.5f * (c.x + cm.x), 0.5f * (c.y - cm.y));
+    const float2 su = make_float2(0.5f * (c.y + cm.y), -0.5f * (c.x - cm.x));
+    const float2 c2 = C2[F::fidx<true>(k)];
+    float2 ob, ou, oz;
+    if (k == 0) {
+      ob = make_float2(sb.x * sc, 0.f);
+      ou = make_float2(su.x * sc, 0.f);
+      oz = make_float2(c2.x * sc, 0.f);
+    } else if (k == hN) {
+      ob = make_float2(2.f * sb.x * sc, 0.f);
+      ou = make_float2(2.f * su.x * sc, 0.f);
+      oz = make_float2(2.f * c2.x * sc, 0.f);
+    } else {
+      ob = make_float2(sb.x * sc, sb.y * sc);
+      ou = make_float2(su.x * sc, su.y * sc);
+      oz = make_float2(c2.x * sc, c2.y * sc);
+    }
+    a.out[0][ro + k] = ob;
+    a.out[1][ro + k] = ou;
+    a.out[2][ro + k] = oz;
+  }
+}
+
 }  // namespace
 
 void launch_round_f32(const double2* in, float2* out, long long n, cudaStream_t st) {
@@ -297,11 +392,30 @@ size_t xprod32_smem_bytes(int M, int nptw) {
 }
 
 cudaError_t set_mixed_smem_limits(int bytes) {
-  return cudaFuncSetAttribute(k_xprod32, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e = cudaFuncSetAttribute(k_xprod32, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_xprod32_b<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_xprod32_b<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 void launch_xprod32(const XProdArgs32& a, cudaStream_t st) {
   k_xprod32<<<a.Nz, 256, xprod32_smem_bytes(a.M, a.nptw), st>>>(a);
+}
+
+size_t xprod32_b_smem_bytes(int M, int nptw) {
+  const size_t Ms = (size_t)((M + 7) & ~7);
+  return (8 * Ms + (size_t)nptw) * sizeof(float2);
+}
+
+bool xprod32_b_fits(int M, int nptw) { return xprod32_b_smem_bytes(M, nptw) <= 227 * 1024; }
+
+void launch_xprod32_b(const XProdArgs32& a, cudaStream_t st) {
+  const size_t smem = xprod32_b_smem_bytes(a.M, a.nptw);
+  if (2 * smem <= 227 * 1024)
+    k_xprod32_b<256><<<a.Nz, 256, smem, st>>>(a);
+  else
+    k_xprod32_b<512><<<a.Nz, 512, smem, st>>>(a);
 }
 
 }  // namespace tb

@@ -287,8 +287,9 @@ __global__ void __launch_bounds__(32 * kFactorWarps) k_tau_factor(TauArgs a) {
 // NL..31 mirror lanes 0..NL-1 (same arithmetic, so the unrolled sweeps stay
 // branch free) and only the owner lanes store.
 //
-// The npad band rows are split into P partitions of Lp = npad/P rows, warp w
-// owning rows [w Lp, (w+1) Lp).  Both triangular sweeps are linear
+// The npad band rows are split into P partitions of whole backward windows
+// (tau_part_row0: equal for P = 4, as even as windows go for P = 8), warp w
+// owning partition w.  Both triangular sweeps are linear
 // recurrences whose state crossing a partition boundary is small: the 4
 // pending entries of the forward window and the 12 latest unknowns of the
 // backward window.  Every warp sweeps its own rows from a guessed boundary
@@ -302,17 +303,20 @@ __global__ void __launch_bounds__(32 * kFactorWarps) k_tau_factor(TauArgs a) {
 //       response G (held in the backward record, applied when y is read);
 //   B1  backward sweep of every partition from a zero window (the last warp
 //       stores X; the others keep their unknowns in shared memory);
-//   B2  warp w < P-1 composes its true incoming window with the 12x12
-//       transfer matrices Psi of the partitions below it;
+//   B2  the true incoming windows are carried up from the last partition,
+//       T_{P-2} = Xhat_{P-1}, T_{k-1} = Xhat_k + Psi_k T_k (warp k applies
+//       its 12x12 transfer matrix Psi_k, one barrier per partition);
 //   B3  warp w < P-1 adds the 12-vector response H of each of its unknowns
-//       (one streamed pass, no recurrence) and stores X.
-// Each sequential chain is 2 Lp rows long.  Factor records stream through a
-// per-warp shared-memory ring (cp.async, kPartStages stages of kPartRows
-// rows); each lane pulls its records of a stage into registers with 16-byte
-// loads before the stage's arithmetic.
+//       (one streamed pass, no recurrence) and stores X; the last warp's
+//       unknowns are final after B1 and are stored there.
+// Each sequential chain is about 2 npad/P rows long.  Factor records stream
+// through a per-warp shared-memory ring (cp.async, ring_doubles<P>() doubles
+// split into as many stages of kPartRows rows as each phase's records fill);
+// each lane pulls its records of a stage into registers with 16-byte loads
+// before the stage's arithmetic.
 // ---------------------------------------------------------------------------
 constexpr int kPartRows = 6;    // rows per ring stage (the forward window)
-constexpr int kPartStages = 4;  // ring depth
+constexpr int kPartStages = 4;  // ring depth in stages of the largest record (1 and 4 partitions)
 // exchange doubles per (warp, lane): D(4) Z(4) Xhat(12), padded to 21 so that
 // the 16 lanes of a warp read distinct banks
 constexpr int kXch = 21;
@@ -340,6 +344,29 @@ __host__ __device__ constexpr size_t part_stage_doubles() {
   constexpr size_t H = kPartRows * (2 * MP * kHRec);
   return F > B ? (F > H ? F : H) : (B > H ? B : H);
 }
+// Doubles of one warp's ring: kPartStages of the largest stage, two with 8
+// partitions (eight warps' rings and the y store share one SM's 227 KB).
+template <int P>
+__host__ __device__ constexpr size_t ring_doubles() {
+  return (P > kTauParts ? 2 : kPartStages) * part_stage_doubles<P>();
+}
+// Ring stages of each phase: the ring split into stages of that phase's
+// records.  With 1 and 4 partitions this is the fixed depth kPartStages for
+// the sweeps and six H stages; with 8 the forward records (smaller than the
+// backward ones) get three stages in the ring of two backward stages.
+template <int P>
+__host__ __device__ constexpr int fwd_stages() {
+  constexpr size_t F = kPartRows * (2 * kSolveModes * kFwdRec + 2 * 2 * kSolveModes);
+  return P > kTauParts ? (int)(ring_doubles<P>() / F) : kPartStages;
+}
+template <int P>
+__host__ __device__ constexpr int bwd_stages() {
+  return P > kTauParts ? 2 : kPartStages;
+}
+template <int P>
+__host__ __device__ constexpr int h_stages() {
+  return P > kTauParts ? (int)(ring_doubles<P>() / (kPartRows * 2 * kSolveModes * kHRec)) : 6;
+}
 
 // X (the state planes) and the tau rows are one allocation, so a 32-bit
 // element offset from X addresses both; code = 2 * offset + (1 if the unknown is i
@@ -352,8 +379,8 @@ __device__ __forceinline__ void store_unknown(double* Xd, int code, int m, int p
   }
 }
 
-template <int KL, int KU, int P>
-__global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
+template <int KL, int KU, int P, int PPW>
+__global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   static_assert(KL + 2 == kFwdWin && KL + KU == kBwdWin, "window sizes follow the band shape");
   static_assert(kFwdWin == kPartRows && kBwdWin == 2 * kPartRows, "one forward window per stage, two stages per backward block");
   static_assert(kFwdRec == KL + NBMAX + 2 && kFwdRot == kFwdRec - 1 && kFwdRec % 2 == 0,
@@ -368,58 +395,64 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   constexpr int HREC = 2 * MP * kHRec;    // doubles per H row
   constexpr int RREC = 2 * MP;            // double2 rhs entries per row (class, mode)
   constexpr int FV = kFwdRec / 2, BV = kBwdRec / 2, HV = kHRec / 2;  // 16-byte words per record
-  constexpr int R = kPartRows, NS = kPartStages;
-  constexpr int NL = 4 * MP;  // distinct lanes
+  constexpr int R = kPartRows;
+  constexpr int NL = 4 * MP;  // distinct lanes of a partition
+  constexpr int TPL = 32 / PPW;  // threads per partition (a warp, or a half-warp)
   constexpr int BSUB = 3;     // backward rows whose records are held in registers at once
-  constexpr int STAGE = (int)part_stage_doubles<P>();
-  static_assert(NL <= 32 && 32 % NL == 0, "lane layout");
+  constexpr int RING = (int)ring_doubles<P>();  // doubles of one partition's ring
+  constexpr int NSF = fwd_stages<P>(), NSB = bwd_stages<P>(), NSH = h_stages<P>();
+  constexpr int FST = R * (FREC + 2 * RREC);                    // forward stage: records + rhs
+  constexpr int BST = R * (BREC + (P == 1 ? NL : 0));           // backward stage (+ y with one partition)
+  static_assert(NSF >= 2 && NSF * FST <= RING && NSB >= 2 && NSB * BST <= RING, "ring stages");
+  static_assert(NL <= TPL && TPL % NL == 0 && P % PPW == 0 && (PPW == 1 || PPW == 2), "lane layout");
   static_assert(R % BSUB == 0, "backward sub-blocks");
   extern __shared__ __align__(16) double smem[];
   const int np = a.npad;
   const int Nk = a.Nk;
   const int g = blockIdx.x;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int Lp = np / P, row0 = warp * Lp;
-  const int nst = Lp / R;  // ring stages of this warp's rows
+  // partition pid of this thread: the warp's own (PPW = 1, lanes NL.. mirror
+  // lanes 0..NL-1), or one per half-warp (PPW = 2); tl = lane within it
+  const int pid = warp * PPW + lane / TPL, tl = lane % TPL;
+  const int row0 = tau_part_row0(np, P, pid, PPW), Lp = tau_part_row0(np, P, pid + 1, PPW) - row0;
+  const int nst = Lp / R;  // ring stages of this partition's rows (even: Lp is whole backward windows)
   const int ln = lane % NL;
   const int c = ln / (2 * MP), part = (ln / MP) & 1, mm = ln % MP;
   const int slot = c * MP + mm;
-  const bool owner = lane < NL;
+  const bool owner = tl < NL;
   const int m = g * MP + mm;
   const bool live = owner && m < Nk;
-  double* ring = smem + (size_t)warp * NS * STAGE;
-  // [row][ln]: y, then (rows of warps < P-1) particular x.  With one partition
+  double* ring = smem + (size_t)pid * RING;
+  // [row][ln]: y, then (rows of partitions < P-1) particular x.  With one partition
   // the group's y column lives in global scratch (written by F1 and read back
   // by B1 of the same CTA while it is still in L2), which halves the shared
   // memory of a CTA and doubles the resident groups per SM.
-  double* ysave = (P == 1) ? a.ysave + (size_t)g * np * NL : smem + (size_t)P * NS * STAGE;
-  double* xch = smem + (size_t)P * NS * STAGE + (P == 1 ? 0 : (size_t)np * NL);  // [warp][ln][kXch]
+  double* ysave = (P == 1) ? a.ysave + (size_t)g * np * NL : smem + (size_t)P * RING;
+  double* xch = smem + (size_t)P * RING + (P == 1 ? 0 : (size_t)np * NL);  // [partition][ln][kXch]
   int* rofs = reinterpret_cast<int*>(xch + (size_t)P * NL * kXch);
   // [row][class] right-hand-side code: 2 * element offset + (1 for a u_x momentum
   // row, scaled by -i on load), -1 for none
-  for (int q = threadIdx.x; q < np / 2; q += 32 * P) cp_async16(rofs + 4 * q, a.rhs_off + 4 * q, true);
+  for (int q = threadIdx.x; q < np / 2; q += blockDim.x) cp_async16(rofs + 4 * q, a.rhs_off + 4 * q, true);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
   const double* FRg = a.cls[0].FR + (size_t)g * np * FREC;
   const double* BRg = a.cls[0].BR + (size_t)g * np * BREC;
   const double* HRg = a.HR + (size_t)g * np * HREC;
-  const double* trg = a.PP + (((size_t)g * P * 2 + c) * MP + mm) * kTransfer;  // partition k: + k 2 MP kTransfer
-  constexpr size_t TRK = (size_t)2 * MP * kTransfer;
   double* Xd = reinterpret_cast<double*>(a.X);
 
-  // ---- F1: forward sweep over this warp's rows: y = L^-1 P r, boundary rows accumulate z ----
+  // ---- F1: forward sweep over this partition's rows: y = L^-1 P r, boundary rows accumulate z ----
   double y[kFwdWin];
   double z[NBMAX];
-  auto issue_fwd = [&](int s) {  // local stage s: rows row0 + s R ..; stage nst is the first of the next warp
+  auto issue_fwd = [&](int s) {  // local stage s: rows row0 + s R ..; stage nst is the first of the next partition
     const int r0 = row0 + s * R;
     if (s <= nst) {
-      double* dst = ring + (size_t)(s % NS) * STAGE;
+      double* dst = ring + (size_t)(s % NSF) * FST;
       if (r0 < np)
-        for (int q = lane; q < R * FREC / 2; q += 32) cp_async16(dst + 2 * q, FRg + (size_t)r0 * FREC + 2 * q, true);
+        for (int q = tl; q < R * FREC / 2; q += TPL) cp_async16(dst + 2 * q, FRg + (size_t)r0 * FREC + 2 * q, true);
       // right-hand sides (zero-filled past the last row)
       double2* rdst = reinterpret_cast<double2*>(dst + R * FREC);
-      for (int q = lane; q < R * RREC; q += 32) {
+      for (int q = tl; q < R * RREC; q += TPL) {
         const int r = q / RREC, cc = (q / MP) % 2, md = q % MP;
         const int mq = g * MP + md;
         const int code = (r0 + r < np) ? rofs[2 * (r0 + r) + cc] : -1;
@@ -434,16 +467,16 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   auto rhs_at = [&](int s, int u) -> double {
     const int j = row0 + s * R + u;
     if (j >= np) return 0.0;
-    const double* rb = ring + (size_t)(s % NS) * STAGE + R * FREC + (size_t)(u * RREC + slot) * 2;
+    const double* rb = ring + (size_t)(s % NSF) * FST + R * FREC + (size_t)(u * RREC + slot) * 2;
     const int rot = rofs[2 * j + c] & 1;
     const double v = rb[part ^ rot];
     return (rot & part) ? -v : v;
   };
 #pragma unroll
   for (int b = 0; b < NBMAX; ++b)
-    z[b] = (warp == 0 && part == 0 && m < Nk && m % a.Nkm == 0 && b < a.cls[c].nb) ? a.beta * a.cls[c].bc_rhs[b]
-                                                                                   : 0.0;
-  if (a.bcdyn != nullptr && warp == 0 && m < Nk) {
+    z[b] = (pid == 0 && part == 0 && m < Nk && m % a.Nkm == 0 && b < a.cls[c].nb) ? a.beta * a.cls[c].bc_rhs[b]
+                                                                                  : 0.0;
+  if (a.bcdyn != nullptr && pid == 0 && m < Nk) {
     // dynamic wall values of b: boundary row 0 of class c is the parity-c
     // combination of the walls, (top + bottom)/2 (c = 0) or (top - bottom)/2,
     // with both walls at the stage time (value + rate * t)
@@ -454,16 +487,16 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
     const double top = part ? fma(v1t.y, t, v0t.y) : fma(v1t.x, t, v0t.x);
     z[0] = a.beta * 0.5 * (c == 0 ? top + bot : top - bot);
   }
-  for (int s = 0; s < NS - 1; ++s) issue_fwd(s);
+  for (int s = 0; s < NSF - 1; ++s) issue_fwd(s);
   for (int s = 0; s < nst; ++s) {
-    issue_fwd(s + NS - 1);    // refills the slot of stage s-1
-    cp_async_wait<NS - 2>();  // stages s and s+1 are resident
+    issue_fwd(s + NSF - 1);    // refills the slot of stage s-1
+    cp_async_wait<NSF - 2>();  // stages s and s+1 are resident
     __syncwarp();
     if (s == 0) {
 #pragma unroll
       for (int t = 0; t < kFwdWin; ++t) y[t] = rhs_at(0, t);
     }
-    const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NS) * STAGE + (size_t)slot * kFwdRec);
+    const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NSF) * FST + (size_t)slot * kFwdRec);
     double2 rv[kFwdWin][FV];
 #pragma unroll
     for (int u = 0; u < kFwdWin; ++u)
@@ -473,7 +506,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
     // past the last row), -i applied to u_x momentum rows by the record's flag
     double incoming[kFwdWin];
     {
-      const double* rb = ring + (size_t)((s + 1) % NS) * STAGE + R * FREC + (size_t)slot * 2;
+      const double* rb = ring + (size_t)((s + 1) % NSF) * FST + R * FREC + (size_t)slot * 2;
 #pragma unroll
       for (int u = 0; u < kFwdWin; ++u) {
         const int rot = __double2loint(rv[u][FV - 1].y);
@@ -503,29 +536,29 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
     }
     __syncwarp();  // the slot of stage s is refilled next
   }
-  double* myx = xch + ((size_t)warp * NL + ln) * kXch;
-  // exit window minus the raw right-hand side of the next warp's first rows (the
+  double* myx = xch + ((size_t)pid * NL + ln) * kXch;
+  // exit window minus the raw right-hand side of the next partition's first rows (the
   // ring still holds that stage)
 #pragma unroll
   for (int t = 0; t < 4; ++t) myx[t] = y[t] - rhs_at(nst, t);
   cp_async_wait<0>();
   if constexpr (P == 1) __threadfence();  // y stores of all lanes reach L2 before their cp.async reloads
   __syncwarp();
-  // The ring is free: stage the Schur inverse of the group and this warp's
-  // forward transfer data (Phi_k for k < warp, Gz_warp) while the other warps
+  // The ring is free: stage the Schur inverse of the group and this partition's
+  // forward transfer data (Phi_k for k < pid, Gz_pid) while the other partitions
   // finish their sweeps.
   constexpr int TRF = 32;  // Phi (16) + Gz (16) per (partition, record slot)
   // shared-memory stride of a staged (partition, slot) record: 34 doubles, so
   // that the 8 slots a warp reads at once fall in distinct banks
   constexpr int TRS = TRF + 2;
-  static_assert(2 * NBMAX * NBMAX * MP + (P - 1) * 2 * MP * TRS <= NS * STAGE, "Schur inverse and Phi fit the ring");
+  static_assert(2 * NBMAX * NBMAX * MP + (P - 1) * 2 * MP * TRS <= RING, "Schur inverse and Phi fit the ring");
   double* sSI = ring;                         // [class][4][4][mode], 2*16*MP doubles
   double* sTR = ring + 2 * NBMAX * NBMAX * MP;  // [k-1][slot][TRS]
   {
     const double* SIg = a.cls[0].SI + (size_t)g * 2 * NBMAX * NBMAX * MP;
-    for (int q = lane; q < NBMAX * NBMAX * MP; q += 32) cp_async16(sSI + 2 * q, SIg + 2 * q, true);
-    if (P > 1 && warp > 0) {
-      for (int q = lane; q < warp * 2 * MP * (TRF / 2); q += 32) {
+    for (int q = tl; q < NBMAX * NBMAX * MP; q += TPL) cp_async16(sSI + 2 * q, SIg + 2 * q, true);
+    if (P > 1 && pid > 0) {
+      for (int q = tl; q < pid * 2 * MP * (TRF / 2); q += TPL) {
         const int k = 1 + q / (2 * MP * (TRF / 2)), rs = (q / (TRF / 2)) % (2 * MP), h = q % (TRF / 2);
         const double* rec = a.PP + (((size_t)g * P + k) * 2 * MP + rs) * kTransfer;
         const double* src = (h < 8) ? rec + kTrPhi + 2 * h : rec + kTrGz + 2 * (h - 8);
@@ -536,15 +569,15 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   }
 
   // ---- F2: true starting window of this partition, border accumulators ----
-  double d[4] = {0.0, 0.0, 0.0, 0.0};  // starting-window correction (0 for warp 0)
+  double d[4] = {0.0, 0.0, 0.0, 0.0};  // starting-window correction (0 for partition 0)
   if constexpr (P > 1) {
     __syncthreads();
     cp_async_wait<0>();
     __syncwarp();
-    if (warp > 0) {
+    if (pid > 0) {
 #pragma unroll
       for (int t = 0; t < 4; ++t) d[t] = xch[(size_t)ln * kXch + t];  // delta_1 = D_0
-      for (int k = 1; k < warp; ++k) {
+      for (int k = 1; k < pid; ++k) {
         const double* phi = sTR + ((size_t)(k - 1) * 2 * MP + slot) * TRS;
         const double* Dk = xch + ((size_t)k * NL + ln) * kXch;
         double nd[4];
@@ -558,7 +591,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 #pragma unroll
         for (int o = 0; o < 4; ++o) d[o] = nd[o];
       }
-      const double* gz = sTR + ((size_t)(warp - 1) * 2 * MP + slot) * TRS + 16;
+      const double* gz = sTR + ((size_t)(pid - 1) * 2 * MP + slot) * TRS + 16;
 #pragma unroll
       for (int b = 0; b < NBMAX; ++b)
 #pragma unroll
@@ -592,32 +625,32 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   }
   __syncwarp();  // the ring is reused by B1
 
-  // ---- B1: backward sweep over this warp's rows, x = U^-1 (y - B x1), from a zero window ----
+  // ---- B1: backward sweep over this partition's rows, x = U^-1 (y - B x1), from a zero window ----
   // (the particular unknowns replace y in shared memory; B3 completes and stores them)
   double xw[kBwdWin];  // x_j lives in slot j % kBwdWin
 #pragma unroll
   for (int t = 0; t < kBwdWin; ++t) xw[t] = 0.0;
   auto issue_bwd = [&](int s) {  // local stage s from the bottom: rows row0 + Lp - (s+1) R ..
     if (s < nst) {
-      double* dst = ring + (size_t)(s % NS) * STAGE;
+      double* dst = ring + (size_t)(s % NSB) * BST;
       const int lo = row0 + Lp - (s + 1) * R;
-      for (int q = lane; q < R * BREC / 2; q += 32) cp_async16(dst + 2 * q, BRg + (size_t)lo * BREC + 2 * q, true);
+      for (int q = tl; q < R * BREC / 2; q += TPL) cp_async16(dst + 2 * q, BRg + (size_t)lo * BREC + 2 * q, true);
       if constexpr (P == 1)
-        for (int q = lane; q < R * NL / 2; q += 32)
+        for (int q = tl; q < R * NL / 2; q += TPL)
           cp_async16(dst + R * BREC + 2 * q, ysave + (size_t)lo * NL + 2 * q, true);
     }
     cp_async_commit();
   };
-  for (int s = 0; s < NS - 1; ++s) issue_bwd(s);
+  for (int s = 0; s < NSB - 1; ++s) issue_bwd(s);
   for (int s0 = 0; s0 < nst; s0 += 2) {
     const int q0 = row0 + Lp - (s0 + 2) * R;  // block rows q0 .. q0 + kBwdWin - 1, q0 % kBwdWin == 0
 #pragma unroll
     for (int hs = 0; hs < 2; ++hs) {
       const int s = s0 + hs;
-      issue_bwd(s + NS - 1);
-      cp_async_wait<NS - 1>();  // stage s is resident
+      issue_bwd(s + NSB - 1);
+      cp_async_wait<NSB - 1>();  // stage s is resident
       __syncwarp();
-      const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NS) * STAGE + (size_t)slot * kBwdRec);
+      const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NSB) * BST + (size_t)slot * kBwdRec);
 #pragma unroll
       for (int h = 0; h < R / BSUB; ++h) {
         // rows q0 + kBwdWin - 1 - u for u = hs R + h BSUB + w; stage row index R - 1 - (h BSUB + w)
@@ -634,7 +667,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
           double* yx = ysave + (size_t)j * NL + ln;
           double acc0;
           if constexpr (P == 1)
-            acc0 = ring[(size_t)(s % NS) * STAGE + R * BREC + (R - 1 - (h * BSUB + w)) * NL + ln];
+            acc0 = ring[(size_t)(s % NSB) * BST + R * BREC + (R - 1 - (h * BSUB + w)) * NL + ln];
           else
             acc0 = *yx;
           double acc1 = 0.0, acc2 = 0.0;
@@ -655,7 +688,7 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
           const double sacc = fma(-rec(1), xw[(kBwdWin - u) % kBwdWin], acc0 + (acc1 + acc2));
           const double xj = sacc * rec(0);
           xw[(kBwdWin - 1 - u) % kBwdWin] = xj;
-          if constexpr (P == 1)
+          if (P == 1 || pid == P - 1)
             store_unknown(Xd, __double2loint(rec(kBwdCode)), m, part, xj, live);  // final: no correction
           else
             *yx = xj;
@@ -668,96 +701,114 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
   __syncwarp();
 
   // ---- B2: true incoming window T of this partition (zero for the last) ----
-  const bool last = (warp == P - 1);
+  const bool last = (pid == P - 1);
   double T[kBwdWin];
 #pragma unroll
   for (int t = 0; t < kBwdWin; ++t) T[t] = 0.0;
   if constexpr (P > 1) {
-    // stage Psi_k, k = warp+1 .. P-2, in the ring while the other warps finish B1
-    // [k-warp-1][slot][PS]; the stride PS = 146 doubles puts the 8 slots a
-    // warp reads at once in distinct banks
+    // Carry from the bottom: T_{P-2} = Xhat_{P-1} (the last partition's top
+    // window is exact), T_{k-1} = Xhat_k + Psi_k T_k.  Partition k (1 <= k <=
+    // P-2) stages its own Psi_k in its ring while the others finish B1,
+    // [slot][PS] with the stride PS = 146 doubles putting the 8 slots read at
+    // once in distinct banks; at step k it overwrites its published Xhat_k
+    // with T_{k-1}, which partition k-1 reads after the barrier.
     constexpr int PS = kBwdWin * kBwdWin + 2;
-    static_assert((P > 2 ? P - 2 : 0) * 2 * MP * PS <= NS * STAGE, "Psi fits the ring");
+    static_assert(2 * MP * PS <= RING, "Psi fits the ring");
     double* sPsi = ring;
-    const int npsi = (P - 2 - warp) > 0 ? (P - 2 - warp) : 0;
-    for (int q = lane; q < npsi * 2 * MP * 72; q += 32) {
-      const int kk = q / (2 * MP * 72), rs = (q / 72) % (2 * MP), h = q % 72;
-      const double* rec = a.PP + (((size_t)g * P + warp + 1 + kk) * 2 * MP + rs) * kTransfer + kTrPsi;
-      cp_async16(sPsi + ((size_t)kk * 2 * MP + rs) * PS + 2 * h, rec + 2 * h, true);
+    if (pid >= 1 && pid <= P - 2) {
+      for (int q = tl; q < 2 * MP * 72; q += TPL) {
+        const int rs = q / 72, h = q % 72;
+        const double* rec = a.PP + (((size_t)g * P + pid) * 2 * MP + rs) * kTransfer + kTrPsi;
+        cp_async16(sPsi + (size_t)rs * PS + 2 * h, rec + 2 * h, true);
+      }
     }
     cp_async_commit();
     double* myxh = myx + 8;
 #pragma unroll
     for (int t = 0; t < kBwdWin; ++t) myxh[t] = xw[t];
-    __syncthreads();
     cp_async_wait<0>();
-    __syncwarp();
-    if (!last) {
+    __syncthreads();
+    if (pid == P - 2) {
       const double* Xl = xch + ((size_t)(P - 1) * NL + ln) * kXch + 8;
 #pragma unroll
       for (int t = 0; t < kBwdWin; ++t) T[t] = Xl[t];
-      for (int k = P - 2; k > warp; --k) {
-        const double* psi = sPsi + ((size_t)(k - warp - 1) * 2 * MP + slot) * PS;
-        const double* Xk = xch + ((size_t)k * NL + ln) * kXch + 8;
+    }
+    for (int k = P - 2; k >= 1; --k) {
+      if (pid == k) {
+        const double* psi = sPsi + (size_t)slot * PS;
         double nt[kBwdWin];
 #pragma unroll
         for (int o = 0; o < kBwdWin; ++o) {
-          double acc = Xk[o];
+          double acc = xw[o];
 #pragma unroll
           for (int i = 0; i < kBwdWin; ++i) acc = fma(psi[o * kBwdWin + i], T[i], acc);
           nt[o] = acc;
         }
 #pragma unroll
-        for (int o = 0; o < kBwdWin; ++o) T[o] = nt[o];
+        for (int o = 0; o < kBwdWin; ++o) myxh[o] = nt[o];  // lanes ln and ln + NL write the same values
+      }
+      __syncthreads();
+      if (pid == k - 1) {
+        const double* Xk = xch + ((size_t)k * NL + ln) * kXch + 8;
+#pragma unroll
+        for (int t = 0; t < kBwdWin; ++t) T[t] = Xk[t];
       }
     }
     __syncwarp();  // the ring is reused by B3
   }
 
   // ---- B3: x_j = particular + H_j . T over the rows of this partition, stored to X ----
+  // (the last partition stored its unknowns in B1: its threads run the loop
+  // without loads or stores, so the warp-wide syncs see every lane)
   if constexpr (P > 1) {
-    constexpr int NS3 = 6;            // H ring: NS3 slots of R rows
-    constexpr int SLOT3 = R * HREC;
-    static_assert(NS3 * SLOT3 <= NS * STAGE, "H ring fits the warp's ring");
-    constexpr int LG = 32 / NL;  // lane groups: each takes every LG-th row of a stage
-    const int grp = lane / NL;
+    constexpr int SLOT3 = R * HREC;  // H ring: NSH slots of R rows
+    static_assert(NSH >= 2 && NSH * SLOT3 <= RING, "H ring fits the partition's ring");
+    constexpr int LG = TPL / NL;  // lane groups: each takes every LG-th row of a stage
+    const int grp = tl / NL;
+    const int nst3 = last ? 0 : nst;  // stages this partition streams
+    const int nloop = __shfl_sync(0xffffffffu, nst3, 0) > __shfl_sync(0xffffffffu, nst3, 31)
+                          ? __shfl_sync(0xffffffffu, nst3, 0)
+                          : __shfl_sync(0xffffffffu, nst3, 31);  // the warp's trip count
     auto issue_h = [&](int s) {
-      if (s < nst) {
-        double* dst = ring + (size_t)(s % NS3) * SLOT3;
+      if (s < nst3) {
+        double* dst = ring + (size_t)(s % NSH) * SLOT3;
         const int lo = row0 + s * R;
-        for (int q = lane; q < R * HREC / 2; q += 32) cp_async16(dst + 2 * q, HRg + (size_t)lo * HREC + 2 * q, true);
+        for (int q = tl; q < R * HREC / 2; q += TPL) cp_async16(dst + 2 * q, HRg + (size_t)lo * HREC + 2 * q, true);
       }
       cp_async_commit();
     };
-    for (int s = 0; s < NS3 - 1; ++s) issue_h(s);
-    for (int s = 0; s < nst; ++s) {
-      issue_h(s + NS3 - 1);
-      cp_async_wait<NS3 - 1>();
+    for (int s = 0; s < NSH - 1; ++s) issue_h(s);
+    for (int s = 0; s < nloop; ++s) {
+      issue_h(s + NSH - 1);
+      cp_async_wait<NSH - 1>();
       __syncwarp();
-      const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NS3) * SLOT3 + (size_t)slot * kHRec);
-      // no recurrence here: the lane groups take interleaved rows
+      if (s < nst3) {
+        const double2* st =
+            reinterpret_cast<const double2*>(ring + (size_t)(s % NSH) * SLOT3 + (size_t)slot * kHRec);
+        // no recurrence here: the lane groups take interleaved rows
 #pragma unroll
-      for (int q = 0; q < (R + LG - 1) / LG; ++q) {
-        const int u = q * LG + grp;
-        if (u >= R) break;
-        double2 hv[HV];
+        for (int q = 0; q < (R + LG - 1) / LG; ++q) {
+          const int u = q * LG + grp;
+          if (u >= R) break;
+          double2 hv[HV];
 #pragma unroll
-        for (int v = 0; v < HV; ++v) hv[v] = st[u * (HREC / 2) + v];
-        const int j = row0 + s * R + u;
-        double acc0 = ysave[(size_t)j * NL + ln], acc1 = 0.0;
+          for (int v = 0; v < HV; ++v) hv[v] = st[u * (HREC / 2) + v];
+          const int j = row0 + s * R + u;
+          double acc0 = ysave[(size_t)j * NL + ln], acc1 = 0.0;
 #pragma unroll
-        for (int i = 0; i < kBwdWin; i += 2) {
-          acc0 = fma(hv[i / 2].x, T[i], acc0);
-          acc1 = fma(hv[i / 2].y, T[i + 1], acc1);
+          for (int i = 0; i < kBwdWin; i += 2) {
+            acc0 = fma(hv[i / 2].x, T[i], acc0);
+            acc1 = fma(hv[i / 2].y, T[i + 1], acc1);
+          }
+          store_unknown(Xd, __double2loint(hv[HV - 1].x), m, part, acc0 + acc1, m < Nk);
         }
-        store_unknown(Xd, __double2loint(hv[HV - 1].x), m, part, acc0 + acc1, m < Nk);
       }
       __syncwarp();
     }
     cp_async_wait<0>();
   }
   // border unknowns
-  if (warp == 0) {
+  if (pid == 0) {
 #pragma unroll
     for (int b = 0; b < NBMAX; ++b) {
       if (live && b < a.cls[c].nb) store_unknown(Xd, a.cls[c].left_code[b], m, part, x1[b], true);
@@ -768,16 +819,17 @@ __global__ void __launch_bounds__(32 * P) k_tau_solve(TauArgs a) {
 // ---------------------------------------------------------------------------
 // Partition responses of the solve, one thread per (mode, class, partition,
 // unit vector), from the factor records (the arithmetic of the sweeps in
-// k_tau_solve).  Partition k owns rows [k Lp, (k+1) Lp).  For k >= 1
+// k_tau_solve).  Partition k owns rows [r0, r1) = [tau_part_row0(k),
+// tau_part_row0(k + 1)).  For k >= 1
 // (forward, started from unit pending entry i of the window and a zero
 // right-hand side):
 //   G of row j (backward record slots kBwdG..) = y_j,
 //   Phi_k[o][i] = exit pending entry o,  Gz_k[b][i] = border accumulator b.
-// For k <= P-2 (backward from unit window entry i, row (k+1) Lp + i, with zero
+// For k <= P-2 (backward from unit window entry i, row r1 + i, with zero
 // y and border unknowns):
-//   H of row j (H record) = x_j,  Psi_k[o][i] = x of row k Lp + o.
+//   H of row j (H record) = x_j,  Psi_k[o][i] = x of row r0 + o.
 // ---------------------------------------------------------------------------
-template <int KL, int KU, int P>
+template <int KL, int KU, int P, int PPW>
 __global__ void __launch_bounds__(128) k_tau_transfer(TauArgs a) {
   // one thread per (mode, class, partition, unit): forward unit i < 4,
   // backward unit i - 4 < 12
@@ -785,11 +837,11 @@ __global__ void __launch_bounds__(128) k_tau_transfer(TauArgs a) {
   const int c = blockIdx.y & 1, k = blockIdx.y >> 1;
   const int i = blockIdx.z;
   if (m >= a.Nk) return;
-  const int np = a.npad, Lp = np / P;
+  const int np = a.npad;
   const int g = m / kSolveModes, mm = m % kSolveModes;
   // Phi, Gz, Psi exist only for P > 1 (a.PP is null otherwise)
   double* tr = P > 1 ? a.PP + ((((size_t)g * P + k) * 2 + c) * kSolveModes + mm) * kTransfer : nullptr;
-  const int r0 = k * Lp, r1 = (k + 1) * Lp;
+  const int r0 = tau_part_row0(np, P, k, PPW), r1 = tau_part_row0(np, P, k + 1, PPW);
   if (i < 4) {
     if (k < 1) return;
     double y[kFwdWin], z[NBMAX] = {0.0, 0.0, 0.0, 0.0};
@@ -816,18 +868,7 @@ __global__ void __launch_bounds__(128) k_tau_transfer(TauArgs a) {
     return;
   }
   const int ib = i - 4;
-  if (k == P - 1) {
-    // the last partition's unknowns need no correction: zero H, store codes
-    for (int j = r0; j < r1; ++j) {
-      double* hr = a.HR + ((((size_t)g * np + j) * 2 + c) * kSolveModes + mm) * kHRec;
-      hr[ib] = 0.0;
-      if (ib == 0) {
-        hr[kBwdWin] = bwd_record(a.cls[0].BR, np, m, j, c)[kBwdCode];
-        hr[kBwdWin + 1] = 0.0;
-      }
-    }
-    return;
-  }
+  if (k == P - 1) return;  // the last partition's unknowns need no correction (stored by its backward sweep)
   double xw[kBwdWin];
   for (int t = 0; t < kBwdWin; ++t) xw[t] = (t == ib) ? 1.0 : 0.0;
   for (int j = r1 - 1; j >= r0; --j) {
@@ -1031,33 +1072,43 @@ template <int KL, int KU>
 void transfer_impl(const TauArgs& a, int parts, cudaStream_t st) {
   // one partition: the sweeps need no transfer responses (B1 stores x directly)
   const int tgx = (a.Nk + 127) / 128;
-  if (parts == kTauParts) k_tau_transfer<KL, KU, kTauParts><<<dim3(tgx, 2 * kTauParts, 16), 128, 0, st>>>(a);
+  if (parts == kTauParts) k_tau_transfer<KL, KU, kTauParts, 1><<<dim3(tgx, 2 * kTauParts, 16), 128, 0, st>>>(a);
+  if (parts == kTauParts8)
+    k_tau_transfer<KL, KU, kTauParts8, kTau8PerWarp><<<dim3(tgx, 2 * kTauParts8, 16), 128, 0, st>>>(a);
 }
 
 template <int P>
 size_t solve_smem_bytes(int npad) {
   constexpr size_t NL = 4 * kSolveModes;
   const size_t ys = P == 1 ? 0 : (size_t)npad * NL;  // one partition keeps y in global scratch
-  return ((size_t)P * kPartStages * part_stage_doubles<P>() + ys + (size_t)P * NL * kXch) * sizeof(double) +
+  return ((size_t)P * ring_doubles<P>() + ys + (size_t)P * NL * kXch) * sizeof(double) +
          (size_t)npad * 2 * sizeof(int);
 }
 
 template <int KL, int KU>
 void solve_impl(const TauArgs& a, int parts, cudaStream_t st) {
   const int groups = (a.Nk + kSolveModes - 1) / kSolveModes;
-  if (parts == kTauParts)
-    k_tau_solve<KL, KU, kTauParts><<<groups, 32 * kTauParts, solve_smem_bytes<kTauParts>(a.npad), st>>>(a);
+  if (parts == kTauParts8)
+    k_tau_solve<KL, KU, kTauParts8, kTau8PerWarp>
+        <<<groups, 32 * kTauParts8 / kTau8PerWarp, solve_smem_bytes<kTauParts8>(a.npad), st>>>(a);
+  else if (parts == kTauParts)
+    k_tau_solve<KL, KU, kTauParts, 1><<<groups, 32 * kTauParts, solve_smem_bytes<kTauParts>(a.npad), st>>>(a);
   else
-    k_tau_solve<KL, KU, 1><<<groups, 32, solve_smem_bytes<1>(a.npad), st>>>(a);
+    k_tau_solve<KL, KU, 1, 1><<<groups, 32, solve_smem_bytes<1>(a.npad), st>>>(a);
 }
 
 }  // namespace
 
 
 cudaError_t set_tau_smem_limits(int bytes) {
-  cudaError_t e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e =
+      cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU, kTauParts>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU, kTauParts, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           bytes);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU, kTauParts8, kTau8PerWarp>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
   const void* fns[] = {(const void*)k_rk_final<1>,  (const void*)k_rk_final<2>,  (const void*)k_rk_final<3>,
                        (const void*)k_rk_final<4>,  (const void*)k_rk_final<5>,  (const void*)k_rk_final<6>,
@@ -1071,6 +1122,7 @@ cudaError_t set_tau_smem_limits(int bytes) {
 }
 
 size_t tau_solve_smem_bytes(int npad, int parts) {
+  if (parts == kTauParts8) return solve_smem_bytes<kTauParts8>(npad);
   return parts == kTauParts ? solve_smem_bytes<kTauParts>(npad) : solve_smem_bytes<1>(npad);
 }
 

@@ -602,6 +602,182 @@ __global__ void __launch_bounds__(256, 2) k_xprod(XProdArgs a) {
   }
 }
 
+// One Stockham pass over NA arrays of length n stored Ms apart: the
+// (array, butterfly) pairs are spread over the CTA, so the arrays share the
+// pass's barrier.  Same arithmetic as fft_pass_pt for each array.
+template <int R>
+__device__ __forceinline__ void fft_pass_multi(const double2* __restrict__ in, double2* __restrict__ out, int NA,
+                                               int Ms, int n, int Ns, const double2* __restrict__ pt, int sign) {
+  const int nR = n / R, total = NA * nR;
+  for (int item = threadIdx.x; item < total; item += blockDim.x) {
+    const int arr = item / nR, idx = item - arr * nR;
+    const double2* ia = in + (size_t)arr * Ms;
+    double2* oa = out + (size_t)arr * Ms;
+    const int j = idx % Ns, k = idx / Ns;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = ia[fidx<true>(idx + r * nR)];
+    if (Ns > 1) {
+      double2 w1 = pt[j];
+      if (sign > 0) w1.y = -w1.y;
+      if constexpr (R == 8) {
+        const double2 w2 = cmul(w1, w1), w4 = cmul(w2, w2), w3 = cmul(w1, w2);
+        v[1] = cmul(v[1], w1);
+        v[2] = cmul(v[2], w2);
+        v[3] = cmul(v[3], w3);
+        v[4] = cmul(v[4], w4);
+        v[5] = cmul(v[5], cmul(w1, w4));
+        v[6] = cmul(v[6], cmul(w2, w4));
+        v[7] = cmul(v[7], cmul(w3, w4));
+      } else if constexpr (R == 4) {
+        const double2 w2 = cmul(w1, w1);
+        v[1] = cmul(v[1], w1);
+        v[2] = cmul(v[2], w2);
+        v[3] = cmul(v[3], cmul(w1, w2));
+      } else if constexpr (R == 3) {
+        v[1] = cmul(v[1], w1);
+        v[2] = cmul(v[2], cmul(w1, w1));
+      } else {
+        v[1] = cmul(v[1], w1);
+      }
+    }
+    dft_small<R>(v, sign);
+    const int ob = k * Ns * R + j;
+#pragma unroll
+    for (int r = 0; r < R; ++r) oa[fidx<true>(ob + r * Ns)] = v[r];
+  }
+}
+
+// NA length-fp.n transforms at a[arr * Ms], ping-ponging with b[arr * Ms];
+// returns the block (a or b) holding the results.
+__device__ double2* fft_cta_multi(double2* a, double2* b, int NA, int Ms, const FftPlan& fp,
+                                  const double2* __restrict__ pt, int sign) {
+  const int n = fp.n;
+  int Ns = 1;
+  double2* in = a;
+  double2* out = b;
+  for (int s = 0; s < fp.nstages; ++s) {
+    const int R = fp.radix[s];
+    if (R == 8)
+      fft_pass_multi<8>(in, out, NA, Ms, n, Ns, pt, sign);
+    else if (R == 4)
+      fft_pass_multi<4>(in, out, NA, Ms, n, Ns, pt, sign);
+    else if (R == 2)
+      fft_pass_multi<2>(in, out, NA, Ms, n, Ns, pt, sign);
+    else
+      fft_pass_multi<3>(in, out, NA, Ms, n, Ns, pt, sign);
+    __syncthreads();
+    double2* t = in;
+    in = out;
+    out = t;
+    pt += Ns;
+    Ns *= R;
+  }
+  return in;
+}
+
+// The same row products as k_xprod with the transforms batched: the velocity
+// and the three gradient spectra are built in one sweep over the half-plane
+// inputs (each value and z-derivative bin read once), go through one set of
+// inverse passes together (4 arrays, one barrier per pass), the products
+// are formed for all three fields at once, and the two forward transforms
+// share their passes too: about 10 barriers per row instead of 27.  Shared
+// memory: two blocks of 4 arrays (ping-pong) and the per-pass twiddles.
+template <int NT>
+__global__ void __launch_bounds__(NT, NT == 256 ? 2 : 1) k_xprod_b(XProdArgs a) {
+  extern __shared__ double2 sm[];
+  const int M = a.M, N = a.Nx, Nk = a.Nk;
+  const int Ms = (M + 7) & ~7;
+  double2* A = sm;           // 4 arrays: U spectrum, then gradient spectra of b, ux, uz
+  double2* Bk = sm + 4 * Ms;  // ping-pong partner block
+  double2* tw = sm + 8 * Ms;
+  const int hN = N / 2;
+  for (int t = threadIdx.x; t < a.nptw; t += blockDim.x) tw[t] = a.ptw[t];
+  const int z = blockIdx.x;
+  const int zm = a.Nz - 1 - z;
+  const bool lower = z <= zm;
+  const size_t ld = a.ld > 0 ? (size_t)a.ld : (size_t)Nk, col0 = (size_t)blockIdx.y * Nk;
+  const size_t rr = (size_t)(lower ? z : zm) * ld + col0;
+  auto hbin = [&](double2 v, int q) -> double2 {
+    if (q == 0) return make_double2(v.x, 0.0);
+    if (q == hN) return make_double2(0.5 * v.x, 0.0);
+    return v;
+  };
+  auto put2 = [&](double2* dst, int q, double2 P, double2 Q) {
+    dst[fidx<true>(q)] = pack2(P, Q);
+    if (q > 0) dst[fidx<true>(M - q)] = pack2_mirror(P, Q);
+  };
+  // 1. all four inverse-transform inputs from one read of the six rows
+  for (int q = threadIdx.x; q <= hN; q += blockDim.x) {
+    double2 g[3], d[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const double2 e = a.ev[f][rr + q], o = a.ov[f][rr + q];
+      const double2 ed = a.ed[f][rr + q], od = a.od[f][rr + q];
+      g[f] = lower ? make_double2(e.x + o.x, e.y + o.y) : make_double2(e.x - o.x, e.y - o.y);
+      d[f] = lower ? make_double2(ed.x + od.x, ed.y + od.y) : make_double2(od.x - ed.x, od.y - ed.y);
+    }
+    put2(A, q, hbin(g[1], q), hbin(g[2], q));
+    const double kk = a.k0 * q;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      double2 Ax = make_double2(0.0, 0.0);
+      if (q > 0 && q < hN) Ax = make_double2(-kk * g[f].y, kk * g[f].x);  // i k g
+      put2(A + (size_t)(1 + f) * Ms, q, Ax, hbin(d[f], q));
+    }
+  }
+  for (int k = hN + 1 + threadIdx.x; k < M - hN; k += blockDim.x)  // bins N/2 < k < M - N/2 are zero
+#pragma unroll
+    for (int arr = 0; arr < 4; ++arr) A[(size_t)arr * Ms + fidx<true>(k)] = make_double2(0.0, 0.0);
+  __syncthreads();
+  double2* Rb = fft_cta_multi(A, Bk, 4, Ms, a.fp, tw, +1);
+  double2* Fb = (Rb == A) ? Bk : A;  // the free block
+  // 2. products -(u d_x f + w d_z f) for f = b, ux, uz: (b + i ux) and (uz) spectra inputs
+  for (int p = threadIdx.x; p < M; p += blockDim.x) {
+    const int ps = fidx<true>(p);
+    const double2 u = Rb[ps];
+    double pr[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const double2 gg = Rb[(size_t)(1 + f) * Ms + ps];
+      pr[f] = -(u.x * gg.x + u.y * gg.y);
+    }
+    Fb[ps] = make_double2(pr[0], pr[1]);
+    Fb[(size_t)Ms + ps] = make_double2(pr[2], 0.0);
+  }
+  __syncthreads();
+  // 3. both forward transforms through the same passes (Rb's first two arrays are free)
+  double2* Cb = fft_cta_multi(Fb, Rb, 2, Ms, a.fp, tw, -1);
+  const double2* C1 = Cb;
+  const double2* C2 = Cb + Ms;
+  const double sc = 1.0 / ((double)M * (double)N);
+  const size_t ro = (size_t)z * ld + col0;
+  for (int k = threadIdx.x; k < Nk; k += blockDim.x) {
+    const double2 c = C1[fidx<true>(k)];
+    const double2 cm = C1[fidx<true>((M - k) % M)];
+    const double2 sb = make_double2(0.5 * (c.x + cm.x), 0.5 * (c.y - cm.y));
+    const double2 su = make_double2(0.5 * (c.y + cm.y), -0.5 * (c.x - cm.x));
+    const double2 c2 = C2[fidx<true>(k)];
+    double2 ob, ou, oz;
+    if (k == 0) {
+      ob = make_double2(sb.x * sc, 0.0);
+      ou = make_double2(su.x * sc, 0.0);
+      oz = make_double2(c2.x * sc, 0.0);
+    } else if (k == hN) {
+      ob = make_double2(2.0 * sb.x * sc, 0.0);
+      ou = make_double2(2.0 * su.x * sc, 0.0);
+      oz = make_double2(2.0 * c2.x * sc, 0.0);
+    } else {
+      ob = cscale(sb, sc);
+      ou = cscale(su, sc);
+      oz = cscale(c2, sc);
+    }
+    a.out[0][ro + k] = ob;
+    a.out[1][ro + k] = ou;
+    a.out[2][ro + k] = oz;
+  }
+}
+
 // rfft of real rows (unnormalised), via a complex FFT of the row.
 __global__ void __launch_bounds__(256) k_x_rfft(const double* __restrict__ grid, double2* __restrict__ spec,
                                                 int Nx, FftPlan fp, const double2* __restrict__ tw) {
@@ -718,6 +894,10 @@ cudaError_t set_transform_smem_limits(int bytes) {
       cudaSuccess)
     return e;
   if ((e = cudaFuncSetAttribute(k_xprod, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_xprod_b<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(k_xprod_b<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
+    return e;
   if ((e = cudaFuncSetAttribute(k_x_rfft, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_x_irfft, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_x_dealias_mul, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -732,6 +912,23 @@ size_t xprod_smem_bytes(int M, int Nk, int nptw) {
 void launch_xprod(const XProdArgs& a, cudaStream_t st) {
   size_t smem = xprod_smem_bytes(a.M, a.Nk, a.nptw);
   k_xprod<<<dim3(a.Nz, a.instances > 0 ? a.instances : 1), 256, smem, st>>>(a);
+}
+
+size_t xprod_b_smem_bytes(int M, int nptw) {
+  const size_t Ms = (size_t)((M + 7) & ~7);
+  return (8 * Ms + (size_t)nptw) * sizeof(double2);
+}
+
+bool xprod_b_fits(int M, int nptw) { return xprod_b_smem_bytes(M, nptw) <= 227 * 1024; }
+
+void launch_xprod_b(const XProdArgs& a, cudaStream_t st) {
+  const size_t smem = xprod_b_smem_bytes(a.M, a.nptw);
+  const dim3 grid(a.Nz, a.instances > 0 ? a.instances : 1);
+  // two CTAs of 256 threads per SM while both fit, else one of 512
+  if (2 * smem <= 227 * 1024)
+    k_xprod_b<256><<<grid, 256, smem, st>>>(a);
+  else
+    k_xprod_b<512><<<grid, 512, smem, st>>>(a);
 }
 
 void launch_x_rfft(const double* grid, double2* spec, int nrows, int Nx, const FftPlan& fp, const double2* tw,

@@ -13,6 +13,7 @@ pytestmark = pytest.mark.gpu
 def test_tau_partitions_give_the_oracle_solution(tb):
     p = RBCParams(Nx=48, Nz=24, Lx=4.0, Lz=1.0, Ra=1e8)
     sim = run_rbc(p, "RK443", 0.01, 4, seed=42)
+    # Nz = 24: 48 band rows, 4 windows of 12, so 8 partitions do not fit (refused)
     for parts in (4, 1):
         dom = tb.ChannelDomain(48, 24, Lx=4.0, Lz=1.0)
         plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 1)
@@ -22,6 +23,84 @@ def test_tau_partitions_give_the_oracle_solution(tb):
         plan.step(0.01, 4)
         for f, want in ((0, sim.b), (1, sim.ux), (2, sim.uz)):
             assert rel_l2(plan.get_state(f), want) < 1e-10
+    dom = tb.ChannelDomain(48, 24, Lx=4.0, Lz=1.0)
+    plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 1)
+    with pytest.raises(tb.TarangError):
+        plan.set_variant(tau_parts=8)
+
+
+@pytest.mark.parametrize("scheme,ts", [("RK443", 1), ("SBDF2", 3)])
+def test_uneven_eight_partitions_give_the_oracle_solution(tb, scheme, ts):
+    # Nz = 64: 132 band rows per class, padded to 144 = 12 windows of 12 rows,
+    # so eight partitions take 1 or 2 windows each
+    p = RBCParams(Nx=64, Nz=64, Lx=4.0, Lz=1.0, Ra=1e8)
+    sim = run_rbc(p, scheme, 0.01, 5, seed=42)
+    states = {}
+    for parts in (8, 4, 1):
+        dom = tb.ChannelDomain(64, 64, Lx=4.0, Lz=1.0)
+        plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, ts)
+        plan.set_variant(tau_parts=parts)
+        assert plan.variant()[0] == parts
+        plan.set_state(0, forward_2d(rbc_initial_b(p, 42)))
+        plan.step(0.01, 5)
+        for f, want in ((0, sim.b), (1, sim.ux), (2, sim.uz)):
+            assert rel_l2(plan.get_state(f), want) < 1e-10, (parts, f)
+        states[parts] = [plan.get_state(f) for f in (0, 1, 2, 3)]
+    for parts in (8, 4):
+        for a, b in zip(states[parts], states[1]):
+            assert rel_l2(a, b) < 1e-12 or np.abs(b).max() == 0.0
+
+
+@pytest.mark.parametrize("key", ["16x11", "24x16", "96x24"])
+def test_batched_x_products_match_golden_rhs(tb, golden_dir, key):
+    import os
+
+    d = np.load(os.path.join(golden_dir, "transforms.npz"))
+    Nx, Nz = map(int, key.split("x"))
+    p = RBCParams(Nx=Nx, Nz=Nz)
+    dom = tb.ChannelDomain(Nx, Nz)
+    outs = {}
+    for form in (1, 2):
+        plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 0)
+        plan.set_variant(xrows=form)
+        assert plan.variant()[1] == form
+        outs[form] = plan.rhs_advection(*(d[f"rhs_in{i}_{key}"] for i in range(3)))
+        for i in range(3):
+            assert rel_l2(outs[form][i], d[f"rhs_out{i}_{key}"]) < 1e-12
+    for a, b in zip(outs[1], outs[2]):
+        assert rel_l2(a, b) < 1e-14
+
+
+@pytest.mark.parametrize("scheme,ts", [("RK443", 1), ("SBDF2", 3)])
+def test_batched_x_products_steps_match_oracle(tb, scheme, ts):
+    p = RBCParams(Nx=256, Nz=64, Lx=4.0, Lz=1.0, Ra=1e8)
+    sim = run_rbc(p, scheme, 0.01, 4, seed=42)
+    dom = tb.ChannelDomain(256, 64, Lx=4.0, Lz=1.0)
+    plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, ts)
+    plan.set_variant(xrows=2)
+    plan.set_state(0, forward_2d(rbc_initial_b(p, 42)))
+    plan.step(0.01, 4)
+    for f, want in ((0, sim.b), (1, sim.ux), (2, sim.uz)):
+        assert rel_l2(plan.get_state(f), want) < 1e-10
+
+
+def test_batched_x_products_mixed_precision(tb):
+    # the FP32 batched kernel against the FP32 per-field kernel and the FP64 oracle RHS
+    from oracle.tarang_oracle import RBC2D
+
+    Nx, Nz = 96, 24
+    rng = np.random.default_rng(6)
+    ins = [forward_2d(rng.standard_normal((Nz, Nx))) for _ in range(3)]
+    p = RBCParams(Nx=Nx, Nz=Nz)
+    dom = tb.ChannelDomain(Nx, Nz)
+    outs = {}
+    for form in (1, 2):
+        plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 0, precision=tb._lib.TB_PREC_MIXED)
+        plan.set_variant(xrows=form)
+        outs[form] = plan.rhs_advection(*ins)
+    ref = RBC2D(p).rhs(*ins)
+    for a, b, r in zip(outs[1], outs[2], ref):
+        assert rel_l2(b, a) < 1e-5 and rel_l2(b, r) < 1e-5
 
 
 def test_xpass_rows_and_tau_partitions_agree_in_3d(tb):
@@ -53,7 +132,7 @@ def test_plan_tune_keeps_state_and_picks_a_feasible_shape(tb):
     plan.step(0.02, 2)
     before = [plan.get_state(f) for f in (0, 1, 2)]
     parts, rows = plan.tune(0.02, trial_steps=3)
-    assert parts in (1, 4) and rows == 0 and plan.variant()[0] == parts
+    assert parts in (1, 4, 8) and rows in (1, 2) and plan.variant() == (parts, rows)
     for f, b in zip((0, 1, 2), before):
         assert np.array_equal(plan.get_state(f), b)
     plan.step(0.02, 2)  # steps on with the chosen shape
@@ -72,6 +151,6 @@ def test_ensemble_tune_applies_one_partitioning_to_all_members(tb):
     before = [pl.get_state(0) for pl in plans]
     ens.tune(0.02, trial_steps=2)
     parts = {pl.variant()[0] for pl in plans}
-    assert len(parts) == 1 and parts <= {1, 4}
+    assert len(parts) == 1 and parts <= {1, 4, 8}
     for pl, b in zip(plans, before):
         assert np.array_equal(pl.get_state(0), b)
