@@ -46,6 +46,11 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--tau-parts", type=int, default=0, choices=[0, 1, 4, 8],
                     help="tau-solve partitions of the headline plan (0: chosen by the plan's tuner)")
+    ap.add_argument("--precision", choices=["f64", "mixed"], default="f64",
+                    help="arithmetic of the headline plan (mixed: FP32 transforms and products, FP64 tau LU)")
+    ap.add_argument("--x-form", type=int, default=0, choices=[0, 1, 2],
+                    help="x-products kernel of the headline plan: 1 per field, 2 batched (0: the tuner's choice; "
+                         "with --tau-parts the plan's default, 1)")
     ap.add_argument("--cpu-steps", type=int, default=10,
                     help="timed steps of the CPU baseline leg (about 1 s each on 16 host threads)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -396,16 +401,19 @@ def run_ours(args, cfg, scheme, dist):
     torch.cuda.set_device(dev)
     dom = tb.ChannelDomain(cfg.Nx, cfg.Nz, Lx=cfg.Lx, Lz=cfg.Lz, arch=tb.GPU(dev))
     ts = {"RK222": 0, "RK443": 1, "SBDF2": 3}[scheme]
-    plan = tb.Plan(dom, cfg.kappa, cfg.nu, cfg.Lz, 0.0, ts)
+    from tarang_b200._lib import TB_PREC_F64, TB_PREC_MIXED
+
+    plan = tb.Plan(dom, cfg.kappa, cfg.nu, cfg.Lz, 0.0, ts,
+                   precision=TB_PREC_MIXED if args.precision == "mixed" else TB_PREC_F64)
     b0 = plan.forward(W.rbc_initial_grid(cfg))
     plan.set_state(TB_FIELD_B, b0)
 
     # warm-up (the first call factors the tau systems and captures the step graph),
     # then the plan's kernel shapes are tuned on a few steps (state restored)
-    if args.tau_parts:
-        plan.set_variant(tau_parts=args.tau_parts)
+    if args.tau_parts or args.x_form:
+        plan.set_variant(tau_parts=args.tau_parts, xrows=args.x_form)
     plan.step(cfg.dt, args.warmup)
-    tuned = (args.tau_parts, 0) if args.tau_parts else plan.tune(cfg.dt, trial_steps=3)
+    tuned = plan.variant() if (args.tau_parts or args.x_form) else plan.tune(cfg.dt, trial_steps=3)
     plan.step(cfg.dt, 1)
 
     # timed region: K graph replays, device time from CUDA events on the plan's stream
@@ -501,7 +509,8 @@ def run_ours(args, cfg, scheme, dist):
         cpu = cpu_baseline(cfg, scheme, args.cpu_steps)
     if dist.rank == 0:
         out = {
-            "metric": f"RBC 2D steps/s ({cfg.Nx}x{cfg.Nz}, {scheme}, Float64)",
+            "metric": f"RBC 2D steps/s ({cfg.Nx}x{cfg.Nz}, {scheme}, "
+                      f"{'Float64' if args.precision == 'f64' else 'FP32 transforms + FP64 tau LU'})",
             "value": value,
             "unit": "steps/s",
             "n_gpus": dist.world,
@@ -555,9 +564,23 @@ def run_ours(args, cfg, scheme, dist):
     # sharded across every rank (collective statistics: all ranks take part)
     if not args.no_ensemble:
         try:
-            ens_out = run_ensemble(args, dev, dist)
+            ens_out = run_ensemble(args, dev, dist, keep_states=True)
         except Exception as exc:  # reported, never fatal to the headline line
             ens_out = {"error": f"{type(exc).__name__}: {exc}"}
+        try:
+            ens_mixed = run_ensemble(args, dev, dist, mixed=True, keep_states=True)
+            f64s, mxs = ens_out.pop("final_states", None), ens_mixed.pop("final_states", None)
+            if f64s and mxs:
+                import numpy as np
+
+                ens_mixed["max_rel_l2_vs_f64_members"] = float(max(
+                    np.linalg.norm(m[i] - f[i]) / np.linalg.norm(f[i]) for m, f in zip(mxs, f64s) for i in (0, 1)))
+            if "plain_gpu" in ens_out:
+                ens_mixed["speedup_vs_f64_plain_gpu"] = ens_mixed["value"] / ens_out["plain_gpu"]["value"]
+            ens_out["mixed"] = ens_mixed
+        except Exception as exc:  # reported, never fatal to the headline line
+            ens_out["mixed"] = {"error": f"{type(exc).__name__}: {exc}"}
+        ens_out.pop("final_states", None)
     if not args.no_serving:
         try:
             srv_out = run_serving(args, dev, dist)
@@ -599,7 +622,10 @@ def summarize(out: dict) -> dict:
     if "ensemble" in out:
         s["ensemble"] = {"fused": g(out, "ensemble", "value"),
                          "per_member_streams": g(out, "ensemble", "per_member_streams", "value"),
-                         "plain_gpu": g(out, "ensemble", "plain_gpu", "value")}
+                         "plain_gpu": g(out, "ensemble", "plain_gpu", "value"),
+                         "mixed": g(out, "ensemble", "mixed", "value"),
+                         "mixed_vs_f64_plain": g(out, "ensemble", "mixed", "speedup_vs_f64_plain_gpu"),
+                         "mixed_err": g(out, "ensemble", "mixed", "max_rel_l2_vs_f64_members")}
     if "serving" in out:
         s["serving"] = {"saturated": g(out, "serving", "saturated", "solves_per_s"),
                         "plain_saturated": g(out, "serving", "plain_gpu_saturated", "solves_per_s"),
@@ -608,7 +634,7 @@ def summarize(out: dict) -> dict:
     return s
 
 
-def run_ensemble(args, dev, dist=None):
+def run_ensemble(args, dev, dist=None, mixed=False, keep_states=False):
     """Batched ensemble (independent 2D RBC instances of uneven size, RK222):
     instance steps per second of the ensemble runner against the plain GPU form
     (the same plans stepped one after another), and time-to-solution p50/p99.
@@ -627,10 +653,13 @@ def run_ensemble(args, dev, dist=None):
     rank = dist.rank if dist else 0
     shards = W.shard_instances([W.instance_cost(c) for c in members], world)
     members = [members[i] for i in shards[rank]]
+    from tarang_b200._lib import TB_PREC_F64, TB_PREC_MIXED
+
+    prec = TB_PREC_MIXED if mixed else TB_PREC_F64
     plans, init = [], []
     for c in members:
         dom = tb.ChannelDomain(c.Nx, c.Nz, Lx=c.Lx, Lz=c.Lz, arch=tb.GPU(dev))
-        plan = tb.Plan(dom, c.kappa, c.nu, c.Lz, 0.0, 0)
+        plan = tb.Plan(dom, c.kappa, c.nu, c.Lz, 0.0, 0, precision=prec)
         b0 = plan.forward(W.rbc_initial_grid(c))
         plan.set_state(0, b0)
         plans.append(plan)
@@ -679,6 +708,7 @@ def run_ensemble(args, dev, dist=None):
     part = {"steps": len(plans) * n, "total_ms": float(total), "ms": [float(v) for v in ms], "plain_s": plain_s,
             "plain_done_ms": done, "finite": bool(finite),
             "streams_total_ms": None if stream_total is None else float(stream_total)}
+    final = [(p.get_state(0), p.get_state(2)) for p in plans] if keep_states else None
     parts = dist.gather(part) if dist else [part]
     agg = W.combine_ensemble(parts)
     sizes = {}
@@ -695,7 +725,8 @@ def run_ensemble(args, dev, dist=None):
         "sharding": "members assigned to ranks by cost (longest processing time first), no collective"
                     if world > 1 else "one GPU",
         "scheme": "RK222",
-        "dtype": "f64",
+        "dtype": "f32 transforms/products, f64 tau LU" if mixed else "f64",
+        "final_states": final,
         "tuned": {"worker_streams": streams, "steps_per_graph": gsteps, "tau_solve_partitions": tuned_parts,
                   "fused_form": tuned_fused, "stacked_group_plans": tuned_groups},
         "time_to_solution_ms": {"p50": agg["p50_ms"], "p99": agg["p99_ms"], "max": agg["total_ms"]},

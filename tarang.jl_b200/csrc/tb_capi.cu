@@ -312,7 +312,9 @@ void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2row
   xa.nptw = (int)(P->ptwM32.bytes / sizeof(float2));
   xa.fp = P->fpM;
   xa.Nx = P->Nx;
-  xa.Nk = P->Nk;
+  xa.Nk = P->Nkm;
+  xa.ld = P->Nk;
+  xa.instances = P->B;
   xa.M = P->M;
   xa.Nz = N;
   xa.k0 = (float)P->k0;
@@ -676,10 +678,9 @@ void tb::plan_launch_steps(tb_plan* P, double dt, int nsteps, cudaStream_t s, in
 }
 
 // The batched 2D x-products kernel fits shared memory (F64 or the FP32 form of
-// a mixed plan); single-instance FP32 plans only (the FP32 kernel has no
-// stacked-instance form).
+// a mixed plan).
 static bool xprod2d_batched_fits(const tb_plan* P) {
-  if (P->mixed) return P->B <= 1 && xprod32_b_fits(P->M, (int)(P->ptwM32.bytes / sizeof(float2)));
+  if (P->mixed) return xprod32_b_fits(P->M, (int)(P->ptwM32.bytes / sizeof(float2)));
   return xprod_b_fits(P->M, (int)(P->ptwM.bytes / sizeof(double2)));
 }
 

@@ -11,7 +11,7 @@
 // tuner times candidate settings on the ensemble itself (from a snapshot that
 // is restored afterwards) and keeps the fastest.
 //
-// Fused form: members of one shape (Nx, Nz, domain, walls, RK stepper, FP64)
+// Fused form: members of one shape (Nx, Nz, domain, walls, RK stepper, precision)
 // that step at the same dt are stacked along the mode axis into one plan
 // (build_plan with B instances): every kernel of a step then covers the whole
 // group in one launch - the tau solves over all the group's mode groups, the
@@ -69,14 +69,14 @@ void ensure_streams(tb_ensemble* E, int n) {
 }
 
 bool fusible(const tb_plan* P) {
-  return P->ndim == 2 && P->B == 1 && !P->mixed && !P->bc_dynamic && P->d.program == TB_PROGRAM_RBC &&
+  return P->ndim == 2 && P->B == 1 && !P->bc_dynamic && P->d.program == TB_PROGRAM_RBC &&
          (P->d.timestepper == TB_RK222 || P->d.timestepper == TB_RK443);
 }
 
 bool same_shape(const tb_plan* a, const tb_plan* b) {
   const tb_problem_desc &x = a->d, &y = b->d;
   return x.Nx == y.Nx && x.Nz == y.Nz && x.Lx == y.Lx && x.Lz == y.Lz && x.timestepper == y.timestepper &&
-         x.b_bottom == y.b_bottom && x.b_top == y.b_top;
+         x.b_bottom == y.b_bottom && x.b_top == y.b_top && x.precision == y.precision;
 }
 
 // Groups of at least two same-shape fusible members, each as a stacked plan.

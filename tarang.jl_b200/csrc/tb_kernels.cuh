@@ -40,10 +40,15 @@ void launch_gemm_tc32(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int 
                       cudaStream_t st);
 cudaError_t set_tc32_smem_limits();
 int tc32_status();  // 1 once a tensor-core GEMM's bounded wait gave up, -1 if unreadable
-// tensor cores when asked for and the shapes fit, else the SIMT kernel
+// Column tiles each CTA of the tensor-core GEMM walks through (one wave of
+// CTAs, one per SM).
+int gemm_tc32_tiles_per_cta(int ncol, int nbatch);
+// tensor cores when asked for, the shapes fit and each CTA has at most two
+// column tiles (its tile loop loads, multiplies and stores one tile at a time,
+// so long loops - wide stacked plans - stay on the SIMT kernel), else SIMT
 inline void launch_gemm_f32_path(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows,
                                  bool out_f64, cudaStream_t st, bool tensor_cores) {
-  if (tensor_cores && gemm_tc32_supported(bt, nbatch))
+  if (tensor_cores && gemm_tc32_supported(bt, nbatch) && gemm_tc32_tiles_per_cta(ncol, nbatch) <= 2)
     launch_gemm_tc32(bt, nbatch, ncol, ldb, ldc, Nrows, out_f64, st);
   else
     launch_gemm_f32(bt, nbatch, ncol, ldb, ldc, Nrows, out_f64, st);
@@ -60,6 +65,8 @@ struct XProdArgs32 {
   FftPlan fp;
   int Nx, Nk, M, Nz;
   float k0;
+  int ld;         // row stride of the planes (Nk, or instances x Nk in a stacked plan)
+  int instances;  // instances stacked along the mode axis (grid.y)
 };
 void launch_xprod32(const XProdArgs32& a, cudaStream_t st);
 void launch_xprod32_b(const XProdArgs32& a, cudaStream_t st);  // transforms batched (as launch_xprod_b)

@@ -155,7 +155,8 @@ __global__ void __launch_bounds__(256, 2) k_xprod32(XProdArgs32 a) {
   const int z = blockIdx.x;
   const int zm = a.Nz - 1 - z;
   const bool lower = z <= zm;
-  const size_t rr = (size_t)(lower ? z : zm) * Nk;
+  const size_t ld = a.ld > 0 ? (size_t)a.ld : (size_t)Nk, col0 = (size_t)blockIdx.y * Nk;
+  const size_t rr = (size_t)(lower ? z : zm) * ld + col0;
   auto value = [&](int f, int q) -> float2 {
     const float2 e = a.ev[f][rr + q], o = a.ov[f][rr + q];
     return lower ? make_float2(e.x + o.x, e.y + o.y) : make_float2(e.x - o.x, e.y - o.y);
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(256, 2) k_xprod32(XProdArgs32 a) {
       float2* C1 = F::fft<true>(P, G, a.fp, tw, -1);
       float2* C2 = F::fft<true>(Gf, U, a.fp, tw, -1);
       const float sc = 1.0f / ((float)M * (float)N);
-      const size_t ro = (size_t)z * Nk;
+      const size_t ro = (size_t)z * ld + col0;
       for (int k = threadIdx.x; k < Nk; k += blockDim.x) {
         const float2 c = C1[F::fidx<true>(k)];
         const float2 cm = C1[F::fidx<true>((M - k) % M)];
@@ -289,7 +290,8 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 2 : 1) k_xprod32_b(XProdArgs32
   const int z = blockIdx.x;
   const int zm = a.Nz - 1 - z;
   const bool lower = z <= zm;
-  const size_t rr = (size_t)(lower ? z : zm) * Nk;
+  const size_t ld = a.ld > 0 ? (size_t)a.ld : (size_t)Nk, col0 = (size_t)blockIdx.y * Nk;
+  const size_t rr = (size_t)(lower ? z : zm) * ld + col0;
   auto hbin = [&](float2 v, int q) -> float2 {
     if (q == 0) return make_float2(v.x, 0.f);
     if (q == hN) return make_float2(0.5f * v.x, 0.f);
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 2 : 1) k_xprod32_b(XProdArgs32
   const float2* C1 = Cb;
   const float2* C2 = Cb + Ms;
   const float sc = 1.0f / ((float)M * (float)N);
-  const size_t ro = (size_t)z * Nk;
+  const size_t ro = (size_t)z * ld + col0;
   for (int k = threadIdx.x; k < Nk; k += blockDim.x) {
     const float2 c = C1[F::fidx<true>(k)];
     const float2 cm = C1[F::fidx<true>((M - k) % M)];
@@ -400,7 +402,7 @@ cudaError_t set_mixed_smem_limits(int bytes) {
 }
 
 void launch_xprod32(const XProdArgs32& a, cudaStream_t st) {
-  k_xprod32<<<a.Nz, 256, xprod32_smem_bytes(a.M, a.nptw), st>>>(a);
+  k_xprod32<<<dim3(a.Nz, a.instances > 0 ? a.instances : 1), 256, xprod32_smem_bytes(a.M, a.nptw), st>>>(a);
 }
 
 size_t xprod32_b_smem_bytes(int M, int nptw) {
@@ -412,10 +414,11 @@ bool xprod32_b_fits(int M, int nptw) { return xprod32_b_smem_bytes(M, nptw) <= 2
 
 void launch_xprod32_b(const XProdArgs32& a, cudaStream_t st) {
   const size_t smem = xprod32_b_smem_bytes(a.M, a.nptw);
+  const dim3 grid(a.Nz, a.instances > 0 ? a.instances : 1);
   if (2 * smem <= 227 * 1024)
-    k_xprod32_b<256><<<a.Nz, 256, smem, st>>>(a);
+    k_xprod32_b<256><<<grid, 256, smem, st>>>(a);
   else
-    k_xprod32_b<512><<<a.Nz, 512, smem, st>>>(a);
+    k_xprod32_b<512><<<grid, 512, smem, st>>>(a);
 }
 
 }  // namespace tb

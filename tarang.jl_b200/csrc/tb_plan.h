@@ -181,7 +181,7 @@ struct tb_plan {
   FftPlan fpNy{};
   DevBuf ptwNy, tmp3;
   int xrows = 1;  // padded y rows per x-pass CTA (a tuned shape)
-  bool tc32 = false;  // mixed precision: FP32 transform GEMMs on the tensor cores (when the shapes fit)
+  bool tc32 = true;  // mixed precision: FP32 transform GEMMs on the tensor cores (when the shapes fit)
   // transform constants
   DevBuf bwd, fwd, s3, twM, twN, ptwM;
   // parity halves of the Chebyshev matrices (H = ceil(Nz/2) rows/cols)

@@ -660,7 +660,9 @@ void enqueue_rhs_t(tb_plan* P, const double2* Xin, double2* out4) {
         bt.item[4 * f + w] = GemmItem32{Am[w], reinterpret_cast<const float*>(Xc + (size_t)f * plane),
                                         G + (size_t)(4 * f + w) * hplane, H, (w & 1) ? P->Ko : P->Ke,
                                         pad16((w & 1) ? P->Ko : P->Ke), GEMM_PARITY, w & 1};
-    timed(P, "z_backward_gemm", [&] { launch_gemm_f32_path(bt, 16, ncol, ncol, ncol, N, false, P->st, P->tc32); });
+    // SIMT here: the 3D GEMMs stream 33k-column planes near the HBM bound, and
+    // the tensor-core kernel's serial tile loop (no prefetch) does not beat it
+    timed(P, "z_backward_gemm", [&] { launch_gemm_f32(bt, 16, ncol, ncol, ncol, N, false, P->st); });
   } else {
     GemmBatch bt{};
     const double* Am[4] = {P->bEv.as<double>(), P->bOv.as<double>(), P->bEd.as<double>(), P->bOd.as<double>()};
@@ -699,7 +701,7 @@ void enqueue_rhs_t(tb_plan* P, const double2* Xin, double2* out4) {
       bf.item[nb++] = GemmItem32{P->sfE32.as<float>(), in, out, P->Ke, H, pad16(H), GEMM_MIRROR, 0};
       bf.item[nb++] = GemmItem32{P->sfO32.as<float>(), in, out, P->Ko, H, pad16(H), GEMM_MIRROR, 1};
     }
-    timed(P, "z_forward_gemm", [&] { launch_gemm_f32_path(bf, nb, ncol, ncol, ncol, N, true, P->st, P->tc32); });
+    timed(P, "z_forward_gemm", [&] { launch_gemm_f32(bf, nb, ncol, ncol, ncol, N, true, P->st); });
   } else {
     GemmBatch bf{};
     int nb = 0;

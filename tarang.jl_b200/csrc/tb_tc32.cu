@@ -237,12 +237,25 @@ cudaError_t set_tc32_smem_limits() {
   return cudaFuncSetAttribute(k_gemm_tc32<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
 }
 
-void launch_gemm_tc32(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
-                      cudaStream_t st) {
+namespace {
+int tc32_ctas_per_item(int ncol, int nbatch) {
   const int ntiles = (ncol + kTcN - 1) / kTcN;
   int per = 148 / nbatch;  // one wave of CTAs (one per SM by shared memory)
   if (per < 1) per = 1;
   if (per > ntiles) per = ntiles;
+  return per;
+}
+}  // namespace
+
+int gemm_tc32_tiles_per_cta(int ncol, int nbatch) {
+  const int ntiles = (ncol + kTcN - 1) / kTcN;
+  const int per = tc32_ctas_per_item(ncol, nbatch);
+  return (ntiles + per - 1) / per;
+}
+
+void launch_gemm_tc32(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
+                      cudaStream_t st) {
+  const int per = tc32_ctas_per_item(ncol, nbatch);
   dim3 grid(per, 1, nbatch);
   if (out_f64)
     k_gemm_tc32<double><<<grid, kTcThreads, kTcSmem, st>>>(bt, ncol, ldb, ldc, Nrows);

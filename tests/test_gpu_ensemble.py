@@ -24,11 +24,12 @@ MEMBERS = [
 ]
 
 
-def build(tb, spec, seed):
+def build(tb, spec, seed, precision=None):
     Nx, Nz, Ra, scheme, _ = spec
     p = RBCParams(Nx=Nx, Nz=Nz, Lx=4.0, Lz=1.0, Ra=Ra)
     dom = tb.ChannelDomain(Nx, Nz, Lx=4.0, Lz=1.0)
-    plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, TS[scheme])
+    prec = tb._lib.TB_PREC_F64 if precision is None else precision
+    plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, TS[scheme], precision=prec)
     plan.set_state(0, forward_2d(rbc_initial_b(p, seed)))
     return p, plan
 
@@ -139,6 +140,38 @@ def test_fused_form_matches_solo_runs_and_oracle(tb):
     _, again = build(tb, FUSED[2], 72)
     again.step(FUSED[2][4], nsteps + 2)
     assert rel_l2(plans[2].get_state(0), again.get_state(0)) < 1e-12
+
+
+@pytest.mark.parametrize("form", [1, 2])
+def test_fused_form_with_mixed_precision_members(tb, form):
+    # mixed members stack like Float64 ones; each matches its solo mixed run
+    # to FP32 rounding and the FP64 oracle at the mixed bar (1e-6)
+    nsteps = 5
+    mixed = tb._lib.TB_PREC_MIXED
+    solo = []
+    for k, spec in enumerate(FUSED):
+        _, plan = build(tb, spec, 70 + k, mixed)
+        plan.set_variant(xrows=form)
+        plan.step(spec[4], nsteps)
+        solo.append(states(plan))
+    pairs = [build(tb, spec, 70 + k, mixed) for k, spec in enumerate(FUSED)]
+    plans = [pl for _, pl in pairs]
+    for pl in plans:
+        pl.set_variant(xrows=form)
+    ens = tb.Ensemble(plans)
+    ens.set_form(True)
+    ens.set_config(2, 2)
+    ens.run([s[4] for s in FUSED], nsteps)
+    fused, groups = ens.form()
+    assert fused and groups == 2
+    for k, plan in enumerate(plans):
+        for a, b in zip(states(plan), solo[k]):
+            assert rel_l2(a, b) < 1e-6, f"member {k}"
+    for k in (0, 1, 3):
+        p, _ = pairs[k]
+        ref = run_rbc(p, FUSED[k][3], FUSED[k][4], nsteps, seed=70 + k)
+        assert rel_l2(plans[k].get_state(0), ref.b) < 1e-6
+        assert rel_l2(plans[k].get_state(2), ref.uz) < 1e-6
 
 
 def test_tuner_may_choose_the_fused_form(tb):

@@ -48,7 +48,8 @@ def test_uneven_eight_partitions_give_the_oracle_solution(tb, scheme, ts):
         states[parts] = [plan.get_state(f) for f in (0, 1, 2, 3)]
     for parts in (8, 4):
         for a, b in zip(states[parts], states[1]):
-            assert rel_l2(a, b) < 1e-12 or np.abs(b).max() == 0.0
+            # partitions change the rounding of the sweeps (responses), not the solution
+            assert rel_l2(a, b) < 1e-11 or np.abs(b).max() == 0.0
 
 
 @pytest.mark.parametrize("key", ["16x11", "24x16", "96x24"])
@@ -57,8 +58,8 @@ def test_batched_x_products_match_golden_rhs(tb, golden_dir, key):
 
     d = np.load(os.path.join(golden_dir, "transforms.npz"))
     Nx, Nz = map(int, key.split("x"))
-    p = RBCParams(Nx=Nx, Nz=Nz)
-    dom = tb.ChannelDomain(Nx, Nz)
+    p = RBCParams(Nx=Nx, Nz=Nz)  # the fixture's parameters (Lx 4, Lz 1)
+    dom = tb.ChannelDomain(Nx, Nz, Lx=p.Lx, Lz=p.Lz)
     outs = {}
     for form in (1, 2):
         plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 0)
@@ -92,7 +93,7 @@ def test_batched_x_products_mixed_precision(tb):
     rng = np.random.default_rng(6)
     ins = [forward_2d(rng.standard_normal((Nz, Nx))) for _ in range(3)]
     p = RBCParams(Nx=Nx, Nz=Nz)
-    dom = tb.ChannelDomain(Nx, Nz)
+    dom = tb.ChannelDomain(Nx, Nz, Lx=p.Lx, Lz=p.Lz)
     outs = {}
     for form in (1, 2):
         plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 0, precision=tb._lib.TB_PREC_MIXED)
@@ -100,7 +101,7 @@ def test_batched_x_products_mixed_precision(tb):
         outs[form] = plan.rhs_advection(*ins)
     ref = RBC2D(p).rhs(*ins)
     for a, b, r in zip(outs[1], outs[2], ref):
-        assert rel_l2(b, a) < 1e-5 and rel_l2(b, r) < 1e-5
+        assert rel_l2(b, a) < 1e-6 and rel_l2(b, r) < 1e-5
 
 
 def test_xpass_rows_and_tau_partitions_agree_in_3d(tb):

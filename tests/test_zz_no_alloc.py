@@ -45,7 +45,7 @@ def test_noalloc_product_matches_plan_entry_point_on_two_calls(tb):
     rng = np.random.default_rng(11)
     # calls in a row with different sizes: each rewrites the shared twiddles.
     # Nx = 2048 (padded length 3072) fills the static array exactly.
-    for Nx, Nz in ((256, 64), (96, 17), (2048, 4), (256, 64)):
+    for Nx, Nz in ((256, 64), (96, 17), (2048, 8), (256, 64)):
         a = rng.standard_normal((Nz, Nx))
         b = rng.standard_normal((Nz, Nx))
         want = _plan_product(tb, Nx, Nz, a, b)
