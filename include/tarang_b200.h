@@ -190,9 +190,12 @@ tb_status tb_checkpoint_load(tb_plan* plan, const double* grid, int where, const
  *              shortest latency for one plan - or 1 (no response records, the
  *              least device work per solve; needs npad/12 >= parts);
  *   xrows      3D: padded y rows per x-pass CTA, 1, 2 or 4; 2D (Float64
- *              plans): the x-products kernel, 1 = the three gradient
- *              transforms one after another, 2 = all inverse and forward
- *              transforms of a row batched through shared passes.
+ *              and mixed plans): the x-products kernel, 1 = the three
+ *              gradient transforms one after another, 2 = all inverse and
+ *              forward transforms of a row batched through shared passes,
+ *              3 = batched and in place (decimation in frequency for the
+ *              inverse, in time for the forward transforms; half the shared
+ *              memory of 2).
  * 0 keeps a setting.  A change drops the plan's factors and step graphs; the
  * next step rebuilds them.  tb_plan_tune times trial_steps steps of every
  * feasible combination from the current state (the state is restored after
@@ -203,8 +206,8 @@ tb_status tb_plan_get_variant(const tb_plan* plan, int* tau_parts, int* xrows);
 tb_status tb_plan_tune(tb_plan* plan, double dt, int trial_steps, int* tau_parts, int* xrows);
 /* FP32 Chebyshev transform GEMMs of a 2D mixed-precision plan: tensor_cores =
  * 1 runs them on the tcgen05 tensor cores in TF32 with three products per
- * term (FP32 accuracy) wherever Nz <= 256, 0 on the SIMT FP32 kernel (3D
- * plans always use the SIMT kernel).  No counterpart in the reference, whose GPU Chebyshev transforms are
+ * term (FP32 accuracy) wherever Nz <= 256, 0 (the default) on the SIMT FP32
+ * kernel (3D plans always use the SIMT kernel).  No counterpart in the reference, whose GPU Chebyshev transforms are
  * cuFFT DCT-Is (ext/cuda/cheb_deriv.jl:503-596).  A change drops the plan's
  * step graphs. */
 tb_status tb_plan_set_gemm_path(tb_plan* plan, int tensor_cores);

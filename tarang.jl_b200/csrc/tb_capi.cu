@@ -140,6 +140,23 @@ std::vector<double2> pass_twiddles(const FftPlan& fp) {
   return t;
 }
 
+// In-place (DIF/DIT) twiddles: per pass s, exp(-2 pi i j / L_s) for j < L_s / R_s,
+// L_s = n / (R_0 ... R_{s-1}) (the layout fftg::fft_ip_dif / fft_ip_dit read)
+std::vector<double2> ip_twiddles(const FftPlan& fp) {
+  std::vector<double2> t;
+  const long double pi = 3.141592653589793238462643383279502884L;
+  int L = fp.n;
+  for (int s = 0; s < fp.nstages; ++s) {
+    const int m = L / fp.radix[s];
+    for (int j = 0; j < m; ++j) {
+      const long double a = -2.0L * pi * (long double)j / (long double)L;
+      t.push_back(make_double2((double)cosl(a), (double)sinl(a)));
+    }
+    L = m;
+  }
+  return t;
+}
+
 std::vector<double2> twiddles(int n) {
   std::vector<double2> t(n);
   const long double pi = 3.141592653589793238462643383279502884L;
@@ -318,8 +335,12 @@ void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2row
   xa.M = P->M;
   xa.Nz = N;
   xa.k0 = (float)P->k0;
+  xa.iptw = P->iptwM32.as<float2>();
+  xa.niptw = (int)(P->iptwM32.bytes / sizeof(float2));
   timed(P, "x_fft_products", [&] {
-    if (P->xrows == 2)
+    if (P->xrows == 3)
+      launch_xprod32_ip(xa, P->st);  // transforms in place (DIF / DIT)
+    else if (P->xrows == 2)
       launch_xprod32_b(xa, P->st);  // transforms batched through shared passes
     else
       launch_xprod32(xa, P->st);
@@ -376,8 +397,12 @@ void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
   xa.M = P->M;
   xa.Nz = N;
   xa.k0 = P->k0;
+  xa.iptw = P->iptwM.as<double2>();
+  xa.niptw = (int)(P->iptwM.bytes / sizeof(double2));
   timed(P, "x_fft_products", [&] {
-    if (P->xrows == 2)
+    if (P->xrows == 3)
+      launch_xprod_ip(xa, P->st);  // transforms in place (DIF / DIT)
+    else if (P->xrows == 2)
       launch_xprod_b(xa, P->st);  // transforms batched through shared passes
     else
       launch_xprod(xa, P->st);
@@ -677,11 +702,15 @@ void tb::plan_launch_steps(tb_plan* P, double dt, int nsteps, cudaStream_t s, in
   }
 }
 
-// The batched 2D x-products kernel fits shared memory (F64 or the FP32 form of
-// a mixed plan).
-static bool xprod2d_batched_fits(const tb_plan* P) {
-  if (P->mixed) return xprod32_b_fits(P->M, (int)(P->ptwM32.bytes / sizeof(float2)));
-  return xprod_b_fits(P->M, (int)(P->ptwM.bytes / sizeof(double2)));
+// The 2D x-products kernel of form 2 (batched, ping-pong) or 3 (batched, in
+// place) fits shared memory (F64, or the FP32 kernel of a mixed plan).
+static bool xprod2d_form_fits(const tb_plan* P, int form) {
+  if (form == 1) return true;
+  if (P->mixed)
+    return form == 2 ? xprod32_b_fits(P->M, (int)(P->ptwM32.bytes / sizeof(float2)))
+                     : xprod32_ip_fits(P->M, (int)(P->iptwM32.bytes / sizeof(float2)));
+  return form == 2 ? xprod_b_fits(P->M, (int)(P->ptwM.bytes / sizeof(double2)))
+                   : xprod_ip_fits(P->M, (int)(P->iptwM.bytes / sizeof(double2)));
 }
 
 bool tb::plan_tau_parts_ok(const tb_plan* P, int parts) {
@@ -712,8 +741,8 @@ void tb::plan_set_variant(tb_plan* P, int tau_parts, int xrows) {
     if (P->ndim == 3)
       TB_REQUIRE(rbc3d_xrows_ok(P, xrows), TB_ENOTSUPPORTED, "x-pass rows must be 1, 2 or 4 and fit");
     else
-      TB_REQUIRE(xrows == 1 || (xrows == 2 && xprod2d_batched_fits(P)), TB_ENOTSUPPORTED,
-                 "2D x-products form must be 1 (per field) or 2 (batched) and fit");
+      TB_REQUIRE(xrows >= 1 && xrows <= 3 && xprod2d_form_fits(P, xrows), TB_ENOTSUPPORTED,
+                 "2D x-products form must be 1 (per field), 2 (batched) or 3 (batched in place) and fit");
     TB_CUDA_TRY(cudaStreamSynchronize(P->st));
     P->xrows = xrows;
     changed = true;
@@ -1001,10 +1030,9 @@ void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, i
   for (int b = 1; b < B; ++b)
     TB_REQUIRE(descs[b].ndim == 2 && descs[0].ndim == 2 && descs[b].Nx == descs[0].Nx && descs[b].Nz == descs[0].Nz &&
                    descs[b].Lx == descs[0].Lx && descs[b].Lz == descs[0].Lz &&
-                   descs[b].timestepper == descs[0].timestepper && descs[b].precision == TB_PREC_F64 &&
-                   descs[0].precision == TB_PREC_F64 && descs[b].b_bottom == descs[0].b_bottom &&
-                   descs[b].b_top == descs[0].b_top,
-               TB_EINVAL, "stacked instances must share the 2D shape, walls and stepper (FP64)");
+                   descs[b].timestepper == descs[0].timestepper && descs[b].precision == descs[0].precision &&
+                   descs[b].b_bottom == descs[0].b_bottom && descs[b].b_top == descs[0].b_top,
+               TB_EINVAL, "stacked instances must share the 2D shape, walls, stepper and precision");
     validate_desc(desc);
     TB_CUDA_TRY(cudaSetDevice(ctx->device));
     P->ctx = ctx;
@@ -1079,6 +1107,7 @@ void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, i
     upload(P->s3, cm.s3);
     upload(P->twM, twiddles(P->M));
     upload(P->ptwM, pass_twiddles(P->fpM));
+    upload(P->iptwM, ip_twiddles(P->fpM));
     upload(P->twN, twiddles(P->Nx));
     P->mixed = desc->precision == TB_PREC_MIXED;
     if (P->mixed) {
@@ -1099,6 +1128,10 @@ void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, i
       std::vector<float2> pt32(pt.size());
       for (size_t i = 0; i < pt.size(); ++i) pt32[i] = make_float2((float)pt[i].x, (float)pt[i].y);
       upload(P->ptwM32, pt32);
+      const std::vector<double2> it = ip_twiddles(P->fpM);
+      std::vector<float2> it32(it.size());
+      for (size_t i = 0; i < it.size(); ++i) it32[i] = make_float2((float)it[i].x, (float)it[i].y);
+      upload(P->iptwM32, it32);
       TB_REQUIRE(xprod32_smem_bytes(P->M, (int)pt32.size()) <= 227 * 1024, TB_ENOTSUPPORTED,
                  "Nx too large for the FP32 x kernel");
       TB_CUDA_TRY(set_mixed_smem_limits(227 * 1024));
@@ -1450,8 +1483,8 @@ tb_status tb_plan_tune(tb_plan* P, double dt, int trial_steps, int* tau_parts, i
       for (int r : {1, 2, 4})
         if (rbc3d_xrows_ok(P, r)) rows_c.push_back(r);
     } else {
-      rows_c.push_back(1);  // per-field x products
-      if (xprod2d_batched_fits(P)) rows_c.push_back(2);  // batched
+      for (int form : {1, 2, 3})  // per field, batched, batched in place
+        if (xprod2d_form_fits(P, form)) rows_c.push_back(form);
     }
     float best = 1e30f;
     int bp = P->sys[0].tau_parts, br = P->xrows;

@@ -511,5 +511,205 @@ __host__ __device__ inline int pass_twiddle_count(const FftPlan& fp) {
   return c;
 }
 
+// ---------------------------------------------------------------------------
+// In-place mixed-radix passes over NA arrays (Ms apart), without a ping-pong
+// buffer: decimation in frequency (natural order in, digit-reversed order
+// out) and decimation in time (digit-reversed in, natural out) over the same
+// radix sequence R_0 .. R_{S-1}.  Pass s works on blocks of L_s = n / (R_0 ...
+// R_{s-1}) entries with butterfly stride m_s = L_s / R_s; each butterfly reads
+// and writes the same R entries, so a pass needs one barrier.  A DIF inverse
+// transform, a pointwise product and a DIT forward transform give the natural
+// order result without any permutation pass (the digit reversal cancels).
+// Twiddles: per pass s, exp(-2 pi i j / L_s) for j < m_s (ip_twiddle_count
+// entries, the passes one after another); sign > 0 conjugates them.
+// ---------------------------------------------------------------------------
+template <int R, bool SW, bool DIF, class C>
+__device__ __forceinline__ void pass_ip(C* __restrict__ buf, int NA, int Ms, int n, int L,
+                                        const C* __restrict__ pt, int sign) {
+  const int m = L / R, nb = n / R, total = NA * nb;
+  for (int item = threadIdx.x; item < total; item += blockDim.x) {
+    const int arr = item / nb, b = item - arr * nb;
+    C* x = buf + (size_t)arr * Ms;
+    const int block = b / m, j = b - block * m;
+    const int base = block * L + j;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = x[fidx<SW>(base + r * m)];
+    if constexpr (DIF) {
+      dft_small<R>(v, sign);
+      if (m > 1) {
+        C w1 = pt[j];
+        if (sign > 0) w1.y = -w1.y;
+        twiddle_apply<R>(v, w1);
+      }
+    } else {
+      if (m > 1) {
+        C w1 = pt[j];
+        if (sign > 0) w1.y = -w1.y;
+        twiddle_apply<R>(v, w1);
+      }
+      dft_small<R>(v, sign);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[fidx<SW>(base + r * m)] = v[r];
+  }
+}
+
+template <bool SW, bool DIF, class C>
+__device__ __forceinline__ void pass_ip_r(int R, C* buf, int NA, int Ms, int n, int L, const C* pt, int sign) {
+  if (R == 8)
+    pass_ip<8, SW, DIF>(buf, NA, Ms, n, L, pt, sign);
+  else if (R == 4)
+    pass_ip<4, SW, DIF>(buf, NA, Ms, n, L, pt, sign);
+  else if (R == 2)
+    pass_ip<2, SW, DIF>(buf, NA, Ms, n, L, pt, sign);
+  else
+    pass_ip<3, SW, DIF>(buf, NA, Ms, n, L, pt, sign);
+}
+
+// DIF: natural order in, digit-reversed out (in place)
+template <bool SW, class C>
+__device__ void fft_ip_dif(C* buf, int NA, int Ms, const FftPlan& fp, const C* __restrict__ pt, int sign) {
+  int L = fp.n;
+  for (int s = 0; s < fp.nstages; ++s) {
+    const int R = fp.radix[s];
+    pass_ip_r<SW, true>(R, buf, NA, Ms, fp.n, L, pt, sign);
+    __syncthreads();
+    pt += L / R;
+    L /= R;
+  }
+}
+
+// DIT: digit-reversed order in (as fft_ip_dif leaves it), natural out (in place)
+template <bool SW, class C>
+__device__ void fft_ip_dit(C* buf, int NA, int Ms, const FftPlan& fp, const C* __restrict__ pt, int sign) {
+  for (int s = fp.nstages - 1; s >= 0; --s) {
+    int L = fp.n, off = 0;  // block length and twiddle offset of pass s
+    for (int t = 0; t < s; ++t) {
+      off += L / fp.radix[t];
+      L /= fp.radix[t];
+    }
+    pass_ip_r<SW, false>(fp.radix[s], buf, NA, Ms, fp.n, L, pt + off, sign);
+    __syncthreads();
+  }
+}
+
+__host__ __device__ inline int ip_twiddle_count(const FftPlan& fp) {
+  int L = fp.n, c = 0;
+  for (int s = 0; s < fp.nstages; ++s) {
+    c += L / fp.radix[s];
+    L /= fp.radix[s];
+  }
+  return c;
+}
+
+// Row advection products with the transforms in place (k_xprod's arithmetic,
+// batched): per grid row z (and stacked instance y) the velocity spectrum and
+// the three gradient spectra are built from one read of the six half-plane
+// inputs, transformed to the padded grid together by DIF passes (results in
+// digit-reversed order), multiplied pointwise, and the two product spectra
+// go back by DIT passes into natural order for the truncation.  Shared
+// memory: four arrays of the padded length and the in-place twiddles, so two
+// CTAs share an SM at the 1536-point length in FP64.  Args: XProdArgs-like
+// (ev, ov, ed, od, out, iptw, fp, Nx, Nk, M, Nz, k0, ld, instances).
+template <int NT, class C, class Args>
+__global__ void __launch_bounds__(NT, NT == 256 ? 2 : 1) k_xprod_ip(Args a) {
+  using Rt = typename Real<C>::type;
+  extern __shared__ __align__(16) unsigned char xip_raw[];
+  C* sm = reinterpret_cast<C*>(xip_raw);
+  const int M = a.M, N = a.Nx, Nk = a.Nk;
+  const int Ms = (M + 7) & ~7;
+  C* A = sm;
+  C* tw = sm + 4 * Ms;
+  const int hN = N / 2;
+  for (int t = threadIdx.x; t < a.niptw; t += blockDim.x) tw[t] = a.iptw[t];
+  const int z = blockIdx.x;
+  const int zm = a.Nz - 1 - z;
+  const bool lower = z <= zm;
+  const size_t ld = a.ld > 0 ? (size_t)a.ld : (size_t)Nk, col0 = (size_t)blockIdx.y * Nk;
+  const size_t rr = (size_t)(lower ? z : zm) * ld + col0;
+  auto hbin = [&](C v, int q) -> C {
+    if (q == 0) return mk<C>(v.x, Rt(0));
+    if (q == hN) return mk<C>(Rt(0.5) * v.x, Rt(0));
+    return v;
+  };
+  auto put2 = [&](C* dst, int q, C P, C Q) {  // spectrum of P + i Q (half spectra) on M points
+    dst[fidx<true>(q)] = mk<C>(P.x - Q.y, P.y + Q.x);
+    if (q > 0) dst[fidx<true>(M - q)] = mk<C>(P.x + Q.y, -P.y + Q.x);
+  };
+  for (int q = threadIdx.x; q <= hN; q += blockDim.x) {
+    C g[3], d[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const C e = a.ev[f][rr + q], o = a.ov[f][rr + q];
+      const C ed = a.ed[f][rr + q], od = a.od[f][rr + q];
+      g[f] = lower ? mk<C>(e.x + o.x, e.y + o.y) : mk<C>(e.x - o.x, e.y - o.y);
+      d[f] = lower ? mk<C>(ed.x + od.x, ed.y + od.y) : mk<C>(od.x - ed.x, od.y - ed.y);
+    }
+    put2(A, q, hbin(g[1], q), hbin(g[2], q));
+    const Rt kk = a.k0 * (Rt)q;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      C Ax = mk<C>(Rt(0), Rt(0));
+      if (q > 0 && q < hN) Ax = mk<C>(-kk * g[f].y, kk * g[f].x);  // i k g
+      put2(A + (size_t)(1 + f) * Ms, q, Ax, hbin(d[f], q));
+    }
+  }
+  for (int k = hN + 1 + threadIdx.x; k < M - hN; k += blockDim.x)  // bins N/2 < k < M - N/2 are zero
+#pragma unroll
+    for (int arr = 0; arr < 4; ++arr) A[(size_t)arr * Ms + fidx<true>(k)] = mk<C>(Rt(0), Rt(0));
+  __syncthreads();
+  fft_ip_dif<true>(A, 4, Ms, a.fp, tw, +1);
+  // products at every (permuted) grid point: (b + i ux) into array 0, uz into array 1
+  for (int p = threadIdx.x; p < M; p += blockDim.x) {
+    const int ps = fidx<true>(p);
+    const C u = A[ps];
+    Rt pr[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const C gg = A[(size_t)(1 + f) * Ms + ps];
+      pr[f] = -(u.x * gg.x + u.y * gg.y);
+    }
+    A[ps] = mk<C>(pr[0], pr[1]);
+    A[(size_t)Ms + ps] = mk<C>(pr[2], Rt(0));
+  }
+  __syncthreads();
+  fft_ip_dit<true>(A, 2, Ms, a.fp, tw, -1);
+  const C* C1 = A;
+  const C* C2 = A + Ms;
+  const Rt sc = Rt(1) / ((Rt)M * (Rt)N);
+  const size_t ro = (size_t)z * ld + col0;
+  for (int k = threadIdx.x; k < Nk; k += blockDim.x) {
+    const C c = C1[fidx<true>(k)];
+    const C cm = C1[fidx<true>((M - k) % M)];
+    const C sb = mk<C>(Rt(0.5) * (c.x + cm.x), Rt(0.5) * (c.y - cm.y));
+    const C su = mk<C>(Rt(0.5) * (c.y + cm.y), Rt(-0.5) * (c.x - cm.x));
+    const C c2 = C2[fidx<true>(k)];
+    C ob, ou, oz;
+    if (k == 0) {
+      ob = mk<C>(sb.x * sc, Rt(0));
+      ou = mk<C>(su.x * sc, Rt(0));
+      oz = mk<C>(c2.x * sc, Rt(0));
+    } else if (k == hN) {
+      ob = mk<C>(Rt(2) * sb.x * sc, Rt(0));
+      ou = mk<C>(Rt(2) * su.x * sc, Rt(0));
+      oz = mk<C>(Rt(2) * c2.x * sc, Rt(0));
+    } else {
+      ob = mk<C>(sb.x * sc, sb.y * sc);
+      ou = mk<C>(su.x * sc, su.y * sc);
+      oz = mk<C>(c2.x * sc, c2.y * sc);
+    }
+    a.out[0][ro + k] = ob;
+    a.out[1][ro + k] = ou;
+    a.out[2][ro + k] = oz;
+  }
+}
+
+template <class C>
+inline size_t xprod_ip_smem_bytes(int M, int niptw) {
+  const size_t Ms = (size_t)((M + 7) & ~7);
+  return (4 * Ms + (size_t)niptw) * sizeof(C);
+}
+
 }  // namespace fftg
 }  // namespace tb

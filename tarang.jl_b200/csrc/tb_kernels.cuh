@@ -67,8 +67,12 @@ struct XProdArgs32 {
   float k0;
   int ld;         // row stride of the planes (Nk, or instances x Nk in a stacked plan)
   int instances;  // instances stacked along the mode axis (grid.y)
+  const float2* iptw;  // in-place (DIF/DIT) FP32 twiddles of the length-M plan
+  int niptw;
 };
 void launch_xprod32(const XProdArgs32& a, cudaStream_t st);
+void launch_xprod32_ip(const XProdArgs32& a, cudaStream_t st);  // transforms in place (fftg::k_xprod_ip)
+bool xprod32_ip_fits(int M, int niptw);
 void launch_xprod32_b(const XProdArgs32& a, cudaStream_t st);  // transforms batched (as launch_xprod_b)
 bool xprod32_b_fits(int M, int nptw);
 size_t xprod32_smem_bytes(int M, int nptw);
@@ -89,8 +93,14 @@ struct XProdArgs {
   double k0;             // 2 pi / Lx
   int ld;                // row stride of the planes (Nk, or instances x Nk in a batched plan)
   int instances;         // instances stacked along the mode axis (grid.y)
+  const double2* iptw;   // in-place (DIF/DIT) twiddles of the length-M plan (fftg::ip_twiddle_count)
+  int niptw;
 };
 void launch_xprod(const XProdArgs& a, cudaStream_t st);
+// The same products with the transforms in place: DIF inverse passes,
+// pointwise products, DIT forward passes (four arrays of shared memory).
+void launch_xprod_ip(const XProdArgs& a, cudaStream_t st);
+bool xprod_ip_fits(int M, int niptw);
 size_t xprod_smem_bytes(int M, int Nk, int nptw);
 // The same products with the inverse and forward transforms batched through
 // shared passes (two 4-array blocks of shared memory).

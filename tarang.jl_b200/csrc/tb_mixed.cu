@@ -396,6 +396,12 @@ size_t xprod32_smem_bytes(int M, int nptw) {
 cudaError_t set_mixed_smem_limits(int bytes) {
   cudaError_t e = cudaFuncSetAttribute(k_xprod32, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(F::k_xprod_ip<256, float2, XProdArgs32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           bytes);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(F::k_xprod_ip<512, float2, XProdArgs32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           bytes);
+  if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_xprod32_b<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_xprod32_b<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -411,6 +417,17 @@ size_t xprod32_b_smem_bytes(int M, int nptw) {
 }
 
 bool xprod32_b_fits(int M, int nptw) { return xprod32_b_smem_bytes(M, nptw) <= 227 * 1024; }
+
+bool xprod32_ip_fits(int M, int niptw) { return F::xprod_ip_smem_bytes<float2>(M, niptw) <= 227 * 1024; }
+
+void launch_xprod32_ip(const XProdArgs32& a, cudaStream_t st) {
+  const size_t smem = F::xprod_ip_smem_bytes<float2>(a.M, a.niptw);
+  const dim3 grid(a.Nz, a.instances > 0 ? a.instances : 1);
+  if (2 * smem <= 227 * 1024)
+    F::k_xprod_ip<256, float2, XProdArgs32><<<grid, 256, smem, st>>>(a);
+  else
+    F::k_xprod_ip<512, float2, XProdArgs32><<<grid, 512, smem, st>>>(a);
+}
 
 void launch_xprod32_b(const XProdArgs32& a, cudaStream_t st) {
   const size_t smem = xprod32_b_smem_bytes(a.M, a.nptw);

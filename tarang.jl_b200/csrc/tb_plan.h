@@ -181,9 +181,9 @@ struct tb_plan {
   FftPlan fpNy{};
   DevBuf ptwNy, tmp3;
   int xrows = 1;  // padded y rows per x-pass CTA (a tuned shape)
-  bool tc32 = true;  // mixed precision: FP32 transform GEMMs on the tensor cores (when the shapes fit)
+  bool tc32 = false;  // mixed precision: FP32 transform GEMMs on the tensor cores (opt-in: the SIMT kernel is faster at these sizes)
   // transform constants
-  DevBuf bwd, fwd, s3, twM, twN, ptwM;
+  DevBuf bwd, fwd, s3, twM, twN, ptwM, iptwM;
   // parity halves of the Chebyshev matrices (H = ceil(Nz/2) rows/cols)
   DevBuf bEv, bOv, bEd, bOd, fE, fO, sfE, sfO;
   int Hz = 0, Ke = 0, Ko = 0;  // Hz = ceil(Nz/2)
@@ -217,7 +217,7 @@ struct tb_plan {
   int kernels_per_step = 0;
   // mixed precision (TB_PREC_MIXED): FP32 copies for the RHS program
   bool mixed = false;
-  DevBuf X32, G32, H32, bEv32, bOv32, bEd32, bOd32, fE32, fO32, sfE32, sfO32, ptwM32;
+  DevBuf X32, G32, H32, bEv32, bOv32, bEd32, bOd32, fE32, fO32, sfE32, sfO32, ptwM32, iptwM32;
   // profiling: eager launches bracketed by events, accumulated per kernel name
   bool profiling = false;
   struct ProfRec {

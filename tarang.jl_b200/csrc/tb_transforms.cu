@@ -12,6 +12,7 @@
 //     (src/core/nonlinear/nonlinear_padding.jl:103-108,182-226,294-346,359-443)
 #include <cuda_runtime.h>
 
+#include "tb_fft.cuh"
 #include "tb_kernels.cuh"
 
 namespace tb {
@@ -898,6 +899,12 @@ cudaError_t set_transform_smem_limits(int bytes) {
     return e;
   if ((e = cudaFuncSetAttribute(k_xprod_b<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
+  if ((e = cudaFuncSetAttribute(fftg::k_xprod_ip<256, double2, XProdArgs>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                bytes)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(fftg::k_xprod_ip<512, double2, XProdArgs>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                bytes)) != cudaSuccess)
+    return e;
   if ((e = cudaFuncSetAttribute(k_x_rfft, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_x_irfft, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_x_dealias_mul, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -920,6 +927,17 @@ size_t xprod_b_smem_bytes(int M, int nptw) {
 }
 
 bool xprod_b_fits(int M, int nptw) { return xprod_b_smem_bytes(M, nptw) <= 227 * 1024; }
+
+bool xprod_ip_fits(int M, int niptw) { return fftg::xprod_ip_smem_bytes<double2>(M, niptw) <= 227 * 1024; }
+
+void launch_xprod_ip(const XProdArgs& a, cudaStream_t st) {
+  const size_t smem = fftg::xprod_ip_smem_bytes<double2>(a.M, a.niptw);
+  const dim3 grid(a.Nz, a.instances > 0 ? a.instances : 1);
+  if (2 * smem <= 227 * 1024)  // two CTAs of 256 threads per SM while both fit
+    fftg::k_xprod_ip<256, double2, XProdArgs><<<grid, 256, smem, st>>>(a);
+  else
+    fftg::k_xprod_ip<512, double2, XProdArgs><<<grid, 512, smem, st>>>(a);
+}
 
 void launch_xprod_b(const XProdArgs& a, cudaStream_t st) {
   const size_t smem = xprod_b_smem_bytes(a.M, a.nptw);

@@ -61,24 +61,26 @@ def test_batched_x_products_match_golden_rhs(tb, golden_dir, key):
     p = RBCParams(Nx=Nx, Nz=Nz)  # the fixture's parameters (Lx 4, Lz 1)
     dom = tb.ChannelDomain(Nx, Nz, Lx=p.Lx, Lz=p.Lz)
     outs = {}
-    for form in (1, 2):
+    for form in (1, 2, 3):
         plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 0)
         plan.set_variant(xrows=form)
         assert plan.variant()[1] == form
         outs[form] = plan.rhs_advection(*(d[f"rhs_in{i}_{key}"] for i in range(3)))
         for i in range(3):
             assert rel_l2(outs[form][i], d[f"rhs_out{i}_{key}"]) < 1e-12
-    for a, b in zip(outs[1], outs[2]):
-        assert rel_l2(a, b) < 1e-14
+    for form in (2, 3):
+        for a, b in zip(outs[1], outs[form]):
+            assert rel_l2(a, b) < 1e-14
 
 
+@pytest.mark.parametrize("form", [2, 3])
 @pytest.mark.parametrize("scheme,ts", [("RK443", 1), ("SBDF2", 3)])
-def test_batched_x_products_steps_match_oracle(tb, scheme, ts):
+def test_batched_x_products_steps_match_oracle(tb, scheme, ts, form):
     p = RBCParams(Nx=256, Nz=64, Lx=4.0, Lz=1.0, Ra=1e8)
     sim = run_rbc(p, scheme, 0.01, 4, seed=42)
     dom = tb.ChannelDomain(256, 64, Lx=4.0, Lz=1.0)
     plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, ts)
-    plan.set_variant(xrows=2)
+    plan.set_variant(xrows=form)
     plan.set_state(0, forward_2d(rbc_initial_b(p, 42)))
     plan.step(0.01, 4)
     for f, want in ((0, sim.b), (1, sim.ux), (2, sim.uz)):
@@ -95,13 +97,14 @@ def test_batched_x_products_mixed_precision(tb):
     p = RBCParams(Nx=Nx, Nz=Nz)
     dom = tb.ChannelDomain(Nx, Nz, Lx=p.Lx, Lz=p.Lz)
     outs = {}
-    for form in (1, 2):
+    for form in (1, 2, 3):
         plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 0, precision=tb._lib.TB_PREC_MIXED)
         plan.set_variant(xrows=form)
         outs[form] = plan.rhs_advection(*ins)
     ref = RBC2D(p).rhs(*ins)
-    for a, b, r in zip(outs[1], outs[2], ref):
-        assert rel_l2(b, a) < 1e-6 and rel_l2(b, r) < 1e-5
+    for form in (2, 3):
+        for a, b, r in zip(outs[1], outs[form], ref):
+            assert rel_l2(b, a) < 1e-6 and rel_l2(b, r) < 1e-5
 
 
 def test_xpass_rows_and_tau_partitions_agree_in_3d(tb):
@@ -133,7 +136,7 @@ def test_plan_tune_keeps_state_and_picks_a_feasible_shape(tb):
     plan.step(0.02, 2)
     before = [plan.get_state(f) for f in (0, 1, 2)]
     parts, rows = plan.tune(0.02, trial_steps=3)
-    assert parts in (1, 4, 8) and rows in (1, 2) and plan.variant() == (parts, rows)
+    assert parts in (1, 4, 8) and rows in (1, 2, 3) and plan.variant() == (parts, rows)
     for f, b in zip((0, 1, 2), before):
         assert np.array_equal(plan.get_state(f), b)
     plan.step(0.02, 2)  # steps on with the chosen shape
