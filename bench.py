@@ -48,7 +48,9 @@ def parse_args():
                     help="tau-solve partitions of the headline plan (0: chosen by the plan's tuner)")
     ap.add_argument("--precision", choices=["f64", "mixed"], default="f64",
                     help="arithmetic of the headline plan (mixed: FP32 transforms and products, FP64 tau LU)")
-    ap.add_argument("--x-form", type=int, default=0, choices=[0, 1, 2],
+    ap.add_argument("--tensor-cores", action="store_true",
+                    help="mixed headline plan: transform GEMMs on the tcgen05 tensor cores (TF32)")
+    ap.add_argument("--x-form", type=int, default=0, choices=[0, 1, 2, 3],
                     help="x-products kernel of the headline plan: 1 per field, 2 batched (0: the tuner's choice; "
                          "with --tau-parts the plan's default, 1)")
     ap.add_argument("--cpu-steps", type=int, default=10,
@@ -405,6 +407,8 @@ def run_ours(args, cfg, scheme, dist):
 
     plan = tb.Plan(dom, cfg.kappa, cfg.nu, cfg.Lz, 0.0, ts,
                    precision=TB_PREC_MIXED if args.precision == "mixed" else TB_PREC_F64)
+    if args.tensor_cores:
+        plan.set_gemm_path(True)
     b0 = plan.forward(W.rbc_initial_grid(cfg))
     plan.set_state(TB_FIELD_B, b0)
 

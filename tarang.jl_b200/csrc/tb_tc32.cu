@@ -8,6 +8,11 @@
 // B[2k + par] (parity), B[j] + sgn B[N-1-j] (mirror, output row 2r + par).
 //
 // One CTA of 4 warps owns one item and a strided set of 64-column tiles.
+// Operands are split into TF32 hi/lo while they are staged: A rows as float4
+// chunks, B as four K-consecutive values of one column per thread, each
+// written as one 16-byte swizzled chunk (the eight lanes of a shared-memory
+// phase hit eight distinct chunks: no bank conflicts).  The accumulator goes
+// back through shared memory so the global stores are row-contiguous.
 // Shared memory (1024-byte aligned, the 128-byte swizzle's period):
 //   A_hi, A_lo: 128 x 128 TF32, K-major, 128-byte swizzle, loaded once;
 //   B_hi, B_lo:  64 x 128 TF32, K-major, 128-byte swizzle, one tile at a time.
@@ -67,11 +72,12 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
   return r;
 }
 
-__device__ __forceinline__ void split_store(uint8_t* base_hi, uint8_t* base_lo, uint32_t off, float v) {
-  const uint32_t hi = to_tf32(v);
-  const float lo = v - __uint_as_float(hi);
-  *reinterpret_cast<uint32_t*>(base_hi + off) = hi;
-  *reinterpret_cast<uint32_t*>(base_lo + off) = to_tf32(lo);
+__device__ __forceinline__ void split_store4(uint8_t* base_hi, uint8_t* base_lo, uint32_t off, float4 v) {
+  const uint32_t h0 = to_tf32(v.x), h1 = to_tf32(v.y), h2 = to_tf32(v.z), h3 = to_tf32(v.w);
+  *reinterpret_cast<uint4*>(base_hi + off) = make_uint4(h0, h1, h2, h3);
+  *reinterpret_cast<uint4*>(base_lo + off) =
+      make_uint4(to_tf32(v.x - __uint_as_float(h0)), to_tf32(v.y - __uint_as_float(h1)),
+                 to_tf32(v.z - __uint_as_float(h2)), to_tf32(v.w - __uint_as_float(h3)));
 }
 
 __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
@@ -121,11 +127,25 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
   }
-  // A once: rows >= M and columns >= K are zero (they meet zero B rows)
-  for (int idx = tid; idx < kTcM * kTcK; idx += kTcThreads) {
-    const int r = idx / kTcK, k = idx % kTcK;
-    const float v = (r < Mo && k < K) ? A[(size_t)r * Kp + k] : 0.f;
-    split_store(sm + kOffAhi, sm + kOffAlo, sw128_off(r, k, kTcM), v);
+  // A once, four K-consecutive values per thread and step (Kpad is a multiple
+  // of 16 and the padding columns are zero); rows >= M are zero
+  // (eight loads in flight per thread before any is split and stored)
+  constexpr int AQ = kTcM * (kTcK / 4) / kTcThreads, AB = 8;  // float4 per thread, per batch
+  static_assert(AQ % AB == 0, "A batches");
+  for (int q0 = 0; q0 < AQ; q0 += AB) {
+    float4 v[AB];
+#pragma unroll
+    for (int i = 0; i < AB; ++i) {
+      const int idx = tid + (q0 + i) * kTcThreads;
+      const int r = idx / (kTcK / 4), k = 4 * (idx % (kTcK / 4));
+      v[i] = (r < Mo && k < Kp) ? *reinterpret_cast<const float4*>(A + (size_t)r * Kp + k)
+                                : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int i = 0; i < AB; ++i) {
+      const int idx = tid + (q0 + i) * kTcThreads;
+      split_store4(sm + kOffAhi, sm + kOffAlo, sw128_off(idx / (kTcK / 4), 4 * (idx % (kTcK / 4)), kTcM), v[i]);
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
   __syncthreads();
@@ -136,26 +156,39 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int
   bool ok = true;
   for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
     const int n0 = t * kTcN;
-    // B' tile, two columns per thread and step: rows k (mapped), columns n0..n0+63
-    for (int idx = tid; idx < kTcK * (kTcN / 2); idx += kTcThreads) {
-      const int k = idx / (kTcN / 2), n = 2 * (idx % (kTcN / 2));
-      const int gc = n0 + n;
-      float2 v = make_float2(0.f, 0.f);
-      if (k < K && gc < ncol) {
-        const int srow = mode == GEMM_PARITY ? 2 * k + par : k;
-        v = *reinterpret_cast<const float2*>(B + (size_t)srow * ldb + gc);
-        if (mirror) {
-          if (k == midk) {
-            if (par) v = make_float2(0.f, 0.f);
-          } else {
-            const float2 w = *reinterpret_cast<const float2*>(B + (size_t)(Nrows - 1 - k) * ldb + gc);
-            v = make_float2(fmaf(sgn, w.x, v.x), fmaf(sgn, w.y, v.y));
+    // B' tile: thread (column n, K-chunk kc) loads rows 4 kc .. 4 kc + 3 of
+    // column n0 + n (the lanes of a warp read consecutive columns of one row)
+    {
+      const int n = tid % kTcN, gc = n0 + n;
+      const bool colok = gc < ncol;
+      constexpr int KCS = kTcThreads / kTcN;       // K-chunks started per step (2)
+      constexpr int NKC = kTcK / 4 / KCS;          // K-chunks per thread (16)
+      constexpr int CB = 4;                        // chunks per batch: 16 loads in flight
+      static_assert(NKC % CB == 0, "B batches");
+      for (int c0 = 0; c0 < NKC; c0 += CB) {
+        float e[CB][4], w[CB][4];
+#pragma unroll
+        for (int c = 0; c < CB; ++c)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int k = 4 * (tid / kTcN + (c0 + c) * KCS) + i;
+            const bool ok = colok && k < K;
+            const int srow = mode == GEMM_PARITY ? 2 * k + par : k;
+            e[c][i] = ok ? B[(size_t)srow * ldb + gc] : 0.f;
+            w[c][i] = (ok && mirror && k != midk) ? B[(size_t)(Nrows - 1 - k) * ldb + gc] : 0.f;
           }
+#pragma unroll
+        for (int c = 0; c < CB; ++c) {
+          const int kc = tid / kTcN + (c0 + c) * KCS;
+          float f[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int k = 4 * kc + i;
+            f[i] = mirror ? ((k == midk) ? (par ? 0.f : e[c][i]) : fmaf(sgn, w[c][i], e[c][i])) : e[c][i];
+          }
+          split_store4(sm + kOffBhi, sm + kOffBlo, sw128_off(n, 4 * kc, kTcN), make_float4(f[0], f[1], f[2], f[3]));
         }
-        if (gc + 1 >= ncol) v.y = 0.f;
       }
-      split_store(sm + kOffBhi, sm + kOffBlo, sw128_off(n, k, kTcN), v.x);
-      split_store(sm + kOffBhi, sm + kOffBlo, sw128_off(n + 1, k, kTcN), v.y);
     }
     // generic-proxy stores -> visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -190,7 +223,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int
     }
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
     const int r = warp * 32 + lane;  // accumulator lane = output row of this thread
-    const int orow = mirror ? 2 * r + par : r;
+    OutT* stage = reinterpret_cast<OutT*>(sm + kOffBhi);  // [row][33]: the MMAs no longer read B
+    constexpr int SLD = 33;
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
       uint32_t v[32];
@@ -204,14 +238,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int
             "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-      if (r < Mo) {
-        OutT* C = reinterpret_cast<OutT*>(it.C) + (size_t)orow * ldc;
 #pragma unroll
-        for (int c = 0; c < 32; ++c) {
-          const int gc = n0 + half * 32 + c;
-          if (gc < ncol) C[gc] = (OutT)__uint_as_float(v[c]);
+      for (int c = 0; c < 32; ++c) stage[r * SLD + c] = (OutT)__uint_as_float(v[c]);
+      __syncthreads();
+      // row-contiguous stores: a warp writes 32 consecutive columns of one row
+      for (int idx = tid; idx < kTcM * 32; idx += kTcThreads) {
+        const int rr = idx / 32, c = idx % 32;
+        const int gc = n0 + half * 32 + c;
+        if (rr < Mo && gc < ncol) {
+          const int orow = mirror ? 2 * rr + par : rr;
+          reinterpret_cast<OutT*>(it.C)[(size_t)orow * ldc + gc] = stage[rr * SLD + c];
         }
       }
+      __syncthreads();
     }
     // every warp has read the accumulator and the MMAs have read B: the next
     // tile may overwrite both
