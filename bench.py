@@ -44,7 +44,7 @@ def parse_args():
     ap.add_argument("--scheme", choices=["RK443", "RK222", "SBDF2"], default="RK443")
     ap.add_argument("--config", choices=["c2", "c1"], default="c2")
     ap.add_argument("--e2e-steps", type=int, default=20)
-    ap.add_argument("--tau-parts", type=int, default=0, choices=[0, 1, 4, 8],
+    ap.add_argument("--tau-parts", type=int, default=0, choices=[0, 1, 4, 8, 16],
                     help="tau-solve partitions of the headline plan (0: chosen by the plan's tuner)")
     ap.add_argument("--precision", choices=["f64", "mixed"], default="f64",
                     help="arithmetic of the headline plan (mixed: FP32 transforms and products, FP64 tau LU)")

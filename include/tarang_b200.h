@@ -185,10 +185,11 @@ tb_status tb_checkpoint_load(tb_plan* plan, const double* grid, int where, const
 
 /* Kernel shapes of a plan (the library's own autotuning; the reference tunes
  * FFTW plans instead, transform_fourier.jl plan cache):
- *   tau_parts  row partitions of each 4-mode group's tau solves: 8 (one per
- *              half-warp, four warps) or 4 (one per warp) - partitioned, the
- *              shortest latency for one plan - or 1 (no response records, the
- *              least device work per solve; needs npad/12 >= parts);
+ *   tau_parts  row partitions of each 4-mode group's tau solves: 16 (one
+ *              per half-warp, eight warps), 8 (one per half-warp, four
+ *              warps) or 4 (one per warp) - partitioned, the shortest
+ *              latency for one plan - or 1 (no response records, the least
+ *              device work per solve); needs npad/12 >= parts;
  *   xrows      3D: padded y rows per x-pass CTA, 1, 2 or 4; 2D (Float64
  *              and mixed plans): the x-products kernel, 1 = the three
  *              gradient transforms one after another, 2 = all inverse and

@@ -714,7 +714,7 @@ static bool xprod2d_form_fits(const tb_plan* P, int form) {
 }
 
 bool tb::plan_tau_parts_ok(const tb_plan* P, int parts) {
-  if (parts != 1 && parts != kTauParts && parts != kTauParts8) return false;
+  if (parts != 1 && parts != kTauParts && parts != kTauParts8 && parts != kTauParts16) return false;
   for (int sy = 0; sy < P->nsys; ++sy) {
     if (tau_solve_smem_bytes(P->sys[sy].npad, parts) > 227 * 1024) return false;
     if (P->sys[sy].npad / kBwdWin < parts) return false;  // every partition at least one window
@@ -725,7 +725,7 @@ bool tb::plan_tau_parts_ok(const tb_plan* P, int parts) {
 void tb::plan_set_variant(tb_plan* P, int tau_parts, int xrows) {
   bool changed = false;
   if (tau_parts > 0) {
-    TB_REQUIRE(plan_tau_parts_ok(P, tau_parts), TB_ENOTSUPPORTED, "tau solve partitions must be 1, 4 or 8 and fit");
+    TB_REQUIRE(plan_tau_parts_ok(P, tau_parts), TB_ENOTSUPPORTED, "tau solve partitions must be 1, 4, 8 or 16 and fit");
     for (int sy = 0; sy < P->nsys; ++sy) {
       TauSystem& S = P->sys[sy];
       if (S.tau_parts == tau_parts) continue;
@@ -1477,7 +1477,7 @@ tb_status tb_plan_tune(tb_plan* P, double dt, int trial_steps, int* tau_parts, i
     PlanSnapshot snap;
     plan_snapshot(P, &snap);
     std::vector<int> parts_c, rows_c;
-    for (int p : {kTauParts8, kTauParts, 1})
+    for (int p : {kTauParts16, kTauParts8, kTauParts, 1})
       if (plan_tau_parts_ok(P, p)) parts_c.push_back(p);
     if (P->ndim == 3) {
       for (int r : {1, 2, 4})

@@ -162,8 +162,12 @@ __host__ __device__ inline int tau_part_row0(int np, int P, int k, int ppw = 1) 
   const int b0 = (int)(((long long)w * pairs) / nw), b1 = (int)(((long long)(w + 1) * pairs) / nw);
   return 2 * kBwdWin * b0 + h * kBwdWin * (b1 - b0);
 }
-// Partitions per warp of the 8-partition solve (two: each half-warp sweeps one).
+// Partitions per warp of the 8- and 16-partition solves (two: each half-warp
+// sweeps one).  The 16-partition form (eight warps per group) streams its
+// records in stages of 3 rows and keeps y and the particular unknowns in
+// global scratch (prefetched with the records), so that 16 rings fit one SM.
 constexpr int kTau8PerWarp = 2;
+constexpr int kTauParts16 = 16;
 struct ClassDev {
   int n, nb, kl, ku;
   const short* row_eq;
@@ -224,8 +228,8 @@ struct TauArgs {
   double bc_toff;
   int* err_mode;       // first singular mode, or -1
 };
-// parts: kTauParts or kTauParts8 (partitioned solve, needs a.PP) or 1 (one
-// warp per group).
+// parts: kTauParts, kTauParts8 or kTauParts16 (partitioned solve, needs a.PP)
+// or 1 (one warp per group).
 // launch_tau_factor factors modes a.mode0 .. a.mode0 + a.Nkm - 1; the
 // partition responses (launch_tau_transfer) are then computed for all modes.
 void launch_tau_factor(const TauArgs& a, int parts, cudaStream_t st);

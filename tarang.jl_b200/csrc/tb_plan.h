@@ -109,7 +109,7 @@ struct TauSystem {
   DevBuf rhs_off;  // [row][class] right-hand-side codes
   std::vector<DevBuf> mband, mbord;  // stacked instances: band / border coefficients [instance][class]
   std::vector<std::unique_ptr<FactorSet>> factors;
-  int tau_parts = 1;  // partitions of the solve (kTauParts8, kTauParts or 1)
+  int tau_parts = 1;  // partitions of the solve (kTauParts16, kTauParts8, kTauParts or 1)
   int npad = 0;       // band rows padded to a multiple of kTauRowPad
 };
 
@@ -310,7 +310,7 @@ void timed(tb_plan* P, const char* name, F&& fn) {
 void rbc3d_setup(tb_plan* P);
 void rbc3d_enqueue_rhs(tb_plan* P, const double2* Xin, double2* out4);
 bool rbc3d_xrows_ok(const tb_plan* P, int rows);
-// Tunable kernel shapes of a plan: tau-solve partitions (1, kTauParts or kTauParts8, for
+// Tunable kernel shapes of a plan: tau-solve partitions (1, 4, 8 or 16, for
 // every tau system) and, in 3D, x-pass rows per CTA (1, 2, 4).  Changing one
 // drops the plan's factors and step graphs (rebuilt on the next step).
 bool plan_tau_parts_ok(const tb_plan* P, int parts);

@@ -334,30 +334,49 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// Doubles per ring stage; with one partition a backward stage also carries the
-// stage's y values (kPartRows x 4 kSolveModes), prefetched from global scratch.
+// Rows per ring stage: one forward window (6) with up to 8 partitions, half
+// of one (3) with 16, whose sixteen rings share one SM's shared memory.
+template <int P>
+__host__ __device__ constexpr int part_rows() {
+  return P > kTauParts8 ? kPartRows / 2 : kPartRows;
+}
+// With 1 and 16 partitions the y column of a group and the particular
+// unknowns live in global scratch (L2) and are prefetched with the records;
+// with 4 and 8 they stay in shared memory.
+template <int P>
+__host__ __device__ constexpr bool ys_global() {
+  return P == 1 || P > kTauParts8;
+}
+// Doubles per ring stage (the largest of the three phases): forward records
+// and right-hand sides; backward records (+ the stage's y values with y in
+// global scratch); H records (+ the stage's particular unknowns with 16).
 template <int P>
 __host__ __device__ constexpr size_t part_stage_doubles() {
-  constexpr size_t MP = kSolveModes;
-  constexpr size_t F = kPartRows * (2 * MP * kFwdRec + 2 * 2 * MP);
-  constexpr size_t B = kPartRows * (2 * MP * kBwdRec + (P == 1 ? 4 * MP : 0));
-  constexpr size_t H = kPartRows * (2 * MP * kHRec);
+  constexpr size_t MP = kSolveModes, R = part_rows<P>(), NL = 4 * MP;
+  constexpr size_t F = R * (2 * MP * kFwdRec + 2 * 2 * MP);
+  constexpr size_t B = R * (2 * MP * kBwdRec + (ys_global<P>() ? NL : 0));
+  constexpr size_t H = R * (2 * MP * kHRec + (P > kTauParts8 ? NL : 0));
   return F > B ? (F > H ? F : H) : (B > H ? B : H);
 }
-// Doubles of one warp's ring: kPartStages of the largest stage, two with 8
-// partitions (eight warps' rings and the y store share one SM's 227 KB).
+// Doubles of one partition's ring: kPartStages of the largest stage (1 and 4
+// partitions), two (8: eight rings and the y store share one SM's 227 KB),
+// two or the 12x12 Psi of the group's slots if larger (16).
 template <int P>
 __host__ __device__ constexpr size_t ring_doubles() {
+  if (P > kTauParts8) {
+    constexpr size_t b2 = 2 * part_stage_doubles<P>(), psi = 2 * kSolveModes * (kBwdWin * kBwdWin + 2);
+    return b2 > psi ? b2 : psi;
+  }
   return (P > kTauParts ? 2 : kPartStages) * part_stage_doubles<P>();
 }
 // Ring stages of each phase: the ring split into stages of that phase's
-// records.  With 1 and 4 partitions this is the fixed depth kPartStages for
-// the sweeps and six H stages; with 8 the forward records (smaller than the
-// backward ones) get three stages in the ring of two backward stages.
+// records.  Forward: as many (record, right-hand side) stage pairs as fit;
+// backward: the fixed depth kPartStages (1 and 4 partitions) or two; H: six
+// stages (1 and 4 partitions) or as many as fit.
 template <int P>
 __host__ __device__ constexpr int fwd_stages() {
-  constexpr size_t F = kPartRows * (2 * kSolveModes * kFwdRec + 2 * 2 * kSolveModes);
-  return P > kTauParts ? (int)(ring_doubles<P>() / F) : kPartStages;
+  constexpr size_t F = part_rows<P>() * (2 * kSolveModes * kFwdRec + 2 * 2 * kSolveModes);
+  return (int)(ring_doubles<P>() / F);
 }
 template <int P>
 __host__ __device__ constexpr int bwd_stages() {
@@ -365,7 +384,9 @@ __host__ __device__ constexpr int bwd_stages() {
 }
 template <int P>
 __host__ __device__ constexpr int h_stages() {
-  return P > kTauParts ? (int)(ring_doubles<P>() / (kPartRows * 2 * kSolveModes * kHRec)) : 6;
+  constexpr size_t H =
+      part_rows<P>() * (2 * kSolveModes * kHRec + (P > kTauParts8 ? 4 * kSolveModes : 0));
+  return P > kTauParts ? (int)(ring_doubles<P>() / H) : 6;
 }
 
 // X (the state planes) and the tau rows are one allocation, so a 32-bit
@@ -382,7 +403,8 @@ __device__ __forceinline__ void store_unknown(double* Xd, int code, int m, int p
 template <int KL, int KU, int P, int PPW>
 __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   static_assert(KL + 2 == kFwdWin && KL + KU == kBwdWin, "window sizes follow the band shape");
-  static_assert(kFwdWin == kPartRows && kBwdWin == 2 * kPartRows, "one forward window per stage, two stages per backward block");
+  constexpr int R = part_rows<P>();  // rows per ring stage
+  static_assert(kFwdWin % R == 0 && kBwdWin % R == 0, "whole stages per forward window and per backward block");
   static_assert(kFwdRec == KL + NBMAX + 2 && kFwdRot == kFwdRec - 1 && kFwdRec % 2 == 0,
                 "forward record: pivot, l, border, rotation flag of the entering row");
   static_assert(kBwdCode == KL + KU + 1 + NBMAX && kBwdG == kBwdCode + 1 && kBwdRec == kBwdG + 4 && kBwdRec % 2 == 0,
@@ -395,15 +417,18 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   constexpr int HREC = 2 * MP * kHRec;    // doubles per H row
   constexpr int RREC = 2 * MP;            // double2 rhs entries per row (class, mode)
   constexpr int FV = kFwdRec / 2, BV = kBwdRec / 2, HV = kHRec / 2;  // 16-byte words per record
-  constexpr int R = kPartRows;
   constexpr int NL = 4 * MP;  // distinct lanes of a partition
   constexpr int TPL = 32 / PPW;  // threads per partition (a warp, or a half-warp)
   constexpr int BSUB = 3;     // backward rows whose records are held in registers at once
   constexpr int RING = (int)ring_doubles<P>();  // doubles of one partition's ring
+  constexpr bool YG = ys_global<P>();  // y and particular unknowns in global scratch
   constexpr int NSF = fwd_stages<P>(), NSB = bwd_stages<P>(), NSH = h_stages<P>();
-  constexpr int FST = R * (FREC + 2 * RREC);                    // forward stage: records + rhs
-  constexpr int BST = R * (BREC + (P == 1 ? NL : 0));           // backward stage (+ y with one partition)
-  static_assert(NSF >= 2 && NSF * FST <= RING && NSB >= 2 && NSB * BST <= RING, "ring stages");
+  constexpr int WS = kFwdWin / R;      // ring stages per forward window
+  constexpr int KB = kBwdWin / R;      // ring stages per backward block
+  constexpr int FRS = R * FREC;        // forward stage: records,
+  constexpr int FHS = R * 2 * RREC;    // and right-hand sides (separate slots)
+  constexpr int BST = R * (BREC + (YG ? NL : 0));  // backward stage (+ y)
+  static_assert(NSF >= 2 * WS && NSF * (FRS + FHS) <= RING && NSB >= 2 && NSB * BST <= RING, "ring stages");
   static_assert(NL <= TPL && TPL % NL == 0 && P % PPW == 0 && (PPW == 1 || PPW == 2), "lane layout");
   static_assert(R % BSUB == 0, "backward sub-blocks");
   extern __shared__ __align__(16) double smem[];
@@ -423,12 +448,12 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   const int m = g * MP + mm;
   const bool live = owner && m < Nk;
   double* ring = smem + (size_t)pid * RING;
-  // [row][ln]: y, then (rows of partitions < P-1) particular x.  With one partition
-  // the group's y column lives in global scratch (written by F1 and read back
-  // by B1 of the same CTA while it is still in L2), which halves the shared
-  // memory of a CTA and doubles the resident groups per SM.
-  double* ysave = (P == 1) ? a.ysave + (size_t)g * np * NL : smem + (size_t)P * RING;
-  double* xch = smem + (size_t)P * RING + (P == 1 ? 0 : (size_t)np * NL);  // [partition][ln][kXch]
+  // [row][ln]: y, then (rows of partitions < P-1) particular x.  With 1 and 16
+  // partitions the group's column lives in global scratch (written by F1 and
+  // B1 and read back, through the rings, by B1 and B3 of the same CTA while it
+  // is still in L2), which leaves the shared memory to the rings.
+  double* ysave = YG ? a.ysave + (size_t)g * np * NL : smem + (size_t)P * RING;
+  double* xch = smem + (size_t)P * RING + (YG ? 0 : (size_t)np * NL);  // [partition][ln][kXch]
   int* rofs = reinterpret_cast<int*>(xch + (size_t)P * NL * kXch);
   // [row][class] right-hand-side code: 2 * element offset + (1 for a u_x momentum
   // row, scaled by -i on load), -1 for none
@@ -444,14 +469,22 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   // ---- F1: forward sweep over this partition's rows: y = L^-1 P r, boundary rows accumulate z ----
   double y[kFwdWin];
   double z[NBMAX];
-  auto issue_fwd = [&](int s) {  // local stage s: rows row0 + s R ..; stage nst is the first of the next partition
-    const int r0 = row0 + s * R;
-    if (s <= nst) {
-      double* dst = ring + (size_t)(s % NSF) * FST;
-      if (r0 < np)
-        for (int q = tl; q < R * FREC / 2; q += TPL) cp_async16(dst + 2 * q, FRg + (size_t)r0 * FREC + 2 * q, true);
-      // right-hand sides (zero-filled past the last row)
-      double2* rdst = reinterpret_cast<double2*>(dst + R * FREC);
+  // Ring: NSF record slots, then NSF right-hand-side slots.  Group k (k >= -WS)
+  // loads the records of stage k (0 <= k < nst) and the right-hand sides of
+  // stage k + WS (rows past the partition are the next partition's first rows,
+  // zero-filled past the last row): a window's records arrive with the
+  // right-hand sides of the rows that enter the window as it is swept.
+  auto frec = [&](int st) { return ring + (size_t)(st % NSF) * FRS; };
+  auto frhs = [&](int st) { return ring + (size_t)NSF * FRS + (size_t)(st % NSF) * FHS; };
+  auto issue_fwd = [&](int k) {
+    if (k >= 0 && k < nst) {
+      double* dst = frec(k);
+      const double* src = FRg + (size_t)(row0 + k * R) * FREC;
+      for (int q = tl; q < FRS / 2; q += TPL) cp_async16(dst + 2 * q, src + 2 * q, true);
+    }
+    if (k < nst) {
+      const int r0 = row0 + (k + WS) * R;
+      double2* rdst = reinterpret_cast<double2*>(frhs(k + WS));
       for (int q = tl; q < R * RREC; q += TPL) {
         const int r = q / RREC, cc = (q / MP) % 2, md = q % MP;
         const int mq = g * MP + md;
@@ -462,12 +495,12 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
     }
     cp_async_commit();
   };
-  // right-hand side of row r0 + u of local stage s for this lane (0 past the last row);
+  // right-hand side of row row0 + rr for this lane (0 past the last row);
   // u_x momentum rows are scaled by -i, i.e. (re, im) -> (im, -re)
-  auto rhs_at = [&](int s, int u) -> double {
-    const int j = row0 + s * R + u;
+  auto rhs_at = [&](int rr) -> double {
+    const int j = row0 + rr;
     if (j >= np) return 0.0;
-    const double* rb = ring + (size_t)(s % NSF) * FST + R * FREC + (size_t)(u * RREC + slot) * 2;
+    const double* rb = frhs(rr / R) + (size_t)((rr % R) * RREC + slot) * 2;
     const int rot = rofs[2 * j + c] & 1;
     const double v = rb[part ^ rot];
     return (rot & part) ? -v : v;
@@ -487,32 +520,33 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
     const double top = part ? fma(v1t.y, t, v0t.y) : fma(v1t.x, t, v0t.x);
     z[0] = a.beta * 0.5 * (c == 0 ? top + bot : top - bot);
   }
-  for (int s = 0; s < NSF - 1; ++s) issue_fwd(s);
-  for (int s = 0; s < nst; ++s) {
-    issue_fwd(s + NSF - 1);    // refills the slot of stage s-1
-    cp_async_wait<NSF - 2>();  // stages s and s+1 are resident
-    __syncwarp();
-    if (s == 0) {
+  for (int k = -WS; k < NSF - WS; ++k) issue_fwd(k);
+  cp_async_wait<NSF - WS>();  // groups -WS..-1: the right-hand sides of the first window
+  __syncwarp();
 #pragma unroll
-      for (int t = 0; t < kFwdWin; ++t) y[t] = rhs_at(0, t);
-    }
-    const double2* st = reinterpret_cast<const double2*>(ring + (size_t)(s % NSF) * FST + (size_t)slot * kFwdRec);
+  for (int t = 0; t < kFwdWin; ++t) y[t] = rhs_at(t);
+  __syncwarp();  // those slots are refilled next
+  for (int s = 0; s < nst; s += WS) {
+    for (int k = s + NSF - WS; k < s + NSF; ++k) issue_fwd(k);  // the previous window's slots
+    cp_async_wait<NSF - WS>();  // groups up to s + WS - 1 are resident
+    __syncwarp();
     double2 rv[kFwdWin][FV];
 #pragma unroll
-    for (int u = 0; u < kFwdWin; ++u)
+    for (int u = 0; u < kFwdWin; ++u) {
+      const double2* st =
+          reinterpret_cast<const double2*>(frec(s + u / R) + (size_t)(u % R) * FREC + (size_t)slot * kFwdRec);
 #pragma unroll
-      for (int v = 0; v < FV; ++v) rv[u][v] = st[u * (FREC / 2) + v];
-    // right-hand sides of the rows entering the window (stage s+1, zero-filled
-    // past the last row), -i applied to u_x momentum rows by the record's flag
+      for (int v = 0; v < FV; ++v) rv[u][v] = st[v];
+    }
+    // right-hand sides of the rows entering the window (zero-filled past the
+    // last row), -i applied to u_x momentum rows by the record's flag
     double incoming[kFwdWin];
-    {
-      const double* rb = ring + (size_t)((s + 1) % NSF) * FST + R * FREC + (size_t)slot * 2;
 #pragma unroll
-      for (int u = 0; u < kFwdWin; ++u) {
-        const int rot = __double2loint(rv[u][FV - 1].y);
-        const double v = rb[u * RREC * 2 + (part ^ rot)];
-        incoming[u] = (rot & part) ? -v : v;
-      }
+    for (int u = 0; u < kFwdWin; ++u) {
+      const double* rb = frhs(s + WS + u / R) + (size_t)((u % R) * RREC + slot) * 2;
+      const int rot = __double2loint(rv[u][FV - 1].y);
+      const double v = rb[part ^ rot];
+      incoming[u] = (rot & part) ? -v : v;
     }
     double* ys = ysave + (size_t)(row0 + s * R) * NL + ln;
 #pragma unroll
@@ -534,35 +568,40 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
       for (int b = 0; b < NBMAX; ++b) z[b] = fma(-rec(1 + KL + b), yj, z[b]);
       y[u] = incoming[u];
     }
-    __syncwarp();  // the slot of stage s is refilled next
+    __syncwarp();  // the window's slots are refilled next
   }
   double* myx = xch + ((size_t)pid * NL + ln) * kXch;
   // exit window minus the raw right-hand side of the next partition's first rows (the
-  // ring still holds that stage)
+  // ring still holds those right-hand sides)
 #pragma unroll
-  for (int t = 0; t < 4; ++t) myx[t] = y[t] - rhs_at(nst, t);
+  for (int t = 0; t < 4; ++t) myx[t] = y[t] - rhs_at(Lp + t);
   cp_async_wait<0>();
-  if constexpr (P == 1) __threadfence();  // y stores of all lanes reach L2 before their cp.async reloads
+  if constexpr (YG) __threadfence();  // y stores of all lanes reach L2 before their cp.async reloads
   __syncwarp();
   // The ring is free: stage the Schur inverse of the group and this partition's
-  // forward transfer data (Phi_k for k < pid, Gz_pid) while the other partitions
-  // finish their sweeps.
+  // forward transfer data while the other partitions finish their sweeps:
+  // Phi_k for k < pid and Gz_pid (up to 8 partitions: each partition composes
+  // its own starting window), or its own Phi_pid and Gz_pid (16 partitions:
+  // the windows are carried down one partition at a time).
+  constexpr bool CARRY = P > kTauParts8;
   constexpr int TRF = 32;  // Phi (16) + Gz (16) per (partition, record slot)
   // shared-memory stride of a staged (partition, slot) record: 34 doubles, so
   // that the 8 slots a warp reads at once fall in distinct banks
   constexpr int TRS = TRF + 2;
-  static_assert(2 * NBMAX * NBMAX * MP + (P - 1) * 2 * MP * TRS <= RING, "Schur inverse and Phi fit the ring");
+  static_assert(2 * NBMAX * NBMAX * MP + (CARRY ? 1 : P - 1) * 2 * MP * TRS <= RING,
+                "Schur inverse and Phi fit the ring");
   double* sSI = ring;                         // [class][4][4][mode], 2*16*MP doubles
-  double* sTR = ring + 2 * NBMAX * NBMAX * MP;  // [k-1][slot][TRS]
+  double* sTR = ring + 2 * NBMAX * NBMAX * MP;  // [k-1][slot][TRS] (carry: [slot][TRS] of Phi_pid)
   {
     const double* SIg = a.cls[0].SI + (size_t)g * 2 * NBMAX * NBMAX * MP;
     for (int q = tl; q < NBMAX * NBMAX * MP; q += TPL) cp_async16(sSI + 2 * q, SIg + 2 * q, true);
     if (P > 1 && pid > 0) {
-      for (int q = tl; q < pid * 2 * MP * (TRF / 2); q += TPL) {
-        const int k = 1 + q / (2 * MP * (TRF / 2)), rs = (q / (TRF / 2)) % (2 * MP), h = q % (TRF / 2);
+      const int k1 = CARRY ? pid : 1;  // first staged partition (slot 0)
+      for (int q = tl; q < (pid - k1 + 1) * 2 * MP * (TRF / 2); q += TPL) {
+        const int k = k1 + q / (2 * MP * (TRF / 2)), rs = (q / (TRF / 2)) % (2 * MP), h = q % (TRF / 2);
         const double* rec = a.PP + (((size_t)g * P + k) * 2 * MP + rs) * kTransfer;
         const double* src = (h < 8) ? rec + kTrPhi + 2 * h : rec + kTrGz + 2 * (h - 8);
-        cp_async16(sTR + ((size_t)(k - 1) * 2 * MP + rs) * TRS + 2 * h, src, true);
+        cp_async16(sTR + ((size_t)(k - k1) * 2 * MP + rs) * TRS + 2 * h, src, true);
       }
     }
     cp_async_commit();
@@ -574,18 +613,54 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
     __syncthreads();
     cp_async_wait<0>();
     __syncwarp();
-    if (pid > 0) {
+    if constexpr (CARRY) {
+      // delta_1 = D_0, delta_{k+1} = D_k + Phi_k delta_k: partition k reads
+      // delta_k (published by k-1 in the exchange slots of its Xhat, free
+      // until B2), publishes delta_{k+1}, one barrier per partition
+      for (int k = 1; k < P; ++k) {
+        if (pid == k) {
+          const double* src = xch + ((size_t)(k - 1) * NL + ln) * kXch + (k == 1 ? 0 : 8);
+#pragma unroll
+          for (int t = 0; t < 4; ++t) d[t] = src[t];
+          if (k < P - 1) {
+            const double* phi = sTR + (size_t)slot * TRS;
+            const double* Dk = xch + ((size_t)k * NL + ln) * kXch;
+            double nd[4];
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+              double acc = Dk[o];
+#pragma unroll
+              for (int i = 0; i < 4; ++i) acc = fma(phi[o * 4 + i], d[i], acc);
+              nd[o] = acc;
+            }
+#pragma unroll
+            for (int o = 0; o < 4; ++o) myx[8 + o] = nd[o];
+          }
+        }
+        __syncthreads();
+      }
+      if (pid > 0) {
+        const double* gz = sTR + (size_t)slot * TRS + 16;
+#pragma unroll
+        for (int b = 0; b < NBMAX; ++b)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) z[b] = fma(gz[b * 4 + i], d[i], z[b]);
+      }
+    } else if (pid > 0) {
 #pragma unroll
       for (int t = 0; t < 4; ++t) d[t] = xch[(size_t)ln * kXch + t];  // delta_1 = D_0
       for (int k = 1; k < pid; ++k) {
-        const double* phi = sTR + ((size_t)(k - 1) * 2 * MP + slot) * TRS;
+        const double2* phi = reinterpret_cast<const double2*>(sTR + ((size_t)(k - 1) * 2 * MP + slot) * TRS);
         const double* Dk = xch + ((size_t)k * NL + ln) * kXch;
         double nd[4];
 #pragma unroll
         for (int o = 0; o < 4; ++o) {
+          const double2 w0 = phi[2 * o], w1 = phi[2 * o + 1];
           double acc = Dk[o];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) acc = fma(phi[o * 4 + i], d[i], acc);
+          acc = fma(w0.x, d[0], acc);
+          acc = fma(w0.y, d[1], acc);
+          acc = fma(w1.x, d[2], acc);
+          acc = fma(w1.y, d[3], acc);
           nd[o] = acc;
         }
 #pragma unroll
@@ -635,17 +710,17 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
       double* dst = ring + (size_t)(s % NSB) * BST;
       const int lo = row0 + Lp - (s + 1) * R;
       for (int q = tl; q < R * BREC / 2; q += TPL) cp_async16(dst + 2 * q, BRg + (size_t)lo * BREC + 2 * q, true);
-      if constexpr (P == 1)
+      if constexpr (YG)
         for (int q = tl; q < R * NL / 2; q += TPL)
           cp_async16(dst + R * BREC + 2 * q, ysave + (size_t)lo * NL + 2 * q, true);
     }
     cp_async_commit();
   };
   for (int s = 0; s < NSB - 1; ++s) issue_bwd(s);
-  for (int s0 = 0; s0 < nst; s0 += 2) {
-    const int q0 = row0 + Lp - (s0 + 2) * R;  // block rows q0 .. q0 + kBwdWin - 1, q0 % kBwdWin == 0
+  for (int s0 = 0; s0 < nst; s0 += KB) {
+    const int q0 = row0 + Lp - (s0 + KB) * R;  // block rows q0 .. q0 + kBwdWin - 1, q0 % kBwdWin == 0
 #pragma unroll
-    for (int hs = 0; hs < 2; ++hs) {
+    for (int hs = 0; hs < KB; ++hs) {
       const int s = s0 + hs;
       issue_bwd(s + NSB - 1);
       cp_async_wait<NSB - 1>();  // stage s is resident
@@ -666,7 +741,7 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
           auto rec = [&](int k) -> double { return (k & 1) ? rv[w][k >> 1].y : rv[w][k >> 1].x; };
           double* yx = ysave + (size_t)j * NL + ln;
           double acc0;
-          if constexpr (P == 1)
+          if constexpr (YG)
             acc0 = ring[(size_t)(s % NSB) * BST + R * BREC + (R - 1 - (h * BSUB + w)) * NL + ln];
           else
             acc0 = *yx;
@@ -698,6 +773,7 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
     }
   }
   cp_async_wait<0>();
+  if constexpr (YG && P > 1) __threadfence();  // particular x of all lanes reach L2 before B3 reloads them
   __syncwarp();
 
   // ---- B2: true incoming window T of this partition (zero for the last) ----
@@ -705,16 +781,36 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   double T[kBwdWin];
 #pragma unroll
   for (int t = 0; t < kBwdWin; ++t) T[t] = 0.0;
+  // B3's H ring: NSH slots of R rows (+ the particular x with y in global scratch)
+  constexpr int SLOT3 = R * HREC + (YG ? R * NL : 0);
+  static_assert(P == 1 || (NSH >= 2 && NSH * SLOT3 <= RING), "H ring fits the partition's ring");
+  const int nst3 = last ? 0 : nst;  // H stages this partition streams
+  auto issue_h = [&](int s) {
+    if (s < nst3) {
+      double* dst = ring + (size_t)(s % NSH) * SLOT3;
+      const int lo = row0 + s * R;
+      for (int q = tl; q < R * HREC / 2; q += TPL) cp_async16(dst + 2 * q, HRg + (size_t)lo * HREC + 2 * q, true);
+      if constexpr (YG)
+        for (int q = tl; q < R * NL / 2; q += TPL)
+          cp_async16(dst + R * HREC + 2 * q, ysave + (size_t)lo * NL + 2 * q, true);
+    }
+    cp_async_commit();
+  };
+  // Psi sits at the end of the ring, so the first H stages of B3 (the ring's
+  // front) stream in while the windows are carried
+  constexpr int PS = kBwdWin * kBwdWin + 2;
+  constexpr int PSI = 2 * MP * PS;
+  constexpr int NPRE = (RING - PSI) / SLOT3 < NSH - 1 ? (RING - PSI) / SLOT3 : NSH - 1;  // H stages prefetched
   if constexpr (P > 1) {
     // Carry from the bottom: T_{P-2} = Xhat_{P-1} (the last partition's top
     // window is exact), T_{k-1} = Xhat_k + Psi_k T_k.  Partition k (1 <= k <=
-    // P-2) stages its own Psi_k in its ring while the others finish B1,
+    // P-2) stages its own Psi_k (transposed: row i holds the responses of the
+    // 12 outputs to input i) in its ring while the others finish B1,
     // [slot][PS] with the stride PS = 146 doubles putting the 8 slots read at
     // once in distinct banks; at step k it overwrites its published Xhat_k
     // with T_{k-1}, which partition k-1 reads after the barrier.
-    constexpr int PS = kBwdWin * kBwdWin + 2;
-    static_assert(2 * MP * PS <= RING, "Psi fits the ring");
-    double* sPsi = ring;
+    static_assert(PSI <= RING, "Psi fits the ring");
+    double* sPsi = ring + (RING - PSI);
     if (pid >= 1 && pid <= P - 2) {
       for (int q = tl; q < 2 * MP * 72; q += TPL) {
         const int rs = q / 72, h = q % 72;
@@ -723,10 +819,11 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
       }
     }
     cp_async_commit();
+    for (int s = 0; s < NPRE; ++s) issue_h(s);
     double* myxh = myx + 8;
 #pragma unroll
     for (int t = 0; t < kBwdWin; ++t) myxh[t] = xw[t];
-    cp_async_wait<0>();
+    cp_async_wait<NPRE>();  // Psi (the H stages may still be in flight)
     __syncthreads();
     if (pid == P - 2) {
       const double* Xl = xch + ((size_t)(P - 1) * NL + ln) * kXch + 8;
@@ -735,15 +832,20 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
     }
     for (int k = P - 2; k >= 1; --k) {
       if (pid == k) {
-        const double* psi = sPsi + (size_t)slot * PS;
+        // twelve independent accumulators, input by input (16-byte rows of Psi^T);
+        // each output still sums its inputs in order 0..11
+        const double2* psi = reinterpret_cast<const double2*>(sPsi + (size_t)slot * PS);
         double nt[kBwdWin];
 #pragma unroll
-        for (int o = 0; o < kBwdWin; ++o) {
-          double acc = xw[o];
+        for (int o = 0; o < kBwdWin; ++o) nt[o] = xw[o];
 #pragma unroll
-          for (int i = 0; i < kBwdWin; ++i) acc = fma(psi[o * kBwdWin + i], T[i], acc);
-          nt[o] = acc;
-        }
+        for (int i = 0; i < kBwdWin; ++i)
+#pragma unroll
+          for (int o = 0; o < kBwdWin; o += 2) {
+            const double2 w = psi[(i * kBwdWin + o) / 2];
+            nt[o] = fma(w.x, T[i], nt[o]);
+            nt[o + 1] = fma(w.y, T[i], nt[o + 1]);
+          }
 #pragma unroll
         for (int o = 0; o < kBwdWin; ++o) myxh[o] = nt[o];  // lanes ln and ln + NL write the same values
       }
@@ -761,23 +863,12 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   // (the last partition stored its unknowns in B1: its threads run the loop
   // without loads or stores, so the warp-wide syncs see every lane)
   if constexpr (P > 1) {
-    constexpr int SLOT3 = R * HREC;  // H ring: NSH slots of R rows
-    static_assert(NSH >= 2 && NSH * SLOT3 <= RING, "H ring fits the partition's ring");
     constexpr int LG = TPL / NL;  // lane groups: each takes every LG-th row of a stage
     const int grp = tl / NL;
-    const int nst3 = last ? 0 : nst;  // stages this partition streams
     const int nloop = __shfl_sync(0xffffffffu, nst3, 0) > __shfl_sync(0xffffffffu, nst3, 31)
                           ? __shfl_sync(0xffffffffu, nst3, 0)
                           : __shfl_sync(0xffffffffu, nst3, 31);  // the warp's trip count
-    auto issue_h = [&](int s) {
-      if (s < nst3) {
-        double* dst = ring + (size_t)(s % NSH) * SLOT3;
-        const int lo = row0 + s * R;
-        for (int q = tl; q < R * HREC / 2; q += TPL) cp_async16(dst + 2 * q, HRg + (size_t)lo * HREC + 2 * q, true);
-      }
-      cp_async_commit();
-    };
-    for (int s = 0; s < NSH - 1; ++s) issue_h(s);
+    for (int s = NPRE; s < NSH - 1; ++s) issue_h(s);
     for (int s = 0; s < nloop; ++s) {
       issue_h(s + NSH - 1);
       cp_async_wait<NSH - 1>();
@@ -794,7 +885,8 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
 #pragma unroll
           for (int v = 0; v < HV; ++v) hv[v] = st[u * (HREC / 2) + v];
           const int j = row0 + s * R + u;
-          double acc0 = ysave[(size_t)j * NL + ln], acc1 = 0.0;
+          double acc0 = YG ? ring[(size_t)(s % NSH) * SLOT3 + R * HREC + u * NL + ln] : ysave[(size_t)j * NL + ln];
+          double acc1 = 0.0;
 #pragma unroll
           for (int i = 0; i < kBwdWin; i += 2) {
             acc0 = fma(hv[i / 2].x, T[i], acc0);
@@ -827,7 +919,8 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
 //   Phi_k[o][i] = exit pending entry o,  Gz_k[b][i] = border accumulator b.
 // For k <= P-2 (backward from unit window entry i, row r1 + i, with zero
 // y and border unknowns):
-//   H of row j (H record) = x_j,  Psi_k[o][i] = x of row r0 + o.
+//   H of row j (H record) = x_j,  Psi_k[o][i] = x of row r0 + o (stored
+//   transposed, [i][o], so the carry reads it by input).
 // ---------------------------------------------------------------------------
 template <int KL, int KU, int P, int PPW>
 __global__ void __launch_bounds__(128) k_tau_transfer(TauArgs a) {
@@ -883,7 +976,7 @@ __global__ void __launch_bounds__(128) k_tau_transfer(TauArgs a) {
       hr[kBwdWin + 1] = 0.0;
     }
   }
-  for (int o = 0; o < kBwdWin; ++o) tr[kTrPsi + o * kBwdWin + ib] = xw[o];
+  for (int o = 0; o < kBwdWin; ++o) tr[kTrPsi + ib * kBwdWin + o] = xw[o];  // Psi^T: row ib
 }
 
 template <int N>
@@ -1075,12 +1168,14 @@ void transfer_impl(const TauArgs& a, int parts, cudaStream_t st) {
   if (parts == kTauParts) k_tau_transfer<KL, KU, kTauParts, 1><<<dim3(tgx, 2 * kTauParts, 16), 128, 0, st>>>(a);
   if (parts == kTauParts8)
     k_tau_transfer<KL, KU, kTauParts8, kTau8PerWarp><<<dim3(tgx, 2 * kTauParts8, 16), 128, 0, st>>>(a);
+  if (parts == kTauParts16)
+    k_tau_transfer<KL, KU, kTauParts16, kTau8PerWarp><<<dim3(tgx, 2 * kTauParts16, 16), 128, 0, st>>>(a);
 }
 
 template <int P>
 size_t solve_smem_bytes(int npad) {
   constexpr size_t NL = 4 * kSolveModes;
-  const size_t ys = P == 1 ? 0 : (size_t)npad * NL;  // one partition keeps y in global scratch
+  const size_t ys = ys_global<P>() ? 0 : (size_t)npad * NL;  // 1 and 16 partitions keep y in global scratch
   return ((size_t)P * ring_doubles<P>() + ys + (size_t)P * NL * kXch) * sizeof(double) +
          (size_t)npad * 2 * sizeof(int);
 }
@@ -1088,7 +1183,10 @@ size_t solve_smem_bytes(int npad) {
 template <int KL, int KU>
 void solve_impl(const TauArgs& a, int parts, cudaStream_t st) {
   const int groups = (a.Nk + kSolveModes - 1) / kSolveModes;
-  if (parts == kTauParts8)
+  if (parts == kTauParts16)
+    k_tau_solve<KL, KU, kTauParts16, kTau8PerWarp>
+        <<<groups, 32 * kTauParts16 / kTau8PerWarp, solve_smem_bytes<kTauParts16>(a.npad), st>>>(a);
+  else if (parts == kTauParts8)
     k_tau_solve<KL, KU, kTauParts8, kTau8PerWarp>
         <<<groups, 32 * kTauParts8 / kTau8PerWarp, solve_smem_bytes<kTauParts8>(a.npad), st>>>(a);
   else if (parts == kTauParts)
@@ -1110,6 +1208,9 @@ cudaError_t set_tau_smem_limits(int bytes) {
   e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU, kTauParts8, kTau8PerWarp>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_tau_solve<kTauKL, kTauKU, kTauParts16, kTau8PerWarp>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
   const void* fns[] = {(const void*)k_rk_final<1>,  (const void*)k_rk_final<2>,  (const void*)k_rk_final<3>,
                        (const void*)k_rk_final<4>,  (const void*)k_rk_final<5>,  (const void*)k_rk_final<6>,
                        (const void*)k_rk_final<7>,  (const void*)k_rk_final<8>,  (const void*)k_rk_final<9>,
@@ -1122,6 +1223,7 @@ cudaError_t set_tau_smem_limits(int bytes) {
 }
 
 size_t tau_solve_smem_bytes(int npad, int parts) {
+  if (parts == kTauParts16) return solve_smem_bytes<kTauParts16>(npad);
   if (parts == kTauParts8) return solve_smem_bytes<kTauParts8>(npad);
   return parts == kTauParts ? solve_smem_bytes<kTauParts>(npad) : solve_smem_bytes<1>(npad);
 }
@@ -1133,7 +1235,7 @@ size_t tau_transfer_doubles(int Nk, int parts) {
 }
 
 size_t tau_solve_scratch_doubles(int Nk, int npad, int parts) {
-  if (parts != 1) return 0;
+  if (parts != 1 && parts != kTauParts16) return 0;
   const size_t groups = (size_t)(Nk + kSolveModes - 1) / kSolveModes;
   return groups * (size_t)npad * 4 * kSolveModes;
 }

@@ -30,20 +30,25 @@ def _fixture(golden_dir, name):
     return np.load(path)
 
 
-def _run_2d(tb, d, precision):
+def _run_2d(tb, d, precision, tau_parts=0):
     Nx, Nz = int(d["Nx"]), int(d["Nz"])
     p = RBCParams(Nx=Nx, Nz=Nz, Lx=4.0, Lz=1.0, Ra=float(d["Ra"]), Pr=1.0)
     dom = tb.ChannelDomain(Nx, Nz, Lx=4.0, Lz=1.0)
     plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, TS[str(d["scheme"])], precision=precision)
+    if tau_parts:
+        plan.set_variant(tau_parts=tau_parts)
     plan.set_state(0, forward_2d(rbc_initial_b(p, 42)))
     plan.step(float(d["dt"]), int(d["nsteps"]))
     return plan
 
 
+@pytest.mark.parametrize("tau_parts", [1, 4, 8, 16])
 @pytest.mark.parametrize("name", ["rbc_c2_rk443_1024x256", "rbc_c2_sbdf2_1024x256"])
-def test_c2_100_steps_f64_every_field(tb, golden_dir, name):
+def test_c2_100_steps_f64_every_field(tb, golden_dir, name, tau_parts):
+    # every tau-solve partitioning (the tuner may pick any of them)
     d = _fixture(golden_dir, name)
-    plan = _run_2d(tb, d, tb._lib.TB_PREC_F64)
+    plan = _run_2d(tb, d, tb._lib.TB_PREC_F64, tau_parts)
+    assert plan.variant()[0] == tau_parts
     for sel, f in ((0, "b"), (1, "ux"), (2, "uz")):
         err = rel_l2(plan.get_state(sel), d[f])
         assert err < F64_BAR, (f, err)

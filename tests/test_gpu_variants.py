@@ -52,6 +52,38 @@ def test_uneven_eight_partitions_give_the_oracle_solution(tb, scheme, ts):
             assert rel_l2(a, b) < 1e-11 or np.abs(b).max() == 0.0
 
 
+@pytest.mark.parametrize("scheme,ts", [("RK443", 1), ("SBDF2", 3)])
+def test_uneven_sixteen_partitions_give_the_oracle_solution(tb, scheme, ts):
+    # Nz = 96: 196 band rows per class, padded to 240 = 20 windows of 12 rows
+    # (10 window pairs over 8 warps), so the sixteen partitions take 1 or 2
+    # windows each; the records stream in 3-row stages, y and the particular
+    # unknowns through global scratch, the starting windows carried down
+    p = RBCParams(Nx=64, Nz=96, Lx=4.0, Lz=1.0, Ra=1e8)
+    sim = run_rbc(p, scheme, 0.01, 5, seed=42)
+    states = {}
+    for parts in (16, 1):
+        dom = tb.ChannelDomain(64, 96, Lx=4.0, Lz=1.0)
+        plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, ts)
+        plan.set_variant(tau_parts=parts)
+        assert plan.variant()[0] == parts
+        plan.set_state(0, forward_2d(rbc_initial_b(p, 42)))
+        plan.step(0.01, 5)
+        for f, want in ((0, sim.b), (1, sim.ux), (2, sim.uz)):
+            assert rel_l2(plan.get_state(f), want) < 1e-10, (parts, f)
+        states[parts] = [plan.get_state(f) for f in (0, 1, 2, 3)]
+    for a, b in zip(states[16], states[1]):
+        assert rel_l2(a, b) < 1e-11 or np.abs(b).max() == 0.0
+
+
+def test_sixteen_partitions_need_sixteen_windows(tb):
+    # Nz = 64: 144 padded band rows = 12 windows, fewer than 16 partitions
+    dom = tb.ChannelDomain(64, 64, Lx=4.0, Lz=1.0)
+    p = RBCParams(Nx=64, Nz=64, Lx=4.0, Lz=1.0, Ra=1e8)
+    plan = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, 1)
+    with pytest.raises(tb.TarangError):
+        plan.set_variant(tau_parts=16)
+
+
 @pytest.mark.parametrize("key", ["16x11", "24x16", "96x24"])
 def test_batched_x_products_match_golden_rhs(tb, golden_dir, key):
     import os
@@ -136,7 +168,7 @@ def test_plan_tune_keeps_state_and_picks_a_feasible_shape(tb):
     plan.step(0.02, 2)
     before = [plan.get_state(f) for f in (0, 1, 2)]
     parts, rows = plan.tune(0.02, trial_steps=3)
-    assert parts in (1, 4, 8) and rows in (1, 2, 3) and plan.variant() == (parts, rows)
+    assert parts in (1, 4, 8, 16) and rows in (1, 2, 3) and plan.variant() == (parts, rows)
     for f, b in zip((0, 1, 2), before):
         assert np.array_equal(plan.get_state(f), b)
     plan.step(0.02, 2)  # steps on with the chosen shape
