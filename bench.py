@@ -607,7 +607,9 @@ def summarize(out: dict) -> dict:
             if not isinstance(d, dict) or k not in d or d[k] is None:
                 return None
             d = d[k]
-        return round(d, 4) if isinstance(d, float) else d
+        if isinstance(d, float):  # 4 decimals, or 3 significant digits for small values (errors)
+            return float(f"{d:.3g}") if 0.0 < abs(d) < 1e-2 else round(d, 4)
+        return d
 
     s = {"steps_per_s": g(out, "value"), "e2e_steps_per_s": g(out, "e2e", "value"),
          "tau_solve_frac": g(out, "roofline", "frac"), "step_model_frac": g(out, "step_roofline", "frac"),

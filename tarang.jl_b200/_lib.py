@@ -11,7 +11,9 @@ import os
 from ctypes import POINTER, Structure, c_char_p, c_double, c_float, c_int, c_longlong, c_size_t, c_void_p
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libtarang_b200.so")
+# TARANG_B200_LIB selects another build of the same ABI (the phase-clock build
+# of solve_clocks.py); the default is the product library beside this file
+LIB_PATH = os.environ.get("TARANG_B200_LIB") or os.path.join(HERE, "libtarang_b200.so")
 
 TB_OK, TB_EINVAL, TB_ENOMEM, TB_ESINGULAR, TB_ETIMEOUT, TB_ECUDA, TB_ENOTSUPPORTED, TB_EBUDGET, TB_ESTATE = range(9)
 TB_HOST, TB_DEVICE = 0, 1

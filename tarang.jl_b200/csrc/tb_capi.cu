@@ -7,6 +7,7 @@
 // One step is captured once per dt as a CUDA graph and replayed.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -155,6 +156,59 @@ std::vector<double2> ip_twiddles(const FftPlan& fp) {
     L = m;
   }
   return t;
+}
+
+// Shared-memory wavefronts of the in-place passes of plan fp (fftg::pass_ip:
+// item = thread + k * blockDim over NA arrays Ms = n apart, a warp = 32
+// consecutive items, lane element base + r m at the XOR-swizzled index
+// fidx), summed over the DIF inverse (4 arrays) and DIT forward (2 arrays)
+// transforms of the x-products kernel.  Elements of esz bytes: 16 (double2,
+// four 8-lane phases over 8 bank quads) or 8 (float2, two 16-lane phases
+// over 16 bank pairs); a phase costs as many wavefronts as the most distinct
+// addresses on one bank group.
+long long ip_wavefronts(const FftPlan& fp, int esz) {
+  const int n = fp.n, lanes = esz == 16 ? 8 : 16, banks = esz == 16 ? 8 : 16;
+  auto swz = [](int i) { return i ^ ((i >> 3) & 7); };
+  long long wf = 0;
+  for (int t = 0; t < 2; ++t) {
+    const int NA = t == 0 ? 4 : 2;
+    int L = n;
+    for (int s = 0; s < fp.nstages; ++s) {
+      const int R = fp.radix[s], m = L / R, nb = n / R, total = NA * nb;
+      for (int w0 = 0; w0 < total; w0 += 32)
+        for (int r = 0; r < R; ++r)
+          for (int ph = w0; ph < w0 + 32 && ph < total; ph += lanes) {
+            std::vector<std::vector<int>> grp(banks);
+            int worst = 0;
+            for (int item = ph; item < ph + lanes && item < total; ++item) {
+              const int arr = item / nb, b = item - arr * nb, base = (b / m) * L + b % m;
+              const int addr = arr * n + swz(base + r * m);
+              auto& g = grp[addr % banks];
+              if (std::find(g.begin(), g.end(), addr) == g.end()) g.push_back(addr);
+              worst = std::max(worst, (int)g.size());
+            }
+            wf += worst;
+          }
+      L = m;
+    }
+  }
+  return wf;
+}
+
+// The order of fp's passes with the fewest in-place wavefronts (ties keep the
+// earlier order in lexicographic sequence, starting from fp's own).
+FftPlan best_ip_order(const FftPlan& fp, int esz) {
+  FftPlan best = fp, cand = fp;
+  long long bw = ip_wavefronts(fp, esz);
+  std::sort(cand.radix, cand.radix + cand.nstages);
+  do {
+    const long long w = ip_wavefronts(cand, esz);
+    if (w < bw) {
+      bw = w;
+      best = cand;
+    }
+  } while (std::next_permutation(cand.radix, cand.radix + cand.nstages));
+  return best;
 }
 
 std::vector<double2> twiddles(int n) {
@@ -327,7 +381,7 @@ void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2row
   }
   xa.ptw = P->ptwM32.as<float2>();
   xa.nptw = (int)(P->ptwM32.bytes / sizeof(float2));
-  xa.fp = P->fpM;
+  xa.fp = P->xrows == 3 ? P->fpMip : P->fpM;  // the in-place kernels run their own pass order
   xa.Nx = P->Nx;
   xa.Nk = P->Nkm;
   xa.ld = P->Nk;
@@ -389,7 +443,7 @@ void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
   }
   xa.ptw = P->ptwM.as<double2>();
   xa.nptw = (int)(P->ptwM.bytes / sizeof(double2));
-  xa.fp = P->fpM;
+  xa.fp = P->xrows == 3 ? P->fpMip : P->fpM;  // the in-place kernels run their own pass order
   xa.Nx = P->Nx;
   xa.Nk = P->Nkm;
   xa.ld = P->Nk;
@@ -1107,9 +1161,10 @@ void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, i
     upload(P->s3, cm.s3);
     upload(P->twM, twiddles(P->M));
     upload(P->ptwM, pass_twiddles(P->fpM));
-    upload(P->iptwM, ip_twiddles(P->fpM));
-    upload(P->twN, twiddles(P->Nx));
     P->mixed = desc->precision == TB_PREC_MIXED;
+    P->fpMip = best_ip_order(P->fpM, P->mixed ? 8 : 16);
+    upload(P->iptwM, ip_twiddles(P->fpMip));
+    upload(P->twN, twiddles(P->Nx));
     if (P->mixed) {
       auto f32 = [](const std::vector<double>& v) {
         std::vector<float> o(v.size());
@@ -1128,7 +1183,7 @@ void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, i
       std::vector<float2> pt32(pt.size());
       for (size_t i = 0; i < pt.size(); ++i) pt32[i] = make_float2((float)pt[i].x, (float)pt[i].y);
       upload(P->ptwM32, pt32);
-      const std::vector<double2> it = ip_twiddles(P->fpM);
+      const std::vector<double2> it = ip_twiddles(P->fpMip);
       std::vector<float2> it32(it.size());
       for (size_t i = 0; i < it.size(); ++i) it32[i] = make_float2((float)it[i].x, (float)it[i].y);
       upload(P->iptwM32, it32);

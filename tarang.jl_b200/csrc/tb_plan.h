@@ -188,6 +188,9 @@ struct tb_plan {
   DevBuf bEv, bOv, bEd, bOd, fE, fO, sfE, sfO;
   int Hz = 0, Ke = 0, Ko = 0;  // Hz = ceil(Nz/2)
   FftPlan fpM{}, fpN{};
+  // the padded length's passes in the order of the in-place x-products kernels
+  // (x-products form 3; the order with the fewest shared-memory bank conflicts)
+  FftPlan fpMip{};
   // tau systems
   TauSystem sys[2];
   int nsys = 1;

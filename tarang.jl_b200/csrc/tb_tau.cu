@@ -17,6 +17,23 @@
 
 namespace tb {
 
+#ifdef TB_SOLVE_CLOCKS
+// Phase clocks of the tau solve (a separate build, `make clocks`): SM cycle
+// counter of lane 0 of every partition at the start of F1, F2, the border
+// solve (B1), B2, B3 and the end, [group][partition][8].
+constexpr int kSolveClockSlots = 1 << 16;
+__device__ long long g_solve_clocks[kSolveClockSlots];
+#define TB_SOLVE_CLOCK(ph)                                                           \
+  do {                                                                             \
+    if (tl == 0 && (g * P + pid) * 8 + (ph) < kSolveClockSlots)                    \
+      g_solve_clocks[(g * P + pid) * 8 + (ph)] = clock64();                        \
+  } while (0)
+#else
+#define TB_SOLVE_CLOCK(ph) \
+  do {                     \
+  } while (0)
+#endif
+
 namespace {
 
 constexpr int NBMAX = 4;
@@ -461,6 +478,7 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
+  TB_SOLVE_CLOCK(0);
   const double* FRg = a.cls[0].FR + (size_t)g * np * FREC;
   const double* BRg = a.cls[0].BR + (size_t)g * np * BREC;
   const double* HRg = a.HR + (size_t)g * np * HREC;
@@ -570,6 +588,7 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
     }
     __syncwarp();  // the window's slots are refilled next
   }
+  TB_SOLVE_CLOCK(1);
   double* myx = xch + ((size_t)pid * NL + ln) * kXch;
   // exit window minus the raw right-hand side of the next partition's first rows (the
   // ring still holds those right-hand sides)
@@ -687,6 +706,7 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   }
 
   // ---- border unknowns from the Schur complement ----
+  TB_SOLVE_CLOCK(2);
   double x1[NBMAX];
   {
     const double* si = sSI + (size_t)c * NBMAX * NBMAX * MP + mm;
@@ -777,6 +797,7 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   __syncwarp();
 
   // ---- B2: true incoming window T of this partition (zero for the last) ----
+  TB_SOLVE_CLOCK(3);
   const bool last = (pid == P - 1);
   double T[kBwdWin];
 #pragma unroll
@@ -860,6 +881,7 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   }
 
   // ---- B3: x_j = particular + H_j . T over the rows of this partition, stored to X ----
+  TB_SOLVE_CLOCK(4);
   // (the last partition stored its unknowns in B1: its threads run the loop
   // without loads or stores, so the warp-wide syncs see every lane)
   if constexpr (P > 1) {
@@ -899,6 +921,7 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
     }
     cp_async_wait<0>();
   }
+  TB_SOLVE_CLOCK(5);
   // border unknowns
   if (pid == 0) {
 #pragma unroll
@@ -1313,3 +1336,11 @@ size_t rk_final_smem_bytes(int Nz) {
 }
 
 }  // namespace tb
+
+#ifdef TB_SOLVE_CLOCKS
+// Copies the first n phase clocks of the last tau solves to host memory.
+extern "C" int tb_solve_clocks(long long* out, int n) {
+  if (!out || n < 0 || n > tb::kSolveClockSlots) return 1;
+  return cudaMemcpyFromSymbol(out, tb::g_solve_clocks, sizeof(long long) * (size_t)n) == cudaSuccess ? 0 : 1;
+}
+#endif

@@ -223,6 +223,34 @@ def test_batched_dense_lu_matches_numpy_and_names_singular_slice(tb):
     assert bad.value == 3
 
 
+@pytest.mark.parametrize("n,batch", [(263, 3), (100, 2), (16, 2), (17, 1), (450, 1)])
+def test_batched_dense_lu_factors_match_lapack(tb, n, batch):
+    # blocked panels of 16 columns (n <= 440: whole panels, a partial last
+    # panel, a single panel) and the unblocked form (n = 450): the same pivots
+    # as LAPACK's zgetrf and factors to rounding
+    import ctypes
+
+    import scipy.linalg as sla
+    import torch
+
+    from tarang_b200 import api
+
+    ctx = api._context(0)
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((batch, n, n)) + 1j * rng.standard_normal((batch, n, n))
+    Ad = torch.as_tensor(np.ascontiguousarray(A.transpose(0, 2, 1)).view(np.float64), device="cuda")
+    piv = torch.zeros(batch * n, dtype=torch.int32, device="cuda")
+    bad = ctypes.c_int(-2)
+    assert tb.lib.tb_batched_lu_factor(ctx, n, batch, ctypes.c_void_p(Ad.data_ptr()), ctypes.c_void_p(piv.data_ptr()),
+                                       ctypes.byref(bad)) == 0
+    LU = Ad.cpu().numpy().view(np.complex128).reshape(batch, n, n).transpose(0, 2, 1)
+    P = piv.cpu().numpy().reshape(batch, n)
+    for s in range(batch):
+        lu_ref, piv_ref = sla.lu_factor(A[s])
+        assert np.array_equal(P[s] - 1, piv_ref)
+        assert np.linalg.norm(LU[s] - lu_ref) / np.linalg.norm(lu_ref) < 1e-12
+
+
 def test_reference_style_script(tb):
     # test/test_subproblem_rk.jl:20-103 written against the mirror API
     Lx, Lz, Nx, Nz, Ra, Pr = 4.0, 1.0, 16, 8, 1e4, 1.0
