@@ -27,6 +27,10 @@ struct GemmItem32 {
   const float* B;  // input rows (ldb floats apart; ldb even)
   void* C;         // output rows (ldc elements)
   int M, K, Kpad, mode, par;
+  // tensor-core path: A's TF32 hi/lo operand image (make_tc32_a_image; null:
+  // SIMT only) and, set by launch_gemm_tc32, the item's B' tile images
+  const float* Aimg = nullptr;
+  const float* Bimg = nullptr;
 };
 struct GemmBatch32 {
   GemmItem32 item[kGemmMaxBatch];
@@ -34,24 +38,29 @@ struct GemmBatch32 {
 void launch_gemm_f32(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
                      cudaStream_t st);
 // The same GEMMs on the tcgen05 tensor cores (TF32, three products per term;
-// tb_tc32.cu) for items with M <= 128 and K <= 128.
+// tb_tc32.cu) for items with M <= 128 and K <= 128.  The operands reach the
+// tensor cores as images of their shared-memory tiles (TF32 hi and lo parts,
+// 128-byte swizzled, K-major), copied in by bulk copies: A's once per plan
+// (make_tc32_a_image, tc32_a_image_floats floats each), B's per call by a
+// staging kernel into scratch (tc32_b_scratch_floats floats for up to
+// kGemmMaxBatch distinct inputs of ncol columns).
 bool gemm_tc32_supported(const GemmBatch32& bt, int nbatch);
-void launch_gemm_tc32(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
-                      cudaStream_t st);
+size_t tc32_a_image_floats();
+size_t tc32_b_scratch_floats(int ncol, int nimages);
+void make_tc32_a_image(const float* A, int M, int Kpad, float* image, cudaStream_t st);
+// false (nothing launched) when an item has no A image or the scratch is too small
+bool launch_gemm_tc32(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
+                      cudaStream_t st, float* bscratch, size_t bscratch_floats);
 cudaError_t set_tc32_smem_limits();
 int tc32_status();  // 1 once a tensor-core GEMM's bounded wait gave up, -1 if unreadable
-// Column tiles each CTA of the tensor-core GEMM walks through (one wave of
-// CTAs, one per SM).
-int gemm_tc32_tiles_per_cta(int ncol, int nbatch);
-// tensor cores when asked for, the shapes fit and each CTA has at most two
-// column tiles (its tile loop loads, multiplies and stores one tile at a time,
-// so long loops - wide stacked plans - stay on the SIMT kernel), else SIMT
+// tensor cores when asked for and the shapes fit, else SIMT
 inline void launch_gemm_f32_path(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows,
-                                 bool out_f64, cudaStream_t st, bool tensor_cores) {
-  if (tensor_cores && gemm_tc32_supported(bt, nbatch) && gemm_tc32_tiles_per_cta(ncol, nbatch) <= 2)
-    launch_gemm_tc32(bt, nbatch, ncol, ldb, ldc, Nrows, out_f64, st);
-  else
-    launch_gemm_f32(bt, nbatch, ncol, ldb, ldc, Nrows, out_f64, st);
+                                 bool out_f64, cudaStream_t st, bool tensor_cores, float* bscratch = nullptr,
+                                 size_t bscratch_floats = 0) {
+  if (tensor_cores && gemm_tc32_supported(bt, nbatch) &&
+      launch_gemm_tc32(bt, nbatch, ncol, ldb, ldc, Nrows, out_f64, st, bscratch, bscratch_floats))
+    return;
+  launch_gemm_f32(bt, nbatch, ncol, ldb, ldc, Nrows, out_f64, st);
 }
 void launch_round_f32(const double2* in, float2* out, long long n, cudaStream_t st);
 struct XProdArgs32 {
@@ -151,15 +160,21 @@ constexpr int kTauParts = 4;
 constexpr int kTauParts8 = 8;
 constexpr int kTauRowPad = kTauParts * kBwdWin;
 // First band row of partition k (0 <= k <= P) of a P-partition solve over
-// np rows (np a multiple of kBwdWin): windows spread as evenly as they go.
-// With two partitions per warp (ppw = 2, np a multiple of 2 kBwdWin) the two
-// partitions of a warp get equal row counts, so the warp's halves sweep in
-// step: warp w takes pairs of windows spread as evenly as they go.
+// np rows (np a multiple of kBwdWin): windows spread as evenly as they go,
+// the spare ones to the upper partitions (the backward carry starts at the
+// bottom, so the lighter lower partitions begin it while the upper ones
+// still sweep).  With two partitions per warp (ppw = 2, np a multiple of
+// 2 kBwdWin) the two partitions of a warp get equal row counts, so the warp's
+// halves sweep in step: warp w takes pairs of windows spread the same way.
 __host__ __device__ inline int tau_part_row0(int np, int P, int k, int ppw = 1) {
-  if (ppw == 1) return kBwdWin * (int)(((long long)k * (np / kBwdWin)) / P);
+  auto first = [](int n, int parts, int i) {  // first unit of part i of n units, spares to the first parts
+    const int q = n / parts, r = n % parts;
+    return i * q + (i < r ? i : r);
+  };
+  if (ppw == 1) return kBwdWin * first(np / kBwdWin, P, k);
   const int nw = P / 2, pairs = np / (2 * kBwdWin);
   const int w = k / 2, h = k % 2;
-  const int b0 = (int)(((long long)w * pairs) / nw), b1 = (int)(((long long)(w + 1) * pairs) / nw);
+  const int b0 = first(pairs, nw, w), b1 = first(pairs, nw, w + 1);
   return 2 * kBwdWin * b0 + h * kBwdWin * (b1 - b0);
 }
 // Partitions per warp of the 8- and 16-partition solves (two: each half-warp

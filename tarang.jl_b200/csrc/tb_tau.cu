@@ -826,11 +826,17 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
     // Carry from the bottom: T_{P-2} = Xhat_{P-1} (the last partition's top
     // window is exact), T_{k-1} = Xhat_k + Psi_k T_k.  Partition k (1 <= k <=
     // P-2) stages its own Psi_k (transposed: row i holds the responses of the
-    // 12 outputs to input i) in its ring while the others finish B1,
-    // [slot][PS] with the stride PS = 146 doubles putting the 8 slots read at
-    // once in distinct banks; at step k it overwrites its published Xhat_k
-    // with T_{k-1}, which partition k-1 reads after the barrier.
+    // 12 outputs to input i) in its ring, [slot][PS] with the stride PS = 146
+    // doubles putting the 8 slots read at once in distinct banks, and
+    // overwrites its published Xhat_k with T_{k-1}, which partition k-1 reads.
+    // The carry runs warp by warp from the bottom as soon as each warp has
+    // finished B1: within a warp the hand-over is a __syncwarp, between warps
+    // w and w-1 the named barrier w (64 threads: w arrives after writing its
+    // lowest partition's output, w-1 before reading it), so the lower warps
+    // carry while the upper ones still sweep, and each partition starts B3 as
+    // soon as it has its window.
     static_assert(PSI <= RING, "Psi fits the ring");
+    static_assert(P / PPW <= 16, "one named barrier per pair of adjacent warps");
     double* sPsi = ring + (RING - PSI);
     if (pid >= 1 && pid <= P - 2) {
       for (int q = tl; q < 2 * MP * 72; q += TPL) {
@@ -845,37 +851,47 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
 #pragma unroll
     for (int t = 0; t < kBwdWin; ++t) myxh[t] = xw[t];
     cp_async_wait<NPRE>();  // Psi (the H stages may still be in flight)
-    __syncthreads();
-    if (pid == P - 2) {
-      const double* Xl = xch + ((size_t)(P - 1) * NL + ln) * kXch + 8;
+    __syncwarp();
+    constexpr int NW = P / PPW;  // warps of the CTA
 #pragma unroll
-      for (int t = 0; t < kBwdWin; ++t) T[t] = Xl[t];
-    }
-    for (int k = P - 2; k >= 1; --k) {
-      if (pid == k) {
-        // twelve independent accumulators, input by input (16-byte rows of Psi^T);
-        // each output still sums its inputs in order 0..11
-        const double2* psi = reinterpret_cast<const double2*>(sPsi + (size_t)slot * PS);
-        double nt[kBwdWin];
+    for (int h = PPW - 1; h >= 0; --h) {
+      const int k = warp * PPW + h;  // the partition of this warp whose window is carried now
+      if (k < P - 1) {
+        // its window T_k is the output of partition k + 1: the warp below
+        // (named barrier warp + 1) or the other half of this warp
+        if (h == PPW - 1) {
+          __syncwarp();  // the whole warp reaches the barrier together
+          if (warp < NW - 1) asm volatile("bar.sync %0, %1;" ::"r"(warp + 1), "r"(64) : "memory");
+        } else {
+          __syncwarp();
+        }
+        if (pid == k) {
+          const double* Xn = xch + ((size_t)(k + 1) * NL + ln) * kXch + 8;
 #pragma unroll
-        for (int o = 0; o < kBwdWin; ++o) nt[o] = xw[o];
+          for (int t = 0; t < kBwdWin; ++t) T[t] = Xn[t];
+          if (k >= 1) {
+            // twelve independent accumulators, input by input (16-byte rows of
+            // Psi^T); each output still sums its inputs in order 0..11
+            const double2* psi = reinterpret_cast<const double2*>(sPsi + (size_t)slot * PS);
+            double nt[kBwdWin];
 #pragma unroll
-        for (int i = 0; i < kBwdWin; ++i)
+            for (int o = 0; o < kBwdWin; ++o) nt[o] = xw[o];
 #pragma unroll
-          for (int o = 0; o < kBwdWin; o += 2) {
-            const double2 w = psi[(i * kBwdWin + o) / 2];
-            nt[o] = fma(w.x, T[i], nt[o]);
-            nt[o + 1] = fma(w.y, T[i], nt[o + 1]);
+            for (int i = 0; i < kBwdWin; ++i)
+#pragma unroll
+              for (int o = 0; o < kBwdWin; o += 2) {
+                const double2 w = psi[(i * kBwdWin + o) / 2];
+                nt[o] = fma(w.x, T[i], nt[o]);
+                nt[o + 1] = fma(w.y, T[i], nt[o + 1]);
+              }
+#pragma unroll
+            for (int o = 0; o < kBwdWin; ++o) myxh[o] = nt[o];  // lanes ln and ln + NL write the same values
           }
-#pragma unroll
-        for (int o = 0; o < kBwdWin; ++o) myxh[o] = nt[o];  // lanes ln and ln + NL write the same values
+        }
       }
-      __syncthreads();
-      if (pid == k - 1) {
-        const double* Xk = xch + ((size_t)k * NL + ln) * kXch + 8;
-#pragma unroll
-        for (int t = 0; t < kBwdWin; ++t) T[t] = Xk[t];
-      }
+      // this warp's lowest partition has written its output: hand it up
+      __syncwarp();
+      if (h == 0 && warp >= 1) asm volatile("bar.sync %0, %1;" ::"r"(warp), "r"(64) : "memory");
     }
     __syncwarp();  // the ring is reused by B3
   }
