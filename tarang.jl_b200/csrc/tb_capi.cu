@@ -352,6 +352,14 @@ FactorSet* get_factors(tb_plan* P, int sy, double alpha, double beta) {
 }
 
 // F = -(u.grad) f in C^(2) rows (sfwd) or T coefficients (fwd) for f = b, ux, uz.
+// TF32 operand image of the mixed plan's transform matrix m (0..3 backward
+// even/odd values and derivatives, 4/5 forward to T rows, 6/7 forward to
+// C^(2) rows), or null when the plan has none (shapes past the tensor-core tile)
+const float* tc32_image(const tb_plan* P, int m) {
+  if (P->tcAimg.bytes < (size_t)(m + 1) * tc32_a_image_floats() * sizeof(float)) return nullptr;
+  return P->tcAimg.as<float>() + (size_t)m * tc32_a_image_floats();
+}
+
 // Mixed precision: the same RHS program on FP32 data; F is written in FP64.
 void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
   const int N = P->Nz, H = P->Hz;
@@ -366,11 +374,16 @@ void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2row
   for (int f = 0; f < 3; ++f) {
     const float* in = reinterpret_cast<const float*>(X32 + (size_t)f * P->plane);
     const float* Am[4] = {P->bEv32.as<float>(), P->bOv32.as<float>(), P->bEd32.as<float>(), P->bOd32.as<float>()};
-    for (int w = 0; w < 4; ++w)
-      bt.item[nb++] = GemmItem32{Am[w], in, gp(f, w), H, (w & 1) ? P->Ko : P->Ke, pad16k((w & 1) ? P->Ko : P->Ke),
-                                 GEMM_PARITY, w & 1};
+    for (int w = 0; w < 4; ++w) {
+      bt.item[nb] = GemmItem32{Am[w], in, gp(f, w), H, (w & 1) ? P->Ko : P->Ke, pad16k((w & 1) ? P->Ko : P->Ke),
+                               GEMM_PARITY, w & 1};
+      bt.item[nb++].Aimg = tc32_image(P, w);
+    }
   }
-  timed(P, "z_backward_gemm", [&] { launch_gemm_f32_path(bt, nb, ncol, ncol, ncol, N, false, P->st, P->tc32); });
+  float* bsc = P->tcBimg.as<float>();
+  const size_t bscn = P->tcBimg.bytes / sizeof(float);
+  timed(P, "z_backward_gemm",
+        [&] { launch_gemm_f32_path(bt, nb, ncol, ncol, ncol, N, false, P->st, P->tc32, bsc, bscn); });
   XProdArgs32 xa{};
   for (int f = 0; f < 3; ++f) {
     xa.ev[f] = gp(f, 0);
@@ -404,13 +417,17 @@ void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2row
   for (int f = 0; f < 3; ++f) {
     const float* in = reinterpret_cast<const float*>(P->H32.as<float2>() + (size_t)f * P->plane);
     double* out = reinterpret_cast<double*>(out3 + (size_t)f * P->plane);
-    bf.item[nb++] = GemmItem32{c2rows ? P->sfE32.as<float>() : P->fE32.as<float>(), in, out, P->Ke, H, pad16k(H),
-                               GEMM_MIRROR, 0};
-    if (P->Ko > 0)
-      bf.item[nb++] = GemmItem32{c2rows ? P->sfO32.as<float>() : P->fO32.as<float>(), in, out, P->Ko, H, pad16k(H),
-                                 GEMM_MIRROR, 1};
+    bf.item[nb] = GemmItem32{c2rows ? P->sfE32.as<float>() : P->fE32.as<float>(), in, out, P->Ke, H, pad16k(H),
+                             GEMM_MIRROR, 0};
+    bf.item[nb++].Aimg = tc32_image(P, c2rows ? 6 : 4);
+    if (P->Ko > 0) {
+      bf.item[nb] = GemmItem32{c2rows ? P->sfO32.as<float>() : P->fO32.as<float>(), in, out, P->Ko, H, pad16k(H),
+                               GEMM_MIRROR, 1};
+      bf.item[nb++].Aimg = tc32_image(P, c2rows ? 7 : 5);
+    }
   }
-  timed(P, "z_forward_gemm", [&] { launch_gemm_f32_path(bf, nb, ncol, ncol, ncol, N, true, P->st, P->tc32); });
+  timed(P, "z_forward_gemm",
+        [&] { launch_gemm_f32_path(bf, nb, ncol, ncol, ncol, N, true, P->st, P->tc32, bsc, bscn); });
 }
 
 void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
@@ -845,8 +862,8 @@ size_t tb::plan_device_bytes(const tb_plan* P) {
   b += rbc3d_device_bytes(P) + P->kappa_m.bytes + P->nu_m.bytes;
   for (const DevBuf& d : P->sys[0].mband) b += d.bytes;
   for (const DevBuf& d : P->sys[0].mbord) b += d.bytes;
-  const DevBuf* m32[] = {&P->X32,  &P->G32,  &P->H32,  &P->bEv32, &P->bOv32, &P->bEd32,
-                         &P->bOd32, &P->fE32, &P->fO32, &P->sfE32, &P->sfO32, &P->ptwM32};
+  const DevBuf* m32[] = {&P->X32,  &P->G32,  &P->H32,  &P->bEv32, &P->bOv32,  &P->bEd32, &P->bOd32,
+                         &P->fE32, &P->fO32, &P->sfE32, &P->sfO32, &P->ptwM32, &P->tcAimg, &P->tcBimg};
   for (const DevBuf* d : m32) b += d->bytes;
   return b;
 }
@@ -1189,6 +1206,22 @@ void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, i
       upload(P->iptwM32, it32);
       TB_REQUIRE(xprod32_smem_bytes(P->M, (int)pt32.size()) <= 227 * 1024, TB_ENOTSUPPORTED,
                  "Nx too large for the FP32 x kernel");
+      // TF32 operand images of the eight transform matrices for the
+      // tensor-core GEMMs, and the scratch of their per-call B images (six
+      // distinct inputs per GEMM), when the shapes fit one tensor-core tile
+      if (P->Hz <= 128 && pad16(P->Ke) <= 128) {
+        const size_t fa = tc32_a_image_floats();
+        P->tcAimg.alloc(8 * fa * sizeof(float));
+        const DevBuf* mats[8] = {&P->bEv32, &P->bOv32, &P->bEd32, &P->bOd32, &P->fE32, &P->fO32, &P->sfE32, &P->sfO32};
+        const int rows[8] = {P->Hz, P->Hz, P->Hz, P->Hz, P->Ke, P->Ko, P->Ke, P->Ko};
+        const int kps[8] = {pad16(P->Ke), pad16(P->Ko), pad16(P->Ke), pad16(P->Ko),
+                            pad16(P->Hz), pad16(P->Hz), pad16(P->Hz), pad16(P->Hz)};
+        for (int m = 0; m < 8; ++m)
+          if (rows[m] > 0) make_tc32_a_image(mats[m]->as<float>(), rows[m], kps[m], P->tcAimg.as<float>() + m * fa, P->st);
+        TB_CUDA_TRY(cudaGetLastError());
+        TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+        P->tcBimg.alloc(tc32_b_scratch_floats(2 * P->Nk, 6) * sizeof(float));
+      }
       TB_CUDA_TRY(set_mixed_smem_limits(227 * 1024));
     }
     // tau systems: the coupled Boussinesq system (with |k| per mode in 3D) and,

@@ -221,6 +221,10 @@ struct tb_plan {
   // mixed precision (TB_PREC_MIXED): FP32 copies for the RHS program
   bool mixed = false;
   DevBuf X32, G32, H32, bEv32, bOv32, bEd32, bOd32, fE32, fO32, sfE32, sfO32, ptwM32, iptwM32;
+  // tensor-core transform GEMMs: TF32 hi/lo images of the eight matrices above
+  // (empty when the shapes exceed one tensor-core tile) and the per-call
+  // scratch of the B-operand images
+  DevBuf tcAimg, tcBimg;
   // profiling: eager launches bracketed by events, accumulated per kernel name
   bool profiling = false;
   struct ProfRec {

@@ -7,21 +7,25 @@
 // C (M x ncol) = A (M x K) . B' (K x ncol), B' row k = B[k] (plain),
 // B[2k + par] (parity), B[j] + sgn B[N-1-j] (mirror, output row 2r + par).
 //
-// One CTA of 4 warps owns one item and a strided set of 64-column tiles.
-// Operands are split into TF32 hi/lo while they are staged: A rows as float4
-// chunks, B as four K-consecutive values of one column per thread, each
-// written as one 16-byte swizzled chunk (the eight lanes of a shared-memory
-// phase hit eight distinct chunks: no bank conflicts).  The accumulator goes
-// back through shared memory so the global stores are row-contiguous.
-// Shared memory (1024-byte aligned, the 128-byte swizzle's period):
-//   A_hi, A_lo: 128 x 128 TF32, K-major, 128-byte swizzle, loaded once;
-//   B_hi, B_lo:  64 x 128 TF32, K-major, 128-byte swizzle, one tile at a time.
-// A K-major tile is stored as [k / 32][row][128 B] with 8-row atoms of 1024 B
-// (stride byte offset 1024) and the 16-byte chunk index of a row XORed with
-// row % 8.  One thread issues the 3 x K/8 MMAs (M 128, N 64, K 8 each),
-// commits them to an mbarrier, and every warp then reads its 32 accumulator
-// lanes (rows) with tcgen05.ld and stores them.  M <= 128 and K <= 128
-// (Chebyshev degrees up to 256); larger shapes use k_gemm_f32.
+// Operand images.  The tensor cores read K-major tiles with the 128-byte
+// swizzle: a tile of `rows` rows is stored as [k / 32][row][128 B], 8-row atoms
+// of 1024 B (stride byte offset 1024), the 16-byte chunk index of a row XORed
+// with row % 8.  Both operands are prepared in global memory in exactly that
+// form, TF32 hi part then lo part:
+//   A (the constant transform matrix, M <= 128, K <= 128): once per plan,
+//     128 KB (k_tc32_image_a);
+//   B' (the data): per call, one 64 KB image per 64-column tile of every
+//     distinct input (k_tc32_image_b; the value and derivative matrices of a
+//     field share one input), the parity / mirror row maps applied while the
+//     image is written.
+// The GEMM kernel then moves operands with bulk copies (cp.async.bulk, one
+// thread, completion on an mbarrier): A once per CTA, B one tile ahead - the
+// next tile's copy is issued as soon as the MMAs of the current one have
+// completed, so it overlaps the epilogue.  One CTA of 4 warps owns one item
+// and a strided set of 64-column tiles; one thread issues the 3 x K/8 MMAs
+// (M 128, N 64, K 8 each) and commits them to an mbarrier; every warp reads its
+// 32 accumulator lanes (rows) with tcgen05.ld and the tile leaves through a
+// shared-memory stage for row-contiguous stores.  Every wait is bounded.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -36,9 +40,13 @@ constexpr int kTcM = 128, kTcN = 64, kTcK = 128, kTcThreads = 128;
 constexpr uint32_t kABytes = kTcM * kTcK * 4;  // one TF32 copy of the A tile
 constexpr uint32_t kBBytes = kTcN * kTcK * 4;  // one TF32 copy of a B tile
 constexpr uint32_t kOffAhi = 0, kOffAlo = kABytes, kOffBhi = 2 * kABytes, kOffBlo = 2 * kABytes + kBBytes;
-constexpr uint32_t kOffBar = 2 * kABytes + 2 * kBBytes;  // mbarrier (8 B), then the TMEM address (4 B)
-constexpr uint32_t kTcSmem = kOffBar + 64 + 1024;        // + alignment slack
-constexpr uint32_t kTmemCols = 64;                       // N fp32 accumulator columns
+constexpr int kStageLd = 33;                                         // epilogue stage row stride (elements)
+constexpr uint32_t kOffStage = 2 * kABytes + 2 * kBBytes;            // [row][33] of the output type
+constexpr uint32_t kOffBar = kOffStage + kTcM * kStageLd * 8;        // mbarriers A, B, MMA (8 B each), TMEM address
+constexpr uint32_t kTcSmem = kOffBar + 64 + 1024;                    // + alignment slack
+static_assert(kTcSmem <= 232448, "one CTA per SM");
+constexpr uint32_t kTmemCols = 64;                                   // N fp32 accumulator columns
+constexpr uint32_t kImageChunk = 16384;                              // bytes per bulk copy
 // spin limit of the MMA-completion wait (about a second); past it the CTA
 // flags the error and skips its stores
 constexpr long long kTcSpinLimit = 1LL << 26;
@@ -97,102 +105,149 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
+// bounded wait on an mbarrier phase: false after kTcSpinLimit polls
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  long long spins = 0;
+  while (!mbar_try_wait(bar, parity))
+    if (++spins > kTcSpinLimit) return false;
+  return true;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// bytes (a multiple of kImageChunk) from global src to shared dst, completing on bar
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  for (uint32_t o = 0; o < bytes; o += kImageChunk)
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst + o),
+        "l"(static_cast<const char*>(src) + o), "r"(kImageChunk), "r"(bar)
+        : "memory");
+}
+
+// A image: rows r < M of A (row stride Kpad, columns past K zero), four
+// K-consecutive values per thread and step, split into TF32 hi / lo.
+__global__ void __launch_bounds__(kTcThreads) k_tc32_image_a(const float* __restrict__ A, int M, int Kp,
+                                                             float* __restrict__ image) {
+  uint8_t* hi = reinterpret_cast<uint8_t*>(image);
+  uint8_t* lo = hi + kABytes;
+  for (int idx = threadIdx.x; idx < kTcM * (kTcK / 4); idx += kTcThreads) {
+    const int r = idx / (kTcK / 4), k = 4 * (idx % (kTcK / 4));
+    const float4 v = (r < M && k < Kp) ? *reinterpret_cast<const float4*>(A + (size_t)r * Kp + k)
+                                       : make_float4(0.f, 0.f, 0.f, 0.f);
+    split_store4(hi, lo, sw128_off(r, k, kTcM), v);
+  }
+}
+
+// B' images: one CTA per (64-column tile, distinct input); thread (column n,
+// K-chunk kc) gathers rows 4 kc .. 4 kc + 3 of column n0 + n through the row
+// map (sixteen loads in flight, mirror partners included) and writes them as
+// one swizzled 16-byte chunk of each of the hi and lo parts.
+struct Tc32BInput {
+  const float* B;
+  float* image;  // ntiles images of 2 kBBytes
+  int K, mode, par;
+};
+struct Tc32BInputs {
+  Tc32BInput in[kGemmMaxBatch];
+};
+__global__ void __launch_bounds__(kTcThreads) k_tc32_image_b(Tc32BInputs bi, int ncol, int ldb, int Nrows) {
+  const Tc32BInput& im = bi.in[blockIdx.y];
+  const float* __restrict__ B = im.B;
+  const int K = im.K, mode = im.mode, par = im.par;
+  const bool mirror = mode == GEMM_MIRROR;
+  const float sgn = par ? -1.f : 1.f;
+  const int midk = (mirror && (Nrows & 1)) ? (Nrows - 1) / 2 : -1;
+  const int tid = threadIdx.x, n0 = blockIdx.x * kTcN;
+  uint8_t* hi = reinterpret_cast<uint8_t*>(im.image) + (size_t)blockIdx.x * 2 * kBBytes;
+  uint8_t* lo = hi + kBBytes;
+  const int n = tid % kTcN, gc = n0 + n;
+  const bool colok = gc < ncol;
+  constexpr int KCS = kTcThreads / kTcN;  // K-chunks started per step (2)
+  constexpr int NKC = kTcK / 4 / KCS;     // K-chunks per thread (16)
+  constexpr int CB = 4;                   // chunks per batch: 16 loads in flight
+  static_assert(NKC % CB == 0, "B batches");
+  for (int c0 = 0; c0 < NKC; c0 += CB) {
+    float e[CB][4], w[CB][4];
+#pragma unroll
+    for (int c = 0; c < CB; ++c)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int k = 4 * (tid / kTcN + (c0 + c) * KCS) + i;
+        const bool ok = colok && k < K;
+        const int srow = mode == GEMM_PARITY ? 2 * k + par : k;
+        e[c][i] = ok ? B[(size_t)srow * ldb + gc] : 0.f;
+        w[c][i] = (ok && mirror && k != midk) ? B[(size_t)(Nrows - 1 - k) * ldb + gc] : 0.f;
+      }
+#pragma unroll
+    for (int c = 0; c < CB; ++c) {
+      const int kc = tid / kTcN + (c0 + c) * KCS;
+      float f[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int k = 4 * kc + i;
+        f[i] = mirror ? ((k == midk) ? (par ? 0.f : e[c][i]) : fmaf(sgn, w[c][i], e[c][i])) : e[c][i];
+      }
+      split_store4(hi, lo, sw128_off(n, 4 * kc, kTcN), make_float4(f[0], f[1], f[2], f[3]));
+    }
+  }
+}
+
 template <class OutT>
-__global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int ncol, int ldb, int ldc, int Nrows) {
+__global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int ncol, int ldc) {
   extern __shared__ uint8_t tc_smem_raw[];
   const uint32_t raw = (uint32_t)__cvta_generic_to_shared(tc_smem_raw);
   const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
   uint8_t* sm = tc_smem_raw + pad;
   const uint32_t sbase = raw + pad;
-  const uint32_t bar = sbase + kOffBar;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kOffBar + 8);
+  const uint32_t barA = sbase + kOffBar, barB = barA + 8, barM = barA + 16;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kOffBar + 24);
 
   const GemmItem32& it = bt.item[blockIdx.z];
-  const float* __restrict__ A = it.A;
-  const float* __restrict__ B = it.B;
-  const int Mo = it.M, K = it.K, Kp = it.Kpad, mode = it.mode, par = it.par;
+  const int Mo = it.M, K = it.K, mode = it.mode, par = it.par;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const int ntiles = (ncol + kTcN - 1) / kTcN;
   const bool mirror = mode == GEMM_MIRROR;
-  const float sgn = par ? -1.f : 1.f;
-  const int midk = (mirror && (Nrows & 1)) ? (Nrows - 1) / 2 : -1;
   const int nk8 = (K + 7) / 8;
+  const int t0 = blockIdx.x;
 
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + kOffBar + 8),
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + kOffBar + 24),
                  "r"(kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
+  // copies in flight (issued by thread 0, waited by every thread)
+  bool a_pending = false, b_pending = false;
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barA));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barB));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barM));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
-  }
-  // A once, four K-consecutive values per thread and step (Kpad is a multiple
-  // of 16 and the padding columns are zero); rows >= M are zero
-  // (eight loads in flight per thread before any is split and stored)
-  constexpr int AQ = kTcM * (kTcK / 4) / kTcThreads, AB = 8;  // float4 per thread, per batch
-  static_assert(AQ % AB == 0, "A batches");
-  for (int q0 = 0; q0 < AQ; q0 += AB) {
-    float4 v[AB];
-#pragma unroll
-    for (int i = 0; i < AB; ++i) {
-      const int idx = tid + (q0 + i) * kTcThreads;
-      const int r = idx / (kTcK / 4), k = 4 * (idx % (kTcK / 4));
-      v[i] = (r < Mo && k < Kp) ? *reinterpret_cast<const float4*>(A + (size_t)r * Kp + k)
-                                : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-#pragma unroll
-    for (int i = 0; i < AB; ++i) {
-      const int idx = tid + (q0 + i) * kTcThreads;
-      split_store4(sm + kOffAhi, sm + kOffAlo, sw128_off(idx / (kTcK / 4), 4 * (idx % (kTcK / 4)), kTcM), v[i]);
+    mbar_expect_tx(barA, 2 * kABytes);
+    bulk_copy(sbase + kOffAhi, it.Aimg, 2 * kABytes, barA);
+    if (t0 < ntiles) {
+      mbar_expect_tx(barB, 2 * kBBytes);
+      bulk_copy(sbase + kOffBhi, it.Bimg + (size_t)t0 * (2 * kBBytes / 4), 2 * kBBytes, barB);
     }
   }
+  a_pending = true;
+  b_pending = t0 < ntiles;
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
   const uint32_t tmem = *tmem_slot;
 
-  uint32_t phase = 0;
-  bool ok = true;
-  for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+  uint32_t pb = 0, pm = 0;
+  bool ok = __syncthreads_and(mbar_wait_bounded(barA, 0)) != 0;  // one decision for the whole CTA
+  if (ok) a_pending = false;
+  bool mma_pending = false;
+  for (int t = t0; t < ntiles && ok; t += gridDim.x) {
     const int n0 = t * kTcN;
-    // B' tile: thread (column n, K-chunk kc) loads rows 4 kc .. 4 kc + 3 of
-    // column n0 + n (the lanes of a warp read consecutive columns of one row)
-    {
-      const int n = tid % kTcN, gc = n0 + n;
-      const bool colok = gc < ncol;
-      constexpr int KCS = kTcThreads / kTcN;       // K-chunks started per step (2)
-      constexpr int NKC = kTcK / 4 / KCS;          // K-chunks per thread (16)
-      constexpr int CB = 4;                        // chunks per batch: 16 loads in flight
-      static_assert(NKC % CB == 0, "B batches");
-      for (int c0 = 0; c0 < NKC; c0 += CB) {
-        float e[CB][4], w[CB][4];
-#pragma unroll
-        for (int c = 0; c < CB; ++c)
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const int k = 4 * (tid / kTcN + (c0 + c) * KCS) + i;
-            const bool ok = colok && k < K;
-            const int srow = mode == GEMM_PARITY ? 2 * k + par : k;
-            e[c][i] = ok ? B[(size_t)srow * ldb + gc] : 0.f;
-            w[c][i] = (ok && mirror && k != midk) ? B[(size_t)(Nrows - 1 - k) * ldb + gc] : 0.f;
-          }
-#pragma unroll
-        for (int c = 0; c < CB; ++c) {
-          const int kc = tid / kTcN + (c0 + c) * KCS;
-          float f[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const int k = 4 * kc + i;
-            f[i] = mirror ? ((k == midk) ? (par ? 0.f : e[c][i]) : fmaf(sgn, w[c][i], e[c][i])) : e[c][i];
-          }
-          split_store4(sm + kOffBhi, sm + kOffBlo, sw128_off(n, 4 * kc, kTcN), make_float4(f[0], f[1], f[2], f[3]));
-        }
-      }
-    }
-    // generic-proxy stores -> visible to the tensor core (async proxy)
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    __syncthreads();
+    ok = __syncthreads_and(mbar_wait_bounded(barB, pb)) != 0;
+    if (!ok) break;
+    b_pending = false;
+    pb ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
     if (tid == 0) {
       for (int j = 0; j < nk8; ++j) {
@@ -204,27 +259,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int
         mma_tf32(tmem, ahi, blo, 1u);
         mma_tf32(tmem, alo, bhi, 1u);
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(barM)
                    : "memory");
     }
-    long long spins = 0;
-    bool done = true;
-    while (!mbar_try_wait(bar, phase)) {
-      if (++spins > kTcSpinLimit) {
-        done = false;
-        break;
-      }
-    }
-    phase ^= 1u;
-    ok = __syncthreads_and(done) != 0;  // one decision for the whole CTA
-    if (!ok) {
-      if (tid == 0) atomicExch(&g_tc_timeout, 1);
-      break;
-    }
+    mma_pending = true;
+    ok = __syncthreads_and(mbar_wait_bounded(barM, pm)) != 0;
+    if (!ok) break;
+    mma_pending = false;
+    pm ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    // the MMAs have read B: the next tile's image streams in during the epilogue
+    const int tn = t + gridDim.x;
+    if (tn < ntiles) {
+      if (tid == 0) {
+        mbar_expect_tx(barB, 2 * kBBytes);
+        bulk_copy(sbase + kOffBhi, it.Bimg + (size_t)tn * (2 * kBBytes / 4), 2 * kBBytes, barB);
+      }
+      b_pending = true;
+    }
     const int r = warp * 32 + lane;  // accumulator lane = output row of this thread
-    OutT* stage = reinterpret_cast<OutT*>(sm + kOffBhi);  // [row][33]: the MMAs no longer read B
-    constexpr int SLD = 33;
+    OutT* stage = reinterpret_cast<OutT*>(sm + kOffStage);
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
       uint32_t v[32];
@@ -239,7 +293,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-      for (int c = 0; c < 32; ++c) stage[r * SLD + c] = (OutT)__uint_as_float(v[c]);
+      for (int c = 0; c < 32; ++c) stage[r * kStageLd + c] = (OutT)__uint_as_float(v[c]);
       __syncthreads();
       // row-contiguous stores: a warp writes 32 consecutive columns of one row
       for (int idx = tid; idx < kTcM * 32; idx += kTcThreads) {
@@ -247,16 +301,25 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int
         const int gc = n0 + half * 32 + c;
         if (rr < Mo && gc < ncol) {
           const int orow = mirror ? 2 * rr + par : rr;
-          reinterpret_cast<OutT*>(it.C)[(size_t)orow * ldc + gc] = stage[rr * SLD + c];
+          reinterpret_cast<OutT*>(it.C)[(size_t)orow * ldc + gc] = stage[rr * kStageLd + c];
         }
       }
       __syncthreads();
     }
-    // every warp has read the accumulator and the MMAs have read B: the next
-    // tile may overwrite both
+    // every warp has read the accumulator: the next tile's MMAs may overwrite it
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  }
+  if (!ok) {
+    // a wait ran out: flag it, give the copies and MMAs still in flight a
+    // bounded time to land (they write this CTA's shared and tensor memory)
+    if (tid == 0) {
+      atomicExch(&g_tc_timeout, 1);
+      if (a_pending) mbar_wait_bounded(barA, 0);
+      if (b_pending) mbar_wait_bounded(barB, pb);
+      if (mma_pending) mbar_wait_bounded(barM, pm);
+    }
   }
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols));
@@ -266,8 +329,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int
 
 bool gemm_tc32_supported(const GemmBatch32& bt, int nbatch) {
   for (int b = 0; b < nbatch; ++b)
-    if (bt.item[b].M > kTcM || bt.item[b].K > kTcK) return false;
+    if (bt.item[b].M > kTcM || bt.item[b].K > kTcK || bt.item[b].Kpad > kTcK) return false;
   return true;
+}
+
+size_t tc32_a_image_floats() { return 2 * kABytes / 4; }
+
+size_t tc32_b_scratch_floats(int ncol, int nimages) {
+  const size_t ntiles = (size_t)(ncol + kTcN - 1) / kTcN;
+  return (size_t)nimages * ntiles * (2 * kBBytes / 4);
+}
+
+void make_tc32_a_image(const float* A, int M, int Kpad, float* image, cudaStream_t st) {
+  k_tc32_image_a<<<1, kTcThreads, 0, st>>>(A, M, Kpad, image);
 }
 
 cudaError_t set_tc32_smem_limits() {
@@ -276,30 +350,38 @@ cudaError_t set_tc32_smem_limits() {
   return cudaFuncSetAttribute(k_gemm_tc32<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
 }
 
-namespace {
-int tc32_ctas_per_item(int ncol, int nbatch) {
+bool launch_gemm_tc32(const GemmBatch32& bt_in, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
+                      cudaStream_t st, float* bscratch, size_t bscratch_floats) {
+  if (!bscratch || nbatch < 1 || nbatch > kGemmMaxBatch) return false;
+  GemmBatch32 bt = bt_in;
+  Tc32BInputs bi{};
+  int nimg = 0;
+  const size_t per = tc32_b_scratch_floats(ncol, 1);
+  for (int b = 0; b < nbatch; ++b) {
+    GemmItem32& it = bt.item[b];
+    if (!it.Aimg) return false;
+    int j = 0;
+    while (j < nimg && !(bi.in[j].B == it.B && bi.in[j].K == it.K && bi.in[j].mode == it.mode &&
+                         (it.mode == GEMM_PLAIN || bi.in[j].par == it.par)))
+      ++j;
+    if (j == nimg) {
+      if ((size_t)(nimg + 1) * per > bscratch_floats) return false;
+      bi.in[nimg] = Tc32BInput{it.B, bscratch + (size_t)nimg * per, it.K, it.mode, it.par};
+      ++nimg;
+    }
+    it.Bimg = bi.in[j].image;
+  }
   const int ntiles = (ncol + kTcN - 1) / kTcN;
-  int per = 148 / nbatch;  // one wave of CTAs (one per SM by shared memory)
-  if (per < 1) per = 1;
-  if (per > ntiles) per = ntiles;
-  return per;
-}
-}  // namespace
-
-int gemm_tc32_tiles_per_cta(int ncol, int nbatch) {
-  const int ntiles = (ncol + kTcN - 1) / kTcN;
-  const int per = tc32_ctas_per_item(ncol, nbatch);
-  return (ntiles + per - 1) / per;
-}
-
-void launch_gemm_tc32(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
-                      cudaStream_t st) {
-  const int per = tc32_ctas_per_item(ncol, nbatch);
-  dim3 grid(per, 1, nbatch);
+  k_tc32_image_b<<<dim3(ntiles, nimg), kTcThreads, 0, st>>>(bi, ncol, ldb, Nrows);
+  int cpi = 148 / nbatch;  // CTAs per item: one wave, one CTA per SM by shared memory
+  if (cpi < 1) cpi = 1;
+  if (cpi > ntiles) cpi = ntiles;
+  dim3 grid(cpi, 1, nbatch);
   if (out_f64)
-    k_gemm_tc32<double><<<grid, kTcThreads, kTcSmem, st>>>(bt, ncol, ldb, ldc, Nrows);
+    k_gemm_tc32<double><<<grid, kTcThreads, kTcSmem, st>>>(bt, ncol, ldc);
   else
-    k_gemm_tc32<float><<<grid, kTcThreads, kTcSmem, st>>>(bt, ncol, ldb, ldc, Nrows);
+    k_gemm_tc32<float><<<grid, kTcThreads, kTcSmem, st>>>(bt, ncol, ldc);
+  return true;
 }
 
 int tc32_status() {
