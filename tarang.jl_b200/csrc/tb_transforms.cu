@@ -19,7 +19,7 @@ namespace tb {
 
 // ---------------------------------------------------------------------------
 // FP64 batched GEMM for the Chebyshev direction on the FP64 tensor cores
-// (mma.sync m16n8k8 .f64).  CTA tile 64 x 64 (4 warps, 32 x 32 each), 16-deep
+// (mma.sync m8n8k4 .f64).  CTA tile 64 x 64 (4 warps, 32 x 32 each), 16-deep
 // K slices double-buffered in shared memory with cp.async.  Each batch entry
 // carries its own A (rows padded to a multiple of 16 doubles) and a B-row map:
 //   GEMM_PLAIN   : B row k = in[k]
@@ -44,23 +44,16 @@ __device__ __forceinline__ void g_commit() { asm volatile("cp.async.commit_group
 __device__ __forceinline__ void g_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 __device__ __forceinline__ void g_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
-// D (16 x 8) += A (16 x 8, row) B (8 x 8, col), FP64.  Lane (g = lane / 4,
-// t = lane % 4) holds A rows g and g + 8 at columns t and t + 4 (a0: (g, t),
-// a1: (g + 8, t), a2: (g, t + 4), a3: (g + 8, t + 4)), B column g at rows t and
-// t + 4 (b0, b1), and D row g (d0, d1) and row g + 8 (d2, d3) at columns
-// 2t, 2t + 1.
-__device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
 }
 
 // SPLITK = false: CTA tile 64 x 64, warp (wm, wn) owns rows wm*32.., cols wn*32..
 // SPLITK = true:  CTA tile 32 x 64 (twice the CTAs for short M), warp (wk, wn)
-//                 owns cols wn*32.. and the 8-deep half wk of every 16-deep
-//                 slice; the two k halves are summed through shared memory.
-// A warp's 32 x 32 block is 2 x 4 m16n8k8 tiles.
+//                 owns cols wn*32.. and the k-steps ks = 2 wk, 2 wk + 1 of every
+//                 16-deep slice; the two k halves are summed through shared memory.
 template <bool SPLITK>
 __global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ldb, int ldc, int Nrows) {
   constexpr int TM = SPLITK ? GBM / 2 : GBM;  // CTA tile rows
@@ -110,13 +103,11 @@ __global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ld
     g_commit();
   };
 
-  double acc[2][4][4];  // [m16 tile][n8 tile][fragment]
+  double acc[4][4][2];
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   const double sgn = par ? -1.0 : 1.0;
   // the middle row of odd N contributes once to the even sum and not at all to the odd one
   const int midk = (mirror && (Nrows & 1)) ? (Nrows - 1) / 2 : -1;
@@ -134,35 +125,26 @@ __global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ld
     const double* bs = Bs[buf];
     const double* bm = Bm[buf];
 #pragma unroll
-    for (int kq = 0; kq < (SPLITK ? 1 : GBK / 8); ++kq) {
-      const int ks = SPLITK ? wk : kq;  // 8-deep step of the slice
-      const int k0 = ks * 8 + tig, k1 = k0 + 4;
-      double a[2][4], b[4][2];
+    for (int kq = 0; kq < (SPLITK ? GBK / 8 : GBK / 4); ++kq) {
+      const int ks = SPLITK ? 2 * wk + kq : kq;
+      const int kk = ks * 4 + tig;
+      double a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int r = wm * 32 + i * 16 + gid;
-        a[i][0] = as[r * ASTR + k0];
-        a[i][1] = as[(r + 8) * ASTR + k0];
-        a[i][2] = as[r * ASTR + k1];
-        a[i][3] = as[(r + 8) * ASTR + k1];
+      for (int i = 0; i < 4; ++i) a[i] = as[(wm * 32 + i * 8 + gid) * ASTR + kk];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int cidx = kk * BSTR + wn * 32 + j * 8 + gid;
+        double v = bs[cidx];
+        if (mirror) {
+          const int gk = t * GBK + kk;
+          v = (gk == midk) ? (par ? 0.0 : v) : fma(sgn, bm[cidx], v);
+        }
+        b[j] = v;
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int kk = h ? k1 : k0;
-          const int cidx = kk * BSTR + wn * 32 + j * 8 + gid;
-          double v = bs[cidx];
-          if (mirror) {
-            const int gk = t * GBK + kk;
-            v = (gk == midk) ? (par ? 0.0 : v) : fma(sgn, bm[cidx], v);
-          }
-          b[j][h] = v;
-        }
-#pragma unroll
-      for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) dmma16(acc[i][j], a[i], b[j]);
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
     }
     __syncthreads();
   }
@@ -172,39 +154,39 @@ __global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ld
     double* red = gsm + (size_t)wn * 32 * 32;
     if (wk == 1) {
 #pragma unroll
-      for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-          for (int e = 0; e < 4; ++e) red[((i * 4 + j) * 4 + e) * 32 + lane] = acc[i][j][e];
+        for (int j = 0; j < 4; ++j) {
+          red[((i * 4 + j) * 2 + 0) * 32 + lane] = acc[i][j][0];
+          red[((i * 4 + j) * 2 + 1) * 32 + lane] = acc[i][j][1];
+        }
     }
     __syncthreads();
     if (wk == 1) return;
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) acc[i][j][e] += red[((i * 4 + j) * 4 + e) * 32 + lane];
-  }
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int hr = 0; hr < 2; ++hr) {
-      const int gr = row0 + wm * 32 + i * 16 + hr * 8 + gid;
-      if (gr >= Mo) continue;
-      const int orow = mirror ? 2 * gr + par : gr;
-      double* C = it.C + (size_t)orow * ldc;
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const int gc = col0 + wn * 32 + j * 8 + tig * 2;
-        if (gc + 1 < ncol) {
-          *reinterpret_cast<double2*>(C + gc) = make_double2(acc[i][j][2 * hr], acc[i][j][2 * hr + 1]);
-        } else if (gc < ncol) {
-          C[gc] = acc[i][j][2 * hr];
-        }
+        acc[i][j][0] += red[((i * 4 + j) * 2 + 0) * 32 + lane];
+        acc[i][j][1] += red[((i * 4 + j) * 2 + 1) * 32 + lane];
+      }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gr = row0 + wm * 32 + i * 8 + gid;
+    if (gr >= Mo) continue;
+    const int orow = mirror ? 2 * gr + par : gr;
+    double* C = it.C + (size_t)orow * ldc;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gc = col0 + wn * 32 + j * 8 + tig * 2;
+      if (gc + 1 < ncol) {
+        *reinterpret_cast<double2*>(C + gc) = make_double2(acc[i][j][0], acc[i][j][1]);
+      } else if (gc < ncol) {
+        C[gc] = acc[i][j][0];
       }
     }
+  }
 }
 }  // namespace
 
