@@ -11,14 +11,16 @@
 // tuner times candidate settings on the ensemble itself (from a snapshot that
 // is restored afterwards) and keeps the fastest.
 //
-// Fused form: members of one shape (Nx, Nz, domain, walls, RK stepper, precision)
+// Fused form: members of one shape (Nx, Nz, domain, walls, stepper, precision)
 // that step at the same dt are stacked along the mode axis into one plan
 // (build_plan with B instances): every kernel of a step then covers the whole
 // group in one launch - the tau solves over all the group's mode groups, the
 // transforms over all its columns - under one CUDA graph per group.  A run
 // gathers the members' states into the group plan, steps it, and scatters
-// the states back (one strided device copy per member each way).  The tuner
-// tries the fused form against the per-member form.
+// the states back (one strided device copy per member each way; SBDF members
+// also carry their history, F and M X of the previous step, and fuse only
+// when all of a group have the same history depth).  The tuner tries the
+// fused form against the per-member form.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -69,9 +71,9 @@ void ensure_streams(tb_ensemble* E, int n) {
 }
 
 bool fusible(const tb_plan* P) {
-  return P->ndim == 2 && P->B == 1 && !P->bc_dynamic && P->d.program == TB_PROGRAM_RBC &&
-         (P->d.timestepper == TB_RK222 || P->d.timestepper == TB_RK443);
+  return P->ndim == 2 && P->B == 1 && !P->bc_dynamic && P->d.program == TB_PROGRAM_RBC;
 }
+bool multistep(const tb_plan* P) { return P->d.timestepper == TB_SBDF1 || P->d.timestepper == TB_SBDF2; }
 
 bool same_shape(const tb_plan* a, const tb_plan* b) {
   const tb_problem_desc &x = a->d, &y = b->d;
@@ -103,19 +105,32 @@ void build_groups(tb_ensemble* E) {
 }
 
 // Copy the members' state rows (state planes and tau rows, Nkm modes each)
-// into / out of their columns of the group plan.
+// into / out of their columns of the group plan; SBDF members also their
+// history (F and M X of the previous step, equation planes of Nz rows) and
+// history depth.
 void move_states(tb_ensemble* E, tb_ensemble::Group& G, cudaStream_t s, bool gather) {
   tb_plan* Q = G.plan.get();
   const size_t w = (size_t)Q->Nkm * sizeof(double2), ldq = (size_t)Q->Nk * sizeof(double2);
   const size_t rows = (size_t)Q->nplanes * Q->Nz + Q->ntau;
+  const bool ms = multistep(Q);
+  const size_t hrows = (size_t)Q->nplanes * Q->Nz;
+  auto move = [&](DevBuf& qb, DevBuf& mb, size_t k, size_t nrows) {
+    char* q = static_cast<char*>(qb.p) + k * w;
+    if (gather)
+      TB_CUDA_TRY(cudaMemcpy2DAsync(q, ldq, mb.p, w, w, nrows, cudaMemcpyDeviceToDevice, s));
+    else
+      TB_CUDA_TRY(cudaMemcpy2DAsync(mb.p, w, q, ldq, w, nrows, cudaMemcpyDeviceToDevice, s));
+  };
   for (size_t k = 0; k < G.idx.size(); ++k) {
     tb_plan* M = E->members[G.idx[k]];
-    char* q = static_cast<char*>(Q->X.p) + k * w;
-    if (gather)
-      TB_CUDA_TRY(cudaMemcpy2DAsync(q, ldq, M->X.p, w, w, rows, cudaMemcpyDeviceToDevice, s));
-    else
-      TB_CUDA_TRY(cudaMemcpy2DAsync(M->X.p, w, q, ldq, w, rows, cudaMemcpyDeviceToDevice, s));
+    move(Q->X, M->X, k, rows);
+    if (ms && (gather ? M->ms_history : Q->ms_history) > 0) {
+      move(Q->Fprev, M->Fprev, k, hrows);
+      move(Q->MXprev, M->MXprev, k, hrows);
+    }
+    if (!gather && ms) M->ms_history = Q->ms_history;
   }
+  if (gather && ms) Q->ms_history = E->members[G.idx[0]]->ms_history;
 }
 
 // Fused run: each group (members at one dt) as its stacked plan on its own
@@ -129,7 +144,11 @@ void run_fused(tb_ensemble* E, const double* dt, int nsteps, int streams, int gs
   std::vector<tb_ensemble::Group*> live;
   for (auto& G : E->groups) {
     bool same_dt = true;
-    for (int j : G.idx) same_dt = same_dt && dt[j] == dt[G.idx[0]];
+    for (int j : G.idx) {
+      same_dt = same_dt && dt[j] == dt[G.idx[0]];
+      // multistep members fuse only at one history depth
+      same_dt = same_dt && E->members[j]->ms_history == E->members[G.idx[0]]->ms_history;
+    }
     if (!same_dt) continue;
     for (int j : G.idx) gi[j] = (int)live.size();
     live.push_back(&G);

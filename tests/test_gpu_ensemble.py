@@ -174,6 +174,44 @@ def test_fused_form_with_mixed_precision_members(tb, form):
         assert rel_l2(plans[k].get_state(2), ref.uz) < 1e-6
 
 
+FUSED_SBDF = [
+    (48, 24, 1e7, "SBDF2", 0.01),
+    (32, 16, 1e6, "SBDF2", 0.02),
+    (48, 24, 1e8, "SBDF2", 0.01),
+    (32, 16, 1e5, "SBDF2", 0.02),
+]
+
+
+def test_fused_form_with_multistep_members(tb):
+    # SBDF2 members stack with their history (F and M X of the previous step):
+    # the first fused run starts at SBDF1 and carries the history out; the
+    # second continues at SBDF2 from the scattered history
+    nsteps = 4
+    solo = []
+    for k, spec in enumerate(FUSED_SBDF):
+        _, plan = build(tb, spec, 110 + k)
+        plan.step(spec[4], nsteps + 3)
+        solo.append(states(plan))
+    pairs = [build(tb, spec, 110 + k) for k, spec in enumerate(FUSED_SBDF)]
+    plans = [pl for _, pl in pairs]
+    ens = tb.Ensemble(plans)
+    ens.set_form(True)
+    ens.set_config(2, 2)
+    ens.run([s[4] for s in FUSED_SBDF], nsteps)
+    fused, groups = ens.form()
+    assert fused and groups == 2
+    for k in (0, 3):
+        p, _ = pairs[k]
+        ref = run_rbc(p, "SBDF2", FUSED_SBDF[k][4], nsteps, seed=110 + k)
+        for got, want in zip(states(plans[k]), (ref.b, ref.ux, ref.uz)):
+            assert rel_l2(got, want) < 1e-10
+    ens.run([s[4] for s in FUSED_SBDF], 3)
+    for k, plan in enumerate(plans):
+        for a, b in zip(states(plan), solo[k]):
+            assert rel_l2(a, b) < 1e-12, f"member {k}"
+        assert abs(plan.sim_time() - (nsteps + 3) * FUSED_SBDF[k][4]) < 1e-12
+
+
 def test_tuner_may_choose_the_fused_form(tb):
     plans = [build(tb, spec, 90 + k)[1] for k, spec in enumerate(FUSED)]
     before = [pl.get_state(0) for pl in plans]
