@@ -121,9 +121,23 @@ __global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ld
       g_commit();
     g_wait1();
     __syncthreads();
+    if (mirror) {
+      // fold the mirror partners into the B slice once, in place: row j of
+      // B' = in[j] + sgn in[N-1-j] (the middle row of odd N once / not at all)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int ch = tid + q * GTH;
+        const int kk = ch >> 5, cc = (ch & 31) * 2;
+        const int gk = t * GBK + kk;
+        double2* bp = reinterpret_cast<double2*>(&Bs[buf][kk * BSTR + cc]);
+        const double2 v = *bp, w = *reinterpret_cast<const double2*>(&Bm[buf][kk * BSTR + cc]);
+        *bp = (gk == midk) ? (par ? make_double2(0.0, 0.0) : v)
+                           : make_double2(fma(sgn, w.x, v.x), fma(sgn, w.y, v.y));
+      }
+      __syncthreads();
+    }
     const double* as = As[buf];
     const double* bs = Bs[buf];
-    const double* bm = Bm[buf];
 #pragma unroll
     for (int kq = 0; kq < (SPLITK ? GBK / 8 : GBK / 4); ++kq) {
       const int ks = SPLITK ? 2 * wk + kq : kq;
@@ -132,15 +146,7 @@ __global__ void __launch_bounds__(GTH) k_gemm_f64(GemmBatch bt, int ncol, int ld
 #pragma unroll
       for (int i = 0; i < 4; ++i) a[i] = as[(wm * 32 + i * 8 + gid) * ASTR + kk];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int cidx = kk * BSTR + wn * 32 + j * 8 + gid;
-        double v = bs[cidx];
-        if (mirror) {
-          const int gk = t * GBK + kk;
-          v = (gk == midk) ? (par ? 0.0 : v) : fma(sgn, bm[cidx], v);
-        }
-        b[j] = v;
-      }
+      for (int j = 0; j < 4; ++j) b[j] = bs[kk * BSTR + wn * 32 + j * 8 + gid];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
