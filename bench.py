@@ -635,6 +635,7 @@ def summarize(out: dict) -> dict:
     if "serving" in out:
         s["serving"] = {"saturated": g(out, "serving", "saturated", "solves_per_s"),
                         "plain_saturated": g(out, "serving", "plain_gpu_saturated", "solves_per_s"),
+                        "saturated_cohorts": g(out, "serving", "saturated_with_cohorts", "solves_per_s"),
                         "replay_p50_ms": g(out, "serving", "replay", "p50_ms"),
                         "replay_p99_ms": g(out, "serving", "replay", "p99_ms")}
     return s
@@ -1219,9 +1220,10 @@ def run_serving(args, dev, dist=None):
             prepared.append((tb.turb_desc(r.N, r.N, r.nu), r.dt, r.nsteps, W.turb_initial_spec(r.N, r.seed)))
     budget = int(args.serve_budget_gb * (1 << 30))
 
-    def replay(max_running, timed_arrivals, chunk=10, subset=None):
+    def replay(max_running, timed_arrivals, chunk=10, subset=None, cohort=1):
         subset = mine if subset is None else (subset & mine)
         srv = tb.Server(budget_bytes=budget, max_running=max_running, chunk_steps=chunk, device=dev)
+        srv.set_cohort(cohort)
         t0 = time.perf_counter()
         ids, steps = [], 0
         for k, r in enumerate(reqs):
@@ -1243,7 +1245,8 @@ def run_serving(args, dev, dist=None):
         part = {"completed": int(st["completed"]), "steps": steps, "wall_s": wall,
                 "tts_ms": [float(p[1]) for p in polls], "failed": int(st["failed"]), "all_done": ok,
                 "peak_running": int(st["peak_running"]), "peak_bytes": int(st["peak_bytes"]),
-                "mean_wait_ms": float(st["mean_wait_ms"]), "mean_setup_ms": float(st["mean_setup_ms"])}
+                "mean_wait_ms": float(st["mean_wait_ms"]), "mean_setup_ms": float(st["mean_setup_ms"]),
+                "peak_cohort": int(st["peak_cohort"]), "cohort_requests": int(st["cohort_requests"])}
         parts = dist.gather(part) if dist else [part]
         agg = W.combine_serving(parts)
         return {"solves_per_s": agg["solves_per_s"], "steps_per_s": agg["steps_per_s"], "p50_ms": agg["p50_ms"],
@@ -1252,7 +1255,9 @@ def run_serving(args, dev, dist=None):
                 "peak_running": max(p["peak_running"] for p in parts),
                 "peak_budgeted_bytes": max(p["peak_bytes"] for p in parts), "completed": agg["completed"],
                 "failed": sum(p["failed"] for p in parts), "wall_s": agg["wall_s"],
-                "all_done": all(p["all_done"] for p in parts)}
+                "all_done": all(p["all_done"] for p in parts),
+                "peak_cohort": max(p["peak_cohort"] for p in parts),
+                "cohort_requests": sum(p["cohort_requests"] for p in parts)}
 
     # warm-up: one request of every kind and size (kernel loading, first-use costs)
     seen, warm = set(), set()
@@ -1268,11 +1273,14 @@ def run_serving(args, dev, dist=None):
     plain = replay(1, True, chunk=50)
     # saturated capacity: the host-side plan setup and the shared device make
     # single replays vary by up to 2x, so each form is replayed three times
-    # (alternating) and the median run by solves/s is reported
+    # (alternating) and the median run by solves/s is reported; one more run
+    # stacks same-shape requests with similar step counts into cohorts (up to
+    # 16 members per stacked plan)
     sat_runs, plain_runs = [], []
     for _ in range(3):
         sat_runs.append(replay(16, False))
         plain_runs.append(replay(1, False, chunk=50))
+    sat_cohort = replay(16, False, cohort=16)
 
     def median_run(runs):
         return sorted(runs, key=lambda r: r["solves_per_s"])[len(runs) // 2]
@@ -1296,6 +1304,8 @@ def run_serving(args, dev, dist=None):
         "saturated": sat,
         "plain_gpu_saturated": sat_plain,
         "saturated_speedup_vs_plain_gpu": sat["solves_per_s"] / max(sat_plain["solves_per_s"], 1e-30),
+        "saturated_with_cohorts": {k: sat_cohort[k] for k in ("solves_per_s", "p50_ms", "p99_ms", "mean_setup_ms",
+                                                              "peak_running", "peak_cohort", "cohort_requests")},
         "dtype": {"rbc": "f64", "turbulence": "f32"},
         "data": "synthetic: seeded arrivals (seed 11), sizes and parameters; RBC noise seed 5000+k, "
                 "turbulence k^-3 spectrum seed 7000+k",

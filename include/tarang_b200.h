@@ -375,9 +375,19 @@ typedef struct tb_server_stats {
   size_t peak_bytes, budget_bytes;
   int peak_running;
   double mean_setup_ms; /* admission to ready: plan build, factors, graph capture */
+  int peak_cohort;      /* most requests that ran as one stacked plan (1: none stacked) */
+  long long cohort_requests; /* requests that completed as members of a stacked run */
 } tb_server_stats;
 typedef struct tb_server tb_server;
 tb_status tb_server_create(tb_context* ctx, size_t budget_bytes, int max_running, int chunk_steps, tb_server** out);
+/* Cohorts: RBC requests of one shape (grid, box, walls, stepper, precision)
+ * and one dt, with step counts within 25 % of each other, queued together
+ * are admitted as one run of a stacked plan (the ensemble's fused form), up
+ * to max_members (1..64; 1, the default, runs every request alone).  Each
+ * member leaves the run with its result when its own step count is reached.  A member's result equals its solo run to rounding
+ * (the stacked kernels sum in a different order); with max_members = 1 it is
+ * bitwise the solo result. */
+tb_status tb_server_set_cohort(tb_server* srv, int max_members);
 tb_status tb_server_submit(tb_server* srv, const tb_request* req, long long* id);
 tb_status tb_server_poll(tb_server* srv, long long id, int* state, double* tts_ms);
 tb_status tb_server_result(tb_server* srv, long long id, int field, double* host_out, size_t* ndoubles);

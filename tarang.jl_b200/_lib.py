@@ -56,6 +56,7 @@ class tb_server_stats(Structure):
         ("queued", c_longlong), ("elapsed_ms", c_double), ("solves_per_s", c_double), ("steps_per_s", c_double),
         ("p50_ms", c_double), ("p99_ms", c_double), ("mean_wait_ms", c_double), ("peak_bytes", c_size_t),
         ("budget_bytes", c_size_t), ("peak_running", c_int), ("mean_setup_ms", c_double),
+        ("peak_cohort", c_int), ("cohort_requests", c_longlong),
     ]
 
 
@@ -129,6 +130,7 @@ SIGNATURES = {
     "tb_turb_get_vorticity": (c_int, [c_void_p, c_void_p]),
     "tb_server_create": (c_int, [c_void_p, c_size_t, c_int, c_int, POINTER(c_void_p)]),
     "tb_server_submit": (c_int, [c_void_p, POINTER(tb_request), POINTER(c_longlong)]),
+    "tb_server_set_cohort": (c_int, [c_void_p, c_int]),
     "tb_server_poll": (c_int, [c_void_p, c_longlong, POINTER(c_int), POINTER(c_double)]),
     "tb_server_result": (c_int, [c_void_p, c_longlong, c_int, c_void_p, POINTER(c_size_t)]),
     "tb_server_wait_all": (c_int, [c_void_p]),

@@ -663,6 +663,12 @@ class Server:
             lib.tb_server_destroy(ptr)
             self.ptr = None
 
+    def set_cohort(self, max_members: int) -> None:
+        """Same-shape RBC requests at one dt, with step counts within 25 % of
+        each other, queued together run as one stacked plan of up to
+        ``max_members`` (1, the default: every request alone)."""
+        check(lib.tb_server_set_cohort(self.ptr, int(max_members)), self.ctx)
+
     def submit(self, desc, dt: float, nsteps: int, init: np.ndarray) -> int:
         if desc.program == L.TB_PROGRAM_TURB2D:
             data = np.ascontiguousarray(init, dtype=np.complex128)

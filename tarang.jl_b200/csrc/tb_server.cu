@@ -13,8 +13,17 @@
 //     that arrives while others run joins as soon as memory frees up;
 //   - completion: the final state is copied to host memory, the plan and its
 //     device memory are released, and the time from submission is recorded.
-// Each request's arithmetic is exactly what it would be alone (its own plan,
-// its own graphs); only the interleaving on the device differs.
+//   - cohorts (tb_server_set_cohort; off by default): RBC requests of one
+//     shape (grid, box, walls, stepper, precision) and one dt, with step
+//     counts within 25 % of each other, that are queued together are
+//     admitted as one run of a stacked plan (the ensemble's fused form: each member's modes are
+//     columns of one plan, with its own kappa / nu), stepped by one graph per
+//     chunk; each member leaves with its state copied out of its columns when
+//     its own step count is reached (the chunks stop at that count), the
+//     others step on.
+// A request run alone has exactly its arithmetic on its own; in a cohort its
+// solves and transforms run in kernels over the stacked columns, which
+// changes only the rounding (within 1e-12).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -78,6 +87,25 @@ struct RbcJob : Job {
   void prepare(double dt, int chunk) override { plan_prepare(P, dt, chunk); }
 };
 
+// Same-shape RBC requests stacked into one plan (build_plan with B instances).
+struct CohortJob : Job {
+  std::unique_ptr<tb_plan> P;
+  cudaStream_t stream() const override { return P->st; }
+  void launch(double dt, int steps) override { plan_launch_steps(P.get(), dt, steps, P->st, steps); }
+  size_t device_bytes() const override { return plan_device_bytes(P.get()); }
+  int nfields() const override { return 3; }
+  size_t field_doubles(int) const override { return (size_t)2 * P->Nz * P->Nkm; }
+  // member k's columns of field f, as its own plan would hold them ([Nz][Nkm])
+  void fetch_member(int k, int field, double* host) {
+    const size_t w = (size_t)P->Nkm * sizeof(double2);
+    TB_CUDA_TRY(cudaMemcpy2DAsync(host, w, P->Xp(field) + (size_t)k * P->Nkm, (size_t)P->Nk * sizeof(double2), w,
+                                  P->Nz, cudaMemcpyDeviceToHost, P->st));
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  }
+  void fetch(int field, double* host) override { fetch_member(0, field, host); }
+  void prepare(double dt, int chunk) override { plan_prepare(P.get(), dt, chunk); }
+};
+
 struct TurbJob : Job {
   tb_turb* T = nullptr;
   ~TurbJob() override {
@@ -119,7 +147,29 @@ struct Request {
   cudaEvent_t ev[2] = {nullptr, nullptr};
   int inflight = 0, head = 0;
   std::vector<std::vector<double>> result;
+  // cohort leader: every member (itself first) and, per member, whether its
+  // result has been taken; `hold` stops new chunks until the in-flight ones
+  // retire (a member reached its step count)
+  std::vector<Request*> cohort;
+  std::vector<bool> finished;
+  bool hold = false;
+  Request* leader = nullptr;  // members other than the leader
+  bool solo = false;          // runs alone (its cohort's stacked plan could not be built)
 };
+
+// Requests that can share one stacked plan.
+bool cohort_fusible(const Request& r) {
+  return r.desc.program == TB_PROGRAM_RBC && r.desc.ndim == 2 && !r.solo;
+}
+// A stacked run steps every column until its longest member is done, so
+// members join only with step counts within 25 % of each other.
+bool cohort_compatible(const Request& a, const Request& b) {
+  const tb_problem_desc &x = a.desc, &y = b.desc;
+  const int lo = std::min(a.nsteps, b.nsteps), hi = std::max(a.nsteps, b.nsteps);
+  return cohort_fusible(a) && cohort_fusible(b) && a.dt == b.dt && x.Nx == y.Nx && x.Nz == y.Nz && x.Lx == y.Lx &&
+         x.Lz == y.Lz && x.timestepper == y.timestepper && x.b_bottom == y.b_bottom && x.b_top == y.b_top &&
+         x.precision == y.precision && 4 * hi <= 5 * lo;
+}
 
 }  // namespace
 
@@ -127,6 +177,7 @@ struct tb_server {
   tb_context* ctx = nullptr;
   size_t budget = 0;
   int max_running = 1, chunk = 1;
+  int cohort_max = 1;  // members of one stacked run (1, the default: every request alone)
   std::mutex mu;
   std::condition_variable cv;
   std::deque<Request*> queue;     // submitted, not admitted
@@ -146,7 +197,8 @@ struct tb_server {
   std::thread worker;
   // statistics
   size_t used = 0, peak = 0;
-  int peak_running = 0;
+  int peak_running = 0, peak_cohort = 1;
+  long long cohort_requests = 0;
   long long completed = 0, failed = 0, steps_done = 0;
   double first_submit = -1, last_done = 0;
   std::vector<double> tts, waits, setups;
@@ -159,9 +211,45 @@ struct tb_server {
   void release_zombies();
   void fail_admitted(Request* r, const std::string& msg);
   void fail_running(Request* r, const std::string& msg);
+  void progress_cohort(Request* r);
+  void finish_locked(Request* m);
+  bool requeue_cohort(Request* r);
 };
 
 namespace {
+
+// One stacked plan for the cohort's members: member k's modes are columns
+// k Nkm .. (k+1) Nkm - 1; its initial b grid goes through the plan's x FFT and
+// forward Chebyshev GEMM straight into its columns (u = 0).
+std::unique_ptr<Job> make_cohort_job(tb_context* ctx, const std::vector<Request*>& members) {
+  std::vector<tb_problem_desc> descs;
+  for (const Request* m : members) descs.push_back(m->desc);
+  auto j = std::make_unique<CohortJob>();
+  j->P = std::make_unique<tb_plan>();
+  build_plan(j->P.get(), ctx, descs.data(), (int)descs.size());
+  tb_plan* P = j->P.get();
+  if (plan_tau_parts_ok(P, 1)) plan_set_variant(P, 1, 0);  // the one-warp solve, as for single requests
+  StreamBuf grid;
+  grid.alloc((size_t)P->Nz * P->Nx * sizeof(double), P->st);
+  TB_CUDA_TRY(cudaMemsetAsync(P->X.p, 0, P->X.bytes, P->st));
+  const int Hp = (P->Hz + 15) / 16 * 16;
+  for (size_t k = 0; k < members.size(); ++k) {
+    TB_CUDA_TRY(cudaMemcpyAsync(grid.p, members[k]->init.data(), grid.bytes, cudaMemcpyHostToDevice, P->st));
+    double2* mixed = P->tmpgrid.as<double2>();  // [Nz][Nkm]
+    launch_x_rfft(grid.as<double>(), mixed, P->Nz, P->Nx, P->fpN, P->twN.as<double2>(), P->st);
+    double* out = reinterpret_cast<double*>(P->Xp(0) + k * P->Nkm);
+    GemmBatch bt{};
+    bt.item[0] = GemmItem{P->fE.as<double>(), reinterpret_cast<const double*>(mixed), out, P->Ke, P->Hz, Hp,
+                          GEMM_MIRROR, 0};
+    bt.item[1] = GemmItem{P->fO.as<double>(), reinterpret_cast<const double*>(mixed), out, P->Ko, P->Hz, Hp,
+                          GEMM_MIRROR, 1};
+    launch_gemm_f64(bt, P->Ko > 0 ? 2 : 1, 2 * P->Nkm, 2 * P->Nkm, 2 * P->Nk, P->Nz, P->st);
+    TB_CUDA_TRY(cudaGetLastError());
+    // the staging grid is rewritten for the next member only after these ran
+    TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  }
+  return j;
+}
 
 std::unique_ptr<Job> make_job(tb_context* ctx, const Request& r) {
   if (r.desc.program == TB_PROGRAM_TURB2D) {
@@ -215,6 +303,23 @@ void tb_server::admit() {
     }
     queue.pop_front();
     used += h->bytes;
+    // cohort: later queued requests of h's shape and dt join it while they fit
+    h->cohort.clear();
+    if (cohort_max > 1 && cohort_fusible(*h)) {
+      h->cohort.push_back(h);
+      for (auto it = queue.begin(); it != queue.end() && (int)h->cohort.size() < cohort_max;) {
+        Request* c = *it;
+        if (cohort_compatible(*h, *c) && used + zombie_bytes + c->bytes <= budget) {
+          used += c->bytes;
+          c->leader = h;
+          h->cohort.push_back(c);
+          it = queue.erase(it);
+        } else {
+          ++it;
+        }
+      }
+      if (h->cohort.size() < 2) h->cohort.clear();
+    }
     peak = std::max(peak, used);
     setupq.push_back(h);
     setup_cv.notify_one();
@@ -242,28 +347,44 @@ void tb_server::setup_loop() {
     }
     try {
       r->t_start = now_ms();
-      r->job = make_job(ctx, *r);
+      r->job = r->cohort.empty() ? make_job(ctx, *r) : make_cohort_job(ctx, r->cohort);
       r->job->prepare(r->dt, chunk);
       for (auto& e : r->ev) TB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       r->t_ready = now_ms();
       std::lock_guard<std::mutex> lk(mu);
-      setups.push_back(r->t_ready - r->t_start);
       --setting_up;
-      r->state = TB_REQ_RUNNING;
+      if (r->cohort.empty()) {
+        setups.push_back(r->t_ready - r->t_start);
+        r->state = TB_REQ_RUNNING;
+      } else {
+        r->finished.assign(r->cohort.size(), false);
+        r->hold = false;
+        peak_cohort = std::max(peak_cohort, (int)r->cohort.size());
+        for (Request* m : r->cohort) {
+          m->t_start = r->t_start;
+          m->t_ready = r->t_ready;
+          setups.push_back(r->t_ready - r->t_start);
+          m->state = TB_REQ_RUNNING;
+        }
+      }
       running.push_back(r);
       peak_running = std::max(peak_running, (int)running.size());
     } catch (const Error& e) {
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        --setting_up;
+      if (!requeue_cohort(r)) {
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          --setting_up;
+        }
+        fail_admitted(r, e.msg);
       }
-      fail_admitted(r, e.msg);
     } catch (const std::exception& e) {
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        --setting_up;
+      if (!requeue_cohort(r)) {
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          --setting_up;
+        }
+        fail_admitted(r, e.what());
       }
-      fail_admitted(r, e.what());
     }
   }
 }
@@ -275,10 +396,125 @@ void tb_server::fail_admitted(Request* r, const std::string& msg) {
     e = nullptr;
   }
   std::lock_guard<std::mutex> lk(mu);
-  used -= r->bytes;
-  r->state = TB_REQ_FAILED;
-  r->error = msg;
-  ++failed;
+  std::vector<Request*> all_m = r->cohort.empty() ? std::vector<Request*>{r} : r->cohort;
+  for (Request* m : all_m) {  // a cohort fails with its stacked plan
+    used -= m->bytes;
+    m->state = TB_REQ_FAILED;
+    m->error = msg;
+    ++failed;
+  }
+  cv.notify_all();
+}
+
+// A cohort whose stacked plan could not be built goes back to the head of the
+// queue as single requests, so that each one succeeds or fails on its own.
+bool tb_server::requeue_cohort(Request* r) {
+  if (r->cohort.empty()) return false;
+  r->job.reset();
+  for (auto& e : r->ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  --setting_up;
+  std::vector<Request*> members = r->cohort;
+  r->cohort.clear();
+  for (auto it = members.rbegin(); it != members.rend(); ++it) {
+    Request* m = *it;
+    used -= m->bytes;
+    m->solo = true;
+    m->leader = nullptr;
+    m->state = TB_REQ_QUEUED;
+    queue.push_front(m);
+  }
+  cv.notify_all();
+  return true;
+}
+
+// (mu held) statistics of a finished request
+void tb_server::finish_locked(Request* m) {
+  m->t_done = now_ms();
+  m->state = TB_REQ_DONE;
+  ++completed;
+  steps_done += m->nsteps;
+  last_done = m->t_done;
+  tts.push_back(m->t_done - m->t_submit);
+  waits.push_back(m->t_start - m->t_submit);
+}
+
+// A cohort's chunks step every member; a chunk never passes the step count
+// of a member still running, and when one reaches its count no further chunk
+// is queued until the in-flight ones retire and its columns are copied out.
+void tb_server::progress_cohort(Request* r) {
+  auto* job = static_cast<CohortJob*>(r->job.get());
+  while (r->inflight > 0) {
+    const cudaError_t e = cudaEventQuery(r->ev[r->head]);
+    if (e == cudaErrorNotReady) {
+      cudaGetLastError();
+      break;
+    }
+    if (e != cudaSuccess) throw Error{TB_ECUDA, std::string("request stream: ") + cudaGetErrorString(e)};
+    r->head ^= 1;
+    --r->inflight;
+  }
+  const size_t n = r->cohort.size();
+  if (r->inflight == 0) {
+    // members at their count: results out of their columns
+    for (size_t k = 0; k < n; ++k) {
+      Request* m = r->cohort[k];
+      if (r->finished[k] || m->left > 0) continue;
+      m->result.resize(job->nfields());
+      for (int f = 0; f < job->nfields(); ++f) {
+        m->result[f].resize(job->field_doubles(f));
+        job->fetch_member((int)k, f, m->result[f].data());
+      }
+      r->finished[k] = true;
+      std::lock_guard<std::mutex> lk(mu);
+      finish_locked(m);
+      ++cohort_requests;
+      cv.notify_all();
+    }
+    r->hold = false;
+  }
+  bool active = false;
+  int cmin = chunk;
+  for (size_t k = 0; k < n; ++k)
+    if (r->cohort[k]->left > 0) {
+      active = true;
+      cmin = std::min(cmin, r->cohort[k]->left);
+    }
+  while (active && !r->hold && r->inflight < kChunksAhead) {
+    job->launch(r->dt, cmin);
+    TB_CUDA_TRY(cudaEventRecord(r->ev[(r->head + r->inflight) & 1], job->stream()));
+    ++r->inflight;
+    active = false;
+    int next = chunk;
+    for (size_t k = 0; k < n; ++k) {
+      Request* m = r->cohort[k];
+      if (m->left <= 0) continue;
+      m->left -= cmin;
+      if (m->left == 0) r->hold = true;  // its result is taken once this chunk retires
+      if (m->left > 0) {
+        active = true;
+        next = std::min(next, m->left);
+      }
+    }
+    cmin = next;
+  }
+  if (active || r->inflight > 0) return;
+  for (size_t k = 0; k < n; ++k)
+    if (!r->finished[k]) return;  // results still to take (next round)
+  for (auto& e : r->ev) {
+    cudaEventDestroy(e);
+    e = nullptr;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  size_t bytes = 0;
+  for (Request* m : r->cohort) bytes += m->bytes;
+  zombies.push_back(std::move(r->job));
+  zombie_bytes += bytes;
+  used -= bytes;
+  running.erase(std::find(running.begin(), running.end(), r));
   cv.notify_all();
 }
 
@@ -289,6 +525,16 @@ void tb_server::progress() {
     act = running;
   }
   for (Request* r : act) {
+    if (!r->cohort.empty()) {
+      try {
+        progress_cohort(r);
+      } catch (const Error& e) {
+        fail_running(r, e.msg);
+      } catch (const std::exception& e) {
+        fail_running(r, e.what());
+      }
+      continue;
+    }
     try {
       // retire the chunks that have finished, oldest first
       while (r->inflight > 0) {
@@ -349,11 +595,16 @@ void tb_server::fail_running(Request* r, const std::string& msg) {
     e = nullptr;
   }
   std::lock_guard<std::mutex> lk(mu);
-  r->state = TB_REQ_FAILED;
-  r->error = msg;
   running.erase(std::find(running.begin(), running.end(), r));
-  used -= r->bytes;
-  ++failed;
+  std::vector<Request*> all_m = r->cohort.empty() ? std::vector<Request*>{r} : r->cohort;
+  for (size_t k = 0; k < all_m.size(); ++k) {
+    Request* m = all_m[k];
+    used -= m->bytes;
+    if (!r->cohort.empty() && r->finished[k]) continue;  // its result was already taken
+    m->state = TB_REQ_FAILED;
+    m->error = msg;
+    ++failed;
+  }
   cv.notify_all();
 }
 
@@ -391,6 +642,13 @@ tb_status tb_server_create(tb_context* ctx, size_t budget_bytes, int max_running
     for (int i = 0, n = setup_threads(); i < n; ++i) S->setup_workers.emplace_back([raw] { raw->setup_loop(); });
     *out = S.release();
   });
+}
+
+tb_status tb_server_set_cohort(tb_server* S, int max_members) {
+  if (!S || max_members < 1 || max_members > 64) return TB_EINVAL;
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->cohort_max = max_members;
+  return TB_OK;
 }
 
 tb_status tb_server_submit(tb_server* S, const tb_request* req, long long* id) {
@@ -480,6 +738,8 @@ tb_status tb_server_get_stats(tb_server* S, tb_server_stats* out) {
   double su = 0;
   for (double x : S->setups) su += x;
   st.mean_setup_ms = S->setups.empty() ? 0.0 : su / S->setups.size();
+  st.peak_cohort = S->peak_cohort;
+  st.cohort_requests = S->cohort_requests;
   *out = st;
   return TB_OK;
 }

@@ -1,7 +1,8 @@
 """Request server: continuous batching of RBC and turbulence requests.
 
-Each result must be the same alone and in the mix (the server gives each
-request its own plan and graphs; only the interleaving on the device differs),
+Each result must be the same alone and in the mix: bitwise for a request on
+its own plan and graphs (only the interleaving on the device differs), to
+rounding (1e-12) for a member of a cohort stepped as one stacked plan;
 admission must respect the device-memory budget, and the statistics report
 time to solution."""
 import numpy as np
@@ -47,6 +48,67 @@ def test_results_same_alone_and_in_mix(tb):
     assert stats["completed"] == len(reqs) and stats["failed"] == 0
     assert stats["peak_running"] >= 2
     assert stats["p99_ms"] >= stats["p50_ms"] > 0
+    s.close()
+
+
+def test_cohort_results_match_solo_runs_and_oracle(tb):
+    # five RBC requests of one shape at one dt (their own Ra, seeds and step
+    # counts within 25 % of each other) run as one stacked plan, each leaving
+    # at its own count; a request of the same shape with a far step count, one
+    # of another shape and a turbulence request run alone
+    specs = [(1e6, 9), (1e7, 8), (2e6, 10), (1e5, 9), (5e6, 8), (3e6, 30)]
+    reqs = []
+    for k, (Ra, n) in enumerate(specs):
+        p, d, b0 = rbc_req(tb, 48, 24, Ra, 400 + k)
+        reqs.append((p, d, 0.02, n, b0))
+    alone = []
+    for p, d, dt, n, b0 in reqs:
+        s = tb.Server(budget_bytes=1 << 30, max_running=1, chunk_steps=4)
+        rid = s.submit(d, dt, n, b0)
+        s.wait_all()
+        alone.append(s.result(rid))
+        s.close()
+    s = tb.Server(budget_bytes=1 << 30, max_running=8, chunk_steps=4)
+    s.set_cohort(16)
+    ids = [s.submit(d, dt, n, b0) for _, d, dt, n, b0 in reqs]
+    _, od, ob = rbc_req(tb, 32, 16, 1e6, 450)
+    oid = s.submit(od, 0.02, 5, ob)
+    tid = s.submit(tb.turb_desc(32, 32, 1e-3), 2e-3, 6, turb_initial_spec(32, 32, seed=460))
+    s.wait_all()
+    for rid, want in zip(ids + [oid, tid], alone + [None, None]):
+        assert s.poll(rid)[0] == tb._lib.TB_REQ_DONE
+        if want is not None:
+            for a, b in zip(s.result(rid), want):
+                # the stacked kernels change only the rounding
+                assert rel_l2(a, b) < 1e-12
+    for k in (0, 2):
+        p, _, dt, n, _ = reqs[k]
+        sim = run_rbc(p, "RK222", dt, n, seed=400 + k)
+        b, ux, uz = s.result(ids[k])
+        assert rel_l2(b, sim.b) < 1e-10 and rel_l2(uz, sim.uz) < 1e-10
+    st = s.stats()
+    assert st["completed"] == 8 and st["failed"] == 0
+    assert st["peak_cohort"] >= 2 and st["cohort_requests"] >= 2
+    s.close()
+
+
+def test_cohorts_off_gives_solo_results_bitwise(tb):
+    reqs = [rbc_req(tb, 48, 24, Ra, 500 + k) for k, Ra in enumerate((1e6, 3e6, 1e7))]
+    alone = []
+    for p, d, b0 in reqs:
+        s = tb.Server(budget_bytes=1 << 30, max_running=1, chunk_steps=3)
+        rid = s.submit(d, 0.02, 6, b0)
+        s.wait_all()
+        alone.append(s.result(rid))
+        s.close()
+    s = tb.Server(budget_bytes=1 << 30, max_running=8, chunk_steps=3)
+    s.set_cohort(1)
+    ids = [s.submit(d, 0.02, 6, b0) for _, d, b0 in reqs]
+    s.wait_all()
+    for rid, want in zip(ids, alone):
+        for a, b in zip(s.result(rid), want):
+            assert np.array_equal(a, b)
+    assert s.stats()["peak_cohort"] == 1
     s.close()
 
 
