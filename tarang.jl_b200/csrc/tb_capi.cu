@@ -270,6 +270,7 @@ TauArgs tau_args(tb_plan* P, int sy, FactorSet* f, const double2* rhsP) {
   a.PP = f ? f->PP.as<double>() : nullptr;
   a.HR = f ? f->HR.as<double>() : nullptr;
   a.rhs_off = P->sys[sy].rhs_off.as<int>();
+  a.xcode = P->sys[sy].xcode.as<short>();
   a.err_mode = P->err_mode.as<int>();
   a.ysave = P->solve_scratch.as<double>();
   a.Nkm = P->Nkm;
@@ -850,7 +851,7 @@ size_t tb::plan_device_bytes(const tb_plan* P) {
   for (int i = 0; i < 4; ++i) b += P->FP[i].bytes + P->LXP[i].bytes;
   for (int sy = 0; sy < P->nsys; ++sy) {
     const TauSystem& S = P->sys[sy];
-    b += S.rhs_off.bytes;
+    b += S.rhs_off.bytes + S.xcode.bytes;
     for (int c = 0; c < 2; ++c) {
       const ClassTables& t = S.ct[c];
       const DevBuf* tb_[] = {&t.row_eq, &t.row_k, &t.col_unk, &t.col_k, &t.left_unk, &t.left_k, &t.bc_rhs, &t.band,
@@ -1002,6 +1003,17 @@ void install_system(tb_plan* P, int sy, TauLayout lay) {
   for (int j = 0; j < n; ++j)
     for (int c = 0; c < 2; ++c) ro[2 * j + c] = to_int(rhs_code(P, sy, lay.cls[c].row_eq[j], lay.cls[c].row_k[j]));
   upload(S.rhs_off, ro);
+  // per (band row, class) store target in 16 bits: the code is 2 * R * Nk +
+  // flag for the element row R of the unknown, kept as 2 R + flag
+  std::vector<short> xc((size_t)2 * S.npad, (short)-1);
+  for (int j = 0; j < n; ++j)
+    for (int c = 0; c < 2; ++c) {
+      const long long code = store_code(P, sy, lay.cls[c].col_unk[j], lay.cls[c].col_k[j]);
+      const long long R = (code >> 1) / P->Nk;
+      TB_REQUIRE((code >> 1) % P->Nk == 0 && 2 * R + 1 < 0x7fff, TB_ENOTSUPPORTED, "store code outside 16 bits");
+      xc[2 * j + c] = (short)(2 * R + (code & 1));
+    }
+  upload(S.xcode, xc);
   S.lay = std::move(lay);
 }
 

@@ -147,8 +147,9 @@ constexpr int kFwdRot = kFwdRec - 1;
 constexpr int kBwdCode = 1 + kTauKL + kTauKU + 4;
 constexpr int kBwdG = kBwdCode + 1;
 constexpr int kBwdRec = kBwdG + 4;
-// per-row backward responses H of the partitioned solve: 12 entries, store code, pad
-constexpr int kHRec = kTauKL + kTauKU + 2;
+// per-row backward responses H of the partitioned solve: 12 entries (the
+// rows' store codes come from the per-row table TauArgs::xcode)
+constexpr int kHRec = kTauKL + kTauKU;
 // Register windows of the solve sweeps.  The solve splits the band rows into
 // partitions (one warp each), each a whole number of backward windows; rows
 // are padded with identity rows to a multiple of kTauParts * kBwdWin
@@ -226,9 +227,13 @@ struct TauArgs {
   // [row][class] over npad rows: 2 * (element offset of band row j's right-hand
   // side in rhsP) + 1 for a u_x momentum row, -1 for none
   const int* rhs_off;
+  // [row][class] over npad rows: store target of band column j packed in 16
+  // bits, 2 * (its element offset / Nk) + (1 if the unknown is i times the
+  // solved column), -1 for none (the store code is 2 * offset + flag)
+  const short* xcode;
   // partition responses of the solve, written by the factorisation:
   // PP[group][partition][class][mode] = Phi (4x4), Psi (12x12), Gz (4x4);
-  // HR[group][row][class][mode][kHRec] = H (12), store code, pad
+  // HR[group][row][class][mode][kHRec] = H (12)
   double* PP;
   double* HR;
   double* ysave;       // one-partition solve: [group][row][lane] y scratch (tau_solve_scratch_doubles)

@@ -107,6 +107,7 @@ struct TauSystem {
   TauLayout lay;
   ClassTables ct[2];
   DevBuf rhs_off;  // [row][class] right-hand-side codes
+  DevBuf xcode;    // [row][class] store targets of the band columns, 16-bit (TauArgs::xcode)
   std::vector<DevBuf> mband, mbord;  // stacked instances: band / border coefficients [instance][class]
   std::vector<std::unique_ptr<FactorSet>> factors;
   int tau_parts = 1;  // partitions of the solve (kTauParts16, kTauParts8, kTauParts or 1)

@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
                 "forward record: pivot, l, border, rotation flag of the entering row");
   static_assert(kBwdCode == KL + KU + 1 + NBMAX && kBwdG == kBwdCode + 1 && kBwdRec == kBwdG + 4 && kBwdRec % 2 == 0,
                 "backward record: 1/d, u, border, code, G");
-  static_assert(kHRec == kBwdWin + 2, "H record: 12 responses, code, pad");
+  static_assert(kHRec == kBwdWin && kHRec % 2 == 0, "H record: the 12 responses");
   constexpr int MP = kSolveModes;
   constexpr int W1 = KL + KU + 1;
   constexpr int FREC = 2 * MP * kFwdRec;  // doubles per forward row (both classes)
@@ -475,6 +475,9 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   // [row][class] right-hand-side code: 2 * element offset + (1 for a u_x momentum
   // row, scaled by -i on load), -1 for none
   for (int q = threadIdx.x; q < np / 2; q += blockDim.x) cp_async16(rofs + 4 * q, a.rhs_off + 4 * q, true);
+  // [row][class] 16-bit store targets of the H pass (2 R + flag, -1 for none)
+  short* xcs = reinterpret_cast<short*>(rofs + 2 * np);
+  for (int q = threadIdx.x; q < np / 4; q += blockDim.x) cp_async16(xcs + 8 * q, a.xcode + 8 * q, true);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
@@ -930,7 +933,8 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
             acc0 = fma(hv[i / 2].x, T[i], acc0);
             acc1 = fma(hv[i / 2].y, T[i + 1], acc1);
           }
-          store_unknown(Xd, __double2loint(hv[HV - 1].x), m, part, acc0 + acc1, m < Nk);
+          const int xc = xcs[2 * j + c];  // 2 R + flag -> store code 2 R Nk + flag
+          store_unknown(Xd, xc < 0 ? -1 : 2 * (xc >> 1) * Nk + (xc & 1), m, part, acc0 + acc1, m < Nk);
         }
       }
       __syncwarp();
@@ -1010,10 +1014,6 @@ __global__ void __launch_bounds__(128) k_tau_transfer(TauArgs a) {
     xw[j % kBwdWin] = acc * br[0];
     double* hr = a.HR + ((((size_t)g * np + j) * 2 + c) * kSolveModes + mm) * kHRec;
     hr[ib] = xw[j % kBwdWin];
-    if (ib == 0) {
-      hr[kBwdWin] = br[kBwdCode];
-      hr[kBwdWin + 1] = 0.0;
-    }
   }
   for (int o = 0; o < kBwdWin; ++o) tr[kTrPsi + ib * kBwdWin + o] = xw[o];  // Psi^T: row ib
 }
@@ -1216,7 +1216,7 @@ size_t solve_smem_bytes(int npad) {
   constexpr size_t NL = 4 * kSolveModes;
   const size_t ys = ys_global<P>() ? 0 : (size_t)npad * NL;  // 1 and 16 partitions keep y in global scratch
   return ((size_t)P * ring_doubles<P>() + ys + (size_t)P * NL * kXch) * sizeof(double) +
-         (size_t)npad * 2 * sizeof(int);
+         (size_t)npad * 2 * (sizeof(int) + sizeof(short));
 }
 
 template <int KL, int KU>
