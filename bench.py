@@ -63,6 +63,8 @@ def parse_args():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision summary in the rbc line")
     ap.add_argument("--no-rbc3d", action="store_true", help="skip the 3D (256x256x128) summary in the rbc line")
     ap.add_argument("--rbc3d-grid", default="256x256x128", help="Nx x Ny x Nz of the 3D workload")
+    ap.add_argument("--rbc3d-gemm", choices=["simt", "tensor"], default="tensor",
+                    help="3D z-transform GEMMs: SIMT FP32 or the streaming tcgen05 TF32x3 kernel")
     ap.add_argument("--rbc3d-quick", action="store_true",
                     help="3D workload without the FP64 comparison and the end-to-end run (profiling)")
     ap.add_argument("--serve-requests", type=int, default=60)
@@ -1055,6 +1057,7 @@ def run_rbc3d(args, dev, with_cpu=True):
     grid = W.rbc3_initial_grid(c)
     t0 = time.perf_counter()
     plan = tb.Plan3D(c.Nx, c.Ny, c.Nz, c.kappa, c.nu, 0, c.Lx, c.Ly, c.Lz, precision=TB_PREC_MIXED, device=dev)
+    plan.set_gemm_path(args.rbc3d_gemm == "tensor")
     b0 = plan.forward(grid)
     plan.set_state(TB_FIELD_B, b0)
     plan.step(c.dt, 1)  # factors both tau systems for this dt and captures the step graph

@@ -205,12 +205,14 @@ tb_status tb_checkpoint_load(tb_plan* plan, const double* grid, int where, const
 tb_status tb_plan_set_variant(tb_plan* plan, int tau_parts, int xrows);
 tb_status tb_plan_get_variant(const tb_plan* plan, int* tau_parts, int* xrows);
 tb_status tb_plan_tune(tb_plan* plan, double dt, int trial_steps, int* tau_parts, int* xrows);
-/* FP32 Chebyshev transform GEMMs of a 2D mixed-precision plan: tensor_cores =
- * 1 runs them on the tcgen05 tensor cores in TF32 with three products per
- * term (FP32 accuracy) wherever Nz <= 256, 0 (the default) on the SIMT FP32
- * kernel (3D plans always use the SIMT kernel).  No counterpart in the reference, whose GPU Chebyshev transforms are
- * cuFFT DCT-Is (ext/cuda/cheb_deriv.jl:503-596).  A change drops the plan's
- * step graphs. */
+/* FP32 Chebyshev transform GEMMs of a mixed-precision plan: tensor_cores = 1
+ * runs them on the tcgen05 tensor cores in TF32 with three products per term
+ * (FP32 accuracy), 0 on the SIMT FP32 kernel.  2D: tensor cores wherever
+ * Nz <= 256, SIMT by default.  3D: the streaming tensor-core kernel (TMA
+ * tiles of the raw planes) wherever Nz <= 128, and there it is the default;
+ * SIMT above.  No counterpart in the reference, whose GPU Chebyshev transforms
+ * are cuFFT DCT-Is (ext/cuda/cheb_deriv.jl:503-596).  A change drops the
+ * plan's step graphs. */
 tb_status tb_plan_set_gemm_path(tb_plan* plan, int tensor_cores);
 tb_status tb_plan_get_gemm_path(const tb_plan* plan, int* tensor_cores);
 

@@ -376,7 +376,8 @@ class Plan:
 
     def set_gemm_path(self, tensor_cores: bool) -> None:
         """Mixed precision: FP32 transform GEMMs on the tcgen05 tensor cores
-        (True) or on the SIMT FP32 kernel (False, the default)."""
+        (True) or on the SIMT FP32 kernel (False).  The default is the SIMT
+        kernel in 2D and the tensor cores in 3D (Nz <= 128)."""
         check(lib.tb_plan_set_gemm_path(self.ptr, 1 if tensor_cores else 0), self.ctx)
 
     def gemm_path(self) -> bool:

@@ -740,13 +740,26 @@ void tb::plan_launch_steps(tb_plan* P, double dt, int nsteps, cudaStream_t s, in
     const int chunk = uniform ? std::min(left, graph_steps) : 1;
     prepare_kind(P, dt, kind);
     if (P->profiling) {
+      // The profiled steps run as a graph of their own in which an event
+      // record node brackets every kernel, so a kernel's time is its device
+      // time between its neighbours, without the host's launch latency that
+      // eager launches would add to the short kernels.
       if (s != P->st) throw Error{TB_EINVAL, "profiled steps run on the plan's own stream"};
-      for (int i = 0; i < chunk; ++i) {
-        if (kind == 0)
-          enqueue_rk_step(P, dt);
-        else
-          enqueue_sbdf_step(P, dt, kind);
+      TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+      cudaGraphExec_t ex = nullptr;
+      try {
+        ex = capture_steps(P, dt, kind, chunk);
+      } catch (...) {
+        for (auto& r : P->pending) {
+          P->event_pool.push_back(r.a);
+          P->event_pool.push_back(r.b);
+        }
+        P->pending.clear();
+        throw;
       }
+      const cudaError_t e = cudaGraphLaunch(ex, P->st);
+      cudaGraphExecDestroy(ex);
+      if (e != cudaSuccess) throw Error{TB_ECUDA, std::string("profiled step: ") + cudaGetErrorString(e)};
       check_launch("profiled step");
     } else if (chunk < graph_steps || chunk == 1) {
       // single steps (also for a partial last chunk, so the graph of
@@ -1218,10 +1231,11 @@ void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, i
       upload(P->iptwM32, it32);
       TB_REQUIRE(xprod32_smem_bytes(P->M, (int)pt32.size()) <= 227 * 1024, TB_ENOTSUPPORTED,
                  "Nx too large for the FP32 x kernel");
-      // TF32 operand images of the eight transform matrices for the
+      // TF32 operand images of the eight transform matrices for the 2D
       // tensor-core GEMMs, and the scratch of their per-call B images (six
       // distinct inputs per GEMM), when the shapes fit one tensor-core tile
-      if (P->Hz <= 128 && pad16(P->Ke) <= 128) {
+      // (3D plans stream their planes through the form made in rbc3d_setup)
+      if (P->ndim == 2 && P->Hz <= 128 && pad16(P->Ke) <= 128) {
         const size_t fa = tc32_a_image_floats();
         P->tcAimg.alloc(8 * fa * sizeof(float));
         const DevBuf* mats[8] = {&P->bEv32, &P->bOv32, &P->bEd32, &P->bOd32, &P->fE32, &P->fO32, &P->sfE32, &P->sfO32};

@@ -52,6 +52,23 @@ void make_tc32_a_image(const float* A, int M, int Kpad, float* image, cudaStream
 bool launch_gemm_tc32(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
                       cudaStream_t st, float* bscratch, size_t bscratch_floats);
 cudaError_t set_tc32_smem_limits();
+// Streaming form for the 3D z transforms (even N <= 128 rows, ncol a multiple
+// of 4): the raw FP32 planes of nfields fields (N x ncol each, contiguous) are
+// read through a TMA tensor map, the row maps live in the A operands
+// (tc32s_image_floats floats, made once per plan by make_tc32s_images from
+// the eight FP32 transform matrices).  Backward: C_w (N/2 x ncol) of field f
+// at out + (4 f + w) N/2 ncol, w = parity + 2 derivative; forward: FP64 rows
+// of field f at out + f N ncol.
+struct alignas(64) TmaDesc {
+  unsigned char bytes[128];
+};
+bool tc32s_supported(int N, int ncol);
+size_t tc32s_image_floats();
+void make_tc32s_images(const float* Ev, const float* Ov, const float* Ed, const float* Od, int kpe, int kpo,
+                       const float* sfE, const float* sfO, int kph, int N, float* images, cudaStream_t st);
+bool make_tc32s_tmap(TmaDesc* d, const float* planes, int nfields, int N, int ncol);  // false: unsupported
+void launch_tc32s(bool backward, const TmaDesc& d, const float* images, void* out, int nfields, int N, int ncol,
+                  cudaStream_t st);
 int tc32_status();  // 1 once a tensor-core GEMM's bounded wait gave up, -1 if unreadable
 // tensor cores when asked for and the shapes fit, else SIMT
 inline void launch_gemm_f32_path(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows,

@@ -182,7 +182,7 @@ struct tb_plan {
   FftPlan fpNy{};
   DevBuf ptwNy, tmp3;
   int xrows = 1;  // padded y rows per x-pass CTA (a tuned shape)
-  bool tc32 = false;  // mixed precision: FP32 transform GEMMs on the tensor cores (opt-in: the SIMT kernel is faster at these sizes)
+  bool tc32 = false;  // mixed precision: FP32 transform GEMMs on the tensor cores (2D opt-in; the 3D default where supported)
   // transform constants
   DevBuf bwd, fwd, s3, twM, twN, ptwM, iptwM;
   // parity halves of the Chebyshev matrices (H = ceil(Nz/2) rows/cols)
@@ -226,6 +226,11 @@ struct tb_plan {
   // (empty when the shapes exceed one tensor-core tile) and the per-call
   // scratch of the B-operand images
   DevBuf tcAimg, tcBimg;
+  // 3D: the streaming tensor-core form of the z transforms (A operands and
+  // the tensor maps of the two input plane sets), when the shapes allow it
+  bool tc3 = false;
+  DevBuf tc3img;
+  tb::TmaDesc tc3Xc, tc3H3;
   // profiling: eager launches bracketed by events, accumulated per kernel name
   bool profiling = false;
   struct ProfRec {
@@ -287,7 +292,8 @@ void plan_snapshot(tb_plan* P, PlanSnapshot* snap);
 void plan_restore(tb_plan* P, const PlanSnapshot& snap);
 
 // Profiling hook: runs fn (which enqueues one kernel) and, with profiling on,
-// brackets it with events collected after the step.
+// brackets it with events collected after the step (recorded as event nodes
+// when the profiled steps are captured into a graph).
 inline cudaEvent_t take_event(tb_plan* P) {
   if (!P->event_pool.empty()) {
     cudaEvent_t e = P->event_pool.back();
@@ -305,9 +311,9 @@ void timed(tb_plan* P, const char* name, F&& fn) {
     return;
   }
   cudaEvent_t a = take_event(P), b = take_event(P);
-  TB_CUDA_TRY(cudaEventRecord(a, P->st));
+  TB_CUDA_TRY(cudaEventRecordWithFlags(a, P->st, cudaEventRecordExternal));
   fn();
-  TB_CUDA_TRY(cudaEventRecord(b, P->st));
+  TB_CUDA_TRY(cudaEventRecordWithFlags(b, P->st, cudaEventRecordExternal));
   P->pending.push_back({name, a, b});
 }
 

@@ -660,9 +660,12 @@ void enqueue_rhs_t(tb_plan* P, const double2* Xin, double2* out4) {
         bt.item[4 * f + w] = GemmItem32{Am[w], reinterpret_cast<const float*>(Xc + (size_t)f * plane),
                                         G + (size_t)(4 * f + w) * hplane, H, (w & 1) ? P->Ko : P->Ke,
                                         pad16((w & 1) ? P->Ko : P->Ke), GEMM_PARITY, w & 1};
-    // SIMT here: the 3D GEMMs stream 33k-column planes near the HBM bound, and
-    // the tensor-core kernel's serial tile loop (no prefetch) does not beat it
-    timed(P, "z_backward_gemm", [&] { launch_gemm_f32(bt, 16, ncol, ncol, ncol, N, false, P->st); });
+    if (P->tc32 && P->tc3)
+      timed(P, "z_backward_gemm", [&] {
+        launch_tc32s(true, P->tc3Xc, P->tc3img.as<float>(), G, 4, N, ncol, P->st);
+      });
+    else
+      timed(P, "z_backward_gemm", [&] { launch_gemm_f32(bt, 16, ncol, ncol, ncol, N, false, P->st); });
   } else {
     GemmBatch bt{};
     const double* Am[4] = {P->bEv.as<double>(), P->bOv.as<double>(), P->bEd.as<double>(), P->bOd.as<double>()};
@@ -701,7 +704,12 @@ void enqueue_rhs_t(tb_plan* P, const double2* Xin, double2* out4) {
       bf.item[nb++] = GemmItem32{P->sfE32.as<float>(), in, out, P->Ke, H, pad16(H), GEMM_MIRROR, 0};
       bf.item[nb++] = GemmItem32{P->sfO32.as<float>(), in, out, P->Ko, H, pad16(H), GEMM_MIRROR, 1};
     }
-    timed(P, "z_forward_gemm", [&] { launch_gemm_f32(bf, nb, ncol, ncol, ncol, N, true, P->st); });
+    if (P->tc32 && P->tc3)
+      timed(P, "z_forward_gemm", [&] {
+        launch_tc32s(false, P->tc3H3, P->tc3img.as<float>(), out4, 4, N, ncol, P->st);
+      });
+    else
+      timed(P, "z_forward_gemm", [&] { launch_gemm_f32(bf, nb, ncol, ncol, ncol, N, true, P->st); });
   } else {
     GemmBatch bf{};
     int nb = 0;
@@ -732,6 +740,22 @@ void setup_t(tb_plan* P) {
   P->mix3.alloc(12 * slab * sizeof(C));
   P->pm3.alloc(4 * slab * sizeof(C));
   P->H3.alloc(4 * plane * sizeof(C));
+  if constexpr (std::is_same<C, float2>::value) {
+    // the streaming tensor-core form of the z transforms
+    const int N = P->Nz, ncol = 2 * P->Nk;
+    P->tc3 = false;
+    if (tc32s_supported(N, ncol)) {
+      P->tc3img.alloc(tc32s_image_floats() * sizeof(float));
+      make_tc32s_images(P->bEv32.as<float>(), P->bOv32.as<float>(), P->bEd32.as<float>(), P->bOd32.as<float>(),
+                        pad16(P->Ke), pad16(P->Ko), P->sfE32.as<float>(), P->sfO32.as<float>(), pad16(N / 2), N,
+                        P->tc3img.as<float>(), P->st);
+      TB_CUDA_TRY(cudaGetLastError());
+      TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+      P->tc3 = make_tc32s_tmap(&P->tc3Xc, reinterpret_cast<const float*>(P->Xc.p), 4, N, ncol) &&
+               make_tc32s_tmap(&P->tc3H3, reinterpret_cast<const float*>(P->H3.p), 4, N, ncol);
+    }
+    P->tc32 = P->tc3;  // the default GEMM path of a 3D plan: faster than SIMT at every supported size measured
+  }
   auto table = [&](const FftPlan& fp) {
     if (std::is_same<C, float2>::value && fp.n == 384) {
       std::vector<C> t(384);

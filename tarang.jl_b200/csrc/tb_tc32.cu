@@ -26,9 +26,26 @@
 // (M 128, N 64, K 8 each) and commits them to an mbarrier; every warp reads its
 // 32 accumulator lanes (rows) with tcgen05.ld and the tile leaves through a
 // shared-memory stage for row-contiguous stores.  Every wait is bounded.
+//
+// Streaming form for the 3D planes (k_tc32s, Nz <= 128): the raw FP32 input
+// planes are read by TMA tile by tile (N <= 128 rows x 32 columns, no swizzle) and
+// split into the TF32 hi / lo images in shared memory by the CTA's own
+// threads; the row maps are folded into constant A operands instead:
+//   backward (value and z-derivative on the half grid from the even and odd
+//     coefficients): per parity p one A of 128 rows, [value rows; derivative
+//     rows] of that parity's columns, times B_p = the tile's rows 2k + p;
+//   forward (the C^(2) coefficients 2r + par from the grid): one A of 128
+//     rows, [even outputs; odd outputs] over all N grid rows, the mirror sum
+//     B[j] + sgn B[N-1-j] folded into the columns (A'[r][j] = A[r][j] for
+//     j < N/2, sgn A[r][N-1-j] above), times the tile's N natural rows.
+// One persistent CTA per SM runs (field, 32-column tile) tasks with its warps
+// specialised: TMA loads, the split, the MMAs (into one of two accumulator
+// buffers in tensor memory) and the epilogue of consecutive tiles overlap.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "tb_kernels.cuh"
 
@@ -325,6 +342,374 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols));
 }
 
+
+// ---- streaming form (3D planes) ----
+constexpr int kSN = 32;                                  // columns per tile
+constexpr int kSRows = 128;                              // input rows per tile (N <= 128)
+constexpr uint32_t kSRawBytes = kSRows * kSN * 4;        // 16 KB raw tile
+constexpr uint32_t kSOffA = 0;                           // A images, 128 KB
+constexpr uint32_t kSOffB = 128 * 1024;                  // two hi/lo B buffers of 32 KB
+constexpr uint32_t kSOffRaw = kSOffB + 2 * 32 * 1024;    // two raw tiles of 16 KB
+constexpr uint32_t kSOffBar = kSOffRaw + 2 * kSRawBytes;  // 13 mbarriers, TMEM address, abort flag
+constexpr uint32_t kSSmem = kSOffBar + 128 + 1024;        // + alignment slack
+static_assert(kSSmem <= 232448, "one CTA per SM");
+constexpr uint32_t kSTmemCols = 128;  // two buffers of (up to) two 32-column accumulators
+constexpr size_t kSImageFloats = 2 * 2 * 128 * 64 + 2 * 128 * 128;  // backward pair (K 64), forward (K 128); hi and lo
+// instruction descriptor: D F32, A and B TF32, both K-major, N 32, M 128
+constexpr uint32_t kSIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kSN >> 3) << 17) |
+                             ((uint32_t)(kTcM >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32_n32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kSIdesc), "r"(accumulate));
+}
+
+// TF32 hi / lo images of the streaming form's A operands, K-major, 128-byte
+// swizzled, 128 rows each: blockIdx.x 0 and 1 the backward parities (K 64:
+// rows r < 64 value, r >= 64 derivative, of the columns 2k + p), 2 the
+// forward operand (K 128, the mirror folded in, rows r < 64 the even
+// outputs 2r, r >= 64 the odd ones 2(r - 64) + 1).
+__global__ void __launch_bounds__(kTcThreads) k_tc32s_image(const float* __restrict__ Ev, const float* __restrict__ Ov,
+                                                            const float* __restrict__ Ed, const float* __restrict__ Od,
+                                                            int kpe, int kpo, const float* __restrict__ sfE,
+                                                            const float* __restrict__ sfO, int kph, int N,
+                                                            float* __restrict__ images) {
+  const int H = N / 2, Ke = (N + 1) / 2, Ko = N / 2;
+  const int img = blockIdx.x;
+  const int kt = img < 2 ? 64 : 128;  // K extent of this image
+  const uint32_t half = 128u * kt * 4u;  // bytes of its hi part
+  uint8_t* hi = reinterpret_cast<uint8_t*>(images) + (size_t)(img < 2 ? img : 2) * 2 * 128 * 64 * 4;
+  uint8_t* lo = hi + half;
+  for (int idx = threadIdx.x; idx < 128 * (kt / 4); idx += kTcThreads) {
+    const int r = idx / (kt / 4), k0 = 4 * (idx % (kt / 4));
+    float f[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int k = k0 + i;
+      float v = 0.f;
+      if (img < 2) {
+        const int p = img, K = p ? Ko : Ke, kp = p ? kpo : kpe, rr = r & 63;
+        const float* src = r < 64 ? (p ? Ov : Ev) : (p ? Od : Ed);
+        if (rr < H && k < K) v = src[(size_t)rr * kp + k];
+      } else {
+        const int par = r >= 64, rr = r & 63, M = par ? Ko : Ke;
+        const float* src = par ? sfO : sfE;
+        if (rr < M && k < N) v = k < H ? src[(size_t)rr * kph + k] : (par ? -1.f : 1.f) * src[(size_t)rr * kph + (N - 1 - k)];
+      }
+      f[i] = v;
+    }
+    split_store4(hi, lo, sw128_off(r, k0, 128), make_float4(f[0], f[1], f[2], f[3]));
+  }
+}
+
+// 3D tile load: 32 columns x N rows of field z from the tensor map into dst
+__device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* map, int x, int z, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(0), "r"(z), "r"(bar)
+      : "memory");
+}
+
+// Roles (10 warps): warps 0-3 the epilogue (warp w reads accumulator lanes
+// 32w..32w+31), warps 4-7 the split, warp 8 the TMA producer, warp 9 the MMA
+// issuer.  Stage s = tile % 2 of the raw tile and of its hi / lo images,
+// accumulator buffer a = tile % 2; the hand-offs are mbarriers: full (TMA ->
+// split), rawfree (split -> producer), splitfull (split -> MMA), accfull (MMA
+// completion, by tcgen05.commit), accfree (epilogue -> MMA), stagefree
+// (epilogue -> split).  Once the MMAs of a tile have completed, its hi / lo
+// buffer is the epilogue's staging area: each epilogue warp writes its 32
+// accumulator rows there (16-byte chunks XOR-swizzled by row) and reads them
+// back row by row for full-line global stores; the split refills the buffer
+// after that.
+constexpr int kSThreads = 320;
+constexpr int kSEpi = 0, kSSplit = 4, kSProd = 8, kSMma = 9;  // first warp of each role
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+
+// bounded wait that also gives up once another role has aborted
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t bar, uint32_t parity, volatile int* abort) {
+  long long spins = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    ++spins;
+    if ((spins & 255) == 0 && *abort) return false;
+    if (spins > kTcSpinLimit) {
+      *abort = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
+// BWD: C_w (H x ncol, w = p + 2 d for parity p, derivative d) of each field
+// f at out + (4 f + w) * H * ncol; forward: rows 2r + par of each field at
+// out + f * N * ncol (FP64).
+template <bool BWD>
+__global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ CUtensorMap map,
+                                                        const float* __restrict__ images, void* out, int nfields,
+                                                        int N, int ncol) {
+  extern __shared__ uint8_t tc_smem_raw[];
+  const uint32_t raw = (uint32_t)__cvta_generic_to_shared(tc_smem_raw);
+  const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
+  uint8_t* sm = tc_smem_raw + pad;
+  const uint32_t sbase = raw + pad;
+  // mbarriers: A, then per stage / buffer b: full, rawfree, splitfull, hilofree, accfull, accfree
+  const uint32_t barA = sbase + kSOffBar;
+  auto bar = [&](int kind, int b) { return barA + 8u + 16u * (uint32_t)kind + 8u * (uint32_t)b; };
+  enum { FULL = 0, RAWFREE, SPLITFULL, STAGEFREE, ACCFULL, ACCFREE };
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kSOffBar + 112);
+  volatile int* abort = reinterpret_cast<volatile int*>(sm + kSOffBar + 120);
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int H = N / 2, Ke = (N + 1) / 2, Ko = N / 2;
+  const int ntiles = (ncol + kSN - 1) / kSN;
+  const int ntask = nfields * ntiles;
+  const uint32_t tile_bytes = (uint32_t)(kSN * N * 4);  // one TMA box: 32 columns x N rows
+  // local tiles i = 0 .. n-1 are the tasks blockIdx.x + i gridDim.x
+  const int n = blockIdx.x < ntask ? (ntask - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  auto task = [&](int i, int* f, int* n0) {
+    const int t = blockIdx.x + i * gridDim.x;
+    *f = t / ntiles;
+    *n0 = (t % ntiles) * kSN;
+  };
+  auto ph = [](int i) { return (uint32_t)(i >> 1) & 1u; };       // phase parity of tile i's use of its stage
+  auto ph_prev = [](int i) { return (uint32_t)((i >> 1) - 1) & 1u; };  // of tile i - 2 (i >= 2)
+
+  if (warp == kSEpi) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + kSOffBar + 112),
+                 "r"(kSTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  const uint32_t abytes = BWD ? 4u * 128u * 64u * 4u : 2u * 128u * 128u * 4u;  // 128 KB either way
+  const float* aimg = images + (BWD ? 0 : 2 * 2 * 128 * 64);
+  if (tid == 0) {
+    *abort = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barA));
+    for (int b = 0; b < 2; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar(FULL, b)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(bar(RAWFREE, b)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(bar(SPLITFULL, b)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(bar(STAGEFREE, b)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar(ACCFULL, b)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(bar(ACCFREE, b)));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tmem_slot;
+  bool a_pending = false;
+  int last_load[2] = {-1, -1}, last_mma = -1;  // for the bounded drain after an abort
+
+  if (warp == kSProd) {
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map)) : "memory");
+      mbar_expect_tx(barA, abytes);
+      bulk_copy(sbase + kSOffA, aimg, abytes, barA);
+      a_pending = true;
+      for (int i = 0; i < n; ++i) {
+        const int s = i & 1;
+        if (i >= 2 && !mbar_wait_or_abort(bar(RAWFREE, s), ph_prev(i), abort)) break;
+        int f, n0;
+        task(i, &f, &n0);
+        mbar_expect_tx(bar(FULL, s), tile_bytes);
+        tma_load_tile(sbase + kSOffRaw + (uint32_t)s * kSRawBytes, &map, n0, f, bar(FULL, s));
+        last_load[s] = i;
+      }
+    }
+  } else if (warp >= kSSplit && warp < kSSplit + 4) {
+    const int t = tid - 32 * kSSplit;
+    for (int i = 0; i < n; ++i) {
+      const int s = i & 1;
+      if (!mbar_wait_or_abort(bar(FULL, s), ph(i), abort)) break;
+      if (i >= 2 && !mbar_wait_or_abort(bar(STAGEFREE, s), ph_prev(i), abort)) break;
+      // split the raw tile [row < N][32 columns] into the K-major hi / lo
+      // images (rows past N are zero)
+      const float* rt = reinterpret_cast<const float*>(sm + kSOffRaw + (uint32_t)s * kSRawBytes);
+      uint8_t* hb = sm + kSOffB + (uint32_t)s * 32768u;
+      auto row = [&](int j, int nn) { return j < N ? rt[(size_t)j * kSN + nn] : 0.f; };
+      if constexpr (BWD) {
+        for (int it = t; it < 2 * 16 * kSN; it += 128) {
+          const int nn = it % kSN, kc = (it / kSN) % 16, p = it / (16 * kSN);
+          const int j0 = 8 * kc + p;  // rows 2 (4 kc + i) + p
+          const float4 v = make_float4(row(j0, nn), row(j0 + 2, nn), row(j0 + 4, nn), row(j0 + 6, nn));
+          split_store4(hb + p * 16384, hb + p * 16384 + 8192, sw128_off(nn, 4 * kc, kSN), v);
+        }
+      } else {
+        for (int it = t; it < 32 * kSN; it += 128) {
+          const int nn = it % kSN, kc = it / kSN, j0 = 4 * kc;
+          const float4 v = make_float4(row(j0, nn), row(j0 + 1, nn), row(j0 + 2, nn), row(j0 + 3, nn));
+          split_store4(hb, hb + 16384, sw128_off(nn, 4 * kc, kSN), v);
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      mbar_arrive(bar(RAWFREE, s));
+      mbar_arrive(bar(SPLITFULL, s));
+    }
+  } else if (warp == kSMma) {
+    if (lane == 0) {
+      mbar_wait_or_abort(barA, 0, abort);  // (sets the abort flag when it runs out)
+      for (int i = 0; i < n && !*abort; ++i) {
+        const int s = i & 1, a = i & 1;
+        if (!mbar_wait_or_abort(bar(SPLITFULL, s), ph(i), abort)) break;
+        if (i >= 2 && !mbar_wait_or_abort(bar(ACCFREE, a), ph_prev(i), abort)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        if constexpr (BWD) {
+#pragma unroll
+          for (int p = 0; p < 2; ++p) {
+            const uint64_t ahi = sw128_desc(sbase + kSOffA + (uint32_t)p * 65536u);
+            const uint64_t alo = sw128_desc(sbase + kSOffA + (uint32_t)p * 65536u + 32768u);
+            const uint64_t bhi = sw128_desc(sbase + kSOffB + (uint32_t)s * 32768u + (uint32_t)p * 16384u);
+            const uint64_t blo = sw128_desc(sbase + kSOffB + (uint32_t)s * 32768u + (uint32_t)p * 16384u + 8192u);
+            const uint32_t d = tmem + (uint32_t)(a * 64 + p * 32);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              // start-address field += byte offset / 16 (all offsets stay below 256 KB)
+              const uint64_t ka = ((uint64_t)(j >> 2) * (128u * 128u) + (uint64_t)(j & 3) * 32u) >> 4;
+              const uint64_t kb = ((uint64_t)(j >> 2) * (kSN * 128u) + (uint64_t)(j & 3) * 32u) >> 4;
+              mma_tf32_n32(d, ahi + ka, bhi + kb, j > 0 ? 1u : 0u);
+              mma_tf32_n32(d, ahi + ka, blo + kb, 1u);
+              mma_tf32_n32(d, alo + ka, bhi + kb, 1u);
+            }
+          }
+        } else {
+          const uint64_t ahi = sw128_desc(sbase + kSOffA), alo = sw128_desc(sbase + kSOffA + 65536u);
+          const uint64_t bhi = sw128_desc(sbase + kSOffB + (uint32_t)s * 32768u);
+          const uint64_t blo = sw128_desc(sbase + kSOffB + (uint32_t)s * 32768u + 16384u);
+          const uint32_t d = tmem + (uint32_t)(a * 64);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const uint64_t ka = ((uint64_t)(j >> 2) * (128u * 128u) + (uint64_t)(j & 3) * 32u) >> 4;
+            const uint64_t kb = ((uint64_t)(j >> 2) * (kSN * 128u) + (uint64_t)(j & 3) * 32u) >> 4;
+            mma_tf32_n32(d, ahi + ka, bhi + kb, j > 0 ? 1u : 0u);
+            mma_tf32_n32(d, ahi + ka, blo + kb, 1u);
+            mma_tf32_n32(d, alo + ka, bhi + kb, 1u);
+          }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                         bar(ACCFULL, a))
+                     : "memory");
+        last_mma = i;
+      }
+    }
+  } else if (warp < kSEpi + 4) {
+    const int r = warp * 32 + lane;  // accumulator lane = A row of this thread
+    for (int i = 0; i < n; ++i) {
+      const int a = i & 1;
+      // one decision per warp: the accumulator loads below are warp-wide
+      if (!__all_sync(0xffffffffu, mbar_wait_or_abort(bar(ACCFULL, a), ph(i), abort))) break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      int f, n0;
+      task(i, &f, &n0);
+      const bool full = n0 + kSN <= ncol;
+      uint32_t v[BWD ? 2 : 1][32];
+#pragma unroll
+      for (int acc = 0; acc < (BWD ? 2 : 1); ++acc) {
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * 64 + acc * 32);
+        uint32_t* w = v[acc];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+            : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]),
+              "=r"(w[8]), "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]), "=r"(w[15]),
+              "=r"(w[16]), "=r"(w[17]), "=r"(w[18]), "=r"(w[19]), "=r"(w[20]), "=r"(w[21]), "=r"(w[22]),
+              "=r"(w[23]), "=r"(w[24]), "=r"(w[25]), "=r"(w[26]), "=r"(w[27]), "=r"(w[28]), "=r"(w[29]),
+              "=r"(w[30]), "=r"(w[31])
+            : "r"(taddr));
+      }
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      // the accumulator buffer is read: the MMAs of tile i + 2 may overwrite it
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+      mbar_arrive(bar(ACCFREE, a));
+      // stage this warp's 32 rows in the tile's hi / lo buffer (its MMAs have
+      // completed), [acc][row][32 values] with 16-byte chunk c of row r at
+      // c ^ (r & 7), then store whole rows
+      uint8_t* stg = sm + kSOffB + (uint32_t)a * 32768u;
+      constexpr int VB = BWD ? 4 : 8;                // bytes per output value
+      constexpr int RB = kSN * VB;                   // bytes per staged row
+      constexpr int CH = RB / 16;                    // 16-byte chunks per row
+#pragma unroll
+      for (int acc = 0; acc < (BWD ? 2 : 1); ++acc) {
+        uint8_t* srow = stg + (size_t)acc * 128 * RB + (size_t)r * RB;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+          uint4 q;
+          if constexpr (BWD) {
+            q = make_uint4(v[acc][4 * c], v[acc][4 * c + 1], v[acc][4 * c + 2], v[acc][4 * c + 3]);
+          } else {
+            const double2 lo = make_double2((double)__uint_as_float(v[acc][2 * c]), (double)__uint_as_float(v[acc][2 * c + 1]));
+            q = *reinterpret_cast<const uint4*>(&lo);
+          }
+          *reinterpret_cast<uint4*>(srow + ((c ^ (r & 7)) << 4)) = q;
+        }
+      }
+      __syncwarp();
+      // row-wise stores: RPI rows per instruction, CH lanes of 16 bytes per row
+      constexpr int RPI = 32 / CH;
+#pragma unroll
+      for (int acc = 0; acc < (BWD ? 2 : 1); ++acc) {
+#pragma unroll 4
+        for (int r0 = 0; r0 < 32; r0 += RPI) {
+          const int rl = r0 + lane / CH, c = lane % CH;  // row within the warp's 32, chunk
+          const int rg = warp * 32 + rl;                  // accumulator row
+          const uint4 q = *reinterpret_cast<const uint4*>(stg + (size_t)acc * 128 * RB + (size_t)rg * RB +
+                                                           ((c ^ (rg & 7)) << 4));
+          const int hh = rg >> 6, rh = rg & 63;
+          const int col = n0 + c * (16 / VB);  // first column of this chunk
+          if constexpr (BWD) {
+            // parity acc, half hh (0 value, 1 derivative): item acc + 2 hh
+            if (rh < H) {
+              float* dst = reinterpret_cast<float*>(out) + ((size_t)(4 * f + acc + 2 * hh) * H + rh) * ncol + col;
+              if (full) {
+                *reinterpret_cast<uint4*>(dst) = q;
+              } else {
+                const float e[4] = {__uint_as_float(q.x), __uint_as_float(q.y), __uint_as_float(q.z),
+                                    __uint_as_float(q.w)};
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                  if (col + k < ncol) dst[k] = e[k];
+              }
+            }
+          } else {
+            // half hh is the output parity: row 2 rh + hh
+            if (rh < (hh ? Ko : Ke)) {
+              double* dst = reinterpret_cast<double*>(out) + ((size_t)f * N + 2 * rh + hh) * ncol + col;
+              if (full) {
+                *reinterpret_cast<uint4*>(dst) = q;
+              } else {
+                const double2 e = *reinterpret_cast<const double2*>(&q);
+                if (col < ncol) dst[0] = e.x;
+                if (col + 1 < ncol) dst[1] = e.y;
+              }
+            }
+          }
+        }
+      }
+      __syncwarp();
+      mbar_arrive(bar(STAGEFREE, a));  // the split may refill this buffer
+    }
+  }
+  __syncthreads();
+  if (*abort) {
+    // a wait ran out: flag it and give the copies and MMAs still in flight a
+    // bounded time to land (they write this CTA's shared and tensor memory)
+    if (warp == kSProd && lane == 0) {
+      atomicExch(&g_tc_timeout, 1);
+      if (a_pending) mbar_wait_bounded(barA, 0);
+      for (int s = 0; s < 2; ++s)
+        if (last_load[s] >= 0) mbar_wait_bounded(bar(FULL, s), ph(last_load[s]));
+    }
+    if (warp == kSMma && lane == 0 && last_mma >= 0) mbar_wait_bounded(bar(ACCFULL, last_mma & 1), ph(last_mma));
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  if (warp == kSEpi) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kSTmemCols));
+}
+
 }  // namespace
 
 bool gemm_tc32_supported(const GemmBatch32& bt, int nbatch) {
@@ -347,7 +732,11 @@ void make_tc32_a_image(const float* A, int M, int Kpad, float* image, cudaStream
 cudaError_t set_tc32_smem_limits() {
   cudaError_t e = cudaFuncSetAttribute(k_gemm_tc32<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_gemm_tc32<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+  e = cudaFuncSetAttribute(k_gemm_tc32<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_tc32s<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_tc32s<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSSmem);
 }
 
 bool launch_gemm_tc32(const GemmBatch32& bt_in, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
@@ -382,6 +771,65 @@ bool launch_gemm_tc32(const GemmBatch32& bt_in, int nbatch, int ncol, int ldb, i
   else
     k_gemm_tc32<float><<<grid, kTcThreads, kTcSmem, st>>>(bt, ncol, ldc);
   return true;
+}
+
+bool tc32s_supported(int N, int ncol) { return N >= 2 && N <= kSRows && N % 2 == 0 && ncol > 0 && ncol % 4 == 0; }
+
+size_t tc32s_image_floats() { return kSImageFloats; }
+
+void make_tc32s_images(const float* Ev, const float* Ov, const float* Ed, const float* Od, int kpe, int kpo,
+                       const float* sfE, const float* sfO, int kph, int N, float* images, cudaStream_t st) {
+  k_tc32s_image<<<3, kTcThreads, 0, st>>>(Ev, Ov, Ed, Od, kpe, kpo, sfE, sfO, kph, N, images);
+}
+
+namespace {
+// cuTensorMapEncodeTiled, reached through the runtime's driver entry point
+// (no link-time dependency on the driver library)
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_tiled() {
+  static EncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  });
+  return fn;
+}
+}  // namespace
+
+bool make_tc32s_tmap(TmaDesc* d, const float* planes, int nfields, int N, int ncol) {
+  static_assert(sizeof(TmaDesc) == sizeof(CUtensorMap) && alignof(TmaDesc) >= alignof(CUtensorMap), "tensor map");
+  const EncodeTiled enc = encode_tiled();
+  if (!enc || !tc32s_supported(N, ncol) || nfields < 1 || (reinterpret_cast<uintptr_t>(planes) & 15u)) return false;
+  // fields of N rows of ncol floats; boxes of 32 columns x N rows of one
+  // field (columns past ncol read as zero)
+  const cuuint64_t dims[3] = {(cuuint64_t)ncol, (cuuint64_t)N, (cuuint64_t)nfields};
+  const cuuint64_t strides[2] = {(cuuint64_t)ncol * 4, (cuuint64_t)N * ncol * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)kSN, (cuuint32_t)N, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(reinterpret_cast<CUtensorMap*>(d), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(planes), dims,
+             strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+void launch_tc32s(bool backward, const TmaDesc& d, const float* images, void* out, int nfields, int N, int ncol,
+                  cudaStream_t st) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int ntask = nfields * ((ncol + kSN - 1) / kSN);
+  const int grid = sms < ntask ? sms : ntask;
+  CUtensorMap map;
+  static_assert(sizeof(map) == sizeof(d.bytes), "tensor map");
+  for (size_t i = 0; i < sizeof(map); ++i) reinterpret_cast<unsigned char*>(&map)[i] = d.bytes[i];
+  if (backward)
+    k_tc32s<true><<<grid, kSThreads, kSSmem, st>>>(map, images, out, nfields, N, ncol);
+  else
+    k_tc32s<false><<<grid, kSThreads, kSSmem, st>>>(map, images, out, nfields, N, ncol);
 }
 
 int tc32_status() {

@@ -74,13 +74,15 @@ def test_c2_100_steps_mixed_against_f64_oracle(tb, golden_dir, name):
         assert err < MIXED_BAR, ("p", err)
 
 
-@pytest.mark.parametrize("precision,bar", [("F64", F64_BAR), ("MIXED", MIXED_BAR)])
-def test_3d_20_steps_against_oracle(tb, golden_dir, precision, bar):
+@pytest.mark.parametrize("precision,bar,tensor_cores", [("F64", F64_BAR, False), ("MIXED", MIXED_BAR, False),
+                                                      ("MIXED", MIXED_BAR, True)])
+def test_3d_20_steps_against_oracle(tb, golden_dir, precision, bar, tensor_cores):
     d = _fixture(golden_dir, "rbc3_rk222_64x64x32")
     Nx, Ny, Nz = int(d["Nx"]), int(d["Ny"]), int(d["Nz"])
     p = RBC3Params(Nx=Nx, Ny=Ny, Nz=Nz, Ra=float(d["Ra"]))
     plan = tb.Plan3D(Nx, Ny, Nz, p.kappa, p.nu, TS[str(d["scheme"])], p.Lx, p.Ly, p.Lz,
                      precision=getattr(tb._lib, f"TB_PREC_{precision}"))
+    plan.set_gemm_path(tensor_cores)
     plan.set_state(tb._lib.TB_FIELD_B, plan.forward(rbc3_initial_b(p, 42)))
     plan.step(float(d["dt"]), int(d["nsteps"]))
     for name, f in (("b", 0), ("ux", 1), ("uy", 5), ("uz", 2)):

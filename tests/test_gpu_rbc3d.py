@@ -23,10 +23,11 @@ CASES = [
 ]
 
 
-def _run(tb, case, precision, seed=42):
+def _run(tb, case, precision, seed=42, tensor_cores=False):
     Nx, Ny, Nz, Lx, Ly, Ra, scheme, dt, n = case
     p = RBC3Params(Nx=Nx, Ny=Ny, Nz=Nz, Lx=Lx, Ly=Ly, Lz=1.0, Ra=Ra)
     plan = tb.Plan3D(Nx, Ny, Nz, p.kappa, p.nu, TS[scheme], Lx, Ly, 1.0, precision=precision)
+    plan.set_gemm_path(tensor_cores)
     plan.set_state(tb._lib.TB_FIELD_B, plan.forward(rbc3_initial_b(p, seed, amp=1e-2)))
     plan.step(dt, n)
     sim = RBC3D(p)
@@ -52,6 +53,17 @@ def test_rbc3d_f64_matches_oracle(tb, case):
 @pytest.mark.parametrize("case", CASES[:2] + CASES[-2:])
 def test_rbc3d_mixed_matches_oracle(tb, case):
     plan, sim = _run(tb, case, tb._lib.TB_PREC_MIXED)
+    for name, f in FIELDS:
+        assert rel_l2(plan.get_state(f), getattr(sim, name)) < 1e-6, name
+
+
+@pytest.mark.parametrize("case", CASES[:2] + CASES[-3:])
+def test_rbc3d_mixed_tensor_cores_match_oracle(tb, case):
+    # the z transforms on the streaming tcgen05 kernel (TF32, three products
+    # per term): partial 32-column tiles (216 and 224 columns), 2 to 150
+    # tiles per field
+    plan, sim = _run(tb, case, tb._lib.TB_PREC_MIXED, tensor_cores=True)
+    assert plan.gemm_path()
     for name, f in FIELDS:
         assert rel_l2(plan.get_state(f), getattr(sim, name)) < 1e-6, name
 

@@ -63,3 +63,35 @@ def test_beyond_the_tensor_core_tile_falls_back(tb):
         outs[tc] = plan.rhs_advection(*ins)
     for a, b in zip(outs[True], outs[False]):
         assert np.array_equal(a, b)  # the same SIMT kernel ran
+
+
+def _plan3(tb, Nx, Ny, Nz, tensor_cores):
+    from oracle.tarang_oracle import RBC3Params, rbc3_initial_b
+
+    p = RBC3Params(Nx=Nx, Ny=Ny, Nz=Nz, Lx=4.0, Ly=4.0, Lz=1.0, Ra=1e7)
+    plan = tb.Plan3D(Nx, Ny, Nz, p.kappa, p.nu, TS["RK222"], 4.0, 4.0, 1.0, precision=tb._lib.TB_PREC_MIXED)
+    plan.set_gemm_path(tensor_cores)
+    plan.set_state(tb._lib.TB_FIELD_B, plan.forward(rbc3_initial_b(p, 42, amp=1e-2)))
+    return plan
+
+
+@pytest.mark.parametrize("Nx,Ny,Nz", [(128, 96, 64), (64, 64, 128)])
+def test_3d_streaming_tensor_cores_match_simt(tb, Nx, Ny, Nz):
+    # many (field, 32-column tile) tasks per persistent CTA (12480 and 4224
+    # columns), the largest supported Nz; both paths are FP32-accurate
+    plans = {tc: _plan3(tb, Nx, Ny, Nz, tc) for tc in (True, False)}
+    for pl in plans.values():
+        pl.step(0.005, 3)
+    for f in (0, 1, 2, 5):
+        a, b = plans[True].get_state(f), plans[False].get_state(f)
+        assert np.isfinite(a).all()
+        assert rel_l2(a, b) < 1e-6, f
+
+
+def test_3d_beyond_the_streaming_tile_falls_back(tb):
+    # Nz = 136 > 128 rows per tile: the SIMT kernel runs
+    plans = {tc: _plan3(tb, 8, 8, 136, tc) for tc in (True, False)}
+    for pl in plans.values():
+        pl.step(0.001, 2)
+    for f in (0, 1, 2, 5):
+        assert np.array_equal(plans[True].get_state(f), plans[False].get_state(f))
