@@ -523,48 +523,108 @@ __host__ __device__ inline int pass_twiddle_count(const FftPlan& fp) {
 // Twiddles: per pass s, exp(-2 pi i j / L_s) for j < m_s (ip_twiddle_count
 // entries, the passes one after another); sign > 0 conjugates them.
 // ---------------------------------------------------------------------------
-template <int R, bool SW, bool DIF, class C>
+// powers w^r (r = 1 .. R-1) of a pass twiddle, formed as twiddle_apply forms
+// them (the same products, so the results are bitwise those of twiddle_apply)
+template <int R, class C>
+__device__ __forceinline__ void twiddle_powers(C (&w)[R], C w1) {
+  w[1] = w1;
+  if constexpr (R == 8) {
+    w[2] = mul(w1, w1);
+    w[4] = mul(w[2], w[2]);
+    w[3] = mul(w1, w[2]);
+    w[5] = mul(w1, w[4]);
+    w[6] = mul(w[2], w[4]);
+    w[7] = mul(w[3], w[4]);
+  } else if constexpr (R == 4) {
+    w[2] = mul(w1, w1);
+    w[3] = mul(w1, w[2]);
+  } else if constexpr (R == 3) {
+    w[2] = mul(w1, w1);
+  }
+}
+
+// G arrays per item (the same butterfly of G arrays: independent arithmetic
+// chains that share one set of twiddle powers)
+template <int R, bool SW, bool DIF, int G, class C>
 __device__ __forceinline__ void pass_ip(C* __restrict__ buf, int NA, int Ms, int n, int L,
                                         const C* __restrict__ pt, int sign) {
-  const int m = L / R, nb = n / R, total = NA * nb;
+  const int m = L / R, nb = n / R, total = (NA / G) * nb;
   for (int item = threadIdx.x; item < total; item += blockDim.x) {
-    const int arr = item / nb, b = item - arr * nb;
-    C* x = buf + (size_t)arr * Ms;
+    const int grp = item / nb, b = item - grp * nb;
+    C* x = buf + (size_t)grp * G * Ms;
     const int block = b / m, j = b - block * m;
     const int base = block * L + j;
-    C v[R];
+    C v[G][R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = x[fidx<SW>(base + r * m)];
-    if constexpr (DIF) {
-      dft_small<R>(v, sign);
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[g][r] = x[(size_t)g * Ms + fidx<SW>(base + r * m)];
+    if constexpr (G == 1) {
+      // one array: the powers formed as they are applied (fewer live registers)
+      C w1 = mk<C>(0, 0);
       if (m > 1) {
-        C w1 = pt[j];
+        w1 = pt[j];
         if (sign > 0) w1.y = -w1.y;
-        twiddle_apply<R>(v, w1);
+      }
+      if constexpr (DIF) {
+        dft_small<R>(v[0], sign);
+        if (m > 1) twiddle_apply<R>(v[0], w1);
+      } else {
+        if (m > 1) twiddle_apply<R>(v[0], w1);
+        dft_small<R>(v[0], sign);
       }
     } else {
+      C w[R];
       if (m > 1) {
         C w1 = pt[j];
         if (sign > 0) w1.y = -w1.y;
-        twiddle_apply<R>(v, w1);
+        twiddle_powers<R>(w, w1);
       }
-      dft_small<R>(v, sign);
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        if constexpr (DIF) {
+          dft_small<R>(v[g], sign);
+          if (m > 1)
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[g][r] = mul(v[g][r], w[r]);
+        } else {
+          if (m > 1)
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[g][r] = mul(v[g][r], w[r]);
+          dft_small<R>(v[g], sign);
+        }
+      }
     }
 #pragma unroll
-    for (int r = 0; r < R; ++r) x[fidx<SW>(base + r * m)] = v[r];
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[(size_t)g * Ms + fidx<SW>(base + r * m)] = v[g][r];
   }
 }
 
 template <bool SW, bool DIF, class C>
 __device__ __forceinline__ void pass_ip_r(int R, C* buf, int NA, int Ms, int n, int L, const C* pt, int sign) {
-  if (R == 8)
-    pass_ip<8, SW, DIF>(buf, NA, Ms, n, L, pt, sign);
-  else if (R == 4)
-    pass_ip<4, SW, DIF>(buf, NA, Ms, n, L, pt, sign);
-  else if (R == 2)
-    pass_ip<2, SW, DIF>(buf, NA, Ms, n, L, pt, sign);
-  else
-    pass_ip<3, SW, DIF>(buf, NA, Ms, n, L, pt, sign);
+  // FP32: arrays in pairs when their count is even (FP64 pairs run out of
+  // registers at two CTAs per SM and were no faster)
+  if (sizeof(C) == sizeof(float2) && NA % 2 == 0) {
+    if (R == 8)
+      pass_ip<8, SW, DIF, 2>(buf, NA, Ms, n, L, pt, sign);
+    else if (R == 4)
+      pass_ip<4, SW, DIF, 2>(buf, NA, Ms, n, L, pt, sign);
+    else if (R == 2)
+      pass_ip<2, SW, DIF, 2>(buf, NA, Ms, n, L, pt, sign);
+    else
+      pass_ip<3, SW, DIF, 2>(buf, NA, Ms, n, L, pt, sign);
+  } else {
+    if (R == 8)
+      pass_ip<8, SW, DIF, 1>(buf, NA, Ms, n, L, pt, sign);
+    else if (R == 4)
+      pass_ip<4, SW, DIF, 1>(buf, NA, Ms, n, L, pt, sign);
+    else if (R == 2)
+      pass_ip<2, SW, DIF, 1>(buf, NA, Ms, n, L, pt, sign);
+    else
+      pass_ip<3, SW, DIF, 1>(buf, NA, Ms, n, L, pt, sign);
+  }
 }
 
 // DIF: natural order in, digit-reversed out (in place)
