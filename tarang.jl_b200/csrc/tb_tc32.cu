@@ -418,14 +418,14 @@ __device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* m
 // issuer.  Stage s = tile % 2 of the raw tile and of its hi / lo images,
 // accumulator buffer a = tile % 2; the hand-offs are mbarriers: full (TMA ->
 // split), rawfree (split -> producer), splitfull (split -> MMA), accfull (MMA
-// completion, by tcgen05.commit), accfree (epilogue -> MMA), stagefree
-// (epilogue -> split).  Once the MMAs of a tile have completed, its hi / lo
-// buffer is the epilogue's staging area: each epilogue warp writes its 32
-// accumulator rows there (16-byte chunks XOR-swizzled by row) and reads them
-// back row by row for full-line global stores; the split refills the buffer
-// after that.
-constexpr int kSThreads = 320;
-constexpr int kSEpi = 0, kSSplit = 4, kSProd = 8, kSMma = 9;  // first warp of each role
+// completion, by tcgen05.commit), hilofree (MMA completion -> split), accfree
+// (epilogue -> MMA).  The epilogue reads the accumulator in the 16 x 256-bit
+// shape (four lanes per row, two columns each), so that every store of a
+// warp writes whole 32-byte sectors straight from registers.
+constexpr int kSSplitWarps = 4;  // warps of the split role
+constexpr int kSSplitThreads = 32 * kSSplitWarps;
+constexpr int kSEpi = 0, kSSplit = 4, kSProd = kSSplit + kSSplitWarps, kSMma = kSProd + 1;  // first warp of each role
+constexpr int kSThreads = 32 * (kSMma + 1);
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
   // mbarriers: A, then per stage / buffer b: full, rawfree, splitfull, hilofree, accfull, accfree
   const uint32_t barA = sbase + kSOffBar;
   auto bar = [&](int kind, int b) { return barA + 8u + 16u * (uint32_t)kind + 8u * (uint32_t)b; };
-  enum { FULL = 0, RAWFREE, SPLITFULL, STAGEFREE, ACCFULL, ACCFREE };
+  enum { FULL = 0, RAWFREE, SPLITFULL, HILOFREE, ACCFULL, ACCFREE };
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kSOffBar + 112);
   volatile int* abort = reinterpret_cast<volatile int*>(sm + kSOffBar + 120);
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
@@ -490,9 +490,9 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barA));
     for (int b = 0; b < 2; ++b) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar(FULL, b)));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(bar(RAWFREE, b)));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(bar(SPLITFULL, b)));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(bar(STAGEFREE, b)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar(RAWFREE, b)), "r"(kSSplitThreads));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar(SPLITFULL, b)), "r"(kSSplitThreads));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar(HILOFREE, b)));
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar(ACCFULL, b)));
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(bar(ACCFREE, b)));
     }
@@ -521,26 +521,26 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
         last_load[s] = i;
       }
     }
-  } else if (warp >= kSSplit && warp < kSSplit + 4) {
+  } else if (warp >= kSSplit && warp < kSSplit + kSSplitWarps) {
     const int t = tid - 32 * kSSplit;
     for (int i = 0; i < n; ++i) {
       const int s = i & 1;
       if (!mbar_wait_or_abort(bar(FULL, s), ph(i), abort)) break;
-      if (i >= 2 && !mbar_wait_or_abort(bar(STAGEFREE, s), ph_prev(i), abort)) break;
+      if (i >= 2 && !mbar_wait_or_abort(bar(HILOFREE, s), ph_prev(i), abort)) break;
       // split the raw tile [row < N][32 columns] into the K-major hi / lo
       // images (rows past N are zero)
       const float* rt = reinterpret_cast<const float*>(sm + kSOffRaw + (uint32_t)s * kSRawBytes);
       uint8_t* hb = sm + kSOffB + (uint32_t)s * 32768u;
       auto row = [&](int j, int nn) { return j < N ? rt[(size_t)j * kSN + nn] : 0.f; };
       if constexpr (BWD) {
-        for (int it = t; it < 2 * 16 * kSN; it += 128) {
+        for (int it = t; it < 2 * 16 * kSN; it += kSSplitThreads) {
           const int nn = it % kSN, kc = (it / kSN) % 16, p = it / (16 * kSN);
           const int j0 = 8 * kc + p;  // rows 2 (4 kc + i) + p
           const float4 v = make_float4(row(j0, nn), row(j0 + 2, nn), row(j0 + 4, nn), row(j0 + 6, nn));
           split_store4(hb + p * 16384, hb + p * 16384 + 8192, sw128_off(nn, 4 * kc, kSN), v);
         }
       } else {
-        for (int it = t; it < 32 * kSN; it += 128) {
+        for (int it = t; it < 32 * kSN; it += kSSplitThreads) {
           const int nn = it % kSN, kc = it / kSN, j0 = 4 * kc;
           const float4 v = make_float4(row(j0, nn), row(j0 + 1, nn), row(j0 + 2, nn), row(j0 + 3, nn));
           split_store4(hb, hb + 16384, sw128_off(nn, 4 * kc, kSN), v);
@@ -591,13 +591,18 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
           }
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                         bar(HILOFREE, s))
+                     : "memory");
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                          bar(ACCFULL, a))
                      : "memory");
         last_mma = i;
       }
     }
   } else if (warp < kSEpi + 4) {
-    const int r = warp * 32 + lane;  // accumulator lane = A row of this thread
+    // 16 x 256-bit accumulator loads: lane l of the warp holds rows
+    // l / 4 and l / 4 + 8 of a 16-row block, columns 8 k + 2 (l % 4) + {0, 1}
+    // of repetition k (registers 4 k .. 4 k + 3: row l / 4, then row l / 4 + 8)
     for (int i = 0; i < n; ++i) {
       const int a = i & 1;
       // one decision per warp: the accumulator loads below are warp-wide
@@ -606,91 +611,65 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
       int f, n0;
       task(i, &f, &n0);
       const bool full = n0 + kSN <= ncol;
-      uint32_t v[BWD ? 2 : 1][32];
+      constexpr int NACC = BWD ? 2 : 1;
+      uint32_t v[NACC][2][16];
 #pragma unroll
-      for (int acc = 0; acc < (BWD ? 2 : 1); ++acc) {
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * 64 + acc * 32);
-        uint32_t* w = v[acc];
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
-            : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]),
-              "=r"(w[8]), "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]), "=r"(w[15]),
-              "=r"(w[16]), "=r"(w[17]), "=r"(w[18]), "=r"(w[19]), "=r"(w[20]), "=r"(w[21]), "=r"(w[22]),
-              "=r"(w[23]), "=r"(w[24]), "=r"(w[25]), "=r"(w[26]), "=r"(w[27]), "=r"(w[28]), "=r"(w[29]),
-              "=r"(w[30]), "=r"(w[31])
-            : "r"(taddr));
-      }
+      for (int acc = 0; acc < NACC; ++acc)
+#pragma unroll
+        for (int hb = 0; hb < 2; ++hb) {
+          const uint32_t taddr =
+              tmem + ((uint32_t)(warp * 32 + hb * 16) << 16) + (uint32_t)(a * 64 + acc * 32);
+          uint32_t* w = v[acc][hb];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+              "[%16];\n"
+              : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]),
+                "=r"(w[8]), "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]),
+                "=r"(w[15])
+              : "r"(taddr));
+        }
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
       // the accumulator buffer is read: the MMAs of tile i + 2 may overwrite it
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
       mbar_arrive(bar(ACCFREE, a));
-      // stage this warp's 32 rows in the tile's hi / lo buffer (its MMAs have
-      // completed), [acc][row][32 values] with 16-byte chunk c of row r at
-      // c ^ (r & 7), then store whole rows
-      uint8_t* stg = sm + kSOffB + (uint32_t)a * 32768u;
-      constexpr int VB = BWD ? 4 : 8;                // bytes per output value
-      constexpr int RB = kSN * VB;                   // bytes per staged row
-      constexpr int CH = RB / 16;                    // 16-byte chunks per row
 #pragma unroll
-      for (int acc = 0; acc < (BWD ? 2 : 1); ++acc) {
-        uint8_t* srow = stg + (size_t)acc * 128 * RB + (size_t)r * RB;
+      for (int acc = 0; acc < NACC; ++acc)
 #pragma unroll
-        for (int c = 0; c < CH; ++c) {
-          uint4 q;
-          if constexpr (BWD) {
-            q = make_uint4(v[acc][4 * c], v[acc][4 * c + 1], v[acc][4 * c + 2], v[acc][4 * c + 3]);
-          } else {
-            const double2 lo = make_double2((double)__uint_as_float(v[acc][2 * c]), (double)__uint_as_float(v[acc][2 * c + 1]));
-            q = *reinterpret_cast<const uint4*>(&lo);
-          }
-          *reinterpret_cast<uint4*>(srow + ((c ^ (r & 7)) << 4)) = q;
-        }
-      }
-      __syncwarp();
-      // row-wise stores: RPI rows per instruction, CH lanes of 16 bytes per row
-      constexpr int RPI = 32 / CH;
+        for (int hb = 0; hb < 2; ++hb)
 #pragma unroll
-      for (int acc = 0; acc < (BWD ? 2 : 1); ++acc) {
-#pragma unroll 4
-        for (int r0 = 0; r0 < 32; r0 += RPI) {
-          const int rl = r0 + lane / CH, c = lane % CH;  // row within the warp's 32, chunk
-          const int rg = warp * 32 + rl;                  // accumulator row
-          const uint4 q = *reinterpret_cast<const uint4*>(stg + (size_t)acc * 128 * RB + (size_t)rg * RB +
-                                                           ((c ^ (rg & 7)) << 4));
-          const int hh = rg >> 6, rh = rg & 63;
-          const int col = n0 + c * (16 / VB);  // first column of this chunk
-          if constexpr (BWD) {
-            // parity acc, half hh (0 value, 1 derivative): item acc + 2 hh
-            if (rh < H) {
-              float* dst = reinterpret_cast<float*>(out) + ((size_t)(4 * f + acc + 2 * hh) * H + rh) * ncol + col;
-              if (full) {
-                *reinterpret_cast<uint4*>(dst) = q;
+          for (int rh2 = 0; rh2 < 2; ++rh2) {
+            const int rg = warp * 32 + hb * 16 + lane / 4 + 8 * rh2;  // accumulator row
+            const int hh = rg >> 6, rh = rg & 63;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int col = n0 + 8 * k + 2 * (lane % 4);
+              const float x0 = __uint_as_float(v[acc][hb][4 * k + 2 * rh2]);
+              const float x1 = __uint_as_float(v[acc][hb][4 * k + 2 * rh2 + 1]);
+              if constexpr (BWD) {
+                // parity acc, half hh (0 value, 1 derivative): item acc + 2 hh
+                if (rh < H) {
+                  float* dst = reinterpret_cast<float*>(out) + ((size_t)(4 * f + acc + 2 * hh) * H + rh) * ncol + col;
+                  if (full) {
+                    *reinterpret_cast<float2*>(dst) = make_float2(x0, x1);
+                  } else {
+                    if (col < ncol) dst[0] = x0;
+                    if (col + 1 < ncol) dst[1] = x1;
+                  }
+                }
               } else {
-                const float e[4] = {__uint_as_float(q.x), __uint_as_float(q.y), __uint_as_float(q.z),
-                                    __uint_as_float(q.w)};
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                  if (col + k < ncol) dst[k] = e[k];
-              }
-            }
-          } else {
-            // half hh is the output parity: row 2 rh + hh
-            if (rh < (hh ? Ko : Ke)) {
-              double* dst = reinterpret_cast<double*>(out) + ((size_t)f * N + 2 * rh + hh) * ncol + col;
-              if (full) {
-                *reinterpret_cast<uint4*>(dst) = q;
-              } else {
-                const double2 e = *reinterpret_cast<const double2*>(&q);
-                if (col < ncol) dst[0] = e.x;
-                if (col + 1 < ncol) dst[1] = e.y;
+                // half hh is the output parity: row 2 rh + hh
+                if (rh < (hh ? Ko : Ke)) {
+                  double* dst = reinterpret_cast<double*>(out) + ((size_t)f * N + 2 * rh + hh) * ncol + col;
+                  if (full) {
+                    *reinterpret_cast<double2*>(dst) = make_double2((double)x0, (double)x1);
+                  } else {
+                    if (col < ncol) dst[0] = (double)x0;
+                    if (col + 1 < ncol) dst[1] = (double)x1;
+                  }
+                }
               }
             }
           }
-        }
-      }
-      __syncwarp();
-      mbar_arrive(bar(STAGEFREE, a));  // the split may refill this buffer
     }
   }
   __syncthreads();
