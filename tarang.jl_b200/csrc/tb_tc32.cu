@@ -344,33 +344,43 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc32(GemmBatch32 bt, int
 
 
 // ---- streaming form (3D planes) ----
-constexpr int kSN = 32;                                  // columns per tile
+constexpr int kSN = 64;                                  // columns per tile (the MMA's N)
 constexpr int kSRows = 128;                              // input rows per tile (N <= 128)
-constexpr uint32_t kSRawBytes = kSRows * kSN * 4;        // 16 KB raw tile
-constexpr uint32_t kSOffA = 0;                           // A images, 128 KB
-constexpr uint32_t kSOffB = 128 * 1024;                  // two hi/lo B buffers of 32 KB
-constexpr uint32_t kSOffRaw = kSOffB + 2 * 32 * 1024;    // two raw tiles of 16 KB
-constexpr uint32_t kSOffBar = kSOffRaw + 2 * kSRawBytes;  // 13 mbarriers, TMEM address, abort flag
-constexpr uint32_t kSSmem = kSOffBar + 128 + 1024;        // + alignment slack
+constexpr int kSNR = 2;                                  // raw tile stages
+constexpr int kSNH = 2;                                  // hi / lo image stages
+constexpr uint32_t kSRawBytes = kSRows * kSN * 4;        // 32 KB raw tile
+constexpr uint32_t kSHiloBytes = 2 * kSRows * kSN * 4;   // 64 KB of hi and lo images
+constexpr uint32_t kSAtom = kSN * 128;                   // bytes of one 32-wide K atom of a B image
+constexpr uint32_t kSOffRaw = 0;
+constexpr uint32_t kSOffB = kSOffRaw + kSNR * kSRawBytes;
+constexpr uint32_t kSOffBar = kSOffB + kSNH * kSHiloBytes;  // mbarriers, TMEM address, abort flag
+constexpr uint32_t kSSmem = kSOffBar + 256 + 1024;          // + alignment slack
 static_assert(kSSmem <= 232448, "one CTA per SM");
-constexpr uint32_t kSTmemCols = 128;  // two buffers of (up to) two 32-column accumulators
-constexpr size_t kSImageFloats = 2 * 2 * 128 * 64 + 2 * 128 * 128;  // backward pair (K 64), forward (K 128); hi and lo
-// instruction descriptor: D F32, A and B TF32, both K-major, N 32, M 128
+// Tensor memory: the A operands (hi and lo, 256 columns: backward parity p
+// hi / lo at 64 (2p + h), forward hi at 0, lo at 128), then two accumulator
+// buffers of 128 columns from column 256 (backward parity p at + 64 p).
+constexpr uint32_t kSTmemCols = 512;
+constexpr uint32_t kSTmemAcc = 256;
+constexpr size_t kSImageFloats = 2 * 2 * 128 * 64 + 2 * 128 * 128;  // backward parts (K 64), forward (K 128)
+// instruction descriptor: D F32, A and B TF32, both K-major, N 64, M 128
 constexpr uint32_t kSIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kSN >> 3) << 17) |
                              ((uint32_t)(kTcM >> 4) << 24);
 
-__device__ __forceinline__ void mma_tf32_n32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+// D (tensor memory) += A (tensor memory, 128 lanes x 8 columns) . B (shared memory)
+__device__ __forceinline__ void mma_tf32_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(kSIdesc), "r"(accumulate));
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(bdesc), "r"(kSIdesc), "r"(accumulate));
 }
 
-// TF32 hi / lo images of the streaming form's A operands, K-major, 128-byte
-// swizzled, 128 rows each: blockIdx.x 0 and 1 the backward parities (K 64:
-// rows r < 64 value, r >= 64 derivative, of the columns 2k + p), 2 the
-// forward operand (K 128, the mirror folded in, rows r < 64 the even
-// outputs 2r, r >= 64 the odd ones 2(r - 64) + 1).
+// TF32 hi / lo parts of the streaming form's A operands, row-major (128 rows
+// of K values each, the layout the epilogue warps copy into tensor memory):
+// blockIdx.x 0 and 1 the backward parities (K 64: rows r < 64 value, r >= 64
+// derivative, of the columns 2k + p), 2 the forward operand (K 128, the mirror
+// folded in, rows r < 64 the even outputs 2r, r >= 64 the odd ones).
+// Parts: backward parity p hi at 2p, lo at 2p + 1 (128 x 64 each), then the
+// forward hi and lo (128 x 128 each).
 __global__ void __launch_bounds__(kTcThreads) k_tc32s_image(const float* __restrict__ Ev, const float* __restrict__ Ov,
                                                             const float* __restrict__ Ed, const float* __restrict__ Od,
                                                             int kpe, int kpo, const float* __restrict__ sfE,
@@ -378,33 +388,28 @@ __global__ void __launch_bounds__(kTcThreads) k_tc32s_image(const float* __restr
                                                             float* __restrict__ images) {
   const int H = N / 2, Ke = (N + 1) / 2, Ko = N / 2;
   const int img = blockIdx.x;
-  const int kt = img < 2 ? 64 : 128;  // K extent of this image
-  const uint32_t half = 128u * kt * 4u;  // bytes of its hi part
-  uint8_t* hi = reinterpret_cast<uint8_t*>(images) + (size_t)(img < 2 ? img : 2) * 2 * 128 * 64 * 4;
-  uint8_t* lo = hi + half;
-  for (int idx = threadIdx.x; idx < 128 * (kt / 4); idx += kTcThreads) {
-    const int r = idx / (kt / 4), k0 = 4 * (idx % (kt / 4));
-    float f[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int k = k0 + i;
-      float v = 0.f;
-      if (img < 2) {
-        const int p = img, K = p ? Ko : Ke, kp = p ? kpo : kpe, rr = r & 63;
-        const float* src = r < 64 ? (p ? Ov : Ev) : (p ? Od : Ed);
-        if (rr < H && k < K) v = src[(size_t)rr * kp + k];
-      } else {
-        const int par = r >= 64, rr = r & 63, M = par ? Ko : Ke;
-        const float* src = par ? sfO : sfE;
-        if (rr < M && k < N) v = k < H ? src[(size_t)rr * kph + k] : (par ? -1.f : 1.f) * src[(size_t)rr * kph + (N - 1 - k)];
-      }
-      f[i] = v;
+  const int kt = img < 2 ? 64 : 128;  // K extent of this operand
+  float* hi = images + (size_t)(img < 2 ? img : 2) * 2 * 128 * 64;
+  float* lo = hi + (size_t)128 * kt;
+  for (int idx = threadIdx.x; idx < 128 * kt; idx += kTcThreads) {
+    const int r = idx / kt, k = idx % kt;
+    float v = 0.f;
+    if (img < 2) {
+      const int p = img, K = p ? Ko : Ke, kp = p ? kpo : kpe, rr = r & 63;
+      const float* src = r < 64 ? (p ? Ov : Ev) : (p ? Od : Ed);
+      if (rr < H && k < K) v = src[(size_t)rr * kp + k];
+    } else {
+      const int par = r >= 64, rr = r & 63, M = par ? Ko : Ke;
+      const float* src = par ? sfO : sfE;
+      if (rr < M && k < N) v = k < H ? src[(size_t)rr * kph + k] : (par ? -1.f : 1.f) * src[(size_t)rr * kph + (N - 1 - k)];
     }
-    split_store4(hi, lo, sw128_off(r, k0, 128), make_float4(f[0], f[1], f[2], f[3]));
+    const uint32_t h = to_tf32(v);
+    hi[idx] = __uint_as_float(h);
+    lo[idx] = __uint_as_float(to_tf32(v - __uint_as_float(h)));
   }
 }
 
-// 3D tile load: 32 columns x N rows of field z from the tensor map into dst
+// 3D tile load: 64 columns x N rows of field z from the tensor map into dst
 __device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* map, int x, int z, uint32_t bar) {
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
@@ -413,15 +418,19 @@ __device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* m
       : "memory");
 }
 
-// Roles (10 warps): warps 0-3 the epilogue (warp w reads accumulator lanes
-// 32w..32w+31), warps 4-7 the split, warp 8 the TMA producer, warp 9 the MMA
-// issuer.  Stage s = tile % 2 of the raw tile and of its hi / lo images,
-// accumulator buffer a = tile % 2; the hand-offs are mbarriers: full (TMA ->
-// split), rawfree (split -> producer), splitfull (split -> MMA), accfull (MMA
-// completion, by tcgen05.commit), hilofree (MMA completion -> split), accfree
-// (epilogue -> MMA).  The epilogue reads the accumulator in the 16 x 256-bit
-// shape (four lanes per row, two columns each), so that every store of a
-// warp writes whole 32-byte sectors straight from registers.
+// Roles (10 warps): warps 0-3 the epilogue (warp w owns tensor-memory lanes
+// 32w..32w+31; before the tiles they copy the A operands into tensor memory),
+// warps 4-7 the split, warp 8 the TMA producer, warp 9 the MMA issuer.  Raw
+// stage i % kSNR, hi / lo stage i % kSNH and accumulator buffer i % 2 of tile
+// i; the hand-offs are mbarriers: aload (A in tensor memory -> MMA), full (TMA
+// -> split), rawfree (split -> producer), splitfull (split -> MMA), hilofree
+// and accfull (MMA completion, by tcgen05.commit), accfree (epilogue -> MMA).
+// A in tensor memory leaves the MMAs only B to read from shared memory and
+// the shared memory to tiles of 64 columns (N 64 per MMA: half the MMA
+// instructions per column of N 32, whose fixed cost per instruction bounded
+// the kernel).  The epilogue reads the accumulator in the 16 x 256-bit shape
+// (four lanes per row, two columns each), so that every store of a warp
+// writes whole 32-byte sectors straight from registers.
 constexpr int kSSplitWarps = 4;  // warps of the split role
 constexpr int kSSplitThreads = 32 * kSSplitWarps;
 constexpr int kSEpi = 0, kSSplit = 4, kSProd = kSSplit + kSSplitWarps, kSMma = kSProd + 1;  // first warp of each role
@@ -457,17 +466,23 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
   const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
   uint8_t* sm = tc_smem_raw + pad;
   const uint32_t sbase = raw + pad;
-  // mbarriers: A, then per stage / buffer b: full, rawfree, splitfull, hilofree, accfull, accfree
-  const uint32_t barA = sbase + kSOffBar;
-  auto bar = [&](int kind, int b) { return barA + 8u + 16u * (uint32_t)kind + 8u * (uint32_t)b; };
-  enum { FULL = 0, RAWFREE, SPLITFULL, HILOFREE, ACCFULL, ACCFREE };
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kSOffBar + 112);
-  volatile int* abort = reinterpret_cast<volatile int*>(sm + kSOffBar + 120);
+  // mbarriers: aload, full[kSNR], rawfree[kSNR], splitfull[kSNH], hilofree[kSNH], accfull[2], accfree[2]
+  const uint32_t barL = sbase + kSOffBar;
+  auto barFull = [&](int r) { return barL + 8u + 8u * (uint32_t)r; };
+  auto barRawFree = [&](int r) { return barL + 8u + 8u * (uint32_t)(kSNR + r); };
+  auto barSplitFull = [&](int h) { return barL + 8u + 8u * (uint32_t)(2 * kSNR + h); };
+  auto barHiloFree = [&](int h) { return barL + 8u + 8u * (uint32_t)(2 * kSNR + kSNH + h); };
+  auto barAccFull = [&](int a) { return barL + 8u + 8u * (uint32_t)(2 * kSNR + 2 * kSNH + a); };
+  auto barAccFree = [&](int a) { return barL + 8u + 8u * (uint32_t)(2 * kSNR + 2 * kSNH + 2 + a); };
+  constexpr uint32_t kBarBytes = 8u * (1 + 2 * kSNR + 2 * kSNH + 4);
+  static_assert(kBarBytes + 16 <= 256, "barrier area");
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kSOffBar + kBarBytes);
+  volatile int* abort = reinterpret_cast<volatile int*>(sm + kSOffBar + kBarBytes + 8);
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const int H = N / 2, Ke = (N + 1) / 2, Ko = N / 2;
   const int ntiles = (ncol + kSN - 1) / kSN;
   const int ntask = nfields * ntiles;
-  const uint32_t tile_bytes = (uint32_t)(kSN * N * 4);  // one TMA box: 32 columns x N rows
+  const uint32_t tile_bytes = (uint32_t)(kSN * N * 4);  // one TMA box: 64 columns x N rows
   // local tiles i = 0 .. n-1 are the tasks blockIdx.x + i gridDim.x
   const int n = blockIdx.x < ntask ? (ntask - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   auto task = [&](int i, int* f, int* n0) {
@@ -475,26 +490,30 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
     *f = t / ntiles;
     *n0 = (t % ntiles) * kSN;
   };
-  auto ph = [](int i) { return (uint32_t)(i >> 1) & 1u; };       // phase parity of tile i's use of its stage
-  auto ph_prev = [](int i) { return (uint32_t)((i >> 1) - 1) & 1u; };  // of tile i - 2 (i >= 2)
+  // phase parity of tile i's use of a ring of depth D, and of tile i - D's
+  auto ph = [](int i, int D) { return (uint32_t)(i / D) & 1u; };
+  auto ph_prev = [](int i, int D) { return (uint32_t)(i / D - 1) & 1u; };
 
   if (warp == kSEpi) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + kSOffBar + 112),
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + kSOffBar +
+                                                                                            kBarBytes),
                  "r"(kSTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
-  const uint32_t abytes = BWD ? 4u * 128u * 64u * 4u : 2u * 128u * 128u * 4u;  // 128 KB either way
-  const float* aimg = images + (BWD ? 0 : 2 * 2 * 128 * 64);
   if (tid == 0) {
     *abort = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barA));
-    for (int b = 0; b < 2; ++b) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar(FULL, b)));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar(RAWFREE, b)), "r"(kSSplitThreads));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar(SPLITFULL, b)), "r"(kSSplitThreads));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar(HILOFREE, b)));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar(ACCFULL, b)));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(bar(ACCFREE, b)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(barL));
+    for (int r = 0; r < kSNR; ++r) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barFull(r)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(barRawFree(r)), "r"(kSSplitThreads));
+    }
+    for (int h = 0; h < kSNH; ++h) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(barSplitFull(h)), "r"(kSSplitThreads));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barHiloFree(h)));
+    }
+    for (int a = 0; a < 2; ++a) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barAccFull(a)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(barAccFree(a)));
     }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
   }
@@ -502,138 +521,170 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
   const uint32_t tmem = *tmem_slot;
-  bool a_pending = false;
-  int last_load[2] = {-1, -1}, last_mma = -1;  // for the bounded drain after an abort
+  int last_load[kSNR], last_mma = -1;  // for the bounded drain after an abort
+#pragma unroll
+  for (int r = 0; r < kSNR; ++r) last_load[r] = -1;
 
   if (warp == kSProd) {
     if (lane == 0) {
       asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map)) : "memory");
-      mbar_expect_tx(barA, abytes);
-      bulk_copy(sbase + kSOffA, aimg, abytes, barA);
-      a_pending = true;
       for (int i = 0; i < n; ++i) {
-        const int s = i & 1;
-        if (i >= 2 && !mbar_wait_or_abort(bar(RAWFREE, s), ph_prev(i), abort)) break;
+        const int r = i % kSNR;
+        if (i >= kSNR && !mbar_wait_or_abort(barRawFree(r), ph_prev(i, kSNR), abort)) break;
         int f, n0;
         task(i, &f, &n0);
-        mbar_expect_tx(bar(FULL, s), tile_bytes);
-        tma_load_tile(sbase + kSOffRaw + (uint32_t)s * kSRawBytes, &map, n0, f, bar(FULL, s));
-        last_load[s] = i;
+        mbar_expect_tx(barFull(r), tile_bytes);
+        tma_load_tile(sbase + kSOffRaw + (uint32_t)r * kSRawBytes, &map, n0, f, barFull(r));
+        last_load[r] = i;
       }
     }
   } else if (warp >= kSSplit && warp < kSSplit + kSSplitWarps) {
     const int t = tid - 32 * kSSplit;
     for (int i = 0; i < n; ++i) {
-      const int s = i & 1;
-      if (!mbar_wait_or_abort(bar(FULL, s), ph(i), abort)) break;
-      if (i >= 2 && !mbar_wait_or_abort(bar(HILOFREE, s), ph_prev(i), abort)) break;
-      // split the raw tile [row < N][32 columns] into the K-major hi / lo
-      // images (rows past N are zero)
-      const float* rt = reinterpret_cast<const float*>(sm + kSOffRaw + (uint32_t)s * kSRawBytes);
-      uint8_t* hb = sm + kSOffB + (uint32_t)s * 32768u;
+      const int r = i % kSNR, hs = i % kSNH;
+      if (!mbar_wait_or_abort(barFull(r), ph(i, kSNR), abort)) break;
+      if (i >= kSNH && !mbar_wait_or_abort(barHiloFree(hs), ph_prev(i, kSNH), abort)) break;
+      // split the raw tile [row < N][64 columns] into the K-major hi / lo
+      // images (rows past N are zero): backward, per parity a hi and a lo
+      // image of K 64 (16 KB each); forward, hi and lo of K 128 (32 KB each)
+      const float* rt = reinterpret_cast<const float*>(sm + kSOffRaw + (uint32_t)r * kSRawBytes);
+      uint8_t* hb = sm + kSOffB + (uint32_t)hs * kSHiloBytes;
       auto row = [&](int j, int nn) { return j < N ? rt[(size_t)j * kSN + nn] : 0.f; };
       if constexpr (BWD) {
         for (int it = t; it < 2 * 16 * kSN; it += kSSplitThreads) {
           const int nn = it % kSN, kc = (it / kSN) % 16, p = it / (16 * kSN);
           const int j0 = 8 * kc + p;  // rows 2 (4 kc + i) + p
           const float4 v = make_float4(row(j0, nn), row(j0 + 2, nn), row(j0 + 4, nn), row(j0 + 6, nn));
-          split_store4(hb + p * 16384, hb + p * 16384 + 8192, sw128_off(nn, 4 * kc, kSN), v);
+          split_store4(hb + p * 32768, hb + p * 32768 + 16384, sw128_off(nn, 4 * kc, kSN), v);
         }
       } else {
         for (int it = t; it < 32 * kSN; it += kSSplitThreads) {
           const int nn = it % kSN, kc = it / kSN, j0 = 4 * kc;
           const float4 v = make_float4(row(j0, nn), row(j0 + 1, nn), row(j0 + 2, nn), row(j0 + 3, nn));
-          split_store4(hb, hb + 16384, sw128_off(nn, 4 * kc, kSN), v);
+          split_store4(hb, hb + 32768, sw128_off(nn, 4 * kc, kSN), v);
         }
       }
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      mbar_arrive(bar(RAWFREE, s));
-      mbar_arrive(bar(SPLITFULL, s));
+      mbar_arrive(barRawFree(r));
+      mbar_arrive(barSplitFull(hs));
     }
   } else if (warp == kSMma) {
     if (lane == 0) {
-      mbar_wait_or_abort(barA, 0, abort);  // (sets the abort flag when it runs out)
+      mbar_wait_or_abort(barL, 0, abort);  // A in tensor memory (sets the abort flag when it runs out)
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
       for (int i = 0; i < n && !*abort; ++i) {
-        const int s = i & 1, a = i & 1;
-        if (!mbar_wait_or_abort(bar(SPLITFULL, s), ph(i), abort)) break;
-        if (i >= 2 && !mbar_wait_or_abort(bar(ACCFREE, a), ph_prev(i), abort)) break;
+        const int hs = i % kSNH, a = i & 1;
+        if (!mbar_wait_or_abort(barSplitFull(hs), ph(i, kSNH), abort)) break;
+        if (i >= 2 && !mbar_wait_or_abort(barAccFree(a), ph_prev(i, 2), abort)) break;
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        const uint32_t bb = sbase + kSOffB + (uint32_t)hs * kSHiloBytes;
         if constexpr (BWD) {
 #pragma unroll
           for (int p = 0; p < 2; ++p) {
-            const uint64_t ahi = sw128_desc(sbase + kSOffA + (uint32_t)p * 65536u);
-            const uint64_t alo = sw128_desc(sbase + kSOffA + (uint32_t)p * 65536u + 32768u);
-            const uint64_t bhi = sw128_desc(sbase + kSOffB + (uint32_t)s * 32768u + (uint32_t)p * 16384u);
-            const uint64_t blo = sw128_desc(sbase + kSOffB + (uint32_t)s * 32768u + (uint32_t)p * 16384u + 8192u);
-            const uint32_t d = tmem + (uint32_t)(a * 64 + p * 32);
+            const uint32_t ahi = tmem + (uint32_t)(64 * (2 * p)), alo = tmem + (uint32_t)(64 * (2 * p + 1));
+            const uint64_t bhi = sw128_desc(bb + (uint32_t)p * 32768u), blo = sw128_desc(bb + (uint32_t)p * 32768u + 16384u);
+            const uint32_t d = tmem + kSTmemAcc + (uint32_t)(a * 128 + p * 64);
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-              // start-address field += byte offset / 16 (all offsets stay below 256 KB)
-              const uint64_t ka = ((uint64_t)(j >> 2) * (128u * 128u) + (uint64_t)(j & 3) * 32u) >> 4;
-              const uint64_t kb = ((uint64_t)(j >> 2) * (kSN * 128u) + (uint64_t)(j & 3) * 32u) >> 4;
-              mma_tf32_n32(d, ahi + ka, bhi + kb, j > 0 ? 1u : 0u);
-              mma_tf32_n32(d, ahi + ka, blo + kb, 1u);
-              mma_tf32_n32(d, alo + ka, bhi + kb, 1u);
+              // B: start-address field += byte offset / 16 (offsets stay below 256 KB); A: 8 columns per step
+              const uint64_t kb = ((uint64_t)(j >> 2) * kSAtom + (uint64_t)(j & 3) * 32u) >> 4;
+              mma_tf32_ts(d, ahi + 8u * j, bhi + kb, j > 0 ? 1u : 0u);
+              mma_tf32_ts(d, ahi + 8u * j, blo + kb, 1u);
+              mma_tf32_ts(d, alo + 8u * j, bhi + kb, 1u);
             }
           }
         } else {
-          const uint64_t ahi = sw128_desc(sbase + kSOffA), alo = sw128_desc(sbase + kSOffA + 65536u);
-          const uint64_t bhi = sw128_desc(sbase + kSOffB + (uint32_t)s * 32768u);
-          const uint64_t blo = sw128_desc(sbase + kSOffB + (uint32_t)s * 32768u + 16384u);
-          const uint32_t d = tmem + (uint32_t)(a * 64);
+          const uint32_t ahi = tmem, alo = tmem + 128u;
+          const uint64_t bhi = sw128_desc(bb), blo = sw128_desc(bb + 32768u);
+          const uint32_t d = tmem + kSTmemAcc + (uint32_t)(a * 128);
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
-            const uint64_t ka = ((uint64_t)(j >> 2) * (128u * 128u) + (uint64_t)(j & 3) * 32u) >> 4;
-            const uint64_t kb = ((uint64_t)(j >> 2) * (kSN * 128u) + (uint64_t)(j & 3) * 32u) >> 4;
-            mma_tf32_n32(d, ahi + ka, bhi + kb, j > 0 ? 1u : 0u);
-            mma_tf32_n32(d, ahi + ka, blo + kb, 1u);
-            mma_tf32_n32(d, alo + ka, bhi + kb, 1u);
+            const uint64_t kb = ((uint64_t)(j >> 2) * kSAtom + (uint64_t)(j & 3) * 32u) >> 4;
+            mma_tf32_ts(d, ahi + 8u * j, bhi + kb, j > 0 ? 1u : 0u);
+            mma_tf32_ts(d, ahi + 8u * j, blo + kb, 1u);
+            mma_tf32_ts(d, alo + 8u * j, bhi + kb, 1u);
           }
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                         bar(HILOFREE, s))
+                         barHiloFree(hs))
                      : "memory");
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                         bar(ACCFULL, a))
+                         barAccFull(a))
                      : "memory");
         last_mma = i;
       }
     }
   } else if (warp < kSEpi + 4) {
+    // A operands into tensor memory: thread (warp w, lane l) owns row 32 w + l
+    // and copies its K values of each part, 32 columns per store
+    {
+      const int r = warp * 32 + lane;
+      constexpr int NPART = BWD ? 4 : 2, KP = BWD ? 64 : 128;
+      const float* src = images + (BWD ? 0 : 2 * 2 * 128 * 64);
+#pragma unroll 1
+      for (int q = 0; q < NPART; ++q)
+#pragma unroll 1
+        for (int c = 0; c < KP / 32; ++c) {
+          const float4* rowp = reinterpret_cast<const float4*>(src + ((size_t)q * 128 + r) * KP + 32 * c);
+          uint32_t w[32];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const float4 x = rowp[k];
+            w[4 * k] = __float_as_uint(x.x);
+            w[4 * k + 1] = __float_as_uint(x.y);
+            w[4 * k + 2] = __float_as_uint(x.z);
+            w[4 * k + 3] = __float_as_uint(x.w);
+          }
+          const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(q * KP + 32 * c);
+          asm volatile(
+              "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+              "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n" ::"r"(taddr),
+              "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]), "r"(w[8]),
+              "r"(w[9]), "r"(w[10]), "r"(w[11]), "r"(w[12]), "r"(w[13]), "r"(w[14]), "r"(w[15]), "r"(w[16]),
+              "r"(w[17]), "r"(w[18]), "r"(w[19]), "r"(w[20]), "r"(w[21]), "r"(w[22]), "r"(w[23]), "r"(w[24]),
+              "r"(w[25]), "r"(w[26]), "r"(w[27]), "r"(w[28]), "r"(w[29]), "r"(w[30]), "r"(w[31])
+              : "memory");
+        }
+      asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+      mbar_arrive(barL);
+    }
     // 16 x 256-bit accumulator loads: lane l of the warp holds rows
     // l / 4 and l / 4 + 8 of a 16-row block, columns 8 k + 2 (l % 4) + {0, 1}
     // of repetition k (registers 4 k .. 4 k + 3: row l / 4, then row l / 4 + 8)
     for (int i = 0; i < n; ++i) {
       const int a = i & 1;
       // one decision per warp: the accumulator loads below are warp-wide
-      if (!__all_sync(0xffffffffu, mbar_wait_or_abort(bar(ACCFULL, a), ph(i), abort))) break;
+      if (!__all_sync(0xffffffffu, mbar_wait_or_abort(barAccFull(a), ph(i, 2), abort))) break;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
       int f, n0;
       task(i, &f, &n0);
       const bool full = n0 + kSN <= ncol;
       constexpr int NACC = BWD ? 2 : 1;
-      uint32_t v[NACC][2][16];
+#pragma unroll 1
+      for (int acc = 0; acc < NACC; ++acc) {
+        uint32_t v[2][2][16];  // [lane half][32-column half][registers]
 #pragma unroll
-      for (int acc = 0; acc < NACC; ++acc)
+        for (int hb = 0; hb < 2; ++hb)
 #pragma unroll
-        for (int hb = 0; hb < 2; ++hb) {
-          const uint32_t taddr =
-              tmem + ((uint32_t)(warp * 32 + hb * 16) << 16) + (uint32_t)(a * 64 + acc * 32);
-          uint32_t* w = v[acc][hb];
-          asm volatile(
-              "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-              "[%16];\n"
-              : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]),
-                "=r"(w[8]), "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]),
-                "=r"(w[15])
-              : "r"(taddr));
+          for (int ch = 0; ch < 2; ++ch) {
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32 + hb * 16) << 16) + kSTmemAcc +
+                                   (uint32_t)(a * 128 + acc * 64 + ch * 32);
+            uint32_t* w = v[hb][ch];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];\n"
+                : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]),
+                  "=r"(w[8]), "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]),
+                  "=r"(w[15])
+                : "r"(taddr));
+          }
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (acc == NACC - 1) {
+          // the accumulator buffer is read: the MMAs of tile i + 2 may overwrite it
+          asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+          mbar_arrive(barAccFree(a));
         }
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-      // the accumulator buffer is read: the MMAs of tile i + 2 may overwrite it
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
-      mbar_arrive(bar(ACCFREE, a));
-#pragma unroll
-      for (int acc = 0; acc < NACC; ++acc)
 #pragma unroll
         for (int hb = 0; hb < 2; ++hb)
 #pragma unroll
@@ -641,35 +692,39 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
             const int rg = warp * 32 + hb * 16 + lane / 4 + 8 * rh2;  // accumulator row
             const int hh = rg >> 6, rh = rg & 63;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              const int col = n0 + 8 * k + 2 * (lane % 4);
-              const float x0 = __uint_as_float(v[acc][hb][4 * k + 2 * rh2]);
-              const float x1 = __uint_as_float(v[acc][hb][4 * k + 2 * rh2 + 1]);
-              if constexpr (BWD) {
-                // parity acc, half hh (0 value, 1 derivative): item acc + 2 hh
-                if (rh < H) {
-                  float* dst = reinterpret_cast<float*>(out) + ((size_t)(4 * f + acc + 2 * hh) * H + rh) * ncol + col;
-                  if (full) {
-                    *reinterpret_cast<float2*>(dst) = make_float2(x0, x1);
-                  } else {
-                    if (col < ncol) dst[0] = x0;
-                    if (col + 1 < ncol) dst[1] = x1;
+            for (int ch = 0; ch < 2; ++ch)
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                const int col = n0 + 32 * ch + 8 * k + 2 * (lane % 4);
+                const float x0 = __uint_as_float(v[hb][ch][4 * k + 2 * rh2]);
+                const float x1 = __uint_as_float(v[hb][ch][4 * k + 2 * rh2 + 1]);
+                if constexpr (BWD) {
+                  // parity acc, half hh (0 value, 1 derivative): item acc + 2 hh
+                  if (rh < H) {
+                    float* dst =
+                        reinterpret_cast<float*>(out) + ((size_t)(4 * f + acc + 2 * hh) * H + rh) * ncol + col;
+                    if (full) {
+                      *reinterpret_cast<float2*>(dst) = make_float2(x0, x1);
+                    } else {
+                      if (col < ncol) dst[0] = x0;
+                      if (col + 1 < ncol) dst[1] = x1;
+                    }
                   }
-                }
-              } else {
-                // half hh is the output parity: row 2 rh + hh
-                if (rh < (hh ? Ko : Ke)) {
-                  double* dst = reinterpret_cast<double*>(out) + ((size_t)f * N + 2 * rh + hh) * ncol + col;
-                  if (full) {
-                    *reinterpret_cast<double2*>(dst) = make_double2((double)x0, (double)x1);
-                  } else {
-                    if (col < ncol) dst[0] = (double)x0;
-                    if (col + 1 < ncol) dst[1] = (double)x1;
+                } else {
+                  // half hh is the output parity: row 2 rh + hh
+                  if (rh < (hh ? Ko : Ke)) {
+                    double* dst = reinterpret_cast<double*>(out) + ((size_t)f * N + 2 * rh + hh) * ncol + col;
+                    if (full) {
+                      *reinterpret_cast<double2*>(dst) = make_double2((double)x0, (double)x1);
+                    } else {
+                      if (col < ncol) dst[0] = (double)x0;
+                      if (col + 1 < ncol) dst[1] = (double)x1;
+                    }
                   }
                 }
               }
-            }
           }
+      }
     }
   }
   __syncthreads();
@@ -678,11 +733,10 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
     // bounded time to land (they write this CTA's shared and tensor memory)
     if (warp == kSProd && lane == 0) {
       atomicExch(&g_tc_timeout, 1);
-      if (a_pending) mbar_wait_bounded(barA, 0);
-      for (int s = 0; s < 2; ++s)
-        if (last_load[s] >= 0) mbar_wait_bounded(bar(FULL, s), ph(last_load[s]));
+      for (int r = 0; r < kSNR; ++r)
+        if (last_load[r] >= 0) mbar_wait_bounded(barFull(r), ph(last_load[r], kSNR));
     }
-    if (warp == kSMma && lane == 0 && last_mma >= 0) mbar_wait_bounded(bar(ACCFULL, last_mma & 1), ph(last_mma));
+    if (warp == kSMma && lane == 0 && last_mma >= 0) mbar_wait_bounded(barAccFull(last_mma & 1), ph(last_mma, 2));
   }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
