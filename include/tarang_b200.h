@@ -201,7 +201,10 @@ tb_status tb_checkpoint_load(tb_plan* plan, const double* grid, int where, const
  * next step rebuilds them.  tb_plan_tune times trial_steps steps of every
  * feasible combination from the current state (the state is restored after
  * each trial and at the end) and keeps the fastest; *tau_parts / *xrows get
- * the choice. */
+ * the choice.  It then times at least 10 steps with and without the step's
+ * independent kernels (M X, L X, the SBDF history copies) overlapped on a
+ * second stream beside the right-hand side and keeps the faster; untuned
+ * plans run them in line. */
 tb_status tb_plan_set_variant(tb_plan* plan, int tau_parts, int xrows);
 tb_status tb_plan_get_variant(const tb_plan* plan, int* tau_parts, int* xrows);
 tb_status tb_plan_tune(tb_plan* plan, double dt, int trial_steps, int* tau_parts, int* xrows);

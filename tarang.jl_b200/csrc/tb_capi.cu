@@ -492,6 +492,26 @@ void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
   timed(P, "z_forward_gemm", [&] { launch_gemm_f64(bf, nb, ncol, ncol, ncol, N, P->st); });
 }
 
+// The side stream: side(P) is the stream for work forked off the step's main
+// chain when the plan overlaps (the plan's own stream otherwise, and when
+// profiling, so that every kernel's events bracket it alone); fork_side
+// orders it after everything enqueued so far, join_side makes the main stream
+// wait for it.  Whether overlapping pays depends on the size: the small
+// latency-bound steps gain, the large ones lose a little to the concurrent
+// kernel, so tb_plan_tune decides.
+bool use_side(const tb_plan* P) { return P->overlap && !P->profiling; }
+cudaStream_t side(const tb_plan* P) { return use_side(P) ? P->st2 : P->st; }
+void fork_side(tb_plan* P) {
+  if (!use_side(P)) return;
+  TB_CUDA_TRY(cudaEventRecord(P->ev_fork, P->st));
+  TB_CUDA_TRY(cudaStreamWaitEvent(P->st2, P->ev_fork, 0));
+}
+void join_side(tb_plan* P) {
+  if (!use_side(P)) return;
+  TB_CUDA_TRY(cudaEventRecord(P->ev_join, P->st2));
+  TB_CUDA_TRY(cudaStreamWaitEvent(P->st, P->ev_join, 0));
+}
+
 void enqueue_rk_step(tb_plan* P, double dt) {
   const Tableau T = tableau(P->d.timestepper);
   const double gamma = T.AI[1][1];
@@ -501,8 +521,10 @@ void enqueue_rk_step(tb_plan* P, double dt) {
   const long long cnt = (long long)P->nplanes * (long long)P->plane;
   double2* X = P->X.as<double2>();
   const bool d3 = P->ndim == 3;
+  // M X_0 on the side stream, beside the first right-hand side
+  fork_side(P);
   timed(P, "mass_apply", [&] {
-    launch_mass_apply(X, P->MX0.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 0, P->nf, P->st, P->Nkm);
+    launch_mass_apply(X, P->MX0.as<double2>(), P->s3.as<double>(), P->Nz, P->Nk, P->Nx, 0, P->nf, side(P), P->Nkm);
   });
   int nk = 1;
   for (int i = 0; i < T.s; ++i) {
@@ -535,14 +557,16 @@ void enqueue_rk_step(tb_plan* P, double dt) {
         timed(P, "tau_solve_perp", [&] { launch_tau_solve(a2, P->sys[1].tau_parts, P->st); });
         ++nk;
       }
+      // L X_i = (rhs - M X_i) / beta on the side stream, beside F(X_i)
+      fork_side(P);
       timed(P, "lx_finalize", [&] {
         launch_lx_finalize(P->LXP[i].as<double2>(), X, P->s3.as<double>(), P->Nz, P->Nk, d3 ? 0 : P->Nx, P->k0, P->s,
-                           P->d.kappa, P->d.nu, beta, P->nf, P->st, P->Nkm, P->kappa_m.as<double>(),
+                           P->d.kappa, P->d.nu, beta, P->nf, side(P), P->Nkm, P->kappa_m.as<double>(),
                            P->nu_m.as<double>());
       });
       nk += 3;
       if (d3) {
-        rbc3d_lx_project(P, P->LXP[i].as<double2>(), beta);
+        rbc3d_lx_project(P, P->LXP[i].as<double2>(), beta, side(P));
         ++nk;
       }
     }
@@ -553,6 +577,7 @@ void enqueue_rk_step(tb_plan* P, double dt) {
       enqueue_rhs(P, X, P->FP[i].as<double2>() + P->plane, true);
       nk += P->mixed ? 4 : 3;
     }
+    join_side(P);  // M X_0 or L X_i is in place before the next combination
   }
   LinComb lc{};
   lc.in[lc.n] = P->MX0.as<double2>();
@@ -611,19 +636,22 @@ void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
   double2* MXcur = P->MX0.as<double2>();
   const bool d3 = P->ndim == 3;
   int extra = 0;
+  // M X of the projected fields (2D drops Im at the DC / Nyquist modes; 3D
+  // subtracts M delta on the kx = 0 / Nyquist planes) on the side stream,
+  // beside the right-hand side
+  fork_side(P);
+  timed(P, "mass_apply", [&] {
+    launch_mass_apply(X, MXcur, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, d3 ? 0 : 1, P->nf, side(P), P->Nkm);
+  });
+  if (d3) {
+    rbc3d_mx_project(P, MXcur, side(P));
+    ++extra;
+  }
   if (d3)
     rbc3d_enqueue_rhs(P, X, Fcur + P->plane);
   else
     enqueue_rhs(P, X, Fcur + P->plane, true);
-  // M X of the projected fields: 2D drops Im at the DC / Nyquist modes; 3D
-  // subtracts M delta on the kx = 0 / Nyquist planes
-  timed(P, "mass_apply", [&] {
-    launch_mass_apply(X, MXcur, P->s3.as<double>(), P->Nz, P->Nk, P->Nx, d3 ? 0 : 1, P->nf, P->st, P->Nkm);
-  });
-  if (d3) {
-    rbc3d_mx_project(P, MXcur);
-    ++extra;
-  }
+  join_side(P);
   LinComb lc{};
   lc.in[lc.n] = Fcur;
   lc.w[lc.n++] = c1;
@@ -636,6 +664,11 @@ void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
     lc.w[lc.n++] = -a2;
   }
   timed(P, "stage_lincomb", [&] { launch_lincomb(lc, P->Rsb.as<double2>(), cnt, P->st); });
+  // the history for the next step (read by the combination above) is copied
+  // on the side stream while the tau systems are solved
+  fork_side(P);
+  TB_CUDA_TRY(cudaMemcpyAsync(P->Fprev.p, Fcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, side(P)));
+  TB_CUDA_TRY(cudaMemcpyAsync(P->MXprev.p, MXcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, side(P)));
   TauArgs a = tau_args(P, 0, fs, P->Rsb.as<double2>());
   if (P->bc_dynamic) {  // wall values at t_{n+1}
     a.bcdyn = P->bcdyn.as<double2>();
@@ -648,8 +681,7 @@ void enqueue_sbdf_step(tb_plan* P, double dt, int order) {
     timed(P, "tau_solve_perp", [&] { launch_tau_solve(a2, P->sys[1].tau_parts, P->st); });
     ++extra;
   }
-  TB_CUDA_TRY(cudaMemcpyAsync(P->Fprev.p, Fcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
-  TB_CUDA_TRY(cudaMemcpyAsync(P->MXprev.p, MXcur, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, P->st));
+  join_side(P);
   P->kernels_per_step = (d3 ? (P->mixed ? 6 : 5) : (P->mixed ? 4 : 3)) + 1 + 1 + 1 + extra;
   if (P->bc_dynamic) {
     launch_advance_time(P->t_dev.as<double>(), dt, P->st);
@@ -1162,6 +1194,9 @@ void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, i
       TB_REQUIRE(xprod_smem_bytes(P->M, P->Nk, (int)pass_twiddles(P->fpM).size()) <= 227 * 1024, TB_ENOTSUPPORTED,
                  "Nx too large for the fused x kernel");
     TB_CUDA_TRY(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking));
+    TB_CUDA_TRY(cudaStreamCreateWithFlags(&P->st2, cudaStreamNonBlocking));
+    TB_CUDA_TRY(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
+    TB_CUDA_TRY(cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming));
     TB_CUDA_TRY(cudaEventCreate(&P->ev0));
     TB_CUDA_TRY(cudaEventCreate(&P->ev1));
     TB_CUDA_TRY(set_transform_smem_limits(227 * 1024));
@@ -1623,6 +1658,33 @@ tb_status tb_plan_tune(tb_plan* P, double dt, int trial_steps, int* tau_parts, i
         }
       }
     plan_set_variant(P, bp, br);
+    // then the side stream on or off, on a longer trial (the difference is a
+    // few percent)
+    const int ov_steps = std::max(trial_steps, 10);
+    float ov_ms[2] = {1e30f, 1e30f};  // best of two alternating trials each
+    for (int t = 0; t < 4; ++t) {
+      const int ov = t & 1;
+      if (P->overlap != (ov == 1)) {
+        P->overlap = ov == 1;
+        drop_step_graphs(P);
+      }
+      plan_launch_steps(P, dt, 2, P->st, 1);
+      TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+      plan_restore(P, snap);
+      TB_CUDA_TRY(cudaEventRecord(P->ev0, P->st));
+      plan_launch_steps(P, dt, ov_steps, P->st, 1);
+      TB_CUDA_TRY(cudaEventRecord(P->ev1, P->st));
+      TB_CUDA_TRY(cudaEventSynchronize(P->ev1));
+      float ms = 0.f;
+      TB_CUDA_TRY(cudaEventElapsedTime(&ms, P->ev0, P->ev1));
+      ov_ms[ov] = std::min(ov_ms[ov], ms);
+      plan_restore(P, snap);
+    }
+    const bool ov_best = ov_ms[1] < ov_ms[0];
+    if (P->overlap != ov_best) {
+      P->overlap = ov_best;
+      drop_step_graphs(P);
+    }
     plan_restore(P, snap);
     if (tau_parts) *tau_parts = bp;
     if (xrows) *xrows = br;

@@ -208,6 +208,12 @@ struct tb_plan {
   // caller's host buffer on a side stream while the plan steps on
   DevBuf stage_grid;
   cudaStream_t io_st = nullptr;
+  // side stream of the step: work independent of the RHS chain (L X
+  // finalisation, M X, the SBDF history copies) forks onto it and joins back
+  // before its results are used, inside the captured step graphs
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool overlap = false;  // use the side stream (chosen by tb_plan_tune; a change drops the step graphs)
   cudaEvent_t io_ready = nullptr, io_done = nullptr;
   // stepping state
   double last_dt = 0.0;
@@ -249,6 +255,12 @@ struct tb_plan {
     }
     if (gexec) cudaGraphExecDestroy(gexec);
     if (multi.exec) cudaGraphExecDestroy(multi.exec);
+    if (st2) {
+      cudaStreamSynchronize(st2);
+      cudaStreamDestroy(st2);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     if (io_st) {
       cudaStreamSynchronize(io_st);
       cudaStreamDestroy(io_st);
@@ -329,8 +341,8 @@ bool rbc3d_xrows_ok(const tb_plan* P, int rows);
 // drops the plan's factors and step graphs (rebuilt on the next step).
 bool plan_tau_parts_ok(const tb_plan* P, int parts);
 void plan_set_variant(tb_plan* P, int tau_parts, int xrows);
-void rbc3d_lx_project(tb_plan* P, double2* LX, double beta);
-void rbc3d_mx_project(tb_plan* P, double2* MX);
+void rbc3d_lx_project(tb_plan* P, double2* LX, double beta, cudaStream_t st = nullptr);  // null: the plan's stream
+void rbc3d_mx_project(tb_plan* P, double2* MX, cudaStream_t st = nullptr);
 size_t rbc3d_device_bytes(const tb_plan* P);
 // 3D transforms between grid (Nz, Ny, Nx) real and coefficients (Nz, Ny, Nx/2+1)
 // complex (kx fastest), device pointers, one field.

@@ -804,18 +804,18 @@ void rbc3d_enqueue_rhs(tb_plan* P, const double2* Xin, double2* out4) {
     enqueue_rhs_t<double2>(P, Xin, out4);
 }
 
-void rbc3d_lx_project(tb_plan* P, double2* LX, double beta) {
+void rbc3d_lx_project(tb_plan* P, double2* LX, double beta, cudaStream_t st) {
   const R3Args a = args_of(P);
   timed(P, "lx_project", [&] {
-    k3_lx_project<false><<<dim3((2 * P->Ny + 127) / 128, P->Nz), 128, 0, P->st>>>(
+    k3_lx_project<false><<<dim3((2 * P->Ny + 127) / 128, P->Nz), 128, 0, st ? st : P->st>>>(
         a, LX, P->X.as<double2>(), P->s3.as<double>(), P->s, P->d.kappa, P->d.nu, beta);
   });
 }
 
-void rbc3d_mx_project(tb_plan* P, double2* MX) {
+void rbc3d_mx_project(tb_plan* P, double2* MX, cudaStream_t st) {
   const R3Args a = args_of(P);
   timed(P, "mx_project", [&] {
-    k3_lx_project<true><<<dim3((2 * P->Ny + 127) / 128, P->Nz), 128, 0, P->st>>>(
+    k3_lx_project<true><<<dim3((2 * P->Ny + 127) / 128, P->Nz), 128, 0, st ? st : P->st>>>(
         a, MX, P->X.as<double2>(), P->s3.as<double>(), P->s, P->d.kappa, P->d.nu, 1.0);
   });
 }
