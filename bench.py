@@ -484,10 +484,14 @@ def run_ours(args, cfg, scheme, dist):
         step_roof["measured_frac"] = meas / step_s / (step_roof["peak_gbs"] * 1e9)
         step_roof["measured_source"] = tpath.replace(ROOT + os.sep, "")
 
-    # end to end through the C ABI with host buffers: per step, upload the state
-    # from pinned host memory, one step, download the state
-    # one pinned host buffer holding b, u_x, u_z, p and the taus back to back
-    # (the device order), so each direction is one copy
+    # end to end through the C ABI with host buffers: per step, upload the
+    # step's inputs from pinned host memory, one step, download the whole
+    # state.  One pinned host buffer holds b, u_x, u_z, p and the taus back to
+    # back (the device order), so each direction is one copy.  The inputs are
+    # the prognostic fields b, u_x, u_z: p and the taus are outputs of the
+    # step's tau solves (the IMEX tableaus never apply L to the step's initial
+    # state, and M has no p or tau columns; tests/test_gpu_state_io.py checks
+    # that they do not change the step), so only the first three planes go up.
     nk = cfg.Nx // 2 + 1
     pinned = torch.empty((4 * cfg.Nz + 7) * nk, dtype=torch.complex128, pin_memory=True).numpy()
     host = {f: pinned[f * cfg.Nz * nk:(f + 1) * cfg.Nz * nk].reshape(cfg.Nz, nk)
@@ -498,16 +502,18 @@ def run_ours(args, cfg, scheme, dist):
     ne = args.e2e_steps
     dist.barrier()
     t0 = time.perf_counter()
+    inputs = {f: host[f] for f in (TB_FIELD_B, TB_FIELD_UX, TB_FIELD_UZ)}
     for _ in range(ne):
-        plan.set_states(host)
+        plan.set_states(inputs, keep_history=True)
         plan.step(cfg.dt, 1)
         plan.get_states(host)
     e2e_el = dist.max(time.perf_counter() - t0)
     sbytes = W.state_bytes(cfg)
-    e2e = {"value": dist.world * ne / e2e_el, "unit": "steps/s", "h2d_bytes_per_step": sbytes,
+    ibytes = 16 * 3 * cfg.Nz * nk
+    e2e = {"value": dist.world * ne / e2e_el, "unit": "steps/s", "h2d_bytes_per_step": ibytes,
            "d2h_bytes_per_step": sbytes, "steps": ne,
-           "what": "per step: tb_set_states of b,ux,uz,p,taus from one pinned host buffer, tb_step(1), "
-                   "tb_get_states of all fields back into it (one copy and one wait per call)"}
+           "what": "per step: tb_set_states of the step's inputs b,ux,uz from one pinned host buffer, tb_step(1), "
+                   "tb_get_states of all fields (b,ux,uz,p,taus) back into it (one copy and one wait per call)"}
 
     finite = all(np.isfinite(plan.get_state(f)).all() for f in (TB_FIELD_B, TB_FIELD_UZ))
     cpu = None

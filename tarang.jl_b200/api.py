@@ -286,10 +286,12 @@ class Plan:
         pa = (c_void_p * len(fields))(*[a.ctypes.data for a in arrs])
         return fields, arrs, fa, pa
 
-    def set_states(self, arrays: Dict[int, np.ndarray]) -> None:
-        """Several fields from host arrays in one call (one wait for all copies)."""
+    def set_states(self, arrays: Dict[int, np.ndarray], keep_history: bool = False) -> None:
+        """Several fields from host arrays in one call (one wait for all copies).
+        A set restarts the multistep (SBDF) history unless keep_history."""
         fields, arrs, fa, pa = self._field_arrays(arrays, False)
-        check(lib.tb_set_states(self.ptr, len(fields), fa, pa, L.TB_HOST), self.ctx)
+        where = L.TB_HOST | (L.TB_KEEP_HISTORY if keep_history else 0)
+        check(lib.tb_set_states(self.ptr, len(fields), fa, pa, where), self.ctx)
 
     def get_states(self, out: Dict[int, np.ndarray]) -> Dict[int, np.ndarray]:
         """Fill out[field] (C-contiguous complex128 of the field's shape, e.g.

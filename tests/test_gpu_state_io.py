@@ -80,3 +80,28 @@ def test_states_through_one_contiguous_buffer(tb):
     a.get_states(views)
     for f in FIELDS:
         assert np.array_equal(views[f], b.get_state(f))
+
+
+@pytest.mark.parametrize("scheme", [0, 1])  # RK222, RK443
+def test_rk_step_does_not_read_p_or_taus(tb, scheme):
+    # the IMEX RK tableaus never apply L to the step's initial state (their
+    # first implicit column and bI[0] are zero) and M has no p or tau columns,
+    # so a step's p and taus are outputs only: the end-to-end bench uploads
+    # b, u_x, u_z alone
+    p = RBCParams(Nx=64, Nz=32, Lx=4.0, Lz=1.0, Ra=1e7)
+    plans = []
+    for seed in (None, 5):
+        dom = tb.ChannelDomain(p.Nx, p.Nz, Lx=4.0, Lz=1.0)
+        pl = tb.Plan(dom, p.kappa, p.nu, 1.0, 0.0, scheme)
+        pl.set_state(0, forward_2d(rbc_initial_b(p, 42)))
+        pl.step(0.01, 2)
+        if seed is not None:
+            rng = np.random.default_rng(seed)
+            for f in (3, 4):
+                shape = pl._field_shape(f)
+                pl.set_state(f, rng.standard_normal(shape) + 1j * rng.standard_normal(shape))
+        plans.append(pl)
+    for pl in plans:
+        pl.step(0.01, 2)
+    for f in FIELDS:
+        assert np.array_equal(plans[0].get_state(f), plans[1].get_state(f)), f
