@@ -383,8 +383,16 @@ void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2row
   }
   float* bsc = P->tcBimg.as<float>();
   const size_t bscn = P->tcBimg.bytes / sizeof(float);
-  timed(P, "z_backward_gemm",
-        [&] { launch_gemm_f32_path(bt, nb, ncol, ncol, ncol, N, false, P->st, P->tc32, bsc, bscn); });
+  // tensor cores: the plane form where its A operands exist (the C^(2) rows
+  // of the step; the plain forward rows keep the image form)
+  const bool plane = P->tc32 && P->tc2img.p != nullptr;
+  if (plane)
+    timed(P, "z_backward_gemm", [&] {
+      launch_tc32p(true, reinterpret_cast<const float*>(X32), P->tc2img.as<float>(), G, 3, N, ncol, P->st);
+    });
+  else
+    timed(P, "z_backward_gemm",
+          [&] { launch_gemm_f32_path(bt, nb, ncol, ncol, ncol, N, false, P->st, P->tc32, bsc, bscn); });
   XProdArgs32 xa{};
   for (int f = 0; f < 3; ++f) {
     xa.ev[f] = gp(f, 0);
@@ -427,8 +435,14 @@ void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2row
       bf.item[nb++].Aimg = tc32_image(P, c2rows ? 7 : 5);
     }
   }
-  timed(P, "z_forward_gemm",
-        [&] { launch_gemm_f32_path(bf, nb, ncol, ncol, ncol, N, true, P->st, P->tc32, bsc, bscn); });
+  if (plane && c2rows && P->tc2fwd)
+    timed(P, "z_forward_gemm", [&] {
+      launch_tc32p(false, reinterpret_cast<const float*>(P->H32.as<float2>()), P->tc2img.as<float>(), out3, 3, N,
+                   ncol, P->st);
+    });
+  else
+    timed(P, "z_forward_gemm",
+          [&] { launch_gemm_f32_path(bf, nb, ncol, ncol, ncol, N, true, P->st, P->tc32, bsc, bscn); });
 }
 
 void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
@@ -909,7 +923,7 @@ size_t tb::plan_device_bytes(const tb_plan* P) {
   for (const DevBuf& d : P->sys[0].mband) b += d.bytes;
   for (const DevBuf& d : P->sys[0].mbord) b += d.bytes;
   const DevBuf* m32[] = {&P->X32,  &P->G32,  &P->H32,  &P->bEv32, &P->bOv32,  &P->bEd32, &P->bOd32,
-                         &P->fE32, &P->fO32, &P->sfE32, &P->sfO32, &P->ptwM32, &P->tcAimg, &P->tcBimg};
+                         &P->fE32, &P->fO32, &P->sfE32, &P->sfO32, &P->ptwM32, &P->tcAimg, &P->tcBimg, &P->tc2img};
   for (const DevBuf* d : m32) b += d->bytes;
   return b;
 }
@@ -1287,6 +1301,15 @@ void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, i
         TB_CUDA_TRY(cudaGetLastError());
         TB_CUDA_TRY(cudaStreamSynchronize(P->st));
         P->tcBimg.alloc(tc32_b_scratch_floats(2 * P->Nk, 6) * sizeof(float));
+      }
+      // the plane form (A in tensor memory, tiles read from the planes)
+      if (P->ndim == 2 && tc32p_supported(N, 2 * P->Nk)) {
+        P->tc2img.alloc(tc32p_image_floats() * sizeof(float));
+        make_tc32p_images(P->bEv32.as<float>(), P->bOv32.as<float>(), P->bEd32.as<float>(), P->bOd32.as<float>(),
+                          pad16(P->Ke), pad16(P->Ko), P->sfE32.as<float>(), P->sfO32.as<float>(), pad16(P->Hz), N,
+                          P->tc2img.as<float>(), P->st);
+        TB_CUDA_TRY(cudaGetLastError());
+        TB_CUDA_TRY(cudaStreamSynchronize(P->st));
       }
       TB_CUDA_TRY(set_mixed_smem_limits(227 * 1024));
     }

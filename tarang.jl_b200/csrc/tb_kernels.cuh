@@ -69,6 +69,17 @@ void make_tc32s_images(const float* Ev, const float* Ov, const float* Ed, const 
 bool make_tc32s_tmap(TmaDesc* d, const float* planes, int nfields, int N, int ncol);  // false: unsupported
 void launch_tc32s(bool backward, const TmaDesc& d, const float* images, void* out, int nfields, int N, int ncol,
                   cudaStream_t st);
+// Plane form for the 2D z transforms (even N <= 256 rows, even ncol): the same
+// products with each CTA serving one A operand held in tensor memory (4
+// backward roles, 2 forward), the tiles read straight from the planes (whose
+// rows need not be 16-byte aligned).  Same outputs as launch_tc32s for
+// nfields fields; A parts from make_tc32p_images (tc32p_image_floats floats).
+bool tc32p_supported(int N, int ncol);
+size_t tc32p_image_floats();
+void make_tc32p_images(const float* Ev, const float* Ov, const float* Ed, const float* Od, int kpe, int kpo,
+                       const float* sfE, const float* sfO, int kph, int N, float* images, cudaStream_t st);
+void launch_tc32p(bool backward, const float* in, const float* images, void* out, int nfields, int N, int ncol,
+                  cudaStream_t st);
 int tc32_status();  // 1 once a tensor-core GEMM's bounded wait gave up, -1 if unreadable
 // tensor cores when asked for and the shapes fit, else SIMT
 inline void launch_gemm_f32_path(const GemmBatch32& bt, int nbatch, int ncol, int ldb, int ldc, int Nrows,

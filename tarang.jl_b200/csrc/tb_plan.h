@@ -236,6 +236,11 @@ struct tb_plan {
   // the tensor maps of the two input plane sets), when the shapes allow it
   bool tc3 = false;
   DevBuf tc3img;
+  // 2D: the plane form's A operands (empty when the shapes do not allow it);
+  // its forward transform is slower than the SIMT kernel at the measured
+  // sizes (one task per CTA), so only the backward one runs on it by default
+  DevBuf tc2img;
+  bool tc2fwd = false;
   tb::TmaDesc tc3Xc, tc3H3;
   // profiling: eager launches bracketed by events, accumulated per kernel name
   bool profiling = false;

@@ -743,6 +743,340 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
   if (warp == kSEpi) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kSTmemCols));
 }
 
+
+// ---- plane form (2D, N <= 256 rows, K <= 128 per operand) ----
+// The 2D planes have an odd number of complex columns (Nx/2 + 1 per row), so
+// their rows are 8-byte but not 16-byte aligned and no TMA tensor map can
+// describe them; the split warps read the tile straight from global memory
+// (8-byte loads, a warp covering 256 contiguous bytes of a row) and write the
+// hi / lo images.  Each CTA serves one A operand (an M-tile role) held in
+// tensor memory: backward, role q = p + 2 d is item w = q of a field (value
+// or z-derivative of parity p, K = Ke or Ko over the rows 2k + p); forward,
+// role par is the C^(2) rows 2r + par (K = N/2 over the mirror sums
+// B[k] +- B[N-1-k]).  CTAs of one role share its (field, 64-column tile)
+// tasks.
+constexpr int kPN = 64;                                  // columns per tile
+constexpr int kPK = 128;                                 // K extent of an operand
+constexpr uint32_t kPHilo = 2 * kPK * kPN * 4;           // 64 KB of hi and lo images
+constexpr int kPNH = 2;                                  // image stages
+constexpr uint32_t kPOffBar = kPNH * kPHilo;
+constexpr uint32_t kPSmem = kPOffBar + 256 + 1024;
+constexpr uint32_t kPAtom = kPN * 128;
+constexpr int kPThreads = 32 * 10;  // epilogue 0-3, split 4-7, MMA 8 (even K steps) and 9 (odd)
+constexpr size_t kPImageFloats = (size_t)6 * 2 * 128 * kPK;  // 4 backward roles, 2 forward; hi and lo
+constexpr uint32_t kPIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kPN >> 3) << 17) |
+                             ((uint32_t)(kTcM >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32_ts_n64(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(bdesc), "r"(kPIdesc), "r"(acc));
+}
+
+// A parts of the plane form, 128 x 128 each, hi then lo per role: roles 0-3
+// backward (Ev, Ov, Ed, Od: H x Kp row-major sources), 4-5 forward (sfE, sfO:
+// Ke / Ko x Hp sources).  Layout [k / 4][row][k % 4]: the CTA stages a part
+// in shared memory with bulk copies and thread `row` reads its 16-byte chunks
+// of consecutive rows without bank conflicts.
+__global__ void __launch_bounds__(kTcThreads) k_tc32p_image(const float* __restrict__ Ev, const float* __restrict__ Ov,
+                                                            const float* __restrict__ Ed, const float* __restrict__ Od,
+                                                            int kpe, int kpo, const float* __restrict__ sfE,
+                                                            const float* __restrict__ sfO, int kph, int N,
+                                                            float* __restrict__ images) {
+  const int H = N / 2, Ke = (N + 1) / 2, Ko = N / 2;
+  const int q = blockIdx.x;
+  float* hi = images + (size_t)q * 2 * 128 * kPK;
+  float* lo = hi + (size_t)128 * kPK;
+  for (int idx = threadIdx.x; idx < 128 * kPK; idx += kTcThreads) {
+    const int r = idx / kPK, k = idx % kPK;
+    float v = 0.f;
+    if (q < 4) {
+      const int p = q & 1, K = p ? Ko : Ke, kp = p ? kpo : kpe;
+      const float* src = q == 0 ? Ev : q == 1 ? Ov : q == 2 ? Ed : Od;
+      if (r < H && k < K) v = src[(size_t)r * kp + k];
+    } else {
+      const int par = q - 4, M = par ? Ko : Ke;
+      const float* src = par ? sfO : sfE;
+      if (r < M && k < H) v = src[(size_t)r * kph + k];
+    }
+    const uint32_t h = to_tf32(v);
+    const size_t o = ((size_t)(k / 4) * 128 + r) * 4 + (k % 4);
+    hi[o] = __uint_as_float(h);
+    lo[o] = __uint_as_float(to_tf32(v - __uint_as_float(h)));
+  }
+}
+
+// in: nfields planes of N rows x ncol floats; BWD out: C_w (H x ncol) of
+// field f at out + (4 f + w) H ncol; forward out: FP64 rows 2r + par at
+// out + f N ncol.
+template <bool BWD>
+__global__ void __launch_bounds__(kPThreads, 1) k_tc32p(const float* __restrict__ in, const float* __restrict__ images,
+                                                        void* out, int nfields, int N, int ncol) {
+  extern __shared__ uint8_t tc_smem_raw[];
+  const uint32_t raw = (uint32_t)__cvta_generic_to_shared(tc_smem_raw);
+  const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
+  uint8_t* sm = tc_smem_raw + pad;
+  const uint32_t sbase = raw + pad;
+  const uint32_t barL = sbase + kPOffBar;
+  auto barSplitFull = [&](int h) { return barL + 8u + 8u * (uint32_t)h; };
+  auto barHiloFree = [&](int h) { return barL + 8u + 8u * (uint32_t)(kPNH + h); };
+  auto barAccFull = [&](int a) { return barL + 8u + 8u * (uint32_t)(2 * kPNH + a); };
+  auto barAccFree = [&](int a) { return barL + 8u + 8u * (uint32_t)(2 * kPNH + 2 + a); };
+  const uint32_t barA = barL + 8u + 8u * (uint32_t)(2 * kPNH + 4);  // A staged in shared memory
+  constexpr uint32_t kBarBytes = 8u * (1 + 2 * kPNH + 4 + 1);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kPOffBar + kBarBytes);
+  volatile int* abort = reinterpret_cast<volatile int*>(sm + kPOffBar + kBarBytes + 8);
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int H = N / 2, Ke = (N + 1) / 2, Ko = N / 2;
+  constexpr int Q = BWD ? 4 : 2;  // roles
+  const int q = blockIdx.x % Q, rank = blockIdx.x / Q, nq = ((int)gridDim.x - q + Q - 1) / Q;
+  const int par = BWD ? (q & 1) : q;  // backward: parity of the rows read; forward: output parity
+  const int K = BWD ? (par ? Ko : Ke) : H;
+  const int nk8 = (K + 7) / 8;
+  const int M = BWD ? H : (par ? Ko : Ke);  // valid output rows
+  const int ntiles = (ncol + kPN - 1) / kPN;
+  const int ntask = nfields * ntiles;
+  const int n = rank < ntask ? (ntask - 1 - rank) / nq + 1 : 0;
+  auto task = [&](int i, int* f, int* n0) {
+    const int t = rank + i * nq;
+    *f = t / ntiles;
+    *n0 = (t % ntiles) * kPN;
+  };
+  auto ph = [](int i, int D) { return (uint32_t)(i / D) & 1u; };
+  auto ph_prev = [](int i, int D) { return (uint32_t)(i / D - 1) & 1u; };
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + kPOffBar +
+                                                                                            kBarBytes),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    *abort = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(barL));
+    // hilofree and accfull complete on the commits of both MMA issuers
+    for (int h = 0; h < kPNH; ++h) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(barSplitFull(h)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;\n" ::"r"(barHiloFree(h)));
+    }
+    for (int a = 0; a < 2; ++a) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;\n" ::"r"(barAccFull(a)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(barAccFree(a)));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barA));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    // this role's A parts (hi, lo: 128 KB) into the image stages, which the
+    // split fills only after they have gone on into tensor memory
+    static_assert(2 * 128 * kPK * 4 <= kPNH * kPHilo, "A staging fits the image stages");
+    mbar_expect_tx(barA, 2u * 128u * kPK * 4u);
+    bulk_copy(sbase, images + (size_t)((BWD ? 0 : 4) + q) * 2 * 128 * kPK, 2u * 128u * kPK * 4u, barA);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tmem_slot;  // A hi at 0, lo at 128; accumulator pairs at 256 + 128 a
+  int last_mma = -1;
+
+  if (warp >= 4 && warp < 8) {
+    // split: thread t loads rows 4 kc .. 4 kc + 3 of the operand (through the
+    // row map) at columns 2 nn2, 2 nn2 + 1 of the tile and writes two K-major
+    // chunks; the loads of all its items are issued before the first store
+    const int t = tid - 128;
+    bool need_a = true;  // the first stores wait until A has left the staging area
+    for (int i = 0; i < n && !*abort; ++i) {
+      const int hs = i % kPNH;
+      if (i >= kPNH && !mbar_wait_or_abort(barHiloFree(hs), ph_prev(i, kPNH), abort)) break;
+      int f, n0;
+      task(i, &f, &n0);
+      const float* src = in + (size_t)f * N * ncol;
+      uint8_t* hb = sm + (uint32_t)hs * kPHilo;
+      for (int it0 = t; it0 < (kPK / 4) * (kPN / 2); it0 += 8 * 128) {
+        float2 v[8][4];  // all eight items of the thread loaded before the first store
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int it = it0 + u * 128;
+          const int nn2 = it % (kPN / 2), kc = it / (kPN / 2);
+          const int col = n0 + 2 * nn2;
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int k = 4 * kc + e;
+            float2 x = make_float2(0.f, 0.f);
+            if (k < K && col < ncol) {
+              if constexpr (BWD) {
+                x = *reinterpret_cast<const float2*>(src + (size_t)(2 * k + par) * ncol + col);
+              } else {
+                const float2 a = *reinterpret_cast<const float2*>(src + (size_t)k * ncol + col);
+                const float2 b = *reinterpret_cast<const float2*>(src + (size_t)(N - 1 - k) * ncol + col);
+                x = par ? make_float2(a.x - b.x, a.y - b.y) : make_float2(a.x + b.x, a.y + b.y);
+              }
+            }
+            v[u][e] = x;
+          }
+        }
+        if (need_a) {
+          // (the loads above overlap the A staging)
+          if (!mbar_wait_or_abort(barL, 0, abort)) break;
+          need_a = false;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int it = it0 + u * 128;
+          const int nn2 = it % (kPN / 2), kc = it / (kPN / 2);
+          split_store4(hb, hb + kPHilo / 2, sw128_off(2 * nn2, 4 * kc, kPN),
+                       make_float4(v[u][0].x, v[u][1].x, v[u][2].x, v[u][3].x));
+          split_store4(hb, hb + kPHilo / 2, sw128_off(2 * nn2 + 1, 4 * kc, kPN),
+                       make_float4(v[u][0].y, v[u][1].y, v[u][2].y, v[u][3].y));
+        }
+      }
+      if (need_a) break;  // aborted while waiting for A
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      mbar_arrive(barSplitFull(hs));
+    }
+  } else if (warp == 8 || warp == 9) {
+    const int jpar = warp - 8;  // this issuer's K steps: j % 2 == jpar, into accumulator jpar
+    if (lane == 0) {
+      mbar_wait_or_abort(barL, 0, abort);  // A in tensor memory
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      for (int i = 0; i < n && !*abort; ++i) {
+        const int hs = i % kPNH, a = i & 1;
+        if (!mbar_wait_or_abort(barSplitFull(hs), ph(i, kPNH), abort)) break;
+        if (i >= 2 && !mbar_wait_or_abort(barAccFree(a), ph_prev(i, 2), abort)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        const uint32_t bb = sbase + (uint32_t)hs * kPHilo;
+        const uint64_t bhi = sw128_desc(bb), blo = sw128_desc(bb + kPHilo / 2);
+        // two accumulators, the even and the odd K steps, issued by the two
+        // issuers in parallel (the epilogue adds them)
+        const uint32_t d = tmem + 256u + (uint32_t)(a * 128 + jpar * 64);
+        for (int j = jpar; j < nk8; j += 2) {
+          const uint64_t kb = ((uint64_t)(j >> 2) * kPAtom + (uint64_t)(j & 3) * 32u) >> 4;
+          const uint32_t acc = j > 1 ? 1u : 0u;
+          mma_tf32_ts_n64(d, tmem + 8u * j, bhi + kb, acc);
+          mma_tf32_ts_n64(d, tmem + 8u * j, blo + kb, 1u);
+          mma_tf32_ts_n64(d, tmem + 128u + 8u * j, bhi + kb, 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                         barHiloFree(hs))
+                     : "memory");
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                         barAccFull(a))
+                     : "memory");
+        last_mma = i;
+      }
+    }
+  } else if (warp < 4) {
+    {
+      // this role's A (hi, lo) from its shared-memory staging into tensor
+      // memory: thread row r = 32 w + l, 16-byte chunk c of part h at
+      // [h][c][r] (consecutive rows in consecutive chunks)
+      const int r = warp * 32 + lane;
+      const bool staged = __all_sync(0xffffffffu, mbar_wait_or_abort(barA, 0, abort));
+      const float4* stA = reinterpret_cast<const float4*>(sm);
+#pragma unroll 1
+      for (int h = 0; h < 2 && staged; ++h)
+#pragma unroll 1
+        for (int c = 0; c < kPK / 32; ++c) {
+          uint32_t w[32];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const float4 x = stA[((size_t)h * (kPK / 4) + 8 * c + k) * 128 + r];
+            w[4 * k] = __float_as_uint(x.x);
+            w[4 * k + 1] = __float_as_uint(x.y);
+            w[4 * k + 2] = __float_as_uint(x.z);
+            w[4 * k + 3] = __float_as_uint(x.w);
+          }
+          const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * 128 + 32 * c);
+          asm volatile(
+              "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+              "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n" ::"r"(taddr),
+              "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]), "r"(w[8]),
+              "r"(w[9]), "r"(w[10]), "r"(w[11]), "r"(w[12]), "r"(w[13]), "r"(w[14]), "r"(w[15]), "r"(w[16]),
+              "r"(w[17]), "r"(w[18]), "r"(w[19]), "r"(w[20]), "r"(w[21]), "r"(w[22]), "r"(w[23]), "r"(w[24]),
+              "r"(w[25]), "r"(w[26]), "r"(w[27]), "r"(w[28]), "r"(w[29]), "r"(w[30]), "r"(w[31])
+              : "memory");
+        }
+      asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+      mbar_arrive(barL);
+    }
+    // epilogue: 16 x 256-bit accumulator loads (lane l: rows l / 4, l / 4 + 8
+    // of a 16-row block, columns 8 k + 2 (l % 4) + {0, 1})
+    for (int i = 0; i < n; ++i) {
+      const int a = i & 1;
+      if (!__all_sync(0xffffffffu, mbar_wait_or_abort(barAccFull(a), ph(i, 2), abort))) break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      int f, n0;
+      task(i, &f, &n0);
+      uint32_t v[2][2][16];  // [lane half][32-column half][registers]
+      float vs[2][2][16];    // the sum of the two K-step accumulators
+      const int nkh = nk8 > 1 ? 2 : 1;  // a single K step leaves the odd accumulator unused
+#pragma unroll 1
+      for (int kh = 0; kh < nkh; ++kh) {
+#pragma unroll
+        for (int hb = 0; hb < 2; ++hb)
+#pragma unroll
+          for (int ch = 0; ch < 2; ++ch) {
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32 + hb * 16) << 16) + 256u +
+                                   (uint32_t)(a * 128 + kh * 64 + ch * 32);
+            uint32_t* w = v[hb][ch];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];\n"
+                : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]),
+                  "=r"(w[8]), "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]),
+                  "=r"(w[15])
+                : "r"(taddr));
+          }
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+        for (int hb = 0; hb < 2; ++hb)
+#pragma unroll
+          for (int ch = 0; ch < 2; ++ch)
+#pragma unroll
+            for (int e = 0; e < 16; ++e)
+              vs[hb][ch][e] = kh ? vs[hb][ch][e] + __uint_as_float(v[hb][ch][e]) : __uint_as_float(v[hb][ch][e]);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+      mbar_arrive(barAccFree(a));
+#pragma unroll
+      for (int hb = 0; hb < 2; ++hb)
+#pragma unroll
+        for (int rh2 = 0; rh2 < 2; ++rh2) {
+          const int r = warp * 32 + hb * 16 + lane / 4 + 8 * rh2;  // output row of the role
+          if (r >= M) continue;
+#pragma unroll
+          for (int ch = 0; ch < 2; ++ch)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int col = n0 + 32 * ch + 8 * k + 2 * (lane % 4);
+              if (col >= ncol) continue;  // ncol is even: col + 1 < ncol too
+              const float x0 = vs[hb][ch][4 * k + 2 * rh2];
+              const float x1 = vs[hb][ch][4 * k + 2 * rh2 + 1];
+              if constexpr (BWD) {
+                float* dst = reinterpret_cast<float*>(out) + ((size_t)(4 * f + q) * H + r) * ncol + col;
+                *reinterpret_cast<float2*>(dst) = make_float2(x0, x1);
+              } else {
+                double* dst = reinterpret_cast<double*>(out) + ((size_t)f * N + 2 * r + par) * ncol + col;
+                *reinterpret_cast<double2*>(dst) = make_double2((double)x0, (double)x1);
+              }
+            }
+        }
+    }
+  }
+  __syncthreads();
+  if (*abort) {
+    if (tid == 0) {
+      atomicExch(&g_tc_timeout, 1);
+      mbar_wait_bounded(barA, 0);  // the A staging copy
+    }
+    if ((warp == 8 || warp == 9) && lane == 0 && last_mma >= 0)
+      mbar_wait_bounded(barAccFull(last_mma & 1), ph(last_mma, 2));
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512));
+}
+
 }  // namespace
 
 bool gemm_tc32_supported(const GemmBatch32& bt, int nbatch) {
@@ -769,7 +1103,11 @@ cudaError_t set_tc32_smem_limits() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_tc32s<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSSmem);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_tc32s<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSSmem);
+  e = cudaFuncSetAttribute(k_tc32s<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSSmem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_tc32p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_tc32p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPSmem);
 }
 
 bool launch_gemm_tc32(const GemmBatch32& bt_in, int nbatch, int ncol, int ldb, int ldc, int Nrows, bool out_f64,
@@ -863,6 +1201,29 @@ void launch_tc32s(bool backward, const TmaDesc& d, const float* images, void* ou
     k_tc32s<true><<<grid, kSThreads, kSSmem, st>>>(map, images, out, nfields, N, ncol);
   else
     k_tc32s<false><<<grid, kSThreads, kSSmem, st>>>(map, images, out, nfields, N, ncol);
+}
+
+bool tc32p_supported(int N, int ncol) { return N >= 2 && N <= 2 * kPK && N % 2 == 0 && ncol > 0 && ncol % 2 == 0; }
+
+size_t tc32p_image_floats() { return kPImageFloats; }
+
+void make_tc32p_images(const float* Ev, const float* Ov, const float* Ed, const float* Od, int kpe, int kpo,
+                       const float* sfE, const float* sfO, int kph, int N, float* images, cudaStream_t st) {
+  k_tc32p_image<<<6, kTcThreads, 0, st>>>(Ev, Ov, Ed, Od, kpe, kpo, sfE, sfO, kph, N, images);
+}
+
+void launch_tc32p(bool backward, const float* in, const float* images, void* out, int nfields, int N, int ncol,
+                  cudaStream_t st) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // every role gets at least one CTA and no CTA is left without a task
+  const int Q = backward ? 4 : 2;
+  const int ntask = nfields * ((ncol + kPN - 1) / kPN);
+  const int grid = sms < Q * ntask ? sms : Q * ntask;
+  if (backward)
+    k_tc32p<true><<<grid, kPThreads, kPSmem, st>>>(in, images, out, nfields, N, ncol);
+  else
+    k_tc32p<false><<<grid, kPThreads, kPSmem, st>>>(in, images, out, nfields, N, ncol);
 }
 
 int tc32_status() {
