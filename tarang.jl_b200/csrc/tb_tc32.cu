@@ -434,7 +434,7 @@ __device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* m
 constexpr int kSSplitWarps = 4;  // warps of the split role
 constexpr int kSSplitThreads = 32 * kSSplitWarps;
 constexpr int kSEpi = 0, kSSplit = 4, kSProd = kSSplit + kSSplitWarps, kSMma = kSProd + 1;  // first warp of each role
-constexpr int kSThreads = 32 * (kSMma + 1);
+constexpr int kSThreads = 32 * (kSMma + 2);  // two MMA issuer warps
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
@@ -507,12 +507,13 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barFull(r)));
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(barRawFree(r)), "r"(kSSplitThreads));
     }
+    // hilofree and accfull complete on the commits of both MMA issuers
     for (int h = 0; h < kSNH; ++h) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(barSplitFull(h)), "r"(kSSplitThreads));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barHiloFree(h)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;\n" ::"r"(barHiloFree(h)));
     }
     for (int a = 0; a < 2; ++a) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barAccFull(a)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;\n" ::"r"(barAccFull(a)));
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(barAccFree(a)));
     }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
@@ -568,7 +569,11 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
       mbar_arrive(barRawFree(r));
       mbar_arrive(barSplitFull(hs));
     }
-  } else if (warp == kSMma) {
+  } else if (warp == kSMma || warp == kSMma + 1) {
+    // two issuers: backward, one parity each; forward, the first issues every
+    // K step into one accumulator (splitting the steps over two accumulators
+    // measured slower) and the second only commits
+    const int jpar = warp - kSMma;
     if (lane == 0) {
       mbar_wait_or_abort(barL, 0, abort);  // A in tensor memory (sets the abort flag when it runs out)
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
@@ -579,8 +584,8 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
         const uint32_t bb = sbase + kSOffB + (uint32_t)hs * kSHiloBytes;
         if constexpr (BWD) {
-#pragma unroll
-          for (int p = 0; p < 2; ++p) {
+          {
+            const int p = jpar;
             const uint32_t ahi = tmem + (uint32_t)(64 * (2 * p)), alo = tmem + (uint32_t)(64 * (2 * p + 1));
             const uint64_t bhi = sw128_desc(bb + (uint32_t)p * 32768u), blo = sw128_desc(bb + (uint32_t)p * 32768u + 16384u);
             const uint32_t d = tmem + kSTmemAcc + (uint32_t)(a * 128 + p * 64);
@@ -598,7 +603,7 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
           const uint64_t bhi = sw128_desc(bb), blo = sw128_desc(bb + 32768u);
           const uint32_t d = tmem + kSTmemAcc + (uint32_t)(a * 128);
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
+          for (int j = 0; j < (jpar == 0 ? 16 : 0); ++j) {
             const uint64_t kb = ((uint64_t)(j >> 2) * kSAtom + (uint64_t)(j & 3) * 32u) >> 4;
             mma_tf32_ts(d, ahi + 8u * j, bhi + kb, j > 0 ? 1u : 0u);
             mma_tf32_ts(d, ahi + 8u * j, blo + kb, 1u);
@@ -664,22 +669,34 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
 #pragma unroll 1
       for (int acc = 0; acc < NACC; ++acc) {
         uint32_t v[2][2][16];  // [lane half][32-column half][registers]
+        {
+          constexpr int kh = 0;
+          uint32_t u[2][2][16];
 #pragma unroll
-        for (int hb = 0; hb < 2; ++hb)
+          for (int hb = 0; hb < 2; ++hb)
 #pragma unroll
-          for (int ch = 0; ch < 2; ++ch) {
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32 + hb * 16) << 16) + kSTmemAcc +
-                                   (uint32_t)(a * 128 + acc * 64 + ch * 32);
-            uint32_t* w = v[hb][ch];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                "[%16];\n"
-                : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]),
-                  "=r"(w[8]), "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]),
-                  "=r"(w[15])
-                : "r"(taddr));
-          }
-        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            for (int ch = 0; ch < 2; ++ch) {
+              const uint32_t taddr = tmem + ((uint32_t)(warp * 32 + hb * 16) << 16) + kSTmemAcc +
+                                     (uint32_t)(a * 128 + (acc + kh) * 64 + ch * 32);
+              uint32_t* w = u[hb][ch];
+              asm volatile(
+                  "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                  "[%16];\n"
+                  : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]),
+                    "=r"(w[8]), "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]),
+                    "=r"(w[15])
+                  : "r"(taddr));
+            }
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+          for (int hb = 0; hb < 2; ++hb)
+#pragma unroll
+            for (int ch = 0; ch < 2; ++ch)
+#pragma unroll
+              for (int e = 0; e < 16; ++e)
+                v[hb][ch][e] = kh ? __float_as_uint(__uint_as_float(v[hb][ch][e]) + __uint_as_float(u[hb][ch][e]))
+                                  : u[hb][ch][e];
+        }
         if (acc == NACC - 1) {
           // the accumulator buffer is read: the MMAs of tile i + 2 may overwrite it
           asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
@@ -736,7 +753,8 @@ __global__ void __launch_bounds__(kSThreads, 1) k_tc32s(const __grid_constant__ 
       for (int r = 0; r < kSNR; ++r)
         if (last_load[r] >= 0) mbar_wait_bounded(barFull(r), ph(last_load[r], kSNR));
     }
-    if (warp == kSMma && lane == 0 && last_mma >= 0) mbar_wait_bounded(barAccFull(last_mma & 1), ph(last_mma, 2));
+    if ((warp == kSMma || warp == kSMma + 1) && lane == 0 && last_mma >= 0)
+      mbar_wait_bounded(barAccFull(last_mma & 1), ph(last_mma, 2));
   }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
