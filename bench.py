@@ -63,8 +63,8 @@ def parse_args():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision summary in the rbc line")
     ap.add_argument("--no-rbc3d", action="store_true", help="skip the 3D (256x256x128) summary in the rbc line")
     ap.add_argument("--rbc3d-grid", default="256x256x128", help="Nx x Ny x Nz of the 3D workload")
-    ap.add_argument("--rbc3d-gemm", choices=["simt", "tensor"], default="tensor",
-                    help="3D z-transform GEMMs: SIMT FP32 or the streaming tcgen05 TF32x3 kernel")
+    ap.add_argument("--rbc3d-gemm", choices=["auto", "simt", "tensor"], default="auto",
+                    help="3D z-transform GEMMs: the tuner's choice, SIMT FP32 or the streaming tcgen05 TF32x3 kernel")
     ap.add_argument("--rbc3d-quick", action="store_true",
                     help="3D workload without the FP64 comparison and the end-to-end run (profiling)")
     ap.add_argument("--serve-requests", type=int, default=60)
@@ -420,6 +420,8 @@ def run_ours(args, cfg, scheme, dist):
         plan.set_variant(tau_parts=args.tau_parts, xrows=args.x_form)
     plan.step(cfg.dt, args.warmup)
     tuned = plan.variant() if (args.tau_parts or args.x_form) else plan.tune(cfg.dt, trial_steps=3)
+    if args.tensor_cores:
+        plan.set_gemm_path(True)  # (the tuner picks a path of its own)
     plan.step(cfg.dt, 1)
 
     # timed region: K graph replays, device time from CUDA events on the plan's stream
@@ -1063,13 +1065,14 @@ def run_rbc3d(args, dev, with_cpu=True):
     grid = W.rbc3_initial_grid(c)
     t0 = time.perf_counter()
     plan = tb.Plan3D(c.Nx, c.Ny, c.Nz, c.kappa, c.nu, 0, c.Lx, c.Ly, c.Lz, precision=TB_PREC_MIXED, device=dev)
-    plan.set_gemm_path(args.rbc3d_gemm == "tensor")
     b0 = plan.forward(grid)
     plan.set_state(TB_FIELD_B, b0)
     plan.step(c.dt, 1)  # factors both tau systems for this dt and captures the step graph
     setup_s = time.perf_counter() - t0
     t1 = time.perf_counter()
     tuned = plan.tune(c.dt, trial_steps=3)  # kernel shapes (tau partitions, x-pass rows), state kept
+    if args.rbc3d_gemm != "auto":
+        plan.set_gemm_path(args.rbc3d_gemm == "tensor")
     tune_s = time.perf_counter() - t1
     plan.step(c.dt, max(args.warmup, 3))
     torch.cuda.synchronize()
@@ -1152,7 +1155,8 @@ def run_rbc3d(args, dev, with_cpu=True):
                    "l2": "working set (~15 GB of factors and stage vectors) far exceeds the 126 MB L2"},
         "data": "synthetic: b0 = Lz - z + 1e-3 z (Lz - z) xi, xi ~ N(0,1) from PCG64(42), u = 0",
         "setup_s": setup_s,
-        "tuned": {"tau_solve_partitions": tuned[0], "xpass_rows_per_cta": tuned[1], "tune_s": tune_s},
+        "tuned": {"tau_solve_partitions": tuned[0], "xpass_rows_per_cta": tuned[1],
+                  "tensor_core_gemms": plan.gemm_path(), "tune_s": tune_s},
         "clocks": clk.summary(),
         "gpu_launches": kps * c.steps,
         "kernels_per_step": kps,

@@ -204,16 +204,19 @@ tb_status tb_checkpoint_load(tb_plan* plan, const double* grid, int where, const
  * the choice.  It then times at least 10 steps with and without the step's
  * independent kernels (M X, L X, the SBDF history copies) overlapped on a
  * second stream beside the right-hand side and keeps the faster; untuned
- * plans run them in line. */
+ * plans run them in line.  Mixed plans with a tensor-core form of their
+ * transform GEMMs (tb_plan_set_gemm_path) get the faster GEMM path the same
+ * way. */
 tb_status tb_plan_set_variant(tb_plan* plan, int tau_parts, int xrows);
 tb_status tb_plan_get_variant(const tb_plan* plan, int* tau_parts, int* xrows);
 tb_status tb_plan_tune(tb_plan* plan, double dt, int trial_steps, int* tau_parts, int* xrows);
 /* FP32 Chebyshev transform GEMMs of a mixed-precision plan: tensor_cores = 1
  * runs them on the tcgen05 tensor cores in TF32 with three products per term
  * (FP32 accuracy), 0 on the SIMT FP32 kernel.  2D: tensor cores wherever
- * Nz <= 256, SIMT by default.  3D: the streaming tensor-core kernel (TMA
- * tiles of the raw planes) wherever Nz <= 128, and there it is the default;
- * SIMT above.  No counterpart in the reference, whose GPU Chebyshev transforms
+ * Nz <= 256 (the backward transform of even Nz on the plane form, the rest on
+ * the operand-image form), SIMT by default.  3D: the streaming tensor-core
+ * kernel (TMA tiles of the raw planes) wherever Nz <= 128, and there it is
+ * the default; SIMT above.  tb_plan_tune picks the faster path.  No counterpart in the reference, whose GPU Chebyshev transforms
  * are cuFFT DCT-Is (ext/cuda/cheb_deriv.jl:503-596).  A change drops the
  * plan's step graphs. */
 tb_status tb_plan_set_gemm_path(tb_plan* plan, int tensor_cores);

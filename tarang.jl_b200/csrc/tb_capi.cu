@@ -1713,6 +1713,34 @@ tb_status tb_plan_tune(tb_plan* P, double dt, int trial_steps, int* tau_parts, i
       P->overlap = ov_best;
       drop_step_graphs(P);
     }
+    // mixed plans with a tensor-core form of their transforms: that form or
+    // the SIMT kernel, whichever is faster at this size
+    if (P->mixed && (P->tc2img.p != nullptr || P->tc3)) {
+      float tc_ms[2] = {1e30f, 1e30f};
+      for (int t = 0; t < 4; ++t) {
+        const int tc = t & 1;
+        if (P->tc32 != (tc == 1)) {
+          P->tc32 = tc == 1;
+          drop_step_graphs(P);
+        }
+        plan_launch_steps(P, dt, 2, P->st, 1);
+        TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+        plan_restore(P, snap);
+        TB_CUDA_TRY(cudaEventRecord(P->ev0, P->st));
+        plan_launch_steps(P, dt, ov_steps, P->st, 1);
+        TB_CUDA_TRY(cudaEventRecord(P->ev1, P->st));
+        TB_CUDA_TRY(cudaEventSynchronize(P->ev1));
+        float ms = 0.f;
+        TB_CUDA_TRY(cudaEventElapsedTime(&ms, P->ev0, P->ev1));
+        tc_ms[tc] = std::min(tc_ms[tc], ms);
+        plan_restore(P, snap);
+      }
+      const bool tc_best = tc_ms[1] < tc_ms[0];
+      if (P->tc32 != tc_best) {
+        P->tc32 = tc_best;
+        drop_step_graphs(P);
+      }
+    }
     plan_restore(P, snap);
     if (tau_parts) *tau_parts = bp;
     if (xrows) *xrows = br;
