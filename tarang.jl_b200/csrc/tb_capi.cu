@@ -1207,13 +1207,10 @@ void tb::build_plan(tb_plan* P, tb_context* ctx, const tb_problem_desc* descs, i
     if (desc->ndim == 2)
       TB_REQUIRE(xprod_smem_bytes(P->M, P->Nk, (int)pass_twiddles(P->fpM).size()) <= 227 * 1024, TB_ENOTSUPPORTED,
                  "Nx too large for the fused x kernel");
-    // the step's main chain on a high-priority stream, the work forked off it
-    // on a low-priority one, so that the forked kernels take the SMs the main
-    // chain leaves idle rather than competing with it
-    int prio_low = 0, prio_high = 0;
-    TB_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
-    TB_CUDA_TRY(cudaStreamCreateWithPriority(&P->st, cudaStreamNonBlocking, prio_high));
-    TB_CUDA_TRY(cudaStreamCreateWithPriority(&P->st2, cudaStreamNonBlocking, prio_low));
+    // the step's main chain on a work stream, the work forked off it on a
+    // side stream of least priority (create_work_stream)
+    TB_CUDA_TRY(create_work_stream(&P->st));
+    TB_CUDA_TRY(create_work_stream(&P->st2, true));
     TB_CUDA_TRY(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
     TB_CUDA_TRY(cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming));
     TB_CUDA_TRY(cudaEventCreate(&P->ev0));

@@ -65,7 +65,7 @@ constexpr int kMaxWorkerStreams = 32;
 void ensure_streams(tb_ensemble* E, int n) {
   while ((int)E->ws.size() < n) {
     cudaStream_t s;
-    TB_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    TB_CUDA_TRY(create_work_stream(&s));
     E->ws.push_back(s);
   }
 }

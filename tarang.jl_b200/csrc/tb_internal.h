@@ -22,6 +22,18 @@ struct tb_context {
 
 namespace tb {
 
+// Work streams of the library (plans, turbulence plans, ensemble workers) are
+// created at the device's greatest priority, all alike, so that the only
+// streams that yield are the plans' step side streams (least priority): the
+// forked kernels of a step fill the SMs its main chain leaves idle, while the
+// plans of an ensemble or a server compete on equal terms.
+inline cudaError_t create_work_stream(cudaStream_t* s, bool side = false) {
+  int least = 0, greatest = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (e != cudaSuccess) return e;
+  return cudaStreamCreateWithPriority(s, cudaStreamNonBlocking, side ? least : greatest);
+}
+
 // ---------------------------------------------------------------------------
 // Error plumbing: every failure becomes a tb_status plus a message stored in
 // the context; nothing escapes the C ABI as an exception.

@@ -64,7 +64,7 @@ tb_status tb_periodic_create(tb_context* ctx, int Nx, int Ny, tb_periodic** out)
                "Nx, Ny must be of the form 2^a 3^b");
     TB_CUDA_TRY(cudaSetDevice(ctx->device));
     TB_CUDA_TRY(set_transform_smem_limits(227 * 1024));
-    TB_CUDA_TRY(cudaStreamCreateWithFlags(&T->st, cudaStreamNonBlocking));
+    TB_CUDA_TRY(create_work_stream(&T->st));
     upload(T->twN, host_twiddles(Nx));
     upload(T->ptwNy, host_pass_twiddles(T->fpNy));
     T->grid.alloc((size_t)Ny * Nx * sizeof(double));

@@ -502,7 +502,7 @@ tb_turb* tb::turb_create(tb_context* ctx, const tb_problem_desc& d, const double
   TB_REQUIRE(make_fft_plan(T->Mx, &T->fpMx) && make_fft_plan(T->My, &T->fpMy), TB_ENOTSUPPORTED,
              "Nx, Ny must be of the form 2^a 3^b");
   TB_CUDA_TRY(cudaSetDevice(ctx->device));
-  TB_CUDA_TRY(cudaStreamCreateWithFlags(&T->st, cudaStreamNonBlocking));
+  TB_CUDA_TRY(create_work_stream(&T->st));
   const size_t spec = (size_t)T->Kx * T->Ny * sizeof(float2);
   for (auto& b : T->Q) b.alloc(spec);
   if (T->rk) {
