@@ -236,11 +236,10 @@ struct tb_plan {
   // the tensor maps of the two input plane sets), when the shapes allow it
   bool tc3 = false;
   DevBuf tc3img;
-  // 2D: the plane form's A operands (empty when the shapes do not allow it);
-  // its forward transform is slower than the SIMT kernel at the measured
-  // sizes (one task per CTA), so only the backward one runs on it by default
+  // 2D: the plane form's A operands (empty when the shapes do not allow it),
+  // and whether its forward transform runs on it too (the C^(2) rows)
   DevBuf tc2img;
-  bool tc2fwd = false;
+  bool tc2fwd = true;
   tb::TmaDesc tc3Xc, tc3H3;
   // profiling: eager launches bracketed by events, accumulated per kernel name
   bool profiling = false;

@@ -909,28 +909,37 @@ __global__ void __launch_bounds__(kPThreads, 1) k_tc32p(const float* __restrict_
       task(i, &f, &n0);
       const float* src = in + (size_t)f * N * ncol;
       uint8_t* hb = sm + (uint32_t)hs * kPHilo;
-      for (int it0 = t; it0 < (kPK / 4) * (kPN / 2); it0 += 8 * 128) {
-        float2 v[8][4];  // all eight items of the thread loaded before the first store
+      // items per load batch: all eight of the thread in the backward
+      // transform; four in the forward one, whose values take two loads each
+      // (the mirror rows), so that a batch's loads all stay in flight
+      constexpr int UB = BWD ? 8 : 4;
+      for (int it0 = t; it0 < (kPK / 4) * (kPN / 2); it0 += UB * 128) {
+        float2 v[UB][4], w[UB][4];  // w: the mirror rows of the forward transform
+        // every load of the batch first (no arithmetic between them, so that
+        // they are all in flight), then the mirror sums
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+        for (int u = 0; u < UB; ++u) {
           const int it = it0 + u * 128;
           const int nn2 = it % (kPN / 2), kc = it / (kPN / 2);
           const int col = n0 + 2 * nn2;
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const int k = 4 * kc + e;
-            float2 x = make_float2(0.f, 0.f);
-            if (k < K && col < ncol) {
-              if constexpr (BWD) {
-                x = *reinterpret_cast<const float2*>(src + (size_t)(2 * k + par) * ncol + col);
-              } else {
-                const float2 a = *reinterpret_cast<const float2*>(src + (size_t)k * ncol + col);
-                const float2 b = *reinterpret_cast<const float2*>(src + (size_t)(N - 1 - k) * ncol + col);
-                x = par ? make_float2(a.x - b.x, a.y - b.y) : make_float2(a.x + b.x, a.y + b.y);
-              }
-            }
-            v[u][e] = x;
+            const bool ok = k < K && col < ncol;
+            const int row = BWD ? 2 * k + par : k;
+            v[u][e] = ok ? *reinterpret_cast<const float2*>(src + (size_t)row * ncol + col) : make_float2(0.f, 0.f);
+            if constexpr (!BWD)
+              w[u][e] = ok ? *reinterpret_cast<const float2*>(src + (size_t)(N - 1 - k) * ncol + col)
+                           : make_float2(0.f, 0.f);
           }
+        }
+        if constexpr (!BWD) {
+#pragma unroll
+          for (int u = 0; u < UB; ++u)
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+              v[u][e] = par ? make_float2(v[u][e].x - w[u][e].x, v[u][e].y - w[u][e].y)
+                            : make_float2(v[u][e].x + w[u][e].x, v[u][e].y + w[u][e].y);
         }
         if (need_a) {
           // (the loads above overlap the A staging)
@@ -938,7 +947,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_tc32p(const float* __restrict_
           need_a = false;
         }
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+        for (int u = 0; u < UB; ++u) {
           const int it = it0 + u * 128;
           const int nn2 = it % (kPN / 2), kc = it / (kPN / 2);
           split_store4(hb, hb + kPHilo / 2, sw128_off(2 * nn2, 4 * kc, kPN),
