@@ -395,6 +395,33 @@ tb_status tb_ensemble_tune(tb_ensemble* E, const double* dt, int trial_steps, in
       for (auto& G : E->groups) plan_set_variant(G.plan.get(), bp, 0);
     E->streams = bs;
     E->graph_steps = bg;
+    // mixed members with a tensor-core form of their transform GEMMs: that
+    // form or the SIMT kernel, timed on the chosen configuration (best of two
+    // alternating trials each)
+    std::vector<tb_plan*> all(E->members.begin(), E->members.end());
+    if (bf)
+      for (auto& G : E->groups) all.push_back(G.plan.get());
+    bool any_tc = false;
+    for (auto* m : all) any_tc = any_tc || (m->mixed && (m->tc2img.p != nullptr || m->tc3));
+    if (any_tc) {
+      auto set_tc = [&](bool on) {
+        for (auto* m : all)
+          if (m->mixed && m->tc32 != on)
+            TB_REQUIRE(tb_plan_set_gemm_path(m, on ? 1 : 0) == TB_OK, TB_ECUDA, "setting a member's GEMM path");
+      };
+      float tt[2] = {1e30f, 1e30f};
+      for (int t = 0; t < 4; ++t) {
+        const int tc = t & 1;
+        set_tc(tc == 1);
+        run(E, dt, trial_steps, bs, bg, nullptr, nullptr);  // captures the graphs of this path
+        restore();
+        float tot = 0.f;
+        run(E, dt, trial_steps, bs, bg, nullptr, &tot);
+        restore();
+        tt[tc] = std::min(tt[tc], tot);
+      }
+      set_tc(tt[1] < tt[0]);
+    }
     if (streams) *streams = bs;
     if (graph_steps) *graph_steps = bg;
   });
