@@ -361,15 +361,24 @@ const float* tc32_image(const tb_plan* P, int m) {
   return P->tcAimg.as<float>() + (size_t)m * tc32_a_image_floats();
 }
 
+// Mixed 2D plans: the stage solves also write the FP32 copy of the b, u_x,
+// u_z planes that the next right-hand side reads (its rounding pass skipped).
+void set_x32(const tb_plan* P, TauArgs* a) {
+  if (P->mixed && P->ndim == 2) {
+    a->X32 = P->X32.as<float>();
+    a->x32_lim = 3LL * (long long)P->plane * 2;
+  }
+}
+
 // Mixed precision: the same RHS program on FP32 data; F is written in FP64.
-void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
+void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2rows, bool x32_fresh) {
   const int N = P->Nz, H = P->Hz;
   const int ncol = 2 * P->Nk;
   const size_t hplane = (size_t)H * P->Nk;
   float2* X32 = P->X32.as<float2>();
   float2* G = P->G32.as<float2>();
   auto gp = [&](int f, int w) { return G + (size_t)(4 * f + w) * hplane; };
-  timed(P, "round_f32", [&] { launch_round_f32(Xin, X32, 3LL * (long long)P->plane, P->st); });
+  if (!x32_fresh) timed(P, "round_f32", [&] { launch_round_f32(Xin, X32, 3LL * (long long)P->plane, P->st); });
   GemmBatch32 bt{};
   int nb = 0;
   for (int f = 0; f < 3; ++f) {
@@ -445,9 +454,11 @@ void enqueue_rhs_mixed(tb_plan* P, const double2* Xin, double2* out3, bool c2row
           [&] { launch_gemm_f32_path(bf, nb, ncol, ncol, ncol, N, true, P->st, P->tc32, bsc, bscn); });
 }
 
-void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows) {
+// x32_fresh: the FP32 copy of Xin's planes is current (written by the solve
+// that produced Xin), so the mixed program skips its rounding pass.
+void enqueue_rhs(tb_plan* P, const double2* Xin, double2* out3, bool c2rows, bool x32_fresh = false) {
   if (P->mixed) {
-    enqueue_rhs_mixed(P, Xin, out3, c2rows);
+    enqueue_rhs_mixed(P, Xin, out3, c2rows, x32_fresh);
     return;
   }
   const int N = P->Nz, H = P->Hz;
@@ -558,6 +569,7 @@ void enqueue_rk_step(tb_plan* P, double dt) {
       }
       timed(P, "stage_lincomb", [&] { launch_lincomb(lc, P->LXP[i].as<double2>(), cnt, P->st); });
       TauArgs a = tau_args(P, 0, fs, P->LXP[i].as<double2>());
+      set_x32(P, &a);
       if (P->bc_dynamic) {  // wall values at the stage time t_n + c_i dt
         double ci = 0.0;
         for (int j = 0; j < i; ++j) ci += T.AE[i][j];
@@ -588,8 +600,9 @@ void enqueue_rk_step(tb_plan* P, double dt) {
       rbc3d_enqueue_rhs(P, X, P->FP[i].as<double2>() + P->plane);
       nk += P->mixed ? 6 : 5;
     } else {
-      enqueue_rhs(P, X, P->FP[i].as<double2>() + P->plane, true);
-      nk += P->mixed ? 4 : 3;
+      // the stage solve (i > 0) has written the FP32 copy of X_i
+      enqueue_rhs(P, X, P->FP[i].as<double2>() + P->plane, true, i > 0);
+      nk += P->mixed && i == 0 ? 4 : 3;
     }
     join_side(P);  // M X_0 or L X_i is in place before the next combination
   }

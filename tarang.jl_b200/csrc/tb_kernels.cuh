@@ -259,6 +259,10 @@ struct TauArgs {
   // bits, 2 * (its element offset / Nk) + (1 if the unknown is i times the
   // solved column), -1 for none (the store code is 2 * offset + flag)
   const short* xcode;
+  // optional FP32 copy of the first x32_lim doubles of X (mixed 2D plans: the
+  // b, u_x, u_z planes), written beside X by the solve; null for none
+  float* X32;
+  long long x32_lim;
   // partition responses of the solve, written by the factorisation:
   // PP[group][partition][class][mode] = Phi (4x4), Psi (12x12), Gz (4x4);
   // HR[group][row][class][mode][kHRec] = H (12)

@@ -410,10 +410,17 @@ __host__ __device__ constexpr int h_stages() {
 // element offset from X addresses both; code = 2 * offset + (1 if the unknown is i
 // times the solved real-ified column), -1 for no store.  u_x = i v gives
 // re(u_x) = -v_im (part-1 lane) and im(u_x) = v_re (part-0 lane).
-__device__ __forceinline__ void store_unknown(double* Xd, int code, int m, int part, double x, bool on) {
+// With X32 non-null the value also goes, rounded, to the FP32 copy of the
+// first x32_lim doubles of X (the b, u_x, u_z planes the mixed RHS reads), so
+// that no rounding pass has to run before the stage's right-hand side.
+__device__ __forceinline__ void store_unknown(double* Xd, int code, int m, int part, double x, bool on,
+                                              float* X32 = nullptr, long long x32_lim = 0) {
   if (on && code >= 0) {
     const int rl = code & 1;
-    Xd[2 * ((size_t)(code >> 1) + m) + (part ^ rl)] = (rl & part) ? -x : x;
+    const size_t i = 2 * ((size_t)(code >> 1) + m) + (part ^ rl);
+    const double v = (rl & part) ? -x : x;
+    Xd[i] = v;
+    if (X32 != nullptr && (long long)i < x32_lim) X32[i] = (float)v;
   }
 }
 
@@ -787,7 +794,8 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
           const double xj = sacc * rec(0);
           xw[(kBwdWin - 1 - u) % kBwdWin] = xj;
           if (P == 1 || pid == P - 1)
-            store_unknown(Xd, __double2loint(rec(kBwdCode)), m, part, xj, live);  // final: no correction
+            store_unknown(Xd, __double2loint(rec(kBwdCode)), m, part, xj, live, a.X32,
+                          a.x32_lim);  // final: no correction
           else
             *yx = xj;
         }
@@ -934,7 +942,8 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
             acc1 = fma(hv[i / 2].y, T[i + 1], acc1);
           }
           const int xc = xcs[2 * j + c];  // 2 R + flag -> store code 2 R Nk + flag
-          store_unknown(Xd, xc < 0 ? -1 : 2 * (xc >> 1) * Nk + (xc & 1), m, part, acc0 + acc1, m < Nk);
+          store_unknown(Xd, xc < 0 ? -1 : 2 * (xc >> 1) * Nk + (xc & 1), m, part, acc0 + acc1, m < Nk, a.X32,
+                        a.x32_lim);
         }
       }
       __syncwarp();
@@ -946,7 +955,8 @@ __global__ void __launch_bounds__(32 * P / PPW) k_tau_solve(TauArgs a) {
   if (pid == 0) {
 #pragma unroll
     for (int b = 0; b < NBMAX; ++b) {
-      if (live && b < a.cls[c].nb) store_unknown(Xd, a.cls[c].left_code[b], m, part, x1[b], true);
+      if (live && b < a.cls[c].nb)
+        store_unknown(Xd, a.cls[c].left_code[b], m, part, x1[b], true, a.X32, a.x32_lim);
     }
   }
 }
