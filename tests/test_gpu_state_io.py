@@ -105,3 +105,25 @@ def test_rk_step_does_not_read_p_or_taus(tb, scheme):
         pl.step(0.01, 2)
     for f in FIELDS:
         assert np.array_equal(plans[0].get_state(f), plans[1].get_state(f)), f
+
+
+def test_async_step_then_states_read_back_like_the_synchronous_step(tb):
+    # tb_set_states, tb_step_async, tb_get_states per step (the end-to-end
+    # bench's loop): the read-back copy queues behind the step on the plan's
+    # stream, so it sees the finished step, bitwise as after tb_step
+    p = RBCParams(Nx=64, Nz=32, Lx=4.0, Lz=1.0, Ra=1e7)
+    a, b = _plan(tb, p), _plan(tb, p)
+    Nz, nk = p.Nz, p.Nx // 2 + 1
+    buf = np.empty((4 * Nz + 7) * nk, np.complex128)
+    views = {f: buf[f * Nz * nk:(f + 1) * Nz * nk].reshape(Nz, nk) for f in (0, 1, 2, 3)}
+    views[4] = buf[4 * Nz * nk:].reshape(7, nk)
+    a.get_states(views)
+    for _ in range(3):
+        step_in = {f: views[f].copy() for f in (0, 1, 2)}
+        a.set_states(step_in, keep_history=True)
+        a.step_async(0.01, 1)
+        a.get_states(views)
+        b.set_states(step_in, keep_history=True)
+        b.step(0.01, 1)
+        for f in FIELDS:
+            assert np.array_equal(views[f], b.get_state(f)), f
