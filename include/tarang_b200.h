@@ -49,6 +49,14 @@ enum { TB_HOST = 0, TB_DEVICE = 1 };
  * into a live state field (timestepper_data, src/core/timesteppers/state.jl:47-91),
  * and a plain write restarts the history at SBDF1. */
 enum { TB_KEEP_HISTORY = 0x10 };
+/* OR'ed into where of tb_set_states: return once the copies are queued on the
+ * plan's stream instead of waiting for them (cudaMemcpyAsync semantics).  A
+ * pinned host source must then stay unchanged until the plan's next wait
+ * (tb_step, tb_get_states, tb_plan_wait, tb_synchronize); a pageable source
+ * is consumed before the call returns (the runtime stages it).  The next
+ * step or read-back queues behind the copies.  tb_get_states refuses it
+ * (TB_EINVAL): its data is read by the caller after the return. */
+enum { TB_NO_WAIT = 0x20 };
 
 /* Time steppers (src/core/timesteppers/types.jl:49-167, 217). */
 enum { TB_RK222 = 0, TB_RK443 = 1, TB_SBDF1 = 2, TB_SBDF2 = 3 };

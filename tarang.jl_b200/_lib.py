@@ -18,6 +18,7 @@ LIB_PATH = os.environ.get("TARANG_B200_LIB") or os.path.join(HERE, "libtarang_b2
 TB_OK, TB_EINVAL, TB_ENOMEM, TB_ESINGULAR, TB_ETIMEOUT, TB_ECUDA, TB_ENOTSUPPORTED, TB_EBUDGET, TB_ESTATE = range(9)
 TB_HOST, TB_DEVICE = 0, 1
 TB_KEEP_HISTORY = 0x10
+TB_NO_WAIT = 0x20
 TB_RK222, TB_RK443, TB_SBDF1, TB_SBDF2 = 0, 1, 2, 3
 TB_PROGRAM_RBC = 0
 TB_PROGRAM_TURB2D = 1

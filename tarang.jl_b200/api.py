@@ -286,11 +286,14 @@ class Plan:
         pa = (c_void_p * len(fields))(*[a.ctypes.data for a in arrs])
         return fields, arrs, fa, pa
 
-    def set_states(self, arrays: Dict[int, np.ndarray], keep_history: bool = False) -> None:
+    def set_states(self, arrays: Dict[int, np.ndarray], keep_history: bool = False, wait: bool = True) -> None:
         """Several fields from host arrays in one call (one wait for all copies).
-        A set restarts the multistep (SBDF) history unless keep_history."""
+        A set restarts the multistep (SBDF) history unless keep_history.  With
+        wait=False the call returns once the copies are queued (TB_NO_WAIT): a
+        pinned source must stay unchanged until the plan's next wait (step,
+        get_states, wait); the next step queues behind the copies."""
         fields, arrs, fa, pa = self._field_arrays(arrays, False)
-        where = L.TB_HOST | (L.TB_KEEP_HISTORY if keep_history else 0)
+        where = L.TB_HOST | (L.TB_KEEP_HISTORY if keep_history else 0) | (0 if wait else L.TB_NO_WAIT)
         check(lib.tb_set_states(self.ptr, len(fields), fa, pa, where), self.ctx)
 
     def get_states(self, out: Dict[int, np.ndarray]) -> Dict[int, np.ndarray]:

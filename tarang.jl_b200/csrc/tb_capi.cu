@@ -1454,7 +1454,8 @@ namespace {
 // Copies of several 2D state fields on the plan's stream, one wait.  Fields
 // that are neighbours in the device state (b, u_x, u_z, p, then the taus, one
 // allocation) and whose caller buffers are neighbours too go as one copy.
-void copy_state_fields(tb_plan* P, int nfields, const int* fields, void* const* data, int where, bool to_device) {
+void copy_state_fields(tb_plan* P, int nfields, const int* fields, void* const* data, int where, bool to_device,
+                       bool wait = true) {
   TB_REQUIRE(P->ndim == 2, TB_ENOTSUPPORTED, "multi-field state I/O is for 2D plans (use the single-field call in 3D)");
   for (int i = 0; i < nfields; ++i) {
     TB_REQUIRE(fields[i] >= TB_FIELD_B && fields[i] <= TB_FIELD_TAU, TB_EINVAL, "bad field selector");
@@ -1479,7 +1480,7 @@ void copy_state_fields(tb_plan* P, int nfields, const int* fields, void* const* 
       TB_CUDA_TRY(cudaMemcpyAsync(h0, d0, bytes, kind, P->st));
     i = k;
   }
-  TB_CUDA_TRY(cudaStreamSynchronize(P->st));
+  if (wait) TB_CUDA_TRY(cudaStreamSynchronize(P->st));
 }
 }  // namespace
 
@@ -1487,16 +1488,16 @@ extern "C" {
 
 tb_status tb_set_states(tb_plan* P, int nfields, const int* fields, const void* const* data, int where) {
   if (!P || nfields < 0 || (nfields > 0 && (!fields || !data))) return TB_EINVAL;
-  const bool keep = (where & TB_KEEP_HISTORY) != 0;
-  where &= ~TB_KEEP_HISTORY;
+  const bool keep = (where & TB_KEEP_HISTORY) != 0, nowait = (where & TB_NO_WAIT) != 0;
+  where &= ~(TB_KEEP_HISTORY | TB_NO_WAIT);
   return guard(P->ctx, [&] {
-    copy_state_fields(P, nfields, fields, const_cast<void* const*>(data), where, true);
+    copy_state_fields(P, nfields, fields, const_cast<void* const*>(data), where, true, !nowait);
     if (!keep) P->ms_history = 0;  // a new state restarts multistep history
   });
 }
 
 tb_status tb_get_states(tb_plan* P, int nfields, const int* fields, void* const* data, int where) {
-  if (!P || nfields < 0 || (nfields > 0 && (!fields || !data))) return TB_EINVAL;
+  if (!P || nfields < 0 || (nfields > 0 && (!fields || !data)) || (where & TB_NO_WAIT)) return TB_EINVAL;
   return guard(P->ctx, [&] { copy_state_fields(P, nfields, fields, data, where, false); });
 }
 

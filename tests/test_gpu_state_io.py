@@ -108,9 +108,10 @@ def test_rk_step_does_not_read_p_or_taus(tb, scheme):
 
 
 def test_async_step_then_states_read_back_like_the_synchronous_step(tb):
-    # tb_set_states, tb_step_async, tb_get_states per step (the end-to-end
-    # bench's loop): the read-back copy queues behind the step on the plan's
-    # stream, so it sees the finished step, bitwise as after tb_step
+    # tb_set_states (TB_NO_WAIT), tb_step_async, tb_get_states per step (the
+    # end-to-end bench's loop): the step queues behind the upload and the
+    # read-back behind the step on the plan's stream, so the one wait sees
+    # the finished step, bitwise as after waiting copies and tb_step
     p = RBCParams(Nx=64, Nz=32, Lx=4.0, Lz=1.0, Ra=1e7)
     a, b = _plan(tb, p), _plan(tb, p)
     Nz, nk = p.Nz, p.Nx // 2 + 1
@@ -120,10 +121,16 @@ def test_async_step_then_states_read_back_like_the_synchronous_step(tb):
     a.get_states(views)
     for _ in range(3):
         step_in = {f: views[f].copy() for f in (0, 1, 2)}
-        a.set_states(step_in, keep_history=True)
+        a.set_states(step_in, keep_history=True, wait=False)
         a.step_async(0.01, 1)
         a.get_states(views)
         b.set_states(step_in, keep_history=True)
         b.step(0.01, 1)
         for f in FIELDS:
             assert np.array_equal(views[f], b.get_state(f)), f
+    # a read-back cannot skip its wait (the caller reads the data on return)
+    fields = (ctypes.c_int * 1)(0)
+    ptrs = (ctypes.c_void_p * 1)(views[0].ctypes.data)
+    before = views[0].copy()
+    assert tb.lib.tb_get_states(a.ptr, 1, fields, ptrs, tb._lib.TB_HOST | tb._lib.TB_NO_WAIT) == tb._lib.TB_EINVAL
+    assert np.array_equal(views[0], before)
